@@ -1,0 +1,318 @@
+"""Benchmark of the B200 CubismUP_2D timestep pipeline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload swimmer|cylinder]
+
+Workload (default): the self-propelled swimmer on a 1024x512 grid (32x16
+blocks of 32x32), StefanFish L=0.2, T=1 at (0.4, 0.25), nu = 2e-5
+(Re = (L/T) L / nu = 2000), free-space FFT Poisson, fp64 fields, from rest
+plus seeded 1e-6 uniform noise on u, v.  A step is one pass of
+Simulation::simulate's loop: calcMaxTimestep, PutObjectsOnGrid, advDiff,
+PressureSingle, ComputeForces.  The metric is cell-steps per second
+(Nx*Ny per completed step), reported in Gcell-steps/s.
+
+Timing: W warm-up steps, then K steps each bracketed by CUDA events on the
+library's stream; between timed steps the L2 is flushed by writing a 256 MB
+buffer (the working set, ~45 MB, would otherwise stay L2-resident).  Under
+torchrun each rank advances its own independent replica (the path does not
+shard: "replicas only") and rank 0 reports the max time over ranks.
+
+--impl reference times the reference's own C++ operators (compiled from its
+sources by oracle/Makefile into oracle/_ref) on the host cores, same workload
+and metric, rank 0 only.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "swimmer": ("swimmer_1024x512_fp64",
+                "-bpdx 32 -bpdy 16 -extent 1 -CFL 0.1 -nu 2e-5 -lambda 1e4 -poissonType freespace "
+                "-muteAll 1 -shapes 'stefanfish L=0.2 T=1 xpos=0.4 ypos=0.25'"),
+    "cylinder": ("forced_cylinder_re100_512x256_fp64",
+                 "-bpdx 16 -bpdy 8 -extent 1 -CFL 0.1 -nu 1.5e-4 -lambda 1e4 -poissonType freespace "
+                 "-muteAll 1 -shapes 'disk radius=0.0375 xpos=0.2 ypos=0.25 bForced=1 bFixed=1 xvel=0.2'"),
+}
+
+# fp64 bytes per cell that each dense kernel must move (reads + writes once)
+ALGO_BYTES_PER_CELL = {
+    "advdiff": 32,        # read u, v; write u, v
+    "rhs_div": 24,        # read u, v; write rhs
+    "pcorr": 40,          # read p, u, v; write u, v
+    "fft_rows_fwd": 24,   # read rhs (8); write half spectrum (16)
+    "fft_cols": 40,       # read spectrum (16) + G^ (8); write spectrum (16)
+    "fft_rows_inv": 24,   # read spectrum (16); write p (8)
+    "max_u": 16,          # read u, v
+}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[3 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(pg, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args, world, rank, pg):
+    """The reference's own operators (oracle/_ref) on the host cores."""
+    name, argline = WORKLOADS[args.workload]
+    if rank != 0:
+        return None
+    from oracle.refsim import RefSim
+    from cubismup_2d_b200.synthetic import noise_field
+    cores = os.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    r = RefSim(argline)
+    for comp, fname in enumerate(("u", "v")):
+        r.set(fname, r.get(fname) + noise_field(0, comp, r.ny, r.nx))
+    for _ in range(args.warmup):
+        r.step()
+    r.profile_reset()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r.step()
+    el = time.perf_counter() - t0
+    cells = r.nx * r.ny
+    val = cells * args.steps / el / 1e9
+    prof = r.profile()
+    line = {
+        "impl": "reference", "metric": "cell-steps/s", "value": val, "unit": "Gcell-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": name, "cells": cells},
+        "cpu_baseline": {"value": val, "unit": "Gcell-steps/s", "cores": cores, "kind": "reference",
+                         "sample": f"{args.steps} timed steps after {args.warmup} warm-up steps; "
+                                   "reference operators compiled from its sources with OpenMP; "
+                                   "FFT = project FFTW-API stand-in (FFTW absent)"},
+        "e2e": {"value": val, "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "stage_seconds": {k: round(v, 4) for k, v in prof.items()},
+    }
+    return line
+
+
+def cpu_baseline_sample(argline, nsteps=3):
+    from oracle.refsim import RefSim
+    from cubismup_2d_b200.synthetic import noise_field
+    r = RefSim(argline)
+    for comp, fname in enumerate(("u", "v")):
+        r.set(fname, r.get(fname) + noise_field(0, comp, r.ny, r.nx))
+    r.step()
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        r.step()
+    el = time.perf_counter() - t0
+    return r.nx * r.ny * nsteps / el / 1e9, os.cpu_count(), nsteps
+
+
+def run_ours(args, world, rank, local, pg):
+    import torch
+    from cubismup_2d_b200 import Simulation
+    from cubismup_2d_b200.synthetic import noise_field
+    name, argline = WORKLOADS[args.workload]
+    torch.cuda.set_device(local)
+    sim = Simulation(argline)
+    sim.cfg.device = local
+    sim.init()
+    ctx = sim.ctx
+    for comp, fname in enumerate(("u", "v")):
+        ctx.set(fname, ctx.get(fname) + noise_field(rank, comp, ctx.ny, ctx.nx))
+    cells = ctx.nx * ctx.ny
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    # warm-up (also captures the step graph)
+    ctx.advance(max(args.warmup, 3))
+    ctx.sync()
+
+    # timed region: K steps, each between CUDA events on the library's stream
+    # (cudaEvent records from the host are placed by the library's sync
+    # points; the stream is private, so events are recorded via the torch
+    # stream after a full sync of the library stream)
+    launches0 = ctx.kernel_launches()
+    step_ms = []
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)                 # evict L2 between timed steps
+            torch.cuda.synchronize()
+            ms = ctx.time_step()
+            step_ms.append(ms)
+        torch.cuda.synchronize()
+    launches = ctx.kernel_launches() - launches0
+    total_ms = float(np.sum(step_ms))
+    total_ms = max_over_ranks(pg, total_ms)
+    value = world * cells * args.steps / (total_ms / 1e3) / 1e9
+
+    # e2e: the reference's own loop through the C ABI with host transfers per
+    # step: dt read back (calcMaxTimestep prints it), dt passed to the four
+    # operators, shape state (forces) read back for the force log.
+    ne = max(20, args.steps // 5)
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(ne):
+        dt = sim.calcMaxTimestep()
+        for op in sim.pipeline:
+            op(dt)
+        ctx.end_step()
+        _ = ctx.shape(0)
+    ctx.sync()
+    e2e_s = max_over_ranks(pg, time.perf_counter() - t0)
+    e2e = world * cells * ne / e2e_s / 1e9
+
+    # roofline of the dominant dense kernel, timed live with CUDA events
+    peak, peak_kind = measured_peaks()
+    kt = {}
+    for kname in ("fft_cols", "advdiff", "pcorr", "fft_rows_fwd", "fft_rows_inv", "rhs_div", "max_u"):
+        kt[kname] = ctx.time_kernel(kname, 50)
+    dom = max(kt, key=kt.get)
+    achieved = ALGO_BYTES_PER_CELL[dom] * cells / (kt[dom] * 1e-3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            traffic = json.load(f).get(args.workload, {}).get(dom)
+    ctx.sync()
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            try:
+                v, cores, n = cpu_baseline_sample(argline, nsteps=args.cpu_steps)
+                cpu = {"value": v, "unit": "Gcell-steps/s", "cores": cores, "kind": "reference",
+                       "sample": f"{n} steps of the same workload after 1 warm-up step; reference "
+                                 "operators compiled from its sources (OpenMP, all host cores); "
+                                 "FFT = project FFTW-API stand-in (FFTW absent)"}
+            except Exception as e:  # noqa: BLE001
+                cpu = {"value": None, "unit": "Gcell-steps/s", "cores": os.cpu_count(), "kind": "reference",
+                       "sample": f"unavailable: {e}"}
+        line = {
+            "metric": "cell-steps/s", "value": value, "unit": "Gcell-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": name, "cells": cells, "parallelism": f"replicas{world}",
+                       "l2": "flushed between timed steps (256 MB write)"},
+            "clocks": clk.summary(),
+            "e2e": {"value": e2e, "unit": "Gcell-steps/s", "h2d_bytes_per_step": 8,
+                    "d2h_bytes_per_step": 8 + 42 * 8, "steps": ne},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic,
+                         "algorithmic_bytes_per_launch": ALGO_BYTES_PER_CELL[dom] * cells},
+            "kernel_ms": {k: round(v, 5) for k, v in kt.items()},
+            "cpu_baseline": cpu,
+        }
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="swimmer", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-steps", type=int, default=6)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local, pg = dist_setup()
+    if args.impl == "reference":
+        # each step of the reference at 1024x512 takes ~1 s on 8 cores: bound the sample
+        args.steps = min(args.steps, 20)
+        args.warmup = min(args.warmup, 3)
+        line = run_reference(args, world, rank, pg)
+    else:
+        line = run_ours(args, world, rank, local, pg)
+    if rank == 0 and line is not None:
+        print(json.dumps(line))
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,385 @@
+"""ctypes binding of libcup2d.so (include/cup2d.h) and a host-side mirror of
+the reference's Simulation / Operator interface.
+
+The reference drives its pipeline from C++ (Simulation.cpp:175-305); the
+mirror below accepts the same command-line arguments (Simulation.cpp:66-104)
+and shape descriptors (Simulation.cpp:106-173) and exposes the same calls:
+``init()``, ``calcMaxTimestep()``, ``advance(dt)``, ``simulate()`` and the
+four pipeline operators with ``operator()(dt)`` / ``getName()``.
+
+There is no CPU fallback: if the CUDA library is missing or no GPU is
+visible, creating a context raises.
+"""
+import ctypes
+import os
+import shlex
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcup2d.so")
+
+OK, EINVAL, ECUDA, ENAN, EDOMAIN, ECAPACITY, ENOTSUP, ESTATE, ENOMEM = range(9)
+ERRORS = {EINVAL: "EINVAL", ECUDA: "ECUDA", ENAN: "ENAN", EDOMAIN: "EDOMAIN",
+          ECAPACITY: "ECAPACITY", ENOTSUP: "ENOTSUP", ESTATE: "ESTATE", ENOMEM: "ENOMEM"}
+POISSON = {"freespace": 0, "periodic": 1, "": 2, "cosine": 2}
+PREC_FP64, PREC_FP32 = 0, 1
+FIELDS = {"u": 0, "v": 1, "chi": 2, "pres": 3, "tmp": 4, "udef_x": 5, "udef_y": 6, "sdf": 7}
+SHAPE_KINDS = {"disk": 0, "stefanfish": 1, "carlingfish": 2}
+
+# the exported entry points, in include/cup2d.h order
+EXPORTS = [
+    "cup2d_config_default", "cup2d_create", "cup2d_destroy", "cup2d_last_error",
+    "cup2d_shape_params_default", "cup2d_add_shape", "cup2d_init", "cup2d_calc_dt",
+    "cup2d_put_objects", "cup2d_adv_diff", "cup2d_pressure_single", "cup2d_compute_forces",
+    "cup2d_end_step", "cup2d_advance", "cup2d_sync", "cup2d_get_field", "cup2d_set_field",
+    "cup2d_get_shape", "cup2d_set_shape", "cup2d_get_scalars", "cup2d_set_scalars",
+    "cup2d_grid_size", "cup2d_kernel_launches", "cup2d_time_kernel", "cup2d_advance_timed",
+]
+KERNELS = {"advdiff": 0, "rhs_div": 1, "pcorr": 2, "fft_rows_fwd": 3, "fft_cols": 4,
+           "fft_rows_inv": 5, "max_u": 6, "objects": 7}
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("bpdx", ctypes.c_int), ("bpdy", ctypes.c_int), ("extent", ctypes.c_double),
+                ("CFL", ctypes.c_double), ("lambda_", ctypes.c_double), ("dlm", ctypes.c_double),
+                ("nu", ctypes.c_double), ("fadeLen", ctypes.c_double), ("nsteps", ctypes.c_int),
+                ("tend", ctypes.c_double), ("poisson", ctypes.c_int), ("precision", ctypes.c_int),
+                ("device", ctypes.c_int)]
+
+
+class ShapeParams(ctypes.Structure):
+    _fields_ = [("xpos", ctypes.c_double), ("ypos", ctypes.c_double), ("angle", ctypes.c_double),
+                ("rhoS", ctypes.c_double), ("bFixed", ctypes.c_int), ("bFixedx", ctypes.c_int),
+                ("bFixedy", ctypes.c_int), ("bForced", ctypes.c_int), ("bForcedx", ctypes.c_int),
+                ("bForcedy", ctypes.c_int), ("bBlockAng", ctypes.c_int), ("xvel", ctypes.c_double),
+                ("yvel", ctypes.c_double), ("angvel", ctypes.c_double), ("timeForced", ctypes.c_double),
+                ("radius", ctypes.c_double), ("tAccel", ctypes.c_double), ("L", ctypes.c_double),
+                ("T", ctypes.c_double), ("phi", ctypes.c_double), ("amplitudeFactor", ctypes.c_double)]
+
+
+SHAPE_STATE_FIELDS = [
+    "center_x", "center_y", "com_x", "com_y", "orientation", "u", "v", "omega",
+    "M", "J", "d_gm_x", "d_gm_y", "lab_com_x", "lab_com_y",
+    "penalM", "penalJ", "penalDX", "penalDY", "fluidMomX", "fluidMomY", "fluidAngMom",
+    "perimeter", "forcex", "forcey", "forcex_P", "forcey_P", "forcex_V", "forcey_V",
+    "torque", "torque_P", "torque_V", "drag", "thrust", "circulation",
+    "Pout", "PoutBnd", "defPower", "defPowerBnd", "Pthrust", "Pdrag", "EffPDef", "EffPDefBnd",
+]
+
+
+class ShapeState(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in SHAPE_STATE_FIELDS]
+
+
+_lib = None
+
+
+def lib():
+    """Load libcup2d.so (building it first if this tree has nvcc and no .so)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build as _build
+        _build.build()
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    L.cup2d_config_default.argtypes = [ctypes.POINTER(Config)]
+    L.cup2d_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(vp)]
+    L.cup2d_destroy.argtypes = [vp]
+    L.cup2d_last_error.argtypes = [vp]
+    L.cup2d_last_error.restype = ctypes.c_char_p
+    L.cup2d_shape_params_default.argtypes = [ctypes.POINTER(ShapeParams)]
+    L.cup2d_add_shape.argtypes = [vp, i, ctypes.POINTER(ShapeParams), ip]
+    L.cup2d_init.argtypes = [vp]
+    L.cup2d_calc_dt.argtypes = [vp, dp]
+    for name in ("cup2d_put_objects", "cup2d_adv_diff", "cup2d_pressure_single", "cup2d_compute_forces"):
+        getattr(L, name).argtypes = [vp, d]
+    L.cup2d_end_step.argtypes = [vp]
+    L.cup2d_advance.argtypes = [vp, i]
+    L.cup2d_sync.argtypes = [vp]
+    L.cup2d_get_field.argtypes = [vp, i, dp]
+    L.cup2d_set_field.argtypes = [vp, i, dp]
+    L.cup2d_get_shape.argtypes = [vp, i, ctypes.POINTER(ShapeState)]
+    L.cup2d_set_shape.argtypes = [vp, i, ctypes.POINTER(ShapeState)]
+    L.cup2d_get_scalars.argtypes = [vp, dp, dp, ip, dp, dp]
+    L.cup2d_set_scalars.argtypes = [vp, d, d, i, d, d]
+    L.cup2d_grid_size.argtypes = [vp, ip, ip, dp]
+    L.cup2d_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.cup2d_time_kernel.argtypes = [vp, i, i, dp]
+    L.cup2d_advance_timed.argtypes = [vp, i, dp]
+    for name in EXPORTS:
+        if name != "cup2d_last_error":
+            getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+class Cup2DError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def parse_args(argline):
+    """Simulation::parseRuntime / createShapes restated for the Python mirror.
+
+    Returns (Config, [(kind, ShapeParams)]).  Keys are taken with or without
+    their leading '-'; -bpdx/-bpdy are required (strict mode, Simulation.cpp:72-75).
+    """
+    toks = shlex.split(argline)
+    args = {}
+    k = 0
+    while k < len(toks):
+        t = toks[k]
+        if t.startswith("-") and len(t) > 1 and not (t[1].isdigit() or t[1] == "."):
+            vals = []
+            k += 1
+            while k < len(toks) and not (toks[k].startswith("-") and len(toks[k]) > 1 and
+                                         not (toks[k][1].isdigit() or toks[k][1] == ".")):
+                vals.append(toks[k]); k += 1
+            args[t[1:]] = " ".join(vals)
+        else:
+            k += 1
+    cfg = Config()
+    lib().cup2d_config_default(ctypes.byref(cfg))
+    if "bpdx" not in args or "bpdy" not in args:
+        raise Cup2DError(EINVAL, "runtime arguments -bpdx and -bpdy are required")
+    cfg.bpdx = int(args["bpdx"]); cfg.bpdy = int(args["bpdy"])
+    cfg.extent = float(args.get("extent", 1))
+    cfg.nsteps = int(args.get("nsteps", 0))
+    cfg.tend = float(args.get("tend", 0))
+    cfg.CFL = float(args.get("CFL", 0.1))
+    cfg.lambda_ = float(args.get("lambda", 1e3 / cfg.CFL))
+    cfg.dlm = float(args.get("dlm", 0))
+    cfg.nu = float(args.get("nu", 1e-2))
+    cfg.fadeLen = float(args.get("fadeLen", 0.01))
+    ptype = args.get("poissonType", "")
+    if ptype not in POISSON:
+        raise Cup2DError(ENOTSUP, f"poissonType {ptype!r} is not available")
+    cfg.poisson = POISSON[ptype]
+    cfg.precision = {"fp64": PREC_FP64, "fp32": PREC_FP32}[args.get("precision", "fp64")]
+    shapes = []
+    for lines in args.get("shapes", "").split("\n"):
+        lines = lines.replace("_", " ")
+        for line in lines.split(","):
+            parts = line.split()
+            if not parts or parts[0].startswith("#"):
+                continue
+            name = parts[0]
+            if name not in SHAPE_KINDS:
+                raise Cup2DError(ENOTSUP, f"shape {name!r} is not available")
+            kv = {}
+            for p in parts[1:]:
+                if "=" in p:
+                    key, val = p.split("=", 1)
+                    kv[key.strip().lstrip("-")] = val.strip()
+            sp = ShapeParams()
+            lib().cup2d_shape_params_default(ctypes.byref(sp))
+            fl = {"xpos": "xpos", "ypos": "ypos", "angle": "angle", "rhoS": "rhoS", "xvel": "xvel",
+                  "yvel": "yvel", "angvel": "angvel", "timeForced": "timeForced", "radius": "radius",
+                  "tAccel": "tAccel", "L": "L", "T": "T", "phi": "phi",
+                  "amplitudeFactor": "amplitudeFactor"}
+            for key, field in fl.items():
+                if key in kv:
+                    setattr(sp, field, float(kv[key]))
+            for key in ("bFixed", "bFixedx", "bFixedy", "bForced", "bForcedx", "bForcedy", "bBlockAng"):
+                if key in kv:
+                    v = kv[key]
+                    setattr(sp, key, 1 if v in ("1", "true", "True") else (0 if v in ("0", "false", "False") else int(v) != 0))
+            for key in ("pid", "pidpos"):
+                if key in kv and int(kv[key]) != 0:
+                    raise Cup2DError(ENOTSUP, "the fish PID controllers are not available")
+            shapes.append((SHAPE_KINDS[name], sp))
+    return cfg, shapes
+
+
+class Context:
+    """One device context: grid, shapes and Poisson solver (SimulationData)."""
+
+    def __init__(self, cfg, shapes):
+        self.L = lib()
+        h = ctypes.c_void_p()
+        rc = self.L.cup2d_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != OK:
+            raise Cup2DError(rc, "cup2d_create failed")
+        self.h_ = h
+        self.cfg = cfg
+        for kind, sp in shapes:
+            sid = ctypes.c_int()
+            self._ck(self.L.cup2d_add_shape(self.h_, kind, ctypes.byref(sp), ctypes.byref(sid)))
+        nx, ny, hh = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        self.L.cup2d_grid_size(self.h_, ctypes.byref(nx), ctypes.byref(ny), ctypes.byref(hh))
+        self.nx, self.ny, self.h = nx.value, ny.value, hh.value
+        self.nshapes = len(shapes)
+
+    def _ck(self, rc):
+        if rc != OK:
+            raise Cup2DError(rc, self.L.cup2d_last_error(self.h_).decode())
+
+    def close(self):
+        if getattr(self, "h_", None):
+            self.L.cup2d_destroy(self.h_)
+            self.h_ = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init(self):
+        self._ck(self.L.cup2d_init(self.h_))
+
+    def calc_dt(self, sync=True):
+        if sync:
+            dt = ctypes.c_double()
+            self._ck(self.L.cup2d_calc_dt(self.h_, ctypes.byref(dt)))
+            return dt.value
+        self._ck(self.L.cup2d_calc_dt(self.h_, None))
+
+    def put_objects(self, dt=-1.0):
+        self._ck(self.L.cup2d_put_objects(self.h_, dt))
+
+    def adv_diff(self, dt=-1.0):
+        self._ck(self.L.cup2d_adv_diff(self.h_, dt))
+
+    def pressure_single(self, dt=-1.0):
+        self._ck(self.L.cup2d_pressure_single(self.h_, dt))
+
+    def compute_forces(self, dt=-1.0):
+        self._ck(self.L.cup2d_compute_forces(self.h_, dt))
+
+    def end_step(self):
+        self._ck(self.L.cup2d_end_step(self.h_))
+
+    def advance(self, nsteps=1):
+        self._ck(self.L.cup2d_advance(self.h_, nsteps))
+
+    def sync(self):
+        self._ck(self.L.cup2d_sync(self.h_))
+
+    def get(self, name):
+        a = np.empty((self.ny, self.nx), dtype=np.float64)
+        self._ck(self.L.cup2d_get_field(self.h_, FIELDS[name], _dp(a)))
+        return a
+
+    def set(self, name, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        assert a.shape == (self.ny, self.nx)
+        self._ck(self.L.cup2d_set_field(self.h_, FIELDS[name], _dp(a)))
+
+    def shape(self, k=0):
+        s = ShapeState()
+        self._ck(self.L.cup2d_get_shape(self.h_, k, ctypes.byref(s)))
+        return {n: getattr(s, n) for n in SHAPE_STATE_FIELDS}
+
+    def set_shape(self, k, state):
+        s = ShapeState()
+        self._ck(self.L.cup2d_get_shape(self.h_, k, ctypes.byref(s)))
+        for n, v in state.items():
+            setattr(s, n, v)
+        self._ck(self.L.cup2d_set_shape(self.h_, k, ctypes.byref(s)))
+
+    def scalars(self):
+        t, dt, ux, uy = ctypes.c_double(), ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        st = ctypes.c_int()
+        self._ck(self.L.cup2d_get_scalars(self.h_, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(st),
+                                          ctypes.byref(ux), ctypes.byref(uy)))
+        return {"time": t.value, "dt": dt.value, "step": st.value, "uinfx": ux.value, "uinfy": uy.value}
+
+    def set_scalars(self, time, dt, step, uinfx, uinfy):
+        self._ck(self.L.cup2d_set_scalars(self.h_, time, dt, step, uinfx, uinfy))
+
+    def time_step(self, nsteps=1):
+        """cup2d_advance between CUDA events on the library's stream (ms)."""
+        ms = ctypes.c_double()
+        self._ck(self.L.cup2d_advance_timed(self.h_, nsteps, ctypes.byref(ms)))
+        return ms.value
+
+    def time_kernel(self, name, reps):
+        ms = ctypes.c_double()
+        self._ck(self.L.cup2d_time_kernel(self.h_, KERNELS[name], reps, ctypes.byref(ms)))
+        return ms.value
+
+    def kernel_launches(self):
+        n = ctypes.c_longlong()
+        self._ck(self.L.cup2d_kernel_launches(self.h_, ctypes.byref(n)))
+        return n.value
+
+
+class Operator:
+    """Operator.h:14-27: one pipeline stage, called as op(dt)."""
+    name = ""
+    _fn = ""
+
+    def __init__(self, sim):
+        self.sim = sim
+
+    def __call__(self, dt):
+        getattr(self.sim.ctx, self._fn)(dt)
+
+    def getName(self):
+        return self.name
+
+
+class PutObjectsOnGrid(Operator):
+    name, _fn = "PutObjectsOnGrid", "put_objects"
+
+
+class advDiff(Operator):
+    name, _fn = "advDiff", "adv_diff"
+
+
+class PressureSingle(Operator):
+    name, _fn = "PressureSingle", "pressure_single"
+
+
+class ComputeForces(Operator):
+    name, _fn = "ComputeForces", "compute_forces"
+
+
+class Simulation:
+    """Simulation.h:19-40 on the device pipeline."""
+
+    def __init__(self, argline):
+        self.cfg, self.shape_params = parse_args(argline)
+        self.ctx = None
+        self.pipeline = []
+
+    def init(self):
+        self.ctx = Context(self.cfg, self.shape_params)
+        self.pipeline = [PutObjectsOnGrid(self), advDiff(self), PressureSingle(self), ComputeForces(self)]
+        self.ctx.init()
+
+    def calcMaxTimestep(self):
+        return self.ctx.calc_dt(sync=True)
+
+    def advance(self, dt):
+        for op in self.pipeline:
+            op(dt)
+        self.ctx.end_step()
+        st = self.ctx.scalars()
+        return self.bOver(st)
+
+    def bOver(self, st=None):  # SimulationData.cpp:172-177
+        st = st or self.ctx.scalars()
+        timeEnd = self.cfg.tend > 0 and st["time"] >= self.cfg.tend
+        stepEnd = self.cfg.nsteps > 0 and st["step"] > self.cfg.nsteps
+        return timeEnd or stepEnd
+
+    def simulate(self):
+        """Runs nsteps+1 steps as Simulation::simulate does, on the graph path."""
+        if self.cfg.nsteps <= 0:
+            raise Cup2DError(EINVAL, "simulate() needs -nsteps")
+        self.ctx.advance(self.cfg.nsteps + 1)
+        self.ctx.sync()
+
+    def getShapes(self):
+        return [self.ctx.shape(k) for k in range(self.ctx.nshapes)]

@@ -1,0 +1,608 @@
+// The C ABI (include/cup2d.h): context lifetime, shapes, the pipeline stages
+// in Simulation::advance order, CUDA-graph replay of whole steps, and state
+// exchange.  No entry point aborts: failures come back as status codes.
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+#include "context.hpp"
+#include "fish.cuh"
+
+using namespace cup2d;
+
+struct cup2d_ctx { Ctx c; };
+
+namespace {
+
+#define CK(call)                                                                \
+  do {                                                                          \
+    cudaError_t e_ = (call);                                                    \
+    if (e_ != cudaSuccess) {                                                    \
+      ctx->c.err = std::string(#call) + ": " + cudaGetErrorString(e_);          \
+      return CUP2D_ECUDA;                                                       \
+    }                                                                           \
+  } while (0)
+
+int fail(cup2d_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->c.err = msg;
+  return code;
+}
+
+int check_launch(cup2d_ctx* ctx) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(ctx, CUP2D_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return CUP2D_OK;
+}
+
+template <typename T>
+int dalloc(cup2d_ctx* ctx, T** p, size_t n) {
+  if (cudaMalloc((void**)p, sizeof(T) * (n ? n : 1)) != cudaSuccess)
+    return fail(ctx, CUP2D_ENOMEM, "cudaMalloc failed");
+  return CUP2D_OK;
+}
+
+// Natural cubic spline, IF2D_Interpolation1D::naturalCubicSpline
+// (FishUtilities.h:85-130): second derivatives by the tridiagonal sweep,
+// then bisection and the cubic in the bracketing interval.
+void natural_spline(const double* x, const double* y, int n, const double* xx, double* yy, int nn) {
+  std::vector<double> y2(n), u(n > 1 ? n - 1 : 1);
+  y2[0] = 0; u[0] = 0;
+  for (int i = 1; i < n - 1; i++) {
+    const double sig = (x[i] - x[i - 1]) / (x[i + 1] - x[i - 1]);
+    const double p = sig * y2[i - 1] + 2;
+    y2[i] = (sig - 1) / p;
+    u[i] = (y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1]);
+    u[i] = (6 * u[i] / (x[i + 1] - x[i - 1]) - sig * u[i - 1]) / p;
+  }
+  const double qn = 0, un = 0;
+  y2[n - 1] = (un - qn * u[n - 2]) / (qn * y2[n - 2] + 1);
+  for (int k = n - 2; k > 0; k--) y2[k] = y2[k] * y2[k + 1] + u[k];
+  for (int j = 0; j < nn; j++) {
+    unsigned klo = 0, khi = n - 1, k = 0;
+    while (khi - klo > 1) {
+      k = (khi + klo) >> 1;
+      if (x[k] > (xx[j] + 0)) khi = k; else klo = k;
+    }
+    const double h = x[khi] - x[klo];
+    const double a = (x[khi] - (xx[j] + 0)) / h;
+    const double b = ((xx[j] + 0) - x[klo]) / h;
+    yy[j] = a * y[klo] + b * y[khi] + ((a * a * a - a) * y2[klo] + (b * b * b - b) * y2[khi]) * (h * h) / 6;
+  }
+}
+
+// FishData arclength grid (FishLibrary.cpp:14-38, FishLibrary.h:62-74) and
+// the width profile of CurvatureFish/AmplitudeFish (StefanFish.cpp:175-182).
+bool fish_grid(double L, double h, std::vector<double>& rS, std::vector<double>& width) {
+  const double fracRefined = 0.1, fracMid = 1 - 2 * fracRefined;
+  const double dSmid_tgt = h / std::sqrt(2);
+  const double dSrefine_tgt = 0.125 * h;
+  const int Nmid = (int)std::ceil(L * fracMid / dSmid_tgt / 8) * 8;
+  const double dSmid = L * fracMid / Nmid;
+  const int Nend = (int)std::ceil(fracRefined * L * 2 / (dSmid + dSrefine_tgt) / 4) * 4;
+  const double dSref = fracRefined * L * 2 / Nend - dSmid;
+  const int Nm = Nmid + 2 * Nend + 1;
+  if (!(dSref > 0)) return false;       // FishLibrary.cpp:21 assert(dSref > 0)
+  rS.assign(Nm, 0.0);
+  int k = 0;
+  for (int i = 0; i < Nend; ++i, k++) rS[k + 1] = rS[k] + dSref + (dSmid - dSref) * i / ((double)Nend - 1.);
+  for (int i = 0; i < Nmid; ++i, k++) rS[k + 1] = rS[k] + dSmid;
+  for (int i = 0; i < Nend; ++i, k++)
+    rS[k + 1] = rS[k] + dSref + (dSmid - dSref) * (Nend - i - 1) / ((double)Nend - 1.);
+  rS[k] = std::min(rS[k], L);
+  width.assign(Nm, 0.0);
+  for (int i = 0; i < Nm; i++) {
+    const double s = rS[i];
+    const double sb = .04 * L, st = .95 * L, wt = .01 * L, wh = .04 * L;
+    double w;
+    if (s < 0 or s > L) w = 0;
+    else w = (s < sb ? std::sqrt(2 * wh * s - s * s) : (s < st ? wh - (wh - wt) * ((s - sb) / (st - sb)) : (wt * (L - s) / (L - st))));
+    width[i] = w;
+  }
+  return true;
+}
+
+int upload_shapes(cup2d_ctx* ctx) {
+  Ctx& c = ctx->c;
+  if (c.nshapes == 0) return CUP2D_OK;
+  CK(cudaMemcpyAsync(c.dshapes, c.hshapes.data(), sizeof(DevShape) * c.nshapes, cudaMemcpyHostToDevice, c.stream));
+  return CUP2D_OK;
+}
+
+int upload_scalars_reset(cup2d_ctx* ctx) {
+  Ctx& c = ctx->c;
+  Scalars s{};
+  s.time = 0; s.dt = 0; s.uinfx = 0; s.uinfy = 0; s.lambda = c.cfg.lambda;
+  s.step = 0; s.status = 0;
+  for (int i = 0; i < 100; i++) {        // Simulation.cpp:266-267, evaluated with the host libm
+    const double x = (i + 1.0) / 100;
+    s.rampCFL[i] = std::exp(std::log(1e-3) * (1 - x) + std::log(c.cfg.CFL) * x);
+  }
+  CK(cudaMemcpyAsync(c.dsc, &s, sizeof(Scalars), cudaMemcpyHostToDevice, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  return CUP2D_OK;
+}
+
+void invalidate_graph(Ctx& c) {
+  if (c.graph) { cudaGraphExecDestroy(c.graph); c.graph = nullptr; }
+}
+
+// one pass of Simulation::simulate's loop body (Simulation.cpp:245-251)
+void enqueue_step(Ctx& c) {
+  launch_max_u_dt(c);
+  launch_objects(c);
+  launch_advdiff(c);
+  launch_outflow(c);
+  launch_rhs_div(c);
+  launch_rhs_obstacles(c);
+  launch_fade_sums(c);
+  poisson_solve(c);
+  launch_pcorr(c);
+  launch_momenta_penalize(c);
+  launch_forces(c);
+  launch_end_step(c);
+}
+
+} // namespace
+
+extern "C" {
+
+int cup2d_config_default(cup2d_config* cfg) {
+  if (!cfg) return CUP2D_EINVAL;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->bpdx = 0; cfg->bpdy = 0;
+  cfg->extent = 1;
+  cfg->CFL = 0.1;
+  cfg->lambda = 1e3 / cfg->CFL;
+  cfg->dlm = 0;
+  cfg->nu = 1e-2;
+  cfg->fadeLen = 0.01;
+  cfg->nsteps = 0; cfg->tend = 0;
+  cfg->poisson = CUP2D_POISSON_COSINE;   // -poissonType "" selects FFTW_dirichlet
+  cfg->precision = CUP2D_PREC_FP64;
+  cfg->device = 0;
+  return CUP2D_OK;
+}
+
+const char* cup2d_last_error(const cup2d_ctx* ctx) {
+  return ctx ? ctx->c.err.c_str() : "null context";
+}
+
+int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
+  if (!cfg || !out) return CUP2D_EINVAL;
+  *out = nullptr;
+  if (cfg->bpdx <= 0 || cfg->bpdy <= 0) return CUP2D_EINVAL;
+  if (cfg->precision != CUP2D_PREC_FP64) return CUP2D_ENOTSUP;
+  cup2d_ctx* ctx = new (std::nothrow) cup2d_ctx();
+  if (!ctx) return CUP2D_ENOMEM;
+  Ctx& c = ctx->c;
+  c.cfg = *cfg;
+  c.device = cfg->device;
+  if (cudaSetDevice(c.device) != cudaSuccess) { delete ctx; return CUP2D_ECUDA; }
+  if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return CUP2D_ECUDA; }
+  GridDesc& g = c.g;
+  g.bpdx = cfg->bpdx; g.bpdy = cfg->bpdy;
+  g.nx = BS * g.bpdx; g.ny = BS * g.bpdy; g.nblocks = g.bpdx * g.bpdy;
+  g.extent = cfg->extent;
+  g.h = cfg->extent / std::max(g.bpdx * BS, g.bpdy * BS);     // Cubism Grid spacing
+  g.ext[0] = g.bpdx * g.h * BS;                                // SimulationData.cpp:34-35
+  g.ext[1] = g.bpdy * g.h * BS;
+  g.nu = cfg->nu; g.CFL = cfg->CFL; g.dlm = cfg->dlm;
+  g.fadeLenX = cfg->fadeLen * cfg->extent;                     // Simulation.cpp:97-98
+  g.fadeLenY = cfg->fadeLen * cfg->extent;
+  const size_t n = c.ncells();
+  int rc = CUP2D_OK;
+  for (int b = 0; b < 2 && !rc; b++)
+    for (int d = 0; d < 2 && !rc; d++) rc = dalloc(ctx, &c.vel[b][d], n);
+  if (!rc) rc = dalloc(ctx, &c.chi, n);
+  if (!rc) rc = dalloc(ctx, &c.pres, n);
+  if (!rc) rc = dalloc(ctx, &c.rhs, n);
+  if (!rc) rc = dalloc(ctx, &c.sdf, n);
+  if (!rc) rc = dalloc(ctx, &c.udefx, n);
+  if (!rc) rc = dalloc(ctx, &c.udefy, n);
+  if (!rc) rc = dalloc(ctx, &c.dsc, 1);
+  if (!rc) rc = dalloc(ctx, &c.dshapes, MAX_SHAPES);
+  if (!rc) rc = dalloc(ctx, &c.counters, Ctx::NCOUNTERS);
+  if (rc) { cup2d_destroy(ctx); return rc; }
+  if (cudaMemset(c.counters, 0, sizeof(unsigned) * Ctx::NCOUNTERS) != cudaSuccess) { cup2d_destroy(ctx); return CUP2D_ECUDA; }
+  c.poisson = poisson_create(c);
+  if (!c.poisson) { cup2d_destroy(ctx); return CUP2D_ENOTSUP; }
+  if (cudaStreamSynchronize(c.stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+    cup2d_destroy(ctx); return CUP2D_ECUDA;
+  }
+  *out = ctx;
+  return CUP2D_OK;
+}
+
+int cup2d_destroy(cup2d_ctx* ctx) {
+  if (!ctx) return CUP2D_OK;
+  Ctx& c = ctx->c;
+  if (c.stream) cudaStreamSynchronize(c.stream);
+  invalidate_graph(c);
+  for (int b = 0; b < 2; b++) for (int d = 0; d < 2; d++) cudaFree(c.vel[b][d]);
+  cudaFree(c.chi); cudaFree(c.pres); cudaFree(c.rhs); cudaFree(c.sdf);
+  cudaFree(c.udefx); cudaFree(c.udefy); cudaFree(c.dsc); cudaFree(c.dshapes);
+  cudaFree(c.counters); cudaFree(c.partials);
+  for (auto& t : c.tiles) {
+    cudaFree(t.tiles); cudaFree(t.slot); cudaFree(t.chi); cudaFree(t.dist); cudaFree(t.udx);
+    cudaFree(t.udy); cudaFree(t.sD); cudaFree(t.sdx); cudaFree(t.sdy);
+  }
+  for (auto& f : c.fish) {
+    cudaFree(f.rS); cudaFree(f.rX); cudaFree(f.rY); cudaFree(f.vX); cudaFree(f.vY);
+    cudaFree(f.norX); cudaFree(f.norY); cudaFree(f.vNorX); cudaFree(f.vNorY); cudaFree(f.width);
+    cudaFree(f.rK); cudaFree(f.vK); cudaFree(f.p1f); cudaFree(f.seg);
+  }
+  poisson_destroy(c.poisson);
+  if (c.stream) cudaStreamDestroy(c.stream);
+  delete ctx;
+  return CUP2D_OK;
+}
+
+int cup2d_shape_params_default(cup2d_shape_params* p) {
+  if (!p) return CUP2D_EINVAL;
+  std::memset(p, 0, sizeof(*p));
+  p->xpos = -1; p->ypos = -1;     // -1: centre of the domain (Simulation.cpp:132-135)
+  p->angle = 0; p->rhoS = 1;
+  p->bFixed = 0; p->bFixedx = -1; p->bFixedy = -1;
+  p->bForced = 0; p->bForcedx = -1; p->bForcedy = -1; p->bBlockAng = -1;
+  p->xvel = 0; p->yvel = 0; p->angvel = 0;
+  p->timeForced = DBL_MAX;
+  p->radius = 0.1; p->tAccel = -1;
+  p->L = 0.1; p->T = 1; p->phi = 0; p->amplitudeFactor = 1;
+  return CUP2D_OK;
+}
+
+int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* id) {
+  if (!ctx || !p) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  if (c.initialised) return fail(ctx, CUP2D_ESTATE, "shapes must be added before cup2d_init");
+  if (c.nshapes >= MAX_SHAPES) return fail(ctx, CUP2D_EINVAL, "too many shapes");
+  if (kind != CUP2D_SHAPE_DISK && kind != CUP2D_SHAPE_STEFANFISH && kind != CUP2D_SHAPE_CARLINGFISH)
+    return fail(ctx, CUP2D_ENOTSUP, "unknown shape kind");
+  if (std::fabs(p->rhoS - 1.0) > DBL_EPSILON)
+    return fail(ctx, CUP2D_ENOTSUP, "rhoS != 1 selects the variable-density pipeline (Simulation.cpp:185-204)");
+  DevShape S{};
+  ShapeCfg& f = S.cfg;
+  f.kind = kind;
+  f.rhoS = p->rhoS;
+  const int bFixed = p->bFixed != 0, bForced = p->bForced != 0;
+  f.bFixedx = p->bFixedx < 0 ? bFixed : p->bFixedx != 0;      // Shape.cpp:335-341
+  f.bFixedy = p->bFixedy < 0 ? bFixed : p->bFixedy != 0;
+  f.bForcedx = p->bForcedx < 0 ? bForced : p->bForcedx != 0;
+  f.bForcedy = p->bForcedy < 0 ? bForced : p->bForcedy != 0;
+  f.bBlockang = p->bBlockAng < 0 ? (f.bForcedx || f.bForcedy) : p->bBlockAng != 0;
+  f.forcedu = -p->xvel; f.forcedv = -p->yvel; f.forcedomega = -p->angvel;
+  f.timeForced = p->timeForced;
+  f.origC[0] = p->xpos < 0 ? .5 * c.g.ext[0] : p->xpos;
+  f.origC[1] = p->ypos < 0 ? .5 * c.g.ext[1] : p->ypos;
+  f.origAng = p->angle * M_PI / 180;
+  f.radius = p->radius; f.tAccel = p->tAccel;
+  f.length = p->L; f.Tperiod = p->T; f.phaseShift = p->phi; f.ampFac = p->amplitudeFactor;
+  const double h = c.g.h;
+  double span;
+  if (kind == CUP2D_SHAPE_DISK) span = 2 * (f.radius + 2 * h);
+  else span = 2 * (1.2 * f.length + 8 * h);
+  int nb1 = (int)std::ceil(span / (BS * h)) + 2;
+  int cap = nb1 * nb1;
+  if (cap > c.g.nblocks) cap = c.g.nblocks;
+  f.capacity = cap;
+  S.rhoTile = kind == CUP2D_SHAPE_DISK ? f.rhoS : 1.0;
+  ObstTiles t{};
+  t.capacity = cap;
+  int rc = dalloc(ctx, &t.tiles, cap);
+  if (!rc) rc = dalloc(ctx, &t.slot, c.g.nblocks);
+  double** arrs[] = {&t.chi, &t.dist, &t.udx, &t.udy, &t.sD, &t.sdx, &t.sdy};
+  for (auto a : arrs) if (!rc) rc = dalloc(ctx, a, (size_t)cap * BS2);
+  if (rc) return rc;
+  CK(cudaMemset(t.slot, 0xff, sizeof(int) * c.g.nblocks));
+  FishArrays F{};
+  if (kind != CUP2D_SHAPE_DISK) {
+    std::vector<double> rS, width;
+    if (!fish_grid(f.length, h, rS, width))
+      return fail(ctx, CUP2D_EINVAL, "fish midline spacing degenerate at this resolution (dSref <= 0, FishLibrary.cpp:21)");
+    const int Nm = (int)rS.size();
+    f.nm = Nm;
+    F.nm = Nm; F.nseg = (Nm - 1) / 8;
+    double** fa[] = {&F.rS, &F.rX, &F.rY, &F.vX, &F.vY, &F.norX, &F.norY, &F.vNorX, &F.vNorY,
+                     &F.width, &F.rK, &F.vK, &F.p1f};
+    for (auto a : fa) if (!rc) rc = dalloc(ctx, a, Nm);
+    if (!rc) rc = dalloc(ctx, &F.seg, F.nseg);
+    if (rc) return rc;
+    // curvature control values, StefanFish.cpp:187-193, splined onto rS
+    const double L = f.length;
+    const double pts[6] = {0, .15 * L, .4 * L, .65 * L, .9 * L, L};
+    const double vals[6] = {0.82014 / L, 1.46515 / L, 2.57136 / L, 3.75425 / L, 5.09147 / L, 5.70449 / L};
+    std::vector<double> p1f(Nm);
+    natural_spline(pts, vals, 6, rS.data(), p1f.data(), Nm);
+    CK(cudaMemcpy(F.rS, rS.data(), sizeof(double) * Nm, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(F.width, width.data(), sizeof(double) * Nm, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(F.p1f, p1f.data(), sizeof(double) * Nm, cudaMemcpyHostToDevice));
+  }
+  c.hshapes.push_back(S);
+  c.tiles.push_back(t);
+  c.fish.push_back(F);
+  if (id) *id = c.nshapes;
+  c.nshapes++;
+  if (cap > c.maxCapacity) c.maxCapacity = cap;
+  return CUP2D_OK;
+}
+
+int cup2d_init(cup2d_ctx* ctx) {
+  if (!ctx) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  if (c.nshapes == 0) return fail(ctx, CUP2D_EINVAL, "no shapes (Simulation.cpp:167-169)");
+  invalidate_graph(c);
+  // reduction scratch: dense region + per-shape tile regions
+  cudaFree(c.partials);
+  c.npartials = (size_t)3 * c.g.nblocks + 4096 + (size_t)MAX_SHAPES * c.maxCapacity * 24;
+  int rc = dalloc(ctx, &c.partials, c.npartials);
+  if (rc) return rc;
+  c.cur = 0;
+  // Simulation::reset (Simulation.cpp:232-241): resetAll, IC, objects at t=0, ApplyObjVel
+  if ((rc = upload_scalars_reset(ctx))) return rc;
+  for (int k = 0; k < c.nshapes; k++) {
+    DevShape& S = c.hshapes[k];
+    const ShapeCfg& f = S.cfg;
+    std::memset(&S.s, 0, sizeof(S.s));
+    std::memset(&S.f, 0, sizeof(S.f));
+    S.s.center[0] = S.s.com[0] = f.origC[0];
+    S.s.center[1] = S.s.com[1] = f.origC[1];
+    S.s.orientation = f.origAng;
+    S.s.u = f.forcedu; S.s.v = f.forcedv; S.s.omega = f.forcedomega;
+    S.ntiles = 0; S.ntilesPrev = 0;
+    CK(cudaMemsetAsync(c.tiles[k].slot, 0xff, sizeof(int) * c.g.nblocks, c.stream));
+  }
+  if ((rc = upload_shapes(ctx))) return rc;
+  launch_ic(c);
+  launch_set_dt(c, 0.0);
+  launch_objects(c);
+  launch_obj_vel_on_grid(c);
+  launch_apply_obj_vel(c);
+  CK(cudaStreamSynchronize(c.stream));
+  if ((rc = check_launch(ctx))) return rc;
+  c.initialised = true;
+  return CUP2D_OK;
+}
+
+int cup2d_calc_dt(cup2d_ctx* ctx, double* dt_out) {
+  if (!ctx || !ctx->c.initialised) return ctx ? fail(ctx, CUP2D_ESTATE, "not initialised") : CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  launch_max_u_dt(c);
+  int rc = check_launch(ctx);
+  if (rc) return rc;
+  if (dt_out) {
+    CK(cudaMemcpyAsync(dt_out, &c.dsc->dt, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+  }
+  return CUP2D_OK;
+}
+
+#define STAGE_PROLOGUE                                                           \
+  if (!ctx) return CUP2D_EINVAL;                                                 \
+  Ctx& c = ctx->c;                                                               \
+  if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");         \
+  if (dt >= 0) launch_set_dt(c, dt);
+
+int cup2d_put_objects(cup2d_ctx* ctx, double dt) {
+  STAGE_PROLOGUE
+  launch_objects(c);
+  return check_launch(ctx);
+}
+
+int cup2d_adv_diff(cup2d_ctx* ctx, double dt) {
+  STAGE_PROLOGUE
+  launch_advdiff(c);
+  launch_outflow(c);
+  return check_launch(ctx);
+}
+
+int cup2d_pressure_single(cup2d_ctx* ctx, double dt) {
+  STAGE_PROLOGUE
+  launch_rhs_div(c);
+  launch_rhs_obstacles(c);
+  launch_fade_sums(c);
+  poisson_solve(c);
+  launch_pcorr(c);
+  launch_momenta_penalize(c);
+  return check_launch(ctx);
+}
+
+int cup2d_compute_forces(cup2d_ctx* ctx, double dt) {
+  STAGE_PROLOGUE
+  launch_forces(c);
+  return check_launch(ctx);
+}
+
+int cup2d_end_step(cup2d_ctx* ctx) {
+  if (!ctx) return CUP2D_EINVAL;
+  launch_end_step(ctx->c);
+  return check_launch(ctx);
+}
+
+int cup2d_advance(cup2d_ctx* ctx, int nsteps) {
+  if (!ctx) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
+  if (nsteps <= 0) return CUP2D_OK;
+  if (c.cur != 0) {
+    // a stage was called on its own: finish in eager mode until parity returns
+    return fail(ctx, CUP2D_ESTATE, "velocity buffers out of step order");
+  }
+  if (!c.graph) {
+    const long long before = c.launches;
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(c);
+    const cudaError_t e = cudaStreamEndCapture(c.stream, &graph);
+    if (e != cudaSuccess) return fail(ctx, CUP2D_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    c.launchesInGraph = (int)(c.launches - before);
+    c.launches = before;
+    const cudaError_t e2 = cudaGraphInstantiate(&c.graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e2 != cudaSuccess) { c.graph = nullptr; return fail(ctx, CUP2D_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e2)); }
+  }
+  for (int s = 0; s < nsteps; s++) {
+    CK(cudaGraphLaunch(c.graph, c.stream));
+    c.launches += c.launchesInGraph;
+  }
+  return CUP2D_OK;
+}
+
+int cup2d_sync(cup2d_ctx* ctx) {
+  if (!ctx) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  CK(cudaStreamSynchronize(c.stream));
+  int rc = check_launch(ctx);
+  if (rc) return rc;
+  int status = 0;
+  CK(cudaMemcpy(&status, &c.dsc->status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (status & ST_NAN) return fail(ctx, CUP2D_ENAN, "non-finite velocity detected");
+  if (status & ST_DOMAIN) return fail(ctx, CUP2D_EDOMAIN, "body out of domain");
+  if (status & ST_CAPACITY) return fail(ctx, CUP2D_ECAPACITY, "obstacle tiles exceed capacity");
+  return CUP2D_OK;
+}
+
+static double* field_ptr(Ctx& c, int which) {
+  switch (which) {
+    case CUP2D_FIELD_U: return c.u();
+    case CUP2D_FIELD_V: return c.v();
+    case CUP2D_FIELD_CHI: return c.chi;
+    case CUP2D_FIELD_PRES: return c.pres;
+    case CUP2D_FIELD_TMP: return c.rhs;
+    case CUP2D_FIELD_UDEF_X: return c.udefx;
+    case CUP2D_FIELD_UDEF_Y: return c.udefy;
+    case CUP2D_FIELD_SDF: return c.sdf;
+    default: return nullptr;
+  }
+}
+
+int cup2d_get_field(cup2d_ctx* ctx, int which, double* host_out) {
+  if (!ctx || !host_out) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  double* p = field_ptr(c, which);
+  if (!p) return fail(ctx, CUP2D_EINVAL, "unknown field");
+  CK(cudaStreamSynchronize(c.stream));
+  CK(cudaMemcpy(host_out, p, sizeof(double) * c.ncells(), cudaMemcpyDeviceToHost));
+  return CUP2D_OK;
+}
+
+int cup2d_set_field(cup2d_ctx* ctx, int which, const double* host_in) {
+  if (!ctx || !host_in) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  double* p = field_ptr(c, which);
+  if (!p) return fail(ctx, CUP2D_EINVAL, "unknown field");
+  CK(cudaStreamSynchronize(c.stream));
+  CK(cudaMemcpy(p, host_in, sizeof(double) * c.ncells(), cudaMemcpyHostToDevice));
+  return CUP2D_OK;
+}
+
+int cup2d_get_shape(cup2d_ctx* ctx, int id, cup2d_shape_state* out) {
+  if (!ctx || !out) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  if (id < 0 || id >= c.nshapes) return fail(ctx, CUP2D_EINVAL, "bad shape id");
+  CK(cudaStreamSynchronize(c.stream));
+  CK(cudaMemcpy(&c.hshapes[id], c.dshapes + id, sizeof(DevShape), cudaMemcpyDeviceToHost));
+  *out = c.hshapes[id].s;
+  return CUP2D_OK;
+}
+
+int cup2d_set_shape(cup2d_ctx* ctx, int id, const cup2d_shape_state* in) {
+  if (!ctx || !in) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  if (id < 0 || id >= c.nshapes) return fail(ctx, CUP2D_EINVAL, "bad shape id");
+  CK(cudaStreamSynchronize(c.stream));
+  CK(cudaMemcpy(&c.hshapes[id], c.dshapes + id, sizeof(DevShape), cudaMemcpyDeviceToHost));
+  c.hshapes[id].s = *in;
+  CK(cudaMemcpy(c.dshapes + id, &c.hshapes[id], sizeof(DevShape), cudaMemcpyHostToDevice));
+  return CUP2D_OK;
+}
+
+int cup2d_get_scalars(cup2d_ctx* ctx, double* time, double* dt, int* step, double* uinfx, double* uinfy) {
+  if (!ctx) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  Scalars s;
+  CK(cudaStreamSynchronize(c.stream));
+  CK(cudaMemcpy(&s, c.dsc, sizeof(Scalars), cudaMemcpyDeviceToHost));
+  if (time) *time = s.time;
+  if (dt) *dt = s.dt;
+  if (step) *step = s.step;
+  if (uinfx) *uinfx = s.uinfx;
+  if (uinfy) *uinfy = s.uinfy;
+  return CUP2D_OK;
+}
+
+int cup2d_set_scalars(cup2d_ctx* ctx, double time, double dt, int step, double uinfx, double uinfy) {
+  if (!ctx) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  Scalars s;
+  CK(cudaStreamSynchronize(c.stream));
+  CK(cudaMemcpy(&s, c.dsc, sizeof(Scalars), cudaMemcpyDeviceToHost));
+  s.time = time; s.dt = dt; s.step = step; s.uinfx = uinfx; s.uinfy = uinfy;
+  CK(cudaMemcpy(c.dsc, &s, sizeof(Scalars), cudaMemcpyHostToDevice));
+  return CUP2D_OK;
+}
+
+int cup2d_grid_size(const cup2d_ctx* ctx, int* nx, int* ny, double* h) {
+  if (!ctx) return CUP2D_EINVAL;
+  if (nx) *nx = ctx->c.g.nx;
+  if (ny) *ny = ctx->c.g.ny;
+  if (h) *h = ctx->c.g.h;
+  return CUP2D_OK;
+}
+
+int cup2d_kernel_launches(const cup2d_ctx* ctx, long long* count) {
+  if (!ctx || !count) return CUP2D_EINVAL;
+  *count = ctx->c.launches;
+  return CUP2D_OK;
+}
+
+int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, double* ms_per_launch) {
+  if (!ctx || !ms_per_launch || reps <= 0) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
+  if (which < 0 || which > CUP2D_KERNEL_OBJECTS) return fail(ctx, CUP2D_EINVAL, "unknown kernel");
+  auto one = [&]() {
+    switch (which) {
+      case CUP2D_KERNEL_ADVDIFF: launch_advdiff(c); launch_advdiff_undo(c); break;
+      case CUP2D_KERNEL_RHS_DIV: launch_rhs_div(c); break;
+      case CUP2D_KERNEL_PCORR: launch_pcorr(c); launch_pcorr_undo(c); break;
+      case CUP2D_KERNEL_FFT_ROWS_FWD: poisson_rows_fwd(c); break;
+      case CUP2D_KERNEL_FFT_COLS: poisson_cols(c); break;
+      case CUP2D_KERNEL_FFT_ROWS_INV: poisson_rows_inv(c); break;
+      case CUP2D_KERNEL_MAX_U: launch_max_u_dt(c); break;
+      case CUP2D_KERNEL_OBJECTS: launch_objects(c); break;
+    }
+  };
+  one();   // warm
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0)); CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, c.stream));
+  for (int r = 0; r < reps; r++) one();
+  CK(cudaEventRecord(e1, c.stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0); cudaEventDestroy(e1);
+  *ms_per_launch = (double)ms / reps;
+  return check_launch(ctx);
+}
+
+int cup2d_advance_timed(cup2d_ctx* ctx, int nsteps, double* ms) {
+  if (!ctx || !ms) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0)); CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, c.stream));
+  int rc = cup2d_advance(ctx, nsteps);
+  if (rc) { cudaEventDestroy(e0); cudaEventDestroy(e1); return rc; }
+  CK(cudaEventRecord(e1, c.stream));
+  CK(cudaEventSynchronize(e1));
+  float f = 0;
+  CK(cudaEventElapsedTime(&f, e0, e1));
+  cudaEventDestroy(e0); cudaEventDestroy(e1);
+  *ms = f;
+  return CUP2D_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,71 @@
+// Host-side context: the device-resident counterpart of the reference's
+// SimulationData (SimulationData.h:17-116) plus its shapes and solver.
+#pragma once
+#include <string>
+#include <vector>
+#include "internal.cuh"
+#include "launch.hpp"
+
+namespace cup2d {
+
+struct Ctx {
+  cup2d_config cfg{};
+  GridDesc g{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool initialised = false;
+
+  // dense fields (fp64 planes, Ny x Nx)
+  double* vel[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [buffer][component]
+  int cur = 0;                  // buffer holding the current velocity
+  double* chi = nullptr;        // SimulationData::chi
+  double* pres = nullptr;       // SimulationData::pres
+  double* rhs = nullptr;        // SimulationData::tmp as used by PressureSingle
+  double* sdf = nullptr;        // SimulationData::tmp as used by PutObjectsOnGrid
+  double* udefx = nullptr;      // SimulationData::uDef
+  double* udefy = nullptr;
+
+  Scalars* dsc = nullptr;       // device scalars
+  DevShape* dshapes = nullptr;  // device shape array [MAX_SHAPES]
+  std::vector<DevShape> hshapes;
+  std::vector<ObstTiles> tiles;
+  std::vector<FishArrays> fish;
+  int nshapes = 0;
+  int maxCapacity = 0;
+
+  // reduction scratch: per-CTA partial sums and "last CTA" tickets
+  double* partials = nullptr;
+  size_t npartials = 0;
+  unsigned* counters = nullptr;
+  static constexpr int NCOUNTERS = 256;
+
+  Poisson* poisson = nullptr;
+
+  cudaGraphExec_t graph = nullptr;
+  long long launches = 0;
+  int launchesInGraph = 0;
+  std::string err;
+
+  double* u() const { return vel[cur][0]; }
+  double* v() const { return vel[cur][1]; }
+  double* uo() const { return vel[1 - cur][0]; }
+  double* vo() const { return vel[1 - cur][1]; }
+  size_t ncells() const { return (size_t)g.nx * g.ny; }
+};
+
+// counter slots used by the kernels (each last-CTA reduction owns one)
+enum CounterSlot : int {
+  CNT_MAXU = 0, CNT_ADV = 1, CNT_FADE = 2,
+  CNT_CHI = 8,          // + shape
+  CNT_RHSOBST = 24,     // + shape
+  CNT_FORCES = 40,      // + shape
+};
+// partials offsets (doubles)
+inline size_t part_off(int region, const Ctx& c) {
+  // regions: 0 dense reductions, 1.. per-shape tile reductions
+  return (size_t)region * (c.npartials / 16);
+}
+
+#define CUP2D_LAUNCHED(c) ((c).launches++)
+
+} // namespace cup2d

@@ -1,0 +1,503 @@
+// Fish on the device.
+//
+// k_fish_kinematics (one CTA per fish) is Fish::create up to the block
+// intersection (Fish.cpp:20-110) for the two midline models of the reference:
+//  - StefanFish's CurvatureFish::computeMidline (StefanFish.cpp:154-206):
+//    the curvature scheduler ramp (FishUtilities.h:171-258), the travelling
+//    curvature wave and the Frenet integration (FishUtilities.h:15-79);
+//  - CarlingFish's AmplitudeFish::computeMidline (CarlingFish.cpp:16-88);
+// then the midline integrals and frame changes (FishLibrary.cpp:66-176) and
+// the AreaSegment boxes (Fish.cpp:78-110, FishLibrary.cpp:295-342).
+// The Frenet recurrence is serial in s and runs on one thread; everything
+// else is parallel over midline points.
+//
+// k_fish_raster (one CTA per obstacle tile, one thread per cell) is
+// PutFishOnBlocks (FishLibrary.cpp:403-638).  The reference scatters every
+// surface / interior point of every intersecting segment onto the block;
+// here every cell gathers those points in the reference's loop order
+// (segment, s index, side / width offset), so its "keep the nearest"
+// updates, ties included, and its hat-kernel sums see exactly the same
+// sequence as in the reference.
+#include <cmath>
+#include "context.hpp"
+#include "fish.cuh"
+
+namespace cup2d {
+
+namespace {
+
+constexpr double EPSd = 2.220446049250313e-16;
+
+__device__ __forceinline__ double sq(double x) { return x * x; }
+
+// IF2D_Interpolation1D::cubicInterpolation (FishUtilities.h:132-145)
+__device__ __forceinline__ void cubic_interp(double x0, double x1, double x, double y0, double y1,
+                                             double dy0, double dy1, double& y, double& dy)
+{
+  const double xrel = (x - x0);
+  const double deltax = (x1 - x0);
+  const double a = (dy0 + dy1) / (deltax * deltax) - 2 * (y1 - y0) / (deltax * deltax * deltax);
+  const double b = (-2 * dy0 - dy1) / deltax + 3 * (y1 - y0) / (deltax * deltax);
+  const double c = dy0;
+  const double d = y0;
+  y = a * xrel * xrel * xrel + b * xrel * xrel + c * xrel + d;
+  dy = 3 * a * xrel * xrel + 2 * b * xrel + c;
+}
+
+__global__ void __launch_bounds__(512)
+k_fish_kinematics(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays F)
+{
+  __shared__ double red[32 * 5];
+  __shared__ double bc[8];
+  DevShape& S = sh[k];
+  const int Nm = F.nm, tid = threadIdx.x, nt = blockDim.x;
+  const double t = sc->time;
+  const double L = S.cfg.length, T = S.cfg.Tperiod;
+  double* rS = F.rS; double* rX = F.rX; double* rY = F.rY; double* vX = F.vX; double* vY = F.vY;
+  double* norX = F.norX; double* norY = F.norY; double* vNorX = F.vNorX; double* vNorY = F.vNorY;
+  const double* width = F.width;
+
+  if (S.cfg.kind == CUP2D_SHAPE_STEFANFISH) {
+    // curvature scheduler: after transition(0, 0, T, zeros, values) the start
+    // state and slope are zero and the end state is the spline p1f
+    // (StefanFish.cpp:197-204); the RL bending wave is identically zero
+    // without actions, and the PID terms are zero with -pid 0 -pidpos 0.
+    const double waveLength = 1, amp = S.cfg.ampFac, phaseShift = S.cfg.phaseShift;
+    const double periodPIDval = T, time0 = 0, timeshift = 0;
+    const double diffT = 1;
+    const double darg = 2 * M_PI / periodPIDval * diffT;
+    const double arg0 = 2 * M_PI * ((t - time0) / periodPIDval + timeshift) + M_PI * phaseShift;
+    for (int i = tid; i < Nm; i += nt) {
+      double rC, vC;
+      if (t > T) { rC = F.p1f[i]; vC = 0; }
+      else cubic_interp(0.0, T, t, 0.0, F.p1f[i], 0.0, 0.0, rC, vC);
+      const double rB = 0, vB = 0, fac = 0, dif = 0;
+      const double arg = arg0 - 2 * M_PI * rS[i] / L / waveLength;
+      F.rK[i] = amp * rC * (sin(arg) + rB + fac);
+      F.vK[i] = amp * (vC * (sin(arg) + rB + fac) + rC * (cos(arg) * darg + vB + dif));
+    }
+    __syncthreads();
+    if (tid == 0) {                                     // IF2D_Frenet2D::solve
+      const double* curv = F.rK; const double* curv_dt = F.vK;
+      rX[0] = 0.0; rY[0] = 0.0; norX[0] = 0.0; norY[0] = 1.0;
+      double ksiX = 1.0, ksiY = 0.0;
+      vX[0] = 0.0; vY[0] = 0.0; vNorX[0] = 0.0; vNorY[0] = 0.0;
+      double vKsiX = 0.0, vKsiY = 0.0;
+      for (int i = 1; i < Nm; i++) {
+        const double dksiX = curv[i - 1] * norX[i - 1];
+        const double dksiY = curv[i - 1] * norY[i - 1];
+        const double dnuX = -curv[i - 1] * ksiX;
+        const double dnuY = -curv[i - 1] * ksiY;
+        const double dvKsiX = curv_dt[i - 1] * norX[i - 1] + curv[i - 1] * vNorX[i - 1];
+        const double dvKsiY = curv_dt[i - 1] * norY[i - 1] + curv[i - 1] * vNorY[i - 1];
+        const double dvNuX = -curv_dt[i - 1] * ksiX - curv[i - 1] * vKsiX;
+        const double dvNuY = -curv_dt[i - 1] * ksiY - curv[i - 1] * vKsiY;
+        const double ds = rS[i] - rS[i - 1];
+        rX[i] = rX[i - 1] + ds * ksiX;
+        rY[i] = rY[i - 1] + ds * ksiY;
+        norX[i] = norX[i - 1] + ds * dnuX;
+        norY[i] = norY[i - 1] + ds * dnuY;
+        ksiX += ds * dksiX;
+        ksiY += ds * dksiY;
+        vX[i] = vX[i - 1] + ds * vKsiX;
+        vY[i] = vY[i - 1] + ds * vKsiY;
+        vNorX[i] = vNorX[i - 1] + ds * dvNuX;
+        vNorY[i] = vNorY[i - 1] + ds * dvNuY;
+        vKsiX += ds * dvKsiX;
+        vKsiY += ds * dvKsiY;
+        const double d1 = ksiX * ksiX + ksiY * ksiY;
+        const double d2 = norX[i] * norX[i] + norY[i] * norY[i];
+        if (d1 > EPSd) { const double nf = 1 / sqrt(d1); ksiX *= nf; ksiY *= nf; }
+        if (d2 > EPSd) { const double nf = 1 / sqrt(d2); norX[i] *= nf; norY[i] *= nf; }
+      }
+    }
+    __syncthreads();
+  } else {
+    // AmplitudeFish::computeMidline (CarlingFish.cpp:70-107)
+    const double phaseShift = S.cfg.phaseShift;
+    const double rampFac = t < T ? sin(0.5 * M_PI * t / T) : 1.0;
+    const double rampFacVel = t < T ? 0.5 * M_PI / T * cos(0.5 * M_PI * t / T) : 0.0;
+    auto latPos = [&](double s) {
+      const double arg = 2 * M_PI * (s / L - t / T + phaseShift);
+      return 4. / 33. * (s + 0.03125 * L) * sin(arg);
+    };
+    auto latVel = [&](double s) {
+      const double arg = 2 * M_PI * (s / L - t / T + phaseShift);
+      return -4. / 33. * (s + 0.03125 * L) * (2 * M_PI / T) * cos(arg);
+    };
+    for (int i = tid; i < Nm; i += nt) {
+      rY[i] = rampFac * latPos(rS[i]);
+      vY[i] = rampFac * latVel(rS[i]) + rampFacVel * latPos(rS[i]);
+    }
+    __syncthreads();
+    for (int i = 1 + tid; i < Nm; i += nt) {
+      const double dy = rY[i] - rY[i - 1], ds = rS[i] - rS[i - 1];
+      const double dx = sqrt(ds * ds - dy * dy);
+      const double dVy = vY[i] - vY[i - 1];
+      const double dVx = -dy / dx * dVy;
+      F.rK[i] = dx; F.vK[i] = dVx;                      // increments, summed below
+      norX[i - 1] = -dy / ds; norY[i - 1] = dx / ds;
+      vNorX[i - 1] = -dVy / ds; vNorY[i - 1] = dVx / ds;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      rX[0] = 0.0; vX[0] = 0.0;
+      for (int i = 1; i < Nm; i++) { rX[i] = F.rK[i] + rX[i - 1]; vX[i] = F.vK[i] + vX[i - 1]; }
+      norX[Nm - 1] = norX[Nm - 2]; norY[Nm - 1] = norY[Nm - 2];
+      vNorX[Nm - 1] = vNorX[Nm - 2]; vNorY[Nm - 1] = vNorY[Nm - 2];
+    }
+    __syncthreads();
+  }
+
+  // FishData::_d_ds / _integrationFac* (FishLibrary.h:79-95)
+  auto d_ds = [&](int idx, const double* vals) -> double {
+    if (idx == 0) return (vals[idx + 1] - vals[idx]) / (rS[idx + 1] - rS[idx]);
+    else if (idx == Nm - 1) return (vals[idx] - vals[idx - 1]) / (rS[idx] - rS[idx - 1]);
+    else return ((vals[idx + 1] - vals[idx]) / (rS[idx + 1] - rS[idx]) +
+                 (vals[idx] - vals[idx - 1]) / (rS[idx] - rS[idx - 1])) / 2;
+  };
+  auto dsOf = [&](int i) -> double {
+    return (i == 0) ? rS[1] - rS[0] : ((i == Nm - 1) ? rS[Nm - 1] - rS[Nm - 2] : rS[i + 1] - rS[i - 1]);
+  };
+  // integrateLinearMomentum (FishLibrary.cpp:86-117)
+  {
+    double a[5] = {0, 0, 0, 0, 0};
+    for (int i = tid; i < Nm; i += nt) {
+      const double ds = dsOf(i);
+      const double fac1 = 2 * width[i];
+      const double fac2 = 2 * pow(width[i], 3.0) * (d_ds(i, norX) * norY[i] - d_ds(i, norY) * norX[i]) / 3;
+      a[0] += fac1 * ds / 2;
+      a[1] += (rX[i] * fac1 + norX[i] * fac2) * ds / 2;
+      a[2] += (rY[i] * fac1 + norY[i] * fac2) * ds / 2;
+      a[3] += (vX[i] * fac1 + vNorX[i] * fac2) * ds / 2;
+      a[4] += (vY[i] * fac1 + vNorY[i] * fac2) * ds / 2;
+    }
+    block_sum<5>(a, red);
+    if (tid == 0) {
+      const double area = a[0];
+      S.f.area_internal = area;
+      S.f.CoM_internal[0] = a[1] / area; S.f.CoM_internal[1] = a[2] / area;
+      S.f.vCoM_internal[0] = a[3] / area; S.f.vCoM_internal[1] = a[4] / area;
+      bc[0] = S.f.CoM_internal[0]; bc[1] = S.f.CoM_internal[1];
+      bc[2] = S.f.vCoM_internal[0]; bc[3] = S.f.vCoM_internal[1];
+    }
+    __syncthreads();
+  }
+  for (int i = tid; i < Nm; i += nt) {                  // changeToCoMFrameLinear
+    rX[i] -= bc[0]; rY[i] -= bc[1]; vX[i] -= bc[2]; vY[i] -= bc[3];
+  }
+  __syncthreads();
+  // integrateAngularMomentum (FishLibrary.cpp:119-150)
+  {
+    double a[2] = {0, 0};
+    for (int i = tid; i < Nm; i += nt) {
+      const double ds = dsOf(i);
+      const double w3 = pow(width[i], 3.0);
+      const double fac1 = 2 * width[i];
+      const double fac2 = 2 * w3 * (d_ds(i, norX) * norY[i] - d_ds(i, norY) * norX[i]) / 3;
+      const double fac3 = 2 * w3 / 3;
+      const double tmp_M = (rX[i] * vY[i] - rY[i] * vX[i]) * fac1
+        + (rX[i] * vNorY[i] - rY[i] * vNorX[i] + vY[i] * norX[i] - vX[i] * norY[i]) * fac2
+        + (norX[i] * vNorY[i] - norY[i] * vNorX[i]) * fac3;
+      const double tmp_J = (rX[i] * rX[i] + rY[i] * rY[i]) * fac1
+        + 2 * (rX[i] * norX[i] + rY[i] * norY[i]) * fac2 + fac3;
+      a[0] += tmp_M * ds / 2;
+      a[1] += tmp_J * ds / 2;
+    }
+    block_sum<2>(a, red);
+    if (tid == 0) {
+      S.f.angvel_internal_prev = S.f.angvel_internal;
+      S.f.J_internal = a[1];
+      S.f.angvel_internal = a[0] / a[1];
+      bc[4] = S.f.theta_internal; bc[5] = S.f.angvel_internal;
+    }
+    __syncthreads();
+  }
+  {                                                     // changeToCoMFrameAngular
+    const double Ain = bc[4], vAin = bc[5];
+    const double R00 = cos(Ain), R01 = -sin(Ain), R10 = sin(Ain), R11 = cos(Ain);
+    for (int i = tid; i < Nm; i += nt) {
+      vX[i] += vAin * rY[i];
+      vY[i] -= vAin * rX[i];
+      const double px = rX[i], py = rY[i];
+      rX[i] = R00 * px + R01 * py; rY[i] = R10 * px + R11 * py;
+      const double qx = vX[i], qy = vY[i];
+      vX[i] = R00 * qx + R01 * qy; vY[i] = R10 * qx + R11 * qy;
+    }
+    __syncthreads();
+    for (int i = tid; i < Nm - 1; i += nt) {            // _computeMidlineNormals
+      const double ds = rS[i + 1] - rS[i];
+      const double tX = rX[i + 1] - rX[i], tY = rY[i + 1] - rY[i];
+      const double tVX = vX[i + 1] - vX[i], tVY = vY[i + 1] - vY[i];
+      norX[i] = -tY / ds; norY[i] = tX / ds;
+      vNorX[i] = -tVY / ds; vNorY[i] = tVX / ds;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      norX[Nm - 1] = norX[Nm - 2]; norY[Nm - 1] = norY[Nm - 2];
+      vNorX[Nm - 1] = vNorX[Nm - 2]; vNorY[Nm - 1] = vNorY[Nm - 2];
+    }
+    __syncthreads();
+  }
+  // AreaSegments (Fish.cpp:118-150) in the computational frame
+  const int Nseg = F.nseg;
+  const double angle = S.s.orientation;
+  const double R00 = cos(angle), R01 = -sin(angle), R10 = sin(angle), R11 = cos(angle);
+  for (int i = tid; i < Nseg; i += nt) {
+    const int next_idx = (i + 1) * (Nm - 1) / Nseg, idx = i * (Nm - 1) / Nseg;
+    double bb[2][2] = {{1e9, -1e9}, {1e9, -1e9}};
+    for (int ss = idx; ss <= next_idx; ++ss) {
+      const double xB0 = rX[ss] - norX[ss] * width[ss], xB1 = rX[ss] + norX[ss] * width[ss];
+      const double yB0 = rY[ss] - norY[ss] * width[ss], yB1 = rY[ss] + norY[ss] * width[ss];
+      const double maxX = fmax(xB0, xB1), minX = fmin(xB0, xB1);
+      const double maxY = fmax(yB0, yB1), minY = fmin(yB0, yB1);
+      bb[0][0] = fmin(bb[0][0], minX); bb[0][1] = fmax(bb[0][1], maxX);
+      bb[1][0] = fmin(bb[1][0], minY); bb[1][1] = fmax(bb[1][1], maxY);
+    }
+    const double safe = 2 * g.h;
+    Segment sg;
+    sg.first = idx; sg.second = next_idx;
+    sg.w[0] = (bb[0][1] - bb[0][0]) / 2 + safe; sg.w[1] = (bb[1][1] - bb[1][0]) / 2 + safe;
+    const double c0 = (bb[0][1] + bb[0][0]) / 2, c1 = (bb[1][1] + bb[1][0]) / 2;
+    // AreaSegment::changeToComputationalFrame (FishLibrary.cpp:295-342)
+    double nI0 = R00 * 1 + R01 * 0, nI1 = R10 * 1 + R11 * 0;
+    double nJ0 = R00 * 0 + R01 * 1, nJ1 = R10 * 0 + R11 * 1;
+    sg.c[0] = R00 * c0 + R01 * c1 + S.s.center[0];
+    sg.c[1] = R10 * c0 + R11 * c1 + S.s.center[1];
+    const double magI = sqrt(nI0 * nI0 + nI1 * nI1), magJ = sqrt(nJ0 * nJ0 + nJ1 * nJ1);
+    const double invMagI = 1 / magI, invMagJ = 1 / magJ;
+    sg.normalI[0] = fabs(nI0) * invMagI; sg.normalI[1] = fabs(nI1) * invMagI;
+    sg.normalJ[0] = fabs(nJ0) * invMagJ; sg.normalJ[1] = fabs(nJ1) * invMagJ;
+    const double wX[2] = {sg.w[0] * sg.normalI[0], sg.w[0] * sg.normalI[1]};
+    const double wY[2] = {sg.w[1] * sg.normalJ[0], sg.w[1] * sg.normalJ[1]};
+    for (int d = 0; d < 2; d++) {
+      sg.boxLab[d][0] = sg.c[d] - wX[d] - wY[d];
+      sg.boxLab[d][1] = sg.c[d] + wX[d] + wY[d];
+      sg.boxObj[d][0] = sg.c[d] - sg.w[d];
+      sg.boxObj[d][1] = sg.c[d] + sg.w[d];
+    }
+    F.seg[i] = sg;
+  }
+  if (tid == 0) S.nseg = Nseg;
+}
+
+struct SurfPt { double myP[2], pP[2], pM[2], ud[2]; int iap[2], ss, valid; };
+struct IntPt { double xp[2], ud[2], w[2][2]; int iap[2], valid; };
+
+constexpr int MAX_SEG_PER_TILE = 512;
+constexpr int SURF_CHUNK = 64;
+constexpr int INT_CHUNK = 256;
+
+__global__ void __launch_bounds__(1024)
+k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, double* sdfg)
+{
+  __shared__ int segList[MAX_SEG_PER_TILE];
+  __shared__ int nSegList;
+  __shared__ int warpCount[32];
+  __shared__ SurfPt sp[SURF_CHUNK];
+  __shared__ IntPt ip[INT_CHUNK];
+  const DevShape& S = sh[k];
+  const int s = blockIdx.x;
+  if (s >= S.ntiles) return;
+  const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+  const int tid = threadIdx.x + BS * threadIdx.y, lane = tid & 31, wid = tid >> 5;
+  const int ix = threadIdx.x, iy = threadIdx.y;
+  const double h = g.h, invh = 1.0 / h;
+  const double org0 = cell_x(g, bx, 0), org1 = cell_y(g, by, 0);
+  const double angle = S.s.orientation;
+  const double R00 = cos(angle), R01 = -sin(angle), R10 = sin(angle), R11 = cos(angle);
+  const double pos0 = S.s.center[0], pos1 = S.s.center[1];
+  const int Nm = F.nm;
+  const double* rX = F.rX; const double* rY = F.rY; const double* width = F.width;
+  const double* norX = F.norX; const double* norY = F.norY;
+  const double* vX = F.vX; const double* vY = F.vY;
+  const double* vNorX = F.vNorX; const double* vNorY = F.vNorY;
+
+  // ordered list of the segments intersecting this block (Fish.cpp:167-173)
+  if (tid == 0) nSegList = 0;
+  __syncthreads();
+  {
+    const double start[2] = {org0, org1};
+    const double end[2] = {cell_x(g, bx, BS - 1), cell_y(g, by, BS - 1)};
+    for (int s0 = 0; s0 < S.nseg; s0 += 1024) {
+      const int q = s0 + tid;
+      const bool f = q < S.nseg && segment_hits_block(F.seg[q], start, end, 2 * h);
+      const unsigned m = __ballot_sync(0xffffffffu, f);
+      if (lane == 0) warpCount[wid] = __popc(m);
+      __syncthreads();
+      int off = nSegList;
+      for (int w = 0; w < wid; w++) off += warpCount[w];
+      const int p = off + __popc(m & ((1u << lane) - 1u));
+      if (f && p < MAX_SEG_PER_TILE) segList[p] = q;
+      __syncthreads();
+      if (tid == 0) { int tot = 0; for (int w = 0; w < 32; w++) tot += warpCount[w]; nSegList += tot; }
+      __syncthreads();
+    }
+  }
+  const int nsl = nSegList < MAX_SEG_PER_TILE ? nSegList : MAX_SEG_PER_TILE;
+  const double px = cell_x(g, bx, ix), py = cell_y(g, by, iy);   // info.pos(p, sx, sy)
+
+  // constructSurface (FishLibrary.cpp:438-573)
+  double dist = -1, chi = 0, ud0 = 0, ud1 = 0;
+  for (int si = 0; si < nsl; si++) {
+    const Segment& sg = F.seg[segList[si]];
+    const int firstSegm = max(sg.first, 1), lastSegm = min(sg.second, Nm - 2);
+    const int npts = (lastSegm - firstSegm + 1) * 2;
+    for (int c0 = 0; c0 < npts; c0 += SURF_CHUNK) {
+      const int nc = min(SURF_CHUNK, npts - c0);
+      __syncthreads();
+      if (tid < nc) {
+        const int q = c0 + tid, ss = firstSegm + q / 2, signp = (q & 1) ? 1 : -1;
+        SurfPt P;
+        P.ss = ss;
+        double m0 = rX[ss + 0] + width[ss + 0] * signp * norX[ss + 0];
+        double m1 = rY[ss + 0] + width[ss + 0] * signp * norY[ss + 0];
+        P.myP[0] = R00 * m0 + R01 * m1 + pos0; P.myP[1] = R10 * m0 + R11 * m1 + pos1;
+        P.iap[0] = (int)floor((P.myP[0] - org0) * invh);
+        P.iap[1] = (int)floor((P.myP[1] - org1) * invh);
+        P.valid = !(P.iap[0] + 3 <= 0 || P.iap[0] - 1 >= BS) && !(P.iap[1] + 3 <= 0 || P.iap[1] - 1 >= BS);
+        if (P.valid) {
+          m0 = rX[ss + 1] + width[ss + 1] * signp * norX[ss + 1];
+          m1 = rY[ss + 1] + width[ss + 1] * signp * norY[ss + 1];
+          P.pP[0] = R00 * m0 + R01 * m1 + pos0; P.pP[1] = R10 * m0 + R11 * m1 + pos1;
+          m0 = rX[ss - 1] + width[ss - 1] * signp * norX[ss - 1];
+          m1 = rY[ss - 1] + width[ss - 1] * signp * norY[ss - 1];
+          P.pM[0] = R00 * m0 + R01 * m1 + pos0; P.pM[1] = R10 * m0 + R11 * m1 + pos1;
+          const double u0 = vX[ss + 0] + width[ss + 0] * signp * vNorX[ss + 0];
+          const double u1 = vY[ss + 0] + width[ss + 0] * signp * vNorY[ss + 0];
+          P.ud[0] = R00 * u0 + R01 * u1; P.ud[1] = R10 * u0 + R11 * u1;
+        }
+        sp[tid] = P;
+      }
+      __syncthreads();
+      for (int q = 0; q < nc; q++) {
+        const SurfPt& P = sp[q];
+        if (!P.valid) continue;
+        if (iy < max(0, P.iap[1] - 1) || iy >= min(P.iap[1] + 3, BS)) continue;
+        if (ix < max(0, P.iap[0] - 1) || ix >= min(P.iap[0] + 3, BS)) continue;
+        const double dist0 = sq(px - P.myP[0]) + sq(py - P.myP[1]);
+        const double distP = sq(px - P.pP[0]) + sq(py - P.pP[1]);
+        const double distM = sq(px - P.pM[0]) + sq(py - P.pM[1]);
+        if (fabs(dist) < fmin(fmin(dist0, distP), distM)) continue;
+        // changeFromComputationalFrame (FishLibrary.h:194-200)
+        const double q0 = px - pos0, q1 = py - pos1;
+        const double p0 = R00 * q0 + R10 * q1, p1 = R01 * q0 + R11 * q1;
+        const int ss = P.ss;
+        int close_s = ss, secnd_s = ss + (distP < distM ? 1 : -1);
+        double dist1 = dist0, dist2 = distP < distM ? distP : distM;
+        if (distP < dist0 || distM < dist0) {
+          dist1 = dist2; dist2 = dist0;
+          close_s = secnd_s; secnd_s = ss;
+        }
+        const double dSsq = sq(rX[close_s] - rX[secnd_s]) + sq(rY[close_s] - rY[secnd_s]);
+        const double cnt2ML = sq(width[close_s]);
+        const double nxt2ML = sq(width[secnd_s]);
+        const double safeW = fmax(width[close_s], width[secnd_s]) + 2 * h;
+        const double grd2ML = sq(p0 - rX[close_s]) + sq(p1 - rY[close_s]);
+        const double diffH = fabs(width[close_s] - width[secnd_s]);
+        double sign2d = 0;
+        if (dSsq > diffH * diffH || grd2ML > safeW * safeW) {
+          sign2d = grd2ML > cnt2ML ? -1 : 1;
+        } else {
+          const double corr = 2 * sqrt(cnt2ML * nxt2ML);
+          const double Rsq = (cnt2ML + nxt2ML - corr + dSsq) * (cnt2ML + nxt2ML + corr + dSsq) / 4 / dSsq;
+          const double maxAx = fmax(cnt2ML, nxt2ML);
+          const int idAx1 = cnt2ML > nxt2ML ? close_s : secnd_s;
+          const int idAx2 = idAx1 == close_s ? secnd_s : close_s;
+          const double d = sqrt((Rsq - maxAx) / dSsq);
+          const double xC0 = rX[idAx1] + (rX[idAx1] - rX[idAx2]) * d;
+          const double xC1 = rY[idAx1] + (rY[idAx1] - rY[idAx2]) * d;
+          const double grd2Core = sq(p0 - xC0) + sq(p1 - xC1);
+          sign2d = grd2Core > Rsq ? -1 : 1;
+        }
+        if (fabs(dist) > dist1) {
+          const double W = 1 - sqrt(dist1) * (invh / 3);
+          ud0 = W * P.ud[0]; ud1 = W * P.ud[1];
+          dist = sign2d * dist1;
+          chi = W;
+        }
+      }
+    }
+  }
+
+  // constructInternl (FishLibrary.cpp:575-638)
+  for (int si = 0; si < nsl; si++) {
+    const Segment& sg = F.seg[segList[si]];
+    const int firstSegm = max(sg.first, 1), lastSegm = min(sg.second, Nm - 2);
+    // points of this segment: for ss, iw in (-Nw, Nw)
+    int npts = 0;
+    for (int ss = firstSegm; ss <= lastSegm; ss++) {
+      const int Nw = (int)floor(width[ss] / h);
+      npts += Nw > 0 ? 2 * Nw - 1 : 0;
+    }
+    for (int c0 = 0; c0 < npts; c0 += INT_CHUNK) {
+      const int nc = min(INT_CHUNK, npts - c0);
+      __syncthreads();
+      if (tid < nc) {
+        int q = c0 + tid, ss = firstSegm, Nw = 0;
+        for (;; ss++) {
+          Nw = (int)floor(width[ss] / h);
+          const int n = Nw > 0 ? 2 * Nw - 1 : 0;
+          if (q < n) break;
+          q -= n;
+        }
+        const int iw = -Nw + 1 + q;
+        const double offsetW = iw * h;
+        IntPt P;
+        const double m0 = rX[ss] + offsetW * norX[ss], m1 = rY[ss] + offsetW * norY[ss];
+        P.xp[0] = ((R00 * m0 + R01 * m1 + pos0) - org0) * invh;
+        P.xp[1] = ((R10 * m0 + R11 * m1 + pos1) - org1) * invh;
+        const double ap0 = floor(P.xp[0]), ap1 = floor(P.xp[1]);
+        P.iap[0] = (int)ap0; P.iap[1] = (int)ap1;
+        P.valid = !(P.iap[0] + 2 <= 0 || P.iap[0] >= BS) && !(P.iap[1] + 2 <= 0 || P.iap[1] >= BS);
+        const double u0 = vX[ss] + offsetW * vNorX[ss], u1 = vY[ss] + offsetW * vNorY[ss];
+        P.ud[0] = R00 * u0 + R01 * u1; P.ud[1] = R10 * u0 + R11 * u1;
+        P.w[0][0] = 1 - fabs(P.xp[0] - ap0); P.w[0][1] = 1 - fabs(P.xp[0] - (ap0 + 1));
+        P.w[1][0] = 1 - fabs(P.xp[1] - ap1); P.w[1][1] = 1 - fabs(P.xp[1] - (ap1 + 1));
+        ip[tid] = P;
+      }
+      __syncthreads();
+      for (int q = 0; q < nc; q++) {
+        const IntPt& P = ip[q];
+        if (!P.valid) continue;
+        if (iy < max(0, P.iap[1]) || iy >= min(P.iap[1] + 2, BS)) continue;
+        if (ix < max(0, P.iap[0]) || ix >= min(P.iap[0] + 2, BS)) continue;
+        const int sx = ix - P.iap[0], sy = iy - P.iap[1];
+        const double wxwy = P.w[1][sy] * P.w[0][sx];
+        ud0 += wxwy * P.ud[0];
+        ud1 += wxwy * P.ud[1];
+        chi += wxwy;
+        if (fabs(dist + 1) < EPSd) dist = 1;
+      }
+    }
+  }
+
+  // signedDistanceSqrt (FishLibrary.cpp:419-436)
+  const double normfac = chi > EPSd ? chi : 1;
+  ud0 /= normfac; ud1 /= normfac;
+  dist = dist >= 0 ? sqrt(dist) : -sqrt(-dist);
+  const size_t o = (size_t)s * BS2 + iy * BS + ix;
+  t.dist[o] = dist; t.chi[o] = 0; t.udx[o] = ud0; t.udy[o] = ud1;
+  atomic_max_double(&sdfg[(size_t)(by * BS + iy) * g.nx + bx * BS + ix], dist);
+}
+
+} // namespace
+
+FishSegPtrs fish_seg_ptrs(const Ctx& c) {
+  FishSegPtrs p{};
+  for (int k = 0; k < c.nshapes; k++) p.seg[k] = c.fish[k].seg;
+  return p;
+}
+
+void launch_fish_kinematics(Ctx& c, int k) {
+  k_fish_kinematics<<<1, 512, 0, c.stream>>>(c.g, c.dsc, c.dshapes, k, c.fish[k]);
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_fish_raster(Ctx& c, int k) {
+  k_fish_raster<<<c.tiles[k].capacity, dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
+                                                                   c.fish[k], c.sdf);
+  CUP2D_LAUNCHED(c);
+}
+
+} // namespace cup2d

@@ -1,0 +1,336 @@
+// Dense grid kernels of the timestep: findMaxU + dt, advDiff, the outflow
+// correction, the pressure RHS divergence, the fade reductions of cub2rhs,
+// the pressure correction, IC and ApplyObjVel.
+//
+// Every kernel maps one CTA to one 32x32 reference block (blockDim 32x8,
+// 4 rows per thread): a warp reads one 256-byte fp64 row segment, the
+// 5-point halo comes from L1/L2 (neighbour rows are read by the CTA itself,
+// neighbour columns by the adjacent CTA), so DRAM sees each plane once.
+// Arithmetic is written in the reference's operation order and the library
+// is compiled without FMA contraction, so a stage fed the same inputs as the
+// reference reproduces it bit for bit (reductions excepted: their order
+// differs).
+#include <cmath>
+#include "context.hpp"
+
+namespace cup2d {
+
+namespace {
+
+constexpr double EPSd = 2.220446049250313e-16;   // std::numeric_limits<double>::epsilon()
+
+__global__ void k_max_u_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh,
+                           const double* __restrict__ u, const double* __restrict__ v,
+                           double* partials, unsigned* counter)
+{
+  __shared__ double red[64];
+  const double UINF = sc->uinfx, VINF = sc->uinfy;
+  double m = 0.0; int bad = 0;
+  const size_t n = (size_t)g.nx * g.ny;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double a = u[i], b = v[i];
+    // Helpers.cpp:160-166: max of |u+uinf|, |v+vinf|, |u|, |v|
+    m = fmax(m, fmax(fmax(fabs(a + UINF), fabs(b + VINF)), fmax(fabs(a), fabs(b))));
+    bad |= !isfinite(a) || !isfinite(b);
+  }
+  m = block_max(m, red);
+  const int anyBad = __syncthreads_or(bad);
+  if (lin_tid() == 0) {
+    partials[blockIdx.x] = m;
+    if (anyBad) atomicOr(&sc->status, ST_NAN);
+  }
+  if (!last_block_done(counter, gridDim.x)) return;
+  double mm = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) mm = fmax(mm, partials[i]);
+  mm = block_max(mm, red);
+  if (threadIdx.x != 0) return;
+  // Simulation::calcMaxTimestep (Simulation.cpp:254-277)
+  const double maxU = mm, h = g.h;
+  const double dtFourier = h * h / g.nu, dtCFL = maxU < 2.2e-16 ? 1 : h / maxU;
+  double maxUb = 0;                                   // SimulationData::maxRelSpeed
+  for (int k = 0; k < nsh; k++) {
+    const double su = sh[k].s.u, sv = sh[k].s.v;
+    maxUb = fmax(maxUb, sqrt(su * su + sv * sv));     // Shape::getMaxVel
+  }
+  const double dtBody = maxUb < 2.2e-16 ? 1 : h / maxUb;
+  double mn = dtCFL;
+  if (dtFourier < mn) mn = dtFourier;
+  if (dtBody < mn) mn = dtBody;
+  double dt = g.CFL * mn;
+  if (sc->step < 100) dt = sc->rampCFL[sc->step] * mn;
+  sc->dt = dt;
+  sc->maxU = maxU;
+  if (g.dlm > 0) sc->lambda = g.dlm / dt;
+}
+
+__global__ void k_set_dt(Scalars* sc, double dt) { sc->dt = dt; }
+
+__global__ void k_end_step(Scalars* sc) {
+  sc->time += sc->dt;
+  sc->step += 1;
+}
+
+// advDiff.cpp:14-87.  Ghosts: neighbour cells, or at the domain edge the
+// zero-gradient copy scaled by the inflow fade of advDiff.cpp:50-55,68-71.
+__global__ void __launch_bounds__(256)
+k_advdiff(GridDesc g, const Scalars* sc,
+          const double* __restrict__ u, const double* __restrict__ v,
+          double* __restrict__ un, double* __restrict__ vn,
+          double* partials, unsigned* counter, Scalars* scw)
+{
+  __shared__ double red[32];
+  const double dt = sc->dt, h = g.h;
+  const double UINF0 = sc->uinfx, UINF1 = sc->uinfy;
+  const double dfac = (g.nu / h) * (dt / h), afac = -0.5 * dt / h;
+  const double norUinf = fmax(fmax(fabs(UINF0), fabs(UINF1)), EPSd);
+  const double rW = fmax(UINF0, 0.0) / norUinf, rS = fmax(UINF1, 0.0) / norUinf;
+  const double rE = fmin(UINF0, 0.0) / norUinf, rN = fmin(UINF1, 0.0) / norUinf;
+  const double fadeW = 1 - rW * rW / 100, fadeS = 1 - rS * rS / 100;
+  const double fadeE = 1 - rE * rE / 100, fadeN = 1 - rN * rN / 100;
+  const int nx = g.nx, ny = g.ny;
+  const int gx = blockIdx.x * BS + threadIdx.x;
+  double IF = 0;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int gy = blockIdx.y * BS + threadIdx.y + 8 * r;
+    const size_t c = (size_t)gy * nx + gx;
+    const double ucc = u[c], vcc = v[c];
+    double ulx, vlx, upx, vpx, uly, vly, upy, vpy;
+    if (gx > 0) { ulx = u[c - 1]; vlx = v[c - 1]; } else { ulx = ucc * fadeW; vlx = vcc * fadeW; }
+    if (gx < nx - 1) { upx = u[c + 1]; vpx = v[c + 1]; } else { upx = ucc * fadeE; vpx = vcc * fadeE; }
+    if (gy > 0) { uly = u[c - nx]; vly = v[c - nx]; } else { uly = ucc * fadeS; vly = vcc * fadeS; }
+    if (gy < ny - 1) { upy = u[c + nx]; vpy = v[c + nx]; } else { upy = ucc * fadeN; vpy = vcc * fadeN; }
+    const double dUadv = (ucc + UINF0) * (upx - ulx) + (vcc + UINF1) * (upy - uly);
+    const double dUdif = upx + upy + ulx + uly - 4 * ucc;
+    const double dVadv = (ucc + UINF0) * (vpx - vlx) + (vcc + UINF1) * (vpy - vly);
+    const double dVdif = vpx + vpy + vlx + vly - 4 * vcc;
+    const double unew = ucc + (afac * dUadv + dfac * dUdif);
+    const double vnew = vcc + (afac * dVadv + dfac * dVdif);
+    un[c] = unew; vn[c] = vnew;
+    // advDiff.cpp:93-102: net outflow through the domain boundary
+    if (gx == 0) IF -= unew;
+    if (gx == nx - 1) IF += unew;
+    if (gy == 0) IF -= vnew;
+    if (gy == ny - 1) IF += vnew;
+  }
+  const bool edgeBlock = blockIdx.x == 0 || blockIdx.y == 0 ||
+                         blockIdx.x == gridDim.x - 1 || blockIdx.y == gridDim.y - 1;
+  const unsigned nb = gridDim.x * gridDim.y, bid = blockIdx.x + gridDim.x * blockIdx.y;
+  if (edgeBlock) {
+    double s[1] = {IF};
+    block_sum<1>(s, red);
+    if (threadIdx.x == 0 && threadIdx.y == 0) partials[bid] = s[0];
+  } else if (threadIdx.x == 0 && threadIdx.y == 0) {
+    partials[bid] = 0.0;
+  }
+  if (!last_block_done(counter, nb)) return;
+  const int tid = threadIdx.x + 32 * threadIdx.y;
+  double s[1] = {0.0};
+  for (unsigned i = tid; i < nb; i += 256) s[0] += partials[i];
+  block_sum<1>(s, red);
+  if (tid == 0)  // advDiff.cpp:105
+    scw->outflowCorr = s[0] / (2 * (BS * g.bpdy - 0) + 2 * (BS * g.bpdx - 0));
+}
+
+// advDiff.cpp:107-115
+__global__ void k_outflow(GridDesc g, const Scalars* sc, double* __restrict__ u, double* __restrict__ v)
+{
+  const double corr = sc->outflowCorr;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nx = g.nx, ny = g.ny;
+  if (i < ny) {
+    u[(size_t)i * nx] += corr;
+    u[(size_t)i * nx + nx - 1] -= corr;
+  }
+  if (i < nx) {
+    v[i] += corr;
+    v[(size_t)(ny - 1) * nx + i] -= corr;
+  }
+}
+
+// PressureSingle.cpp:112-128: tmp = (h / 2dt) * div_2h(u); zero-gradient ghosts
+__global__ void __launch_bounds__(256)
+k_rhs_div(GridDesc g, const Scalars* sc, const double* __restrict__ u,
+          const double* __restrict__ v, double* __restrict__ rhs)
+{
+  const double h = g.h, facDiv = 0.5 * h / sc->dt;
+  const int nx = g.nx, ny = g.ny;
+  const int gx = blockIdx.x * BS + threadIdx.x;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int gy = blockIdx.y * BS + threadIdx.y + 8 * r;
+    const size_t c = (size_t)gy * nx + gx;
+    const double uW = u[gx > 0 ? c - 1 : c], uE = u[gx < nx - 1 ? c + 1 : c];
+    const double vS = v[gy > 0 ? c - nx : c], vN = v[gy < ny - 1 ? c + nx : c];
+    const double divVx = uE - uW, divVy = vN - vS;
+    rhs[c] = facDiv * (divVx + divVy);
+  }
+}
+
+// PressureSingle.cpp:216-241: V += -(dt/2h) grad_2h P; zero-gradient P ghosts.
+// Reads the velocity written by advDiff (ui, vi) and writes the current one.
+__global__ void __launch_bounds__(256)
+k_pcorr(GridDesc g, const Scalars* sc, const double* __restrict__ p,
+        const double* __restrict__ ui, const double* __restrict__ vi,
+        double* __restrict__ uo, double* __restrict__ vo)
+{
+  const double pFac = -0.5 * sc->dt / g.h;
+  const int nx = g.nx, ny = g.ny;
+  const int gx = blockIdx.x * BS + threadIdx.x;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int gy = blockIdx.y * BS + threadIdx.y + 8 * r;
+    const size_t c = (size_t)gy * nx + gx;
+    const double pW = p[gx > 0 ? c - 1 : c], pE = p[gx < nx - 1 ? c + 1 : c];
+    const double pS = p[gy > 0 ? c - nx : c], pN = p[gy < ny - 1 ? c + nx : c];
+    uo[c] = ui[c] + pFac * (pE - pW);
+    vo[c] = vi[c] + pFac * (pN - pS);
+  }
+}
+
+// PoissonSolver.cpp:61-100: sums of the faded RHS over the boundary strip.
+// One CTA per block; blocks that do not touch the strip (the test of
+// PoissonSolver.cpp:71-79) contribute zero.
+__global__ void __launch_bounds__(256)
+k_fade_sums(GridDesc g, Scalars* sc, const double* __restrict__ rhs,
+            double* partials, unsigned* counter)
+{
+  __shared__ double red[96];
+  const int bx = blockIdx.x, by = blockIdx.y;
+  const unsigned nb = gridDim.x * gridDim.y, bid = bx + gridDim.x * by;
+  const double fadeLenX = g.fadeLenX, invFadeX = 1 / fmax(fadeLenX, EPSd);
+  const double fadeLenY = g.fadeLenY, invFadeY = 1 / fmax(fadeLenY, EPSd);
+  const double minx = cell_x(g, bx, 0), maxx = cell_x(g, bx, BS - 1);
+  const double miny = cell_y(g, by, 0), maxy = cell_y(g, by, BS - 1);
+  const bool touch = fadeLenX >= minx || fadeLenX >= g.ext[0] - maxx ||
+                     fadeLenY >= miny || fadeLenY >= g.ext[1] - maxy;
+  double s[3] = {0, 0, 0};   // sumRHS, sumPOS, sumNEG
+  if (touch) {
+    const int ix = threadIdx.x;
+    const double px = cell_x(g, bx, ix);
+    for (int r = 0; r < 4; r++) {
+      const int iy = threadIdx.y + 8 * r;
+      const double py = cell_y(g, by, iy);
+      const double yt = invFadeY * fmax(0.0, fadeLenY - g.ext[1] + py);
+      const double yb = invFadeY * fmax(0.0, fadeLenY - py);
+      const double xt = invFadeX * fmax(0.0, fadeLenX - g.ext[0] + px);
+      const double xb = invFadeX * fmax(0.0, fadeLenX - px);
+      const double fadeArg = fmin(fmax(fmax(yt, yb), fmax(xt, xb)), 1.0);
+      const double b = rhs[(size_t)(by * BS + iy) * g.nx + bx * BS + ix];
+      const double fadedRHS = b * (fadeArg * fadeArg);
+      if (fadedRHS < 0) s[2] -= fadedRHS;
+      if (fadedRHS > 0) s[1] += fadedRHS;
+      s[0] += fadedRHS;
+    }
+  }
+  block_sum<3>(s, red);
+  const int tid = threadIdx.x + 32 * threadIdx.y;
+  if (tid == 0) for (int k = 0; k < 3; k++) partials[3 * bid + k] = s[k];
+  if (!last_block_done(counter, nb)) return;
+  double t[3] = {0, 0, 0};
+  for (unsigned i = tid; i < nb; i += 256)
+    for (int k = 0; k < 3; k++) t[k] += partials[3 * i + k];
+  block_sum<3>(t, red);
+  if (tid == 0) {
+    const double sumNEG = fmax(t[2], EPSd), sumPOS = fmax(t[1], EPSd);
+    sc->fadeCorr = t[0] > 0 ? t[0] / sumPOS : t[0] / sumNEG;   // PoissonSolver.cpp:86
+  }
+}
+
+__global__ void k_ic(size_t n, double* u, double* v, double* chi, double* pres,
+                     double* rhs, double* sdf, double* udx, double* udy)
+{
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    u[i] = 0; v[i] = 0; chi[i] = 0; pres[i] = 0; rhs[i] = 0;
+    sdf[i] = -1; udx[i] = 0; udy[i] = 0;
+  }
+}
+
+// Helpers.cpp:290-307: u <- u (1 - chi) + udef chi
+__global__ void k_apply_obj_vel(size_t n, double* u, double* v, const double* chi,
+                                const double* udx, const double* udy)
+{
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double X = chi[i];
+    u[i] = u[i] * (1 - X) + udx[i] * X;
+    v[i] = v[i] * (1 - X) + udy[i] * X;
+  }
+}
+
+inline int reduce_grid(const Ctx& c) {
+  int n = (int)((c.ncells() + 255) / 256);
+  return n < 148 * 8 ? n : 148 * 8;
+}
+
+} // namespace
+
+void launch_max_u_dt(Ctx& c) {
+  const int nb = reduce_grid(c);
+  k_max_u_dt<<<nb, 256, 0, c.stream>>>(c.g, c.dsc, c.dshapes, c.nshapes, c.u(), c.v(),
+                                        c.partials, c.counters + CNT_MAXU);
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_set_dt(Ctx& c, double dt) {
+  k_set_dt<<<1, 1, 0, c.stream>>>(c.dsc, dt);
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_end_step(Ctx& c) {
+  k_end_step<<<1, 1, 0, c.stream>>>(c.dsc);
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_advdiff(Ctx& c) {
+  dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
+  k_advdiff<<<grid, block, 0, c.stream>>>(c.g, c.dsc, c.u(), c.v(), c.uo(), c.vo(),
+                                          c.partials, c.counters + CNT_ADV, c.dsc);
+  CUP2D_LAUNCHED(c);
+  c.cur = 1 - c.cur;   // advDiff.cpp:81-87: the new field becomes the velocity
+}
+
+// timing helpers: return the velocity to the buffer it came from (no launch)
+void launch_advdiff_undo(Ctx& c) { c.cur = 1 - c.cur; }
+void launch_pcorr_undo(Ctx& c) { c.cur = 1 - c.cur; }
+
+void launch_outflow(Ctx& c) {
+  const int n = c.g.nx > c.g.ny ? c.g.nx : c.g.ny;
+  k_outflow<<<(n + 255) / 256, 256, 0, c.stream>>>(c.g, c.dsc, c.u(), c.v());
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_rhs_div(Ctx& c) {
+  dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
+  k_rhs_div<<<grid, block, 0, c.stream>>>(c.g, c.dsc, c.u(), c.v(), c.rhs);
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_fade_sums(Ctx& c) {
+  dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
+  k_fade_sums<<<grid, block, 0, c.stream>>>(c.g, c.dsc, c.rhs, c.partials, c.counters + CNT_FADE);
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_pcorr(Ctx& c) {
+  dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
+  k_pcorr<<<grid, block, 0, c.stream>>>(c.g, c.dsc, c.pres, c.u(), c.v(), c.uo(), c.vo());
+  CUP2D_LAUNCHED(c);
+  c.cur = 1 - c.cur;
+}
+
+void launch_ic(Ctx& c) {
+  k_ic<<<reduce_grid(c), 256, 0, c.stream>>>(c.ncells(), c.u(), c.v(), c.chi, c.pres, c.rhs,
+                                              c.sdf, c.udefx, c.udefy);
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_apply_obj_vel(Ctx& c) {
+  k_apply_obj_vel<<<reduce_grid(c), 256, 0, c.stream>>>(c.ncells(), c.u(), c.v(), c.chi,
+                                                         c.udefx, c.udefy);
+  CUP2D_LAUNCHED(c);
+}
+
+} // namespace cup2d

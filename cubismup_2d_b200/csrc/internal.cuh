@@ -1,0 +1,206 @@
+// Internal device-side data model of the B200 pipeline.
+//
+// Layout (all in HBM, one context = one grid):
+//  - dense fields are row-major planes of Ny x Nx values (x fastest), one
+//    plane per component (SoA): u, v, chi, pres, rhs (the reference's "tmp"
+//    during PressureSingle), sdf (the reference's "tmp" during
+//    PutObjectsOnGrid).  Nx = 32*bpdx is a multiple of 32, so every row is a
+//    whole number of 256-byte (fp64) segments and every 32x32 reference block
+//    is the tile at (32*bx, 32*by).
+//  - obstacle data is sparse: per shape, a list of touched 32x32 tiles (the
+//    reference's obstacleBlocks[blockID] != nullptr, Shape.h:20) with a dense
+//    32x32 payload per tile (ObstacleBlock.h:25-31): chi, dist, udef and the
+//    surface delta/normal of putChiOnGrid.
+//  - scalars (time, dt, u_inf, ...) and rigid-body state live in device
+//    memory so a whole timestep needs no host round trip.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "../../include/cup2d.h"
+
+namespace cup2d {
+
+constexpr int BS = 32;            // _BS_ of the reference (Definitions.h:30-32)
+constexpr int BS2 = BS * BS;
+constexpr int MAX_SHAPES = 8;
+constexpr int NFORCE = 17;        // additive sums of ObstacleBlock.h:33-36
+
+// Device status flags (bit set = raised); cup2d_sync reports the first.
+enum : int { ST_NAN = 1, ST_DOMAIN = 2, ST_CAPACITY = 4 };
+
+struct GridDesc {
+  int nx, ny, bpdx, bpdy, nblocks;
+  double h, extent;
+  double ext[2];                  // SimulationData::extents (SimulationData.cpp:34-35)
+  double nu, CFL, dlm;
+  double fadeLenX, fadeLenY;
+};
+
+// Per-step scalars (SimulationData.h:45-49 plus values passed between kernels).
+struct Scalars {
+  double time, dt, uinfx, uinfy, lambda;
+  double maxU;
+  double outflowCorr;             // advDiff.cpp:105
+  double fadeCorr;                // PoissonSolver.cpp:86
+  int step;
+  int status;
+  double rampCFL[100];            // Simulation.cpp:266-267, host-evaluated
+};
+
+struct ShapeCfg {
+  int kind;
+  double rhoS;
+  int bFixedx, bFixedy, bForcedx, bForcedy, bBlockang;
+  double forcedu, forcedv, forcedomega, timeForced;
+  double origC[2], origAng;
+  double radius, tAccel;                          // Disk
+  double length, Tperiod, phaseShift, ampFac;     // Fish
+  int capacity;                                   // obstacle tile slots
+  int nm;                                         // fish midline points
+};
+
+// Fish frame bookkeeping (Fish.h:21-23).
+struct FishState {
+  double area_internal, J_internal;
+  double CoM_internal[2], vCoM_internal[2];
+  double theta_internal, angvel_internal, angvel_internal_prev;
+};
+
+struct DevShape {
+  cup2d_shape_state s;
+  ShapeCfg cfg;
+  FishState f;
+  int ntiles;                     // obstacle tiles this step
+  int ntilesPrev;
+  double rhoTile;                 // ObstacleBlock::rho: rhoS (disk), 1 (fish)
+  double rhsCorr;                 // PressureSingle.cpp:183-186 corr of this shape
+  double bbox[2][2];              // disk bounding box (ShapeLibrary.h:40-43)
+  int nseg;                       // fish AreaSegments this step
+};
+
+// One fish AreaSegment (FishLibrary.h:149-168) in the computational frame.
+struct Segment {
+  int first, second;              // s_range
+  double w[2], c[2];
+  double normalI[2], normalJ[2];
+  double boxLab[2][2], boxObj[2][2];
+};
+
+// Pointers to one shape's obstacle tiles (passed by value to kernels).
+struct ObstTiles {
+  int* tiles;                     // [capacity] block index of each slot
+  int* slot;                      // [nblocks] slot of each block or -1
+  double* chi;                    // [capacity][32][32]
+  double* dist;
+  double* udx;
+  double* udy;
+  double* sD;                     // surface delta D (0: not a surface point)
+  double* sdx;                    // dchidx = -D * gradUX (ObstacleBlock.h:98)
+  double* sdy;
+  int capacity;
+};
+
+// Fish midline arrays (FishLibrary.h:49-60) for one fish.
+struct FishArrays {
+  double* rS; double* rX; double* rY; double* vX; double* vY;
+  double* norX; double* norY; double* vNorX; double* vNorY; double* width;
+  double* rK; double* vK;                 // curvature and its rate (StefanFish.cpp:213-223)
+  double* p1f;                            // spline of the curvature control values at rS
+  Segment* seg;                           // [nseg]
+  int nm, nseg;
+};
+
+// ---- small device helpers ------------------------------------------------
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ int lin_tid() {
+  return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+}
+__device__ __forceinline__ int lin_nthreads() { return blockDim.x * blockDim.y * blockDim.z; }
+
+// Block-wide sum of K values per thread; result valid in linear thread 0.
+// smem must hold 32*K doubles.  Fixed reduction order: deterministic.
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K], double* smem) {
+  const int t = lin_tid(), lane = t & 31, wid = t >> 5;
+  const int nw = (lin_nthreads() + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < K; k++) v[k] = warp_sum(v[k]);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; k++) smem[wid * K + k] = v[k];
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      double x = lane < nw ? smem[lane * K + k] : 0.0;
+      v[k] = warp_sum(x);
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ double block_max(double v, double* smem) {
+  const int t = lin_tid(), lane = t & 31, wid = t >> 5;
+  const int nw = (lin_nthreads() + 31) >> 5;
+  v = warp_max(v);
+  __syncthreads();
+  if (lane == 0) smem[wid] = v;
+  __syncthreads();
+  if (wid == 0) v = warp_max(lane < nw ? smem[lane] : 0.0);
+  __syncthreads();
+  return v;
+}
+
+// "last block done" ticket: returns true in every thread of the CTA that
+// finished last.  The counter is re-armed by that CTA.
+__device__ __forceinline__ bool last_block_done(unsigned* counter, unsigned nblocks) {
+  __shared__ bool amLast;
+  __threadfence();
+  __syncthreads();
+  if (lin_tid() == 0) {
+    const unsigned t = atomicAdd(counter, 1u);
+    amLast = (t == nblocks - 1);
+    if (amLast) *counter = 0;
+  }
+  __syncthreads();
+  if (amLast) __threadfence();
+  return amLast;
+}
+
+// atomic max on doubles through the ordered-integer mapping of IEEE-754
+__device__ __forceinline__ void atomic_max_double(double* addr, double val) {
+  unsigned long long* a = reinterpret_cast<unsigned long long*>(addr);
+  unsigned long long old = *a, assumed;
+  do {
+    assumed = old;
+    if (__longlong_as_double(assumed) >= val) return;
+    old = atomicCAS(a, assumed, __double_as_longlong(val));
+  } while (old != assumed);
+}
+
+// Cell-centre position of cell (ix,iy) of block (bx,by); the same expression
+// as the oracle's BlockInfo::pos (origin + h*(i + 1/2), origin = 32*b*h).
+__device__ __forceinline__ double cell_x(const GridDesc& g, int bx, int ix) {
+  return (double)(bx * BS) * g.h + g.h * (ix + 0.5);
+}
+__device__ __forceinline__ double cell_y(const GridDesc& g, int by, int iy) {
+  return (double)(by * BS) * g.h + g.h * (iy + 0.5);
+}
+__device__ __forceinline__ double gx_pos(const GridDesc& g, int gx) {
+  return cell_x(g, gx >> 5, gx & 31);
+}
+__device__ __forceinline__ double gy_pos(const GridDesc& g, int gy) {
+  return cell_y(g, gy >> 5, gy & 31);
+}
+
+} // namespace cup2d

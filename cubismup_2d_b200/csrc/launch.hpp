@@ -1,0 +1,39 @@
+// Host-side launchers of the pipeline kernels (one per reference function).
+#pragma once
+#include "internal.cuh"
+
+namespace cup2d {
+
+struct Ctx;
+
+// fluid.cu
+void launch_max_u_dt(Ctx& c);                        // Helpers.cpp:136-176 + Simulation.cpp:254-277
+void launch_set_dt(Ctx& c, double dt);               // Operator::operator()(dt) argument
+void launch_advdiff(Ctx& c);                         // advDiff.cpp:36-87
+void launch_advdiff_undo(Ctx& c);
+void launch_pcorr_undo(Ctx& c);
+void launch_outflow(Ctx& c);                         // advDiff.cpp:89-116
+void launch_rhs_div(Ctx& c);                         // PressureSingle.cpp:112-128
+void launch_fade_sums(Ctx& c);                       // PoissonSolver.cpp:61-100
+void launch_pcorr(Ctx& c);                           // PressureSingle.cpp:216-241
+void launch_end_step(Ctx& c);                        // Simulation.cpp:289-290
+void launch_ic(Ctx& c);                              // Helpers.cpp:38-82
+void launch_apply_obj_vel(Ctx& c);                   // Helpers.cpp:290-307
+
+// obstacles.cu
+void launch_objects(Ctx& c);                         // PutObjectsOnGrid.cpp:186-241
+void launch_obj_vel_on_grid(Ctx& c);                 // PutObjectsOnGrid.cpp:149-184
+void launch_rhs_obstacles(Ctx& c);                   // PressureSingle.cpp:130-213
+void launch_momenta_penalize(Ctx& c);                // PressureSingle.cpp:23-108, 243-344, 362-372
+void launch_forces(Ctx& c);                          // ComputeForces.cpp:16-111
+
+// poisson.cu
+struct Poisson;
+Poisson* poisson_create(Ctx& c);
+void poisson_destroy(Poisson* p);
+void poisson_solve(Ctx& c);                          // PoissonSolver::solve of the chosen solver
+void poisson_rows_fwd(Ctx& c);
+void poisson_cols(Ctx& c);
+void poisson_rows_inv(Ctx& c);
+
+} // namespace cup2d

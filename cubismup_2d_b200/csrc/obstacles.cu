@@ -1,0 +1,688 @@
+// Obstacle kernels: PutObjectsOnGrid (body motion, obstacle tile lists,
+// disk signed distance, Towers chi and surface delta, moment removal), the
+// obstacle terms of PressureSingle (RHS source and perimeter correction,
+// momentum integrals + 3x3 rigid-body solve, collisions, penalization) and
+// ComputeForces.
+//
+// Obstacle work is sparse: each shape owns a list of touched 32x32 tiles
+// (the reference's obstacleBlocks), built on the device every step in
+// increasing block order.  Per-tile kernels run one CTA of 32x32 threads per
+// tile, one thread per cell, so every per-cell sequence of the reference
+// (including the "first writer wins" tests) is evaluated in the reference's
+// order; sums are block reductions per tile followed by a fixed-order sum
+// over tiles.
+#include <cmath>
+#include "context.hpp"
+#include "rigid_body.cuh"
+#include "fish.cuh"
+
+namespace cup2d {
+
+namespace {
+
+constexpr double EPSd = 2.220446049250313e-16;
+
+struct AllTiles { ObstTiles t[MAX_SHAPES]; };
+
+inline AllTiles all_tiles(const Ctx& c) {
+  AllTiles a{};
+  for (int k = 0; k < c.nshapes; k++) a.t[k] = c.tiles[k];
+  return a;
+}
+
+// ---------------------------------------------------------------------------
+// PutObjectsOnGrid.cpp:201-220: lab velocity from fixed bodies, then
+// Shape::updatePosition; a body whose centre leaves the domain raises
+// ST_DOMAIN (the reference exits).
+__global__ void k_obj_begin(GridDesc g, Scalars* sc, DevShape* sh, int nsh)
+{
+  if (threadIdx.x != 0) return;
+  const double dt = sc->dt;
+  int nSum[2] = {0, 0}; double uSum[2] = {0, 0};
+  for (int k = 0; k < nsh; k++) {                       // Shape::updateLabVelocity
+    if (sh[k].cfg.bFixedx) { nSum[0]++; uSum[0] -= sh[k].s.u; }
+    if (sh[k].cfg.bFixedy) { nSum[1]++; uSum[1] -= sh[k].s.v; }
+  }
+  if (nSum[0] > 0) sc->uinfx = uSum[0] / nSum[0];
+  if (nSum[1] > 0) sc->uinfy = uSum[1] / nSum[1];
+  for (int k = 0; k < nsh; k++) {
+    DevShape& S = sh[k];
+    shape_update_position(S, dt, sc->uinfx, sc->uinfy);
+    const double p0 = S.s.center[0], p1 = S.s.center[1];
+    if (p0 < 0 || p0 > g.ext[0] || p1 < 0 || p1 > g.ext[1]) atomicOr(&sc->status, ST_DOMAIN);
+    S.ntilesPrev = S.ntiles;
+    if (S.cfg.kind == CUP2D_SHAPE_DISK) {               // FillBlocks_Cylinder bbox
+      const double safety = 2 * g.h, R = S.cfg.radius;
+      S.bbox[0][0] = p0 - R - safety; S.bbox[0][1] = p0 + R + safety;
+      S.bbox[1][0] = p1 - R - safety; S.bbox[1][1] = p1 + R + safety;
+    }
+  }
+}
+
+// Reset the grid cells of last step's tiles: chi = 0 (PutObjectsOnGrid.cpp:193)
+// and sdf = -1 (:194); drop the slot mapping.
+__global__ void __launch_bounds__(256)
+k_clear_old(GridDesc g, const DevShape* sh, AllTiles T, double* chi, double* sdf)
+{
+  const int k = blockIdx.y, s = blockIdx.x;
+  if (s >= sh[k].ntilesPrev) return;
+  const ObstTiles& t = T.t[k];
+  const int b = t.tiles[s];
+  const int bx = b % g.bpdx, by = b / g.bpdx;
+  for (int i = threadIdx.x; i < BS2; i += blockDim.x) {
+    const size_t c = (size_t)(by * BS + i / BS) * g.nx + bx * BS + (i % BS);
+    chi[c] = 0; sdf[c] = -1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) t.slot[b] = -1;
+}
+
+__device__ __forceinline__ bool disk_touching(const GridDesc& g, const DevShape& S, int bx, int by) {
+  // _is_touching, ShapeLibrary.h:24-36
+  const double MINP0 = cell_x(g, bx, 0), MINP1 = cell_y(g, by, 0);
+  const double MAXP0 = cell_x(g, bx, BS - 1), MAXP1 = cell_y(g, by, BS - 1);
+  const double i00 = fmax(MINP0, S.bbox[0][0]), i01 = fmin(MAXP0, S.bbox[0][1]);
+  const double i10 = fmax(MINP1, S.bbox[1][0]), i11 = fmin(MAXP1, S.bbox[1][1]);
+  return i01 - i00 > 0 && i11 - i10 > 0;
+}
+
+// Deterministic compaction of the touched blocks, in increasing block order
+// (Disk::create, ShapesSimple.cpp:14-35; Fish::create, Fish.cpp:78-110).
+__global__ void __launch_bounds__(1024)
+k_tiles(GridDesc g, DevShape* sh, AllTiles T, FishSegPtrs segs, Scalars* sc)
+{
+  __shared__ int warpCount[32];
+  __shared__ int base;
+  const int k = blockIdx.x;
+  DevShape& S = sh[k];
+  const ObstTiles& t = T.t[k];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) base = 0;
+  __syncthreads();
+  for (int b0 = 0; b0 < g.nblocks; b0 += 1024) {
+    const int b = b0 + tid;
+    bool f = false;
+    if (b < g.nblocks) {
+      const int bx = b % g.bpdx, by = b / g.bpdx;
+      if (S.cfg.kind == CUP2D_SHAPE_DISK) f = disk_touching(g, S, bx, by);
+      else f = fish_block_touching(g, segs.seg[k], S.nseg, bx, by);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) warpCount[wid] = __popc(m);
+    __syncthreads();
+    int off = 0;
+    for (int w = 0; w < wid; w++) off += warpCount[w];
+    const int pos = base + off + __popc(m & ((1u << lane) - 1u));
+    if (f) {
+      if (pos < t.capacity) { t.tiles[pos] = b; t.slot[b] = pos; }
+      else atomicOr(&sc->status, ST_CAPACITY);
+    }
+    __syncthreads();
+    if (tid == 0) { int tot = 0; for (int w = 0; w < 32; w++) tot += warpCount[w]; base += tot; }
+    __syncthreads();
+  }
+  if (tid == 0) S.ntiles = base < t.capacity ? base : t.capacity;
+}
+
+// FillBlocks_Cylinder::operator() (ShapeLibrary.cpp:21-34): dist = R - |p - c|
+// on every cell of a touched block; tmp = max(tmp, dist); rho = rhoS.
+__global__ void __launch_bounds__(1024)
+k_raster_disk(GridDesc g, const DevShape* sh, AllTiles T, double* sdf)
+{
+  const int k = blockIdx.y, s = blockIdx.x;
+  const DevShape& S = sh[k];
+  if (S.cfg.kind != CUP2D_SHAPE_DISK || s >= S.ntiles) return;
+  const ObstTiles& t = T.t[k];
+  const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+  const int ix = threadIdx.x, iy = threadIdx.y, i = iy * BS + ix;
+  const double pos0 = S.s.center[0], pos1 = S.s.center[1];
+  const double x = cell_x(g, bx, ix) - pos0, y = cell_y(g, by, iy) - pos1;
+  const double dist = S.cfg.radius - sqrt(x * x + y * y);
+  const size_t o = (size_t)s * BS2 + i;
+  t.dist[o] = dist; t.chi[o] = 0; t.udx[o] = 0; t.udy[o] = 0;
+  atomic_max_double(&sdf[(size_t)(by * BS + iy) * g.nx + bx * BS + ix], dist);
+}
+
+// PutObjectsOnGrid::putChiOnGrid (PutObjectsOnGrid.cpp:17-124): Towers chi
+// from the shape's signed distance (ghosts from the max-SDF grid), chi grid
+// = max over shapes, CoM sums, and the surface delta list.
+__global__ void __launch_bounds__(1024)
+k_chi(GridDesc g, const DevShape* sh, AllTiles T, const double* __restrict__ sdfg,
+      double* chig, double* partials, int partStride)
+{
+  __shared__ double red[32 * 3];
+  __shared__ double tile[BS][BS + 1];
+  const int k = blockIdx.y, s = blockIdx.x;
+  const DevShape& S = sh[k];
+  double acc[3] = {0, 0, 0};
+  if (s < S.ntiles) {
+    const ObstTiles& t = T.t[k];
+    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+    const int ix = threadIdx.x, iy = threadIdx.y;
+    const size_t o = (size_t)s * BS2 + iy * BS + ix;
+    const double sdf = t.dist[o];
+    tile[iy][ix] = sdf;
+    __syncthreads();
+    const double h = g.h, i2h = 0.5 / h, fac = 0.5 * h;
+    const int gx = bx * BS + ix, gy = by * BS + iy;
+    auto G = [&](int x, int y) -> double {        // ScalarLab on tmp, zero-gradient
+      x = x < 0 ? 0 : (x >= g.nx ? g.nx - 1 : x);
+      y = y < 0 ? 0 : (y >= g.ny ? g.ny - 1 : y);
+      return sdfg[(size_t)y * g.nx + x];
+    };
+    const double distPx = ix + 1 == BS ? G(gx + 1, gy) : tile[iy][ix + 1];
+    const double distMx = ix == 0 ? G(gx - 1, gy) : tile[iy][ix - 1];
+    const double distPy = iy + 1 == BS ? G(gx, gy + 1) : tile[iy + 1][ix];
+    const double distMy = iy == 0 ? G(gx, gy - 1) : tile[iy - 1][ix];
+    double X;
+    if (sdf > +2 * h || sdf < -2 * h) {
+      X = sdf > 0 ? 1 : 0;
+    } else {
+      const double IplusX = distPx < 0 ? 0 : distPx, IminuX = distMx < 0 ? 0 : distMx;
+      const double IplusY = distPy < 0 ? 0 : distPy, IminuY = distMy < 0 ? 0 : distMy;
+      const double gradIX = i2h * (IplusX - IminuX), gradIY = i2h * (IplusY - IminuY);
+      const double gradUX = i2h * (distPx - distMx), gradUY = i2h * (distPy - distMy);
+      const double gradUSq = gradUX * gradUX + gradUY * gradUY;
+      const double denum = 1 / (gradUSq < EPSd ? EPSd : gradUSq);
+      X = (gradIX * gradUX + gradIY * gradUY) * denum;
+    }
+    t.chi[o] = X;
+    atomic_max_double(&chig[(size_t)gy * g.nx + gx], X);   // CHI = max over shapes (:69-73)
+    if (X > 0) {
+      const double rho = S.rhoTile;
+      const double p0 = cell_x(g, bx, ix), p1 = cell_y(g, by, iy);
+      acc[0] = rho * X * h * h * (p0 - S.s.com[0]);
+      acc[1] = rho * X * h * h * (p1 - S.s.com[1]);
+      acc[2] = rho * X * h * h;
+    }
+    double D = 0, sdx = 0, sdy = 0;
+    if (!(sdf > +2 * h || sdf < -2 * h)) {                   // :86-106 (shift = 0)
+      const double HplusX = fabs(distPx) < EPSd ? 0.5 : (distPx < 0 ? 0 : 1);
+      const double HminuX = fabs(distMx) < EPSd ? 0.5 : (distMx < 0 ? 0 : 1);
+      const double HplusY = fabs(distPy) < EPSd ? 0.5 : (distPy < 0 ? 0 : 1);
+      const double HminuY = fabs(distMy) < EPSd ? 0.5 : (distMy < 0 ? 0 : 1);
+      const double gradUX = i2h * (distPx - distMx), gradUY = i2h * (distPy - distMy);
+      const double gradHX = (HplusX - HminuX), gradHY = (HplusY - HminuY);
+      const double gradUSq = gradUX * gradUX + gradUY * gradUY;
+      const double denum = 1 / (gradUSq < EPSd ? EPSd : gradUSq);
+      const double Dv = fac * (gradHX * gradUX + gradHY * gradUY) * denum;
+      if (Dv > 0) { D = Dv; sdx = -Dv * gradUX; sdy = -Dv * gradUY; }  // ObstacleBlock::write
+    }
+    t.sD[o] = D; t.sdx[o] = sdx; t.sdy[o] = sdy;
+  }
+  block_sum<3>(acc, red);
+  if (lin_tid() == 0 && s < S.ntiles)
+    for (int q = 0; q < 3; q++) partials[(size_t)k * partStride + 3 * s + q] = acc[q];
+}
+
+// PutObjectsOnGrid.cpp:118-122 (CoM correction) + Shape::removeMoments
+// (Shape.cpp:117-212): one CTA per shape walks all of its tiles.
+__global__ void __launch_bounds__(1024)
+k_moments(GridDesc g, DevShape* sh, AllTiles T, const double* partials, int partStride)
+{
+  __shared__ double red[32 * 7];
+  __shared__ double bc[5];
+  const int k = blockIdx.x;
+  DevShape& S = sh[k];
+  const ObstTiles& t = T.t[k];
+  const int nt = S.ntiles, tid = threadIdx.x;
+  double a3[3] = {0, 0, 0};
+  for (int s = tid; s < nt; s += blockDim.x)
+    for (int q = 0; q < 3; q++) a3[q] += partials[(size_t)k * partStride + 3 * s + q];
+  block_sum<3>(a3, red);
+  if (tid == 0) {
+    if (a3[2] > EPSd) {
+      S.s.com[0] += a3[0] / a3[2];
+      S.s.com[1] += a3[1] / a3[2];
+      S.s.M = a3[2];
+    }
+    bc[0] = S.s.com[0]; bc[1] = S.s.com[1];
+  }
+  __syncthreads();
+  const double C0 = bc[0], C1 = bc[1];
+  const double hsq = g.h * g.h, rho = S.rhoTile;
+  double I[7] = {0, 0, 0, 0, 0, 0, 0};   // x, y, m, j, u, v, a
+  for (int s = 0; s < nt; s++) {
+    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+    const int ix = tid % BS, iy = tid / BS;
+    const size_t o = (size_t)s * BS2 + tid;
+    const double X = t.chi[o];
+    if (X <= 0) continue;
+    const double p0 = cell_x(g, bx, ix) - C0, p1 = cell_y(g, by, iy) - C1;
+    const double rhochi = X * rho * hsq;
+    const double ux = t.udx[o], uy = t.udy[o];
+    I[0] += rhochi * p0;
+    I[1] += rhochi * p1;
+    I[2] += rhochi;
+    I[3] += rhochi * (p0 * p0 + p1 * p1);
+    I[4] += rhochi * ux;
+    I[5] += rhochi * uy;
+    I[6] += rhochi * (p0 * uy - p1 * ux);
+  }
+  block_sum<7>(I, red);
+  if (tid == 0) {
+    const double Iu = I[4] / I[2], Iv = I[5] / I[2], Ia = I[6] / I[3];
+    S.s.M = I[2]; S.s.J = I[3];
+    const double dCx = S.s.center[0] - S.s.com[0], dCy = S.s.center[1] - S.s.com[1];
+    const double co = cos(S.s.orientation), si = sin(S.s.orientation);
+    S.s.d_gm[0] = dCx * co + dCy * si;
+    S.s.d_gm[1] = -dCx * si + dCy * co;
+    bc[2] = Iu; bc[3] = Iv; bc[4] = Ia;
+  }
+  __syncthreads();
+  const double Iu = bc[2], Iv = bc[3], Ia = bc[4];
+  for (int s = 0; s < nt; s++) {
+    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+    const int ix = tid % BS, iy = tid / BS;
+    const size_t o = (size_t)s * BS2 + tid;
+    const double p0 = cell_x(g, bx, ix) - C0, p1 = cell_y(g, by, iy) - C1;
+    t.udx[o] -= Iu - Ia * p1;
+    t.udy[o] -= Iv + Ia * p0;
+  }
+}
+
+// PutObjectsOnGrid::putObjectVelOnGrid (PutObjectsOnGrid.cpp:149-184), used at
+// reset for ApplyObjVel; one launch per shape, in shape order.
+__global__ void __launch_bounds__(1024)
+k_udef_grid(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* chig,
+            double* udx, double* udy)
+{
+  const int s = blockIdx.x;
+  if (s >= sh[k].ntiles) return;
+  const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+  const int ix = threadIdx.x, iy = threadIdx.y;
+  const size_t o = (size_t)s * BS2 + iy * BS + ix;
+  const size_t c = (size_t)(by * BS + iy) * g.nx + bx * BS + ix;
+  const double X = t.chi[o];
+  if (X < chig[c] || X <= 0) return;
+  udx[c] += t.udx[o];
+  udy[c] += t.udy[o];
+}
+
+// ---------------------------------------------------------------------------
+// PressureSingle::updatePressureRHS, per-shape source (PressureSingle.cpp:136-168)
+__global__ void __launch_bounds__(1024)
+k_rhs_obst(GridDesc g, DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
+           double* rhs, double* partials, unsigned* counter)
+{
+  __shared__ double red[32 * 3];
+  DevShape& S = sh[k];
+  const int s = blockIdx.x;
+  double acc[3] = {0, 0, 0};   // sumRHS, posRHS, negRHS
+  if (s < S.ntiles) {
+    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+    const int ix = threadIdx.x, iy = threadIdx.y;
+    const int gx = bx * BS + ix, gy = by * BS + iy;
+    auto CHI = [&](int x, int y) -> double {
+      x = x < 0 ? 0 : (x >= g.nx ? g.nx - 1 : x);
+      y = y < 0 ? 0 : (y >= g.ny ? g.ny - 1 : y);
+      return chig[(size_t)y * g.nx + x];
+    };
+    const double chi = t.chi[(size_t)s * BS2 + iy * BS + ix];
+    if (!(CHI(gx, gy) > chi)) {
+      const double gradXx = CHI(gx + 1, gy) - CHI(gx - 1, gy);
+      const double gradXy = CHI(gx, gy + 1) - CHI(gx, gy - 1);
+      const size_t c = (size_t)gy * g.nx + gx;
+      const double tmp0 = rhs[c];
+      const double srcBulk = -chi * tmp0;
+      acc[0] = srcBulk;
+      const double tmp = tmp0 + srcBulk;
+      rhs[c] = tmp;
+      const bool isPerim = gradXx * gradXx + gradXy * gradXy > 0;
+      if (isPerim && tmp > 0) acc[1] = tmp;
+      if (isPerim && tmp < 0) acc[2] = -tmp;
+    }
+  }
+  block_sum<3>(acc, red);
+  if (lin_tid() == 0) for (int q = 0; q < 3; q++) partials[3 * s + q] = acc[q];
+  if (!last_block_done(counter, gridDim.x)) return;
+  double tot[3] = {0, 0, 0};
+  const int n = S.ntiles;
+  for (int i = lin_tid(); i < n; i += 1024)
+    for (int q = 0; q < 3; q++) tot[q] += partials[3 * i + q];
+  block_sum<3>(tot, red);
+  if (lin_tid() == 0) {                                  // PressureSingle.cpp:185-186
+    const double corrDenom = tot[0] > 0 ? tot[1] : tot[2];
+    S.rhsCorr = tot[0] / fmax(corrDenom, EPSd);
+  }
+}
+
+// PressureSingle.cpp:173-212: perimeter correction of the same-sign RHS
+__global__ void __launch_bounds__(1024)
+k_rhs_corr(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
+           double* rhs)
+{
+  const DevShape& S = sh[k];
+  const int s = blockIdx.x;
+  if (s >= S.ntiles) return;
+  const double corr = S.rhsCorr;
+  const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+  const int ix = threadIdx.x, iy = threadIdx.y;
+  const int gx = bx * BS + ix, gy = by * BS + iy;
+  auto CHI = [&](int x, int y) -> double {
+    x = x < 0 ? 0 : (x >= g.nx ? g.nx - 1 : x);
+    y = y < 0 ? 0 : (y >= g.ny ? g.ny - 1 : y);
+    return chig[(size_t)y * g.nx + x];
+  };
+  const double chi = t.chi[(size_t)s * BS2 + iy * BS + ix];
+  if (CHI(gx, gy) > chi) return;
+  const double gradXx = CHI(gx + 1, gy) - CHI(gx - 1, gy);
+  const double gradXy = CHI(gx, gy + 1) - CHI(gx, gy - 1);
+  const bool isPerim = gradXx * gradXx + gradXy * gradXy > 0;
+  const size_t c = (size_t)gy * g.nx + gx;
+  const double tmp = rhs[c];
+  if (isPerim && tmp > 0 && corr > 0) rhs[c] = tmp - corr * tmp;
+  else if (isPerim && tmp < 0 && corr < 0) rhs[c] = tmp + corr * tmp;
+}
+
+// PressureSingle::integrateMomenta (PressureSingle.cpp:23-67) with the
+// EXPL_INTEGRATE_MOM weights (:20), then Shape::updateVelocity.
+__global__ void __launch_bounds__(1024)
+k_momenta(GridDesc g, const Scalars* sc, DevShape* sh, AllTiles T,
+          const double* __restrict__ u, const double* __restrict__ v)
+{
+  __shared__ double red[32 * 7];
+  const int k = blockIdx.x, tid = threadIdx.x;
+  DevShape& S = sh[k];
+  const ObstTiles& t = T.t[k];
+  const double Cx = S.s.com[0], Cy = S.s.com[1];
+  const double hsq = g.h * g.h, rho = S.rhoTile;
+  double A[7] = {0, 0, 0, 0, 0, 0, 0};   // PM, PJ, PX, PY, UM, VM, AM
+  for (int s = 0; s < S.ntiles; s++) {
+    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+    const int ix = tid % BS, iy = tid / BS;
+    const size_t o = (size_t)s * BS2 + tid;
+    const double chi = t.chi[o];
+    if (chi <= 0) continue;
+    const size_t c = (size_t)(by * BS + iy) * g.nx + bx * BS + ix;
+    const double ud0 = u[c] - t.udx[o], ud1 = v[c] - t.udy[o];
+    const double F = hsq * rho * chi;
+    const double p0 = cell_x(g, bx, ix) - Cx, p1 = cell_y(g, by, iy) - Cy;
+    A[0] += F;
+    A[1] += F * (p0 * p0 + p1 * p1);
+    A[2] += F * p0;
+    A[3] += F * p1;
+    A[4] += F * ud0;
+    A[5] += F * ud1;
+    A[6] += F * (p0 * ud1 - p1 * ud0);
+  }
+  block_sum<7>(A, red);
+  if (tid == 0) {
+    S.s.fluidAngMom = A[6]; S.s.fluidMomX = A[4]; S.s.fluidMomY = A[5];
+    S.s.penalDX = A[2]; S.s.penalDY = A[3]; S.s.penalM = A[0]; S.s.penalJ = A[1];
+    shape_update_velocity(S, sc->dt, sc->time);
+  }
+}
+
+// PressureSingle::preventCollidingObstacles (PressureSingle.cpp:243-344).
+// As in the reference, shape i's overlap sums accumulate over every j != i
+// before the impulses are applied once per j.
+__global__ void __launch_bounds__(1024)
+k_collide(GridDesc g, const Scalars* sc, DevShape* sh, int nsh, AllTiles T)
+{
+  __shared__ double red[32 * 10];
+  __shared__ double coll[MAX_SHAPES][10];
+  const int tid = threadIdx.x;
+  for (int i = 0; i < nsh; i++) {
+    double a[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int j = 0; j < nsh; j++) {
+      if (i == j) continue;
+      const DevShape& Si = sh[i]; const DevShape& Sj = sh[j];
+      const double iUl = Si.s.u, iVl = Si.s.v, iW = Si.s.omega;
+      const double jUl = Sj.s.u, jVl = Sj.s.v, jW = Sj.s.omega;
+      const double iCx = Si.s.com[0], iCy = Si.s.com[1], jCx = Sj.s.com[0], jCy = Sj.s.com[1];
+      for (int s = 0; s < Si.ntiles; s++) {
+        const int b = T.t[i].tiles[s];
+        const int sj = T.t[j].slot[b];
+        if (sj < 0) continue;
+        const int bx = b % g.bpdx, by = b / g.bpdx, ix = tid % BS, iy = tid / BS;
+        const double iChi = T.t[i].chi[(size_t)s * BS2 + tid], jChi = T.t[j].chi[(size_t)sj * BS2 + tid];
+        if (iChi <= 0 || jChi <= 0) continue;
+        const double p0 = cell_x(g, bx, ix), p1 = cell_y(g, by, iy);
+        const double iUr = -iW * (p1 - iCy), iVr = iW * (p0 - iCx);
+        const double jUr = -jW * (p1 - jCy), jVr = jW * (p0 - jCx);
+        a[0] += iChi; a[1] += iChi * p0; a[2] += iChi * p1;
+        a[3] += iChi * (iUl + iUr + T.t[i].udx[(size_t)s * BS2 + tid]);
+        a[4] += iChi * (iVl + iVr + T.t[i].udy[(size_t)s * BS2 + tid]);
+        a[5] += jChi; a[6] += jChi * p0; a[7] += jChi * p1;
+        a[8] += jChi * (jUl + jUr + T.t[j].udx[(size_t)sj * BS2 + tid]);
+        a[9] += jChi * (jVl + jVr + T.t[j].udy[(size_t)sj * BS2 + tid]);
+      }
+    }
+    block_sum<10>(a, red);
+    if (tid == 0) for (int q = 0; q < 10; q++) coll[i][q] = a[q];
+    __syncthreads();
+  }
+  if (tid != 0) return;
+  const double time = sc->time;
+  for (int i = 0; i < nsh; i++)
+  for (int j = 0; j < nsh; j++) {
+    if (i == j) continue;
+    const double* cl = coll[i];
+    if (cl[0] < 1 || cl[5] < 1) continue;
+    const double iPX = cl[1] / cl[0], iPY = cl[2] / cl[0];
+    const double iUX = cl[3] / cl[0], iUY = cl[4] / cl[0];
+    const double jPX = cl[6] / cl[5], jPY = cl[7] / cl[5];
+    const double jUX = cl[8] / cl[5], jUY = cl[9] / cl[5];
+    const double CX = (iPX + jPX) / 2, CY = (iPY + jPY) / 2;
+    const double dirX = iPX - jPX, dirY = iPY - jPY;
+    const double hitVelX = jUX - iUX, hitVelY = jUY - iUY;
+    const double normF = fmax(sqrt(dirX * dirX + dirY * dirY), EPSd);
+    const double NX = dirX / normF, NY = dirY / normF;
+    const double projVel = hitVelX * NX + hitVelY * NY;
+    if (projVel <= 0) continue;
+    DevShape& Si = sh[i]; const DevShape& Sj = sh[j];
+    const bool iForcedX = Si.cfg.bForcedx && time < Si.cfg.timeForced;
+    const bool iForcedY = Si.cfg.bForcedy && time < Si.cfg.timeForced;
+    const bool iForcedA = Si.cfg.bBlockang && time < Si.cfg.timeForced;
+    const bool jForcedX = Sj.cfg.bForcedx && time < Sj.cfg.timeForced;
+    const bool jForcedY = Sj.cfg.bForcedy && time < Sj.cfg.timeForced;
+    const double iInvMassX = iForcedX ? 0 : 1 / Si.s.M, iInvMassY = iForcedY ? 0 : 1 / Si.s.M;
+    const double jInvMassX = jForcedX ? 0 : 1 / Sj.s.M, jInvMassY = jForcedY ? 0 : 1 / Sj.s.M;
+    const double iInvJ = iForcedA ? 0 : 1 / Si.s.J;
+    const double meanMassX = 2 / fmax(iInvMassX + jInvMassX, EPSd);
+    const double meanMassY = 2 / fmax(iInvMassY + jInvMassY, EPSd);
+    const double FXdt = meanMassX * projVel * NX, FYdt = meanMassY * projVel * NY;
+    Si.s.u += FXdt * iInvMassX;
+    Si.s.v += FYdt * iInvMassY;
+    const double RcrossF = (CX - Si.s.com[0]) * FYdt - (CY - Si.s.com[1]) * FXdt;
+    Si.s.omega += iInvJ * RcrossF;
+  }
+}
+
+// PressureSingle::penalize (PressureSingle.cpp:69-108), alpha = 1 - chi
+__global__ void __launch_bounds__(1024)
+k_penalize(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
+           double* u, double* v)
+{
+  const DevShape& S = sh[k];
+  const int s = blockIdx.x;
+  if (s >= S.ntiles) return;
+  const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+  const int ix = threadIdx.x, iy = threadIdx.y;
+  const size_t o = (size_t)s * BS2 + iy * BS + ix;
+  const size_t c = (size_t)(by * BS + iy) * g.nx + bx * BS + ix;
+  const double X = t.chi[o];
+  if (chig[c] > X) return;
+  if (X <= 0) return;
+  const double p0 = cell_x(g, bx, ix) - S.s.com[0], p1 = cell_y(g, by, iy) - S.s.com[1];
+  const double alpha = 1 - X;
+  const double US = S.s.u - S.s.omega * p1 + t.udx[o];
+  const double VS = S.s.v + S.s.omega * p0 + t.udy[o];
+  u[c] = alpha * u[c] + (1 - alpha) * US;
+  v[c] = alpha * v[c] + (1 - alpha) * VS;
+}
+
+// ComputeForces::operator() (ComputeForces.cpp:16-111) + Shape::computeForces
+// (Shape.cpp:252-282): per surface point traction, 17 sums per tile, then
+// the fixed-order sum over tiles and the derived powers/efficiencies.
+__global__ void __launch_bounds__(1024)
+k_forces(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ u,
+         const double* __restrict__ v, const double* __restrict__ p,
+         double* partials, int partStride, unsigned* counters)
+{
+  __shared__ double red[32 * NFORCE];
+  const int k = blockIdx.y, s = blockIdx.x;
+  DevShape& S = sh[k];
+  const ObstTiles& t = T.t[k];
+  double F[NFORCE];
+#pragma unroll
+  for (int q = 0; q < NFORCE; q++) F[q] = 0;
+  if (s < S.ntiles) {
+    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+    const int ix = threadIdx.x, iy = threadIdx.y;
+    const size_t o = (size_t)s * BS2 + iy * BS + ix;
+    if (t.sD[o] > 0) {
+      const int gx = bx * BS + ix, gy = by * BS + iy;
+      auto I = [&](int x, int y) -> size_t {
+        x = x < 0 ? 0 : (x >= g.nx ? g.nx - 1 : x);
+        y = y < 0 ? 0 : (y >= g.ny ? g.ny - 1 : y);
+        return (size_t)y * g.nx + x;
+      };
+      const double NUoH = g.nu / g.h;
+      const double Cx = S.s.com[0], Cy = S.s.com[1];
+      const double vel_norm = sqrt(S.s.u * S.s.u + S.s.v * S.s.v);
+      const double vu0 = vel_norm > 0 ? S.s.u / vel_norm : 0.0;
+      const double vu1 = vel_norm > 0 ? S.s.v / vel_norm : 0.0;
+      const double p0 = cell_x(g, bx, ix), p1 = cell_y(g, by, iy);
+      const double D11 = NUoH * (u[I(gx + 1, gy)] - u[I(gx - 1, gy)]);
+      const double D22 = NUoH * (v[I(gx, gy + 1)] - v[I(gx, gy - 1)]);
+      const double D12 = NUoH / 2 * (u[I(gx, gy + 1)] - u[I(gx, gy - 1)]
+                                     + v[I(gx + 1, gy)] - v[I(gx - 1, gy)]);
+      const double normX = t.sdx[o], normY = t.sdy[o];
+      const double P = p[I(gx, gy)];
+      const double fXV = D11 * normX + D12 * normY, fXP = -P * normX;
+      const double fYV = D12 * normX + D22 * normY, fYP = -P * normY;
+      const double fXT = fXV + fXP, fYT = fYV + fYP;
+      const double vx = u[I(gx, gy)], vy = v[I(gx, gy)];
+      const double vxDef = t.udx[o], vyDef = t.udy[o];
+      F[0] = sqrt(normX * normX + normY * normY);          // perimeter
+      F[1] = fXT; F[2] = fYT;                               // forcex, forcey
+      F[3] = fXP; F[4] = fYP;                               // forcex_P, forcey_P
+      F[5] = fXV; F[6] = fYV;                               // forcex_V, forcey_V
+      F[7] = (p0 - Cx) * fYT - (p1 - Cy) * fXT;             // torque
+      F[8] = (p0 - Cx) * fYP - (p1 - Cy) * fXP;             // torque_P
+      F[9] = (p0 - Cx) * fYV - (p1 - Cy) * fXV;             // torque_V
+      const double forcePar = fXT * vu0 + fYT * vu1;
+      F[10] = -(.5 * (forcePar - fabs(forcePar)));          // drag
+      F[11] = .5 * (forcePar + fabs(forcePar));             // thrust
+      F[12] = normX * vy - normY * vx;                      // circulation
+      const double powOut = fXT * vx + fYT * vy;
+      const double powDef = fXT * vxDef + fYT * vyDef;
+      F[13] = powOut;                                       // Pout
+      F[14] = fmin(0.0, powOut);                            // PoutBnd
+      F[15] = powDef;                                       // defPower
+      F[16] = fmin(0.0, powDef);                            // defPowerBnd
+    }
+  }
+  block_sum<NFORCE>(F, red);
+  double* part = partials + (size_t)k * partStride;
+  if (lin_tid() == 0) for (int q = 0; q < NFORCE; q++) part[NFORCE * s + q] = F[q];
+  if (!last_block_done(counters + k, gridDim.x)) return;
+  double tot[NFORCE];
+#pragma unroll
+  for (int q = 0; q < NFORCE; q++) tot[q] = 0;
+  for (int i = lin_tid(); i < S.ntiles; i += 1024)
+    for (int q = 0; q < NFORCE; q++) tot[q] += part[NFORCE * i + q];
+  block_sum<NFORCE>(tot, red);
+  if (lin_tid() != 0) return;
+  cup2d_shape_state& st = S.s;
+  st.perimeter = tot[0]; st.forcex = tot[1]; st.forcey = tot[2];
+  st.forcex_P = tot[3]; st.forcey_P = tot[4]; st.forcex_V = tot[5]; st.forcey_V = tot[6];
+  st.torque = tot[7]; st.torque_P = tot[8]; st.torque_V = tot[9];
+  st.drag = tot[10]; st.thrust = tot[11]; st.circulation = tot[12];
+  st.Pout = tot[13]; st.PoutBnd = tot[14]; st.defPower = tot[15]; st.defPowerBnd = tot[16];
+  const double un = sqrt(st.u * st.u + st.v * st.v);
+  st.Pthrust = st.thrust * un;
+  st.Pdrag = st.drag * un;
+  const double denUnb = st.Pthrust - fmin(st.defPower, 0.0);
+  const double demBnd = st.Pthrust - st.defPowerBnd;
+  st.EffPDef = st.Pthrust / fmax(denUnb, EPSd);
+  st.EffPDefBnd = st.Pthrust / fmax(demBnd, EPSd);
+}
+
+inline size_t shape_region(const Ctx& c) { return (size_t)c.maxCapacity * 24; }
+inline double* shape_partials(const Ctx& c) { return c.partials + (size_t)3 * c.g.nblocks + 4096; }
+
+} // namespace
+
+void launch_objects(Ctx& c) {
+  if (c.nshapes == 0) return;
+  const AllTiles T = all_tiles(c);
+  const int cap = c.maxCapacity;
+  k_obj_begin<<<1, 32, 0, c.stream>>>(c.g, c.dsc, c.dshapes, c.nshapes);
+  CUP2D_LAUNCHED(c);
+  k_clear_old<<<dim3(cap, c.nshapes), 256, 0, c.stream>>>(c.g, c.dshapes, T, c.chi, c.sdf);
+  CUP2D_LAUNCHED(c);
+  // fish midlines, frames and AreaSegments (Fish::create, Fish.cpp:20-110)
+  for (int k = 0; k < c.nshapes; k++)
+    if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_kinematics(c, k);
+  k_tiles<<<c.nshapes, 1024, 0, c.stream>>>(c.g, c.dshapes, T, fish_seg_ptrs(c), c.dsc);
+  CUP2D_LAUNCHED(c);
+  bool anyDisk = false, anyFish = false;
+  for (int k = 0; k < c.nshapes; k++) {
+    if (c.hshapes[k].cfg.kind == CUP2D_SHAPE_DISK) anyDisk = true; else anyFish = true;
+  }
+  if (anyDisk) {
+    k_raster_disk<<<dim3(cap, c.nshapes), dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, T, c.sdf);
+    CUP2D_LAUNCHED(c);
+  }
+  if (anyFish)
+    for (int k = 0; k < c.nshapes; k++)
+      if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_raster(c, k);
+  const int stride = (int)shape_region(c);
+  k_chi<<<dim3(cap, c.nshapes), dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, T, c.sdf, c.chi,
+                                                              shape_partials(c), stride);
+  CUP2D_LAUNCHED(c);
+  k_moments<<<c.nshapes, 1024, 0, c.stream>>>(c.g, c.dshapes, T, shape_partials(c), stride);
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_obj_vel_on_grid(Ctx& c) {
+  for (int k = 0; k < c.nshapes; k++) {
+    k_udef_grid<<<c.tiles[k].capacity, dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
+                                                                   c.chi, c.udefx, c.udefy);
+    CUP2D_LAUNCHED(c);
+  }
+}
+
+void launch_rhs_obstacles(Ctx& c) {
+  for (int k = 0; k < c.nshapes; k++) {
+    k_rhs_obst<<<c.tiles[k].capacity, dim3(32, 32), 0, c.stream>>>(
+        c.g, c.dshapes, k, c.tiles[k], c.chi, c.rhs, shape_partials(c) + (size_t)k * shape_region(c),
+        c.counters + CNT_RHSOBST + k);
+    CUP2D_LAUNCHED(c);
+  }
+  for (int k = 0; k < c.nshapes; k++) {
+    k_rhs_corr<<<c.tiles[k].capacity, dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
+                                                                  c.chi, c.rhs);
+    CUP2D_LAUNCHED(c);
+  }
+}
+
+void launch_momenta_penalize(Ctx& c) {
+  if (c.nshapes == 0) return;
+  const AllTiles T = all_tiles(c);
+  k_momenta<<<c.nshapes, 1024, 0, c.stream>>>(c.g, c.dsc, c.dshapes, T, c.u(), c.v());
+  CUP2D_LAUNCHED(c);
+  if (c.nshapes > 1) {
+    k_collide<<<1, 1024, 0, c.stream>>>(c.g, c.dsc, c.dshapes, c.nshapes, T);
+    CUP2D_LAUNCHED(c);
+  }
+  for (int k = 0; k < c.nshapes; k++) {
+    k_penalize<<<c.tiles[k].capacity, dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
+                                                                  c.chi, c.u(), c.v());
+    CUP2D_LAUNCHED(c);
+  }
+}
+
+void launch_forces(Ctx& c) {
+  if (c.nshapes == 0) return;
+  const AllTiles T = all_tiles(c);
+  k_forces<<<dim3(c.maxCapacity, c.nshapes), dim3(32, 32), 0, c.stream>>>(
+      c.g, c.dshapes, T, c.u(), c.v(), c.pres, shape_partials(c), (int)shape_region(c),
+      c.counters + CNT_FORCES);
+  CUP2D_LAUNCHED(c);
+}
+
+} // namespace cup2d

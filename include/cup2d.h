@@ -1,0 +1,184 @@
+/*
+ * cup2d.h -- C ABI of the B200-native CubismUP_2D timestep pipeline.
+ *
+ * The reference has no foreign-function interface: its plugin points are the
+ * C++ classes Operator (Operator.h:14-27, one virtual operator()(double dt)
+ * per pipeline stage), Shape (Shape.h:15-191) and SimulationData
+ * (SimulationData.h:17-116), driven by Simulation::advance
+ * (Simulation.cpp:279-305).  Each entry point below replaces one of those
+ * calls; the C++ drop-in Operator subclasses that forward to them are shown
+ * in INTEGRATION.md.
+ *
+ * Conventions
+ *  - every function returns an int status: CUP2D_OK (0) or a CUP2D_E* code;
+ *    cup2d_last_error() gives the message.  Nothing aborts or exits.
+ *  - a context owns one grid, its shapes and one CUDA stream; calls on one
+ *    context come from one host thread.
+ *  - all field and shape state is device-resident; stage calls only enqueue
+ *    work on the context's stream.  Host copies happen only in the
+ *    cup2d_get_* / cup2d_set_* calls (which synchronise).
+ *  - fields cross the ABI as row-major Ny x Nx doubles (x fastest), i.e. the
+ *    reference's blocks placed at (index[0]*32, index[1]*32).
+ */
+#ifndef CUP2D_H
+#define CUP2D_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUP2D_OK 0
+#define CUP2D_EINVAL 1       /* bad argument or configuration               */
+#define CUP2D_ECUDA 2        /* CUDA runtime error                          */
+#define CUP2D_ENAN 3         /* non-finite value detected (Helpers.cpp:178)  */
+#define CUP2D_EDOMAIN 4      /* body left the domain (PutObjectsOnGrid.cpp:214) */
+#define CUP2D_ECAPACITY 5    /* obstacle tiles exceed the preallocated slots */
+#define CUP2D_ENOTSUP 6      /* feature outside this build                  */
+#define CUP2D_ESTATE 7       /* call out of order (e.g. before init)        */
+#define CUP2D_ENOMEM 8       /* device allocation failed                    */
+
+/* Poisson solver selection, Poisson/PoissonSolver.cpp:23-59 (makeSolver) */
+#define CUP2D_POISSON_FREESPACE 0   /* "freespace": FFTW_freespace.cpp        */
+#define CUP2D_POISSON_PERIODIC 1    /* "periodic" : FFTW_periodic.h           */
+#define CUP2D_POISSON_COSINE 2      /* "" (default): FFTW_dirichlet.h (DCT)   */
+
+/* arithmetic of the grid fields and of the Poisson solve */
+#define CUP2D_PREC_FP64 0
+#define CUP2D_PREC_FP32 1
+
+/* field identifiers for cup2d_get_field / cup2d_set_field
+ * (SimulationData.h:21-35) */
+#define CUP2D_FIELD_U 0
+#define CUP2D_FIELD_V 1
+#define CUP2D_FIELD_CHI 2
+#define CUP2D_FIELD_PRES 3
+#define CUP2D_FIELD_TMP 4       /* pressure RHS after PressureSingle        */
+#define CUP2D_FIELD_UDEF_X 5    /* deformation velocity on the grid          */
+#define CUP2D_FIELD_UDEF_Y 6
+#define CUP2D_FIELD_SDF 7       /* max signed distance of all shapes         */
+
+/* Simulation parameters: the runtime arguments parsed by
+ * Simulation::parseRuntime (Simulation.cpp:66-104). */
+typedef struct cup2d_config {
+  int bpdx, bpdy;          /* blocks of 32x32 cells per direction (-bpdx/-bpdy) */
+  double extent;           /* -extent (default 1)                               */
+  double CFL;              /* -CFL (default 0.1)                                */
+  double lambda;           /* -lambda (default 1e3/CFL)                         */
+  double dlm;              /* -dlm (default 0)                                  */
+  double nu;               /* -nu (default 1e-2)                                */
+  double fadeLen;          /* -fadeLen (default 0.01), times extent             */
+  int nsteps;              /* -nsteps (0: inactive)                             */
+  double tend;             /* -tend (0: inactive)                               */
+  int poisson;             /* CUP2D_POISSON_*                                   */
+  int precision;           /* CUP2D_PREC_*                                      */
+  int device;              /* CUDA device ordinal                               */
+} cup2d_config;
+
+/* Shape descriptors (the key=value parameters of Shape.cpp:331-345,
+ * ShapesSimple.h:19-22, Fish.h:27-29, StefanFish.cpp:246-293). */
+typedef struct cup2d_shape_params {
+  double xpos, ypos;       /* -xpos/-ypos                                      */
+  double angle;            /* -angle in degrees                                */
+  double rhoS;             /* -rhoS (1)                                        */
+  int bFixed, bFixedx, bFixedy;      /* -1 means "default" as in Shape.cpp     */
+  int bForced, bForcedx, bForcedy, bBlockAng;
+  double xvel, yvel, angvel;         /* forcedu = -xvel etc (Shape.cpp:342)    */
+  double timeForced;       /* default: +inf                                    */
+  /* disk */
+  double radius;           /* -radius (0.1)                                    */
+  double tAccel;           /* -tAccel (-1)                                     */
+  /* fish */
+  double L, T, phi;        /* -L (0.1), -T (1), -phi (0)                       */
+  double amplitudeFactor;  /* -amplitudeFactor (1)                             */
+} cup2d_shape_params;
+
+#define CUP2D_SHAPE_DISK 0
+#define CUP2D_SHAPE_STEFANFISH 1
+#define CUP2D_SHAPE_CARLINGFISH 2
+
+/* Rigid-body state and force sums of one shape, in the order of
+ * Shape.h:22-62 (42 doubles). */
+typedef struct cup2d_shape_state {
+  double center[2], com[2], orientation, u, v, omega, M, J, d_gm[2], lab_com[2];
+  double penalM, penalJ, penalDX, penalDY, fluidMomX, fluidMomY, fluidAngMom;
+  double perimeter, forcex, forcey, forcex_P, forcey_P, forcex_V, forcey_V;
+  double torque, torque_P, torque_V, drag, thrust, circulation;
+  double Pout, PoutBnd, defPower, defPowerBnd, Pthrust, Pdrag, EffPDef, EffPDefBnd;
+} cup2d_shape_state;
+
+typedef struct cup2d_ctx cup2d_ctx;
+
+/* ---- lifetime --------------------------------------------------------- */
+/* Fills *cfg with the defaults of Simulation::parseRuntime. */
+int cup2d_config_default(cup2d_config* cfg);
+/* SimulationData::allocateGrid (SimulationData.cpp:17-47) + solver setup
+ * (PressureSingle ctor -> PoissonSolver::makeSolver). */
+int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out);
+int cup2d_destroy(cup2d_ctx* ctx);
+const char* cup2d_last_error(const cup2d_ctx* ctx);
+/* Simulation::createShapes (Simulation.cpp:106-173), one shape per call.   */
+int cup2d_shape_params_default(cup2d_shape_params* p);
+int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* id);
+/* Simulation::init's tail + reset (Simulation.cpp:180-241): IC, objects at
+ * t=0, ApplyObjVel.  Must follow the last cup2d_add_shape. */
+int cup2d_init(cup2d_ctx* ctx);
+
+/* ---- the pipeline (Simulation::advance order) ------------------------- */
+/* Simulation::calcMaxTimestep (Simulation.cpp:254-277) incl. findMaxU
+ * (Helpers.cpp:136-176).  dt stays on the device; if dt_out is non-NULL the
+ * call synchronises and returns it. */
+int cup2d_calc_dt(cup2d_ctx* ctx, double* dt_out);
+/* One Operator::operator()(dt) each.  dt < 0 means "use the device dt from
+ * cup2d_calc_dt"; dt >= 0 overrides it, as the reference's argument does.  */
+int cup2d_put_objects(cup2d_ctx* ctx, double dt);      /* PutObjectsOnGrid.cpp:186-241 */
+int cup2d_adv_diff(cup2d_ctx* ctx, double dt);         /* advDiff.cpp:36-118            */
+int cup2d_pressure_single(cup2d_ctx* ctx, double dt);  /* PressureSingle.cpp:346-373    */
+int cup2d_compute_forces(cup2d_ctx* ctx, double dt);   /* ComputeForces.cpp:16-111      */
+/* time += dt; step++ (Simulation.cpp:289-290). */
+int cup2d_end_step(cup2d_ctx* ctx);
+/* calc_dt + the four operators + end_step, i.e. one pass of
+ * Simulation::simulate's loop; replayed from a captured CUDA graph after the
+ * first call.  nsteps steps are enqueued without host synchronisation. */
+int cup2d_advance(cup2d_ctx* ctx, int nsteps);
+/* Blocks until queued work finished; returns the first device status flag
+ * raised (CUP2D_ENAN, CUP2D_EDOMAIN, CUP2D_ECAPACITY) or CUP2D_OK. */
+int cup2d_sync(cup2d_ctx* ctx);
+
+/* ---- state exchange --------------------------------------------------- */
+int cup2d_get_field(cup2d_ctx* ctx, int which, double* host_out);
+int cup2d_set_field(cup2d_ctx* ctx, int which, const double* host_in);
+int cup2d_get_shape(cup2d_ctx* ctx, int id, cup2d_shape_state* out);
+int cup2d_set_shape(cup2d_ctx* ctx, int id, const cup2d_shape_state* in);
+/* time, dt, step, uinf (SimulationData.h:45-49) */
+int cup2d_get_scalars(cup2d_ctx* ctx, double* time, double* dt, int* step,
+                      double* uinfx, double* uinfy);
+int cup2d_set_scalars(cup2d_ctx* ctx, double time, double dt, int step,
+                      double uinfx, double uinfy);
+int cup2d_grid_size(const cup2d_ctx* ctx, int* nx, int* ny, double* h);
+/* Number of kernels this context launched since creation (every launch,
+ * including those replayed inside CUDA graphs). */
+int cup2d_kernel_launches(const cup2d_ctx* ctx, long long* count);
+
+/* Measurement hook (no reference counterpart): launches one pipeline kernel
+ * `reps` times back to back on the context's stream between two CUDA events
+ * and returns the mean milliseconds per launch.  The kernels re-read and
+ * re-write their own buffers, so state stays valid but is not a physical
+ * step.  which: CUP2D_KERNEL_*. */
+#define CUP2D_KERNEL_ADVDIFF 0
+#define CUP2D_KERNEL_RHS_DIV 1
+#define CUP2D_KERNEL_PCORR 2
+#define CUP2D_KERNEL_FFT_ROWS_FWD 3
+#define CUP2D_KERNEL_FFT_COLS 4
+#define CUP2D_KERNEL_FFT_ROWS_INV 5
+#define CUP2D_KERNEL_MAX_U 6
+#define CUP2D_KERNEL_OBJECTS 7
+int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, double* ms_per_launch);
+/* Measurement hook (no reference counterpart): cup2d_advance(ctx, nsteps)
+ * bracketed by CUDA events on the context's stream; returns the elapsed
+ * milliseconds (synchronises). */
+int cup2d_advance_timed(cup2d_ctx* ctx, int nsteps, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUP2D_H */
