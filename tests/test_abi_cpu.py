@@ -1,0 +1,61 @@
+"""CPU-only checks of the C ABI library: it loads without a GPU and exports
+every entry point that include/cup2d.h declares."""
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "cup2d.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\**\s+\**(cup2d_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    from cubismup_2d_b200 import abi
+    abi.lib()
+    out = subprocess.run(["nm", "-D", "--defined-only", abi.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT (cup2d_\w+)", out))
+    declared = declared_functions()
+    assert declared, "no declarations parsed"
+    missing = [f for f in declared if f not in exported]
+    assert not missing, missing
+    assert set(abi.EXPORTS) <= exported
+
+
+def test_context_creation_fails_loudly_without_gpu():
+    from cubismup_2d_b200 import Simulation, Cup2DError
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    sim = Simulation("-bpdx 2 -bpdy 1 -poissonType freespace -shapes 'disk radius=0.1'")
+    with pytest.raises(Cup2DError):
+        sim.init()
+
+
+def test_argument_parsing_follows_parse_runtime():
+    from cubismup_2d_b200 import parse_args
+    cfg, shapes = parse_args("-bpdx 16 -bpdy 8 -nu 1.5e-4 -poissonType freespace "
+                             "-shapes 'disk radius=0.0375 xpos=0.2 ypos=0.25 bForced=1 bFixed=1 xvel=0.2,"
+                             "stefanfish L=0.2 T=1'")
+    assert (cfg.bpdx, cfg.bpdy) == (16, 8)
+    assert cfg.CFL == 0.1 and cfg.lambda_ == 1e3 / 0.1 and cfg.extent == 1   # Simulation.cpp:92-93
+    assert cfg.fadeLen == 0.01 and cfg.poisson == 0
+    assert [k for k, _ in shapes] == [0, 1]
+    d = shapes[0][1]
+    assert d.radius == 0.0375 and d.xvel == 0.2 and d.bForced == 1 and d.bFixed == 1
+    f = shapes[1][1]
+    assert f.L == 0.2 and f.T == 1
+
+
+def test_missing_grid_arguments_are_an_error():
+    from cubismup_2d_b200 import parse_args, Cup2DError
+    with pytest.raises(Cup2DError):
+        parse_args("-nu 1e-3")
