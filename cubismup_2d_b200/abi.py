@@ -19,9 +19,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcup2d.so")
 
-OK, EINVAL, ECUDA, ENAN, EDOMAIN, ECAPACITY, ENOTSUP, ESTATE, ENOMEM = range(9)
+OK, EINVAL, ECUDA, ENAN, EDOMAIN, ECAPACITY, ENOTSUP, ESTATE, ENOMEM, ETOOLARGE = range(10)
 ERRORS = {EINVAL: "EINVAL", ECUDA: "ECUDA", ENAN: "ENAN", EDOMAIN: "EDOMAIN",
-          ECAPACITY: "ECAPACITY", ENOTSUP: "ENOTSUP", ESTATE: "ESTATE", ENOMEM: "ENOMEM"}
+          ECAPACITY: "ECAPACITY", ENOTSUP: "ENOTSUP", ESTATE: "ESTATE", ENOMEM: "ENOMEM",
+          ETOOLARGE: "ETOOLARGE"}
 POISSON = {"freespace": 0, "periodic": 1, "": 2, "cosine": 2}
 PREC_FP64, PREC_FP32 = 0, 1
 FIELDS = {"u": 0, "v": 1, "chi": 2, "pres": 3, "tmp": 4, "udef_x": 5, "udef_y": 6, "sdf": 7}
@@ -35,6 +36,7 @@ EXPORTS = [
     "cup2d_end_step", "cup2d_advance", "cup2d_sync", "cup2d_get_field", "cup2d_set_field",
     "cup2d_get_shape", "cup2d_set_shape", "cup2d_get_scalars", "cup2d_set_scalars",
     "cup2d_grid_size", "cup2d_kernel_launches", "cup2d_time_kernel", "cup2d_advance_timed",
+    "cup2d_adv_diff_noalloc",
 ]
 KERNELS = {"advdiff": 0, "rhs_div": 1, "pcorr": 2, "fft_rows_fwd": 3, "fft_cols": 4,
            "fft_rows_inv": 5, "max_u": 6, "objects": 7}
@@ -110,6 +112,7 @@ def lib():
     L.cup2d_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.cup2d_time_kernel.argtypes = [vp, i, i, dp]
     L.cup2d_advance_timed.argtypes = [vp, i, dp]
+    L.cup2d_adv_diff_noalloc.argtypes = [vp, vp, vp, vp, i, i, d, d, d, d, d, vp]
     for name in EXPORTS:
         if name != "cup2d_last_error":
             getattr(L, name).restype = ctypes.c_int

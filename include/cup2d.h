@@ -178,6 +178,33 @@ int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, double* ms_per_launch
  * milliseconds (synchronises). */
 int cup2d_advance_timed(cup2d_ctx* ctx, int nsteps, double* ms);
 
+/* ---- allocation-free advDiff ------------------------------------------ */
+/* This entry point has no counterpart in the reference.  It is advDiff
+ * (advDiff.cpp:36-118: explicit Euler step of central advection and 5-point
+ * diffusion, inflow-fade ghosts, boundary outflow correction) applied to
+ * device buffers the caller owns, for callers that cannot allocate device
+ * memory: hosts whose own pool or caching allocator owns the GPU's memory,
+ * and latency-critical loops that must not call cudaMalloc/cudaFree (they
+ * synchronise the device).  It allocates nothing; its reduction scratch is
+ * one fixed device array inside the library (about 128 KB, held on every GPU
+ * that loads the library until exit).
+ *  - u, v: current velocity, u_out, v_out: result; row-major
+ *    (32 bpdy) x (32 bpdx) doubles on the current device; the outputs must
+ *    not alias the inputs.  h, nu, dt, uinf as in SimulationData.
+ *  - grids of more than CUP2D_NOALLOC_MAX_BLOCKS blocks return
+ *    CUP2D_ETOOLARGE without launching anything.
+ *  - the first call on a device looks up the scratch address on that device
+ *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - calls share the scratch: calls that overlap on the GPU race and give
+ *    wrong results; serialise them (one stream, or events).
+ *  - stream: a cudaStream_t (NULL = legacy default stream); the call only
+ *    enqueues work. */
+#define CUP2D_ETOOLARGE 9
+#define CUP2D_NOALLOC_MAX_BLOCKS 16384
+int cup2d_adv_diff_noalloc(const double* u, const double* v, double* u_out, double* v_out,
+                           int bpdx, int bpdy, double h, double nu, double dt,
+                           double uinfx, double uinfy, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
