@@ -129,18 +129,50 @@ void invalidate_graph(Ctx& c) {
 }
 
 // one pass of Simulation::simulate's loop body (Simulation.cpp:245-251)
+// Routes the launches of one scope to another stream (graph branch).
+struct StreamScope {
+  Ctx& c; cudaStream_t saved;
+  StreamScope(Ctx& cc, cudaStream_t s) : c(cc), saved(cc.stream) { c.stream = s; }
+  ~StreamScope() { c.stream = saved; }
+};
+
+// One pass of Simulation::simulate's loop body (Simulation.cpp:245-251) as a
+// graph with three branches:
+//   main : dt -> body motion -> advDiff, outflow, RHS divergence ->
+//          [join obstacles] -> RHS obstacle terms, fade, Poisson, pressure
+//          correction, momenta, penalization, forces -> [join midline] -> t += dt
+//   side : the fish midlines of the next step (they depend on time only)
+//   side2: obstacle tiles, SDF, Towers chi, moments (advDiff does not read them)
 void enqueue_step(Ctx& c) {
   launch_max_u_dt(c);
-  launch_objects(c);
+  bool anyFish = false;
+  for (int k = 0; k < c.nshapes; k++) anyFish |= c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK;
+  if (anyFish) {
+    cudaEventRecord(c.evFork, c.stream);
+    cudaStreamWaitEvent(c.side, c.evFork, 0);
+    for (int k = 0; k < c.nshapes; k++)
+      if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.side, 1);
+    cudaEventRecord(c.evJoin, c.side);
+  }
+  launch_objects_begin(c, /*midlineReady=*/true);
+  cudaEventRecord(c.evObj, c.stream);
+  cudaStreamWaitEvent(c.side2, c.evObj, 0);
+  {
+    StreamScope scope(c, c.side2);
+    launch_objects_rest(c);
+  }
+  cudaEventRecord(c.evObjDone, c.side2);
   launch_advdiff(c);
   launch_outflow(c);
   launch_rhs_div(c);
+  cudaStreamWaitEvent(c.stream, c.evObjDone, 0);
   launch_rhs_obstacles(c);
   launch_fade_sums(c);
   poisson_solve(c);
   launch_pcorr(c);
   launch_momenta_penalize(c);
   launch_forces(c);
+  if (anyFish) cudaStreamWaitEvent(c.stream, c.evJoin, 0);
   launch_end_step(c);
 }
 
@@ -204,6 +236,15 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
   if (!rc) rc = dalloc(ctx, &c.dsc, 1);
   if (!rc) rc = dalloc(ctx, &c.dshapes, MAX_SHAPES);
   if (!rc) rc = dalloc(ctx, &c.counters, Ctx::NCOUNTERS);
+  if (!rc) rc = dalloc(ctx, &c.tileFlags, (size_t)MAX_SHAPES * g.nblocks);
+  if (!rc && (cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking) != cudaSuccess ||
+              cudaStreamCreateWithFlags(&c.side2, cudaStreamNonBlocking) != cudaSuccess ||
+              cudaEventCreateWithFlags(&c.evFork, cudaEventDisableTiming) != cudaSuccess ||
+              cudaEventCreateWithFlags(&c.evJoin, cudaEventDisableTiming) != cudaSuccess ||
+              cudaEventCreateWithFlags(&c.evObj, cudaEventDisableTiming) != cudaSuccess ||
+              cudaEventCreateWithFlags(&c.evObjDone, cudaEventDisableTiming) != cudaSuccess))
+    rc = fail(ctx, CUP2D_ECUDA, "stream/event creation failed");
+  if (!rc) fish_setup_kernels();
   if (rc) { cup2d_destroy(ctx); return rc; }
   if (cudaMemset(c.counters, 0, sizeof(unsigned) * Ctx::NCOUNTERS) != cudaSuccess) { cup2d_destroy(ctx); return CUP2D_ECUDA; }
   c.poisson = poisson_create(c);
@@ -223,16 +264,18 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   for (int b = 0; b < 2; b++) for (int d = 0; d < 2; d++) cudaFree(c.vel[b][d]);
   cudaFree(c.chi); cudaFree(c.pres); cudaFree(c.rhs); cudaFree(c.sdf);
   cudaFree(c.udefx); cudaFree(c.udefy); cudaFree(c.dsc); cudaFree(c.dshapes);
-  cudaFree(c.counters); cudaFree(c.partials);
+  cudaFree(c.counters); cudaFree(c.partials); cudaFree(c.tileFlags);
+  if (c.side) cudaStreamDestroy(c.side);
+  if (c.side2) cudaStreamDestroy(c.side2);
+  if (c.evObj) cudaEventDestroy(c.evObj);
+  if (c.evObjDone) cudaEventDestroy(c.evObjDone);
+  if (c.evFork) cudaEventDestroy(c.evFork);
+  if (c.evJoin) cudaEventDestroy(c.evJoin);
   for (auto& t : c.tiles) {
     cudaFree(t.tiles); cudaFree(t.slot); cudaFree(t.chi); cudaFree(t.dist); cudaFree(t.udx);
     cudaFree(t.udy); cudaFree(t.sD); cudaFree(t.sdx); cudaFree(t.sdy);
   }
-  for (auto& f : c.fish) {
-    cudaFree(f.rS); cudaFree(f.rX); cudaFree(f.rY); cudaFree(f.vX); cudaFree(f.vY);
-    cudaFree(f.norX); cudaFree(f.norY); cudaFree(f.vNorX); cudaFree(f.vNorY); cudaFree(f.width);
-    cudaFree(f.rK); cudaFree(f.vK); cudaFree(f.p1f); cudaFree(f.seg);
-  }
+  for (auto& f : c.fish) { cudaFree(f.pool); cudaFree(f.seg); }
   poisson_destroy(c.poisson);
   if (c.stream) cudaStreamDestroy(c.stream);
   delete ctx;
@@ -304,11 +347,20 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
     const int Nm = (int)rS.size();
     f.nm = Nm;
     F.nm = Nm; F.nseg = (Nm - 1) / 8;
-    double** fa[] = {&F.rS, &F.rX, &F.rY, &F.vX, &F.vY, &F.norX, &F.norY, &F.vNorX, &F.vNorY,
-                     &F.width, &F.rK, &F.vK, &F.p1f};
-    for (auto a : fa) if (!rc) rc = dalloc(ctx, a, Nm);
+    // 3 static arrays + 3 midlines of 8 arrays + 16 integrals, one allocation
+    if (!rc) rc = dalloc(ctx, &F.pool, (size_t)27 * Nm + 16);
     if (!rc) rc = dalloc(ctx, &F.seg, F.nseg);
     if (rc) return rc;
+    {
+      double* q = F.pool;
+      F.rS = q; q += Nm; F.width = q; q += Nm; F.p1f = q; q += Nm;
+      FishMidline* mids[3] = {&F.mid[0], &F.mid[1], &F.frame};
+      for (FishMidline* m : mids) {
+        double** a[8] = {&m->rX, &m->rY, &m->vX, &m->vY, &m->norX, &m->norY, &m->vNorX, &m->vNorY};
+        for (auto x : a) { *x = q; q += Nm; }
+      }
+      F.integ = q;
+    }
     // curvature control values, StefanFish.cpp:187-193, splined onto rS
     const double L = f.length;
     const double pts[6] = {0, .15 * L, .4 * L, .65 * L, .9 * L, L};
@@ -356,7 +408,7 @@ int cup2d_init(cup2d_ctx* ctx) {
   if ((rc = upload_shapes(ctx))) return rc;
   launch_ic(c);
   launch_set_dt(c, 0.0);
-  launch_objects(c);
+  launch_objects(c, false);
   launch_obj_vel_on_grid(c);
   launch_apply_obj_vel(c);
   CK(cudaStreamSynchronize(c.stream));
@@ -386,7 +438,7 @@ int cup2d_calc_dt(cup2d_ctx* ctx, double* dt_out) {
 
 int cup2d_put_objects(cup2d_ctx* ctx, double dt) {
   STAGE_PROLOGUE
-  launch_objects(c);
+  launch_objects(c, false);
   return check_launch(ctx);
 }
 
@@ -571,7 +623,7 @@ int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, double* ms_per_launch
       case CUP2D_KERNEL_FFT_COLS: poisson_cols(c); break;
       case CUP2D_KERNEL_FFT_ROWS_INV: poisson_rows_inv(c); break;
       case CUP2D_KERNEL_MAX_U: launch_max_u_dt(c); break;
-      case CUP2D_KERNEL_OBJECTS: launch_objects(c); break;
+      case CUP2D_KERNEL_OBJECTS: launch_objects(c, false); break;
     }
   };
   one();   // warm

@@ -40,6 +40,10 @@ struct Ctx {
   static constexpr int NCOUNTERS = 256;
 
   Poisson* poisson = nullptr;
+  int* tileFlags = nullptr;     // [MAX_SHAPES][nblocks] touched-block flags
+  cudaStream_t side = nullptr;  // branch for the next step's fish midlines
+  cudaStream_t side2 = nullptr; // branch for the obstacle chain, beside advDiff
+  cudaEvent_t evFork = nullptr, evJoin = nullptr, evObj = nullptr, evObjDone = nullptr;
 
   cudaGraphExec_t graph = nullptr;
   long long launches = 0;
@@ -59,6 +63,8 @@ enum CounterSlot : int {
   CNT_CHI = 8,          // + shape
   CNT_RHSOBST = 24,     // + shape
   CNT_FORCES = 40,      // + shape
+  CNT_MOMENTS = 56,     // + shape
+  CNT_MOMENTA = 72,     // + shape
 };
 // partials offsets (doubles)
 inline size_t part_off(int region, const Ctx& c) {

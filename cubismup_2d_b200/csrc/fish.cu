@@ -1,23 +1,28 @@
-// Fish on the device.
+// Fish on the device: Fish::create (Fish.cpp:20-178) in three kernels.
 //
-// k_fish_kinematics (one CTA per fish) is Fish::create up to the block
-// intersection (Fish.cpp:20-110) for the two midline models of the reference:
-//  - StefanFish's CurvatureFish::computeMidline (StefanFish.cpp:154-206):
-//    the curvature scheduler ramp (FishUtilities.h:171-258), the travelling
-//    curvature wave and the Frenet integration (FishUtilities.h:15-79);
-//  - CarlingFish's AmplitudeFish::computeMidline (CarlingFish.cpp:16-88);
-// then the midline integrals and frame changes (FishLibrary.cpp:66-176) and
-// the AreaSegment boxes (Fish.cpp:78-110, FishLibrary.cpp:295-342).
-// The Frenet recurrence is serial in s and runs on one thread; everything
-// else is parallel over midline points.
-//
-// k_fish_raster (one CTA per obstacle tile, one thread per cell) is
-// PutFishOnBlocks (FishLibrary.cpp:403-638).  The reference scatters every
-// surface / interior point of every intersecting segment onto the block;
-// here every cell gathers those points in the reference's loop order
-// (segment, s index, side / width offset), so its "keep the nearest"
-// updates, ties included, and its hat-kernel sums see exactly the same
-// sequence as in the reference.
+// k_fish_midline (one CTA per fish): the midline at time t for the two
+//   midline models of the reference -- StefanFish's
+//   CurvatureFish::computeMidline (StefanFish.cpp:154-206: curvature
+//   scheduler ramp, travelling curvature wave, Frenet integration
+//   FishUtilities.h:15-79) and CarlingFish's AmplitudeFish::computeMidline
+//   (CarlingFish.cpp:16-88) -- then integrateLinearMomentum,
+//   changeToCoMFrameLinear and integrateAngularMomentum
+//   (FishLibrary.cpp:86-159).  None of this depends on the flow or on the
+//   body's position, only on t, so the pipeline computes the midline of step
+//   n+1 on a side branch while step n runs (double buffer by step parity).
+//   The Frenet recurrence is serial in s; it runs on one thread with its
+//   inputs and outputs in shared memory.
+// k_fish_frame (one CTA per fish): changeToCoMFrameAngular with the current
+//   theta_internal (FishLibrary.cpp:161-176) and the AreaSegment boxes in the
+//   computational frame (Fish.cpp:118-150, FishLibrary.cpp:295-342).
+// k_fish_raster (16 CTAs per obstacle tile, one per 8x8 cells):
+//   PutFishOnBlocks (FishLibrary.cpp:403-638).  The reference scatters every
+//   surface / interior point of every intersecting segment onto the block;
+//   here each CTA keeps, in the reference's loop order (segment, s index,
+//   side or width offset), only the points whose support reaches its 8x8
+//   cells, and every cell applies them in that order, so its "keep the
+//   nearest" updates (ties included) and its hat-kernel sums see exactly the
+//   reference's sequence.
 #include <cmath>
 #include "context.hpp"
 #include "fish.cuh"
@@ -44,18 +49,27 @@ __device__ __forceinline__ void cubic_interp(double x0, double x1, double x, dou
   dy = 3 * a * xrel * xrel + 2 * b * xrel + c;
 }
 
+// mode 0: midline at sc->time into buffer (step & 1);
+// mode 1: midline at sc->time + sc->dt (the next step) into buffer ((step + 1) & 1)
 __global__ void __launch_bounds__(512)
-k_fish_kinematics(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays F)
+k_fish_midline(const Scalars* sc, const DevShape* sh, int k, FishArrays F, int mode)
 {
+  extern __shared__ double smem[];
   __shared__ double red[32 * 5];
-  __shared__ double bc[8];
-  DevShape& S = sh[k];
+  __shared__ double bc[4];
+  const DevShape& S = sh[k];
   const int Nm = F.nm, tid = threadIdx.x, nt = blockDim.x;
-  const double t = sc->time;
+  const double t = mode ? sc->time + sc->dt : sc->time;
+  const int p = mode ? (sc->step + 1) & 1 : sc->step & 1;
   const double L = S.cfg.length, T = S.cfg.Tperiod;
-  double* rS = F.rS; double* rX = F.rX; double* rY = F.rY; double* vX = F.vX; double* vY = F.vY;
-  double* norX = F.norX; double* norY = F.norY; double* vNorX = F.vNorX; double* vNorY = F.vNorY;
-  const double* width = F.width;
+  double* rS = smem;          double* width = rS + Nm;
+  double* rK = width + Nm;    double* vK = rK + Nm;
+  double* rX = vK + Nm;       double* rY = rX + Nm;
+  double* vX = rY + Nm;       double* vY = vX + Nm;
+  double* norX = vY + Nm;     double* norY = norX + Nm;
+  double* vNorX = norY + Nm;  double* vNorY = vNorX + Nm;
+  for (int i = tid; i < Nm; i += nt) { rS[i] = F.rS[i]; width[i] = F.width[i]; }
+  __syncthreads();
 
   if (S.cfg.kind == CUP2D_SHAPE_STEFANFISH) {
     // curvature scheduler: after transition(0, 0, T, zeros, values) the start
@@ -73,42 +87,51 @@ k_fish_kinematics(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays
       else cubic_interp(0.0, T, t, 0.0, F.p1f[i], 0.0, 0.0, rC, vC);
       const double rB = 0, vB = 0, fac = 0, dif = 0;
       const double arg = arg0 - 2 * M_PI * rS[i] / L / waveLength;
-      F.rK[i] = amp * rC * (sin(arg) + rB + fac);
-      F.vK[i] = amp * (vC * (sin(arg) + rB + fac) + rC * (cos(arg) * darg + vB + dif));
+      rK[i] = amp * rC * (sin(arg) + rB + fac);
+      vK[i] = amp * (vC * (sin(arg) + rB + fac) + rC * (cos(arg) * darg + vB + dif));
     }
     __syncthreads();
     if (tid == 0) {                                     // IF2D_Frenet2D::solve
-      const double* curv = F.rK; const double* curv_dt = F.vK;
-      rX[0] = 0.0; rY[0] = 0.0; norX[0] = 0.0; norY[0] = 1.0;
+      const double* curv = rK; const double* curv_dt = vK;
+      rX[0] = 0.0; rY[0] = 0.0;
+      double nX = 0.0, nY = 1.0;                        // norX[i-1], norY[i-1]
       double ksiX = 1.0, ksiY = 0.0;
-      vX[0] = 0.0; vY[0] = 0.0; vNorX[0] = 0.0; vNorY[0] = 0.0;
+      vX[0] = 0.0; vY[0] = 0.0;
+      double vnX = 0.0, vnY = 0.0;                      // vNorX[i-1], vNorY[i-1]
       double vKsiX = 0.0, vKsiY = 0.0;
+      double rx = 0.0, ry = 0.0, vx = 0.0, vy = 0.0;
+      norX[0] = nX; norY[0] = nY; vNorX[0] = vnX; vNorY[0] = vnY;
+      double sPrev = rS[0];
       for (int i = 1; i < Nm; i++) {
-        const double dksiX = curv[i - 1] * norX[i - 1];
-        const double dksiY = curv[i - 1] * norY[i - 1];
-        const double dnuX = -curv[i - 1] * ksiX;
-        const double dnuY = -curv[i - 1] * ksiY;
-        const double dvKsiX = curv_dt[i - 1] * norX[i - 1] + curv[i - 1] * vNorX[i - 1];
-        const double dvKsiY = curv_dt[i - 1] * norY[i - 1] + curv[i - 1] * vNorY[i - 1];
-        const double dvNuX = -curv_dt[i - 1] * ksiX - curv[i - 1] * vKsiX;
-        const double dvNuY = -curv_dt[i - 1] * ksiY - curv[i - 1] * vKsiY;
-        const double ds = rS[i] - rS[i - 1];
-        rX[i] = rX[i - 1] + ds * ksiX;
-        rY[i] = rY[i - 1] + ds * ksiY;
-        norX[i] = norX[i - 1] + ds * dnuX;
-        norY[i] = norY[i - 1] + ds * dnuY;
+        const double c = curv[i - 1], cd = curv_dt[i - 1], sNow = rS[i];
+        const double dksiX = c * nX;
+        const double dksiY = c * nY;
+        const double dnuX = -c * ksiX;
+        const double dnuY = -c * ksiY;
+        const double dvKsiX = cd * nX + c * vnX;
+        const double dvKsiY = cd * nY + c * vnY;
+        const double dvNuX = -cd * ksiX - c * vKsiX;
+        const double dvNuY = -cd * ksiY - c * vKsiY;
+        const double ds = sNow - sPrev;
+        rx = rx + ds * ksiX;
+        ry = ry + ds * ksiY;
+        nX = nX + ds * dnuX;
+        nY = nY + ds * dnuY;
         ksiX += ds * dksiX;
         ksiY += ds * dksiY;
-        vX[i] = vX[i - 1] + ds * vKsiX;
-        vY[i] = vY[i - 1] + ds * vKsiY;
-        vNorX[i] = vNorX[i - 1] + ds * dvNuX;
-        vNorY[i] = vNorY[i - 1] + ds * dvNuY;
+        vx = vx + ds * vKsiX;
+        vy = vy + ds * vKsiY;
+        vnX = vnX + ds * dvNuX;
+        vnY = vnY + ds * dvNuY;
         vKsiX += ds * dvKsiX;
         vKsiY += ds * dvKsiY;
         const double d1 = ksiX * ksiX + ksiY * ksiY;
-        const double d2 = norX[i] * norX[i] + norY[i] * norY[i];
+        const double d2 = nX * nX + nY * nY;
         if (d1 > EPSd) { const double nf = 1 / sqrt(d1); ksiX *= nf; ksiY *= nf; }
-        if (d2 > EPSd) { const double nf = 1 / sqrt(d2); norX[i] *= nf; norY[i] *= nf; }
+        if (d2 > EPSd) { const double nf = 1 / sqrt(d2); nX *= nf; nY *= nf; }
+        rX[i] = rx; rY[i] = ry; vX[i] = vx; vY[i] = vy;
+        norX[i] = nX; norY[i] = nY; vNorX[i] = vnX; vNorY[i] = vnY;
+        sPrev = sNow;
       }
     }
     __syncthreads();
@@ -135,14 +158,14 @@ k_fish_kinematics(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays
       const double dx = sqrt(ds * ds - dy * dy);
       const double dVy = vY[i] - vY[i - 1];
       const double dVx = -dy / dx * dVy;
-      F.rK[i] = dx; F.vK[i] = dVx;                      // increments, summed below
+      rK[i] = dx; vK[i] = dVx;                          // increments, summed below
       norX[i - 1] = -dy / ds; norY[i - 1] = dx / ds;
       vNorX[i - 1] = -dVy / ds; vNorY[i - 1] = dVx / ds;
     }
     __syncthreads();
     if (tid == 0) {
       rX[0] = 0.0; vX[0] = 0.0;
-      for (int i = 1; i < Nm; i++) { rX[i] = F.rK[i] + rX[i - 1]; vX[i] = F.vK[i] + vX[i - 1]; }
+      for (int i = 1; i < Nm; i++) { rX[i] = rK[i] + rX[i - 1]; vX[i] = vK[i] + vX[i - 1]; }
       norX[Nm - 1] = norX[Nm - 2]; norY[Nm - 1] = norY[Nm - 2];
       vNorX[Nm - 1] = vNorX[Nm - 2]; vNorY[Nm - 1] = vNorY[Nm - 2];
     }
@@ -159,8 +182,8 @@ k_fish_kinematics(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays
   auto dsOf = [&](int i) -> double {
     return (i == 0) ? rS[1] - rS[0] : ((i == Nm - 1) ? rS[Nm - 1] - rS[Nm - 2] : rS[i + 1] - rS[i - 1]);
   };
-  // integrateLinearMomentum (FishLibrary.cpp:86-117)
-  {
+  double* integ = F.integ + 8 * p;
+  {                                                     // integrateLinearMomentum
     double a[5] = {0, 0, 0, 0, 0};
     for (int i = tid; i < Nm; i += nt) {
       const double ds = dsOf(i);
@@ -175,11 +198,10 @@ k_fish_kinematics(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays
     block_sum<5>(a, red);
     if (tid == 0) {
       const double area = a[0];
-      S.f.area_internal = area;
-      S.f.CoM_internal[0] = a[1] / area; S.f.CoM_internal[1] = a[2] / area;
-      S.f.vCoM_internal[0] = a[3] / area; S.f.vCoM_internal[1] = a[4] / area;
-      bc[0] = S.f.CoM_internal[0]; bc[1] = S.f.CoM_internal[1];
-      bc[2] = S.f.vCoM_internal[0]; bc[3] = S.f.vCoM_internal[1];
+      integ[0] = area;
+      integ[1] = a[1] / area; integ[2] = a[2] / area;
+      integ[3] = a[3] / area; integ[4] = a[4] / area;
+      bc[0] = integ[1]; bc[1] = integ[2]; bc[2] = integ[3]; bc[3] = integ[4];
     }
     __syncthreads();
   }
@@ -187,8 +209,7 @@ k_fish_kinematics(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays
     rX[i] -= bc[0]; rY[i] -= bc[1]; vX[i] -= bc[2]; vY[i] -= bc[3];
   }
   __syncthreads();
-  // integrateAngularMomentum (FishLibrary.cpp:119-150)
-  {
+  {                                                     // integrateAngularMomentum
     double a[2] = {0, 0};
     for (int i = tid; i < Nm; i += nt) {
       const double ds = dsOf(i);
@@ -205,37 +226,56 @@ k_fish_kinematics(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays
       a[1] += tmp_J * ds / 2;
     }
     block_sum<2>(a, red);
-    if (tid == 0) {
-      S.f.angvel_internal_prev = S.f.angvel_internal;
-      S.f.J_internal = a[1];
-      S.f.angvel_internal = a[0] / a[1];
-      bc[4] = S.f.theta_internal; bc[5] = S.f.angvel_internal;
-    }
-    __syncthreads();
+    if (tid == 0) { integ[5] = a[1]; integ[6] = a[0] / a[1]; integ[7] = t; }
   }
+  const FishMidline& M = F.mid[p];
+  for (int i = tid; i < Nm; i += nt) {
+    M.rX[i] = rX[i]; M.rY[i] = rY[i]; M.vX[i] = vX[i]; M.vY[i] = vY[i];
+    M.norX[i] = norX[i]; M.norY[i] = norY[i]; M.vNorX[i] = vNorX[i]; M.vNorY[i] = vNorY[i];
+  }
+}
+
+__global__ void __launch_bounds__(512)
+k_fish_frame(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays F)
+{
+  __shared__ double bc[2];
+  DevShape& S = sh[k];
+  const int Nm = F.nm, tid = threadIdx.x, nt = blockDim.x;
+  const int p = sc->step & 1;
+  const double* integ = F.integ + 8 * p;
+  if (tid == 0) {                                       // Fish.cpp:87-93 bookkeeping
+    S.f.area_internal = integ[0];
+    S.f.CoM_internal[0] = integ[1]; S.f.CoM_internal[1] = integ[2];
+    S.f.vCoM_internal[0] = integ[3]; S.f.vCoM_internal[1] = integ[4];
+    S.f.angvel_internal_prev = S.f.angvel_internal;
+    S.f.J_internal = integ[5];
+    S.f.angvel_internal = integ[6];
+    bc[0] = S.f.theta_internal; bc[1] = integ[6];
+  }
+  __syncthreads();
+  const FishMidline& M = F.mid[p];
+  const FishMidline& R = F.frame;
   {                                                     // changeToCoMFrameAngular
-    const double Ain = bc[4], vAin = bc[5];
+    const double Ain = bc[0], vAin = bc[1];
     const double R00 = cos(Ain), R01 = -sin(Ain), R10 = sin(Ain), R11 = cos(Ain);
     for (int i = tid; i < Nm; i += nt) {
-      vX[i] += vAin * rY[i];
-      vY[i] -= vAin * rX[i];
-      const double px = rX[i], py = rY[i];
-      rX[i] = R00 * px + R01 * py; rY[i] = R10 * px + R11 * py;
-      const double qx = vX[i], qy = vY[i];
-      vX[i] = R00 * qx + R01 * qy; vY[i] = R10 * qx + R11 * qy;
+      const double px = M.rX[i], py = M.rY[i];
+      const double qx = M.vX[i] + vAin * py, qy = M.vY[i] - vAin * px;
+      R.rX[i] = R00 * px + R01 * py; R.rY[i] = R10 * px + R11 * py;
+      R.vX[i] = R00 * qx + R01 * qy; R.vY[i] = R10 * qx + R11 * qy;
     }
     __syncthreads();
     for (int i = tid; i < Nm - 1; i += nt) {            // _computeMidlineNormals
-      const double ds = rS[i + 1] - rS[i];
-      const double tX = rX[i + 1] - rX[i], tY = rY[i + 1] - rY[i];
-      const double tVX = vX[i + 1] - vX[i], tVY = vY[i + 1] - vY[i];
-      norX[i] = -tY / ds; norY[i] = tX / ds;
-      vNorX[i] = -tVY / ds; vNorY[i] = tVX / ds;
+      const double ds = F.rS[i + 1] - F.rS[i];
+      const double tX = R.rX[i + 1] - R.rX[i], tY = R.rY[i + 1] - R.rY[i];
+      const double tVX = R.vX[i + 1] - R.vX[i], tVY = R.vY[i + 1] - R.vY[i];
+      R.norX[i] = -tY / ds; R.norY[i] = tX / ds;
+      R.vNorX[i] = -tVY / ds; R.vNorY[i] = tVX / ds;
     }
     __syncthreads();
     if (tid == 0) {
-      norX[Nm - 1] = norX[Nm - 2]; norY[Nm - 1] = norY[Nm - 2];
-      vNorX[Nm - 1] = vNorX[Nm - 2]; vNorY[Nm - 1] = vNorY[Nm - 2];
+      R.norX[Nm - 1] = R.norX[Nm - 2]; R.norY[Nm - 1] = R.norY[Nm - 2];
+      R.vNorX[Nm - 1] = R.vNorX[Nm - 2]; R.vNorY[Nm - 1] = R.vNorY[Nm - 2];
     }
     __syncthreads();
   }
@@ -243,6 +283,8 @@ k_fish_kinematics(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays
   const int Nseg = F.nseg;
   const double angle = S.s.orientation;
   const double R00 = cos(angle), R01 = -sin(angle), R10 = sin(angle), R11 = cos(angle);
+  const double* rX = R.rX; const double* rY = R.rY;
+  const double* norX = R.norX; const double* norY = R.norY; const double* width = F.width;
   for (int i = tid; i < Nseg; i += nt) {
     const int next_idx = (i + 1) * (Nm - 1) / Nseg, idx = i * (Nm - 1) / Nseg;
     double bb[2][2] = {{1e9, -1e9}, {1e9, -1e9}};
@@ -260,8 +302,8 @@ k_fish_kinematics(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays
     sg.w[0] = (bb[0][1] - bb[0][0]) / 2 + safe; sg.w[1] = (bb[1][1] - bb[1][0]) / 2 + safe;
     const double c0 = (bb[0][1] + bb[0][0]) / 2, c1 = (bb[1][1] + bb[1][0]) / 2;
     // AreaSegment::changeToComputationalFrame (FishLibrary.cpp:295-342)
-    double nI0 = R00 * 1 + R01 * 0, nI1 = R10 * 1 + R11 * 0;
-    double nJ0 = R00 * 0 + R01 * 1, nJ1 = R10 * 0 + R11 * 1;
+    const double nI0 = R00 * 1 + R01 * 0, nI1 = R10 * 1 + R11 * 0;
+    const double nJ0 = R00 * 0 + R01 * 1, nJ1 = R10 * 0 + R11 * 1;
     sg.c[0] = R00 * c0 + R01 * c1 + S.s.center[0];
     sg.c[1] = R10 * c0 + R11 * c1 + S.s.center[1];
     const double magI = sqrt(nI0 * nI0 + nI1 * nI1), magJ = sqrt(nJ0 * nJ0 + nJ1 * nJ1);
@@ -281,37 +323,50 @@ k_fish_kinematics(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays
   if (tid == 0) S.nseg = Nseg;
 }
 
-struct SurfPt { double myP[2], pP[2], pM[2], ud[2]; int iap[2], ss, valid; };
-struct IntPt { double xp[2], ud[2], w[2][2]; int iap[2], valid; };
+struct SurfPt { double myP[2], pP[2], pM[2], ud[2]; int iap[2], ss; };
+struct IntPt { double ud[2], w[2][2]; int iap[2]; };
 
+constexpr int SUB = 8;                      // cells per sub-tile edge
+constexpr int NSUB = (BS / SUB) * (BS / SUB);
+constexpr int RT = SUB * SUB;               // threads per CTA (one per cell)
 constexpr int MAX_SEG_PER_TILE = 512;
-constexpr int SURF_CHUNK = 64;
-constexpr int INT_CHUNK = 256;
 
-__global__ void __launch_bounds__(1024)
+// order-preserving compaction over the CTA's two warps; returns the count
+__device__ __forceinline__ int compact_slot(bool keep, int* wc, int& pos) {
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const unsigned m = __ballot_sync(0xffffffffu, keep);
+  if (lane == 0) wc[wid] = __popc(m);
+  __syncthreads();
+  pos = (wid == 1 ? wc[0] : 0) + __popc(m & ((1u << lane) - 1u));
+  return wc[0] + wc[1];
+}
+
+__global__ void __launch_bounds__(RT)
 k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, double* sdfg)
 {
   __shared__ int segList[MAX_SEG_PER_TILE];
   __shared__ int nSegList;
-  __shared__ int warpCount[32];
-  __shared__ SurfPt sp[SURF_CHUNK];
-  __shared__ IntPt ip[INT_CHUNK];
+  __shared__ int wc[2];
+  __shared__ SurfPt sp[RT];
+  __shared__ IntPt ip[RT];
   const DevShape& S = sh[k];
-  const int s = blockIdx.x;
+  const int s = blockIdx.x / NSUB, sub = blockIdx.x % NSUB;
   if (s >= S.ntiles) return;
   const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
-  const int tid = threadIdx.x + BS * threadIdx.y, lane = tid & 31, wid = tid >> 5;
-  const int ix = threadIdx.x, iy = threadIdx.y;
+  const int tid = threadIdx.x;
+  const int sx0 = (sub % (BS / SUB)) * SUB, sy0 = (sub / (BS / SUB)) * SUB;
+  const int ix = sx0 + tid % SUB, iy = sy0 + tid / SUB;
   const double h = g.h, invh = 1.0 / h;
   const double org0 = cell_x(g, bx, 0), org1 = cell_y(g, by, 0);
   const double angle = S.s.orientation;
   const double R00 = cos(angle), R01 = -sin(angle), R10 = sin(angle), R11 = cos(angle);
   const double pos0 = S.s.center[0], pos1 = S.s.center[1];
   const int Nm = F.nm;
-  const double* rX = F.rX; const double* rY = F.rY; const double* width = F.width;
-  const double* norX = F.norX; const double* norY = F.norY;
-  const double* vX = F.vX; const double* vY = F.vY;
-  const double* vNorX = F.vNorX; const double* vNorY = F.vNorY;
+  const FishMidline& R = F.frame;
+  const double* rX = R.rX; const double* rY = R.rY; const double* width = F.width;
+  const double* norX = R.norX; const double* norY = R.norY;
+  const double* vX = R.vX; const double* vY = R.vY;
+  const double* vNorX = R.vNorX; const double* vNorY = R.vNorY;
 
   // ordered list of the segments intersecting this block (Fish.cpp:167-173)
   if (tid == 0) nSegList = 0;
@@ -319,18 +374,14 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
   {
     const double start[2] = {org0, org1};
     const double end[2] = {cell_x(g, bx, BS - 1), cell_y(g, by, BS - 1)};
-    for (int s0 = 0; s0 < S.nseg; s0 += 1024) {
+    for (int s0 = 0; s0 < S.nseg; s0 += RT) {
       const int q = s0 + tid;
       const bool f = q < S.nseg && segment_hits_block(F.seg[q], start, end, 2 * h);
-      const unsigned m = __ballot_sync(0xffffffffu, f);
-      if (lane == 0) warpCount[wid] = __popc(m);
+      int pos;
+      const int tot = compact_slot(f, wc, pos);
+      if (f && nSegList + pos < MAX_SEG_PER_TILE) segList[nSegList + pos] = q;
       __syncthreads();
-      int off = nSegList;
-      for (int w = 0; w < wid; w++) off += warpCount[w];
-      const int p = off + __popc(m & ((1u << lane) - 1u));
-      if (f && p < MAX_SEG_PER_TILE) segList[p] = q;
-      __syncthreads();
-      if (tid == 0) { int tot = 0; for (int w = 0; w < 32; w++) tot += warpCount[w]; nSegList += tot; }
+      if (tid == 0) nSegList += tot;
       __syncthreads();
     }
   }
@@ -343,20 +394,23 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
     const Segment& sg = F.seg[segList[si]];
     const int firstSegm = max(sg.first, 1), lastSegm = min(sg.second, Nm - 2);
     const int npts = (lastSegm - firstSegm + 1) * 2;
-    for (int c0 = 0; c0 < npts; c0 += SURF_CHUNK) {
-      const int nc = min(SURF_CHUNK, npts - c0);
-      __syncthreads();
-      if (tid < nc) {
-        const int q = c0 + tid, ss = firstSegm + q / 2, signp = (q & 1) ? 1 : -1;
-        SurfPt P;
+    for (int c0 = 0; c0 < npts; c0 += RT) {
+      SurfPt P;
+      bool keep = false;
+      const int q = c0 + tid;
+      if (q < npts) {
+        const int ss = firstSegm + q / 2, signp = (q & 1) ? 1 : -1;
         P.ss = ss;
         double m0 = rX[ss + 0] + width[ss + 0] * signp * norX[ss + 0];
         double m1 = rY[ss + 0] + width[ss + 0] * signp * norY[ss + 0];
         P.myP[0] = R00 * m0 + R01 * m1 + pos0; P.myP[1] = R10 * m0 + R11 * m1 + pos1;
         P.iap[0] = (int)floor((P.myP[0] - org0) * invh);
         P.iap[1] = (int)floor((P.myP[1] - org1) * invh);
-        P.valid = !(P.iap[0] + 3 <= 0 || P.iap[0] - 1 >= BS) && !(P.iap[1] + 3 <= 0 || P.iap[1] - 1 >= BS);
-        if (P.valid) {
+        const bool valid = !(P.iap[0] + 3 <= 0 || P.iap[0] - 1 >= BS) && !(P.iap[1] + 3 <= 0 || P.iap[1] - 1 >= BS);
+        // support [iap-1, iap+3) clipped to the block, intersected with this sub-tile
+        keep = valid && max(max(0, P.iap[0] - 1), sx0) < min(min(P.iap[0] + 3, BS), sx0 + SUB)
+                     && max(max(0, P.iap[1] - 1), sy0) < min(min(P.iap[1] + 3, BS), sy0 + SUB);
+        if (keep) {
           m0 = rX[ss + 1] + width[ss + 1] * signp * norX[ss + 1];
           m1 = rY[ss + 1] + width[ss + 1] * signp * norY[ss + 1];
           P.pP[0] = R00 * m0 + R01 * m1 + pos0; P.pP[1] = R10 * m0 + R11 * m1 + pos1;
@@ -367,22 +421,23 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
           const double u1 = vY[ss + 0] + width[ss + 0] * signp * vNorY[ss + 0];
           P.ud[0] = R00 * u0 + R01 * u1; P.ud[1] = R10 * u0 + R11 * u1;
         }
-        sp[tid] = P;
       }
+      int pos;
+      const int nc = compact_slot(keep, wc, pos);
+      if (keep) sp[pos] = P;
       __syncthreads();
-      for (int q = 0; q < nc; q++) {
-        const SurfPt& P = sp[q];
-        if (!P.valid) continue;
-        if (iy < max(0, P.iap[1] - 1) || iy >= min(P.iap[1] + 3, BS)) continue;
-        if (ix < max(0, P.iap[0] - 1) || ix >= min(P.iap[0] + 3, BS)) continue;
-        const double dist0 = sq(px - P.myP[0]) + sq(py - P.myP[1]);
-        const double distP = sq(px - P.pP[0]) + sq(py - P.pP[1]);
-        const double distM = sq(px - P.pM[0]) + sq(py - P.pM[1]);
+      for (int qq = 0; qq < nc; qq++) {
+        const SurfPt& Q = sp[qq];
+        if (iy < max(0, Q.iap[1] - 1) || iy >= min(Q.iap[1] + 3, BS)) continue;
+        if (ix < max(0, Q.iap[0] - 1) || ix >= min(Q.iap[0] + 3, BS)) continue;
+        const double dist0 = sq(px - Q.myP[0]) + sq(py - Q.myP[1]);
+        const double distP = sq(px - Q.pP[0]) + sq(py - Q.pP[1]);
+        const double distM = sq(px - Q.pM[0]) + sq(py - Q.pM[1]);
         if (fabs(dist) < fmin(fmin(dist0, distP), distM)) continue;
         // changeFromComputationalFrame (FishLibrary.h:194-200)
         const double q0 = px - pos0, q1 = py - pos1;
         const double p0 = R00 * q0 + R10 * q1, p1 = R01 * q0 + R11 * q1;
-        const int ss = P.ss;
+        const int ss = Q.ss;
         int close_s = ss, secnd_s = ss + (distP < distM ? 1 : -1);
         double dist1 = dist0, dist2 = distP < distM ? distP : distM;
         if (distP < dist0 || distM < dist0) {
@@ -412,11 +467,12 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
         }
         if (fabs(dist) > dist1) {
           const double W = 1 - sqrt(dist1) * (invh / 3);
-          ud0 = W * P.ud[0]; ud1 = W * P.ud[1];
+          ud0 = W * Q.ud[0]; ud1 = W * Q.ud[1];
           dist = sign2d * dist1;
           chi = W;
         }
       }
+      __syncthreads();
     }
   }
 
@@ -424,17 +480,17 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
   for (int si = 0; si < nsl; si++) {
     const Segment& sg = F.seg[segList[si]];
     const int firstSegm = max(sg.first, 1), lastSegm = min(sg.second, Nm - 2);
-    // points of this segment: for ss, iw in (-Nw, Nw)
-    int npts = 0;
+    int npts = 0;                                       // sum over ss of (2 Nw - 1)
     for (int ss = firstSegm; ss <= lastSegm; ss++) {
       const int Nw = (int)floor(width[ss] / h);
       npts += Nw > 0 ? 2 * Nw - 1 : 0;
     }
-    for (int c0 = 0; c0 < npts; c0 += INT_CHUNK) {
-      const int nc = min(INT_CHUNK, npts - c0);
-      __syncthreads();
-      if (tid < nc) {
-        int q = c0 + tid, ss = firstSegm, Nw = 0;
+    for (int c0 = 0; c0 < npts; c0 += RT) {
+      IntPt P;
+      bool keep = false;
+      const int q0 = c0 + tid;
+      if (q0 < npts) {
+        int q = q0, ss = firstSegm, Nw = 0;
         for (;; ss++) {
           Nw = (int)floor(width[ss] / h);
           const int n = Nw > 0 ? 2 * Nw - 1 : 0;
@@ -443,32 +499,37 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
         }
         const int iw = -Nw + 1 + q;
         const double offsetW = iw * h;
-        IntPt P;
         const double m0 = rX[ss] + offsetW * norX[ss], m1 = rY[ss] + offsetW * norY[ss];
-        P.xp[0] = ((R00 * m0 + R01 * m1 + pos0) - org0) * invh;
-        P.xp[1] = ((R10 * m0 + R11 * m1 + pos1) - org1) * invh;
-        const double ap0 = floor(P.xp[0]), ap1 = floor(P.xp[1]);
+        const double xp0 = ((R00 * m0 + R01 * m1 + pos0) - org0) * invh;
+        const double xp1 = ((R10 * m0 + R11 * m1 + pos1) - org1) * invh;
+        const double ap0 = floor(xp0), ap1 = floor(xp1);
         P.iap[0] = (int)ap0; P.iap[1] = (int)ap1;
-        P.valid = !(P.iap[0] + 2 <= 0 || P.iap[0] >= BS) && !(P.iap[1] + 2 <= 0 || P.iap[1] >= BS);
-        const double u0 = vX[ss] + offsetW * vNorX[ss], u1 = vY[ss] + offsetW * vNorY[ss];
-        P.ud[0] = R00 * u0 + R01 * u1; P.ud[1] = R10 * u0 + R11 * u1;
-        P.w[0][0] = 1 - fabs(P.xp[0] - ap0); P.w[0][1] = 1 - fabs(P.xp[0] - (ap0 + 1));
-        P.w[1][0] = 1 - fabs(P.xp[1] - ap1); P.w[1][1] = 1 - fabs(P.xp[1] - (ap1 + 1));
-        ip[tid] = P;
+        const bool valid = !(P.iap[0] + 2 <= 0 || P.iap[0] >= BS) && !(P.iap[1] + 2 <= 0 || P.iap[1] >= BS);
+        keep = valid && max(max(0, P.iap[0]), sx0) < min(min(P.iap[0] + 2, BS), sx0 + SUB)
+                     && max(max(0, P.iap[1]), sy0) < min(min(P.iap[1] + 2, BS), sy0 + SUB);
+        if (keep) {
+          const double u0 = vX[ss] + offsetW * vNorX[ss], u1 = vY[ss] + offsetW * vNorY[ss];
+          P.ud[0] = R00 * u0 + R01 * u1; P.ud[1] = R10 * u0 + R11 * u1;
+          P.w[0][0] = 1 - fabs(xp0 - ap0); P.w[0][1] = 1 - fabs(xp0 - (ap0 + 1));
+          P.w[1][0] = 1 - fabs(xp1 - ap1); P.w[1][1] = 1 - fabs(xp1 - (ap1 + 1));
+        }
       }
+      int pos;
+      const int nc = compact_slot(keep, wc, pos);
+      if (keep) ip[pos] = P;
       __syncthreads();
-      for (int q = 0; q < nc; q++) {
-        const IntPt& P = ip[q];
-        if (!P.valid) continue;
-        if (iy < max(0, P.iap[1]) || iy >= min(P.iap[1] + 2, BS)) continue;
-        if (ix < max(0, P.iap[0]) || ix >= min(P.iap[0] + 2, BS)) continue;
-        const int sx = ix - P.iap[0], sy = iy - P.iap[1];
-        const double wxwy = P.w[1][sy] * P.w[0][sx];
-        ud0 += wxwy * P.ud[0];
-        ud1 += wxwy * P.ud[1];
+      for (int qq = 0; qq < nc; qq++) {
+        const IntPt& Q = ip[qq];
+        if (iy < max(0, Q.iap[1]) || iy >= min(Q.iap[1] + 2, BS)) continue;
+        if (ix < max(0, Q.iap[0]) || ix >= min(Q.iap[0] + 2, BS)) continue;
+        const int sx = ix - Q.iap[0], sy = iy - Q.iap[1];
+        const double wxwy = Q.w[1][sy] * Q.w[0][sx];
+        ud0 += wxwy * Q.ud[0];
+        ud1 += wxwy * Q.ud[1];
         chi += wxwy;
         if (fabs(dist + 1) < EPSd) dist = 1;
       }
+      __syncthreads();
     }
   }
 
@@ -481,6 +542,8 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
   atomic_max_double(&sdfg[(size_t)(by * BS + iy) * g.nx + bx * BS + ix], dist);
 }
 
+size_t midline_smem(int Nm) { return sizeof(double) * 12 * (size_t)Nm; }
+
 } // namespace
 
 FishSegPtrs fish_seg_ptrs(const Ctx& c) {
@@ -489,14 +552,26 @@ FishSegPtrs fish_seg_ptrs(const Ctx& c) {
   return p;
 }
 
+void fish_setup_kernels() {
+  int dev = 0, maxOptin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncSetAttribute((const void*)k_fish_midline, cudaFuncAttributeMaxDynamicSharedMemorySize, maxOptin);
+}
+
+void launch_fish_midline(Ctx& c, int k, cudaStream_t stream, int mode) {
+  k_fish_midline<<<1, 512, midline_smem(c.fish[k].nm), stream>>>(c.dsc, c.dshapes, k, c.fish[k], mode);
+  CUP2D_LAUNCHED(c);
+}
+
 void launch_fish_kinematics(Ctx& c, int k) {
-  k_fish_kinematics<<<1, 512, 0, c.stream>>>(c.g, c.dsc, c.dshapes, k, c.fish[k]);
+  k_fish_frame<<<1, 512, 0, c.stream>>>(c.g, c.dsc, c.dshapes, k, c.fish[k]);
   CUP2D_LAUNCHED(c);
 }
 
 void launch_fish_raster(Ctx& c, int k) {
-  k_fish_raster<<<c.tiles[k].capacity, dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
-                                                                   c.fish[k], c.sdf);
+  k_fish_raster<<<c.tiles[k].capacity * NSUB, RT, 0, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
+                                                                c.fish[k], c.sdf);
   CUP2D_LAUNCHED(c);
 }
 

@@ -8,6 +8,8 @@ struct Ctx;
 
 struct FishSegPtrs { const Segment* seg[MAX_SHAPES]; };
 FishSegPtrs fish_seg_ptrs(const Ctx& c);
+void fish_setup_kernels();
+void launch_fish_midline(Ctx& c, int k, cudaStream_t stream, int mode);
 void launch_fish_kinematics(Ctx& c, int k);
 void launch_fish_raster(Ctx& c, int k);
 

@@ -76,6 +76,9 @@ struct DevShape {
   double rhsCorr;                 // PressureSingle.cpp:183-186 corr of this shape
   double bbox[2][2];              // disk bounding box (ShapeLibrary.h:40-43)
   int nseg;                       // fish AreaSegments this step
+  // rigid part of udef removed by Shape::removeMoments (Shape.cpp:197-204):
+  // consumers read udef - (Iu - Ia p_y, Iv + Ia p_x), the same expression
+  double Iu, Iv, Ia;
 };
 
 // One fish AreaSegment (FishLibrary.h:149-168) in the computational frame.
@@ -100,13 +103,24 @@ struct ObstTiles {
   int capacity;
 };
 
-// Fish midline arrays (FishLibrary.h:49-60) for one fish.
+// One fish midline (the arrays of FishLibrary.h:49-60).
+struct FishMidline {
+  double *rX, *rY, *vX, *vY, *norX, *norY, *vNorX, *vNorY;
+};
+
+// Per-fish device arrays.  The midline depends only on time, so the one for
+// step n+1 is computed while step n runs: mid[] is double-buffered by step
+// parity and holds the midline in the CoM frame with its integrals
+// (integ[p*8 + ..]: area, CoM_internal[2], vCoM_internal[2], J_internal,
+// angvel_internal, time); frame holds it rotated by theta_internal, which is
+// what PutFishOnBlocks reads.
 struct FishArrays {
-  double* rS; double* rX; double* rY; double* vX; double* vY;
-  double* norX; double* norY; double* vNorX; double* vNorY; double* width;
-  double* rK; double* vK;                 // curvature and its rate (StefanFish.cpp:213-223)
-  double* p1f;                            // spline of the curvature control values at rS
+  double *rS, *width, *p1f;
+  FishMidline mid[2];
+  double* integ;
+  FishMidline frame;
   Segment* seg;                           // [nseg]
+  double* pool;                           // single allocation behind all arrays
   int nm, nseg;
 };
 
@@ -186,6 +200,14 @@ __device__ __forceinline__ void atomic_max_double(double* addr, double val) {
     if (__longlong_as_double(assumed) >= val) return;
     old = atomicCAS(a, assumed, __double_as_longlong(val));
   } while (old != assumed);
+}
+
+// Per-tile udef after Shape::removeMoments (Shape.cpp:197-204), evaluated
+// where it is read: udef - (I.u - I.a p1), udef - (I.v + I.a p0), p = x - CoM.
+__device__ __forceinline__ void udef_at(const ObstTiles& t, size_t o, const DevShape& S,
+                                        double p0, double p1, double& u0, double& u1) {
+  u0 = t.udx[o] - (S.Iu - S.Ia * p1);
+  u1 = t.udy[o] - (S.Iv + S.Ia * p0);
 }
 
 // Cell-centre position of cell (ix,iy) of block (bx,by); the same expression

@@ -86,10 +86,35 @@ __device__ __forceinline__ bool disk_touching(const GridDesc& g, const DevShape&
   return i01 - i00 > 0 && i11 - i10 > 0;
 }
 
-// Deterministic compaction of the touched blocks, in increasing block order
-// (Disk::create, ShapesSimple.cpp:14-35; Fish::create, Fish.cpp:78-110).
+// Touched-block flags (Disk: _is_touching, ShapeLibrary.h:24-36; Fish: any
+// AreaSegment intersects the block, Fish.cpp:158-173): one warp per block,
+// the lanes split the fish's segments.
+__global__ void __launch_bounds__(256)
+k_tile_flags(GridDesc g, const DevShape* sh, FishSegPtrs segs, int* flags)
+{
+  const int k = blockIdx.y;
+  const DevShape& S = sh[k];
+  const int lane = threadIdx.x & 31;
+  const int b = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (b >= g.nblocks) return;
+  const int bx = b % g.bpdx, by = b / g.bpdx;
+  bool f = false;
+  if (S.cfg.kind == CUP2D_SHAPE_DISK) {
+    f = lane == 0 && disk_touching(g, S, bx, by);
+  } else {
+    const double start[2] = {cell_x(g, bx, 0), cell_y(g, by, 0)};
+    const double end[2] = {cell_x(g, bx, BS - 1), cell_y(g, by, BS - 1)};
+    for (int q = lane; q < S.nseg && !f; q += 32)
+      f = segment_hits_block(segs.seg[k][q], start, end, 2 * g.h);
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, f);
+  if (lane == 0) flags[(size_t)k * g.nblocks + b] = m != 0;
+}
+
+// Deterministic compaction of the touched blocks in increasing block order
+// (the order of obstacleBlocks[blockID]).
 __global__ void __launch_bounds__(1024)
-k_tiles(GridDesc g, DevShape* sh, AllTiles T, FishSegPtrs segs, Scalars* sc)
+k_tile_compact(GridDesc g, DevShape* sh, AllTiles T, const int* flags, Scalars* sc)
 {
   __shared__ int warpCount[32];
   __shared__ int base;
@@ -101,12 +126,7 @@ k_tiles(GridDesc g, DevShape* sh, AllTiles T, FishSegPtrs segs, Scalars* sc)
   __syncthreads();
   for (int b0 = 0; b0 < g.nblocks; b0 += 1024) {
     const int b = b0 + tid;
-    bool f = false;
-    if (b < g.nblocks) {
-      const int bx = b % g.bpdx, by = b / g.bpdx;
-      if (S.cfg.kind == CUP2D_SHAPE_DISK) f = disk_touching(g, S, bx, by);
-      else f = fish_block_touching(g, segs.seg[k], S.nseg, bx, by);
-    }
+    const bool f = b < g.nblocks && flags[(size_t)k * g.nblocks + b];
     const unsigned m = __ballot_sync(0xffffffffu, f);
     if (lane == 0) warpCount[wid] = __popc(m);
     __syncthreads();
@@ -216,69 +236,70 @@ k_chi(GridDesc g, const DevShape* sh, AllTiles T, const double* __restrict__ sdf
 }
 
 // PutObjectsOnGrid.cpp:118-122 (CoM correction) + Shape::removeMoments
-// (Shape.cpp:117-212): one CTA per shape walks all of its tiles.
+// (Shape.cpp:117-212).  Every CTA forms the corrected CoM from putChiOnGrid's
+// per-tile sums (same fixed order in every CTA), integrates its own tile;
+// the last CTA of the shape finalises M, J, d_gm and the rigid udef part,
+// which consumers subtract where they read udef (udef_at).
 __global__ void __launch_bounds__(1024)
-k_moments(GridDesc g, DevShape* sh, AllTiles T, const double* partials, int partStride)
+k_moments(GridDesc g, DevShape* sh, AllTiles T, const double* chiParts, double* parts,
+          int partStride, unsigned* counters)
 {
   __shared__ double red[32 * 7];
-  __shared__ double bc[5];
-  const int k = blockIdx.x;
+  __shared__ double bc[3];
+  const int k = blockIdx.y, s = blockIdx.x, tid = lin_tid();
   DevShape& S = sh[k];
   const ObstTiles& t = T.t[k];
-  const int nt = S.ntiles, tid = threadIdx.x;
-  double a3[3] = {0, 0, 0};
-  for (int s = tid; s < nt; s += blockDim.x)
-    for (int q = 0; q < 3; q++) a3[q] += partials[(size_t)k * partStride + 3 * s + q];
-  block_sum<3>(a3, red);
-  if (tid == 0) {
-    if (a3[2] > EPSd) {
-      S.s.com[0] += a3[0] / a3[2];
-      S.s.com[1] += a3[1] / a3[2];
-      S.s.M = a3[2];
+  const int nt = S.ntiles;
+  const double* cp = chiParts + (size_t)k * partStride;
+  double* mp = parts + (size_t)k * partStride;
+  {                                   // every CTA (the last one included) forms the CoM
+    double a3[3] = {0, 0, 0};
+    for (int i = tid; i < nt; i += 1024)
+      for (int q = 0; q < 3; q++) a3[q] += cp[3 * i + q];
+    block_sum<3>(a3, red);
+    if (tid == 0) {
+      double c0 = S.s.com[0], c1 = S.s.com[1], M = -1;
+      if (a3[2] > EPSd) { c0 += a3[0] / a3[2]; c1 += a3[1] / a3[2]; M = a3[2]; }
+      bc[0] = c0; bc[1] = c1; bc[2] = M;
     }
-    bc[0] = S.s.com[0]; bc[1] = S.s.com[1];
+    __syncthreads();
   }
-  __syncthreads();
-  const double C0 = bc[0], C1 = bc[1];
-  const double hsq = g.h * g.h, rho = S.rhoTile;
-  double I[7] = {0, 0, 0, 0, 0, 0, 0};   // x, y, m, j, u, v, a
-  for (int s = 0; s < nt; s++) {
+  if (s < nt) {
+    const double C0 = bc[0], C1 = bc[1];
+    const double hsq = g.h * g.h, rho = S.rhoTile;
+    double I[7] = {0, 0, 0, 0, 0, 0, 0};   // x, y, m, j, u, v, a
     const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
     const int ix = tid % BS, iy = tid / BS;
     const size_t o = (size_t)s * BS2 + tid;
     const double X = t.chi[o];
-    if (X <= 0) continue;
-    const double p0 = cell_x(g, bx, ix) - C0, p1 = cell_y(g, by, iy) - C1;
-    const double rhochi = X * rho * hsq;
-    const double ux = t.udx[o], uy = t.udy[o];
-    I[0] += rhochi * p0;
-    I[1] += rhochi * p1;
-    I[2] += rhochi;
-    I[3] += rhochi * (p0 * p0 + p1 * p1);
-    I[4] += rhochi * ux;
-    I[5] += rhochi * uy;
-    I[6] += rhochi * (p0 * uy - p1 * ux);
+    if (X > 0) {
+      const double p0 = cell_x(g, bx, ix) - C0, p1 = cell_y(g, by, iy) - C1;
+      const double rhochi = X * rho * hsq;
+      const double ux = t.udx[o], uy = t.udy[o];
+      I[0] = rhochi * p0;
+      I[1] = rhochi * p1;
+      I[2] = rhochi;
+      I[3] = rhochi * (p0 * p0 + p1 * p1);
+      I[4] = rhochi * ux;
+      I[5] = rhochi * uy;
+      I[6] = rhochi * (p0 * uy - p1 * ux);
+    }
+    block_sum<7>(I, red);
+    if (tid == 0) for (int q = 0; q < 7; q++) mp[3 * t.capacity + 7 * s + q] = I[q];
   }
+  if (!last_block_done(counters + k, gridDim.x)) return;
+  double I[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int i = tid; i < nt; i += 1024)
+    for (int q = 0; q < 7; q++) I[q] += mp[3 * t.capacity + 7 * i + q];
   block_sum<7>(I, red);
-  if (tid == 0) {
-    const double Iu = I[4] / I[2], Iv = I[5] / I[2], Ia = I[6] / I[3];
-    S.s.M = I[2]; S.s.J = I[3];
-    const double dCx = S.s.center[0] - S.s.com[0], dCy = S.s.center[1] - S.s.com[1];
-    const double co = cos(S.s.orientation), si = sin(S.s.orientation);
-    S.s.d_gm[0] = dCx * co + dCy * si;
-    S.s.d_gm[1] = -dCx * si + dCy * co;
-    bc[2] = Iu; bc[3] = Iv; bc[4] = Ia;
-  }
-  __syncthreads();
-  const double Iu = bc[2], Iv = bc[3], Ia = bc[4];
-  for (int s = 0; s < nt; s++) {
-    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
-    const int ix = tid % BS, iy = tid / BS;
-    const size_t o = (size_t)s * BS2 + tid;
-    const double p0 = cell_x(g, bx, ix) - C0, p1 = cell_y(g, by, iy) - C1;
-    t.udx[o] -= Iu - Ia * p1;
-    t.udy[o] -= Iv + Ia * p0;
-  }
+  if (tid != 0 || nt == 0) return;
+  if (bc[2] > 0) { S.s.com[0] = bc[0]; S.s.com[1] = bc[1]; S.s.M = bc[2]; }
+  S.Iu = I[4] / I[2]; S.Iv = I[5] / I[2]; S.Ia = I[6] / I[3];
+  S.s.M = I[2]; S.s.J = I[3];
+  const double dCx = S.s.center[0] - S.s.com[0], dCy = S.s.center[1] - S.s.com[1];
+  const double co = cos(S.s.orientation), si = sin(S.s.orientation);
+  S.s.d_gm[0] = dCx * co + dCy * si;
+  S.s.d_gm[1] = -dCx * si + dCy * co;
 }
 
 // PutObjectsOnGrid::putObjectVelOnGrid (PutObjectsOnGrid.cpp:149-184), used at
@@ -295,8 +316,11 @@ k_udef_grid(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* ch
   const size_t c = (size_t)(by * BS + iy) * g.nx + bx * BS + ix;
   const double X = t.chi[o];
   if (X < chig[c] || X <= 0) return;
-  udx[c] += t.udx[o];
-  udy[c] += t.udy[o];
+  const DevShape& S = sh[k];
+  double u0, u1;
+  udef_at(t, o, S, cell_x(g, bx, ix) - S.s.com[0], cell_y(g, by, iy) - S.s.com[1], u0, u1);
+  udx[c] += u0;
+  udy[c] += u1;
 }
 
 // ---------------------------------------------------------------------------
@@ -376,42 +400,54 @@ k_rhs_corr(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __r
 }
 
 // PressureSingle::integrateMomenta (PressureSingle.cpp:23-67) with the
-// EXPL_INTEGRATE_MOM weights (:20), then Shape::updateVelocity.
+// EXPL_INTEGRATE_MOM weights (:20): 7 sums per tile, then the last CTA of
+// the shape runs Shape::updateVelocity.
 __global__ void __launch_bounds__(1024)
 k_momenta(GridDesc g, const Scalars* sc, DevShape* sh, AllTiles T,
-          const double* __restrict__ u, const double* __restrict__ v)
+          const double* __restrict__ u, const double* __restrict__ v,
+          double* parts, int partStride, unsigned* counters)
 {
   __shared__ double red[32 * 7];
-  const int k = blockIdx.x, tid = threadIdx.x;
+  const int k = blockIdx.y, s = blockIdx.x, tid = lin_tid();
   DevShape& S = sh[k];
   const ObstTiles& t = T.t[k];
-  const double Cx = S.s.com[0], Cy = S.s.com[1];
-  const double hsq = g.h * g.h, rho = S.rhoTile;
-  double A[7] = {0, 0, 0, 0, 0, 0, 0};   // PM, PJ, PX, PY, UM, VM, AM
-  for (int s = 0; s < S.ntiles; s++) {
+  const int nt = S.ntiles;
+  double* mp = parts + (size_t)k * partStride + 10 * (size_t)t.capacity;
+  if (s < nt) {
+    const double Cx = S.s.com[0], Cy = S.s.com[1];
+    const double hsq = g.h * g.h, rho = S.rhoTile;
+    double A[7] = {0, 0, 0, 0, 0, 0, 0};   // PM, PJ, PX, PY, UM, VM, AM
     const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
     const int ix = tid % BS, iy = tid / BS;
     const size_t o = (size_t)s * BS2 + tid;
     const double chi = t.chi[o];
-    if (chi <= 0) continue;
-    const size_t c = (size_t)(by * BS + iy) * g.nx + bx * BS + ix;
-    const double ud0 = u[c] - t.udx[o], ud1 = v[c] - t.udy[o];
-    const double F = hsq * rho * chi;
-    const double p0 = cell_x(g, bx, ix) - Cx, p1 = cell_y(g, by, iy) - Cy;
-    A[0] += F;
-    A[1] += F * (p0 * p0 + p1 * p1);
-    A[2] += F * p0;
-    A[3] += F * p1;
-    A[4] += F * ud0;
-    A[5] += F * ud1;
-    A[6] += F * (p0 * ud1 - p1 * ud0);
+    if (chi > 0) {
+      const size_t c = (size_t)(by * BS + iy) * g.nx + bx * BS + ix;
+      const double p0 = cell_x(g, bx, ix) - Cx, p1 = cell_y(g, by, iy) - Cy;
+      double ux, uy;
+      udef_at(t, o, S, p0, p1, ux, uy);
+      const double ud0 = u[c] - ux, ud1 = v[c] - uy;
+      const double F = hsq * rho * chi;
+      A[0] = F;
+      A[1] = F * (p0 * p0 + p1 * p1);
+      A[2] = F * p0;
+      A[3] = F * p1;
+      A[4] = F * ud0;
+      A[5] = F * ud1;
+      A[6] = F * (p0 * ud1 - p1 * ud0);
+    }
+    block_sum<7>(A, red);
+    if (tid == 0) for (int q = 0; q < 7; q++) mp[7 * s + q] = A[q];
   }
+  if (!last_block_done(counters + k, gridDim.x)) return;
+  double A[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int i = tid; i < nt; i += 1024)
+    for (int q = 0; q < 7; q++) A[q] += mp[7 * i + q];
   block_sum<7>(A, red);
-  if (tid == 0) {
-    S.s.fluidAngMom = A[6]; S.s.fluidMomX = A[4]; S.s.fluidMomY = A[5];
-    S.s.penalDX = A[2]; S.s.penalDY = A[3]; S.s.penalM = A[0]; S.s.penalJ = A[1];
-    shape_update_velocity(S, sc->dt, sc->time);
-  }
+  if (tid != 0) return;
+  S.s.fluidAngMom = A[6]; S.s.fluidMomX = A[4]; S.s.fluidMomY = A[5];
+  S.s.penalDX = A[2]; S.s.penalDY = A[3]; S.s.penalM = A[0]; S.s.penalJ = A[1];
+  shape_update_velocity(S, sc->dt, sc->time);
 }
 
 // PressureSingle::preventCollidingObstacles (PressureSingle.cpp:243-344).
@@ -442,11 +478,14 @@ k_collide(GridDesc g, const Scalars* sc, DevShape* sh, int nsh, AllTiles T)
         const double iUr = -iW * (p1 - iCy), iVr = iW * (p0 - iCx);
         const double jUr = -jW * (p1 - jCy), jVr = jW * (p0 - jCx);
         a[0] += iChi; a[1] += iChi * p0; a[2] += iChi * p1;
-        a[3] += iChi * (iUl + iUr + T.t[i].udx[(size_t)s * BS2 + tid]);
-        a[4] += iChi * (iVl + iVr + T.t[i].udy[(size_t)s * BS2 + tid]);
+        double iu0, iu1, ju0, ju1;
+        udef_at(T.t[i], (size_t)s * BS2 + tid, Si, p0 - iCx, p1 - iCy, iu0, iu1);
+        udef_at(T.t[j], (size_t)sj * BS2 + tid, Sj, p0 - jCx, p1 - jCy, ju0, ju1);
+        a[3] += iChi * (iUl + iUr + iu0);
+        a[4] += iChi * (iVl + iVr + iu1);
         a[5] += jChi; a[6] += jChi * p0; a[7] += jChi * p1;
-        a[8] += jChi * (jUl + jUr + T.t[j].udx[(size_t)sj * BS2 + tid]);
-        a[9] += jChi * (jVl + jVr + T.t[j].udy[(size_t)sj * BS2 + tid]);
+        a[8] += jChi * (jUl + jUr + ju0);
+        a[9] += jChi * (jVl + jVr + ju1);
       }
     }
     block_sum<10>(a, red);
@@ -507,8 +546,10 @@ k_penalize(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __r
   if (X <= 0) return;
   const double p0 = cell_x(g, bx, ix) - S.s.com[0], p1 = cell_y(g, by, iy) - S.s.com[1];
   const double alpha = 1 - X;
-  const double US = S.s.u - S.s.omega * p1 + t.udx[o];
-  const double VS = S.s.v + S.s.omega * p0 + t.udy[o];
+  double ux, uy;
+  udef_at(t, o, S, p0, p1, ux, uy);
+  const double US = S.s.u - S.s.omega * p1 + ux;
+  const double VS = S.s.v + S.s.omega * p0 + uy;
   u[c] = alpha * u[c] + (1 - alpha) * US;
   v[c] = alpha * v[c] + (1 - alpha) * VS;
 }
@@ -555,7 +596,8 @@ k_forces(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ u,
       const double fYV = D12 * normX + D22 * normY, fYP = -P * normY;
       const double fXT = fXV + fXP, fYT = fYV + fYP;
       const double vx = u[I(gx, gy)], vy = v[I(gx, gy)];
-      const double vxDef = t.udx[o], vyDef = t.udy[o];
+      double vxDef, vyDef;
+      udef_at(t, o, S, p0 - Cx, p1 - Cy, vxDef, vyDef);
       F[0] = sqrt(normX * normX + normY * normY);          // perimeter
       F[1] = fXT; F[2] = fYT;                               // forcex, forcey
       F[3] = fXP; F[4] = fYP;                               // forcex_P, forcey_P
@@ -575,9 +617,11 @@ k_forces(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ u,
       F[16] = fmin(0.0, powDef);                            // defPowerBnd
     }
   }
-  block_sum<NFORCE>(F, red);
   double* part = partials + (size_t)k * partStride;
-  if (lin_tid() == 0) for (int q = 0; q < NFORCE; q++) part[NFORCE * s + q] = F[q];
+  if (s < S.ntiles) {
+    block_sum<NFORCE>(F, red);
+    if (lin_tid() == 0) for (int q = 0; q < NFORCE; q++) part[NFORCE * s + q] = F[q];
+  }
   if (!last_block_done(counters + k, gridDim.x)) return;
   double tot[NFORCE];
 #pragma unroll
@@ -606,18 +650,30 @@ inline double* shape_partials(const Ctx& c) { return c.partials + (size_t)3 * c.
 
 } // namespace
 
-void launch_objects(Ctx& c) {
+void launch_objects_begin(Ctx& c, bool midlineReady) {
+  if (c.nshapes == 0) return;
+  // fish midlines at the current time (Fish.cpp:79-95) unless the previous
+  // step already computed them on its side branch
+  if (!midlineReady)
+    for (int k = 0; k < c.nshapes; k++)
+      if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.stream, 0);
+  k_obj_begin<<<1, 32, 0, c.stream>>>(c.g, c.dsc, c.dshapes, c.nshapes);
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_objects_rest(Ctx& c) {
   if (c.nshapes == 0) return;
   const AllTiles T = all_tiles(c);
   const int cap = c.maxCapacity;
-  k_obj_begin<<<1, 32, 0, c.stream>>>(c.g, c.dsc, c.dshapes, c.nshapes);
-  CUP2D_LAUNCHED(c);
   k_clear_old<<<dim3(cap, c.nshapes), 256, 0, c.stream>>>(c.g, c.dshapes, T, c.chi, c.sdf);
   CUP2D_LAUNCHED(c);
-  // fish midlines, frames and AreaSegments (Fish::create, Fish.cpp:20-110)
+  // frames and AreaSegments (Fish.cpp:95-150)
   for (int k = 0; k < c.nshapes; k++)
     if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_kinematics(c, k);
-  k_tiles<<<c.nshapes, 1024, 0, c.stream>>>(c.g, c.dshapes, T, fish_seg_ptrs(c), c.dsc);
+  k_tile_flags<<<dim3((c.g.nblocks + 7) / 8, c.nshapes), 256, 0, c.stream>>>(c.g, c.dshapes, fish_seg_ptrs(c),
+                                                                              c.tileFlags);
+  CUP2D_LAUNCHED(c);
+  k_tile_compact<<<c.nshapes, 1024, 0, c.stream>>>(c.g, c.dshapes, T, c.tileFlags, c.dsc);
   CUP2D_LAUNCHED(c);
   bool anyDisk = false, anyFish = false;
   for (int k = 0; k < c.nshapes; k++) {
@@ -634,8 +690,14 @@ void launch_objects(Ctx& c) {
   k_chi<<<dim3(cap, c.nshapes), dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, T, c.sdf, c.chi,
                                                               shape_partials(c), stride);
   CUP2D_LAUNCHED(c);
-  k_moments<<<c.nshapes, 1024, 0, c.stream>>>(c.g, c.dshapes, T, shape_partials(c), stride);
+  k_moments<<<dim3(cap, c.nshapes), 1024, 0, c.stream>>>(c.g, c.dshapes, T, shape_partials(c),
+                                                          shape_partials(c), stride, c.counters + CNT_MOMENTS);
   CUP2D_LAUNCHED(c);
+}
+
+void launch_objects(Ctx& c, bool midlineReady) {
+  launch_objects_begin(c, midlineReady);
+  launch_objects_rest(c);
 }
 
 void launch_obj_vel_on_grid(Ctx& c) {
@@ -663,7 +725,8 @@ void launch_rhs_obstacles(Ctx& c) {
 void launch_momenta_penalize(Ctx& c) {
   if (c.nshapes == 0) return;
   const AllTiles T = all_tiles(c);
-  k_momenta<<<c.nshapes, 1024, 0, c.stream>>>(c.g, c.dsc, c.dshapes, T, c.u(), c.v());
+  k_momenta<<<dim3(c.maxCapacity, c.nshapes), 1024, 0, c.stream>>>(
+      c.g, c.dsc, c.dshapes, T, c.u(), c.v(), shape_partials(c), (int)shape_region(c), c.counters + CNT_MOMENTA);
   CUP2D_LAUNCHED(c);
   if (c.nshapes > 1) {
     k_collide<<<1, 1024, 0, c.stream>>>(c.g, c.dsc, c.dshapes, c.nshapes, T);

@@ -85,8 +85,12 @@ def test_advdiff_stage_bitwise(ref):
     compare_fields(r, s, ["u", "v"], 1e-14, "advDiff")
 
 
-def test_pressure_stage(ref):
-    r, s = make_pair(ref, DISK, noise_seed=11)
+DISK_PERIODIC = DISK.replace("freespace", "periodic")
+
+
+@pytest.mark.parametrize("args", [DISK, DISK_PERIODIC], ids=["freespace", "periodic"])
+def test_pressure_stage(ref, args):
+    r, s = make_pair(ref, args, noise_seed=11)
     dt = 1e-3
     r.run_op("advDiff", dt); s.ctx.adv_diff(dt)
     r.run_op("PressureSingle", dt); s.ctx.pressure_single(dt)
@@ -148,9 +152,10 @@ def test_degenerate_fish_midline_is_rejected():
     assert "EINVAL" in str(e.value)
 
 
-def test_graph_replay_matches_eager():
-    a = Simulation(DISK); a.init()
-    b = Simulation(DISK); b.init()
+@pytest.mark.parametrize("args", [DISK, FISH], ids=["disk", "fish"])
+def test_graph_replay_matches_eager(args):
+    a = Simulation(args); a.init()
+    b = Simulation(args); b.init()
     for comp, name in enumerate(("u", "v")):
         n = noise_field(1, comp, a.ctx.ny, a.ctx.nx)
         a.ctx.set(name, n); b.ctx.set(name, n)
