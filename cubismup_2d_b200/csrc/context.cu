@@ -212,6 +212,8 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
   c.cfg = *cfg;
   c.device = cfg->device;
   if (cudaSetDevice(c.device) != cudaSuccess) { delete ctx; return CUP2D_ECUDA; }
+  cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, c.device);
+  if (c.sms <= 0) c.sms = 1;
   if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return CUP2D_ECUDA; }
   GridDesc& g = c.g;
   g.bpdx = cfg->bpdx; g.bpdy = cfg->bpdy;
@@ -275,7 +277,10 @@ int cup2d_destroy(cup2d_ctx* ctx) {
     cudaFree(t.tiles); cudaFree(t.slot); cudaFree(t.chi); cudaFree(t.dist); cudaFree(t.udx);
     cudaFree(t.udy); cudaFree(t.sD); cudaFree(t.sdx); cudaFree(t.sdy);
   }
-  for (auto& f : c.fish) { cudaFree(f.pool); cudaFree(f.seg); }
+  for (auto& f : c.fish) {
+    cudaFree(f.pool); cudaFree(f.seg); cudaFree(f.nw); cudaFree(f.off);
+    cudaFree(f.sp); cudaFree(f.su); cudaFree(f.ip); cudaFree(f.iu); cudaFree(f.ipIdx);
+  }
   poisson_destroy(c.poisson);
   if (c.stream) cudaStreamDestroy(c.stream);
   delete ctx;
@@ -361,6 +366,28 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
       }
       F.integ = q;
     }
+    // interior-point layout of PutFishOnBlocks::constructInternl
+    // (FishLibrary.cpp:594-596): Nw = floor(width/h) points each side
+    std::vector<int> nw(Nm), off(Nm + 1, 0);
+    for (int i = 0; i < Nm; i++) {
+      nw[i] = (int)std::floor(width[i] / h);
+      off[i + 1] = off[i] + (nw[i] > 0 ? 2 * nw[i] - 1 : 0);
+    }
+    F.nint = off[Nm];
+    if (!rc) rc = dalloc(ctx, &F.nw, Nm);
+    if (!rc) rc = dalloc(ctx, &F.off, Nm + 1);
+    if (!rc) rc = dalloc(ctx, &F.sp, 2 * (size_t)Nm);
+    if (!rc) rc = dalloc(ctx, &F.su, 2 * (size_t)Nm);
+    if (!rc) rc = dalloc(ctx, &F.ip, (size_t)F.nint);
+    if (!rc) rc = dalloc(ctx, &F.iu, (size_t)F.nint);
+    if (!rc) rc = dalloc(ctx, &F.ipIdx, (size_t)F.nint);
+    if (rc) return rc;
+    std::vector<int2> ipIdx(F.nint);
+    for (int i = 0; i < Nm; i++)
+      for (int j = 0; j < (nw[i] > 0 ? 2 * nw[i] - 1 : 0); j++) ipIdx[off[i] + j] = make_int2(i, -nw[i] + 1 + j);
+    CK(cudaMemcpy(F.ipIdx, ipIdx.data(), sizeof(int2) * F.nint, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(F.nw, nw.data(), sizeof(int) * Nm, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(F.off, off.data(), sizeof(int) * (Nm + 1), cudaMemcpyHostToDevice));
     // curvature control values, StefanFish.cpp:187-193, splined onto rS
     const double L = f.length;
     const double pts[6] = {0, .15 * L, .4 * L, .65 * L, .9 * L, L};
@@ -658,3 +685,34 @@ int cup2d_advance_timed(cup2d_ctx* ctx, int nsteps, double* ms) {
 }
 
 } // extern "C"
+
+#ifdef CUP2D_TRACE
+// Timeline read-back of the optional trace build: out[2*id] / out[2*id+1]
+// are the first entry / last exit (%globaltimer, ns) of kernel id since the
+// last reset; reset re-arms the slots.
+namespace cup2d {
+void trace_bind_fluid(unsigned long long*);
+void trace_bind_obstacles(unsigned long long*);
+void trace_bind_fish(unsigned long long*);
+void trace_bind_poisson(unsigned long long*);
+}
+extern "C" int cup2d_trace(cup2d_ctx* ctx, unsigned long long* out, int reset) {
+  using namespace cup2d;
+  static unsigned long long* buf = nullptr;
+  if (!ctx) return CUP2D_EINVAL;
+  cudaSetDevice(ctx->c.device);
+  if (!buf) {
+    if (cudaMalloc(&buf, sizeof(unsigned long long) * 2 * TR_N) != cudaSuccess) return CUP2D_ENOMEM;
+    trace_bind_fluid(buf); trace_bind_obstacles(buf); trace_bind_fish(buf); trace_bind_poisson(buf);
+    reset = 1;
+  }
+  cudaDeviceSynchronize();
+  if (out) cudaMemcpy(out, buf, sizeof(unsigned long long) * 2 * TR_N, cudaMemcpyDeviceToHost);
+  if (reset) {
+    std::vector<unsigned long long> init(2 * TR_N);
+    for (int i = 0; i < TR_N; i++) { init[2 * i] = ~0ULL; init[2 * i + 1] = 0; }
+    cudaMemcpy(buf, init.data(), sizeof(unsigned long long) * 2 * TR_N, cudaMemcpyHostToDevice);
+  }
+  return CUP2D_OK;
+}
+#endif

@@ -12,6 +12,7 @@ struct Ctx {
   cup2d_config cfg{};
   GridDesc g{};
   int device = 0;
+  int sms = 148;                // streaming multiprocessors of the device
   cudaStream_t stream = nullptr;
   bool initialised = false;
 

@@ -15,12 +15,13 @@
 // k_fish_frame (one CTA per fish): changeToCoMFrameAngular with the current
 //   theta_internal (FishLibrary.cpp:161-176) and the AreaSegment boxes in the
 //   computational frame (Fish.cpp:118-150, FishLibrary.cpp:295-342).
-// k_fish_raster (16 CTAs per obstacle tile, one per 8x8 cells):
+// k_fish_raster (4 CTAs per obstacle tile, one per 16x16 cells):
 //   PutFishOnBlocks (FishLibrary.cpp:403-638).  The reference scatters every
 //   surface / interior point of every intersecting segment onto the block;
-//   here each CTA keeps, in the reference's loop order (segment, s index,
-//   side or width offset), only the points whose support reaches its 8x8
-//   cells, and every cell applies them in that order, so its "keep the
+//   here each CTA walks the points of the block's segments in the
+//   reference's loop order (segment, s index, side or width offset), keeps
+//   those whose support reaches its 16x16 cells, and every cell applies them
+//   in that order, so its "keep the
 //   nearest" updates (ties included) and its hat-kernel sums see exactly the
 //   reference's sequence.
 #include <cmath>
@@ -54,6 +55,7 @@ __device__ __forceinline__ void cubic_interp(double x0, double x1, double x, dou
 __global__ void __launch_bounds__(512)
 k_fish_midline(const Scalars* sc, const DevShape* sh, int k, FishArrays F, int mode)
 {
+  CUP2D_TRACE_SCOPE(TR_MIDLINE);
   extern __shared__ double smem[];
   __shared__ double red[32 * 5];
   __shared__ double bc[4];
@@ -127,8 +129,10 @@ k_fish_midline(const Scalars* sc, const DevShape* sh, int k, FishArrays F, int m
         vKsiY += ds * dvKsiY;
         const double d1 = ksiX * ksiX + ksiY * ksiY;
         const double d2 = nX * nX + nY * nY;
-        if (d1 > EPSd) { const double nf = 1 / sqrt(d1); ksiX *= nf; ksiY *= nf; }
-        if (d2 > EPSd) { const double nf = 1 / sqrt(d2); nX *= nf; nY *= nf; }
+        // both factors first, so the two sqrt/divide sequences overlap
+        const double nf1 = 1 / sqrt(d1), nf2 = 1 / sqrt(d2);
+        if (d1 > EPSd) { ksiX *= nf1; ksiY *= nf1; }
+        if (d2 > EPSd) { nX *= nf2; nY *= nf2; }
         rX[i] = rx; rY[i] = ry; vX[i] = vx; vY[i] = vy;
         norX[i] = nX; norY[i] = nY; vNorX[i] = vnX; vNorY[i] = vnY;
         sPrev = sNow;
@@ -238,6 +242,8 @@ k_fish_midline(const Scalars* sc, const DevShape* sh, int k, FishArrays F, int m
 __global__ void __launch_bounds__(512)
 k_fish_frame(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays F)
 {
+  CUP2D_TRACE_SCOPE(TR_FRAME);
+  extern __shared__ double fsm[];                      // the frame midline, staged
   __shared__ double bc[2];
   DevShape& S = sh[k];
   const int Nm = F.nm, tid = threadIdx.x, nt = blockDim.x;
@@ -252,6 +258,12 @@ k_fish_frame(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays F)
     S.f.angvel_internal = integ[6];
     bc[0] = S.f.theta_internal; bc[1] = integ[6];
   }
+  double* rX = fsm;           double* rY = rX + Nm;
+  double* vX = rY + Nm;       double* vY = vX + Nm;
+  double* norX = vY + Nm;     double* norY = norX + Nm;
+  double* vNorX = norY + Nm;  double* vNorY = vNorX + Nm;
+  double* width = vNorY + Nm; double* rS = width + Nm;
+  for (int i = tid; i < Nm; i += nt) { width[i] = F.width[i]; rS[i] = F.rS[i]; }
   __syncthreads();
   const FishMidline& M = F.mid[p];
   const FishMidline& R = F.frame;
@@ -261,21 +273,20 @@ k_fish_frame(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays F)
     for (int i = tid; i < Nm; i += nt) {
       const double px = M.rX[i], py = M.rY[i];
       const double qx = M.vX[i] + vAin * py, qy = M.vY[i] - vAin * px;
-      R.rX[i] = R00 * px + R01 * py; R.rY[i] = R10 * px + R11 * py;
-      R.vX[i] = R00 * qx + R01 * qy; R.vY[i] = R10 * qx + R11 * qy;
+      const double a = R00 * px + R01 * py, b = R10 * px + R11 * py;
+      const double c = R00 * qx + R01 * qy, d = R10 * qx + R11 * qy;
+      rX[i] = a; rY[i] = b; vX[i] = c; vY[i] = d;
+      R.rX[i] = a; R.rY[i] = b; R.vX[i] = c; R.vY[i] = d;
     }
     __syncthreads();
-    for (int i = tid; i < Nm - 1; i += nt) {            // _computeMidlineNormals
-      const double ds = F.rS[i + 1] - F.rS[i];
-      const double tX = R.rX[i + 1] - R.rX[i], tY = R.rY[i + 1] - R.rY[i];
-      const double tVX = R.vX[i + 1] - R.vX[i], tVY = R.vY[i + 1] - R.vY[i];
-      R.norX[i] = -tY / ds; R.norY[i] = tX / ds;
-      R.vNorX[i] = -tVY / ds; R.vNorY[i] = tVX / ds;
-    }
-    __syncthreads();
-    if (tid == 0) {
-      R.norX[Nm - 1] = R.norX[Nm - 2]; R.norY[Nm - 1] = R.norY[Nm - 2];
-      R.vNorX[Nm - 1] = R.vNorX[Nm - 2]; R.vNorY[Nm - 1] = R.vNorY[Nm - 2];
+    for (int i = tid; i < Nm; i += nt) {                // _computeMidlineNormals
+      const int j = i < Nm - 1 ? i : Nm - 2;            // the last copies its neighbour
+      const double ds = rS[j + 1] - rS[j];
+      const double tX = rX[j + 1] - rX[j], tY = rY[j + 1] - rY[j];
+      const double tVX = vX[j + 1] - vX[j], tVY = vY[j + 1] - vY[j];
+      const double a = -tY / ds, b = tX / ds, c = -tVY / ds, d = tVX / ds;
+      norX[i] = a; norY[i] = b; vNorX[i] = c; vNorY[i] = d;
+      R.norX[i] = a; R.norY[i] = b; R.vNorX[i] = c; R.vNorY[i] = d;
     }
     __syncthreads();
   }
@@ -283,8 +294,6 @@ k_fish_frame(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays F)
   const int Nseg = F.nseg;
   const double angle = S.s.orientation;
   const double R00 = cos(angle), R01 = -sin(angle), R10 = sin(angle), R11 = cos(angle);
-  const double* rX = R.rX; const double* rY = R.rY;
-  const double* norX = R.norX; const double* norY = R.norY; const double* width = F.width;
   for (int i = tid; i < Nseg; i += nt) {
     const int next_idx = (i + 1) * (Nm - 1) / Nseg, idx = i * (Nm - 1) / Nseg;
     double bb[2][2] = {{1e9, -1e9}, {1e9, -1e9}};
@@ -320,55 +329,127 @@ k_fish_frame(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays F)
     }
     F.seg[i] = sg;
   }
+  // surface points of constructSurface (FishLibrary.cpp:470-486) and interior
+  // points of constructInternl (FishLibrary.cpp:597-610), computational frame
+  const double pos0 = S.s.center[0], pos1 = S.s.center[1];
+  for (int q = tid; q < 2 * Nm; q += nt) {
+    const int ss = q >> 1, signp = (q & 1) ? 1 : -1;
+    const double m0 = rX[ss] + width[ss] * signp * norX[ss];
+    const double m1 = rY[ss] + width[ss] * signp * norY[ss];
+    F.sp[q] = make_double2(R00 * m0 + R01 * m1 + pos0, R10 * m0 + R11 * m1 + pos1);
+    const double u0 = vX[ss] + width[ss] * signp * vNorX[ss];
+    const double u1 = vY[ss] + width[ss] * signp * vNorY[ss];
+    F.su[q] = make_double2(R00 * u0 + R01 * u1, R10 * u0 + R11 * u1);
+  }
+  const double h = g.h;
+  for (int q = tid; q < F.nint; q += nt) {
+    const int2 si = F.ipIdx[q];
+    const int ss = si.x, iw = si.y;
+    const double offsetW = iw * h;
+    const double m0 = rX[ss] + offsetW * norX[ss], m1 = rY[ss] + offsetW * norY[ss];
+    F.ip[q] = make_double2(R00 * m0 + R01 * m1 + pos0, R10 * m0 + R11 * m1 + pos1);
+    const double u0 = vX[ss] + offsetW * vNorX[ss], u1 = vY[ss] + offsetW * vNorY[ss];
+    F.iu[q] = make_double2(R00 * u0 + R01 * u1, R10 * u0 + R11 * u1);
+  }
   if (tid == 0) S.nseg = Nseg;
 }
 
 struct SurfPt { double myP[2], pP[2], pM[2], ud[2]; int iap[2], ss; };
 struct IntPt { double ud[2], w[2][2]; int iap[2]; };
 
-constexpr int SUB = 8;                      // cells per sub-tile edge
+constexpr int SUB = 16;                     // cells per sub-tile edge
 constexpr int NSUB = (BS / SUB) * (BS / SUB);
 constexpr int RT = SUB * SUB;               // threads per CTA (one per cell)
-constexpr int MAX_SEG_PER_TILE = 512;
+constexpr int NWARP = RT / 32;
+constexpr int MAX_SEG_PER_TILE = 256;
 
-// order-preserving compaction over the CTA's two warps; returns the count
+// order-preserving compaction over the CTA's warps; returns the count
 __device__ __forceinline__ int compact_slot(bool keep, int* wc, int& pos) {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const unsigned m = __ballot_sync(0xffffffffu, keep);
   if (lane == 0) wc[wid] = __popc(m);
   __syncthreads();
-  pos = (wid == 1 ? wc[0] : 0) + __popc(m & ((1u << lane) - 1u));
-  return wc[0] + wc[1];
+  int off = 0, tot = 0;
+  for (int w = 0; w < NWARP; w++) { if (w < wid) off += wc[w]; tot += wc[w]; }
+  pos = off + __popc(m & ((1u << lane) - 1u));
+  return tot;
+}
+
+// index of the list entry whose range [start[i], start[i+1]) holds q
+__device__ __forceinline__ int find_range(const int* start, int n, int q) {
+  int lo = 0, hi = n;            // start[0] = 0 <= q < start[n]
+  while (hi - lo > 1) { const int mid = (lo + hi) >> 1; if (start[mid] <= q) lo = mid; else hi = mid; }
+  return lo;
+}
+
+// Row lists: warp w owns the sub-tile rows 2w (lanes 0-15) and 2w+1 (lanes
+// 16-31).  It walks the chunk's kept points in order, 32 at a time, and
+// appends (ballot + popc, so order is kept) those whose support covers each
+// of its rows.  Every cell then visits only its row's points, in the
+// reference's order, and skips those whose columns miss it.
+struct RowLists {
+  unsigned short idx[SUB][RT];
+  int n[SUB];
+};
+
+__device__ __forceinline__ void rows_build(RowLists& Lr, const uchar4* supp, int nc, int sy0) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int rA = 2 * w, rB = 2 * w + 1;
+  int nA = 0, nB = 0;
+  for (int p0 = 0; p0 < nc; p0 += 32) {
+    const int p = p0 + lane;
+    bool inA = false, inB = false;
+    if (p < nc) {
+      const uchar4 sp = supp[p];          // x lo, x hi, y lo, y hi relative to the sub-tile
+      inA = sp.z <= rA && rA < sp.w;
+      inB = sp.z <= rB && rB < sp.w;
+    }
+    const unsigned mA = __ballot_sync(0xffffffffu, inA), mB = __ballot_sync(0xffffffffu, inB);
+    const unsigned lt = (1u << lane) - 1u;
+    if (inA) Lr.idx[rA][nA + __popc(mA & lt)] = (unsigned short)p;
+    if (inB) Lr.idx[rB][nB + __popc(mB & lt)] = (unsigned short)p;
+    nA += __popc(mA); nB += __popc(mB);
+  }
+  if (lane == 0) { Lr.n[rA] = nA; Lr.n[rB] = nB; }
+  __syncwarp();
+  (void)sy0;
 }
 
 __global__ void __launch_bounds__(RT)
 k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, double* sdfg)
 {
-  __shared__ int segList[MAX_SEG_PER_TILE];
+  CUP2D_TRACE_SCOPE(TR_RASTER);
+  __shared__ int segFst[MAX_SEG_PER_TILE];       // first s index of the segment's points (>= 1)
+  __shared__ int segIntBase[MAX_SEG_PER_TILE];   // its first interior point
+  __shared__ int segSurfCnt[MAX_SEG_PER_TILE], segIntCnt[MAX_SEG_PER_TILE];
+  __shared__ int surfStart[MAX_SEG_PER_TILE + 1];
+  __shared__ int intStart[MAX_SEG_PER_TILE + 1];
   __shared__ int nSegList;
-  __shared__ int wc[2];
-  __shared__ SurfPt sp[RT];
-  __shared__ IntPt ip[RT];
+  __shared__ int wc[NWARP];
+  __shared__ RowLists Lr;
+  __shared__ uchar4 supp[RT];
+  __shared__ union { SurfPt s[RT]; IntPt i[RT]; } pts;
+  extern __shared__ double msm[];                       // frame midline x, y and width
   const DevShape& S = sh[k];
-  const int s = blockIdx.x / NSUB, sub = blockIdx.x % NSUB;
-  if (s >= S.ntiles) return;
-  const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+  const int nwork = S.ntiles * NSUB;
+  if ((int)blockIdx.x >= nwork) return;
   const int tid = threadIdx.x;
-  const int sx0 = (sub % (BS / SUB)) * SUB, sy0 = (sub / (BS / SUB)) * SUB;
-  const int ix = sx0 + tid % SUB, iy = sy0 + tid / SUB;
+  const int Nm = F.nm;
+  double* rX = msm; double* rY = msm + Nm; double* width = msm + 2 * Nm;
+  for (int i = tid; i < Nm; i += RT) { rX[i] = F.frame.rX[i]; rY[i] = F.frame.rY[i]; width[i] = F.width[i]; }
   const double h = g.h, invh = 1.0 / h;
-  const double org0 = cell_x(g, bx, 0), org1 = cell_y(g, by, 0);
   const double angle = S.s.orientation;
   const double R00 = cos(angle), R01 = -sin(angle), R10 = sin(angle), R11 = cos(angle);
   const double pos0 = S.s.center[0], pos1 = S.s.center[1];
-  const int Nm = F.nm;
-  const FishMidline& R = F.frame;
-  const double* rX = R.rX; const double* rY = R.rY; const double* width = F.width;
-  const double* norX = R.norX; const double* norY = R.norY;
-  const double* vX = R.vX; const double* vY = R.vY;
-  const double* vNorX = R.vNorX; const double* vNorY = R.vNorY;
+  for (int wi = blockIdx.x; wi < nwork; wi += gridDim.x) {
+  const int s = wi / NSUB, sub = wi % NSUB;
+  const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+  const int sx0 = (sub % (BS / SUB)) * SUB, sy0 = (sub / (BS / SUB)) * SUB;
+  const int ix = sx0 + tid % SUB, iy = sy0 + tid / SUB;
+  const double org0 = cell_x(g, bx, 0), org1 = cell_y(g, by, 0);
 
-  // ordered list of the segments intersecting this block (Fish.cpp:167-173)
+  // ordered list of the segments intersecting this block (Fish.cpp:167-173),
+  // each with its point ranges of constructSurface / constructInternl
   if (tid == 0) nSegList = 0;
   __syncthreads();
   {
@@ -376,161 +457,167 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
     const double end[2] = {cell_x(g, bx, BS - 1), cell_y(g, by, BS - 1)};
     for (int s0 = 0; s0 < S.nseg; s0 += RT) {
       const int q = s0 + tid;
-      const bool f = q < S.nseg && segment_hits_block(F.seg[q], start, end, 2 * h);
+      bool f = false;
+      int fst = 0, sc = 0, ib = 0, ic = 0;
+      if (q < S.nseg) {
+        const Segment& sg = F.seg[q];
+        f = segment_hits_block(sg, start, end, 2 * h);
+        if (f) {
+          fst = max(sg.first, 1);
+          const int lst = min(sg.second, Nm - 2);
+          sc = max(0, (lst - fst + 1) * 2);
+          ib = F.off[fst];
+          ic = max(0, F.off[lst + 1] - ib);
+        }
+      }
       int pos;
       const int tot = compact_slot(f, wc, pos);
-      if (f && nSegList + pos < MAX_SEG_PER_TILE) segList[nSegList + pos] = q;
+      const int at = nSegList + pos;
+      if (f && at < MAX_SEG_PER_TILE) { segFst[at] = fst; segIntBase[at] = ib; segSurfCnt[at] = sc; segIntCnt[at] = ic; }
       __syncthreads();
       if (tid == 0) nSegList += tot;
       __syncthreads();
     }
   }
   const int nsl = nSegList < MAX_SEG_PER_TILE ? nSegList : MAX_SEG_PER_TILE;
+  if (tid == 0) {
+    surfStart[0] = 0; intStart[0] = 0;
+    for (int i = 0; i < nsl; i++) {
+      surfStart[i + 1] = surfStart[i] + segSurfCnt[i];
+      intStart[i + 1] = intStart[i] + segIntCnt[i];
+    }
+  }
+  __syncthreads();
+  const int totSurf = surfStart[nsl], totInt = intStart[nsl];
   const double px = cell_x(g, bx, ix), py = cell_y(g, by, iy);   // info.pos(p, sx, sy)
 
   // constructSurface (FishLibrary.cpp:438-573)
   double dist = -1, chi = 0, ud0 = 0, ud1 = 0;
-  for (int si = 0; si < nsl; si++) {
-    const Segment& sg = F.seg[segList[si]];
-    const int firstSegm = max(sg.first, 1), lastSegm = min(sg.second, Nm - 2);
-    const int npts = (lastSegm - firstSegm + 1) * 2;
-    for (int c0 = 0; c0 < npts; c0 += RT) {
-      SurfPt P;
-      bool keep = false;
-      const int q = c0 + tid;
-      if (q < npts) {
-        const int ss = firstSegm + q / 2, signp = (q & 1) ? 1 : -1;
-        P.ss = ss;
-        double m0 = rX[ss + 0] + width[ss + 0] * signp * norX[ss + 0];
-        double m1 = rY[ss + 0] + width[ss + 0] * signp * norY[ss + 0];
-        P.myP[0] = R00 * m0 + R01 * m1 + pos0; P.myP[1] = R10 * m0 + R11 * m1 + pos1;
-        P.iap[0] = (int)floor((P.myP[0] - org0) * invh);
-        P.iap[1] = (int)floor((P.myP[1] - org1) * invh);
-        const bool valid = !(P.iap[0] + 3 <= 0 || P.iap[0] - 1 >= BS) && !(P.iap[1] + 3 <= 0 || P.iap[1] - 1 >= BS);
-        // support [iap-1, iap+3) clipped to the block, intersected with this sub-tile
-        keep = valid && max(max(0, P.iap[0] - 1), sx0) < min(min(P.iap[0] + 3, BS), sx0 + SUB)
-                     && max(max(0, P.iap[1] - 1), sy0) < min(min(P.iap[1] + 3, BS), sy0 + SUB);
-        if (keep) {
-          m0 = rX[ss + 1] + width[ss + 1] * signp * norX[ss + 1];
-          m1 = rY[ss + 1] + width[ss + 1] * signp * norY[ss + 1];
-          P.pP[0] = R00 * m0 + R01 * m1 + pos0; P.pP[1] = R10 * m0 + R11 * m1 + pos1;
-          m0 = rX[ss - 1] + width[ss - 1] * signp * norX[ss - 1];
-          m1 = rY[ss - 1] + width[ss - 1] * signp * norY[ss - 1];
-          P.pM[0] = R00 * m0 + R01 * m1 + pos0; P.pM[1] = R10 * m0 + R11 * m1 + pos1;
-          const double u0 = vX[ss + 0] + width[ss + 0] * signp * vNorX[ss + 0];
-          const double u1 = vY[ss + 0] + width[ss + 0] * signp * vNorY[ss + 0];
-          P.ud[0] = R00 * u0 + R01 * u1; P.ud[1] = R10 * u0 + R11 * u1;
-        }
-      }
-      int pos;
-      const int nc = compact_slot(keep, wc, pos);
-      if (keep) sp[pos] = P;
-      __syncthreads();
-      for (int qq = 0; qq < nc; qq++) {
-        const SurfPt& Q = sp[qq];
-        if (iy < max(0, Q.iap[1] - 1) || iy >= min(Q.iap[1] + 3, BS)) continue;
-        if (ix < max(0, Q.iap[0] - 1) || ix >= min(Q.iap[0] + 3, BS)) continue;
-        const double dist0 = sq(px - Q.myP[0]) + sq(py - Q.myP[1]);
-        const double distP = sq(px - Q.pP[0]) + sq(py - Q.pP[1]);
-        const double distM = sq(px - Q.pM[0]) + sq(py - Q.pM[1]);
-        if (fabs(dist) < fmin(fmin(dist0, distP), distM)) continue;
-        // changeFromComputationalFrame (FishLibrary.h:194-200)
-        const double q0 = px - pos0, q1 = py - pos1;
-        const double p0 = R00 * q0 + R10 * q1, p1 = R01 * q0 + R11 * q1;
-        const int ss = Q.ss;
-        int close_s = ss, secnd_s = ss + (distP < distM ? 1 : -1);
-        double dist1 = dist0, dist2 = distP < distM ? distP : distM;
-        if (distP < dist0 || distM < dist0) {
-          dist1 = dist2; dist2 = dist0;
-          close_s = secnd_s; secnd_s = ss;
-        }
-        const double dSsq = sq(rX[close_s] - rX[secnd_s]) + sq(rY[close_s] - rY[secnd_s]);
-        const double cnt2ML = sq(width[close_s]);
-        const double nxt2ML = sq(width[secnd_s]);
-        const double safeW = fmax(width[close_s], width[secnd_s]) + 2 * h;
-        const double grd2ML = sq(p0 - rX[close_s]) + sq(p1 - rY[close_s]);
-        const double diffH = fabs(width[close_s] - width[secnd_s]);
-        double sign2d = 0;
-        if (dSsq > diffH * diffH || grd2ML > safeW * safeW) {
-          sign2d = grd2ML > cnt2ML ? -1 : 1;
-        } else {
-          const double corr = 2 * sqrt(cnt2ML * nxt2ML);
-          const double Rsq = (cnt2ML + nxt2ML - corr + dSsq) * (cnt2ML + nxt2ML + corr + dSsq) / 4 / dSsq;
-          const double maxAx = fmax(cnt2ML, nxt2ML);
-          const int idAx1 = cnt2ML > nxt2ML ? close_s : secnd_s;
-          const int idAx2 = idAx1 == close_s ? secnd_s : close_s;
-          const double d = sqrt((Rsq - maxAx) / dSsq);
-          const double xC0 = rX[idAx1] + (rX[idAx1] - rX[idAx2]) * d;
-          const double xC1 = rY[idAx1] + (rY[idAx1] - rY[idAx2]) * d;
-          const double grd2Core = sq(p0 - xC0) + sq(p1 - xC1);
-          sign2d = grd2Core > Rsq ? -1 : 1;
-        }
-        if (fabs(dist) > dist1) {
-          const double W = 1 - sqrt(dist1) * (invh / 3);
-          ud0 = W * Q.ud[0]; ud1 = W * Q.ud[1];
-          dist = sign2d * dist1;
-          chi = W;
-        }
-      }
-      __syncthreads();
+  for (int c0 = 0; c0 < totSurf; c0 += RT) {
+    SurfPt P;
+    bool keep = false;
+    int xlo = 0, xhi = 0, ylo = 0, yhi = 0;
+    const int q = c0 + tid;
+    if (q < totSurf) {
+      const int si = find_range(surfStart, nsl, q);
+      const int r = q - surfStart[si];
+      const int ss = segFst[si] + r / 2, side = r & 1;
+      const double2 my = F.sp[2 * ss + side], pp = F.sp[2 * (ss + 1) + side];
+      const double2 pm = F.sp[2 * (ss - 1) + side], u = F.su[2 * ss + side];
+      P.ss = ss;
+      P.myP[0] = my.x; P.myP[1] = my.y;
+      P.pP[0] = pp.x; P.pP[1] = pp.y; P.pM[0] = pm.x; P.pM[1] = pm.y;
+      P.ud[0] = u.x; P.ud[1] = u.y;
+      P.iap[0] = (int)floor((P.myP[0] - org0) * invh);
+      P.iap[1] = (int)floor((P.myP[1] - org1) * invh);
+      // support [iap-1, iap+3) clipped to the block, intersected with this sub-tile
+      xlo = max(max(0, P.iap[0] - 1), sx0); xhi = min(min(P.iap[0] + 3, BS), sx0 + SUB);
+      ylo = max(max(0, P.iap[1] - 1), sy0); yhi = min(min(P.iap[1] + 3, BS), sy0 + SUB);
+      keep = xlo < xhi && ylo < yhi;
     }
+    int pos;
+    const int nc = compact_slot(keep, wc, pos);
+    if (keep) {
+      pts.s[pos] = P;
+      supp[pos] = make_uchar4(xlo - sx0, xhi - sx0, ylo - sy0, yhi - sy0);
+    }
+    __syncthreads();
+    rows_build(Lr, supp, nc, sy0);
+    const int row = iy - sy0, col = ix - sx0;
+    const int n = Lr.n[row];
+    for (int e = 0; e < n; e++) {
+      const int qi = Lr.idx[row][e];
+      const uchar4 sp = supp[qi];
+      if (col < sp.x || col >= sp.y) continue;
+      const SurfPt& Q = pts.s[qi];
+      const double dist0 = sq(px - Q.myP[0]) + sq(py - Q.myP[1]);
+      const double distP = sq(px - Q.pP[0]) + sq(py - Q.pP[1]);
+      const double distM = sq(px - Q.pM[0]) + sq(py - Q.pM[1]);
+      if (fabs(dist) < fmin(fmin(dist0, distP), distM)) continue;
+      // changeFromComputationalFrame (FishLibrary.h:194-200)
+      const double q0 = px - pos0, q1 = py - pos1;
+      const double p0 = R00 * q0 + R10 * q1, p1 = R01 * q0 + R11 * q1;
+      const int ss = Q.ss;
+      int close_s = ss, secnd_s = ss + (distP < distM ? 1 : -1);
+      double dist1 = dist0, dist2 = distP < distM ? distP : distM;
+      if (distP < dist0 || distM < dist0) {
+        dist1 = dist2; dist2 = dist0;
+        close_s = secnd_s; secnd_s = ss;
+      }
+      const double dSsq = sq(rX[close_s] - rX[secnd_s]) + sq(rY[close_s] - rY[secnd_s]);
+      const double cnt2ML = sq(width[close_s]);
+      const double nxt2ML = sq(width[secnd_s]);
+      const double safeW = fmax(width[close_s], width[secnd_s]) + 2 * h;
+      const double grd2ML = sq(p0 - rX[close_s]) + sq(p1 - rY[close_s]);
+      const double diffH = fabs(width[close_s] - width[secnd_s]);
+      double sign2d = 0;
+      if (dSsq > diffH * diffH || grd2ML > safeW * safeW) {
+        sign2d = grd2ML > cnt2ML ? -1 : 1;
+      } else {
+        const double corr = 2 * sqrt(cnt2ML * nxt2ML);
+        const double Rsq = (cnt2ML + nxt2ML - corr + dSsq) * (cnt2ML + nxt2ML + corr + dSsq) / 4 / dSsq;
+        const double maxAx = fmax(cnt2ML, nxt2ML);
+        const int idAx1 = cnt2ML > nxt2ML ? close_s : secnd_s;
+        const int idAx2 = idAx1 == close_s ? secnd_s : close_s;
+        const double d = sqrt((Rsq - maxAx) / dSsq);
+        const double xC0 = rX[idAx1] + (rX[idAx1] - rX[idAx2]) * d;
+        const double xC1 = rY[idAx1] + (rY[idAx1] - rY[idAx2]) * d;
+        const double grd2Core = sq(p0 - xC0) + sq(p1 - xC1);
+        sign2d = grd2Core > Rsq ? -1 : 1;
+      }
+      if (fabs(dist) > dist1) {
+        const double W = 1 - sqrt(dist1) * (invh / 3);
+        ud0 = W * Q.ud[0]; ud1 = W * Q.ud[1];
+        dist = sign2d * dist1;
+        chi = W;
+      }
+    }
+    __syncthreads();
   }
 
   // constructInternl (FishLibrary.cpp:575-638)
-  for (int si = 0; si < nsl; si++) {
-    const Segment& sg = F.seg[segList[si]];
-    const int firstSegm = max(sg.first, 1), lastSegm = min(sg.second, Nm - 2);
-    int npts = 0;                                       // sum over ss of (2 Nw - 1)
-    for (int ss = firstSegm; ss <= lastSegm; ss++) {
-      const int Nw = (int)floor(width[ss] / h);
-      npts += Nw > 0 ? 2 * Nw - 1 : 0;
+  for (int c0 = 0; c0 < totInt; c0 += RT) {
+    IntPt P;
+    bool keep = false;
+    int xlo = 0, xhi = 0, ylo = 0, yhi = 0;
+    const int q = c0 + tid;
+    if (q < totInt) {
+      const int si = find_range(intStart, nsl, q);
+      const int gq = segIntBase[si] + (q - intStart[si]);
+      const double2 xw = F.ip[gq], u = F.iu[gq];
+      const double xp0 = (xw.x - org0) * invh, xp1 = (xw.y - org1) * invh;
+      const double ap0 = floor(xp0), ap1 = floor(xp1);
+      P.iap[0] = (int)ap0; P.iap[1] = (int)ap1;
+      xlo = max(max(0, P.iap[0]), sx0); xhi = min(min(P.iap[0] + 2, BS), sx0 + SUB);
+      ylo = max(max(0, P.iap[1]), sy0); yhi = min(min(P.iap[1] + 2, BS), sy0 + SUB);
+      keep = xlo < xhi && ylo < yhi;
+      P.ud[0] = u.x; P.ud[1] = u.y;
+      P.w[0][0] = 1 - fabs(xp0 - ap0); P.w[0][1] = 1 - fabs(xp0 - (ap0 + 1));
+      P.w[1][0] = 1 - fabs(xp1 - ap1); P.w[1][1] = 1 - fabs(xp1 - (ap1 + 1));
     }
-    for (int c0 = 0; c0 < npts; c0 += RT) {
-      IntPt P;
-      bool keep = false;
-      const int q0 = c0 + tid;
-      if (q0 < npts) {
-        int q = q0, ss = firstSegm, Nw = 0;
-        for (;; ss++) {
-          Nw = (int)floor(width[ss] / h);
-          const int n = Nw > 0 ? 2 * Nw - 1 : 0;
-          if (q < n) break;
-          q -= n;
-        }
-        const int iw = -Nw + 1 + q;
-        const double offsetW = iw * h;
-        const double m0 = rX[ss] + offsetW * norX[ss], m1 = rY[ss] + offsetW * norY[ss];
-        const double xp0 = ((R00 * m0 + R01 * m1 + pos0) - org0) * invh;
-        const double xp1 = ((R10 * m0 + R11 * m1 + pos1) - org1) * invh;
-        const double ap0 = floor(xp0), ap1 = floor(xp1);
-        P.iap[0] = (int)ap0; P.iap[1] = (int)ap1;
-        const bool valid = !(P.iap[0] + 2 <= 0 || P.iap[0] >= BS) && !(P.iap[1] + 2 <= 0 || P.iap[1] >= BS);
-        keep = valid && max(max(0, P.iap[0]), sx0) < min(min(P.iap[0] + 2, BS), sx0 + SUB)
-                     && max(max(0, P.iap[1]), sy0) < min(min(P.iap[1] + 2, BS), sy0 + SUB);
-        if (keep) {
-          const double u0 = vX[ss] + offsetW * vNorX[ss], u1 = vY[ss] + offsetW * vNorY[ss];
-          P.ud[0] = R00 * u0 + R01 * u1; P.ud[1] = R10 * u0 + R11 * u1;
-          P.w[0][0] = 1 - fabs(xp0 - ap0); P.w[0][1] = 1 - fabs(xp0 - (ap0 + 1));
-          P.w[1][0] = 1 - fabs(xp1 - ap1); P.w[1][1] = 1 - fabs(xp1 - (ap1 + 1));
-        }
-      }
-      int pos;
-      const int nc = compact_slot(keep, wc, pos);
-      if (keep) ip[pos] = P;
-      __syncthreads();
-      for (int qq = 0; qq < nc; qq++) {
-        const IntPt& Q = ip[qq];
-        if (iy < max(0, Q.iap[1]) || iy >= min(Q.iap[1] + 2, BS)) continue;
-        if (ix < max(0, Q.iap[0]) || ix >= min(Q.iap[0] + 2, BS)) continue;
-        const int sx = ix - Q.iap[0], sy = iy - Q.iap[1];
-        const double wxwy = Q.w[1][sy] * Q.w[0][sx];
-        ud0 += wxwy * Q.ud[0];
-        ud1 += wxwy * Q.ud[1];
-        chi += wxwy;
-        if (fabs(dist + 1) < EPSd) dist = 1;
-      }
-      __syncthreads();
+    int pos;
+    const int nc = compact_slot(keep, wc, pos);
+    if (keep) {
+      pts.i[pos] = P;
+      supp[pos] = make_uchar4(xlo - sx0, xhi - sx0, ylo - sy0, yhi - sy0);
     }
+    __syncthreads();
+    rows_build(Lr, supp, nc, sy0);
+    const int row = iy - sy0, col = ix - sx0;
+    const int n = Lr.n[row];
+    for (int e = 0; e < n; e++) {
+      const int qi = Lr.idx[row][e];
+      const uchar4 sp = supp[qi];
+      if (col < sp.x || col >= sp.y) continue;
+      const IntPt& Q = pts.i[qi];
+      const int sx = ix - Q.iap[0], sy = iy - Q.iap[1];
+      const double wxwy = Q.w[1][sy] * Q.w[0][sx];
+      ud0 += wxwy * Q.ud[0];
+      ud1 += wxwy * Q.ud[1];
+      chi += wxwy;
+      if (fabs(dist + 1) < EPSd) dist = 1;
+    }
+    __syncthreads();
   }
 
   // signedDistanceSqrt (FishLibrary.cpp:419-436)
@@ -540,9 +627,12 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
   const size_t o = (size_t)s * BS2 + iy * BS + ix;
   t.dist[o] = dist; t.chi[o] = 0; t.udx[o] = ud0; t.udy[o] = ud1;
   atomic_max_double(&sdfg[(size_t)(by * BS + iy) * g.nx + bx * BS + ix], dist);
+  __syncthreads();                                      // shared state is reused by the next item
+  }
 }
 
 size_t midline_smem(int Nm) { return sizeof(double) * 12 * (size_t)Nm; }
+size_t frame_smem(int Nm) { return sizeof(double) * 10 * (size_t)Nm; }
 
 } // namespace
 
@@ -557,6 +647,8 @@ void fish_setup_kernels() {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaFuncSetAttribute((const void*)k_fish_midline, cudaFuncAttributeMaxDynamicSharedMemorySize, maxOptin);
+  cudaFuncSetAttribute((const void*)k_fish_frame, cudaFuncAttributeMaxDynamicSharedMemorySize, maxOptin);
+  cudaFuncSetAttribute((const void*)k_fish_raster, cudaFuncAttributeMaxDynamicSharedMemorySize, maxOptin);
 }
 
 void launch_fish_midline(Ctx& c, int k, cudaStream_t stream, int mode) {
@@ -565,14 +657,21 @@ void launch_fish_midline(Ctx& c, int k, cudaStream_t stream, int mode) {
 }
 
 void launch_fish_kinematics(Ctx& c, int k) {
-  k_fish_frame<<<1, 512, 0, c.stream>>>(c.g, c.dsc, c.dshapes, k, c.fish[k]);
+  k_fish_frame<<<1, 512, frame_smem(c.fish[k].nm), c.stream>>>(c.g, c.dsc, c.dshapes, k, c.fish[k]);
   CUP2D_LAUNCHED(c);
 }
 
 void launch_fish_raster(Ctx& c, int k) {
-  k_fish_raster<<<c.tiles[k].capacity * NSUB, RT, 0, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
+  // two resident CTAs per SM at most (registers); each loops over
+  // (tile, sub-tile) items
+  const int items = c.tiles[k].capacity * NSUB, grid = items < 2 * c.sms ? items : 2 * c.sms;
+  k_fish_raster<<<grid, RT, sizeof(double) * 3 * (size_t)c.fish[k].nm, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
                                                                 c.fish[k], c.sdf);
   CUP2D_LAUNCHED(c);
 }
 
 } // namespace cup2d
+
+#ifdef CUP2D_TRACE
+namespace cup2d { void trace_bind_fish(unsigned long long* p) { trace_bind_this_unit(p); } }
+#endif

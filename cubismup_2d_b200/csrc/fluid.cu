@@ -23,16 +23,20 @@ __global__ void k_max_u_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh,
                            const double* __restrict__ u, const double* __restrict__ v,
                            double* partials, unsigned* counter)
 {
+  CUP2D_TRACE_SCOPE(TR_MAXU);
   __shared__ double red[64];
   const double UINF = sc->uinfx, VINF = sc->uinfy;
   double m = 0.0; int bad = 0;
-  const size_t n = (size_t)g.nx * g.ny;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+  const size_t n2 = (size_t)g.nx * g.ny / 2;        // Nx is a multiple of 32
+  const double2* u2 = reinterpret_cast<const double2*>(u);
+  const double2* v2 = reinterpret_cast<const double2*>(v);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2;
        i += (size_t)gridDim.x * blockDim.x) {
-    const double a = u[i], b = v[i];
+    const double2 a2 = u2[i], b2 = v2[i];
     // Helpers.cpp:160-166: max of |u+uinf|, |v+vinf|, |u|, |v|
-    m = fmax(m, fmax(fmax(fabs(a + UINF), fabs(b + VINF)), fmax(fabs(a), fabs(b))));
-    bad |= !isfinite(a) || !isfinite(b);
+    m = fmax(m, fmax(fmax(fabs(a2.x + UINF), fabs(b2.x + VINF)), fmax(fabs(a2.x), fabs(b2.x))));
+    m = fmax(m, fmax(fmax(fabs(a2.y + UINF), fabs(b2.y + VINF)), fmax(fabs(a2.y), fabs(b2.y))));
+    bad |= !isfinite(a2.x) || !isfinite(b2.x) || !isfinite(a2.y) || !isfinite(b2.y);
   }
   m = block_max(m, red);
   const int anyBad = __syncthreads_or(bad);
@@ -42,7 +46,7 @@ __global__ void k_max_u_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh,
   }
   if (!last_block_done(counter, gridDim.x)) return;
   double mm = 0.0;
-  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) mm = fmax(mm, partials[i]);
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) mm = fmax(mm, __ldcg(&partials[i]));
   mm = block_max(mm, red);
   if (threadIdx.x != 0) return;
   // Simulation::calcMaxTimestep (Simulation.cpp:254-277)
@@ -64,9 +68,9 @@ __global__ void k_max_u_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh,
   if (g.dlm > 0) sc->lambda = g.dlm / dt;
 }
 
-__global__ void k_set_dt(Scalars* sc, double dt) { sc->dt = dt; }
+__global__ void k_set_dt(Scalars* sc, double dt) { CUP2D_TRACE_SCOPE(TR_SETDT); sc->dt = dt; }
 
-__global__ void k_end_step(Scalars* sc) {
+__global__ void k_end_step(Scalars* sc) { CUP2D_TRACE_SCOPE(TR_ENDSTEP);
   sc->time += sc->dt;
   sc->step += 1;
 }
@@ -79,6 +83,7 @@ k_advdiff(GridDesc g, const Scalars* sc,
           double* __restrict__ un, double* __restrict__ vn,
           double* partials, unsigned* counter, Scalars* scw)
 {
+  CUP2D_TRACE_SCOPE(TR_ADVDIFF);
   __shared__ double red[32];
   const double dt = sc->dt, h = g.h;
   const double UINF0 = sc->uinfx, UINF1 = sc->uinfy;
@@ -127,25 +132,23 @@ k_advdiff(GridDesc g, const Scalars* sc,
   if (!last_block_done(counter, nb)) return;
   const int tid = threadIdx.x + 32 * threadIdx.y;
   double s[1] = {0.0};
-  for (unsigned i = tid; i < nb; i += 256) s[0] += partials[i];
+  for (unsigned i = tid; i < nb; i += 256) s[0] += __ldcg(&partials[i]);
   block_sum<1>(s, red);
-  if (tid == 0)  // advDiff.cpp:105
-    scw->outflowCorr = s[0] / (2 * (BS * g.bpdy - 0) + 2 * (BS * g.bpdx - 0));
-}
-
-// advDiff.cpp:107-115
-__global__ void k_outflow(GridDesc g, const Scalars* sc, double* __restrict__ u, double* __restrict__ v)
-{
-  const double corr = sc->outflowCorr;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nx = g.nx, ny = g.ny;
-  if (i < ny) {
-    u[(size_t)i * nx] += corr;
-    u[(size_t)i * nx + nx - 1] -= corr;
+  __shared__ double corrS;
+  if (tid == 0) {  // advDiff.cpp:105
+    corrS = s[0] / (2 * (BS * g.bpdy - 0) + 2 * (BS * g.bpdx - 0));
+    scw->outflowCorr = corrS;
   }
-  if (i < nx) {
-    v[i] += corr;
-    v[(size_t)(ny - 1) * nx + i] -= corr;
+  __syncthreads();
+  // advDiff.cpp:107-115, applied by this last CTA once every new value exists
+  const double corr = corrS;
+  for (int i = tid; i < ny; i += 256) {
+    un[(size_t)i * nx] = __ldcg(&un[(size_t)i * nx]) + corr;
+    un[(size_t)i * nx + nx - 1] = __ldcg(&un[(size_t)i * nx + nx - 1]) - corr;
+  }
+  for (int i = tid; i < nx; i += 256) {
+    vn[i] = __ldcg(&vn[i]) + corr;
+    vn[(size_t)(ny - 1) * nx + i] = __ldcg(&vn[(size_t)(ny - 1) * nx + i]) - corr;
   }
 }
 
@@ -154,6 +157,7 @@ __global__ void __launch_bounds__(256)
 k_rhs_div(GridDesc g, const Scalars* sc, const double* __restrict__ u,
           const double* __restrict__ v, double* __restrict__ rhs)
 {
+  CUP2D_TRACE_SCOPE(TR_RHSDIV);
   const double h = g.h, facDiv = 0.5 * h / sc->dt;
   const int nx = g.nx, ny = g.ny;
   const int gx = blockIdx.x * BS + threadIdx.x;
@@ -175,6 +179,7 @@ k_pcorr(GridDesc g, const Scalars* sc, const double* __restrict__ p,
         const double* __restrict__ ui, const double* __restrict__ vi,
         double* __restrict__ uo, double* __restrict__ vo)
 {
+  CUP2D_TRACE_SCOPE(TR_PCORR);
   const double pFac = -0.5 * sc->dt / g.h;
   const int nx = g.nx, ny = g.ny;
   const int gx = blockIdx.x * BS + threadIdx.x;
@@ -196,6 +201,7 @@ __global__ void __launch_bounds__(256)
 k_fade_sums(GridDesc g, Scalars* sc, const double* __restrict__ rhs,
             double* partials, unsigned* counter)
 {
+  CUP2D_TRACE_SCOPE(TR_FADE);
   __shared__ double red[96];
   const int bx = blockIdx.x, by = blockIdx.y;
   const unsigned nb = gridDim.x * gridDim.y, bid = bx + gridDim.x * by;
@@ -224,13 +230,17 @@ k_fade_sums(GridDesc g, Scalars* sc, const double* __restrict__ rhs,
       s[0] += fadedRHS;
     }
   }
-  block_sum<3>(s, red);
   const int tid = threadIdx.x + 32 * threadIdx.y;
-  if (tid == 0) for (int k = 0; k < 3; k++) partials[3 * bid + k] = s[k];
+  if (touch) {
+    block_sum<3>(s, red);
+    if (tid == 0) for (int k = 0; k < 3; k++) partials[3 * bid + k] = s[k];
+  } else if (tid == 0) {
+    for (int k = 0; k < 3; k++) partials[3 * bid + k] = 0.0;
+  }
   if (!last_block_done(counter, nb)) return;
   double t[3] = {0, 0, 0};
   for (unsigned i = tid; i < nb; i += 256)
-    for (int k = 0; k < 3; k++) t[k] += partials[3 * i + k];
+    for (int k = 0; k < 3; k++) t[k] += __ldcg(&partials[3 * i + k]);
   block_sum<3>(t, red);
   if (tid == 0) {
     const double sumNEG = fmax(t[2], EPSd), sumPOS = fmax(t[1], EPSd);
@@ -264,12 +274,16 @@ inline int reduce_grid(const Ctx& c) {
   int n = (int)((c.ncells() + 255) / 256);
   return n < 148 * 8 ? n : 148 * 8;
 }
+inline int max_grid(const Ctx& c) {
+  int n = (int)((c.ncells() / 2 + 511) / 512);
+  return n < 148 * 2 ? n : 148 * 2;
+}
 
 } // namespace
 
 void launch_max_u_dt(Ctx& c) {
-  const int nb = reduce_grid(c);
-  k_max_u_dt<<<nb, 256, 0, c.stream>>>(c.g, c.dsc, c.dshapes, c.nshapes, c.u(), c.v(),
+  const int nb = max_grid(c);
+  k_max_u_dt<<<nb, 512, 0, c.stream>>>(c.g, c.dsc, c.dshapes, c.nshapes, c.u(), c.v(),
                                         c.partials, c.counters + CNT_MAXU);
   CUP2D_LAUNCHED(c);
 }
@@ -297,9 +311,8 @@ void launch_advdiff_undo(Ctx& c) { c.cur = 1 - c.cur; }
 void launch_pcorr_undo(Ctx& c) { c.cur = 1 - c.cur; }
 
 void launch_outflow(Ctx& c) {
-  const int n = c.g.nx > c.g.ny ? c.g.nx : c.g.ny;
-  k_outflow<<<(n + 255) / 256, 256, 0, c.stream>>>(c.g, c.dsc, c.u(), c.v());
-  CUP2D_LAUNCHED(c);
+  // applied by the last CTA of k_advdiff (advDiff.cpp:89-116)
+  (void)c;
 }
 
 void launch_rhs_div(Ctx& c) {
@@ -334,3 +347,7 @@ void launch_apply_obj_vel(Ctx& c) {
 }
 
 } // namespace cup2d
+
+#ifdef CUP2D_TRACE
+namespace cup2d { void trace_bind_fluid(unsigned long long* p) { trace_bind_this_unit(p); } }
+#endif

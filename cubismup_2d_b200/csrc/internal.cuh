@@ -114,6 +114,11 @@ struct FishMidline {
 // (integ[p*8 + ..]: area, CoM_internal[2], vCoM_internal[2], J_internal,
 // angvel_internal, time); frame holds it rotated by theta_internal, which is
 // what PutFishOnBlocks reads.
+// PutFishOnBlocks' points in the computational frame, computed once per step:
+// surface points sp[2 ss + (signp > 0)] = midline +- width * normal, with
+// their deformation velocity su[]; interior points of midline index ss are
+// ip[off[ss] .. off[ss+1]) for width offsets iw = -Nw+1 .. Nw-1
+// (Nw = floor(width/h), time-independent), with velocities iu[].
 struct FishArrays {
   double *rS, *width, *p1f;
   FishMidline mid[2];
@@ -121,8 +126,47 @@ struct FishArrays {
   FishMidline frame;
   Segment* seg;                           // [nseg]
   double* pool;                           // single allocation behind all arrays
-  int nm, nseg;
+  int* nw;                                // [nm] floor(width / h)
+  int* off;                               // [nm + 1] interior point offsets
+  double2* sp; double2* su;               // [2 nm]
+  double2* ip; double2* iu;               // [nint]
+  int2* ipIdx;                            // [nint] (ss, iw) of each interior point
+  int nm, nseg, nint;
 };
+
+// ---- optional in-graph timeline ------------------------------------------
+// Built with -DCUP2D_TRACE, thread 0 of every CTA of every kernel records
+// the %globaltimer at entry (atomicMin into slot 2*id) and at exit
+// (atomicMax into slot 2*id+1), so one step's overlapped schedule can be
+// read back.  Without the define the scope compiles to nothing.
+enum TraceId : int {
+  TR_MAXU, TR_SETDT, TR_ENDSTEP, TR_ADVDIFF, TR_RHSDIV, TR_PCORR, TR_FADE,
+  TR_OBJBEGIN, TR_CLEAR, TR_FLAGS, TR_COMPACT, TR_RASTER_DISK, TR_CHI, TR_MOMENTS,
+  TR_UDEF, TR_RHSOBST, TR_RHSCORR, TR_MOMENTA, TR_COLLIDE, TR_PENALIZE, TR_FORCES,
+  TR_MIDLINE, TR_FRAME, TR_RASTER, TR_R2C, TR_COLS, TR_C2R, TR_DCT_FWD, TR_DCT_COLS,
+  TR_DCT_INV, TR_N
+};
+#ifdef CUP2D_TRACE
+static __device__ unsigned long long* g_trace = nullptr;   // one copy per translation unit
+__device__ __forceinline__ unsigned long long global_timer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+struct TraceScope {
+  int id;
+  __device__ explicit TraceScope(int i) : id(i) {
+    if (g_trace && threadIdx.x + threadIdx.y + threadIdx.z == 0) atomicMin(&g_trace[2 * id], global_timer());
+  }
+  __device__ ~TraceScope() {
+    if (g_trace && threadIdx.x + threadIdx.y + threadIdx.z == 0) atomicMax(&g_trace[2 * id + 1], global_timer());
+  }
+};
+#define CUP2D_TRACE_SCOPE(id) TraceScope cup2d_trace_scope_(id)
+static inline void trace_bind_this_unit(unsigned long long* p) { cudaMemcpyToSymbol(g_trace, &p, sizeof(p)); }
+#else
+#define CUP2D_TRACE_SCOPE(id) ((void)0)
+#endif
 
 // ---- small device helpers ------------------------------------------------
 
@@ -176,18 +220,21 @@ __device__ __forceinline__ double block_max(double v, double* smem) {
 }
 
 // "last block done" ticket: returns true in every thread of the CTA that
-// finished last.  The counter is re-armed by that CTA.
+// finished last.  The counter is re-armed by that CTA.  As in a grid-wide
+// barrier, the CTA barrier orders every thread's earlier writes before
+// thread 0's gpu-scope fence (fences are cumulative), so one fence before
+// the ticket releases the whole CTA's writes, and one fence after it, in
+// the last CTA, acquires everybody else's before the closing barrier.
 __device__ __forceinline__ bool last_block_done(unsigned* counter, unsigned nblocks) {
   __shared__ bool amLast;
-  __threadfence();
   __syncthreads();
   if (lin_tid() == 0) {
+    __threadfence();
     const unsigned t = atomicAdd(counter, 1u);
     amLast = (t == nblocks - 1);
-    if (amLast) *counter = 0;
+    if (amLast) { *counter = 0; __threadfence(); }
   }
   __syncthreads();
-  if (amLast) __threadfence();
   return amLast;
 }
 

@@ -36,6 +36,7 @@ inline AllTiles all_tiles(const Ctx& c) {
 // ST_DOMAIN (the reference exits).
 __global__ void k_obj_begin(GridDesc g, Scalars* sc, DevShape* sh, int nsh)
 {
+  CUP2D_TRACE_SCOPE(TR_OBJBEGIN);
   if (threadIdx.x != 0) return;
   const double dt = sc->dt;
   int nSum[2] = {0, 0}; double uSum[2] = {0, 0};
@@ -64,17 +65,18 @@ __global__ void k_obj_begin(GridDesc g, Scalars* sc, DevShape* sh, int nsh)
 __global__ void __launch_bounds__(256)
 k_clear_old(GridDesc g, const DevShape* sh, AllTiles T, double* chi, double* sdf)
 {
-  const int k = blockIdx.y, s = blockIdx.x;
-  if (s >= sh[k].ntilesPrev) return;
+  CUP2D_TRACE_SCOPE(TR_CLEAR);
+  const int k = blockIdx.y;
   const ObstTiles& t = T.t[k];
-  const int b = t.tiles[s];
-  const int bx = b % g.bpdx, by = b / g.bpdx;
-  for (int i = threadIdx.x; i < BS2; i += blockDim.x) {
-    const size_t c = (size_t)(by * BS + i / BS) * g.nx + bx * BS + (i % BS);
-    chi[c] = 0; sdf[c] = -1;
+  for (int s = blockIdx.x; s < sh[k].ntilesPrev; s += gridDim.x) {
+    const int b = t.tiles[s];
+    const int bx = b % g.bpdx, by = b / g.bpdx;
+    for (int i = threadIdx.x; i < BS2; i += blockDim.x) {
+      const size_t c = (size_t)(by * BS + i / BS) * g.nx + bx * BS + (i % BS);
+      chi[c] = 0; sdf[c] = -1;
+    }
+    if (threadIdx.x == 0) t.slot[b] = -1;
   }
-  __syncthreads();
-  if (threadIdx.x == 0) t.slot[b] = -1;
 }
 
 __device__ __forceinline__ bool disk_touching(const GridDesc& g, const DevShape& S, int bx, int by) {
@@ -92,6 +94,7 @@ __device__ __forceinline__ bool disk_touching(const GridDesc& g, const DevShape&
 __global__ void __launch_bounds__(256)
 k_tile_flags(GridDesc g, const DevShape* sh, FishSegPtrs segs, int* flags)
 {
+  CUP2D_TRACE_SCOPE(TR_FLAGS);
   const int k = blockIdx.y;
   const DevShape& S = sh[k];
   const int lane = threadIdx.x & 31;
@@ -116,6 +119,7 @@ k_tile_flags(GridDesc g, const DevShape* sh, FishSegPtrs segs, int* flags)
 __global__ void __launch_bounds__(1024)
 k_tile_compact(GridDesc g, DevShape* sh, AllTiles T, const int* flags, Scalars* sc)
 {
+  CUP2D_TRACE_SCOPE(TR_COMPACT);
   __shared__ int warpCount[32];
   __shared__ int base;
   const int k = blockIdx.x;
@@ -149,18 +153,21 @@ k_tile_compact(GridDesc g, DevShape* sh, AllTiles T, const int* flags, Scalars* 
 __global__ void __launch_bounds__(1024)
 k_raster_disk(GridDesc g, const DevShape* sh, AllTiles T, double* sdf)
 {
-  const int k = blockIdx.y, s = blockIdx.x;
+  CUP2D_TRACE_SCOPE(TR_RASTER_DISK);
+  const int k = blockIdx.y;
   const DevShape& S = sh[k];
-  if (S.cfg.kind != CUP2D_SHAPE_DISK || s >= S.ntiles) return;
+  if (S.cfg.kind != CUP2D_SHAPE_DISK) return;
   const ObstTiles& t = T.t[k];
-  const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
-  const int ix = threadIdx.x, iy = threadIdx.y, i = iy * BS + ix;
-  const double pos0 = S.s.center[0], pos1 = S.s.center[1];
-  const double x = cell_x(g, bx, ix) - pos0, y = cell_y(g, by, iy) - pos1;
-  const double dist = S.cfg.radius - sqrt(x * x + y * y);
-  const size_t o = (size_t)s * BS2 + i;
-  t.dist[o] = dist; t.chi[o] = 0; t.udx[o] = 0; t.udy[o] = 0;
-  atomic_max_double(&sdf[(size_t)(by * BS + iy) * g.nx + bx * BS + ix], dist);
+  for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
+    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+    const int ix = threadIdx.x, iy = threadIdx.y, i = iy * BS + ix;
+    const double pos0 = S.s.center[0], pos1 = S.s.center[1];
+    const double x = cell_x(g, bx, ix) - pos0, y = cell_y(g, by, iy) - pos1;
+    const double dist = S.cfg.radius - sqrt(x * x + y * y);
+    const size_t o = (size_t)s * BS2 + i;
+    t.dist[o] = dist; t.chi[o] = 0; t.udx[o] = 0; t.udy[o] = 0;
+    atomic_max_double(&sdf[(size_t)(by * BS + iy) * g.nx + bx * BS + ix], dist);
+  }
 }
 
 // PutObjectsOnGrid::putChiOnGrid (PutObjectsOnGrid.cpp:17-124): Towers chi
@@ -170,12 +177,14 @@ __global__ void __launch_bounds__(1024)
 k_chi(GridDesc g, const DevShape* sh, AllTiles T, const double* __restrict__ sdfg,
       double* chig, double* partials, int partStride)
 {
+  CUP2D_TRACE_SCOPE(TR_CHI);
   __shared__ double red[32 * 3];
   __shared__ double tile[BS][BS + 1];
-  const int k = blockIdx.y, s = blockIdx.x;
+  const int k = blockIdx.y;
   const DevShape& S = sh[k];
+  for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
   double acc[3] = {0, 0, 0};
-  if (s < S.ntiles) {
+  {
     const ObstTiles& t = T.t[k];
     const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
     const int ix = threadIdx.x, iy = threadIdx.y;
@@ -231,8 +240,9 @@ k_chi(GridDesc g, const DevShape* sh, AllTiles T, const double* __restrict__ sdf
     t.sD[o] = D; t.sdx[o] = sdx; t.sdy[o] = sdy;
   }
   block_sum<3>(acc, red);
-  if (lin_tid() == 0 && s < S.ntiles)
+  if (lin_tid() == 0)
     for (int q = 0; q < 3; q++) partials[(size_t)k * partStride + 3 * s + q] = acc[q];
+  }
 }
 
 // PutObjectsOnGrid.cpp:118-122 (CoM correction) + Shape::removeMoments
@@ -244,15 +254,17 @@ __global__ void __launch_bounds__(1024)
 k_moments(GridDesc g, DevShape* sh, AllTiles T, const double* chiParts, double* parts,
           int partStride, unsigned* counters)
 {
+  CUP2D_TRACE_SCOPE(TR_MOMENTS);
   __shared__ double red[32 * 7];
   __shared__ double bc[3];
-  const int k = blockIdx.y, s = blockIdx.x, tid = lin_tid();
+  const int k = blockIdx.y, tid = lin_tid();
   DevShape& S = sh[k];
   const ObstTiles& t = T.t[k];
   const int nt = S.ntiles;
   const double* cp = chiParts + (size_t)k * partStride;
   double* mp = parts + (size_t)k * partStride;
-  {                                   // every CTA (the last one included) forms the CoM
+  // the corrected CoM, formed by every CTA with a tile and by the last CTA
+  auto form_com = [&]() {
     double a3[3] = {0, 0, 0};
     for (int i = tid; i < nt; i += 1024)
       for (int q = 0; q < 3; q++) a3[q] += cp[3 * i + q];
@@ -263,8 +275,9 @@ k_moments(GridDesc g, DevShape* sh, AllTiles T, const double* chiParts, double* 
       bc[0] = c0; bc[1] = c1; bc[2] = M;
     }
     __syncthreads();
-  }
-  if (s < nt) {
+  };
+  if ((int)blockIdx.x < nt) form_com();
+  for (int s = blockIdx.x; s < nt; s += gridDim.x) {
     const double C0 = bc[0], C1 = bc[1];
     const double hsq = g.h * g.h, rho = S.rhoTile;
     double I[7] = {0, 0, 0, 0, 0, 0, 0};   // x, y, m, j, u, v, a
@@ -288,9 +301,10 @@ k_moments(GridDesc g, DevShape* sh, AllTiles T, const double* chiParts, double* 
     if (tid == 0) for (int q = 0; q < 7; q++) mp[3 * t.capacity + 7 * s + q] = I[q];
   }
   if (!last_block_done(counters + k, gridDim.x)) return;
+  if ((int)blockIdx.x >= nt) form_com();
   double I[7] = {0, 0, 0, 0, 0, 0, 0};
   for (int i = tid; i < nt; i += 1024)
-    for (int q = 0; q < 7; q++) I[q] += mp[3 * t.capacity + 7 * i + q];
+    for (int q = 0; q < 7; q++) I[q] += __ldcg(&mp[3 * t.capacity + 7 * i + q]);
   block_sum<7>(I, red);
   if (tid != 0 || nt == 0) return;
   if (bc[2] > 0) { S.s.com[0] = bc[0]; S.s.com[1] = bc[1]; S.s.M = bc[2]; }
@@ -308,19 +322,20 @@ __global__ void __launch_bounds__(1024)
 k_udef_grid(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* chig,
             double* udx, double* udy)
 {
-  const int s = blockIdx.x;
-  if (s >= sh[k].ntiles) return;
-  const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
-  const int ix = threadIdx.x, iy = threadIdx.y;
-  const size_t o = (size_t)s * BS2 + iy * BS + ix;
-  const size_t c = (size_t)(by * BS + iy) * g.nx + bx * BS + ix;
-  const double X = t.chi[o];
-  if (X < chig[c] || X <= 0) return;
-  const DevShape& S = sh[k];
-  double u0, u1;
-  udef_at(t, o, S, cell_x(g, bx, ix) - S.s.com[0], cell_y(g, by, iy) - S.s.com[1], u0, u1);
-  udx[c] += u0;
-  udy[c] += u1;
+  CUP2D_TRACE_SCOPE(TR_UDEF);
+  for (int s = blockIdx.x; s < sh[k].ntiles; s += gridDim.x) {
+    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+    const int ix = threadIdx.x, iy = threadIdx.y;
+    const size_t o = (size_t)s * BS2 + iy * BS + ix;
+    const size_t c = (size_t)(by * BS + iy) * g.nx + bx * BS + ix;
+    const double X = t.chi[o];
+    if (X < chig[c] || X <= 0) continue;
+    const DevShape& S = sh[k];
+    double u0, u1;
+    udef_at(t, o, S, cell_x(g, bx, ix) - S.s.com[0], cell_y(g, by, iy) - S.s.com[1], u0, u1);
+    udx[c] += u0;
+    udy[c] += u1;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -329,11 +344,12 @@ __global__ void __launch_bounds__(1024)
 k_rhs_obst(GridDesc g, DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
            double* rhs, double* partials, unsigned* counter)
 {
+  CUP2D_TRACE_SCOPE(TR_RHSOBST);
   __shared__ double red[32 * 3];
   DevShape& S = sh[k];
-  const int s = blockIdx.x;
+  for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
   double acc[3] = {0, 0, 0};   // sumRHS, posRHS, negRHS
-  if (s < S.ntiles) {
+  {
     const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
     const int ix = threadIdx.x, iy = threadIdx.y;
     const int gx = bx * BS + ix, gy = by * BS + iy;
@@ -359,11 +375,12 @@ k_rhs_obst(GridDesc g, DevShape* sh, int k, ObstTiles t, const double* __restric
   }
   block_sum<3>(acc, red);
   if (lin_tid() == 0) for (int q = 0; q < 3; q++) partials[3 * s + q] = acc[q];
+  }
   if (!last_block_done(counter, gridDim.x)) return;
   double tot[3] = {0, 0, 0};
   const int n = S.ntiles;
   for (int i = lin_tid(); i < n; i += 1024)
-    for (int q = 0; q < 3; q++) tot[q] += partials[3 * i + q];
+    for (int q = 0; q < 3; q++) tot[q] += __ldcg(&partials[3 * i + q]);
   block_sum<3>(tot, red);
   if (lin_tid() == 0) {                                  // PressureSingle.cpp:185-186
     const double corrDenom = tot[0] > 0 ? tot[1] : tot[2];
@@ -376,27 +393,28 @@ __global__ void __launch_bounds__(1024)
 k_rhs_corr(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
            double* rhs)
 {
+  CUP2D_TRACE_SCOPE(TR_RHSCORR);
   const DevShape& S = sh[k];
-  const int s = blockIdx.x;
-  if (s >= S.ntiles) return;
   const double corr = S.rhsCorr;
-  const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
-  const int ix = threadIdx.x, iy = threadIdx.y;
-  const int gx = bx * BS + ix, gy = by * BS + iy;
   auto CHI = [&](int x, int y) -> double {
     x = x < 0 ? 0 : (x >= g.nx ? g.nx - 1 : x);
     y = y < 0 ? 0 : (y >= g.ny ? g.ny - 1 : y);
     return chig[(size_t)y * g.nx + x];
   };
-  const double chi = t.chi[(size_t)s * BS2 + iy * BS + ix];
-  if (CHI(gx, gy) > chi) return;
-  const double gradXx = CHI(gx + 1, gy) - CHI(gx - 1, gy);
-  const double gradXy = CHI(gx, gy + 1) - CHI(gx, gy - 1);
-  const bool isPerim = gradXx * gradXx + gradXy * gradXy > 0;
-  const size_t c = (size_t)gy * g.nx + gx;
-  const double tmp = rhs[c];
-  if (isPerim && tmp > 0 && corr > 0) rhs[c] = tmp - corr * tmp;
-  else if (isPerim && tmp < 0 && corr < 0) rhs[c] = tmp + corr * tmp;
+  for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
+    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+    const int ix = threadIdx.x, iy = threadIdx.y;
+    const int gx = bx * BS + ix, gy = by * BS + iy;
+    const double chi = t.chi[(size_t)s * BS2 + iy * BS + ix];
+    if (CHI(gx, gy) > chi) continue;
+    const double gradXx = CHI(gx + 1, gy) - CHI(gx - 1, gy);
+    const double gradXy = CHI(gx, gy + 1) - CHI(gx, gy - 1);
+    const bool isPerim = gradXx * gradXx + gradXy * gradXy > 0;
+    const size_t c = (size_t)gy * g.nx + gx;
+    const double tmp = rhs[c];
+    if (isPerim && tmp > 0 && corr > 0) rhs[c] = tmp - corr * tmp;
+    else if (isPerim && tmp < 0 && corr < 0) rhs[c] = tmp + corr * tmp;
+  }
 }
 
 // PressureSingle::integrateMomenta (PressureSingle.cpp:23-67) with the
@@ -407,13 +425,14 @@ k_momenta(GridDesc g, const Scalars* sc, DevShape* sh, AllTiles T,
           const double* __restrict__ u, const double* __restrict__ v,
           double* parts, int partStride, unsigned* counters)
 {
+  CUP2D_TRACE_SCOPE(TR_MOMENTA);
   __shared__ double red[32 * 7];
-  const int k = blockIdx.y, s = blockIdx.x, tid = lin_tid();
+  const int k = blockIdx.y, tid = lin_tid();
   DevShape& S = sh[k];
   const ObstTiles& t = T.t[k];
   const int nt = S.ntiles;
   double* mp = parts + (size_t)k * partStride + 10 * (size_t)t.capacity;
-  if (s < nt) {
+  for (int s = blockIdx.x; s < nt; s += gridDim.x) {
     const double Cx = S.s.com[0], Cy = S.s.com[1];
     const double hsq = g.h * g.h, rho = S.rhoTile;
     double A[7] = {0, 0, 0, 0, 0, 0, 0};   // PM, PJ, PX, PY, UM, VM, AM
@@ -442,7 +461,7 @@ k_momenta(GridDesc g, const Scalars* sc, DevShape* sh, AllTiles T,
   if (!last_block_done(counters + k, gridDim.x)) return;
   double A[7] = {0, 0, 0, 0, 0, 0, 0};
   for (int i = tid; i < nt; i += 1024)
-    for (int q = 0; q < 7; q++) A[q] += mp[7 * i + q];
+    for (int q = 0; q < 7; q++) A[q] += __ldcg(&mp[7 * i + q]);
   block_sum<7>(A, red);
   if (tid != 0) return;
   S.s.fluidAngMom = A[6]; S.s.fluidMomX = A[4]; S.s.fluidMomY = A[5];
@@ -456,6 +475,7 @@ k_momenta(GridDesc g, const Scalars* sc, DevShape* sh, AllTiles T,
 __global__ void __launch_bounds__(1024)
 k_collide(GridDesc g, const Scalars* sc, DevShape* sh, int nsh, AllTiles T)
 {
+  CUP2D_TRACE_SCOPE(TR_COLLIDE);
   __shared__ double red[32 * 10];
   __shared__ double coll[MAX_SHAPES][10];
   const int tid = threadIdx.x;
@@ -534,24 +554,25 @@ __global__ void __launch_bounds__(1024)
 k_penalize(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
            double* u, double* v)
 {
+  CUP2D_TRACE_SCOPE(TR_PENALIZE);
   const DevShape& S = sh[k];
-  const int s = blockIdx.x;
-  if (s >= S.ntiles) return;
-  const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
-  const int ix = threadIdx.x, iy = threadIdx.y;
-  const size_t o = (size_t)s * BS2 + iy * BS + ix;
-  const size_t c = (size_t)(by * BS + iy) * g.nx + bx * BS + ix;
-  const double X = t.chi[o];
-  if (chig[c] > X) return;
-  if (X <= 0) return;
-  const double p0 = cell_x(g, bx, ix) - S.s.com[0], p1 = cell_y(g, by, iy) - S.s.com[1];
-  const double alpha = 1 - X;
-  double ux, uy;
-  udef_at(t, o, S, p0, p1, ux, uy);
-  const double US = S.s.u - S.s.omega * p1 + ux;
-  const double VS = S.s.v + S.s.omega * p0 + uy;
-  u[c] = alpha * u[c] + (1 - alpha) * US;
-  v[c] = alpha * v[c] + (1 - alpha) * VS;
+  for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
+    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+    const int ix = threadIdx.x, iy = threadIdx.y;
+    const size_t o = (size_t)s * BS2 + iy * BS + ix;
+    const size_t c = (size_t)(by * BS + iy) * g.nx + bx * BS + ix;
+    const double X = t.chi[o];
+    if (chig[c] > X) continue;
+    if (X <= 0) continue;
+    const double p0 = cell_x(g, bx, ix) - S.s.com[0], p1 = cell_y(g, by, iy) - S.s.com[1];
+    const double alpha = 1 - X;
+    double ux, uy;
+    udef_at(t, o, S, p0, p1, ux, uy);
+    const double US = S.s.u - S.s.omega * p1 + ux;
+    const double VS = S.s.v + S.s.omega * p0 + uy;
+    u[c] = alpha * u[c] + (1 - alpha) * US;
+    v[c] = alpha * v[c] + (1 - alpha) * VS;
+  }
 }
 
 // ComputeForces::operator() (ComputeForces.cpp:16-111) + Shape::computeForces
@@ -562,14 +583,17 @@ k_forces(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ u,
          const double* __restrict__ v, const double* __restrict__ p,
          double* partials, int partStride, unsigned* counters)
 {
+  CUP2D_TRACE_SCOPE(TR_FORCES);
   __shared__ double red[32 * NFORCE];
-  const int k = blockIdx.y, s = blockIdx.x;
+  const int k = blockIdx.y;
   DevShape& S = sh[k];
   const ObstTiles& t = T.t[k];
+  double* part = partials + (size_t)k * partStride;
+  for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
   double F[NFORCE];
 #pragma unroll
   for (int q = 0; q < NFORCE; q++) F[q] = 0;
-  if (s < S.ntiles) {
+  {
     const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
     const int ix = threadIdx.x, iy = threadIdx.y;
     const size_t o = (size_t)s * BS2 + iy * BS + ix;
@@ -617,17 +641,15 @@ k_forces(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ u,
       F[16] = fmin(0.0, powDef);                            // defPowerBnd
     }
   }
-  double* part = partials + (size_t)k * partStride;
-  if (s < S.ntiles) {
-    block_sum<NFORCE>(F, red);
-    if (lin_tid() == 0) for (int q = 0; q < NFORCE; q++) part[NFORCE * s + q] = F[q];
+  block_sum<NFORCE>(F, red);
+  if (lin_tid() == 0) for (int q = 0; q < NFORCE; q++) part[NFORCE * s + q] = F[q];
   }
   if (!last_block_done(counters + k, gridDim.x)) return;
   double tot[NFORCE];
 #pragma unroll
   for (int q = 0; q < NFORCE; q++) tot[q] = 0;
   for (int i = lin_tid(); i < S.ntiles; i += 1024)
-    for (int q = 0; q < NFORCE; q++) tot[q] += part[NFORCE * i + q];
+    for (int q = 0; q < NFORCE; q++) tot[q] += __ldcg(&part[NFORCE * i + q]);
   block_sum<NFORCE>(tot, red);
   if (lin_tid() != 0) return;
   cup2d_shape_state& st = S.s;
@@ -646,6 +668,9 @@ k_forces(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ u,
 }
 
 inline size_t shape_region(const Ctx& c) { return (size_t)c.maxCapacity * 24; }
+// CTAs per shape of the per-tile kernels: one wave at most; each CTA loops
+// over tiles s = blockIdx.x, blockIdx.x + gridDim.x, ... < ntiles
+inline int tile_ctas(const Ctx& c, int capacity) { return capacity < c.sms ? capacity : c.sms; }
 inline double* shape_partials(const Ctx& c) { return c.partials + (size_t)3 * c.g.nblocks + 4096; }
 
 } // namespace
@@ -665,7 +690,7 @@ void launch_objects_rest(Ctx& c) {
   if (c.nshapes == 0) return;
   const AllTiles T = all_tiles(c);
   const int cap = c.maxCapacity;
-  k_clear_old<<<dim3(cap, c.nshapes), 256, 0, c.stream>>>(c.g, c.dshapes, T, c.chi, c.sdf);
+  k_clear_old<<<dim3(tile_ctas(c, cap), c.nshapes), 256, 0, c.stream>>>(c.g, c.dshapes, T, c.chi, c.sdf);
   CUP2D_LAUNCHED(c);
   // frames and AreaSegments (Fish.cpp:95-150)
   for (int k = 0; k < c.nshapes; k++)
@@ -680,17 +705,17 @@ void launch_objects_rest(Ctx& c) {
     if (c.hshapes[k].cfg.kind == CUP2D_SHAPE_DISK) anyDisk = true; else anyFish = true;
   }
   if (anyDisk) {
-    k_raster_disk<<<dim3(cap, c.nshapes), dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, T, c.sdf);
+    k_raster_disk<<<dim3(tile_ctas(c, cap), c.nshapes), dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, T, c.sdf);
     CUP2D_LAUNCHED(c);
   }
   if (anyFish)
     for (int k = 0; k < c.nshapes; k++)
       if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_raster(c, k);
   const int stride = (int)shape_region(c);
-  k_chi<<<dim3(cap, c.nshapes), dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, T, c.sdf, c.chi,
+  k_chi<<<dim3(tile_ctas(c, cap), c.nshapes), dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, T, c.sdf, c.chi,
                                                               shape_partials(c), stride);
   CUP2D_LAUNCHED(c);
-  k_moments<<<dim3(cap, c.nshapes), 1024, 0, c.stream>>>(c.g, c.dshapes, T, shape_partials(c),
+  k_moments<<<dim3(tile_ctas(c, cap), c.nshapes), 1024, 0, c.stream>>>(c.g, c.dshapes, T, shape_partials(c),
                                                           shape_partials(c), stride, c.counters + CNT_MOMENTS);
   CUP2D_LAUNCHED(c);
 }
@@ -702,7 +727,7 @@ void launch_objects(Ctx& c, bool midlineReady) {
 
 void launch_obj_vel_on_grid(Ctx& c) {
   for (int k = 0; k < c.nshapes; k++) {
-    k_udef_grid<<<c.tiles[k].capacity, dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
+    k_udef_grid<<<tile_ctas(c, c.tiles[k].capacity), dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
                                                                    c.chi, c.udefx, c.udefy);
     CUP2D_LAUNCHED(c);
   }
@@ -710,13 +735,13 @@ void launch_obj_vel_on_grid(Ctx& c) {
 
 void launch_rhs_obstacles(Ctx& c) {
   for (int k = 0; k < c.nshapes; k++) {
-    k_rhs_obst<<<c.tiles[k].capacity, dim3(32, 32), 0, c.stream>>>(
+    k_rhs_obst<<<tile_ctas(c, c.tiles[k].capacity), dim3(32, 32), 0, c.stream>>>(
         c.g, c.dshapes, k, c.tiles[k], c.chi, c.rhs, shape_partials(c) + (size_t)k * shape_region(c),
         c.counters + CNT_RHSOBST + k);
     CUP2D_LAUNCHED(c);
   }
   for (int k = 0; k < c.nshapes; k++) {
-    k_rhs_corr<<<c.tiles[k].capacity, dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
+    k_rhs_corr<<<tile_ctas(c, c.tiles[k].capacity), dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
                                                                   c.chi, c.rhs);
     CUP2D_LAUNCHED(c);
   }
@@ -725,7 +750,7 @@ void launch_rhs_obstacles(Ctx& c) {
 void launch_momenta_penalize(Ctx& c) {
   if (c.nshapes == 0) return;
   const AllTiles T = all_tiles(c);
-  k_momenta<<<dim3(c.maxCapacity, c.nshapes), 1024, 0, c.stream>>>(
+  k_momenta<<<dim3(tile_ctas(c, c.maxCapacity), c.nshapes), 1024, 0, c.stream>>>(
       c.g, c.dsc, c.dshapes, T, c.u(), c.v(), shape_partials(c), (int)shape_region(c), c.counters + CNT_MOMENTA);
   CUP2D_LAUNCHED(c);
   if (c.nshapes > 1) {
@@ -733,7 +758,7 @@ void launch_momenta_penalize(Ctx& c) {
     CUP2D_LAUNCHED(c);
   }
   for (int k = 0; k < c.nshapes; k++) {
-    k_penalize<<<c.tiles[k].capacity, dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
+    k_penalize<<<tile_ctas(c, c.tiles[k].capacity), dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
                                                                   c.chi, c.u(), c.v());
     CUP2D_LAUNCHED(c);
   }
@@ -742,10 +767,14 @@ void launch_momenta_penalize(Ctx& c) {
 void launch_forces(Ctx& c) {
   if (c.nshapes == 0) return;
   const AllTiles T = all_tiles(c);
-  k_forces<<<dim3(c.maxCapacity, c.nshapes), dim3(32, 32), 0, c.stream>>>(
+  k_forces<<<dim3(tile_ctas(c, c.maxCapacity), c.nshapes), dim3(32, 32), 0, c.stream>>>(
       c.g, c.dshapes, T, c.u(), c.v(), c.pres, shape_partials(c), (int)shape_region(c),
       c.counters + CNT_FORCES);
   CUP2D_LAUNCHED(c);
 }
 
 } // namespace cup2d
+
+#ifdef CUP2D_TRACE
+namespace cup2d { void trace_bind_obstacles(unsigned long long* p) { trace_bind_this_unit(p); } }
+#endif

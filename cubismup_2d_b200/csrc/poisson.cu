@@ -28,6 +28,9 @@ namespace cup2d {
 
 struct Poisson {
   int type = CUP2D_POISSON_FREESPACE;
+  float* cosX = nullptr;     // cosine solver: float tables of FFTW_dirichlet.h:75-76
+  float* cosY = nullptr;
+  double tol = 0.1;          // FFTW_dirichlet.h:51
   int Lrow = 0;          // complex FFT length of the row passes (M/2)
   int Lcol = 0;          // complex FFT length of the column pass
   int nkx = 0;           // spectrum columns (Lrow + 1)
@@ -48,60 +51,116 @@ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_doub
 __device__ __forceinline__ double2 conjg(double2 a) { return make_double2(a.x, -a.y); }
 
 __device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
-template <int L> struct Len { static constexpr int SL = L + L / 16; };   // padded stride
 
-// Stockham autosort FFT (radix-4 stages, plus one radix-2 stage first when
-// log2 L is odd) of nseq sequences of length L stored at A + q*SL (padded
-// indexing), B scratch.  Forward exp(-2 pi i jk/L), inverse exp(+...),
-// unnormalised.  Returns the buffer holding the result.
+constexpr int FFT_R = 2;   // radix-4 butterflies per thread and stage
+
+// Per transform length L: padded stride SL of one sequence (one spare
+// element per 16, plus 4 so that consecutive sequences start in different
+// halves of the shared-memory banks), the twiddles the stages use
+// (w^j, j < 3L/4), the sequences per CTA B and the threads per CTA NT.
+template <int L> struct Len {
+  static constexpr int SL = L + L / 16 + 4;
+  static constexpr int TW = 3 * L / 4;
+  static constexpr int B = 2048 / L < 1 ? 1 : (2048 / L > 8 ? 8 : 2048 / L);
+  static constexpr int NT0 = B * L / (4 * FFT_R);
+  static constexpr int NT = NT0 < 64 ? 64 : (NT0 > 512 ? 512 : NT0);
+  static constexpr int MINB = 65536 / (NT * 64);   // caps registers at 64
+};
+
+// Twiddles w^j = exp(-2 pi i j / L), j < 3L/4, staged in shared memory.
+template <int L>
+__device__ __forceinline__ void load_twiddles(double2* tws, const double2* __restrict__ tw, int twLen) {
+  const int step = twLen / L;
+  for (int j = threadIdx.x; j < Len<L>::TW; j += blockDim.x) tws[j] = tw[j * step];
+}
+
+// asynchronous global -> shared copies (sm_80+ cp.async), so that every
+// load of a CTA's rows or columns is in flight at once
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n"
+               :: "r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n"
+               :: "r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory");
+}
+
+// In-place Stockham autosort FFT (radix-4 stages, plus one radix-2 stage
+// first when log2 L is odd) of nseq sequences of length L stored at
+// A + q*SL (padded indexing); tws holds the L twiddles.  Every stage loads
+// its inputs to registers, synchronises, then stores, so one buffer
+// suffices.  Forward exp(-2 pi i jk/L), inverse exp(+...), unnormalised.
+// Each thread owns FFT_R radix-4 butterflies per stage: blockDim.x * FFT_R
+// must be at least nseq * L/4.
+
 template <int L, bool INV>
-__device__ double2* fft4(double2* A, double2* B, int nseq, const double2* __restrict__ tw, int twLen)
+__device__ void fft_inplace(double2* A, int nseq, const double2* tws)
 {
-  constexpr int SL = Len<L>::SL, Q = L / 4, H = L / 2;
-  const int tid = threadIdx.x, nt = blockDim.x;
+  constexpr int SL = Len<L>::SL, Q = L / 4, H = L / 2, R = FFT_R;
+  int qq[R], jj[R];
+  bool act[R];
+#pragma unroll
+  for (int u = 0; u < R; u++) {
+    const int t = threadIdx.x + u * blockDim.x;
+    act[u] = t < nseq * Q;
+    qq[u] = act[u] ? t / Q : 0;
+    jj[u] = t - qq[u] * Q;
+  }
   int Ns = 1;
   if ((__builtin_ctz(L) & 1) == 1) {
-    for (int idx = tid; idx < nseq * H; idx += nt) {
-      const int q = idx / H, j = idx - q * H;
-      const double2* a = A + q * SL;
-      double2* b = B + q * SL;
-      const double2 x0 = a[pad(j)], x1 = a[pad(j + H)];
-      b[pad(2 * j)] = cadd(x0, x1);
-      b[pad(2 * j + 1)] = csub(x0, x1);
+    double2 x[R][4];
+#pragma unroll
+    for (int u = 0; u < R; u++) if (act[u]) {
+      const double2* a = A + qq[u] * SL; const int j = jj[u];
+      x[u][0] = a[pad(j)]; x[u][1] = a[pad(j + H)]; x[u][2] = a[pad(j + Q)]; x[u][3] = a[pad(j + Q + H)];
     }
     __syncthreads();
-    double2* T = A; A = B; B = T;
+#pragma unroll
+    for (int u = 0; u < R; u++) if (act[u]) {
+      double2* a = A + qq[u] * SL; const int j = jj[u];
+      a[pad(2 * j)] = cadd(x[u][0], x[u][1]); a[pad(2 * j + 1)] = csub(x[u][0], x[u][1]);
+      a[pad(2 * (j + Q))] = cadd(x[u][2], x[u][3]); a[pad(2 * (j + Q) + 1)] = csub(x[u][2], x[u][3]);
+    }
+    __syncthreads();
     Ns = 2;
   }
   for (; Ns < L; Ns <<= 2) {
-    const int twStep = twLen / (4 * Ns);
-    for (int idx = tid; idx < nseq * Q; idx += nt) {
-      const int q = idx / Q, j = idx - q * Q;
-      const double2* a = A + q * SL;
-      double2* b = B + q * SL;
+    double2 x[R][4];
+#pragma unroll
+    for (int u = 0; u < R; u++) if (act[u]) {
+      const double2* a = A + qq[u] * SL; const int j = jj[u];
+      x[u][0] = a[pad(j)]; x[u][1] = a[pad(j + Q)]; x[u][2] = a[pad(j + 2 * Q)]; x[u][3] = a[pad(j + 3 * Q)];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < R; u++) if (act[u]) {
+      double2* a = A + qq[u] * SL; const int j = jj[u];
       const int k = j & (Ns - 1);
-      double2 x0 = a[pad(j)], x1 = a[pad(j + Q)], x2 = a[pad(j + 2 * Q)], x3 = a[pad(j + 3 * Q)];
+      double2 x0 = x[u][0], x1 = x[u][1], x2 = x[u][2], x3 = x[u][3];
       if (k) {
-        double2 w1 = tw[k * twStep], w2 = tw[2 * k * twStep], w3 = tw[3 * k * twStep];
+        const int st = L / (4 * Ns);
+        double2 w1 = tws[k * st], w2 = tws[2 * k * st], w3 = tws[3 * k * st];
         if (INV) { w1.y = -w1.y; w2.y = -w2.y; w3.y = -w3.y; }
         x1 = cmul(w1, x1); x2 = cmul(w2, x2); x3 = cmul(w3, x3);
       }
       const double2 t0 = cadd(x0, x2), t1 = csub(x0, x2), t2 = cadd(x1, x3), t3 = csub(x1, x3);
       const int o = ((j - k) << 2) + k;
-      b[pad(o)] = cadd(t0, t2);
-      b[pad(o + 2 * Ns)] = csub(t0, t2);
+      a[pad(o)] = cadd(t0, t2);
+      a[pad(o + 2 * Ns)] = csub(t0, t2);
       if (!INV) {
-        b[pad(o + Ns)] = make_double2(t1.x + t3.y, t1.y - t3.x);       // t1 - i t3
-        b[pad(o + 3 * Ns)] = make_double2(t1.x - t3.y, t1.y + t3.x);   // t1 + i t3
+        a[pad(o + Ns)] = make_double2(t1.x + t3.y, t1.y - t3.x);       // t1 - i t3
+        a[pad(o + 3 * Ns)] = make_double2(t1.x - t3.y, t1.y + t3.x);   // t1 + i t3
       } else {
-        b[pad(o + Ns)] = make_double2(t1.x - t3.y, t1.y + t3.x);
-        b[pad(o + 3 * Ns)] = make_double2(t1.x + t3.y, t1.y - t3.x);
+        a[pad(o + Ns)] = make_double2(t1.x - t3.y, t1.y + t3.x);
+        a[pad(o + 3 * Ns)] = make_double2(t1.x + t3.y, t1.y - t3.x);
       }
     }
     __syncthreads();
-    double2* T = A; A = B; B = T;
   }
-  return A;
 }
 
 struct FadeArgs {
@@ -129,44 +188,40 @@ __device__ __forceinline__ double fade_cell(const GridDesc& g, int gx, int gy, d
 }
 
 // inMode 0: rows of `in`; 1: the free-space Green's function on the padded
-// grid (FFTW_freespace.cpp:108-119) computed on the fly.
+// grid (FFTW_freespace.cpp:108-119) computed on the fly.  Each row of 2L
+// reals is the complex sequence (x[2n], x[2n+1]) of length L.
 template <int L>
-__global__ void __launch_bounds__(1024)
+__global__ void __launch_bounds__(Len<L>::NT, Len<L>::MINB)
 k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
-           double2* __restrict__ out, int outStride, int rb,
+           double2* __restrict__ out, int outStride,
            const double2* __restrict__ tw, int twLen, FadeArgs fa, double h, int Nx, int Ny)
 {
-  constexpr int SL = Len<L>::SL;
+  CUP2D_TRACE_SCOPE(TR_R2C);
+  constexpr int SL = Len<L>::SL, RB = Len<L>::B, NT = Len<L>::NT;
   extern __shared__ double2 sm[];
   double2* A = sm;
-  double2* B = sm + rb * SL;
-  const int row0 = blockIdx.x * rb;
-  const int nb = min(rb, nrows - row0);
-  const double corr = fa.enabled ? fa.sc->fadeCorr : 0.0;
-  // fade band: cells within fadeLen (+2 cells margin) of an edge
-  const int bandX = fa.enabled ? (int)(fa.g.fadeLenX / fa.g.h) + 2 : 0;
-  const int bandY = fa.enabled ? (int)(fa.g.fadeLenY / fa.g.h) + 2 : 0;
-  for (int idx = threadIdx.x; idx < nb * L; idx += blockDim.x) {
-    const int r = idx / L, n = idx - r * L, row = row0 + r;
-    double x[2];
-    if (inMode == 0 && 2 * n + 1 < ncolsIn) {
-      const double2 v2 = *reinterpret_cast<const double2*>(in + (size_t)row * inStride + 2 * n);
-      x[0] = v2.x; x[1] = v2.y;
-      if (fa.enabled) {
-        const bool rowBand = row < bandY || row >= fa.g.ny - bandY;
-        for (int q = 0; q < 2; q++) {
-          const int col = 2 * n + q;
-          if (rowBand || col < bandX || col >= fa.g.nx - bandX) {
-            x[q] = fade_cell(fa.g, col, row, x[q], corr);
-            fa.writeback[(size_t)row * inStride + col] = x[q];
-          }
-        }
-      }
-    } else {
+  double2* tws = sm + RB * SL;
+  const int row0 = blockIdx.x * RB;
+  const int nb = min(RB, nrows - row0);
+  if (inMode == 0) {
+    for (int idx = threadIdx.x; idx < RB * L; idx += NT) {
+      const int r = idx / L, n = idx & (L - 1), row = row0 + r;
+      if (r >= nb) continue;
+      double2* dst = A + r * SL + pad(n);
+      if (2 * n + 1 < ncolsIn) cp_async16(dst, in + (size_t)row * inStride + 2 * n);
+      else if (2 * n < ncolsIn) *dst = make_double2(in[(size_t)row * inStride + 2 * n], 0);
+      else *dst = make_double2(0, 0);
+    }
+    cp_async_commit();
+  } else {
+    for (int idx = threadIdx.x; idx < RB * L; idx += NT) {
+      const int r = idx / L, n = idx & (L - 1), row = row0 + r;
+      if (r >= nb) continue;
+      double x[2];
       for (int q = 0; q < 2; q++) {
         const int col = 2 * n + q;
         double val = 0;
-        if (col < ncolsIn && inMode == 1) {
+        if (col < ncolsIn) {
           const int MX = 2 * Nx, MY = 2 * Ny;
           const double fac = 1 / (2 * M_PI);
           if (row == 0 && col == 0) {
@@ -177,22 +232,46 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
             const double rr = sqrt(xi * xi + yi * yi);
             val = fac * log(h * rr);
           }
-        } else if (col < ncolsIn) {
-          val = in[(size_t)row * inStride + col];
         }
         x[q] = val;
       }
+      A[r * SL + pad(n)] = make_double2(x[0], x[1]);
     }
-    A[r * SL + pad(n)] = make_double2(x[0], x[1]);
   }
+  load_twiddles<L>(tws, tw, twLen);
+  cp_async_wait<0>();
   __syncthreads();
-  double2* Z = fft4<L, false>(A, B, nb, tw, twLen);
+  if (fa.enabled) {
+    // fade band: cells within fadeLen (+2 cells margin) of an edge, faded in
+    // place and written back (cub2rhs, PoissonSolver.cpp:61-141)
+    const double corr = fa.sc->fadeCorr;
+    const int bandX = (int)(fa.g.fadeLenX / fa.g.h) + 2;
+    const int bandY = (int)(fa.g.fadeLenY / fa.g.h) + 2;
+    for (int idx = threadIdx.x; idx < RB * L; idx += NT) {
+      const int r = idx / L, n = idx & (L - 1), row = row0 + r;
+      if (r >= nb || 2 * n + 1 >= ncolsIn) continue;
+      const bool rowBand = row < bandY || row >= fa.g.ny - bandY;
+      if (!rowBand && 2 * n >= bandX && 2 * n + 1 < fa.g.nx - bandX) continue;   // both cells inside
+      double2 v = A[r * SL + pad(n)];
+      double* x = &v.x;
+      for (int q = 0; q < 2; q++) {
+        const int col = 2 * n + q;
+        if (rowBand || col < bandX || col >= fa.g.nx - bandX) {
+          x[q] = fade_cell(fa.g, col, row, x[q], corr);
+          fa.writeback[(size_t)row * inStride + col] = x[q];
+        }
+      }
+      A[r * SL + pad(n)] = v;
+    }
+    __syncthreads();
+  }
+  fft_inplace<L, false>(A, nb, tws);
   // even/odd split: X[k] = Fe[k] + W^k Fo[k], W = exp(-i pi / L), k in [0, L]
   const int twStep = twLen / (2 * L);
-  for (int idx = threadIdx.x; idx < nb * (L + 1); idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < nb * (L + 1); idx += NT) {
     const int r = idx / (L + 1), k = idx - r * (L + 1);
-    const double2 Zk = Z[r * SL + pad(k == L ? 0 : k)];
-    const double2 Zc = conjg(Z[r * SL + pad(k == 0 ? 0 : L - k)]);
+    const double2 Zk = A[r * SL + pad(k == L ? 0 : k)];
+    const double2 Zc = conjg(A[r * SL + pad(k == 0 ? 0 : L - k)]);
     const double2 Fe = make_double2(0.5 * (Zk.x + Zc.x), 0.5 * (Zk.y + Zc.y));
     const double2 d = csub(Zk, Zc);
     const double2 Fo = make_double2(0.5 * d.y, -0.5 * d.x);   // (Zk - Zc) / (2i)
@@ -204,37 +283,58 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
 // mode 0: forward, x G^ (real, symmetric in ky), inverse, keep nrowsOut rows
 // mode 1: forward; write Re * norm for ky <= L/2 into ghat (kernel set-up)
 // mode 2: forward, periodic multiplier -1/|k|^2 / (MX MY), inverse
+// Rows r >= nrowsIn of the input are zero and never read.
 template <int L>
-__global__ void __launch_bounds__(1024)
-k_cols(double2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrowsOut, int cb,
-       double* __restrict__ ghat, int mode, const double2* __restrict__ tw, int twLen, double norm,
-       int MXp, int MYp)
+__global__ void __launch_bounds__(Len<L>::NT, Len<L>::MINB)
+k_cols(double2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrowsOut,
+       const double* __restrict__ ghatIn, double* __restrict__ ghatOut, int mode,
+       const double2* __restrict__ tw, int twLen, double norm, int MXp, int MYp)
 {
-  constexpr int SL = Len<L>::SL;
+  CUP2D_TRACE_SCOPE(TR_COLS);
+  constexpr int SL = Len<L>::SL, CB = Len<L>::B, NT = Len<L>::NT, GR = L / 2 + 1;
   extern __shared__ double2 sm[];
   double2* A = sm;
-  double2* B = sm + cb * SL;
-  const int c0 = blockIdx.x * cb;
-  const int nb = min(cb, ncols - c0);
-  for (int idx = threadIdx.x; idx < nb * L; idx += blockDim.x) {
-    const int r = idx / nb, j = idx - r * nb;     // consecutive threads: consecutive columns
-    A[j * SL + pad(r)] = r < nrowsIn ? data[(size_t)r * stride + c0 + j] : make_double2(0, 0);
+  double2* tws = sm + CB * SL;
+  double* Gs = reinterpret_cast<double*>(tws + Len<L>::TW);   // [GR][CB] kernel rows
+  const int c0 = blockIdx.x * CB;
+  const int nb = min(CB, ncols - c0);
+  // consecutive threads take consecutive columns of one row
+  for (int idx = threadIdx.x; idx < CB * nrowsIn; idx += NT) {
+    const int r = idx / CB, j = idx & (CB - 1);
+    if (j < nb) cp_async16(A + j * SL + pad(r), data + (size_t)r * stride + c0 + j);
   }
+  cp_async_commit();
+  if (mode == 0) {
+    for (int idx = threadIdx.x; idx < CB * GR; idx += NT) {
+      const int r = idx / CB, j = idx & (CB - 1);
+      if (j < nb) cp_async8(Gs + r * CB + j, ghatIn + (size_t)r * stride + c0 + j);
+    }
+  }
+  cp_async_commit();
+  for (int idx = threadIdx.x; idx < CB * (L - nrowsIn); idx += NT) {
+    const int r = nrowsIn + idx / CB, j = idx & (CB - 1);
+    A[j * SL + pad(r)] = make_double2(0, 0);
+  }
+  load_twiddles<L>(tws, tw, twLen);
+  cp_async_wait<1>();          // the columns (the kernel rows may still be in flight)
   __syncthreads();
-  double2* Z = fft4<L, false>(A, B, nb, tw, twLen);
+  fft_inplace<L, false>(A, nb, tws);
   if (mode == 1) {
-    for (int idx = threadIdx.x; idx < nb * nrowsOut; idx += blockDim.x) {
-      const int r = idx / nb, j = idx - r * nb;
-      ghat[(size_t)r * stride + c0 + j] = Z[j * SL + pad(r)].x * norm;
+    for (int idx = threadIdx.x; idx < CB * nrowsOut; idx += NT) {
+      const int r = idx / CB, j = idx & (CB - 1);
+      if (j < nb) ghatOut[(size_t)r * stride + c0 + j] = A[j * SL + pad(r)].x * norm;
     }
     return;
   }
-  for (int idx = threadIdx.x; idx < nb * L; idx += blockDim.x) {
-    const int r = idx / nb, j = idx - r * nb;
+  cp_async_wait<0>();
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < CB * L; idx += NT) {
+    const int r = idx / CB, j = idx & (CB - 1);
+    if (j >= nb) continue;
     double f;
     if (mode == 0) {
       const int ky = r <= L / 2 ? r : L - r;
-      f = ghat[(size_t)ky * stride + c0 + j];
+      f = Gs[ky * CB + j];
     } else {
       // FFTW_periodic::_solve_spectral (FFTW_periodic.h:77-92)
       const int i = c0 + j;
@@ -244,52 +344,244 @@ k_cols(double2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrows
       const double kinv = -1 / (rkx * rkx + rky * rky);
       f = (i == 0 && r == 0) ? 0.0 : kinv * norm;
     }
-    double2 z = Z[j * SL + pad(r)];
+    double2 z = A[j * SL + pad(r)];
     if (mode == 2 && c0 + j == 0 && r == 0) z = make_double2(0, 0);
-    Z[j * SL + pad(r)] = make_double2(z.x * f, z.y * f);
+    A[j * SL + pad(r)] = make_double2(z.x * f, z.y * f);
   }
   __syncthreads();
-  double2* Bn = (Z == A) ? B : A;
-  double2* Y = fft4<L, true>(Z, Bn, nb, tw, twLen);
-  for (int idx = threadIdx.x; idx < nb * nrowsOut; idx += blockDim.x) {
-    const int r = idx / nb, j = idx - r * nb;
-    data[(size_t)r * stride + c0 + j] = Y[j * SL + pad(r)];
+  fft_inplace<L, true>(A, nb, tws);
+  for (int idx = threadIdx.x; idx < CB * nrowsOut; idx += NT) {
+    const int r = idx / CB, j = idx & (CB - 1);
+    if (j < nb) data[(size_t)r * stride + c0 + j] = A[j * SL + pad(r)];
   }
 }
 
 // inverse real FFT of length 2L from X[0..L]; writes the first ncolsOut values
 template <int L>
-__global__ void __launch_bounds__(1024)
+__global__ void __launch_bounds__(Len<L>::NT, Len<L>::MINB)
 k_rows_c2r(const double2* __restrict__ in, int inStride, int nrows, double* __restrict__ out,
-           int outStride, int ncolsOut, int rb, const double2* __restrict__ tw, int twLen)
+           int outStride, int ncolsOut, const double2* __restrict__ tw, int twLen)
 {
-  constexpr int SL = Len<L>::SL;
+  CUP2D_TRACE_SCOPE(TR_C2R);
+  constexpr int SL = Len<L>::SL, RB = Len<L>::B, NT = Len<L>::NT, H = L / 2;
   extern __shared__ double2 sm[];
   double2* A = sm;
-  double2* B = sm + rb * SL;
-  const int row0 = blockIdx.x * rb;
-  const int nb = min(rb, nrows - row0);
+  double2* tws = sm + RB * SL;
+  const int row0 = blockIdx.x * RB;
+  const int nb = min(RB, nrows - row0);
   const int twStep = twLen / (2 * L);
-  for (int idx = threadIdx.x; idx < nb * L; idx += blockDim.x) {
-    const int r = idx / L, k = idx - r * L;
-    const double2* X = in + (size_t)(row0 + r) * inStride;
-    double2 Xk = X[k], XL = X[L - k];
-    if (k == 0) { Xk.y = 0; XL.y = 0; }         // c2r ignores Im X[0], Im X[L]
-    const double2 Xc = conjg(XL);
-    const double2 s = cadd(Xk, Xc), d = csub(Xk, Xc);
-    const double2 wi = conjg(tw[k * twStep]);   // W^-k
-    const double2 t = cmul(wi, d);
-    A[r * SL + pad(k)] = make_double2(s.x - t.y, s.y + t.x);   // s + i t
+  // X[0..L] of each row; X[L] lands in the spare slot pad(L) < SL
+  for (int idx = threadIdx.x; idx < RB * (L + 1); idx += NT) {
+    const int r = idx / (L + 1), k = idx - r * (L + 1);
+    if (r < nb) cp_async16(A + r * SL + pad(k), in + (size_t)(row0 + r) * inStride + k);
+  }
+  cp_async_commit();
+  load_twiddles<L>(tws, tw, twLen);
+  cp_async_wait<0>();
+  __syncthreads();
+  // z[k] = s + i t, s = X_k + conj(X_{L-k}), t = W^-k (X_k - conj(X_{L-k})):
+  // thread (r, k), k < L/2, forms the pair k, L-k in place; k = 0 also L/2
+  for (int idx = threadIdx.x; idx < RB * H; idx += NT) {
+    const int r = idx / H, k = idx & (H - 1);
+    if (r >= nb) continue;
+    double2* a = A + r * SL;
+    const int kk[2] = {k, k == 0 ? H : L - k};
+    double2 Xa = a[pad(k)], Xb = a[pad(k == 0 ? L : L - k)];
+    if (k == 0) { Xa.y = 0; Xb.y = 0; }         // c2r ignores Im X[0], Im X[L]
+    double2 res[2];
+    for (int e = 0; e < 2; e++) {
+      const int kq = kk[e];
+      double2 Xk, XL;
+      if (e == 0) { Xk = Xa; XL = Xb; }
+      else if (k == 0) { Xk = a[pad(H)]; XL = Xk; }
+      else { Xk = Xb; XL = Xa; }
+      const double2 Xc = conjg(XL);
+      const double2 sv = cadd(Xk, Xc), d = csub(Xk, Xc);
+      const double2 wi = conjg(tw[kq * twStep]);   // W^-k
+      const double2 t = cmul(wi, d);
+      res[e] = make_double2(sv.x - t.y, sv.y + t.x);
+    }
+    a[pad(kk[0])] = res[0];
+    a[pad(kk[1])] = res[1];
   }
   __syncthreads();
-  double2* z = fft4<L, true>(A, B, nb, tw, twLen);
+  fft_inplace<L, true>(A, nb, tws);
   const int half = (ncolsOut + 1) / 2;
-  for (int idx = threadIdx.x; idx < nb * half; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < nb * half; idx += NT) {
     const int r = idx / half, n = idx - r * half;
-    const double2 v = z[r * SL + pad(n)];
+    const double2 v = A[r * SL + pad(n)];
     double* o = out + (size_t)(row0 + r) * outStride;
     if (2 * n + 1 < ncolsOut) *reinterpret_cast<double2*>(o + 2 * n) = v;
     else o[2 * n] = v.x;
+  }
+}
+
+// ---- cosine-transform solver (FFTW_dirichlet.h:30-130) --------------------
+// DCT-II (FFTW REDFT10, Y_k = 2 sum x_j cos(pi (j+1/2) k / n)) is the real
+// FFT of the even extension y = [x, reversed x] of length 2n:
+// Y_k = exp(-i pi k / 2n) FFT_2n(y)_k.  DCT-III (REDFT01,
+// x'_m = Y_0 + 2 sum_{k>=1} Y_k cos(pi k (m+1/2) / n)) is the inverse real FFT
+// of length 2n of Z_k = exp(+i pi k / 2n) Y_k (Z_n = 0), first n outputs.
+
+// rows: fade on load, DCT-II along x into D (real, Ny x Nx); L = Nx
+template <int L>
+__global__ void __launch_bounds__(Len<L>::NT, Len<L>::MINB)
+k_dct_rows_fwd(const double* in, int Nx, int nrows, double* __restrict__ D, int rb,
+               const double2* __restrict__ tw, int twLen, FadeArgs fa)
+{
+  CUP2D_TRACE_SCOPE(TR_DCT_FWD);
+  constexpr int SL = Len<L>::SL;
+  extern __shared__ double2 sm[];
+  double2* A = sm;
+  double2* tws = sm + rb * SL;
+  double* Bx = reinterpret_cast<double*>(tws + Len<L>::TW);     // staged real row values
+  load_twiddles<L>(tws, tw, twLen);
+  const int row0 = blockIdx.x * rb;
+  const int nb = min(rb, nrows - row0);
+  const double corr = fa.sc->fadeCorr;
+  const int bandX = (int)(fa.g.fadeLenX / fa.g.h) + 2;
+  const int bandY = (int)(fa.g.fadeLenY / fa.g.h) + 2;
+  // faded row values, then the even extension y[j] = x[j] (j < n), x[2n-1-j]
+  for (int idx = threadIdx.x; idx < nb * L; idx += blockDim.x) {
+    const int r = idx / L, col = idx - r * L, row = row0 + r;
+    double v = in[(size_t)row * Nx + col];
+    if (row < bandY || row >= fa.g.ny - bandY || col < bandX || col >= fa.g.nx - bandX) {
+      v = fade_cell(fa.g, col, row, v, corr);
+      fa.writeback[(size_t)row * Nx + col] = v;
+    }
+    Bx[r * L + col] = v;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < nb * L; idx += blockDim.x) {
+    const int r = idx / L, n = idx - r * L;
+    const int j0 = 2 * n, j1 = 2 * n + 1;
+    const double y0 = Bx[r * L + (j0 < L ? j0 : 2 * L - 1 - j0)];
+    const double y1 = Bx[r * L + (j1 < L ? j1 : 2 * L - 1 - j1)];
+    A[r * SL + pad(n)] = make_double2(y0, y1);
+  }
+  __syncthreads();
+  fft_inplace<L, false>(A, nb, tws);
+  double2* Z = A;
+  const int st2 = twLen / (2 * L), st4 = twLen / (4 * L);
+  for (int idx = threadIdx.x; idx < nb * L; idx += blockDim.x) {
+    const int r = idx / L, k = idx - r * L;
+    const double2 Zk = Z[r * SL + pad(k)];
+    const double2 Zc = conjg(Z[r * SL + pad(k == 0 ? 0 : L - k)]);
+    const double2 Fe = make_double2(0.5 * (Zk.x + Zc.x), 0.5 * (Zk.y + Zc.y));
+    const double2 d = csub(Zk, Zc);
+    const double2 Fo = make_double2(0.5 * d.y, -0.5 * d.x);
+    const double2 X = cadd(Fe, cmul(tw[k * st2], Fo));          // FFT_2n(y)_k
+    const double2 Y = cmul(tw[k * st4], X);                     // exp(-i pi k/2n) X_k
+    D[(size_t)(row0 + r) * Nx + k] = Y.x;
+  }
+}
+
+// columns, two per complex FFT of length L = 2 Ny: DCT-II along y, the
+// multiplier of FFTW_dirichlet::_solve (FFTW_dirichlet.h:49-61), DCT-III.
+template <int L>
+__global__ void __launch_bounds__(Len<L>::NT, Len<L>::MINB)
+k_dct_cols(double* D, int Nx, int Ny, int cb, const float* __restrict__ cosX, const float* __restrict__ cosY,
+           double tol, const double2* __restrict__ tw, int twLen)
+{
+  CUP2D_TRACE_SCOPE(TR_DCT_COLS);
+  constexpr int SL = Len<L>::SL;
+  extern __shared__ double2 sm[];
+  double2* A = sm;
+  double2* tws = sm + cb * SL;
+  load_twiddles<L>(tws, tw, twLen);
+  const int n = Ny;                                   // L = 2n
+  const int c0 = blockIdx.x * cb * 2;                 // first column of this CTA
+  const int np = min(cb, (Nx - c0) / 2);              // column pairs
+  for (int idx = threadIdx.x; idx < np * L; idx += blockDim.x) {
+    const int j = idx / np, q = idx - j * np;         // j: extended row index
+    const int row = j < n ? j : 2 * n - 1 - j;
+    const double2 ab = *reinterpret_cast<const double2*>(D + (size_t)row * Nx + c0 + 2 * q);
+    A[q * SL + pad(j)] = ab;                          // a + i b
+  }
+  __syncthreads();
+  fft_inplace<L, false>(A, np, tws);
+  double2* Z = A;
+  // each thread reads the pair (k, L-k) before writing the same pair, and
+  // slot n is read by none, so the inverse input overwrites Z in place
+  double2* W = Z;
+  const int st4 = twLen / (2 * L);                    // exp(-i pi k/2n) = tw[k twLen/(4n)]
+  const double MX = Nx, MY = Ny;
+  const double waveFactX = M_PI / MX, waveFactY = M_PI / MY;
+  const double norm_factor = 0.25 / (MX * MY);
+  // separate the two real columns, DCT-II values, multiplier, then the
+  // Hermitian spectra of both DCT-III inputs packed as Za + i Zb
+  for (int idx = threadIdx.x; idx < np * n; idx += blockDim.x) {
+    const int q = idx / n, k = idx - q * n;
+    const double2 Zk = Z[q * SL + pad(k)];
+    const double2 Zc = conjg(Z[q * SL + pad(k == 0 ? 0 : L - k)]);
+    const double2 Ak = make_double2(0.5 * (Zk.x + Zc.x), 0.5 * (Zk.y + Zc.y));     // FFT of a
+    const double2 dd = csub(Zk, Zc);
+    const double2 Bk = make_double2(0.5 * dd.y, -0.5 * dd.x);                      // FFT of b
+    const double2 w = tw[k * st4];
+    double ya = cmul(w, Ak).x, yb = cmul(w, Bk).x;                                 // DCT-II
+    for (int e = 0; e < 2; e++) {
+      const int i = c0 + 2 * q + e, jj = k;
+      const double rkx = (i + 0.5) * waveFactX, rky = (jj + 0.5) * waveFactY;
+      const float denomF = 1 - cosX[i] / 2 - cosY[jj] / 2;                         // float, as written
+      const double denomFD = denomF;
+      const double denomSP = rkx * rkx + rky * rky;
+      double& y = e == 0 ? ya : yb;
+      y *= -norm_factor / ((1 - tol) * denomFD + tol * denomSP);
+      if (i == 0 && jj == 0) y = 0;                                                // in_out[0] = 0
+    }
+    // Z_k = exp(+i pi k/2n) Y_k for both columns, packed
+    const double2 wc = conjg(w);
+    const double2 za = make_double2(wc.x * ya, wc.y * ya), zb = make_double2(wc.x * yb, wc.y * yb);
+    W[q * SL + pad(k)] = make_double2(za.x - zb.y, za.y + zb.x);                     // za + i zb
+    if (k > 0) {   // k' = 2n - k: conj(za) + i conj(zb)
+      W[q * SL + pad(L - k)] = make_double2(za.x + zb.y, -za.y + zb.x);
+    }
+  }
+  for (int q = threadIdx.x; q < np; q += blockDim.x) W[q * SL + pad(n)] = make_double2(0, 0);
+  __syncthreads();
+  fft_inplace<L, true>(W, np, tws);
+  double2* Y = W;
+  for (int idx = threadIdx.x; idx < np * n; idx += blockDim.x) {
+    const int m = idx / np, q = idx - m * np;
+    *reinterpret_cast<double2*>(D + (size_t)m * Nx + c0 + 2 * q) = Y[q * SL + pad(m)];
+  }
+}
+
+// rows: DCT-III along x from D into p; L = Nx
+template <int L>
+__global__ void __launch_bounds__(Len<L>::NT, Len<L>::MINB)
+k_dct_rows_inv(const double* __restrict__ D, int Nx, int nrows, double* __restrict__ out, int rb,
+               const double2* __restrict__ tw, int twLen)
+{
+  CUP2D_TRACE_SCOPE(TR_DCT_INV);
+  constexpr int SL = Len<L>::SL;
+  extern __shared__ double2 sm[];
+  double2* A = sm;
+  double2* tws = sm + rb * SL;
+  load_twiddles<L>(tws, tw, twLen);
+  const int row0 = blockIdx.x * rb;
+  const int nb = min(rb, nrows - row0);
+  const int st2 = twLen / (2 * L), st4 = twLen / (4 * L);
+  for (int idx = threadIdx.x; idx < nb * L; idx += blockDim.x) {
+    const int r = idx / L, k = idx - r * L;
+    const double* Yr = D + (size_t)(row0 + r) * Nx;
+    // X_k = exp(i pi k/2n) Y_k, X_n = 0; then the c2r combination of k_rows_c2r
+    const double2 wk = conjg(tw[k * st4]);
+    double2 Xk = make_double2(wk.x * Yr[k], wk.y * Yr[k]);
+    double2 XL = make_double2(0, 0);
+    if (k > 0) { const double2 wl = conjg(tw[(L - k) * st4]); XL = make_double2(wl.x * Yr[L - k], wl.y * Yr[L - k]); }
+    if (k == 0) { Xk.y = 0; XL.y = 0; }
+    const double2 Xc = conjg(XL);
+    const double2 s = cadd(Xk, Xc), d = csub(Xk, Xc);
+    const double2 t = cmul(conjg(tw[k * st2]), d);
+    A[r * SL + pad(k)] = make_double2(s.x - t.y, s.y + t.x);
+  }
+  __syncthreads();
+  fft_inplace<L, true>(A, nb, tws);
+  double2* z = A;
+  for (int idx = threadIdx.x; idx < nb * (L / 2); idx += blockDim.x) {
+    const int r = idx / (L / 2), m = idx - r * (L / 2);
+    *reinterpret_cast<double2*>(out + (size_t)(row0 + r) * Nx + 2 * m) = z[r * SL + pad(m)];
   }
 }
 
@@ -304,25 +596,26 @@ void set_smem(const void* f) {
   cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, maxOptin);
 }
 
-inline int batch_for(int L) { int b = 2048 / L; return b < 1 ? 1 : (b > 8 ? 8 : b); }
-inline int threads_for(int L, int b) { int t = b * L / 4; return t < 64 ? 64 : (t > 1024 ? 1024 : t); }
-template <int L> inline size_t smem_for(int b) { return sizeof(double2) * 2 * (size_t)b * Len<L>::SL; }
+// B padded sequences, the staged twiddles, and extraReals doubles
+template <int L> inline size_t smem_for(size_t extraReals = 0) {
+  return sizeof(double2) * ((size_t)Len<L>::B * Len<L>::SL + Len<L>::TW) + sizeof(double) * extraReals;
+}
 
 #define CUP2D_FFT_LENGTHS(X) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
 
 void set_all_smem() {
 #define X(L) set_smem((const void*)k_rows_r2c<L>); set_smem((const void*)k_rows_c2r<L>); \
-             set_smem((const void*)k_cols<L>);
+             set_smem((const void*)k_cols<L>); set_smem((const void*)k_dct_rows_fwd<L>); \
+             set_smem((const void*)k_dct_cols<L>); set_smem((const void*)k_dct_rows_inv<L>);
   CUP2D_FFT_LENGTHS(X)
 #undef X
 }
 
 bool rows_r2c(int L, cudaStream_t st, const double* in, int inStride, int nrows, int ncolsIn, int inMode,
               double2* out, int outStride, const double2* tw, int twLen, FadeArgs fa, double h, int Nx, int Ny) {
-  const int b = batch_for(L), grid = (nrows + b - 1) / b, thr = threads_for(L, b);
   switch (L) {
-#define X(LL) case LL: k_rows_r2c<LL><<<grid, thr, smem_for<LL>(b), st>>>(in, inStride, nrows, ncolsIn, \
-                  inMode, out, outStride, b, tw, twLen, fa, h, Nx, Ny); return true;
+#define X(LL) case LL: k_rows_r2c<LL><<<(nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st>>>( \
+                  in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, Nx, Ny); return true;
     CUP2D_FFT_LENGTHS(X)
 #undef X
   }
@@ -331,10 +624,10 @@ bool rows_r2c(int L, cudaStream_t st, const double* in, int inStride, int nrows,
 
 bool cols(int L, cudaStream_t st, double2* data, int stride, int ncols, int nrowsIn, int nrowsOut,
           double* ghat, int mode, const double2* tw, int twLen, double norm, int MXp, int MYp) {
-  const int b = batch_for(L), grid = (ncols + b - 1) / b, thr = threads_for(L, b);
   switch (L) {
-#define X(LL) case LL: k_cols<LL><<<grid, thr, smem_for<LL>(b), st>>>(data, stride, ncols, nrowsIn, \
-                  nrowsOut, b, ghat, mode, tw, twLen, norm, MXp, MYp); return true;
+#define X(LL) case LL: k_cols<LL><<<(ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, \
+                  smem_for<LL>((size_t)(LL / 2 + 1) * Len<LL>::B), st>>>(data, stride, ncols, nrowsIn, \
+                  nrowsOut, ghat, ghat, mode, tw, twLen, norm, MXp, MYp); return true;
     CUP2D_FFT_LENGTHS(X)
 #undef X
   }
@@ -343,10 +636,43 @@ bool cols(int L, cudaStream_t st, double2* data, int stride, int ncols, int nrow
 
 bool rows_c2r(int L, cudaStream_t st, const double2* in, int inStride, int nrows, double* out, int outStride,
               int ncolsOut, const double2* tw, int twLen) {
-  const int b = batch_for(L), grid = (nrows + b - 1) / b, thr = threads_for(L, b);
   switch (L) {
-#define X(LL) case LL: k_rows_c2r<LL><<<grid, thr, smem_for<LL>(b), st>>>(in, inStride, nrows, out, \
-                  outStride, ncolsOut, b, tw, twLen); return true;
+#define X(LL) case LL: k_rows_c2r<LL><<<(nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st>>>( \
+                  in, inStride, nrows, out, outStride, ncolsOut, tw, twLen); return true;
+    CUP2D_FFT_LENGTHS(X)
+#undef X
+  }
+  return false;
+}
+
+bool dct_rows_fwd(int L, cudaStream_t st, const double* in, int Nx, int nrows, double* D,
+                  const double2* tw, int twLen, FadeArgs fa) {
+  switch (L) {
+#define X(LL) case LL: k_dct_rows_fwd<LL><<<(nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, \
+                  smem_for<LL>((size_t)Len<LL>::B * LL), st>>>(in, Nx, nrows, D, Len<LL>::B, tw, twLen, fa); return true;
+    CUP2D_FFT_LENGTHS(X)
+#undef X
+  }
+  return false;
+}
+
+bool dct_cols(int L, cudaStream_t st, double* D, int Nx, int Ny, const float* cx, const float* cy, double tol,
+              const double2* tw, int twLen) {
+  const int pairs = Nx / 2;
+  switch (L) {
+#define X(LL) case LL: k_dct_cols<LL><<<(pairs + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st>>>( \
+                  D, Nx, Ny, Len<LL>::B, cx, cy, tol, tw, twLen); return true;
+    CUP2D_FFT_LENGTHS(X)
+#undef X
+  }
+  return false;
+}
+
+bool dct_rows_inv(int L, cudaStream_t st, const double* D, int Nx, int nrows, double* out,
+                  const double2* tw, int twLen) {
+  switch (L) {
+#define X(LL) case LL: k_dct_rows_inv<LL><<<(nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st>>>( \
+                  D, Nx, nrows, out, Len<LL>::B, tw, twLen); return true;
     CUP2D_FFT_LENGTHS(X)
 #undef X
   }
@@ -366,13 +692,13 @@ Poisson* poisson_create(Ctx& c) {
     P->Lrow = Nx / 2;      // real length Nx
     P->Lcol = Ny;
   } else {
-    delete P;
-    return nullptr;        // cosine transform solver: not in this build
+    P->Lrow = Nx;          // DCT of length Nx via a real FFT of length 2Nx
+    P->Lcol = 2 * Ny;      // DCT of length Ny via a complex FFT of length 2Ny
   }
   if (!is_pow2(P->Lrow) || !is_pow2(P->Lcol) || P->Lrow < 64 || P->Lcol < 64 ||
       P->Lrow > 4096 || P->Lcol > 4096) { delete P; return nullptr; }   // shared-memory limit
   P->nkx = P->Lrow + 1;
-  P->twLen = 2 * (P->Lrow > P->Lcol ? P->Lrow : P->Lcol);
+  P->twLen = 4 * (P->Lrow > P->Lcol ? P->Lrow : P->Lcol);
   std::vector<double2> tw(P->twLen);
   for (int k = 0; k < P->twLen; k++) {
     const long double a = -2.0L * 3.14159265358979323846264338327950288L * k / P->twLen;
@@ -383,6 +709,16 @@ Poisson* poisson_create(Ctx& c) {
   const size_t specRows = (size_t)P->Lcol;
   if (cudaMalloc(&P->spec, sizeof(double2) * specRows * P->nkx) != cudaSuccess) { poisson_destroy(P); return nullptr; }
   set_all_smem();
+  if (P->type == CUP2D_POISSON_COSINE) {
+    // FFTW_dirichlet constructor (FFTW_dirichlet.h:74-76): cosines stored as float
+    std::vector<float> cx(Nx), cy(Ny);
+    for (int j = 0; j < Ny; j++) cy[j] = (float)std::cos(M_PI / Ny * 2.0 * j);
+    for (int i = 0; i < Nx; i++) cx[i] = (float)std::cos(M_PI / Nx * 2.0 * i);
+    if (cudaMalloc(&P->cosX, sizeof(float) * Nx) != cudaSuccess ||
+        cudaMalloc(&P->cosY, sizeof(float) * Ny) != cudaSuccess) { poisson_destroy(P); return nullptr; }
+    cudaMemcpy(P->cosX, cx.data(), sizeof(float) * Nx, cudaMemcpyHostToDevice);
+    cudaMemcpy(P->cosY, cy.data(), sizeof(float) * Ny, cudaMemcpyHostToDevice);
+  }
   if (P->type == CUP2D_POISSON_FREESPACE) {
     // G^ = Re FFT[G] / (MX MY) on the (2Ny) x (2Nx) grid, kept for ky <= Ny
     if (cudaMalloc(&P->ghat, sizeof(double) * (P->Lcol / 2 + 1) * P->nkx) != cudaSuccess) { poisson_destroy(P); return nullptr; }
@@ -399,7 +735,7 @@ Poisson* poisson_create(Ctx& c) {
 
 void poisson_destroy(Poisson* P) {
   if (!P) return;
-  cudaFree(P->spec); cudaFree(P->ghat); cudaFree(P->tw);
+  cudaFree(P->spec); cudaFree(P->ghat); cudaFree(P->tw); cudaFree(P->cosX); cudaFree(P->cosY);
   delete P;
 }
 
@@ -409,6 +745,11 @@ void poisson_rows_fwd(Ctx& c) {
   Poisson* P = c.poisson;
   const int Nx = c.g.nx, Ny = c.g.ny;
   FadeArgs fa{1, c.dsc, c.g, c.rhs};
+  if (P->type == CUP2D_POISSON_COSINE) {
+    dct_rows_fwd(P->Lrow, c.stream, c.rhs, Nx, Ny, reinterpret_cast<double*>(P->spec), P->tw, P->twLen, fa);
+    CUP2D_LAUNCHED(c);
+    return;
+  }
   rows_r2c(P->Lrow, c.stream, c.rhs, Nx, Ny, Nx, 0, P->spec, P->nkx, P->tw, P->twLen, fa, c.g.h, Nx, Ny);
   CUP2D_LAUNCHED(c);
 }
@@ -416,7 +757,9 @@ void poisson_rows_fwd(Ctx& c) {
 void poisson_cols(Ctx& c) {
   Poisson* P = c.poisson;
   const int Nx = c.g.nx, Ny = c.g.ny;
-  if (P->type == CUP2D_POISSON_FREESPACE) {
+  if (P->type == CUP2D_POISSON_COSINE) {
+    dct_cols(P->Lcol, c.stream, reinterpret_cast<double*>(P->spec), Nx, Ny, P->cosX, P->cosY, P->tol, P->tw, P->twLen);
+  } else if (P->type == CUP2D_POISSON_FREESPACE) {
     cols(P->Lcol, c.stream, P->spec, P->nkx, P->nkx, Ny, Ny, P->ghat, 0, P->tw, P->twLen, 0.0, 0, 0);
   } else {
     const double norm = 1.0 / ((double)Nx * (double)Ny);
@@ -428,6 +771,11 @@ void poisson_cols(Ctx& c) {
 void poisson_rows_inv(Ctx& c) {
   Poisson* P = c.poisson;
   const int Nx = c.g.nx, Ny = c.g.ny;
+  if (P->type == CUP2D_POISSON_COSINE) {
+    dct_rows_inv(P->Lrow, c.stream, reinterpret_cast<const double*>(P->spec), Nx, Ny, c.pres, P->tw, P->twLen);
+    CUP2D_LAUNCHED(c);
+    return;
+  }
   rows_c2r(P->Lrow, c.stream, P->spec, P->nkx, Ny, c.pres, Nx, Nx, P->tw, P->twLen);
   CUP2D_LAUNCHED(c);
 }
@@ -439,3 +787,7 @@ void poisson_solve(Ctx& c) {
 }
 
 } // namespace cup2d
+
+#ifdef CUP2D_TRACE
+namespace cup2d { void trace_bind_poisson(unsigned long long* p) { trace_bind_this_unit(p); } }
+#endif

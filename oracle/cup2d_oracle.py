@@ -217,13 +217,14 @@ def poisson_cosine(rhs, tol=0.1):
     finite-difference / spectral multiplier with float cosine tables, DCT-III."""
     ny, nx = rhs.shape
     F = scipy.fft.dctn(rhs, type=2)             # = FFTW REDFT10 (unnormalised)
-    cx = np.cos(np.pi / nx * 2.0 * np.arange(nx)).astype(np.float32).astype(np.float64)
-    cy = np.cos(np.pi / ny * 2.0 * np.arange(ny)).astype(np.float32).astype(np.float64)
+    cx = np.cos(np.pi / nx * 2.0 * np.arange(nx)).astype(np.float32)
+    cy = np.cos(np.pi / ny * 2.0 * np.arange(ny)).astype(np.float32)
     rkx = (np.arange(nx) + 0.5) * (np.pi / nx)
     rky = (np.arange(ny) + 0.5) * (np.pi / ny)
     RKX, RKY = np.meshgrid(rkx, rky)
     CX, CY = np.meshgrid(cx, cy)
-    denomFD = 1 - CX / 2 - CY / 2
+    # float tables and float arithmetic, as FFTW_dirichlet.h:59 evaluates it
+    denomFD = (np.float32(1) - CX / np.float32(2) - CY / np.float32(2)).astype(np.float64)
     denomSP = RKX * RKX + RKY * RKY
     norm = 0.25 / (nx * ny)
     with np.errstate(divide="ignore", invalid="ignore"):

@@ -86,9 +86,10 @@ def test_advdiff_stage_bitwise(ref):
 
 
 DISK_PERIODIC = DISK.replace("freespace", "periodic")
+DISK_COSINE = DISK.replace("-poissonType freespace ", "")      # "" selects FFTW_dirichlet
 
 
-@pytest.mark.parametrize("args", [DISK, DISK_PERIODIC], ids=["freespace", "periodic"])
+@pytest.mark.parametrize("args", [DISK, DISK_PERIODIC, DISK_COSINE], ids=["freespace", "periodic", "cosine"])
 def test_pressure_stage(ref, args):
     r, s = make_pair(ref, args, noise_seed=11)
     dt = 1e-3
@@ -113,7 +114,7 @@ def test_forces_stage(ref):
     assert abs(a["perimeter"] - b["perimeter"]) <= 1e-12 * b["perimeter"]
 
 
-@pytest.mark.parametrize("args", [DISK, DISK_FREE], ids=["forced_disk", "free_disk"])
+@pytest.mark.parametrize("args", [DISK, DISK_FREE, DISK_COSINE], ids=["forced_disk", "free_disk", "cosine"])
 def test_steps_disk(ref, args):
     r, s = make_pair(ref, args, noise_seed=5)
     for it in range(12):
