@@ -136,15 +136,39 @@ struct StreamScope {
   ~StreamScope() { c.stream = saved; }
 };
 
+// PressureSingle.cpp:216-241 and 362-372: the pressure correction and the
+// momentum integrals run side by side (the integrals evaluate the corrected
+// velocity of their own cells), then collisions and penalization.
+void launch_pressure_tail(Ctx& c) {
+  const double* ui = c.u();
+  const double* vi = c.v();
+  if (c.nshapes > 0) {
+    cudaEventRecord(c.evPres, c.stream);
+    cudaStreamWaitEvent(c.side2, c.evPres, 0);
+    {
+      StreamScope scope(c, c.side2);
+      launch_momenta(c, ui, vi);
+    }
+    cudaEventRecord(c.evMom, c.side2);
+  }
+  launch_pcorr(c);
+  if (c.nshapes > 0) {
+    cudaStreamWaitEvent(c.stream, c.evMom, 0);
+    launch_collide_penalize(c);
+  }
+}
+
 // One pass of Simulation::simulate's loop body (Simulation.cpp:245-251) as a
 // graph with three branches:
-//   main : dt -> body motion -> advDiff, outflow, RHS divergence ->
-//          [join obstacles] -> RHS obstacle terms, fade, Poisson, pressure
-//          correction, momenta, penalization, forces -> [join midline] -> t += dt
+//   main : dt + reset of last step's tiles + body motion -> advDiff (with
+//          outflow), RHS divergence -> [join obstacles] -> RHS obstacle
+//          terms, fade, Poisson -> pressure correction [beside momenta on
+//          side2] -> collisions, penalization, forces -> [join midline] -> t += dt
 //   side : the fish midlines of the next step (they depend on time only)
-//   side2: obstacle tiles, SDF, Towers chi, moments (advDiff does not read them)
+//   side2: obstacle tiles, SDF, Towers chi, moments (advDiff does not read
+//          them); later the momentum integrals
 void enqueue_step(Ctx& c) {
-  launch_max_u_dt(c);
+  launch_step_begin(c);                     // dt, last step's tiles reset, body motion
   bool anyFish = false;
   for (int k = 0; k < c.nshapes; k++) anyFish |= c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK;
   if (anyFish) {
@@ -154,14 +178,19 @@ void enqueue_step(Ctx& c) {
       if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.side, 1);
     cudaEventRecord(c.evJoin, c.side);
   }
-  launch_objects_begin(c, /*midlineReady=*/true);
   cudaEventRecord(c.evObj, c.stream);
   cudaStreamWaitEvent(c.side2, c.evObj, 0);
   {
     StreamScope scope(c, c.side2);
+    c.recordPlaced = c.nshapes > 0;
     launch_objects_rest(c);
+    c.recordPlaced = false;
   }
   cudaEventRecord(c.evObjDone, c.side2);
+  // advDiff starts once the tiles are placed: the placement kernels are
+  // single-CTA latency chains that a full-GPU kernel beside them slows,
+  // while the rasters after them leave most SMs free
+  if (c.nshapes > 0) cudaStreamWaitEvent(c.stream, c.evPlaced, 0);
   launch_advdiff(c);
   launch_outflow(c);
   launch_rhs_div(c);
@@ -169,8 +198,7 @@ void enqueue_step(Ctx& c) {
   launch_rhs_obstacles(c);
   launch_fade_sums(c);
   poisson_solve(c);
-  launch_pcorr(c);
-  launch_momenta_penalize(c);
+  launch_pressure_tail(c);
   launch_forces(c);
   if (anyFish) cudaStreamWaitEvent(c.stream, c.evJoin, 0);
   launch_end_step(c);
@@ -238,15 +266,22 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
   if (!rc) rc = dalloc(ctx, &c.dsc, 1);
   if (!rc) rc = dalloc(ctx, &c.dshapes, MAX_SHAPES);
   if (!rc) rc = dalloc(ctx, &c.counters, Ctx::NCOUNTERS);
-  if (!rc) rc = dalloc(ctx, &c.tileFlags, (size_t)MAX_SHAPES * g.nblocks);
+  // the obstacle branch is the step's critical path: its CTAs go first when
+  // advDiff's compete for the SMs (kernel nodes keep the stream priority)
+  int prLeast = 0, prGreatest = 0;
+  cudaDeviceGetStreamPriorityRange(&prLeast, &prGreatest);
   if (!rc && (cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking) != cudaSuccess ||
-              cudaStreamCreateWithFlags(&c.side2, cudaStreamNonBlocking) != cudaSuccess ||
+              cudaStreamCreateWithPriority(&c.side2, cudaStreamNonBlocking, prGreatest) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evFork, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evJoin, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evObj, cudaEventDisableTiming) != cudaSuccess ||
-              cudaEventCreateWithFlags(&c.evObjDone, cudaEventDisableTiming) != cudaSuccess))
+              cudaEventCreateWithFlags(&c.evObjDone, cudaEventDisableTiming) != cudaSuccess ||
+              cudaEventCreateWithFlags(&c.evPres, cudaEventDisableTiming) != cudaSuccess ||
+              cudaEventCreateWithFlags(&c.evMom, cudaEventDisableTiming) != cudaSuccess ||
+              cudaEventCreateWithFlags(&c.evPlaced, cudaEventDisableTiming) != cudaSuccess))
     rc = fail(ctx, CUP2D_ECUDA, "stream/event creation failed");
-  if (!rc) fish_setup_kernels();
+  if (!rc && fish_setup_kernels() != cudaSuccess)
+    rc = fail(ctx, CUP2D_ECUDA, "shared-memory limits of the fish kernels could not be set");
   if (rc) { cup2d_destroy(ctx); return rc; }
   if (cudaMemset(c.counters, 0, sizeof(unsigned) * Ctx::NCOUNTERS) != cudaSuccess) { cup2d_destroy(ctx); return CUP2D_ECUDA; }
   c.poisson = poisson_create(c);
@@ -266,13 +301,16 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   for (int b = 0; b < 2; b++) for (int d = 0; d < 2; d++) cudaFree(c.vel[b][d]);
   cudaFree(c.chi); cudaFree(c.pres); cudaFree(c.rhs); cudaFree(c.sdf);
   cudaFree(c.udefx); cudaFree(c.udefy); cudaFree(c.dsc); cudaFree(c.dshapes);
-  cudaFree(c.counters); cudaFree(c.partials); cudaFree(c.tileFlags);
+  cudaFree(c.counters); cudaFree(c.partials);
   if (c.side) cudaStreamDestroy(c.side);
   if (c.side2) cudaStreamDestroy(c.side2);
   if (c.evObj) cudaEventDestroy(c.evObj);
   if (c.evObjDone) cudaEventDestroy(c.evObjDone);
   if (c.evFork) cudaEventDestroy(c.evFork);
   if (c.evJoin) cudaEventDestroy(c.evJoin);
+  if (c.evPres) cudaEventDestroy(c.evPres);
+  if (c.evMom) cudaEventDestroy(c.evMom);
+  if (c.evPlaced) cudaEventDestroy(c.evPlaced);
   for (auto& t : c.tiles) {
     cudaFree(t.tiles); cudaFree(t.slot); cudaFree(t.chi); cudaFree(t.dist); cudaFree(t.udx);
     cudaFree(t.udy); cudaFree(t.sD); cudaFree(t.sdx); cudaFree(t.sdy);
@@ -482,8 +520,7 @@ int cup2d_pressure_single(cup2d_ctx* ctx, double dt) {
   launch_rhs_obstacles(c);
   launch_fade_sums(c);
   poisson_solve(c);
-  launch_pcorr(c);
-  launch_momenta_penalize(c);
+  launch_pressure_tail(c);
   return check_launch(ctx);
 }
 
@@ -517,7 +554,7 @@ int cup2d_advance(cup2d_ctx* ctx, int nsteps) {
     if (e != cudaSuccess) return fail(ctx, CUP2D_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
     c.launchesInGraph = (int)(c.launches - before);
     c.launches = before;
-    const cudaError_t e2 = cudaGraphInstantiate(&c.graph, graph, 0);
+    const cudaError_t e2 = cudaGraphInstantiate(&c.graph, graph, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(graph);
     if (e2 != cudaSuccess) { c.graph = nullptr; return fail(ctx, CUP2D_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e2)); }
   }
@@ -702,16 +739,16 @@ extern "C" int cup2d_trace(cup2d_ctx* ctx, unsigned long long* out, int reset) {
   if (!ctx) return CUP2D_EINVAL;
   cudaSetDevice(ctx->c.device);
   if (!buf) {
-    if (cudaMalloc(&buf, sizeof(unsigned long long) * 2 * TR_N) != cudaSuccess) return CUP2D_ENOMEM;
+    if (cudaMalloc(&buf, sizeof(unsigned long long) * (2 * TR_N + 8 * TRACE_ITEMS)) != cudaSuccess) return CUP2D_ENOMEM;
     trace_bind_fluid(buf); trace_bind_obstacles(buf); trace_bind_fish(buf); trace_bind_poisson(buf);
     reset = 1;
   }
   cudaDeviceSynchronize();
-  if (out) cudaMemcpy(out, buf, sizeof(unsigned long long) * 2 * TR_N, cudaMemcpyDeviceToHost);
+  if (out) cudaMemcpy(out, buf, sizeof(unsigned long long) * (2 * TR_N + 8 * TRACE_ITEMS), cudaMemcpyDeviceToHost);
   if (reset) {
-    std::vector<unsigned long long> init(2 * TR_N);
+    std::vector<unsigned long long> init(2 * TR_N + 8 * TRACE_ITEMS, 0);
     for (int i = 0; i < TR_N; i++) { init[2 * i] = ~0ULL; init[2 * i + 1] = 0; }
-    cudaMemcpy(buf, init.data(), sizeof(unsigned long long) * 2 * TR_N, cudaMemcpyHostToDevice);
+    cudaMemcpy(buf, init.data(), sizeof(unsigned long long) * init.size(), cudaMemcpyHostToDevice);
   }
   return CUP2D_OK;
 }

@@ -41,10 +41,12 @@ struct Ctx {
   static constexpr int NCOUNTERS = 256;
 
   Poisson* poisson = nullptr;
-  int* tileFlags = nullptr;     // [MAX_SHAPES][nblocks] touched-block flags
   cudaStream_t side = nullptr;  // branch for the next step's fish midlines
   cudaStream_t side2 = nullptr; // branch for the obstacle chain, beside advDiff
   cudaEvent_t evFork = nullptr, evJoin = nullptr, evObj = nullptr, evObjDone = nullptr;
+  cudaEvent_t evPres = nullptr, evMom = nullptr;
+  cudaEvent_t evPlaced = nullptr;   // recorded after the obstacle tiles are placed
+  bool recordPlaced = false;
 
   cudaGraphExec_t graph = nullptr;
   long long launches = 0;

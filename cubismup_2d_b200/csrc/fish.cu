@@ -239,12 +239,15 @@ k_fish_midline(const Scalars* sc, const DevShape* sh, int k, FishArrays F, int m
   }
 }
 
-__global__ void __launch_bounds__(512)
-k_fish_frame(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays F)
+// 1024 threads of at most 64 registers take a whole SM's register file, so
+// no other kernel's CTA shares (and slows) the SM of this latency-bound CTA.
+__global__ void __launch_bounds__(1024)
+k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTiles t)
 {
   CUP2D_TRACE_SCOPE(TR_FRAME);
+  CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 0);
   extern __shared__ double fsm[];                      // the frame midline, staged
-  __shared__ double bc[2];
+  __shared__ double bc[3];
   DevShape& S = sh[k];
   const int Nm = F.nm, tid = threadIdx.x, nt = blockDim.x;
   const int p = sc->step & 1;
@@ -256,20 +259,22 @@ k_fish_frame(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays F)
     S.f.angvel_internal_prev = S.f.angvel_internal;
     S.f.J_internal = integ[5];
     S.f.angvel_internal = integ[6];
-    bc[0] = S.f.theta_internal; bc[1] = integ[6];
+    bc[0] = S.f.cosTh; bc[1] = S.f.sinTh; bc[2] = integ[6];   // theta_internal, angvel
   }
   double* rX = fsm;           double* rY = rX + Nm;
   double* vX = rY + Nm;       double* vY = vX + Nm;
   double* norX = vY + Nm;     double* norY = norX + Nm;
   double* vNorX = norY + Nm;  double* vNorY = vNorX + Nm;
   double* width = vNorY + Nm; double* rS = width + Nm;
+  Segment* segS = reinterpret_cast<Segment*>(rS + Nm);  // this step's segments, also kept on chip
   for (int i = tid; i < Nm; i += nt) { width[i] = F.width[i]; rS[i] = F.rS[i]; }
   __syncthreads();
+  CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 1);
   const FishMidline& M = F.mid[p];
   const FishMidline& R = F.frame;
   {                                                     // changeToCoMFrameAngular
-    const double Ain = bc[0], vAin = bc[1];
-    const double R00 = cos(Ain), R01 = -sin(Ain), R10 = sin(Ain), R11 = cos(Ain);
+    const double vAin = bc[2];
+    const double R00 = bc[0], R01 = -bc[1], R10 = bc[1], R11 = bc[0];   // rotation by theta_internal
     for (int i = tid; i < Nm; i += nt) {
       const double px = M.rX[i], py = M.rY[i];
       const double qx = M.vX[i] + vAin * py, qy = M.vY[i] - vAin * px;
@@ -279,6 +284,7 @@ k_fish_frame(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays F)
       R.rX[i] = a; R.rY[i] = b; R.vX[i] = c; R.vY[i] = d;
     }
     __syncthreads();
+  CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 2);
     for (int i = tid; i < Nm; i += nt) {                // _computeMidlineNormals
       const int j = i < Nm - 1 ? i : Nm - 2;            // the last copies its neighbour
       const double ds = rS[j + 1] - rS[j];
@@ -289,12 +295,19 @@ k_fish_frame(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays F)
       R.norX[i] = a; R.norY[i] = b; R.vNorX[i] = c; R.vNorY[i] = d;
     }
     __syncthreads();
+  CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 3);
   }
-  // AreaSegments (Fish.cpp:118-150) in the computational frame
+  // Warps 0-1 build the AreaSegments and their bounding box (the chain to
+  // the tile search); warps 2.. generate the surface and interior points
+  // meanwhile (only the raster reads them).
   const int Nseg = F.nseg;
-  const double angle = S.s.orientation;
-  const double R00 = cos(angle), R01 = -sin(angle), R10 = sin(angle), R11 = cos(angle);
-  for (int i = tid; i < Nseg; i += nt) {
+  const double R00 = S.cosO, R01 = -S.sinO, R10 = S.sinO, R11 = S.cosO;   // rotation by the orientation
+  const double h = g.h;
+  __shared__ double box[4];
+  constexpr int SEGT = 64;                              // threads of the segment warps
+  if (tid < SEGT) {
+  // AreaSegments (Fish.cpp:118-150) in the computational frame
+  for (int i = tid; i < Nseg; i += SEGT) {
     const int next_idx = (i + 1) * (Nm - 1) / Nseg, idx = i * (Nm - 1) / Nseg;
     double bb[2][2] = {{1e9, -1e9}, {1e9, -1e9}};
     for (int ss = idx; ss <= next_idx; ++ss) {
@@ -328,11 +341,29 @@ k_fish_frame(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays F)
       sg.boxObj[d][1] = sg.c[d] + sg.w[d];
     }
     F.seg[i] = sg;
+    segS[i] = sg;
   }
+  CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 4);
+  asm volatile("bar.sync 1, %0;" :: "n"(SEGT) : "memory");   // the segment warps only
+  if (tid < 32) {                                       // one warp: bounding box of boxLab
+    double lo0 = 1e300, hi0 = -1e300, lo1 = 1e300, hi1 = -1e300;
+    for (int i = tid; i < Nseg; i += 32) {
+      const Segment& sg = segS[i];
+      lo0 = fmin(lo0, sg.boxLab[0][0]); hi0 = fmax(hi0, sg.boxLab[0][1]);
+      lo1 = fmin(lo1, sg.boxLab[1][0]); hi1 = fmax(hi1, sg.boxLab[1][1]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      lo0 = fmin(lo0, __shfl_xor_sync(0xffffffffu, lo0, o)); hi0 = fmax(hi0, __shfl_xor_sync(0xffffffffu, hi0, o));
+      lo1 = fmin(lo1, __shfl_xor_sync(0xffffffffu, lo1, o)); hi1 = fmax(hi1, __shfl_xor_sync(0xffffffffu, hi1, o));
+    }
+    if (tid == 0) { box[0] = lo0; box[1] = hi0; box[2] = lo1; box[3] = hi1; S.nseg = Nseg; }
+  }
+  } else {
   // surface points of constructSurface (FishLibrary.cpp:470-486) and interior
   // points of constructInternl (FishLibrary.cpp:597-610), computational frame
+  const int pt = tid - SEGT, pnt = nt - SEGT;
   const double pos0 = S.s.center[0], pos1 = S.s.center[1];
-  for (int q = tid; q < 2 * Nm; q += nt) {
+  for (int q = pt; q < 2 * Nm; q += pnt) {
     const int ss = q >> 1, signp = (q & 1) ? 1 : -1;
     const double m0 = rX[ss] + width[ss] * signp * norX[ss];
     const double m1 = rY[ss] + width[ss] * signp * norY[ss];
@@ -341,8 +372,7 @@ k_fish_frame(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays F)
     const double u1 = vY[ss] + width[ss] * signp * vNorY[ss];
     F.su[q] = make_double2(R00 * u0 + R01 * u1, R10 * u0 + R11 * u1);
   }
-  const double h = g.h;
-  for (int q = tid; q < F.nint; q += nt) {
+  for (int q = pt; q < F.nint; q += pnt) {
     const int2 si = F.ipIdx[q];
     const int ss = si.x, iw = si.y;
     const double offsetW = iw * h;
@@ -351,7 +381,55 @@ k_fish_frame(GridDesc g, const Scalars* sc, DevShape* sh, int k, FishArrays F)
     const double u0 = vX[ss] + offsetW * vNorX[ss], u1 = vY[ss] + offsetW * vNorY[ss];
     F.iu[q] = make_double2(R00 * u0 + R01 * u1, R10 * u0 + R11 * u1);
   }
-  if (tid == 0) S.nseg = Nseg;
+  }
+  CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 5);
+  // the obstacle tiles: blocks any segment intersects (Fish.cpp:158-173),
+  // searched inside the segments' bounding box only
+  __syncthreads();
+  CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 6);
+  CUP2D_TRACE_SCOPE(TR_SELECT);
+  int bx0, bx1, by0, by1;
+  block_range(box[0], box[1], h, 2 * h, bx0, bx1);
+  block_range(box[2], box[3], h, 2 * h, by0, by1);
+  clip_rect(g, bx0, bx1, by0, by1);
+  const int W = bx1 - bx0 + 1, H = by1 - by0 + 1, ncand = (W > 0 && H > 0) ? W * H : 0;
+  // candidates in chunks of one per thread, in increasing block order; the
+  // (candidate, segment) pairs of a chunk are spread over the threads
+  __shared__ unsigned char hit[1024];
+  __shared__ int wcnt[32];
+  __shared__ int base;
+  const int lane = tid & 31, wid = tid >> 5, nwarps = nt >> 5;
+  if (tid == 0) base = 0;
+  for (int c0 = 0; c0 < ncand; c0 += nt) {
+    const int nq = min(nt, ncand - c0);
+    if (tid < nq) hit[tid] = 0;
+    __syncthreads();
+    for (int pr = tid; pr < nq * Nseg; pr += nt) {
+      const int cq = pr / Nseg, si = pr - cq * Nseg;
+      if (hit[cq]) continue;
+      const int q = c0 + cq, by = by0 + q / W, bx = bx0 + q % W;
+      const double start[2] = {cell_x(g, bx, 0), cell_y(g, by, 0)};
+      const double end[2] = {cell_x(g, bx, BS - 1), cell_y(g, by, BS - 1)};
+      if (segment_hits_block(segS[si], start, end, 2 * h)) hit[cq] = 1;
+    }
+    __syncthreads();
+    const bool f = tid < nq && hit[tid];
+    const unsigned m = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) wcnt[wid] = __popc(m);
+    __syncthreads();
+    int off = 0, tot = 0;
+    for (int w = 0; w < nwarps; w++) { if (w < wid) off += wcnt[w]; tot += wcnt[w]; }
+    const int pos = base + off + __popc(m & ((1u << lane) - 1u));
+    if (f) {
+      const int q = c0 + tid, b = (by0 + q / W) * g.bpdx + bx0 + q % W;
+      if (pos < t.capacity) { t.tiles[pos] = b; t.slot[b] = pos; }
+      else atomicOr(&sc->status, ST_CAPACITY);
+    }
+    __syncthreads();
+    if (tid == 0) base += tot;
+  }
+  __syncthreads();
+  if (tid == 0) S.ntiles = base < t.capacity ? base : t.capacity;
 }
 
 struct SurfPt { double myP[2], pP[2], pM[2], ud[2]; int iap[2], ss; };
@@ -361,6 +439,8 @@ constexpr int SUB = 16;                     // cells per sub-tile edge
 constexpr int NSUB = (BS / SUB) * (BS / SUB);
 constexpr int RT = SUB * SUB;               // threads per CTA (one per cell)
 constexpr int NWARP = RT / 32;
+constexpr int CH = 4;                       // candidate points per thread and chunk
+constexpr int CAP = RT * CH;                // points per chunk
 constexpr int MAX_SEG_PER_TILE = 256;
 
 // order-preserving compaction over the CTA's warps; returns the count
@@ -375,6 +455,28 @@ __device__ __forceinline__ int compact_slot(bool keep, int* wc, int& pos) {
   return tot;
 }
 
+// The same for CH candidates per thread, candidate r of thread t being
+// number r*RT + t of the chunk: positions follow that order.  One barrier.
+__device__ __forceinline__ int compact_chunk(const bool (&keep)[CH], int (*wc)[NWARP], int (&pos)[CH]) {
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  unsigned m[CH];
+#pragma unroll
+  for (int r = 0; r < CH; r++) {
+    m[r] = __ballot_sync(0xffffffffu, keep[r]);
+    if (lane == 0) wc[r][wid] = __popc(m[r]);
+  }
+  __syncthreads();
+  int base = 0;
+#pragma unroll
+  for (int r = 0; r < CH; r++) {
+    int off = 0, tot = 0;
+    for (int w = 0; w < NWARP; w++) { if (w < wid) off += wc[r][w]; tot += wc[r][w]; }
+    pos[r] = base + off + __popc(m[r] & ((1u << lane) - 1u));
+    base += tot;
+  }
+  return base;
+}
+
 // index of the list entry whose range [start[i], start[i+1]) holds q
 __device__ __forceinline__ int find_range(const int* start, int n, int q) {
   int lo = 0, hi = n;            // start[0] = 0 <= q < start[n]
@@ -387,14 +489,11 @@ __device__ __forceinline__ int find_range(const int* start, int n, int q) {
 // appends (ballot + popc, so order is kept) those whose support covers each
 // of its rows.  Every cell then visits only its row's points, in the
 // reference's order, and skips those whose columns miss it.
-struct RowLists {
-  unsigned short idx[SUB][RT];
-  int n[SUB];
-};
-
-__device__ __forceinline__ void rows_build(RowLists& Lr, const uchar4* supp, int nc, int sy0) {
+__device__ __forceinline__ void rows_build(unsigned short* rowIdx, int* rowN, const uchar4* supp, int nc) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int rA = 2 * w, rB = 2 * w + 1;
+  unsigned short* lA = rowIdx + rA * CAP;
+  unsigned short* lB = rowIdx + rB * CAP;
   int nA = 0, nB = 0;
   for (int p0 = 0; p0 < nc; p0 += 32) {
     const int p = p0 + lane;
@@ -406,13 +505,19 @@ __device__ __forceinline__ void rows_build(RowLists& Lr, const uchar4* supp, int
     }
     const unsigned mA = __ballot_sync(0xffffffffu, inA), mB = __ballot_sync(0xffffffffu, inB);
     const unsigned lt = (1u << lane) - 1u;
-    if (inA) Lr.idx[rA][nA + __popc(mA & lt)] = (unsigned short)p;
-    if (inB) Lr.idx[rB][nB + __popc(mB & lt)] = (unsigned short)p;
+    if (inA) lA[nA + __popc(mA & lt)] = (unsigned short)p;
+    if (inB) lB[nB + __popc(mB & lt)] = (unsigned short)p;
     nA += __popc(mA); nB += __popc(mB);
   }
-  if (lane == 0) { Lr.n[rA] = nA; Lr.n[rB] = nB; }
+  if (lane == 0) { rowN[rA] = nA; rowN[rB] = nB; }
   __syncwarp();
-  (void)sy0;
+}
+
+// dynamic shared memory of the raster: frame midline x, y, width (3 Nm
+// doubles), the chunk's points, their supports and the row lists
+inline size_t raster_smem(int Nm) {
+  const size_t pts = CAP * (sizeof(SurfPt) > sizeof(IntPt) ? sizeof(SurfPt) : sizeof(IntPt));
+  return sizeof(double) * 3 * (size_t)Nm + pts + sizeof(uchar4) * CAP + sizeof(unsigned short) * SUB * CAP;
 }
 
 __global__ void __launch_bounds__(RT)
@@ -426,26 +531,31 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
   __shared__ int intStart[MAX_SEG_PER_TILE + 1];
   __shared__ int nSegList;
   __shared__ int wc[NWARP];
-  __shared__ RowLists Lr;
-  __shared__ uchar4 supp[RT];
-  __shared__ union { SurfPt s[RT]; IntPt i[RT]; } pts;
-  extern __shared__ double msm[];                       // frame midline x, y and width
+  __shared__ int wcc[CH][NWARP];
+  __shared__ int rowN[SUB];
+  extern __shared__ double msm[];
   const DevShape& S = sh[k];
   const int nwork = S.ntiles * NSUB;
   if ((int)blockIdx.x >= nwork) return;
   const int tid = threadIdx.x;
   const int Nm = F.nm;
   double* rX = msm; double* rY = msm + Nm; double* width = msm + 2 * Nm;
+  SurfPt* ptsS = reinterpret_cast<SurfPt*>(msm + 3 * Nm);
+  IntPt* ptsI = reinterpret_cast<IntPt*>(msm + 3 * Nm);
+  uchar4* supp = reinterpret_cast<uchar4*>(reinterpret_cast<char*>(msm + 3 * Nm) +
+                                           CAP * (sizeof(SurfPt) > sizeof(IntPt) ? sizeof(SurfPt) : sizeof(IntPt)));
+  unsigned short* rowIdx = reinterpret_cast<unsigned short*>(supp + CAP);
   for (int i = tid; i < Nm; i += RT) { rX[i] = F.frame.rX[i]; rY[i] = F.frame.rY[i]; width[i] = F.width[i]; }
   const double h = g.h, invh = 1.0 / h;
-  const double angle = S.s.orientation;
-  const double R00 = cos(angle), R01 = -sin(angle), R10 = sin(angle), R11 = cos(angle);
+  const double R00 = S.cosO, R01 = -S.sinO, R10 = S.sinO, R11 = S.cosO;   // rotation by the orientation
   const double pos0 = S.s.center[0], pos1 = S.s.center[1];
   for (int wi = blockIdx.x; wi < nwork; wi += gridDim.x) {
   const int s = wi / NSUB, sub = wi % NSUB;
+  CUP2D_TRACE_MARK(wi, 0);
   const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
   const int sx0 = (sub % (BS / SUB)) * SUB, sy0 = (sub / (BS / SUB)) * SUB;
   const int ix = sx0 + tid % SUB, iy = sy0 + tid / SUB;
+  const int row = iy - sy0, col = ix - sx0;
   const double org0 = cell_x(g, bx, 0), org1 = cell_y(g, by, 0);
 
   // ordered list of the segments intersecting this block (Fish.cpp:167-173),
@@ -489,51 +599,85 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
   }
   __syncthreads();
   const int totSurf = surfStart[nsl], totInt = intStart[nsl];
+  CUP2D_TRACE_MARK(wi, 1);
   const double px = cell_x(g, bx, ix), py = cell_y(g, by, iy);   // info.pos(p, sx, sy)
 
-  // constructSurface (FishLibrary.cpp:438-573)
+  // constructSurface (FishLibrary.cpp:438-573).  A point changes the cell
+  // only if its nearest-of-three squared distance dist1 = min(dist0, distP,
+  // distM) is below |dist|, and then |dist| becomes dist1 (sign2d is +-1):
+  // the cell ends with the first point, in the reference's order, attaining
+  // the strict running minimum, so the sign, weight and velocity are
+  // evaluated once, for that point.
   double dist = -1, chi = 0, ud0 = 0, ud1 = 0;
-  for (int c0 = 0; c0 < totSurf; c0 += RT) {
-    SurfPt P;
-    bool keep = false;
-    int xlo = 0, xhi = 0, ylo = 0, yhi = 0;
-    const int q = c0 + tid;
-    if (q < totSurf) {
-      const int si = find_range(surfStart, nsl, q);
-      const int r = q - surfStart[si];
-      const int ss = segFst[si] + r / 2, side = r & 1;
-      const double2 my = F.sp[2 * ss + side], pp = F.sp[2 * (ss + 1) + side];
-      const double2 pm = F.sp[2 * (ss - 1) + side], u = F.su[2 * ss + side];
-      P.ss = ss;
-      P.myP[0] = my.x; P.myP[1] = my.y;
-      P.pP[0] = pp.x; P.pP[1] = pp.y; P.pM[0] = pm.x; P.pM[1] = pm.y;
-      P.ud[0] = u.x; P.ud[1] = u.y;
-      P.iap[0] = (int)floor((P.myP[0] - org0) * invh);
-      P.iap[1] = (int)floor((P.myP[1] - org1) * invh);
-      // support [iap-1, iap+3) clipped to the block, intersected with this sub-tile
-      xlo = max(max(0, P.iap[0] - 1), sx0); xhi = min(min(P.iap[0] + 3, BS), sx0 + SUB);
-      ylo = max(max(0, P.iap[1] - 1), sy0); yhi = min(min(P.iap[1] + 3, BS), sy0 + SUB);
-      keep = xlo < xhi && ylo < yhi;
+  double best = 1.0;                                    // |dist| of the initial -1
+  for (int c0 = 0; c0 < totSurf; c0 += CAP) {
+    // the keep test needs the point itself only; kept points load the rest
+    // (neighbours, velocity) after the compaction
+    int gs[CH];                                       // sp / su index of the candidate
+    double2 my[CH];
+    bool keep[CH];
+    uchar4 sup[CH];
+#pragma unroll
+    for (int r = 0; r < CH; r++) {
+      keep[r] = false;
+      gs[r] = 0;
+      const int q = c0 + r * RT + tid;
+      if (q < totSurf) {
+        const int si = find_range(surfStart, nsl, q);
+        const int rr = q - surfStart[si];
+        const int ss = segFst[si] + rr / 2, side = rr & 1;
+        gs[r] = 2 * ss + side;
+        my[r] = F.sp[gs[r]];
+      }
     }
-    int pos;
-    const int nc = compact_slot(keep, wc, pos);
-    if (keep) {
-      pts.s[pos] = P;
-      supp[pos] = make_uchar4(xlo - sx0, xhi - sx0, ylo - sy0, yhi - sy0);
+#pragma unroll
+    for (int r = 0; r < CH; r++) {
+      const int q = c0 + r * RT + tid;
+      if (q < totSurf) {
+        const int iap0 = (int)floor((my[r].x - org0) * invh), iap1 = (int)floor((my[r].y - org1) * invh);
+        // support [iap-1, iap+3) clipped to the block, intersected with this sub-tile
+        const int xlo = max(max(0, iap0 - 1), sx0), xhi = min(min(iap0 + 3, BS), sx0 + SUB);
+        const int ylo = max(max(0, iap1 - 1), sy0), yhi = min(min(iap1 + 3, BS), sy0 + SUB);
+        keep[r] = xlo < xhi && ylo < yhi;
+        sup[r] = make_uchar4(xlo - sx0, xhi - sx0, ylo - sy0, yhi - sy0);
+      }
     }
+    int pos[CH];
+    const int nc = compact_chunk(keep, wcc, pos);
+#pragma unroll
+    for (int r = 0; r < CH; r++)
+      if (keep[r]) {
+        SurfPt& Pr = ptsS[pos[r]];
+        const double2 pp = F.sp[gs[r] + 2], pm = F.sp[gs[r] - 2], u = F.su[gs[r]];
+        Pr.ss = gs[r] >> 1;
+        Pr.myP[0] = my[r].x; Pr.myP[1] = my[r].y;
+        Pr.pP[0] = pp.x; Pr.pP[1] = pp.y; Pr.pM[0] = pm.x; Pr.pM[1] = pm.y;
+        Pr.ud[0] = u.x; Pr.ud[1] = u.y;
+        supp[pos[r]] = sup[r];
+      }
     __syncthreads();
-    rows_build(Lr, supp, nc, sy0);
-    const int row = iy - sy0, col = ix - sx0;
-    const int n = Lr.n[row];
+    rows_build(rowIdx, rowN, supp, nc);
+    const int n = rowN[row];
+    const unsigned short* l = rowIdx + row * CAP;
+    int winner = -1;
     for (int e = 0; e < n; e++) {
-      const int qi = Lr.idx[row][e];
+      const int qi = l[e];
       const uchar4 sp = supp[qi];
       if (col < sp.x || col >= sp.y) continue;
-      const SurfPt& Q = pts.s[qi];
+      const SurfPt& Q = ptsS[qi];
       const double dist0 = sq(px - Q.myP[0]) + sq(py - Q.myP[1]);
       const double distP = sq(px - Q.pP[0]) + sq(py - Q.pP[1]);
       const double distM = sq(px - Q.pM[0]) + sq(py - Q.pM[1]);
-      if (fabs(dist) < fmin(fmin(dist0, distP), distM)) continue;
+      const double dist1 = fmin(fmin(dist0, distP), distM);
+      if (best > dist1) { best = dist1; winner = qi; }
+    }
+    if (winner >= 0) {
+      // evaluate the winner of this chunk now (its point data is in shared
+      // memory only until the next chunk); a later chunk's winner replaces it
+      const SurfPt& Q = ptsS[winner];
+      const double dist0 = sq(px - Q.myP[0]) + sq(py - Q.myP[1]);
+      const double distP = sq(px - Q.pP[0]) + sq(py - Q.pP[1]);
+      const double distM = sq(px - Q.pM[0]) + sq(py - Q.pM[1]);
       // changeFromComputationalFrame (FishLibrary.h:194-200)
       const double q0 = px - pos0, q1 = py - pos1;
       const double p0 = R00 * q0 + R10 * q1, p1 = R01 * q0 + R11 * q1;
@@ -565,51 +709,67 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
         const double grd2Core = sq(p0 - xC0) + sq(p1 - xC1);
         sign2d = grd2Core > Rsq ? -1 : 1;
       }
-      if (fabs(dist) > dist1) {
-        const double W = 1 - sqrt(dist1) * (invh / 3);
-        ud0 = W * Q.ud[0]; ud1 = W * Q.ud[1];
-        dist = sign2d * dist1;
-        chi = W;
-      }
+      const double W = 1 - sqrt(dist1) * (invh / 3);
+      ud0 = W * Q.ud[0]; ud1 = W * Q.ud[1];
+      dist = sign2d * dist1;
+      chi = W;
     }
     __syncthreads();
   }
 
+  CUP2D_TRACE_MARK(wi, 2);
   // constructInternl (FishLibrary.cpp:575-638)
-  for (int c0 = 0; c0 < totInt; c0 += RT) {
-    IntPt P;
-    bool keep = false;
-    int xlo = 0, xhi = 0, ylo = 0, yhi = 0;
-    const int q = c0 + tid;
-    if (q < totInt) {
-      const int si = find_range(intStart, nsl, q);
-      const int gq = segIntBase[si] + (q - intStart[si]);
-      const double2 xw = F.ip[gq], u = F.iu[gq];
-      const double xp0 = (xw.x - org0) * invh, xp1 = (xw.y - org1) * invh;
-      const double ap0 = floor(xp0), ap1 = floor(xp1);
-      P.iap[0] = (int)ap0; P.iap[1] = (int)ap1;
-      xlo = max(max(0, P.iap[0]), sx0); xhi = min(min(P.iap[0] + 2, BS), sx0 + SUB);
-      ylo = max(max(0, P.iap[1]), sy0); yhi = min(min(P.iap[1] + 2, BS), sy0 + SUB);
-      keep = xlo < xhi && ylo < yhi;
-      P.ud[0] = u.x; P.ud[1] = u.y;
-      P.w[0][0] = 1 - fabs(xp0 - ap0); P.w[0][1] = 1 - fabs(xp0 - (ap0 + 1));
-      P.w[1][0] = 1 - fabs(xp1 - ap1); P.w[1][1] = 1 - fabs(xp1 - (ap1 + 1));
+  for (int c0 = 0; c0 < totInt; c0 += CAP) {
+    int gq[CH];
+    double2 xw[CH];
+    bool keep[CH];
+    uchar4 sup[CH];
+#pragma unroll
+    for (int r = 0; r < CH; r++) {
+      keep[r] = false;
+      gq[r] = 0;
+      const int q = c0 + r * RT + tid;
+      if (q < totInt) {
+        const int si = find_range(intStart, nsl, q);
+        gq[r] = segIntBase[si] + (q - intStart[si]);
+        xw[r] = F.ip[gq[r]];
+      }
     }
-    int pos;
-    const int nc = compact_slot(keep, wc, pos);
-    if (keep) {
-      pts.i[pos] = P;
-      supp[pos] = make_uchar4(xlo - sx0, xhi - sx0, ylo - sy0, yhi - sy0);
+#pragma unroll
+    for (int r = 0; r < CH; r++) {
+      const int q = c0 + r * RT + tid;
+      if (q < totInt) {
+        const int iap0 = (int)floor((xw[r].x - org0) * invh), iap1 = (int)floor((xw[r].y - org1) * invh);
+        const int xlo = max(max(0, iap0), sx0), xhi = min(min(iap0 + 2, BS), sx0 + SUB);
+        const int ylo = max(max(0, iap1), sy0), yhi = min(min(iap1 + 2, BS), sy0 + SUB);
+        keep[r] = xlo < xhi && ylo < yhi;
+        sup[r] = make_uchar4(xlo - sx0, xhi - sx0, ylo - sy0, yhi - sy0);
+      }
     }
+    int pos[CH];
+    const int nc = compact_chunk(keep, wcc, pos);
+#pragma unroll
+    for (int r = 0; r < CH; r++)
+      if (keep[r]) {
+        IntPt& Pr = ptsI[pos[r]];
+        const double2 u = F.iu[gq[r]];
+        const double xp0 = (xw[r].x - org0) * invh, xp1 = (xw[r].y - org1) * invh;
+        const double ap0 = floor(xp0), ap1 = floor(xp1);
+        Pr.iap[0] = (int)ap0; Pr.iap[1] = (int)ap1;
+        Pr.ud[0] = u.x; Pr.ud[1] = u.y;
+        Pr.w[0][0] = 1 - fabs(xp0 - ap0); Pr.w[0][1] = 1 - fabs(xp0 - (ap0 + 1));
+        Pr.w[1][0] = 1 - fabs(xp1 - ap1); Pr.w[1][1] = 1 - fabs(xp1 - (ap1 + 1));
+        supp[pos[r]] = sup[r];
+      }
     __syncthreads();
-    rows_build(Lr, supp, nc, sy0);
-    const int row = iy - sy0, col = ix - sx0;
-    const int n = Lr.n[row];
+    rows_build(rowIdx, rowN, supp, nc);
+    const int n = rowN[row];
+    const unsigned short* l = rowIdx + row * CAP;
     for (int e = 0; e < n; e++) {
-      const int qi = Lr.idx[row][e];
+      const int qi = l[e];
       const uchar4 sp = supp[qi];
       if (col < sp.x || col >= sp.y) continue;
-      const IntPt& Q = pts.i[qi];
+      const IntPt& Q = ptsI[qi];
       const int sx = ix - Q.iap[0], sy = iy - Q.iap[1];
       const double wxwy = Q.w[1][sy] * Q.w[0][sx];
       ud0 += wxwy * Q.ud[0];
@@ -620,6 +780,7 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
     __syncthreads();
   }
 
+  CUP2D_TRACE_MARK(wi, 3);
   // signedDistanceSqrt (FishLibrary.cpp:419-436)
   const double normfac = chi > EPSd ? chi : 1;
   ud0 /= normfac; ud1 /= normfac;
@@ -628,27 +789,27 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
   t.dist[o] = dist; t.chi[o] = 0; t.udx[o] = ud0; t.udy[o] = ud1;
   atomic_max_double(&sdfg[(size_t)(by * BS + iy) * g.nx + bx * BS + ix], dist);
   __syncthreads();                                      // shared state is reused by the next item
+  CUP2D_TRACE_MARK(wi, 4);
+#ifdef CUP2D_TRACE
+  if (threadIdx.x == 0 && wi < TRACE_ITEMS && g_trace) {   // counts of the trace build
+    g_trace[2 * TR_N + 8 * wi + 5] = totSurf; g_trace[2 * TR_N + 8 * wi + 6] = totInt;
+    g_trace[2 * TR_N + 8 * wi + 7] = nsl;
+  }
+#endif
   }
 }
 
 size_t midline_smem(int Nm) { return sizeof(double) * 12 * (size_t)Nm; }
-size_t frame_smem(int Nm) { return sizeof(double) * 10 * (size_t)Nm; }
+size_t frame_smem(int Nm, int nseg) { return sizeof(double) * 10 * (size_t)Nm + sizeof(Segment) * (size_t)nseg; }
 
 } // namespace
 
-FishSegPtrs fish_seg_ptrs(const Ctx& c) {
-  FishSegPtrs p{};
-  for (int k = 0; k < c.nshapes; k++) p.seg[k] = c.fish[k].seg;
-  return p;
-}
 
-void fish_setup_kernels() {
-  int dev = 0, maxOptin = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&maxOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  cudaFuncSetAttribute((const void*)k_fish_midline, cudaFuncAttributeMaxDynamicSharedMemorySize, maxOptin);
-  cudaFuncSetAttribute((const void*)k_fish_frame, cudaFuncAttributeMaxDynamicSharedMemorySize, maxOptin);
-  cudaFuncSetAttribute((const void*)k_fish_raster, cudaFuncAttributeMaxDynamicSharedMemorySize, maxOptin);
+cudaError_t fish_setup_kernels() {
+  cudaError_t e = allow_max_dynamic_smem((const void*)k_fish_midline);
+  if (e == cudaSuccess) e = allow_max_dynamic_smem((const void*)k_fish_frame);
+  if (e == cudaSuccess) e = allow_max_dynamic_smem((const void*)k_fish_raster);
+  return e;
 }
 
 void launch_fish_midline(Ctx& c, int k, cudaStream_t stream, int mode) {
@@ -656,8 +817,8 @@ void launch_fish_midline(Ctx& c, int k, cudaStream_t stream, int mode) {
   CUP2D_LAUNCHED(c);
 }
 
-void launch_fish_kinematics(Ctx& c, int k) {
-  k_fish_frame<<<1, 512, frame_smem(c.fish[k].nm), c.stream>>>(c.g, c.dsc, c.dshapes, k, c.fish[k]);
+void launch_fish_place(Ctx& c, int k) {
+  k_fish_frame<<<1, 1024, frame_smem(c.fish[k].nm, c.fish[k].nseg), c.stream>>>(c.g, c.dsc, c.dshapes, k, c.fish[k], c.tiles[k]);
   CUP2D_LAUNCHED(c);
 }
 
@@ -665,7 +826,7 @@ void launch_fish_raster(Ctx& c, int k) {
   // two resident CTAs per SM at most (registers); each loops over
   // (tile, sub-tile) items
   const int items = c.tiles[k].capacity * NSUB, grid = items < 2 * c.sms ? items : 2 * c.sms;
-  k_fish_raster<<<grid, RT, sizeof(double) * 3 * (size_t)c.fish[k].nm, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
+  k_fish_raster<<<grid, RT, raster_smem(c.fish[k].nm), c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
                                                                 c.fish[k], c.sdf);
   CUP2D_LAUNCHED(c);
 }

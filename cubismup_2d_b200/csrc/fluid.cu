@@ -12,6 +12,7 @@
 // differs).
 #include <cmath>
 #include "context.hpp"
+#include "step_begin.cuh"
 
 namespace cup2d {
 
@@ -19,53 +20,14 @@ namespace {
 
 constexpr double EPSd = 2.220446049250313e-16;   // std::numeric_limits<double>::epsilon()
 
-__global__ void k_max_u_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh,
-                           const double* __restrict__ u, const double* __restrict__ v,
-                           double* partials, unsigned* counter)
+__global__ void __launch_bounds__(512)
+k_max_u_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh,
+           const double* __restrict__ u, const double* __restrict__ v,
+           double* partials, unsigned* counter)
 {
   CUP2D_TRACE_SCOPE(TR_MAXU);
   __shared__ double red[64];
-  const double UINF = sc->uinfx, VINF = sc->uinfy;
-  double m = 0.0; int bad = 0;
-  const size_t n2 = (size_t)g.nx * g.ny / 2;        // Nx is a multiple of 32
-  const double2* u2 = reinterpret_cast<const double2*>(u);
-  const double2* v2 = reinterpret_cast<const double2*>(v);
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const double2 a2 = u2[i], b2 = v2[i];
-    // Helpers.cpp:160-166: max of |u+uinf|, |v+vinf|, |u|, |v|
-    m = fmax(m, fmax(fmax(fabs(a2.x + UINF), fabs(b2.x + VINF)), fmax(fabs(a2.x), fabs(b2.x))));
-    m = fmax(m, fmax(fmax(fabs(a2.y + UINF), fabs(b2.y + VINF)), fmax(fabs(a2.y), fabs(b2.y))));
-    bad |= !isfinite(a2.x) || !isfinite(b2.x) || !isfinite(a2.y) || !isfinite(b2.y);
-  }
-  m = block_max(m, red);
-  const int anyBad = __syncthreads_or(bad);
-  if (lin_tid() == 0) {
-    partials[blockIdx.x] = m;
-    if (anyBad) atomicOr(&sc->status, ST_NAN);
-  }
-  if (!last_block_done(counter, gridDim.x)) return;
-  double mm = 0.0;
-  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) mm = fmax(mm, __ldcg(&partials[i]));
-  mm = block_max(mm, red);
-  if (threadIdx.x != 0) return;
-  // Simulation::calcMaxTimestep (Simulation.cpp:254-277)
-  const double maxU = mm, h = g.h;
-  const double dtFourier = h * h / g.nu, dtCFL = maxU < 2.2e-16 ? 1 : h / maxU;
-  double maxUb = 0;                                   // SimulationData::maxRelSpeed
-  for (int k = 0; k < nsh; k++) {
-    const double su = sh[k].s.u, sv = sh[k].s.v;
-    maxUb = fmax(maxUb, sqrt(su * su + sv * sv));     // Shape::getMaxVel
-  }
-  const double dtBody = maxUb < 2.2e-16 ? 1 : h / maxUb;
-  double mn = dtCFL;
-  if (dtFourier < mn) mn = dtFourier;
-  if (dtBody < mn) mn = dtBody;
-  double dt = g.CFL * mn;
-  if (sc->step < 100) dt = sc->rampCFL[sc->step] * mn;
-  sc->dt = dt;
-  sc->maxU = maxU;
-  if (g.dlm > 0) sc->lambda = g.dlm / dt;
+  max_u_dt_cta(g, sc, sh, nsh, u, v, partials, counter, red);
 }
 
 __global__ void k_set_dt(Scalars* sc, double dt) { CUP2D_TRACE_SCOPE(TR_SETDT); sc->dt = dt; }

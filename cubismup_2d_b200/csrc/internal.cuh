@@ -64,6 +64,7 @@ struct FishState {
   double area_internal, J_internal;
   double CoM_internal[2], vCoM_internal[2];
   double theta_internal, angvel_internal, angvel_internal_prev;
+  double cosTh, sinTh;            // cos/sin(theta_internal), set where theta_internal moves
 };
 
 struct DevShape {
@@ -75,6 +76,7 @@ struct DevShape {
   double rhoTile;                 // ObstacleBlock::rho: rhoS (disk), 1 (fish)
   double rhsCorr;                 // PressureSingle.cpp:183-186 corr of this shape
   double bbox[2][2];              // disk bounding box (ShapeLibrary.h:40-43)
+  double cosO, sinO;              // cos/sin(orientation), set where the orientation moves
   int nseg;                       // fish AreaSegments this step
   // rigid part of udef removed by Shape::removeMoments (Shape.cpp:197-204):
   // consumers read udef - (Iu - Ia p_y, Iv + Ia p_x), the same expression
@@ -144,8 +146,10 @@ enum TraceId : int {
   TR_OBJBEGIN, TR_CLEAR, TR_FLAGS, TR_COMPACT, TR_RASTER_DISK, TR_CHI, TR_MOMENTS,
   TR_UDEF, TR_RHSOBST, TR_RHSCORR, TR_MOMENTA, TR_COLLIDE, TR_PENALIZE, TR_FORCES,
   TR_MIDLINE, TR_FRAME, TR_RASTER, TR_R2C, TR_COLS, TR_C2R, TR_DCT_FWD, TR_DCT_COLS,
-  TR_DCT_INV, TR_N
+  TR_DCT_INV, TR_SELECT, TR_N
 };
+// per-work-item phase stamps of the trace build: slot 2*TR_N + 8*item + phase
+constexpr int TRACE_ITEMS = 4096;
 #ifdef CUP2D_TRACE
 static __device__ unsigned long long* g_trace = nullptr;   // one copy per translation unit
 __device__ __forceinline__ unsigned long long global_timer() {
@@ -162,11 +166,32 @@ struct TraceScope {
     if (g_trace && threadIdx.x + threadIdx.y + threadIdx.z == 0) atomicMax(&g_trace[2 * id + 1], global_timer());
   }
 };
-#define CUP2D_TRACE_SCOPE(id) TraceScope cup2d_trace_scope_(id)
+#define CUP2D_TRACE_CAT2(a, b) a##b
+#define CUP2D_TRACE_CAT(a, b) CUP2D_TRACE_CAT2(a, b)
+#define CUP2D_TRACE_SCOPE(id) TraceScope CUP2D_TRACE_CAT(cup2d_trace_scope_, __LINE__)(id)
+#define CUP2D_TRACE_MARK(item, phase) \
+  do { if (g_trace && threadIdx.x + threadIdx.y + threadIdx.z == 0 && (item) < TRACE_ITEMS) \
+         g_trace[2 * TR_N + 8 * (item) + (phase)] = global_timer(); } while (0)
 static inline void trace_bind_this_unit(unsigned long long* p) { cudaMemcpyToSymbol(g_trace, &p, sizeof(p)); }
 #else
 #define CUP2D_TRACE_SCOPE(id) ((void)0)
+#define CUP2D_TRACE_MARK(item, phase) ((void)0)
 #endif
+
+// Raise a kernel's dynamic shared-memory limit to what the device allows
+// beside the kernel's static shared memory (opt-in maximum minus static).
+// Done once per kernel with the device's maximum, so a context with a small
+// grid never lowers the limit under a larger one.
+inline cudaError_t allow_max_dynamic_smem(const void* f) {
+  int dev = 0, maxOptin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&maxOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes a{};
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, f);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, maxOptin - (int)a.sharedSizeBytes);
+  return e;
+}
 
 // ---- small device helpers ------------------------------------------------
 

@@ -24,9 +24,11 @@ void launch_apply_obj_vel(Ctx& c);                   // Helpers.cpp:290-307
 void launch_objects(Ctx& c, bool midlineReady);     // PutObjectsOnGrid.cpp:186-241
 void launch_objects_begin(Ctx& c, bool midlineReady);  // lab velocity + body motion
 void launch_objects_rest(Ctx& c);                    // tiles, SDF, chi, moments
+void launch_step_begin(Ctx& c);                      // dt + tile reset + body motion, fused
 void launch_obj_vel_on_grid(Ctx& c);                 // PutObjectsOnGrid.cpp:149-184
 void launch_rhs_obstacles(Ctx& c);                   // PressureSingle.cpp:130-213
-void launch_momenta_penalize(Ctx& c);                // PressureSingle.cpp:23-108, 243-344, 362-372
+void launch_momenta(Ctx& c, const double* ui, const double* vi);  // PressureSingle.cpp:23-67, 362-372
+void launch_collide_penalize(Ctx& c);                // PressureSingle.cpp:69-108, 243-344
 void launch_forces(Ctx& c);                          // ComputeForces.cpp:16-111
 
 // poisson.cu

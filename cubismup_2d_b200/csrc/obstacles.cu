@@ -14,6 +14,7 @@
 #include <cmath>
 #include "context.hpp"
 #include "rigid_body.cuh"
+#include "step_begin.cuh"
 #include "fish.cuh"
 
 namespace cup2d {
@@ -31,52 +32,30 @@ inline AllTiles all_tiles(const Ctx& c) {
 }
 
 // ---------------------------------------------------------------------------
-// PutObjectsOnGrid.cpp:201-220: lab velocity from fixed bodies, then
-// Shape::updatePosition; a body whose centre leaves the domain raises
-// ST_DOMAIN (the reference exits).
-__global__ void k_obj_begin(GridDesc g, Scalars* sc, DevShape* sh, int nsh)
+// PutObjectsOnGrid.cpp:186-220 for the operator entry point: last step's
+// tiles are reset on the grid (all CTAs), then thread 0 of CTA 0 moves the
+// bodies.  The step graph runs the same work inside k_step_begin instead.
+__global__ void __launch_bounds__(256)
+k_obj_begin(GridDesc g, Scalars* sc, DevShape* sh, int nsh, AllTiles T, double* chi, double* sdf)
 {
   CUP2D_TRACE_SCOPE(TR_OBJBEGIN);
-  if (threadIdx.x != 0) return;
-  const double dt = sc->dt;
-  int nSum[2] = {0, 0}; double uSum[2] = {0, 0};
-  for (int k = 0; k < nsh; k++) {                       // Shape::updateLabVelocity
-    if (sh[k].cfg.bFixedx) { nSum[0]++; uSum[0] -= sh[k].s.u; }
-    if (sh[k].cfg.bFixedy) { nSum[1]++; uSum[1] -= sh[k].s.v; }
-  }
-  if (nSum[0] > 0) sc->uinfx = uSum[0] / nSum[0];
-  if (nSum[1] > 0) sc->uinfy = uSum[1] / nSum[1];
-  for (int k = 0; k < nsh; k++) {
-    DevShape& S = sh[k];
-    shape_update_position(S, dt, sc->uinfx, sc->uinfy);
-    const double p0 = S.s.center[0], p1 = S.s.center[1];
-    if (p0 < 0 || p0 > g.ext[0] || p1 < 0 || p1 > g.ext[1]) atomicOr(&sc->status, ST_DOMAIN);
-    S.ntilesPrev = S.ntiles;
-    if (S.cfg.kind == CUP2D_SHAPE_DISK) {               // FillBlocks_Cylinder bbox
-      const double safety = 2 * g.h, R = S.cfg.radius;
-      S.bbox[0][0] = p0 - R - safety; S.bbox[0][1] = p0 + R + safety;
-      S.bbox[1][0] = p1 - R - safety; S.bbox[1][1] = p1 + R + safety;
-    }
-  }
+  clear_old_tiles(g, sh, nsh, T.t, chi, sdf, blockIdx.x, gridDim.x);
+  if (threadIdx.x == 0 && blockIdx.x == 0) bodies_motion(g, sc, sh, nsh);
 }
 
-// Reset the grid cells of last step's tiles: chi = 0 (PutObjectsOnGrid.cpp:193)
-// and sdf = -1 (:194); drop the slot mapping.
-__global__ void __launch_bounds__(256)
-k_clear_old(GridDesc g, const DevShape* sh, AllTiles T, double* chi, double* sdf)
+// Fused start of a graph step: calcMaxTimestep's reduction (every CTA), the
+// reset of last step's tiles (every CTA; neither reads the other's data) and,
+// in the thread that formed dt, the body motion of PutObjectsOnGrid.
+__global__ void __launch_bounds__(512)
+k_step_begin(GridDesc g, Scalars* sc, DevShape* sh, int nsh, AllTiles T, double* chi, double* sdf,
+             const double* __restrict__ u, const double* __restrict__ v, double* partials, unsigned* counter,
+             PrefetchList pf)
 {
-  CUP2D_TRACE_SCOPE(TR_CLEAR);
-  const int k = blockIdx.y;
-  const ObstTiles& t = T.t[k];
-  for (int s = blockIdx.x; s < sh[k].ntilesPrev; s += gridDim.x) {
-    const int b = t.tiles[s];
-    const int bx = b % g.bpdx, by = b / g.bpdx;
-    for (int i = threadIdx.x; i < BS2; i += blockDim.x) {
-      const size_t c = (size_t)(by * BS + i / BS) * g.nx + bx * BS + (i % BS);
-      chi[c] = 0; sdf[c] = -1;
-    }
-    if (threadIdx.x == 0) t.slot[b] = -1;
-  }
+  CUP2D_TRACE_SCOPE(TR_MAXU);
+  __shared__ double red[64];
+  prefetch_region(pf, blockIdx.x);
+  clear_old_tiles(g, sh, nsh, T.t, chi, sdf, blockIdx.x, gridDim.x);
+  if (max_u_dt_cta(g, sc, sh, nsh, u, v, partials, counter, red)) bodies_motion(g, sc, sh, nsh);
 }
 
 __device__ __forceinline__ bool disk_touching(const GridDesc& g, const DevShape& S, int bx, int by) {
@@ -88,64 +67,20 @@ __device__ __forceinline__ bool disk_touching(const GridDesc& g, const DevShape&
   return i01 - i00 > 0 && i11 - i10 > 0;
 }
 
-// Touched-block flags (Disk: _is_touching, ShapeLibrary.h:24-36; Fish: any
-// AreaSegment intersects the block, Fish.cpp:158-173): one warp per block,
-// the lanes split the fish's segments.
-__global__ void __launch_bounds__(256)
-k_tile_flags(GridDesc g, const DevShape* sh, FishSegPtrs segs, int* flags)
-{
-  CUP2D_TRACE_SCOPE(TR_FLAGS);
-  const int k = blockIdx.y;
-  const DevShape& S = sh[k];
-  const int lane = threadIdx.x & 31;
-  const int b = blockIdx.x * 8 + (threadIdx.x >> 5);
-  if (b >= g.nblocks) return;
-  const int bx = b % g.bpdx, by = b / g.bpdx;
-  bool f = false;
-  if (S.cfg.kind == CUP2D_SHAPE_DISK) {
-    f = lane == 0 && disk_touching(g, S, bx, by);
-  } else {
-    const double start[2] = {cell_x(g, bx, 0), cell_y(g, by, 0)};
-    const double end[2] = {cell_x(g, bx, BS - 1), cell_y(g, by, BS - 1)};
-    for (int q = lane; q < S.nseg && !f; q += 32)
-      f = segment_hits_block(segs.seg[k][q], start, end, 2 * g.h);
-  }
-  const unsigned m = __ballot_sync(0xffffffffu, f);
-  if (lane == 0) flags[(size_t)k * g.nblocks + b] = m != 0;
-}
-
-// Deterministic compaction of the touched blocks in increasing block order
-// (the order of obstacleBlocks[blockID]).
-__global__ void __launch_bounds__(1024)
-k_tile_compact(GridDesc g, DevShape* sh, AllTiles T, const int* flags, Scalars* sc)
+// Obstacle tiles of the disks (_is_touching, ShapeLibrary.h:24-36): one CTA
+// per shape, searching the blocks under the disk's bounding box.
+__global__ void __launch_bounds__(512)
+k_disk_place(GridDesc g, Scalars* sc, DevShape* sh, AllTiles T)
 {
   CUP2D_TRACE_SCOPE(TR_COMPACT);
-  __shared__ int warpCount[32];
-  __shared__ int base;
   const int k = blockIdx.x;
   DevShape& S = sh[k];
-  const ObstTiles& t = T.t[k];
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  if (tid == 0) base = 0;
-  __syncthreads();
-  for (int b0 = 0; b0 < g.nblocks; b0 += 1024) {
-    const int b = b0 + tid;
-    const bool f = b < g.nblocks && flags[(size_t)k * g.nblocks + b];
-    const unsigned m = __ballot_sync(0xffffffffu, f);
-    if (lane == 0) warpCount[wid] = __popc(m);
-    __syncthreads();
-    int off = 0;
-    for (int w = 0; w < wid; w++) off += warpCount[w];
-    const int pos = base + off + __popc(m & ((1u << lane) - 1u));
-    if (f) {
-      if (pos < t.capacity) { t.tiles[pos] = b; t.slot[b] = pos; }
-      else atomicOr(&sc->status, ST_CAPACITY);
-    }
-    __syncthreads();
-    if (tid == 0) { int tot = 0; for (int w = 0; w < 32; w++) tot += warpCount[w]; base += tot; }
-    __syncthreads();
-  }
-  if (tid == 0) S.ntiles = base < t.capacity ? base : t.capacity;
+  if (S.cfg.kind != CUP2D_SHAPE_DISK) return;
+  int bx0, bx1, by0, by1;
+  block_range(S.bbox[0][0], S.bbox[0][1], g.h, 0.0, bx0, bx1);
+  block_range(S.bbox[1][0], S.bbox[1][1], g.h, 0.0, by0, by1);
+  select_tiles(g, T.t[k], bx0, bx1, by0, by1,
+               [&](int, int bx, int by) { return disk_touching(g, S, bx, by); }, &S.ntiles, &sc->status);
 }
 
 // FillBlocks_Cylinder::operator() (ShapeLibrary.cpp:21-34): dist = R - |p - c|
@@ -311,7 +246,7 @@ k_moments(GridDesc g, DevShape* sh, AllTiles T, const double* chiParts, double* 
   S.Iu = I[4] / I[2]; S.Iv = I[5] / I[2]; S.Ia = I[6] / I[3];
   S.s.M = I[2]; S.s.J = I[3];
   const double dCx = S.s.center[0] - S.s.com[0], dCy = S.s.center[1] - S.s.com[1];
-  const double co = cos(S.s.orientation), si = sin(S.s.orientation);
+  const double co = S.cosO, si = S.sinO;         // cos/sin(orientation)
   S.s.d_gm[0] = dCx * co + dCy * si;
   S.s.d_gm[1] = -dCx * si + dCy * co;
 }
@@ -419,10 +354,13 @@ k_rhs_corr(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __r
 
 // PressureSingle::integrateMomenta (PressureSingle.cpp:23-67) with the
 // EXPL_INTEGRATE_MOM weights (:20): 7 sums per tile, then the last CTA of
-// the shape runs Shape::updateVelocity.
+// the shape runs Shape::updateVelocity.  It runs beside the pressure
+// correction: the corrected velocity of each cell it reads is evaluated
+// here with k_pcorr's expression (PressureSingle.cpp:216-241) from the
+// pressure and the advected velocity (ui, vi).
 __global__ void __launch_bounds__(1024)
-k_momenta(GridDesc g, const Scalars* sc, DevShape* sh, AllTiles T,
-          const double* __restrict__ u, const double* __restrict__ v,
+k_momenta(GridDesc g, const Scalars* sc, DevShape* sh, AllTiles T, const double* __restrict__ p,
+          const double* __restrict__ ui, const double* __restrict__ vi,
           double* parts, int partStride, unsigned* counters)
 {
   CUP2D_TRACE_SCOPE(TR_MOMENTA);
@@ -441,11 +379,16 @@ k_momenta(GridDesc g, const Scalars* sc, DevShape* sh, AllTiles T,
     const size_t o = (size_t)s * BS2 + tid;
     const double chi = t.chi[o];
     if (chi > 0) {
-      const size_t c = (size_t)(by * BS + iy) * g.nx + bx * BS + ix;
+      const int gx = bx * BS + ix, gy = by * BS + iy, nx = g.nx, ny = g.ny;
+      const size_t c = (size_t)gy * nx + gx;
+      const double pFac = -0.5 * sc->dt / g.h;
+      const double pW = p[gx > 0 ? c - 1 : c], pE = p[gx < nx - 1 ? c + 1 : c];
+      const double pS = p[gy > 0 ? c - nx : c], pN = p[gy < ny - 1 ? c + nx : c];
+      const double uc = ui[c] + pFac * (pE - pW), vc = vi[c] + pFac * (pN - pS);
       const double p0 = cell_x(g, bx, ix) - Cx, p1 = cell_y(g, by, iy) - Cy;
       double ux, uy;
       udef_at(t, o, S, p0, p1, ux, uy);
-      const double ud0 = u[c] - ux, ud1 = v[c] - uy;
+      const double ud0 = uc - ux, ud1 = vc - uy;
       const double F = hsq * rho * chi;
       A[0] = F;
       A[1] = F * (p0 * p0 + p1 * p1);
@@ -682,7 +625,28 @@ void launch_objects_begin(Ctx& c, bool midlineReady) {
   if (!midlineReady)
     for (int k = 0; k < c.nshapes; k++)
       if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.stream, 0);
-  k_obj_begin<<<1, 32, 0, c.stream>>>(c.g, c.dsc, c.dshapes, c.nshapes);
+  k_obj_begin<<<tile_ctas(c, c.maxCapacity), 256, 0, c.stream>>>(
+      c.g, c.dsc, c.dshapes, c.nshapes, all_tiles(c), c.chi, c.sdf);
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_step_begin(Ctx& c) {
+  int nb = (int)((c.ncells() / 2 + 511) / 512);
+  if (nb > 2 * c.sms) nb = 2 * c.sms;
+  PrefetchList pf{};
+  auto add = [&](const void* p, size_t bytes) {
+    if (p && bytes && pf.n < MAX_PREFETCH) { pf.p[pf.n] = (const char*)p; pf.bytes[pf.n] = bytes; pf.n++; }
+  };
+  add(c.dsc, sizeof(Scalars));
+  add(c.dshapes, sizeof(DevShape) * c.nshapes);
+  for (int k = 0; k < c.nshapes; k++)
+    if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) {
+      const FishArrays& F = c.fish[k];
+      add(F.pool, sizeof(double) * (27 * (size_t)F.nm + 16));
+      add(F.ipIdx, sizeof(int2) * (size_t)F.nint);
+    }
+  k_step_begin<<<nb, 512, 0, c.stream>>>(c.g, c.dsc, c.dshapes, c.nshapes, all_tiles(c), c.chi, c.sdf,
+                                         c.u(), c.v(), c.partials, c.counters + CNT_MAXU, pf);
   CUP2D_LAUNCHED(c);
 }
 
@@ -690,20 +654,18 @@ void launch_objects_rest(Ctx& c) {
   if (c.nshapes == 0) return;
   const AllTiles T = all_tiles(c);
   const int cap = c.maxCapacity;
-  k_clear_old<<<dim3(tile_ctas(c, cap), c.nshapes), 256, 0, c.stream>>>(c.g, c.dshapes, T, c.chi, c.sdf);
-  CUP2D_LAUNCHED(c);
-  // frames and AreaSegments (Fish.cpp:95-150)
-  for (int k = 0; k < c.nshapes; k++)
-    if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_kinematics(c, k);
-  k_tile_flags<<<dim3((c.g.nblocks + 7) / 8, c.nshapes), 256, 0, c.stream>>>(c.g, c.dshapes, fish_seg_ptrs(c),
-                                                                              c.tileFlags);
-  CUP2D_LAUNCHED(c);
-  k_tile_compact<<<c.nshapes, 1024, 0, c.stream>>>(c.g, c.dshapes, T, c.tileFlags, c.dsc);
-  CUP2D_LAUNCHED(c);
   bool anyDisk = false, anyFish = false;
   for (int k = 0; k < c.nshapes; k++) {
     if (c.hshapes[k].cfg.kind == CUP2D_SHAPE_DISK) anyDisk = true; else anyFish = true;
   }
+  // frames, AreaSegments and the touched tiles (Fish.cpp:95-173)
+  for (int k = 0; k < c.nshapes; k++)
+    if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_place(c, k);
+  if (anyDisk) {
+    k_disk_place<<<c.nshapes, 512, 0, c.stream>>>(c.g, c.dsc, c.dshapes, T);
+    CUP2D_LAUNCHED(c);
+  }
+  if (c.recordPlaced) cudaEventRecord(c.evPlaced, c.stream);
   if (anyDisk) {
     k_raster_disk<<<dim3(tile_ctas(c, cap), c.nshapes), dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, T, c.sdf);
     CUP2D_LAUNCHED(c);
@@ -747,12 +709,17 @@ void launch_rhs_obstacles(Ctx& c) {
   }
 }
 
-void launch_momenta_penalize(Ctx& c) {
+void launch_momenta(Ctx& c, const double* ui, const double* vi) {
+  if (c.nshapes == 0) return;
+  k_momenta<<<dim3(tile_ctas(c, c.maxCapacity), c.nshapes), 1024, 0, c.stream>>>(
+      c.g, c.dsc, c.dshapes, all_tiles(c), c.pres, ui, vi, shape_partials(c), (int)shape_region(c),
+      c.counters + CNT_MOMENTA);
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_collide_penalize(Ctx& c) {
   if (c.nshapes == 0) return;
   const AllTiles T = all_tiles(c);
-  k_momenta<<<dim3(tile_ctas(c, c.maxCapacity), c.nshapes), 1024, 0, c.stream>>>(
-      c.g, c.dsc, c.dshapes, T, c.u(), c.v(), shape_partials(c), (int)shape_region(c), c.counters + CNT_MOMENTA);
-  CUP2D_LAUNCHED(c);
   if (c.nshapes > 1) {
     k_collide<<<1, 1024, 0, c.stream>>>(c.g, c.dsc, c.dshapes, c.nshapes, T);
     CUP2D_LAUNCHED(c);

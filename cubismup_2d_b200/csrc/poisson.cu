@@ -52,26 +52,40 @@ __device__ __forceinline__ double2 conjg(double2 a) { return make_double2(a.x, -
 
 __device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
 
-constexpr int FFT_R = 2;   // radix-4 butterflies per thread and stage
-
 // Per transform length L: padded stride SL of one sequence (one spare
 // element per 16, plus 4 so that consecutive sequences start in different
-// halves of the shared-memory banks), the twiddles the stages use
-// (w^j, j < 3L/4), the sequences per CTA B and the threads per CTA NT.
+// halves of the shared-memory banks), the staged quarter twiddle table
+// (w^j, j < L/4), the sequences per CTA B and the threads per CTA NT
+// (L/16 per sequence: every thread owns 16 elements of a pass).
 template <int L> struct Len {
   static constexpr int SL = L + L / 16 + 4;
-  static constexpr int TW = 3 * L / 4;
+  static constexpr int TW = L / 4;
   static constexpr int B = 2048 / L < 1 ? 1 : (2048 / L > 8 ? 8 : 2048 / L);
-  static constexpr int NT0 = B * L / (4 * FFT_R);
+  static constexpr int NT0 = B * L / 16;
   static constexpr int NT = NT0 < 64 ? 64 : (NT0 > 512 ? 512 : NT0);
-  static constexpr int MINB = 65536 / (NT * 64);   // caps registers at 64
+  static constexpr int MINB = 65536 / (NT * 128) < 1 ? 1 : 65536 / (NT * 128);   // <= 128 registers
 };
 
-// Twiddles w^j = exp(-2 pi i j / L), j < 3L/4, staged in shared memory.
+// Twiddles w^j = exp(-2 pi i j / L), j < L/4, staged in shared memory.
 template <int L>
 __device__ __forceinline__ void load_twiddles(double2* tws, const double2* __restrict__ tw, int twLen) {
   const int step = twLen / L;
   for (int j = threadIdx.x; j < Len<L>::TW; j += blockDim.x) tws[j] = tw[j * step];
+}
+
+// w^idx (idx < L) from the quarter table: w^(qL/4 + r) = (-i)^q w^r, the
+// rotation being exact; conjugated for the inverse transform.
+template <int L, bool INV>
+__device__ __forceinline__ double2 twiddle(const double2* tws, int idx) {
+  const int q = idx / (L / 4), r = idx & (L / 4 - 1);
+  const double2 w = tws[r];
+  double2 v;
+  if (q == 0) v = w;
+  else if (q == 1) v = make_double2(w.y, -w.x);
+  else if (q == 2) v = make_double2(-w.x, -w.y);
+  else v = make_double2(-w.y, w.x);
+  if (INV) v.y = -v.y;
+  return v;
 }
 
 // asynchronous global -> shared copies (sm_80+ cp.async), so that every
@@ -89,78 +103,137 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory");
 }
 
-// In-place Stockham autosort FFT (radix-4 stages, plus one radix-2 stage
-// first when log2 L is odd) of nseq sequences of length L stored at
-// A + q*SL (padded indexing); tws holds the L twiddles.  Every stage loads
-// its inputs to registers, synchronises, then stores, so one buffer
-// suffices.  Forward exp(-2 pi i jk/L), inverse exp(+...), unnormalised.
-// Each thread owns FFT_R radix-4 butterflies per stage: blockDim.x * FFT_R
-// must be at least nseq * L/4.
+// ---- small DFTs in registers (forward exp(-2 pi i mq/R), inverse exp(+)) --
+// multiply by -i (forward) or +i (inverse)
+template <bool INV> __device__ __forceinline__ double2 mul_mi(double2 a) {
+  return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+template <bool INV>
+__device__ __forceinline__ void dft4(double2& x0, double2& x1, double2& x2, double2& x3) {
+  const double2 t0 = cadd(x0, x2), t1 = csub(x0, x2), t2 = cadd(x1, x3), t3 = mul_mi<INV>(csub(x1, x3));
+  x0 = cadd(t0, t2); x2 = csub(t0, t2);
+  x1 = cadd(t1, t3); x3 = csub(t1, t3);
+}
+constexpr double C8 = 0.92387953251128675613;   // cos(pi/8)
+constexpr double S8 = 0.38268343236508977173;   // sin(pi/8)
+constexpr double R2 = 0.70710678118654752440;   // sqrt(2)/2
+// W16^e for e in [0, 16): the first quadrant from (1, C8, R2, S8), the rest
+// by exact quarter turns
+template <bool INV>
+__device__ __forceinline__ double2 w16(int e) {
+  const int q = e >> 2, r = e & 3;
+  const double cr = r == 0 ? 1.0 : (r == 1 ? C8 : (r == 2 ? R2 : S8));
+  const double sr = r == 0 ? 0.0 : (r == 1 ? S8 : (r == 2 ? R2 : C8));
+  double2 v = make_double2(cr, -sr);
+  for (int k = 0; k < q; k++) v = make_double2(v.y, -v.x);
+  if (INV) v.y = -v.y;
+  return v;
+}
+// DFT of R values in x[0..R); the result for output q is in x[out_reg<R>(q)]
+template <int R> __device__ __forceinline__ constexpr int out_reg(int q) {
+  return R == 16 ? 4 * (q & 3) + (q >> 2) : q;
+}
+template <int R, bool INV> __device__ __forceinline__ void dft(double2* x);
+template <> __device__ __forceinline__ void dft<2, false>(double2* x) { const double2 t = x[0]; x[0] = cadd(t, x[1]); x[1] = csub(t, x[1]); }
+template <> __device__ __forceinline__ void dft<2, true>(double2* x) { const double2 t = x[0]; x[0] = cadd(t, x[1]); x[1] = csub(t, x[1]); }
+template <> __device__ __forceinline__ void dft<4, false>(double2* x) { dft4<false>(x[0], x[1], x[2], x[3]); }
+template <> __device__ __forceinline__ void dft<4, true>(double2* x) { dft4<true>(x[0], x[1], x[2], x[3]); }
+template <bool INV> __device__ __forceinline__ void dft8(double2* x) {
+  // m = m1 + 2 m2: DFT4 over m2, twiddle W8^(m1 q2), DFT2 over m1
+  dft4<INV>(x[0], x[2], x[4], x[6]);
+  dft4<INV>(x[1], x[3], x[5], x[7]);
+  double2 y[8];
+#pragma unroll
+  for (int q2 = 0; q2 < 4; q2++) {
+    const double2 z0 = x[2 * q2], z1 = cmul(x[2 * q2 + 1], w16<INV>(2 * q2));
+    y[q2] = cadd(z0, z1); y[q2 + 4] = csub(z0, z1);
+  }
+#pragma unroll
+  for (int q = 0; q < 8; q++) x[q] = y[q];
+}
+template <> __device__ __forceinline__ void dft<8, false>(double2* x) { dft8<false>(x); }
+template <> __device__ __forceinline__ void dft<8, true>(double2* x) { dft8<true>(x); }
+template <bool INV> __device__ __forceinline__ void dft16(double2* x) {
+  // m = m1 + 4 m2: DFT4 over m2 (result z[m1][q2] in x[m1 + 4 q2]),
+  // twiddle W16^(m1 q2), DFT4 over m1 (output q2 + 4 q1 in x[4 q2 + q1])
+#pragma unroll
+  for (int m1 = 0; m1 < 4; m1++) dft4<INV>(x[m1], x[m1 + 4], x[m1 + 8], x[m1 + 12]);
+#pragma unroll
+  for (int m1 = 1; m1 < 4; m1++)
+#pragma unroll
+    for (int q2 = 1; q2 < 4; q2++) x[m1 + 4 * q2] = cmul(x[m1 + 4 * q2], w16<INV>(m1 * q2));
+#pragma unroll
+  for (int q2 = 0; q2 < 4; q2++) dft4<INV>(x[4 * q2], x[4 * q2 + 1], x[4 * q2 + 2], x[4 * q2 + 3]);
+}
+template <> __device__ __forceinline__ void dft<16, false>(double2* x) { dft16<false>(x); }
+template <> __device__ __forceinline__ void dft<16, true>(double2* x) { dft16<true>(x); }
 
-template <int L, bool INV>
+// One in-place Stockham pass of radix R over sub-transforms of size NS on
+// nseq sequences A + q*SL: butterfly j (k = j mod NS) reads x_m =
+// a[j + m L/R], scales by w^(m k L/(R NS)), takes the DFT_R and writes
+// output q at (j - k) R + k + q NS.  Thread t of a sequence owns the 16/R
+// butterflies t + u L/16.  Loads go to registers before the barrier,
+// stores after it, so one buffer suffices.
+template <int L, int R, int NS, bool INV, bool HIN, bool HOUT>
+__device__ __forceinline__ void fft_pass(double2* A, int nseq, const double2* tws)
+{
+  constexpr int SL = Len<L>::SL, T = L / 16, NB = 16 / R, Q = L / R;
+  // first pass of an input whose upper half is zero: inputs m >= R/2 sit at
+  // indices >= L/2 (then NB == 1); last pass of which only the lower half of
+  // the output is kept: outputs q >= R/2 land at indices >= L/2
+  constexpr bool ZIN = HIN && NS == 1, HALFO = HOUT && NS * R == L;
+  const int tid = threadIdx.x;
+  const bool act = tid < nseq * T;
+  const int sq = act ? tid / T : 0, j = tid - sq * T;
+  double2* a = A + sq * SL;
+  double2 x[16];
+  if (act) {
+#pragma unroll
+    for (int u = 0; u < NB; u++)
+#pragma unroll
+      for (int m = 0; m < R; m++)
+        x[u * R + m] = (ZIN && m >= R / 2) ? make_double2(0, 0) : a[pad(j + u * T + m * Q)];
+  }
+  __syncthreads();
+  if (act) {
+#pragma unroll
+    for (int u = 0; u < NB; u++) {
+      double2* xb = x + u * R;
+      const int jb = j + u * T, k = jb & (NS - 1);
+      if (NS > 1 && k) {
+        const int base = k * (L / (R * NS));
+#pragma unroll
+        for (int m = 1; m < R; m++) xb[m] = cmul(xb[m], twiddle<L, INV>(tws, m * base));
+      }
+      dft<R, INV>(xb);
+      const int o = (jb - k) * R + k;
+#pragma unroll
+      for (int q = 0; q < (HALFO ? R / 2 : R); q++) a[pad(o + q * NS)] = xb[out_reg<R>(q)];
+    }
+  }
+  __syncthreads();
+}
+
+template <int L, int NS, bool INV, bool HIN, bool HOUT>
+__device__ __forceinline__ void fft_passes(double2* A, int nseq, const double2* tws) {
+  if constexpr (NS * 16 <= L) {
+    fft_pass<L, 16, NS, INV, HIN, HOUT>(A, nseq, tws);
+    fft_passes<L, NS * 16, INV, HIN, HOUT>(A, nseq, tws);
+  } else if constexpr (NS < L) {
+    fft_pass<L, L / NS, NS, INV, HIN, HOUT>(A, nseq, tws);
+  }
+}
+
+// In-place Stockham autosort FFT of nseq sequences of length L (A + q*SL,
+// padded indexing; a power of two >= 64): radix-16 passes and one radix
+// 2/4/8 pass for the remaining factor.  Forward exp(-2 pi i jk/L), inverse
+// exp(+...), unnormalised.  Needs blockDim.x >= nseq * L/16.  HIN: the
+// upper half of the input is zero and never read; HOUT: only the lower half
+// of the output is written.
+template <int L, bool INV, bool HIN = false, bool HOUT = false>
 __device__ void fft_inplace(double2* A, int nseq, const double2* tws)
 {
-  constexpr int SL = Len<L>::SL, Q = L / 4, H = L / 2, R = FFT_R;
-  int qq[R], jj[R];
-  bool act[R];
-#pragma unroll
-  for (int u = 0; u < R; u++) {
-    const int t = threadIdx.x + u * blockDim.x;
-    act[u] = t < nseq * Q;
-    qq[u] = act[u] ? t / Q : 0;
-    jj[u] = t - qq[u] * Q;
-  }
-  int Ns = 1;
-  if ((__builtin_ctz(L) & 1) == 1) {
-    double2 x[R][4];
-#pragma unroll
-    for (int u = 0; u < R; u++) if (act[u]) {
-      const double2* a = A + qq[u] * SL; const int j = jj[u];
-      x[u][0] = a[pad(j)]; x[u][1] = a[pad(j + H)]; x[u][2] = a[pad(j + Q)]; x[u][3] = a[pad(j + Q + H)];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < R; u++) if (act[u]) {
-      double2* a = A + qq[u] * SL; const int j = jj[u];
-      a[pad(2 * j)] = cadd(x[u][0], x[u][1]); a[pad(2 * j + 1)] = csub(x[u][0], x[u][1]);
-      a[pad(2 * (j + Q))] = cadd(x[u][2], x[u][3]); a[pad(2 * (j + Q) + 1)] = csub(x[u][2], x[u][3]);
-    }
-    __syncthreads();
-    Ns = 2;
-  }
-  for (; Ns < L; Ns <<= 2) {
-    double2 x[R][4];
-#pragma unroll
-    for (int u = 0; u < R; u++) if (act[u]) {
-      const double2* a = A + qq[u] * SL; const int j = jj[u];
-      x[u][0] = a[pad(j)]; x[u][1] = a[pad(j + Q)]; x[u][2] = a[pad(j + 2 * Q)]; x[u][3] = a[pad(j + 3 * Q)];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < R; u++) if (act[u]) {
-      double2* a = A + qq[u] * SL; const int j = jj[u];
-      const int k = j & (Ns - 1);
-      double2 x0 = x[u][0], x1 = x[u][1], x2 = x[u][2], x3 = x[u][3];
-      if (k) {
-        const int st = L / (4 * Ns);
-        double2 w1 = tws[k * st], w2 = tws[2 * k * st], w3 = tws[3 * k * st];
-        if (INV) { w1.y = -w1.y; w2.y = -w2.y; w3.y = -w3.y; }
-        x1 = cmul(w1, x1); x2 = cmul(w2, x2); x3 = cmul(w3, x3);
-      }
-      const double2 t0 = cadd(x0, x2), t1 = csub(x0, x2), t2 = cadd(x1, x3), t3 = csub(x1, x3);
-      const int o = ((j - k) << 2) + k;
-      a[pad(o)] = cadd(t0, t2);
-      a[pad(o + 2 * Ns)] = csub(t0, t2);
-      if (!INV) {
-        a[pad(o + Ns)] = make_double2(t1.x + t3.y, t1.y - t3.x);       // t1 - i t3
-        a[pad(o + 3 * Ns)] = make_double2(t1.x - t3.y, t1.y + t3.x);   // t1 + i t3
-      } else {
-        a[pad(o + Ns)] = make_double2(t1.x - t3.y, t1.y + t3.x);
-        a[pad(o + 3 * Ns)] = make_double2(t1.x + t3.y, t1.y - t3.x);
-      }
-    }
-    __syncthreads();
-  }
+  fft_passes<L, 1, INV, HIN, HOUT>(A, nseq, tws);
 }
 
 struct FadeArgs {
@@ -184,13 +257,13 @@ __device__ __forceinline__ double fade_cell(const GridDesc& g, int gx, int gy, d
   const double f2 = fadeArg * fadeArg;
   const double fadeRHS = b * f2;
   const double fadeCorrection = corr * (corr > 0 ? fmax(fadeRHS, 0.0) : -fmin(fadeRHS, 0.0));
-  return b * (1 - f2) + fadeCorrection;
+  return __dadd_rn(__dmul_rn(b, 1 - f2), fadeCorrection);   // never contracted into an FMA
 }
 
 // inMode 0: rows of `in`; 1: the free-space Green's function on the padded
 // grid (FFTW_freespace.cpp:108-119) computed on the fly.  Each row of 2L
 // reals is the complex sequence (x[2n], x[2n+1]) of length L.
-template <int L>
+template <int L, bool HIN>
 __global__ void __launch_bounds__(Len<L>::NT, Len<L>::MINB)
 k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
            double2* __restrict__ out, int outStride,
@@ -210,7 +283,7 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
       double2* dst = A + r * SL + pad(n);
       if (2 * n + 1 < ncolsIn) cp_async16(dst, in + (size_t)row * inStride + 2 * n);
       else if (2 * n < ncolsIn) *dst = make_double2(in[(size_t)row * inStride + 2 * n], 0);
-      else *dst = make_double2(0, 0);
+      else if (!HIN) *dst = make_double2(0, 0);       // with HIN the zero half is never read
     }
     cp_async_commit();
   } else {
@@ -265,7 +338,7 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
     }
     __syncthreads();
   }
-  fft_inplace<L, false>(A, nb, tws);
+  fft_inplace<L, false, HIN>(A, nb, tws);
   // even/odd split: X[k] = Fe[k] + W^k Fo[k], W = exp(-i pi / L), k in [0, L]
   const int twStep = twLen / (2 * L);
   for (int idx = threadIdx.x; idx < nb * (L + 1); idx += NT) {
@@ -284,7 +357,7 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
 // mode 1: forward; write Re * norm for ky <= L/2 into ghat (kernel set-up)
 // mode 2: forward, periodic multiplier -1/|k|^2 / (MX MY), inverse
 // Rows r >= nrowsIn of the input are zero and never read.
-template <int L>
+template <int L, bool FS>
 __global__ void __launch_bounds__(Len<L>::NT, Len<L>::MINB)
 k_cols(double2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrowsOut,
        const double* __restrict__ ghatIn, double* __restrict__ ghatOut, int mode,
@@ -311,14 +384,15 @@ k_cols(double2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrows
     }
   }
   cp_async_commit();
-  for (int idx = threadIdx.x; idx < CB * (L - nrowsIn); idx += NT) {
-    const int r = nrowsIn + idx / CB, j = idx & (CB - 1);
-    A[j * SL + pad(r)] = make_double2(0, 0);
-  }
+  if (!FS)                                            // the free-space solve never reads them
+    for (int idx = threadIdx.x; idx < CB * (L - nrowsIn); idx += NT) {
+      const int r = nrowsIn + idx / CB, j = idx & (CB - 1);
+      A[j * SL + pad(r)] = make_double2(0, 0);
+    }
   load_twiddles<L>(tws, tw, twLen);
   cp_async_wait<1>();          // the columns (the kernel rows may still be in flight)
   __syncthreads();
-  fft_inplace<L, false>(A, nb, tws);
+  fft_inplace<L, false, FS>(A, nb, tws);
   if (mode == 1) {
     for (int idx = threadIdx.x; idx < CB * nrowsOut; idx += NT) {
       const int r = idx / CB, j = idx & (CB - 1);
@@ -349,7 +423,7 @@ k_cols(double2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrows
     A[j * SL + pad(r)] = make_double2(z.x * f, z.y * f);
   }
   __syncthreads();
-  fft_inplace<L, true>(A, nb, tws);
+  fft_inplace<L, true, false, FS>(A, nb, tws);
   for (int idx = threadIdx.x; idx < CB * nrowsOut; idx += NT) {
     const int r = idx / CB, j = idx & (CB - 1);
     if (j < nb) data[(size_t)r * stride + c0 + j] = A[j * SL + pad(r)];
@@ -357,7 +431,7 @@ k_cols(double2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrows
 }
 
 // inverse real FFT of length 2L from X[0..L]; writes the first ncolsOut values
-template <int L>
+template <int L, bool HOUT>
 __global__ void __launch_bounds__(Len<L>::NT, Len<L>::MINB)
 k_rows_c2r(const double2* __restrict__ in, int inStride, int nrows, double* __restrict__ out,
            int outStride, int ncolsOut, const double2* __restrict__ tw, int twLen)
@@ -405,7 +479,7 @@ k_rows_c2r(const double2* __restrict__ in, int inStride, int nrows, double* __re
     a[pad(kk[1])] = res[1];
   }
   __syncthreads();
-  fft_inplace<L, true>(A, nb, tws);
+  fft_inplace<L, true, false, HOUT>(A, nb, tws);
   const int half = (ncolsOut + 1) / 2;
   for (int idx = threadIdx.x; idx < nb * half; idx += NT) {
     const int r = idx / half, n = idx - r * half;
@@ -539,7 +613,7 @@ k_dct_cols(double* D, int Nx, int Ny, int cb, const float* __restrict__ cosX, co
   }
   for (int q = threadIdx.x; q < np; q += blockDim.x) W[q * SL + pad(n)] = make_double2(0, 0);
   __syncthreads();
-  fft_inplace<L, true>(W, np, tws);
+  fft_inplace<L, true, false, true>(W, np, tws);          // outputs m < n = L/2
   double2* Y = W;
   for (int idx = threadIdx.x; idx < np * n; idx += blockDim.x) {
     const int m = idx / np, q = idx - m * np;
@@ -577,7 +651,7 @@ k_dct_rows_inv(const double* __restrict__ D, int Nx, int nrows, double* __restri
     A[r * SL + pad(k)] = make_double2(s.x - t.y, s.y + t.x);
   }
   __syncthreads();
-  fft_inplace<L, true>(A, nb, tws);
+  fft_inplace<L, true, false, true>(A, nb, tws);          // outputs m < L/2
   double2* z = A;
   for (int idx = threadIdx.x; idx < nb * (L / 2); idx += blockDim.x) {
     const int r = idx / (L / 2), m = idx - r * (L / 2);
@@ -587,14 +661,8 @@ k_dct_rows_inv(const double* __restrict__ D, int Nx, int nrows, double* __restri
 
 inline bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
-// The opt-in limit is raised to the device maximum once per kernel, so a
-// context with a smaller grid never lowers it under a larger one.
-void set_smem(const void* f) {
-  int dev = 0, maxOptin = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&maxOptin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, maxOptin);
-}
+bool g_smemOk = true;
+void set_smem(const void* f) { if (allow_max_dynamic_smem(f) != cudaSuccess) g_smemOk = false; }
 
 // B padded sequences, the staged twiddles, and extraReals doubles
 template <int L> inline size_t smem_for(size_t extraReals = 0) {
@@ -604,18 +672,25 @@ template <int L> inline size_t smem_for(size_t extraReals = 0) {
 #define CUP2D_FFT_LENGTHS(X) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
 
 void set_all_smem() {
-#define X(L) set_smem((const void*)k_rows_r2c<L>); set_smem((const void*)k_rows_c2r<L>); \
-             set_smem((const void*)k_cols<L>); set_smem((const void*)k_dct_rows_fwd<L>); \
+#define X(L) set_smem((const void*)k_rows_r2c<L, false>); set_smem((const void*)k_rows_r2c<L, true>); \
+             set_smem((const void*)k_rows_c2r<L, false>); set_smem((const void*)k_rows_c2r<L, true>); \
+             set_smem((const void*)k_cols<L, false>); set_smem((const void*)k_cols<L, true>); \
+             set_smem((const void*)k_dct_rows_fwd<L>); \
              set_smem((const void*)k_dct_cols<L>); set_smem((const void*)k_dct_rows_inv<L>);
   CUP2D_FFT_LENGTHS(X)
 #undef X
 }
 
 bool rows_r2c(int L, cudaStream_t st, const double* in, int inStride, int nrows, int ncolsIn, int inMode,
-              double2* out, int outStride, const double2* tw, int twLen, FadeArgs fa, double h, int Nx, int Ny) {
+              double2* out, int outStride, const double2* tw, int twLen, FadeArgs fa, double h, int Nx, int Ny,
+              bool halfIn) {
   switch (L) {
-#define X(LL) case LL: k_rows_r2c<LL><<<(nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st>>>( \
-                  in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, Nx, Ny); return true;
+#define X(LL) case LL: \
+    if (halfIn) k_rows_r2c<LL, true><<<(nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st>>>( \
+        in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, Nx, Ny); \
+    else k_rows_r2c<LL, false><<<(nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st>>>( \
+        in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, Nx, Ny); \
+    return true;
     CUP2D_FFT_LENGTHS(X)
 #undef X
   }
@@ -625,9 +700,14 @@ bool rows_r2c(int L, cudaStream_t st, const double* in, int inStride, int nrows,
 bool cols(int L, cudaStream_t st, double2* data, int stride, int ncols, int nrowsIn, int nrowsOut,
           double* ghat, int mode, const double2* tw, int twLen, double norm, int MXp, int MYp) {
   switch (L) {
-#define X(LL) case LL: k_cols<LL><<<(ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, \
-                  smem_for<LL>((size_t)(LL / 2 + 1) * Len<LL>::B), st>>>(data, stride, ncols, nrowsIn, \
-                  nrowsOut, ghat, ghat, mode, tw, twLen, norm, MXp, MYp); return true;
+#define X(LL) case LL: \
+    if (mode == 0) k_cols<LL, true><<<(ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, \
+        smem_for<LL>((size_t)(LL / 2 + 1) * Len<LL>::B), st>>>(data, stride, ncols, nrowsIn, \
+        nrowsOut, ghat, ghat, mode, tw, twLen, norm, MXp, MYp); \
+    else k_cols<LL, false><<<(ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, \
+        smem_for<LL>((size_t)(LL / 2 + 1) * Len<LL>::B), st>>>(data, stride, ncols, nrowsIn, \
+        nrowsOut, ghat, ghat, mode, tw, twLen, norm, MXp, MYp); \
+    return true;
     CUP2D_FFT_LENGTHS(X)
 #undef X
   }
@@ -635,10 +715,14 @@ bool cols(int L, cudaStream_t st, double2* data, int stride, int ncols, int nrow
 }
 
 bool rows_c2r(int L, cudaStream_t st, const double2* in, int inStride, int nrows, double* out, int outStride,
-              int ncolsOut, const double2* tw, int twLen) {
+              int ncolsOut, const double2* tw, int twLen, bool halfOut) {
   switch (L) {
-#define X(LL) case LL: k_rows_c2r<LL><<<(nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st>>>( \
-                  in, inStride, nrows, out, outStride, ncolsOut, tw, twLen); return true;
+#define X(LL) case LL: \
+    if (halfOut) k_rows_c2r<LL, true><<<(nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st>>>( \
+        in, inStride, nrows, out, outStride, ncolsOut, tw, twLen); \
+    else k_rows_c2r<LL, false><<<(nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st>>>( \
+        in, inStride, nrows, out, outStride, ncolsOut, tw, twLen); \
+    return true;
     CUP2D_FFT_LENGTHS(X)
 #undef X
   }
@@ -709,6 +793,7 @@ Poisson* poisson_create(Ctx& c) {
   const size_t specRows = (size_t)P->Lcol;
   if (cudaMalloc(&P->spec, sizeof(double2) * specRows * P->nkx) != cudaSuccess) { poisson_destroy(P); return nullptr; }
   set_all_smem();
+  if (!g_smemOk) { poisson_destroy(P); return nullptr; }
   if (P->type == CUP2D_POISSON_COSINE) {
     // FFTW_dirichlet constructor (FFTW_dirichlet.h:74-76): cosines stored as float
     std::vector<float> cx(Nx), cy(Ny);
@@ -724,7 +809,7 @@ Poisson* poisson_create(Ctx& c) {
     if (cudaMalloc(&P->ghat, sizeof(double) * (P->Lcol / 2 + 1) * P->nkx) != cudaSuccess) { poisson_destroy(P); return nullptr; }
     FadeArgs fa{}; fa.enabled = 0;
     const int MYr = 2 * Ny;
-    rows_r2c(P->Lrow, c.stream, nullptr, 0, MYr, 2 * Nx, 1, P->spec, P->nkx, P->tw, P->twLen, fa, c.g.h, Nx, Ny);
+    rows_r2c(P->Lrow, c.stream, nullptr, 0, MYr, 2 * Nx, 1, P->spec, P->nkx, P->tw, P->twLen, fa, c.g.h, Nx, Ny, false);
     CUP2D_LAUNCHED(c);
     const double norm = 1.0 / ((double)(2 * Nx) * (double)(2 * Ny));
     cols(P->Lcol, c.stream, P->spec, P->nkx, P->nkx, MYr, P->Lcol / 2 + 1, P->ghat, 1, P->tw, P->twLen, norm, 0, 0);
@@ -750,7 +835,9 @@ void poisson_rows_fwd(Ctx& c) {
     CUP2D_LAUNCHED(c);
     return;
   }
-  rows_r2c(P->Lrow, c.stream, c.rhs, Nx, Ny, Nx, 0, P->spec, P->nkx, P->tw, P->twLen, fa, c.g.h, Nx, Ny);
+  // free space: the row's zero padding is the upper half of the length-Lrow sequence
+  rows_r2c(P->Lrow, c.stream, c.rhs, Nx, Ny, Nx, 0, P->spec, P->nkx, P->tw, P->twLen, fa, c.g.h, Nx, Ny,
+           P->type == CUP2D_POISSON_FREESPACE);
   CUP2D_LAUNCHED(c);
 }
 
@@ -776,7 +863,8 @@ void poisson_rows_inv(Ctx& c) {
     CUP2D_LAUNCHED(c);
     return;
   }
-  rows_c2r(P->Lrow, c.stream, P->spec, P->nkx, Ny, c.pres, Nx, Nx, P->tw, P->twLen);
+  rows_c2r(P->Lrow, c.stream, P->spec, P->nkx, Ny, c.pres, Nx, Nx, P->tw, P->twLen,
+           P->type == CUP2D_POISSON_FREESPACE);                 // free space keeps the first half
   CUP2D_LAUNCHED(c);
 }
 

@@ -78,10 +78,14 @@ __device__ __forceinline__ void shape_update_position(DevShape& S, const double 
   s.orientation = s.orientation > M_PI ? s.orientation - 2 * M_PI : s.orientation;
   s.orientation = s.orientation < -M_PI ? s.orientation + 2 * M_PI : s.orientation;
   const double cosang = cos(s.orientation), sinang = sin(s.orientation);
+  S.cosO = cosang; S.sinO = sinang;             // reused by the kernels of this step
   s.center[0] = s.com[0] + cosang * s.d_gm[0] - sinang * s.d_gm[1];
   s.center[1] = s.com[1] + sinang * s.d_gm[0] + cosang * s.d_gm[1];
-  if (S.cfg.kind != CUP2D_SHAPE_DISK)           // Fish::updatePosition (Fish.cpp:180-185)
+  if (S.cfg.kind != CUP2D_SHAPE_DISK) {         // Fish::updatePosition (Fish.cpp:180-185)
     S.f.theta_internal -= dt * S.f.angvel_internal;
+    S.f.cosTh = cos(S.f.theta_internal);
+    S.f.sinTh = sin(S.f.theta_internal);
+  }
 }
 
 } // namespace cup2d

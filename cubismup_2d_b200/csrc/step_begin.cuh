@@ -1,0 +1,127 @@
+// Start of a step, shared by the stand-alone kernels (calcMaxTimestep,
+// PutObjectsOnGrid's motion update) and the fused step-begin kernel of the
+// step graph.
+#pragma once
+#include "internal.cuh"
+#include "rigid_body.cuh"
+
+namespace cup2d {
+
+// Small device regions the start of a step reads with dependent loads (the
+// scalars, the shapes, the fish midline arrays): the step-begin kernel
+// prefetches them into L2 first, one region per CTA.
+constexpr int MAX_PREFETCH = 8;
+struct PrefetchList {
+  const char* p[MAX_PREFETCH];
+  size_t bytes[MAX_PREFETCH];
+  int n;
+};
+
+__device__ __forceinline__ void prefetch_region(const PrefetchList& pf, int r) {
+  if (r >= pf.n) return;
+  const char* base = pf.p[r];
+  for (size_t o = (size_t)lin_tid() * 128; o < pf.bytes[r]; o += (size_t)lin_nthreads() * 128)
+    asm volatile("prefetch.global.L2 [%0];" :: "l"(base + o));
+}
+
+// Helpers.cpp:136-176 (findMaxU) + Simulation::calcMaxTimestep
+// (Simulation.cpp:254-277) over a 1D grid: per-CTA maxima, the last CTA
+// forms dt.  Returns true in thread 0 of the CTA that set sc->dt.
+// red must hold 64 doubles.
+__device__ __forceinline__ bool max_u_dt_cta(const GridDesc& g, Scalars* sc, const DevShape* sh, int nsh,
+                                             const double* __restrict__ u, const double* __restrict__ v,
+                                             double* partials, unsigned* counter, double* red)
+{
+  const double UINF = sc->uinfx, VINF = sc->uinfy;
+  double m = 0.0; int bad = 0;
+  const size_t n2 = (size_t)g.nx * g.ny / 2;        // Nx is a multiple of 32
+  const double2* u2 = reinterpret_cast<const double2*>(u);
+  const double2* v2 = reinterpret_cast<const double2*>(v);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double2 a2 = u2[i], b2 = v2[i];
+    // Helpers.cpp:160-166: max of |u+uinf|, |v+vinf|, |u|, |v|
+    m = fmax(m, fmax(fmax(fabs(a2.x + UINF), fabs(b2.x + VINF)), fmax(fabs(a2.x), fabs(b2.x))));
+    m = fmax(m, fmax(fmax(fabs(a2.y + UINF), fabs(b2.y + VINF)), fmax(fabs(a2.y), fabs(b2.y))));
+    bad |= !isfinite(a2.x) || !isfinite(b2.x) || !isfinite(a2.y) || !isfinite(b2.y);
+  }
+  m = block_max(m, red);
+  const int anyBad = __syncthreads_or(bad);
+  if (lin_tid() == 0) {
+    partials[blockIdx.x] = m;
+    if (anyBad) atomicOr(&sc->status, ST_NAN);
+  }
+  if (!last_block_done(counter, gridDim.x)) return false;
+  double mm = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) mm = fmax(mm, __ldcg(&partials[i]));
+  mm = block_max(mm, red);
+  if (threadIdx.x != 0) return false;
+  const double maxU = mm, h = g.h;
+  const double dtFourier = h * h / g.nu, dtCFL = maxU < 2.2e-16 ? 1 : h / maxU;
+  double maxUb = 0;                                   // SimulationData::maxRelSpeed
+  for (int k = 0; k < nsh; k++) {
+    const double su = sh[k].s.u, sv = sh[k].s.v;
+    maxUb = fmax(maxUb, sqrt(su * su + sv * sv));     // Shape::getMaxVel
+  }
+  const double dtBody = maxUb < 2.2e-16 ? 1 : h / maxUb;
+  double mn = dtCFL;
+  if (dtFourier < mn) mn = dtFourier;
+  if (dtBody < mn) mn = dtBody;
+  double dt = g.CFL * mn;
+  if (sc->step < 100) dt = sc->rampCFL[sc->step] * mn;
+  sc->dt = dt;
+  sc->maxU = maxU;
+  if (g.dlm > 0) sc->lambda = g.dlm / dt;
+  return true;
+}
+
+// PutObjectsOnGrid.cpp:201-220 (one thread): lab velocity from fixed
+// bodies, then Shape::updatePosition; a body whose centre leaves the domain
+// raises ST_DOMAIN (the reference exits).
+__device__ __forceinline__ void bodies_motion(const GridDesc& g, Scalars* sc, DevShape* sh, int nsh)
+{
+  const double dt = sc->dt;
+  int nSum[2] = {0, 0}; double uSum[2] = {0, 0};
+  for (int k = 0; k < nsh; k++) {                       // Shape::updateLabVelocity
+    if (sh[k].cfg.bFixedx) { nSum[0]++; uSum[0] -= sh[k].s.u; }
+    if (sh[k].cfg.bFixedy) { nSum[1]++; uSum[1] -= sh[k].s.v; }
+  }
+  if (nSum[0] > 0) sc->uinfx = uSum[0] / nSum[0];
+  if (nSum[1] > 0) sc->uinfy = uSum[1] / nSum[1];
+  for (int k = 0; k < nsh; k++) {
+    DevShape& S = sh[k];
+    shape_update_position(S, dt, sc->uinfx, sc->uinfy);
+    const double p0 = S.s.center[0], p1 = S.s.center[1];
+    if (p0 < 0 || p0 > g.ext[0] || p1 < 0 || p1 > g.ext[1]) atomicOr(&sc->status, ST_DOMAIN);
+    S.ntilesPrev = S.ntiles;
+    if (S.cfg.kind == CUP2D_SHAPE_DISK) {               // FillBlocks_Cylinder bbox
+      const double safety = 2 * g.h, R = S.cfg.radius;
+      S.bbox[0][0] = p0 - R - safety; S.bbox[0][1] = p0 + R + safety;
+      S.bbox[1][0] = p1 - R - safety; S.bbox[1][1] = p1 + R + safety;
+    }
+  }
+}
+
+// Reset the grid cells of last step's tiles of every shape, chi = 0
+// (PutObjectsOnGrid.cpp:193) and sdf = -1 (:194), and drop their slot
+// mapping; CTA `cta` of `ncta` takes tiles cta, cta + ncta, ...
+__device__ __forceinline__ void clear_old_tiles(const GridDesc& g, const DevShape* sh, int nsh,
+                                                const ObstTiles* T, double* chi, double* sdf,
+                                                int cta, int ncta)
+{
+  const int tid = lin_tid(), nt = lin_nthreads();
+  for (int k = 0; k < nsh; k++) {
+    const ObstTiles& t = T[k];
+    for (int s = cta; s < sh[k].ntiles; s += ncta) {
+      const int b = t.tiles[s];
+      const int bx = b % g.bpdx, by = b / g.bpdx;
+      for (int i = tid; i < BS2; i += nt) {
+        const size_t c = (size_t)(by * BS + i / BS) * g.nx + bx * BS + (i % BS);
+        chi[c] = 0; sdf[c] = -1;
+      }
+      if (tid == 0) t.slot[b] = -1;
+    }
+  }
+}
+
+} // namespace cup2d
