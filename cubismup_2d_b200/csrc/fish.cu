@@ -55,6 +55,7 @@ __device__ __forceinline__ void cubic_interp(double x0, double x1, double x, dou
 __global__ void __launch_bounds__(512)
 k_fish_midline(const Scalars* sc, const DevShape* sh, int k, FishArrays F, int mode)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_MIDLINE);
   extern __shared__ double smem[];
   __shared__ double red[32 * 5];
@@ -244,6 +245,7 @@ k_fish_midline(const Scalars* sc, const DevShape* sh, int k, FishArrays F, int m
 __global__ void __launch_bounds__(1024)
 k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTiles t)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_FRAME);
   CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 0);
   extern __shared__ double fsm[];                      // the frame midline, staged
@@ -523,6 +525,7 @@ inline size_t raster_smem(int Nm) {
 __global__ void __launch_bounds__(RT)
 k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, double* sdfg)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_RASTER);
   __shared__ int segFst[MAX_SEG_PER_TILE];       // first s index of the segment's points (>= 1)
   __shared__ int segIntBase[MAX_SEG_PER_TILE];   // its first interior point
@@ -813,12 +816,12 @@ cudaError_t fish_setup_kernels() {
 }
 
 void launch_fish_midline(Ctx& c, int k, cudaStream_t stream, int mode) {
-  k_fish_midline<<<1, 512, midline_smem(c.fish[k].nm), stream>>>(c.dsc, c.dshapes, k, c.fish[k], mode);
+  launch_k(k_fish_midline, 1, 512, midline_smem(c.fish[k].nm), stream, c.dsc, c.dshapes, k, c.fish[k], mode);
   CUP2D_LAUNCHED(c);
 }
 
 void launch_fish_place(Ctx& c, int k) {
-  k_fish_frame<<<1, 1024, frame_smem(c.fish[k].nm, c.fish[k].nseg), c.stream>>>(c.g, c.dsc, c.dshapes, k, c.fish[k], c.tiles[k]);
+  launch_k(k_fish_frame, 1, 1024, frame_smem(c.fish[k].nm, c.fish[k].nseg), c.stream, c.g, c.dsc, c.dshapes, k, c.fish[k], c.tiles[k]);
   CUP2D_LAUNCHED(c);
 }
 
@@ -826,7 +829,7 @@ void launch_fish_raster(Ctx& c, int k) {
   // two resident CTAs per SM at most (registers); each loops over
   // (tile, sub-tile) items
   const int items = c.tiles[k].capacity * NSUB, grid = items < 2 * c.sms ? items : 2 * c.sms;
-  k_fish_raster<<<grid, RT, raster_smem(c.fish[k].nm), c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
+  launch_k(k_fish_raster, grid, RT, raster_smem(c.fish[k].nm), c.stream, c.g, c.dshapes, k, c.tiles[k],
                                                                 c.fish[k], c.sdf);
   CUP2D_LAUNCHED(c);
 }

@@ -25,14 +25,15 @@ k_max_u_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh,
            const double* __restrict__ u, const double* __restrict__ v,
            double* partials, unsigned* counter)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_MAXU);
   __shared__ double red[64];
   max_u_dt_cta(g, sc, sh, nsh, u, v, partials, counter, red);
 }
 
-__global__ void k_set_dt(Scalars* sc, double dt) { CUP2D_TRACE_SCOPE(TR_SETDT); sc->dt = dt; }
+__global__ void k_set_dt(Scalars* sc, double dt) { pdl_begin(); CUP2D_TRACE_SCOPE(TR_SETDT); sc->dt = dt; }
 
-__global__ void k_end_step(Scalars* sc) { CUP2D_TRACE_SCOPE(TR_ENDSTEP);
+__global__ void k_end_step(Scalars* sc) { pdl_begin(); CUP2D_TRACE_SCOPE(TR_ENDSTEP);
   sc->time += sc->dt;
   sc->step += 1;
 }
@@ -45,6 +46,7 @@ k_advdiff(GridDesc g, const Scalars* sc,
           double* __restrict__ un, double* __restrict__ vn,
           double* partials, unsigned* counter, Scalars* scw)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_ADVDIFF);
   __shared__ double red[32];
   const double dt = sc->dt, h = g.h;
@@ -119,6 +121,7 @@ __global__ void __launch_bounds__(256)
 k_rhs_div(GridDesc g, const Scalars* sc, const double* __restrict__ u,
           const double* __restrict__ v, double* __restrict__ rhs)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_RHSDIV);
   const double h = g.h, facDiv = 0.5 * h / sc->dt;
   const int nx = g.nx, ny = g.ny;
@@ -141,6 +144,7 @@ k_pcorr(GridDesc g, const Scalars* sc, const double* __restrict__ p,
         const double* __restrict__ ui, const double* __restrict__ vi,
         double* __restrict__ uo, double* __restrict__ vo)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_PCORR);
   const double pFac = -0.5 * sc->dt / g.h;
   const int nx = g.nx, ny = g.ny;
@@ -163,6 +167,7 @@ __global__ void __launch_bounds__(256)
 k_fade_sums(GridDesc g, Scalars* sc, const double* __restrict__ rhs,
             double* partials, unsigned* counter)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_FADE);
   __shared__ double red[96];
   const int bx = blockIdx.x, by = blockIdx.y;
@@ -213,6 +218,7 @@ k_fade_sums(GridDesc g, Scalars* sc, const double* __restrict__ rhs,
 __global__ void k_ic(size_t n, double* u, double* v, double* chi, double* pres,
                      double* rhs, double* sdf, double* udx, double* udy)
 {
+  pdl_begin();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     u[i] = 0; v[i] = 0; chi[i] = 0; pres[i] = 0; rhs[i] = 0;
@@ -224,6 +230,7 @@ __global__ void k_ic(size_t n, double* u, double* v, double* chi, double* pres,
 __global__ void k_apply_obj_vel(size_t n, double* u, double* v, const double* chi,
                                 const double* udx, const double* udy)
 {
+  pdl_begin();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     const double X = chi[i];
@@ -245,24 +252,24 @@ inline int max_grid(const Ctx& c) {
 
 void launch_max_u_dt(Ctx& c) {
   const int nb = max_grid(c);
-  k_max_u_dt<<<nb, 512, 0, c.stream>>>(c.g, c.dsc, c.dshapes, c.nshapes, c.u(), c.v(),
+  launch_k(k_max_u_dt, nb, 512, 0, c.stream, c.g, c.dsc, c.dshapes, c.nshapes, c.u(), c.v(),
                                         c.partials, c.counters + CNT_MAXU);
   CUP2D_LAUNCHED(c);
 }
 
 void launch_set_dt(Ctx& c, double dt) {
-  k_set_dt<<<1, 1, 0, c.stream>>>(c.dsc, dt);
+  launch_k(k_set_dt, 1, 1, 0, c.stream, c.dsc, dt);
   CUP2D_LAUNCHED(c);
 }
 
 void launch_end_step(Ctx& c) {
-  k_end_step<<<1, 1, 0, c.stream>>>(c.dsc);
+  launch_k(k_end_step, 1, 1, 0, c.stream, c.dsc);
   CUP2D_LAUNCHED(c);
 }
 
 void launch_advdiff(Ctx& c) {
   dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
-  k_advdiff<<<grid, block, 0, c.stream>>>(c.g, c.dsc, c.u(), c.v(), c.uo(), c.vo(),
+  launch_k(k_advdiff, grid, block, 0, c.stream, c.g, c.dsc, c.u(), c.v(), c.uo(), c.vo(),
                                           c.partials, c.counters + CNT_ADV, c.dsc);
   CUP2D_LAUNCHED(c);
   c.cur = 1 - c.cur;   // advDiff.cpp:81-87: the new field becomes the velocity
@@ -279,31 +286,31 @@ void launch_outflow(Ctx& c) {
 
 void launch_rhs_div(Ctx& c) {
   dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
-  k_rhs_div<<<grid, block, 0, c.stream>>>(c.g, c.dsc, c.u(), c.v(), c.rhs);
+  launch_k(k_rhs_div, grid, block, 0, c.stream, c.g, c.dsc, c.u(), c.v(), c.rhs);
   CUP2D_LAUNCHED(c);
 }
 
 void launch_fade_sums(Ctx& c) {
   dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
-  k_fade_sums<<<grid, block, 0, c.stream>>>(c.g, c.dsc, c.rhs, c.partials, c.counters + CNT_FADE);
+  launch_k(k_fade_sums, grid, block, 0, c.stream, c.g, c.dsc, c.rhs, c.partials, c.counters + CNT_FADE);
   CUP2D_LAUNCHED(c);
 }
 
 void launch_pcorr(Ctx& c) {
   dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
-  k_pcorr<<<grid, block, 0, c.stream>>>(c.g, c.dsc, c.pres, c.u(), c.v(), c.uo(), c.vo());
+  launch_k(k_pcorr, grid, block, 0, c.stream, c.g, c.dsc, c.pres, c.u(), c.v(), c.uo(), c.vo());
   CUP2D_LAUNCHED(c);
   c.cur = 1 - c.cur;
 }
 
 void launch_ic(Ctx& c) {
-  k_ic<<<reduce_grid(c), 256, 0, c.stream>>>(c.ncells(), c.u(), c.v(), c.chi, c.pres, c.rhs,
+  launch_k(k_ic, reduce_grid(c), 256, 0, c.stream, c.ncells(), c.u(), c.v(), c.chi, c.pres, c.rhs,
                                               c.sdf, c.udefx, c.udefy);
   CUP2D_LAUNCHED(c);
 }
 
 void launch_apply_obj_vel(Ctx& c) {
-  k_apply_obj_vel<<<reduce_grid(c), 256, 0, c.stream>>>(c.ncells(), c.u(), c.v(), c.chi,
+  launch_k(k_apply_obj_vel, reduce_grid(c), 256, 0, c.stream, c.ncells(), c.u(), c.v(), c.chi,
                                                          c.udefx, c.udefy);
   CUP2D_LAUNCHED(c);
 }

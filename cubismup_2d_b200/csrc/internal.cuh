@@ -193,6 +193,16 @@ inline cudaError_t allow_max_dynamic_smem(const void* f) {
   return e;
 }
 
+// ---- programmatic dependent launch ---------------------------------------
+// Every pipeline kernel is launched with programmatic stream serialization
+// (launch_k): the next kernel of the stream is launched as the CTAs of the
+// previous one exit (the implicit trigger), without waiting for the grid's
+// completion to be signalled.  Each kernel first waits for its predecessor's
+// completion and memory, so completion stays transitive along the stream.
+__device__ __forceinline__ void pdl_begin() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // ---- small device helpers ------------------------------------------------
 
 __device__ __forceinline__ double warp_sum(double v) {

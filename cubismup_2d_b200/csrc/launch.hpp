@@ -2,9 +2,24 @@
 #pragma once
 #include "internal.cuh"
 
+#include <utility>
+
 namespace cup2d {
 
 struct Ctx;
+
+// Kernel launch with programmatic stream serialization (see pdl_begin).
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                            cudaStream_t stream, Args&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid; cfg.blockDim = block; cfg.dynamicSmemBytes = smem; cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr; cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // fluid.cu
 void launch_max_u_dt(Ctx& c);                        // Helpers.cpp:136-176 + Simulation.cpp:254-277

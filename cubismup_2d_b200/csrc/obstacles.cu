@@ -38,6 +38,7 @@ inline AllTiles all_tiles(const Ctx& c) {
 __global__ void __launch_bounds__(256)
 k_obj_begin(GridDesc g, Scalars* sc, DevShape* sh, int nsh, AllTiles T, double* chi, double* sdf)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_OBJBEGIN);
   clear_old_tiles(g, sh, nsh, T.t, chi, sdf, blockIdx.x, gridDim.x);
   if (threadIdx.x == 0 && blockIdx.x == 0) bodies_motion(g, sc, sh, nsh);
@@ -51,6 +52,7 @@ k_step_begin(GridDesc g, Scalars* sc, DevShape* sh, int nsh, AllTiles T, double*
              const double* __restrict__ u, const double* __restrict__ v, double* partials, unsigned* counter,
              PrefetchList pf)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_MAXU);
   __shared__ double red[64];
   prefetch_region(pf, blockIdx.x);
@@ -72,6 +74,7 @@ __device__ __forceinline__ bool disk_touching(const GridDesc& g, const DevShape&
 __global__ void __launch_bounds__(512)
 k_disk_place(GridDesc g, Scalars* sc, DevShape* sh, AllTiles T)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_COMPACT);
   const int k = blockIdx.x;
   DevShape& S = sh[k];
@@ -88,6 +91,7 @@ k_disk_place(GridDesc g, Scalars* sc, DevShape* sh, AllTiles T)
 __global__ void __launch_bounds__(1024)
 k_raster_disk(GridDesc g, const DevShape* sh, AllTiles T, double* sdf)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_RASTER_DISK);
   const int k = blockIdx.y;
   const DevShape& S = sh[k];
@@ -112,6 +116,7 @@ __global__ void __launch_bounds__(1024)
 k_chi(GridDesc g, const DevShape* sh, AllTiles T, const double* __restrict__ sdfg,
       double* chig, double* partials, int partStride)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_CHI);
   __shared__ double red[32 * 3];
   __shared__ double tile[BS][BS + 1];
@@ -189,6 +194,7 @@ __global__ void __launch_bounds__(1024)
 k_moments(GridDesc g, DevShape* sh, AllTiles T, const double* chiParts, double* parts,
           int partStride, unsigned* counters)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_MOMENTS);
   __shared__ double red[32 * 7];
   __shared__ double bc[3];
@@ -257,6 +263,7 @@ __global__ void __launch_bounds__(1024)
 k_udef_grid(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* chig,
             double* udx, double* udy)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_UDEF);
   for (int s = blockIdx.x; s < sh[k].ntiles; s += gridDim.x) {
     const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
@@ -279,6 +286,7 @@ __global__ void __launch_bounds__(1024)
 k_rhs_obst(GridDesc g, DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
            double* rhs, double* partials, unsigned* counter)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_RHSOBST);
   __shared__ double red[32 * 3];
   DevShape& S = sh[k];
@@ -328,6 +336,7 @@ __global__ void __launch_bounds__(1024)
 k_rhs_corr(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
            double* rhs)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_RHSCORR);
   const DevShape& S = sh[k];
   const double corr = S.rhsCorr;
@@ -363,6 +372,7 @@ k_momenta(GridDesc g, const Scalars* sc, DevShape* sh, AllTiles T, const double*
           const double* __restrict__ ui, const double* __restrict__ vi,
           double* parts, int partStride, unsigned* counters)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_MOMENTA);
   __shared__ double red[32 * 7];
   const int k = blockIdx.y, tid = lin_tid();
@@ -418,6 +428,7 @@ k_momenta(GridDesc g, const Scalars* sc, DevShape* sh, AllTiles T, const double*
 __global__ void __launch_bounds__(1024)
 k_collide(GridDesc g, const Scalars* sc, DevShape* sh, int nsh, AllTiles T)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_COLLIDE);
   __shared__ double red[32 * 10];
   __shared__ double coll[MAX_SHAPES][10];
@@ -497,6 +508,7 @@ __global__ void __launch_bounds__(1024)
 k_penalize(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
            double* u, double* v)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_PENALIZE);
   const DevShape& S = sh[k];
   for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
@@ -526,6 +538,7 @@ k_forces(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ u,
          const double* __restrict__ v, const double* __restrict__ p,
          double* partials, int partStride, unsigned* counters)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_FORCES);
   __shared__ double red[32 * NFORCE];
   const int k = blockIdx.y;
@@ -625,7 +638,7 @@ void launch_objects_begin(Ctx& c, bool midlineReady) {
   if (!midlineReady)
     for (int k = 0; k < c.nshapes; k++)
       if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.stream, 0);
-  k_obj_begin<<<tile_ctas(c, c.maxCapacity), 256, 0, c.stream>>>(
+  launch_k(k_obj_begin, tile_ctas(c, c.maxCapacity), 256, 0, c.stream, 
       c.g, c.dsc, c.dshapes, c.nshapes, all_tiles(c), c.chi, c.sdf);
   CUP2D_LAUNCHED(c);
 }
@@ -645,7 +658,7 @@ void launch_step_begin(Ctx& c) {
       add(F.pool, sizeof(double) * (27 * (size_t)F.nm + 16));
       add(F.ipIdx, sizeof(int2) * (size_t)F.nint);
     }
-  k_step_begin<<<nb, 512, 0, c.stream>>>(c.g, c.dsc, c.dshapes, c.nshapes, all_tiles(c), c.chi, c.sdf,
+  launch_k(k_step_begin, nb, 512, 0, c.stream, c.g, c.dsc, c.dshapes, c.nshapes, all_tiles(c), c.chi, c.sdf,
                                          c.u(), c.v(), c.partials, c.counters + CNT_MAXU, pf);
   CUP2D_LAUNCHED(c);
 }
@@ -662,22 +675,22 @@ void launch_objects_rest(Ctx& c) {
   for (int k = 0; k < c.nshapes; k++)
     if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_place(c, k);
   if (anyDisk) {
-    k_disk_place<<<c.nshapes, 512, 0, c.stream>>>(c.g, c.dsc, c.dshapes, T);
+    launch_k(k_disk_place, c.nshapes, 512, 0, c.stream, c.g, c.dsc, c.dshapes, T);
     CUP2D_LAUNCHED(c);
   }
   if (c.recordPlaced) cudaEventRecord(c.evPlaced, c.stream);
   if (anyDisk) {
-    k_raster_disk<<<dim3(tile_ctas(c, cap), c.nshapes), dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, T, c.sdf);
+    launch_k(k_raster_disk, dim3(tile_ctas(c, cap), c.nshapes), dim3(32, 32), 0, c.stream, c.g, c.dshapes, T, c.sdf);
     CUP2D_LAUNCHED(c);
   }
   if (anyFish)
     for (int k = 0; k < c.nshapes; k++)
       if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_raster(c, k);
   const int stride = (int)shape_region(c);
-  k_chi<<<dim3(tile_ctas(c, cap), c.nshapes), dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, T, c.sdf, c.chi,
+  launch_k(k_chi, dim3(tile_ctas(c, cap), c.nshapes), dim3(32, 32), 0, c.stream, c.g, c.dshapes, T, c.sdf, c.chi,
                                                               shape_partials(c), stride);
   CUP2D_LAUNCHED(c);
-  k_moments<<<dim3(tile_ctas(c, cap), c.nshapes), 1024, 0, c.stream>>>(c.g, c.dshapes, T, shape_partials(c),
+  launch_k(k_moments, dim3(tile_ctas(c, cap), c.nshapes), 1024, 0, c.stream, c.g, c.dshapes, T, shape_partials(c),
                                                           shape_partials(c), stride, c.counters + CNT_MOMENTS);
   CUP2D_LAUNCHED(c);
 }
@@ -689,7 +702,7 @@ void launch_objects(Ctx& c, bool midlineReady) {
 
 void launch_obj_vel_on_grid(Ctx& c) {
   for (int k = 0; k < c.nshapes; k++) {
-    k_udef_grid<<<tile_ctas(c, c.tiles[k].capacity), dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
+    launch_k(k_udef_grid, tile_ctas(c, c.tiles[k].capacity), dim3(32, 32), 0, c.stream, c.g, c.dshapes, k, c.tiles[k],
                                                                    c.chi, c.udefx, c.udefy);
     CUP2D_LAUNCHED(c);
   }
@@ -697,13 +710,13 @@ void launch_obj_vel_on_grid(Ctx& c) {
 
 void launch_rhs_obstacles(Ctx& c) {
   for (int k = 0; k < c.nshapes; k++) {
-    k_rhs_obst<<<tile_ctas(c, c.tiles[k].capacity), dim3(32, 32), 0, c.stream>>>(
+    launch_k(k_rhs_obst, tile_ctas(c, c.tiles[k].capacity), dim3(32, 32), 0, c.stream, 
         c.g, c.dshapes, k, c.tiles[k], c.chi, c.rhs, shape_partials(c) + (size_t)k * shape_region(c),
         c.counters + CNT_RHSOBST + k);
     CUP2D_LAUNCHED(c);
   }
   for (int k = 0; k < c.nshapes; k++) {
-    k_rhs_corr<<<tile_ctas(c, c.tiles[k].capacity), dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
+    launch_k(k_rhs_corr, tile_ctas(c, c.tiles[k].capacity), dim3(32, 32), 0, c.stream, c.g, c.dshapes, k, c.tiles[k],
                                                                   c.chi, c.rhs);
     CUP2D_LAUNCHED(c);
   }
@@ -711,7 +724,7 @@ void launch_rhs_obstacles(Ctx& c) {
 
 void launch_momenta(Ctx& c, const double* ui, const double* vi) {
   if (c.nshapes == 0) return;
-  k_momenta<<<dim3(tile_ctas(c, c.maxCapacity), c.nshapes), 1024, 0, c.stream>>>(
+  launch_k(k_momenta, dim3(tile_ctas(c, c.maxCapacity), c.nshapes), 1024, 0, c.stream, 
       c.g, c.dsc, c.dshapes, all_tiles(c), c.pres, ui, vi, shape_partials(c), (int)shape_region(c),
       c.counters + CNT_MOMENTA);
   CUP2D_LAUNCHED(c);
@@ -721,11 +734,11 @@ void launch_collide_penalize(Ctx& c) {
   if (c.nshapes == 0) return;
   const AllTiles T = all_tiles(c);
   if (c.nshapes > 1) {
-    k_collide<<<1, 1024, 0, c.stream>>>(c.g, c.dsc, c.dshapes, c.nshapes, T);
+    launch_k(k_collide, 1, 1024, 0, c.stream, c.g, c.dsc, c.dshapes, c.nshapes, T);
     CUP2D_LAUNCHED(c);
   }
   for (int k = 0; k < c.nshapes; k++) {
-    k_penalize<<<tile_ctas(c, c.tiles[k].capacity), dim3(32, 32), 0, c.stream>>>(c.g, c.dshapes, k, c.tiles[k],
+    launch_k(k_penalize, tile_ctas(c, c.tiles[k].capacity), dim3(32, 32), 0, c.stream, c.g, c.dshapes, k, c.tiles[k],
                                                                   c.chi, c.u(), c.v());
     CUP2D_LAUNCHED(c);
   }
@@ -734,7 +747,7 @@ void launch_collide_penalize(Ctx& c) {
 void launch_forces(Ctx& c) {
   if (c.nshapes == 0) return;
   const AllTiles T = all_tiles(c);
-  k_forces<<<dim3(tile_ctas(c, c.maxCapacity), c.nshapes), dim3(32, 32), 0, c.stream>>>(
+  launch_k(k_forces, dim3(tile_ctas(c, c.maxCapacity), c.nshapes), dim3(32, 32), 0, c.stream, 
       c.g, c.dshapes, T, c.u(), c.v(), c.pres, shape_partials(c), (int)shape_region(c),
       c.counters + CNT_FORCES);
   CUP2D_LAUNCHED(c);

@@ -269,6 +269,7 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
            double2* __restrict__ out, int outStride,
            const double2* __restrict__ tw, int twLen, FadeArgs fa, double h, int Nx, int Ny)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_R2C);
   constexpr int SL = Len<L>::SL, RB = Len<L>::B, NT = Len<L>::NT;
   extern __shared__ double2 sm[];
@@ -363,6 +364,7 @@ k_cols(double2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrows
        const double* __restrict__ ghatIn, double* __restrict__ ghatOut, int mode,
        const double2* __restrict__ tw, int twLen, double norm, int MXp, int MYp)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_COLS);
   constexpr int SL = Len<L>::SL, CB = Len<L>::B, NT = Len<L>::NT, GR = L / 2 + 1;
   extern __shared__ double2 sm[];
@@ -436,6 +438,7 @@ __global__ void __launch_bounds__(Len<L>::NT, Len<L>::MINB)
 k_rows_c2r(const double2* __restrict__ in, int inStride, int nrows, double* __restrict__ out,
            int outStride, int ncolsOut, const double2* __restrict__ tw, int twLen)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_C2R);
   constexpr int SL = Len<L>::SL, RB = Len<L>::B, NT = Len<L>::NT, H = L / 2;
   extern __shared__ double2 sm[];
@@ -503,6 +506,7 @@ __global__ void __launch_bounds__(Len<L>::NT, Len<L>::MINB)
 k_dct_rows_fwd(const double* in, int Nx, int nrows, double* __restrict__ D, int rb,
                const double2* __restrict__ tw, int twLen, FadeArgs fa)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_DCT_FWD);
   constexpr int SL = Len<L>::SL;
   extern __shared__ double2 sm[];
@@ -557,6 +561,7 @@ __global__ void __launch_bounds__(Len<L>::NT, Len<L>::MINB)
 k_dct_cols(double* D, int Nx, int Ny, int cb, const float* __restrict__ cosX, const float* __restrict__ cosY,
            double tol, const double2* __restrict__ tw, int twLen)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_DCT_COLS);
   constexpr int SL = Len<L>::SL;
   extern __shared__ double2 sm[];
@@ -627,6 +632,7 @@ __global__ void __launch_bounds__(Len<L>::NT, Len<L>::MINB)
 k_dct_rows_inv(const double* __restrict__ D, int Nx, int nrows, double* __restrict__ out, int rb,
                const double2* __restrict__ tw, int twLen)
 {
+  pdl_begin();
   CUP2D_TRACE_SCOPE(TR_DCT_INV);
   constexpr int SL = Len<L>::SL;
   extern __shared__ double2 sm[];
@@ -686,9 +692,9 @@ bool rows_r2c(int L, cudaStream_t st, const double* in, int inStride, int nrows,
               bool halfIn) {
   switch (L) {
 #define X(LL) case LL: \
-    if (halfIn) k_rows_r2c<LL, true><<<(nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st>>>( \
+    if (halfIn) launch_k(k_rows_r2c<LL, true>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st,  \
         in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, Nx, Ny); \
-    else k_rows_r2c<LL, false><<<(nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st>>>( \
+    else launch_k(k_rows_r2c<LL, false>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st,  \
         in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, Nx, Ny); \
     return true;
     CUP2D_FFT_LENGTHS(X)
@@ -701,11 +707,11 @@ bool cols(int L, cudaStream_t st, double2* data, int stride, int ncols, int nrow
           double* ghat, int mode, const double2* tw, int twLen, double norm, int MXp, int MYp) {
   switch (L) {
 #define X(LL) case LL: \
-    if (mode == 0) k_cols<LL, true><<<(ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, \
-        smem_for<LL>((size_t)(LL / 2 + 1) * Len<LL>::B), st>>>(data, stride, ncols, nrowsIn, \
+    if (mode == 0) launch_k(k_cols<LL, true>, (ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, \
+        smem_for<LL>((size_t)(LL / 2 + 1) * Len<LL>::B), st, data, stride, ncols, nrowsIn, \
         nrowsOut, ghat, ghat, mode, tw, twLen, norm, MXp, MYp); \
-    else k_cols<LL, false><<<(ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, \
-        smem_for<LL>((size_t)(LL / 2 + 1) * Len<LL>::B), st>>>(data, stride, ncols, nrowsIn, \
+    else launch_k(k_cols<LL, false>, (ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, \
+        smem_for<LL>((size_t)(LL / 2 + 1) * Len<LL>::B), st, data, stride, ncols, nrowsIn, \
         nrowsOut, ghat, ghat, mode, tw, twLen, norm, MXp, MYp); \
     return true;
     CUP2D_FFT_LENGTHS(X)
@@ -718,9 +724,9 @@ bool rows_c2r(int L, cudaStream_t st, const double2* in, int inStride, int nrows
               int ncolsOut, const double2* tw, int twLen, bool halfOut) {
   switch (L) {
 #define X(LL) case LL: \
-    if (halfOut) k_rows_c2r<LL, true><<<(nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st>>>( \
+    if (halfOut) launch_k(k_rows_c2r<LL, true>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st,  \
         in, inStride, nrows, out, outStride, ncolsOut, tw, twLen); \
-    else k_rows_c2r<LL, false><<<(nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st>>>( \
+    else launch_k(k_rows_c2r<LL, false>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st,  \
         in, inStride, nrows, out, outStride, ncolsOut, tw, twLen); \
     return true;
     CUP2D_FFT_LENGTHS(X)
@@ -732,8 +738,8 @@ bool rows_c2r(int L, cudaStream_t st, const double2* in, int inStride, int nrows
 bool dct_rows_fwd(int L, cudaStream_t st, const double* in, int Nx, int nrows, double* D,
                   const double2* tw, int twLen, FadeArgs fa) {
   switch (L) {
-#define X(LL) case LL: k_dct_rows_fwd<LL><<<(nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, \
-                  smem_for<LL>((size_t)Len<LL>::B * LL), st>>>(in, Nx, nrows, D, Len<LL>::B, tw, twLen, fa); return true;
+#define X(LL) case LL: launch_k(k_dct_rows_fwd<LL>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, \
+                  smem_for<LL>((size_t)Len<LL>::B * LL), st, in, Nx, nrows, D, Len<LL>::B, tw, twLen, fa); return true;
     CUP2D_FFT_LENGTHS(X)
 #undef X
   }
@@ -744,7 +750,7 @@ bool dct_cols(int L, cudaStream_t st, double* D, int Nx, int Ny, const float* cx
               const double2* tw, int twLen) {
   const int pairs = Nx / 2;
   switch (L) {
-#define X(LL) case LL: k_dct_cols<LL><<<(pairs + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st>>>( \
+#define X(LL) case LL: launch_k(k_dct_cols<LL>, (pairs + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st,  \
                   D, Nx, Ny, Len<LL>::B, cx, cy, tol, tw, twLen); return true;
     CUP2D_FFT_LENGTHS(X)
 #undef X
@@ -755,7 +761,7 @@ bool dct_cols(int L, cudaStream_t st, double* D, int Nx, int Ny, const float* cx
 bool dct_rows_inv(int L, cudaStream_t st, const double* D, int Nx, int nrows, double* out,
                   const double2* tw, int twLen) {
   switch (L) {
-#define X(LL) case LL: k_dct_rows_inv<LL><<<(nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st>>>( \
+#define X(LL) case LL: launch_k(k_dct_rows_inv<LL>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st,  \
                   D, Nx, nrows, out, Len<LL>::B, tw, twLen); return true;
     CUP2D_FFT_LENGTHS(X)
 #undef X
