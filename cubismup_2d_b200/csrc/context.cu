@@ -138,24 +138,22 @@ struct StreamScope {
 
 // PressureSingle.cpp:216-241 and 362-372: the pressure correction and the
 // momentum integrals run side by side (the integrals evaluate the corrected
-// velocity of their own cells), then collisions and penalization.
+// velocity of their own cells), then collisions and penalization.  The
+// integrals, the longer of the two, stay on the main stream.
 void launch_pressure_tail(Ctx& c) {
   const double* ui = c.u();
   const double* vi = c.v();
-  if (c.nshapes > 0) {
-    cudaEventRecord(c.evPres, c.stream);
-    cudaStreamWaitEvent(c.side2, c.evPres, 0);
-    {
-      StreamScope scope(c, c.side2);
-      launch_momenta(c, ui, vi);
-    }
-    cudaEventRecord(c.evMom, c.side2);
+  if (c.nshapes == 0) { launch_pcorr(c); return; }
+  cudaEventRecord(c.evPres, c.stream);
+  cudaStreamWaitEvent(c.side2, c.evPres, 0);
+  {
+    StreamScope scope(c, c.side2);
+    launch_pcorr(c);                        // flips the current velocity buffer
   }
-  launch_pcorr(c);
-  if (c.nshapes > 0) {
-    cudaStreamWaitEvent(c.stream, c.evMom, 0);
-    launch_collide_penalize(c);
-  }
+  cudaEventRecord(c.evMom, c.side2);
+  launch_momenta(c, ui, vi);
+  cudaStreamWaitEvent(c.stream, c.evMom, 0);
+  launch_collide_penalize(c);
 }
 
 // One pass of Simulation::simulate's loop body (Simulation.cpp:245-251) as a

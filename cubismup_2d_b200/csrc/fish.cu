@@ -269,6 +269,7 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
   double* vNorX = norY + Nm;  double* vNorY = vNorX + Nm;
   double* width = vNorY + Nm; double* rS = width + Nm;
   Segment* segS = reinterpret_cast<Segment*>(rS + Nm);  // this step's segments, also kept on chip
+#pragma unroll 1
   for (int i = tid; i < Nm; i += nt) { width[i] = F.width[i]; rS[i] = F.rS[i]; }
   __syncthreads();
   CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 1);
@@ -277,6 +278,7 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
   {                                                     // changeToCoMFrameAngular
     const double vAin = bc[2];
     const double R00 = bc[0], R01 = -bc[1], R10 = bc[1], R11 = bc[0];   // rotation by theta_internal
+#pragma unroll 1
     for (int i = tid; i < Nm; i += nt) {
       const double px = M.rX[i], py = M.rY[i];
       const double qx = M.vX[i] + vAin * py, qy = M.vY[i] - vAin * px;
@@ -287,6 +289,7 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
     }
     __syncthreads();
   CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 2);
+#pragma unroll 1
     for (int i = tid; i < Nm; i += nt) {                // _computeMidlineNormals
       const int j = i < Nm - 1 ? i : Nm - 2;            // the last copies its neighbour
       const double ds = rS[j + 1] - rS[j];
@@ -309,9 +312,12 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
   constexpr int SEGT = 64;                              // threads of the segment warps
   if (tid < SEGT) {
   // AreaSegments (Fish.cpp:118-150) in the computational frame
+#pragma unroll 1
   for (int i = tid; i < Nseg; i += SEGT) {
+    CUP2D_TRACE_MARK(TRACE_ITEMS - 2, 0);
     const int next_idx = (i + 1) * (Nm - 1) / Nseg, idx = i * (Nm - 1) / Nseg;
     double bb[2][2] = {{1e9, -1e9}, {1e9, -1e9}};
+#pragma unroll 1
     for (int ss = idx; ss <= next_idx; ++ss) {
       const double xB0 = rX[ss] - norX[ss] * width[ss], xB1 = rX[ss] + norX[ss] * width[ss];
       const double yB0 = rY[ss] - norY[ss] * width[ss], yB1 = rY[ss] + norY[ss] * width[ss];
@@ -320,6 +326,7 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
       bb[0][0] = fmin(bb[0][0], minX); bb[0][1] = fmax(bb[0][1], maxX);
       bb[1][0] = fmin(bb[1][0], minY); bb[1][1] = fmax(bb[1][1], maxY);
     }
+    CUP2D_TRACE_MARK_AFTER(TRACE_ITEMS - 2, 1, bb[0][0] + bb[1][1]);
     const double safe = 2 * g.h;
     Segment sg;
     sg.first = idx; sg.second = next_idx;
@@ -330,10 +337,12 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
     const double nJ0 = R00 * 0 + R01 * 1, nJ1 = R10 * 0 + R11 * 1;
     sg.c[0] = R00 * c0 + R01 * c1 + S.s.center[0];
     sg.c[1] = R10 * c0 + R11 * c1 + S.s.center[1];
+    CUP2D_TRACE_MARK_AFTER(TRACE_ITEMS - 2, 2, sg.c[0] + sg.c[1]);
     const double magI = sqrt(nI0 * nI0 + nI1 * nI1), magJ = sqrt(nJ0 * nJ0 + nJ1 * nJ1);
     const double invMagI = 1 / magI, invMagJ = 1 / magJ;
     sg.normalI[0] = fabs(nI0) * invMagI; sg.normalI[1] = fabs(nI1) * invMagI;
     sg.normalJ[0] = fabs(nJ0) * invMagJ; sg.normalJ[1] = fabs(nJ1) * invMagJ;
+    CUP2D_TRACE_MARK_AFTER(TRACE_ITEMS - 2, 3, sg.normalI[0] + sg.normalJ[1]);
     const double wX[2] = {sg.w[0] * sg.normalI[0], sg.w[0] * sg.normalI[1]};
     const double wY[2] = {sg.w[1] * sg.normalJ[0], sg.w[1] * sg.normalJ[1]};
     for (int d = 0; d < 2; d++) {
@@ -342,13 +351,16 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
       sg.boxObj[d][0] = sg.c[d] - sg.w[d];
       sg.boxObj[d][1] = sg.c[d] + sg.w[d];
     }
+    CUP2D_TRACE_MARK_AFTER(TRACE_ITEMS - 2, 4, sg.boxLab[1][1] + sg.boxObj[0][0]);
     F.seg[i] = sg;
     segS[i] = sg;
+    CUP2D_TRACE_MARK(TRACE_ITEMS - 2, 5);
   }
   CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 4);
   asm volatile("bar.sync 1, %0;" :: "n"(SEGT) : "memory");   // the segment warps only
   if (tid < 32) {                                       // one warp: bounding box of boxLab
     double lo0 = 1e300, hi0 = -1e300, lo1 = 1e300, hi1 = -1e300;
+#pragma unroll 1
     for (int i = tid; i < Nseg; i += 32) {
       const Segment& sg = segS[i];
       lo0 = fmin(lo0, sg.boxLab[0][0]); hi0 = fmax(hi0, sg.boxLab[0][1]);
@@ -365,6 +377,7 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
   // points of constructInternl (FishLibrary.cpp:597-610), computational frame
   const int pt = tid - SEGT, pnt = nt - SEGT;
   const double pos0 = S.s.center[0], pos1 = S.s.center[1];
+#pragma unroll 1
   for (int q = pt; q < 2 * Nm; q += pnt) {
     const int ss = q >> 1, signp = (q & 1) ? 1 : -1;
     const double m0 = rX[ss] + width[ss] * signp * norX[ss];
@@ -374,6 +387,7 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
     const double u1 = vY[ss] + width[ss] * signp * vNorY[ss];
     F.su[q] = make_double2(R00 * u0 + R01 * u1, R10 * u0 + R11 * u1);
   }
+#pragma unroll 1
   for (int q = pt; q < F.nint; q += pnt) {
     const int2 si = F.ipIdx[q];
     const int ss = si.x, iw = si.y;
@@ -402,10 +416,12 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
   __shared__ int base;
   const int lane = tid & 31, wid = tid >> 5, nwarps = nt >> 5;
   if (tid == 0) base = 0;
+#pragma unroll 1
   for (int c0 = 0; c0 < ncand; c0 += nt) {
     const int nq = min(nt, ncand - c0);
     if (tid < nq) hit[tid] = 0;
     __syncthreads();
+#pragma unroll 1
     for (int pr = tid; pr < nq * Nseg; pr += nt) {
       const int cq = pr / Nseg, si = pr - cq * Nseg;
       if (hit[cq]) continue;

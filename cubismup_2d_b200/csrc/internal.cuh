@@ -169,6 +169,15 @@ struct TraceScope {
 #define CUP2D_TRACE_CAT2(a, b) a##b
 #define CUP2D_TRACE_CAT(a, b) CUP2D_TRACE_CAT2(a, b)
 #define CUP2D_TRACE_SCOPE(id) TraceScope CUP2D_TRACE_CAT(cup2d_trace_scope_, __LINE__)(id)
+__device__ __forceinline__ unsigned long long global_timer_after(double dep) {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t) : "d"(dep));
+  return t;
+}
+// the stamp is taken once dep has been computed
+#define CUP2D_TRACE_MARK_AFTER(item, phase, dep) \
+  do { if (g_trace && threadIdx.x + threadIdx.y + threadIdx.z == 0 && (item) < TRACE_ITEMS) \
+         g_trace[2 * TR_N + 8 * (item) + (phase)] = global_timer_after(dep); } while (0)
 #define CUP2D_TRACE_MARK(item, phase) \
   do { if (g_trace && threadIdx.x + threadIdx.y + threadIdx.z == 0 && (item) < TRACE_ITEMS) \
          g_trace[2 * TR_N + 8 * (item) + (phase)] = global_timer(); } while (0)
@@ -176,6 +185,7 @@ static inline void trace_bind_this_unit(unsigned long long* p) { cudaMemcpyToSym
 #else
 #define CUP2D_TRACE_SCOPE(id) ((void)0)
 #define CUP2D_TRACE_MARK(item, phase) ((void)0)
+#define CUP2D_TRACE_MARK_AFTER(item, phase, dep) ((void)0)
 #endif
 
 // Raise a kernel's dynamic shared-memory limit to what the device allows
@@ -219,25 +229,65 @@ __device__ __forceinline__ int lin_tid() {
 }
 __device__ __forceinline__ int lin_nthreads() { return blockDim.x * blockDim.y * blockDim.z; }
 
-// Block-wide sum of K values per thread; result valid in linear thread 0.
-// smem must hold 32*K doubles.  Fixed reduction order: deterministic.
+// Warp reduce-scatter of KP (a power of two <= 32) values per lane: at each
+// xor step (offsets 16, 8, .., 1) a lane keeps half of its list and adds
+// its partner's copy of that half, so value k ends up, fully summed, in
+// lanes k*32/KP .. k*32/KP + 32/KP - 1.  Every value is summed over the same
+// xor pairing tree as a per-value butterfly: the totals are bitwise those
+// of warp_sum, with KP - 1 + 5 - log2(KP) shuffles instead of 5 per value.
+template <int KP>
+__device__ __forceinline__ double warp_reduce_scatter(double (&x)[KP], int lane) {
+  int m = KP;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    if (m > 1) {
+      const int half = m >> 1;
+      const bool upper = (lane & o) != 0;
+#pragma unroll
+      for (int i = 0; i < KP / 2; i++) {
+        if (i < half) {
+          const double lo = x[i], hi = x[i + half];
+          const double recv = __shfl_xor_sync(0xffffffffu, upper ? lo : hi, o);
+          x[i] = (upper ? hi : lo) + recv;
+        }
+      }
+      m = half;
+    } else {
+      x[0] += __shfl_xor_sync(0xffffffffu, x[0], o);
+    }
+  }
+  return x[0];
+}
+
+template <int K> struct Pow2Up { static constexpr int v = K <= 1 ? 1 : K <= 2 ? 2 : K <= 4 ? 4 : K <= 8 ? 8 : K <= 16 ? 16 : 32; };
+
+// Block-wide sum of K (<= 32) values per thread; result valid in linear
+// thread 0.  smem must hold 32*K doubles.  Fixed reduction order
+// (deterministic): the xor tree within each warp, then the xor tree over
+// the warps' partial sums.
 template <int K>
 __device__ __forceinline__ void block_sum(double (&v)[K], double* smem) {
+  constexpr int KP = Pow2Up<K>::v, STRIDE = 32 / KP;
   const int t = lin_tid(), lane = t & 31, wid = t >> 5;
   const int nw = (lin_nthreads() + 31) >> 5;
+  double x[KP];
 #pragma unroll
-  for (int k = 0; k < K; k++) v[k] = warp_sum(v[k]);
+  for (int k = 0; k < KP; k++) x[k] = k < K ? v[k] : 0.0;
+  const double r = warp_reduce_scatter<KP>(x, lane);
   __syncthreads();
-  if (lane == 0)
-#pragma unroll
-    for (int k = 0; k < K; k++) smem[wid * K + k] = v[k];
+  if (lane % STRIDE == 0 && lane / STRIDE < K) smem[wid * K + lane / STRIDE] = r;
   __syncthreads();
   if (wid == 0) {
+    double y[KP];
 #pragma unroll
-    for (int k = 0; k < K; k++) {
-      double x = lane < nw ? smem[lane * K + k] : 0.0;
-      v[k] = warp_sum(x);
-    }
+    for (int k = 0; k < KP; k++) y[k] = (k < K && lane < nw) ? smem[lane * K + k] : 0.0;
+    const double r2 = warp_reduce_scatter<KP>(y, lane);
+    __syncwarp();
+    if (lane % STRIDE == 0 && lane / STRIDE < K) smem[lane / STRIDE] = r2;
+    __syncwarp();
+    if (lane == 0)
+#pragma unroll
+      for (int k = 0; k < K; k++) v[k] = smem[k];
   }
   __syncthreads();
 }
