@@ -55,6 +55,20 @@ ALGO_BYTES_PER_CELL = {
 }
 
 
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# dense kernels on the swimmer workload, from one ncu capture of
+# `python bench.py --steps 4 --warmup 3 --no-cpu-baseline` (summarised in
+# profiles/fft_cols_swimmer_1024x512_fp64.md).  Writes stay in the 126 MB L2
+# within a launch, so the captured figure is the reads.
+TRAFFIC_BYTES = {
+    ("swimmer", "fft_cols"): 12672768,
+    ("swimmer", "fft_rows_fwd"): 4269312,
+    ("swimmer", "advdiff"): 8416768,
+    ("swimmer", "rhs_div"): 8396032,
+    ("swimmer", "pcorr"): 12591360,
+}
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -248,11 +262,7 @@ def run_ours(args, world, rank, local, pg):
         kt[kname] = ctx.time_kernel(kname, 50)
     dom = max(kt, key=kt.get)
     achieved = ALGO_BYTES_PER_CELL[dom] * cells / (kt[dom] * 1e-3) / 1e9
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tfile):
-        with open(tfile) as f:
-            traffic = json.load(f).get(args.workload, {}).get(dom)
+    traffic = TRAFFIC_BYTES.get((args.workload, dom))
     ctx.sync()
 
     line = None

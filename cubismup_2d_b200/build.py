@@ -1,6 +1,6 @@
 """Build the CUDA library libcup2d.so in-tree for sm_100a.
 
-    python -m cubismup_2d_b200.build [--force]
+    python -m cubismup_2d_b200.build [--force] [--trace]
 
 Every translation unit is compiled by nvcc with
 ``-gencode arch=compute_100a,code=sm_100a`` and, except the FFT-based
@@ -41,18 +41,27 @@ def _newer(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force=False, verbose=False):
-    os.makedirs(BUILD, exist_ok=True)
+TRACE_LIB = os.path.join(HERE, "libcup2d_trace.so")
+
+
+def build(force=False, verbose=False, trace=False):
+    """Build libcup2d.so, or with trace=True the timeline build
+    libcup2d_trace.so (-DCUP2D_TRACE: every kernel stamps %globaltimer at
+    entry and exit; read back by cubismup_2d_b200.timeline)."""
+    build_dir = os.path.join(BUILD, "trace") if trace else BUILD
+    lib = TRACE_LIB if trace else LIB
+    extra = ["-DCUP2D_TRACE"] if trace else []
+    os.makedirs(build_dir, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp"))]
     headers.append(os.path.join(INCLUDE, "cup2d.h"))
     jobs = []
     objs = []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        o = os.path.join(build_dir, src.replace(".cu", ".o"))
         objs.append(o)
         if force or _newer(o, [s] + headers):
-            jobs.append([NVCC] + flags_for(src) + ["-c", s, "-o", o])
+            jobs.append([NVCC] + flags_for(src) + extra + ["-c", s, "-o", o])
 
     def run(cmd):
         r = subprocess.run(cmd, capture_output=True, text=True)
@@ -63,11 +72,10 @@ def build(force=False, verbose=False):
 
     with concurrent.futures.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
         list(ex.map(run, jobs))
-    if force or jobs or _newer(LIB, objs):
-        run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB] + objs + ["-lcudart"])
-    return LIB
+    if force or jobs or _newer(lib, objs):
+        run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", lib] + objs + ["-lcudart"])
+    return lib
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True)
-    print(LIB)
+    print(build(force="--force" in sys.argv, verbose=True, trace="--trace" in sys.argv))

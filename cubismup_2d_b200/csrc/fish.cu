@@ -314,7 +314,6 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
   // AreaSegments (Fish.cpp:118-150) in the computational frame
 #pragma unroll 1
   for (int i = tid; i < Nseg; i += SEGT) {
-    CUP2D_TRACE_MARK(TRACE_ITEMS - 2, 0);
     const int next_idx = (i + 1) * (Nm - 1) / Nseg, idx = i * (Nm - 1) / Nseg;
     double bb[2][2] = {{1e9, -1e9}, {1e9, -1e9}};
 #pragma unroll 1
@@ -326,7 +325,6 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
       bb[0][0] = fmin(bb[0][0], minX); bb[0][1] = fmax(bb[0][1], maxX);
       bb[1][0] = fmin(bb[1][0], minY); bb[1][1] = fmax(bb[1][1], maxY);
     }
-    CUP2D_TRACE_MARK_AFTER(TRACE_ITEMS - 2, 1, bb[0][0] + bb[1][1]);
     const double safe = 2 * g.h;
     Segment sg;
     sg.first = idx; sg.second = next_idx;
@@ -337,12 +335,10 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
     const double nJ0 = R00 * 0 + R01 * 1, nJ1 = R10 * 0 + R11 * 1;
     sg.c[0] = R00 * c0 + R01 * c1 + S.s.center[0];
     sg.c[1] = R10 * c0 + R11 * c1 + S.s.center[1];
-    CUP2D_TRACE_MARK_AFTER(TRACE_ITEMS - 2, 2, sg.c[0] + sg.c[1]);
     const double magI = sqrt(nI0 * nI0 + nI1 * nI1), magJ = sqrt(nJ0 * nJ0 + nJ1 * nJ1);
     const double invMagI = 1 / magI, invMagJ = 1 / magJ;
     sg.normalI[0] = fabs(nI0) * invMagI; sg.normalI[1] = fabs(nI1) * invMagI;
     sg.normalJ[0] = fabs(nJ0) * invMagJ; sg.normalJ[1] = fabs(nJ1) * invMagJ;
-    CUP2D_TRACE_MARK_AFTER(TRACE_ITEMS - 2, 3, sg.normalI[0] + sg.normalJ[1]);
     const double wX[2] = {sg.w[0] * sg.normalI[0], sg.w[0] * sg.normalI[1]};
     const double wY[2] = {sg.w[1] * sg.normalJ[0], sg.w[1] * sg.normalJ[1]};
     for (int d = 0; d < 2; d++) {
@@ -351,10 +347,8 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
       sg.boxObj[d][0] = sg.c[d] - sg.w[d];
       sg.boxObj[d][1] = sg.c[d] + sg.w[d];
     }
-    CUP2D_TRACE_MARK_AFTER(TRACE_ITEMS - 2, 4, sg.boxLab[1][1] + sg.boxObj[0][0]);
     F.seg[i] = sg;
     segS[i] = sg;
-    CUP2D_TRACE_MARK(TRACE_ITEMS - 2, 5);
   }
   CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 4);
   asm volatile("bar.sync 1, %0;" :: "n"(SEGT) : "memory");   // the segment warps only

@@ -143,7 +143,7 @@ struct FishArrays {
 // read back.  Without the define the scope compiles to nothing.
 enum TraceId : int {
   TR_MAXU, TR_SETDT, TR_ENDSTEP, TR_ADVDIFF, TR_RHSDIV, TR_PCORR, TR_FADE,
-  TR_OBJBEGIN, TR_CLEAR, TR_FLAGS, TR_COMPACT, TR_RASTER_DISK, TR_CHI, TR_MOMENTS,
+  TR_OBJBEGIN, TR_DISK_PLACE, TR_RASTER_DISK, TR_CHI, TR_MOMENTS,
   TR_UDEF, TR_RHSOBST, TR_RHSCORR, TR_MOMENTA, TR_COLLIDE, TR_PENALIZE, TR_FORCES,
   TR_MIDLINE, TR_FRAME, TR_RASTER, TR_R2C, TR_COLS, TR_C2R, TR_DCT_FWD, TR_DCT_COLS,
   TR_DCT_INV, TR_SELECT, TR_N

@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(512)
 k_disk_place(GridDesc g, Scalars* sc, DevShape* sh, AllTiles T)
 {
   pdl_begin();
-  CUP2D_TRACE_SCOPE(TR_COMPACT);
+  CUP2D_TRACE_SCOPE(TR_DISK_PLACE);
   const int k = blockIdx.x;
   DevShape& S = sh[k];
   if (S.cfg.kind != CUP2D_SHAPE_DISK) return;

@@ -225,7 +225,7 @@ __device__ __forceinline__ void fft_passes(double2* A, int nseq, const double2* 
 }
 
 // In-place Stockham autosort FFT of nseq sequences of length L (A + q*SL,
-// padded indexing; a power of two >= 64): radix-16 passes and one radix
+// padded indexing; a power of two >= 16): radix-16 passes and one radix
 // 2/4/8 pass for the remaining factor.  Forward exp(-2 pi i jk/L), inverse
 // exp(+...), unnormalised.  Needs blockDim.x >= nseq * L/16.  HIN: the
 // upper half of the input is zero and never read; HOUT: only the lower half
@@ -675,7 +675,7 @@ template <int L> inline size_t smem_for(size_t extraReals = 0) {
   return sizeof(double2) * ((size_t)Len<L>::B * Len<L>::SL + Len<L>::TW) + sizeof(double) * extraReals;
 }
 
-#define CUP2D_FFT_LENGTHS(X) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
+#define CUP2D_FFT_LENGTHS(X) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
 
 void set_all_smem() {
 #define X(L) set_smem((const void*)k_rows_r2c<L, false>); set_smem((const void*)k_rows_r2c<L, true>); \
@@ -785,7 +785,7 @@ Poisson* poisson_create(Ctx& c) {
     P->Lrow = Nx;          // DCT of length Nx via a real FFT of length 2Nx
     P->Lcol = 2 * Ny;      // DCT of length Ny via a complex FFT of length 2Ny
   }
-  if (!is_pow2(P->Lrow) || !is_pow2(P->Lcol) || P->Lrow < 64 || P->Lcol < 64 ||
+  if (!is_pow2(P->Lrow) || !is_pow2(P->Lcol) || P->Lrow < 16 || P->Lcol < 16 ||
       P->Lrow > 4096 || P->Lcol > 4096) { delete P; return nullptr; }   // shared-memory limit
   P->nkx = P->Lrow + 1;
   P->twLen = 4 * (P->Lrow > P->Lcol ? P->Lrow : P->Lcol);

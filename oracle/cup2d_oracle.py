@@ -205,9 +205,9 @@ def poisson_periodic(rhs):
     ky = np.where(j <= ny // 2, j, ny - j)
     rkx, rky = kx * (2 * np.pi / nx), ky * (2 * np.pi / ny)
     RKX, RKY = np.meshgrid(rkx, rky)
-    with np.errstate(divide="ignore"):
+    with np.errstate(divide="ignore", invalid="ignore"):     # k = 0: zeroed below
         kinv = -1 / (RKX * RKX + RKY * RKY)
-    F = F * (kinv * (1.0 / (nx * ny)))
+        F = F * (kinv * (1.0 / (nx * ny)))
     F[0, 0] = 0
     return np.fft.irfft2(F, s=(ny, nx)) * (nx * ny)
 

@@ -167,3 +167,49 @@ def test_graph_replay_matches_eager(args):
     for name in ("u", "v", "pres", "chi"):
         assert np.array_equal(a.ctx.get(name), b.ctx.get(name)), name
     assert a.ctx.shape() == b.ctx.shape()
+
+
+# ---- against the committed golden fixtures (no reference build needed) -------
+
+GOLDEN_DIR = __import__("os").path.join(__import__("os").path.dirname(__import__("os").path.abspath(__file__)), "golden")
+
+
+def _golden(name):
+    z = np.load(__import__("os").path.join(GOLDEN_DIR, name + ".npz"))
+    d = {k: z[k] for k in z.files}
+    d["shape"] = dict(zip(d["shape_keys"].tolist(), d["shape_values"].tolist()))
+    return d
+
+
+@pytest.mark.parametrize("name", ["disk_forced_freespace", "disk_free_periodic", "disk_free_cosine",
+                                  "stefanfish", "carlingfish"])
+def test_steps_match_golden(name):
+    """Same configuration, noise and step count as tests/golden/make_golden.py;
+    the fixtures hold the reference's own outputs."""
+    g = _golden(name)
+    s = Simulation(str(g["args"]))
+    s.init()
+    seed = int(g["noise_seed"])
+    for comp, f in enumerate(("u", "v")):
+        s.ctx.set(f, s.ctx.get(f) + noise_field(seed, comp, s.ctx.ny, s.ctx.nx))
+    chi0 = s.ctx.get("chi")
+    if name.startswith("disk"):
+        assert np.array_equal(chi0, g["init_chi"])               # Towers chi: same arithmetic
+    else:
+        assert rel_err(chi0, g["init_chi"]) < 1e-12              # the reference's own run-to-run level
+    dts = []
+    for _ in range(int(g["nsteps"])):
+        dts.append(s.calcMaxTimestep())
+        s.advance(dts[-1])
+    assert rel_err(np.array(dts), g["dt"]) < 1e-12
+    if "final_u" in g:
+        assert rel_err(s.ctx.get("u"), g["final_u"]) < 1e-9
+        assert rel_err(s.ctx.get("v"), g["final_v"]) < 1e-9
+        assert rel_err(s.ctx.get("pres"), g["final_pres"]) < 1e-8
+        assert rel_err(s.ctx.get("chi"), g["final_chi"]) < 1e-12
+    a, b = s.ctx.shape(0), g["shape"]
+    for key in ("com_x", "com_y", "u", "v", "omega", "orientation"):
+        assert abs(a[key] - b[key]) <= 1e-9 * max(abs(b[key]), 1e-3), (key, a[key], b[key])
+    fs = max(abs(b["forcex"]), abs(b["forcey"]))
+    for key in ("forcex", "forcey", "torque"):
+        assert abs(a[key] - b[key]) <= 1e-7 * fs, (key, a[key], b[key])
