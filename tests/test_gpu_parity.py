@@ -213,3 +213,27 @@ def test_steps_match_golden(name):
     fs = max(abs(b["forcex"]), abs(b["forcey"]))
     for key in ("forcex", "forcey", "torque"):
         assert abs(a[key] - b[key]) <= 1e-7 * fs, (key, a[key], b[key])
+
+
+CYLINDER_RE100 = ("-bpdx 16 -bpdy 8 -extent 1 -CFL 0.1 -nu 1.5e-4 -lambda 1e4 -poissonType freespace "
+                  "-muteAll 1 -shapes 'disk radius=0.0375 xpos=0.2 ypos=0.25 bForced=1 bFixed=1 xvel=0.2'")
+
+
+def test_cylinder_re100_cd_200_steps(ref):
+    """The forced cylinder at Re = 100 (512x256), 200 steps from rest plus
+    seeded noise: drag and lift coefficients Cd = 2 Fx / (U^2 2R),
+    Cl = 2 Fy / (U^2 2R) within 1e-4 relative of the reference's
+    (Cl relative to Cd's scale: it starts at rounding level)."""
+    r, s = make_pair(ref, CYLINDER_RE100, noise_seed=3)
+    U, D = 0.2, 2 * 0.0375
+    for _ in range(200):
+        dt_r = r.step()
+        dt_s = s.calcMaxTimestep()
+        s.advance(dt_s)
+        assert abs(dt_s - dt_r) <= 1e-10 * dt_r
+    a, b = s.ctx.shape(0), r.shape(0)
+    cd_s, cd_r = 2 * a["forcex"] / (U * U * D), 2 * b["forcex"] / (U * U * D)
+    cl_s, cl_r = 2 * a["forcey"] / (U * U * D), 2 * b["forcey"] / (U * U * D)
+    assert abs(cd_s - cd_r) <= 1e-4 * abs(cd_r), (cd_s, cd_r)
+    assert abs(cl_s - cl_r) <= 1e-4 * abs(cd_r), (cl_s, cl_r)
+    compare_fields(r, s, ["u", "v", "pres"], 1e-6, "200 steps")
