@@ -199,10 +199,16 @@ void enqueue_step(Ctx& c) {
   launch_pressure_tail(c);
   launch_forces(c);
   if (anyFish) cudaStreamWaitEvent(c.stream, c.evJoin, 0);
-  launch_end_step(c);
+  launch_end_step_dt(c);                    // t += dt, and the next step's dt
 }
 
 } // namespace
+
+// The graph step's calcMaxTimestep reuses the maximum formed at the end of
+// the previous graph step only while nothing else has touched the state.
+cudaError_t invalidate_dt_next(Ctx& c) {
+  return cudaMemsetAsync(&c.dsc->dtNextValid, 0, sizeof(int), c.stream);
+}
 
 extern "C" {
 
@@ -299,7 +305,7 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   for (int b = 0; b < 2; b++) for (int d = 0; d < 2; d++) cudaFree(c.vel[b][d]);
   cudaFree(c.chi); cudaFree(c.pres); cudaFree(c.rhs); cudaFree(c.sdf);
   cudaFree(c.udefx); cudaFree(c.udefy); cudaFree(c.dsc); cudaFree(c.dshapes);
-  cudaFree(c.counters); cudaFree(c.partials);
+  cudaFree(c.counters); cudaFree(c.partials); cudaFree(c.maxParts);
   if (c.side) cudaStreamDestroy(c.side);
   if (c.side2) cudaStreamDestroy(c.side2);
   if (c.evObj) cudaEventDestroy(c.evObj);
@@ -453,6 +459,11 @@ int cup2d_init(cup2d_ctx* ctx) {
   c.npartials = (size_t)3 * c.g.nblocks + 4096 + (size_t)MAX_SHAPES * c.maxCapacity * 24;
   int rc = dalloc(ctx, &c.partials, c.npartials);
   if (rc) return rc;
+  cudaFree(c.maxParts);
+  c.maxParts = nullptr;
+  c.nMaxParts = c.g.nblocks + c.nshapes * (c.maxCapacity < c.sms ? c.maxCapacity : c.sms);
+  rc = dalloc(ctx, &c.maxParts, (size_t)c.g.nblocks + (size_t)MAX_SHAPES * c.sms);
+  if (rc) return rc;
   c.cur = 0;
   // Simulation::reset (Simulation.cpp:232-241): resetAll, IC, objects at t=0, ApplyObjVel
   if ((rc = upload_scalars_reset(ctx))) return rc;
@@ -497,6 +508,7 @@ int cup2d_calc_dt(cup2d_ctx* ctx, double* dt_out) {
   if (!ctx) return CUP2D_EINVAL;                                                 \
   Ctx& c = ctx->c;                                                               \
   if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");         \
+  CK(invalidate_dt_next(c));                                                     \
   if (dt >= 0) launch_set_dt(c, dt);
 
 int cup2d_put_objects(cup2d_ctx* ctx, double dt) {
@@ -608,6 +620,7 @@ int cup2d_set_field(cup2d_ctx* ctx, int which, const double* host_in) {
   if (!p) return fail(ctx, CUP2D_EINVAL, "unknown field");
   CK(cudaStreamSynchronize(c.stream));
   CK(cudaMemcpy(p, host_in, sizeof(double) * c.ncells(), cudaMemcpyHostToDevice));
+  CK(invalidate_dt_next(c));
   return CUP2D_OK;
 }
 
@@ -629,6 +642,7 @@ int cup2d_set_shape(cup2d_ctx* ctx, int id, const cup2d_shape_state* in) {
   CK(cudaMemcpy(&c.hshapes[id], c.dshapes + id, sizeof(DevShape), cudaMemcpyDeviceToHost));
   c.hshapes[id].s = *in;
   CK(cudaMemcpy(c.dshapes + id, &c.hshapes[id], sizeof(DevShape), cudaMemcpyHostToDevice));
+  CK(invalidate_dt_next(c));
   return CUP2D_OK;
 }
 
@@ -653,6 +667,7 @@ int cup2d_set_scalars(cup2d_ctx* ctx, double time, double dt, int step, double u
   CK(cudaStreamSynchronize(c.stream));
   CK(cudaMemcpy(&s, c.dsc, sizeof(Scalars), cudaMemcpyDeviceToHost));
   s.time = time; s.dt = dt; s.step = step; s.uinfx = uinfx; s.uinfy = uinfy;
+  s.dtNextValid = 0;
   CK(cudaMemcpy(c.dsc, &s, sizeof(Scalars), cudaMemcpyHostToDevice));
   return CUP2D_OK;
 }
@@ -676,6 +691,7 @@ int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, double* ms_per_launch
   Ctx& c = ctx->c;
   if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
   if (which < 0 || which > CUP2D_KERNEL_OBJECTS) return fail(ctx, CUP2D_EINVAL, "unknown kernel");
+  CK(invalidate_dt_next(c));
   auto one = [&]() {
     switch (which) {
       case CUP2D_KERNEL_ADVDIFF: launch_advdiff(c); launch_advdiff_undo(c); break;

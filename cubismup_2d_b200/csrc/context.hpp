@@ -37,6 +37,10 @@ struct Ctx {
   // reduction scratch: per-CTA partial sums and "last CTA" tickets
   double* partials = nullptr;
   size_t npartials = 0;
+  // per-CTA maxima of the next step's findMaxU: [nblocks] from the pressure
+  // correction, then [MAX_SHAPES][sms] from the force pass
+  double* maxParts = nullptr;
+  int nMaxParts = 0;
   unsigned* counters = nullptr;
   static constexpr int NCOUNTERS = 256;
 

@@ -496,32 +496,38 @@ __device__ __forceinline__ int find_range(const int* start, int n, int q) {
   return lo;
 }
 
-// Row lists: warp w owns the sub-tile rows 2w (lanes 0-15) and 2w+1 (lanes
-// 16-31).  It walks the chunk's kept points in order, 32 at a time, and
-// appends (ballot + popc, so order is kept) those whose support covers each
-// of its rows.  Every cell then visits only its row's points, in the
-// reference's order, and skips those whose columns miss it.
+// Half-row lists: warp w owns the sub-tile rows 2w (lanes 0-15) and 2w+1
+// (lanes 16-31), each split into two halves of 8 columns, i.e. four lists
+// (list 2*row + half).  The warp walks the chunk's kept points in order, 32
+// at a time, and appends (ballot + popc, so order is kept) those whose
+// support covers the list's row and reaches its half.  Every cell then
+// visits only its half-row's points, in the reference's order, and skips
+// those whose columns miss it.
+constexpr int NLIST = 2 * SUB;
+
 __device__ __forceinline__ void rows_build(unsigned short* rowIdx, int* rowN, const uchar4* supp, int nc) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int rA = 2 * w, rB = 2 * w + 1;
-  unsigned short* lA = rowIdx + rA * CAP;
-  unsigned short* lB = rowIdx + rB * CAP;
-  int nA = 0, nB = 0;
+  int n[4] = {0, 0, 0, 0};
   for (int p0 = 0; p0 < nc; p0 += 32) {
     const int p = p0 + lane;
-    bool inA = false, inB = false;
+    bool in[4] = {false, false, false, false};
     if (p < nc) {
       const uchar4 sp = supp[p];          // x lo, x hi, y lo, y hi relative to the sub-tile
-      inA = sp.z <= rA && rA < sp.w;
-      inB = sp.z <= rB && rB < sp.w;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int r = 2 * w + (q >> 1), h0 = 8 * (q & 1);
+        in[q] = sp.z <= r && r < sp.w && sp.x < h0 + 8 && h0 < sp.y;
+      }
     }
-    const unsigned mA = __ballot_sync(0xffffffffu, inA), mB = __ballot_sync(0xffffffffu, inB);
     const unsigned lt = (1u << lane) - 1u;
-    if (inA) lA[nA + __popc(mA & lt)] = (unsigned short)p;
-    if (inB) lB[nB + __popc(mB & lt)] = (unsigned short)p;
-    nA += __popc(mA); nB += __popc(mB);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const unsigned m = __ballot_sync(0xffffffffu, in[q]);
+      if (in[q]) rowIdx[(4 * w + q) * CAP + n[q] + __popc(m & lt)] = (unsigned short)p;
+      n[q] += __popc(m);
+    }
   }
-  if (lane == 0) { rowN[rA] = nA; rowN[rB] = nB; }
+  if (lane < 4) rowN[4 * w + lane] = lane == 0 ? n[0] : lane == 1 ? n[1] : lane == 2 ? n[2] : n[3];
   __syncwarp();
 }
 
@@ -529,7 +535,7 @@ __device__ __forceinline__ void rows_build(unsigned short* rowIdx, int* rowN, co
 // doubles), the chunk's points, their supports and the row lists
 inline size_t raster_smem(int Nm) {
   const size_t pts = CAP * (sizeof(SurfPt) > sizeof(IntPt) ? sizeof(SurfPt) : sizeof(IntPt));
-  return sizeof(double) * 3 * (size_t)Nm + pts + sizeof(uchar4) * CAP + sizeof(unsigned short) * SUB * CAP;
+  return sizeof(double) * 3 * (size_t)Nm + pts + sizeof(uchar4) * CAP + sizeof(unsigned short) * NLIST * CAP;
 }
 
 __global__ void __launch_bounds__(RT)
@@ -545,7 +551,7 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
   __shared__ int nSegList;
   __shared__ int wc[NWARP];
   __shared__ int wcc[CH][NWARP];
-  __shared__ int rowN[SUB];
+  __shared__ int rowN[NLIST];
   extern __shared__ double msm[];
   const DevShape& S = sh[k];
   const int nwork = S.ntiles * NSUB;
@@ -670,8 +676,9 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
       }
     __syncthreads();
     rows_build(rowIdx, rowN, supp, nc);
-    const int n = rowN[row];
-    const unsigned short* l = rowIdx + row * CAP;
+    const int li = 2 * row + (col >> 3);                // this cell's half-row list
+    const int n = rowN[li];
+    const unsigned short* l = rowIdx + li * CAP;
     int winner = -1;
     for (int e = 0; e < n; e++) {
       const int qi = l[e];
@@ -776,8 +783,9 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
       }
     __syncthreads();
     rows_build(rowIdx, rowN, supp, nc);
-    const int n = rowN[row];
-    const unsigned short* l = rowIdx + row * CAP;
+    const int li = 2 * row + (col >> 3);                // this cell's half-row list
+    const int n = rowN[li];
+    const unsigned short* l = rowIdx + li * CAP;
     for (int e = 0; e < n; e++) {
       const int qi = l[e];
       const uchar4 sp = supp[qi];

@@ -38,6 +38,27 @@ __global__ void k_end_step(Scalars* sc) { pdl_begin(); CUP2D_TRACE_SCOPE(TR_ENDS
   sc->step += 1;
 }
 
+// End of a graph step: t += dt, step += 1, then the next step's
+// calcMaxTimestep from the maxima left by the pressure correction (cells
+// without obstacle) and the force pass (obstacle cells after penalization).
+// max is exact in any order, so dtNext equals what k_max_u_dt would form.
+__global__ void __launch_bounds__(256)
+k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh, const double* maxParts, int nParts)
+{
+  pdl_begin();
+  CUP2D_TRACE_SCOPE(TR_ENDSTEP);
+  __shared__ double red[32];
+  double m = 0.0;
+  for (int i = threadIdx.x; i < nParts; i += blockDim.x) m = fmax(m, maxParts[i]);
+  m = block_max(m, red);
+  if (threadIdx.x != 0) return;
+  sc->time += sc->dt;
+  sc->step += 1;
+  sc->dtNext = dt_from_max_u(g, sc, sh, nsh, m);
+  sc->maxUNext = m;
+  sc->dtNextValid = 1;
+}
+
 // advDiff.cpp:14-87.  Ghosts: neighbour cells, or at the domain edge the
 // zero-gradient copy scaled by the inflow fade of advDiff.cpp:50-55,68-71.
 __global__ void __launch_bounds__(256)
@@ -140,23 +161,38 @@ k_rhs_div(GridDesc g, const Scalars* sc, const double* __restrict__ u,
 // PressureSingle.cpp:216-241: V += -(dt/2h) grad_2h P; zero-gradient P ghosts.
 // Reads the velocity written by advDiff (ui, vi) and writes the current one.
 __global__ void __launch_bounds__(256)
-k_pcorr(GridDesc g, const Scalars* sc, const double* __restrict__ p,
+k_pcorr(GridDesc g, Scalars* sc, const double* __restrict__ p,
         const double* __restrict__ ui, const double* __restrict__ vi,
-        double* __restrict__ uo, double* __restrict__ vo)
+        double* __restrict__ uo, double* __restrict__ vo,
+        const double* __restrict__ chig, double* maxParts)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_PCORR);
+  __shared__ double red[32];
   const double pFac = -0.5 * sc->dt / g.h;
+  const double UINF = sc->uinfx, VINF = sc->uinfy;
   const int nx = g.nx, ny = g.ny;
   const int gx = blockIdx.x * BS + threadIdx.x;
+  double m = 0.0;
+  int bad = 0;
 #pragma unroll
   for (int r = 0; r < 4; r++) {
     const int gy = blockIdx.y * BS + threadIdx.y + 8 * r;
     const size_t c = (size_t)gy * nx + gx;
     const double pW = p[gx > 0 ? c - 1 : c], pE = p[gx < nx - 1 ? c + 1 : c];
     const double pS = p[gy > 0 ? c - nx : c], pN = p[gy < ny - 1 ? c + nx : c];
-    uo[c] = ui[c] + pFac * (pE - pW);
-    vo[c] = vi[c] + pFac * (pN - pS);
+    const double un = ui[c] + pFac * (pE - pW), vn = vi[c] + pFac * (pN - pS);
+    uo[c] = un;
+    vo[c] = vn;
+    // next step's findMaxU over the cells penalization leaves alone (chi = 0)
+    if (!(chig[c] > 0)) m = fmax(m, cell_speed(un, vn, UINF, VINF));
+    bad |= !isfinite(un) || !isfinite(vn);
+  }
+  m = block_max(m, red);
+  const int anyBad = __syncthreads_or(bad);
+  if (lin_tid() == 0) {
+    maxParts[blockIdx.x + gridDim.x * blockIdx.y] = m;
+    if (anyBad) atomicOr(&sc->status, ST_NAN);
   }
 }
 
@@ -267,6 +303,11 @@ void launch_end_step(Ctx& c) {
   CUP2D_LAUNCHED(c);
 }
 
+void launch_end_step_dt(Ctx& c) {
+  launch_k(k_end_step_dt, 1, 256, 0, c.stream, c.g, c.dsc, c.dshapes, c.nshapes, c.maxParts, c.nMaxParts);
+  CUP2D_LAUNCHED(c);
+}
+
 void launch_advdiff(Ctx& c) {
   dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
   launch_k(k_advdiff, grid, block, 0, c.stream, c.g, c.dsc, c.u(), c.v(), c.uo(), c.vo(),
@@ -298,7 +339,8 @@ void launch_fade_sums(Ctx& c) {
 
 void launch_pcorr(Ctx& c) {
   dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
-  launch_k(k_pcorr, grid, block, 0, c.stream, c.g, c.dsc, c.pres, c.u(), c.v(), c.uo(), c.vo());
+  launch_k(k_pcorr, grid, block, 0, c.stream, c.g, c.dsc, c.pres, c.u(), c.v(), c.uo(), c.vo(),
+           c.chi, c.maxParts);
   CUP2D_LAUNCHED(c);
   c.cur = 1 - c.cur;
 }

@@ -45,6 +45,11 @@ struct Scalars {
   int step;
   int status;
   double rampCFL[100];            // Simulation.cpp:266-267, host-evaluated
+  // calcMaxTimestep of the next step, formed at the end of a graph step from
+  // the maxima the pressure correction and the force pass leave behind;
+  // dtNextValid is cleared by every host-side change of the state
+  double dtNext, maxUNext;
+  int dtNextValid;
 };
 
 struct ShapeCfg {

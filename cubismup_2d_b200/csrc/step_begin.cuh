@@ -24,6 +24,31 @@ __device__ __forceinline__ void prefetch_region(const PrefetchList& pf, int r) {
     asm volatile("prefetch.global.L2 [%0];" :: "l"(base + o));
 }
 
+// Helpers.cpp:160-166: the velocity magnitude findMaxU maximises for one cell
+__device__ __forceinline__ double cell_speed(double u, double v, double UINF, double VINF) {
+  return fmax(fmax(fabs(u + UINF), fabs(v + VINF)), fmax(fabs(u), fabs(v)));
+}
+
+// Simulation::calcMaxTimestep (Simulation.cpp:254-277) from the maximum
+// speed; one thread.
+__device__ __forceinline__ double dt_from_max_u(const GridDesc& g, const Scalars* sc, const DevShape* sh,
+                                                int nsh, double maxU) {
+  const double h = g.h;
+  const double dtFourier = h * h / g.nu, dtCFL = maxU < 2.2e-16 ? 1 : h / maxU;
+  double maxUb = 0;                                   // SimulationData::maxRelSpeed
+  for (int k = 0; k < nsh; k++) {
+    const double su = sh[k].s.u, sv = sh[k].s.v;
+    maxUb = fmax(maxUb, sqrt(su * su + sv * sv));     // Shape::getMaxVel
+  }
+  const double dtBody = maxUb < 2.2e-16 ? 1 : h / maxUb;
+  double mn = dtCFL;
+  if (dtFourier < mn) mn = dtFourier;
+  if (dtBody < mn) mn = dtBody;
+  double dt = g.CFL * mn;
+  if (sc->step < 100) dt = sc->rampCFL[sc->step] * mn;
+  return dt;
+}
+
 // Helpers.cpp:136-176 (findMaxU) + Simulation::calcMaxTimestep
 // (Simulation.cpp:254-277) over a 1D grid: per-CTA maxima, the last CTA
 // forms dt.  Returns true in thread 0 of the CTA that set sc->dt.
@@ -41,8 +66,8 @@ __device__ __forceinline__ bool max_u_dt_cta(const GridDesc& g, Scalars* sc, con
        i += (size_t)gridDim.x * blockDim.x) {
     const double2 a2 = u2[i], b2 = v2[i];
     // Helpers.cpp:160-166: max of |u+uinf|, |v+vinf|, |u|, |v|
-    m = fmax(m, fmax(fmax(fabs(a2.x + UINF), fabs(b2.x + VINF)), fmax(fabs(a2.x), fabs(b2.x))));
-    m = fmax(m, fmax(fmax(fabs(a2.y + UINF), fabs(b2.y + VINF)), fmax(fabs(a2.y), fabs(b2.y))));
+    m = fmax(m, cell_speed(a2.x, b2.x, UINF, VINF));
+    m = fmax(m, cell_speed(a2.y, b2.y, UINF, VINF));
     bad |= !isfinite(a2.x) || !isfinite(b2.x) || !isfinite(a2.y) || !isfinite(b2.y);
   }
   m = block_max(m, red);
@@ -56,21 +81,9 @@ __device__ __forceinline__ bool max_u_dt_cta(const GridDesc& g, Scalars* sc, con
   for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) mm = fmax(mm, __ldcg(&partials[i]));
   mm = block_max(mm, red);
   if (threadIdx.x != 0) return false;
-  const double maxU = mm, h = g.h;
-  const double dtFourier = h * h / g.nu, dtCFL = maxU < 2.2e-16 ? 1 : h / maxU;
-  double maxUb = 0;                                   // SimulationData::maxRelSpeed
-  for (int k = 0; k < nsh; k++) {
-    const double su = sh[k].s.u, sv = sh[k].s.v;
-    maxUb = fmax(maxUb, sqrt(su * su + sv * sv));     // Shape::getMaxVel
-  }
-  const double dtBody = maxUb < 2.2e-16 ? 1 : h / maxUb;
-  double mn = dtCFL;
-  if (dtFourier < mn) mn = dtFourier;
-  if (dtBody < mn) mn = dtBody;
-  double dt = g.CFL * mn;
-  if (sc->step < 100) dt = sc->rampCFL[sc->step] * mn;
+  const double dt = dt_from_max_u(g, sc, sh, nsh, mm);
   sc->dt = dt;
-  sc->maxU = maxU;
+  sc->maxU = mm;
   if (g.dlm > 0) sc->lambda = g.dlm / dt;
   return true;
 }
