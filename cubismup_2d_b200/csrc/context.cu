@@ -136,6 +136,19 @@ struct StreamScope {
   ~StreamScope() { c.stream = saved; }
 };
 
+// A graph step's final velocity is set once penalization is done: its
+// findMaxU for the next step runs on side2 beside the force pass and joins
+// before the step ends (evMaxFree).
+void launch_max_next_beside(Ctx& c) {
+  cudaEventRecord(c.evPres, c.stream);
+  cudaStreamWaitEvent(c.side2, c.evPres, 0);
+  {
+    StreamScope scope(c, c.side2);
+    launch_max_next(c);
+  }
+  cudaEventRecord(c.evMaxFree, c.side2);
+}
+
 // PressureSingle.cpp:216-241 and 362-372: the pressure correction and the
 // momentum integrals run side by side (the integrals evaluate the corrected
 // velocity of their own cells), then collisions and penalization.  The
@@ -143,7 +156,11 @@ struct StreamScope {
 void launch_pressure_tail(Ctx& c) {
   const double* ui = c.u();
   const double* vi = c.v();
-  if (c.nshapes == 0) { launch_pcorr(c); return; }
+  if (c.nshapes == 0) {
+    launch_pcorr(c);
+    if (c.graphStep) launch_max_next_beside(c);
+    return;
+  }
   cudaEventRecord(c.evPres, c.stream);
   cudaStreamWaitEvent(c.side2, c.evPres, 0);
   {
@@ -154,6 +171,7 @@ void launch_pressure_tail(Ctx& c) {
   launch_momenta(c, ui, vi);
   cudaStreamWaitEvent(c.stream, c.evMom, 0);
   launch_collide_penalize(c);
+  if (c.graphStep) launch_max_next_beside(c);
 }
 
 // One pass of Simulation::simulate's loop body (Simulation.cpp:245-251) as a
@@ -166,6 +184,8 @@ void launch_pressure_tail(Ctx& c) {
 //   side2: obstacle tiles, SDF, Towers chi, moments (advDiff does not read
 //          them); later the momentum integrals
 void enqueue_step(Ctx& c) {
+  struct GraphStepFlag { Ctx& c; explicit GraphStepFlag(Ctx& cc) : c(cc) { c.graphStep = true; }
+                         ~GraphStepFlag() { c.graphStep = false; } } flag(c);
   launch_step_begin(c);                     // dt, last step's tiles reset, body motion
   bool anyFish = false;
   for (int k = 0; k < c.nshapes; k++) anyFish |= c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK;
@@ -199,6 +219,7 @@ void enqueue_step(Ctx& c) {
   launch_pressure_tail(c);
   launch_forces(c);
   if (anyFish) cudaStreamWaitEvent(c.stream, c.evJoin, 0);
+  cudaStreamWaitEvent(c.stream, c.evMaxFree, 0);
   launch_end_step_dt(c);                    // t += dt, and the next step's dt
 }
 
@@ -282,7 +303,8 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
               cudaEventCreateWithFlags(&c.evObjDone, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evPres, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evMom, cudaEventDisableTiming) != cudaSuccess ||
-              cudaEventCreateWithFlags(&c.evPlaced, cudaEventDisableTiming) != cudaSuccess))
+              cudaEventCreateWithFlags(&c.evPlaced, cudaEventDisableTiming) != cudaSuccess ||
+              cudaEventCreateWithFlags(&c.evMaxFree, cudaEventDisableTiming) != cudaSuccess))
     rc = fail(ctx, CUP2D_ECUDA, "stream/event creation failed");
   if (!rc && fish_setup_kernels() != cudaSuccess)
     rc = fail(ctx, CUP2D_ECUDA, "shared-memory limits of the fish kernels could not be set");
@@ -305,7 +327,7 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   for (int b = 0; b < 2; b++) for (int d = 0; d < 2; d++) cudaFree(c.vel[b][d]);
   cudaFree(c.chi); cudaFree(c.pres); cudaFree(c.rhs); cudaFree(c.sdf);
   cudaFree(c.udefx); cudaFree(c.udefy); cudaFree(c.dsc); cudaFree(c.dshapes);
-  cudaFree(c.counters); cudaFree(c.partials); cudaFree(c.maxParts);
+  cudaFree(c.counters); cudaFree(c.partials);
   if (c.side) cudaStreamDestroy(c.side);
   if (c.side2) cudaStreamDestroy(c.side2);
   if (c.evObj) cudaEventDestroy(c.evObj);
@@ -315,6 +337,7 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   if (c.evPres) cudaEventDestroy(c.evPres);
   if (c.evMom) cudaEventDestroy(c.evMom);
   if (c.evPlaced) cudaEventDestroy(c.evPlaced);
+  if (c.evMaxFree) cudaEventDestroy(c.evMaxFree);
   for (auto& t : c.tiles) {
     cudaFree(t.tiles); cudaFree(t.slot); cudaFree(t.chi); cudaFree(t.dist); cudaFree(t.udx);
     cudaFree(t.udy); cudaFree(t.sD); cudaFree(t.sdx); cudaFree(t.sdy);
@@ -458,11 +481,6 @@ int cup2d_init(cup2d_ctx* ctx) {
   cudaFree(c.partials);
   c.npartials = (size_t)3 * c.g.nblocks + 4096 + (size_t)MAX_SHAPES * c.maxCapacity * 24;
   int rc = dalloc(ctx, &c.partials, c.npartials);
-  if (rc) return rc;
-  cudaFree(c.maxParts);
-  c.maxParts = nullptr;
-  c.nMaxParts = c.g.nblocks + c.nshapes * (c.maxCapacity < c.sms ? c.maxCapacity : c.sms);
-  rc = dalloc(ctx, &c.maxParts, (size_t)c.g.nblocks + (size_t)MAX_SHAPES * c.sms);
   if (rc) return rc;
   c.cur = 0;
   // Simulation::reset (Simulation.cpp:232-241): resetAll, IC, objects at t=0, ApplyObjVel

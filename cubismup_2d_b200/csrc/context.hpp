@@ -37,10 +37,7 @@ struct Ctx {
   // reduction scratch: per-CTA partial sums and "last CTA" tickets
   double* partials = nullptr;
   size_t npartials = 0;
-  // per-CTA maxima of the next step's findMaxU: [nblocks] from the pressure
-  // correction, then [MAX_SHAPES][sms] from the force pass
-  double* maxParts = nullptr;
-  int nMaxParts = 0;
+
   unsigned* counters = nullptr;
   static constexpr int NCOUNTERS = 256;
 
@@ -51,6 +48,8 @@ struct Ctx {
   cudaEvent_t evPres = nullptr, evMom = nullptr;
   cudaEvent_t evPlaced = nullptr;   // recorded after the obstacle tiles are placed
   bool recordPlaced = false;
+  cudaEvent_t evMaxFree = nullptr;  // the next step's speed maximum over free cells
+  bool graphStep = false;           // enqueue_step is recording a graph step
 
   cudaGraphExec_t graph = nullptr;
   long long launches = 0;

@@ -39,19 +39,13 @@ __global__ void k_end_step(Scalars* sc) { pdl_begin(); CUP2D_TRACE_SCOPE(TR_ENDS
 }
 
 // End of a graph step: t += dt, step += 1, then the next step's
-// calcMaxTimestep from the maxima left by the pressure correction (cells
-// without obstacle) and the force pass (obstacle cells after penalization).
-// max is exact in any order, so dtNext equals what k_max_u_dt would form.
-__global__ void __launch_bounds__(256)
-k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh, const double* maxParts, int nParts)
+// calcMaxTimestep from the maximum k_max_next formed on the final velocity
+// (max is exact in any order: dtNext equals what k_max_u_dt would form).
+__global__ void k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_ENDSTEP);
-  __shared__ double red[32];
-  double m = 0.0;
-  for (int i = threadIdx.x; i < nParts; i += blockDim.x) m = fmax(m, maxParts[i]);
-  m = block_max(m, red);
-  if (threadIdx.x != 0) return;
+  const double m = sc->maxNext;
   sc->time += sc->dt;
   sc->step += 1;
   sc->dtNext = dt_from_max_u(g, sc, sh, nsh, m);
@@ -161,37 +155,51 @@ k_rhs_div(GridDesc g, const Scalars* sc, const double* __restrict__ u,
 // PressureSingle.cpp:216-241: V += -(dt/2h) grad_2h P; zero-gradient P ghosts.
 // Reads the velocity written by advDiff (ui, vi) and writes the current one.
 __global__ void __launch_bounds__(256)
-k_pcorr(GridDesc g, Scalars* sc, const double* __restrict__ p,
+k_pcorr(GridDesc g, const Scalars* sc, const double* __restrict__ p,
         const double* __restrict__ ui, const double* __restrict__ vi,
-        double* __restrict__ uo, double* __restrict__ vo,
-        const double* __restrict__ chig, double* maxParts)
+        double* __restrict__ uo, double* __restrict__ vo)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_PCORR);
-  __shared__ double red[32];
   const double pFac = -0.5 * sc->dt / g.h;
-  const double UINF = sc->uinfx, VINF = sc->uinfy;
   const int nx = g.nx, ny = g.ny;
   const int gx = blockIdx.x * BS + threadIdx.x;
-  double m = 0.0;
-  int bad = 0;
 #pragma unroll
   for (int r = 0; r < 4; r++) {
     const int gy = blockIdx.y * BS + threadIdx.y + 8 * r;
     const size_t c = (size_t)gy * nx + gx;
     const double pW = p[gx > 0 ? c - 1 : c], pE = p[gx < nx - 1 ? c + 1 : c];
     const double pS = p[gy > 0 ? c - nx : c], pN = p[gy < ny - 1 ? c + nx : c];
-    const double un = ui[c] + pFac * (pE - pW), vn = vi[c] + pFac * (pN - pS);
-    uo[c] = un;
-    vo[c] = vn;
-    // next step's findMaxU over the cells penalization leaves alone (chi = 0)
-    if (!(chig[c] > 0)) m = fmax(m, cell_speed(un, vn, UINF, VINF));
-    bad |= !isfinite(un) || !isfinite(vn);
+    uo[c] = ui[c] + pFac * (pE - pW);
+    vo[c] = vi[c] + pFac * (pN - pS);
+  }
+}
+
+// The next step's findMaxU (Helpers.cpp:136-176) on the step's final
+// velocity, beside the force pass (which only reads it).  Per-CTA maxima
+// meet in sc->maxNext by exact atomic max.
+__global__ void __launch_bounds__(256)
+k_max_next(GridDesc g, Scalars* sc, const double* __restrict__ u, const double* __restrict__ v)
+{
+  pdl_begin();
+  CUP2D_TRACE_SCOPE(TR_MAXNEXT);
+  __shared__ double red[32];
+  const double UINF = sc->uinfx, VINF = sc->uinfy;
+  double m = 0.0;
+  int bad = 0;
+  const size_t n2 = (size_t)g.nx * g.ny / 2;
+  const double2* u2 = reinterpret_cast<const double2*>(u);
+  const double2* v2 = reinterpret_cast<const double2*>(v);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 a = u2[i], b = v2[i];
+    m = fmax(m, cell_speed(a.x, b.x, UINF, VINF));
+    m = fmax(m, cell_speed(a.y, b.y, UINF, VINF));
+    bad |= !isfinite(a.x) || !isfinite(b.x) || !isfinite(a.y) || !isfinite(b.y);
   }
   m = block_max(m, red);
   const int anyBad = __syncthreads_or(bad);
   if (lin_tid() == 0) {
-    maxParts[blockIdx.x + gridDim.x * blockIdx.y] = m;
+    atomic_max_double(&sc->maxNext, m);
     if (anyBad) atomicOr(&sc->status, ST_NAN);
   }
 }
@@ -303,8 +311,13 @@ void launch_end_step(Ctx& c) {
   CUP2D_LAUNCHED(c);
 }
 
+void launch_max_next(Ctx& c) {
+  launch_k(k_max_next, max_grid(c), 256, 0, c.stream, c.g, c.dsc, c.u(), c.v());
+  CUP2D_LAUNCHED(c);
+}
+
 void launch_end_step_dt(Ctx& c) {
-  launch_k(k_end_step_dt, 1, 256, 0, c.stream, c.g, c.dsc, c.dshapes, c.nshapes, c.maxParts, c.nMaxParts);
+  launch_k(k_end_step_dt, 1, 1, 0, c.stream, c.g, c.dsc, c.dshapes, c.nshapes);
   CUP2D_LAUNCHED(c);
 }
 
@@ -339,8 +352,7 @@ void launch_fade_sums(Ctx& c) {
 
 void launch_pcorr(Ctx& c) {
   dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
-  launch_k(k_pcorr, grid, block, 0, c.stream, c.g, c.dsc, c.pres, c.u(), c.v(), c.uo(), c.vo(),
-           c.chi, c.maxParts);
+  launch_k(k_pcorr, grid, block, 0, c.stream, c.g, c.dsc, c.pres, c.u(), c.v(), c.uo(), c.vo());
   CUP2D_LAUNCHED(c);
   c.cur = 1 - c.cur;
 }

@@ -50,6 +50,9 @@ struct Scalars {
   // dtNextValid is cleared by every host-side change of the state
   double dtNext, maxUNext;
   int dtNextValid;
+  // the next step's findMaxU maximum over the final velocity of a graph
+  // step, accumulated by exact atomic max; reset at the start of the step
+  double maxNext;
 };
 
 struct ShapeCfg {
@@ -151,7 +154,7 @@ enum TraceId : int {
   TR_OBJBEGIN, TR_DISK_PLACE, TR_RASTER_DISK, TR_CHI, TR_MOMENTS,
   TR_UDEF, TR_RHSOBST, TR_RHSCORR, TR_MOMENTA, TR_COLLIDE, TR_PENALIZE, TR_FORCES,
   TR_MIDLINE, TR_FRAME, TR_RASTER, TR_R2C, TR_COLS, TR_C2R, TR_DCT_FWD, TR_DCT_COLS,
-  TR_DCT_INV, TR_SELECT, TR_N
+  TR_DCT_INV, TR_SELECT, TR_MAXNEXT, TR_N
 };
 // per-work-item phase stamps of the trace build: slot 2*TR_N + 8*item + phase
 constexpr int TRACE_ITEMS = 4096;

@@ -33,6 +33,7 @@ void launch_fade_sums(Ctx& c);                       // PoissonSolver.cpp:61-100
 void launch_pcorr(Ctx& c);                           // PressureSingle.cpp:216-241
 void launch_end_step(Ctx& c);                        // Simulation.cpp:289-290
 void launch_end_step_dt(Ctx& c);                     // the same + the next step's calcMaxTimestep
+void launch_max_next(Ctx& c);                        // its findMaxU on the final velocity
 void launch_ic(Ctx& c);                              // Helpers.cpp:38-82
 void launch_apply_obj_vel(Ctx& c);                   // Helpers.cpp:290-307
 

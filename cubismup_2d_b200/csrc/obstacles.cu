@@ -57,6 +57,7 @@ k_step_begin(GridDesc g, Scalars* sc, DevShape* sh, int nsh, AllTiles T, double*
   __shared__ double red[64];
   prefetch_region(pf, blockIdx.x);
   clear_old_tiles(g, sh, nsh, T.t, chi, sdf, blockIdx.x, gridDim.x);
+  if (blockIdx.x == 0 && threadIdx.x == 0) sc->maxNext = 0.0;
   if (sc->dtNextValid) {
     // calcMaxTimestep was formed at the end of the previous graph step from
     // this very state (any host-side change since would have cleared the flag)
@@ -546,10 +547,9 @@ k_penalize(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __r
 // (Shape.cpp:252-282): per surface point traction, 17 sums per tile, then
 // the fixed-order sum over tiles and the derived powers/efficiencies.
 __global__ void __launch_bounds__(1024)
-k_forces(GridDesc g, Scalars* sc, DevShape* sh, AllTiles T, const double* __restrict__ u,
+k_forces(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ u,
          const double* __restrict__ v, const double* __restrict__ p,
-         double* partials, int partStride, unsigned* counters,
-         const double* __restrict__ chig, double* maxParts)
+         double* partials, int partStride, unsigned* counters)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_FORCES);
@@ -558,21 +558,7 @@ k_forces(GridDesc g, Scalars* sc, DevShape* sh, AllTiles T, const double* __rest
   DevShape& S = sh[k];
   const ObstTiles& t = T.t[k];
   double* part = partials + (size_t)k * partStride;
-  // next step's findMaxU over this shape's obstacle cells (chi > 0), which
-  // penalization has just set; the pressure correction covered the rest
-  const double UINF = sc->uinfx, VINF = sc->uinfy;
-  double mU = 0.0;
-  int bad = 0;
   for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
-  {
-    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
-    const size_t c = (size_t)(by * BS + threadIdx.y) * g.nx + bx * BS + threadIdx.x;
-    if (chig[c] > 0) {
-      const double uc = u[c], vc = v[c];
-      mU = fmax(mU, cell_speed(uc, vc, UINF, VINF));
-      bad |= !isfinite(uc) || !isfinite(vc);
-    }
-  }
   double F[NFORCE];
 #pragma unroll
   for (int q = 0; q < NFORCE; q++) F[q] = 0;
@@ -626,12 +612,6 @@ k_forces(GridDesc g, Scalars* sc, DevShape* sh, AllTiles T, const double* __rest
   }
   block_sum<NFORCE>(F, red);
   if (lin_tid() == 0) for (int q = 0; q < NFORCE; q++) part[NFORCE * s + q] = F[q];
-  }
-  mU = block_max(mU, red);
-  const int anyBad = __syncthreads_or(bad);
-  if (lin_tid() == 0) {
-    maxParts[g.nblocks + blockIdx.y * gridDim.x + blockIdx.x] = mU;
-    if (anyBad) atomicOr(&sc->status, ST_NAN);
   }
   if (!last_block_done(counters + k, gridDim.x)) return;
   double tot[NFORCE];
@@ -781,8 +761,8 @@ void launch_forces(Ctx& c) {
   if (c.nshapes == 0) return;
   const AllTiles T = all_tiles(c);
   launch_k(k_forces, dim3(tile_ctas(c, c.maxCapacity), c.nshapes), dim3(32, 32), 0, c.stream,
-      c.g, c.dsc, c.dshapes, T, c.u(), c.v(), c.pres, shape_partials(c), (int)shape_region(c),
-      c.counters + CNT_FORCES, c.chi, c.maxParts);
+      c.g, c.dshapes, T, c.u(), c.v(), c.pres, shape_partials(c), (int)shape_region(c),
+      c.counters + CNT_FORCES);
   CUP2D_LAUNCHED(c);
 }
 

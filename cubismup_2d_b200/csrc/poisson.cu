@@ -56,15 +56,23 @@ __device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
 // element per 16, plus 4 so that consecutive sequences start in different
 // halves of the shared-memory banks), the staged quarter twiddle table
 // (w^j, j < L/4), the sequences per CTA B and the threads per CTA NT
-// (L/16 per sequence: every thread owns 16 elements of a pass).
-template <int L> struct Len {
+// (L/E per sequence: every thread owns E = 16 or 8 elements of a pass).
+template <int L, int E = 16> struct Len {
   static constexpr int SL = L + L / 16 + 4;
   static constexpr int TW = L / 4;
   static constexpr int B = 2048 / L < 1 ? 1 : (2048 / L > 8 ? 8 : 2048 / L);
-  static constexpr int NT0 = B * L / 16;
+  static constexpr int NT0 = B * L / E;
   static constexpr int NT = NT0 < 64 ? 64 : (NT0 > 512 ? 512 : NT0);
-  static constexpr int MINB = 65536 / (NT * 128) < 1 ? 1 : 65536 / (NT * 128);   // <= 128 registers
+  static constexpr int REGS = E == 16 ? 128 : 64;   // register budget per thread
+  static constexpr int MINB = 65536 / (NT * REGS) < 1 ? 1 : 65536 / (NT * REGS);
 };
+// elements per thread of the forward row pass (few rows: twice the threads
+// of E = 16 for latency hiding, at one more shared-memory pass; measured
+// faster), of the inverse row pass and of the column pass (measured faster
+// with E = 16)
+constexpr int E_ROWS = 8;
+constexpr int E_C2R = 16;
+constexpr int E_COLS = 16;
 
 // Twiddles w^j = exp(-2 pi i j / L), j < L/4, staged in shared memory.
 template <int L>
@@ -174,10 +182,10 @@ template <> __device__ __forceinline__ void dft<16, true>(double2* x) { dft16<tr
 // output q at (j - k) R + k + q NS.  Thread t of a sequence owns the 16/R
 // butterflies t + u L/16.  Loads go to registers before the barrier,
 // stores after it, so one buffer suffices.
-template <int L, int R, int NS, bool INV, bool HIN, bool HOUT>
+template <int L, int R, int NS, bool INV, bool HIN, bool HOUT, int E>
 __device__ __forceinline__ void fft_pass(double2* A, int nseq, const double2* tws)
 {
-  constexpr int SL = Len<L>::SL, T = L / 16, NB = 16 / R, Q = L / R;
+  constexpr int SL = Len<L>::SL, T = L / E, NB = E / R, Q = L / R;
   // first pass of an input whose upper half is zero: inputs m >= R/2 sit at
   // indices >= L/2 (then NB == 1); last pass of which only the lower half of
   // the output is kept: outputs q >= R/2 land at indices >= L/2
@@ -186,7 +194,7 @@ __device__ __forceinline__ void fft_pass(double2* A, int nseq, const double2* tw
   const bool act = tid < nseq * T;
   const int sq = act ? tid / T : 0, j = tid - sq * T;
   double2* a = A + sq * SL;
-  double2 x[16];
+  double2 x[E];
   if (act) {
 #pragma unroll
     for (int u = 0; u < NB; u++)
@@ -214,26 +222,26 @@ __device__ __forceinline__ void fft_pass(double2* A, int nseq, const double2* tw
   __syncthreads();
 }
 
-template <int L, int NS, bool INV, bool HIN, bool HOUT>
+template <int L, int NS, bool INV, bool HIN, bool HOUT, int E>
 __device__ __forceinline__ void fft_passes(double2* A, int nseq, const double2* tws) {
-  if constexpr (NS * 16 <= L) {
-    fft_pass<L, 16, NS, INV, HIN, HOUT>(A, nseq, tws);
-    fft_passes<L, NS * 16, INV, HIN, HOUT>(A, nseq, tws);
+  if constexpr (NS * E <= L) {
+    fft_pass<L, E, NS, INV, HIN, HOUT, E>(A, nseq, tws);
+    fft_passes<L, NS * E, INV, HIN, HOUT, E>(A, nseq, tws);
   } else if constexpr (NS < L) {
-    fft_pass<L, L / NS, NS, INV, HIN, HOUT>(A, nseq, tws);
+    fft_pass<L, L / NS, NS, INV, HIN, HOUT, E>(A, nseq, tws);
   }
 }
 
 // In-place Stockham autosort FFT of nseq sequences of length L (A + q*SL,
 // padded indexing; a power of two >= 16): radix-16 passes and one radix
 // 2/4/8 pass for the remaining factor.  Forward exp(-2 pi i jk/L), inverse
-// exp(+...), unnormalised.  Needs blockDim.x >= nseq * L/16.  HIN: the
+// exp(+...), unnormalised.  Needs blockDim.x >= nseq * L/E.  HIN: the
 // upper half of the input is zero and never read; HOUT: only the lower half
 // of the output is written.
-template <int L, bool INV, bool HIN = false, bool HOUT = false>
+template <int L, bool INV, bool HIN = false, bool HOUT = false, int E = 16>
 __device__ void fft_inplace(double2* A, int nseq, const double2* tws)
 {
-  fft_passes<L, 1, INV, HIN, HOUT>(A, nseq, tws);
+  fft_passes<L, 1, INV, HIN, HOUT, E>(A, nseq, tws);
 }
 
 struct FadeArgs {
@@ -264,14 +272,14 @@ __device__ __forceinline__ double fade_cell(const GridDesc& g, int gx, int gy, d
 // grid (FFTW_freespace.cpp:108-119) computed on the fly.  Each row of 2L
 // reals is the complex sequence (x[2n], x[2n+1]) of length L.
 template <int L, bool HIN>
-__global__ void __launch_bounds__(Len<L>::NT, Len<L>::MINB)
+__global__ void __launch_bounds__(Len<L, E_ROWS>::NT, Len<L, E_ROWS>::MINB)
 k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
            double2* __restrict__ out, int outStride,
            const double2* __restrict__ tw, int twLen, FadeArgs fa, double h, int Nx, int Ny)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_R2C);
-  constexpr int SL = Len<L>::SL, RB = Len<L>::B, NT = Len<L>::NT;
+  constexpr int SL = Len<L, E_ROWS>::SL, RB = Len<L, E_ROWS>::B, NT = Len<L, E_ROWS>::NT;
   extern __shared__ double2 sm[];
   double2* A = sm;
   double2* tws = sm + RB * SL;
@@ -339,7 +347,7 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
     }
     __syncthreads();
   }
-  fft_inplace<L, false, HIN>(A, nb, tws);
+  fft_inplace<L, false, HIN, false, E_ROWS>(A, nb, tws);
   // even/odd split: X[k] = Fe[k] + W^k Fo[k], W = exp(-i pi / L), k in [0, L]
   const int twStep = twLen / (2 * L);
   for (int idx = threadIdx.x; idx < nb * (L + 1); idx += NT) {
@@ -359,14 +367,14 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
 // mode 2: forward, periodic multiplier -1/|k|^2 / (MX MY), inverse
 // Rows r >= nrowsIn of the input are zero and never read.
 template <int L, bool FS>
-__global__ void __launch_bounds__(Len<L>::NT, Len<L>::MINB)
+__global__ void __launch_bounds__(Len<L, E_COLS>::NT, Len<L, E_COLS>::MINB)
 k_cols(double2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrowsOut,
        const double* __restrict__ ghatIn, double* __restrict__ ghatOut, int mode,
        const double2* __restrict__ tw, int twLen, double norm, int MXp, int MYp)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_COLS);
-  constexpr int SL = Len<L>::SL, CB = Len<L>::B, NT = Len<L>::NT, GR = L / 2 + 1;
+  constexpr int SL = Len<L, E_COLS>::SL, CB = Len<L, E_COLS>::B, NT = Len<L, E_COLS>::NT, GR = L / 2 + 1;
   extern __shared__ double2 sm[];
   double2* A = sm;
   double2* tws = sm + CB * SL;
@@ -394,7 +402,7 @@ k_cols(double2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrows
   load_twiddles<L>(tws, tw, twLen);
   cp_async_wait<1>();          // the columns (the kernel rows may still be in flight)
   __syncthreads();
-  fft_inplace<L, false, FS>(A, nb, tws);
+  fft_inplace<L, false, FS, false, E_COLS>(A, nb, tws);
   if (mode == 1) {
     for (int idx = threadIdx.x; idx < CB * nrowsOut; idx += NT) {
       const int r = idx / CB, j = idx & (CB - 1);
@@ -425,7 +433,7 @@ k_cols(double2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrows
     A[j * SL + pad(r)] = make_double2(z.x * f, z.y * f);
   }
   __syncthreads();
-  fft_inplace<L, true, false, FS>(A, nb, tws);
+  fft_inplace<L, true, false, FS, E_COLS>(A, nb, tws);
   for (int idx = threadIdx.x; idx < CB * nrowsOut; idx += NT) {
     const int r = idx / CB, j = idx & (CB - 1);
     if (j < nb) data[(size_t)r * stride + c0 + j] = A[j * SL + pad(r)];
@@ -434,13 +442,13 @@ k_cols(double2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrows
 
 // inverse real FFT of length 2L from X[0..L]; writes the first ncolsOut values
 template <int L, bool HOUT>
-__global__ void __launch_bounds__(Len<L>::NT, Len<L>::MINB)
+__global__ void __launch_bounds__(Len<L, E_C2R>::NT, Len<L, E_C2R>::MINB)
 k_rows_c2r(const double2* __restrict__ in, int inStride, int nrows, double* __restrict__ out,
            int outStride, int ncolsOut, const double2* __restrict__ tw, int twLen)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_C2R);
-  constexpr int SL = Len<L>::SL, RB = Len<L>::B, NT = Len<L>::NT, H = L / 2;
+  constexpr int SL = Len<L, E_C2R>::SL, RB = Len<L, E_C2R>::B, NT = Len<L, E_C2R>::NT, H = L / 2;
   extern __shared__ double2 sm[];
   double2* A = sm;
   double2* tws = sm + RB * SL;
@@ -482,7 +490,7 @@ k_rows_c2r(const double2* __restrict__ in, int inStride, int nrows, double* __re
     a[pad(kk[1])] = res[1];
   }
   __syncthreads();
-  fft_inplace<L, true, false, HOUT>(A, nb, tws);
+  fft_inplace<L, true, false, HOUT, E_C2R>(A, nb, tws);
   const int half = (ncolsOut + 1) / 2;
   for (int idx = threadIdx.x; idx < nb * half; idx += NT) {
     const int r = idx / half, n = idx - r * half;
@@ -692,9 +700,9 @@ bool rows_r2c(int L, cudaStream_t st, const double* in, int inStride, int nrows,
               bool halfIn) {
   switch (L) {
 #define X(LL) case LL: \
-    if (halfIn) launch_k(k_rows_r2c<LL, true>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st,  \
+    if (halfIn) launch_k(k_rows_r2c<LL, true>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_ROWS>::NT, smem_for<LL>(), st,  \
         in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, Nx, Ny); \
-    else launch_k(k_rows_r2c<LL, false>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st,  \
+    else launch_k(k_rows_r2c<LL, false>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_ROWS>::NT, smem_for<LL>(), st,  \
         in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, Nx, Ny); \
     return true;
     CUP2D_FFT_LENGTHS(X)
@@ -707,10 +715,10 @@ bool cols(int L, cudaStream_t st, double2* data, int stride, int ncols, int nrow
           double* ghat, int mode, const double2* tw, int twLen, double norm, int MXp, int MYp) {
   switch (L) {
 #define X(LL) case LL: \
-    if (mode == 0) launch_k(k_cols<LL, true>, (ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, \
+    if (mode == 0) launch_k(k_cols<LL, true>, (ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_COLS>::NT, \
         smem_for<LL>((size_t)(LL / 2 + 1) * Len<LL>::B), st, data, stride, ncols, nrowsIn, \
         nrowsOut, ghat, ghat, mode, tw, twLen, norm, MXp, MYp); \
-    else launch_k(k_cols<LL, false>, (ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, \
+    else launch_k(k_cols<LL, false>, (ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_COLS>::NT, \
         smem_for<LL>((size_t)(LL / 2 + 1) * Len<LL>::B), st, data, stride, ncols, nrowsIn, \
         nrowsOut, ghat, ghat, mode, tw, twLen, norm, MXp, MYp); \
     return true;
@@ -724,9 +732,9 @@ bool rows_c2r(int L, cudaStream_t st, const double2* in, int inStride, int nrows
               int ncolsOut, const double2* tw, int twLen, bool halfOut) {
   switch (L) {
 #define X(LL) case LL: \
-    if (halfOut) launch_k(k_rows_c2r<LL, true>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st,  \
+    if (halfOut) launch_k(k_rows_c2r<LL, true>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_C2R>::NT, smem_for<LL>(), st,  \
         in, inStride, nrows, out, outStride, ncolsOut, tw, twLen); \
-    else launch_k(k_rows_c2r<LL, false>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL>::NT, smem_for<LL>(), st,  \
+    else launch_k(k_rows_c2r<LL, false>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_C2R>::NT, smem_for<LL>(), st,  \
         in, inStride, nrows, out, outStride, ncolsOut, tw, twLen); \
     return true;
     CUP2D_FFT_LENGTHS(X)

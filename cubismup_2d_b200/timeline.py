@@ -26,7 +26,7 @@ KERNELS = ["step_begin/max_u", "set_dt", "end_step", "advdiff", "rhs_div", "pcor
            "obj_begin", "disk_place", "raster_disk", "chi", "moments", "udef_grid",
            "rhs_obst", "rhs_corr", "momenta", "collide", "penalize", "forces", "fish_midline",
            "fish_frame", "fish_raster", "rows_r2c", "cols", "rows_c2r", "dct_rows_fwd", "dct_cols",
-           "dct_rows_inv", "fish_tile_search"]
+           "dct_rows_inv", "fish_tile_search", "max_next"]
 TRACE_ITEMS = 4096
 WORKLOADS = {"swimmer": SWIMMER_1024x512, "cylinder": FORCED_CYLINDER_RE100}
 
