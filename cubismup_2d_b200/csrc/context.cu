@@ -176,13 +176,15 @@ void launch_pressure_tail(Ctx& c) {
 
 // One pass of Simulation::simulate's loop body (Simulation.cpp:245-251) as a
 // graph with three branches:
-//   main : dt + reset of last step's tiles + body motion -> advDiff (with
-//          outflow), RHS divergence -> [join obstacles] -> RHS obstacle
-//          terms, fade, Poisson -> pressure correction [beside momenta on
-//          side2] -> collisions, penalization, forces -> [join midline] -> t += dt
+//   main : dt + reset of last step's tiles + body motion -> fish frames and
+//          tile search, rasters, Towers chi, moments -> [join side2] -> RHS
+//          obstacle terms, fade, Poisson -> momentum integrals [beside the
+//          pressure correction on side2] -> collisions, penalization, forces
+//          -> [join side, side2] -> t += dt and the next step's dt
 //   side : the fish midlines of the next step (they depend on time only)
-//   side2: obstacle tiles, SDF, Towers chi, moments (advDiff does not read
-//          them); later the momentum integrals
+//   side2: advDiff (with outflow) and the RHS divergence once the tiles are
+//          placed (advDiff reads no obstacle data); later the pressure
+//          correction, then the next step's findMaxU beside the force pass
 void enqueue_step(Ctx& c) {
   struct GraphStepFlag { Ctx& c; explicit GraphStepFlag(Ctx& cc) : c(cc) { c.graphStep = true; }
                          ~GraphStepFlag() { c.graphStep = false; } } flag(c);
@@ -196,22 +198,23 @@ void enqueue_step(Ctx& c) {
       if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.side, 1);
     cudaEventRecord(c.evJoin, c.side);
   }
-  cudaEventRecord(c.evObj, c.stream);
-  cudaStreamWaitEvent(c.side2, c.evObj, 0);
+  // the obstacle chain, the step's critical path, stays on the main stream
+  // (programmatic launches chain only within a stream)
+  c.recordPlaced = c.nshapes > 0;
+  if (!c.recordPlaced) cudaEventRecord(c.evPlaced, c.stream);
+  launch_objects_rest(c);
+  c.recordPlaced = false;
+  // advDiff and the RHS divergence beside it, once the tiles are placed: the
+  // placement kernels are single-CTA latency chains that a full-GPU kernel
+  // beside them slows, while the rasters after them leave most SMs free
+  cudaStreamWaitEvent(c.side2, c.evPlaced, 0);
   {
     StreamScope scope(c, c.side2);
-    c.recordPlaced = c.nshapes > 0;
-    launch_objects_rest(c);
-    c.recordPlaced = false;
+    launch_advdiff(c);
+    launch_outflow(c);
+    launch_rhs_div(c);
   }
   cudaEventRecord(c.evObjDone, c.side2);
-  // advDiff starts once the tiles are placed: the placement kernels are
-  // single-CTA latency chains that a full-GPU kernel beside them slows,
-  // while the rasters after them leave most SMs free
-  if (c.nshapes > 0) cudaStreamWaitEvent(c.stream, c.evPlaced, 0);
-  launch_advdiff(c);
-  launch_outflow(c);
-  launch_rhs_div(c);
   cudaStreamWaitEvent(c.stream, c.evObjDone, 0);
   launch_rhs_obstacles(c);
   launch_fade_sums(c);
@@ -267,7 +270,14 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
   if (cudaSetDevice(c.device) != cudaSuccess) { delete ctx; return CUP2D_ECUDA; }
   cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, c.device);
   if (c.sms <= 0) c.sms = 1;
-  if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return CUP2D_ECUDA; }
+  // the main stream carries the step's critical path (the obstacle chain):
+  // its CTAs go first when side-branch kernels compete for the SMs (graph
+  // kernel nodes keep the stream priority)
+  int prLeast = 0, prGreatest = 0;
+  cudaDeviceGetStreamPriorityRange(&prLeast, &prGreatest);
+  if (cudaStreamCreateWithPriority(&c.stream, cudaStreamNonBlocking, prGreatest) != cudaSuccess) {
+    delete ctx; return CUP2D_ECUDA;
+  }
   GridDesc& g = c.g;
   g.bpdx = cfg->bpdx; g.bpdy = cfg->bpdy;
   g.nx = BS * g.bpdx; g.ny = BS * g.bpdy; g.nblocks = g.bpdx * g.bpdy;
@@ -291,12 +301,8 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
   if (!rc) rc = dalloc(ctx, &c.dsc, 1);
   if (!rc) rc = dalloc(ctx, &c.dshapes, MAX_SHAPES);
   if (!rc) rc = dalloc(ctx, &c.counters, Ctx::NCOUNTERS);
-  // the obstacle branch is the step's critical path: its CTAs go first when
-  // advDiff's compete for the SMs (kernel nodes keep the stream priority)
-  int prLeast = 0, prGreatest = 0;
-  cudaDeviceGetStreamPriorityRange(&prLeast, &prGreatest);
   if (!rc && (cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking) != cudaSuccess ||
-              cudaStreamCreateWithPriority(&c.side2, cudaStreamNonBlocking, prGreatest) != cudaSuccess ||
+              cudaStreamCreateWithFlags(&c.side2, cudaStreamNonBlocking) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evFork, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evJoin, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evObj, cudaEventDisableTiming) != cudaSuccess ||
