@@ -57,6 +57,7 @@ k_fish_midline(const Scalars* sc, const DevShape* sh, int k, FishArrays F, int m
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_MIDLINE);
+  CUP2D_TRACE_MARK(TRACE_ITEMS - 3, 0);
   extern __shared__ double smem[];
   __shared__ double red[32 * 5];
   __shared__ double bc[4];
@@ -73,6 +74,7 @@ k_fish_midline(const Scalars* sc, const DevShape* sh, int k, FishArrays F, int m
   double* vNorX = norY + Nm;  double* vNorY = vNorX + Nm;
   for (int i = tid; i < Nm; i += nt) { rS[i] = F.rS[i]; width[i] = F.width[i]; }
   __syncthreads();
+  CUP2D_TRACE_MARK(TRACE_ITEMS - 3, 1);
 
   if (S.cfg.kind == CUP2D_SHAPE_STEFANFISH) {
     // curvature scheduler: after transition(0, 0, T, zeros, values) the start
@@ -94,6 +96,7 @@ k_fish_midline(const Scalars* sc, const DevShape* sh, int k, FishArrays F, int m
       vK[i] = amp * (vC * (sin(arg) + rB + fac) + rC * (cos(arg) * darg + vB + dif));
     }
     __syncthreads();
+  CUP2D_TRACE_MARK(TRACE_ITEMS - 3, 2);
     if (tid == 0) {                                     // IF2D_Frenet2D::solve
       const double* curv = rK; const double* curv_dt = vK;
       rX[0] = 0.0; rY[0] = 0.0;
@@ -140,6 +143,7 @@ k_fish_midline(const Scalars* sc, const DevShape* sh, int k, FishArrays F, int m
       }
     }
     __syncthreads();
+  CUP2D_TRACE_MARK(TRACE_ITEMS - 3, 3);
   } else {
     // AmplitudeFish::computeMidline (CarlingFish.cpp:70-107)
     const double phaseShift = S.cfg.phaseShift;
@@ -209,11 +213,13 @@ k_fish_midline(const Scalars* sc, const DevShape* sh, int k, FishArrays F, int m
       bc[0] = integ[1]; bc[1] = integ[2]; bc[2] = integ[3]; bc[3] = integ[4];
     }
     __syncthreads();
+  CUP2D_TRACE_MARK(TRACE_ITEMS - 3, 4);
   }
   for (int i = tid; i < Nm; i += nt) {                  // changeToCoMFrameLinear
     rX[i] -= bc[0]; rY[i] -= bc[1]; vX[i] -= bc[2]; vY[i] -= bc[3];
   }
   __syncthreads();
+  CUP2D_TRACE_MARK(TRACE_ITEMS - 3, 5);
   {                                                     // integrateAngularMomentum
     double a[2] = {0, 0};
     for (int i = tid; i < Nm; i += nt) {

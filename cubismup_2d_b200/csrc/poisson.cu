@@ -244,6 +244,79 @@ __device__ void fft_inplace(double2* A, int nseq, const double2* tws)
   fft_passes<L, 1, INV, HIN, HOUT, E>(A, nseq, tws);
 }
 
+// sub-transform size NS of the last pass of fft_inplace<L, ..., E>
+template <int L, int E> constexpr int last_ns() {
+  int ns = 1;
+  while (ns * E <= L) ns *= E;
+  return ns == L ? ns / E : ns;
+}
+// the passes of fft_passes<L, NS, ...> whose sub-transform size is below NSEND
+template <int L, int NS, int NSEND, bool INV, bool HIN, int E>
+__device__ __forceinline__ void fft_passes_below(double2* A, int nseq, const double2* tws) {
+  if constexpr (NS < NSEND) {
+    constexpr int R = NS * E <= L ? E : L / NS;
+    fft_pass<L, R, NS, INV, HIN, false, E>(A, nseq, tws);
+    fft_passes_below<L, NS * R, NSEND, INV, HIN, E>(A, nseq, tws);
+  }
+}
+
+// Spectral convolution of nseq sequences in place: fft_inplace<L, false,
+// HIN>, X[r] = mul(sequence, r, X[r]), fft_inplace<L, true, false, HOUT>.  The
+// last forward pass, the multiplier and the first inverse pass run in
+// registers: butterfly jb = j + u L/E of the last forward pass (radix R,
+// NS = L/R, no stride: k = jb) produces X[jb + q NS] = X[j + (u + (E/R) q)
+// L/E], which is input m = u + (E/R) q of thread j's radix-E first inverse
+// butterfly (NS = 1).  With L <= E (one pass each way) the three steps run
+// one after the other.
+template <int L, bool HIN, bool HOUT, int E, class Mul>
+__device__ __forceinline__ void fft_convolve(double2* A, int nseq, const double2* tws, Mul mul)
+{
+  constexpr int SL = Len<L>::SL, T = L / E, NS = last_ns<L, E>(), R = L / NS, NB = E / R;
+  if constexpr (L <= E) {
+    fft_inplace<L, false, HIN, false, E>(A, nseq, tws);
+    for (int idx = threadIdx.x; idx < nseq * L; idx += blockDim.x) {
+      const int sq = idx / L, r = idx - sq * L;
+      A[sq * SL + pad(r)] = mul(sq, r, A[sq * SL + pad(r)]);
+    }
+    __syncthreads();
+    fft_inplace<L, true, false, HOUT, E>(A, nseq, tws);
+    return;
+  }
+  fft_passes_below<L, 1, NS, false, HIN, E>(A, nseq, tws);
+  const int tid = threadIdx.x;
+  const bool act = tid < nseq * T;
+  const int sq = act ? tid / T : 0, j = tid - sq * T;
+  double2* a = A + sq * SL;
+  double2 x[E];
+  if (act) {
+#pragma unroll
+    for (int u = 0; u < NB; u++)
+#pragma unroll
+      for (int m = 0; m < R; m++) x[u * R + m] = a[pad(j + u * T + m * NS)];
+  }
+  __syncthreads();
+  if (act) {
+    double2 y[E];
+#pragma unroll
+    for (int u = 0; u < NB; u++) {
+      double2* xb = x + u * R;
+      const int jb = j + u * T;
+      if (jb) {
+#pragma unroll
+        for (int m = 1; m < R; m++) xb[m] = cmul(xb[m], twiddle<L, false>(tws, m * jb));
+      }
+      dft<R, false>(xb);
+#pragma unroll
+      for (int q = 0; q < R; q++) y[u + NB * q] = mul(sq, jb + q * NS, xb[out_reg<R>(q)]);
+    }
+    dft<E, true>(y);
+#pragma unroll
+    for (int q = 0; q < E; q++) a[pad(j * E + q)] = y[out_reg<E>(q)];
+  }
+  __syncthreads();
+  fft_passes<L, E, true, false, HOUT, E>(A, nseq, tws);
+}
+
 struct FadeArgs {
   int enabled;
   const Scalars* sc;
@@ -400,40 +473,36 @@ k_cols(double2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrows
       A[j * SL + pad(r)] = make_double2(0, 0);
     }
   load_twiddles<L>(tws, tw, twLen);
-  cp_async_wait<1>();          // the columns (the kernel rows may still be in flight)
-  __syncthreads();
-  fft_inplace<L, false, FS, false, E_COLS>(A, nb, tws);
   if (mode == 1) {
+    cp_async_wait<0>();
+    __syncthreads();
+    fft_inplace<L, false, FS, false, E_COLS>(A, nb, tws);
     for (int idx = threadIdx.x; idx < CB * nrowsOut; idx += NT) {
       const int r = idx / CB, j = idx & (CB - 1);
       if (j < nb) ghatOut[(size_t)r * stride + c0 + j] = A[j * SL + pad(r)].x * norm;
     }
     return;
   }
-  cp_async_wait<0>();
+  cp_async_wait<0>();          // the columns and the kernel rows
   __syncthreads();
-  for (int idx = threadIdx.x; idx < CB * L; idx += NT) {
-    const int r = idx / CB, j = idx & (CB - 1);
-    if (j >= nb) continue;
-    double f;
-    if (mode == 0) {
+  if (mode == 0) {
+    fft_convolve<L, FS, FS, E_COLS>(A, nb, tws, [&](int j, int r, double2 z) {
       const int ky = r <= L / 2 ? r : L - r;
-      f = Gs[ky * CB + j];
-    } else {
+      const double f = Gs[ky * CB + j];
+      return make_double2(z.x * f, z.y * f);
+    });
+  } else {
+    fft_convolve<L, FS, FS, E_COLS>(A, nb, tws, [&](int j, int r, double2 z) {
       // FFTW_periodic::_solve_spectral (FFTW_periodic.h:77-92)
       const int i = c0 + j;
+      if (i == 0 && r == 0) return make_double2(0, 0);
       const int kx = i <= MXp / 2 ? i : MXp - i, ky = r <= MYp / 2 ? r : MYp - r;
       const double waveFactX = 2 * M_PI / MXp, waveFactY = 2 * M_PI / MYp;
       const double rkx = kx * waveFactX, rky = ky * waveFactY;
-      const double kinv = -1 / (rkx * rkx + rky * rky);
-      f = (i == 0 && r == 0) ? 0.0 : kinv * norm;
-    }
-    double2 z = A[j * SL + pad(r)];
-    if (mode == 2 && c0 + j == 0 && r == 0) z = make_double2(0, 0);
-    A[j * SL + pad(r)] = make_double2(z.x * f, z.y * f);
+      const double f = -1 / (rkx * rkx + rky * rky) * norm;
+      return make_double2(z.x * f, z.y * f);
+    });
   }
-  __syncthreads();
-  fft_inplace<L, true, false, FS, E_COLS>(A, nb, tws);
   for (int idx = threadIdx.x; idx < CB * nrowsOut; idx += NT) {
     const int r = idx / CB, j = idx & (CB - 1);
     if (j < nb) data[(size_t)r * stride + c0 + j] = A[j * SL + pad(r)];
