@@ -178,7 +178,7 @@ void launch_pressure_tail(Ctx& c) {
 // graph with three branches:
 //   main : dt + reset of last step's tiles + body motion -> fish frames and
 //          tile search, rasters, Towers chi, moments -> [join side2] -> RHS
-//          obstacle terms, fade, Poisson -> momentum integrals [beside the
+//          obstacle terms, Poisson -> momentum integrals [beside the
 //          pressure correction on side2] -> collisions, penalization, forces
 //          -> [join side, side2] -> t += dt and the next step's dt
 //   side : the fish midlines of the next step (they depend on time only)
@@ -217,7 +217,6 @@ void enqueue_step(Ctx& c) {
   cudaEventRecord(c.evObjDone, c.side2);
   cudaStreamWaitEvent(c.stream, c.evObjDone, 0);
   launch_rhs_obstacles(c);
-  launch_fade_sums(c);
   poisson_solve(c);
   launch_pressure_tail(c);
   launch_forces(c);
@@ -333,7 +332,7 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   for (int b = 0; b < 2; b++) for (int d = 0; d < 2; d++) cudaFree(c.vel[b][d]);
   cudaFree(c.chi); cudaFree(c.pres); cudaFree(c.rhs); cudaFree(c.sdf);
   cudaFree(c.udefx); cudaFree(c.udefy); cudaFree(c.dsc); cudaFree(c.dshapes);
-  cudaFree(c.counters); cudaFree(c.partials);
+  cudaFree(c.counters); cudaFree(c.partials); cudaFree(c.fadeSlot);
   if (c.side) cudaStreamDestroy(c.side);
   if (c.side2) cudaStreamDestroy(c.side2);
   if (c.evObj) cudaEventDestroy(c.evObj);
@@ -488,6 +487,10 @@ int cup2d_init(cup2d_ctx* ctx) {
   c.npartials = (size_t)3 * c.g.nblocks + 4096 + (size_t)MAX_SHAPES * c.maxCapacity * 24;
   int rc = dalloc(ctx, &c.partials, c.npartials);
   if (rc) return rc;
+  cudaFree(c.fadeSlot);
+  c.fadeSlot = nullptr;
+  if ((rc = dalloc(ctx, &c.fadeSlot, (size_t)c.g.nblocks + 1))) return rc;
+  if ((c.nfade = build_fade_slots(c)) < 0) return fail(ctx, CUP2D_ECUDA, "fade strip table");
   c.cur = 0;
   // Simulation::reset (Simulation.cpp:232-241): resetAll, IC, objects at t=0, ApplyObjVel
   if ((rc = upload_scalars_reset(ctx))) return rc;
@@ -552,7 +555,6 @@ int cup2d_pressure_single(cup2d_ctx* ctx, double dt) {
   STAGE_PROLOGUE
   launch_rhs_div(c);
   launch_rhs_obstacles(c);
-  launch_fade_sums(c);
   poisson_solve(c);
   launch_pressure_tail(c);
   return check_launch(ctx);

@@ -37,6 +37,11 @@ struct Ctx {
   // reduction scratch: per-CTA partial sums and "last CTA" tickets
   double* partials = nullptr;
   size_t npartials = 0;
+  // blocks that reach the fade strip: fadeSlot[block] = rank among them in
+  // block order, or -1 ([nblocks] = their number nfade); their fade sums sit
+  // at fade_partials(c)[3 slot ..]
+  int* fadeSlot = nullptr;
+  int nfade = 0;
 
   unsigned* counters = nullptr;
   static constexpr int NCOUNTERS = 256;
@@ -65,18 +70,17 @@ struct Ctx {
 
 // counter slots used by the kernels (each last-CTA reduction owns one)
 enum CounterSlot : int {
-  CNT_MAXU = 0, CNT_ADV = 1, CNT_FADE = 2,
+  CNT_MAXU = 0, CNT_ADV = 1,
   CNT_CHI = 8,          // + shape
   CNT_RHSOBST = 24,     // + shape
   CNT_FORCES = 40,      // + shape
   CNT_MOMENTS = 56,     // + shape
   CNT_MOMENTA = 72,     // + shape
 };
-// partials offsets (doubles)
-inline size_t part_off(int region, const Ctx& c) {
-  // regions: 0 dense reductions, 1.. per-shape tile reductions
-  return (size_t)region * (c.npartials / 16);
-}
+// partials: [0, 3 nblocks) the grid reductions (findMaxU, advDiff's outflow,
+// the fade sums: three per strip block), then 4096 spare, then the
+// per-shape tile reductions
+inline double* fade_partials(const Ctx& c) { return c.partials; }
 
 #define CUP2D_LAUNCHED(c) ((c).launches++)
 

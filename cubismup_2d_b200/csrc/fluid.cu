@@ -18,8 +18,6 @@ namespace cup2d {
 
 namespace {
 
-constexpr double EPSd = 2.220446049250313e-16;   // std::numeric_limits<double>::epsilon()
-
 __global__ void __launch_bounds__(512)
 k_max_u_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh,
            const double* __restrict__ u, const double* __restrict__ v,
@@ -134,22 +132,47 @@ k_advdiff(GridDesc g, const Scalars* sc,
 // PressureSingle.cpp:112-128: tmp = (h / 2dt) * div_2h(u); zero-gradient ghosts
 __global__ void __launch_bounds__(256)
 k_rhs_div(GridDesc g, const Scalars* sc, const double* __restrict__ u,
-          const double* __restrict__ v, double* __restrict__ rhs)
+          const double* __restrict__ v, double* __restrict__ rhs,
+          const int* __restrict__ fadeSlot, double* __restrict__ fadePartials)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_RHSDIV);
   const double h = g.h, facDiv = 0.5 * h / sc->dt;
   const int nx = g.nx, ny = g.ny;
-  const int gx = blockIdx.x * BS + threadIdx.x;
+  const int bx = blockIdx.x, by = blockIdx.y;
+  const int gx = bx * BS + threadIdx.x;
+  const bool touch = fade_touch(g, bx, by);
+  double s[3] = {0, 0, 0};
 #pragma unroll
   for (int r = 0; r < 4; r++) {
-    const int gy = blockIdx.y * BS + threadIdx.y + 8 * r;
+    const int iy = threadIdx.y + 8 * r, gy = by * BS + iy;
     const size_t c = (size_t)gy * nx + gx;
     const double uW = u[gx > 0 ? c - 1 : c], uE = u[gx < nx - 1 ? c + 1 : c];
     const double vS = v[gy > 0 ? c - nx : c], vN = v[gy < ny - 1 ? c + nx : c];
     const double divVx = uE - uW, divVy = vN - vS;
-    rhs[c] = facDiv * (divVx + divVy);
+    const double b = facDiv * (divVx + divVy);
+    rhs[c] = b;
+    if (touch) fade_accumulate(g, bx, by, threadIdx.x, iy, b, s);
   }
+  // a strip block's fade sums of the RHS as it leaves the divergence; the
+  // obstacle terms rewrite those of their own tiles
+  if (touch) {
+    __shared__ double red[96];
+    block_sum<3>(s, red);
+    if (lin_tid() == 0) {
+      const int q = fadeSlot[bx + g.bpdx * by];
+      for (int k = 0; k < 3; k++) fadePartials[3 * q + k] = s[k];
+    }
+  }
+}
+
+// fadeSlot[b] = rank of block b among the strip blocks (block order), or -1;
+// fadeSlot[nblocks] = their number.  Once per grid, one thread.
+__global__ void k_fade_slots(GridDesc g, int* fadeSlot)
+{
+  int n = 0;
+  for (int b = 0; b < g.nblocks; b++) fadeSlot[b] = fade_touch(g, b % g.bpdx, b / g.bpdx) ? n++ : -1;
+  fadeSlot[g.nblocks] = n;
 }
 
 // PressureSingle.cpp:216-241: V += -(dt/2h) grad_2h P; zero-gradient P ghosts.
@@ -201,61 +224,6 @@ k_max_next(GridDesc g, Scalars* sc, const double* __restrict__ u, const double* 
   if (lin_tid() == 0) {
     atomic_max_double(&sc->maxNext, m);
     if (anyBad) atomicOr(&sc->status, ST_NAN);
-  }
-}
-
-// PoissonSolver.cpp:61-100: sums of the faded RHS over the boundary strip.
-// One CTA per block; blocks that do not touch the strip (the test of
-// PoissonSolver.cpp:71-79) contribute zero.
-__global__ void __launch_bounds__(256)
-k_fade_sums(GridDesc g, Scalars* sc, const double* __restrict__ rhs,
-            double* partials, unsigned* counter)
-{
-  pdl_begin();
-  CUP2D_TRACE_SCOPE(TR_FADE);
-  __shared__ double red[96];
-  const int bx = blockIdx.x, by = blockIdx.y;
-  const unsigned nb = gridDim.x * gridDim.y, bid = bx + gridDim.x * by;
-  const double fadeLenX = g.fadeLenX, invFadeX = 1 / fmax(fadeLenX, EPSd);
-  const double fadeLenY = g.fadeLenY, invFadeY = 1 / fmax(fadeLenY, EPSd);
-  const double minx = cell_x(g, bx, 0), maxx = cell_x(g, bx, BS - 1);
-  const double miny = cell_y(g, by, 0), maxy = cell_y(g, by, BS - 1);
-  const bool touch = fadeLenX >= minx || fadeLenX >= g.ext[0] - maxx ||
-                     fadeLenY >= miny || fadeLenY >= g.ext[1] - maxy;
-  double s[3] = {0, 0, 0};   // sumRHS, sumPOS, sumNEG
-  if (touch) {
-    const int ix = threadIdx.x;
-    const double px = cell_x(g, bx, ix);
-    for (int r = 0; r < 4; r++) {
-      const int iy = threadIdx.y + 8 * r;
-      const double py = cell_y(g, by, iy);
-      const double yt = invFadeY * fmax(0.0, fadeLenY - g.ext[1] + py);
-      const double yb = invFadeY * fmax(0.0, fadeLenY - py);
-      const double xt = invFadeX * fmax(0.0, fadeLenX - g.ext[0] + px);
-      const double xb = invFadeX * fmax(0.0, fadeLenX - px);
-      const double fadeArg = fmin(fmax(fmax(yt, yb), fmax(xt, xb)), 1.0);
-      const double b = rhs[(size_t)(by * BS + iy) * g.nx + bx * BS + ix];
-      const double fadedRHS = b * (fadeArg * fadeArg);
-      if (fadedRHS < 0) s[2] -= fadedRHS;
-      if (fadedRHS > 0) s[1] += fadedRHS;
-      s[0] += fadedRHS;
-    }
-  }
-  const int tid = threadIdx.x + 32 * threadIdx.y;
-  if (touch) {
-    block_sum<3>(s, red);
-    if (tid == 0) for (int k = 0; k < 3; k++) partials[3 * bid + k] = s[k];
-  } else if (tid == 0) {
-    for (int k = 0; k < 3; k++) partials[3 * bid + k] = 0.0;
-  }
-  if (!last_block_done(counter, nb)) return;
-  double t[3] = {0, 0, 0};
-  for (unsigned i = tid; i < nb; i += 256)
-    for (int k = 0; k < 3; k++) t[k] += __ldcg(&partials[3 * i + k]);
-  block_sum<3>(t, red);
-  if (tid == 0) {
-    const double sumNEG = fmax(t[2], EPSd), sumPOS = fmax(t[1], EPSd);
-    sc->fadeCorr = t[0] > 0 ? t[0] / sumPOS : t[0] / sumNEG;   // PoissonSolver.cpp:86
   }
 }
 
@@ -340,14 +308,18 @@ void launch_outflow(Ctx& c) {
 
 void launch_rhs_div(Ctx& c) {
   dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
-  launch_k(k_rhs_div, grid, block, 0, c.stream, c.g, c.dsc, c.u(), c.v(), c.rhs);
+  launch_k(k_rhs_div, grid, block, 0, c.stream, c.g, c.dsc, c.u(), c.v(), c.rhs, (const int*)c.fadeSlot,
+           fade_partials(c));
   CUP2D_LAUNCHED(c);
 }
 
-void launch_fade_sums(Ctx& c) {
-  dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
-  launch_k(k_fade_sums, grid, block, 0, c.stream, c.g, c.dsc, c.rhs, c.partials, c.counters + CNT_FADE);
-  CUP2D_LAUNCHED(c);
+int build_fade_slots(Ctx& c) {
+  k_fade_slots<<<1, 1, 0, c.stream>>>(c.g, c.fadeSlot);
+  int n = -1;
+  if (cudaGetLastError() != cudaSuccess ||
+      cudaMemcpyAsync(&n, c.fadeSlot + c.g.nblocks, sizeof(int), cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+      cudaStreamSynchronize(c.stream) != cudaSuccess) return -1;
+  return n;
 }
 
 void launch_pcorr(Ctx& c) {

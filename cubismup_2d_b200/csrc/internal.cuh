@@ -22,6 +22,7 @@ namespace cup2d {
 
 constexpr int BS = 32;            // _BS_ of the reference (Definitions.h:30-32)
 constexpr int BS2 = BS * BS;
+constexpr double EPSd = 2.220446049250313e-16;   // std::numeric_limits<double>::epsilon()
 constexpr int MAX_SHAPES = 8;
 constexpr int NFORCE = 17;        // additive sums of ObstacleBlock.h:33-36
 
@@ -363,6 +364,66 @@ __device__ __forceinline__ double gx_pos(const GridDesc& g, int gx) {
 }
 __device__ __forceinline__ double gy_pos(const GridDesc& g, int gy) {
   return cell_y(g, gy >> 5, gy & 31);
+}
+
+// ---- fade sums of PoissonSolver::solve (PoissonSolver.cpp:61-100) ----------
+// The strip blocks (those that reach the boundary fade strip, the test of
+// PoissonSolver.cpp:71-79) each own three sums of the faded RHS (sumRHS,
+// sumPOS, sumNEG), kept at rank slot (block order among strip blocks).
+// Both producers of a block's sums (the RHS divergence, and the RHS
+// correction of an obstacle tile in the strip) use one order: 32 x 8
+// threads, thread (tx, ty) adds rows ty + 8r, r = 0..3, then block_sum<3>
+// over the CTA (further warps adding zeros), so the sums are the same
+// whichever kernel wrote them last.
+__device__ __forceinline__ bool fade_touch(const GridDesc& g, int bx, int by) {
+  const double minx = cell_x(g, bx, 0), maxx = cell_x(g, bx, BS - 1);
+  const double miny = cell_y(g, by, 0), maxy = cell_y(g, by, BS - 1);
+  return g.fadeLenX >= minx || g.fadeLenX >= g.ext[0] - maxx ||
+         g.fadeLenY >= miny || g.fadeLenY >= g.ext[1] - maxy;
+}
+// adds cell (ix, iy) of block (bx, by), of RHS b, to s (PoissonSolver.cpp:86-95)
+__device__ __forceinline__ void fade_accumulate(const GridDesc& g, int bx, int by, int ix, int iy,
+                                                double b, double (&s)[3]) {
+  const double fadeLenX = g.fadeLenX, invFadeX = 1 / fmax(fadeLenX, EPSd);
+  const double fadeLenY = g.fadeLenY, invFadeY = 1 / fmax(fadeLenY, EPSd);
+  const double px = cell_x(g, bx, ix), py = cell_y(g, by, iy);
+  const double yt = invFadeY * fmax(0.0, fadeLenY - g.ext[1] + py);
+  const double yb = invFadeY * fmax(0.0, fadeLenY - py);
+  const double xt = invFadeX * fmax(0.0, fadeLenX - g.ext[0] + px);
+  const double xb = invFadeX * fmax(0.0, fadeLenX - px);
+  const double fadeArg = fmin(fmax(fmax(yt, yb), fmax(xt, xb)), 1.0);
+  const double fadedRHS = b * (fadeArg * fadeArg);
+  if (fadedRHS < 0) s[2] -= fadedRHS;
+  if (fadedRHS > 0) s[1] += fadedRHS;
+  s[0] += fadedRHS;
+}
+// fadeCorr (PoissonSolver.cpp:80-86) from the sums of the n strip blocks,
+// formed by one warp (all 32 lanes call it) in an order that depends on n
+// alone: lane l adds slots l, l + 32, ... (loads issued four at a time),
+// then an xor butterfly, which leaves the same sums in every lane.  Every
+// CTA that needs the value forms it itself and all get the same bits.
+__device__ __forceinline__ double fade_corr(const double* partials, int n) {
+  const int lane = threadIdx.x & 31;
+  double t[3] = {0, 0, 0};
+  for (int i0 = 0; i0 < n; i0 += 128) {
+    double v[4][3];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int i = i0 + lane + 32 * u;
+#pragma unroll
+      for (int k = 0; k < 3; k++) v[u][k] = i < n ? __ldcg(&partials[3 * i + k]) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int k = 0; k < 3; k++) t[k] += v[u][k];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int k = 0; k < 3; k++) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
+  const double sumNEG = fmax(t[2], EPSd), sumPOS = fmax(t[1], EPSd);
+  return t[0] > 0 ? t[0] / sumPOS : t[0] / sumNEG;
 }
 
 } // namespace cup2d

@@ -29,7 +29,7 @@ void launch_advdiff_undo(Ctx& c);
 void launch_pcorr_undo(Ctx& c);
 void launch_outflow(Ctx& c);                         // advDiff.cpp:89-116
 void launch_rhs_div(Ctx& c);                         // PressureSingle.cpp:112-128
-void launch_fade_sums(Ctx& c);                       // PoissonSolver.cpp:61-100
+int build_fade_slots(Ctx& c);                        // PoissonSolver.cpp:71-79, once per grid
 void launch_pcorr(Ctx& c);                           // PressureSingle.cpp:216-241
 void launch_end_step(Ctx& c);                        // Simulation.cpp:289-290
 void launch_end_step_dt(Ctx& c);                     // the same + the next step's calcMaxTimestep

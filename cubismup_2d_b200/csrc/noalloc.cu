@@ -31,7 +31,6 @@
 namespace cup2d {
 namespace {
 
-constexpr double EPSd = 2.220446049250313e-16;
 constexpr int kMaxDevices = 64;
 constexpr int kScratchHead = 32;   // [0] ticket counter, [1] outflow correction
 

@@ -21,8 +21,6 @@ namespace cup2d {
 
 namespace {
 
-constexpr double EPSd = 2.220446049250313e-16;
-
 struct AllTiles { ObstTiles t[MAX_SHAPES]; };
 
 inline AllTiles all_tiles(const Ctx& c) {
@@ -344,13 +342,16 @@ k_rhs_obst(GridDesc g, DevShape* sh, int k, ObstTiles t, const double* __restric
   }
 }
 
-// PressureSingle.cpp:173-212: perimeter correction of the same-sign RHS
+// PressureSingle.cpp:173-212: perimeter correction of the same-sign RHS.
+// A tile that reaches the fade strip then rewrites its block's fade sums
+// (PoissonSolver.cpp:61-100) from the final RHS.
 __global__ void __launch_bounds__(1024)
 k_rhs_corr(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
-           double* rhs)
+           double* rhs, const int* __restrict__ fadeSlot, double* fadePartials)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_RHSCORR);
+  __shared__ double red[32 * 3];
   const DevShape& S = sh[k];
   const double corr = S.rhsCorr;
   auto CHI = [&](int x, int y) -> double {
@@ -363,14 +364,27 @@ k_rhs_corr(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __r
     const int ix = threadIdx.x, iy = threadIdx.y;
     const int gx = bx * BS + ix, gy = by * BS + iy;
     const double chi = t.chi[(size_t)s * BS2 + iy * BS + ix];
-    if (CHI(gx, gy) > chi) continue;
-    const double gradXx = CHI(gx + 1, gy) - CHI(gx - 1, gy);
-    const double gradXy = CHI(gx, gy + 1) - CHI(gx, gy - 1);
-    const bool isPerim = gradXx * gradXx + gradXy * gradXy > 0;
-    const size_t c = (size_t)gy * g.nx + gx;
-    const double tmp = rhs[c];
-    if (isPerim && tmp > 0 && corr > 0) rhs[c] = tmp - corr * tmp;
-    else if (isPerim && tmp < 0 && corr < 0) rhs[c] = tmp + corr * tmp;
+    if (!(CHI(gx, gy) > chi)) {
+      const double gradXx = CHI(gx + 1, gy) - CHI(gx - 1, gy);
+      const double gradXy = CHI(gx, gy + 1) - CHI(gx, gy - 1);
+      const bool isPerim = gradXx * gradXx + gradXy * gradXy > 0;
+      const size_t c = (size_t)gy * g.nx + gx;
+      const double tmp = rhs[c];
+      if (isPerim && tmp > 0 && corr > 0) rhs[c] = tmp - corr * tmp;
+      else if (isPerim && tmp < 0 && corr < 0) rhs[c] = tmp + corr * tmp;
+    }
+    if (fade_touch(g, bx, by)) {                         // uniform over the CTA
+      __syncthreads();                                   // the tile's final RHS
+      double f[3] = {0, 0, 0};
+      if (iy < 8)
+        for (int r = 0; r < 4; r++)
+          fade_accumulate(g, bx, by, ix, iy + 8 * r, rhs[(size_t)(by * BS + iy + 8 * r) * g.nx + gx], f);
+      block_sum<3>(f, red);
+      if (lin_tid() == 0) {
+        const int q = fadeSlot[b];
+        for (int k2 = 0; k2 < 3; k2++) fadePartials[3 * q + k2] = f[k2];
+      }
+    }
   }
 }
 
@@ -730,7 +744,7 @@ void launch_rhs_obstacles(Ctx& c) {
   }
   for (int k = 0; k < c.nshapes; k++) {
     launch_k(k_rhs_corr, tile_ctas(c, c.tiles[k].capacity), dim3(32, 32), 0, c.stream, c.g, c.dshapes, k, c.tiles[k],
-                                                                  c.chi, c.rhs);
+             (const double*)c.chi, c.rhs, (const int*)c.fadeSlot, fade_partials(c));
     CUP2D_LAUNCHED(c);
   }
 }

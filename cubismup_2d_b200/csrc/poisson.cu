@@ -176,6 +176,23 @@ template <bool INV> __device__ __forceinline__ void dft16(double2* x) {
 template <> __device__ __forceinline__ void dft<16, false>(double2* x) { dft16<false>(x); }
 template <> __device__ __forceinline__ void dft<16, true>(double2* x) { dft16<true>(x); }
 
+// pad(j + u T + m Q) given pj = pad(j): a multiple C of 16 added to an index
+// adds C + C/16 to its padded position, an immediate offset
+template <int T, int Q>
+__device__ __forceinline__ int pad_at(int pj, int j, int u, int m) {
+  if constexpr (T % 16 == 0 && Q % 16 == 0) return pj + u * (T + T / 16) + m * (Q + Q / 16);
+  else return pad(j + u * T + m * Q);
+}
+// pad(o + q NS) given po = pad(o), for an output o of a pass over sub-transforms
+// of size NS: with NS = 1, o is a multiple of R (a divisor of 16) and q < R
+// stays inside o's group of 16
+template <int NS>
+__device__ __forceinline__ int pad_out(int po, int o, int q) {
+  if constexpr (NS % 16 == 0) return po + q * (NS + NS / 16);
+  else if constexpr (NS == 1) return po + q;
+  else return pad(o + q * NS);
+}
+
 // One in-place Stockham pass of radix R over sub-transforms of size NS on
 // nseq sequences A + q*SL: butterfly j (k = j mod NS) reads x_m =
 // a[j + m L/R], scales by w^(m k L/(R NS)), takes the DFT_R and writes
@@ -196,11 +213,13 @@ __device__ __forceinline__ void fft_pass(double2* A, int nseq, const double2* tw
   double2* a = A + sq * SL;
   double2 x[E];
   if (act) {
+    const int pj = pad(j);
 #pragma unroll
     for (int u = 0; u < NB; u++)
 #pragma unroll
       for (int m = 0; m < R; m++)
-        x[u * R + m] = (ZIN && m >= R / 2) ? make_double2(0, 0) : a[pad(j + u * T + m * Q)];
+        x[u * R + m] = (ZIN && m >= R / 2) ? make_double2(0, 0)
+                                           : a[pad_at<T, Q>(pj, j, u, m)];
   }
   __syncthreads();
   if (act) {
@@ -214,9 +233,9 @@ __device__ __forceinline__ void fft_pass(double2* A, int nseq, const double2* tw
         for (int m = 1; m < R; m++) xb[m] = cmul(xb[m], twiddle<L, INV>(tws, m * base));
       }
       dft<R, INV>(xb);
-      const int o = (jb - k) * R + k;
+      const int o = (jb - k) * R + k, po = pad(o);
 #pragma unroll
-      for (int q = 0; q < (HALFO ? R / 2 : R); q++) a[pad(o + q * NS)] = xb[out_reg<R>(q)];
+      for (int q = 0; q < (HALFO ? R / 2 : R); q++) a[pad_out<NS>(po, o, q)] = xb[out_reg<R>(q)];
     }
   }
   __syncthreads();
@@ -289,10 +308,11 @@ __device__ __forceinline__ void fft_convolve(double2* A, int nseq, const double2
   double2* a = A + sq * SL;
   double2 x[E];
   if (act) {
+    const int pj = pad(j);
 #pragma unroll
     for (int u = 0; u < NB; u++)
 #pragma unroll
-      for (int m = 0; m < R; m++) x[u * R + m] = a[pad(j + u * T + m * NS)];
+      for (int m = 0; m < R; m++) x[u * R + m] = a[pad_at<T, NS>(pj, j, u, m)];
   }
   __syncthreads();
   if (act) {
@@ -311,7 +331,7 @@ __device__ __forceinline__ void fft_convolve(double2* A, int nseq, const double2
     }
     dft<E, true>(y);
 #pragma unroll
-    for (int q = 0; q < E; q++) a[pad(j * E + q)] = y[out_reg<E>(q)];
+    for (int q = 0; q < E; q++) a[pad_out<1>(pad(j * E), j * E, q)] = y[out_reg<E>(q)];
   }
   __syncthreads();
   fft_passes<L, E, true, false, HOUT, E>(A, nseq, tws);
@@ -319,14 +339,27 @@ __device__ __forceinline__ void fft_convolve(double2* A, int nseq, const double2
 
 struct FadeArgs {
   int enabled;
-  const Scalars* sc;
+  Scalars* sc;           // receives fadeCorr (from the first CTA)
   GridDesc g;
   double* writeback;     // rhs buffer receives the faded values (cub2rhs writes tmp)
+  const double* partials;   // fade sums of the strip blocks, three each
+  int nstrip;
 };
+
+// fadeCorr for this CTA, formed by warp 0 (blockDim.x >= 32) into *s;
+// visible to the CTA after its next barrier
+__device__ __forceinline__ void fade_corr_cta(const FadeArgs& fa, double* s) {
+  if (threadIdx.x < 32) {
+    const double corr = fade_corr(fa.partials, fa.nstrip);
+    if (threadIdx.x == 0) {
+      *s = corr;
+      if (blockIdx.x == 0) fa.sc->fadeCorr = corr;
+    }
+  }
+}
 
 // PoissonSolver::cub2rhs (PoissonSolver.cpp:101-125) for one cell
 __device__ __forceinline__ double fade_cell(const GridDesc& g, int gx, int gy, double b, double corr) {
-  const double EPSd = 2.220446049250313e-16;
   const double fadeLenX = g.fadeLenX, invFadeX = 1 / fmax(fadeLenX, EPSd);
   const double fadeLenY = g.fadeLenY, invFadeY = 1 / fmax(fadeLenY, EPSd);
   const double px = gx_pos(g, gx), py = gy_pos(g, gy);
@@ -393,13 +426,15 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
       A[r * SL + pad(n)] = make_double2(x[0], x[1]);
     }
   }
+  __shared__ double sCorr;
+  if (fa.enabled) fade_corr_cta(fa, &sCorr);   // while the rows are in flight
   load_twiddles<L>(tws, tw, twLen);
   cp_async_wait<0>();
   __syncthreads();
   if (fa.enabled) {
     // fade band: cells within fadeLen (+2 cells margin) of an edge, faded in
     // place and written back (cub2rhs, PoissonSolver.cpp:61-141)
-    const double corr = fa.sc->fadeCorr;
+    const double corr = sCorr;
     const int bandX = (int)(fa.g.fadeLenX / fa.g.h) + 2;
     const int bandY = (int)(fa.g.fadeLenY / fa.g.h) + 2;
     for (int idx = threadIdx.x; idx < RB * L; idx += NT) {
@@ -590,10 +625,13 @@ k_dct_rows_fwd(const double* in, int Nx, int nrows, double* __restrict__ D, int 
   double2* A = sm;
   double2* tws = sm + rb * SL;
   double* Bx = reinterpret_cast<double*>(tws + Len<L>::TW);     // staged real row values
+  __shared__ double sCorr;
+  fade_corr_cta(fa, &sCorr);
   load_twiddles<L>(tws, tw, twLen);
   const int row0 = blockIdx.x * rb;
   const int nb = min(rb, nrows - row0);
-  const double corr = fa.sc->fadeCorr;
+  __syncthreads();
+  const double corr = sCorr;
   const int bandX = (int)(fa.g.fadeLenX / fa.g.h) + 2;
   const int bandY = (int)(fa.g.fadeLenY / fa.g.h) + 2;
   // faded row values, then the even extension y[j] = x[j] (j < n), x[2n-1-j]
@@ -907,12 +945,13 @@ void poisson_destroy(Poisson* P) {
   delete P;
 }
 
-// PoissonSolver::solve: cub2rhs (fade, reductions in launch_fade_sums), the
+// PoissonSolver::solve: cub2rhs (the fade; every CTA of the first row pass
+// forms fadeCorr from the strip blocks' sums that the RHS kernels left), the
 // transform passes, sol2cub (the inverse row pass writes pres directly).
 void poisson_rows_fwd(Ctx& c) {
   Poisson* P = c.poisson;
   const int Nx = c.g.nx, Ny = c.g.ny;
-  FadeArgs fa{1, c.dsc, c.g, c.rhs};
+  FadeArgs fa{1, c.dsc, c.g, c.rhs, fade_partials(c), c.nfade};
   if (P->type == CUP2D_POISSON_COSINE) {
     dct_rows_fwd(P->Lrow, c.stream, c.rhs, Nx, Ny, reinterpret_cast<double*>(P->spec), P->tw, P->twLen, fa);
     CUP2D_LAUNCHED(c);
