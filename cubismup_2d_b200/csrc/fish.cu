@@ -460,6 +460,7 @@ constexpr int NWARP = RT / 32;
 constexpr int CH = 4;                       // candidate points per thread and chunk
 constexpr int CAP = RT * CH;                // points per chunk
 constexpr int MAX_SEG_PER_TILE = 256;
+constexpr int WU = 4;                       // list entries a cell evaluates at a time
 
 // order-preserving compaction over the CTA's warps; returns the count
 __device__ __forceinline__ int compact_slot(bool keep, int* wc, int& pos) {
@@ -639,7 +640,7 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
     // the keep test needs the point itself only; kept points load the rest
     // (neighbours, velocity) after the compaction
     int gs[CH];                                       // sp / su index of the candidate
-    double2 my[CH];
+    double2 my[CH], pp[CH], pm[CH], uu[CH];
     bool keep[CH];
     uchar4 sup[CH];
 #pragma unroll
@@ -652,7 +653,10 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
         const int rr = q - surfStart[si];
         const int ss = segFst[si] + rr / 2, side = rr & 1;
         gs[r] = 2 * ss + side;
-        my[r] = F.sp[gs[r]];
+        // the point, its neighbours along the midline and its velocity, in
+        // one round of loads (most candidates are dropped, but the loads
+        // overlap)
+        my[r] = F.sp[gs[r]]; pp[r] = F.sp[gs[r] + 2]; pm[r] = F.sp[gs[r] - 2]; uu[r] = F.su[gs[r]];
       }
     }
 #pragma unroll
@@ -673,29 +677,41 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
     for (int r = 0; r < CH; r++)
       if (keep[r]) {
         SurfPt& Pr = ptsS[pos[r]];
-        const double2 pp = F.sp[gs[r] + 2], pm = F.sp[gs[r] - 2], u = F.su[gs[r]];
         Pr.ss = gs[r] >> 1;
         Pr.myP[0] = my[r].x; Pr.myP[1] = my[r].y;
-        Pr.pP[0] = pp.x; Pr.pP[1] = pp.y; Pr.pM[0] = pm.x; Pr.pM[1] = pm.y;
-        Pr.ud[0] = u.x; Pr.ud[1] = u.y;
+        Pr.pP[0] = pp[r].x; Pr.pP[1] = pp[r].y; Pr.pM[0] = pm[r].x; Pr.pM[1] = pm[r].y;
+        Pr.ud[0] = uu[r].x; Pr.ud[1] = uu[r].y;
         supp[pos[r]] = sup[r];
       }
     __syncthreads();
+    CUP2D_TRACE_MARK(wi + 2048, 0);
     rows_build(rowIdx, rowN, supp, nc);
+    CUP2D_TRACE_MARK(wi + 2048, 1);
     const int li = 2 * row + (col >> 3);                // this cell's half-row list
     const int n = rowN[li];
     const unsigned short* l = rowIdx + li * CAP;
     int winner = -1;
-    for (int e = 0; e < n; e++) {
-      const int qi = l[e];
-      const uchar4 sp = supp[qi];
-      if (col < sp.x || col >= sp.y) continue;
-      const SurfPt& Q = ptsS[qi];
-      const double dist0 = sq(px - Q.myP[0]) + sq(py - Q.myP[1]);
-      const double distP = sq(px - Q.pP[0]) + sq(py - Q.pP[1]);
-      const double distM = sq(px - Q.pM[0]) + sq(py - Q.pM[1]);
-      const double dist1 = fmin(fmin(dist0, distP), distM);
-      if (best > dist1) { best = dist1; winner = qi; }
+    // WU list entries at a time: their loads and distances are independent,
+    // the running minimum then takes them in list order
+    for (int e0 = 0; e0 < n; e0 += WU) {
+      double d1[WU];
+      int qs[WU];
+      bool ok[WU];
+#pragma unroll
+      for (int u = 0; u < WU; u++) {
+        const int e = e0 + u;
+        qs[u] = l[e < n ? e : e0];
+        const uchar4 sp = supp[qs[u]];
+        ok[u] = e < n && col >= sp.x && col < sp.y;
+        const SurfPt& Q = ptsS[qs[u]];
+        const double dist0 = sq(px - Q.myP[0]) + sq(py - Q.myP[1]);
+        const double distP = sq(px - Q.pP[0]) + sq(py - Q.pP[1]);
+        const double distM = sq(px - Q.pM[0]) + sq(py - Q.pM[1]);
+        d1[u] = fmin(fmin(dist0, distP), distM);
+      }
+#pragma unroll
+      for (int u = 0; u < WU; u++)
+        if (ok[u] && best > d1[u]) { best = d1[u]; winner = qs[u]; }
     }
     if (winner >= 0) {
       // evaluate the winner of this chunk now (its point data is in shared
@@ -747,7 +763,7 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
   // constructInternl (FishLibrary.cpp:575-638)
   for (int c0 = 0; c0 < totInt; c0 += CAP) {
     int gq[CH];
-    double2 xw[CH];
+    double2 xw[CH], uw[CH];
     bool keep[CH];
     uchar4 sup[CH];
 #pragma unroll
@@ -758,7 +774,7 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
       if (q < totInt) {
         const int si = find_range(intStart, nsl, q);
         gq[r] = segIntBase[si] + (q - intStart[si]);
-        xw[r] = F.ip[gq[r]];
+        xw[r] = F.ip[gq[r]]; uw[r] = F.iu[gq[r]];
       }
     }
 #pragma unroll
@@ -778,7 +794,7 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
     for (int r = 0; r < CH; r++)
       if (keep[r]) {
         IntPt& Pr = ptsI[pos[r]];
-        const double2 u = F.iu[gq[r]];
+        const double2 u = uw[r];
         const double xp0 = (xw[r].x - org0) * invh, xp1 = (xw[r].y - org1) * invh;
         const double ap0 = floor(xp0), ap1 = floor(xp1);
         Pr.iap[0] = (int)ap0; Pr.iap[1] = (int)ap1;
@@ -789,20 +805,33 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
       }
     __syncthreads();
     rows_build(rowIdx, rowN, supp, nc);
+    CUP2D_TRACE_MARK(wi + 2048, 2);
     const int li = 2 * row + (col >> 3);                // this cell's half-row list
     const int n = rowN[li];
     const unsigned short* l = rowIdx + li * CAP;
-    for (int e = 0; e < n; e++) {
-      const int qi = l[e];
-      const uchar4 sp = supp[qi];
-      if (col < sp.x || col >= sp.y) continue;
-      const IntPt& Q = ptsI[qi];
-      const int sx = ix - Q.iap[0], sy = iy - Q.iap[1];
-      const double wxwy = Q.w[1][sy] * Q.w[0][sx];
-      ud0 += wxwy * Q.ud[0];
-      ud1 += wxwy * Q.ud[1];
-      chi += wxwy;
-      if (fabs(dist + 1) < EPSd) dist = 1;
+    for (int e0 = 0; e0 < n; e0 += WU) {
+      double w[WU], a0[WU], a1[WU];
+      bool ok[WU];
+#pragma unroll
+      for (int u = 0; u < WU; u++) {
+        const int e = e0 + u;
+        const int qi = l[e < n ? e : e0];
+        const uchar4 sp = supp[qi];
+        ok[u] = e < n && col >= sp.x && col < sp.y;
+        const IntPt& Q = ptsI[qi];
+        // a kept entry's cell lies in its 2x2 support (sx, sy in {0, 1})
+        const int sx = ok[u] ? ix - Q.iap[0] : 0, sy = ok[u] ? iy - Q.iap[1] : 0;
+        w[u] = Q.w[1][sy] * Q.w[0][sx];
+        a0[u] = Q.ud[0]; a1[u] = Q.ud[1];
+      }
+#pragma unroll
+      for (int u = 0; u < WU; u++)
+        if (ok[u]) {
+          ud0 += w[u] * a0[u];
+          ud1 += w[u] * a1[u];
+          chi += w[u];
+          if (fabs(dist + 1) < EPSd) dist = 1;
+        }
     }
     __syncthreads();
   }

@@ -53,7 +53,7 @@ __global__ void k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int n
 
 // advDiff.cpp:14-87.  Ghosts: neighbour cells, or at the domain edge the
 // zero-gradient copy scaled by the inflow fade of advDiff.cpp:50-55,68-71.
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 k_advdiff(GridDesc g, const Scalars* sc,
           const double* __restrict__ u, const double* __restrict__ v,
           double* __restrict__ un, double* __restrict__ vn,
@@ -64,12 +64,30 @@ k_advdiff(GridDesc g, const Scalars* sc,
   __shared__ double red[32];
   const double dt = sc->dt, h = g.h;
   const double UINF0 = sc->uinfx, UINF1 = sc->uinfy;
-  const double dfac = (g.nu / h) * (dt / h), afac = -0.5 * dt / h;
-  const double norUinf = fmax(fmax(fabs(UINF0), fabs(UINF1)), EPSd);
-  const double rW = fmax(UINF0, 0.0) / norUinf, rS = fmax(UINF1, 0.0) / norUinf;
-  const double rE = fmin(UINF0, 0.0) / norUinf, rN = fmin(UINF1, 0.0) / norUinf;
-  const double fadeW = 1 - rW * rW / 100, fadeS = 1 - rS * rS / 100;
-  const double fadeE = 1 - rE * rE / 100, fadeN = 1 - rN * rN / 100;
+  // the step's coefficients dfac = (nu/h)(dt/h), afac = -0.5 dt/h and the
+  // inflow fades 1 - r^2/100 of r = max/min(U, 0)/max(|U|): seven quotients
+  // (eleven divisions), each evaluated by its own lane of the warp (lane =
+  // threadIdx.x) and shared by shuffles, the same operations as evaluating
+  // all of them in every thread
+  double qa = 1.0, qb = 1.0;
+  {
+    const double norUinf = fmax(fmax(fabs(UINF0), fabs(UINF1)), EPSd);
+    switch (threadIdx.x) {
+      case 0: qa = -0.5 * dt; qb = h; break;
+      case 1: qa = g.nu; qb = h; break;
+      case 2: qa = dt; qb = h; break;
+      case 3: qa = fmax(UINF0, 0.0); qb = norUinf; break;     // W
+      case 4: qa = fmax(UINF1, 0.0); qb = norUinf; break;     // S
+      case 5: qa = fmin(UINF0, 0.0); qb = norUinf; break;     // E
+      case 6: qa = fmin(UINF1, 0.0); qb = norUinf; break;     // N
+      default: break;
+    }
+  }
+  const double q = qa / qb, fq = 1 - q * q / 100;
+  const double afac = __shfl_sync(0xffffffffu, q, 0);
+  const double dfac = __shfl_sync(0xffffffffu, q, 1) * __shfl_sync(0xffffffffu, q, 2);
+  const double fadeW = __shfl_sync(0xffffffffu, fq, 3), fadeS = __shfl_sync(0xffffffffu, fq, 4);
+  const double fadeE = __shfl_sync(0xffffffffu, fq, 5), fadeN = __shfl_sync(0xffffffffu, fq, 6);
   const int nx = g.nx, ny = g.ny;
   const int gx = blockIdx.x * BS + threadIdx.x;
   double IF = 0;
@@ -117,15 +135,36 @@ k_advdiff(GridDesc g, const Scalars* sc,
     scw->outflowCorr = corrS;
   }
   __syncthreads();
-  // advDiff.cpp:107-115, applied by this last CTA once every new value exists
+  // advDiff.cpp:107-115, applied by this last CTA once every new value exists.
+  // Item k < ny is row k (u at its west and east cells), item ny + i column
+  // i (v at its south and north cells); a thread loads the pairs of UB
+  // items before it stores any, so their L2 round trips overlap.
   const double corr = corrS;
-  for (int i = tid; i < ny; i += 256) {
-    un[(size_t)i * nx] = __ldcg(&un[(size_t)i * nx]) + corr;
-    un[(size_t)i * nx + nx - 1] = __ldcg(&un[(size_t)i * nx + nx - 1]) - corr;
-  }
-  for (int i = tid; i < nx; i += 256) {
-    vn[i] = __ldcg(&vn[i]) + corr;
-    vn[(size_t)(ny - 1) * nx + i] = __ldcg(&vn[(size_t)(ny - 1) * nx + i]) - corr;
+  constexpr int UB = 4;
+  const int nitems = ny + nx;
+  for (int k0 = tid; k0 < nitems; k0 += 256 * UB) {
+    double lo[UB], hi[UB];
+    size_t alo[UB], ahi[UB];
+    bool isU[UB];
+#pragma unroll
+    for (int u = 0; u < UB; u++) {
+      const int k = k0 + 256 * u;
+      isU[u] = k < ny;
+      alo[u] = isU[u] ? (size_t)k * nx : (size_t)(k - ny);
+      ahi[u] = isU[u] ? (size_t)k * nx + nx - 1 : (size_t)(ny - 1) * nx + (k - ny);
+      if (k < nitems) {
+        const double* f = isU[u] ? un : vn;
+        lo[u] = __ldcg(&f[alo[u]]);
+        hi[u] = __ldcg(&f[ahi[u]]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < UB; u++)
+      if (k0 + 256 * u < nitems) {
+        double* f = isU[u] ? un : vn;
+        f[alo[u]] = lo[u] + corr;
+        f[ahi[u]] = hi[u] - corr;
+      }
   }
 }
 
