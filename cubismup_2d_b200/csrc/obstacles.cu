@@ -120,23 +120,36 @@ k_raster_disk(GridDesc g, const DevShape* sh, AllTiles T, double* sdf)
   }
 }
 
-// PutObjectsOnGrid::putChiOnGrid (PutObjectsOnGrid.cpp:17-124): Towers chi
-// from the shape's signed distance (ghosts from the max-SDF grid), chi grid
-// = max over shapes, CoM sums, and the surface delta list.
+// PutObjectsOnGrid::putChiOnGrid (PutObjectsOnGrid.cpp:17-124) and the
+// moments of the CoM correction (:118-122) + Shape::removeMoments
+// (Shape.cpp:117-212) in one pass over the tiles: Towers chi from the
+// shape's signed distance (ghosts from the max-SDF grid), chi grid = max
+// over shapes, the surface delta list, and per tile seven integrals of
+// w = rho chi h^2 about the shape's CoM C before its correction:
+//   J = sum w p, M = sum w, Q = sum w |p|^2, U = sum w u, V = sum w v,
+//   A = sum w (p_x v - p_y u)       (p = x - C, u = udef).
+// J/M is the CoM correction d of putChiOnGrid; the moments about the
+// corrected CoM C + d that removeMoments integrates follow exactly in
+// algebra: M, U, V unchanged, Q - 2 d.J + M |d|^2, A - d_x V + d_y U.  The
+// last CTA of the shape adds the tile sums (fixed order) and finalises M,
+// J, the rigid udef part (removed where udef is read, udef_at) and d_gm.
 __global__ void __launch_bounds__(1024)
-k_chi(GridDesc g, const DevShape* sh, AllTiles T, const double* __restrict__ sdfg,
-      double* chig, double* partials, int partStride)
+k_chi_moments(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ sdfg,
+              double* chig, double* partials, int partStride, unsigned* counters)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_CHI);
-  __shared__ double red[32 * 3];
+  __shared__ double red[32 * 7];
   __shared__ double tile[BS][BS + 1];
   const int k = blockIdx.y;
-  const DevShape& S = sh[k];
+  DevShape& S = sh[k];
+  const ObstTiles& t = T.t[k];
+  const int nt = S.ntiles;
+  double* mp = partials + (size_t)k * partStride;
+  const double C0 = S.s.com[0], C1 = S.s.com[1];
   for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
-  double acc[3] = {0, 0, 0};
+  double I[7] = {0, 0, 0, 0, 0, 0, 0};
   {
-    const ObstTiles& t = T.t[k];
     const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
     const int ix = threadIdx.x, iy = threadIdx.y;
     const size_t o = (size_t)s * BS2 + iy * BS + ix;
@@ -169,11 +182,16 @@ k_chi(GridDesc g, const DevShape* sh, AllTiles T, const double* __restrict__ sdf
     t.chi[o] = X;
     atomic_max_double(&chig[(size_t)gy * g.nx + gx], X);   // CHI = max over shapes (:69-73)
     if (X > 0) {
-      const double rho = S.rhoTile;
-      const double p0 = cell_x(g, bx, ix), p1 = cell_y(g, by, iy);
-      acc[0] = rho * X * h * h * (p0 - S.s.com[0]);
-      acc[1] = rho * X * h * h * (p1 - S.s.com[1]);
-      acc[2] = rho * X * h * h;
+      const double p0 = cell_x(g, bx, ix) - C0, p1 = cell_y(g, by, iy) - C1;
+      const double w = X * S.rhoTile * (h * h);
+      const double ux = t.udx[o], uy = t.udy[o];
+      I[0] = w * p0;
+      I[1] = w * p1;
+      I[2] = w;
+      I[3] = w * (p0 * p0 + p1 * p1);
+      I[4] = w * ux;
+      I[5] = w * uy;
+      I[6] = w * (p0 * uy - p1 * ux);
     }
     double D = 0, sdx = 0, sdy = 0;
     if (!(sdf > +2 * h || sdf < -2 * h)) {                   // :86-106 (shift = 0)
@@ -190,78 +208,26 @@ k_chi(GridDesc g, const DevShape* sh, AllTiles T, const double* __restrict__ sdf
     }
     t.sD[o] = D; t.sdx[o] = sdx; t.sdy[o] = sdy;
   }
-  block_sum<3>(acc, red);
-  if (lin_tid() == 0)
-    for (int q = 0; q < 3; q++) partials[(size_t)k * partStride + 3 * s + q] = acc[q];
-  }
-}
-
-// PutObjectsOnGrid.cpp:118-122 (CoM correction) + Shape::removeMoments
-// (Shape.cpp:117-212).  Every CTA forms the corrected CoM from putChiOnGrid's
-// per-tile sums (same fixed order in every CTA), integrates its own tile;
-// the last CTA of the shape finalises M, J, d_gm and the rigid udef part,
-// which consumers subtract where they read udef (udef_at).
-__global__ void __launch_bounds__(1024)
-k_moments(GridDesc g, DevShape* sh, AllTiles T, const double* chiParts, double* parts,
-          int partStride, unsigned* counters)
-{
-  pdl_begin();
-  CUP2D_TRACE_SCOPE(TR_MOMENTS);
-  __shared__ double red[32 * 7];
-  __shared__ double bc[3];
-  const int k = blockIdx.y, tid = lin_tid();
-  DevShape& S = sh[k];
-  const ObstTiles& t = T.t[k];
-  const int nt = S.ntiles;
-  const double* cp = chiParts + (size_t)k * partStride;
-  double* mp = parts + (size_t)k * partStride;
-  // the corrected CoM, formed by every CTA with a tile and by the last CTA
-  auto form_com = [&]() {
-    double a3[3] = {0, 0, 0};
-    for (int i = tid; i < nt; i += 1024)
-      for (int q = 0; q < 3; q++) a3[q] += cp[3 * i + q];
-    block_sum<3>(a3, red);
-    if (tid == 0) {
-      double c0 = S.s.com[0], c1 = S.s.com[1], M = -1;
-      if (a3[2] > EPSd) { c0 += a3[0] / a3[2]; c1 += a3[1] / a3[2]; M = a3[2]; }
-      bc[0] = c0; bc[1] = c1; bc[2] = M;
-    }
-    __syncthreads();
-  };
-  if ((int)blockIdx.x < nt) form_com();
-  for (int s = blockIdx.x; s < nt; s += gridDim.x) {
-    const double C0 = bc[0], C1 = bc[1];
-    const double hsq = g.h * g.h, rho = S.rhoTile;
-    double I[7] = {0, 0, 0, 0, 0, 0, 0};   // x, y, m, j, u, v, a
-    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
-    const int ix = tid % BS, iy = tid / BS;
-    const size_t o = (size_t)s * BS2 + tid;
-    const double X = t.chi[o];
-    if (X > 0) {
-      const double p0 = cell_x(g, bx, ix) - C0, p1 = cell_y(g, by, iy) - C1;
-      const double rhochi = X * rho * hsq;
-      const double ux = t.udx[o], uy = t.udy[o];
-      I[0] = rhochi * p0;
-      I[1] = rhochi * p1;
-      I[2] = rhochi;
-      I[3] = rhochi * (p0 * p0 + p1 * p1);
-      I[4] = rhochi * ux;
-      I[5] = rhochi * uy;
-      I[6] = rhochi * (p0 * uy - p1 * ux);
-    }
-    block_sum<7>(I, red);
-    if (tid == 0) for (int q = 0; q < 7; q++) mp[3 * t.capacity + 7 * s + q] = I[q];
+  block_sum<7>(I, red);
+  if (lin_tid() == 0) for (int q = 0; q < 7; q++) mp[7 * s + q] = I[q];
   }
   if (!last_block_done(counters + k, gridDim.x)) return;
-  if ((int)blockIdx.x >= nt) form_com();
+  const int tid = lin_tid();
   double I[7] = {0, 0, 0, 0, 0, 0, 0};
   for (int i = tid; i < nt; i += 1024)
-    for (int q = 0; q < 7; q++) I[q] += __ldcg(&mp[3 * t.capacity + 7 * i + q]);
+    for (int q = 0; q < 7; q++) I[q] += __ldcg(&mp[7 * i + q]);
   block_sum<7>(I, red);
   if (tid != 0 || nt == 0) return;
-  if (bc[2] > 0) { S.s.com[0] = bc[0]; S.s.com[1] = bc[1]; S.s.M = bc[2]; }
-  S.Iu = I[4] / I[2]; S.Iv = I[5] / I[2]; S.Ia = I[6] / I[3];
-  S.s.M = I[2]; S.s.J = I[3];
+  const double M = I[2];
+  double d0 = 0, d1 = 0;
+  if (M > EPSd) {                                      // PutObjectsOnGrid.cpp:118-122
+    d0 = I[0] / M; d1 = I[1] / M;
+    S.s.com[0] = C0 + d0; S.s.com[1] = C1 + d1;
+  }
+  const double Q = I[3] - 2 * (d0 * I[0] + d1 * I[1]) + M * (d0 * d0 + d1 * d1);
+  const double A = I[6] - d0 * I[5] + d1 * I[4];
+  S.Iu = I[4] / M; S.Iv = I[5] / M; S.Ia = A / Q;
+  S.s.M = M; S.s.J = Q;
   const double dCx = S.s.center[0] - S.s.com[0], dCy = S.s.center[1] - S.s.com[1];
   const double co = S.cosO, si = S.sinO;         // cos/sin(orientation)
   S.s.d_gm[0] = dCx * co + dCy * si;
@@ -714,11 +680,8 @@ void launch_objects_rest(Ctx& c) {
     for (int k = 0; k < c.nshapes; k++)
       if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_raster(c, k);
   const int stride = (int)shape_region(c);
-  launch_k(k_chi, dim3(tile_ctas(c, cap), c.nshapes), dim3(32, 32), 0, c.stream, c.g, c.dshapes, T, c.sdf, c.chi,
-                                                              shape_partials(c), stride);
-  CUP2D_LAUNCHED(c);
-  launch_k(k_moments, dim3(tile_ctas(c, cap), c.nshapes), 1024, 0, c.stream, c.g, c.dshapes, T, shape_partials(c),
-                                                          shape_partials(c), stride, c.counters + CNT_MOMENTS);
+  launch_k(k_chi_moments, dim3(tile_ctas(c, cap), c.nshapes), dim3(32, 32), 0, c.stream, c.g, c.dshapes, T,
+           (const double*)c.sdf, c.chi, shape_partials(c), stride, c.counters + CNT_MOMENTS);
   CUP2D_LAUNCHED(c);
 }
 
