@@ -177,22 +177,23 @@ void launch_pressure_tail(Ctx& c) {
 // One pass of Simulation::simulate's loop body (Simulation.cpp:245-251) as a
 // graph with three branches:
 //   main : dt + reset of last step's tiles + body motion -> fish frames and
-//          tile search, rasters, Towers chi, moments -> [join side2] -> RHS
+//          tile search, rasters, Towers chi with the moments -> [join side2] -> RHS
 //          obstacle terms, Poisson -> momentum integrals [beside the
 //          pressure correction on side2] -> collisions, penalization, forces
 //          -> [join side, side2] -> t += dt and the next step's dt
 //   side : the fish midlines of the next step (they depend on time only)
-//   side2: advDiff (with outflow) and the RHS divergence once the tiles are
-//          placed (advDiff reads no obstacle data); later the pressure
-//          correction, then the next step's findMaxU beside the force pass
+//   side2: once the tiles are placed, advDiff's outflow flux, then advDiff
+//          with the RHS divergence in place (advDiff reads no obstacle data);
+//          later the pressure correction, then the next step's findMaxU
+//          beside the force pass
 void enqueue_step(Ctx& c) {
   struct GraphStepFlag { Ctx& c; explicit GraphStepFlag(Ctx& cc) : c(cc) { c.graphStep = true; }
                          ~GraphStepFlag() { c.graphStep = false; } } flag(c);
   launch_step_begin(c);                     // dt, last step's tiles reset, body motion
   bool anyFish = false;
   for (int k = 0; k < c.nshapes; k++) anyFish |= c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK;
+  cudaEventRecord(c.evFork, c.stream);
   if (anyFish) {
-    cudaEventRecord(c.evFork, c.stream);
     cudaStreamWaitEvent(c.side, c.evFork, 0);
     for (int k = 0; k < c.nshapes; k++)
       if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.side, 1);
@@ -204,15 +205,15 @@ void enqueue_step(Ctx& c) {
   if (!c.recordPlaced) cudaEventRecord(c.evPlaced, c.stream);
   launch_objects_rest(c);
   c.recordPlaced = false;
-  // advDiff and the RHS divergence beside it, once the tiles are placed: the
-  // placement kernels are single-CTA latency chains that a full-GPU kernel
-  // beside them slows, while the rasters after them leave most SMs free
+  // advDiff and the RHS divergence beside the obstacle chain, once the tiles
+  // are placed: the placement kernels are single-CTA latency chains that any
+  // kernel beside them slows (measured: even the 12-CTA outflow flux), while
+  // the rasters after them leave most SMs free
   cudaStreamWaitEvent(c.side2, c.evPlaced, 0);
   {
     StreamScope scope(c, c.side2);
-    launch_advdiff(c);
-    launch_outflow(c);
-    launch_rhs_div(c);
+    launch_outflow_flux(c);
+    launch_advdiff_rhs_div(c);              // the update with the flux's correction, then the RHS
   }
   cudaEventRecord(c.evObjDone, c.side2);
   cudaStreamWaitEvent(c.stream, c.evObjDone, 0);

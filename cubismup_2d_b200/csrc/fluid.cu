@@ -51,120 +51,178 @@ __global__ void k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int n
   sc->dtNextValid = 1;
 }
 
-// advDiff.cpp:14-87.  Ghosts: neighbour cells, or at the domain edge the
-// zero-gradient copy scaled by the inflow fade of advDiff.cpp:50-55,68-71.
-__global__ void __launch_bounds__(256, 4)
-k_advdiff(GridDesc g, const Scalars* sc,
-          const double* __restrict__ u, const double* __restrict__ v,
-          double* __restrict__ un, double* __restrict__ vn,
-          double* partials, unsigned* counter, Scalars* scw)
-{
-  pdl_begin();
-  CUP2D_TRACE_SCOPE(TR_ADVDIFF);
-  __shared__ double red[32];
+// ---- advDiff (advDiff.cpp:14-116) -------------------------------------------
+// The step's coefficients dfac = (nu/h)(dt/h), afac = -0.5 dt/h and the
+// inflow fades 1 - r^2/100 of r = max/min(U, 0)/max(|U|, eps): seven
+// quotients (eleven divisions), each evaluated by its own lane of the warp
+// and shared by shuffles -- the same operations as evaluating all of them in
+// every thread.  Every lane of the warp calls it.
+struct AdvCoef { double afac, dfac, fadeW, fadeS, fadeE, fadeN, U0, U1; };
+__device__ __forceinline__ AdvCoef adv_coef(const GridDesc& g, const Scalars* sc) {
   const double dt = sc->dt, h = g.h;
-  const double UINF0 = sc->uinfx, UINF1 = sc->uinfy;
-  // the step's coefficients dfac = (nu/h)(dt/h), afac = -0.5 dt/h and the
-  // inflow fades 1 - r^2/100 of r = max/min(U, 0)/max(|U|): seven quotients
-  // (eleven divisions), each evaluated by its own lane of the warp (lane =
-  // threadIdx.x) and shared by shuffles, the same operations as evaluating
-  // all of them in every thread
+  AdvCoef k;
+  k.U0 = sc->uinfx; k.U1 = sc->uinfy;
   double qa = 1.0, qb = 1.0;
   {
-    const double norUinf = fmax(fmax(fabs(UINF0), fabs(UINF1)), EPSd);
-    switch (threadIdx.x) {
+    const double norUinf = fmax(fmax(fabs(k.U0), fabs(k.U1)), EPSd);
+    switch (lin_tid() & 31) {
       case 0: qa = -0.5 * dt; qb = h; break;
       case 1: qa = g.nu; qb = h; break;
       case 2: qa = dt; qb = h; break;
-      case 3: qa = fmax(UINF0, 0.0); qb = norUinf; break;     // W
-      case 4: qa = fmax(UINF1, 0.0); qb = norUinf; break;     // S
-      case 5: qa = fmin(UINF0, 0.0); qb = norUinf; break;     // E
-      case 6: qa = fmin(UINF1, 0.0); qb = norUinf; break;     // N
+      case 3: qa = fmax(k.U0, 0.0); qb = norUinf; break;     // W
+      case 4: qa = fmax(k.U1, 0.0); qb = norUinf; break;     // S
+      case 5: qa = fmin(k.U0, 0.0); qb = norUinf; break;     // E
+      case 6: qa = fmin(k.U1, 0.0); qb = norUinf; break;     // N
       default: break;
     }
   }
   const double q = qa / qb, fq = 1 - q * q / 100;
-  const double afac = __shfl_sync(0xffffffffu, q, 0);
-  const double dfac = __shfl_sync(0xffffffffu, q, 1) * __shfl_sync(0xffffffffu, q, 2);
-  const double fadeW = __shfl_sync(0xffffffffu, fq, 3), fadeS = __shfl_sync(0xffffffffu, fq, 4);
-  const double fadeE = __shfl_sync(0xffffffffu, fq, 5), fadeN = __shfl_sync(0xffffffffu, fq, 6);
+  k.afac = __shfl_sync(0xffffffffu, q, 0);
+  k.dfac = __shfl_sync(0xffffffffu, q, 1) * __shfl_sync(0xffffffffu, q, 2);
+  k.fadeW = __shfl_sync(0xffffffffu, fq, 3); k.fadeS = __shfl_sync(0xffffffffu, fq, 4);
+  k.fadeE = __shfl_sync(0xffffffffu, fq, 5); k.fadeN = __shfl_sync(0xffffffffu, fq, 6);
+  return k;
+}
+
+// advDiff.cpp:57-87 for cell (gx, gy): the new velocity before the outflow
+// correction.  Ghosts: neighbour cells, or at the domain edge the
+// zero-gradient copy scaled by the inflow fade of advDiff.cpp:50-55,68-71.
+__device__ __forceinline__ void adv_cell(const GridDesc& g, const AdvCoef& k, const double* __restrict__ u,
+                                         const double* __restrict__ v, int gx, int gy,
+                                         double& unew, double& vnew) {
   const int nx = g.nx, ny = g.ny;
-  const int gx = blockIdx.x * BS + threadIdx.x;
+  const size_t c = (size_t)gy * nx + gx;
+  const double ucc = u[c], vcc = v[c];
+  double ulx, vlx, upx, vpx, uly, vly, upy, vpy;
+  if (gx > 0) { ulx = u[c - 1]; vlx = v[c - 1]; } else { ulx = ucc * k.fadeW; vlx = vcc * k.fadeW; }
+  if (gx < nx - 1) { upx = u[c + 1]; vpx = v[c + 1]; } else { upx = ucc * k.fadeE; vpx = vcc * k.fadeE; }
+  if (gy > 0) { uly = u[c - nx]; vly = v[c - nx]; } else { uly = ucc * k.fadeS; vly = vcc * k.fadeS; }
+  if (gy < ny - 1) { upy = u[c + nx]; vpy = v[c + nx]; } else { upy = ucc * k.fadeN; vpy = vcc * k.fadeN; }
+  const double dUadv = (ucc + k.U0) * (upx - ulx) + (vcc + k.U1) * (upy - uly);
+  const double dUdif = upx + upy + ulx + uly - 4 * ucc;
+  const double dVadv = (ucc + k.U0) * (vpx - vlx) + (vcc + k.U1) * (vpy - vly);
+  const double dVdif = vpx + vpy + vlx + vly - 4 * vcc;
+  unew = ucc + (k.afac * dUadv + k.dfac * dUdif);
+  vnew = vcc + (k.afac * dVadv + k.dfac * dVdif);
+}
+
+// advDiff.cpp:89-106: the net outflow of the new velocity through the domain
+// boundary and its correction per boundary cell.  The boundary cells' new
+// values depend on the old velocity only, so they are formed here, before
+// the update, with the update's own arithmetic (adv_cell).  Item k walks
+// the west column (-u), the east column (+u), the south row (-v) and the
+// north row (+v); the CTA sums, then the last CTA sums those in block order.
+__global__ void __launch_bounds__(256)
+k_outflow_flux(GridDesc g, const Scalars* sc, const double* __restrict__ u, const double* __restrict__ v,
+               double* partials, unsigned* counter, Scalars* scw)
+{
+  pdl_begin();
+  CUP2D_TRACE_SCOPE(TR_ADVDIFF);
+  __shared__ double red[32];
+  const AdvCoef kc = adv_coef(g, sc);
+  const int nx = g.nx, ny = g.ny, nitems = 2 * (nx + ny);
   double IF = 0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nitems; q += gridDim.x * blockDim.x) {
+    int gx, gy, comp;
+    double sgn;
+    if (q < ny) { gx = 0; gy = q; comp = 0; sgn = -1; }
+    else if (q < 2 * ny) { gx = nx - 1; gy = q - ny; comp = 0; sgn = 1; }
+    else if (q < 2 * ny + nx) { gx = q - 2 * ny; gy = 0; comp = 1; sgn = -1; }
+    else { gx = q - 2 * ny - nx; gy = ny - 1; comp = 1; sgn = 1; }
+    double un, vn;
+    adv_cell(g, kc, u, v, gx, gy, un, vn);
+    const double f = comp == 0 ? un : vn;
+    if (sgn < 0) IF -= f; else IF += f;
+  }
+  double s1[1] = {IF};
+  block_sum<1>(s1, red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s1[0];
+  if (!last_block_done(counter, gridDim.x)) return;
+  double t1[1] = {0.0};
+  for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) t1[0] += __ldcg(&partials[i]);
+  block_sum<1>(t1, red);
+  if (threadIdx.x == 0)                                   // advDiff.cpp:105
+    scw->outflowCorr = t1[0] / (2 * (BS * g.bpdy - 0) + 2 * (BS * g.bpdx - 0));
+}
+
+// advDiff.cpp:57-116: the update with the outflow correction of
+// k_outflow_flux applied to the boundary cells (u on the west / east
+// columns, v on the south / north rows).  With DIV, the divergence RHS of
+// PressureSingle.cpp:112-128 and the block's fade sums follow in place: the
+// CTA keeps its new u with one halo column each side and its new v with one
+// halo row each side in shared memory, the halo cells updated here too (they
+// are never on the boundary column or row whose correction they would need;
+// at the domain edge the zero-gradient ghost is the cell itself).
+template <bool DIV>
+__global__ void __launch_bounds__(256, 4)
+k_advdiff(GridDesc g, const Scalars* sc,
+          const double* __restrict__ u, const double* __restrict__ v,
+          double* __restrict__ un, double* __restrict__ vn,
+          double* __restrict__ rhs, const int* __restrict__ fadeSlot, double* __restrict__ fadePartials)
+{
+  pdl_begin();
+  CUP2D_TRACE_SCOPE(TR_ADVDIFF);
+  __shared__ double su[DIV ? BS : 1][BS + 2];
+  __shared__ double sv[DIV ? BS + 2 : 1][BS];
+  const AdvCoef kc = adv_coef(g, sc);
+  const double corr = sc->outflowCorr;
+  const int nx = g.nx, ny = g.ny;
+  const int bx = blockIdx.x, by = blockIdx.y, tx = threadIdx.x, ty = threadIdx.y;
+  const int gx = bx * BS + tx;
 #pragma unroll
   for (int r = 0; r < 4; r++) {
-    const int gy = blockIdx.y * BS + threadIdx.y + 8 * r;
+    const int iy = ty + 8 * r, gy = by * BS + iy;
+    double unew, vnew;
+    adv_cell(g, kc, u, v, gx, gy, unew, vnew);
+    if (gx == 0) unew = unew + corr;                     // advDiff.cpp:107-115
+    if (gx == nx - 1) unew = unew - corr;
+    if (gy == 0) vnew = vnew + corr;
+    if (gy == ny - 1) vnew = vnew - corr;
     const size_t c = (size_t)gy * nx + gx;
-    const double ucc = u[c], vcc = v[c];
-    double ulx, vlx, upx, vpx, uly, vly, upy, vpy;
-    if (gx > 0) { ulx = u[c - 1]; vlx = v[c - 1]; } else { ulx = ucc * fadeW; vlx = vcc * fadeW; }
-    if (gx < nx - 1) { upx = u[c + 1]; vpx = v[c + 1]; } else { upx = ucc * fadeE; vpx = vcc * fadeE; }
-    if (gy > 0) { uly = u[c - nx]; vly = v[c - nx]; } else { uly = ucc * fadeS; vly = vcc * fadeS; }
-    if (gy < ny - 1) { upy = u[c + nx]; vpy = v[c + nx]; } else { upy = ucc * fadeN; vpy = vcc * fadeN; }
-    const double dUadv = (ucc + UINF0) * (upx - ulx) + (vcc + UINF1) * (upy - uly);
-    const double dUdif = upx + upy + ulx + uly - 4 * ucc;
-    const double dVadv = (ucc + UINF0) * (vpx - vlx) + (vcc + UINF1) * (vpy - vly);
-    const double dVdif = vpx + vpy + vlx + vly - 4 * vcc;
-    const double unew = ucc + (afac * dUadv + dfac * dUdif);
-    const double vnew = vcc + (afac * dVadv + dfac * dVdif);
     un[c] = unew; vn[c] = vnew;
-    // advDiff.cpp:93-102: net outflow through the domain boundary
-    if (gx == 0) IF -= unew;
-    if (gx == nx - 1) IF += unew;
-    if (gy == 0) IF -= vnew;
-    if (gy == ny - 1) IF += vnew;
+    if (DIV) { su[iy][tx + 1] = unew; sv[iy + 1][tx] = vnew; }
   }
-  const bool edgeBlock = blockIdx.x == 0 || blockIdx.y == 0 ||
-                         blockIdx.x == gridDim.x - 1 || blockIdx.y == gridDim.y - 1;
-  const unsigned nb = gridDim.x * gridDim.y, bid = blockIdx.x + gridDim.x * blockIdx.y;
-  if (edgeBlock) {
-    double s[1] = {IF};
-    block_sum<1>(s, red);
-    if (threadIdx.x == 0 && threadIdx.y == 0) partials[bid] = s[0];
-  } else if (threadIdx.x == 0 && threadIdx.y == 0) {
-    partials[bid] = 0.0;
-  }
-  if (!last_block_done(counter, nb)) return;
-  const int tid = threadIdx.x + 32 * threadIdx.y;
-  double s[1] = {0.0};
-  for (unsigned i = tid; i < nb; i += 256) s[0] += __ldcg(&partials[i]);
-  block_sum<1>(s, red);
-  __shared__ double corrS;
-  if (tid == 0) {  // advDiff.cpp:105
-    corrS = s[0] / (2 * (BS * g.bpdy - 0) + 2 * (BS * g.bpdx - 0));
-    scw->outflowCorr = corrS;
-  }
-  __syncthreads();
-  // advDiff.cpp:107-115, applied by this last CTA once every new value exists.
-  // Item k < ny is row k (u at its west and east cells), item ny + i column
-  // i (v at its south and north cells); a thread loads the pairs of UB
-  // items before it stores any, so their L2 round trips overlap.
-  const double corr = corrS;
-  constexpr int UB = 4;
-  const int nitems = ny + nx;
-  for (int k0 = tid; k0 < nitems; k0 += 256 * UB) {
-    double lo[UB], hi[UB];
-    size_t alo[UB], ahi[UB];
-    bool isU[UB];
-#pragma unroll
-    for (int u = 0; u < UB; u++) {
-      const int k = k0 + 256 * u;
-      isU[u] = k < ny;
-      alo[u] = isU[u] ? (size_t)k * nx : (size_t)(k - ny);
-      ahi[u] = isU[u] ? (size_t)k * nx + nx - 1 : (size_t)(ny - 1) * nx + (k - ny);
-      if (k < nitems) {
-        const double* f = isU[u] ? un : vn;
-        lo[u] = __ldcg(&f[alo[u]]);
-        hi[u] = __ldcg(&f[ahi[u]]);
+  if constexpr (DIV) {
+    // halo: warps 0-3, one lane per cell (u west / east column, v south /
+    // north row of the neighbouring blocks)
+    if (ty < 4) {
+      const int side = ty;
+      double unew, vnew;
+      const bool have = side == 0 ? bx > 0 : side == 1 ? bx < g.bpdx - 1 : side == 2 ? by > 0 : by < g.bpdy - 1;
+      if (have) {
+        const int hx = side == 0 ? bx * BS - 1 : side == 1 ? bx * BS + BS : bx * BS + tx;
+        const int hy = side == 2 ? by * BS - 1 : side == 3 ? by * BS + BS : by * BS + tx;
+        adv_cell(g, kc, u, v, hx, hy, unew, vnew);
+        if (side == 0) su[tx][0] = unew;
+        else if (side == 1) su[tx][BS + 1] = unew;
+        else if (side == 2) sv[0][tx] = vnew;
+        else sv[BS + 1][tx] = vnew;
       }
     }
+    __syncthreads();
+    const double facDiv = 0.5 * g.h / sc->dt;
+    const bool touch = fade_touch(g, bx, by);
+    double s[3] = {0, 0, 0};
 #pragma unroll
-    for (int u = 0; u < UB; u++)
-      if (k0 + 256 * u < nitems) {
-        double* f = isU[u] ? un : vn;
-        f[alo[u]] = lo[u] + corr;
-        f[ahi[u]] = hi[u] - corr;
+    for (int r = 0; r < 4; r++) {
+      const int iy = ty + 8 * r, gy = by * BS + iy;
+      const double uW = gx > 0 ? su[iy][tx] : su[iy][tx + 1];
+      const double uE = gx < nx - 1 ? su[iy][tx + 2] : su[iy][tx + 1];
+      const double vS = gy > 0 ? sv[iy][tx] : sv[iy + 1][tx];
+      const double vN = gy < ny - 1 ? sv[iy + 2][tx] : sv[iy + 1][tx];
+      const double divVx = uE - uW, divVy = vN - vS;
+      const double b = facDiv * (divVx + divVy);
+      rhs[(size_t)gy * nx + gx] = b;
+      if (touch) fade_accumulate(g, bx, by, tx, iy, b, s);
+    }
+    if (touch) {                                         // uniform over the CTA
+      __shared__ double red[96];
+      block_sum<3>(s, red);
+      if (lin_tid() == 0) {
+        const int q = fadeSlot[bx + g.bpdx * by];
+        for (int k = 0; k < 3; k++) fadePartials[3 * q + k] = s[k];
       }
+    }
   }
 }
 
@@ -328,12 +386,34 @@ void launch_end_step_dt(Ctx& c) {
   CUP2D_LAUNCHED(c);
 }
 
-void launch_advdiff(Ctx& c) {
+void launch_outflow_flux(Ctx& c) {
+  const int items = 2 * (c.g.nx + c.g.ny);
+  int grid = (items + 255) / 256;
+  if (grid > c.sms) grid = c.sms;
+  launch_k(k_outflow_flux, grid, 256, 0, c.stream, c.g, (const Scalars*)c.dsc, (const double*)c.u(),
+           (const double*)c.v(), c.partials, c.counters + CNT_ADV, c.dsc);
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_advdiff_update(Ctx& c) {
   dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
-  launch_k(k_advdiff, grid, block, 0, c.stream, c.g, c.dsc, c.u(), c.v(), c.uo(), c.vo(),
-                                          c.partials, c.counters + CNT_ADV, c.dsc);
+  launch_k(k_advdiff<false>, grid, block, 0, c.stream, c.g, (const Scalars*)c.dsc, (const double*)c.u(),
+           (const double*)c.v(), c.uo(), c.vo(), (double*)nullptr, (const int*)nullptr, (double*)nullptr);
   CUP2D_LAUNCHED(c);
   c.cur = 1 - c.cur;   // advDiff.cpp:81-87: the new field becomes the velocity
+}
+
+void launch_advdiff(Ctx& c) {
+  launch_outflow_flux(c);
+  launch_advdiff_update(c);
+}
+
+void launch_advdiff_rhs_div(Ctx& c) {
+  dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
+  launch_k(k_advdiff<true>, grid, block, 0, c.stream, c.g, (const Scalars*)c.dsc, (const double*)c.u(),
+           (const double*)c.v(), c.uo(), c.vo(), c.rhs, (const int*)c.fadeSlot, fade_partials(c));
+  CUP2D_LAUNCHED(c);
+  c.cur = 1 - c.cur;
 }
 
 // timing helpers: return the velocity to the buffer it came from (no launch)
@@ -341,7 +421,8 @@ void launch_advdiff_undo(Ctx& c) { c.cur = 1 - c.cur; }
 void launch_pcorr_undo(Ctx& c) { c.cur = 1 - c.cur; }
 
 void launch_outflow(Ctx& c) {
-  // applied by the last CTA of k_advdiff (advDiff.cpp:89-116)
+  // formed by k_outflow_flux before the update, applied by k_advdiff
+  // (advDiff.cpp:89-116)
   (void)c;
 }
 

@@ -25,6 +25,9 @@ inline cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, siz
 void launch_max_u_dt(Ctx& c);                        // Helpers.cpp:136-176 + Simulation.cpp:254-277
 void launch_set_dt(Ctx& c, double dt);               // Operator::operator()(dt) argument
 void launch_advdiff(Ctx& c);                         // advDiff.cpp:36-87
+void launch_outflow_flux(Ctx& c);                     // advDiff.cpp:89-106, before the update
+void launch_advdiff_update(Ctx& c);                   // advDiff.cpp:14-116 with the flux's correction
+void launch_advdiff_rhs_div(Ctx& c);                  // the update, then PressureSingle.cpp:112-128 in place
 void launch_advdiff_undo(Ctx& c);
 void launch_pcorr_undo(Ctx& c);
 void launch_outflow(Ctx& c);                         // advDiff.cpp:89-116
