@@ -350,7 +350,7 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   }
   for (auto& f : c.fish) {
     cudaFree(f.pool); cudaFree(f.seg); cudaFree(f.nw); cudaFree(f.off);
-    cudaFree(f.sp); cudaFree(f.su); cudaFree(f.ip); cudaFree(f.iu); cudaFree(f.ipIdx);
+    cudaFree(f.ipIdx);
   }
   poisson_destroy(c.poisson);
   if (c.stream) cudaStreamDestroy(c.stream);
@@ -423,6 +423,8 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
     const int Nm = (int)rS.size();
     f.nm = Nm;
     F.nm = Nm; F.nseg = (Nm - 1) / 8;
+    if (!fish_fits_on_chip(Nm, F.nseg, c.device))
+      return fail(ctx, CUP2D_ENOTSUP, "fish midline too fine: its kernels' staged arrays exceed shared memory");
     // 3 static arrays + 3 midlines of 8 arrays + 16 integrals, one allocation
     if (!rc) rc = dalloc(ctx, &F.pool, (size_t)27 * Nm + 16);
     if (!rc) rc = dalloc(ctx, &F.seg, F.nseg);
@@ -447,10 +449,6 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
     F.nint = off[Nm];
     if (!rc) rc = dalloc(ctx, &F.nw, Nm);
     if (!rc) rc = dalloc(ctx, &F.off, Nm + 1);
-    if (!rc) rc = dalloc(ctx, &F.sp, 2 * (size_t)Nm);
-    if (!rc) rc = dalloc(ctx, &F.su, 2 * (size_t)Nm);
-    if (!rc) rc = dalloc(ctx, &F.ip, (size_t)F.nint);
-    if (!rc) rc = dalloc(ctx, &F.iu, (size_t)F.nint);
     if (!rc) rc = dalloc(ctx, &F.ipIdx, (size_t)F.nint);
     if (rc) return rc;
     std::vector<int2> ipIdx(F.nint);

@@ -308,22 +308,22 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
     __syncthreads();
   CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 3);
   }
-  // Warps 0-1 build the AreaSegments and their bounding box (the chain to
-  // the tile search); warps 2.. generate the surface and interior points
-  // meanwhile (only the raster reads them).
+  // AreaSegments (Fish.cpp:118-150) in the computational frame: 16 lanes per
+  // segment take its midline points (the bounding box is a min / max, exact
+  // in any order), then lane 0 of the group finishes the segment.
   const int Nseg = F.nseg;
   const double R00 = S.cosO, R01 = -S.sinO, R10 = S.sinO, R11 = S.cosO;   // rotation by the orientation
   const double h = g.h;
   __shared__ double box[4];
-  constexpr int SEGT = 64;                              // threads of the segment warps
-  if (tid < SEGT) {
-  // AreaSegments (Fish.cpp:118-150) in the computational frame
+  const int g16 = tid >> 4, l16 = tid & 15;
 #pragma unroll 1
-  for (int i = tid; i < Nseg; i += SEGT) {
-    const int next_idx = (i + 1) * (Nm - 1) / Nseg, idx = i * (Nm - 1) / Nseg;
+  for (int i0 = 0; i0 < Nseg; i0 += nt / 16) {
+    const int i = i0 + g16;
+    int idx = 0, next_idx = -1;
+    if (i < Nseg) { next_idx = (i + 1) * (Nm - 1) / Nseg; idx = i * (Nm - 1) / Nseg; }
     double bb[2][2] = {{1e9, -1e9}, {1e9, -1e9}};
 #pragma unroll 1
-    for (int ss = idx; ss <= next_idx; ++ss) {
+    for (int ss = idx + l16; ss <= next_idx; ss += 16) {
       const double xB0 = rX[ss] - norX[ss] * width[ss], xB1 = rX[ss] + norX[ss] * width[ss];
       const double yB0 = rY[ss] - norY[ss] * width[ss], yB1 = rY[ss] + norY[ss] * width[ss];
       const double maxX = fmax(xB0, xB1), minX = fmin(xB0, xB1);
@@ -331,33 +331,45 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
       bb[0][0] = fmin(bb[0][0], minX); bb[0][1] = fmax(bb[0][1], maxX);
       bb[1][0] = fmin(bb[1][0], minY); bb[1][1] = fmax(bb[1][1], maxY);
     }
-    const double safe = 2 * g.h;
-    Segment sg;
-    sg.first = idx; sg.second = next_idx;
-    sg.w[0] = (bb[0][1] - bb[0][0]) / 2 + safe; sg.w[1] = (bb[1][1] - bb[1][0]) / 2 + safe;
-    const double c0 = (bb[0][1] + bb[0][0]) / 2, c1 = (bb[1][1] + bb[1][0]) / 2;
-    // AreaSegment::changeToComputationalFrame (FishLibrary.cpp:295-342)
-    const double nI0 = R00 * 1 + R01 * 0, nI1 = R10 * 1 + R11 * 0;
-    const double nJ0 = R00 * 0 + R01 * 1, nJ1 = R10 * 0 + R11 * 1;
-    sg.c[0] = R00 * c0 + R01 * c1 + S.s.center[0];
-    sg.c[1] = R10 * c0 + R11 * c1 + S.s.center[1];
-    const double magI = sqrt(nI0 * nI0 + nI1 * nI1), magJ = sqrt(nJ0 * nJ0 + nJ1 * nJ1);
-    const double invMagI = 1 / magI, invMagJ = 1 / magJ;
-    sg.normalI[0] = fabs(nI0) * invMagI; sg.normalI[1] = fabs(nI1) * invMagI;
-    sg.normalJ[0] = fabs(nJ0) * invMagJ; sg.normalJ[1] = fabs(nJ1) * invMagJ;
-    const double wX[2] = {sg.w[0] * sg.normalI[0], sg.w[0] * sg.normalI[1]};
-    const double wY[2] = {sg.w[1] * sg.normalJ[0], sg.w[1] * sg.normalJ[1]};
-    for (int d = 0; d < 2; d++) {
-      sg.boxLab[d][0] = sg.c[d] - wX[d] - wY[d];
-      sg.boxLab[d][1] = sg.c[d] + wX[d] + wY[d];
-      sg.boxObj[d][0] = sg.c[d] - sg.w[d];
-      sg.boxObj[d][1] = sg.c[d] + sg.w[d];
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) {
+      bb[0][0] = fmin(bb[0][0], __shfl_xor_sync(0xffffffffu, bb[0][0], o));
+      bb[0][1] = fmax(bb[0][1], __shfl_xor_sync(0xffffffffu, bb[0][1], o));
+      bb[1][0] = fmin(bb[1][0], __shfl_xor_sync(0xffffffffu, bb[1][0], o));
+      bb[1][1] = fmax(bb[1][1], __shfl_xor_sync(0xffffffffu, bb[1][1], o));
     }
-    F.seg[i] = sg;
-    segS[i] = sg;
+    CUP2D_TRACE_MARK_AFTER(TRACE_ITEMS - 2, 0, bb[1][1]);
+    if (i < Nseg && l16 == 0) {
+      const double safe = 2 * g.h;
+      Segment sg;
+      sg.first = idx; sg.second = next_idx;
+      sg.w[0] = (bb[0][1] - bb[0][0]) / 2 + safe; sg.w[1] = (bb[1][1] - bb[1][0]) / 2 + safe;
+      const double c0 = (bb[0][1] + bb[0][0]) / 2, c1 = (bb[1][1] + bb[1][0]) / 2;
+      // AreaSegment::changeToComputationalFrame (FishLibrary.cpp:295-342)
+      const double nI0 = R00 * 1 + R01 * 0, nI1 = R10 * 1 + R11 * 0;
+      const double nJ0 = R00 * 0 + R01 * 1, nJ1 = R10 * 0 + R11 * 1;
+      sg.c[0] = R00 * c0 + R01 * c1 + S.s.center[0];
+      sg.c[1] = R10 * c0 + R11 * c1 + S.s.center[1];
+      const double magI = sqrt(nI0 * nI0 + nI1 * nI1), magJ = sqrt(nJ0 * nJ0 + nJ1 * nJ1);
+      const double invMagI = 1 / magI, invMagJ = 1 / magJ;
+      CUP2D_TRACE_MARK_AFTER(TRACE_ITEMS - 2, 1, invMagI + invMagJ);
+      sg.normalI[0] = fabs(nI0) * invMagI; sg.normalI[1] = fabs(nI1) * invMagI;
+      sg.normalJ[0] = fabs(nJ0) * invMagJ; sg.normalJ[1] = fabs(nJ1) * invMagJ;
+      const double wX[2] = {sg.w[0] * sg.normalI[0], sg.w[0] * sg.normalI[1]};
+      const double wY[2] = {sg.w[1] * sg.normalJ[0], sg.w[1] * sg.normalJ[1]};
+      for (int d = 0; d < 2; d++) {
+        sg.boxLab[d][0] = sg.c[d] - wX[d] - wY[d];
+        sg.boxLab[d][1] = sg.c[d] + wX[d] + wY[d];
+        sg.boxObj[d][0] = sg.c[d] - sg.w[d];
+        sg.boxObj[d][1] = sg.c[d] + sg.w[d];
+      }
+      F.seg[i] = sg;
+      segS[i] = sg;
+      CUP2D_TRACE_MARK(TRACE_ITEMS - 2, 2);
+    }
   }
+  __syncthreads();
   CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 4);
-  asm volatile("bar.sync 1, %0;" :: "n"(SEGT) : "memory");   // the segment warps only
   if (tid < 32) {                                       // one warp: bounding box of boxLab
     double lo0 = 1e300, hi0 = -1e300, lo1 = 1e300, hi1 = -1e300;
 #pragma unroll 1
@@ -372,32 +384,6 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
     }
     if (tid == 0) { box[0] = lo0; box[1] = hi0; box[2] = lo1; box[3] = hi1; S.nseg = Nseg; }
   }
-  } else {
-  // surface points of constructSurface (FishLibrary.cpp:470-486) and interior
-  // points of constructInternl (FishLibrary.cpp:597-610), computational frame
-  const int pt = tid - SEGT, pnt = nt - SEGT;
-  const double pos0 = S.s.center[0], pos1 = S.s.center[1];
-#pragma unroll 1
-  for (int q = pt; q < 2 * Nm; q += pnt) {
-    const int ss = q >> 1, signp = (q & 1) ? 1 : -1;
-    const double m0 = rX[ss] + width[ss] * signp * norX[ss];
-    const double m1 = rY[ss] + width[ss] * signp * norY[ss];
-    F.sp[q] = make_double2(R00 * m0 + R01 * m1 + pos0, R10 * m0 + R11 * m1 + pos1);
-    const double u0 = vX[ss] + width[ss] * signp * vNorX[ss];
-    const double u1 = vY[ss] + width[ss] * signp * vNorY[ss];
-    F.su[q] = make_double2(R00 * u0 + R01 * u1, R10 * u0 + R11 * u1);
-  }
-#pragma unroll 1
-  for (int q = pt; q < F.nint; q += pnt) {
-    const int2 si = F.ipIdx[q];
-    const int ss = si.x, iw = si.y;
-    const double offsetW = iw * h;
-    const double m0 = rX[ss] + offsetW * norX[ss], m1 = rY[ss] + offsetW * norY[ss];
-    F.ip[q] = make_double2(R00 * m0 + R01 * m1 + pos0, R10 * m0 + R11 * m1 + pos1);
-    const double u0 = vX[ss] + offsetW * vNorX[ss], u1 = vY[ss] + offsetW * vNorY[ss];
-    F.iu[q] = make_double2(R00 * u0 + R01 * u1, R10 * u0 + R11 * u1);
-  }
-  }
   CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 5);
   // the obstacle tiles: blocks any segment intersects (Fish.cpp:158-173),
   // searched inside the segments' bounding box only
@@ -409,6 +395,7 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
   block_range(box[2], box[3], h, 2 * h, by0, by1);
   clip_rect(g, bx0, bx1, by0, by1);
   const int W = bx1 - bx0 + 1, H = by1 - by0 + 1, ncand = (W > 0 && H > 0) ? W * H : 0;
+  CUP2D_TRACE_MARK(TRACE_ITEMS - 2, 3);
   // candidates in chunks of one per thread, in increasing block order; the
   // (candidate, segment) pairs of a chunk are spread over the threads
   __shared__ unsigned char hit[1024];
@@ -421,22 +408,44 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
     const int nq = min(nt, ncand - c0);
     if (tid < nq) hit[tid] = 0;
     __syncthreads();
+    // group g16 takes segments g16, g16 + nt/16, ... and tests each against
+    // the blocks of its own box (block_range keeps a block of margin, so no
+    // block the segment can touch is left out)
 #pragma unroll 1
-    for (int pr = tid; pr < nq * Nseg; pr += nt) {
-      const int cq = pr / Nseg, si = pr - cq * Nseg;
-      if (hit[cq]) continue;
-      const int q = c0 + cq, by = by0 + q / W, bx = bx0 + q % W;
-      const double start[2] = {cell_x(g, bx, 0), cell_y(g, by, 0)};
-      const double end[2] = {cell_x(g, bx, BS - 1), cell_y(g, by, BS - 1)};
-      if (segment_hits_block(segS[si], start, end, 2 * h)) hit[cq] = 1;
+    for (int si = g16; si < Nseg; si += nt / 16) {
+      const Segment& sg = segS[si];
+      int sx0, sx1, sy0, sy1;
+      block_range(sg.boxLab[0][0], sg.boxLab[0][1], h, 2 * h, sx0, sx1);
+      block_range(sg.boxLab[1][0], sg.boxLab[1][1], h, 2 * h, sy0, sy1);
+      sx0 = max(sx0, bx0); sx1 = min(sx1, bx1); sy0 = max(sy0, by0); sy1 = min(sy1, by1);
+      const int sw = sx1 - sx0 + 1, sh = sy1 - sy0 + 1, nblk = (sw > 0 && sh > 0) ? sw * sh : 0;
+#pragma unroll 1
+      for (int j = l16; j < nblk; j += 16) {
+        const int bx = sx0 + j % sw, by = sy0 + j / sw;
+        const int cq = (by - by0) * W + (bx - bx0) - c0;
+        if (cq < 0 || cq >= nq || hit[cq]) continue;
+        const double start[2] = {cell_x(g, bx, 0), cell_y(g, by, 0)};
+        const double end[2] = {cell_x(g, bx, BS - 1), cell_y(g, by, BS - 1)};
+        if (segment_hits_block(sg, start, end, 2 * h)) hit[cq] = 1;
+      }
     }
     __syncthreads();
+    CUP2D_TRACE_MARK(TRACE_ITEMS - 2, 4);
     const bool f = tid < nq && hit[tid];
     const unsigned m = __ballot_sync(0xffffffffu, f);
     if (lane == 0) wcnt[wid] = __popc(m);
     __syncthreads();
-    int off = 0, tot = 0;
-    for (int w = 0; w < nwarps; w++) { if (w < wid) off += wcnt[w]; tot += wcnt[w]; }
+    // exclusive offset of this warp and the chunk's total: a scan of the
+    // warp counts over the lanes
+    int incl = lane < nwarps ? wcnt[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int pre = __shfl_sync(0xffffffffu, incl, wid > 0 ? wid - 1 : 0);
+    const int off = wid > 0 ? pre : 0;
+    const int tot = __shfl_sync(0xffffffffu, incl, nwarps - 1);
     const int pos = base + off + __popc(m & ((1u << lane) - 1u));
     if (f) {
       const int q = c0 + tid, b = (by0 + q / W) * g.bpdx + bx0 + q % W;
@@ -444,9 +453,11 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
       else atomicOr(&sc->status, ST_CAPACITY);
     }
     __syncthreads();
+    CUP2D_TRACE_MARK(TRACE_ITEMS - 2, 5);
     if (tid == 0) base += tot;
   }
   __syncthreads();
+  CUP2D_TRACE_MARK(TRACE_ITEMS - 2, 6);
   if (tid == 0) S.ntiles = base < t.capacity ? base : t.capacity;
 }
 
@@ -538,11 +549,41 @@ __device__ __forceinline__ void rows_build(unsigned short* rowIdx, int* rowN, co
   __syncwarp();
 }
 
-// dynamic shared memory of the raster: frame midline x, y, width (3 Nm
-// doubles), the chunk's points, their supports and the row lists
+// constructSurface's point (FishLibrary.cpp:470-486) of midline index ss on
+// side (0: signp = -1, 1: +1) in the computational frame: rotation by the
+// orientation (R) and, with TRANS, translation by the centre (pos); without
+// it, on the velocity arrays, the point's deformation velocity.  The
+// expressions of the reference, so the values are those it scatters.
+template <bool TRANS>
+__device__ __forceinline__ double2 surf_point(const double* x, const double* y, const double* nx,
+                                              const double* ny, const double* width, int ss, int side,
+                                              double R00, double R01, double R10, double R11,
+                                              double pos0, double pos1) {
+  const int signp = side ? 1 : -1;
+  const double m0 = x[ss] + width[ss] * signp * nx[ss];
+  const double m1 = y[ss] + width[ss] * signp * ny[ss];
+  if (TRANS) return make_double2(R00 * m0 + R01 * m1 + pos0, R10 * m0 + R11 * m1 + pos1);
+  return make_double2(R00 * m0 + R01 * m1, R10 * m0 + R11 * m1);
+}
+// constructInternl's point (FishLibrary.cpp:597-610) of midline index ss at
+// width offset offsetW = iw h, likewise
+template <bool TRANS>
+__device__ __forceinline__ double2 int_point(const double* x, const double* y, const double* nx,
+                                             const double* ny, int ss, double offsetW,
+                                             double R00, double R01, double R10, double R11,
+                                             double pos0, double pos1) {
+  const double m0 = x[ss] + offsetW * nx[ss], m1 = y[ss] + offsetW * ny[ss];
+  if (TRANS) return make_double2(R00 * m0 + R01 * m1 + pos0, R10 * m0 + R11 * m1 + pos1);
+  return make_double2(R00 * m0 + R01 * m1, R10 * m0 + R11 * m1);
+}
+
+// dynamic shared memory of the raster: the frame midline (x, y, normal,
+// velocity, normal velocity) and the width (RSTAGE Nm doubles), the chunk's
+// points, their supports and the row lists
+constexpr int RSTAGE = 9;
 inline size_t raster_smem(int Nm) {
   const size_t pts = CAP * (sizeof(SurfPt) > sizeof(IntPt) ? sizeof(SurfPt) : sizeof(IntPt));
-  return sizeof(double) * 3 * (size_t)Nm + pts + sizeof(uchar4) * CAP + sizeof(unsigned short) * NLIST * CAP;
+  return sizeof(double) * RSTAGE * (size_t)Nm + pts + sizeof(uchar4) * CAP + sizeof(unsigned short) * NLIST * CAP;
 }
 
 __global__ void __launch_bounds__(RT)
@@ -566,12 +607,20 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
   const int tid = threadIdx.x;
   const int Nm = F.nm;
   double* rX = msm; double* rY = msm + Nm; double* width = msm + 2 * Nm;
-  SurfPt* ptsS = reinterpret_cast<SurfPt*>(msm + 3 * Nm);
-  IntPt* ptsI = reinterpret_cast<IntPt*>(msm + 3 * Nm);
-  uchar4* supp = reinterpret_cast<uchar4*>(reinterpret_cast<char*>(msm + 3 * Nm) +
+  double* norX = msm + 3 * Nm; double* norY = msm + 4 * Nm;
+  double* vX = msm + 5 * Nm; double* vY = msm + 6 * Nm;
+  double* vNorX = msm + 7 * Nm; double* vNorY = msm + 8 * Nm;
+  SurfPt* ptsS = reinterpret_cast<SurfPt*>(msm + RSTAGE * Nm);
+  IntPt* ptsI = reinterpret_cast<IntPt*>(msm + RSTAGE * Nm);
+  uchar4* supp = reinterpret_cast<uchar4*>(reinterpret_cast<char*>(msm + RSTAGE * Nm) +
                                            CAP * (sizeof(SurfPt) > sizeof(IntPt) ? sizeof(SurfPt) : sizeof(IntPt)));
   unsigned short* rowIdx = reinterpret_cast<unsigned short*>(supp + CAP);
-  for (int i = tid; i < Nm; i += RT) { rX[i] = F.frame.rX[i]; rY[i] = F.frame.rY[i]; width[i] = F.width[i]; }
+  for (int i = tid; i < Nm; i += RT) {
+    rX[i] = F.frame.rX[i]; rY[i] = F.frame.rY[i]; width[i] = F.width[i];
+    norX[i] = F.frame.norX[i]; norY[i] = F.frame.norY[i];
+    vX[i] = F.frame.vX[i]; vY[i] = F.frame.vY[i];
+    vNorX[i] = F.frame.vNorX[i]; vNorY[i] = F.frame.vNorY[i];
+  }
   const double h = g.h, invh = 1.0 / h;
   const double R00 = S.cosO, R01 = -S.sinO, R10 = S.sinO, R11 = S.cosO;   // rotation by the orientation
   const double pos0 = S.s.center[0], pos1 = S.s.center[1];
@@ -639,8 +688,8 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
   for (int c0 = 0; c0 < totSurf; c0 += CAP) {
     // the keep test needs the point itself only; kept points load the rest
     // (neighbours, velocity) after the compaction
-    int gs[CH];                                       // sp / su index of the candidate
-    double2 my[CH], pp[CH], pm[CH], uu[CH];
+    int gs[CH];                                       // 2 ss + side of the candidate
+    double2 my[CH];
     bool keep[CH];
     uchar4 sup[CH];
 #pragma unroll
@@ -653,10 +702,7 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
         const int rr = q - surfStart[si];
         const int ss = segFst[si] + rr / 2, side = rr & 1;
         gs[r] = 2 * ss + side;
-        // the point, its neighbours along the midline and its velocity, in
-        // one round of loads (most candidates are dropped, but the loads
-        // overlap)
-        my[r] = F.sp[gs[r]]; pp[r] = F.sp[gs[r] + 2]; pm[r] = F.sp[gs[r] - 2]; uu[r] = F.su[gs[r]];
+        my[r] = surf_point<true>(rX, rY, norX, norY, width, ss, side, R00, R01, R10, R11, pos0, pos1);
       }
     }
 #pragma unroll
@@ -677,10 +723,14 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
     for (int r = 0; r < CH; r++)
       if (keep[r]) {
         SurfPt& Pr = ptsS[pos[r]];
-        Pr.ss = gs[r] >> 1;
+        const int ss = gs[r] >> 1, side = gs[r] & 1;
+        const double2 pp = surf_point<true>(rX, rY, norX, norY, width, ss + 1, side, R00, R01, R10, R11, pos0, pos1);
+        const double2 pm = surf_point<true>(rX, rY, norX, norY, width, ss - 1, side, R00, R01, R10, R11, pos0, pos1);
+        const double2 uu = surf_point<false>(vX, vY, vNorX, vNorY, width, ss, side, R00, R01, R10, R11, 0.0, 0.0);
+        Pr.ss = ss;
         Pr.myP[0] = my[r].x; Pr.myP[1] = my[r].y;
-        Pr.pP[0] = pp[r].x; Pr.pP[1] = pp[r].y; Pr.pM[0] = pm[r].x; Pr.pM[1] = pm[r].y;
-        Pr.ud[0] = uu[r].x; Pr.ud[1] = uu[r].y;
+        Pr.pP[0] = pp.x; Pr.pP[1] = pp.y; Pr.pM[0] = pm.x; Pr.pM[1] = pm.y;
+        Pr.ud[0] = uu.x; Pr.ud[1] = uu.y;
         supp[pos[r]] = sup[r];
       }
     __syncthreads();
@@ -762,21 +812,24 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
   CUP2D_TRACE_MARK(wi, 2);
   // constructInternl (FishLibrary.cpp:575-638)
   for (int c0 = 0; c0 < totInt; c0 += CAP) {
-    int gq[CH];
-    double2 xw[CH], uw[CH];
+    int2 sw[CH];                                      // (ss, iw) of the candidate
+    double2 xw[CH];
     bool keep[CH];
     uchar4 sup[CH];
 #pragma unroll
     for (int r = 0; r < CH; r++) {
       keep[r] = false;
-      gq[r] = 0;
+      sw[r] = make_int2(0, 0);
       const int q = c0 + r * RT + tid;
       if (q < totInt) {
         const int si = find_range(intStart, nsl, q);
-        gq[r] = segIntBase[si] + (q - intStart[si]);
-        xw[r] = F.ip[gq[r]]; uw[r] = F.iu[gq[r]];
+        sw[r] = F.ipIdx[segIntBase[si] + (q - intStart[si])];
       }
     }
+#pragma unroll
+    for (int r = 0; r < CH; r++)
+      if (c0 + r * RT + tid < totInt)
+        xw[r] = int_point<true>(rX, rY, norX, norY, sw[r].x, sw[r].y * h, R00, R01, R10, R11, pos0, pos1);
 #pragma unroll
     for (int r = 0; r < CH; r++) {
       const int q = c0 + r * RT + tid;
@@ -794,7 +847,7 @@ k_fish_raster(GridDesc g, const DevShape* sh, int k, ObstTiles t, FishArrays F, 
     for (int r = 0; r < CH; r++)
       if (keep[r]) {
         IntPt& Pr = ptsI[pos[r]];
-        const double2 u = uw[r];
+        const double2 u = int_point<false>(vX, vY, vNorX, vNorY, sw[r].x, sw[r].y * h, R00, R01, R10, R11, 0.0, 0.0);
         const double xp0 = (xw[r].x - org0) * invh, xp1 = (xw[r].y - org1) * invh;
         const double ap0 = floor(xp0), ap1 = floor(xp1);
         Pr.iap[0] = (int)ap0; Pr.iap[1] = (int)ap1;
@@ -860,6 +913,19 @@ size_t frame_smem(int Nm, int nseg) { return sizeof(double) * 10 * (size_t)Nm + 
 
 } // namespace
 
+
+bool fish_fits_on_chip(int Nm, int nseg, int device) {
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) != cudaSuccess) return false;
+  cudaFuncAttributes a{};
+  const size_t need[3] = {midline_smem(Nm), frame_smem(Nm, nseg), raster_smem(Nm)};
+  const void* fn[3] = {(const void*)k_fish_midline, (const void*)k_fish_frame, (const void*)k_fish_raster};
+  for (int i = 0; i < 3; i++) {
+    if (cudaFuncGetAttributes(&a, fn[i]) != cudaSuccess) return false;
+    if (need[i] + a.sharedSizeBytes > (size_t)optin) return false;
+  }
+  return true;
+}
 
 cudaError_t fish_setup_kernels() {
   cudaError_t e = allow_max_dynamic_smem((const void*)k_fish_midline);

@@ -125,11 +125,10 @@ struct FishMidline {
 // (integ[p*8 + ..]: area, CoM_internal[2], vCoM_internal[2], J_internal,
 // angvel_internal, time); frame holds it rotated by theta_internal, which is
 // what PutFishOnBlocks reads.
-// PutFishOnBlocks' points in the computational frame, computed once per step:
-// surface points sp[2 ss + (signp > 0)] = midline +- width * normal, with
-// their deformation velocity su[]; interior points of midline index ss are
-// ip[off[ss] .. off[ss+1]) for width offsets iw = -Nw+1 .. Nw-1
-// (Nw = floor(width/h), time-independent), with velocities iu[].
+// PutFishOnBlocks' interior points: those of midline index ss are numbered
+// off[ss] .. off[ss+1) for width offsets iw = -Nw+1 .. Nw-1 (Nw =
+// floor(width/h), time-independent), ipIdx[] = (ss, iw) of each; the raster
+// forms the points themselves from the frame midline.
 struct FishArrays {
   double *rS, *width, *p1f;
   FishMidline mid[2];
@@ -139,8 +138,6 @@ struct FishArrays {
   double* pool;                           // single allocation behind all arrays
   int* nw;                                // [nm] floor(width / h)
   int* off;                               // [nm + 1] interior point offsets
-  double2* sp; double2* su;               // [2 nm]
-  double2* ip; double2* iu;               // [nint]
   int2* ipIdx;                            // [nint] (ss, iw) of each interior point
   int nm, nseg, nint;
 };
