@@ -251,15 +251,31 @@ k_fish_midline(const Scalars* sc, const DevShape* sh, int k, FishArrays F, int m
 __global__ void __launch_bounds__(1024)
 k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTiles t)
 {
-  pdl_begin();
-  CUP2D_TRACE_SCOPE(TR_FRAME);
-  CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 0);
   extern __shared__ double fsm[];                      // the frame midline, staged
   __shared__ double bc[3];
   DevShape& S = sh[k];
   const int Nm = F.nm, tid = threadIdx.x, nt = blockDim.x;
+  double* rX = fsm;           double* rY = rX + Nm;
+  double* vX = rY + Nm;       double* vY = vX + Nm;
+  double* norX = vY + Nm;     double* norY = norX + Nm;
+  double* vNorX = norY + Nm;  double* vNorY = vNorX + Nm;
+  double* width = vNorY + Nm; double* rS = width + Nm;
+  Segment* segS = reinterpret_cast<Segment*>(rS + Nm);  // this step's segments, also kept on chip
+  // Before the wait: only what earlier steps wrote -- the step parity (set
+  // at the previous step's end), this step's midline (computed during the
+  // previous step, or by a kernel the predecessor already waited for), the
+  // width and the arclength -- staged while the kernel before runs.
   const int p = sc->step & 1;
   const double* integ = F.integ + 8 * p;
+  const FishMidline& M = F.mid[p];
+#pragma unroll 1
+  for (int i = tid; i < Nm; i += nt) {
+    width[i] = F.width[i]; rS[i] = F.rS[i];
+    rX[i] = M.rX[i]; rY[i] = M.rY[i]; vX[i] = M.vX[i]; vY[i] = M.vY[i];
+  }
+  pdl_begin();
+  CUP2D_TRACE_SCOPE(TR_FRAME);
+  CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 0);
   if (tid == 0) {                                       // Fish.cpp:87-93 bookkeeping
     S.f.area_internal = integ[0];
     S.f.CoM_internal[0] = integ[1]; S.f.CoM_internal[1] = integ[2];
@@ -269,25 +285,16 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
     S.f.angvel_internal = integ[6];
     bc[0] = S.f.cosTh; bc[1] = S.f.sinTh; bc[2] = integ[6];   // theta_internal, angvel
   }
-  double* rX = fsm;           double* rY = rX + Nm;
-  double* vX = rY + Nm;       double* vY = vX + Nm;
-  double* norX = vY + Nm;     double* norY = norX + Nm;
-  double* vNorX = norY + Nm;  double* vNorY = vNorX + Nm;
-  double* width = vNorY + Nm; double* rS = width + Nm;
-  Segment* segS = reinterpret_cast<Segment*>(rS + Nm);  // this step's segments, also kept on chip
-#pragma unroll 1
-  for (int i = tid; i < Nm; i += nt) { width[i] = F.width[i]; rS[i] = F.rS[i]; }
   __syncthreads();
   CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 1);
-  const FishMidline& M = F.mid[p];
   const FishMidline& R = F.frame;
   {                                                     // changeToCoMFrameAngular
     const double vAin = bc[2];
     const double R00 = bc[0], R01 = -bc[1], R10 = bc[1], R11 = bc[0];   // rotation by theta_internal
 #pragma unroll 1
-    for (int i = tid; i < Nm; i += nt) {
-      const double px = M.rX[i], py = M.rY[i];
-      const double qx = M.vX[i] + vAin * py, qy = M.vY[i] - vAin * px;
+    for (int i = tid; i < Nm; i += nt) {                // in place: thread i reads and writes entry i
+      const double px = rX[i], py = rY[i];
+      const double qx = vX[i] + vAin * py, qy = vY[i] - vAin * px;
       const double a = R00 * px + R01 * py, b = R10 * px + R11 * py;
       const double c = R00 * qx + R01 * qy, d = R10 * qx + R11 * qy;
       rX[i] = a; rY[i] = b; vX[i] = c; vY[i] = d;

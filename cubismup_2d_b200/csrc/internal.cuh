@@ -218,6 +218,11 @@ inline cudaError_t allow_max_dynamic_smem(const void* f) {
 __device__ __forceinline__ void pdl_begin() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
 }
+// Lets the next kernel of the stream launch now (its CTAs then run up to
+// their pdl_begin, which still waits for this whole grid and its writes).
+__device__ __forceinline__ void pdl_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 
 // ---- small device helpers ------------------------------------------------
 

@@ -50,6 +50,9 @@ k_step_begin(GridDesc g, Scalars* sc, DevShape* sh, int nsh, AllTiles T, double*
              const double* __restrict__ u, const double* __restrict__ v, double* partials, unsigned* counter,
              PrefetchList pf)
 {
+  // the fish frame that follows stages its inputs from the previous step
+  // while this grid runs
+  pdl_launch_dependents();
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_MAXU);
   __shared__ double red[64];
