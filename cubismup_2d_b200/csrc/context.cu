@@ -181,7 +181,9 @@ void launch_pressure_tail(Ctx& c) {
 //          obstacle terms, Poisson -> momentum integrals [beside the
 //          pressure correction on side2] -> collisions, penalization, forces
 //          -> [join side, side2] -> t += dt and the next step's dt
-//   side : the fish midlines of the next step (they depend on time only)
+//   side : the fish midlines of the next step (they depend on time only):
+//          from the graph's start when the step's dt was carried, else
+//          once step_begin has set it
 //   side2: once the tiles are placed, advDiff's outflow flux, then advDiff
 //          with the RHS divergence in place (advDiff reads no obstacle data);
 //          later the pressure correction, then the next step's findMaxU
@@ -189,14 +191,23 @@ void launch_pressure_tail(Ctx& c) {
 void enqueue_step(Ctx& c) {
   struct GraphStepFlag { Ctx& c; explicit GraphStepFlag(Ctx& cc) : c(cc) { c.graphStep = true; }
                          ~GraphStepFlag() { c.graphStep = false; } } flag(c);
-  launch_step_begin(c);                     // dt, last step's tiles reset, body motion
   bool anyFish = false;
   for (int k = 0; k < c.nshapes; k++) anyFish |= c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK;
+  if (anyFish) {
+    // the next step's midlines depend on time only: with a carried dt they
+    // start with the graph, beside the step's own start
+    cudaEventRecord(c.evStart, c.stream);
+    cudaStreamWaitEvent(c.side, c.evStart, 0);
+    for (int k = 0; k < c.nshapes; k++)
+      if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.side, 2);
+  }
+  launch_step_begin(c);                     // dt, last step's tiles reset, body motion
   cudaEventRecord(c.evFork, c.stream);
   if (anyFish) {
+    // otherwise once the step has its dt
     cudaStreamWaitEvent(c.side, c.evFork, 0);
     for (int k = 0; k < c.nshapes; k++)
-      if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.side, 1);
+      if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.side, 3);
     cudaEventRecord(c.evJoin, c.side);
   }
   // the obstacle chain, the step's critical path, stays on the main stream
@@ -304,6 +315,7 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
   if (!rc && (cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking) != cudaSuccess ||
               cudaStreamCreateWithFlags(&c.side2, cudaStreamNonBlocking) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evFork, cudaEventDisableTiming) != cudaSuccess ||
+              cudaEventCreateWithFlags(&c.evStart, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evJoin, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evObj, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evObjDone, cudaEventDisableTiming) != cudaSuccess ||
@@ -339,6 +351,7 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   if (c.evObj) cudaEventDestroy(c.evObj);
   if (c.evObjDone) cudaEventDestroy(c.evObjDone);
   if (c.evFork) cudaEventDestroy(c.evFork);
+  if (c.evStart) cudaEventDestroy(c.evStart);
   if (c.evJoin) cudaEventDestroy(c.evJoin);
   if (c.evPres) cudaEventDestroy(c.evPres);
   if (c.evMom) cudaEventDestroy(c.evMom);

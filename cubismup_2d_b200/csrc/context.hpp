@@ -50,6 +50,7 @@ struct Ctx {
   cudaStream_t side = nullptr;  // branch for the next step's fish midlines
   cudaStream_t side2 = nullptr; // branch for the obstacle chain, beside advDiff
   cudaEvent_t evFork = nullptr, evJoin = nullptr, evObj = nullptr, evObjDone = nullptr;
+  cudaEvent_t evStart = nullptr;   // the start of a graph step (fork of its first side launches)
   cudaEvent_t evPres = nullptr, evMom = nullptr;
   cudaEvent_t evPlaced = nullptr;   // recorded after the obstacle tiles are placed
   bool recordPlaced = false;

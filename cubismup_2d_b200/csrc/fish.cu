@@ -51,20 +51,33 @@ __device__ __forceinline__ void cubic_interp(double x0, double x1, double x, dou
 }
 
 // mode 0: midline at sc->time into buffer (step & 1);
-// mode 1: midline at sc->time + sc->dt (the next step) into buffer ((step + 1) & 1)
+// mode 1: midline at sc->time + sc->dt (the next step) into buffer ((step + 1) & 1);
+// mode 2: mode 1 at the start of a graph step, before the step has set its
+//   dt: runs only if that dt was carried from the previous step
+//   (dtNextValid; the step copies dtNext into dt), and records in
+//   sc->midlineEarly whether it ran.  Reads only the shape's configuration,
+//   time, step and dtNext, which nothing changes before the step's end;
+// mode 3: mode 1 unless mode 2 ran.
 __global__ void __launch_bounds__(512)
-k_fish_midline(const Scalars* sc, const DevShape* sh, int k, FishArrays F, int mode)
+k_fish_midline(Scalars* sc, const DevShape* sh, int k, FishArrays F, int mode)
 {
   pdl_begin();
+  const int tid = threadIdx.x;
+  if (mode == 2) {
+    const int ok = sc->dtNextValid;
+    if (tid == 0) sc->midlineEarly = ok;
+    if (!ok) return;
+  }
+  if (mode == 3 && sc->midlineEarly) return;
   CUP2D_TRACE_SCOPE(TR_MIDLINE);
   CUP2D_TRACE_MARK(TRACE_ITEMS - 3, 0);
   extern __shared__ double smem[];
   __shared__ double red[32 * 5];
   __shared__ double bc[4];
   const DevShape& S = sh[k];
-  const int Nm = F.nm, tid = threadIdx.x, nt = blockDim.x;
-  const double t = mode ? sc->time + sc->dt : sc->time;
-  const int p = mode ? (sc->step + 1) & 1 : sc->step & 1;
+  const int Nm = F.nm, nt = blockDim.x;
+  const double t = mode == 0 ? sc->time : sc->time + (mode == 2 ? sc->dtNext : sc->dt);
+  const int p = mode == 0 ? sc->step & 1 : (sc->step + 1) & 1;
   const double L = S.cfg.length, T = S.cfg.Tperiod;
   double* rS = smem;          double* width = rS + Nm;
   double* rK = width + Nm;    double* vK = rK + Nm;

@@ -54,6 +54,9 @@ struct Scalars {
   // the next step's findMaxU maximum over the final velocity of a graph
   // step, accumulated by exact atomic max; reset at the start of the step
   double maxNext;
+  // set by the midline launched at the start of a graph step: 1 if it could
+  // run (the step's dt was carried), else the launch after the step's dt does
+  int midlineEarly;
 };
 
 struct ShapeCfg {
