@@ -197,18 +197,41 @@ def cpu_baseline_sample(argline, nsteps=3):
     return r.nx * r.ny * nsteps / el / 1e9, os.cpu_count(), nsteps
 
 
-def run_ours(args, world, rank, local, pg):
-    import torch
+def make_sim(argline, local, rank):
     from cubismup_2d_b200 import Simulation
     from cubismup_2d_b200.synthetic import noise_field
-    name, argline = WORKLOADS[args.workload]
-    torch.cuda.set_device(local)
     sim = Simulation(argline)
     sim.cfg.device = local
     sim.init()
     ctx = sim.ctx
     for comp, fname in enumerate(("u", "v")):
         ctx.set(fname, ctx.get(fname) + noise_field(rank, comp, ctx.ny, ctx.nx))
+    return sim
+
+
+def timed_steps(ctx, steps, flush, pg):
+    """K graph steps, each between CUDA events on the library's stream, the
+    L2 flushed before each; returns (total ms, kernel launches)."""
+    import torch
+    launches0 = ctx.kernel_launches()
+    step_ms = []
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    for _ in range(steps):
+        flush.fill_(1.0)                     # evict L2 between timed steps
+        torch.cuda.synchronize()
+        step_ms.append(ctx.time_step())
+    torch.cuda.synchronize()
+    return float(np.sum(step_ms)), ctx.kernel_launches() - launches0
+
+
+def run_ours(args, world, rank, local, pg):
+    import torch
+    name, argline = WORKLOADS[args.workload]
+    torch.cuda.set_device(local)
+    sim = make_sim(argline, local, rank)
+    ctx = sim.ctx
     cells = ctx.nx * ctx.ny
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
@@ -216,26 +239,31 @@ def run_ours(args, world, rank, local, pg):
     ctx.advance(max(args.warmup, 3))
     ctx.sync()
 
-    # timed region: K steps, each between CUDA events on the library's stream
-    # (cudaEvent records from the host are placed by the library's sync
-    # points; the stream is private, so events are recorded via the torch
-    # stream after a full sync of the library stream)
-    launches0 = ctx.kernel_launches()
-    step_ms = []
-    if pg is not None:
-        pg.barrier()
-    torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            flush.fill_(1.0)                 # evict L2 between timed steps
-            torch.cuda.synchronize()
-            ms = ctx.time_step()
-            step_ms.append(ms)
-        torch.cuda.synchronize()
-    launches = ctx.kernel_launches() - launches0
-    total_ms = float(np.sum(step_ms))
+        total_ms, launches = timed_steps(ctx, args.steps, flush, pg)
     total_ms = max_over_ranks(pg, total_ms)
     value = world * cells * args.steps / (total_ms / 1e3) / 1e9
+
+    # the same workload with the FP32 Poisson transforms (CUP2D_PREC_FP32):
+    # pressure after one step from the same state against FP64, then timed
+    fp32 = None
+    if not args.no_fp32:
+        a = make_sim(argline, local, rank)
+        b = make_sim(argline + " -precision fp32", local, rank)
+        a.ctx.advance(1); b.ctx.advance(1)
+        pa, pb = a.ctx.get("pres"), b.ctx.get("pres")
+        perr = float(np.max(np.abs(pb - pa)) / max(np.max(np.abs(pa)), 1e-300))
+        del a
+        b.ctx.advance(max(args.warmup, 3))
+        b.ctx.sync()
+        ms32, _ = timed_steps(b.ctx, args.steps, flush, pg)
+        ms32 = max_over_ranks(pg, ms32)
+        fp32 = {"value": world * cells * args.steps / (ms32 / 1e3) / 1e9, "unit": "Gcell-steps/s",
+                "ms_per_step": ms32 / args.steps, "speedup_vs_fp64": total_ms / ms32,
+                "pres_rel_err_1step": perr,
+                "note": "FP32 free-space Poisson transforms; fields, stencils, obstacle sums and "
+                        "forces FP64; Cd within 1e-4 of FP64 is checked by tests/test_gpu_fp32.py"}
+        del b
 
     # e2e: the reference's own loop through the C ABI with host transfers per
     # step: dt read back (calcMaxTimestep prints it), dt passed to the four
@@ -294,6 +322,7 @@ def run_ours(args, world, rank, local, pg):
                          "traffic": traffic,
                          "algorithmic_bytes_per_launch": ALGO_BYTES_PER_CELL[dom] * cells},
             "kernel_ms": {k: round(v, 5) for k, v in kt.items()},
+            "fp32": fp32,
             "cpu_baseline": cpu,
         }
     return line
@@ -308,6 +337,7 @@ def main():
     ap.add_argument("--workload", default="swimmer", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-Poisson measurement")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     if args.impl == "reference":

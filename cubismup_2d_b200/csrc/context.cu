@@ -272,7 +272,11 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
   if (!cfg || !out) return CUP2D_EINVAL;
   *out = nullptr;
   if (cfg->bpdx <= 0 || cfg->bpdy <= 0) return CUP2D_EINVAL;
-  if (cfg->precision != CUP2D_PREC_FP64) return CUP2D_ENOTSUP;
+  // CUP2D_PREC_FP32: the free-space and periodic Poisson transforms in FP32
+  // (fields, stencils, obstacle sums and forces stay FP64); the cosine solver
+  // has FP64 transforms only
+  if (cfg->precision != CUP2D_PREC_FP64 && cfg->precision != CUP2D_PREC_FP32) return CUP2D_ENOTSUP;
+  if (cfg->precision == CUP2D_PREC_FP32 && cfg->poisson == CUP2D_POISSON_COSINE) return CUP2D_ENOTSUP;
   cup2d_ctx* ctx = new (std::nothrow) cup2d_ctx();
   if (!ctx) return CUP2D_ENOMEM;
   Ctx& c = ctx->c;

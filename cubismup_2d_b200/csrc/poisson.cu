@@ -38,17 +38,28 @@ struct Poisson {
   double* ghat = nullptr;    // [Lcol/2 + 1][nkx] free-space kernel
   double2* tw = nullptr;     // exp(-2 pi i k / twLen)
   int twLen = 0;
+  bool fp32 = false;         // CUP2D_PREC_FP32: float2 spectrum in spec, FP32 passes
+  float2* tw32 = nullptr;    // tw rounded to FP32
+  float* ghat32 = nullptr;   // ghat rounded to FP32
   int rb = 1, cb = 1;        // rows / columns per CTA
 };
 
 namespace {
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+// The transforms are written once for a complex type C: double2 (the FP64
+// solve) or float2 (the FP32 solve of CUP2D_PREC_FP32).
+template <class C> struct CT;
+template <> struct CT<double2> { using R = double; };
+template <> struct CT<float2> { using R = float; };
+template <class C> __device__ __forceinline__ C mk(typename CT<C>::R a, typename CT<C>::R b);
+template <> __device__ __forceinline__ double2 mk<double2>(double a, double b) { return make_double2(a, b); }
+template <> __device__ __forceinline__ float2 mk<float2>(float a, float b) { return make_float2(a, b); }
+template <class C> __device__ __forceinline__ C cmul(C a, C b) {
+  return mk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 conjg(double2 a) { return make_double2(a.x, -a.y); }
+template <class C> __device__ __forceinline__ C cadd(C a, C b) { return mk<C>(a.x + b.x, a.y + b.y); }
+template <class C> __device__ __forceinline__ C csub(C a, C b) { return mk<C>(a.x - b.x, a.y - b.y); }
+template <class C> __device__ __forceinline__ C conjg(C a) { return mk<C>(a.x, -a.y); }
 
 __device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
 
@@ -75,23 +86,23 @@ constexpr int E_C2R = 16;
 constexpr int E_COLS = 16;
 
 // Twiddles w^j = exp(-2 pi i j / L), j < L/4, staged in shared memory.
-template <int L>
-__device__ __forceinline__ void load_twiddles(double2* tws, const double2* __restrict__ tw, int twLen) {
+template <int L, class C>
+__device__ __forceinline__ void load_twiddles(C* tws, const C* __restrict__ tw, int twLen) {
   const int step = twLen / L;
   for (int j = threadIdx.x; j < Len<L>::TW; j += blockDim.x) tws[j] = tw[j * step];
 }
 
 // w^idx (idx < L) from the quarter table: w^(qL/4 + r) = (-i)^q w^r, the
 // rotation being exact; conjugated for the inverse transform.
-template <int L, bool INV>
-__device__ __forceinline__ double2 twiddle(const double2* tws, int idx) {
+template <int L, bool INV, class C>
+__device__ __forceinline__ C twiddle(const C* tws, int idx) {
   const int q = idx / (L / 4), r = idx & (L / 4 - 1);
-  const double2 w = tws[r];
-  double2 v;
+  const C w = tws[r];
+  C v;
   if (q == 0) v = w;
-  else if (q == 1) v = make_double2(w.y, -w.x);
-  else if (q == 2) v = make_double2(-w.x, -w.y);
-  else v = make_double2(-w.y, w.x);
+  else if (q == 1) v = mk<C>(w.y, -w.x);
+  else if (q == 2) v = mk<C>(-w.x, -w.y);
+  else v = mk<C>(-w.y, w.x);
   if (INV) v.y = -v.y;
   return v;
 }
@@ -107,18 +118,22 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
                :: "r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n"
+               :: "r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src) : "memory");
+}
 template <int N> __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory");
 }
 
 // ---- small DFTs in registers (forward exp(-2 pi i mq/R), inverse exp(+)) --
 // multiply by -i (forward) or +i (inverse)
-template <bool INV> __device__ __forceinline__ double2 mul_mi(double2 a) {
-  return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+template <bool INV, class C> __device__ __forceinline__ C mul_mi(C a) {
+  return INV ? mk<C>(-a.y, a.x) : mk<C>(a.y, -a.x);
 }
-template <bool INV>
-__device__ __forceinline__ void dft4(double2& x0, double2& x1, double2& x2, double2& x3) {
-  const double2 t0 = cadd(x0, x2), t1 = csub(x0, x2), t2 = cadd(x1, x3), t3 = mul_mi<INV>(csub(x1, x3));
+template <bool INV, class C>
+__device__ __forceinline__ void dft4(C& x0, C& x1, C& x2, C& x3) {
+  const C t0 = cadd(x0, x2), t1 = csub(x0, x2), t2 = cadd(x1, x3), t3 = mul_mi<INV>(csub(x1, x3));
   x0 = cadd(t0, t2); x2 = csub(t0, t2);
   x1 = cadd(t1, t3); x3 = csub(t1, t3);
 }
@@ -127,13 +142,14 @@ constexpr double S8 = 0.38268343236508977173;   // sin(pi/8)
 constexpr double R2 = 0.70710678118654752440;   // sqrt(2)/2
 // W16^e for e in [0, 16): the first quadrant from (1, C8, R2, S8), the rest
 // by exact quarter turns
-template <bool INV>
-__device__ __forceinline__ double2 w16(int e) {
+template <bool INV, class C>
+__device__ __forceinline__ C w16(int e) {
+  using R = typename CT<C>::R;
   const int q = e >> 2, r = e & 3;
-  const double cr = r == 0 ? 1.0 : (r == 1 ? C8 : (r == 2 ? R2 : S8));
-  const double sr = r == 0 ? 0.0 : (r == 1 ? S8 : (r == 2 ? R2 : C8));
-  double2 v = make_double2(cr, -sr);
-  for (int k = 0; k < q; k++) v = make_double2(v.y, -v.x);
+  const R cr = (R)(r == 0 ? 1.0 : (r == 1 ? C8 : (r == 2 ? R2 : S8)));
+  const R sr = (R)(r == 0 ? 0.0 : (r == 1 ? S8 : (r == 2 ? R2 : C8)));
+  C v = mk<C>(cr, -sr);
+  for (int k = 0; k < q; k++) v = mk<C>(v.y, -v.x);
   if (INV) v.y = -v.y;
   return v;
 }
@@ -141,27 +157,20 @@ __device__ __forceinline__ double2 w16(int e) {
 template <int R> __device__ __forceinline__ constexpr int out_reg(int q) {
   return R == 16 ? 4 * (q & 3) + (q >> 2) : q;
 }
-template <int R, bool INV> __device__ __forceinline__ void dft(double2* x);
-template <> __device__ __forceinline__ void dft<2, false>(double2* x) { const double2 t = x[0]; x[0] = cadd(t, x[1]); x[1] = csub(t, x[1]); }
-template <> __device__ __forceinline__ void dft<2, true>(double2* x) { const double2 t = x[0]; x[0] = cadd(t, x[1]); x[1] = csub(t, x[1]); }
-template <> __device__ __forceinline__ void dft<4, false>(double2* x) { dft4<false>(x[0], x[1], x[2], x[3]); }
-template <> __device__ __forceinline__ void dft<4, true>(double2* x) { dft4<true>(x[0], x[1], x[2], x[3]); }
-template <bool INV> __device__ __forceinline__ void dft8(double2* x) {
+template <bool INV, class C> __device__ __forceinline__ void dft8(C* x) {
   // m = m1 + 2 m2: DFT4 over m2, twiddle W8^(m1 q2), DFT2 over m1
   dft4<INV>(x[0], x[2], x[4], x[6]);
   dft4<INV>(x[1], x[3], x[5], x[7]);
-  double2 y[8];
+  C y[8];
 #pragma unroll
   for (int q2 = 0; q2 < 4; q2++) {
-    const double2 z0 = x[2 * q2], z1 = cmul(x[2 * q2 + 1], w16<INV>(2 * q2));
+    const C z0 = x[2 * q2], z1 = cmul(x[2 * q2 + 1], w16<INV, C>(2 * q2));
     y[q2] = cadd(z0, z1); y[q2 + 4] = csub(z0, z1);
   }
 #pragma unroll
   for (int q = 0; q < 8; q++) x[q] = y[q];
 }
-template <> __device__ __forceinline__ void dft<8, false>(double2* x) { dft8<false>(x); }
-template <> __device__ __forceinline__ void dft<8, true>(double2* x) { dft8<true>(x); }
-template <bool INV> __device__ __forceinline__ void dft16(double2* x) {
+template <bool INV, class C> __device__ __forceinline__ void dft16(C* x) {
   // m = m1 + 4 m2: DFT4 over m2 (result z[m1][q2] in x[m1 + 4 q2]),
   // twiddle W16^(m1 q2), DFT4 over m1 (output q2 + 4 q1 in x[4 q2 + q1])
 #pragma unroll
@@ -169,12 +178,16 @@ template <bool INV> __device__ __forceinline__ void dft16(double2* x) {
 #pragma unroll
   for (int m1 = 1; m1 < 4; m1++)
 #pragma unroll
-    for (int q2 = 1; q2 < 4; q2++) x[m1 + 4 * q2] = cmul(x[m1 + 4 * q2], w16<INV>(m1 * q2));
+    for (int q2 = 1; q2 < 4; q2++) x[m1 + 4 * q2] = cmul(x[m1 + 4 * q2], w16<INV, C>(m1 * q2));
 #pragma unroll
   for (int q2 = 0; q2 < 4; q2++) dft4<INV>(x[4 * q2], x[4 * q2 + 1], x[4 * q2 + 2], x[4 * q2 + 3]);
 }
-template <> __device__ __forceinline__ void dft<16, false>(double2* x) { dft16<false>(x); }
-template <> __device__ __forceinline__ void dft<16, true>(double2* x) { dft16<true>(x); }
+template <int R, bool INV, class C> __device__ __forceinline__ void dft(C* x) {
+  if constexpr (R == 2) { const C t = x[0]; x[0] = cadd(t, x[1]); x[1] = csub(t, x[1]); }
+  else if constexpr (R == 4) dft4<INV>(x[0], x[1], x[2], x[3]);
+  else if constexpr (R == 8) dft8<INV>(x);
+  else dft16<INV>(x);
+}
 
 // pad(j + u T + m Q) given pj = pad(j): a multiple C of 16 added to an index
 // adds C + C/16 to its padded position, an immediate offset
@@ -199,8 +212,8 @@ __device__ __forceinline__ int pad_out(int po, int o, int q) {
 // output q at (j - k) R + k + q NS.  Thread t of a sequence owns the 16/R
 // butterflies t + u L/16.  Loads go to registers before the barrier,
 // stores after it, so one buffer suffices.
-template <int L, int R, int NS, bool INV, bool HIN, bool HOUT, int E>
-__device__ __forceinline__ void fft_pass(double2* A, int nseq, const double2* tws)
+template <int L, int R, int NS, bool INV, bool HIN, bool HOUT, int E, class C>
+__device__ __forceinline__ void fft_pass(C* A, int nseq, const C* tws)
 {
   constexpr int SL = Len<L>::SL, T = L / E, NB = E / R, Q = L / R;
   // first pass of an input whose upper half is zero: inputs m >= R/2 sit at
@@ -210,22 +223,22 @@ __device__ __forceinline__ void fft_pass(double2* A, int nseq, const double2* tw
   const int tid = threadIdx.x;
   const bool act = tid < nseq * T;
   const int sq = act ? tid / T : 0, j = tid - sq * T;
-  double2* a = A + sq * SL;
-  double2 x[E];
+  C* a = A + sq * SL;
+  C x[E];
   if (act) {
     const int pj = pad(j);
 #pragma unroll
     for (int u = 0; u < NB; u++)
 #pragma unroll
       for (int m = 0; m < R; m++)
-        x[u * R + m] = (ZIN && m >= R / 2) ? make_double2(0, 0)
+        x[u * R + m] = (ZIN && m >= R / 2) ? mk<C>(0, 0)
                                            : a[pad_at<T, Q>(pj, j, u, m)];
   }
   __syncthreads();
   if (act) {
 #pragma unroll
     for (int u = 0; u < NB; u++) {
-      double2* xb = x + u * R;
+      C* xb = x + u * R;
       const int jb = j + u * T, k = jb & (NS - 1);
       if (NS > 1 && k) {
         const int base = k * (L / (R * NS));
@@ -241,8 +254,8 @@ __device__ __forceinline__ void fft_pass(double2* A, int nseq, const double2* tw
   __syncthreads();
 }
 
-template <int L, int NS, bool INV, bool HIN, bool HOUT, int E>
-__device__ __forceinline__ void fft_passes(double2* A, int nseq, const double2* tws) {
+template <int L, int NS, bool INV, bool HIN, bool HOUT, int E, class C>
+__device__ __forceinline__ void fft_passes(C* A, int nseq, const C* tws) {
   if constexpr (NS * E <= L) {
     fft_pass<L, E, NS, INV, HIN, HOUT, E>(A, nseq, tws);
     fft_passes<L, NS * E, INV, HIN, HOUT, E>(A, nseq, tws);
@@ -257,8 +270,8 @@ __device__ __forceinline__ void fft_passes(double2* A, int nseq, const double2* 
 // exp(+...), unnormalised.  Needs blockDim.x >= nseq * L/E.  HIN: the
 // upper half of the input is zero and never read; HOUT: only the lower half
 // of the output is written.
-template <int L, bool INV, bool HIN = false, bool HOUT = false, int E = 16>
-__device__ void fft_inplace(double2* A, int nseq, const double2* tws)
+template <int L, bool INV, bool HIN = false, bool HOUT = false, int E = 16, class C>
+__device__ void fft_inplace(C* A, int nseq, const C* tws)
 {
   fft_passes<L, 1, INV, HIN, HOUT, E>(A, nseq, tws);
 }
@@ -270,8 +283,8 @@ template <int L, int E> constexpr int last_ns() {
   return ns == L ? ns / E : ns;
 }
 // the passes of fft_passes<L, NS, ...> whose sub-transform size is below NSEND
-template <int L, int NS, int NSEND, bool INV, bool HIN, int E>
-__device__ __forceinline__ void fft_passes_below(double2* A, int nseq, const double2* tws) {
+template <int L, int NS, int NSEND, bool INV, bool HIN, int E, class C>
+__device__ __forceinline__ void fft_passes_below(C* A, int nseq, const C* tws) {
   if constexpr (NS < NSEND) {
     constexpr int R = NS * E <= L ? E : L / NS;
     fft_pass<L, R, NS, INV, HIN, false, E>(A, nseq, tws);
@@ -287,8 +300,8 @@ __device__ __forceinline__ void fft_passes_below(double2* A, int nseq, const dou
 // L/E], which is input m = u + (E/R) q of thread j's radix-E first inverse
 // butterfly (NS = 1).  With L <= E (one pass each way) the three steps run
 // one after the other.
-template <int L, bool HIN, bool HOUT, int E, class Mul>
-__device__ __forceinline__ void fft_convolve(double2* A, int nseq, const double2* tws, Mul mul)
+template <int L, bool HIN, bool HOUT, int E, class C, class Mul>
+__device__ __forceinline__ void fft_convolve(C* A, int nseq, const C* tws, Mul mul)
 {
   constexpr int SL = Len<L>::SL, T = L / E, NS = last_ns<L, E>(), R = L / NS, NB = E / R;
   if constexpr (L <= E) {
@@ -305,8 +318,8 @@ __device__ __forceinline__ void fft_convolve(double2* A, int nseq, const double2
   const int tid = threadIdx.x;
   const bool act = tid < nseq * T;
   const int sq = act ? tid / T : 0, j = tid - sq * T;
-  double2* a = A + sq * SL;
-  double2 x[E];
+  C* a = A + sq * SL;
+  C x[E];
   if (act) {
     const int pj = pad(j);
 #pragma unroll
@@ -316,10 +329,10 @@ __device__ __forceinline__ void fft_convolve(double2* A, int nseq, const double2
   }
   __syncthreads();
   if (act) {
-    double2 y[E];
+    C y[E];
 #pragma unroll
     for (int u = 0; u < NB; u++) {
-      double2* xb = x + u * R;
+      C* xb = x + u * R;
       const int jb = j + u * T;
       if (jb) {
 #pragma unroll
@@ -605,6 +618,195 @@ k_rows_c2r(const double2* __restrict__ in, int inStride, int nrows, double* __re
   }
 }
 
+// ---- FP32 transforms (CUP2D_PREC_FP32) ------------------------------------
+// The free-space and periodic solves with float2 spectra and FP32 passes:
+// the same kernels' structure, the fade and its write-back in FP64 (so the
+// RHS written back is the one of the FP64 path), rows converted to FP32 as
+// they enter shared memory, the pressure written back in FP64.
+template <int L, bool HIN>
+__global__ void __launch_bounds__(Len<L, E_ROWS>::NT, Len<L, E_ROWS>::MINB)
+k_rows_r2c32(const double* __restrict__ in, int inStride, int nrows, int ncolsIn,
+             float2* __restrict__ out, int outStride, const float2* __restrict__ tw, int twLen, FadeArgs fa)
+{
+  pdl_begin();
+  CUP2D_TRACE_SCOPE(TR_R2C);
+  constexpr int SL = Len<L, E_ROWS>::SL, RB = Len<L, E_ROWS>::B, NT = Len<L, E_ROWS>::NT;
+  constexpr int PER = (RB * L + NT - 1) / NT;          // value pairs per thread
+  extern __shared__ float2 sm32[];
+  float2* A = sm32;
+  float2* tws = sm32 + RB * SL;
+  const int row0 = blockIdx.x * RB;
+  const int nb = min(RB, nrows - row0);
+  double2 v[PER];                                      // this thread's pairs, all loads in flight
+#pragma unroll
+  for (int u = 0; u < PER; u++) {
+    const int idx = threadIdx.x + u * NT;
+    const int r = idx / L, n = idx & (L - 1), row = row0 + r;
+    v[u] = make_double2(0, 0);
+    if (idx < RB * L && r < nb) {
+      if (2 * n + 1 < ncolsIn) v[u] = *reinterpret_cast<const double2*>(in + (size_t)row * inStride + 2 * n);
+      else if (2 * n < ncolsIn) v[u].x = in[(size_t)row * inStride + 2 * n];
+    }
+  }
+  __shared__ double sCorr;
+  if (fa.enabled) fade_corr_cta(fa, &sCorr);
+  load_twiddles<L>(tws, tw, twLen);
+  __syncthreads();
+  const double corr = fa.enabled ? sCorr : 0.0;
+  const int bandX = fa.enabled ? (int)(fa.g.fadeLenX / fa.g.h) + 2 : 0;
+  const int bandY = fa.enabled ? (int)(fa.g.fadeLenY / fa.g.h) + 2 : 0;
+#pragma unroll
+  for (int u = 0; u < PER; u++) {
+    const int idx = threadIdx.x + u * NT;
+    const int r = idx / L, n = idx & (L - 1), row = row0 + r;
+    if (idx >= RB * L || r >= nb) continue;
+    if (HIN && 2 * n >= ncolsIn) continue;             // the zero half is never read
+    if (fa.enabled && 2 * n + 1 < ncolsIn) {
+      // fade band as in k_rows_r2c (cub2rhs, PoissonSolver.cpp:61-141)
+      const bool rowBand = row < bandY || row >= fa.g.ny - bandY;
+      double* x = &v[u].x;
+      for (int q = 0; q < 2; q++) {
+        const int col = 2 * n + q;
+        if (rowBand || col < bandX || col >= fa.g.nx - bandX) {
+          x[q] = fade_cell(fa.g, col, row, x[q], corr);
+          fa.writeback[(size_t)row * inStride + col] = x[q];
+        }
+      }
+    }
+    A[r * SL + pad(n)] = make_float2((float)v[u].x, (float)v[u].y);
+  }
+  __syncthreads();
+  fft_inplace<L, false, HIN, false, E_ROWS>(A, nb, tws);
+  // even/odd split: X[k] = Fe[k] + W^k Fo[k], W = exp(-i pi / L), k in [0, L]
+  const int twStep = twLen / (2 * L);
+  for (int idx = threadIdx.x; idx < nb * (L + 1); idx += NT) {
+    const int r = idx / (L + 1), k = idx - r * (L + 1);
+    const float2 Zk = A[r * SL + pad(k == L ? 0 : k)];
+    const float2 Zc = conjg(A[r * SL + pad(k == 0 ? 0 : L - k)]);
+    const float2 Fe = make_float2(0.5f * (Zk.x + Zc.x), 0.5f * (Zk.y + Zc.y));
+    const float2 d = csub(Zk, Zc);
+    const float2 Fo = make_float2(0.5f * d.y, -0.5f * d.x);
+    out[(size_t)(row0 + r) * outStride + k] = cadd(Fe, cmul(tw[k * twStep], Fo));
+  }
+}
+
+// mode 0: forward, x G^, inverse, keep nrowsOut rows; mode 2: the periodic
+// multiplier -1/|k|^2 / (MX MY) (formed in FP64, applied in FP32)
+template <int L, bool FS>
+__global__ void __launch_bounds__(Len<L, E_COLS>::NT, Len<L, E_COLS>::MINB)
+k_cols32(float2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrowsOut,
+         const float* __restrict__ ghat, int mode, const float2* __restrict__ tw, int twLen,
+         double norm, int MXp, int MYp)
+{
+  pdl_begin();
+  CUP2D_TRACE_SCOPE(TR_COLS);
+  constexpr int SL = Len<L, E_COLS>::SL, CB = Len<L, E_COLS>::B, NT = Len<L, E_COLS>::NT, GR = L / 2 + 1;
+  extern __shared__ float2 sm32[];
+  float2* A = sm32;
+  float2* tws = sm32 + CB * SL;
+  float* Gs = reinterpret_cast<float*>(tws + Len<L>::TW);   // [GR][CB] kernel rows
+  const int c0 = blockIdx.x * CB;
+  const int nb = min(CB, ncols - c0);
+  for (int idx = threadIdx.x; idx < CB * nrowsIn; idx += NT) {
+    const int r = idx / CB, j = idx & (CB - 1);
+    if (j < nb) cp_async8(A + j * SL + pad(r), data + (size_t)r * stride + c0 + j);
+  }
+  if (mode == 0)
+    for (int idx = threadIdx.x; idx < CB * GR; idx += NT) {
+      const int r = idx / CB, j = idx & (CB - 1);
+      if (j < nb) cp_async4(Gs + r * CB + j, ghat + (size_t)r * stride + c0 + j);
+    }
+  cp_async_commit();
+  if (!FS)
+    for (int idx = threadIdx.x; idx < CB * (L - nrowsIn); idx += NT) {
+      const int r = nrowsIn + idx / CB, j = idx & (CB - 1);
+      A[j * SL + pad(r)] = make_float2(0, 0);
+    }
+  load_twiddles<L>(tws, tw, twLen);
+  cp_async_wait<0>();
+  __syncthreads();
+  if (mode == 0) {
+    fft_convolve<L, FS, FS, E_COLS>(A, nb, tws, [&](int j, int r, float2 z) {
+      const int ky = r <= L / 2 ? r : L - r;
+      const float f = Gs[ky * CB + j];
+      return make_float2(z.x * f, z.y * f);
+    });
+  } else {
+    fft_convolve<L, FS, FS, E_COLS>(A, nb, tws, [&](int j, int r, float2 z) {
+      // FFTW_periodic::_solve_spectral (FFTW_periodic.h:77-92)
+      const int i = c0 + j;
+      if (i == 0 && r == 0) return make_float2(0, 0);
+      const int kx = i <= MXp / 2 ? i : MXp - i, ky = r <= MYp / 2 ? r : MYp - r;
+      const double waveFactX = 2 * M_PI / MXp, waveFactY = 2 * M_PI / MYp;
+      const double rkx = kx * waveFactX, rky = ky * waveFactY;
+      const float f = (float)(-1 / (rkx * rkx + rky * rky) * norm);
+      return make_float2(z.x * f, z.y * f);
+    });
+  }
+  for (int idx = threadIdx.x; idx < CB * nrowsOut; idx += NT) {
+    const int r = idx / CB, j = idx & (CB - 1);
+    if (j < nb) data[(size_t)r * stride + c0 + j] = A[j * SL + pad(r)];
+  }
+}
+
+// inverse real FFT of length 2L from X[0..L] (float2); writes the first
+// ncolsOut values in FP64
+template <int L, bool HOUT>
+__global__ void __launch_bounds__(Len<L, E_C2R>::NT, Len<L, E_C2R>::MINB)
+k_rows_c2r32(const float2* __restrict__ in, int inStride, int nrows, double* __restrict__ out, int outStride,
+             int ncolsOut, const float2* __restrict__ tw, int twLen)
+{
+  pdl_begin();
+  CUP2D_TRACE_SCOPE(TR_C2R);
+  constexpr int SL = Len<L, E_C2R>::SL, RB = Len<L, E_C2R>::B, NT = Len<L, E_C2R>::NT, H = L / 2;
+  extern __shared__ float2 sm32[];
+  float2* A = sm32;
+  float2* tws = sm32 + RB * SL;
+  const int row0 = blockIdx.x * RB;
+  const int nb = min(RB, nrows - row0);
+  const int twStep = twLen / (2 * L);
+  for (int idx = threadIdx.x; idx < RB * (L + 1); idx += NT) {
+    const int r = idx / (L + 1), k = idx - r * (L + 1);
+    if (r < nb) cp_async8(A + r * SL + pad(k), in + (size_t)(row0 + r) * inStride + k);
+  }
+  cp_async_commit();
+  load_twiddles<L>(tws, tw, twLen);
+  cp_async_wait<0>();
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < RB * H; idx += NT) {
+    const int r = idx / H, k = idx & (H - 1);
+    if (r >= nb) continue;
+    float2* a = A + r * SL;
+    const int kk[2] = {k, k == 0 ? H : L - k};
+    float2 Xa = a[pad(k)], Xb = a[pad(k == 0 ? L : L - k)];
+    if (k == 0) { Xa.y = 0; Xb.y = 0; }
+    float2 res[2];
+    for (int e = 0; e < 2; e++) {
+      const int kq = kk[e];
+      float2 Xk, XL;
+      if (e == 0) { Xk = Xa; XL = Xb; }
+      else if (k == 0) { Xk = a[pad(H)]; XL = Xk; }
+      else { Xk = Xb; XL = Xa; }
+      const float2 Xc = conjg(XL);
+      const float2 sv = cadd(Xk, Xc), d = csub(Xk, Xc);
+      const float2 t = cmul(conjg(tw[kq * twStep]), d);
+      res[e] = make_float2(sv.x - t.y, sv.y + t.x);
+    }
+    a[pad(kk[0])] = res[0];
+    a[pad(kk[1])] = res[1];
+  }
+  __syncthreads();
+  fft_inplace<L, true, false, HOUT, E_C2R>(A, nb, tws);
+  const int half = (ncolsOut + 1) / 2;
+  for (int idx = threadIdx.x; idx < nb * half; idx += NT) {
+    const int r = idx / half, n = idx - r * half;
+    const float2 v = A[r * SL + pad(n)];
+    double* o = out + (size_t)(row0 + r) * outStride;
+    if (2 * n + 1 < ncolsOut) *reinterpret_cast<double2*>(o + 2 * n) = make_double2(v.x, v.y);
+    else o[2 * n] = v.x;
+  }
+}
+
 // ---- cosine-transform solver (FFTW_dirichlet.h:30-130) --------------------
 // DCT-II (FFTW REDFT10, Y_k = 2 sum x_j cos(pi (j+1/2) k / n)) is the real
 // FFT of the even extension y = [x, reversed x] of length 2n:
@@ -790,6 +992,10 @@ template <int L> inline size_t smem_for(size_t extraReals = 0) {
   return sizeof(double2) * ((size_t)Len<L>::B * Len<L>::SL + Len<L>::TW) + sizeof(double) * extraReals;
 }
 
+template <int L> inline size_t smem_for32(size_t extraReals = 0) {
+  return sizeof(float2) * ((size_t)Len<L>::B * Len<L>::SL + Len<L>::TW) + sizeof(float) * extraReals;
+}
+
 #define CUP2D_FFT_LENGTHS(X) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
 
 void set_all_smem() {
@@ -797,7 +1003,10 @@ void set_all_smem() {
              set_smem((const void*)k_rows_c2r<L, false>); set_smem((const void*)k_rows_c2r<L, true>); \
              set_smem((const void*)k_cols<L, false>); set_smem((const void*)k_cols<L, true>); \
              set_smem((const void*)k_dct_rows_fwd<L>); \
-             set_smem((const void*)k_dct_cols<L>); set_smem((const void*)k_dct_rows_inv<L>);
+             set_smem((const void*)k_dct_cols<L>); set_smem((const void*)k_dct_rows_inv<L>); \
+             set_smem((const void*)k_rows_r2c32<L, false>); set_smem((const void*)k_rows_r2c32<L, true>); \
+             set_smem((const void*)k_rows_c2r32<L, false>); set_smem((const void*)k_rows_c2r32<L, true>); \
+             set_smem((const void*)k_cols32<L, false>); set_smem((const void*)k_cols32<L, true>);
   CUP2D_FFT_LENGTHS(X)
 #undef X
 }
@@ -843,6 +1052,53 @@ bool rows_c2r(int L, cudaStream_t st, const double2* in, int inStride, int nrows
         in, inStride, nrows, out, outStride, ncolsOut, tw, twLen); \
     else launch_k(k_rows_c2r<LL, false>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_C2R>::NT, smem_for<LL>(), st,  \
         in, inStride, nrows, out, outStride, ncolsOut, tw, twLen); \
+    return true;
+    CUP2D_FFT_LENGTHS(X)
+#undef X
+  }
+  return false;
+}
+
+bool rows_r2c32(int L, cudaStream_t st, const double* in, int inStride, int nrows, int ncolsIn,
+                float2* out, int outStride, const float2* tw, int twLen, FadeArgs fa, bool halfIn) {
+  switch (L) {
+#define X(LL) case LL: \
+    if (halfIn) launch_k(k_rows_r2c32<LL, true>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_ROWS>::NT, \
+        smem_for32<LL>(), st, in, inStride, nrows, ncolsIn, out, outStride, tw, twLen, fa); \
+    else launch_k(k_rows_r2c32<LL, false>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_ROWS>::NT, \
+        smem_for32<LL>(), st, in, inStride, nrows, ncolsIn, out, outStride, tw, twLen, fa); \
+    return true;
+    CUP2D_FFT_LENGTHS(X)
+#undef X
+  }
+  return false;
+}
+
+bool cols32(int L, cudaStream_t st, float2* data, int stride, int ncols, int nrowsIn, int nrowsOut,
+            const float* ghat, int mode, const float2* tw, int twLen, double norm, int MXp, int MYp) {
+  switch (L) {
+#define X(LL) case LL: \
+    if (mode == 0) launch_k(k_cols32<LL, true>, (ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_COLS>::NT, \
+        smem_for32<LL>((size_t)(LL / 2 + 1) * Len<LL>::B), st, data, stride, ncols, nrowsIn, nrowsOut, \
+        ghat, mode, tw, twLen, norm, MXp, MYp); \
+    else launch_k(k_cols32<LL, false>, (ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_COLS>::NT, \
+        smem_for32<LL>((size_t)(LL / 2 + 1) * Len<LL>::B), st, data, stride, ncols, nrowsIn, nrowsOut, \
+        ghat, mode, tw, twLen, norm, MXp, MYp); \
+    return true;
+    CUP2D_FFT_LENGTHS(X)
+#undef X
+  }
+  return false;
+}
+
+bool rows_c2r32(int L, cudaStream_t st, const float2* in, int inStride, int nrows, double* out, int outStride,
+                int ncolsOut, const float2* tw, int twLen, bool halfOut) {
+  switch (L) {
+#define X(LL) case LL: \
+    if (halfOut) launch_k(k_rows_c2r32<LL, true>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_C2R>::NT, \
+        smem_for32<LL>(), st, in, inStride, nrows, out, outStride, ncolsOut, tw, twLen); \
+    else launch_k(k_rows_c2r32<LL, false>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_C2R>::NT, \
+        smem_for32<LL>(), st, in, inStride, nrows, out, outStride, ncolsOut, tw, twLen); \
     return true;
     CUP2D_FFT_LENGTHS(X)
 #undef X
@@ -936,12 +1192,31 @@ Poisson* poisson_create(Ctx& c) {
     cols(P->Lcol, c.stream, P->spec, P->nkx, P->nkx, MYr, P->Lcol / 2 + 1, P->ghat, 1, P->tw, P->twLen, norm, 0, 0);
     CUP2D_LAUNCHED(c);
   }
+  if (c.cfg.precision == CUP2D_PREC_FP32) {
+    // the FP32 solve: twiddles and G^ formed in FP64 as above, then rounded
+    P->fp32 = true;
+    std::vector<float2> tw32(P->twLen);
+    for (int k = 0; k < P->twLen; k++) tw32[k] = make_float2((float)tw[k].x, (float)tw[k].y);
+    if (cudaMalloc(&P->tw32, sizeof(float2) * P->twLen) != cudaSuccess) { poisson_destroy(P); return nullptr; }
+    cudaMemcpy(P->tw32, tw32.data(), sizeof(float2) * P->twLen, cudaMemcpyHostToDevice);
+    if (P->type == CUP2D_POISSON_FREESPACE) {
+      const size_t ng = (size_t)(P->Lcol / 2 + 1) * P->nkx;
+      std::vector<double> g64(ng);
+      std::vector<float> g32(ng);
+      if (cudaStreamSynchronize(c.stream) != cudaSuccess ||
+          cudaMemcpy(g64.data(), P->ghat, sizeof(double) * ng, cudaMemcpyDeviceToHost) != cudaSuccess ||
+          cudaMalloc(&P->ghat32, sizeof(float) * ng) != cudaSuccess) { poisson_destroy(P); return nullptr; }
+      for (size_t i = 0; i < ng; i++) g32[i] = (float)g64[i];
+      cudaMemcpy(P->ghat32, g32.data(), sizeof(float) * ng, cudaMemcpyHostToDevice);
+    }
+  }
   return P;
 }
 
 void poisson_destroy(Poisson* P) {
   if (!P) return;
   cudaFree(P->spec); cudaFree(P->ghat); cudaFree(P->tw); cudaFree(P->cosX); cudaFree(P->cosY);
+  cudaFree(P->tw32); cudaFree(P->ghat32);
   delete P;
 }
 
@@ -958,8 +1233,12 @@ void poisson_rows_fwd(Ctx& c) {
     return;
   }
   // free space: the row's zero padding is the upper half of the length-Lrow sequence
-  rows_r2c(P->Lrow, c.stream, c.rhs, Nx, Ny, Nx, 0, P->spec, P->nkx, P->tw, P->twLen, fa, c.g.h, Nx, Ny,
-           P->type == CUP2D_POISSON_FREESPACE);
+  if (P->fp32)
+    rows_r2c32(P->Lrow, c.stream, c.rhs, Nx, Ny, Nx, reinterpret_cast<float2*>(P->spec), P->nkx, P->tw32,
+               P->twLen, fa, P->type == CUP2D_POISSON_FREESPACE);
+  else
+    rows_r2c(P->Lrow, c.stream, c.rhs, Nx, Ny, Nx, 0, P->spec, P->nkx, P->tw, P->twLen, fa, c.g.h, Nx, Ny,
+             P->type == CUP2D_POISSON_FREESPACE);
   CUP2D_LAUNCHED(c);
 }
 
@@ -969,10 +1248,18 @@ void poisson_cols(Ctx& c) {
   if (P->type == CUP2D_POISSON_COSINE) {
     dct_cols(P->Lcol, c.stream, reinterpret_cast<double*>(P->spec), Nx, Ny, P->cosX, P->cosY, P->tol, P->tw, P->twLen);
   } else if (P->type == CUP2D_POISSON_FREESPACE) {
-    cols(P->Lcol, c.stream, P->spec, P->nkx, P->nkx, Ny, Ny, P->ghat, 0, P->tw, P->twLen, 0.0, 0, 0);
+    if (P->fp32)
+      cols32(P->Lcol, c.stream, reinterpret_cast<float2*>(P->spec), P->nkx, P->nkx, Ny, Ny, P->ghat32, 0,
+             P->tw32, P->twLen, 0.0, 0, 0);
+    else
+      cols(P->Lcol, c.stream, P->spec, P->nkx, P->nkx, Ny, Ny, P->ghat, 0, P->tw, P->twLen, 0.0, 0, 0);
   } else {
     const double norm = 1.0 / ((double)Nx * (double)Ny);
-    cols(P->Lcol, c.stream, P->spec, P->nkx, P->nkx, Ny, Ny, nullptr, 2, P->tw, P->twLen, norm, Nx, Ny);
+    if (P->fp32)
+      cols32(P->Lcol, c.stream, reinterpret_cast<float2*>(P->spec), P->nkx, P->nkx, Ny, Ny, nullptr, 2,
+             P->tw32, P->twLen, norm, Nx, Ny);
+    else
+      cols(P->Lcol, c.stream, P->spec, P->nkx, P->nkx, Ny, Ny, nullptr, 2, P->tw, P->twLen, norm, Nx, Ny);
   }
   CUP2D_LAUNCHED(c);
 }
@@ -985,8 +1272,12 @@ void poisson_rows_inv(Ctx& c) {
     CUP2D_LAUNCHED(c);
     return;
   }
-  rows_c2r(P->Lrow, c.stream, P->spec, P->nkx, Ny, c.pres, Nx, Nx, P->tw, P->twLen,
-           P->type == CUP2D_POISSON_FREESPACE);                 // free space keeps the first half
+  if (P->fp32)
+    rows_c2r32(P->Lrow, c.stream, reinterpret_cast<const float2*>(P->spec), P->nkx, Ny, c.pres, Nx, Nx,
+               P->tw32, P->twLen, P->type == CUP2D_POISSON_FREESPACE);
+  else
+    rows_c2r(P->Lrow, c.stream, P->spec, P->nkx, Ny, c.pres, Nx, Nx, P->tw, P->twLen,
+             P->type == CUP2D_POISSON_FREESPACE);                 // free space keeps the first half
   CUP2D_LAUNCHED(c);
 }
 

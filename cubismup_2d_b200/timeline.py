@@ -1,7 +1,7 @@
 """In-graph kernel timeline of one step (the trace build).
 
     python -m cubismup_2d_b200.build --trace
-    python -m cubismup_2d_b200.timeline [swimmer|cylinder] [--steps N] [--noflush]
+    python -m cubismup_2d_b200.timeline [swimmer|cylinder] [--steps N] [--noflush] [--fp32]
 
 Runs the workload on the trace build (libcup2d_trace.so, compiled with
 -DCUP2D_TRACE): thread 0 of every CTA of every kernel stamps %globaltimer at
@@ -9,7 +9,7 @@ entry and exit, so each kernel's first start and last end inside one
 graph-replayed step can be read back.  Prints, per kernel, the median over
 the timed steps of its start, end and duration relative to the step's first
 kernel, with the L2 flushed before every step as in bench.py unless
---noflush is given.
+--noflush is given; --fp32 runs the FP32 Poisson transforms (CUP2D_PREC_FP32).
 """
 import argparse
 import ctypes
@@ -37,12 +37,13 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--noflush", action="store_true")
+    ap.add_argument("--fp32", action="store_true")
     a = ap.parse_args(argv)
     if not os.path.exists(build.TRACE_LIB):
         build.build(trace=True)
     abi.LIB_PATH = build.TRACE_LIB
     import torch
-    sim = abi.Simulation(WORKLOADS[a.workload])
+    sim = abi.Simulation(WORKLOADS[a.workload] + (" -precision fp32" if a.fp32 else ""))
     sim.init()
     ctx = sim.ctx
     for comp, f in enumerate(("u", "v")):

@@ -42,7 +42,11 @@ extern "C" {
 #define CUP2D_POISSON_PERIODIC 1    /* "periodic" : FFTW_periodic.h           */
 #define CUP2D_POISSON_COSINE 2      /* "" (default): FFTW_dirichlet.h (DCT)   */
 
-/* arithmetic of the grid fields and of the Poisson solve */
+/* arithmetic: FP64 everywhere (the reference's Real = double), or FP32 for
+ * the free-space and periodic Poisson transforms only -- fields, stencils,
+ * obstacle sums and forces stay FP64, the RHS fade and the pressure written
+ * back are FP64 (no counterpart in the reference, which is FP64 throughout;
+ * not available with the cosine solver: cup2d_create returns ENOTSUP) */
 #define CUP2D_PREC_FP64 0
 #define CUP2D_PREC_FP32 1
 
