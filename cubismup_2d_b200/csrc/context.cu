@@ -443,12 +443,12 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
     if (!fish_fits_on_chip(Nm, F.nseg, c.device))
       return fail(ctx, CUP2D_ENOTSUP, "fish midline too fine: its kernels' staged arrays exceed shared memory");
     // 3 static arrays + 3 midlines of 8 arrays + 16 integrals, one allocation
-    if (!rc) rc = dalloc(ctx, &F.pool, (size_t)27 * Nm + 16);
+    if (!rc) rc = dalloc(ctx, &F.pool, (size_t)28 * Nm + 16);
     if (!rc) rc = dalloc(ctx, &F.seg, F.nseg);
     if (rc) return rc;
     {
       double* q = F.pool;
-      F.rS = q; q += Nm; F.width = q; q += Nm; F.p1f = q; q += Nm;
+      F.rS = q; q += Nm; F.width = q; q += Nm; F.p1f = q; q += Nm; F.w3 = q; q += Nm;
       FishMidline* mids[3] = {&F.mid[0], &F.mid[1], &F.frame};
       for (FishMidline* m : mids) {
         double** a[8] = {&m->rX, &m->rY, &m->vX, &m->vY, &m->norX, &m->norY, &m->vNorX, &m->vNorY};
@@ -483,6 +483,8 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
     CK(cudaMemcpy(F.rS, rS.data(), sizeof(double) * Nm, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(F.width, width.data(), sizeof(double) * Nm, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(F.p1f, p1f.data(), sizeof(double) * Nm, cudaMemcpyHostToDevice));
+    CK(fish_width_cubes(F, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
   }
   c.hshapes.push_back(S);
   c.tiles.push_back(t);

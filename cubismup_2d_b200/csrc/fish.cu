@@ -121,8 +121,13 @@ k_fish_midline(Scalars* sc, const DevShape* sh, int k, FishArrays F, int mode)
       double rx = 0.0, ry = 0.0, vx = 0.0, vy = 0.0;
       norX[0] = nX; norY[0] = nY; vNorX[0] = vnX; vNorY[0] = vnY;
       double sPrev = rS[0];
+      // the next point's inputs are read one iteration ahead, off the
+      // recurrence's chain
+      double cN = curv[0], cdN = curv_dt[0], sN = rS[1];
+#pragma unroll 2
       for (int i = 1; i < Nm; i++) {
-        const double c = curv[i - 1], cd = curv_dt[i - 1], sNow = rS[i];
+        const double c = cN, cd = cdN, sNow = sN;
+        if (i + 1 < Nm) { cN = curv[i]; cdN = curv_dt[i]; sN = rS[i + 1]; }
         const double dksiX = c * nX;
         const double dksiY = c * nY;
         const double dnuX = -c * ksiX;
@@ -146,8 +151,10 @@ k_fish_midline(Scalars* sc, const DevShape* sh, int k, FishArrays F, int mode)
         vKsiY += ds * dvKsiY;
         const double d1 = ksiX * ksiX + ksiY * ksiY;
         const double d2 = nX * nX + nY * nY;
-        // both factors first, so the two sqrt/divide sequences overlap
-        const double nf1 = 1 / sqrt(d1), nf2 = 1 / sqrt(d2);
+        // 1/sqrt(d) as the reference rounds it: the correctly rounded square
+        // root, then the correctly rounded reciprocal (both factors first, so
+        // the two sequences overlap)
+        const double nf1 = __drcp_rn(__dsqrt_rn(d1)), nf2 = __drcp_rn(__dsqrt_rn(d2));
         if (d1 > EPSd) { ksiX *= nf1; ksiY *= nf1; }
         if (d2 > EPSd) { nX *= nf2; nY *= nf2; }
         rX[i] = rx; rY[i] = ry; vX[i] = vx; vY[i] = vy;
@@ -210,7 +217,7 @@ k_fish_midline(Scalars* sc, const DevShape* sh, int k, FishArrays F, int mode)
     for (int i = tid; i < Nm; i += nt) {
       const double ds = dsOf(i);
       const double fac1 = 2 * width[i];
-      const double fac2 = 2 * pow(width[i], 3.0) * (d_ds(i, norX) * norY[i] - d_ds(i, norY) * norX[i]) / 3;
+      const double fac2 = 2 * F.w3[i] * (d_ds(i, norX) * norY[i] - d_ds(i, norY) * norX[i]) / 3;
       a[0] += fac1 * ds / 2;
       a[1] += (rX[i] * fac1 + norX[i] * fac2) * ds / 2;
       a[2] += (rY[i] * fac1 + norY[i] * fac2) * ds / 2;
@@ -237,7 +244,7 @@ k_fish_midline(Scalars* sc, const DevShape* sh, int k, FishArrays F, int mode)
     double a[2] = {0, 0};
     for (int i = tid; i < Nm; i += nt) {
       const double ds = dsOf(i);
-      const double w3 = pow(width[i], 3.0);
+      const double w3 = F.w3[i];                        // pow(width, 3), formed at set-up
       const double fac1 = 2 * width[i];
       const double fac2 = 2 * w3 * (d_ds(i, norX) * norY[i] - d_ds(i, norY) * norX[i]) / 3;
       const double fac3 = 2 * w3 / 3;
@@ -945,6 +952,18 @@ bool fish_fits_on_chip(int Nm, int nseg, int device) {
     if (need[i] + a.sharedSizeBytes > (size_t)optin) return false;
   }
   return true;
+}
+
+// pow(width, 3) of each midline point (FishLibrary.cpp integrals), formed
+// once on the device with the same pow the per-step integrals used
+__global__ void k_fish_w3(FishArrays F) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F.nm; i += gridDim.x * blockDim.x)
+    F.w3[i] = pow(F.width[i], 3.0);
+}
+
+cudaError_t fish_width_cubes(const FishArrays& F, cudaStream_t st) {
+  k_fish_w3<<<(F.nm + 255) / 256, 256, 0, st>>>(F);
+  return cudaGetLastError();
 }
 
 cudaError_t fish_setup_kernels() {

@@ -7,6 +7,7 @@ namespace cup2d {
 struct Ctx;
 
 cudaError_t fish_setup_kernels();          // dynamic shared-memory limits
+cudaError_t fish_width_cubes(const FishArrays& F, cudaStream_t st);   // F.w3 from F.width
 bool fish_fits_on_chip(int Nm, int nseg, int device);   // staged arrays within the opt-in limit
 void launch_fish_midline(Ctx& c, int k, cudaStream_t stream, int mode);
 void launch_fish_place(Ctx& c, int k);

@@ -134,6 +134,7 @@ struct FishMidline {
 // forms the points themselves from the frame midline.
 struct FishArrays {
   double *rS, *width, *p1f;
+  double* w3;                             // pow(width, 3), time-independent
   FishMidline mid[2];
   double* integ;
   FishMidline frame;
