@@ -212,14 +212,15 @@ void enqueue_step(Ctx& c) {
   }
   // the obstacle chain, the step's critical path, stays on the main stream
   // (programmatic launches chain only within a stream)
-  c.recordPlaced = c.nshapes > 0;
+  // advDiff and the RHS divergence beside the obstacle chain: with a fish,
+  // once the tiles are placed -- the fish frame is a single-CTA latency chain
+  // that any kernel beside it slows (measured: even the 12-CTA outflow flux),
+  // while the rasters after it leave most SMs free; with disks only, from
+  // the step's start (advDiff reads no obstacle data)
+  c.recordPlaced = anyFish;
   if (!c.recordPlaced) cudaEventRecord(c.evPlaced, c.stream);
   launch_objects_rest(c);
   c.recordPlaced = false;
-  // advDiff and the RHS divergence beside the obstacle chain, once the tiles
-  // are placed: the placement kernels are single-CTA latency chains that any
-  // kernel beside them slows (measured: even the 12-CTA outflow flux), while
-  // the rasters after them leave most SMs free
   cudaStreamWaitEvent(c.side2, c.evPlaced, 0);
   {
     StreamScope scope(c, c.side2);
