@@ -146,6 +146,28 @@ def max_over_ranks(pg, x):
     return float(t.item())
 
 
+class stdout_to_stderr:
+    """Sends file descriptor 1 to stderr while the compiled reference runs:
+    it prints its set-up messages with printf, and stdout carries only the
+    one JSON line."""
+
+    def __enter__(self):
+        import ctypes
+        self._libc = ctypes.CDLL(None)
+        sys.stdout.flush()
+        self._libc.fflush(None)
+        self._saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        self._libc.fflush(None)
+        os.dup2(self._saved, 1)
+        os.close(self._saved)
+        return False
+
+
 def run_reference(args, world, rank, pg):
     """The reference's own operators (oracle/_ref) on the host cores."""
     name, argline = WORKLOADS[args.workload]
@@ -155,16 +177,17 @@ def run_reference(args, world, rank, pg):
     from cubismup_2d_b200.synthetic import noise_field
     cores = os.cpu_count()
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    r = RefSim(argline)
-    for comp, fname in enumerate(("u", "v")):
-        r.set(fname, r.get(fname) + noise_field(0, comp, r.ny, r.nx))
-    for _ in range(args.warmup):
-        r.step()
-    r.profile_reset()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        r.step()
-    el = time.perf_counter() - t0
+    with stdout_to_stderr():
+        r = RefSim(argline)
+        for comp, fname in enumerate(("u", "v")):
+            r.set(fname, r.get(fname) + noise_field(0, comp, r.ny, r.nx))
+        for _ in range(args.warmup):
+            r.step()
+        r.profile_reset()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            r.step()
+        el = time.perf_counter() - t0
     cells = r.nx * r.ny
     val = cells * args.steps / el / 1e9
     prof = r.profile()
@@ -186,14 +209,15 @@ def run_reference(args, world, rank, pg):
 def cpu_baseline_sample(argline, nsteps=3):
     from oracle.refsim import RefSim
     from cubismup_2d_b200.synthetic import noise_field
-    r = RefSim(argline)
-    for comp, fname in enumerate(("u", "v")):
-        r.set(fname, r.get(fname) + noise_field(0, comp, r.ny, r.nx))
-    r.step()
-    t0 = time.perf_counter()
-    for _ in range(nsteps):
+    with stdout_to_stderr():
+        r = RefSim(argline)
+        for comp, fname in enumerate(("u", "v")):
+            r.set(fname, r.get(fname) + noise_field(0, comp, r.ny, r.nx))
         r.step()
-    el = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for _ in range(nsteps):
+            r.step()
+        el = time.perf_counter() - t0
     return r.nx * r.ny * nsteps / el / 1e9, os.cpu_count(), nsteps
 
 
