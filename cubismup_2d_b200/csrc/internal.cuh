@@ -307,6 +307,26 @@ __device__ __forceinline__ void block_sum(double (&v)[K], double* smem) {
   __syncthreads();
 }
 
+// One warp's fixed-order sum of K values over n rows (value k of row i at
+// p[stride i + k], read through L2): lane l adds rows l, l + 32, ..., then
+// the xor reduce-scatter of block_sum; every lane returns all K totals.  For
+// the last-CTA finishes, whose rows (tiles) number tens: a CTA-wide
+// block_sum would only add barriers.  All 32 lanes of the warp call it.
+template <int K>
+__device__ __forceinline__ void warp_sum_rows(const double* p, int n, int stride, double (&out)[K]) {
+  constexpr int KP = Pow2Up<K>::v, STRIDE = 32 / KP;
+  const int lane = lin_tid() & 31;
+  double x[KP];
+#pragma unroll
+  for (int k = 0; k < KP; k++) x[k] = 0.0;
+  for (int i = lane; i < n; i += 32)
+#pragma unroll
+    for (int k = 0; k < K; k++) x[k] += __ldcg(&p[(size_t)stride * i + k]);
+  const double r = warp_reduce_scatter<KP>(x, lane);
+#pragma unroll
+  for (int k = 0; k < K; k++) out[k] = __shfl_sync(0xffffffffu, r, k * STRIDE);
+}
+
 __device__ __forceinline__ double block_max(double v, double* smem) {
   const int t = lin_tid(), lane = t & 31, wid = t >> 5;
   const int nw = (lin_nthreads() + 31) >> 5;

@@ -216,10 +216,9 @@ k_chi_moments(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ s
   }
   if (!last_block_done(counters + k, gridDim.x)) return;
   const int tid = lin_tid();
-  double I[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int i = tid; i < nt; i += 1024)
-    for (int q = 0; q < 7; q++) I[q] += __ldcg(&mp[7 * i + q]);
-  block_sum<7>(I, red);
+  if (tid >= 32) return;                               // one warp finishes
+  double I[7];
+  warp_sum_rows<7>(mp, nt, 7, I);
   if (tid != 0 || nt == 0) return;
   const double M = I[2];
   double d0 = 0, d1 = 0;
@@ -300,11 +299,9 @@ k_rhs_obst(GridDesc g, DevShape* sh, int k, ObstTiles t, const double* __restric
   if (lin_tid() == 0) for (int q = 0; q < 3; q++) partials[3 * s + q] = acc[q];
   }
   if (!last_block_done(counter, gridDim.x)) return;
-  double tot[3] = {0, 0, 0};
-  const int n = S.ntiles;
-  for (int i = lin_tid(); i < n; i += 1024)
-    for (int q = 0; q < 3; q++) tot[q] += __ldcg(&partials[3 * i + q]);
-  block_sum<3>(tot, red);
+  if (lin_tid() >= 32) return;                           // one warp finishes
+  double tot[3];
+  warp_sum_rows<3>(partials, S.ntiles, 3, tot);
   if (lin_tid() == 0) {                                  // PressureSingle.cpp:185-186
     const double corrDenom = tot[0] > 0 ? tot[1] : tot[2];
     S.rhsCorr = tot[0] / fmax(corrDenom, EPSd);
@@ -408,10 +405,9 @@ k_momenta(GridDesc g, const Scalars* sc, DevShape* sh, AllTiles T, const double*
     if (tid == 0) for (int q = 0; q < 7; q++) mp[7 * s + q] = A[q];
   }
   if (!last_block_done(counters + k, gridDim.x)) return;
-  double A[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int i = tid; i < nt; i += 1024)
-    for (int q = 0; q < 7; q++) A[q] += __ldcg(&mp[7 * i + q]);
-  block_sum<7>(A, red);
+  if (tid >= 32) return;                                // one warp finishes
+  double A[7];
+  warp_sum_rows<7>(mp, nt, 7, A);
   if (tid != 0) return;
   S.s.fluidAngMom = A[6]; S.s.fluidMomX = A[4]; S.s.fluidMomY = A[5];
   S.s.penalDX = A[2]; S.s.penalDY = A[3]; S.s.penalM = A[0]; S.s.penalJ = A[1];
@@ -597,12 +593,9 @@ k_forces(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ u,
   if (lin_tid() == 0) for (int q = 0; q < NFORCE; q++) part[NFORCE * s + q] = F[q];
   }
   if (!last_block_done(counters + k, gridDim.x)) return;
+  if (lin_tid() >= 32) return;                          // one warp finishes
   double tot[NFORCE];
-#pragma unroll
-  for (int q = 0; q < NFORCE; q++) tot[q] = 0;
-  for (int i = lin_tid(); i < S.ntiles; i += 1024)
-    for (int q = 0; q < NFORCE; q++) tot[q] += __ldcg(&part[NFORCE * i + q]);
-  block_sum<NFORCE>(tot, red);
+  warp_sum_rows<NFORCE>(part, S.ntiles, NFORCE, tot);
   if (lin_tid() != 0) return;
   cup2d_shape_state& st = S.s;
   st.perimeter = tot[0]; st.forcex = tot[1]; st.forcey = tot[2];
