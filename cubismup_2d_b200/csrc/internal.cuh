@@ -340,19 +340,19 @@ __device__ __forceinline__ double block_max(double v, double* smem) {
 }
 
 // "last block done" ticket: returns true in every thread of the CTA that
-// finished last.  The counter is re-armed by that CTA.  As in a grid-wide
-// barrier, the CTA barrier orders every thread's earlier writes before
-// thread 0's gpu-scope fence (fences are cumulative), so one fence before
-// the ticket releases the whole CTA's writes, and one fence after it, in
-// the last CTA, acquires everybody else's before the closing barrier.
+// finished last.  The counter is re-armed by that CTA (its next user is a
+// later kernel).  The CTA barrier orders every thread's earlier writes
+// before thread 0's ticket, an acquire-release atomic at gpu scope: its
+// release covers the whole CTA's writes (cumulativity), and in the last CTA
+// its acquire covers everybody else's before the closing barrier.
 __device__ __forceinline__ bool last_block_done(unsigned* counter, unsigned nblocks) {
   __shared__ bool amLast;
   __syncthreads();
   if (lin_tid() == 0) {
-    __threadfence();
-    const unsigned t = atomicAdd(counter, 1u);
+    unsigned t;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(t) : "l"(counter) : "memory");
     amLast = (t == nblocks - 1);
-    if (amLast) { *counter = 0; __threadfence(); }
+    if (amLast) *counter = 0;
   }
   __syncthreads();
   return amLast;
