@@ -84,6 +84,10 @@ template <int L, int E = 16> struct Len {
 constexpr int E_ROWS = 8;
 constexpr int E_C2R = 16;
 constexpr int E_COLS = 16;
+// the same for the FP32 transforms (half the registers per value)
+constexpr int E_ROWS32 = 8;
+constexpr int E_C2R32 = 8;
+constexpr int E_COLS32 = 16;
 
 // Twiddles w^j = exp(-2 pi i j / L), j < L/4, staged in shared memory.
 template <int L, class C>
@@ -624,13 +628,13 @@ k_rows_c2r(const double2* __restrict__ in, int inStride, int nrows, double* __re
 // RHS written back is the one of the FP64 path), rows converted to FP32 as
 // they enter shared memory, the pressure written back in FP64.
 template <int L, bool HIN>
-__global__ void __launch_bounds__(Len<L, E_ROWS>::NT, Len<L, E_ROWS>::MINB)
+__global__ void __launch_bounds__(Len<L, E_ROWS32>::NT, Len<L, E_ROWS32>::MINB)
 k_rows_r2c32(const double* __restrict__ in, int inStride, int nrows, int ncolsIn,
              float2* __restrict__ out, int outStride, const float2* __restrict__ tw, int twLen, FadeArgs fa)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_R2C);
-  constexpr int SL = Len<L, E_ROWS>::SL, RB = Len<L, E_ROWS>::B, NT = Len<L, E_ROWS>::NT;
+  constexpr int SL = Len<L, E_ROWS32>::SL, RB = Len<L, E_ROWS32>::B, NT = Len<L, E_ROWS32>::NT;
   constexpr int PER = (RB * L + NT - 1) / NT;          // value pairs per thread
   extern __shared__ float2 sm32[];
   float2* A = sm32;
@@ -676,7 +680,7 @@ k_rows_r2c32(const double* __restrict__ in, int inStride, int nrows, int ncolsIn
     A[r * SL + pad(n)] = make_float2((float)v[u].x, (float)v[u].y);
   }
   __syncthreads();
-  fft_inplace<L, false, HIN, false, E_ROWS>(A, nb, tws);
+  fft_inplace<L, false, HIN, false, E_ROWS32>(A, nb, tws);
   // even/odd split: X[k] = Fe[k] + W^k Fo[k], W = exp(-i pi / L), k in [0, L]
   const int twStep = twLen / (2 * L);
   for (int idx = threadIdx.x; idx < nb * (L + 1); idx += NT) {
@@ -693,14 +697,14 @@ k_rows_r2c32(const double* __restrict__ in, int inStride, int nrows, int ncolsIn
 // mode 0: forward, x G^, inverse, keep nrowsOut rows; mode 2: the periodic
 // multiplier -1/|k|^2 / (MX MY) (formed in FP64, applied in FP32)
 template <int L, bool FS>
-__global__ void __launch_bounds__(Len<L, E_COLS>::NT, Len<L, E_COLS>::MINB)
+__global__ void __launch_bounds__(Len<L, E_COLS32>::NT, Len<L, E_COLS32>::MINB)
 k_cols32(float2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrowsOut,
          const float* __restrict__ ghat, int mode, const float2* __restrict__ tw, int twLen,
          double norm, int MXp, int MYp)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_COLS);
-  constexpr int SL = Len<L, E_COLS>::SL, CB = Len<L, E_COLS>::B, NT = Len<L, E_COLS>::NT, GR = L / 2 + 1;
+  constexpr int SL = Len<L, E_COLS32>::SL, CB = Len<L, E_COLS32>::B, NT = Len<L, E_COLS32>::NT, GR = L / 2 + 1;
   extern __shared__ float2 sm32[];
   float2* A = sm32;
   float2* tws = sm32 + CB * SL;
@@ -726,13 +730,13 @@ k_cols32(float2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrow
   cp_async_wait<0>();
   __syncthreads();
   if (mode == 0) {
-    fft_convolve<L, FS, FS, E_COLS>(A, nb, tws, [&](int j, int r, float2 z) {
+    fft_convolve<L, FS, FS, E_COLS32>(A, nb, tws, [&](int j, int r, float2 z) {
       const int ky = r <= L / 2 ? r : L - r;
       const float f = Gs[ky * CB + j];
       return make_float2(z.x * f, z.y * f);
     });
   } else {
-    fft_convolve<L, FS, FS, E_COLS>(A, nb, tws, [&](int j, int r, float2 z) {
+    fft_convolve<L, FS, FS, E_COLS32>(A, nb, tws, [&](int j, int r, float2 z) {
       // FFTW_periodic::_solve_spectral (FFTW_periodic.h:77-92)
       const int i = c0 + j;
       if (i == 0 && r == 0) return make_float2(0, 0);
@@ -752,13 +756,13 @@ k_cols32(float2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrow
 // inverse real FFT of length 2L from X[0..L] (float2); writes the first
 // ncolsOut values in FP64
 template <int L, bool HOUT>
-__global__ void __launch_bounds__(Len<L, E_C2R>::NT, Len<L, E_C2R>::MINB)
+__global__ void __launch_bounds__(Len<L, E_C2R32>::NT, Len<L, E_C2R32>::MINB)
 k_rows_c2r32(const float2* __restrict__ in, int inStride, int nrows, double* __restrict__ out, int outStride,
              int ncolsOut, const float2* __restrict__ tw, int twLen)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_C2R);
-  constexpr int SL = Len<L, E_C2R>::SL, RB = Len<L, E_C2R>::B, NT = Len<L, E_C2R>::NT, H = L / 2;
+  constexpr int SL = Len<L, E_C2R32>::SL, RB = Len<L, E_C2R32>::B, NT = Len<L, E_C2R32>::NT, H = L / 2;
   extern __shared__ float2 sm32[];
   float2* A = sm32;
   float2* tws = sm32 + RB * SL;
@@ -796,7 +800,7 @@ k_rows_c2r32(const float2* __restrict__ in, int inStride, int nrows, double* __r
     a[pad(kk[1])] = res[1];
   }
   __syncthreads();
-  fft_inplace<L, true, false, HOUT, E_C2R>(A, nb, tws);
+  fft_inplace<L, true, false, HOUT, E_C2R32>(A, nb, tws);
   const int half = (ncolsOut + 1) / 2;
   for (int idx = threadIdx.x; idx < nb * half; idx += NT) {
     const int r = idx / half, n = idx - r * half;
@@ -1063,9 +1067,9 @@ bool rows_r2c32(int L, cudaStream_t st, const double* in, int inStride, int nrow
                 float2* out, int outStride, const float2* tw, int twLen, FadeArgs fa, bool halfIn) {
   switch (L) {
 #define X(LL) case LL: \
-    if (halfIn) launch_k(k_rows_r2c32<LL, true>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_ROWS>::NT, \
+    if (halfIn) launch_k(k_rows_r2c32<LL, true>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_ROWS32>::NT, \
         smem_for32<LL>(), st, in, inStride, nrows, ncolsIn, out, outStride, tw, twLen, fa); \
-    else launch_k(k_rows_r2c32<LL, false>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_ROWS>::NT, \
+    else launch_k(k_rows_r2c32<LL, false>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_ROWS32>::NT, \
         smem_for32<LL>(), st, in, inStride, nrows, ncolsIn, out, outStride, tw, twLen, fa); \
     return true;
     CUP2D_FFT_LENGTHS(X)
@@ -1078,10 +1082,10 @@ bool cols32(int L, cudaStream_t st, float2* data, int stride, int ncols, int nro
             const float* ghat, int mode, const float2* tw, int twLen, double norm, int MXp, int MYp) {
   switch (L) {
 #define X(LL) case LL: \
-    if (mode == 0) launch_k(k_cols32<LL, true>, (ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_COLS>::NT, \
+    if (mode == 0) launch_k(k_cols32<LL, true>, (ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_COLS32>::NT, \
         smem_for32<LL>((size_t)(LL / 2 + 1) * Len<LL>::B), st, data, stride, ncols, nrowsIn, nrowsOut, \
         ghat, mode, tw, twLen, norm, MXp, MYp); \
-    else launch_k(k_cols32<LL, false>, (ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_COLS>::NT, \
+    else launch_k(k_cols32<LL, false>, (ncols + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_COLS32>::NT, \
         smem_for32<LL>((size_t)(LL / 2 + 1) * Len<LL>::B), st, data, stride, ncols, nrowsIn, nrowsOut, \
         ghat, mode, tw, twLen, norm, MXp, MYp); \
     return true;
@@ -1095,9 +1099,9 @@ bool rows_c2r32(int L, cudaStream_t st, const float2* in, int inStride, int nrow
                 int ncolsOut, const float2* tw, int twLen, bool halfOut) {
   switch (L) {
 #define X(LL) case LL: \
-    if (halfOut) launch_k(k_rows_c2r32<LL, true>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_C2R>::NT, \
+    if (halfOut) launch_k(k_rows_c2r32<LL, true>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_C2R32>::NT, \
         smem_for32<LL>(), st, in, inStride, nrows, out, outStride, ncolsOut, tw, twLen); \
-    else launch_k(k_rows_c2r32<LL, false>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_C2R>::NT, \
+    else launch_k(k_rows_c2r32<LL, false>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_C2R32>::NT, \
         smem_for32<LL>(), st, in, inStride, nrows, out, outStride, ncolsOut, tw, twLen); \
     return true;
     CUP2D_FFT_LENGTHS(X)
