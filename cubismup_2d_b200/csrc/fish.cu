@@ -296,6 +296,10 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_FRAME);
   CUP2D_TRACE_MARK(TRACE_ITEMS - 1, 0);
+  // the body's motion of this step (written by step_begin), loaded now so
+  // that the reads overlap the rotation and normal phases instead of
+  // stalling the segment chain behind a barrier
+  const double cosO = S.cosO, sinO = S.sinO, cen0 = S.s.center[0], cen1 = S.s.center[1];
   if (tid == 0) {                                       // Fish.cpp:87-93 bookkeeping
     S.f.area_internal = integ[0];
     S.f.CoM_internal[0] = integ[1]; S.f.CoM_internal[1] = integ[2];
@@ -339,7 +343,7 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
   // segment take its midline points (the bounding box is a min / max, exact
   // in any order), then lane 0 of the group finishes the segment.
   const int Nseg = F.nseg;
-  const double R00 = S.cosO, R01 = -S.sinO, R10 = S.sinO, R11 = S.cosO;   // rotation by the orientation
+  const double R00 = cosO, R01 = -sinO, R10 = sinO, R11 = cosO;   // rotation by the orientation
   const double h = g.h;
   __shared__ double box[4];
   const int g16 = tid >> 4, l16 = tid & 15;
@@ -375,8 +379,8 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
       // AreaSegment::changeToComputationalFrame (FishLibrary.cpp:295-342)
       const double nI0 = R00 * 1 + R01 * 0, nI1 = R10 * 1 + R11 * 0;
       const double nJ0 = R00 * 0 + R01 * 1, nJ1 = R10 * 0 + R11 * 1;
-      sg.c[0] = R00 * c0 + R01 * c1 + S.s.center[0];
-      sg.c[1] = R10 * c0 + R11 * c1 + S.s.center[1];
+      sg.c[0] = R00 * c0 + R01 * c1 + cen0;
+      sg.c[1] = R10 * c0 + R11 * c1 + cen1;
       const double magI = sqrt(nI0 * nI0 + nI1 * nI1), magJ = sqrt(nJ0 * nJ0 + nJ1 * nJ1);
       const double invMagI = 1 / magI, invMagJ = 1 / magJ;
       CUP2D_TRACE_MARK_AFTER(TRACE_ITEMS - 2, 1, invMagI + invMagJ);
