@@ -321,6 +321,7 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
               cudaStreamCreateWithFlags(&c.side2, cudaStreamNonBlocking) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evFork, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evStart, cudaEventDisableTiming) != cudaSuccess ||
+              cudaEventCreateWithFlags(&c.evSideMid, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evJoin, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evObj, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evObjDone, cudaEventDisableTiming) != cudaSuccess ||
@@ -357,6 +358,7 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   if (c.evObjDone) cudaEventDestroy(c.evObjDone);
   if (c.evFork) cudaEventDestroy(c.evFork);
   if (c.evStart) cudaEventDestroy(c.evStart);
+  if (c.evSideMid) cudaEventDestroy(c.evSideMid);
   if (c.evJoin) cudaEventDestroy(c.evJoin);
   if (c.evPres) cudaEventDestroy(c.evPres);
   if (c.evMom) cudaEventDestroy(c.evMom);
@@ -457,6 +459,8 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
       }
       F.integ = q;
     }
+    // no midline formed yet: integrals (with their time) NaN (all-ones bytes)
+    CK(cudaMemset(F.integ, 0xff, sizeof(double) * 16));
     // interior-point layout of PutFishOnBlocks::constructInternl
     // (FishLibrary.cpp:594-596): Nw = floor(width/h) points each side
     std::vector<int> nw(Nm), off(Nm + 1, 0);
@@ -534,6 +538,7 @@ int cup2d_init(cup2d_ctx* ctx) {
   CK(cudaStreamSynchronize(c.stream));
   if ((rc = check_launch(ctx))) return rc;
   c.initialised = true;
+  c.midByGraph = false;
   return CUP2D_OK;
 }
 
@@ -560,6 +565,19 @@ int cup2d_calc_dt(cup2d_ctx* ctx, double* dt_out) {
 int cup2d_put_objects(cup2d_ctx* ctx, double dt) {
   STAGE_PROLOGUE
   launch_objects(c, false);
+  // the next step's midlines (time + dt) on the side stream, beside the
+  // rest of this step; the next call takes them if the time matches
+  bool anyFish = false;
+  for (int k = 0; k < c.nshapes; k++) anyFish |= c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK;
+  if (anyFish) {
+    CK(cudaEventRecord(c.evFork, c.stream));
+    CK(cudaStreamWaitEvent(c.side, c.evFork, 0));
+    for (int k = 0; k < c.nshapes; k++)
+      if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.side, 1);
+    CK(cudaEventRecord(c.evSideMid, c.side));
+    c.sideMidPending = true;
+  }
+  c.midByGraph = false;
   return check_launch(ctx);
 }
 
@@ -599,6 +617,17 @@ int cup2d_advance(cup2d_ctx* ctx, int nsteps) {
   if (c.cur != 0) {
     // a stage was called on its own: finish in eager mode until parity returns
     return fail(ctx, CUP2D_ESTATE, "velocity buffers out of step order");
+  }
+  if (c.sideMidPending) {                   // a midline formed ahead by the operator path
+    CK(cudaStreamWaitEvent(c.stream, c.evSideMid, 0));
+    c.sideMidPending = false;
+  }
+  if (!c.midByGraph) {
+    // graph steps form each next step's midline; the first one needs the
+    // current step's (formed here unless already present)
+    for (int k = 0; k < c.nshapes; k++)
+      if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.stream, 4);
+    c.midByGraph = true;
   }
   if (!c.graph) {
     const long long before = c.launches;
@@ -714,6 +743,7 @@ int cup2d_set_scalars(cup2d_ctx* ctx, double time, double dt, int step, double u
   s.time = time; s.dt = dt; s.step = step; s.uinfx = uinfx; s.uinfy = uinfy;
   s.dtNextValid = 0;
   CK(cudaMemcpy(c.dsc, &s, sizeof(Scalars), cudaMemcpyHostToDevice));
+  c.midByGraph = false;
   return CUP2D_OK;
 }
 

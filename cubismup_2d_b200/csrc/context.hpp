@@ -56,6 +56,12 @@ struct Ctx {
   bool recordPlaced = false;
   cudaEvent_t evMaxFree = nullptr;  // the next step's speed maximum over free cells
   bool graphStep = false;           // enqueue_step is recording a graph step
+  // the operator-by-operator path forms the next step's fish midlines on
+  // `side` (evSideMid after them), checked by the next call; midByGraph:
+  // the current step's midlines came from a graph step's side branch
+  cudaEvent_t evSideMid = nullptr;
+  bool sideMidPending = false;
+  bool midByGraph = false;
 
   cudaGraphExec_t graph = nullptr;
   long long launches = 0;

@@ -57,7 +57,10 @@ __device__ __forceinline__ void cubic_interp(double x0, double x1, double x, dou
 //   (dtNextValid; the step copies dtNext into dt), and records in
 //   sc->midlineEarly whether it ran.  Reads only the shape's configuration,
 //   time, step and dtNext, which nothing changes before the step's end;
-// mode 3: mode 1 unless mode 2 ran.
+// mode 3: mode 1 unless mode 2 ran;
+// mode 4: mode 0 unless buffer (step & 1) already holds the midline of
+//   sc->time (the integrals keep the time they were formed at; a fresh
+//   buffer holds NaN), i.e. unless an earlier launch formed it ahead.
 __global__ void __launch_bounds__(512)
 k_fish_midline(Scalars* sc, const DevShape* sh, int k, FishArrays F, int mode)
 {
@@ -69,6 +72,7 @@ k_fish_midline(Scalars* sc, const DevShape* sh, int k, FishArrays F, int mode)
     if (!ok) return;
   }
   if (mode == 3 && sc->midlineEarly) return;
+  if (mode == 4 && F.integ[8 * (sc->step & 1) + 7] == sc->time) return;
   CUP2D_TRACE_SCOPE(TR_MIDLINE);
   CUP2D_TRACE_MARK(TRACE_ITEMS - 3, 0);
   extern __shared__ double smem[];
@@ -76,8 +80,9 @@ k_fish_midline(Scalars* sc, const DevShape* sh, int k, FishArrays F, int mode)
   __shared__ double bc[4];
   const DevShape& S = sh[k];
   const int Nm = F.nm, nt = blockDim.x;
-  const double t = mode == 0 ? sc->time : sc->time + (mode == 2 ? sc->dtNext : sc->dt);
-  const int p = mode == 0 ? sc->step & 1 : (sc->step + 1) & 1;
+  const bool now = mode == 0 || mode == 4;              // this step's midline
+  const double t = now ? sc->time : sc->time + (mode == 2 ? sc->dtNext : sc->dt);
+  const int p = now ? sc->step & 1 : (sc->step + 1) & 1;
   const double L = S.cfg.length, T = S.cfg.Tperiod;
   double* rS = smem;          double* width = rS + Nm;
   double* rK = width + Nm;    double* vK = rK + Nm;

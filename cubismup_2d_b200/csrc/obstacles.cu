@@ -624,9 +624,14 @@ void launch_objects_begin(Ctx& c, bool midlineReady) {
   if (c.nshapes == 0) return;
   // fish midlines at the current time (Fish.cpp:79-95) unless the previous
   // step already computed them on its side branch
-  if (!midlineReady)
+  if (!midlineReady) {
+    if (c.sideMidPending) {                 // formed ahead on the side stream
+      cudaStreamWaitEvent(c.stream, c.evSideMid, 0);
+      c.sideMidPending = false;
+    }
     for (int k = 0; k < c.nshapes; k++)
-      if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.stream, 0);
+      if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.stream, 4);
+  }
   launch_k(k_obj_begin, tile_ctas(c, c.maxCapacity), 256, 0, c.stream, 
       c.g, c.dsc, c.dshapes, c.nshapes, all_tiles(c), c.chi, c.sdf);
   CUP2D_LAUNCHED(c);

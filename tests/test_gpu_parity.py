@@ -182,6 +182,28 @@ def test_graph_replay_matches_eager(args):
         assert a.ctx.shape(k) == b.ctx.shape(k), k
 
 
+@pytest.mark.parametrize("args", [FISH, TANDEM], ids=["fish", "tandem"])
+def test_operator_steps_then_graph_steps(args):
+    """Operator-by-operator steps (which form the next midline ahead on a
+    side stream) followed by graph steps: bitwise the same as operator steps
+    throughout (the graph's first step takes or forms the current midline)."""
+    a = Simulation(args); a.init()
+    b = Simulation(args); b.init()
+    for comp, name in enumerate(("u", "v")):
+        n = noise_field(2, comp, a.ctx.ny, a.ctx.nx)
+        a.ctx.set(name, n); b.ctx.set(name, n)
+    for _ in range(6):
+        a.advance(a.calcMaxTimestep())
+    for _ in range(3):
+        b.advance(b.calcMaxTimestep())
+    b.ctx.advance(3)
+    b.ctx.sync()
+    for name in ("u", "v", "pres", "chi"):
+        assert np.array_equal(a.ctx.get(name), b.ctx.get(name)), name
+    for k in range(args.count("fish ")):
+        assert a.ctx.shape(k) == b.ctx.shape(k), k
+
+
 # ---- against the committed golden fixtures (no reference build needed) -------
 
 GOLDEN_DIR = __import__("os").path.join(__import__("os").path.dirname(__import__("os").path.abspath(__file__)), "golden")
