@@ -243,8 +243,16 @@ void enqueue_step(Ctx& c) {
 // The graph step's calcMaxTimestep reuses the maximum formed at the end of
 // the previous graph step only while nothing else has touched the state.
 cudaError_t invalidate_dt_next(Ctx& c) {
+  if (!c.dtValidMaybe) return cudaSuccess;
+  c.dtValidMaybe = c.dtCarried = false;
   return cudaMemsetAsync(&c.dsc->dtNextValid, 0, sizeof(int), c.stream);
 }
+
+// An ABI call outside the operator sequence: the in-place RHS and the
+// placement mark no longer describe the state the next stage sees.
+void forget_chain(Ctx& c) { c.rhsFresh = false; c.placedPending = false; }
+
+bool same_bits(double a, double b) { return std::memcmp(&a, &b, sizeof(double)) == 0; }
 
 extern "C" {
 
@@ -322,6 +330,8 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
               cudaEventCreateWithFlags(&c.evFork, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evStart, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evSideMid, cudaEventDisableTiming) != cudaSuccess ||
+              cudaEventCreateWithFlags(&c.evDtNext, cudaEventDisableTiming) != cudaSuccess ||
+              cudaMallocHost(&c.pin, sizeof(Ctx::HostPin)) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evJoin, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evObj, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evObjDone, cudaEventDisableTiming) != cudaSuccess ||
@@ -359,6 +369,8 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   if (c.evFork) cudaEventDestroy(c.evFork);
   if (c.evStart) cudaEventDestroy(c.evStart);
   if (c.evSideMid) cudaEventDestroy(c.evSideMid);
+  if (c.evDtNext) cudaEventDestroy(c.evDtNext);
+  if (c.pin) cudaFreeHost(c.pin);
   if (c.evJoin) cudaEventDestroy(c.evJoin);
   if (c.evPres) cudaEventDestroy(c.evPres);
   if (c.evMom) cudaEventDestroy(c.evMom);
@@ -517,6 +529,8 @@ int cup2d_init(cup2d_ctx* ctx) {
   c.cur = 0;
   // Simulation::reset (Simulation.cpp:232-241): resetAll, IC, objects at t=0, ApplyObjVel
   if ((rc = upload_scalars_reset(ctx))) return rc;
+  c.dtValidMaybe = c.dtCarried = false;
+  forget_chain(c);
   for (int k = 0; k < c.nshapes; k++) {
     DevShape& S = c.hshapes[k];
     const ShapeCfg& f = S.cfg;
@@ -532,6 +546,7 @@ int cup2d_init(cup2d_ctx* ctx) {
   if ((rc = upload_shapes(ctx))) return rc;
   launch_ic(c);
   launch_set_dt(c, 0.0);
+  c.devDt = 0.0;
   launch_objects(c, false);
   launch_obj_vel_on_grid(c);
   launch_apply_obj_vel(c);
@@ -545,26 +560,64 @@ int cup2d_init(cup2d_ctx* ctx) {
 int cup2d_calc_dt(cup2d_ctx* ctx, double* dt_out) {
   if (!ctx || !ctx->c.initialised) return ctx ? fail(ctx, CUP2D_ESTATE, "not initialised") : CUP2D_EINVAL;
   Ctx& c = ctx->c;
+  forget_chain(c);                          // sets sc->dt (and overwrites the grid partials)
+  if (c.dtCarried) {
+    // formed by the last step end from this very state
+    launch_take_dt_next(c);
+    int rc = check_launch(ctx);
+    if (rc) return rc;
+    c.devDt = NAN;
+    if (dt_out) {
+      CK(cudaEventSynchronize(c.evDtNext));
+      *dt_out = c.devDt = c.pin->dtNext;
+    }
+    return CUP2D_OK;
+  }
   launch_max_u_dt(c);
   int rc = check_launch(ctx);
   if (rc) return rc;
+  c.devDt = NAN;
   if (dt_out) {
-    CK(cudaMemcpyAsync(dt_out, &c.dsc->dt, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(&c.pin->dt, &c.dsc->dt, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
+    *dt_out = c.devDt = c.pin->dt;
   }
   return CUP2D_OK;
 }
 
+// Every stage: the state changes (a carried dt no longer holds) and the
+// stage's dt argument becomes sim.dt -- each launched only when the host
+// mirrors say the device does not hold it already.  `prologueLaunched`:
+// the stage enqueued work of its own before its body.
 #define STAGE_PROLOGUE                                                           \
   if (!ctx) return CUP2D_EINVAL;                                                 \
   Ctx& c = ctx->c;                                                               \
   if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");         \
+  bool prologueLaunched = c.dtValidMaybe;                                        \
   CK(invalidate_dt_next(c));                                                     \
-  if (dt >= 0) launch_set_dt(c, dt);
+  if (dt >= 0 && !same_bits(dt, c.devDt)) {                                      \
+    launch_set_dt(c, dt);                                                        \
+    c.devDt = dt;                                                                \
+    c.rhsFresh = false;                         /* the RHS scales with 1/dt */   \
+    prologueLaunched = true;                                                     \
+  }                                                                              \
+  (void)prologueLaunched;
 
 int cup2d_put_objects(cup2d_ctx* ctx, double dt) {
   STAGE_PROLOGUE
-  launch_objects(c, false);
+  forget_chain(c);
+  // advDiff may start beside the obstacle chain once the tiles are placed
+  // (with a fish) or right after the body motion (disks only), as in a
+  // graph step
+  bool anyFishShape = false;
+  for (int k = 0; k < c.nshapes; k++) anyFishShape |= c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK;
+  launch_objects_begin(c, false);
+  if (c.nshapes > 0) {
+    c.recordPlaced = anyFishShape;
+    if (!anyFishShape) CK(cudaEventRecord(c.evPlaced, c.stream));
+    launch_objects_rest(c);
+    c.recordPlaced = false;
+  }
   // the next step's midlines (time + dt) on the side stream, beside the
   // rest of this step; the next call takes them if the time matches
   bool anyFish = false;
@@ -578,19 +631,40 @@ int cup2d_put_objects(cup2d_ctx* ctx, double dt) {
     c.sideMidPending = true;
   }
   c.midByGraph = false;
+  c.placedPending = c.nshapes > 0;
   return check_launch(ctx);
 }
 
+// advDiff (advDiff.cpp:14-116) with PressureSingle's RHS divergence
+// (PressureSingle.cpp:112-128) formed in place, as in a graph step; right
+// after PutObjectsOnGrid it runs on side2 beside the obstacle chain (it
+// reads no obstacle data) and joins the main stream before returning.
 int cup2d_adv_diff(cup2d_ctx* ctx, double dt) {
   STAGE_PROLOGUE
-  launch_advdiff(c);
-  launch_outflow(c);
+  const bool beside = c.placedPending && !prologueLaunched;
+  c.placedPending = false;
+  if (beside) {
+    CK(cudaStreamWaitEvent(c.side2, c.evPlaced, 0));
+    {
+      StreamScope scope(c, c.side2);
+      launch_outflow_flux(c);
+      launch_advdiff_rhs_div(c);
+    }
+    CK(cudaEventRecord(c.evObjDone, c.side2));
+    CK(cudaStreamWaitEvent(c.stream, c.evObjDone, 0));
+  } else {
+    launch_outflow_flux(c);
+    launch_advdiff_rhs_div(c);
+  }
+  c.rhsFresh = true;
   return check_launch(ctx);
 }
 
 int cup2d_pressure_single(cup2d_ctx* ctx, double dt) {
   STAGE_PROLOGUE
-  launch_rhs_div(c);
+  c.placedPending = false;
+  if (!c.rhsFresh) launch_rhs_div(c);       // else formed by advDiff at this dt
+  c.rhsFresh = false;
   launch_rhs_obstacles(c);
   poisson_solve(c);
   launch_pressure_tail(c);
@@ -599,13 +673,25 @@ int cup2d_pressure_single(cup2d_ctx* ctx, double dt) {
 
 int cup2d_compute_forces(cup2d_ctx* ctx, double dt) {
   STAGE_PROLOGUE
+  forget_chain(c);
   launch_forces(c);
   return check_launch(ctx);
 }
 
+// Simulation.cpp:289-290 (t += dt, step += 1), ending like a graph step:
+// the next step's calcMaxTimestep is formed on the final velocity and its
+// dt copied to pinned host memory, so that cup2d_calc_dt returns it
+// without a round trip while nothing changes the state in between.
 int cup2d_end_step(cup2d_ctx* ctx) {
   if (!ctx) return CUP2D_EINVAL;
-  launch_end_step(ctx->c);
+  Ctx& c = ctx->c;
+  if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
+  forget_chain(c);
+  launch_max_next(c);                       // sc->maxNext is zero between steps
+  launch_end_step_dt(c);
+  CK(cudaMemcpyAsync(&c.pin->dtNext, &c.dsc->dtNext, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaEventRecord(c.evDtNext, c.stream));
+  c.dtValidMaybe = c.dtCarried = true;
   return check_launch(ctx);
 }
 
@@ -614,6 +700,7 @@ int cup2d_advance(cup2d_ctx* ctx, int nsteps) {
   Ctx& c = ctx->c;
   if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
   if (nsteps <= 0) return CUP2D_OK;
+  forget_chain(c);
   if (c.cur != 0) {
     // a stage was called on its own: finish in eager mode until parity returns
     return fail(ctx, CUP2D_ESTATE, "velocity buffers out of step order");
@@ -646,6 +733,10 @@ int cup2d_advance(cup2d_ctx* ctx, int nsteps) {
     CK(cudaGraphLaunch(c.graph, c.stream));
     c.launches += c.launchesInGraph;
   }
+  // each step set dt on the device and formed the next one
+  c.devDt = NAN;
+  c.dtValidMaybe = true;
+  c.dtCarried = false;
   return CUP2D_OK;
 }
 
@@ -655,8 +746,9 @@ int cup2d_sync(cup2d_ctx* ctx) {
   CK(cudaStreamSynchronize(c.stream));
   int rc = check_launch(ctx);
   if (rc) return rc;
-  int status = 0;
-  CK(cudaMemcpy(&status, &c.dsc->status, sizeof(int), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpyAsync(&c.pin->status, &c.dsc->status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  const int status = c.pin->status;
   if (status & ST_NAN) return fail(ctx, CUP2D_ENAN, "non-finite velocity detected");
   if (status & ST_DOMAIN) return fail(ctx, CUP2D_EDOMAIN, "body out of domain");
   if (status & ST_CAPACITY) return fail(ctx, CUP2D_ECAPACITY, "obstacle tiles exceed capacity");
@@ -694,6 +786,7 @@ int cup2d_set_field(cup2d_ctx* ctx, int which, const double* host_in) {
   if (!p) return fail(ctx, CUP2D_EINVAL, "unknown field");
   CK(cudaStreamSynchronize(c.stream));
   CK(cudaMemcpy(p, host_in, sizeof(double) * c.ncells(), cudaMemcpyHostToDevice));
+  forget_chain(c);
   CK(invalidate_dt_next(c));
   return CUP2D_OK;
 }
@@ -702,8 +795,9 @@ int cup2d_get_shape(cup2d_ctx* ctx, int id, cup2d_shape_state* out) {
   if (!ctx || !out) return CUP2D_EINVAL;
   Ctx& c = ctx->c;
   if (id < 0 || id >= c.nshapes) return fail(ctx, CUP2D_EINVAL, "bad shape id");
+  CK(cudaMemcpyAsync(&c.pin->shape, c.dshapes + id, sizeof(DevShape), cudaMemcpyDeviceToHost, c.stream));
   CK(cudaStreamSynchronize(c.stream));
-  CK(cudaMemcpy(&c.hshapes[id], c.dshapes + id, sizeof(DevShape), cudaMemcpyDeviceToHost));
+  c.hshapes[id] = c.pin->shape;
   *out = c.hshapes[id].s;
   return CUP2D_OK;
 }
@@ -716,6 +810,7 @@ int cup2d_set_shape(cup2d_ctx* ctx, int id, const cup2d_shape_state* in) {
   CK(cudaMemcpy(&c.hshapes[id], c.dshapes + id, sizeof(DevShape), cudaMemcpyDeviceToHost));
   c.hshapes[id].s = *in;
   CK(cudaMemcpy(c.dshapes + id, &c.hshapes[id], sizeof(DevShape), cudaMemcpyHostToDevice));
+  forget_chain(c);
   CK(invalidate_dt_next(c));
   return CUP2D_OK;
 }
@@ -723,9 +818,9 @@ int cup2d_set_shape(cup2d_ctx* ctx, int id, const cup2d_shape_state* in) {
 int cup2d_get_scalars(cup2d_ctx* ctx, double* time, double* dt, int* step, double* uinfx, double* uinfy) {
   if (!ctx) return CUP2D_EINVAL;
   Ctx& c = ctx->c;
-  Scalars s;
+  CK(cudaMemcpyAsync(&c.pin->sc, c.dsc, sizeof(Scalars), cudaMemcpyDeviceToHost, c.stream));
   CK(cudaStreamSynchronize(c.stream));
-  CK(cudaMemcpy(&s, c.dsc, sizeof(Scalars), cudaMemcpyDeviceToHost));
+  const Scalars& s = c.pin->sc;
   if (time) *time = s.time;
   if (dt) *dt = s.dt;
   if (step) *step = s.step;
@@ -744,6 +839,9 @@ int cup2d_set_scalars(cup2d_ctx* ctx, double time, double dt, int step, double u
   s.dtNextValid = 0;
   CK(cudaMemcpy(c.dsc, &s, sizeof(Scalars), cudaMemcpyHostToDevice));
   c.midByGraph = false;
+  c.devDt = dt;
+  c.dtValidMaybe = c.dtCarried = false;
+  forget_chain(c);
   return CUP2D_OK;
 }
 
@@ -767,6 +865,8 @@ int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, double* ms_per_launch
   if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
   if (which < 0 || which > CUP2D_KERNEL_OBJECTS) return fail(ctx, CUP2D_EINVAL, "unknown kernel");
   CK(invalidate_dt_next(c));
+  forget_chain(c);
+  c.devDt = NAN;
   auto one = [&]() {
     switch (which) {
       case CUP2D_KERNEL_ADVDIFF: launch_advdiff(c); launch_advdiff_undo(c); break;

@@ -63,6 +63,24 @@ struct Ctx {
   bool sideMidPending = false;
   bool midByGraph = false;
 
+  // Host mirrors of device state, valid in stream order (what the device
+  // holds once the work enqueued so far has run), kept by the ABI calls so
+  // that the operator-by-operator path launches nothing redundant:
+  //   devDt        sc->dt (NaN: not known on the host)
+  //   dtValidMaybe sc->dtNextValid may be 1 (a step end formed the next dt)
+  //   dtCarried    sc->dtNextValid is 1 and pin->dtNext holds sc->dtNext
+  //                once evDtNext has completed
+  //   rhsFresh     rhs and the fade partials hold the RHS divergence of the
+  //                current velocity at sc->dt (formed in place by advDiff)
+  //   placedPending evPlaced marks the placed tiles of the last
+  //                PutObjectsOnGrid and nothing was enqueued after its chain
+  double devDt = 0.0;
+  bool dtValidMaybe = false, dtCarried = false, rhsFresh = false, placedPending = false;
+  cudaEvent_t evDtNext = nullptr;
+  // pinned host staging of the small read-backs (one copy + one wait each)
+  struct HostPin { double dtNext, dt; int status; Scalars sc; DevShape shape; };
+  HostPin* pin = nullptr;
+
   cudaGraphExec_t graph = nullptr;
   long long launches = 0;
   int launchesInGraph = 0;

@@ -31,12 +31,7 @@ k_max_u_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh,
 
 __global__ void k_set_dt(Scalars* sc, double dt) { pdl_begin(); CUP2D_TRACE_SCOPE(TR_SETDT); sc->dt = dt; }
 
-__global__ void k_end_step(Scalars* sc) { pdl_begin(); CUP2D_TRACE_SCOPE(TR_ENDSTEP);
-  sc->time += sc->dt;
-  sc->step += 1;
-}
-
-// End of a graph step: t += dt, step += 1, then the next step's
+// End of a step (Simulation.cpp:289-290): t += dt, step += 1, then the next step's
 // calcMaxTimestep from the maximum k_max_next formed on the final velocity
 // (max is exact in any order: dtNext equals what k_max_u_dt would form).
 __global__ void k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh)
@@ -49,6 +44,19 @@ __global__ void k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int n
   sc->dtNext = dt_from_max_u(g, sc, sh, nsh, m);
   sc->maxUNext = m;
   sc->dtNextValid = 1;
+  sc->maxNext = 0.0;              // ready for the next step end's maximum
+}
+
+// calcMaxTimestep of a state whose dt the last step end already formed
+// (dtNextValid; nothing has changed the state since): the same values
+// k_max_u_dt would write (Simulation.cpp:254-277), taken from dtNext.
+__global__ void k_take_dt_next(GridDesc g, Scalars* sc) {
+  pdl_begin();
+  CUP2D_TRACE_SCOPE(TR_SETDT);
+  const double dt = sc->dtNext;
+  sc->dt = dt;
+  sc->maxU = sc->maxUNext;
+  if (g.dlm > 0) sc->lambda = g.dlm / dt;
 }
 
 // ---- advDiff (advDiff.cpp:14-116) -------------------------------------------
@@ -371,13 +379,13 @@ void launch_set_dt(Ctx& c, double dt) {
   CUP2D_LAUNCHED(c);
 }
 
-void launch_end_step(Ctx& c) {
-  launch_k(k_end_step, 1, 1, 0, c.stream, c.dsc);
+void launch_max_next(Ctx& c) {
+  launch_k(k_max_next, max_grid(c), 256, 0, c.stream, c.g, c.dsc, c.u(), c.v());
   CUP2D_LAUNCHED(c);
 }
 
-void launch_max_next(Ctx& c) {
-  launch_k(k_max_next, max_grid(c), 256, 0, c.stream, c.g, c.dsc, c.u(), c.v());
+void launch_take_dt_next(Ctx& c) {
+  launch_k(k_take_dt_next, 1, 1, 0, c.stream, c.g, c.dsc);
   CUP2D_LAUNCHED(c);
 }
 

@@ -34,9 +34,9 @@ void launch_outflow(Ctx& c);                         // advDiff.cpp:89-116
 void launch_rhs_div(Ctx& c);                         // PressureSingle.cpp:112-128
 int build_fade_slots(Ctx& c);                        // PoissonSolver.cpp:71-79, once per grid
 void launch_pcorr(Ctx& c);                           // PressureSingle.cpp:216-241
-void launch_end_step(Ctx& c);                        // Simulation.cpp:289-290
-void launch_end_step_dt(Ctx& c);                     // the same + the next step's calcMaxTimestep
+void launch_end_step_dt(Ctx& c);                     // Simulation.cpp:289-290 + the next step's calcMaxTimestep
 void launch_max_next(Ctx& c);                        // its findMaxU on the final velocity
+void launch_take_dt_next(Ctx& c);                    // calcMaxTimestep from the carried dt
 void launch_ic(Ctx& c);                              // Helpers.cpp:38-82
 void launch_apply_obj_vel(Ctx& c);                   // Helpers.cpp:290-307
 

@@ -204,6 +204,57 @@ def test_operator_steps_then_graph_steps(args):
         assert a.ctx.shape(k) == b.ctx.shape(k), k
 
 
+def _operator_step(sim, dt):
+    for op in sim.pipeline:
+        op(dt)
+    sim.ctx.end_step()
+
+
+@pytest.mark.parametrize("args", [DISK, FISH], ids=["disk", "fish"])
+def test_operator_path_call_orders(args):
+    """The operator path skips launches the device state makes redundant (the
+    dt of calcMaxTimestep carried from the step end, sim.dt already set, the
+    RHS divergence formed by advDiff, advDiff beside the obstacle chain).
+    Calls in between that change or re-read the state must leave every
+    result bitwise the same as the plain loop."""
+    a = Simulation(args); a.init()
+    b = Simulation(args); b.init()
+    for comp, name in enumerate(("u", "v")):
+        n = noise_field(4, comp, a.ctx.ny, a.ctx.nx)
+        a.ctx.set(name, n); b.ctx.set(name, n)
+    for _ in range(8):
+        _operator_step(a, a.calcMaxTimestep())
+        _ = a.ctx.shape(0)
+    # 1: calcMaxTimestep twice, the state re-read between stages
+    b.ctx.calc_dt(sync=False); b.calcMaxTimestep(); dt = b.calcMaxTimestep()
+    b.pipeline[0](dt); _ = b.ctx.get("chi"); b.pipeline[1](dt); _ = b.ctx.get("tmp")
+    b.pipeline[2](dt); b.pipeline[3](-1.0); b.ctx.end_step()
+    # 2: a field written back between PutObjectsOnGrid and advDiff, and
+    #    between advDiff and PressureSingle
+    dt = b.calcMaxTimestep()
+    b.pipeline[0](dt); b.ctx.set("u", b.ctx.get("u"))
+    b.pipeline[1](dt); b.ctx.set("v", b.ctx.get("v"))
+    b.pipeline[2](dt); b.pipeline[3](dt); b.ctx.end_step()
+    # 3: the scalars written back (the carried dt is dropped), dt given to
+    #    the first stage only
+    st = b.ctx.scalars()
+    b.ctx.set_scalars(st["time"], st["dt"], st["step"], st["uinfx"], st["uinfy"])
+    dt = b.calcMaxTimestep()
+    b.pipeline[0](dt)
+    for op in b.pipeline[1:]:
+        op(-1.0)
+    b.ctx.end_step()
+    # 4-5: graph steps, then 6-8: operator steps again
+    b.ctx.advance(2)
+    for _ in range(3):
+        _operator_step(b, b.calcMaxTimestep())
+    b.ctx.sync()
+    for name in ("u", "v", "pres", "chi"):
+        assert np.array_equal(a.ctx.get(name), b.ctx.get(name)), name
+    assert a.ctx.shape(0) == b.ctx.shape(0)
+    assert a.ctx.scalars() == b.ctx.scalars()
+
+
 # ---- against the committed golden fixtures (no reference build needed) -------
 
 GOLDEN_DIR = __import__("os").path.join(__import__("os").path.dirname(__import__("os").path.abspath(__file__)), "golden")
