@@ -88,15 +88,58 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples the SM clock, its maximum and the clock-event reasons during
+    the timed region: through NVML (read-only queries, every 5 ms, plus one
+    sample at each end, so that short regions are covered), else through
+    `nvidia-smi -lms 200`."""
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
-        self.index, self.rows, self.proc = index, [], None
+        self.index, self.rows, self.proc, self.nvml = index, [], None, None
+        self.stop = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:                                   # the device torch calls `index`
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+        masks = [getattr(pynvml, "nvmlClocksEventReason" + n, 0) for n in
+                 ("HwSlowdown", "HwThermalSlowdown", "SwThermalSlowdown", "SwPowerCap")]
+        return pynvml, h, masks
+
+    def _nvml_sample(self):
+        pynvml, h, masks = self.nvml
+        sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+        mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        try:
+            r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except Exception:
+            r = pynvml.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        self.rows.append([str(sm), str(mx), ""] + ["Active" if (m and r & m) else "Not Active" for m in masks])
+
+    def _nvml_loop(self):
+        while not self.stop.wait(0.005):
+            try:
+                self._nvml_sample()
+            except Exception:
+                return
 
     def __enter__(self):
+        try:
+            self.nvml = self._nvml_handle()
+            self._nvml_sample()
+            self.t = threading.Thread(target=self._nvml_loop, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
@@ -115,6 +158,13 @@ class ClockSampler:
                 self.rows.append(parts)
 
     def __exit__(self, *a):
+        if self.nvml:
+            self.stop.set()
+            self.t.join(timeout=5)
+            try:
+                self._nvml_sample()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -127,10 +177,10 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
         mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[3 + k].lower() == "active"})
+        reasons = sorted({self.NAMES[k] for r in self.rows for k in range(4) if r[3 + k].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(self.rows)}
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(self.rows),
+                "source": "nvml" if self.nvml else "nvidia-smi"}
 
 
 def dist_setup():

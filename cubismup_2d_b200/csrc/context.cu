@@ -331,6 +331,7 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
               cudaEventCreateWithFlags(&c.evStart, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evSideMid, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evDtNext, cudaEventDisableTiming) != cudaSuccess ||
+              cudaEventCreateWithFlags(&c.evShapes, cudaEventDisableTiming) != cudaSuccess ||
               cudaMallocHost(&c.pin, sizeof(Ctx::HostPin)) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evJoin, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evObj, cudaEventDisableTiming) != cudaSuccess ||
@@ -370,6 +371,7 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   if (c.evStart) cudaEventDestroy(c.evStart);
   if (c.evSideMid) cudaEventDestroy(c.evSideMid);
   if (c.evDtNext) cudaEventDestroy(c.evDtNext);
+  if (c.evShapes) cudaEventDestroy(c.evShapes);
   if (c.pin) cudaFreeHost(c.pin);
   if (c.evJoin) cudaEventDestroy(c.evJoin);
   if (c.evPres) cudaEventDestroy(c.evPres);
@@ -530,6 +532,7 @@ int cup2d_init(cup2d_ctx* ctx) {
   // Simulation::reset (Simulation.cpp:232-241): resetAll, IC, objects at t=0, ApplyObjVel
   if ((rc = upload_scalars_reset(ctx))) return rc;
   c.dtValidMaybe = c.dtCarried = false;
+  c.shapesAtEvent = false;
   forget_chain(c);
   for (int k = 0; k < c.nshapes; k++) {
     DevShape& S = c.hshapes[k];
@@ -593,6 +596,7 @@ int cup2d_calc_dt(cup2d_ctx* ctx, double* dt_out) {
   if (!ctx) return CUP2D_EINVAL;                                                 \
   Ctx& c = ctx->c;                                                               \
   if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");         \
+  c.shapesAtEvent = false;                                                       \
   bool prologueLaunched = c.dtValidMaybe;                                        \
   CK(invalidate_dt_next(c));                                                     \
   if (dt >= 0 && !same_bits(dt, c.devDt)) {                                      \
@@ -611,6 +615,10 @@ int cup2d_put_objects(cup2d_ctx* ctx, double dt) {
   // graph step
   bool anyFishShape = false;
   for (int k = 0; k < c.nshapes; k++) anyFishShape |= c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK;
+  // the next step's midlines (time + dt) need only sim.dt: on the device
+  // they may start from here, while the host launches them after this
+  // step's chain (so that its first kernels are not delayed)
+  if (anyFishShape) CK(cudaEventRecord(c.evFork, c.stream));
   launch_objects_begin(c, false);
   if (c.nshapes > 0) {
     c.recordPlaced = anyFishShape;
@@ -618,12 +626,9 @@ int cup2d_put_objects(cup2d_ctx* ctx, double dt) {
     launch_objects_rest(c);
     c.recordPlaced = false;
   }
-  // the next step's midlines (time + dt) on the side stream, beside the
-  // rest of this step; the next call takes them if the time matches
-  bool anyFish = false;
-  for (int k = 0; k < c.nshapes; k++) anyFish |= c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK;
-  if (anyFish) {
-    CK(cudaEventRecord(c.evFork, c.stream));
+  // the next step's midlines on the side stream, beside the rest of this
+  // step; the next call takes them if the time matches
+  if (anyFishShape) {
     CK(cudaStreamWaitEvent(c.side, c.evFork, 0));
     for (int k = 0; k < c.nshapes; k++)
       if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.side, 1);
@@ -687,8 +692,10 @@ int cup2d_end_step(cup2d_ctx* ctx) {
   Ctx& c = ctx->c;
   if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
   forget_chain(c);
-  launch_max_next(c);                       // sc->maxNext is zero between steps
-  launch_end_step_dt(c);
+  // nothing from here on writes the shape states
+  CK(cudaEventRecord(c.evShapes, c.stream));
+  c.shapesAtEvent = true;
+  launch_end_step_max(c);
   CK(cudaMemcpyAsync(&c.pin->dtNext, &c.dsc->dtNext, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
   CK(cudaEventRecord(c.evDtNext, c.stream));
   c.dtValidMaybe = c.dtCarried = true;
@@ -701,6 +708,7 @@ int cup2d_advance(cup2d_ctx* ctx, int nsteps) {
   if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
   if (nsteps <= 0) return CUP2D_OK;
   forget_chain(c);
+  c.shapesAtEvent = false;
   if (c.cur != 0) {
     // a stage was called on its own: finish in eager mode until parity returns
     return fail(ctx, CUP2D_ESTATE, "velocity buffers out of step order");
@@ -795,8 +803,15 @@ int cup2d_get_shape(cup2d_ctx* ctx, int id, cup2d_shape_state* out) {
   if (!ctx || !out) return CUP2D_EINVAL;
   Ctx& c = ctx->c;
   if (id < 0 || id >= c.nshapes) return fail(ctx, CUP2D_EINVAL, "bad shape id");
-  CK(cudaMemcpyAsync(&c.pin->shape, c.dshapes + id, sizeof(DevShape), cudaMemcpyDeviceToHost, c.stream));
-  CK(cudaStreamSynchronize(c.stream));
+  if (c.shapesAtEvent) {
+    // final since the step end began: read beside its kernels
+    CK(cudaStreamWaitEvent(c.side2, c.evShapes, 0));
+    CK(cudaMemcpyAsync(&c.pin->shape, c.dshapes + id, sizeof(DevShape), cudaMemcpyDeviceToHost, c.side2));
+    CK(cudaStreamSynchronize(c.side2));
+  } else {
+    CK(cudaMemcpyAsync(&c.pin->shape, c.dshapes + id, sizeof(DevShape), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+  }
   c.hshapes[id] = c.pin->shape;
   *out = c.hshapes[id].s;
   return CUP2D_OK;
@@ -811,6 +826,7 @@ int cup2d_set_shape(cup2d_ctx* ctx, int id, const cup2d_shape_state* in) {
   c.hshapes[id].s = *in;
   CK(cudaMemcpy(c.dshapes + id, &c.hshapes[id], sizeof(DevShape), cudaMemcpyHostToDevice));
   forget_chain(c);
+  c.shapesAtEvent = false;
   CK(invalidate_dt_next(c));
   return CUP2D_OK;
 }
@@ -841,6 +857,7 @@ int cup2d_set_scalars(cup2d_ctx* ctx, double time, double dt, int step, double u
   c.midByGraph = false;
   c.devDt = dt;
   c.dtValidMaybe = c.dtCarried = false;
+  c.shapesAtEvent = false;
   forget_chain(c);
   return CUP2D_OK;
 }
@@ -866,6 +883,7 @@ int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, double* ms_per_launch
   if (which < 0 || which > CUP2D_KERNEL_OBJECTS) return fail(ctx, CUP2D_EINVAL, "unknown kernel");
   CK(invalidate_dt_next(c));
   forget_chain(c);
+  c.shapesAtEvent = false;
   c.devDt = NAN;
   auto one = [&]() {
     switch (which) {

@@ -74,9 +74,12 @@ struct Ctx {
   //                current velocity at sc->dt (formed in place by advDiff)
   //   placedPending evPlaced marks the placed tiles of the last
   //                PutObjectsOnGrid and nothing was enqueued after its chain
+  //   shapesAtEvent the shape states are final at evShapes (recorded at a
+  //                step end, before kernels that only read them)
   double devDt = 0.0;
   bool dtValidMaybe = false, dtCarried = false, rhsFresh = false, placedPending = false;
-  cudaEvent_t evDtNext = nullptr;
+  bool shapesAtEvent = false;
+  cudaEvent_t evDtNext = nullptr, evShapes = nullptr;
   // pinned host staging of the small read-backs (one copy + one wait each)
   struct HostPin { double dtNext, dt; int status; Scalars sc; DevShape shape; };
   HostPin* pin = nullptr;

@@ -44,7 +44,25 @@ __global__ void k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int n
   sc->dtNext = dt_from_max_u(g, sc, sh, nsh, m);
   sc->maxUNext = m;
   sc->dtNextValid = 1;
-  sc->maxNext = 0.0;              // ready for the next step end's maximum
+}
+
+// End of an operator-by-operator step: findMaxU on the final velocity (its
+// last CTA), then t += dt, step += 1 and the next step's calcMaxTimestep --
+// a graph step's k_max_next and k_end_step_dt in one launch.
+__global__ void __launch_bounds__(512)
+k_end_step_max(GridDesc g, Scalars* sc, const DevShape* sh, int nsh, const double* __restrict__ u,
+               const double* __restrict__ v, double* partials, unsigned* counter)
+{
+  pdl_begin();
+  CUP2D_TRACE_SCOPE(TR_ENDSTEP);
+  __shared__ double red[64];
+  double m;
+  if (!max_u_cta(g, sc, u, v, partials, counter, red, &m)) return;
+  sc->time += sc->dt;
+  sc->step += 1;
+  sc->dtNext = dt_from_max_u(g, sc, sh, nsh, m);
+  sc->maxUNext = m;
+  sc->dtNextValid = 1;
 }
 
 // calcMaxTimestep of a state whose dt the last step end already formed
@@ -381,6 +399,12 @@ void launch_set_dt(Ctx& c, double dt) {
 
 void launch_max_next(Ctx& c) {
   launch_k(k_max_next, max_grid(c), 256, 0, c.stream, c.g, c.dsc, c.u(), c.v());
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_end_step_max(Ctx& c) {
+  launch_k(k_end_step_max, max_grid(c), 512, 0, c.stream, c.g, c.dsc, (const DevShape*)c.dshapes, c.nshapes,
+           (const double*)c.u(), (const double*)c.v(), c.partials, c.counters + CNT_MAXU);
   CUP2D_LAUNCHED(c);
 }
 

@@ -37,6 +37,7 @@ void launch_pcorr(Ctx& c);                           // PressureSingle.cpp:216-2
 void launch_end_step_dt(Ctx& c);                     // Simulation.cpp:289-290 + the next step's calcMaxTimestep
 void launch_max_next(Ctx& c);                        // its findMaxU on the final velocity
 void launch_take_dt_next(Ctx& c);                    // calcMaxTimestep from the carried dt
+void launch_end_step_max(Ctx& c);                    // findMaxU + Simulation.cpp:289-290 + the next dt
 void launch_ic(Ctx& c);                              // Helpers.cpp:38-82
 void launch_apply_obj_vel(Ctx& c);                   // Helpers.cpp:290-307
 

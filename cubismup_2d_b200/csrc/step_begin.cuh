@@ -49,13 +49,12 @@ __device__ __forceinline__ double dt_from_max_u(const GridDesc& g, const Scalars
   return dt;
 }
 
-// Helpers.cpp:136-176 (findMaxU) + Simulation::calcMaxTimestep
-// (Simulation.cpp:254-277) over a 1D grid: per-CTA maxima, the last CTA
-// forms dt.  Returns true in thread 0 of the CTA that set sc->dt.
-// red must hold 64 doubles.
-__device__ __forceinline__ bool max_u_dt_cta(const GridDesc& g, Scalars* sc, const DevShape* sh, int nsh,
-                                             const double* __restrict__ u, const double* __restrict__ v,
-                                             double* partials, unsigned* counter, double* red)
+// Helpers.cpp:136-176 (findMaxU) over a 1D grid: per-CTA maxima, met by the
+// last CTA (max is exact in any order).  Returns true in thread 0 of that
+// CTA, with the maximum in *mmax.  red must hold 64 doubles.
+__device__ __forceinline__ bool max_u_cta(const GridDesc& g, Scalars* sc,
+                                          const double* __restrict__ u, const double* __restrict__ v,
+                                          double* partials, unsigned* counter, double* red, double* mmax)
 {
   const double UINF = sc->uinfx, VINF = sc->uinfy;
   double m = 0.0; int bad = 0;
@@ -81,6 +80,18 @@ __device__ __forceinline__ bool max_u_dt_cta(const GridDesc& g, Scalars* sc, con
   for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) mm = fmax(mm, __ldcg(&partials[i]));
   mm = block_max(mm, red);
   if (threadIdx.x != 0) return false;
+  *mmax = mm;
+  return true;
+}
+
+// findMaxU + Simulation::calcMaxTimestep (Simulation.cpp:254-277): the last
+// CTA forms dt.  Returns true in thread 0 of the CTA that set sc->dt.
+__device__ __forceinline__ bool max_u_dt_cta(const GridDesc& g, Scalars* sc, const DevShape* sh, int nsh,
+                                             const double* __restrict__ u, const double* __restrict__ v,
+                                             double* partials, unsigned* counter, double* red)
+{
+  double mm;
+  if (!max_u_cta(g, sc, u, v, partials, counter, red, &mm)) return false;
   const double dt = dt_from_max_u(g, sc, sh, nsh, mm);
   sc->dt = dt;
   sc->maxU = mm;

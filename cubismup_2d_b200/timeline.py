@@ -1,7 +1,7 @@
 """In-graph kernel timeline of one step (the trace build).
 
     python -m cubismup_2d_b200.build --trace
-    python -m cubismup_2d_b200.timeline [swimmer|cylinder] [--steps N] [--noflush] [--fp32]
+    python -m cubismup_2d_b200.timeline [swimmer|cylinder] [--steps N] [--noflush] [--fp32] [--operators]
 
 Runs the workload on the trace build (libcup2d_trace.so, compiled with
 -DCUP2D_TRACE): thread 0 of every CTA of every kernel stamps %globaltimer at
@@ -10,11 +10,16 @@ graph-replayed step can be read back.  Prints, per kernel, the median over
 the timed steps of its start, end and duration relative to the step's first
 kernel, with the L2 flushed before every step as in bench.py unless
 --noflush is given; --fp32 runs the FP32 Poisson transforms (CUP2D_PREC_FP32).
+--operators runs the reference's loop through the ABI instead of graph
+steps (calcMaxTimestep with its dt read back, the four operators, the step
+end, the shape state read back; no L2 flush, as in bench.py's e2e) and
+reports the host's wall-clock time per step beside the kernels' spans.
 """
 import argparse
 import ctypes
 import os
 import sys
+import time
 
 import numpy as np
 
@@ -38,6 +43,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--noflush", action="store_true")
     ap.add_argument("--fp32", action="store_true")
+    ap.add_argument("--operators", action="store_true")
     a = ap.parse_args(argv)
     if not os.path.exists(build.TRACE_LIB):
         build.build(trace=True)
@@ -52,24 +58,45 @@ def main(argv=None):
     L.cup2d_trace.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]
     n = len(KERNELS)
     buf = (ctypes.c_ulonglong * (2 * n + 8 * TRACE_ITEMS))()
-    ctx.advance(a.warmup)
+
+    def operator_step():
+        dt = sim.calcMaxTimestep()
+        for op in sim.pipeline:
+            op(dt)
+        ctx.end_step()
+        return ctx.shape(0)
+
+    if a.operators:
+        for _ in range(a.warmup):
+            operator_step()
+    else:
+        ctx.advance(a.warmup)
     ctx.sync()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{sim.cfg.device}")
     spans, steps = {}, []
     for _ in range(a.steps):
-        if not a.noflush:
-            flush.fill_(1.0)
-        torch.cuda.synchronize()
-        L.cup2d_trace(ctx.h_, None, 1)
-        steps.append(ctx.time_step() * 1e3)
+        if a.operators:
+            L.cup2d_trace(ctx.h_, None, 1)
+            t0h = time.perf_counter()
+            operator_step()
+            steps.append((time.perf_counter() - t0h) * 1e6)
+        else:
+            if not a.noflush:
+                flush.fill_(1.0)
+            torch.cuda.synchronize()
+            L.cup2d_trace(ctx.h_, None, 1)
+            steps.append(ctx.time_step() * 1e3)
         L.cup2d_trace(ctx.h_, buf, 0)
         t = np.array(buf[:2 * n], dtype=np.uint64).reshape(n, 2)
         used = t[:, 1] > 0
         t0 = t[used, 0].min()
         for i in np.nonzero(used)[0]:
             spans.setdefault(KERNELS[i], []).append(((t[i, 0] - t0) / 1e3, (t[i, 1] - t0) / 1e3))
-    print(f"step (CUDA events): median {np.median(steps):.1f} us over {a.steps} steps"
-          + (" (no L2 flush)" if a.noflush else " (L2 flushed before each step)"))
+    if a.operators:
+        print(f"operator step (host wall clock): median {np.median(steps):.1f} us over {a.steps} steps")
+    else:
+        print(f"step (CUDA events): median {np.median(steps):.1f} us over {a.steps} steps"
+              + (" (no L2 flush)" if a.noflush else " (L2 flushed before each step)"))
     rows = sorted((np.median(np.array(v)[:, 0]), np.median(np.array(v)[:, 1]), k) for k, v in spans.items())
     print(f"{'kernel':18s} {'start':>8s} {'end':>8s} {'dur':>7s}  (us)")
     for s0, e0, k in rows:
