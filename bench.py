@@ -1,7 +1,7 @@
 """Benchmark of the B200 CubismUP_2D timestep pipeline.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload swimmer|cylinder]
+                    [--workload swimmer|cylinder|tandem|ensemble] [--members M]
 
 Workload (default): the self-propelled swimmer on a 1024x512 grid (32x16
 blocks of 32x32), StefanFish L=0.2, T=1 at (0.4, 0.25), nu = 2e-5
@@ -20,6 +20,14 @@ shard: "replicas only") and rank 0 reports the max time over ranks.
 --impl reference times the reference's own C++ operators (compiled from its
 sources by oracle/Makefile into oracle/_ref) on the host cores, same workload
 and metric, rank 0 only.
+
+--workload ensemble: M (default 64) independent members drawn from a seed
+(cubismup_2d_b200.synthetic.ensemble_configs: 256x128, 512x256 or 1024x512
+grids; a forced cylinder or a StefanFish; Re log-uniform in [100, 1000])
+advanced together, one graph launch per ensemble step (cup2d_ensemble_*);
+the metric is the aggregate cell-steps/s, reported beside the same members
+advanced one after another on their own graphs.  The members' fields
+(~2 GB at M = 64) exceed the L2, so no flush is needed between steps.
 """
 import argparse
 import json
@@ -51,6 +59,8 @@ WORKLOADS = {
                "-muteAll 1 -shapes 'stefanfish L=0.1 T=1 xpos=0.6 ypos=0.5, "
                "stefanfish L=0.1 T=1 xpos=0.75 ypos=0.5 phi=0.5'"),
 }
+
+ENSEMBLE_NAME = "ensemble{}_seed0_fp64"
 
 # fp64 bytes per cell that each dense kernel must move (reads + writes once)
 ALGO_BYTES_PER_CELL = {
@@ -228,37 +238,56 @@ class stdout_to_stderr:
 
 
 def run_reference(args, world, rank, pg):
-    """The reference's own operators (oracle/_ref) on the host cores."""
-    name, argline = WORKLOADS[args.workload]
+    """The reference's own operators (oracle/_ref) on the host cores.  For
+    the ensemble: its first four members one after another, the steps split
+    among them."""
     if rank != 0:
         return None
     from oracle.refsim import RefSim
     from cubismup_2d_b200.synthetic import noise_field
+    if args.workload == "ensemble":
+        from cubismup_2d_b200.synthetic import ensemble_configs
+        name = ENSEMBLE_NAME.format(args.members)
+        cfgs = ensemble_configs(n=args.members, seed=0)[:4]
+        steps = max(1, args.steps // len(cfgs))
+        warm = min(args.warmup, 1)
+        sample = (f"members 0-{len(cfgs) - 1} of the ensemble one after another, {steps} timed steps "
+                  f"each after {warm} warm-up step(s); ")
+    else:
+        name, argline = WORKLOADS[args.workload]
+        cfgs, steps, warm = [argline], args.steps, args.warmup
+        sample = f"{steps} timed steps after {warm} warm-up steps; "
     cores = os.cpu_count()
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    el, cell_steps, prof = 0.0, 0, {}
     with stdout_to_stderr():
-        r = RefSim(argline)
-        for comp, fname in enumerate(("u", "v")):
-            r.set(fname, r.get(fname) + noise_field(0, comp, r.ny, r.nx))
-        for _ in range(args.warmup):
-            r.step()
-        r.profile_reset()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            r.step()
-        el = time.perf_counter() - t0
-    cells = r.nx * r.ny
-    val = cells * args.steps / el / 1e9
-    prof = r.profile()
+        for i, argline in enumerate(cfgs):
+            r = RefSim(argline)
+            for comp, fname in enumerate(("u", "v")):
+                r.set(fname, r.get(fname) + noise_field(i, comp, r.ny, r.nx))
+            for _ in range(warm):
+                r.step()
+            r.profile_reset()
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                r.step()
+            el += time.perf_counter() - t0
+            cell_steps += r.nx * r.ny * steps
+            for k, v in r.profile().items():
+                prof[k] = prof.get(k, 0.0) + v
+            del r
+    val = cell_steps / el / 1e9
+    nsteps = steps * len(cfgs)
     line = {
         "impl": "reference", "metric": "cell-steps/s", "value": val, "unit": "Gcell-steps/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+        "n_gpus": world, "steps": nsteps, "warmup": warm, "ms_per_step": el / nsteps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": name, "cells": cells},
+        "data": "synthetic",
+        "config": {"workload": name,
+                   ("cells_per_member_step" if args.workload == "ensemble" else "cells"): cell_steps // nsteps},
         "cpu_baseline": {"value": val, "unit": "Gcell-steps/s", "cores": cores, "kind": "reference",
-                         "sample": f"{args.steps} timed steps after {args.warmup} warm-up steps; "
-                                   "reference operators compiled from its sources with OpenMP; "
-                                   "FFT = project FFTW-API stand-in (FFTW absent)"},
+                         "sample": sample + "reference operators compiled from its sources with OpenMP; "
+                                            "FFT = project FFTW-API stand-in (FFTW absent)"},
         "e2e": {"value": val, "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "stage_seconds": {k: round(v, 4) for k, v in prof.items()},
     }
@@ -411,13 +440,126 @@ def run_ours(args, world, rank, local, pg):
     return line
 
 
+def run_ensemble(args, world, rank, local, pg):
+    """The batched ensemble: M members, one graph launch per ensemble step."""
+    import torch
+    from cubismup_2d_b200 import Ensemble
+    from cubismup_2d_b200.synthetic import ensemble_configs
+    torch.cuda.set_device(local)
+    cfgs = ensemble_configs(n=args.members, seed=0)
+    sims = [make_sim(a, local, 1000 * rank + i) for i, a in enumerate(cfgs)]
+    sizes = [s.ctx.nx * s.ctx.ny for s in sims]
+    cells = int(sum(sizes))
+    ens = Ensemble(sims)
+    ens.advance(max(args.warmup, 3))
+    ens.sync()
+    launches0 = sum(s.ctx.kernel_launches() for s in sims)
+    with ClockSampler(local) as clk:
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+        total_ms = ens.advance_timed(args.steps)
+    launches = sum(s.ctx.kernel_launches() for s in sims) - launches0
+    total_ms = max_over_ranks(pg, total_ms)
+    value = world * cells * args.steps / (total_ms / 1e3) / 1e9
+
+    # the same members one after another, each on its own step graph
+    for s in sims:
+        s.ctx.advance(3)
+    ens.sync()
+    seq_ms = max_over_ranks(pg, float(sum(s.ctx.time_step(args.steps) for s in sims)))
+    seq_value = world * cells * args.steps / (seq_ms / 1e3) / 1e9
+
+    # e2e: an ensemble step, then every member's shape state read back
+    ne = max(10, args.steps // 10)
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(ne):
+        ens.advance(1)
+        for s in sims:
+            _ = s.ctx.shape(0)
+    ens.sync()
+    e2e_s = max_over_ranks(pg, time.perf_counter() - t0)
+    e2e = world * cells * ne / e2e_s / 1e9
+
+    # FP32 Poisson transforms on the same members
+    fp32 = None
+    if not args.no_fp32:
+        del ens
+        sims32 = [make_sim(a + " -precision fp32", local, 1000 * rank + i) for i, a in enumerate(cfgs)]
+        ens32 = Ensemble(sims32)
+        ens32.advance(max(args.warmup, 3))
+        ens32.sync()
+        ms32 = max_over_ranks(pg, ens32.advance_timed(args.steps))
+        fp32 = {"value": world * cells * args.steps / (ms32 / 1e3) / 1e9, "unit": "Gcell-steps/s",
+                "ms_per_step": ms32 / args.steps, "speedup_vs_fp64": total_ms / ms32,
+                "note": "FP32 free-space Poisson transforms; fields, stencils, obstacle sums and forces FP64"}
+        del ens32, sims32
+
+    # roofline: the dominant dense kernel of the largest member
+    peak, peak_kind = measured_peaks()
+    big = sims[int(np.argmax(sizes))]
+    kt = {k: big.ctx.time_kernel(k, 50) for k in ("fft_cols", "advdiff", "pcorr", "fft_rows_fwd",
+                                                   "fft_rows_inv", "rhs_div", "max_u")}
+    dom = max(kt, key=kt.get)
+    bcells = big.ctx.nx * big.ctx.ny
+    achieved = ALGO_BYTES_PER_CELL[dom] * bcells / (kt[dom] * 1e-3) / 1e9
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            try:
+                v, cores, n = cpu_baseline_sample(cfgs[0], nsteps=args.cpu_steps)
+                cpu = {"value": v, "unit": "Gcell-steps/s", "cores": cores, "kind": "reference",
+                       "sample": f"{n} steps of member 0 ({sims[0].ctx.nx}x{sims[0].ctx.ny}) after 1 "
+                                 "warm-up step; reference operators compiled from its sources (OpenMP, "
+                                 "all host cores); FFT = project FFTW-API stand-in (FFTW absent)"}
+            except Exception as e:  # noqa: BLE001
+                cpu = {"value": None, "unit": "Gcell-steps/s", "cores": os.cpu_count(), "kind": "reference",
+                       "sample": f"unavailable: {e}"}
+        grids = {}
+        for s in sims:
+            key = f"{s.ctx.nx}x{s.ctx.ny}"
+            grids[key] = grids.get(key, 0) + 1
+        line = {
+            "metric": "cell-steps/s", "value": value, "unit": "Gcell-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": ENSEMBLE_NAME.format(args.members), "members": args.members,
+                       "cells": cells, "grids": grids,
+                       "shapes": {"disk": sum("disk" in a for a in cfgs),
+                                  "stefanfish": sum("stefanfish" in a for a in cfgs)},
+                       "parallelism": f"replicas{world}",
+                       "l2": "not flushed: the members' fields (~2 GB at 64 members) exceed the L2"},
+            "clocks": clk.summary(),
+            "sequential": {"value": seq_value, "unit": "Gcell-steps/s", "ms_per_step": seq_ms / args.steps,
+                           "speedup_of_ensemble": seq_ms / total_ms,
+                           "note": "the same members one after another, each on its own step graph"},
+            "e2e": {"value": e2e, "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": len(sims) * 42 * 8, "steps": ne},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": dom, "member": f"{big.ctx.nx}x{big.ctx.ny}",
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "algorithmic_bytes_per_launch": ALGO_BYTES_PER_CELL[dom] * bcells},
+            "fp32": fp32,
+            "cpu_baseline": cpu,
+        }
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="swimmer", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="swimmer", choices=sorted(WORKLOADS) + ["ensemble"])
+    ap.add_argument("--members", type=int, default=64, help="ensemble members (--workload ensemble)")
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-Poisson measurement")
@@ -428,6 +570,8 @@ def main():
         args.steps = min(args.steps, 20)
         args.warmup = min(args.warmup, 3)
         line = run_reference(args, world, rank, pg)
+    elif args.workload == "ensemble":
+        line = run_ensemble(args, world, rank, local, pg)
     else:
         line = run_ours(args, world, rank, local, pg)
     if rank == 0 and line is not None:

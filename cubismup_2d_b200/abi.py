@@ -36,6 +36,8 @@ EXPORTS = [
     "cup2d_end_step", "cup2d_advance", "cup2d_sync", "cup2d_get_field", "cup2d_set_field",
     "cup2d_get_shape", "cup2d_set_shape", "cup2d_get_scalars", "cup2d_set_scalars",
     "cup2d_grid_size", "cup2d_kernel_launches", "cup2d_time_kernel", "cup2d_advance_timed",
+    "cup2d_ensemble_create", "cup2d_ensemble_advance", "cup2d_ensemble_advance_timed",
+    "cup2d_ensemble_sync", "cup2d_ensemble_last_error", "cup2d_ensemble_destroy",
     "cup2d_adv_diff_noalloc",
 ]
 KERNELS = {"advdiff": 0, "rhs_div": 1, "pcorr": 2, "fft_rows_fwd": 3, "fft_cols": 4,
@@ -112,9 +114,16 @@ def lib():
     L.cup2d_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.cup2d_time_kernel.argtypes = [vp, i, i, dp]
     L.cup2d_advance_timed.argtypes = [vp, i, dp]
+    L.cup2d_ensemble_create.argtypes = [ctypes.POINTER(vp), i, ctypes.POINTER(vp)]
+    L.cup2d_ensemble_advance.argtypes = [vp, i]
+    L.cup2d_ensemble_advance_timed.argtypes = [vp, i, dp]
+    L.cup2d_ensemble_sync.argtypes = [vp]
+    L.cup2d_ensemble_last_error.argtypes = [vp]
+    L.cup2d_ensemble_last_error.restype = ctypes.c_char_p
+    L.cup2d_ensemble_destroy.argtypes = [vp]
     L.cup2d_adv_diff_noalloc.argtypes = [vp, vp, vp, vp, i, i, d, d, d, d, d, vp]
     for name in EXPORTS:
-        if name != "cup2d_last_error":
+        if name not in ("cup2d_last_error", "cup2d_ensemble_last_error"):
             getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -386,3 +395,57 @@ class Simulation:
 
     def getShapes(self):
         return [self.ctx.shape(k) for k in range(self.ctx.nshapes)]
+
+
+class Ensemble:
+    """Independent simulations advanced together (cup2d_ensemble_*): one CUDA
+    graph holds one step of every member, so one launch advances them all.
+    Each member ends bitwise where its own ``ctx.advance(n)`` would leave it;
+    members stay usable on their own between ensemble advances."""
+
+    def __init__(self, sims):
+        self.L = lib()
+        self.sims = list(sims)
+        self.ctxs = [s.ctx for s in self.sims]     # keeps the member contexts alive
+        if any(c is None or not getattr(c, "h_", None) for c in self.ctxs):
+            raise Cup2DError(ESTATE, "every member needs a context")
+        handles = (ctypes.c_void_p * len(self.ctxs))(*[c.h_.value for c in self.ctxs])
+        h = ctypes.c_void_p()
+        rc = self.L.cup2d_ensemble_create(handles, len(self.sims), ctypes.byref(h))
+        if rc != OK:
+            raise Cup2DError(rc, "cup2d_ensemble_create failed")
+        self.h_ = h
+
+    def _ck(self, rc):
+        if rc != OK:
+            raise Cup2DError(rc, self.L.cup2d_ensemble_last_error(self.h_).decode())
+
+    def _members_current(self):
+        for i, (s, c) in enumerate(zip(self.sims, self.ctxs)):
+            if s.ctx is not c:
+                raise Cup2DError(ESTATE, f"member {i} has a new context since the ensemble was made")
+
+    def advance(self, nsteps=1):
+        self._members_current()
+        self._ck(self.L.cup2d_ensemble_advance(self.h_, nsteps))
+
+    def advance_timed(self, nsteps=1):
+        """Milliseconds of the graph launches alone (CUDA events; synchronises)."""
+        self._members_current()
+        ms = ctypes.c_double()
+        self._ck(self.L.cup2d_ensemble_advance_timed(self.h_, nsteps, ctypes.byref(ms)))
+        return ms.value
+
+    def sync(self):
+        self._ck(self.L.cup2d_ensemble_sync(self.h_))
+
+    def close(self):
+        if getattr(self, "h_", None):
+            self.L.cup2d_ensemble_destroy(self.h_)
+            self.h_ = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

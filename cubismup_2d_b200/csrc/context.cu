@@ -126,6 +126,7 @@ int upload_scalars_reset(cup2d_ctx* ctx) {
 
 void invalidate_graph(Ctx& c) {
   if (c.graph) { cudaGraphExecDestroy(c.graph); c.graph = nullptr; }
+  c.graphGen++;                             // ensembles holding this context re-capture
 }
 
 // one pass of Simulation::simulate's loop body (Simulation.cpp:245-251)
@@ -702,11 +703,14 @@ int cup2d_end_step(cup2d_ctx* ctx) {
   return check_launch(ctx);
 }
 
-int cup2d_advance(cup2d_ctx* ctx, int nsteps) {
-  if (!ctx) return CUP2D_EINVAL;
+} // extern "C"
+
+namespace cup2d {
+// Before graph steps: the state they require, and what the first of them
+// relies on, enqueued on the context's stream.
+int graph_steps_begin(cup2d_ctx* ctx) {
   Ctx& c = ctx->c;
   if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
-  if (nsteps <= 0) return CUP2D_OK;
   forget_chain(c);
   c.shapesAtEvent = false;
   if (c.cur != 0) {
@@ -724,6 +728,26 @@ int cup2d_advance(cup2d_ctx* ctx, int nsteps) {
       if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.stream, 4);
     c.midByGraph = true;
   }
+  return check_launch(ctx);
+}
+
+// After graph steps: each set dt on the device and formed the next one.
+void graph_steps_end(Ctx& c) {
+  c.devDt = NAN;
+  c.dtValidMaybe = true;
+  c.dtCarried = false;
+}
+} // namespace cup2d
+
+extern "C" {
+
+int cup2d_advance(cup2d_ctx* ctx, int nsteps) {
+  if (!ctx) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
+  if (nsteps <= 0) return CUP2D_OK;
+  int rc = graph_steps_begin(ctx);
+  if (rc) return rc;
   if (!c.graph) {
     const long long before = c.launches;
     cudaGraph_t graph;
@@ -741,10 +765,7 @@ int cup2d_advance(cup2d_ctx* ctx, int nsteps) {
     CK(cudaGraphLaunch(c.graph, c.stream));
     c.launches += c.launchesInGraph;
   }
-  // each step set dt on the device and formed the next one
-  c.devDt = NAN;
-  c.dtValidMaybe = true;
-  c.dtCarried = false;
+  graph_steps_end(c);
   return CUP2D_OK;
 }
 
@@ -925,6 +946,181 @@ int cup2d_advance_timed(cup2d_ctx* ctx, int nsteps, double* ms) {
   CK(cudaEventElapsedTime(&f, e0, e1));
   cudaEventDestroy(e0); cudaEventDestroy(e1);
   *ms = f;
+  return CUP2D_OK;
+}
+
+} // extern "C"
+
+// ---- batched ensemble ------------------------------------------------------
+// One graph per ensemble holds one step of every member: each member's step
+// is enqueue_step on the member's own streams, forked from the ensemble's
+// stream and joined back to it, so the members are independent branches and
+// one launch advances them all (their kernels fill the SMs together).
+struct cup2d_ensemble {
+  std::vector<cup2d_ctx*> m;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t evRoot = nullptr, evEnd = nullptr, ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> evIn, evOut;      // per member
+  std::vector<int> launchesPerStep;          // per member
+  std::vector<unsigned> gens;                // members' graphGen at capture
+  cudaGraphExec_t graph = nullptr;
+  std::string err;
+};
+
+namespace {
+
+#define CKE(call)                                                               \
+  do {                                                                          \
+    cudaError_t e_ = (call);                                                    \
+    if (e_ != cudaSuccess) {                                                    \
+      ens->err = std::string(#call) + ": " + cudaGetErrorString(e_);            \
+      return CUP2D_ECUDA;                                                       \
+    }                                                                           \
+  } while (0)
+
+int ens_fail(cup2d_ensemble* ens, int code, const std::string& msg) {
+  ens->err = msg;
+  return code;
+}
+
+// capture one step of every member into ens->graph
+int ens_capture(cup2d_ensemble* ens) {
+  if (ens->graph) { cudaGraphExecDestroy(ens->graph); ens->graph = nullptr; }
+  const int n = (int)ens->m.size();
+  CKE(cudaStreamBeginCapture(ens->stream, cudaStreamCaptureModeThreadLocal));
+  cudaEventRecord(ens->evRoot, ens->stream);
+  for (int i = 0; i < n; i++) {
+    Ctx& c = ens->m[i]->c;
+    const long long before = c.launches;
+    cudaStreamWaitEvent(c.stream, ens->evRoot, 0);
+    enqueue_step(c);
+    cudaEventRecord(ens->evOut[i], c.stream);
+    cudaStreamWaitEvent(ens->stream, ens->evOut[i], 0);
+    ens->launchesPerStep[i] = (int)(c.launches - before);
+    c.launches = before;
+    ens->gens[i] = c.graphGen;
+  }
+  cudaGraph_t graph;
+  const cudaError_t e = cudaStreamEndCapture(ens->stream, &graph);
+  if (e != cudaSuccess) return ens_fail(ens, CUP2D_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  const cudaError_t e2 = cudaGraphInstantiate(&ens->graph, graph, cudaGraphInstantiateFlagUseNodePriority);
+  cudaGraphDestroy(graph);
+  if (e2 != cudaSuccess) {
+    ens->graph = nullptr;
+    return ens_fail(ens, CUP2D_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e2));
+  }
+  return CUP2D_OK;
+}
+
+// the members' earlier work -> nsteps ensemble steps -> the members' later work
+int ens_advance(cup2d_ensemble* ens, int nsteps, bool timed) {
+  const int n = (int)ens->m.size();
+  bool stale = !ens->graph;
+  for (int i = 0; i < n; i++) {
+    cup2d_ctx* ctx = ens->m[i];
+    const int rc = graph_steps_begin(ctx);
+    if (rc) return ens_fail(ens, rc, "member " + std::to_string(i) + ": " + ctx->c.err);
+    stale |= ens->gens[i] != ctx->c.graphGen;
+  }
+  if (stale) {
+    const int rc = ens_capture(ens);
+    if (rc) return rc;
+  }
+  for (int i = 0; i < n; i++) {
+    CKE(cudaEventRecord(ens->evIn[i], ens->m[i]->c.stream));
+    CKE(cudaStreamWaitEvent(ens->stream, ens->evIn[i], 0));
+  }
+  if (timed) CKE(cudaEventRecord(ens->ev0, ens->stream));
+  for (int s = 0; s < nsteps; s++) {
+    CKE(cudaGraphLaunch(ens->graph, ens->stream));
+    for (int i = 0; i < n; i++) ens->m[i]->c.launches += ens->launchesPerStep[i];
+  }
+  if (timed) CKE(cudaEventRecord(ens->ev1, ens->stream));
+  CKE(cudaEventRecord(ens->evEnd, ens->stream));
+  for (int i = 0; i < n; i++) {
+    Ctx& c = ens->m[i]->c;
+    CKE(cudaStreamWaitEvent(c.stream, ens->evEnd, 0));
+    graph_steps_end(c);
+  }
+  return CUP2D_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int cup2d_ensemble_create(cup2d_ctx* const* members, int n, cup2d_ensemble** out) {
+  if (!members || n <= 0 || !out) return CUP2D_EINVAL;
+  *out = nullptr;
+  for (int i = 0; i < n; i++) {
+    if (!members[i] || !members[i]->c.initialised) return CUP2D_ESTATE;
+    if (members[i]->c.device != members[0]->c.device) return CUP2D_EINVAL;
+    for (int j = 0; j < i; j++)
+      if (members[j] == members[i]) return CUP2D_EINVAL;
+  }
+  cup2d_ensemble* ens = new (std::nothrow) cup2d_ensemble();
+  if (!ens) return CUP2D_ENOMEM;
+  ens->m.assign(members, members + n);
+  ens->evIn.assign(n, nullptr);
+  ens->evOut.assign(n, nullptr);
+  ens->launchesPerStep.assign(n, 0);
+  ens->gens.assign(n, 0);
+  if (cudaSetDevice(members[0]->c.device) != cudaSuccess) { delete ens; return CUP2D_ECUDA; }
+  int prLeast = 0, prGreatest = 0;
+  cudaDeviceGetStreamPriorityRange(&prLeast, &prGreatest);
+  bool ok = cudaStreamCreateWithPriority(&ens->stream, cudaStreamNonBlocking, prGreatest) == cudaSuccess &&
+            cudaEventCreateWithFlags(&ens->evRoot, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&ens->evEnd, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreate(&ens->ev0) == cudaSuccess && cudaEventCreate(&ens->ev1) == cudaSuccess;
+  for (int i = 0; ok && i < n; i++)
+    ok = cudaEventCreateWithFlags(&ens->evIn[i], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&ens->evOut[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) { cup2d_ensemble_destroy(ens); return CUP2D_ECUDA; }
+  *out = ens;
+  return CUP2D_OK;
+}
+
+int cup2d_ensemble_advance(cup2d_ensemble* ens, int nsteps) {
+  if (!ens) return CUP2D_EINVAL;
+  if (nsteps <= 0) return CUP2D_OK;
+  return ens_advance(ens, nsteps, false);
+}
+
+int cup2d_ensemble_advance_timed(cup2d_ensemble* ens, int nsteps, double* ms) {
+  if (!ens || !ms) return CUP2D_EINVAL;
+  if (nsteps <= 0) { *ms = 0; return CUP2D_OK; }
+  const int rc = ens_advance(ens, nsteps, true);
+  if (rc) return rc;
+  CKE(cudaEventSynchronize(ens->ev1));
+  float f = 0;
+  CKE(cudaEventElapsedTime(&f, ens->ev0, ens->ev1));
+  *ms = f;
+  return CUP2D_OK;
+}
+
+int cup2d_ensemble_sync(cup2d_ensemble* ens) {
+  if (!ens) return CUP2D_EINVAL;
+  CKE(cudaStreamSynchronize(ens->stream));
+  for (size_t i = 0; i < ens->m.size(); i++) {
+    const int rc = cup2d_sync(ens->m[i]);
+    if (rc) return ens_fail(ens, rc, "member " + std::to_string(i) + ": " + ens->m[i]->c.err);
+  }
+  return CUP2D_OK;
+}
+
+const char* cup2d_ensemble_last_error(const cup2d_ensemble* ens) {
+  return ens ? ens->err.c_str() : "null ensemble";
+}
+
+int cup2d_ensemble_destroy(cup2d_ensemble* ens) {
+  if (!ens) return CUP2D_EINVAL;
+  if (ens->stream) cudaStreamSynchronize(ens->stream);
+  if (ens->graph) cudaGraphExecDestroy(ens->graph);
+  for (cudaEvent_t e : ens->evIn) if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : ens->evOut) if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : {ens->evRoot, ens->evEnd, ens->ev0, ens->ev1}) if (e) cudaEventDestroy(e);
+  if (ens->stream) cudaStreamDestroy(ens->stream);
+  delete ens;
   return CUP2D_OK;
 }
 

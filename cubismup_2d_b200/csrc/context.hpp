@@ -85,6 +85,7 @@ struct Ctx {
   HostPin* pin = nullptr;
 
   cudaGraphExec_t graph = nullptr;
+  unsigned graphGen = 0;        // bumped whenever what a step captures changes
   long long launches = 0;
   int launchesInGraph = 0;
   std::string err;

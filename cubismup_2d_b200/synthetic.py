@@ -36,3 +36,45 @@ FORCED_CYLINDER_RE100 = (
 SWIMMER_1024x512 = (
     "-bpdx 32 -bpdy 16 -extent 1 -CFL 0.1 -nu 2e-5 -lambda 1e4 -poissonType freespace "
     "-nsteps 2000 -shapes 'stefanfish L=0.2 T=1 xpos=0.4 ypos=0.25'")
+
+# Grids of the ensemble members (blocks of 32x32 cells).  768x384 is left
+# out: its free-space transform lengths (1536) are not powers of two, which
+# the library's radix-16 FFTs require (cup2d_create returns CUP2D_ENOTSUP).
+ENSEMBLE_GRIDS = [(8, 4), (16, 8), (32, 16)]
+
+
+def fish_length_ok(L, h):
+    """Whether FishData's arclength grid exists for a fish of length L on
+    spacing h (FishLibrary.cpp:14-38: the refined end spacing dSref must be
+    positive, the assertion at line 21); the reference aborts otherwise."""
+    ds_mid_tgt, ds_refine_tgt = h / np.sqrt(2.0), 0.125 * h
+    n_mid = int(np.ceil(L * 0.8 / ds_mid_tgt / 8)) * 8
+    ds_mid = L * 0.8 / n_mid
+    n_end = int(np.ceil(0.1 * L * 2 / (ds_mid + ds_refine_tgt) / 4)) * 4
+    return 0.1 * L * 2 / n_end - ds_mid > 0
+
+
+def ensemble_configs(n=64, seed=0):
+    """Reference command lines of n independent members drawn from a seed:
+    the grid from ENSEMBLE_GRIDS; a forced cylinder (radius in [0.02, 0.05],
+    u = 0.2, nu = U 2R / Re) or a StefanFish (L in [0.15, 0.25], redrawn
+    until the fish's arclength grid exists at the member's spacing, T = 1,
+    nu = (L/T) L / Re); Re log-uniform in [100, 1000]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        bx, by = ENSEMBLE_GRIDS[rng.integers(len(ENSEMBLE_GRIDS))]
+        re = float(np.exp(rng.uniform(np.log(100.0), np.log(1000.0))))
+        grid = f"-bpdx {bx} -bpdy {by} -extent 1 -CFL 0.1 -lambda 1e4 -poissonType freespace -nsteps 500"
+        if rng.uniform() < 0.5:
+            r = float(rng.uniform(0.02, 0.05))
+            nu = 0.2 * 2 * r / re
+            out.append(f"{grid} -nu {nu:.17g} -shapes 'disk radius={r:.17g} xpos=0.2 ypos=0.25 "
+                       "bForced=1 bFixed=1 xvel=0.2'")
+        else:
+            L = float(rng.uniform(0.15, 0.25))
+            while not fish_length_ok(L, 1.0 / (32 * max(bx, by))):
+                L = float(rng.uniform(0.15, 0.25))
+            nu = L * L / re
+            out.append(f"{grid} -nu {nu:.17g} -shapes 'stefanfish L={L:.17g} T=1 xpos=0.4 ypos=0.25'")
+    return out

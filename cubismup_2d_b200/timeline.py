@@ -59,12 +59,24 @@ def main(argv=None):
     n = len(KERNELS)
     buf = (ctypes.c_ulonglong * (2 * n + 8 * TRACE_ITEMS))()
 
+    calls = {}
+
     def operator_step():
+        # host time of each call (µs), from the step's start
+        t = [time.perf_counter()]
         dt = sim.calcMaxTimestep()
+        t.append(time.perf_counter())
         for op in sim.pipeline:
             op(dt)
+            t.append(time.perf_counter())
         ctx.end_step()
-        return ctx.shape(0)
+        t.append(time.perf_counter())
+        st = ctx.shape(0)
+        t.append(time.perf_counter())
+        names = ["calcMaxTimestep"] + [op.getName() for op in sim.pipeline] + ["end_step", "shape"]
+        for i, n in enumerate(names):
+            calls.setdefault(n, []).append(((t[i] - t[0]) * 1e6, (t[i + 1] - t[0]) * 1e6))
+        return st
 
     if a.operators:
         for _ in range(a.warmup):
@@ -94,6 +106,10 @@ def main(argv=None):
             spans.setdefault(KERNELS[i], []).append(((t[i, 0] - t0) / 1e3, (t[i, 1] - t0) / 1e3))
     if a.operators:
         print(f"operator step (host wall clock): median {np.median(steps):.1f} us over {a.steps} steps")
+        print(f"{'host call':18s} {'start':>8s} {'end':>8s} {'dur':>7s}  (us, from the step's first call)")
+        for n, v in calls.items():
+            v = np.array(v[-a.steps:])
+            print(f"{n:18s} {np.median(v[:, 0]):8.1f} {np.median(v[:, 1]):8.1f} {np.median(v[:, 1] - v[:, 0]):7.1f}")
     else:
         print(f"step (CUDA events): median {np.median(steps):.1f} us over {a.steps} steps"
               + (" (no L2 flush)" if a.noflush else " (L2 flushed before each step)"))

@@ -182,6 +182,33 @@ int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, double* ms_per_launch
  * milliseconds (synchronises). */
 int cup2d_advance_timed(cup2d_ctx* ctx, int nsteps, double* ms);
 
+/* ---- batched ensemble --------------------------------------------------- */
+/* No counterpart in the reference (it runs one Simulation per process):
+ * n independent simulations on one device, of any grid sizes and shapes,
+ * advanced together.  One step of every member is captured into one CUDA
+ * graph, each member an independent branch on its own streams, so one
+ * launch advances the whole ensemble by a step and the members' kernels
+ * share the SMs.  Each member ends bitwise where cup2d_advance(member,
+ * nsteps) would leave it.
+ *  - members: distinct, initialised contexts on one device (CUP2D_ESTATE /
+ *    CUP2D_EINVAL otherwise), each with its velocity in step order, as
+ *    cup2d_advance requires;
+ *  - the ensemble keeps the member pointers: advance it only while they
+ *    exist; destroying it leaves them untouched;
+ *  - after an advance the members may be used on their own (their streams
+ *    are ordered after the ensemble's work); a member re-initialised since
+ *    the last advance is re-captured;
+ *  - cup2d_ensemble_advance_timed: the graph launches alone bracketed by
+ *    CUDA events (synchronises); cup2d_ensemble_sync: waits and reports the
+ *    first member whose status is not CUP2D_OK (cup2d_sync). */
+typedef struct cup2d_ensemble cup2d_ensemble;
+int cup2d_ensemble_create(cup2d_ctx* const* members, int n, cup2d_ensemble** out);
+int cup2d_ensemble_advance(cup2d_ensemble* ens, int nsteps);
+int cup2d_ensemble_advance_timed(cup2d_ensemble* ens, int nsteps, double* ms);
+int cup2d_ensemble_sync(cup2d_ensemble* ens);
+const char* cup2d_ensemble_last_error(const cup2d_ensemble* ens);
+int cup2d_ensemble_destroy(cup2d_ensemble* ens);
+
 /* ---- allocation-free advDiff ------------------------------------------ */
 /* This entry point has no counterpart in the reference.  It is advDiff
  * (advDiff.cpp:36-118: explicit Euler step of central advection and 5-point

@@ -59,3 +59,19 @@ def test_missing_grid_arguments_are_an_error():
     from cubismup_2d_b200 import parse_args, Cup2DError
     with pytest.raises(Cup2DError):
         parse_args("-nu 1e-3")
+
+
+def test_ensemble_entry_points_reject_bad_arguments():
+    """No GPU needed: the ensemble calls check their arguments before any
+    CUDA call."""
+    import ctypes
+    from cubismup_2d_b200 import abi
+    L = abi.lib()
+    out = ctypes.c_void_p()
+    assert L.cup2d_ensemble_create(None, 0, ctypes.byref(out)) == abi.EINVAL
+    assert L.cup2d_ensemble_create(None, 2, ctypes.byref(out)) == abi.EINVAL
+    assert L.cup2d_ensemble_advance(None, 1) == abi.EINVAL
+    assert L.cup2d_ensemble_advance_timed(None, 1, None) == abi.EINVAL
+    assert L.cup2d_ensemble_sync(None) == abi.EINVAL
+    assert L.cup2d_ensemble_destroy(None) == abi.EINVAL
+    assert L.cup2d_ensemble_last_error(None) == b"null ensemble"
