@@ -622,6 +622,11 @@ inline double* shape_partials(const Ctx& c) { return c.partials + (size_t)3 * c.
 
 void launch_objects_begin(Ctx& c, bool midlineReady) {
   if (c.nshapes == 0) return;
+  // the last step's tiles reset and the body motion first: the midline
+  // reads neither (a graph step runs them side by side)
+  launch_k(k_obj_begin, tile_ctas(c, c.maxCapacity), 256, 0, c.stream, 
+      c.g, c.dsc, c.dshapes, c.nshapes, all_tiles(c), c.chi, c.sdf);
+  CUP2D_LAUNCHED(c);
   // fish midlines at the current time (Fish.cpp:79-95) unless the previous
   // step already computed them on its side branch
   if (!midlineReady) {
@@ -632,9 +637,6 @@ void launch_objects_begin(Ctx& c, bool midlineReady) {
     for (int k = 0; k < c.nshapes; k++)
       if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.stream, 4);
   }
-  launch_k(k_obj_begin, tile_ctas(c, c.maxCapacity), 256, 0, c.stream, 
-      c.g, c.dsc, c.dshapes, c.nshapes, all_tiles(c), c.chi, c.sdf);
-  CUP2D_LAUNCHED(c);
 }
 
 void launch_step_begin(Ctx& c) {
