@@ -36,6 +36,7 @@ EXPORTS = [
     "cup2d_end_step", "cup2d_advance", "cup2d_sync", "cup2d_get_field", "cup2d_set_field",
     "cup2d_get_shape", "cup2d_set_shape", "cup2d_get_scalars", "cup2d_set_scalars",
     "cup2d_grid_size", "cup2d_kernel_launches", "cup2d_time_kernel", "cup2d_advance_timed",
+    "cup2d_checkpoint_size", "cup2d_checkpoint_save", "cup2d_checkpoint_load",
     "cup2d_ensemble_create", "cup2d_ensemble_advance", "cup2d_ensemble_advance_timed",
     "cup2d_ensemble_sync", "cup2d_ensemble_last_error", "cup2d_ensemble_destroy",
     "cup2d_adv_diff_noalloc",
@@ -114,6 +115,9 @@ def lib():
     L.cup2d_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.cup2d_time_kernel.argtypes = [vp, i, i, dp]
     L.cup2d_advance_timed.argtypes = [vp, i, dp]
+    L.cup2d_checkpoint_size.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
+    L.cup2d_checkpoint_save.argtypes = [vp, vp, ctypes.c_size_t]
+    L.cup2d_checkpoint_load.argtypes = [vp, vp, ctypes.c_size_t]
     L.cup2d_ensemble_create.argtypes = [ctypes.POINTER(vp), i, ctypes.POINTER(vp)]
     L.cup2d_ensemble_advance.argtypes = [vp, i]
     L.cup2d_ensemble_advance_timed.argtypes = [vp, i, dp]
@@ -133,6 +137,15 @@ class Cup2DError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"{ERRORS.get(code, code)}: {msg}")
         self.code = code
+
+
+def _buffer(obj):
+    """(pointer, bytes) of a contiguous numpy array or a device tensor."""
+    if isinstance(obj, np.ndarray):
+        if not obj.flags["C_CONTIGUOUS"]:
+            raise ValueError("checkpoint buffers must be contiguous")
+        return ctypes.c_void_p(obj.ctypes.data), obj.nbytes
+    return ctypes.c_void_p(obj.data_ptr()), obj.numel() * obj.element_size()
 
 
 def _dp(a):
@@ -319,6 +332,29 @@ class Context:
         ms = ctypes.c_double()
         self._ck(self.L.cup2d_time_kernel(self.h_, KERNELS[name], reps, ctypes.byref(ms)))
         return ms.value
+
+    def checkpoint_size(self):
+        n = ctypes.c_size_t()
+        self._ck(self.L.cup2d_checkpoint_size(self.h_, ctypes.byref(n)))
+        return n.value
+
+    def checkpoint(self, out=None):
+        """The state between steps as a uint8 array (or into ``out``: a host
+        array, or any object with a device pointer ``data_ptr()`` and
+        ``numel()``, e.g. a CUDA uint8 tensor)."""
+        n = self.checkpoint_size()
+        if out is None:
+            out = np.empty(n, dtype=np.uint8)
+        ptr, size = _buffer(out)
+        self._ck(self.L.cup2d_checkpoint_save(self.h_, ptr, size))
+        return out
+
+    def restore(self, blob):
+        """Loads a checkpoint of this configuration (host array or device tensor)."""
+        if isinstance(blob, (bytes, bytearray)):
+            blob = np.frombuffer(blob, dtype=np.uint8)
+        ptr, size = _buffer(blob)
+        self._ck(self.L.cup2d_checkpoint_load(self.h_, ptr, size))
 
     def kernel_launches(self):
         n = ctypes.c_longlong()

@@ -3,6 +3,7 @@
 // exchange.  No entry point aborts: failures come back as status codes.
 #include <cfloat>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <new>
 #include <string>
@@ -461,7 +462,7 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
     if (!fish_fits_on_chip(Nm, F.nseg, c.device))
       return fail(ctx, CUP2D_ENOTSUP, "fish midline too fine: its kernels' staged arrays exceed shared memory");
     // 3 static arrays + 3 midlines of 8 arrays + 16 integrals, one allocation
-    if (!rc) rc = dalloc(ctx, &F.pool, (size_t)28 * Nm + 16);
+    if (!rc) rc = dalloc(ctx, &F.pool, fish_pool_len(Nm));
     if (!rc) rc = dalloc(ctx, &F.seg, F.nseg);
     if (rc) return rc;
     {
@@ -1121,6 +1122,169 @@ int cup2d_ensemble_destroy(cup2d_ensemble* ens) {
   for (cudaEvent_t e : {ens->evRoot, ens->evEnd, ens->ev0, ens->ev1}) if (e) cudaEventDestroy(e);
   if (ens->stream) cudaStreamDestroy(ens->stream);
   delete ens;
+  return CUP2D_OK;
+}
+
+} // extern "C"
+
+// ---- checkpoint / restart ----------------------------------------------------
+// A checkpoint holds every device buffer that carries state from one step to
+// the next (scalars, shapes, the current velocity, the other fields, each
+// shape's obstacle tiles, each fish's midline buffers and segments), behind
+// a header that identifies the configuration.  Derived or per-step data
+// (Poisson tables, fade slots, reduction scratch, tickets) is rebuilt by
+// cup2d_init and not stored.  Sections are copied with cudaMemcpyDefault, so
+// the buffer may be host or device memory.
+namespace {
+
+struct CkptHeader {
+  char magic[8];
+  uint32_t version, nsections;
+  int32_t bpdx, bpdy, poisson, precision, nshapes, reserved;
+  double extent, CFL, lambda, dlm, nu, fadeLen;
+};
+constexpr uint32_t CKPT_VERSION = 1;
+constexpr char CKPT_MAGIC[8] = {'C', 'U', 'P', '2', 'D', 'C', 'K', 0};
+
+struct CkptSection { void* p; size_t bytes; };
+
+std::vector<CkptSection> ckpt_sections(Ctx& c) {
+  std::vector<CkptSection> s;
+  const size_t n = c.ncells() * sizeof(double);
+  s.push_back({c.dsc, sizeof(Scalars)});
+  s.push_back({c.dshapes, sizeof(DevShape) * c.nshapes});
+  s.push_back({c.vel[0][0], n});
+  s.push_back({c.vel[0][1], n});
+  for (double* f : {c.chi, c.pres, c.rhs, c.sdf, c.udefx, c.udefy}) s.push_back({f, n});
+  for (int k = 0; k < c.nshapes; k++) {
+    const ObstTiles& t = c.tiles[k];
+    const size_t tb = (size_t)t.capacity * BS2 * sizeof(double);
+    s.push_back({t.tiles, sizeof(int) * t.capacity});
+    s.push_back({t.slot, sizeof(int) * c.g.nblocks});
+    for (double* a : {t.chi, t.dist, t.udx, t.udy, t.sD, t.sdx, t.sdy}) s.push_back({a, tb});
+    if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) {
+      const FishArrays& F = c.fish[k];
+      s.push_back({F.pool, sizeof(double) * fish_pool_len(F.nm)});
+      s.push_back({F.seg, sizeof(Segment) * F.nseg});
+    }
+  }
+  return s;
+}
+
+CkptHeader ckpt_header(const Ctx& c, size_t nsec) {
+  CkptHeader h;
+  std::memset(&h, 0, sizeof(h));
+  std::memcpy(h.magic, CKPT_MAGIC, sizeof(h.magic));
+  h.version = CKPT_VERSION;
+  h.nsections = (uint32_t)nsec;
+  h.bpdx = c.cfg.bpdx; h.bpdy = c.cfg.bpdy; h.poisson = c.cfg.poisson; h.precision = c.cfg.precision;
+  h.nshapes = c.nshapes;
+  h.extent = c.cfg.extent; h.CFL = c.cfg.CFL; h.lambda = c.cfg.lambda; h.dlm = c.cfg.dlm;
+  h.nu = c.cfg.nu; h.fadeLen = c.cfg.fadeLen;
+  return h;
+}
+
+size_t ckpt_total(const Ctx& c, const std::vector<CkptSection>& s) {
+  size_t b = sizeof(CkptHeader) + sizeof(ShapeCfg) * c.nshapes + sizeof(uint64_t) * s.size();
+  for (const CkptSection& x : s) b += x.bytes;
+  return b;
+}
+
+// nothing in flight may write the buffers while they are copied
+int ckpt_quiesce(cup2d_ctx* ctx) {
+  Ctx& c = ctx->c;
+  CK(cudaStreamSynchronize(c.stream));
+  CK(cudaStreamSynchronize(c.side));
+  CK(cudaStreamSynchronize(c.side2));
+  return CUP2D_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int cup2d_checkpoint_size(cup2d_ctx* ctx, size_t* bytes) {
+  if (!ctx || !bytes) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
+  *bytes = ckpt_total(c, ckpt_sections(c));
+  return CUP2D_OK;
+}
+
+int cup2d_checkpoint_save(cup2d_ctx* ctx, void* buf, size_t bytes) {
+  if (!ctx || !buf) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
+  if (c.cur != 0) return fail(ctx, CUP2D_ESTATE, "checkpoints are taken between steps");
+  const std::vector<CkptSection> secs = ckpt_sections(c);
+  if (bytes < ckpt_total(c, secs)) return fail(ctx, CUP2D_EINVAL, "checkpoint buffer too small");
+  int rc = ckpt_quiesce(ctx);
+  if (rc) return rc;
+  char* out = static_cast<char*>(buf);
+  const CkptHeader h = ckpt_header(c, secs.size());
+  std::vector<ShapeCfg> cfgs(c.nshapes);
+  for (int k = 0; k < c.nshapes; k++) cfgs[k] = c.hshapes[k].cfg;
+  std::vector<uint64_t> sizes(secs.size());
+  for (size_t i = 0; i < secs.size(); i++) sizes[i] = secs[i].bytes;
+  size_t off = 0;
+  CK(cudaMemcpy(out + off, &h, sizeof(h), cudaMemcpyDefault));
+  off += sizeof(h);
+  if (c.nshapes) CK(cudaMemcpy(out + off, cfgs.data(), sizeof(ShapeCfg) * c.nshapes, cudaMemcpyDefault));
+  off += sizeof(ShapeCfg) * c.nshapes;
+  CK(cudaMemcpy(out + off, sizes.data(), sizeof(uint64_t) * sizes.size(), cudaMemcpyDefault));
+  off += sizeof(uint64_t) * sizes.size();
+  for (const CkptSection& x : secs) {
+    CK(cudaMemcpy(out + off, x.p, x.bytes, cudaMemcpyDefault));
+    off += x.bytes;
+  }
+  return CUP2D_OK;
+}
+
+int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes) {
+  if (!ctx || !buf) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
+  const std::vector<CkptSection> secs = ckpt_sections(c);
+  const size_t total = ckpt_total(c, secs);
+  if (bytes < sizeof(CkptHeader)) return fail(ctx, CUP2D_EINVAL, "checkpoint truncated");
+  const char* in = static_cast<const char*>(buf);
+  CkptHeader h;
+  CK(cudaMemcpy(&h, in, sizeof(h), cudaMemcpyDefault));
+  if (std::memcmp(h.magic, CKPT_MAGIC, sizeof(h.magic)) != 0) return fail(ctx, CUP2D_EINVAL, "not a checkpoint");
+  if (h.version != CKPT_VERSION) return fail(ctx, CUP2D_ENOTSUP, "checkpoint version not supported");
+  const CkptHeader mine = ckpt_header(c, secs.size());
+  if (std::memcmp(&h, &mine, sizeof(h)) != 0)
+    return fail(ctx, CUP2D_EINVAL, "checkpoint of another configuration (grid, solver, precision, parameters or shapes)");
+  if (bytes < total) return fail(ctx, CUP2D_EINVAL, "checkpoint truncated");
+  size_t off = sizeof(h);
+  std::vector<ShapeCfg> cfgs(c.nshapes);
+  if (c.nshapes) CK(cudaMemcpy(cfgs.data(), in + off, sizeof(ShapeCfg) * c.nshapes, cudaMemcpyDefault));
+  off += sizeof(ShapeCfg) * c.nshapes;
+  for (int k = 0; k < c.nshapes; k++)
+    if (std::memcmp(&cfgs[k], &c.hshapes[k].cfg, sizeof(ShapeCfg)) != 0)
+      return fail(ctx, CUP2D_EINVAL, "checkpoint of other shapes (shape " + std::to_string(k) + ")");
+  std::vector<uint64_t> sizes(secs.size());
+  CK(cudaMemcpy(sizes.data(), in + off, sizeof(uint64_t) * sizes.size(), cudaMemcpyDefault));
+  off += sizeof(uint64_t) * sizes.size();
+  for (size_t i = 0; i < secs.size(); i++)
+    if (sizes[i] != secs[i].bytes) return fail(ctx, CUP2D_EINVAL, "checkpoint section sizes differ");
+  int rc = ckpt_quiesce(ctx);
+  if (rc) return rc;
+  for (const CkptSection& x : secs) {
+    CK(cudaMemcpy(x.p, in + off, x.bytes, cudaMemcpyDefault));
+    off += x.bytes;
+  }
+  // host state of a context between steps, knowing nothing of the device
+  c.cur = 0;
+  if (c.nshapes)
+    CK(cudaMemcpy(c.hshapes.data(), c.dshapes, sizeof(DevShape) * c.nshapes, cudaMemcpyDeviceToHost));
+  c.devDt = NAN;
+  c.dtValidMaybe = true;
+  c.dtCarried = false;
+  c.shapesAtEvent = false;
+  forget_chain(c);
+  c.sideMidPending = false;
+  c.midByGraph = false;
   return CUP2D_OK;
 }
 

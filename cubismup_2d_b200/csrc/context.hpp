@@ -97,6 +97,10 @@ struct Ctx {
   size_t ncells() const { return (size_t)g.nx * g.ny; }
 };
 
+// doubles behind one fish's arrays (FishArrays::pool): the static profile,
+// two midline buffers, the frame midline and the integrals
+inline size_t fish_pool_len(int nm) { return 28 * (size_t)nm + 16; }
+
 // counter slots used by the kernels (each last-CTA reduction owns one)
 enum CounterSlot : int {
   CNT_MAXU = 0, CNT_ADV = 1,

@@ -23,6 +23,8 @@
 #ifndef CUP2D_H
 #define CUP2D_H
 
+#include <stddef.h>   /* size_t */
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -181,6 +183,24 @@ int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, double* ms_per_launch
  * bracketed by CUDA events on the context's stream; returns the elapsed
  * milliseconds (synchronises). */
 int cup2d_advance_timed(cup2d_ctx* ctx, int nsteps, double* ms);
+
+/* ---- checkpoint / restart ---------------------------------------------- */
+/* The reference parses -restart but restores nothing (Simulation.cpp:68);
+ * these calls save and restore the whole state a step carries to the next:
+ * scalars (time, dt, step, ...), shape states, velocity and the other
+ * fields, the obstacle tiles and the fish midlines.  Continuing from a
+ * restored checkpoint is bitwise the same as continuing the saved run.
+ *  - the buffer may be host or device memory (copied with
+ *    cudaMemcpyDefault); cup2d_checkpoint_size gives its size;
+ *  - save: between steps only (CUP2D_ESTATE after a lone advDiff);
+ *    synchronises the context;
+ *  - load: into an initialised context of the same configuration and
+ *    shapes (the saved one, or a new one built alike); anything else, a
+ *    truncated buffer or a foreign one returns CUP2D_EINVAL (a newer format
+ *    CUP2D_ENOTSUP) without changing the context; synchronises. */
+int cup2d_checkpoint_size(cup2d_ctx* ctx, size_t* bytes);
+int cup2d_checkpoint_save(cup2d_ctx* ctx, void* buf, size_t bytes);
+int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes);
 
 /* ---- batched ensemble --------------------------------------------------- */
 /* No counterpart in the reference (it runs one Simulation per process):

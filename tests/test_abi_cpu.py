@@ -75,3 +75,14 @@ def test_ensemble_entry_points_reject_bad_arguments():
     assert L.cup2d_ensemble_sync(None) == abi.EINVAL
     assert L.cup2d_ensemble_destroy(None) == abi.EINVAL
     assert L.cup2d_ensemble_last_error(None) == b"null ensemble"
+
+
+def test_checkpoint_entry_points_reject_bad_arguments():
+    """No GPU needed: the checkpoint calls check their arguments first."""
+    import ctypes
+    from cubismup_2d_b200 import abi
+    L = abi.lib()
+    n = ctypes.c_size_t()
+    assert L.cup2d_checkpoint_size(None, ctypes.byref(n)) == abi.EINVAL
+    assert L.cup2d_checkpoint_save(None, None, 0) == abi.EINVAL
+    assert L.cup2d_checkpoint_load(None, None, 0) == abi.EINVAL
