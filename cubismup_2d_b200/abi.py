@@ -33,7 +33,8 @@ EXPORTS = [
     "cup2d_config_default", "cup2d_create", "cup2d_destroy", "cup2d_last_error",
     "cup2d_shape_params_default", "cup2d_add_shape", "cup2d_init", "cup2d_calc_dt",
     "cup2d_put_objects", "cup2d_adv_diff", "cup2d_pressure_single", "cup2d_compute_forces",
-    "cup2d_end_step", "cup2d_advance", "cup2d_sync", "cup2d_get_field", "cup2d_set_field",
+    "cup2d_end_step", "cup2d_iteration_stats", "cup2d_advance", "cup2d_sync",
+    "cup2d_get_field", "cup2d_set_field",
     "cup2d_get_shape", "cup2d_set_shape", "cup2d_get_scalars", "cup2d_set_scalars",
     "cup2d_grid_size", "cup2d_kernel_launches", "cup2d_time_kernel", "cup2d_advance_timed",
     "cup2d_checkpoint_size", "cup2d_checkpoint_save", "cup2d_checkpoint_load",
@@ -50,7 +51,7 @@ class Config(ctypes.Structure):
                 ("CFL", ctypes.c_double), ("lambda_", ctypes.c_double), ("dlm", ctypes.c_double),
                 ("nu", ctypes.c_double), ("fadeLen", ctypes.c_double), ("nsteps", ctypes.c_int),
                 ("tend", ctypes.c_double), ("poisson", ctypes.c_int), ("precision", ctypes.c_int),
-                ("device", ctypes.c_int)]
+                ("device", ctypes.c_int), ("iterative", ctypes.c_int)]
 
 
 class ShapeParams(ctypes.Structure):
@@ -103,6 +104,7 @@ def lib():
     for name in ("cup2d_put_objects", "cup2d_adv_diff", "cup2d_pressure_single", "cup2d_compute_forces"):
         getattr(L, name).argtypes = [vp, d]
     L.cup2d_end_step.argtypes = [vp]
+    L.cup2d_iteration_stats.argtypes = [vp, ip, dp]
     L.cup2d_advance.argtypes = [vp, i]
     L.cup2d_sync.argtypes = [vp]
     L.cup2d_get_field.argtypes = [vp, i, dp]
@@ -190,6 +192,7 @@ def parse_args(argline):
         raise Cup2DError(ENOTSUP, f"poissonType {ptype!r} is not available")
     cfg.poisson = POISSON[ptype]
     cfg.precision = {"fp64": PREC_FP64, "fp32": PREC_FP32}[args.get("precision", "fp64")]
+    cfg.iterative = int(args.get("iterativePenalization", 0)) != 0     # Simulation.cpp:101
     shapes = []
     for lines in args.get("shapes", "").split("\n"):
         lines = lines.replace("_", " ")
@@ -333,6 +336,13 @@ class Context:
         self._ck(self.L.cup2d_time_kernel(self.h_, KERNELS[name], reps, ctypes.byref(ms)))
         return ms.value
 
+    def iteration_stats(self):
+        """(iterations, last relative momentum change) of the latest iterated
+        pressure call (-iterativePenalization)."""
+        n, r = ctypes.c_int(), ctypes.c_double()
+        self._ck(self.L.cup2d_iteration_stats(self.h_, ctypes.byref(n), ctypes.byref(r)))
+        return n.value, r.value
+
     def checkpoint_size(self):
         n = ctypes.c_size_t()
         self._ck(self.L.cup2d_checkpoint_size(self.h_, ctypes.byref(n)))
@@ -423,10 +433,15 @@ class Simulation:
         return timeEnd or stepEnd
 
     def simulate(self):
-        """Runs nsteps+1 steps as Simulation::simulate does, on the graph path."""
+        """Runs nsteps+1 steps as Simulation::simulate does: on the graph path,
+        or operator by operator with -iterativePenalization."""
         if self.cfg.nsteps <= 0:
             raise Cup2DError(EINVAL, "simulate() needs -nsteps")
-        self.ctx.advance(self.cfg.nsteps + 1)
+        if self.cfg.iterative:                 # converges on the host: operator by operator
+            for _ in range(self.cfg.nsteps + 1):
+                self.advance(self.calcMaxTimestep())
+        else:
+            self.ctx.advance(self.cfg.nsteps + 1)
         self.ctx.sync()
 
     def getShapes(self):

@@ -1,6 +1,7 @@
 // The C ABI (include/cup2d.h): context lifetime, shapes, the pipeline stages
 // in Simulation::advance order, CUDA-graph replay of whole steps, and state
 // exchange.  No entry point aborts: failures come back as status codes.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
@@ -116,6 +117,7 @@ int upload_scalars_reset(cup2d_ctx* ctx) {
   Scalars s{};
   s.time = 0; s.dt = 0; s.uinfx = 0; s.uinfy = 0; s.lambda = c.cfg.lambda;
   s.step = 0; s.status = 0;
+  s.it.relDF = 0; s.it.target = 1e-4; s.it.oldNsteps = 10000; s.it.last = 0;   // PressureIterator_unif.h:15-16
   for (int i = 0; i < 100; i++) {        // Simulation.cpp:266-267, evaluated with the host libm
     const double x = (i + 1.0) / 100;
     s.rampCFL[i] = std::exp(std::log(1e-3) * (1 - x) + std::log(c.cfg.CFL) * x);
@@ -240,6 +242,51 @@ void enqueue_step(Ctx& c) {
   launch_end_step_dt(c);                    // t += dt, and the next step's dt
 }
 
+// PressureIterator_unif::operator() (PressureIterator_unif.cpp:214-270): the
+// velocity after advDiff kept as TMPV, then per iteration the fluid velocity
+// UF = TMPV - (dt/2h) grad P (P of the previous iteration, or step), the
+// bodies' momenta on UF and their velocities, the penalization of the
+// velocity towards the bodies' with its relative momentum change, the RHS
+// div V - chi div UDEF and a Poisson solve; converged (the change below the
+// adaptive target, or more than 100 iterations, or more than twice the
+// previous call's count), V -= (dt/2h) grad P.  The target then adapts to
+// the count as in the reference.  The change is read back each iteration.
+int pressure_iterative(cup2d_ctx* ctx) {
+  Ctx& c = ctx->c;
+  const size_t nb = sizeof(double) * c.ncells();
+  CK(cudaMemcpyAsync(c.itmp[0], c.u(), nb, cudaMemcpyDeviceToDevice, c.stream));
+  CK(cudaMemcpyAsync(c.itmp[1], c.v(), nb, cudaMemcpyDeviceToDevice, c.stream));
+  CK(cudaMemcpyAsync(&c.pin->it, &c.dsc->it, sizeof(IterState), cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  IterState st = c.pin->it;
+  int iter = 0;
+  double relDF = 1e3;
+  for (iter = 0; iter < 1000; iter++) {
+    launch_pcorr_from(c, c.itmp[0], c.itmp[1], c.ifluid[0], c.ifluid[1]);
+    launch_momenta_iter(c, c.itmp[0], c.itmp[1]);    // UF's values, formed in place
+    launch_penalize_iter(c, c.itmp[0], c.itmp[1], c.ifluid[0], c.ifluid[1]);
+    launch_rhs_iter(c);
+    poisson_solve(c);
+    CK(cudaMemcpyAsync(&c.pin->it.relDF, &c.dsc->it.relDF, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    if (int rc = check_launch(ctx)) return rc;
+    relDF = c.pin->it.relDF;
+    if (relDF < st.target || iter > 100 || iter > 2 * st.oldNsteps) {
+      launch_pcorr(c);                          // finalizePressure
+      break;
+    }
+  }
+  st.oldNsteps = iter + 1;
+  if (st.oldNsteps > 30) st.target = std::max(relDF, st.target);
+  if (st.oldNsteps > 10) st.target *= 1.01;
+  if (st.oldNsteps <= 2) st.target *= 0.99;
+  st.target = std::min(1e-3, std::max(1e-5, st.target));
+  st.relDF = relDF;
+  st.last = iter + 1;
+  launch_set_iter_state(c, st);
+  return check_launch(ctx);
+}
+
 } // namespace
 
 // The graph step's calcMaxTimestep reuses the maximum formed at the end of
@@ -324,6 +371,10 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
   if (!rc) rc = dalloc(ctx, &c.sdf, n);
   if (!rc) rc = dalloc(ctx, &c.udefx, n);
   if (!rc) rc = dalloc(ctx, &c.udefy, n);
+  for (int d = 0; d < 2 && !rc && cfg->iterative; d++) {
+    rc = dalloc(ctx, &c.itmp[d], n);
+    if (!rc) rc = dalloc(ctx, &c.ifluid[d], n);
+  }
   if (!rc) rc = dalloc(ctx, &c.dsc, 1);
   if (!rc) rc = dalloc(ctx, &c.dshapes, MAX_SHAPES);
   if (!rc) rc = dalloc(ctx, &c.counters, Ctx::NCOUNTERS);
@@ -364,6 +415,7 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   for (int b = 0; b < 2; b++) for (int d = 0; d < 2; d++) cudaFree(c.vel[b][d]);
   cudaFree(c.chi); cudaFree(c.pres); cudaFree(c.rhs); cudaFree(c.sdf);
   cudaFree(c.udefx); cudaFree(c.udefy); cudaFree(c.dsc); cudaFree(c.dshapes);
+  for (int d = 0; d < 2; d++) { cudaFree(c.itmp[d]); cudaFree(c.ifluid[d]); }
   cudaFree(c.counters); cudaFree(c.partials); cudaFree(c.fadeSlot);
   if (c.side) cudaStreamDestroy(c.side);
   if (c.side2) cudaStreamDestroy(c.side2);
@@ -562,6 +614,17 @@ int cup2d_init(cup2d_ctx* ctx) {
   return CUP2D_OK;
 }
 
+int cup2d_iteration_stats(cup2d_ctx* ctx, int* iterations, double* rel_df) {
+  if (!ctx) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
+  CK(cudaMemcpyAsync(&c.pin->it, &c.dsc->it, sizeof(IterState), cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  if (iterations) *iterations = c.pin->it.last;
+  if (rel_df) *rel_df = c.pin->it.relDF;
+  return CUP2D_OK;
+}
+
 int cup2d_calc_dt(cup2d_ctx* ctx, double* dt_out) {
   if (!ctx || !ctx->c.initialised) return ctx ? fail(ctx, CUP2D_ESTATE, "not initialised") : CUP2D_EINVAL;
   Ctx& c = ctx->c;
@@ -628,6 +691,13 @@ int cup2d_put_objects(cup2d_ctx* ctx, double dt) {
     launch_objects_rest(c);
     c.recordPlaced = false;
   }
+  if (c.cfg.iterative) {
+    // PutObjectsOnGrid.cpp:195, 237-238: the grid's deformation velocity,
+    // which the iterated operator's RHS reads
+    CK(cudaMemsetAsync(c.udefx, 0, sizeof(double) * c.ncells(), c.stream));
+    CK(cudaMemsetAsync(c.udefy, 0, sizeof(double) * c.ncells(), c.stream));
+    launch_obj_vel_on_grid(c);
+  }
   // the next step's midlines on the side stream, beside the rest of this
   // step; the next call takes them if the time matches
   if (anyFishShape) {
@@ -670,6 +740,10 @@ int cup2d_adv_diff(cup2d_ctx* ctx, double dt) {
 int cup2d_pressure_single(cup2d_ctx* ctx, double dt) {
   STAGE_PROLOGUE
   c.placedPending = false;
+  if (c.cfg.iterative) {
+    c.rhsFresh = false;
+    return pressure_iterative(ctx);
+  }
   if (!c.rhsFresh) launch_rhs_div(c);       // else formed by advDiff at this dt
   c.rhsFresh = false;
   launch_rhs_obstacles(c);
@@ -712,6 +786,9 @@ namespace cup2d {
 int graph_steps_begin(cup2d_ctx* ctx) {
   Ctx& c = ctx->c;
   if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
+  if (c.cfg.iterative)
+    return fail(ctx, CUP2D_ENOTSUP, "the iterated penalization decides convergence on the host: "
+                                    "run it operator by operator");
   forget_chain(c);
   c.shapesAtEvent = false;
   if (c.cur != 0) {

@@ -25,6 +25,10 @@ struct Ctx {
   double* sdf = nullptr;        // SimulationData::tmp as used by PutObjectsOnGrid
   double* udefx = nullptr;      // SimulationData::uDef
   double* udefy = nullptr;
+  // iterated penalization only: SimulationData::tmpV (the velocity before
+  // the operator) and vFluid (the fluid velocity of an iteration)
+  double* itmp[2] = {nullptr, nullptr};
+  double* ifluid[2] = {nullptr, nullptr};
 
   Scalars* dsc = nullptr;       // device scalars
   DevShape* dshapes = nullptr;  // device shape array [MAX_SHAPES]
@@ -81,7 +85,7 @@ struct Ctx {
   bool shapesAtEvent = false;
   cudaEvent_t evDtNext = nullptr, evShapes = nullptr;
   // pinned host staging of the small read-backs (one copy + one wait each)
-  struct HostPin { double dtNext, dt; int status; Scalars sc; DevShape shape; };
+  struct HostPin { double dtNext, dt; int status; IterState it; Scalars sc; DevShape shape; };
   HostPin* pin = nullptr;
 
   cudaGraphExec_t graph = nullptr;

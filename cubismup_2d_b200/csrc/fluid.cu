@@ -289,6 +289,45 @@ k_rhs_div(GridDesc g, const Scalars* sc, const double* __restrict__ u,
   }
 }
 
+// PressureIterator_unif::updatePressureRHS (PressureIterator_unif.cpp:22-49):
+// tmp = (h/2dt) (div V - chi div UDEF) on the penalized velocity and the
+// grid's deformation velocity, zero-gradient ghosts for both (the same
+// VectorLab), with the fade sums of the strip blocks as k_rhs_div forms them.
+__global__ void __launch_bounds__(256)
+k_rhs_iter(GridDesc g, const Scalars* sc, const double* __restrict__ u, const double* __restrict__ v,
+           const double* __restrict__ udx, const double* __restrict__ udy, const double* __restrict__ chi,
+           double* __restrict__ rhs, const int* __restrict__ fadeSlot, double* __restrict__ fadePartials)
+{
+  pdl_begin();
+  CUP2D_TRACE_SCOPE(TR_RHSDIV);
+  const double h = g.h, facDiv = 0.5 * h / sc->dt;
+  const int nx = g.nx, ny = g.ny;
+  const int bx = blockIdx.x, by = blockIdx.y;
+  const int gx = bx * BS + threadIdx.x;
+  const bool touch = fade_touch(g, bx, by);
+  double s[3] = {0, 0, 0};
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int iy = threadIdx.y + 8 * r, gy = by * BS + iy;
+    const size_t c = (size_t)gy * nx + gx;
+    const size_t cW = gx > 0 ? c - 1 : c, cE = gx < nx - 1 ? c + 1 : c;
+    const size_t cS = gy > 0 ? c - nx : c, cN = gy < ny - 1 ? c + nx : c;
+    const double divVx = u[cE] - u[cW], divVy = v[cN] - v[cS];
+    const double divUSx = udx[cE] - udx[cW], divUSy = udy[cN] - udy[cS];
+    const double b = facDiv * (divVx + divVy - chi[c] * (divUSx + divUSy));
+    rhs[c] = b;
+    if (touch) fade_accumulate(g, bx, by, threadIdx.x, iy, b, s);
+  }
+  if (touch) {
+    __shared__ double red[96];
+    block_sum<3>(s, red);
+    if (lin_tid() == 0) {
+      const int q = fadeSlot[bx + g.bpdx * by];
+      for (int k = 0; k < 3; k++) fadePartials[3 * q + k] = s[k];
+    }
+  }
+}
+
 // fadeSlot[b] = rank of block b among the strip blocks (block order), or -1;
 // fadeSlot[nblocks] = their number.  Once per grid, one thread.
 __global__ void k_fade_slots(GridDesc g, int* fadeSlot)
@@ -472,6 +511,20 @@ int build_fade_slots(Ctx& c) {
       cudaMemcpyAsync(&n, c.fadeSlot + c.g.nblocks, sizeof(int), cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
       cudaStreamSynchronize(c.stream) != cudaSuccess) return -1;
   return n;
+}
+
+void launch_rhs_iter(Ctx& c) {
+  dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
+  launch_k(k_rhs_iter, grid, block, 0, c.stream, c.g, (const Scalars*)c.dsc, (const double*)c.u(),
+           (const double*)c.v(), (const double*)c.udefx, (const double*)c.udefy, (const double*)c.chi,
+           c.rhs, (const int*)c.fadeSlot, fade_partials(c));
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_pcorr_from(Ctx& c, const double* ui, const double* vi, double* uo, double* vo) {
+  dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
+  launch_k(k_pcorr, grid, block, 0, c.stream, c.g, c.dsc, c.pres, ui, vi, uo, vo);
+  CUP2D_LAUNCHED(c);
 }
 
 void launch_pcorr(Ctx& c) {

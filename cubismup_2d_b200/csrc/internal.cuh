@@ -37,6 +37,14 @@ struct GridDesc {
   double fadeLenX, fadeLenY;
 };
 
+// PressureIterator_unif's state between steps (PressureIterator_unif.h:15-16)
+// and of its last call: the relative momentum change of the last iteration,
+// the adaptive target, the previous iteration count, the last count.
+struct IterState {
+  double relDF, target;
+  int oldNsteps, last;
+};
+
 // Per-step scalars (SimulationData.h:45-49 plus values passed between kernels).
 struct Scalars {
   double time, dt, uinfx, uinfy, lambda;
@@ -57,6 +65,7 @@ struct Scalars {
   // set by the midline launched at the start of a graph step: 1 if it could
   // run (the step's dt was carried), else the launch after the step's dt does
   int midlineEarly;
+  IterState it;                   // iterated penalization (-iterativePenalization)
 };
 
 struct ShapeCfg {

@@ -32,6 +32,8 @@ void launch_advdiff_undo(Ctx& c);
 void launch_pcorr_undo(Ctx& c);
 void launch_outflow(Ctx& c);                         // advDiff.cpp:89-116
 void launch_rhs_div(Ctx& c);                         // PressureSingle.cpp:112-128
+void launch_rhs_iter(Ctx& c);                        // PressureIterator_unif.cpp:22-49
+void launch_pcorr_from(Ctx& c, const double* ui, const double* vi, double* uo, double* vo);
 int build_fade_slots(Ctx& c);                        // PoissonSolver.cpp:71-79, once per grid
 void launch_pcorr(Ctx& c);                           // PressureSingle.cpp:216-241
 void launch_end_step_dt(Ctx& c);                     // Simulation.cpp:289-290 + the next step's calcMaxTimestep
@@ -49,6 +51,11 @@ void launch_step_begin(Ctx& c);                      // dt + tile reset + body m
 void launch_obj_vel_on_grid(Ctx& c);                 // PutObjectsOnGrid.cpp:149-184
 void launch_rhs_obstacles(Ctx& c);                   // PressureSingle.cpp:130-213
 void launch_momenta(Ctx& c, const double* ui, const double* vi);  // PressureSingle.cpp:23-67, 362-372
+// PressureIterator_unif.cpp (the iterated penalization)
+void launch_momenta_iter(Ctx& c, const double* ui, const double* vi);   // :80-135 + updateVelocity
+void launch_penalize_iter(Ctx& c, const double* tu, const double* tv,
+                          const double* fu, const double* fv);          // :137-187, residual -> sc->it.relDF
+void launch_set_iter_state(Ctx& c, const IterState& st);                // :247-252 state after a call
 void launch_collide_penalize(Ctx& c);                // PressureSingle.cpp:69-108, 243-344
 void launch_forces(Ctx& c);                          // ComputeForces.cpp:16-111
 

@@ -11,6 +11,7 @@
 // (including the "first writer wins" tests) is evaluated in the reference's
 // order; sums are block reductions per tile followed by a fixed-order sum
 // over tiles.
+#include <cfloat>
 #include <cmath>
 #include "context.hpp"
 #include "rigid_body.cuh"
@@ -360,6 +361,10 @@ k_rhs_corr(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __r
 // correction: the corrected velocity of each cell it reads is evaluated
 // here with k_pcorr's expression (PressureSingle.cpp:216-241) from the
 // pressure and the advected velocity (ui, vi).
+// ITER: PressureIterator_unif::integrateMomenta (PressureIterator_unif.cpp:
+// 80-135) on its fluid velocity: F = h^2 chi (no density), the velocity
+// itself instead of its difference to udef, and no displacement sums.
+template <bool ITER>
 __global__ void __launch_bounds__(1024)
 k_momenta(GridDesc g, const Scalars* sc, DevShape* sh, AllTiles T, const double* __restrict__ p,
           const double* __restrict__ ui, const double* __restrict__ vi,
@@ -389,10 +394,13 @@ k_momenta(GridDesc g, const Scalars* sc, DevShape* sh, AllTiles T, const double*
       const double pS = p[gy > 0 ? c - nx : c], pN = p[gy < ny - 1 ? c + nx : c];
       const double uc = ui[c] + pFac * (pE - pW), vc = vi[c] + pFac * (pN - pS);
       const double p0 = cell_x(g, bx, ix) - Cx, p1 = cell_y(g, by, iy) - Cy;
-      double ux, uy;
-      udef_at(t, o, S, p0, p1, ux, uy);
-      const double ud0 = uc - ux, ud1 = vc - uy;
-      const double F = hsq * rho * chi;
+      double ud0 = uc, ud1 = vc;
+      if (!ITER) {
+        double ux, uy;
+        udef_at(t, o, S, p0, p1, ux, uy);
+        ud0 = uc - ux; ud1 = vc - uy;
+      }
+      const double F = ITER ? hsq * chi : hsq * rho * chi;
       A[0] = F;
       A[1] = F * (p0 * p0 + p1 * p1);
       A[2] = F * p0;
@@ -410,9 +418,71 @@ k_momenta(GridDesc g, const Scalars* sc, DevShape* sh, AllTiles T, const double*
   warp_sum_rows<7>(mp, nt, 7, A);
   if (tid != 0) return;
   S.s.fluidAngMom = A[6]; S.s.fluidMomX = A[4]; S.s.fluidMomY = A[5];
-  S.s.penalDX = A[2]; S.s.penalDY = A[3]; S.s.penalM = A[0]; S.s.penalJ = A[1];
+  S.s.penalDX = ITER ? 0.0 : A[2]; S.s.penalDY = ITER ? 0.0 : A[3];
+  S.s.penalM = A[0]; S.s.penalJ = A[1];
   shape_update_velocity(S, sc->dt, sc->time);
 }
+
+// PressureIterator_unif::penalize (PressureIterator_unif.cpp:137-187), one
+// shape (shapes run in order, as the reference's inner loop visits them per
+// cell): where the shape owns chi, V += (TMPV + chi (U_s - UF)) - V, with
+// TMPV the velocity before the operator and UF the fluid velocity of this
+// iteration.  Per CTA: the sums of V^2 and of the change^2 per component.
+__global__ void __launch_bounds__(1024)
+k_penalize_iter(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
+                double* u, double* v, const double* __restrict__ tu, const double* __restrict__ tv,
+                const double* __restrict__ fu, const double* __restrict__ fv, double* part)
+{
+  pdl_begin();
+  CUP2D_TRACE_SCOPE(TR_PENALIZE);
+  __shared__ double red[32 * 4];
+  const DevShape& S = sh[k];
+  double a[4] = {0, 0, 0, 0};                 // MX, MY, DMX, DMY
+  for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
+    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+    const int ix = threadIdx.x, iy = threadIdx.y;
+    const size_t o = (size_t)s * BS2 + iy * BS + ix;
+    const size_t c = (size_t)(by * BS + iy) * g.nx + bx * BS + ix;
+    const double X = t.chi[o];
+    if (chig[c] > X) continue;
+    if (X <= 0) continue;
+    const double p0 = cell_x(g, bx, ix) - S.s.com[0], p1 = cell_y(g, by, iy) - S.s.com[1];
+    double ux, uy;
+    udef_at(t, o, S, p0, p1, ux, uy);
+    const double US = S.s.u - S.s.omega * p1 + ux;
+    const double VS = S.s.v + S.s.omega * p0 + uy;
+    const double DFX = X * (US - fu[c]), DFY = X * (VS - fv[c]);
+    const double DPX = tu[c] + DFX - u[c], DPY = tv[c] + DFY - v[c];
+    const double un = u[c] + DPX, vn = v[c] + DPY;
+    u[c] = un;
+    v[c] = vn;
+    a[0] += un * un; a[1] += vn * vn; a[2] += DPX * DPX; a[3] += DPY * DPY;
+  }
+  block_sum<4>(a, red);
+  if (lin_tid() == 0) for (int q = 0; q < 4; q++) part[4 * blockIdx.x + q] = a[q];
+}
+
+struct PenalCtas { int n[MAX_SHAPES]; };
+
+// The relative momentum change sqrt((DMX + DMY) / (eps + MX + MY)) of all
+// shapes' penalized cells (PressureIterator_unif.cpp:185-186), from the
+// per-CTA sums in a fixed order.
+__global__ void __launch_bounds__(256)
+k_reldf(Scalars* sc, int nsh, PenalCtas nc, const double* __restrict__ parts, int partStride)
+{
+  pdl_begin();
+  __shared__ double red[32 * 4];
+  double a[4] = {0, 0, 0, 0};
+  for (int k = 0; k < nsh; k++) {
+    const double* pk = parts + (size_t)k * partStride;
+    for (int i = threadIdx.x; i < nc.n[k]; i += blockDim.x)
+      for (int q = 0; q < 4; q++) a[q] += pk[4 * i + q];
+  }
+  block_sum<4>(a, red);
+  if (threadIdx.x == 0) sc->it.relDF = sqrt((a[2] + a[3]) / (DBL_EPSILON + a[0] + a[1]));
+}
+
+__global__ void k_set_iter_state(Scalars* sc, IterState st) { pdl_begin(); sc->it = st; }
 
 // PressureSingle::preventCollidingObstacles (PressureSingle.cpp:243-344).
 // As in the reference, shape i's overlap sums accumulate over every j != i
@@ -717,9 +787,38 @@ void launch_rhs_obstacles(Ctx& c) {
 
 void launch_momenta(Ctx& c, const double* ui, const double* vi) {
   if (c.nshapes == 0) return;
-  launch_k(k_momenta, dim3(tile_ctas(c, c.maxCapacity), c.nshapes), 1024, 0, c.stream, 
+  launch_k(k_momenta<false>, dim3(tile_ctas(c, c.maxCapacity), c.nshapes), 1024, 0, c.stream, 
       c.g, c.dsc, c.dshapes, all_tiles(c), c.pres, ui, vi, shape_partials(c), (int)shape_region(c),
       c.counters + CNT_MOMENTA);
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_momenta_iter(Ctx& c, const double* ui, const double* vi) {
+  if (c.nshapes == 0) return;
+  launch_k(k_momenta<true>, dim3(tile_ctas(c, c.maxCapacity), c.nshapes), 1024, 0, c.stream, 
+      c.g, c.dsc, c.dshapes, all_tiles(c), c.pres, ui, vi, shape_partials(c), (int)shape_region(c),
+      c.counters + CNT_MOMENTA);
+  CUP2D_LAUNCHED(c);
+}
+
+// the per-CTA sums of shape k sit at the start of its partial region (free
+// while the iterated operator runs: the placement's sums are consumed)
+void launch_penalize_iter(Ctx& c, const double* tu, const double* tv, const double* fu, const double* fv) {
+  PenalCtas nc{};
+  for (int k = 0; k < c.nshapes; k++) {
+    nc.n[k] = tile_ctas(c, c.tiles[k].capacity);
+    launch_k(k_penalize_iter, nc.n[k], dim3(32, 32), 0, c.stream, c.g, (const DevShape*)c.dshapes, k,
+             c.tiles[k], (const double*)c.chi, c.u(), c.v(), tu, tv, fu, fv,
+             shape_partials(c) + (size_t)k * shape_region(c));
+    CUP2D_LAUNCHED(c);
+  }
+  launch_k(k_reldf, 1, 256, 0, c.stream, c.dsc, c.nshapes, nc, (const double*)shape_partials(c),
+           (int)shape_region(c));
+  CUP2D_LAUNCHED(c);
+}
+
+void launch_set_iter_state(Ctx& c, const IterState& st) {
+  launch_k(k_set_iter_state, 1, 1, 0, c.stream, c.dsc, st);
   CUP2D_LAUNCHED(c);
 }
 

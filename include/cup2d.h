@@ -78,6 +78,9 @@ typedef struct cup2d_config {
   int poisson;             /* CUP2D_POISSON_*                                   */
   int precision;           /* CUP2D_PREC_*                                      */
   int device;              /* CUDA device ordinal                               */
+  int iterative;           /* -iterativePenalization: PressureIterator_unif     */
+                           /* replaces PressureSingle (Simulation.cpp:213-216);  */
+                           /* operator-by-operator steps only                    */
 } cup2d_config;
 
 /* Shape descriptors (the key=value parameters of Shape.cpp:331-345,
@@ -140,6 +143,13 @@ int cup2d_put_objects(cup2d_ctx* ctx, double dt);      /* PutObjectsOnGrid.cpp:1
 int cup2d_adv_diff(cup2d_ctx* ctx, double dt);         /* advDiff.cpp:36-118            */
 int cup2d_pressure_single(cup2d_ctx* ctx, double dt);  /* PressureSingle.cpp:346-373    */
 int cup2d_compute_forces(cup2d_ctx* ctx, double dt);   /* ComputeForces.cpp:16-111      */
+/* With cup2d_config.iterative, cup2d_pressure_single runs the iterated
+ * penalization and projection of PressureIterator_unif::operator()
+ * (PressureIterator_unif.cpp:214-270): it waits for each iteration's
+ * residual on the host, as the reference decides convergence there, and
+ * cup2d_advance / the ensemble return CUP2D_ENOTSUP.  The iteration count
+ * and the last relative momentum change of the latest call: */
+int cup2d_iteration_stats(cup2d_ctx* ctx, int* iterations, double* rel_df);
 /* time += dt; step++ (Simulation.cpp:289-290). */
 int cup2d_end_step(cup2d_ctx* ctx);
 /* calc_dt + the four operators + end_step, i.e. one pass of

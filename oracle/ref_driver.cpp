@@ -5,11 +5,12 @@
 // oracle/shim (Cubism grid/lab/parser, FFTW API, 3x3 GSL LU).  It replaces
 // main.cpp / Simulation.cpp, whose include set drags in the HYPRE-only
 // variable-density operators; the steps below restate Simulation.cpp for the
-// constant-density, non-iterative pipeline:
+// constant-density pipeline (PressureSingle, or PressureIterator_unif under
+// -iterativePenalization 1):
 //   parseRuntime        Simulation.cpp:66-104
 //   createShapes        Simulation.cpp:106-173
-//   init (pipeline)     Simulation.cpp:175-230 (bVariableDensity == false,
-//                       iterativePenalization == 0 branch, :205-221)
+//   init (pipeline)     Simulation.cpp:175-230 (bVariableDensity == false
+//                       branch, :205-221)
 //   reset               Simulation.cpp:232-241
 //   calcMaxTimestep     Simulation.cpp:254-277
 //   advance             Simulation.cpp:279-305
@@ -21,6 +22,7 @@
 #include "Operators/PutObjectsOnGrid.h"
 #include "Operators/advDiff.h"
 #include "Operators/PressureSingle.h"
+#include "Operators/PressureIterator_unif.h"
 #include "Operators/ComputeForces.h"
 #include "Obstacles/ShapesSimple.h"
 #include "Obstacles/StefanFish.h"
@@ -144,7 +146,10 @@ struct RefSim
     sim.bStaggeredGrid = false;
     pipeline.push_back(new PutObjectsOnGrid(sim));
     pipeline.push_back(new advDiff(sim));
-    pipeline.push_back(new PressureSingle(sim));
+    // Simulation.cpp:213-216: -iterativePenalization selects the iterated
+    // penalization/projection operator in place of PressureSingle
+    if (sim.iterativePenalization) pipeline.push_back(new PressureIterator_unif(sim));
+    else pipeline.push_back(new PressureSingle(sim));
     pipeline.push_back(new ComputeForces(sim));
     reset();
     sim.dt = 0;
