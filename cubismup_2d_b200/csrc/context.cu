@@ -386,6 +386,9 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
               cudaEventCreateWithFlags(&c.evDtNext, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evShapes, cudaEventDisableTiming) != cudaSuccess ||
               cudaMallocHost(&c.pin, sizeof(Ctx::HostPin)) != cudaSuccess ||
+              cudaHostAlloc(&c.map, sizeof(Ctx::HostMapped), cudaHostAllocMapped) != cudaSuccess ||
+              cudaHostGetDevicePointer(&c.mapDev, c.map, 0) != cudaSuccess ||
+              cudaEventCreateWithFlags(&c.evForces, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evJoin, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evObj, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evObjDone, cudaEventDisableTiming) != cudaSuccess ||
@@ -427,6 +430,8 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   if (c.evDtNext) cudaEventDestroy(c.evDtNext);
   if (c.evShapes) cudaEventDestroy(c.evShapes);
   if (c.pin) cudaFreeHost(c.pin);
+  if (c.map) cudaFreeHost(c.map);
+  if (c.evForces) cudaEventDestroy(c.evForces);
   if (c.evJoin) cudaEventDestroy(c.evJoin);
   if (c.evPres) cudaEventDestroy(c.evPres);
   if (c.evMom) cudaEventDestroy(c.evMom);
@@ -586,7 +591,7 @@ int cup2d_init(cup2d_ctx* ctx) {
   // Simulation::reset (Simulation.cpp:232-241): resetAll, IC, objects at t=0, ApplyObjVel
   if ((rc = upload_scalars_reset(ctx))) return rc;
   c.dtValidMaybe = c.dtCarried = false;
-  c.shapesAtEvent = false;
+  c.shapesAtEvent = c.shapesMapped = false;
   forget_chain(c);
   for (int k = 0; k < c.nshapes; k++) {
     DevShape& S = c.hshapes[k];
@@ -637,7 +642,7 @@ int cup2d_calc_dt(cup2d_ctx* ctx, double* dt_out) {
     c.devDt = NAN;
     if (dt_out) {
       CK(cudaEventSynchronize(c.evDtNext));
-      *dt_out = c.devDt = c.pin->dtNext;
+      *dt_out = c.devDt = *(volatile const double*)&c.map->dtNext;
     }
     return CUP2D_OK;
   }
@@ -662,6 +667,7 @@ int cup2d_calc_dt(cup2d_ctx* ctx, double* dt_out) {
   Ctx& c = ctx->c;                                                               \
   if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");         \
   c.shapesAtEvent = false;                                                       \
+  c.shapesMapped = false;                                                        \
   bool prologueLaunched = c.dtValidMaybe;                                        \
   CK(invalidate_dt_next(c));                                                     \
   if (dt >= 0 && !same_bits(dt, c.devDt)) {                                      \
@@ -755,7 +761,9 @@ int cup2d_pressure_single(cup2d_ctx* ctx, double dt) {
 int cup2d_compute_forces(cup2d_ctx* ctx, double dt) {
   STAGE_PROLOGUE
   forget_chain(c);
-  launch_forces(c);
+  launch_forces(c, c.mapDev->shapes);       // the final states also to mapped host memory
+  CK(cudaEventRecord(c.evForces, c.stream));
+  c.shapesMapped = true;
   return check_launch(ctx);
 }
 
@@ -771,8 +779,7 @@ int cup2d_end_step(cup2d_ctx* ctx) {
   // nothing from here on writes the shape states
   CK(cudaEventRecord(c.evShapes, c.stream));
   c.shapesAtEvent = true;
-  launch_end_step_max(c);
-  CK(cudaMemcpyAsync(&c.pin->dtNext, &c.dsc->dtNext, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  launch_end_step_max(c, &c.mapDev->dtNext);   // the next dt also to mapped host memory
   CK(cudaEventRecord(c.evDtNext, c.stream));
   c.dtValidMaybe = c.dtCarried = true;
   return check_launch(ctx);
@@ -790,7 +797,7 @@ int graph_steps_begin(cup2d_ctx* ctx) {
     return fail(ctx, CUP2D_ENOTSUP, "the iterated penalization decides convergence on the host: "
                                     "run it operator by operator");
   forget_chain(c);
-  c.shapesAtEvent = false;
+  c.shapesAtEvent = c.shapesMapped = false;
   if (c.cur != 0) {
     // a stage was called on its own: finish in eager mode until parity returns
     return fail(ctx, CUP2D_ESTATE, "velocity buffers out of step order");
@@ -902,6 +909,15 @@ int cup2d_get_shape(cup2d_ctx* ctx, int id, cup2d_shape_state* out) {
   if (!ctx || !out) return CUP2D_EINVAL;
   Ctx& c = ctx->c;
   if (id < 0 || id >= c.nshapes) return fail(ctx, CUP2D_EINVAL, "bad shape id");
+  if (c.shapesMapped) {
+    // written to mapped host memory by the force pass, the last writer
+    CK(cudaEventSynchronize(c.evForces));
+    const volatile double* src = reinterpret_cast<const volatile double*>(&c.map->shapes[id]);
+    double* dst = reinterpret_cast<double*>(&c.hshapes[id].s);
+    for (size_t q = 0; q < sizeof(cup2d_shape_state) / sizeof(double); q++) dst[q] = src[q];
+    *out = c.hshapes[id].s;
+    return CUP2D_OK;
+  }
   if (c.shapesAtEvent) {
     // final since the step end began: read beside its kernels
     CK(cudaStreamWaitEvent(c.side2, c.evShapes, 0));
@@ -925,7 +941,7 @@ int cup2d_set_shape(cup2d_ctx* ctx, int id, const cup2d_shape_state* in) {
   c.hshapes[id].s = *in;
   CK(cudaMemcpy(c.dshapes + id, &c.hshapes[id], sizeof(DevShape), cudaMemcpyHostToDevice));
   forget_chain(c);
-  c.shapesAtEvent = false;
+  c.shapesAtEvent = c.shapesMapped = false;
   CK(invalidate_dt_next(c));
   return CUP2D_OK;
 }
@@ -956,7 +972,7 @@ int cup2d_set_scalars(cup2d_ctx* ctx, double time, double dt, int step, double u
   c.midByGraph = false;
   c.devDt = dt;
   c.dtValidMaybe = c.dtCarried = false;
-  c.shapesAtEvent = false;
+  c.shapesAtEvent = c.shapesMapped = false;
   forget_chain(c);
   return CUP2D_OK;
 }
@@ -982,7 +998,7 @@ int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, double* ms_per_launch
   if (which < 0 || which > CUP2D_KERNEL_OBJECTS) return fail(ctx, CUP2D_EINVAL, "unknown kernel");
   CK(invalidate_dt_next(c));
   forget_chain(c);
-  c.shapesAtEvent = false;
+  c.shapesAtEvent = c.shapesMapped = false;
   c.devDt = NAN;
   auto one = [&]() {
     switch (which) {
@@ -1358,7 +1374,7 @@ int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes) {
   c.devDt = NAN;
   c.dtValidMaybe = true;
   c.dtCarried = false;
-  c.shapesAtEvent = false;
+  c.shapesAtEvent = c.shapesMapped = false;
   forget_chain(c);
   c.sideMidPending = false;
   c.midByGraph = false;

@@ -72,7 +72,7 @@ struct Ctx {
   // that the operator-by-operator path launches nothing redundant:
   //   devDt        sc->dt (NaN: not known on the host)
   //   dtValidMaybe sc->dtNextValid may be 1 (a step end formed the next dt)
-  //   dtCarried    sc->dtNextValid is 1 and pin->dtNext holds sc->dtNext
+  //   dtCarried    sc->dtNextValid is 1 and map->dtNext holds sc->dtNext
   //                once evDtNext has completed
   //   rhsFresh     rhs and the fade partials hold the RHS divergence of the
   //                current velocity at sc->dt (formed in place by advDiff)
@@ -85,8 +85,16 @@ struct Ctx {
   bool shapesAtEvent = false;
   cudaEvent_t evDtNext = nullptr, evShapes = nullptr;
   // pinned host staging of the small read-backs (one copy + one wait each)
-  struct HostPin { double dtNext, dt; int status; IterState it; Scalars sc; DevShape shape; };
+  struct HostPin { double dt; int status; IterState it; Scalars sc; DevShape shape; };
   HostPin* pin = nullptr;
+  // mapped pinned memory the operator path's kernels write directly (no copy
+  // engine): the next dt (step end) and each shape's final state (force
+  // pass).  shapesMapped: map->shapes is current once evForces completes.
+  struct HostMapped { double dtNext; cup2d_shape_state shapes[MAX_SHAPES]; };
+  HostMapped* map = nullptr;      // host address
+  HostMapped* mapDev = nullptr;   // its device address
+  cudaEvent_t evForces = nullptr;
+  bool shapesMapped = false;
 
   cudaGraphExec_t graph = nullptr;
   unsigned graphGen = 0;        // bumped whenever what a step captures changes

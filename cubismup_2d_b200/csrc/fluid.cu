@@ -51,7 +51,7 @@ __global__ void k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int n
 // a graph step's k_max_next and k_end_step_dt in one launch.
 __global__ void __launch_bounds__(512)
 k_end_step_max(GridDesc g, Scalars* sc, const DevShape* sh, int nsh, const double* __restrict__ u,
-               const double* __restrict__ v, double* partials, unsigned* counter)
+               const double* __restrict__ v, double* partials, unsigned* counter, double* dtOut)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_ENDSTEP);
@@ -60,9 +60,11 @@ k_end_step_max(GridDesc g, Scalars* sc, const DevShape* sh, int nsh, const doubl
   if (!max_u_cta(g, sc, u, v, partials, counter, red, &m)) return;
   sc->time += sc->dt;
   sc->step += 1;
-  sc->dtNext = dt_from_max_u(g, sc, sh, nsh, m);
+  const double dtn = dt_from_max_u(g, sc, sh, nsh, m);
+  sc->dtNext = dtn;
   sc->maxUNext = m;
   sc->dtNextValid = 1;
+  if (dtOut) *dtOut = dtn;                    // to mapped host memory
 }
 
 // calcMaxTimestep of a state whose dt the last step end already formed
@@ -441,9 +443,9 @@ void launch_max_next(Ctx& c) {
   CUP2D_LAUNCHED(c);
 }
 
-void launch_end_step_max(Ctx& c) {
+void launch_end_step_max(Ctx& c, double* dtOut) {
   launch_k(k_end_step_max, max_grid(c), 512, 0, c.stream, c.g, c.dsc, (const DevShape*)c.dshapes, c.nshapes,
-           (const double*)c.u(), (const double*)c.v(), c.partials, c.counters + CNT_MAXU);
+           (const double*)c.u(), (const double*)c.v(), c.partials, c.counters + CNT_MAXU, dtOut);
   CUP2D_LAUNCHED(c);
 }
 

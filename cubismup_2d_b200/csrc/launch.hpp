@@ -39,7 +39,8 @@ void launch_pcorr(Ctx& c);                           // PressureSingle.cpp:216-2
 void launch_end_step_dt(Ctx& c);                     // Simulation.cpp:289-290 + the next step's calcMaxTimestep
 void launch_max_next(Ctx& c);                        // its findMaxU on the final velocity
 void launch_take_dt_next(Ctx& c);                    // calcMaxTimestep from the carried dt
-void launch_end_step_max(Ctx& c);                    // findMaxU + Simulation.cpp:289-290 + the next dt
+// findMaxU + Simulation.cpp:289-290 + the next dt (also to dtOut: mapped host memory, or null)
+void launch_end_step_max(Ctx& c, double* dtOut = nullptr);
 void launch_ic(Ctx& c);                              // Helpers.cpp:38-82
 void launch_apply_obj_vel(Ctx& c);                   // Helpers.cpp:290-307
 
@@ -57,7 +58,8 @@ void launch_penalize_iter(Ctx& c, const double* tu, const double* tv,
                           const double* fu, const double* fv);          // :137-187, residual -> sc->it.relDF
 void launch_set_iter_state(Ctx& c, const IterState& st);                // :247-252 state after a call
 void launch_collide_penalize(Ctx& c);                // PressureSingle.cpp:69-108, 243-344
-void launch_forces(Ctx& c);                          // ComputeForces.cpp:16-111
+// ComputeForces.cpp:16-111; out (mapped host memory, or null): each shape's final state
+void launch_forces(Ctx& c, cup2d_shape_state* out = nullptr);
 
 // poisson.cu
 struct Poisson;

@@ -598,7 +598,7 @@ k_penalize(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __r
 __global__ void __launch_bounds__(1024)
 k_forces(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ u,
          const double* __restrict__ v, const double* __restrict__ p,
-         double* partials, int partStride, unsigned* counters)
+         double* partials, int partStride, unsigned* counters, cup2d_shape_state* out)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_FORCES);
@@ -680,6 +680,7 @@ k_forces(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ u,
   const double demBnd = st.Pthrust - st.defPowerBnd;
   st.EffPDef = st.Pthrust / fmax(denUnb, EPSd);
   st.EffPDefBnd = st.Pthrust / fmax(demBnd, EPSd);
+  if (out) out[k] = st;                       // the final state, to mapped host memory
 }
 
 inline size_t shape_region(const Ctx& c) { return (size_t)c.maxCapacity * 24; }
@@ -836,12 +837,12 @@ void launch_collide_penalize(Ctx& c) {
   }
 }
 
-void launch_forces(Ctx& c) {
+void launch_forces(Ctx& c, cup2d_shape_state* out) {
   if (c.nshapes == 0) return;
   const AllTiles T = all_tiles(c);
   launch_k(k_forces, dim3(tile_ctas(c, c.maxCapacity), c.nshapes), dim3(32, 32), 0, c.stream,
       c.g, c.dshapes, T, c.u(), c.v(), c.pres, shape_partials(c), (int)shape_region(c),
-      c.counters + CNT_FORCES);
+      c.counters + CNT_FORCES, out);
   CUP2D_LAUNCHED(c);
 }
 
