@@ -65,7 +65,8 @@ def ensemble_configs(n=64, seed=0):
     for _ in range(n):
         bx, by = ENSEMBLE_GRIDS[rng.integers(len(ENSEMBLE_GRIDS))]
         re = float(np.exp(rng.uniform(np.log(100.0), np.log(1000.0))))
-        grid = f"-bpdx {bx} -bpdy {by} -extent 1 -CFL 0.1 -lambda 1e4 -poissonType freespace -nsteps 500"
+        grid = (f"-bpdx {bx} -bpdy {by} -extent 1 -CFL 0.1 -lambda 1e4 -poissonType freespace -nsteps 500 "
+                "-muteAll 1")
         if rng.uniform() < 0.5:
             r = float(rng.uniform(0.02, 0.05))
             nu = 0.2 * 2 * r / re
