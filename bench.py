@@ -470,7 +470,7 @@ def run_ensemble(args, world, rank, local, pg):
     seq_ms = max_over_ranks(pg, float(sum(s.ctx.time_step(args.steps) for s in sims)))
     seq_value = world * cells * args.steps / (seq_ms / 1e3) / 1e9
 
-    # e2e: an ensemble step, then every member's shape state read back
+    # e2e: an ensemble step, then every member's shape states read back
     ne = max(10, args.steps // 10)
     if pg is not None:
         pg.barrier()
@@ -478,8 +478,7 @@ def run_ensemble(args, world, rank, local, pg):
     t0 = time.perf_counter()
     for _ in range(ne):
         ens.advance(1)
-        for s in sims:
-            _ = s.ctx.shape(0)
+        _ = ens.shape_states()
     ens.sync()
     e2e_s = max_over_ranks(pg, time.perf_counter() - t0)
     e2e = world * cells * ne / e2e_s / 1e9

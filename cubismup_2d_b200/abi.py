@@ -39,7 +39,8 @@ EXPORTS = [
     "cup2d_grid_size", "cup2d_kernel_launches", "cup2d_time_kernel", "cup2d_advance_timed",
     "cup2d_checkpoint_size", "cup2d_checkpoint_save", "cup2d_checkpoint_load",
     "cup2d_ensemble_create", "cup2d_ensemble_advance", "cup2d_ensemble_advance_timed",
-    "cup2d_ensemble_sync", "cup2d_ensemble_last_error", "cup2d_ensemble_destroy",
+    "cup2d_ensemble_sync", "cup2d_ensemble_get_shapes", "cup2d_ensemble_last_error",
+    "cup2d_ensemble_destroy",
     "cup2d_adv_diff_noalloc",
 ]
 KERNELS = {"advdiff": 0, "rhs_div": 1, "pcorr": 2, "fft_rows_fwd": 3, "fft_cols": 4,
@@ -124,6 +125,7 @@ def lib():
     L.cup2d_ensemble_advance.argtypes = [vp, i]
     L.cup2d_ensemble_advance_timed.argtypes = [vp, i, dp]
     L.cup2d_ensemble_sync.argtypes = [vp]
+    L.cup2d_ensemble_get_shapes.argtypes = [vp, ctypes.POINTER(ShapeState), i, ip]
     L.cup2d_ensemble_last_error.argtypes = [vp]
     L.cup2d_ensemble_last_error.restype = ctypes.c_char_p
     L.cup2d_ensemble_destroy.argtypes = [vp]
@@ -489,6 +491,25 @@ class Ensemble:
 
     def sync(self):
         self._ck(self.L.cup2d_ensemble_sync(self.h_))
+
+    def shape_states(self):
+        """Every member's shape states, member by member, as an (n, 42) array
+        in SHAPE_STATE_FIELDS order (one wait after an ensemble advance)."""
+        self._members_current()
+        n = sum(c.nshapes for c in self.ctxs)
+        buf = (ShapeState * max(n, 1))()
+        cnt = ctypes.c_int()
+        self._ck(self.L.cup2d_ensemble_get_shapes(self.h_, buf, n, ctypes.byref(cnt)))
+        return np.ctypeslib.as_array(ctypes.cast(buf, ctypes.POINTER(ctypes.c_double)),
+                                     shape=(n, len(SHAPE_STATE_FIELDS))).copy()
+
+    def shapes(self):
+        """shape_states() as one list of dicts per member."""
+        a, out, o = self.shape_states(), [], 0
+        for c in self.ctxs:
+            out.append([dict(zip(SHAPE_STATE_FIELDS, a[o + k].tolist())) for k in range(c.nshapes)])
+            o += c.nshapes
+        return out
 
     def close(self):
         if getattr(self, "h_", None):

@@ -236,7 +236,7 @@ void enqueue_step(Ctx& c) {
   launch_rhs_obstacles(c);
   poisson_solve(c);
   launch_pressure_tail(c);
-  launch_forces(c);
+  launch_forces(c, c.forcesOut);
   if (anyFish) cudaStreamWaitEvent(c.stream, c.evJoin, 0);
   cudaStreamWaitEvent(c.stream, c.evMaxFree, 0);
   launch_end_step_dt(c);                    // t += dt, and the next step's dt
@@ -592,6 +592,7 @@ int cup2d_init(cup2d_ctx* ctx) {
   if ((rc = upload_scalars_reset(ctx))) return rc;
   c.dtValidMaybe = c.dtCarried = false;
   c.shapesAtEvent = c.shapesMapped = false;
+  c.stateSeq++;
   forget_chain(c);
   for (int k = 0; k < c.nshapes; k++) {
     DevShape& S = c.hshapes[k];
@@ -634,6 +635,7 @@ int cup2d_calc_dt(cup2d_ctx* ctx, double* dt_out) {
   if (!ctx || !ctx->c.initialised) return ctx ? fail(ctx, CUP2D_ESTATE, "not initialised") : CUP2D_EINVAL;
   Ctx& c = ctx->c;
   forget_chain(c);                          // sets sc->dt (and overwrites the grid partials)
+  c.stateSeq++;
   if (c.dtCarried) {
     // formed by the last step end from this very state
     launch_take_dt_next(c);
@@ -668,6 +670,7 @@ int cup2d_calc_dt(cup2d_ctx* ctx, double* dt_out) {
   if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");         \
   c.shapesAtEvent = false;                                                       \
   c.shapesMapped = false;                                                        \
+  c.stateSeq++;                                                                  \
   bool prologueLaunched = c.dtValidMaybe;                                        \
   CK(invalidate_dt_next(c));                                                     \
   if (dt >= 0 && !same_bits(dt, c.devDt)) {                                      \
@@ -776,6 +779,7 @@ int cup2d_end_step(cup2d_ctx* ctx) {
   Ctx& c = ctx->c;
   if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
   forget_chain(c);
+  c.stateSeq++;
   // nothing from here on writes the shape states
   CK(cudaEventRecord(c.evShapes, c.stream));
   c.shapesAtEvent = true;
@@ -798,6 +802,7 @@ int graph_steps_begin(cup2d_ctx* ctx) {
                                     "run it operator by operator");
   forget_chain(c);
   c.shapesAtEvent = c.shapesMapped = false;
+  c.stateSeq++;
   if (c.cur != 0) {
     // a stage was called on its own: finish in eager mode until parity returns
     return fail(ctx, CUP2D_ESTATE, "velocity buffers out of step order");
@@ -901,6 +906,7 @@ int cup2d_set_field(cup2d_ctx* ctx, int which, const double* host_in) {
   CK(cudaStreamSynchronize(c.stream));
   CK(cudaMemcpy(p, host_in, sizeof(double) * c.ncells(), cudaMemcpyHostToDevice));
   forget_chain(c);
+  c.stateSeq++;
   CK(invalidate_dt_next(c));
   return CUP2D_OK;
 }
@@ -942,6 +948,7 @@ int cup2d_set_shape(cup2d_ctx* ctx, int id, const cup2d_shape_state* in) {
   CK(cudaMemcpy(c.dshapes + id, &c.hshapes[id], sizeof(DevShape), cudaMemcpyHostToDevice));
   forget_chain(c);
   c.shapesAtEvent = c.shapesMapped = false;
+  c.stateSeq++;
   CK(invalidate_dt_next(c));
   return CUP2D_OK;
 }
@@ -973,6 +980,7 @@ int cup2d_set_scalars(cup2d_ctx* ctx, double time, double dt, int step, double u
   c.devDt = dt;
   c.dtValidMaybe = c.dtCarried = false;
   c.shapesAtEvent = c.shapesMapped = false;
+  c.stateSeq++;
   forget_chain(c);
   return CUP2D_OK;
 }
@@ -999,6 +1007,7 @@ int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, double* ms_per_launch
   CK(invalidate_dt_next(c));
   forget_chain(c);
   c.shapesAtEvent = c.shapesMapped = false;
+  c.stateSeq++;
   c.devDt = NAN;
   auto one = [&]() {
     switch (which) {
@@ -1059,6 +1068,15 @@ struct cup2d_ensemble {
   std::vector<unsigned> gens;                // members' graphGen at capture
   cudaGraphExec_t graph = nullptr;
   std::string err;
+  // every member's final shape states, written by the captured force passes
+  // into mapped host memory; first[i]: member i's first shape there;
+  // seq[i]: the member's stateSeq after the ensemble's last advance
+  cup2d_shape_state* map = nullptr;
+  cup2d_shape_state* mapDev = nullptr;
+  int mapLen = 0;
+  std::vector<int> first;
+  std::vector<unsigned long long> seq;
+  bool advanced = false;
 };
 
 namespace {
@@ -1081,13 +1099,27 @@ int ens_fail(cup2d_ensemble* ens, int code, const std::string& msg) {
 int ens_capture(cup2d_ensemble* ens) {
   if (ens->graph) { cudaGraphExecDestroy(ens->graph); ens->graph = nullptr; }
   const int n = (int)ens->m.size();
+  int total = 0;
+  for (int i = 0; i < n; i++) { ens->first[i] = total; total += ens->m[i]->c.nshapes; }
+  if (total > ens->mapLen) {
+    CKE(cudaStreamSynchronize(ens->stream));  // earlier launches wrote the old block
+    if (ens->map) cudaFreeHost(ens->map);
+    ens->map = ens->mapDev = nullptr;
+    ens->mapLen = 0;
+    CKE(cudaHostAlloc(&ens->map, sizeof(cup2d_shape_state) * total, cudaHostAllocMapped));
+    CKE(cudaHostGetDevicePointer(&ens->mapDev, ens->map, 0));
+    ens->mapLen = total;
+  }
+  ens->advanced = false;
   CKE(cudaStreamBeginCapture(ens->stream, cudaStreamCaptureModeThreadLocal));
   cudaEventRecord(ens->evRoot, ens->stream);
   for (int i = 0; i < n; i++) {
     Ctx& c = ens->m[i]->c;
     const long long before = c.launches;
     cudaStreamWaitEvent(c.stream, ens->evRoot, 0);
+    c.forcesOut = ens->mapDev + ens->first[i];
     enqueue_step(c);
+    c.forcesOut = nullptr;
     cudaEventRecord(ens->evOut[i], c.stream);
     cudaStreamWaitEvent(ens->stream, ens->evOut[i], 0);
     ens->launchesPerStep[i] = (int)(c.launches - before);
@@ -1135,7 +1167,9 @@ int ens_advance(cup2d_ensemble* ens, int nsteps, bool timed) {
     Ctx& c = ens->m[i]->c;
     CKE(cudaStreamWaitEvent(c.stream, ens->evEnd, 0));
     graph_steps_end(c);
+    ens->seq[i] = c.stateSeq;
   }
+  ens->advanced = true;
   return CUP2D_OK;
 }
 
@@ -1159,6 +1193,8 @@ int cup2d_ensemble_create(cup2d_ctx* const* members, int n, cup2d_ensemble** out
   ens->evOut.assign(n, nullptr);
   ens->launchesPerStep.assign(n, 0);
   ens->gens.assign(n, 0);
+  ens->first.assign(n, 0);
+  ens->seq.assign(n, 0);
   if (cudaSetDevice(members[0]->c.device) != cudaSuccess) { delete ens; return CUP2D_ECUDA; }
   int prLeast = 0, prGreatest = 0;
   cudaDeviceGetStreamPriorityRange(&prLeast, &prGreatest);
@@ -1202,6 +1238,35 @@ int cup2d_ensemble_sync(cup2d_ensemble* ens) {
   return CUP2D_OK;
 }
 
+int cup2d_ensemble_get_shapes(cup2d_ensemble* ens, cup2d_shape_state* out, int capacity, int* count) {
+  if (!ens || !count) return CUP2D_EINVAL;
+  const int n = (int)ens->m.size();
+  int total = 0;
+  for (int i = 0; i < n; i++) total += ens->m[i]->c.nshapes;
+  *count = total;
+  if (!out || capacity < total) return ens_fail(ens, CUP2D_EINVAL, "shape buffer too small");
+  if (ens->advanced) CKE(cudaEventSynchronize(ens->evEnd));
+  int o = 0;
+  for (int i = 0; i < n; i++) {
+    cup2d_ctx* ctx = ens->m[i];
+    Ctx& c = ctx->c;
+    const bool mapped = ens->advanced && ens->seq[i] == c.stateSeq && ens->map &&
+                        ens->first[i] + c.nshapes <= ens->mapLen;
+    for (int k = 0; k < c.nshapes; k++, o++) {
+      if (mapped) {
+        // written by the member's last force pass inside the ensemble's graph
+        const volatile double* src = reinterpret_cast<const volatile double*>(&ens->map[ens->first[i] + k]);
+        double* dst = reinterpret_cast<double*>(&out[o]);
+        for (size_t q = 0; q < sizeof(cup2d_shape_state) / sizeof(double); q++) dst[q] = src[q];
+      } else {
+        const int rc = cup2d_get_shape(ctx, k, &out[o]);
+        if (rc) return ens_fail(ens, rc, "member " + std::to_string(i) + ": " + c.err);
+      }
+    }
+  }
+  return CUP2D_OK;
+}
+
 const char* cup2d_ensemble_last_error(const cup2d_ensemble* ens) {
   return ens ? ens->err.c_str() : "null ensemble";
 }
@@ -1214,6 +1279,7 @@ int cup2d_ensemble_destroy(cup2d_ensemble* ens) {
   for (cudaEvent_t e : ens->evOut) if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : {ens->evRoot, ens->evEnd, ens->ev0, ens->ev1}) if (e) cudaEventDestroy(e);
   if (ens->stream) cudaStreamDestroy(ens->stream);
+  if (ens->map) cudaFreeHost(ens->map);
   delete ens;
   return CUP2D_OK;
 }
@@ -1375,6 +1441,7 @@ int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes) {
   c.dtValidMaybe = true;
   c.dtCarried = false;
   c.shapesAtEvent = c.shapesMapped = false;
+  c.stateSeq++;
   forget_chain(c);
   c.sideMidPending = false;
   c.midByGraph = false;

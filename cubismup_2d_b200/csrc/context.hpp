@@ -95,6 +95,12 @@ struct Ctx {
   HostMapped* mapDev = nullptr;   // its device address
   cudaEvent_t evForces = nullptr;
   bool shapesMapped = false;
+  // a graph step's force pass also writes the final shape states here when
+  // an ensemble captures it (null otherwise)
+  cup2d_shape_state* forcesOut = nullptr;
+  // bumped by every call that may change the state; an ensemble compares it
+  // with the value after its own advance to know a member's read-back is current
+  unsigned long long stateSeq = 0;
 
   cudaGraphExec_t graph = nullptr;
   unsigned graphGen = 0;        // bumped whenever what a step captures changes

@@ -236,6 +236,12 @@ int cup2d_ensemble_create(cup2d_ctx* const* members, int n, cup2d_ensemble** out
 int cup2d_ensemble_advance(cup2d_ensemble* ens, int nsteps);
 int cup2d_ensemble_advance_timed(cup2d_ensemble* ens, int nsteps, double* ms);
 int cup2d_ensemble_sync(cup2d_ensemble* ens);
+/* Every member's shape states, member by member (*count of them; CUP2D_EINVAL
+ * when capacity is smaller), as cup2d_get_shape returns them.  After an
+ * ensemble advance the graph's force passes have written them to mapped host
+ * memory: one wait for all members; a member used on its own since is read
+ * through cup2d_get_shape. */
+int cup2d_ensemble_get_shapes(cup2d_ensemble* ens, cup2d_shape_state* out, int capacity, int* count);
 const char* cup2d_ensemble_last_error(const cup2d_ensemble* ens);
 int cup2d_ensemble_destroy(cup2d_ensemble* ens);
 

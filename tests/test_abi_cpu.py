@@ -73,6 +73,8 @@ def test_ensemble_entry_points_reject_bad_arguments():
     assert L.cup2d_ensemble_advance(None, 1) == abi.EINVAL
     assert L.cup2d_ensemble_advance_timed(None, 1, None) == abi.EINVAL
     assert L.cup2d_ensemble_sync(None) == abi.EINVAL
+    cnt = ctypes.c_int()
+    assert L.cup2d_ensemble_get_shapes(None, None, 0, ctypes.byref(cnt)) == abi.EINVAL
     assert L.cup2d_ensemble_destroy(None) == abi.EINVAL
     assert L.cup2d_ensemble_last_error(None) == b"null ensemble"
 

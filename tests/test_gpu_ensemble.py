@@ -106,3 +106,32 @@ def test_ensemble_rejects_bad_members():
     s.init()                                   # a new context replaces the member's
     with pytest.raises(Cup2DError):
         ens.advance(1)
+
+
+TWO_DISKS = ("-bpdx 8 -bpdy 4 -extent 1 -CFL 0.1 -nu 1e-3 -poissonType freespace "
+             "-shapes 'disk radius=0.06 xpos=0.4375 ypos=0.25 xvel=-0.3 bForced=1, "
+             "disk radius=0.06 xpos=0.5625 ypos=0.26 xvel=0.3'")
+
+
+def test_ensemble_shape_states_read_back():
+    """One batched read-back of every member's shape states equals each
+    member's own read-back: after ensemble steps (from mapped memory), and
+    after a member's own graph or operator step (through the member)."""
+    from cubismup_2d_b200.abi import SHAPE_STATE_FIELDS
+    members = [_member(x, i) for i, x in enumerate(ensemble_configs(n=4, seed=4) + [TWO_DISKS])]
+    ens = Ensemble(members)
+
+    def own():
+        return np.array([[s.ctx.shape(k)[f] for f in SHAPE_STATE_FIELDS]
+                         for s in members for k in range(s.ctx.nshapes)])
+
+    ens.advance(2)
+    a = ens.shape_states()
+    assert a.shape == (6, len(SHAPE_STATE_FIELDS))
+    assert np.array_equal(a, own())
+    members[1].ctx.advance(1)
+    _operator_step(members[4])
+    assert np.array_equal(ens.shape_states(), own())
+    ens.advance(1)
+    assert np.array_equal(ens.shape_states(), own())
+    assert ens.shapes()[4][1]["forcex"] == members[4].ctx.shape(1)["forcex"]
