@@ -88,3 +88,29 @@ def test_checkpoint_entry_points_reject_bad_arguments():
     assert L.cup2d_checkpoint_size(None, ctypes.byref(n)) == abi.EINVAL
     assert L.cup2d_checkpoint_save(None, None, 0) == abi.EINVAL
     assert L.cup2d_checkpoint_load(None, None, 0) == abi.EINVAL
+
+
+def test_header_compiles_as_c_and_matches_the_binding(tmp_path):
+    """include/cup2d.h is plain C (a C caller, not only nvcc, can include it),
+    and the ctypes structures of the Python binding have its layouts."""
+    import ctypes
+    import shutil
+    from cubismup_2d_b200 import abi
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "layout.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "cup2d.h"\n'
+        "int main(void) {\n"
+        '  printf("%zu %zu %zu %zu %zu\\n", sizeof(cup2d_config), sizeof(cup2d_shape_params),\n'
+        "         sizeof(cup2d_shape_state), offsetof(cup2d_config, iterative),\n"
+        "         offsetof(cup2d_shape_state, forcex));\n"
+        "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                        str(src), "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
+    assert got == [ctypes.sizeof(abi.Config), ctypes.sizeof(abi.ShapeParams), ctypes.sizeof(abi.ShapeState),
+                   abi.Config.iterative.offset, abi.ShapeState.forcex.offset]
