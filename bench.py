@@ -64,7 +64,7 @@ ENSEMBLE_NAME = "ensemble{}_seed0_fp64"
 
 # fp64 bytes per cell that each dense kernel must move (reads + writes once)
 ALGO_BYTES_PER_CELL = {
-    "advdiff": 32,        # read u, v; write u, v
+    "advdiff": 40,        # read u, v; write u, v and the RHS divergence (one kernel)
     "rhs_div": 24,        # read u, v; write rhs
     "pcorr": 40,          # read p, u, v; write u, v
     "fft_rows_fwd": 24,   # read rhs (8); write half spectrum (16)
@@ -76,8 +76,7 @@ ALGO_BYTES_PER_CELL = {
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
 # dense kernels on the swimmer workload, from one ncu capture of
-# `python bench.py --steps 4 --warmup 3 --no-cpu-baseline` (summarised in
-# profiles/fft_cols_swimmer_1024x512_fp64.md).  Writes stay in the 126 MB L2
+# `python bench.py --steps 4 --warmup 3 --no-cpu-baseline`.  Writes stay in the 126 MB L2
 # within a launch, so the captured figure is the reads.
 TRAFFIC_BYTES = {
     ("swimmer", "fft_cols"): 12672768,
@@ -338,6 +337,63 @@ def timed_steps(ctx, steps, flush, pg):
     return float(np.sum(step_ms)), ctx.kernel_launches() - launches0
 
 
+DENSE_KERNELS = ("fft_cols", "advdiff", "pcorr", "fft_rows_fwd", "fft_rows_inv", "rhs_div", "max_u")
+
+
+def dense_roofline(ctx, peak, peak_kind, workload, reps=30):
+    """Every dense kernel timed live (CUDA events around each launch on the
+    library's stream, the L2 flushed before every launch, so that inputs
+    come from HBM); the slowest one is the roofline's kernel."""
+    cells = ctx.nx * ctx.ny
+    kt = {k: ctx.time_kernel(k, reps, flush_l2=True) for k in DENSE_KERNELS}
+    dom = max(kt, key=kt.get)
+    achieved = ALGO_BYTES_PER_CELL[dom] * cells / (kt[dom] * 1e-3) / 1e9
+    per = {k: {"ms": round(v, 5), "GB/s": round(ALGO_BYTES_PER_CELL[k] * cells / (v * 1e-3) / 1e9, 1),
+               "frac": round(ALGO_BYTES_PER_CELL[k] * cells / (v * 1e-3) / 1e9 / peak, 4)}
+           for k, v in kt.items()}
+    return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+            "unit": "GB/s", "frac": achieved / peak, "traffic": TRAFFIC_BYTES.get((workload, dom)),
+            "algorithmic_bytes_per_launch": ALGO_BYTES_PER_CELL[dom] * cells,
+            "timing": "CUDA events around each launch, L2 flushed (256 MB write) before each",
+            "kernels": per}
+
+
+def cufft_comparison(ctx, flush, reps=20):
+    """The free-space solve's convolution done by cuFFT (through torch.fft,
+    a comparison only, never on the product path): a double-precision 2D
+    real-to-complex FFT of the zero-padded 2Ny x 2Nx RHS, times the real
+    kernel, and the complex-to-real inverse, timed with CUDA events with the
+    L2 flushed before each solve; beside the sum of this library's three
+    transform passes timed the same way."""
+    import torch
+    nx, ny = ctx.nx, ctx.ny
+    dev = flush.device
+    x = torch.zeros(2 * ny, 2 * nx, dtype=torch.float64, device=dev)
+    x[:ny, :nx] = torch.rand(ny, nx, dtype=torch.float64, device=dev)
+    g = torch.rand(2 * ny, nx + 1, dtype=torch.float64, device=dev)
+    for _ in range(3):
+        y = torch.fft.irfft2(torch.fft.rfft2(x) * g, s=x.shape)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    for _ in range(reps):
+        flush.fill_(1.0)
+        e0.record()
+        y = torch.fft.irfft2(torch.fft.rfft2(x) * g, s=x.shape)
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    del y
+    ours = sum(ctx.time_kernel(k, reps, flush_l2=True) for k in ("fft_rows_fwd", "fft_cols", "fft_rows_inv"))
+    cu = float(np.mean(ms))
+    return {"cufft_ms": round(cu, 5), "ours_ms": round(ours, 5), "ours_speedup": round(cu / ours, 3),
+            "transform": f"D2Z/Z2D {2 * ny}x{2 * nx} (zero-padded free-space convolution), FP64",
+            "note": "cuFFT via torch.fft, comparison only; ours = the three hand-written passes "
+                    "(fade, zero halves skipped, kernel multiply fused)"}
+
+
+LARGE_CASE = "tandem"
+
+
 def run_ours(args, world, rank, local, pg):
     import torch
     name, argline = WORKLOADS[args.workload]
@@ -397,13 +453,22 @@ def run_ours(args, world, rank, local, pg):
 
     # roofline of the dominant dense kernel, timed live with CUDA events
     peak, peak_kind = measured_peaks()
-    kt = {}
-    for kname in ("fft_cols", "advdiff", "pcorr", "fft_rows_fwd", "fft_rows_inv", "rhs_div", "max_u"):
-        kt[kname] = ctx.time_kernel(kname, 50)
-    dom = max(kt, key=kt.get)
-    achieved = ALGO_BYTES_PER_CELL[dom] * cells / (kt[dom] * 1e-3) / 1e9
-    traffic = TRAFFIC_BYTES.get((args.workload, dom))
+    roof = dense_roofline(ctx, peak, peak_kind, args.workload)
+    cufft = None if args.no_cufft else cufft_comparison(ctx, flush)
     ctx.sync()
+    # the same at the large case's size (4096x2048), where the working set
+    # exceeds the L2 by itself
+    roof_large = None
+    if not args.no_large and args.workload != LARGE_CASE:
+        lname, largs = WORKLOADS[LARGE_CASE]
+        big = make_sim(largs, local, rank)
+        big.ctx.advance(3)
+        big.ctx.sync()
+        roof_large = dense_roofline(big.ctx, peak, peak_kind, LARGE_CASE)
+        roof_large["workload"] = lname
+        if not args.no_cufft:
+            roof_large["cufft"] = cufft_comparison(big.ctx, flush)
+        del big
 
     line = None
     if rank == 0:
@@ -423,17 +488,16 @@ def run_ours(args, world, rank, local, pg):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": name, "cells": cells, "parallelism": f"replicas{world}",
+            "config": {"workload": name, "cells": cells},
+            "timing": {"parallelism": f"replicas{world}",
                        "l2": "flushed between timed steps (256 MB write)"},
             "clocks": clk.summary(),
             "e2e": {"value": e2e, "unit": "Gcell-steps/s", "h2d_bytes_per_step": 8,
                     "d2h_bytes_per_step": 8 + 42 * 8, "steps": ne},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic,
-                         "algorithmic_bytes_per_launch": ALGO_BYTES_PER_CELL[dom] * cells},
-            "kernel_ms": {k: round(v, 5) for k, v in kt.items()},
+            "roofline": roof,
+            "roofline_large": roof_large,
+            "poisson_vs_cufft": cufft,
             "fp32": fp32,
             "cpu_baseline": cpu,
         }
@@ -500,11 +564,8 @@ def run_ensemble(args, world, rank, local, pg):
     # roofline: the dominant dense kernel of the largest member
     peak, peak_kind = measured_peaks()
     big = sims[int(np.argmax(sizes))]
-    kt = {k: big.ctx.time_kernel(k, 50) for k in ("fft_cols", "advdiff", "pcorr", "fft_rows_fwd",
-                                                   "fft_rows_inv", "rhs_div", "max_u")}
-    dom = max(kt, key=kt.get)
-    bcells = big.ctx.nx * big.ctx.ny
-    achieved = ALGO_BYTES_PER_CELL[dom] * bcells / (kt[dom] * 1e-3) / 1e9
+    roof = dense_roofline(big.ctx, peak, peak_kind, "ensemble")
+    roof["member"] = f"{big.ctx.nx}x{big.ctx.ny}"
 
     line = None
     if rank == 0:
@@ -531,8 +592,8 @@ def run_ensemble(args, world, rank, local, pg):
             "config": {"workload": ENSEMBLE_NAME.format(args.members), "members": args.members,
                        "cells": cells, "grids": grids,
                        "shapes": {"disk": sum("disk" in a for a in cfgs),
-                                  "stefanfish": sum("stefanfish" in a for a in cfgs)},
-                       "parallelism": f"replicas{world}",
+                                  "stefanfish": sum("stefanfish" in a for a in cfgs)}},
+            "timing": {"parallelism": f"replicas{world}",
                        "l2": "not flushed: the members' fields (~2 GB at 64 members) exceed the L2"},
             "clocks": clk.summary(),
             "sequential": {"value": seq_value, "unit": "Gcell-steps/s", "ms_per_step": seq_ms / args.steps,
@@ -541,10 +602,7 @@ def run_ensemble(args, world, rank, local, pg):
             "e2e": {"value": e2e, "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": len(sims) * 42 * 8, "steps": ne},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": dom, "member": f"{big.ctx.nx}x{big.ctx.ny}",
-                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "algorithmic_bytes_per_launch": ALGO_BYTES_PER_CELL[dom] * bcells},
+            "roofline": roof,
             "fp32": fp32,
             "cpu_baseline": cpu,
         }
@@ -562,12 +620,14 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-Poisson measurement")
+    ap.add_argument("--no-large", action="store_true", help="skip the 4096x2048 kernel roofline")
+    ap.add_argument("--no-cufft", action="store_true", help="skip the cuFFT comparison")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     if args.impl == "reference":
-        # each step of the reference at 1024x512 takes ~1 s on 8 cores: bound the sample
+        # a step of the reference at 1024x512 takes ~0.1 s on 16 host cores:
+        # bound the sample to 20 timed steps (same warm-up as our arm)
         args.steps = min(args.steps, 20)
-        args.warmup = min(args.warmup, 3)
         line = run_reference(args, world, rank, pg)
     elif args.workload == "ensemble":
         line = run_ensemble(args, world, rank, local, pg)

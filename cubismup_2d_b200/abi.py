@@ -19,10 +19,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcup2d.so")
 
-OK, EINVAL, ECUDA, ENAN, EDOMAIN, ECAPACITY, ENOTSUP, ESTATE, ENOMEM, ETOOLARGE = range(10)
+OK, EINVAL, ECUDA, ENAN, EDOMAIN, ECAPACITY, ENOTSUP, ESTATE, ENOMEM, ETOOLARGE, ETIMEOUT = range(11)
 ERRORS = {EINVAL: "EINVAL", ECUDA: "ECUDA", ENAN: "ENAN", EDOMAIN: "EDOMAIN",
           ECAPACITY: "ECAPACITY", ENOTSUP: "ENOTSUP", ESTATE: "ESTATE", ENOMEM: "ENOMEM",
-          ETOOLARGE: "ETOOLARGE"}
+          ETOOLARGE: "ETOOLARGE", ETIMEOUT: "ETIMEOUT"}
 POISSON = {"freespace": 0, "periodic": 1, "": 2, "cosine": 2}
 PREC_FP64, PREC_FP32 = 0, 1
 FIELDS = {"u": 0, "v": 1, "chi": 2, "pres": 3, "tmp": 4, "udef_x": 5, "udef_y": 6, "sdf": 7}
@@ -44,7 +44,7 @@ EXPORTS = [
     "cup2d_adv_diff_noalloc",
 ]
 KERNELS = {"advdiff": 0, "rhs_div": 1, "pcorr": 2, "fft_rows_fwd": 3, "fft_cols": 4,
-           "fft_rows_inv": 5, "max_u": 6, "objects": 7}
+           "fft_rows_inv": 5, "max_u": 6, "objects": 7, "outflow": 8}
 
 
 class Config(ctypes.Structure):
@@ -116,7 +116,7 @@ def lib():
     L.cup2d_set_scalars.argtypes = [vp, d, d, i, d, d]
     L.cup2d_grid_size.argtypes = [vp, ip, ip, dp]
     L.cup2d_kernel_launches.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
-    L.cup2d_time_kernel.argtypes = [vp, i, i, dp]
+    L.cup2d_time_kernel.argtypes = [vp, i, i, i, dp]
     L.cup2d_advance_timed.argtypes = [vp, i, dp]
     L.cup2d_checkpoint_size.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
     L.cup2d_checkpoint_save.argtypes = [vp, vp, ctypes.c_size_t]
@@ -238,7 +238,7 @@ class Context:
         h = ctypes.c_void_p()
         rc = self.L.cup2d_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != OK:
-            raise Cup2DError(rc, "cup2d_create failed")
+            raise Cup2DError(rc, "cup2d_create: " + self.L.cup2d_last_error(None).decode())
         self.h_ = h
         self.cfg = cfg
         for kind, sp in shapes:
@@ -333,9 +333,11 @@ class Context:
         self._ck(self.L.cup2d_advance_timed(self.h_, nsteps, ctypes.byref(ms)))
         return ms.value
 
-    def time_kernel(self, name, reps):
+    def time_kernel(self, name, reps, flush_l2=True):
+        """Mean ms of one launch of a pipeline kernel (CUDA events around each
+        launch); with flush_l2 the L2 is flushed before every launch."""
         ms = ctypes.c_double()
-        self._ck(self.L.cup2d_time_kernel(self.h_, KERNELS[name], reps, ctypes.byref(ms)))
+        self._ck(self.L.cup2d_time_kernel(self.h_, KERNELS[name], reps, int(bool(flush_l2)), ctypes.byref(ms)))
         return ms.value
 
     def iteration_stats(self):

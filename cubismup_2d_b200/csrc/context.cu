@@ -5,6 +5,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -301,6 +302,18 @@ cudaError_t invalidate_dt_next(Ctx& c) {
 // placement mark no longer describe the state the next stage sees.
 void forget_chain(Ctx& c) { c.rhsFresh = false; c.placedPending = false; }
 
+// PutObjectsOnGrid.cpp:195 and 149-184: uDef cleared, then every shape's
+// deformation velocity added where its chi is the grid's, from the tiles of
+// the last placement (their udef is final once removeMoments has run).
+cudaError_t fill_udef_grid(Ctx& c) {
+  cudaError_t e = cudaMemsetAsync(c.udefx, 0, sizeof(double) * c.ncells(), c.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c.udefy, 0, sizeof(double) * c.ncells(), c.stream);
+  if (e != cudaSuccess) return e;
+  launch_obj_vel_on_grid(c);
+  c.udefStale = false;
+  return cudaGetLastError();
+}
+
 bool same_bits(double a, double b) { return std::memcmp(&a, &b, sizeof(double)) == 0; }
 
 extern "C" {
@@ -322,19 +335,29 @@ int cup2d_config_default(cup2d_config* cfg) {
   return CUP2D_OK;
 }
 
+namespace {
+thread_local std::string g_createErr;   // why this thread's last cup2d_create failed
+int create_fail(int code, const std::string& msg) { g_createErr = msg; return code; }
+}
+
 const char* cup2d_last_error(const cup2d_ctx* ctx) {
-  return ctx ? ctx->c.err.c_str() : "null context";
+  return ctx ? ctx->c.err.c_str() : g_createErr.c_str();
 }
 
 int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
-  if (!cfg || !out) return CUP2D_EINVAL;
+  if (!cfg || !out) return create_fail(CUP2D_EINVAL, "null argument");
   *out = nullptr;
-  if (cfg->bpdx <= 0 || cfg->bpdy <= 0) return CUP2D_EINVAL;
+  g_createErr.clear();
+  if (cfg->bpdx <= 0 || cfg->bpdy <= 0) return create_fail(CUP2D_EINVAL, "bpdx and bpdy must be positive");
   // CUP2D_PREC_FP32: the free-space and periodic Poisson transforms in FP32
   // (fields, stencils, obstacle sums and forces stay FP64); the cosine solver
   // has FP64 transforms only
-  if (cfg->precision != CUP2D_PREC_FP64 && cfg->precision != CUP2D_PREC_FP32) return CUP2D_ENOTSUP;
-  if (cfg->precision == CUP2D_PREC_FP32 && cfg->poisson == CUP2D_POISSON_COSINE) return CUP2D_ENOTSUP;
+  if (cfg->precision != CUP2D_PREC_FP64 && cfg->precision != CUP2D_PREC_FP32)
+    return create_fail(CUP2D_ENOTSUP, "unknown precision");
+  if (cfg->precision == CUP2D_PREC_FP32 && cfg->poisson == CUP2D_POISSON_COSINE)
+    return create_fail(CUP2D_ENOTSUP, "the cosine solver has FP64 transforms only");
+  if (!poisson_size_ok(cfg->poisson, 32 * cfg->bpdx, 32 * cfg->bpdy))
+    return create_fail(CUP2D_ENOTSUP, poisson_size_limits(cfg->poisson));
   cup2d_ctx* ctx = new (std::nothrow) cup2d_ctx();
   if (!ctx) return CUP2D_ENOMEM;
   Ctx& c = ctx->c;
@@ -375,6 +398,13 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
     rc = dalloc(ctx, &c.itmp[d], n);
     if (!rc) rc = dalloc(ctx, &c.ifluid[d], n);
   }
+  for (int b = 0; b < 2 && !rc; b++)
+    for (int d = 0; d < 2 && !rc; d++)
+      if (make_tmap_f64(&c.tmVel[b][d], c.vel[b][d], g.nx, g.ny, ADV_HT, ADV_HT) != cudaSuccess)
+        rc = fail(ctx, CUP2D_ECUDA, "TMA tensor maps of the velocity planes could not be made");
+  c.advTx = 2u * ADV_HT * ADV_HT * sizeof(double);
+  if (const char* inj = std::getenv("CUP2D_FAULT_TMA_WAIT"))      // fault injection (cup2d.h)
+    if (std::atoi(inj) != 0) c.advTx += 16;
   if (!rc) rc = dalloc(ctx, &c.dsc, 1);
   if (!rc) rc = dalloc(ctx, &c.dshapes, MAX_SHAPES);
   if (!rc) rc = dalloc(ctx, &c.counters, Ctx::NCOUNTERS);
@@ -402,7 +432,7 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
   if (rc) { cup2d_destroy(ctx); return rc; }
   if (cudaMemset(c.counters, 0, sizeof(unsigned) * Ctx::NCOUNTERS) != cudaSuccess) { cup2d_destroy(ctx); return CUP2D_ECUDA; }
   c.poisson = poisson_create(c);
-  if (!c.poisson) { cup2d_destroy(ctx); return CUP2D_ENOTSUP; }
+  if (!c.poisson) { cup2d_destroy(ctx); return create_fail(CUP2D_ENOMEM, "Poisson solver set-up failed"); }
   if (cudaStreamSynchronize(c.stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
     cup2d_destroy(ctx); return CUP2D_ECUDA;
   }
@@ -420,6 +450,7 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   cudaFree(c.udefx); cudaFree(c.udefy); cudaFree(c.dsc); cudaFree(c.dshapes);
   for (int d = 0; d < 2; d++) { cudaFree(c.itmp[d]); cudaFree(c.ifluid[d]); }
   cudaFree(c.counters); cudaFree(c.partials); cudaFree(c.fadeSlot);
+  if (c.flushBuf) cudaFree(c.flushBuf);
   if (c.side) cudaStreamDestroy(c.side);
   if (c.side2) cudaStreamDestroy(c.side2);
   if (c.evObj) cudaEventDestroy(c.evObj);
@@ -498,6 +529,12 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
   int nb1 = (int)std::ceil(span / (BS * h)) + 2;
   int cap = nb1 * nb1;
   if (cap > c.g.nblocks) cap = c.g.nblocks;
+  // fault injection on the host: a smaller tile capacity makes a body
+  // overflow it, which the tile search reports as CUP2D_ECAPACITY
+  if (const char* inj = std::getenv("CUP2D_FAULT_TILE_CAPACITY")) {
+    const int v = std::atoi(inj);
+    if (v > 0 && v < cap) cap = v;
+  }
   f.capacity = cap;
   S.rhoTile = kind == CUP2D_SHAPE_DISK ? f.rhoS : 1.0;
   ObstTiles t{};
@@ -612,6 +649,7 @@ int cup2d_init(cup2d_ctx* ctx) {
   c.devDt = 0.0;
   launch_objects(c, false);
   launch_obj_vel_on_grid(c);
+  c.udefStale = false;
   launch_apply_obj_vel(c);
   CK(cudaStreamSynchronize(c.stream));
   if ((rc = check_launch(ctx))) return rc;
@@ -703,9 +741,9 @@ int cup2d_put_objects(cup2d_ctx* ctx, double dt) {
   if (c.cfg.iterative) {
     // PutObjectsOnGrid.cpp:195, 237-238: the grid's deformation velocity,
     // which the iterated operator's RHS reads
-    CK(cudaMemsetAsync(c.udefx, 0, sizeof(double) * c.ncells(), c.stream));
-    CK(cudaMemsetAsync(c.udefy, 0, sizeof(double) * c.ncells(), c.stream));
-    launch_obj_vel_on_grid(c);
+    CK(fill_udef_grid(c));
+  } else {
+    c.udefStale = c.nshapes > 0;            // filled when read (cup2d_get_field)
   }
   // the next step's midlines on the side stream, beside the rest of this
   // step; the next call takes them if the time matches
@@ -803,6 +841,7 @@ int graph_steps_begin(cup2d_ctx* ctx) {
   forget_chain(c);
   c.shapesAtEvent = c.shapesMapped = false;
   c.stateSeq++;
+  c.udefStale = c.nshapes > 0;              // graph steps leave the grid's uDef
   if (c.cur != 0) {
     // a stage was called on its own: finish in eager mode until parity returns
     return fail(ctx, CUP2D_ESTATE, "velocity buffers out of step order");
@@ -868,9 +907,13 @@ int cup2d_sync(cup2d_ctx* ctx) {
   CK(cudaMemcpyAsync(&c.pin->status, &c.dsc->status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
   CK(cudaStreamSynchronize(c.stream));
   const int status = c.pin->status;
+  // each raised flag is reported once: a context whose state the caller
+  // repairs (cup2d_set_field, cup2d_set_shape, checkpoint load) runs on
+  if (status) CK(cudaMemsetAsync(&c.dsc->status, 0, sizeof(int), c.stream));
   if (status & ST_NAN) return fail(ctx, CUP2D_ENAN, "non-finite velocity detected");
   if (status & ST_DOMAIN) return fail(ctx, CUP2D_EDOMAIN, "body out of domain");
   if (status & ST_CAPACITY) return fail(ctx, CUP2D_ECAPACITY, "obstacle tiles exceed capacity");
+  if (status & ST_TIMEOUT) return fail(ctx, CUP2D_ETIMEOUT, "a kernel's bounded wait for its tile loads gave up");
   return CUP2D_OK;
 }
 
@@ -893,6 +936,7 @@ int cup2d_get_field(cup2d_ctx* ctx, int which, double* host_out) {
   Ctx& c = ctx->c;
   double* p = field_ptr(c, which);
   if (!p) return fail(ctx, CUP2D_EINVAL, "unknown field");
+  if ((which == CUP2D_FIELD_UDEF_X || which == CUP2D_FIELD_UDEF_Y) && c.udefStale) CK(fill_udef_grid(c));
   CK(cudaStreamSynchronize(c.stream));
   CK(cudaMemcpy(host_out, p, sizeof(double) * c.ncells(), cudaMemcpyDeviceToHost));
   return CUP2D_OK;
@@ -903,6 +947,8 @@ int cup2d_set_field(cup2d_ctx* ctx, int which, const double* host_in) {
   Ctx& c = ctx->c;
   double* p = field_ptr(c, which);
   if (!p) return fail(ctx, CUP2D_EINVAL, "unknown field");
+  // the other uDef component keeps the values a read would have given
+  if ((which == CUP2D_FIELD_UDEF_X || which == CUP2D_FIELD_UDEF_Y) && c.udefStale) CK(fill_udef_grid(c));
   CK(cudaStreamSynchronize(c.stream));
   CK(cudaMemcpy(p, host_in, sizeof(double) * c.ncells(), cudaMemcpyHostToDevice));
   forget_chain(c);
@@ -999,11 +1045,16 @@ int cup2d_kernel_launches(const cup2d_ctx* ctx, long long* count) {
   return CUP2D_OK;
 }
 
-int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, double* ms_per_launch) {
+int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, int flush_l2, double* ms_per_launch) {
   if (!ctx || !ms_per_launch || reps <= 0) return CUP2D_EINVAL;
   Ctx& c = ctx->c;
   if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
-  if (which < 0 || which > CUP2D_KERNEL_OBJECTS) return fail(ctx, CUP2D_EINVAL, "unknown kernel");
+  if (which < 0 || which > CUP2D_KERNEL_OUTFLOW) return fail(ctx, CUP2D_EINVAL, "unknown kernel");
+  constexpr size_t kFlushBytes = (size_t)256 << 20;
+  if (flush_l2 && !c.flushBuf && cudaMalloc(&c.flushBuf, kFlushBytes) != cudaSuccess) {
+    c.flushBuf = nullptr;
+    return fail(ctx, CUP2D_ENOMEM, "L2 flush buffer");
+  }
   CK(invalidate_dt_next(c));
   forget_chain(c);
   c.shapesAtEvent = c.shapesMapped = false;
@@ -1011,7 +1062,7 @@ int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, double* ms_per_launch
   c.devDt = NAN;
   auto one = [&]() {
     switch (which) {
-      case CUP2D_KERNEL_ADVDIFF: launch_advdiff(c); launch_advdiff_undo(c); break;
+      case CUP2D_KERNEL_ADVDIFF: launch_advdiff_rhs_div(c); launch_advdiff_undo(c); break;
       case CUP2D_KERNEL_RHS_DIV: launch_rhs_div(c); break;
       case CUP2D_KERNEL_PCORR: launch_pcorr(c); launch_pcorr_undo(c); break;
       case CUP2D_KERNEL_FFT_ROWS_FWD: poisson_rows_fwd(c); break;
@@ -1019,19 +1070,25 @@ int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, double* ms_per_launch
       case CUP2D_KERNEL_FFT_ROWS_INV: poisson_rows_inv(c); break;
       case CUP2D_KERNEL_MAX_U: launch_max_u_dt(c); break;
       case CUP2D_KERNEL_OBJECTS: launch_objects(c, false); break;
+      case CUP2D_KERNEL_OUTFLOW: launch_outflow_flux(c); break;
     }
   };
   one();   // warm
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0)); CK(cudaEventCreate(&e1));
-  CK(cudaEventRecord(e0, c.stream));
-  for (int r = 0; r < reps; r++) one();
-  CK(cudaEventRecord(e1, c.stream));
-  CK(cudaEventSynchronize(e1));
-  float ms = 0;
-  CK(cudaEventElapsedTime(&ms, e0, e1));
+  double total = 0;
+  for (int r = 0; r < reps; r++) {
+    if (flush_l2) CK(cudaMemsetAsync(c.flushBuf, r & 0xff, kFlushBytes, c.stream));
+    CK(cudaEventRecord(e0, c.stream));
+    one();
+    CK(cudaEventRecord(e1, c.stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    total += ms;
+  }
   cudaEventDestroy(e0); cudaEventDestroy(e1);
-  *ms_per_launch = (double)ms / reps;
+  *ms_per_launch = total / reps;
   return check_launch(ctx);
 }
 
@@ -1244,6 +1301,7 @@ int cup2d_ensemble_get_shapes(cup2d_ensemble* ens, cup2d_shape_state* out, int c
   int total = 0;
   for (int i = 0; i < n; i++) total += ens->m[i]->c.nshapes;
   *count = total;
+  if (!out && capacity == 0) return CUP2D_OK;         // size query
   if (!out || capacity < total) return ens_fail(ens, CUP2D_EINVAL, "shape buffer too small");
   if (ens->advanced) CKE(cudaEventSynchronize(ens->evEnd));
   int o = 0;
@@ -1445,6 +1503,7 @@ int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes) {
   forget_chain(c);
   c.sideMidPending = false;
   c.midByGraph = false;
+  c.udefStale = c.nshapes > 0;              // refilled from the restored tiles when read
   return CUP2D_OK;
 }
 

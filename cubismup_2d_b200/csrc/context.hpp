@@ -5,6 +5,7 @@
 #include <vector>
 #include "internal.cuh"
 #include "launch.hpp"
+#include "tma.cuh"
 
 namespace cup2d {
 
@@ -19,6 +20,11 @@ struct Ctx {
   // dense fields (fp64 planes, Ny x Nx)
   double* vel[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [buffer][component]
   int cur = 0;                  // buffer holding the current velocity
+  // TMA maps of the velocity planes, boxes of the 32x32 block plus a
+  // two-cell halo (advDiff's staged tiles); advTx: the bytes advDiff's tile
+  // barrier expects (its two boxes, unless fault injection adds to it)
+  CUtensorMap tmVel[2][2];
+  unsigned advTx = 0;
   double* chi = nullptr;        // SimulationData::chi
   double* pres = nullptr;       // SimulationData::pres
   double* rhs = nullptr;        // SimulationData::tmp as used by PressureSingle
@@ -80,8 +86,13 @@ struct Ctx {
   //                PutObjectsOnGrid and nothing was enqueued after its chain
   //   shapesAtEvent the shape states are final at evShapes (recorded at a
   //                step end, before kernels that only read them)
+  //   udefStale    the grid's deformation velocity (uDef) is not filled for
+  //                the tiles of the last PutObjectsOnGrid: PressureSingle
+  //                never reads it, so plain and graph steps leave it and
+  //                cup2d_get_field fills it from the tiles on demand
   double devDt = 0.0;
   bool dtValidMaybe = false, dtCarried = false, rhsFresh = false, placedPending = false;
+  bool udefStale = false;
   bool shapesAtEvent = false;
   cudaEvent_t evDtNext = nullptr, evShapes = nullptr;
   // pinned host staging of the small read-backs (one copy + one wait each)
@@ -103,6 +114,7 @@ struct Ctx {
   unsigned long long stateSeq = 0;
 
   cudaGraphExec_t graph = nullptr;
+  void* flushBuf = nullptr;      // cup2d_time_kernel's L2 flush (256 MB, allocated on demand)
   unsigned graphGen = 0;        // bumped whenever what a step captures changes
   long long launches = 0;
   int launchesInGraph = 0;

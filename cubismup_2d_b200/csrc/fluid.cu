@@ -3,9 +3,10 @@
 // the pressure correction, IC and ApplyObjVel.
 //
 // Every kernel maps one CTA to one 32x32 reference block (blockDim 32x8,
-// 4 rows per thread): a warp reads one 256-byte fp64 row segment, the
-// 5-point halo comes from L1/L2 (neighbour rows are read by the CTA itself,
-// neighbour columns by the adjacent CTA), so DRAM sees each plane once.
+// 4 rows per thread): a warp reads one 256-byte fp64 row segment.  advDiff
+// stages its tile with a two-cell halo by TMA; the others take the 5-point
+// halo from L1/L2 (neighbour rows are read by the CTA itself, neighbour
+// columns by the adjacent CTA), so DRAM sees each plane once.
 // Arithmetic is written in the reference's operation order and the library
 // is compiled without FMA contraction, so a stage fed the same inputs as the
 // reference reproduces it bit for bit (reductions excepted: their order
@@ -13,6 +14,7 @@
 #include <cmath>
 #include "context.hpp"
 #include "step_begin.cuh"
+#include "tma.cuh"
 
 namespace cup2d {
 
@@ -173,83 +175,125 @@ k_outflow_flux(GridDesc g, const Scalars* sc, const double* __restrict__ u, cons
     scw->outflowCorr = t1[0] / (2 * (BS * g.bpdy - 0) + 2 * (BS * g.bpdx - 0));
 }
 
-// advDiff.cpp:57-116: the update with the outflow correction of
-// k_outflow_flux applied to the boundary cells (u on the west / east
-// columns, v on the south / north rows).  With DIV, the divergence RHS of
-// PressureSingle.cpp:112-128 and the block's fade sums follow in place: the
-// CTA keeps its new u with one halo column each side and its new v with one
-// halo row each side in shared memory, the halo cells updated here too (they
-// are never on the boundary column or row whose correction they would need;
-// at the domain edge the zero-gradient ghost is the cell itself).
-template <bool DIV>
+// adv_cell on the staged tile: U, V hold the block's cells and a two-cell
+// halo (tile position (lx + 2, ly + 2) for block cell (lx, ly)); the domain
+// edge tests use the global cell (gx, gy), as adv_cell does
+__device__ __forceinline__ void adv_cell_tile(const GridDesc& g, const AdvCoef& k, const double* U,
+                                              const double* V, int lx, int ly, int gx, int gy,
+                                              double& unew, double& vnew) {
+  const int t = (ly + 2) * ADV_HT + lx + 2;
+  const double ucc = U[t], vcc = V[t];
+  double ulx, vlx, upx, vpx, uly, vly, upy, vpy;
+  if (gx > 0) { ulx = U[t - 1]; vlx = V[t - 1]; } else { ulx = ucc * k.fadeW; vlx = vcc * k.fadeW; }
+  if (gx < g.nx - 1) { upx = U[t + 1]; vpx = V[t + 1]; } else { upx = ucc * k.fadeE; vpx = vcc * k.fadeE; }
+  if (gy > 0) { uly = U[t - ADV_HT]; vly = V[t - ADV_HT]; } else { uly = ucc * k.fadeS; vly = vcc * k.fadeS; }
+  if (gy < g.ny - 1) { upy = U[t + ADV_HT]; vpy = V[t + ADV_HT]; } else { upy = ucc * k.fadeN; vpy = vcc * k.fadeN; }
+  const double dUadv = (ucc + k.U0) * (upx - ulx) + (vcc + k.U1) * (upy - uly);
+  const double dUdif = upx + upy + ulx + uly - 4 * ucc;
+  const double dVadv = (ucc + k.U0) * (vpx - vlx) + (vcc + k.U1) * (vpy - vly);
+  const double dVdif = vpx + vpy + vlx + vly - 4 * vcc;
+  unew = ucc + (k.afac * dUadv + k.dfac * dUdif);
+  vnew = vcc + (k.afac * dVadv + k.dfac * dVdif);
+}
+
+// advDiff.cpp:57-116 with PressureSingle.cpp:112-128 in place, one CTA per
+// 32x32 block: one thread loads the block's u and v with a two-cell halo by
+// TMA (the halo beyond the domain reads as zero and is never used: edge
+// cells take the reference's ghosts instead), the CTA forms the new
+// velocity with the outflow correction of k_outflow_flux on the boundary
+// cells (u on the west / east columns, v on the south / north rows), keeps
+// it in shared memory with the new u one column and the new v one row
+// beyond the block (formed here too: they are never on the boundary
+// column or row whose correction they would need; at the domain edge the
+// zero-gradient ghost is the cell itself), and writes the divergence RHS
+// and the strip blocks' fade sums.  Thread (tx, ty) of 32 x 8 takes rows
+// ty + 8 r, the order of every producer of the fade sums.  The tile
+// barrier's wait is bounded: a load that never lands raises ST_TIMEOUT.
 __global__ void __launch_bounds__(256, 4)
-k_advdiff(GridDesc g, const Scalars* sc,
-          const double* __restrict__ u, const double* __restrict__ v,
+k_advdiff(const __grid_constant__ CUtensorMap tmU, const __grid_constant__ CUtensorMap tmV,
+          GridDesc g, Scalars* sc, unsigned txBytes,
           double* __restrict__ un, double* __restrict__ vn,
           double* __restrict__ rhs, const int* __restrict__ fadeSlot, double* __restrict__ fadePartials)
 {
+  __shared__ __align__(128) double tU[ADV_HT * ADV_HT];
+  __shared__ __align__(128) double tV[ADV_HT * ADV_HT];
+  __shared__ __align__(8) unsigned long long bar;
+  __shared__ double su[BS][BS + 2];
+  __shared__ double sv[BS + 2][BS];
+  const int tid = lin_tid();
+  if (tid == 0) mbar_init(&bar, 1);
+  __syncthreads();
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_ADVDIFF);
-  __shared__ double su[DIV ? BS : 1][BS + 2];
-  __shared__ double sv[DIV ? BS + 2 : 1][BS];
-  const AdvCoef kc = adv_coef(g, sc);
-  const double corr = sc->outflowCorr;
-  const int nx = g.nx, ny = g.ny;
   const int bx = blockIdx.x, by = blockIdx.y, tx = threadIdx.x, ty = threadIdx.y;
+  if (tid == 0) {
+    mbar_arrive_expect_tx(&bar, txBytes);
+    tma_load_2d(tU, &tmU, bx * BS - 2, by * BS - 2, &bar);
+    tma_load_2d(tV, &tmV, bx * BS - 2, by * BS - 2, &bar);
+  }
+  const AdvCoef kc = adv_coef(g, sc);          // while the tiles are in flight
+  const double corr = sc->outflowCorr;
+  const double facDiv = 0.5 * g.h / sc->dt;
+  const int nx = g.nx, ny = g.ny;
   const int gx = bx * BS + tx;
+  const bool landed = mbar_wait_bounded(&bar, 0, TMA_WAIT_NS);
+  if (__syncthreads_or(!landed)) {
+    // the loads did not land: report, give them the same time again, leave
+    // (the whole CTA takes this branch)
+    if (tid == 0) atomicOr(&sc->status, ST_TIMEOUT);
+    mbar_wait_bounded(&bar, 0, TMA_WAIT_NS);
+    return;
+  }
 #pragma unroll
   for (int r = 0; r < 4; r++) {
     const int iy = ty + 8 * r, gy = by * BS + iy;
     double unew, vnew;
-    adv_cell(g, kc, u, v, gx, gy, unew, vnew);
+    adv_cell_tile(g, kc, tU, tV, tx, iy, gx, gy, unew, vnew);
     if (gx == 0) unew = unew + corr;                     // advDiff.cpp:107-115
     if (gx == nx - 1) unew = unew - corr;
     if (gy == 0) vnew = vnew + corr;
     if (gy == ny - 1) vnew = vnew - corr;
     const size_t c = (size_t)gy * nx + gx;
     un[c] = unew; vn[c] = vnew;
-    if (DIV) { su[iy][tx + 1] = unew; sv[iy + 1][tx] = vnew; }
+    su[iy][tx + 1] = unew; sv[iy + 1][tx] = vnew;
   }
-  if constexpr (DIV) {
-    // halo: warps 0-3, one lane per cell (u west / east column, v south /
-    // north row of the neighbouring blocks)
-    if (ty < 4) {
-      const int side = ty;
+  // halo: warps 0-3, one lane per cell (u west / east column, v south /
+  // north row of the neighbouring blocks)
+  if (ty < 4) {
+    const int side = ty;
+    const bool have = side == 0 ? bx > 0 : side == 1 ? bx < g.bpdx - 1 : side == 2 ? by > 0 : by < g.bpdy - 1;
+    if (have) {
+      const int lx = side == 0 ? -1 : side == 1 ? BS : tx;
+      const int ly = side == 2 ? -1 : side == 3 ? BS : tx;
       double unew, vnew;
-      const bool have = side == 0 ? bx > 0 : side == 1 ? bx < g.bpdx - 1 : side == 2 ? by > 0 : by < g.bpdy - 1;
-      if (have) {
-        const int hx = side == 0 ? bx * BS - 1 : side == 1 ? bx * BS + BS : bx * BS + tx;
-        const int hy = side == 2 ? by * BS - 1 : side == 3 ? by * BS + BS : by * BS + tx;
-        adv_cell(g, kc, u, v, hx, hy, unew, vnew);
-        if (side == 0) su[tx][0] = unew;
-        else if (side == 1) su[tx][BS + 1] = unew;
-        else if (side == 2) sv[0][tx] = vnew;
-        else sv[BS + 1][tx] = vnew;
-      }
+      adv_cell_tile(g, kc, tU, tV, lx, ly, bx * BS + lx, by * BS + ly, unew, vnew);
+      if (side == 0) su[tx][0] = unew;
+      else if (side == 1) su[tx][BS + 1] = unew;
+      else if (side == 2) sv[0][tx] = vnew;
+      else sv[BS + 1][tx] = vnew;
     }
-    __syncthreads();
-    const double facDiv = 0.5 * g.h / sc->dt;
-    const bool touch = fade_touch(g, bx, by);
-    double s[3] = {0, 0, 0};
+  }
+  __syncthreads();
+  const bool touch = fade_touch(g, bx, by);
+  double s[3] = {0, 0, 0};
 #pragma unroll
-    for (int r = 0; r < 4; r++) {
-      const int iy = ty + 8 * r, gy = by * BS + iy;
-      const double uW = gx > 0 ? su[iy][tx] : su[iy][tx + 1];
-      const double uE = gx < nx - 1 ? su[iy][tx + 2] : su[iy][tx + 1];
-      const double vS = gy > 0 ? sv[iy][tx] : sv[iy + 1][tx];
-      const double vN = gy < ny - 1 ? sv[iy + 2][tx] : sv[iy + 1][tx];
-      const double divVx = uE - uW, divVy = vN - vS;
-      const double b = facDiv * (divVx + divVy);
-      rhs[(size_t)gy * nx + gx] = b;
-      if (touch) fade_accumulate(g, bx, by, tx, iy, b, s);
-    }
-    if (touch) {                                         // uniform over the CTA
-      __shared__ double red[96];
-      block_sum<3>(s, red);
-      if (lin_tid() == 0) {
-        const int q = fadeSlot[bx + g.bpdx * by];
-        for (int k = 0; k < 3; k++) fadePartials[3 * q + k] = s[k];
-      }
+  for (int r = 0; r < 4; r++) {
+    const int iy = ty + 8 * r, gy = by * BS + iy;
+    const double uW = gx > 0 ? su[iy][tx] : su[iy][tx + 1];
+    const double uE = gx < nx - 1 ? su[iy][tx + 2] : su[iy][tx + 1];
+    const double vS = gy > 0 ? sv[iy][tx] : sv[iy + 1][tx];
+    const double vN = gy < ny - 1 ? sv[iy + 2][tx] : sv[iy + 1][tx];
+    const double divVx = uE - uW, divVy = vN - vS;
+    const double b = facDiv * (divVx + divVy);
+    rhs[(size_t)gy * nx + gx] = b;
+    if (touch) fade_accumulate(g, bx, by, tx, iy, b, s);
+  }
+  if (touch) {                                         // uniform over the CTA
+    __shared__ double red[96];
+    block_sum<3>(s, red);
+    if (tid == 0) {
+      const int q = fadeSlot[bx + g.bpdx * by];
+      for (int k = 0; k < 3; k++) fadePartials[3 * q + k] = s[k];
     }
   }
 }
@@ -468,23 +512,10 @@ void launch_outflow_flux(Ctx& c) {
   CUP2D_LAUNCHED(c);
 }
 
-void launch_advdiff_update(Ctx& c) {
-  dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
-  launch_k(k_advdiff<false>, grid, block, 0, c.stream, c.g, (const Scalars*)c.dsc, (const double*)c.u(),
-           (const double*)c.v(), c.uo(), c.vo(), (double*)nullptr, (const int*)nullptr, (double*)nullptr);
-  CUP2D_LAUNCHED(c);
-  c.cur = 1 - c.cur;   // advDiff.cpp:81-87: the new field becomes the velocity
-}
-
-void launch_advdiff(Ctx& c) {
-  launch_outflow_flux(c);
-  launch_advdiff_update(c);
-}
-
 void launch_advdiff_rhs_div(Ctx& c) {
   dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
-  launch_k(k_advdiff<true>, grid, block, 0, c.stream, c.g, (const Scalars*)c.dsc, (const double*)c.u(),
-           (const double*)c.v(), c.uo(), c.vo(), c.rhs, (const int*)c.fadeSlot, fade_partials(c));
+  launch_k(k_advdiff, grid, block, 0, c.stream, c.tmVel[c.cur][0], c.tmVel[c.cur][1], c.g, c.dsc, c.advTx,
+           c.uo(), c.vo(), c.rhs, (const int*)c.fadeSlot, fade_partials(c));
   CUP2D_LAUNCHED(c);
   c.cur = 1 - c.cur;
 }
@@ -492,12 +523,6 @@ void launch_advdiff_rhs_div(Ctx& c) {
 // timing helpers: return the velocity to the buffer it came from (no launch)
 void launch_advdiff_undo(Ctx& c) { c.cur = 1 - c.cur; }
 void launch_pcorr_undo(Ctx& c) { c.cur = 1 - c.cur; }
-
-void launch_outflow(Ctx& c) {
-  // formed by k_outflow_flux before the update, applied by k_advdiff
-  // (advDiff.cpp:89-116)
-  (void)c;
-}
 
 void launch_rhs_div(Ctx& c) {
   dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);

@@ -27,7 +27,7 @@ constexpr int MAX_SHAPES = 8;
 constexpr int NFORCE = 17;        // additive sums of ObstacleBlock.h:33-36
 
 // Device status flags (bit set = raised); cup2d_sync reports the first.
-enum : int { ST_NAN = 1, ST_DOMAIN = 2, ST_CAPACITY = 4 };
+enum : int { ST_NAN = 1, ST_DOMAIN = 2, ST_CAPACITY = 4, ST_TIMEOUT = 8 };
 
 struct GridDesc {
   int nx, ny, bpdx, bpdy, nblocks;

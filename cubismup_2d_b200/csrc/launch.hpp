@@ -24,13 +24,10 @@ inline cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, siz
 // fluid.cu
 void launch_max_u_dt(Ctx& c);                        // Helpers.cpp:136-176 + Simulation.cpp:254-277
 void launch_set_dt(Ctx& c, double dt);               // Operator::operator()(dt) argument
-void launch_advdiff(Ctx& c);                         // advDiff.cpp:36-87
 void launch_outflow_flux(Ctx& c);                     // advDiff.cpp:89-106, before the update
-void launch_advdiff_update(Ctx& c);                   // advDiff.cpp:14-116 with the flux's correction
 void launch_advdiff_rhs_div(Ctx& c);                  // the update, then PressureSingle.cpp:112-128 in place
 void launch_advdiff_undo(Ctx& c);
 void launch_pcorr_undo(Ctx& c);
-void launch_outflow(Ctx& c);                         // advDiff.cpp:89-116
 void launch_rhs_div(Ctx& c);                         // PressureSingle.cpp:112-128
 void launch_rhs_iter(Ctx& c);                        // PressureIterator_unif.cpp:22-49
 void launch_pcorr_from(Ctx& c, const double* ui, const double* vi, double* uo, double* vo);
@@ -64,6 +61,10 @@ void launch_forces(Ctx& c, cup2d_shape_state* out = nullptr);
 // poisson.cu
 struct Poisson;
 Poisson* poisson_create(Ctx& c);
+// whether the chosen solver's transforms exist for an nx x ny grid, and the
+// limits in words (for the error message)
+bool poisson_size_ok(int type, int nx, int ny);
+const char* poisson_size_limits(int type);
 void poisson_destroy(Poisson* p);
 void poisson_solve(Ctx& c);                          // PoissonSolver::solve of the chosen solver
 void poisson_rows_fwd(Ctx& c);

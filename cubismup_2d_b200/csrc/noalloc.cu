@@ -92,7 +92,7 @@ k_advdiff_noalloc(Args a, const double* __restrict__ u, const double* __restrict
   if (!last_block_done(reinterpret_cast<unsigned*>(scratch), nb)) return;
   const int tid = lin_tid();
   double t[1] = {0.0};
-  for (unsigned i = tid; i < nb; i += 256) t[0] += partials[i];
+  for (unsigned i = tid; i < nb; i += 256) t[0] += __ldcg(&partials[i]);
   block_sum<1>(t, red);
   if (tid == 0) scratch[1] = t[0] / (2 * (BS * a.bpdy - 0) + 2 * (BS * a.bpdx - 0));   // advDiff.cpp:105
 }

@@ -42,6 +42,7 @@ struct Poisson {
   float2* tw32 = nullptr;    // tw rounded to FP32
   float* ghat32 = nullptr;   // ghat rounded to FP32
   int rb = 1, cb = 1;        // rows / columns per CTA
+  int MX = 0, MY = 0;        // free space: the padded grid (powers of two >= 2Nx, 2Ny)
 };
 
 namespace {
@@ -391,14 +392,14 @@ __device__ __forceinline__ double fade_cell(const GridDesc& g, int gx, int gy, d
   return __dadd_rn(__dmul_rn(b, 1 - f2), fadeCorrection);   // never contracted into an FMA
 }
 
-// inMode 0: rows of `in`; 1: the free-space Green's function on the padded
-// grid (FFTW_freespace.cpp:108-119) computed on the fly.  Each row of 2L
+// inMode 0: rows of `in`; 1: the free-space Green's function on the MY x MX
+// padded grid (FFTW_freespace.cpp:108-119) computed on the fly.  Each row of 2L
 // reals is the complex sequence (x[2n], x[2n+1]) of length L.
 template <int L, bool HIN>
 __global__ void __launch_bounds__(Len<L, E_ROWS>::NT, Len<L, E_ROWS>::MINB)
 k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
            double2* __restrict__ out, int outStride,
-           const double2* __restrict__ tw, int twLen, FadeArgs fa, double h, int Nx, int Ny)
+           const double2* __restrict__ tw, int twLen, FadeArgs fa, double h, int MX, int MY)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_R2C);
@@ -415,7 +416,7 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
       double2* dst = A + r * SL + pad(n);
       if (2 * n + 1 < ncolsIn) cp_async16(dst, in + (size_t)row * inStride + 2 * n);
       else if (2 * n < ncolsIn) *dst = make_double2(in[(size_t)row * inStride + 2 * n], 0);
-      else if (!HIN) *dst = make_double2(0, 0);       // with HIN the zero half is never read
+      else if (!HIN || n < L / 2) *dst = make_double2(0, 0);   // with HIN the upper half is never read
     }
     cp_async_commit();
   } else {
@@ -427,13 +428,14 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
         const int col = 2 * n + q;
         double val = 0;
         if (col < ncolsIn) {
-          const int MX = 2 * Nx, MY = 2 * Ny;
+          // wrapped offsets: index i stands for offset i below M/2 and for
+          // i - M from M/2 on (offsets beyond N - 1 never reach the domain)
           const double fac = 1 / (2 * M_PI);
           if (row == 0 && col == 0) {
             val = fac / 2 * (2 * log(h / sqrt(M_PI)) - 1);
           } else {
-            const double yi = row >= Ny ? MY - row : row;
-            const double xi = col >= Nx ? MX - col : col;
+            const double yi = row >= MY / 2 ? MY - row : row;
+            const double xi = col >= MX / 2 ? MX - col : col;
             const double rr = sqrt(xi * xi + yi * yi);
             val = fac * log(h * rr);
           }
@@ -519,11 +521,12 @@ k_cols(double2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrows
     }
   }
   cp_async_commit();
-  if (!FS)                                            // the free-space solve never reads them
-    for (int idx = threadIdx.x; idx < CB * (L - nrowsIn); idx += NT) {
-      const int r = nrowsIn + idx / CB, j = idx & (CB - 1);
-      A[j * SL + pad(r)] = make_double2(0, 0);
-    }
+  // rows beyond the input are zero; the free-space solve never reads its
+  // upper half
+  for (int idx = threadIdx.x; idx < CB * ((FS ? L / 2 : L) - nrowsIn); idx += NT) {
+    const int r = nrowsIn + idx / CB, j = idx & (CB - 1);
+    A[j * SL + pad(r)] = make_double2(0, 0);
+  }
   load_twiddles<L>(tws, tw, twLen);
   if (mode == 1) {
     cp_async_wait<0>();
@@ -664,7 +667,7 @@ k_rows_r2c32(const double* __restrict__ in, int inStride, int nrows, int ncolsIn
     const int idx = threadIdx.x + u * NT;
     const int r = idx / L, n = idx & (L - 1), row = row0 + r;
     if (idx >= RB * L || r >= nb) continue;
-    if (HIN && 2 * n >= ncolsIn) continue;             // the zero half is never read
+    if (HIN && n >= L / 2) continue;                   // the zero upper half is never read
     if (fa.enabled && 2 * n + 1 < ncolsIn) {
       // fade band as in k_rows_r2c (cub2rhs, PoissonSolver.cpp:61-141)
       const bool rowBand = row < bandY || row >= fa.g.ny - bandY;
@@ -721,11 +724,12 @@ k_cols32(float2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrow
       if (j < nb) cp_async4(Gs + r * CB + j, ghat + (size_t)r * stride + c0 + j);
     }
   cp_async_commit();
-  if (!FS)
-    for (int idx = threadIdx.x; idx < CB * (L - nrowsIn); idx += NT) {
-      const int r = nrowsIn + idx / CB, j = idx & (CB - 1);
-      A[j * SL + pad(r)] = make_float2(0, 0);
-    }
+  // rows beyond the input are zero; the free-space solve never reads its
+  // upper half
+  for (int idx = threadIdx.x; idx < CB * ((FS ? L / 2 : L) - nrowsIn); idx += NT) {
+    const int r = nrowsIn + idx / CB, j = idx & (CB - 1);
+    A[j * SL + pad(r)] = make_float2(0, 0);
+  }
   load_twiddles<L>(tws, tw, twLen);
   cp_async_wait<0>();
   __syncthreads();
@@ -1016,14 +1020,14 @@ void set_all_smem() {
 }
 
 bool rows_r2c(int L, cudaStream_t st, const double* in, int inStride, int nrows, int ncolsIn, int inMode,
-              double2* out, int outStride, const double2* tw, int twLen, FadeArgs fa, double h, int Nx, int Ny,
+              double2* out, int outStride, const double2* tw, int twLen, FadeArgs fa, double h, int MX, int MY,
               bool halfIn) {
   switch (L) {
 #define X(LL) case LL: \
     if (halfIn) launch_k(k_rows_r2c<LL, true>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_ROWS>::NT, smem_for<LL>(), st,  \
-        in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, Nx, Ny); \
+        in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, MX, MY); \
     else launch_k(k_rows_r2c<LL, false>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_ROWS>::NT, smem_for<LL>(), st,  \
-        in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, Nx, Ny); \
+        in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, MX, MY); \
     return true;
     CUP2D_FFT_LENGTHS(X)
 #undef X
@@ -1146,13 +1150,46 @@ bool dct_rows_inv(int L, cudaStream_t st, const double* D, int Nx, int nrows, do
 
 } // namespace
 
+namespace {
+inline int pow2_at_least(int n) { int p = 1; while (p < n) p <<= 1; return p; }
+}
+
+// The transforms are radix-16 Stockham FFTs of power-of-two lengths 16 ..
+// 4096 held in shared memory.  Free space pads to powers of two, so any
+// grid with Nx <= 4096 and Ny <= 2048 works; the periodic and cosine
+// solvers transform the grid's own lengths, which must be powers of two.
+bool poisson_size_ok(int type, int nx, int ny) {
+  if (type == CUP2D_POISSON_FREESPACE) {
+    const int lrow = pow2_at_least(2 * nx) / 2, lcol = pow2_at_least(2 * ny);
+    return lrow >= 16 && lcol >= 16 && lrow <= 4096 && lcol <= 4096;
+  }
+  if (!is_pow2(nx) || !is_pow2(ny)) return false;
+  const int lrow = type == CUP2D_POISSON_PERIODIC ? nx / 2 : nx;
+  const int lcol = type == CUP2D_POISSON_PERIODIC ? ny : 2 * ny;
+  return lrow >= 16 && lcol >= 16 && lrow <= 4096 && lcol <= 4096;
+}
+
+const char* poisson_size_limits(int type) {
+  if (type == CUP2D_POISSON_FREESPACE)
+    return "grid beyond the free-space solver's transforms: Nx = 32 bpdx <= 4096 and Ny = 32 bpdy <= 2048";
+  if (type == CUP2D_POISSON_PERIODIC)
+    return "grid beyond the periodic solver's transforms: Nx and Ny powers of two, Nx <= 8192, Ny <= 4096";
+  return "grid beyond the cosine solver's transforms: Nx and Ny powers of two, Nx <= 4096, Ny <= 2048";
+}
+
 Poisson* poisson_create(Ctx& c) {
   Poisson* P = new Poisson();
   P->type = c.cfg.poisson;
   const int Nx = c.g.nx, Ny = c.g.ny;
   if (P->type == CUP2D_POISSON_FREESPACE) {
-    P->Lrow = Nx;          // real length 2Nx
-    P->Lcol = 2 * Ny;
+    // the padded grid: any size >= 2N - 1 gives the same linear convolution
+    // on the domain (FFTW_freespace.cpp pads to 2N - 1); powers of two >= 2N
+    // keep every transform a radix-16 Stockham FFT in shared memory
+    P->MX = 2 * Nx; P->MY = 2 * Ny;
+    while (!is_pow2(P->MX)) P->MX++;
+    while (!is_pow2(P->MY)) P->MY++;
+    P->Lrow = P->MX / 2;   // real length MX
+    P->Lcol = P->MY;
   } else if (P->type == CUP2D_POISSON_PERIODIC) {
     P->Lrow = Nx / 2;      // real length Nx
     P->Lcol = Ny;
@@ -1186,14 +1223,14 @@ Poisson* poisson_create(Ctx& c) {
     cudaMemcpy(P->cosY, cy.data(), sizeof(float) * Ny, cudaMemcpyHostToDevice);
   }
   if (P->type == CUP2D_POISSON_FREESPACE) {
-    // G^ = Re FFT[G] / (MX MY) on the (2Ny) x (2Nx) grid, kept for ky <= Ny
+    // G^ = Re FFT[G] / (MX MY) on the MY x MX padded grid, kept for ky <= MY/2
     if (cudaMalloc(&P->ghat, sizeof(double) * (P->Lcol / 2 + 1) * P->nkx) != cudaSuccess) { poisson_destroy(P); return nullptr; }
     FadeArgs fa{}; fa.enabled = 0;
-    const int MYr = 2 * Ny;
-    rows_r2c(P->Lrow, c.stream, nullptr, 0, MYr, 2 * Nx, 1, P->spec, P->nkx, P->tw, P->twLen, fa, c.g.h, Nx, Ny, false);
+    rows_r2c(P->Lrow, c.stream, nullptr, 0, P->MY, P->MX, 1, P->spec, P->nkx, P->tw, P->twLen, fa, c.g.h,
+             P->MX, P->MY, false);
     CUP2D_LAUNCHED(c);
-    const double norm = 1.0 / ((double)(2 * Nx) * (double)(2 * Ny));
-    cols(P->Lcol, c.stream, P->spec, P->nkx, P->nkx, MYr, P->Lcol / 2 + 1, P->ghat, 1, P->tw, P->twLen, norm, 0, 0);
+    const double norm = 1.0 / ((double)P->MX * (double)P->MY);
+    cols(P->Lcol, c.stream, P->spec, P->nkx, P->nkx, P->MY, P->Lcol / 2 + 1, P->ghat, 1, P->tw, P->twLen, norm, 0, 0);
     CUP2D_LAUNCHED(c);
   }
   if (c.cfg.precision == CUP2D_PREC_FP32) {
@@ -1241,7 +1278,7 @@ void poisson_rows_fwd(Ctx& c) {
     rows_r2c32(P->Lrow, c.stream, c.rhs, Nx, Ny, Nx, reinterpret_cast<float2*>(P->spec), P->nkx, P->tw32,
                P->twLen, fa, P->type == CUP2D_POISSON_FREESPACE);
   else
-    rows_r2c(P->Lrow, c.stream, c.rhs, Nx, Ny, Nx, 0, P->spec, P->nkx, P->tw, P->twLen, fa, c.g.h, Nx, Ny,
+    rows_r2c(P->Lrow, c.stream, c.rhs, Nx, Ny, Nx, 0, P->spec, P->nkx, P->tw, P->twLen, fa, c.g.h, P->MX, P->MY,
              P->type == CUP2D_POISSON_FREESPACE);
   CUP2D_LAUNCHED(c);
 }

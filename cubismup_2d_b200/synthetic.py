@@ -37,10 +37,9 @@ SWIMMER_1024x512 = (
     "-bpdx 32 -bpdy 16 -extent 1 -CFL 0.1 -nu 2e-5 -lambda 1e4 -poissonType freespace "
     "-nsteps 2000 -shapes 'stefanfish L=0.2 T=1 xpos=0.4 ypos=0.25'")
 
-# Grids of the ensemble members (blocks of 32x32 cells).  768x384 is left
-# out: its free-space transform lengths (1536) are not powers of two, which
-# the library's radix-16 FFTs require (cup2d_create returns CUP2D_ENOTSUP).
-ENSEMBLE_GRIDS = [(8, 4), (16, 8), (32, 16)]
+# Grids of the ensemble members (blocks of 32x32 cells): 256x128, 512x256,
+# 768x384 and 1024x512.
+ENSEMBLE_GRIDS = [(8, 4), (16, 8), (24, 12), (32, 16)]
 
 
 def fish_length_ok(L, h):

@@ -6,8 +6,8 @@
  * per pipeline stage), Shape (Shape.h:15-191) and SimulationData
  * (SimulationData.h:17-116), driven by Simulation::advance
  * (Simulation.cpp:279-305).  Each entry point below replaces one of those
- * calls; the C++ drop-in Operator subclasses that forward to them are shown
- * in INTEGRATION.md.
+ * calls; thin C++ Operator subclasses forwarding to them plug these into
+ * the unchanged Simulation loop.
  *
  * Conventions
  *  - every function returns an int status: CUP2D_OK (0) or a CUP2D_E* code;
@@ -38,6 +38,8 @@ extern "C" {
 #define CUP2D_ENOTSUP 6      /* feature outside this build                  */
 #define CUP2D_ESTATE 7       /* call out of order (e.g. before init)        */
 #define CUP2D_ENOMEM 8       /* device allocation failed                    */
+#define CUP2D_ETIMEOUT 10    /* a kernel's bounded wait for its tile loads  */
+                             /* gave up (the step's results are not valid)  */
 
 /* Poisson solver selection, Poisson/PoissonSolver.cpp:23-59 (makeSolver) */
 #define CUP2D_POISSON_FREESPACE 0   /* "freespace": FFTW_freespace.cpp        */
@@ -59,7 +61,9 @@ extern "C" {
 #define CUP2D_FIELD_CHI 2
 #define CUP2D_FIELD_PRES 3
 #define CUP2D_FIELD_TMP 4       /* pressure RHS after PressureSingle        */
-#define CUP2D_FIELD_UDEF_X 5    /* deformation velocity on the grid          */
+#define CUP2D_FIELD_UDEF_X 5    /* deformation velocity on the grid, as the  */
+                                /* last PutObjectsOnGrid leaves it (filled    */
+                                /* from the obstacle tiles when read)         */
 #define CUP2D_FIELD_UDEF_Y 6
 #define CUP2D_FIELD_SDF 7       /* max signed distance of all shapes         */
 
@@ -121,7 +125,16 @@ typedef struct cup2d_ctx cup2d_ctx;
 /* Fills *cfg with the defaults of Simulation::parseRuntime. */
 int cup2d_config_default(cup2d_config* cfg);
 /* SimulationData::allocateGrid (SimulationData.cpp:17-47) + solver setup
- * (PressureSingle ctor -> PoissonSolver::makeSolver). */
+ * (PressureSingle ctor -> PoissonSolver::makeSolver).  The Poisson
+ * transforms are power-of-two FFTs of lengths 16..4096 in shared memory:
+ *  - free space pads the grid to powers of two (the reference pads to
+ *    2N - 1; any padding >= 2N - 1 gives the same convolution on the
+ *    domain), so any block counts with Nx = 32 bpdx <= 4096 and
+ *    Ny = 32 bpdy <= 2048;
+ *  - periodic: Nx, Ny powers of two, Nx <= 8192, Ny <= 4096;
+ *  - cosine: Nx, Ny powers of two, Nx <= 4096, Ny <= 2048.
+ * Other grids return CUP2D_ENOTSUP; cup2d_last_error(NULL) gives the
+ * reason of this thread's last failed cup2d_create. */
 int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out);
 int cup2d_destroy(cup2d_ctx* ctx);
 const char* cup2d_last_error(const cup2d_ctx* ctx);
@@ -157,7 +170,18 @@ int cup2d_end_step(cup2d_ctx* ctx);
  * first call.  nsteps steps are enqueued without host synchronisation. */
 int cup2d_advance(cup2d_ctx* ctx, int nsteps);
 /* Blocks until queued work finished; returns the first device status flag
- * raised (CUP2D_ENAN, CUP2D_EDOMAIN, CUP2D_ECAPACITY) or CUP2D_OK. */
+ * raised (CUP2D_ENAN, CUP2D_EDOMAIN, CUP2D_ECAPACITY, CUP2D_ETIMEOUT) or
+ * CUP2D_OK.  The
+ * reference aborts or exits on these (Helpers.cpp:178-288,
+ * PutObjectsOnGrid.cpp:214-218); here the flags are reported once and
+ * cleared, and the context stays usable: a caller that repairs the state
+ * (cup2d_set_field, cup2d_set_shape, cup2d_checkpoint_load) runs on.
+ * Fault injection on the host: the environment variable
+ * CUP2D_FAULT_TILE_CAPACITY=n, read by cup2d_add_shape, caps a shape's
+ * obstacle-tile capacity at n, so a larger body raises CUP2D_ECAPACITY;
+ * CUP2D_FAULT_TMA_WAIT=1, read by cup2d_create, makes advDiff's tile
+ * barrier expect 16 bytes more than its loads bring, so every CTA's bounded
+ * wait runs out (after one second) and the step reports CUP2D_ETIMEOUT. */
 int cup2d_sync(cup2d_ctx* ctx);
 
 /* ---- state exchange --------------------------------------------------- */
@@ -176,11 +200,14 @@ int cup2d_grid_size(const cup2d_ctx* ctx, int* nx, int* ny, double* h);
 int cup2d_kernel_launches(const cup2d_ctx* ctx, long long* count);
 
 /* Measurement hook (no reference counterpart): launches one pipeline kernel
- * `reps` times back to back on the context's stream between two CUDA events
- * and returns the mean milliseconds per launch.  The kernels re-read and
- * re-write their own buffers, so state stays valid but is not a physical
- * step.  which: CUP2D_KERNEL_*. */
-#define CUP2D_KERNEL_ADVDIFF 0
+ * `reps` times on the context's stream and returns the mean milliseconds of
+ * one launch, each launch bracketed by its own CUDA events.  With flush_l2,
+ * a 256 MB device buffer (allocated by the first such call, kept until
+ * cup2d_destroy) is written before every launch, outside the events, so
+ * that each launch reads its inputs from HBM, not from the 126 MB L2.  The
+ * kernels re-read and re-write their own buffers, so state stays valid but
+ * is not a physical step.  which: CUP2D_KERNEL_*. */
+#define CUP2D_KERNEL_ADVDIFF 0      /* advDiff update + RHS divergence (one kernel) */
 #define CUP2D_KERNEL_RHS_DIV 1
 #define CUP2D_KERNEL_PCORR 2
 #define CUP2D_KERNEL_FFT_ROWS_FWD 3
@@ -188,7 +215,8 @@ int cup2d_kernel_launches(const cup2d_ctx* ctx, long long* count);
 #define CUP2D_KERNEL_FFT_ROWS_INV 5
 #define CUP2D_KERNEL_MAX_U 6
 #define CUP2D_KERNEL_OBJECTS 7
-int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, double* ms_per_launch);
+#define CUP2D_KERNEL_OUTFLOW 8      /* advDiff's boundary outflow flux */
+int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, int flush_l2, double* ms_per_launch);
 /* Measurement hook (no reference counterpart): cup2d_advance(ctx, nsteps)
  * bracketed by CUDA events on the context's stream; returns the elapsed
  * milliseconds (synchronises). */
@@ -237,7 +265,8 @@ int cup2d_ensemble_advance(cup2d_ensemble* ens, int nsteps);
 int cup2d_ensemble_advance_timed(cup2d_ensemble* ens, int nsteps, double* ms);
 int cup2d_ensemble_sync(cup2d_ensemble* ens);
 /* Every member's shape states, member by member (*count of them; CUP2D_EINVAL
- * when capacity is smaller), as cup2d_get_shape returns them.  After an
+ * when capacity is smaller; out == NULL with capacity 0 only sets *count),
+ * as cup2d_get_shape returns them.  After an
  * ensemble advance the graph's force passes have written them to mapped host
  * memory: one wait for all members; a member used on its own since is read
  * through cup2d_get_shape. */
@@ -262,6 +291,9 @@ int cup2d_ensemble_destroy(cup2d_ensemble* ens);
  *    CUP2D_ETOOLARGE without launching anything.
  *  - the first call on a device looks up the scratch address on that device
  *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *    The address is kept for the life of the process: after a
+ *    cudaDeviceReset of that device it is stale, so do not call this entry
+ *    point on a device that was reset.
  *  - calls share the scratch: calls that overlap on the GPU race and give
  *    wrong results; serialise them (one stream, or events).
  *  - stream: a cudaStream_t (NULL = legacy default stream); the call only

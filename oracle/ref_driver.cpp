@@ -221,6 +221,16 @@ Real* field_ptr(RefSim* r, int which, size_t b, int ix, int iy) {
 
 thread_local std::string g_err;
 
+// The iterated operator keeps its iteration count (oldNsteps, the
+// iterations of its last call) private.  An explicit template instantiation
+// may name a private member (access is not checked there), which hands the
+// harness a pointer to it without touching the reference's sources.
+struct IterCountTag { typedef int PressureIterator_unif::*type; };
+IterCountTag::type member_of(IterCountTag);
+template <class Tag, typename Tag::type M>
+struct MemberPtr { friend typename Tag::type member_of(Tag) { return M; } };
+template struct MemberPtr<IterCountTag, &PressureIterator_unif::oldNsteps>;
+
 } // namespace
 
 extern "C" {
@@ -262,6 +272,13 @@ void ref_set_time(void* h, double t, int step, double dt) {
 double ref_calc_dt(void* h) { return ((RefSim*)h)->calcMaxTimestep(); }
 int ref_advance(void* h) { return ((RefSim*)h)->advance(((RefSim*)h)->sim.dt) ? 1 : 0; }
 double ref_max_u(void* h) { const auto op = findMaxU(((RefSim*)h)->sim); return op.run(); }
+
+// Iterations of the last PressureIterator_unif call (its oldNsteps), or -1
+// when the pipeline runs PressureSingle.
+int ref_iterations(void* h) {
+  auto* op = dynamic_cast<PressureIterator_unif*>(((RefSim*)h)->pipeline[2]);
+  return op ? op->*member_of(IterCountTag()) : -1;
+}
 
 // op: 0 PutObjectsOnGrid, 1 advDiff, 2 PressureSingle, 3 ComputeForces
 void ref_run_op(void* h, int op, double dt) { (*((RefSim*)h)->pipeline[op])(dt); }

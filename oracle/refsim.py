@@ -18,7 +18,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libcup2d_ref.so")
-REFERENCE_SOURCE = "/root/reference/source"
+# the reference's source tree: $CUP2D_REFERENCE_SOURCE, else a checkout named
+# "reference" beside this repository
+REFERENCE_SOURCE = os.environ.get(
+    "CUP2D_REFERENCE_SOURCE",
+    os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference", "source"))
 
 # order of ref_get_shape's output; the product's cup2d_shape_state matches it
 SHAPE_FIELDS = [
@@ -63,7 +67,7 @@ def lib():
     L.ref_create.argtypes = [ctypes.c_char_p]
     L.ref_last_error.restype = ctypes.c_char_p
     L.ref_destroy.argtypes = [vp]
-    for name in ("ref_nx", "ref_ny", "ref_stepid", "ref_nshapes", "ref_advance"):
+    for name in ("ref_nx", "ref_ny", "ref_stepid", "ref_nshapes", "ref_advance", "ref_iterations"):
         getattr(L, name).argtypes = [vp]
         getattr(L, name).restype = i
     for name in ("ref_h", "ref_time", "ref_dt", "ref_lambda", "ref_calc_dt", "ref_max_u"):
@@ -186,6 +190,11 @@ class RefSim:
         dt = self.calc_dt()
         self.advance()
         return dt
+
+    def iterations(self):
+        """Iterations of the last PressureIterator_unif call (-1 without
+        -iterativePenalization)."""
+        return self.L.ref_iterations(self.h_)
 
     def run_op(self, name, dt):
         self.L.ref_run_op(self.h_, OPS[name], dt)

@@ -20,6 +20,9 @@ MEMBERS = [
      "-shapes 'disk radius=0.04 xpos=0.2 ypos=0.25 bForced=1 bFixed=1 xvel=0.2'"),
     ("-bpdx 8 -bpdy 4 -extent 1 -CFL 0.1 -nu 1e-4 -poissonType periodic "
      "-shapes 'carlingfish L=0.18 T=1 xpos=0.4 ypos=0.25 angle=10'"),
+    # 768x384: free space padded to 2048x1024
+    ("-bpdx 24 -bpdy 12 -extent 1 -CFL 0.1 -nu 1e-4 -lambda 1e4 -poissonType freespace "
+     "-shapes 'disk radius=0.03 xpos=0.2 ypos=0.25 bForced=1 bFixed=1 xvel=0.2'"),
 ]
 
 
@@ -126,6 +129,10 @@ def test_ensemble_shape_states_read_back():
                          for s in members for k in range(s.ctx.nshapes)])
 
     ens.advance(2)
+    # the size query: no buffer, capacity 0
+    import ctypes
+    cnt = ctypes.c_int(-1)
+    assert ens.L.cup2d_ensemble_get_shapes(ens.h_, None, 0, ctypes.byref(cnt)) == 0 and cnt.value == 6
     a = ens.shape_states()
     assert a.shape == (6, len(SHAPE_STATE_FIELDS))
     assert np.array_equal(a, own())

@@ -39,6 +39,9 @@ def test_iterated_steps_match_reference(ref, args):
     for _ in range(3):
         r.step()
         s.advance(s.calcMaxTimestep())
+        # the same number of iterations, step by step (oldNsteps of the
+        # reference's operator)
+        assert s.ctx.iteration_stats()[0] == r.iterations()
     s.ctx.sync()
     errs = {f: _rel(s.ctx.get(f), r.get(f)) for f in ("u", "v", "pres", "chi")}
     assert all(e <= 1e-9 for e in errs.values()), errs
