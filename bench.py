@@ -49,6 +49,11 @@ WORKLOADS = {
     "cylinder": ("forced_cylinder_re100_512x256_fp64",
                  "-bpdx 16 -bpdy 8 -extent 1 -CFL 0.1 -nu 1.5e-4 -lambda 1e4 -poissonType freespace "
                  "-muteAll 1 -shapes 'disk radius=0.0375 xpos=0.2 ypos=0.25 bForced=1 bFixed=1 xvel=0.2'"),
+    # the swimmer with the carangiform curvature envelope of the benchmark
+    # configurations, 0.82 (s/L + 0.0025) / 1.0025 (no reference counterpart)
+    "swimmer_envelope": ("envelope_swimmer_1024x512_fp64",
+                         "-bpdx 32 -bpdy 16 -extent 1 -CFL 0.1 -nu 2e-5 -lambda 1e4 -poissonType freespace "
+                         "-muteAll 1 -shapes 'envelopefish L=0.2 T=1 xpos=0.4 ypos=0.25'"),
     # the large single-GPU case: 4096x2048 on a 2x1 domain, two swimmers
     # L = 0.1 in tandem 0.15 apart, a quarter period out of phase (phi = 0.5,
     # the reference multiplies phi by pi), Re = 5000 on L; the falling
@@ -358,6 +363,58 @@ def dense_roofline(ctx, peak, peak_kind, workload, reps=30):
             "kernels": per}
 
 
+def div_2h(u, v, h):
+    """The divergence of PressureSingle's RHS (PressureSingle.cpp:112-128):
+    central differences over 2h, zero-gradient ghosts at the domain edge."""
+    ue = np.concatenate([u[:, 1:], u[:, -1:]], axis=1)
+    uw = np.concatenate([u[:, :1], u[:, :-1]], axis=1)
+    vn = np.concatenate([v[1:, :], v[-1:, :]], axis=0)
+    vs = np.concatenate([v[:1, :], v[:-1, :]], axis=0)
+    return (ue - uw + vn - vs) / (2 * h)
+
+
+def fp32_error_report(argline, local, rank, nsteps, sample=50):
+    """The FP32-transform path against the FP64 path over nsteps graph steps
+    from the same state: the body's speed (time-averaged over the run and
+    worst sample), its force (worst sample, against the largest force), the
+    fields at the end, and the divergence difference against the FP64 path's
+    own divergence (the discretisation floor: the reference's projection is
+    not discretely divergence-free)."""
+    a = make_sim(argline, local, rank)
+    b = make_sim(argline + " -precision fp32", local, rank)
+    spd_a, spd_b, fx_a, fx_b = [], [], [], []
+    done = 0
+    while done < nsteps:
+        n = min(sample, nsteps - done)
+        a.ctx.advance(n)
+        b.ctx.advance(n)
+        done += n
+        sa, sb = a.ctx.shape(0), b.ctx.shape(0)
+        spd_a.append(np.hypot(sa["u"], sa["v"]))
+        spd_b.append(np.hypot(sb["u"], sb["v"]))
+        fx_a.append(sa["forcex"])
+        fx_b.append(sb["forcex"])
+    a.ctx.sync()
+    b.ctx.sync()
+    spd_a, spd_b, fx_a, fx_b = map(np.array, (spd_a, spd_b, fx_a, fx_b))
+    fields = {}
+    for f in ("u", "v", "pres"):
+        fa, fb = a.ctx.get(f), b.ctx.get(f)
+        fields[f] = float(np.max(np.abs(fb - fa)) / max(np.max(np.abs(fa)), 1e-300))
+    h = a.ctx.h
+    da = div_2h(a.ctx.get("u"), a.ctx.get("v"), h)
+    db = div_2h(b.ctx.get("u"), b.ctx.get("v"), h)
+    fscale = max(np.max(np.abs(fx_a)), 1e-300)
+    return {"steps": nsteps, "sample_every": sample,
+            "speed_mean_rel_err": float(abs(spd_b.mean() - spd_a.mean()) / max(spd_a.mean(), 1e-300)),
+            "speed_max_rel_err": float(np.max(np.abs(spd_b - spd_a)) / max(np.max(spd_a), 1e-300)),
+            "force_x_max_rel_err": float(np.max(np.abs(fx_b - fx_a)) / fscale),
+            "fields_rel_err_end": fields,
+            "div_delta_inf": float(np.max(np.abs(db - da))),
+            "div_fp64_inf": float(np.max(np.abs(da))),
+            "against": "this library's FP64 path (itself parity-tested against the reference)"}
+
+
 def cufft_comparison(ctx, flush, reps=20):
     """The free-space solve's convolution done by cuFFT (through torch.fft,
     a comparison only, never on the product path): a double-precision 2D
@@ -432,6 +489,9 @@ def run_ours(args, world, rank, local, pg):
                 "note": "FP32 free-space Poisson transforms; fields, stencils, obstacle sums and "
                         "forces FP64; Cd within 1e-4 of FP64 is checked by tests/test_gpu_fp32.py"}
         del b
+
+    if fp32 is not None and args.fp32_report_steps > 0:
+        fp32["error_report"] = fp32_error_report(argline, local, rank, args.fp32_report_steps)
 
     # e2e: the reference's own loop through the C ABI with host transfers per
     # step: dt read back (calcMaxTimestep prints it), dt passed to the four
@@ -621,6 +681,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-Poisson measurement")
     ap.add_argument("--no-large", action="store_true", help="skip the 4096x2048 kernel roofline")
+    ap.add_argument("--fp32-report-steps", type=int, default=2000,
+                    help="steps of the FP32-against-FP64 error report (0: skip)")
     ap.add_argument("--no-cufft", action="store_true", help="skip the cuFFT comparison")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()

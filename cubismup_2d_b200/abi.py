@@ -26,7 +26,7 @@ ERRORS = {EINVAL: "EINVAL", ECUDA: "ECUDA", ENAN: "ENAN", EDOMAIN: "EDOMAIN",
 POISSON = {"freespace": 0, "periodic": 1, "": 2, "cosine": 2}
 PREC_FP64, PREC_FP32 = 0, 1
 FIELDS = {"u": 0, "v": 1, "chi": 2, "pres": 3, "tmp": 4, "udef_x": 5, "udef_y": 6, "sdf": 7}
-SHAPE_KINDS = {"disk": 0, "stefanfish": 1, "carlingfish": 2}
+SHAPE_KINDS = {"disk": 0, "stefanfish": 1, "carlingfish": 2, "envelopefish": 3}
 
 # the exported entry points, in include/cup2d.h order
 EXPORTS = [

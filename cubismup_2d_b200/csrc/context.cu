@@ -501,7 +501,8 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
   Ctx& c = ctx->c;
   if (c.initialised) return fail(ctx, CUP2D_ESTATE, "shapes must be added before cup2d_init");
   if (c.nshapes >= MAX_SHAPES) return fail(ctx, CUP2D_EINVAL, "too many shapes");
-  if (kind != CUP2D_SHAPE_DISK && kind != CUP2D_SHAPE_STEFANFISH && kind != CUP2D_SHAPE_CARLINGFISH)
+  if (kind != CUP2D_SHAPE_DISK && kind != CUP2D_SHAPE_STEFANFISH && kind != CUP2D_SHAPE_CARLINGFISH &&
+      kind != CUP2D_SHAPE_ENVELOPEFISH)
     return fail(ctx, CUP2D_ENOTSUP, "unknown shape kind");
   if (std::fabs(p->rhoS - 1.0) > DBL_EPSILON)
     return fail(ctx, CUP2D_ENOTSUP, "rhoS != 1 selects the variable-density pipeline (Simulation.cpp:185-204)");
@@ -594,7 +595,10 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
     const double pts[6] = {0, .15 * L, .4 * L, .65 * L, .9 * L, L};
     const double vals[6] = {0.82014 / L, 1.46515 / L, 2.57136 / L, 3.75425 / L, 5.09147 / L, 5.70449 / L};
     std::vector<double> p1f(Nm);
-    natural_spline(pts, vals, 6, rS.data(), p1f.data(), Nm);
+    if (kind == CUP2D_SHAPE_ENVELOPEFISH)      // the carangiform envelope (cup2d.h)
+      for (int i = 0; i < Nm; i++) p1f[i] = 0.82 * (rS[i] / L + 0.0025) / 1.0025 / L;
+    else
+      natural_spline(pts, vals, 6, rS.data(), p1f.data(), Nm);
     CK(cudaMemcpy(F.rS, rS.data(), sizeof(double) * Nm, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(F.width, width.data(), sizeof(double) * Nm, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(F.p1f, p1f.data(), sizeof(double) * Nm, cudaMemcpyHostToDevice));

@@ -94,9 +94,10 @@ k_fish_midline(Scalars* sc, const DevShape* sh, int k, FishArrays F, int mode)
   __syncthreads();
   CUP2D_TRACE_MARK(TRACE_ITEMS - 3, 1);
 
-  if (S.cfg.kind == CUP2D_SHAPE_STEFANFISH) {
+  if (S.cfg.kind != CUP2D_SHAPE_CARLINGFISH) {
     // curvature scheduler: after transition(0, 0, T, zeros, values) the start
-    // state and slope are zero and the end state is the spline p1f
+    // state and slope are zero and the end state is p1f (StefanFish: the
+    // spline of its control values; the envelope swimmer: its envelope)
     // (StefanFish.cpp:197-204); the RL bending wave is identically zero
     // without actions, and the PID terms are zero with -pid 0 -pidpos 0.
     const double waveLength = 1, amp = S.cfg.ampFac, phaseShift = S.cfg.phaseShift;

@@ -108,6 +108,12 @@ typedef struct cup2d_shape_params {
 #define CUP2D_SHAPE_DISK 0
 #define CUP2D_SHAPE_STEFANFISH 1
 #define CUP2D_SHAPE_CARLINGFISH 2
+/* A curvature swimmer with the carangiform envelope of the benchmark
+ * configurations in place of StefanFish's spline (no counterpart in the
+ * reference): the curvature amplitude along the body is
+ * 0.82 (s/L + 0.0025) / 1.0025 / L, ramped up over the first period and
+ * travelling as in CurvatureFish::computeMidline (StefanFish.cpp:154-206). */
+#define CUP2D_SHAPE_ENVELOPEFISH 3
 
 /* Rigid-body state and force sums of one shape, in the order of
  * Shape.h:22-62 (42 doubles). */
