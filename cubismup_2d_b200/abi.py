@@ -41,6 +41,7 @@ EXPORTS = [
     "cup2d_ensemble_create", "cup2d_ensemble_advance", "cup2d_ensemble_advance_timed",
     "cup2d_ensemble_sync", "cup2d_ensemble_get_shapes", "cup2d_ensemble_last_error",
     "cup2d_ensemble_destroy",
+    "cup2d_fish_act", "cup2d_fish_period", "cup2d_fish_state",
     "cup2d_adv_diff_noalloc",
 ]
 KERNELS = {"advdiff": 0, "rhs_div": 1, "pcorr": 2, "fft_rows_fwd": 3, "fft_cols": 4,
@@ -130,6 +131,9 @@ def lib():
     L.cup2d_ensemble_last_error.restype = ctypes.c_char_p
     L.cup2d_ensemble_destroy.argtypes = [vp]
     L.cup2d_adv_diff_noalloc.argtypes = [vp, vp, vp, vp, i, i, d, d, d, d, d, vp]
+    L.cup2d_fish_act.argtypes = [vp, i, d, dp, i]
+    L.cup2d_fish_period.argtypes = [vp, i, dp]
+    L.cup2d_fish_state.argtypes = [vp, i, i, dp, i]
     for name in EXPORTS:
         if name not in ("cup2d_last_error", "cup2d_ensemble_last_error"):
             getattr(L, name).restype = ctypes.c_int
@@ -369,6 +373,25 @@ class Context:
             blob = np.frombuffer(blob, dtype=np.uint8)
         ptr, size = _buffer(blob)
         self._ck(self.L.cup2d_checkpoint_load(self.h_, ptr, size))
+
+    # ---- RL actuation (StefanFish.cpp:373-577) ----
+    def fish_act(self, k, t_action, action):
+        """StefanFish::act: action[0] turns the body, action[1] (optional)
+        sets the tail period to Tperiod (1 + action[1]), both from t_action."""
+        a = np.ascontiguousarray(action, dtype=np.float64)
+        self._ck(self.L.cup2d_fish_act(self.h_, k, t_action, _dp(a), len(a)))
+
+    def fish_period(self, k):
+        """StefanFish::getLearnTPeriod."""
+        p = ctypes.c_double()
+        self._ck(self.L.cup2d_fish_period(self.h_, k, ctypes.byref(p)))
+        return p.value
+
+    def fish_state(self, k, other):
+        """StefanFish::state(shape other): 16 values (with the head sensors)."""
+        out = np.zeros(16)
+        self._ck(self.L.cup2d_fish_state(self.h_, k, other, _dp(out), 16))
+        return out
 
     def kernel_launches(self):
         n = ctypes.c_longlong()

@@ -568,7 +568,13 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
         double** a[8] = {&m->rX, &m->rY, &m->vX, &m->vY, &m->norX, &m->norY, &m->vNorX, &m->vNorY};
         for (auto x : a) { *x = q; q += Nm; }
       }
-      F.integ = q;
+      F.integ = q; q += 16;
+      for (int b = 0; b < 2; b++) {
+        FishMidline* m = &F.mid[b];
+        double** a[4] = {&m->uX, &m->uY, &m->lX, &m->lY};
+        for (auto x : a) { *x = q; q += Nm; }
+      }
+      F.frame.uX = F.frame.uY = F.frame.lX = F.frame.lY = nullptr;
     }
     // no midline formed yet: integrals (with their time) NaN (all-ones bytes)
     CK(cudaMemset(F.integ, 0xff, sizeof(double) * 16));
@@ -640,6 +646,9 @@ int cup2d_init(cup2d_ctx* ctx) {
     const ShapeCfg& f = S.cfg;
     std::memset(&S.s, 0, sizeof(S.s));
     std::memset(&S.f, 0, sizeof(S.f));
+    std::memset(&S.ctl, 0, sizeof(S.ctl));        // CurvatureFish::resetAll (StefanFish.cpp:64-83)
+    S.ctl.bendT0 = -1;                            // ParameterScheduler: t0 = -1, t1 = 0
+    S.ctl.periodPIDval = f.Tperiod;
     S.s.center[0] = S.s.com[0] = f.origC[0];
     S.s.center[1] = S.s.com[1] = f.origC[1];
     S.s.orientation = f.origAng;
@@ -1364,7 +1373,7 @@ struct CkptHeader {
   int32_t bpdx, bpdy, poisson, precision, nshapes, reserved;
   double extent, CFL, lambda, dlm, nu, fadeLen;
 };
-constexpr uint32_t CKPT_VERSION = 1;
+constexpr uint32_t CKPT_VERSION = 2;
 constexpr char CKPT_MAGIC[8] = {'C', 'U', 'P', '2', 'D', 'C', 'K', 0};
 
 struct CkptSection { void* p; size_t bytes; };
@@ -1543,3 +1552,277 @@ extern "C" int cup2d_trace(cup2d_ctx* ctx, unsigned long long* out, int reset) {
   return CUP2D_OK;
 }
 #endif
+
+// ---- RL actuation of the curvature swimmers ---------------------------------
+// StefanFish::act / getLearnTPeriod / getPhase / state
+// (StefanFish.cpp:373-577) on the device state.  An action changes the
+// midline from its time on, so midlines formed ahead (the operator path's
+// side branch, a graph step's next-step branch) are dropped and re-formed.
+namespace {
+
+int fish_of(cup2d_ctx* ctx, int id) {
+  Ctx& c = ctx->c;
+  if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
+  if (id < 0 || id >= c.nshapes) return fail(ctx, CUP2D_EINVAL, "bad shape id");
+  const int kind = c.hshapes[id].cfg.kind;
+  if (kind != CUP2D_SHAPE_STEFANFISH && kind != CUP2D_SHAPE_ENVELOPEFISH)
+    return fail(ctx, CUP2D_EINVAL, "shape is not a curvature swimmer (StefanFish)");
+  return CUP2D_OK;
+}
+
+int quiesce_all(cup2d_ctx* ctx) {
+  Ctx& c = ctx->c;
+  CK(cudaStreamSynchronize(c.stream));
+  CK(cudaStreamSynchronize(c.side));
+  CK(cudaStreamSynchronize(c.side2));
+  return CUP2D_OK;
+}
+
+// StefanFish::getPhase (StefanFish.cpp:385-395)
+double fish_phase(const DevShape& S, double t) {
+  const double T0 = S.ctl.time0, Ts = S.ctl.timeshift, Tp = S.ctl.periodPIDval;
+  const double arg = 2 * M_PI * ((t - T0) / Tp + Ts) + M_PI * S.cfg.phaseShift;
+  const double phase = std::fmod(arg, 2 * M_PI);
+  return (phase < 0) ? 2 * M_PI + phase : phase;
+}
+
+} // namespace
+
+extern "C" {
+
+int cup2d_fish_act(cup2d_ctx* ctx, int id, double t_action, const double* a, int na) {
+  if (!ctx || !a || na < 1) return ctx ? fail(ctx, CUP2D_EINVAL, "no action") : CUP2D_EINVAL;
+  int rc = fish_of(ctx, id);
+  if (rc) return rc;
+  Ctx& c = ctx->c;
+  if ((rc = quiesce_all(ctx))) return rc;
+  CK(cudaMemcpy(&c.hshapes[id], c.dshapes + id, sizeof(DevShape), cudaMemcpyDeviceToHost));
+  DevShape& S = c.hshapes[id];
+  FishCtl& C = S.ctl;
+  // CurvatureFish::execute (StefanFish.cpp:108-131)
+  C.oldrCurv = C.lastCurv;
+  C.lastCurv = a[0];
+  // ParameterSchedulerLearnWave::Turn (FishUtilities.h:377-384): a node at
+  // the head of the wave, the oldest two dropped
+  C.bendT0 = t_action;
+  for (int i = 6; i > 1; --i) C.bend[i] = C.bend[i - 2];
+  C.bend[1] = a[0];
+  C.bend[0] = 0;
+  if (na > 1) {                             // the tail period
+    C.lastTact = a[1];
+    const double lastArg = (t_action - C.time0) / C.periodPIDval + C.timeshift;
+    C.timeshift = lastArg;
+    C.time0 = t_action;
+    C.periodPIDval = S.cfg.Tperiod * (1 + a[1]);
+    C.periodPIDdif = 0;
+  }
+  CK(cudaMemcpy(&c.dshapes[id].ctl, &C, sizeof(FishCtl), cudaMemcpyHostToDevice));
+  // midlines formed ahead are of the old actuation: mark both buffers empty
+  // (their time NaN) so that the next placement forms its midline again
+  const FishArrays& F = c.fish[id];
+  CK(cudaMemset(F.integ + 7, 0xff, sizeof(double)));
+  CK(cudaMemset(F.integ + 15, 0xff, sizeof(double)));
+  c.sideMidPending = false;
+  c.midByGraph = false;
+  forget_chain(c);
+  c.shapesAtEvent = c.shapesMapped = false;
+  c.stateSeq++;
+  return CUP2D_OK;
+}
+
+int cup2d_fish_period(cup2d_ctx* ctx, int id, double* period) {
+  if (!ctx || !period) return CUP2D_EINVAL;
+  int rc = fish_of(ctx, id);
+  if (rc) return rc;
+  Ctx& c = ctx->c;
+  CK(cudaStreamSynchronize(c.stream));
+  FishCtl C;
+  CK(cudaMemcpy(&C, &c.dshapes[id].ctl, sizeof(FishCtl), cudaMemcpyDeviceToHost));
+  *period = C.periodPIDval;                 // StefanFish::getLearnTPeriod
+  return CUP2D_OK;
+}
+
+// StefanFish::state (StefanFish.cpp:397-577) with the head's shear sensors
+// that StefanFish.h:12 compiles in (16 values).
+int cup2d_fish_state(cup2d_ctx* ctx, int id, int other, double* out, int n) {
+  if (!ctx || !out) return CUP2D_EINVAL;
+  int rc = fish_of(ctx, id);
+  if (rc) return rc;
+  Ctx& c = ctx->c;
+  if (other < 0 || other >= c.nshapes) return fail(ctx, CUP2D_EINVAL, "bad shape id");
+  if (n < 16) return fail(ctx, CUP2D_EINVAL, "the state has 16 values");
+  if ((rc = quiesce_all(ctx))) return rc;
+  DevShape S, P;
+  CK(cudaMemcpy(&S, c.dshapes + id, sizeof(DevShape), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&P, c.dshapes + other, sizeof(DevShape), cudaMemcpyDeviceToHost));
+  Scalars sc;
+  CK(cudaMemcpy(&sc, c.dsc, sizeof(Scalars), cudaMemcpyDeviceToHost));
+  const double L = S.cfg.length, Tp = S.cfg.Tperiod;
+  out[0] = (S.s.center[0] - P.s.center[0]) / L;
+  out[1] = (S.s.center[1] - P.s.center[1]) / L;
+  out[2] = S.s.orientation;
+  out[3] = fish_phase(S, sc.time);
+  out[4] = S.s.u * Tp / L;
+  out[5] = S.s.v * Tp / L;
+  out[6] = S.s.omega * Tp;
+  out[7] = S.ctl.lastTact;
+  out[8] = S.ctl.lastCurv;
+  out[9] = S.ctl.oldrCurv;
+
+  // the skin of the last placement in the computational frame:
+  // surfaceToCOMFrame (FishLibrary.cpp:259-280), surfaceToComputationalFrame
+  // (:282-299), then computeSkinNormals (:196-257) with the midline
+  const FishArrays& F = c.fish[id];
+  const int Nm = F.nm;
+  const FishMidline& M = F.mid[S.f.midBuf & 1];
+  std::vector<double> xu(Nm), yu(Nm), xl(Nm), yl(Nm), rX(Nm), rY(Nm), rS(Nm);
+  CK(cudaMemcpy(xu.data(), M.uX, sizeof(double) * Nm, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(yu.data(), M.uY, sizeof(double) * Nm, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(xl.data(), M.lX, sizeof(double) * Nm, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(yl.data(), M.lY, sizeof(double) * Nm, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(rX.data(), F.frame.rX, sizeof(double) * Nm, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(rY.data(), F.frame.rY, sizeof(double) * Nm, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(rS.data(), F.rS, sizeof(double) * Nm, cudaMemcpyDeviceToHost));
+  auto rotate = [](double c0, double s0, double& x, double& y) {
+    const double p0 = x, p1 = y;
+    x = c0 * p0 + (-s0) * p1;
+    y = s0 * p0 + c0 * p1;
+  };
+  {
+    const double ct = std::cos(S.f.theta_internal), st = std::sin(S.f.theta_internal);
+    const double co = std::cos(S.s.orientation), so = std::sin(S.s.orientation);
+    for (int i = 0; i < Nm; i++) {
+      for (int side = 0; side < 2; side++) {
+        double& x = side ? xl[i] : xu[i];
+        double& y = side ? yl[i] : yu[i];
+        x -= S.f.CoM_internal[0];
+        y -= S.f.CoM_internal[1];
+        rotate(ct, st, x, y);
+        rotate(co, so, x, y);
+        x += S.s.com[0];
+        y += S.s.com[1];
+      }
+      rotate(co, so, rX[i], rY[i]);
+      rX[i] += S.s.com[0];
+      rY[i] += S.s.com[1];
+    }
+  }
+  const int Np = Nm;
+  std::vector<double> midX[2], midY[2], nXs[2], nYs[2];
+  for (int side = 0; side < 2; side++) {
+    const std::vector<double>& xs = side ? xl : xu;
+    const std::vector<double>& ys = side ? yl : yu;
+    midX[side].resize(Np - 1); midY[side].resize(Np - 1); nXs[side].resize(Np - 1); nYs[side].resize(Np - 1);
+    for (int i = 0; i < Np - 1; i++) {
+      midX[side][i] = (xs[i] + xs[i + 1]) / 2;
+      midY[side][i] = (ys[i] + ys[i + 1]) / 2;
+      nXs[side][i] = (ys[i + 1] - ys[i]);
+      nYs[side][i] = -(xs[i + 1] - xs[i]);
+      const double nrm = std::sqrt(std::pow(nXs[side][i], 2) + std::pow(nYs[side][i], 2));
+      nXs[side][i] /= nrm;
+      nYs[side][i] /= nrm;
+      const int ii = (i < 8) ? 8 : ((i > Np - 9) ? Np - 9 : i);
+      const double dir = nXs[side][i] * (midX[side][i] - rX[ii]) + nYs[side][i] * (midY[side][i] - rY[ii]);
+      if (dir < 0) { nXs[side][i] *= -1.0; nYs[side][i] *= -1.0; }
+    }
+  }
+
+  // the obstacle blocks of this fish and the grid's velocity around them
+  const GridDesc& g = c.g;
+  const double h = g.h, invh = 1 / h;
+  std::vector<int> slot(g.nblocks);
+  CK(cudaMemcpy(slot.data(), c.tiles[id].slot, sizeof(int) * g.nblocks, cudaMemcpyDeviceToHost));
+  auto bmin = [&](int b, int d) {
+    const int bi = d == 0 ? b % g.bpdx : b / g.bpdx;
+    return (double)(bi * BS) * h + h * (0 + 0.5) - 0.5 * h;
+  };
+  auto bmax = [&](int b, int d) {
+    const int bi = d == 0 ? b % g.bpdx : b / g.bpdx;
+    return (double)(bi * BS) * h + h * (BS - 1 + 0.5) + 0.5 * h;
+  };
+  bool lost = false;
+  // the block holding (x, y) that has an obstacle block, else of those the
+  // one with the largest outside distance (the order of
+  // std::sort + std::reverse over (distance, index) pairs)
+  auto holding = [&](double x, double y) {
+    std::vector<std::pair<double, int>> d(g.nblocks);
+    for (int b = 0; b < g.nblocks; b++) {
+      const double mn0 = bmin(b, 0), mn1 = bmin(b, 1), mx0 = bmax(b, 0), mx1 = bmax(b, 1);
+      if (x >= mn0 && y >= mn1 && x <= mx0 && y <= mx1 && slot[b] >= 0) return b;
+      d[b] = {std::max(std::max(mn0 - x, x - mx0), std::max(mn1 - y, y - mx1)), b};
+    }
+    std::sort(d.begin(), d.end());
+    std::reverse(d.begin(), d.end());
+    for (auto& e : d) if (slot[e.second] >= 0) return e.second;
+    lost = true;
+    return 0;
+  };
+  auto cell_in = [&](double x, double y, int b, int& ix, int& iy) {
+    const double o0 = (double)((b % g.bpdx) * BS) * h + h * 0.5;
+    const double o1 = (double)((b / g.bpdx) * BS) * h + h * 0.5;
+    ix = std::min(std::max(0, (int)std::round((x - o0) * invh)), BS - 1);
+    iy = std::min(std::max(0, (int)std::round((y - o1) * invh)), BS - 1);
+  };
+  auto skinVel = [&](double x, double y, double* v) -> int {
+    const int b = holding(x, y);
+    if (slot[b] < 0) { lost = true; return CUP2D_OK; }
+    int ix, iy;
+    cell_in(x, y, b, ix, iy);
+    const size_t o = (size_t)slot[b] * BS2 + iy * BS + ix;
+    double ux, uy;
+    CK(cudaMemcpy(&ux, c.tiles[id].udx + o, sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&uy, c.tiles[id].udy + o, sizeof(double), cudaMemcpyDeviceToHost));
+    // the removed rigid part (Shape.cpp:197-204), as udef_at evaluates it
+    const double p0 = cell_x(g, b % g.bpdx, ix) - S.s.com[0], p1 = cell_y(g, b / g.bpdx, iy) - S.s.com[1];
+    ux = ux - (S.Iu - S.Ia * p1);
+    uy = uy - (S.Iv + S.Ia * p0);
+    v[0] = S.s.u - S.s.omega * (y - S.s.com[1]) + ux;
+    v[1] = S.s.v + S.s.omega * (x - S.s.com[0]) + uy;
+    return CUP2D_OK;
+  };
+  auto sensVel = [&](double x, double y, double* v) -> int {
+    const int b = holding(x, y);
+    int ix, iy;
+    cell_in(x, y, b, ix, iy);
+    const size_t q = (size_t)((b / g.bpdx) * BS + iy) * g.nx + (b % g.bpdx) * BS + ix;
+    CK(cudaMemcpy(&v[0], c.u() + q, sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&v[1], c.v() + q, sizeof(double), cudaMemcpyDeviceToHost));
+    return CUP2D_OK;
+  };
+  int iHead = 0;                            // the head side, s = 0.04 L (_width)
+  for (int i = 0; i < Nm - 1; ++i)
+    if (rS[i] <= 0.04 * L && rS[i + 1] > 0.04 * L) iHead = i;
+  double tip[2], low[2], top[2];
+  {
+    const double pSkin[2] = {xu[0], yu[0]};
+    const double nX = (nXs[0][0] + nXs[1][0]) / 2, nY = (nYs[0][0] + nYs[1][0]) / 2;
+    const double pSens[2] = {pSkin[0] + h * nX, pSkin[1] + h * nY};
+    double vSens[2], vSkin[2];
+    if ((rc = sensVel(pSens[0], pSens[1], vSens)) || (rc = skinVel(pSkin[0], pSkin[1], vSkin))) return rc;
+    tip[0] = (vSens[0] - vSkin[0]) * invh;
+    tip[1] = (vSens[1] - vSkin[1]) * invh;
+  }
+  for (int side = 0; side < 2; side++) {
+    const std::vector<double>& xs = side ? xl : xu;
+    const std::vector<double>& ys = side ? yl : yu;
+    const double pSkin[2] = {midX[side][iHead], midY[side][iHead]};
+    const double nX = nXs[side][iHead], nY = nYs[side][iHead];
+    const double pSens[2] = {pSkin[0] + h * nX, pSkin[1] + h * nY};
+    double vSens[2], vSkin[2];
+    if ((rc = sensVel(pSens[0], pSens[1], vSens)) || (rc = skinVel(pSkin[0], pSkin[1], vSkin))) return rc;
+    const double shX = (vSens[0] - vSkin[0]) * invh, shY = (vSens[1] - vSkin[1]) * invh;
+    const double dX = xs[iHead + 1] - xs[iHead], dY = ys[iHead + 1] - ys[iHead];
+    const double proj = dX * nX - dY * nY;
+    const double tX = proj > 0 ? nX : -nX, tY = proj > 0 ? -nY : nY;
+    double* r = side == 0 ? top : low;
+    r[0] = shX * nX + shY * nY;
+    r[1] = shX * tX + shY * tY;
+  }
+  if (lost) return fail(ctx, CUP2D_ESTATE, "a skin point lies outside the fish's obstacle blocks");
+  out[10] = tip[0] * Tp / L; out[11] = tip[1] * Tp / L;
+  out[12] = low[0] * Tp / L; out[13] = low[1] * Tp / L;
+  out[14] = top[0] * Tp / L; out[15] = top[1] * Tp / L;
+  return CUP2D_OK;
+}
+
+} // extern "C"

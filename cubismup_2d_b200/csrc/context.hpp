@@ -128,8 +128,9 @@ struct Ctx {
 };
 
 // doubles behind one fish's arrays (FishArrays::pool): the static profile,
-// two midline buffers, the frame midline and the integrals
-inline size_t fish_pool_len(int nm) { return 28 * (size_t)nm + 16; }
+// two midline buffers, the frame midline, the integrals, then the skins of
+// the two midline buffers
+inline size_t fish_pool_len(int nm) { return 36 * (size_t)nm + 16; }
 
 // counter slots used by the kernels (each last-CTA reduction owns one)
 enum CounterSlot : int {

@@ -98,18 +98,41 @@ k_fish_midline(Scalars* sc, const DevShape* sh, int k, FishArrays F, int mode)
     // curvature scheduler: after transition(0, 0, T, zeros, values) the start
     // state and slope are zero and the end state is p1f (StefanFish: the
     // spline of its control values; the envelope swimmer: its envelope)
-    // (StefanFish.cpp:197-204); the RL bending wave is identically zero
-    // without actions, and the PID terms are zero with -pid 0 -pidpos 0.
+    // (StefanFish.cpp:166-206).  The RL bending wave rB, vB of the learn-wave
+    // scheduler (zero without actions), the tail period and its phase, and
+    // the PID terms come from the actuation state (cup2d_fish_act).
+    const FishCtl& C = S.ctl;
     const double waveLength = 1, amp = S.cfg.ampFac, phaseShift = S.cfg.phaseShift;
-    const double periodPIDval = T, time0 = 0, timeshift = 0;
-    const double diffT = 1;
+    const double periodPIDval = C.periodPIDval, time0 = C.time0, timeshift = C.timeshift;
+    const double diffT = C.TperiodPID ? 1 - (t - time0) * C.periodPIDdif / periodPIDval : 1;
     const double darg = 2 * M_PI / periodPIDval * diffT;
     const double arg0 = 2 * M_PI * ((t - time0) / periodPIDval + timeshift) + M_PI * phaseShift;
+    const double fac = C.pidFac, dif = C.pidDif;
+    // ParameterSchedulerLearnWave<7>::gimmeValues (FishUtilities.h:320-366)
+    // at nodes -.5, -.25, 0, .25, .5, .75, 1 (StefanFish.cpp:163-164)
+    const double _1oL = 1. / L, _1oT = 1. / periodPIDval;
     for (int i = tid; i < Nm; i += nt) {
       double rC, vC;
       if (t > T) { rC = F.p1f[i]; vC = 0; }
       else cubic_interp(0.0, T, t, 0.0, F.p1f[i], 0.0, 0.0, rC, vC);
-      const double rB = 0, vB = 0, fac = 0, dif = 0;
+      double rB = 0, vB = 0;
+      {
+        const double c = rS[i] * _1oL - (t - C.bendT0) * _1oT;   // travelling wave coordinate
+        if (c < -.5) {
+          cubic_interp(c, -.5, c, C.bend[0], C.bend[0], 0.0, 0.0, rB, vB);
+        } else if (c > 1.) {
+          cubic_interp(1., c, c, C.bend[6], C.bend[6], 0.0, 0.0, rB, vB);
+        } else {
+#pragma unroll
+          for (int j = 1; j < 7; ++j) {                 // the last interval holding c wins
+            const double xa = .25 * (j - 1) - .5, xb = .25 * j - .5;
+            if (c >= xa && c <= xb) {
+              cubic_interp(xa, xb, c, C.bend[j - 1], C.bend[j], 0.0, 0.0, rB, vB);
+              vB = -vB * _1oT;
+            }
+          }
+        }
+      }
       const double arg = arg0 - 2 * M_PI * rS[i] / L / waveLength;
       rK[i] = amp * rC * (sin(arg) + rB + fac);
       vK[i] = amp * (vC * (sin(arg) + rB + fac) + rC * (cos(arg) * darg + vB + dif));
@@ -205,6 +228,19 @@ k_fish_midline(Scalars* sc, const DevShape* sh, int k, FishArrays F, int mode)
       vNorX[Nm - 1] = vNorX[Nm - 2]; vNorY[Nm - 1] = vNorY[Nm - 2];
     }
     __syncthreads();
+  }
+
+  // FishData::computeSurface (FishLibrary.cpp:178-194): the skin in the
+  // midline's own frame, kept with this buffer
+  {
+    const FishMidline& M = F.mid[p];
+    for (int i = tid; i < Nm; i += nt) {
+      double n0 = norX[i], n1 = norY[i];
+      const double mod = sqrt(n0 * n0 + n1 * n1);
+      n0 /= mod; n1 /= mod;
+      M.lX[i] = rX[i] - width[i] * n0; M.lY[i] = rY[i] - width[i] * n1;
+      M.uX[i] = rX[i] + width[i] * n0; M.uY[i] = rY[i] + width[i] * n1;
+    }
   }
 
   // FishData::_d_ds / _integrationFac* (FishLibrary.h:79-95)
@@ -307,6 +343,7 @@ k_fish_frame(GridDesc g, Scalars* sc, DevShape* sh, int k, FishArrays F, ObstTil
   // stalling the segment chain behind a barrier
   const double cosO = S.cosO, sinO = S.sinO, cen0 = S.s.center[0], cen1 = S.s.center[1];
   if (tid == 0) {                                       // Fish.cpp:87-93 bookkeeping
+    S.f.midBuf = p;
     S.f.area_internal = integ[0];
     S.f.CoM_internal[0] = integ[1]; S.f.CoM_internal[1] = integ[2];
     S.f.vCoM_internal[0] = integ[3]; S.f.vCoM_internal[1] = integ[4];

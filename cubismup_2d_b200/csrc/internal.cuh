@@ -86,12 +86,27 @@ struct FishState {
   double CoM_internal[2], vCoM_internal[2];
   double theta_internal, angvel_internal, angvel_internal_prev;
   double cosTh, sinTh;            // cos/sin(theta_internal), set where theta_internal moves
+  int midBuf;                     // midline buffer of the last placement
+};
+
+// CurvatureFish's actuation state (StefanFish.cpp:20-51, 85-131): the RL
+// bending wave of ParameterSchedulerLearnWave<7> (node values and the time
+// of the last turn, FishUtilities.h:317-385; t0 = -1 before any), the tail
+// period with its phase bookkeeping, the PID curvature terms and the last
+// actions (for StefanFish::state).
+struct FishCtl {
+  double bend[7], bendT0;
+  double periodPIDval, periodPIDdif, time0, timeshift;
+  double pidFac, pidDif;
+  double lastTact, lastCurv, oldrCurv;
+  int TperiodPID;
 };
 
 struct DevShape {
   cup2d_shape_state s;
   ShapeCfg cfg;
   FishState f;
+  FishCtl ctl;
   int ntiles;                     // obstacle tiles this step
   int ntilesPrev;
   double rhoTile;                 // ObstacleBlock::rho: rhoS (disk), 1 (fish)
@@ -126,9 +141,12 @@ struct ObstTiles {
   int capacity;
 };
 
-// One fish midline (the arrays of FishLibrary.h:49-60).
+// One fish midline (the arrays of FishLibrary.h:49-60); the two step
+// buffers also keep the skin of FishData::computeSurface
+// (FishLibrary.cpp:178-194) in the midline's own frame: upper / lower x, y.
 struct FishMidline {
   double *rX, *rY, *vX, *vY, *norX, *norY, *vNorX, *vNorY;
+  double *uX, *uY, *lX, *lY;
 };
 
 // Per-fish device arrays.  The midline depends only on time, so the one for
@@ -388,10 +406,10 @@ __device__ __forceinline__ void udef_at(const ObstTiles& t, size_t o, const DevS
 
 // Cell-centre position of cell (ix,iy) of block (bx,by); the same expression
 // as the oracle's BlockInfo::pos (origin + h*(i + 1/2), origin = 32*b*h).
-__device__ __forceinline__ double cell_x(const GridDesc& g, int bx, int ix) {
+__host__ __device__ __forceinline__ double cell_x(const GridDesc& g, int bx, int ix) {
   return (double)(bx * BS) * g.h + g.h * (ix + 0.5);
 }
-__device__ __forceinline__ double cell_y(const GridDesc& g, int by, int iy) {
+__host__ __device__ __forceinline__ double cell_y(const GridDesc& g, int by, int iy) {
   return (double)(by * BS) * g.h + g.h * (iy + 0.5);
 }
 __device__ __forceinline__ double gx_pos(const GridDesc& g, int gx) {

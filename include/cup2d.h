@@ -280,6 +280,24 @@ int cup2d_ensemble_get_shapes(cup2d_ensemble* ens, cup2d_shape_state* out, int c
 const char* cup2d_ensemble_last_error(const cup2d_ensemble* ens);
 int cup2d_ensemble_destroy(cup2d_ensemble* ens);
 
+/* ---- RL actuation of the curvature swimmers ---------------------------- */
+/* StefanFish::act (StefanFish.cpp:373-377, CurvatureFish::execute :108-131):
+ * a[0] turns the body (a node at the head of the learn-wave bending
+ * scheduler, FishUtilities.h:377-384, timed t_action); with na > 1, a[1]
+ * sets the tail period to Tperiod (1 + a[1]) from t_action on, keeping the
+ * undulation's phase.  Between steps; the midline is re-formed from the next
+ * placement.  Only for StefanFish / envelope swimmers. */
+int cup2d_fish_act(cup2d_ctx* ctx, int id, double t_action, const double* a, int na);
+/* StefanFish::getLearnTPeriod (StefanFish.cpp:379-383): the current period. */
+int cup2d_fish_period(cup2d_ctx* ctx, int id, double* period);
+/* StefanFish::state (StefanFish.cpp:397-577) relative to shape `other`, with
+ * the head's shear sensors that StefanFish.h:12 compiles in: 16 values
+ * (n >= 16): relative centre / L (2), orientation, undulation phase,
+ * u T/L, v T/L, omega T, the last period and curvature actions, the one
+ * before, then the shear at the tip, lower and upper head side times T/L
+ * (normal, tangential each).  Reads the state after the last placement. */
+int cup2d_fish_state(cup2d_ctx* ctx, int id, int other, double* out, int n);
+
 /* ---- allocation-free advDiff ------------------------------------------ */
 /* This entry point has no counterpart in the reference.  It is advDiff
  * (advDiff.cpp:36-118: explicit Euler step of central advection and 5-point

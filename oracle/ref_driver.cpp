@@ -280,6 +280,35 @@ int ref_iterations(void* h) {
   return op ? op->*member_of(IterCountTag()) : -1;
 }
 
+// The RL actuation of a StefanFish (StefanFish.cpp:373-577): act, the
+// learn period, and its state relative to another shape (16 values with the
+// sensors StefanFish.h:12 compiles in).  Return -1 if `id` is no StefanFish.
+int ref_fish_act(void* h, int id, double t, const double* a, int na) {
+  auto* f = dynamic_cast<StefanFish*>(((RefSim*)h)->sim.shapes[id]);
+  if (!f) return -1;
+  f->act(t, std::vector<double>(a, a + na));
+  return 0;
+}
+void ref_set_pose(void* h, int id, double cx, double cy, double px, double py, double ang) {
+  Shape* s = ((RefSim*)h)->sim.shapes[id];
+  double com[2] = {cx, cy};
+  s->setCenterOfMass(com);
+  s->center[0] = px; s->center[1] = py;
+  s->setOrientation(ang);
+}
+double ref_fish_period(void* h, int id) {
+  auto* f = dynamic_cast<StefanFish*>(((RefSim*)h)->sim.shapes[id]);
+  return f ? f->getLearnTPeriod() : -1;
+}
+int ref_fish_state(void* h, int id, int other, double* out) {
+  RefSim* r = (RefSim*)h;
+  auto* f = dynamic_cast<StefanFish*>(r->sim.shapes[id]);
+  if (!f) return -1;
+  const std::vector<double> s = f->state(r->sim.shapes[other]);
+  for (size_t i = 0; i < s.size(); i++) out[i] = s[i];
+  return (int)s.size();
+}
+
 // op: 0 PutObjectsOnGrid, 1 advDiff, 2 PressureSingle, 3 ComputeForces
 void ref_run_op(void* h, int op, double dt) { (*((RefSim*)h)->pipeline[op])(dt); }
 void ref_reset(void* h) { ((RefSim*)h)->reset(); ((RefSim*)h)->sim.dt = 0; }

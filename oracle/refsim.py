@@ -83,6 +83,13 @@ def lib():
     L.ref_get_shape.argtypes = [vp, i, dp]
     L.ref_get_obstacle.argtypes = [vp, i, dp]
     L.ref_get_obstacle.restype = ctypes.c_long
+    L.ref_set_pose.argtypes = [vp, i, d, d, d, d, d]
+    L.ref_fish_act.argtypes = [vp, i, d, dp, i]
+    L.ref_fish_act.restype = i
+    L.ref_fish_period.argtypes = [vp, i]
+    L.ref_fish_period.restype = d
+    L.ref_fish_state.argtypes = [vp, i, i, dp]
+    L.ref_fish_state.restype = i
     L.ref_profile.argtypes = [vp, ctypes.c_char_p, i, dp, i]
     L.ref_profile.restype = i
     L.ref_profile_reset.argtypes = [vp]
@@ -195,6 +202,26 @@ class RefSim:
         """Iterations of the last PressureIterator_unif call (-1 without
         -iterativePenalization)."""
         return self.L.ref_iterations(self.h_)
+
+    def fish_act(self, k, t, action):
+        """StefanFish::act(t, action) on shape k."""
+        a = np.ascontiguousarray(action, dtype=np.float64)
+        assert self.L.ref_fish_act(self.h_, k, t, _dp(a), len(a)) == 0
+
+    def fish_period(self, k):
+        return self.L.ref_fish_period(self.h_, k)
+
+    def fish_state(self, k, other):
+        """StefanFish::state(shapes[other]) of shape k."""
+        out = np.zeros(32)
+        n = self.L.ref_fish_state(self.h_, k, other, _dp(out))
+        assert n > 0
+        return out[:n]
+
+    def set_shape_pose(self, k, com, center, orientation):
+        """Shape::setCenterOfMass / center / setOrientation (as an RL driver's
+        resetIC does, main_RL_leadFollow.cpp:27-41)."""
+        self.L.ref_set_pose(self.h_, k, com[0], com[1], center[0], center[1], orientation)
 
     def run_op(self, name, dt):
         self.L.ref_run_op(self.h_, OPS[name], dt)
