@@ -41,7 +41,7 @@ EXPORTS = [
     "cup2d_ensemble_create", "cup2d_ensemble_advance", "cup2d_ensemble_advance_timed",
     "cup2d_ensemble_sync", "cup2d_ensemble_get_shapes", "cup2d_ensemble_last_error",
     "cup2d_ensemble_destroy",
-    "cup2d_fish_act", "cup2d_fish_period", "cup2d_fish_state",
+    "cup2d_fish_act", "cup2d_fish_period", "cup2d_fish_state", "cup2d_dump",
     "cup2d_adv_diff_noalloc",
 ]
 KERNELS = {"advdiff": 0, "rhs_div": 1, "pcorr": 2, "fft_rows_fwd": 3, "fft_cols": 4,
@@ -131,6 +131,7 @@ def lib():
     L.cup2d_ensemble_last_error.restype = ctypes.c_char_p
     L.cup2d_ensemble_destroy.argtypes = [vp]
     L.cup2d_adv_diff_noalloc.argtypes = [vp, vp, vp, vp, i, i, d, d, d, d, d, vp]
+    L.cup2d_dump.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p]
     L.cup2d_fish_act.argtypes = [vp, i, d, dp, i]
     L.cup2d_fish_period.argtypes = [vp, i, dp]
     L.cup2d_fish_state.argtypes = [vp, i, i, dp, i]
@@ -374,6 +375,10 @@ class Context:
         ptr, size = _buffer(blob)
         self._ck(self.L.cup2d_checkpoint_load(self.h_, ptr, size))
 
+    def dump(self, directory, name):
+        """SimulationData::dumpAll: velChi, pres, invRho (float32 + XDMF)."""
+        self._ck(self.L.cup2d_dump(self.h_, str(directory).encode(), name.encode()))
+
     # ---- RL actuation (StefanFish.cpp:373-577) ----
     def fish_act(self, k, t_action, action):
         """StefanFish::act: action[0] turns the body, action[1] (optional)
@@ -430,11 +435,31 @@ class ComputeForces(Operator):
     name, _fn = "ComputeForces", "compute_forces"
 
 
+def parse_dump_args(argline):
+    """The dump options of Simulation::parseRuntime (Simulation.cpp:79-83):
+    -fdump (steps between dumps), -tdump (time between dumps),
+    -serialization (directory, default -file, default "./")."""
+    toks = shlex.split(argline)
+    out = {"fdump": 0, "tdump": 0.0, "dir": "./"}
+    for i, t in enumerate(toks[:-1]):
+        if t == "-fdump":
+            out["fdump"] = int(toks[i + 1])
+        elif t == "-tdump":
+            out["tdump"] = float(toks[i + 1])
+        elif t == "-file" and "-serialization" not in toks:
+            out["dir"] = toks[i + 1]
+        elif t == "-serialization":
+            out["dir"] = toks[i + 1]
+    return out
+
+
 class Simulation:
     """Simulation.h:19-40 on the device pipeline."""
 
     def __init__(self, argline):
         self.cfg, self.shape_params = parse_args(argline)
+        self.dumps = parse_dump_args(argline)
+        self.next_dump_time = 0.0
         self.ctx = None
         self.pipeline = []
 
@@ -442,15 +467,30 @@ class Simulation:
         self.ctx = Context(self.cfg, self.shape_params)
         self.pipeline = [PutObjectsOnGrid(self), advDiff(self), PressureSingle(self), ComputeForces(self)]
         self.ctx.init()
+        self.next_dump_time = 0.0
+        if self.dumping():                     # Simulation.cpp:229 (only when dumps are asked for)
+            self.ctx.dump(self.dumps["dir"], "IC")
+
+    def dumping(self):
+        return self.dumps["fdump"] > 0 or self.dumps["tdump"] > 0
+
+    def bDump(self, st):  # SimulationData.cpp:179-185
+        time_dump = self.dumps["tdump"] > 0 and st["time"] >= self.next_dump_time
+        step_dump = self.dumps["fdump"] > 0 and st["step"] % self.dumps["fdump"] == 0
+        return time_dump or step_dump
 
     def calcMaxTimestep(self):
         return self.ctx.calc_dt(sync=True)
 
     def advance(self, dt):
+        dump = self.dumping() and self.bDump(self.ctx.scalars())
         for op in self.pipeline:
             op(dt)
         self.ctx.end_step()
         st = self.ctx.scalars()
+        if dump:                               # Simulation.cpp:293-297
+            self.next_dump_time += self.dumps["tdump"]
+            self.ctx.dump(self.dumps["dir"], "avemaria_")
         return self.bOver(st)
 
     def bOver(self, st=None):  # SimulationData.cpp:172-177
@@ -464,7 +504,7 @@ class Simulation:
         or operator by operator with -iterativePenalization."""
         if self.cfg.nsteps <= 0:
             raise Cup2DError(EINVAL, "simulate() needs -nsteps")
-        if self.cfg.iterative:                 # converges on the host: operator by operator
+        if self.cfg.iterative or self.dumping():   # host decisions between steps
             for _ in range(self.cfg.nsteps + 1):
                 self.advance(self.calcMaxTimestep())
         else:

@@ -1826,3 +1826,76 @@ int cup2d_fish_state(cup2d_ctx* ctx, int id, int other, double* out, int n) {
 }
 
 } // extern "C"
+
+// ---- field dumps --------------------------------------------------------------
+// SimulationData::dumpAll (SimulationData.cpp:207-239): velChi (u, v, chi),
+// pres and invRho as single-precision fields, named like DumpHDF5's files
+// (prefix + name + the step in seven digits).  HDF5 is not available here,
+// so each field is a raw little-endian float32 array (Ny x Nx x channels,
+// x fastest) described by an XDMF file that visualisation tools read.
+namespace {
+
+bool write_file(const std::string& path, const void* data, size_t bytes) {
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) return false;
+  const bool ok = std::fwrite(data, 1, bytes, f) == bytes;
+  return std::fclose(f) == 0 && ok;
+}
+
+bool write_xmf(const std::string& path, const std::string& raw, const char* attr, int channels,
+               int nx, int ny, double h, double time) {
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) return false;
+  const char* type = channels == 1 ? "Scalar" : "Vector";
+  std::fprintf(f,
+      "<?xml version=\"1.0\" ?>\n<!DOCTYPE Xdmf SYSTEM \"Xdmf.dtd\" []>\n<Xdmf Version=\"2.0\">\n"
+      " <Domain>\n  <Grid GridType=\"Uniform\">\n   <Time Value=\"%.17g\"/>\n"
+      "   <Topology TopologyType=\"2DCoRectMesh\" Dimensions=\"%d %d\"/>\n"
+      "   <Geometry GeometryType=\"ORIGIN_DXDY\">\n"
+      "    <DataItem Dimensions=\"2\" NumberType=\"Float\" Precision=\"8\" Format=\"XML\">0 0</DataItem>\n"
+      "    <DataItem Dimensions=\"2\" NumberType=\"Float\" Precision=\"8\" Format=\"XML\">%.17g %.17g</DataItem>\n"
+      "   </Geometry>\n"
+      "   <Attribute Name=\"%s\" AttributeType=\"%s\" Center=\"Cell\">\n"
+      "    <DataItem Dimensions=\"%d %d %d\" NumberType=\"Float\" Precision=\"4\" Endian=\"Little\" "
+      "Format=\"Binary\">%s</DataItem>\n"
+      "   </Attribute>\n  </Grid>\n </Domain>\n</Xdmf>\n",
+      time, ny + 1, nx + 1, h, h, attr, type, ny, nx, channels, raw.c_str());
+  return std::fclose(f) == 0;
+}
+
+} // namespace
+
+extern "C" int cup2d_dump(cup2d_ctx* ctx, const char* dir, const char* name) {
+  if (!ctx || !dir || !name) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
+  Scalars sc;
+  CK(cudaStreamSynchronize(c.stream));
+  CK(cudaMemcpy(&sc, c.dsc, sizeof(Scalars), cudaMemcpyDeviceToHost));
+  const size_t n = c.ncells();
+  std::vector<double> u(n), v(n), chi(n), p(n);
+  CK(cudaMemcpy(u.data(), c.u(), sizeof(double) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(v.data(), c.v(), sizeof(double) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(chi.data(), c.chi, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(p.data(), c.pres, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  char step[16];
+  std::snprintf(step, sizeof(step), "%07d", sc.step);
+  const std::string base = std::string(dir) + (dir[0] && dir[std::strlen(dir) - 1] != '/' ? "/" : "");
+  const std::string tag = std::string(name) + step;
+  std::vector<float> buf(3 * n);
+  for (size_t i = 0; i < n; i++) {                    // StreamerGlue (Definitions.h:210-227)
+    buf[3 * i] = (float)u[i]; buf[3 * i + 1] = (float)v[i]; buf[3 * i + 2] = (float)chi[i];
+  }
+  struct Out { std::string stem; int ch; };
+  const Out outs[3] = {{"velChi_" + tag, 3}, {"pres_" + tag, 1}, {"invRho_" + tag, 1}};
+  for (int k = 0; k < 3; k++) {
+    if (k == 1) for (size_t i = 0; i < n; i++) buf[i] = (float)p[i];
+    if (k == 2) for (size_t i = 0; i < n; i++) buf[i] = 1.0f;   // constant density: invRho = 1
+    const std::string raw = outs[k].stem + ".raw";
+    if (!write_file(base + raw, buf.data(), sizeof(float) * n * outs[k].ch) ||
+        !write_xmf(base + outs[k].stem + ".xmf", raw, k == 0 ? "velChi" : k == 1 ? "pres" : "invRho",
+                   outs[k].ch, c.g.nx, c.g.ny, c.g.h, sc.time))
+      return fail(ctx, CUP2D_EINVAL, "cannot write " + base + raw);
+  }
+  return CUP2D_OK;
+}

@@ -228,6 +228,17 @@ int cup2d_time_kernel(cup2d_ctx* ctx, int which, int reps, int flush_l2, double*
  * milliseconds (synchronises). */
 int cup2d_advance_timed(cup2d_ctx* ctx, int nsteps, double* ms);
 
+/* ---- field dumps ------------------------------------------------------- */
+/* SimulationData::dumpAll (SimulationData.cpp:207-239) as the constant-
+ * density pipeline calls it (Simulation.cpp:229, 282-297): velChi (u, v,
+ * chi), pres and invRho in single precision into directory `dir`, named
+ * "velChi_" name step (seven digits) and so on, as DumpHDF5 names its
+ * files.  HDF5 is not available to this library: each field is a raw
+ * little-endian float32 array (Ny x Nx x channels, x fastest, ".raw") with
+ * an XDMF description (".xmf": cell-centred 2DCoRectMesh, spacing h) that
+ * visualisation tools read.  Synchronises. */
+int cup2d_dump(cup2d_ctx* ctx, const char* dir, const char* name);
+
 /* ---- checkpoint / restart ---------------------------------------------- */
 /* The reference parses -restart but restores nothing (Simulation.cpp:68);
  * these calls save and restore the whole state a step carries to the next:
