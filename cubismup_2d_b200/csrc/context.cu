@@ -451,6 +451,7 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   for (int d = 0; d < 2; d++) { cudaFree(c.itmp[d]); cudaFree(c.ifluid[d]); }
   cudaFree(c.counters); cudaFree(c.partials); cudaFree(c.fadeSlot);
   if (c.flushBuf) cudaFree(c.flushBuf);
+  if (c.hashAcc) cudaFree(c.hashAcc);
   if (c.side) cudaStreamDestroy(c.side);
   if (c.side2) cudaStreamDestroy(c.side2);
   if (c.evObj) cudaEventDestroy(c.evObj);
@@ -1372,8 +1373,41 @@ struct CkptHeader {
   uint32_t version, nsections;
   int32_t bpdx, bpdy, poisson, precision, nshapes, reserved;
   double extent, CFL, lambda, dlm, nu, fadeLen;
+  uint64_t checksum;              // ckpt_hash over the sections (0 in the comparison copy)
 };
-constexpr uint32_t CKPT_VERSION = 2;
+constexpr uint32_t CKPT_VERSION = 3;
+
+// The payload checksum: over each section's 8-byte words (the last one
+// zero-padded), the sum modulo 2^64 of SplitMix64 of the word mixed with its
+// section and word index.  A sum is independent of the order the words are
+// added in, so the device (a grid of atomic adds) and the host (a loop) form
+// the same value.
+__host__ __device__ inline uint64_t ckpt_mix(uint64_t w, uint64_t sec, uint64_t idx) {
+  uint64_t z = w ^ ((sec << 40) + idx) * 0x9E3779B97F4A7C15ull;
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+__host__ __device__ inline uint64_t ckpt_word(const unsigned char* p, size_t bytes, size_t w) {
+  uint64_t v = 0;
+  const size_t o = 8 * w, n = bytes - o < 8 ? bytes - o : 8;
+  for (size_t k = 0; k < n; k++) v |= (uint64_t)p[o + k] << (8 * k);
+  return v;
+}
+__global__ void k_ckpt_hash(const unsigned char* p, size_t bytes, uint64_t sec, unsigned long long* out) {
+  const size_t nw = (bytes + 7) / 8;
+  unsigned long long acc = 0;
+  for (size_t w = blockIdx.x * (size_t)blockDim.x + threadIdx.x; w < nw; w += (size_t)gridDim.x * blockDim.x)
+    acc += ckpt_mix(ckpt_word(p, bytes, w), sec, w);
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, acc);
+}
+uint64_t ckpt_hash_host(const unsigned char* p, size_t bytes, uint64_t sec) {
+  uint64_t acc = 0;
+  for (size_t w = 0; w < (bytes + 7) / 8; w++) acc += ckpt_mix(ckpt_word(p, bytes, w), sec, w);
+  return acc;
+}
 constexpr char CKPT_MAGIC[8] = {'C', 'U', 'P', '2', 'D', 'C', 'K', 0};
 
 struct CkptSection { void* p; size_t bytes; };
@@ -1420,6 +1454,36 @@ size_t ckpt_total(const Ctx& c, const std::vector<CkptSection>& s) {
   return b;
 }
 
+// Checksum of sections (device pointers, or host pointers when onHost).
+int ckpt_hash(cup2d_ctx* ctx, const std::vector<CkptSection>& secs, bool onHost, uint64_t* out) {
+  Ctx& c = ctx->c;
+  if (onHost) {
+    uint64_t h = 0;
+    for (size_t i = 0; i < secs.size(); i++)
+      h += ckpt_hash_host(static_cast<const unsigned char*>(secs[i].p), secs[i].bytes, i);
+    *out = h;
+    return CUP2D_OK;
+  }
+  if (!c.hashAcc && cudaMalloc(&c.hashAcc, sizeof(unsigned long long)) != cudaSuccess) {
+    c.hashAcc = nullptr;
+    return fail(ctx, CUP2D_ENOMEM, "checkpoint checksum accumulator");
+  }
+  unsigned long long* d = c.hashAcc;
+  CK(cudaMemsetAsync(d, 0, sizeof(unsigned long long), c.stream));
+  for (size_t i = 0; i < secs.size(); i++) {
+    const size_t nw = (secs[i].bytes + 7) / 8;
+    if (!nw) continue;
+    int grid = (int)std::min<size_t>((nw + 255) / 256, (size_t)4 * c.sms);
+    k_ckpt_hash<<<grid, 256, 0, c.stream>>>(static_cast<const unsigned char*>(secs[i].p), secs[i].bytes, i, d);
+    CK(cudaGetLastError());
+  }
+  unsigned long long h = 0;
+  CK(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  *out = h;
+  return CUP2D_OK;
+}
+
 // nothing in flight may write the buffers while they are copied
 int ckpt_quiesce(cup2d_ctx* ctx) {
   Ctx& c = ctx->c;
@@ -1451,7 +1515,8 @@ int cup2d_checkpoint_save(cup2d_ctx* ctx, void* buf, size_t bytes) {
   int rc = ckpt_quiesce(ctx);
   if (rc) return rc;
   char* out = static_cast<char*>(buf);
-  const CkptHeader h = ckpt_header(c, secs.size());
+  CkptHeader h = ckpt_header(c, secs.size());
+  if ((rc = ckpt_hash(ctx, secs, false, &h.checksum))) return rc;
   std::vector<ShapeCfg> cfgs(c.nshapes);
   for (int k = 0; k < c.nshapes; k++) cfgs[k] = c.hshapes[k].cfg;
   std::vector<uint64_t> sizes(secs.size());
@@ -1482,6 +1547,8 @@ int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes) {
   CK(cudaMemcpy(&h, in, sizeof(h), cudaMemcpyDefault));
   if (std::memcmp(h.magic, CKPT_MAGIC, sizeof(h.magic)) != 0) return fail(ctx, CUP2D_EINVAL, "not a checkpoint");
   if (h.version != CKPT_VERSION) return fail(ctx, CUP2D_ENOTSUP, "checkpoint version not supported");
+  const uint64_t stored = h.checksum;
+  h.checksum = 0;
   const CkptHeader mine = ckpt_header(c, secs.size());
   if (std::memcmp(&h, &mine, sizeof(h)) != 0)
     return fail(ctx, CUP2D_EINVAL, "checkpoint of another configuration (grid, solver, precision, parameters or shapes)");
@@ -1500,6 +1567,19 @@ int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes) {
     if (sizes[i] != secs[i].bytes) return fail(ctx, CUP2D_EINVAL, "checkpoint section sizes differ");
   int rc = ckpt_quiesce(ctx);
   if (rc) return rc;
+  {
+    // the payload's checksum, read where the buffer lies, before anything is written
+    cudaPointerAttributes pa{};
+    const bool onDevice = cudaPointerGetAttributes(&pa, in) == cudaSuccess &&
+                          (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged);
+    cudaGetLastError();
+    std::vector<CkptSection> src(secs.size());
+    size_t o = off;
+    for (size_t i = 0; i < secs.size(); i++) { src[i] = {const_cast<char*>(in) + o, secs[i].bytes}; o += secs[i].bytes; }
+    uint64_t sum = 0;
+    if ((rc = ckpt_hash(ctx, src, !onDevice, &sum))) return rc;
+    if (sum != stored) return fail(ctx, CUP2D_EINVAL, "checkpoint payload damaged (checksum differs)");
+  }
   for (const CkptSection& x : secs) {
     CK(cudaMemcpy(x.p, in + off, x.bytes, cudaMemcpyDefault));
     off += x.bytes;

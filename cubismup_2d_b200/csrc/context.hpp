@@ -115,6 +115,7 @@ struct Ctx {
 
   cudaGraphExec_t graph = nullptr;
   void* flushBuf = nullptr;      // cup2d_time_kernel's L2 flush (256 MB, allocated on demand)
+  unsigned long long* hashAcc = nullptr;   // checkpoint checksum accumulator (on demand)
   unsigned graphGen = 0;        // bumped whenever what a step captures changes
   long long launches = 0;
   int launchesInGraph = 0;

@@ -249,10 +249,13 @@ int cup2d_dump(cup2d_ctx* ctx, const char* dir, const char* name);
  *    cudaMemcpyDefault); cup2d_checkpoint_size gives its size;
  *  - save: between steps only (CUP2D_ESTATE after a lone advDiff);
  *    synchronises the context;
+ *  - the header carries a 64-bit checksum of the payload (formed on the
+ *    device at save, checked where the buffer lies at load);
  *  - load: into an initialised context of the same configuration and
  *    shapes (the saved one, or a new one built alike); anything else, a
- *    truncated buffer or a foreign one returns CUP2D_EINVAL (a newer format
- *    CUP2D_ENOTSUP) without changing the context; synchronises. */
+ *    truncated, damaged (checksum) or foreign buffer returns CUP2D_EINVAL
+ *    (another format version CUP2D_ENOTSUP) without changing the context;
+ *    synchronises. */
 int cup2d_checkpoint_size(cup2d_ctx* ctx, size_t* bytes);
 int cup2d_checkpoint_save(cup2d_ctx* ctx, void* buf, size_t bytes);
 int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes);

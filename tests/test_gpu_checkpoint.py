@@ -122,4 +122,17 @@ def test_foreign_or_truncated_checkpoints_are_refused():
         a.ctx.restore(blob[: blob.nbytes - 8])
     with pytest.raises(Cup2DError):
         a.ctx.restore(np.zeros(blob.nbytes, dtype=np.uint8))
+    # a damaged payload (one byte of the last section, a field, flipped):
+    # refused by the checksum, in host memory and in device memory
+    bad = blob.copy()
+    bad[-5] ^= 0x10
+    with pytest.raises(Cup2DError) as e:
+        a.ctx.restore(bad)
+    assert "checksum" in str(e.value)
+    import torch
+    dbad = torch.from_numpy(bad).cuda()
+    with pytest.raises(Cup2DError):
+        a.ctx.restore(dbad)
     _assert_same(before, _state(a), "refused")
+    a.ctx.restore(torch.from_numpy(blob).cuda())      # the intact blob, from device memory
+    _assert_same(before, _state(a), "restored")
