@@ -63,7 +63,8 @@ class ShapeParams(ctypes.Structure):
                 ("bForcedy", ctypes.c_int), ("bBlockAng", ctypes.c_int), ("xvel", ctypes.c_double),
                 ("yvel", ctypes.c_double), ("angvel", ctypes.c_double), ("timeForced", ctypes.c_double),
                 ("radius", ctypes.c_double), ("tAccel", ctypes.c_double), ("L", ctypes.c_double),
-                ("T", ctypes.c_double), ("phi", ctypes.c_double), ("amplitudeFactor", ctypes.c_double)]
+                ("T", ctypes.c_double), ("phi", ctypes.c_double), ("amplitudeFactor", ctypes.c_double),
+                ("pid", ctypes.c_int), ("pidpos", ctypes.c_int)]
 
 
 SHAPE_STATE_FIELDS = [
@@ -228,9 +229,9 @@ def parse_args(argline):
                 if key in kv:
                     v = kv[key]
                     setattr(sp, key, 1 if v in ("1", "true", "True") else (0 if v in ("0", "false", "False") else int(v) != 0))
-            for key in ("pid", "pidpos"):
-                if key in kv and int(kv[key]) != 0:
-                    raise Cup2DError(ENOTSUP, "the fish PID controllers are not available")
+            for key in ("pid", "pidpos"):                  # StefanFish.cpp:209-211
+                if key in kv:
+                    setattr(sp, key, int(kv[key]) != 0)
             shapes.append((SHAPE_KINDS[name], sp))
     return cfg, shapes
 

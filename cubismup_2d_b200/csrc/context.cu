@@ -196,25 +196,32 @@ void launch_pressure_tail(Ctx& c) {
 void enqueue_step(Ctx& c) {
   struct GraphStepFlag { Ctx& c; explicit GraphStepFlag(Ctx& cc) : c(cc) { c.graphStep = true; }
                          ~GraphStepFlag() { c.graphStep = false; } } flag(c);
-  bool anyFish = false;
-  for (int k = 0; k < c.nshapes; k++) anyFish |= c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK;
-  if (anyFish) {
+  bool anyFish = false, anyAhead = false;
+  for (int k = 0; k < c.nshapes; k++) {
+    anyFish |= c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK;
+    anyAhead |= midline_ahead(c, k);
+  }
+  if (anyAhead) {
     // the next step's midlines depend on time only: with a carried dt they
     // start with the graph, beside the step's own start
     cudaEventRecord(c.evStart, c.stream);
     cudaStreamWaitEvent(c.side, c.evStart, 0);
     for (int k = 0; k < c.nshapes; k++)
-      if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.side, 2);
+      if (midline_ahead(c, k)) launch_fish_midline(c, k, c.side, 2);
   }
   launch_step_begin(c);                     // dt, last step's tiles reset, body motion
   cudaEventRecord(c.evFork, c.stream);
-  if (anyFish) {
+  if (anyAhead) {
     // otherwise once the step has its dt
     cudaStreamWaitEvent(c.side, c.evFork, 0);
     for (int k = 0; k < c.nshapes; k++)
-      if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.side, 3);
+      if (midline_ahead(c, k)) launch_fish_midline(c, k, c.side, 3);
     cudaEventRecord(c.evJoin, c.side);
   }
+  // a swimmer under PID control forms its midline within the step, after
+  // the controller has run (StefanFish::create)
+  for (int k = 0; k < c.nshapes; k++)
+    if (midline_in_step(c, k)) launch_fish_midline(c, k, c.stream, 0);
   // the obstacle chain, the step's critical path, stays on the main stream
   // (programmatic launches chain only within a stream)
   // advDiff and the RHS divergence beside the obstacle chain: with a fish,
@@ -238,7 +245,7 @@ void enqueue_step(Ctx& c) {
   poisson_solve(c);
   launch_pressure_tail(c);
   launch_forces(c, c.forcesOut);
-  if (anyFish) cudaStreamWaitEvent(c.stream, c.evJoin, 0);
+  if (anyAhead) cudaStreamWaitEvent(c.stream, c.evJoin, 0);
   cudaStreamWaitEvent(c.stream, c.evMaxFree, 0);
   launch_end_step_dt(c);                    // t += dt, and the next step's dt
 }
@@ -524,6 +531,9 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
   f.origAng = p->angle * M_PI / 180;
   f.radius = p->radius; f.tAccel = p->tAccel;
   f.length = p->L; f.Tperiod = p->T; f.phaseShift = p->phi; f.ampFac = p->amplitudeFactor;
+  const bool curvatureFish = kind == CUP2D_SHAPE_STEFANFISH || kind == CUP2D_SHAPE_ENVELOPEFISH;
+  f.pid = curvatureFish && p->pid != 0;             // other shapes ignore -pid (StefanFish.cpp:209-211)
+  f.pidpos = curvatureFish && p->pidpos != 0;
   const double h = c.g.h;
   double span;
   if (kind == CUP2D_SHAPE_DISK) span = 2 * (f.radius + 2 * h);
@@ -761,10 +771,12 @@ int cup2d_put_objects(cup2d_ctx* ctx, double dt) {
   }
   // the next step's midlines on the side stream, beside the rest of this
   // step; the next call takes them if the time matches
-  if (anyFishShape) {
+  bool anyAhead = false;
+  for (int k = 0; k < c.nshapes; k++) anyAhead |= midline_ahead(c, k);
+  if (anyAhead) {
     CK(cudaStreamWaitEvent(c.side, c.evFork, 0));
     for (int k = 0; k < c.nshapes; k++)
-      if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.side, 1);
+      if (midline_ahead(c, k)) launch_fish_midline(c, k, c.side, 1);
     CK(cudaEventRecord(c.evSideMid, c.side));
     c.sideMidPending = true;
   }
@@ -868,7 +880,7 @@ int graph_steps_begin(cup2d_ctx* ctx) {
     // graph steps form each next step's midline; the first one needs the
     // current step's (formed here unless already present)
     for (int k = 0; k < c.nshapes; k++)
-      if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.stream, 4);
+      if (midline_ahead(c, k)) launch_fish_midline(c, k, c.stream, 4);
     c.midByGraph = true;
   }
   return check_launch(ctx);

@@ -128,6 +128,16 @@ struct Ctx {
   size_t ncells() const { return (size_t)g.nx * g.ny; }
 };
 
+// A swimmer whose midline depends on time only is formed a step ahead (on a
+// side branch); one under PID control depends on the body's state at the
+// step's start and is formed within the step, after the controller.
+inline bool midline_in_step(const Ctx& c, int k) {
+  return c.hshapes[k].cfg.pid || c.hshapes[k].cfg.pidpos;
+}
+inline bool midline_ahead(const Ctx& c, int k) {
+  return c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK && !midline_in_step(c, k);
+}
+
 // doubles behind one fish's arrays (FishArrays::pool): the static profile,
 // two midline buffers, the frame midline, the integrals, then the skins of
 // the two midline buffers

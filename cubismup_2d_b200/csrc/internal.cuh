@@ -78,6 +78,7 @@ struct ShapeCfg {
   double length, Tperiod, phaseShift, ampFac;     // Fish
   int capacity;                                   // obstacle tile slots
   int nm;                                         // fish midline points
+  int pid, pidpos;                                // StefanFish -pid / -pidpos (StefanFish.cpp:209-211)
 };
 
 // Fish frame bookkeeping (Fish.h:21-23).
@@ -99,6 +100,8 @@ struct FishCtl {
   double periodPIDval, periodPIDdif, time0, timeshift;
   double pidFac, pidDif;
   double lastTact, lastCurv, oldrCurv;
+  // the PID controllers' exponential averages and memory (StefanFish.cpp:24-41)
+  double avgDeltaY, avgDangle, avgAngVel, lastTime, lastAvel;
   int TperiodPID;
 };
 

@@ -706,7 +706,8 @@ void launch_objects_begin(Ctx& c, bool midlineReady) {
       c.sideMidPending = false;
     }
     for (int k = 0; k < c.nshapes; k++)
-      if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK) launch_fish_midline(c, k, c.stream, 4);
+      if (c.hshapes[k].cfg.kind != CUP2D_SHAPE_DISK)
+        launch_fish_midline(c, k, c.stream, midline_in_step(c, k) ? 0 : 4);
   }
 }
 

@@ -99,9 +99,75 @@ __device__ __forceinline__ bool max_u_dt_cta(const GridDesc& g, Scalars* sc, con
   return true;
 }
 
+// The PID controllers of StefanFish::create (StefanFish.cpp:264-364), run
+// after every body has moved and before the midline of this step is formed:
+// exponential averages of the lateral offset, the angle and the angular
+// velocity, then the curvature correction (-pid: the angle; -pidpos: the
+// position, also through the tail period).
+__device__ __forceinline__ void fish_pid(const Scalars* sc, DevShape& S)
+{
+  FishCtl& C = S.ctl;
+  const ShapeCfg& f = S.cfg;
+  const double Tperiod = f.Tperiod, length = f.length;
+  const double DT = sc->dt / Tperiod, time = sc->time;
+  const double xDiff = (S.s.com[0] - f.origC[0]) / length;
+  const double yDiff = (S.s.com[1] - f.origC[1]) / length;
+  const double angDiff = S.s.orientation - f.origAng;
+  const double relU = (S.s.u + sc->uinfx) / length;
+  const double relV = (S.s.v + sc->uinfy) / length;
+  const double angVel = S.s.omega, lastAngVel = C.lastAvel;
+  const double aVelMidP = (angVel + lastAngVel) * Tperiod / 2;
+  const double aVelDiff = (angVel - lastAngVel) * Tperiod / sc->dt;
+  C.lastAvel = angVel;
+  const double velDAavg = (angDiff - C.avgDangle) / Tperiod + DT * angVel;
+  const double velDYavg = (yDiff - C.avgDeltaY) / Tperiod + DT * relV;
+  const double velAVavg = 10 * ((aVelMidP - C.avgAngVel) / Tperiod + DT * aVelDiff);
+  C.avgDangle = (1.0 - DT) * C.avgDangle + DT * angDiff;
+  C.avgDeltaY = (1.0 - DT) * C.avgDeltaY + DT * yDiff;
+  C.avgAngVel = (1 - 10 * DT) * C.avgAngVel + 10 * DT * aVelMidP;
+  const double avgDangle = C.avgDangle, avgDeltaY = C.avgDeltaY;
+  const double absPy = fabs(yDiff), absIy = fabs(avgDeltaY);
+  const double velAbsPy = yDiff > 0 ? relV : -relV;
+  const double velAbsIy = avgDeltaY > 0 ? velDYavg : -velDYavg;
+  if (f.pidpos && sc->dt > 0) {
+    const double IangPdy = (avgDangle * yDiff < 0) ? avgDangle * absPy : 0;
+    const double PangIdy = (angDiff * avgDeltaY < 0) ? angDiff * absIy : 0;
+    const double IangIdy = (avgDangle * avgDeltaY < 0) ? avgDangle * absIy : 0;
+    const double velIangPdy = velAbsPy * avgDangle + absPy * velDAavg;
+    const double velPangIdy = velAbsIy * angDiff + absIy * angVel;
+    const double velIangIdy = velAbsIy * avgDangle + absIy * velDAavg;
+    const double coefIangPdy = avgDangle * yDiff < 0 ? 1 : 0;
+    const double coefPangIdy = angDiff * avgDeltaY < 0 ? 1 : 0;
+    const double coefIangIdy = avgDangle * avgDeltaY < 0 ? 1 : 0;
+    const double valIangPdy = coefIangPdy * IangPdy, difIangPdy = coefIangPdy * velIangPdy;
+    const double valPangIdy = coefPangIdy * PangIdy, difPangIdy = coefPangIdy * velPangIdy;
+    const double valIangIdy = coefIangIdy * IangIdy, difIangIdy = coefIangIdy * velIangIdy;
+    const double periodFac = 1.0 - xDiff, periodVel = -relU;
+    C.pidFac = valIangPdy + valPangIdy + valIangIdy;      // correctTrajectory
+    C.pidDif = difIangPdy + difPangIdy + difIangIdy;
+    // correctTailPeriod (StefanFish.cpp:92-106)
+    const double lastArg = (C.lastTime - C.time0) / C.periodPIDval + C.timeshift;
+    C.time0 = C.lastTime;
+    C.timeshift = lastArg;
+    C.periodPIDval = Tperiod * periodFac;
+    C.periodPIDdif = Tperiod * periodVel;
+    C.lastTime = time;
+    C.TperiodPID = 1;
+  } else if (f.pid && sc->dt > 0) {
+    const double avgAngVel = C.avgAngVel, absAngVel = fabs(avgAngVel);
+    const double absAvelDiff = avgAngVel > 0 ? velAVavg : -velAVavg;
+    const double coefInst = angDiff * avgAngVel > 0 ? 0.01 : 1, coefAvg = 0.1;
+    const double termInst = angDiff * absAngVel;
+    const double diffInst = angDiff * absAvelDiff + angVel * absAngVel;
+    C.pidFac = coefInst * termInst + coefAvg * avgDangle;
+    C.pidDif = coefInst * diffInst + coefAvg * velDAavg;
+  }
+}
+
 // PutObjectsOnGrid.cpp:201-220 (one thread): lab velocity from fixed
 // bodies, then Shape::updatePosition; a body whose centre leaves the domain
-// raises ST_DOMAIN (the reference exits).
+// raises ST_DOMAIN (the reference exits).  Then the PID controllers of the
+// swimmers that have them (StefanFish::create runs after every body moved).
 __device__ __forceinline__ void bodies_motion(const GridDesc& g, Scalars* sc, DevShape* sh, int nsh)
 {
   const double dt = sc->dt;
@@ -124,6 +190,8 @@ __device__ __forceinline__ void bodies_motion(const GridDesc& g, Scalars* sc, De
       S.bbox[1][0] = p1 - R - safety; S.bbox[1][1] = p1 + R + safety;
     }
   }
+  for (int k = 0; k < nsh; k++)
+    if (sh[k].cfg.pid || sh[k].cfg.pidpos) fish_pid(sc, sh[k]);
 }
 
 // Reset the grid cells of last step's tiles of every shape, chi = 0

@@ -103,6 +103,7 @@ typedef struct cup2d_shape_params {
   /* fish */
   double L, T, phi;        /* -L (0.1), -T (1), -phi (0)                       */
   double amplitudeFactor;  /* -amplitudeFactor (1)                             */
+  int pid, pidpos;         /* StefanFish -pid / -pidpos controllers (0)         */
 } cup2d_shape_params;
 
 #define CUP2D_SHAPE_DISK 0

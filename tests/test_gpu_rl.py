@@ -90,3 +90,46 @@ def test_lead_follow_driver_matches_the_reference_loop(ref):
         rb = r.shape(1)["EffPDefBnd"]
         assert abs(reward - rb) <= 1e-8 * max(abs(rb), 1.0), (reward, rb)
         assert not done and info["reason"] == "running"
+
+
+PID = ("-bpdx 8 -bpdy 4 -extent 1 -CFL 0.1 -nu 1e-4 -poissonType freespace -muteAll 1 "
+       "-shapes 'stefanfish L=0.18 T=1 xpos=0.4 ypos=0.25 angle=4 {}=1'")
+
+
+@pytest.mark.parametrize("flag", ["pid", "pidpos"])
+def test_pid_controllers_match_reference(ref, flag):
+    """StefanFish::create's controllers (StefanFish.cpp:264-364): -pid
+    corrects the heading, -pidpos the position (also through the tail
+    period).  30 operator steps against the reference, then graph steps
+    bitwise equal to operator steps (the midline is formed inside the
+    step, after the controller)."""
+    args = PID.format(flag)
+    r = ref.RefSim(args)
+    s = Simulation(args)
+    s.init()
+    for comp, f in enumerate(("u", "v")):
+        a = r.get(f) + noise_field(12, comp, r.ny, r.nx)
+        r.set(f, a)
+        s.ctx.set(f, a)
+    for _ in range(30):
+        dt_r = r.step()
+        dt_s = s.calcMaxTimestep()
+        s.advance(dt_s)
+        assert abs(dt_s - dt_r) <= 1e-12 * dt_r
+    a, b = s.ctx.shape(0), r.shape(0)
+    for key in ("com_x", "com_y", "orientation"):
+        assert abs(a[key] - b[key]) <= 1e-10, (key, a[key], b[key])
+    for f in ("u", "v", "pres", "chi"):
+        x, y = s.ctx.get(f), r.get(f)
+        assert np.max(np.abs(x - y)) <= 1e-8 * np.max(np.abs(y)), f
+    assert s.ctx.fish_period(0) == pytest.approx(r.fish_period(0), rel=1e-12, abs=0)
+    _state_close(s.ctx.fish_state(0, 0), r.fish_state(0, 0), flag)
+    g = Simulation(args); g.init()
+    o = Simulation(args); o.init()
+    g.ctx.advance(8)
+    for _ in range(8):
+        o.advance(o.calcMaxTimestep())
+    g.ctx.sync()
+    for f in ("u", "v", "chi"):
+        assert np.array_equal(g.ctx.get(f), o.ctx.get(f)), f
+    assert g.ctx.shape(0) == o.ctx.shape(0)
