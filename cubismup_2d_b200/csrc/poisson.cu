@@ -82,9 +82,15 @@ template <int L, int E = 16> struct Len {
 // of E = 16 for latency hiding, at one more shared-memory pass; measured
 // faster), of the inverse row pass and of the column pass (measured faster
 // with E = 16)
+#ifndef CUP2D_E_COLS
+#define CUP2D_E_COLS 16
+#endif
+#ifndef CUP2D_E_C2R
+#define CUP2D_E_C2R 16
+#endif
 constexpr int E_ROWS = 8;
-constexpr int E_C2R = 16;
-constexpr int E_COLS = 16;
+constexpr int E_C2R = CUP2D_E_C2R;
+constexpr int E_COLS = CUP2D_E_COLS;
 // the same for the FP32 transforms (half the registers per value)
 constexpr int E_ROWS32 = 8;
 constexpr int E_C2R32 = 8;
