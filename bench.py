@@ -56,13 +56,22 @@ WORKLOADS = {
                          "-muteAll 1 -shapes 'envelopefish L=0.2 T=1 xpos=0.4 ypos=0.25'"),
     # the large single-GPU case: 4096x2048 on a 2x1 domain, two swimmers
     # L = 0.1 in tandem 0.15 apart, a quarter period out of phase (phi = 0.5,
-    # the reference multiplies phi by pi), Re = 5000 on L; the falling
-    # cylinder of that case (density ratio 1.01) needs the variable-density
-    # pipeline, which this library does not build, so it is left out
+    # the reference multiplies phi by pi), Re = 5000 on L (graph steps)
     "tandem": ("tandem_swimmers_4096x2048_fp64",
                "-bpdx 128 -bpdy 64 -extent 2 -CFL 0.1 -nu 2e-6 -lambda 1e4 -poissonType freespace "
                "-muteAll 1 -shapes 'stefanfish L=0.1 T=1 xpos=0.6 ypos=0.5, "
                "stefanfish L=0.1 T=1 xpos=0.75 ypos=0.5 phi=0.5'"),
+    # ... with the freely falling cylinder of that case (R = 0.03, density
+    # ratio 1.01, gravity 1 in -y): a body of rhoS != 1 runs the reference's
+    # variable-density branch, which needs -iterativePenalization 1
+    # (advDiffGrav + PressureVarRho_approx, Simulation.cpp:183-192); its
+    # convergence is decided on the host each iteration, so operator steps
+    "tandem_falling": ("tandem_swimmers_falling_cylinder_4096x2048_fp64",
+                       "-bpdx 128 -bpdy 64 -extent 2 -CFL 0.1 -nu 2e-6 -lambda 1e4 -poissonType freespace "
+                       "-muteAll 1 -iterativePenalization 1 -gravity '0 -1' "
+                       "-shapes 'stefanfish L=0.1 T=1 xpos=0.6 ypos=0.5, "
+                       "stefanfish L=0.1 T=1 xpos=0.75 ypos=0.5 phi=0.5, "
+                       "disk radius=0.03 xpos=1.4 ypos=0.7 rhoS=1.01'"),
 }
 
 ENSEMBLE_NAME = "ensemble{}_seed0_fp64"
@@ -451,6 +460,49 @@ def cufft_comparison(ctx, flush, reps=20):
 LARGE_CASE = "tandem"
 
 
+def operator_steps(sim, steps, pg):
+    """Steps through the operator path (calcMaxTimestep, the four operators,
+    end_step), as Simulation::advance calls them; the iterated operators read
+    each iteration's change back, so the host waits on the device inside
+    every step anyway.  Returns (host ms of the K steps after a device
+    synchronisation on both sides, iterations per step)."""
+    import torch
+    its = []
+    if pg is not None:
+        pg.barrier()
+    sim.ctx.sync()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dt = sim.calcMaxTimestep()
+        for op in sim.pipeline:
+            op(dt)
+        sim.ctx.end_step()
+        its.append(sim.ctx.iteration_stats()[0])
+    sim.ctx.sync()
+    torch.cuda.synchronize()
+    return (time.perf_counter() - t0) * 1e3, its
+
+
+def falling_measurement(local, rank, pg, warmup=3, steps=6):
+    """The large case with its falling cylinder (variable density)."""
+    name, argline = WORKLOADS["tandem_falling"]
+    sim = make_sim(argline, local, rank)
+    cells = sim.ctx.nx * sim.ctx.ny
+    _, its_w = operator_steps(sim, warmup, pg)
+    ms, its = operator_steps(sim, steps, pg)
+    ms = max_over_ranks(pg, ms)
+    out = {"workload": name, "value": cells * steps / (ms / 1e3) / 1e9, "unit": "Gcell-steps/s",
+           "ms_per_step": ms / steps, "steps": steps, "warmup": warmup,
+           "iterations_per_step": its, "iterations_warmup": its_w,
+           "pipeline": [op.name for op in sim.pipeline],
+           "timing": "host clock around K operator steps, device synchronised on both sides "
+                     "(the iterated operator synchronises every iteration)",
+           "disk_v_after": sim.ctx.shape(2)["v"]}
+    del sim
+    return out
+
+
 def run_ours(args, world, rank, local, pg):
     import torch
     name, argline = WORKLOADS[args.workload]
@@ -529,6 +581,9 @@ def run_ours(args, world, rank, local, pg):
         if not args.no_cufft:
             roof_large["cufft"] = cufft_comparison(big.ctx, flush)
         del big
+    falling = None
+    if not args.no_large and not args.no_falling:
+        falling = falling_measurement(local, rank, pg)
 
     line = None
     if rank == 0:
@@ -559,6 +614,7 @@ def run_ours(args, world, rank, local, pg):
             "roofline_large": roof_large,
             "poisson_vs_cufft": cufft,
             "fp32": fp32,
+            "falling_cylinder_large": falling,
             "cpu_baseline": cpu,
         }
     return line
@@ -675,7 +731,9 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="swimmer", choices=sorted(WORKLOADS) + ["ensemble"])
+    # (tandem_falling is measured beside the headline: its steps are not graph steps)
+    ap.add_argument("--workload", default="swimmer",
+                    choices=sorted(k for k in WORKLOADS if k != "tandem_falling") + ["ensemble"])
     ap.add_argument("--members", type=int, default=64, help="ensemble members (--workload ensemble)")
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -684,6 +742,8 @@ def main():
     ap.add_argument("--fp32-report-steps", type=int, default=2000,
                     help="steps of the FP32-against-FP64 error report (0: skip)")
     ap.add_argument("--no-cufft", action="store_true", help="skip the cuFFT comparison")
+    ap.add_argument("--no-falling", action="store_true",
+                    help="skip the 4096x2048 case with the falling cylinder (variable density)")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     if args.impl == "reference":

@@ -6,7 +6,9 @@ ctypes binding that mirrors the reference's Simulation/Operator interface
 (abi.py).
 """
 from .abi import (Context, Simulation, Operator, PutObjectsOnGrid, advDiff, PressureSingle,
-                  ComputeForces, Cup2DError, Ensemble, parse_args, lib, LIB_PATH, EXPORTS)
+                  PressureIterator_unif, advDiffGrav, PressureVarRho_approx, ComputeForces,
+                  Cup2DError, Ensemble, parse_args, lib, LIB_PATH, EXPORTS)
 
 __all__ = ["Context", "Simulation", "Operator", "PutObjectsOnGrid", "advDiff", "PressureSingle",
-           "ComputeForces", "Cup2DError", "Ensemble", "parse_args", "lib", "LIB_PATH", "EXPORTS"]
+           "PressureIterator_unif", "advDiffGrav", "PressureVarRho_approx", "ComputeForces",
+           "Cup2DError", "Ensemble", "parse_args", "lib", "LIB_PATH", "EXPORTS"]

@@ -25,7 +25,7 @@ ERRORS = {EINVAL: "EINVAL", ECUDA: "ECUDA", ENAN: "ENAN", EDOMAIN: "EDOMAIN",
           ETOOLARGE: "ETOOLARGE", ETIMEOUT: "ETIMEOUT"}
 POISSON = {"freespace": 0, "periodic": 1, "": 2, "cosine": 2}
 PREC_FP64, PREC_FP32 = 0, 1
-FIELDS = {"u": 0, "v": 1, "chi": 2, "pres": 3, "tmp": 4, "udef_x": 5, "udef_y": 6, "sdf": 7}
+FIELDS = {"u": 0, "v": 1, "chi": 2, "pres": 3, "tmp": 4, "udef_x": 5, "udef_y": 6, "sdf": 7, "invRho": 8}
 SHAPE_KINDS = {"disk": 0, "stefanfish": 1, "carlingfish": 2, "envelopefish": 3}
 
 # the exported entry points, in include/cup2d.h order
@@ -41,7 +41,7 @@ EXPORTS = [
     "cup2d_ensemble_create", "cup2d_ensemble_advance", "cup2d_ensemble_advance_timed",
     "cup2d_ensemble_sync", "cup2d_ensemble_get_shapes", "cup2d_ensemble_last_error",
     "cup2d_ensemble_destroy",
-    "cup2d_fish_act", "cup2d_fish_period", "cup2d_fish_state", "cup2d_dump",
+    "cup2d_fish_act", "cup2d_fish_period", "cup2d_fish_state", "cup2d_dump", "cup2d_poisson_solve",
     "cup2d_adv_diff_noalloc",
 ]
 KERNELS = {"advdiff": 0, "rhs_div": 1, "pcorr": 2, "fft_rows_fwd": 3, "fft_cols": 4,
@@ -53,7 +53,8 @@ class Config(ctypes.Structure):
                 ("CFL", ctypes.c_double), ("lambda_", ctypes.c_double), ("dlm", ctypes.c_double),
                 ("nu", ctypes.c_double), ("fadeLen", ctypes.c_double), ("nsteps", ctypes.c_int),
                 ("tend", ctypes.c_double), ("poisson", ctypes.c_int), ("precision", ctypes.c_int),
-                ("device", ctypes.c_int), ("iterative", ctypes.c_int)]
+                ("device", ctypes.c_int), ("iterative", ctypes.c_int),
+                ("gravity", ctypes.c_double * 2), ("implicit_penalization", ctypes.c_int)]
 
 
 class ShapeParams(ctypes.Structure):
@@ -133,6 +134,7 @@ def lib():
     L.cup2d_ensemble_destroy.argtypes = [vp]
     L.cup2d_adv_diff_noalloc.argtypes = [vp, vp, vp, vp, i, i, d, d, d, d, d, vp]
     L.cup2d_dump.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p]
+    L.cup2d_poisson_solve.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     L.cup2d_fish_act.argtypes = [vp, i, d, dp, i]
     L.cup2d_fish_period.argtypes = [vp, i, dp]
     L.cup2d_fish_state.argtypes = [vp, i, i, dp, i]
@@ -201,6 +203,11 @@ def parse_args(argline):
     cfg.poisson = POISSON[ptype]
     cfg.precision = {"fp64": PREC_FP64, "fp32": PREC_FP32}[args.get("precision", "fp64")]
     cfg.iterative = int(args.get("iterativePenalization", 0)) != 0     # Simulation.cpp:101
+    # PressureSingle without EXPL_INTEGRATE_MOM (a compile-time switch there)
+    cfg.implicit_penalization = int(args.get("implicitPenalization", 0)) != 0
+    if "gravity" in args:                  # the reference fixes it at (0, -9.8), SimulationData.h:57
+        gx, gy = (float(x) for x in args["gravity"].split())
+        cfg.gravity[0], cfg.gravity[1] = gx, gy
     shapes = []
     for lines in args.get("shapes", "").split("\n"):
         lines = lines.replace("_", " ")
@@ -291,6 +298,11 @@ class Context:
 
     def compute_forces(self, dt=-1.0):
         self._ck(self.L.cup2d_compute_forces(self.h_, dt))
+
+    def poisson_solve(self, src="tmp", dst="pres"):
+        """PoissonSolver::solve(BSRC, BDST): the context's solver on field
+        src into field dst (src is faded in place, as cub2rhs does)."""
+        self._ck(self.L.cup2d_poisson_solve(self.h_, FIELDS[src], FIELDS[dst]))
 
     def end_step(self):
         self._ck(self.L.cup2d_end_step(self.h_))
@@ -436,6 +448,23 @@ class ComputeForces(Operator):
     name, _fn = "ComputeForces", "compute_forces"
 
 
+class PressureIterator_unif(Operator):
+    name, _fn = "PressureIterator_unif", "pressure_single"
+
+
+class advDiffGrav(Operator):
+    name, _fn = "advDiffGrav", "adv_diff"
+
+
+class PressureVarRho_approx(Operator):
+    name, _fn = "PressureVarRho_approx", "pressure_single"
+
+
+def variable_density(shape_params):
+    """SimulationData::checkVariableDensity (SimulationData.cpp:122-130)."""
+    return any(abs(p.rhoS - 1.0) > 2.220446049250313e-16 for _, p in shape_params)
+
+
 def parse_dump_args(argline):
     """The dump options of Simulation::parseRuntime (Simulation.cpp:79-83):
     -fdump (steps between dumps), -tdump (time between dumps),
@@ -466,7 +495,14 @@ class Simulation:
 
     def init(self):
         self.ctx = Context(self.cfg, self.shape_params)
-        self.pipeline = [PutObjectsOnGrid(self), advDiff(self), PressureSingle(self), ComputeForces(self)]
+        # Simulation.cpp:183-220 (the library routes each call by the same test)
+        if variable_density(self.shape_params):
+            self.pipeline = [PutObjectsOnGrid(self), advDiffGrav(self), PressureVarRho_approx(self)]
+        elif self.cfg.iterative:
+            self.pipeline = [PutObjectsOnGrid(self), advDiff(self), PressureIterator_unif(self)]
+        else:
+            self.pipeline = [PutObjectsOnGrid(self), advDiff(self), PressureSingle(self)]
+        self.pipeline.append(ComputeForces(self))
         self.ctx.init()
         self.next_dump_time = 0.0
         if self.dumping():                     # Simulation.cpp:229 (only when dumps are asked for)

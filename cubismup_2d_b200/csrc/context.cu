@@ -295,6 +295,63 @@ int pressure_iterative(cup2d_ctx* ctx) {
   return check_launch(ctx);
 }
 
+// PressureVarRho_approx::operator() (PressureIterator_approx.cpp:378-468):
+// pressureCorrectionInit (vFluid from the last pressure, the velocity part
+// of the RHS, F = 0, uDef cleared), then per iteration the bodies' momenta
+// on vFluid and their velocities, the penalization force F with its
+// relative change relDF, the RHS, a Poisson solve into tmp (the RHS
+// buffer, as solve(tmp, tmp)), the pressure correction of vFluid with the
+// relative pressure change relDP; converged (max(relDF, relDP) below the
+// adaptive target, or more than 100 iterations, or more than twice the
+// previous call's count), finalizePressure updates the velocity; each
+// iteration ends with pres = tmp.  The target adapts as in the reference.
+}  // namespace
+cudaError_t fill_udef_grid(Ctx& c);
+namespace {
+int pressure_varrho(cup2d_ctx* ctx) {
+  Ctx& c = ctx->c;
+  const size_t nb = sizeof(double) * c.ncells();
+  CK(cudaMemcpyAsync(&c.pin->it, &c.dsc->it, sizeof(IterState), cudaMemcpyDeviceToHost, c.stream));
+  CK(cudaStreamSynchronize(c.stream));
+  IterState st = c.pin->it;
+  if (c.udefStale) CK(fill_udef_grid(c));
+  launch_vr_init(c);
+  CK(cudaMemsetAsync(c.udefx, 0, nb, c.stream));
+  CK(cudaMemsetAsync(c.udefy, 0, nb, c.stream));
+  int iter = 0;
+  double relDF = 1e3, relDP = 1e3;
+  for (iter = 0; iter < 1000; iter++) {
+    launch_momenta_varrho(c, c.ifluid[0], c.ifluid[1]);
+    launch_vr_penalize(c);
+    launch_vr_rhs(c);
+    double* const P = c.pres;
+    c.pres = c.rhs;                               // solve(tmp, tmp)
+    poisson_solve(c);
+    c.pres = P;
+    launch_vr_pcorr(c, false);
+    CK(cudaMemcpyAsync(&c.pin->it, &c.dsc->it, sizeof(IterState), cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    if (int rc = check_launch(ctx)) return rc;
+    relDF = c.pin->it.relDF;
+    relDP = c.pin->it.relDP;
+    const bool converged = std::max(relDF, relDP) < st.target || iter > 2 * st.oldNsteps || iter > 100;
+    if (converged) launch_vr_pcorr(c, true);     // finalizePressure
+    CK(cudaMemcpyAsync(c.pres, c.rhs, nb, cudaMemcpyDeviceToDevice, c.stream));
+    if (converged) break;
+  }
+  st.oldNsteps = iter + 1;
+  if (st.oldNsteps > 30) st.target = std::max({relDF, relDP, st.target});
+  if (st.oldNsteps > 10) st.target *= 1.01;
+  if (st.oldNsteps <= 2) st.target *= 0.99;
+  st.target = std::min(1e-3, std::max(1e-5, st.target));
+  st.relDF = relDF;
+  st.relDP = relDP;
+  st.last = iter + 1;
+  launch_set_iter_state(c, st);
+  c.udefStale = false;                          // cleared by pressureCorrectionInit
+  return check_launch(ctx);
+}
+
 } // namespace
 
 // The graph step's calcMaxTimestep reuses the maximum formed at the end of
@@ -339,6 +396,7 @@ int cup2d_config_default(cup2d_config* cfg) {
   cfg->poisson = CUP2D_POISSON_COSINE;   // -poissonType "" selects FFTW_dirichlet
   cfg->precision = CUP2D_PREC_FP64;
   cfg->device = 0;
+  cfg->gravity[0] = 0; cfg->gravity[1] = -9.8;      // SimulationData.h:57
   return CUP2D_OK;
 }
 
@@ -391,6 +449,7 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
   g.nu = cfg->nu; g.CFL = cfg->CFL; g.dlm = cfg->dlm;
   g.fadeLenX = cfg->fadeLen * cfg->extent;                     // Simulation.cpp:97-98
   g.fadeLenY = cfg->fadeLen * cfg->extent;
+  g.implicitPenal = cfg->implicit_penalization ? 1 : 0;
   const size_t n = c.ncells();
   int rc = CUP2D_OK;
   for (int b = 0; b < 2 && !rc; b++)
@@ -456,6 +515,7 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   cudaFree(c.chi); cudaFree(c.pres); cudaFree(c.rhs); cudaFree(c.sdf);
   cudaFree(c.udefx); cudaFree(c.udefy); cudaFree(c.dsc); cudaFree(c.dshapes);
   for (int d = 0; d < 2; d++) { cudaFree(c.itmp[d]); cudaFree(c.ifluid[d]); }
+  cudaFree(c.invRho); cudaFree(c.prhs);
   cudaFree(c.counters); cudaFree(c.partials); cudaFree(c.fadeSlot);
   if (c.flushBuf) cudaFree(c.flushBuf);
   if (c.hashAcc) cudaFree(c.hashAcc);
@@ -512,8 +572,13 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
   if (kind != CUP2D_SHAPE_DISK && kind != CUP2D_SHAPE_STEFANFISH && kind != CUP2D_SHAPE_CARLINGFISH &&
       kind != CUP2D_SHAPE_ENVELOPEFISH)
     return fail(ctx, CUP2D_ENOTSUP, "unknown shape kind");
-  if (std::fabs(p->rhoS - 1.0) > DBL_EPSILON)
-    return fail(ctx, CUP2D_ENOTSUP, "rhoS != 1 selects the variable-density pipeline (Simulation.cpp:185-204)");
+  // Shape::bVariableDensity (Shape.cpp:21-23) selects the variable-density
+  // pipeline (Simulation.cpp:185-204): advDiffGrav + PressureVarRho_approx
+  // with -iterativePenalization, else PressureVarRho_proper (HYPRE)
+  if (std::fabs(p->rhoS - 1.0) > DBL_EPSILON && !c.cfg.iterative)
+    return fail(ctx, CUP2D_ENOTSUP, "rhoS != 1 without -iterativePenalization selects PressureVarRho_proper, "
+                                    "a HYPRE solver (Simulation.cpp:194-199): set iterative");
+  if (!(p->rhoS > 0)) return fail(ctx, CUP2D_EINVAL, "rhoS must be positive");
   DevShape S{};
   ShapeCfg& f = S.cfg;
   f.kind = kind;
@@ -645,6 +710,18 @@ int cup2d_init(cup2d_ctx* ctx) {
   c.fadeSlot = nullptr;
   if ((rc = dalloc(ctx, &c.fadeSlot, (size_t)c.g.nblocks + 1))) return rc;
   if ((c.nfade = build_fade_slots(c)) < 0) return fail(ctx, CUP2D_ECUDA, "fade strip table");
+  // SimulationData::checkVariableDensity and minRho (SimulationData.cpp:116-130)
+  c.varRho = false;
+  c.rho0 = 1;
+  for (int k = 0; k < c.nshapes; k++) {
+    const double r = c.hshapes[k].cfg.rhoS;
+    c.varRho |= std::fabs(r - 1.0) > DBL_EPSILON;
+    c.rho0 = std::min(c.rho0, r);
+  }
+  if (c.varRho && !c.invRho) {
+    if ((rc = dalloc(ctx, &c.invRho, c.ncells()))) return rc;
+    if ((rc = dalloc(ctx, &c.prhs, c.ncells()))) return rc;
+  }
   c.cur = 0;
   // Simulation::reset (Simulation.cpp:232-241): resetAll, IC, objects at t=0, ApplyObjVel
   if ((rc = upload_scalars_reset(ctx))) return rc;
@@ -672,6 +749,7 @@ int cup2d_init(cup2d_ctx* ctx) {
   launch_set_dt(c, 0.0);
   c.devDt = 0.0;
   launch_objects(c, false);
+  if (c.varRho) launch_invrho(c);
   launch_obj_vel_on_grid(c);
   c.udefStale = false;
   launch_apply_obj_vel(c);
@@ -762,6 +840,7 @@ int cup2d_put_objects(cup2d_ctx* ctx, double dt) {
     launch_objects_rest(c);
     c.recordPlaced = false;
   }
+  if (c.varRho) launch_invrho(c);            // PutObjectsOnGrid.cpp:65-73, 197
   if (c.cfg.iterative) {
     // PutObjectsOnGrid.cpp:195, 237-238: the grid's deformation velocity,
     // which the iterated operator's RHS reads
@@ -791,6 +870,12 @@ int cup2d_put_objects(cup2d_ctx* ctx, double dt) {
 // reads no obstacle data) and joins the main stream before returning.
 int cup2d_adv_diff(cup2d_ctx* ctx, double dt) {
   STAGE_PROLOGUE
+  if (c.varRho) {                           // advDiffGrav reads invRho: after the placement
+    c.placedPending = false;
+    c.rhsFresh = false;
+    launch_advdiff_grav(c);
+    return check_launch(ctx);
+  }
   const bool beside = c.placedPending && !prologueLaunched;
   c.placedPending = false;
   if (beside) {
@@ -813,6 +898,10 @@ int cup2d_adv_diff(cup2d_ctx* ctx, double dt) {
 int cup2d_pressure_single(cup2d_ctx* ctx, double dt) {
   STAGE_PROLOGUE
   c.placedPending = false;
+  if (c.varRho) {
+    c.rhsFresh = false;
+    return pressure_varrho(ctx);
+  }
   if (c.cfg.iterative) {
     c.rhsFresh = false;
     return pressure_iterative(ctx);
@@ -822,6 +911,34 @@ int cup2d_pressure_single(cup2d_ctx* ctx, double dt) {
   launch_rhs_obstacles(c);
   poisson_solve(c);
   launch_pressure_tail(c);
+  return check_launch(ctx);
+}
+
+static double* field_ptr(Ctx& c, int which);
+
+int cup2d_poisson_solve(cup2d_ctx* ctx, int src, int dst) {
+  if (!ctx) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
+  double* ps = field_ptr(c, src);
+  double* pd = field_ptr(c, dst);
+  if (!ps || !pd) return fail(ctx, CUP2D_EINVAL, "unknown field (or invRho of a constant-density context)");
+  if ((src == CUP2D_FIELD_UDEF_X || src == CUP2D_FIELD_UDEF_Y || dst == CUP2D_FIELD_UDEF_X ||
+       dst == CUP2D_FIELD_UDEF_Y) && c.udefStale)
+    CK(fill_udef_grid(c));
+  forget_chain(c);
+  c.shapesAtEvent = c.shapesMapped = false;
+  c.stateSeq++;
+  CK(invalidate_dt_next(c));
+  double* const R = c.rhs;
+  double* const P = c.pres;
+  c.rhs = ps;                                   // the solver reads c.rhs and writes c.pres
+  c.pres = pd;
+  launch_fade_sums(c);
+  poisson_solve(c);
+  c.rhs = R;
+  c.pres = P;
+  if (dst == CUP2D_FIELD_UDEF_X || dst == CUP2D_FIELD_UDEF_Y) c.udefStale = false;
   return check_launch(ctx);
 }
 
@@ -953,6 +1070,7 @@ static double* field_ptr(Ctx& c, int which) {
     case CUP2D_FIELD_UDEF_X: return c.udefx;
     case CUP2D_FIELD_UDEF_Y: return c.udefy;
     case CUP2D_FIELD_SDF: return c.sdf;
+    case CUP2D_FIELD_INVRHO: return c.invRho;
     default: return nullptr;
   }
 }
@@ -961,6 +1079,10 @@ int cup2d_get_field(cup2d_ctx* ctx, int which, double* host_out) {
   if (!ctx || !host_out) return CUP2D_EINVAL;
   Ctx& c = ctx->c;
   double* p = field_ptr(c, which);
+  if (!p && which == CUP2D_FIELD_INVRHO) {  // constant density: 1 everywhere
+    std::fill(host_out, host_out + c.ncells(), 1.0);
+    return CUP2D_OK;
+  }
   if (!p) return fail(ctx, CUP2D_EINVAL, "unknown field");
   if ((which == CUP2D_FIELD_UDEF_X || which == CUP2D_FIELD_UDEF_Y) && c.udefStale) CK(fill_udef_grid(c));
   CK(cudaStreamSynchronize(c.stream));
@@ -972,6 +1094,8 @@ int cup2d_set_field(cup2d_ctx* ctx, int which, const double* host_in) {
   if (!ctx || !host_in) return CUP2D_EINVAL;
   Ctx& c = ctx->c;
   double* p = field_ptr(c, which);
+  if (!p && which == CUP2D_FIELD_INVRHO)
+    return fail(ctx, CUP2D_ESTATE, "invRho is 1 without a body of rhoS != 1 (recomputed by every placement)");
   if (!p) return fail(ctx, CUP2D_EINVAL, "unknown field");
   // the other uDef component keeps the values a read would have given
   if ((which == CUP2D_FIELD_UDEF_X || which == CUP2D_FIELD_UDEF_Y) && c.udefStale) CK(fill_udef_grid(c));
@@ -1383,7 +1507,7 @@ namespace {
 struct CkptHeader {
   char magic[8];
   uint32_t version, nsections;
-  int32_t bpdx, bpdy, poisson, precision, nshapes, reserved;
+  int32_t bpdx, bpdy, poisson, precision, nshapes, flags;   // flags: 1 implicit penalization
   double extent, CFL, lambda, dlm, nu, fadeLen;
   uint64_t checksum;              // ckpt_hash over the sections (0 in the comparison copy)
 };
@@ -1455,6 +1579,7 @@ CkptHeader ckpt_header(const Ctx& c, size_t nsec) {
   h.nsections = (uint32_t)nsec;
   h.bpdx = c.cfg.bpdx; h.bpdy = c.cfg.bpdy; h.poisson = c.cfg.poisson; h.precision = c.cfg.precision;
   h.nshapes = c.nshapes;
+  h.flags = c.cfg.implicit_penalization ? 1 : 0;
   h.extent = c.cfg.extent; h.CFL = c.cfg.CFL; h.lambda = c.cfg.lambda; h.dlm = c.cfg.dlm;
   h.nu = c.cfg.nu; h.fadeLen = c.cfg.fadeLen;
   return h;
@@ -1970,6 +2095,11 @@ extern "C" int cup2d_dump(cup2d_ctx* ctx, const char* dir, const char* name) {
   CK(cudaMemcpy(v.data(), c.v(), sizeof(double) * n, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(chi.data(), c.chi, sizeof(double) * n, cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(p.data(), c.pres, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  std::vector<double> ir;
+  if (c.invRho) {
+    ir.resize(n);
+    CK(cudaMemcpy(ir.data(), c.invRho, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  }
   char step[16];
   std::snprintf(step, sizeof(step), "%07d", sc.step);
   const std::string base = std::string(dir) + (dir[0] && dir[std::strlen(dir) - 1] != '/' ? "/" : "");
@@ -1982,7 +2112,7 @@ extern "C" int cup2d_dump(cup2d_ctx* ctx, const char* dir, const char* name) {
   const Out outs[3] = {{"velChi_" + tag, 3}, {"pres_" + tag, 1}, {"invRho_" + tag, 1}};
   for (int k = 0; k < 3; k++) {
     if (k == 1) for (size_t i = 0; i < n; i++) buf[i] = (float)p[i];
-    if (k == 2) for (size_t i = 0; i < n; i++) buf[i] = 1.0f;   // constant density: invRho = 1
+    if (k == 2) for (size_t i = 0; i < n; i++) buf[i] = ir.empty() ? 1.0f : (float)ir[i];
     const std::string raw = outs[k].stem + ".raw";
     if (!write_file(base + raw, buf.data(), sizeof(float) * n * outs[k].ch) ||
         !write_xmf(base + outs[k].stem + ".xmf", raw, k == 0 ? "velChi" : k == 1 ? "pres" : "invRho",

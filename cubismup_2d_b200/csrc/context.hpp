@@ -35,6 +35,14 @@ struct Ctx {
   // the operator) and vFluid (the fluid velocity of an iteration)
   double* itmp[2] = {nullptr, nullptr};
   double* ifluid[2] = {nullptr, nullptr};
+  // variable density (a body with rhoS != 1, with the iterated
+  // penalization): SimulationData::invRho and pRHS; rho0 = minRho()
+  // (SimulationData.cpp:116-121).  itmp then holds the penalization force
+  // (tmpV) and ifluid the pressure-corrected velocity (vFluid).
+  bool varRho = false;
+  double rho0 = 1.0;
+  double* invRho = nullptr;
+  double* prhs = nullptr;
 
   Scalars* dsc = nullptr;       // device scalars
   DevShape* dshapes = nullptr;  // device shape array [MAX_SHAPES]
@@ -156,6 +164,22 @@ enum CounterSlot : int {
 // the fade sums: three per strip block), then 4096 spare, then the
 // per-shape tile reductions
 inline double* fade_partials(const Ctx& c) { return c.partials; }
+
+// every shape's obstacle tiles, by value (a kernel argument)
+struct AllTiles { ObstTiles t[MAX_SHAPES]; };
+inline AllTiles all_tiles(const Ctx& c) {
+  AllTiles a{};
+  for (int k = 0; k < c.nshapes; k++) a.t[k] = c.tiles[k];
+  return a;
+}
+// CTAs of each shape's per-tile kernel (a kernel argument)
+struct PenalCtas { int n[MAX_SHAPES]; };
+// doubles of one shape's tile-reduction region
+inline size_t shape_region(const Ctx& c) { return (size_t)c.maxCapacity * 24; }
+// CTAs per shape of the per-tile kernels: one wave at most; each CTA loops
+// over tiles s = blockIdx.x, blockIdx.x + gridDim.x, ... < ntiles
+inline int tile_ctas(const Ctx& c, int capacity) { return capacity < c.sms ? capacity : c.sms; }
+inline double* shape_partials(const Ctx& c) { return c.partials + (size_t)3 * c.g.nblocks + 4096; }
 
 #define CUP2D_LAUNCHED(c) ((c).launches++)
 

@@ -335,6 +335,31 @@ k_rhs_div(GridDesc g, const Scalars* sc, const double* __restrict__ u,
   }
 }
 
+// cub2rhs's strip sums (PoissonSolver.cpp:61-100) of a plane as it is, for
+// a Poisson solve called on its own: the same per-block order as the RHS
+// kernels' (32 x 8 threads, rows ty + 8r), written to the strip slots.
+__global__ void __launch_bounds__(256)
+k_fade_sums(GridDesc g, const double* __restrict__ rhs, const int* __restrict__ fadeSlot,
+            double* __restrict__ fadePartials)
+{
+  pdl_begin();
+  const int bx = blockIdx.x, by = blockIdx.y;
+  if (!fade_touch(g, bx, by)) return;                  // uniform over the CTA
+  const int gx = bx * BS + threadIdx.x;
+  double s[3] = {0, 0, 0};
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int iy = threadIdx.y + 8 * r;
+    fade_accumulate(g, bx, by, threadIdx.x, iy, rhs[(size_t)(by * BS + iy) * g.nx + gx], s);
+  }
+  __shared__ double red[96];
+  block_sum<3>(s, red);
+  if (lin_tid() == 0) {
+    const int q = fadeSlot[bx + g.bpdx * by];
+    for (int k = 0; k < 3; k++) fadePartials[3 * q + k] = s[k];
+  }
+}
+
 // PressureIterator_unif::updatePressureRHS (PressureIterator_unif.cpp:22-49):
 // tmp = (h/2dt) (div V - chi div UDEF) on the penalized velocity and the
 // grid's deformation velocity, zero-gradient ghosts for both (the same
@@ -523,6 +548,12 @@ void launch_advdiff_rhs_div(Ctx& c) {
 // timing helpers: return the velocity to the buffer it came from (no launch)
 void launch_advdiff_undo(Ctx& c) { c.cur = 1 - c.cur; }
 void launch_pcorr_undo(Ctx& c) { c.cur = 1 - c.cur; }
+
+void launch_fade_sums(Ctx& c) {
+  launch_k(k_fade_sums, dim3(c.g.bpdx, c.g.bpdy), dim3(32, 8), 0, c.stream, c.g, (const double*)c.rhs,
+           (const int*)c.fadeSlot, fade_partials(c));
+  CUP2D_LAUNCHED(c);
+}
 
 void launch_rhs_div(Ctx& c) {
   dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);

@@ -35,6 +35,7 @@ struct GridDesc {
   double ext[2];                  // SimulationData::extents (SimulationData.cpp:34-35)
   double nu, CFL, dlm;
   double fadeLenX, fadeLenY;
+  int implicitPenal;              // cup2d_config.implicit_penalization
 };
 
 // PressureIterator_unif's state between steps (PressureIterator_unif.h:15-16)
@@ -43,6 +44,7 @@ struct GridDesc {
 struct IterState {
   double relDF, target;
   int oldNsteps, last;
+  double relDP;                   // PressureVarRho_approx: relative pressure change
 };
 
 // Per-step scalars (SimulationData.h:45-49 plus values passed between kernels).

@@ -29,6 +29,7 @@ void launch_advdiff_rhs_div(Ctx& c);                  // the update, then Pressu
 void launch_advdiff_undo(Ctx& c);
 void launch_pcorr_undo(Ctx& c);
 void launch_rhs_div(Ctx& c);                         // PressureSingle.cpp:112-128
+void launch_fade_sums(Ctx& c);                       // PoissonSolver.cpp:61-100 sums of c.rhs as it is
 void launch_rhs_iter(Ctx& c);                        // PressureIterator_unif.cpp:22-49
 void launch_pcorr_from(Ctx& c, const double* ui, const double* vi, double* uo, double* vo);
 int build_fade_slots(Ctx& c);                        // PoissonSolver.cpp:71-79, once per grid
@@ -51,9 +52,20 @@ void launch_rhs_obstacles(Ctx& c);                   // PressureSingle.cpp:130-2
 void launch_momenta(Ctx& c, const double* ui, const double* vi);  // PressureSingle.cpp:23-67, 362-372
 // PressureIterator_unif.cpp (the iterated penalization)
 void launch_momenta_iter(Ctx& c, const double* ui, const double* vi);   // :80-135 + updateVelocity
+// the variable-density pipeline (varrho.cu; PressureIterator_approx.cpp)
+void launch_momenta_varrho(Ctx& c, const double* ui, const double* vi);  // :171-222 + updateVelocity
+void launch_invrho(Ctx& c);                          // PutObjectsOnGrid.cpp:65-73, invRho blend
+void launch_advdiff_grav(Ctx& c);                    // advDiffGrav.cpp:14-137
+void launch_vr_init(Ctx& c);                         // pressureCorrectionInit :81-122
+void launch_vr_penalize(Ctx& c);                     // penalize :224-287 -> sc->it.relDF
+void launch_vr_rhs(Ctx& c);                          // updatePressureRHS :289-335
+void launch_vr_pcorr(Ctx& c, bool final_);           // pressureCorrection / finalizePressure
 void launch_penalize_iter(Ctx& c, const double* tu, const double* tv,
                           const double* fu, const double* fv);          // :137-187, residual -> sc->it.relDF
 void launch_set_iter_state(Ctx& c, const IterState& st);                // :247-252 state after a call
+struct PenalCtas;
+// relDF = sqrt((DMX + DMY) / (eps + MX + MY)) from each shape's per-CTA sums
+void launch_reldf(Ctx& c, const PenalCtas& nc);
 void launch_collide_penalize(Ctx& c);                // PressureSingle.cpp:69-108, 243-344
 // ComputeForces.cpp:16-111; out (mapped host memory, or null): each shape's final state
 void launch_forces(Ctx& c, cup2d_shape_state* out = nullptr);

@@ -22,14 +22,6 @@ namespace cup2d {
 
 namespace {
 
-struct AllTiles { ObstTiles t[MAX_SHAPES]; };
-
-inline AllTiles all_tiles(const Ctx& c) {
-  AllTiles a{};
-  for (int k = 0; k < c.nshapes; k++) a.t[k] = c.tiles[k];
-  return a;
-}
-
 // ---------------------------------------------------------------------------
 // PutObjectsOnGrid.cpp:186-220 for the operator entry point: last step's
 // tiles are reset on the grid (all CTAs), then thread 0 of CTA 0 moves the
@@ -364,7 +356,10 @@ k_rhs_corr(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __r
 // ITER: PressureIterator_unif::integrateMomenta (PressureIterator_unif.cpp:
 // 80-135) on its fluid velocity: F = h^2 chi (no density), the velocity
 // itself instead of its difference to udef, and no displacement sums.
-template <bool ITER>
+// VARRHO: PressureVarRho_approx::integrateMomenta (PressureIterator_approx
+// .cpp:171-222) on its fluid velocity (ui, vi, read as they are):
+// F = h^2 rho chi, the velocity itself, displacement sums kept.
+template <bool ITER, bool VARRHO = false>
 __global__ void __launch_bounds__(1024)
 k_momenta(GridDesc g, const Scalars* sc, DevShape* sh, AllTiles T, const double* __restrict__ p,
           const double* __restrict__ ui, const double* __restrict__ vi,
@@ -389,18 +384,28 @@ k_momenta(GridDesc g, const Scalars* sc, DevShape* sh, AllTiles T, const double*
     if (chi > 0) {
       const int gx = bx * BS + ix, gy = by * BS + iy, nx = g.nx, ny = g.ny;
       const size_t c = (size_t)gy * nx + gx;
-      const double pFac = -0.5 * sc->dt / g.h;
-      const double pW = p[gx > 0 ? c - 1 : c], pE = p[gx < nx - 1 ? c + 1 : c];
-      const double pS = p[gy > 0 ? c - nx : c], pN = p[gy < ny - 1 ? c + nx : c];
-      const double uc = ui[c] + pFac * (pE - pW), vc = vi[c] + pFac * (pN - pS);
+      double uc, vc;
+      if (VARRHO) {
+        uc = ui[c]; vc = vi[c];
+      } else {
+        const double pFac = -0.5 * sc->dt / g.h;
+        const double pW = p[gx > 0 ? c - 1 : c], pE = p[gx < nx - 1 ? c + 1 : c];
+        const double pS = p[gy > 0 ? c - nx : c], pN = p[gy < ny - 1 ? c + nx : c];
+        uc = ui[c] + pFac * (pE - pW); vc = vi[c] + pFac * (pN - pS);
+      }
       const double p0 = cell_x(g, bx, ix) - Cx, p1 = cell_y(g, by, iy) - Cy;
       double ud0 = uc, ud1 = vc;
-      if (!ITER) {
+      if (!ITER && !VARRHO) {
         double ux, uy;
         udef_at(t, o, S, p0, p1, ux, uy);
         ud0 = uc - ux; ud1 = vc - uy;
       }
-      const double F = ITER ? hsq * chi : hsq * rho * chi;
+      double F;
+      if (ITER) F = hsq * chi;
+      else if (!VARRHO && g.implicitPenal) {            // PressureSingle.cpp:39-40, 51-53
+        const double Xlamdt = chi * (sc->lambda * sc->dt);
+        F = hsq * rho * Xlamdt / (1 + Xlamdt);
+      } else F = hsq * rho * chi;
       A[0] = F;
       A[1] = F * (p0 * p0 + p1 * p1);
       A[2] = F * p0;
@@ -461,8 +466,6 @@ k_penalize_iter(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double
   block_sum<4>(a, red);
   if (lin_tid() == 0) for (int q = 0; q < 4; q++) part[4 * blockIdx.x + q] = a[q];
 }
-
-struct PenalCtas { int n[MAX_SHAPES]; };
 
 // The relative momentum change sqrt((DMX + DMY) / (eps + MX + MY)) of all
 // shapes' penalized cells (PressureIterator_unif.cpp:185-186), from the
@@ -567,8 +570,8 @@ k_collide(GridDesc g, const Scalars* sc, DevShape* sh, int nsh, AllTiles T)
 
 // PressureSingle::penalize (PressureSingle.cpp:69-108), alpha = 1 - chi
 __global__ void __launch_bounds__(1024)
-k_penalize(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
-           double* u, double* v)
+k_penalize(GridDesc g, const Scalars* sc, const DevShape* sh, int k, ObstTiles t,
+           const double* __restrict__ chig, double* u, double* v)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_PENALIZE);
@@ -582,7 +585,8 @@ k_penalize(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __r
     if (chig[c] > X) continue;
     if (X <= 0) continue;
     const double p0 = cell_x(g, bx, ix) - S.s.com[0], p1 = cell_y(g, by, iy) - S.s.com[1];
-    const double alpha = 1 - X;
+    // PressureSingle.cpp:93-97: 1 / (1 + lambda dt X) without EXPL_INTEGRATE_MOM
+    const double alpha = g.implicitPenal ? 1 / (1 + sc->lambda * sc->dt * X) : 1 - X;
     double ux, uy;
     udef_at(t, o, S, p0, p1, ux, uy);
     const double US = S.s.u - S.s.omega * p1 + ux;
@@ -683,11 +687,6 @@ k_forces(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ u,
   if (out) out[k] = st;                       // the final state, to mapped host memory
 }
 
-inline size_t shape_region(const Ctx& c) { return (size_t)c.maxCapacity * 24; }
-// CTAs per shape of the per-tile kernels: one wave at most; each CTA loops
-// over tiles s = blockIdx.x, blockIdx.x + gridDim.x, ... < ntiles
-inline int tile_ctas(const Ctx& c, int capacity) { return capacity < c.sms ? capacity : c.sms; }
-inline double* shape_partials(const Ctx& c) { return c.partials + (size_t)3 * c.g.nblocks + 4096; }
 
 } // namespace
 
@@ -795,6 +794,13 @@ void launch_momenta(Ctx& c, const double* ui, const double* vi) {
   CUP2D_LAUNCHED(c);
 }
 
+void launch_momenta_varrho(Ctx& c, const double* ui, const double* vi) {
+  if (c.nshapes == 0) return;
+  launch_k(k_momenta<false, true>, dim3(tile_ctas(c, c.maxCapacity), c.nshapes), 1024, 0, c.stream,
+      c.g, c.dsc, c.dshapes, all_tiles(c), (const double*)nullptr, ui, vi, shape_partials(c), (int)shape_region(c),
+      c.counters + CNT_MOMENTA);
+  CUP2D_LAUNCHED(c);
+}
 void launch_momenta_iter(Ctx& c, const double* ui, const double* vi) {
   if (c.nshapes == 0) return;
   launch_k(k_momenta<true>, dim3(tile_ctas(c, c.maxCapacity), c.nshapes), 1024, 0, c.stream, 
@@ -814,6 +820,10 @@ void launch_penalize_iter(Ctx& c, const double* tu, const double* tv, const doub
              shape_partials(c) + (size_t)k * shape_region(c));
     CUP2D_LAUNCHED(c);
   }
+  launch_reldf(c, nc);
+}
+
+void launch_reldf(Ctx& c, const PenalCtas& nc) {
   launch_k(k_reldf, 1, 256, 0, c.stream, c.dsc, c.nshapes, nc, (const double*)shape_partials(c),
            (int)shape_region(c));
   CUP2D_LAUNCHED(c);
@@ -832,8 +842,8 @@ void launch_collide_penalize(Ctx& c) {
     CUP2D_LAUNCHED(c);
   }
   for (int k = 0; k < c.nshapes; k++) {
-    launch_k(k_penalize, tile_ctas(c, c.tiles[k].capacity), dim3(32, 32), 0, c.stream, c.g, c.dshapes, k, c.tiles[k],
-                                                                  c.chi, c.u(), c.v());
+    launch_k(k_penalize, tile_ctas(c, c.tiles[k].capacity), dim3(32, 32), 0, c.stream, c.g,
+             (const Scalars*)c.dsc, (const DevShape*)c.dshapes, k, c.tiles[k], (const double*)c.chi, c.u(), c.v());
     CUP2D_LAUNCHED(c);
   }
 }

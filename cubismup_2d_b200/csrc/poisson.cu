@@ -361,6 +361,69 @@ __device__ __forceinline__ void fft_convolve(C* A, int nseq, const C* tws, Mul m
   fft_passes<L, E, true, false, HOUT, E>(A, nseq, tws);
 }
 
+// The first pass of a forward FFT (NS = 1, radix R) with its inputs read
+// straight from global memory (ld(sequence, index)) into registers: the
+// sequence is never staged in shared memory before the pass.  With ZIN the
+// upper half of the input is zero and not read.  The outputs go to
+// shared memory; the caller's barrier makes them visible.
+template <int L, int R, bool ZIN, int E, class C, class Ld>
+__device__ __forceinline__ void fft_first_pass_global(C* A, int nseq, Ld ld)
+{
+  constexpr int SL = Len<L>::SL, T = L / E, NB = E / R, Q = L / R;
+  const int tid = threadIdx.x;
+  if (tid >= nseq * T) return;
+  const int sq = tid / T, j = tid - sq * T;
+  C* a = A + sq * SL;
+  C x[E];
+#pragma unroll
+  for (int u = 0; u < NB; u++)
+#pragma unroll
+    for (int m = 0; m < R; m++)
+      x[u * R + m] = (ZIN && m >= R / 2) ? mk<C>(0, 0) : ld(sq, j + u * T + m * Q);
+#pragma unroll
+  for (int u = 0; u < NB; u++) {
+    C* xb = x + u * R;
+    dft<R, false>(xb);
+    const int o = (j + u * T) * R, po = pad(o);
+#pragma unroll
+    for (int q = 0; q < R; q++) a[pad_out<1>(po, o, q)] = xb[out_reg<R>(q)];
+  }
+}
+
+// The last pass of an inverse FFT (NS * R = L) with its outputs written
+// straight to global memory (st(sequence, index, value)) from registers;
+// with HOUT only the lower half of the output is formed.
+template <int L, int R, int NS, bool HOUT, int E, class C, class St>
+__device__ __forceinline__ void fft_last_pass_global(C* A, int nseq, const C* tws, St st)
+{
+  static_assert(NS * R == L, "the last pass");
+  constexpr int SL = Len<L>::SL, T = L / E, NB = E / R, Q = L / R;
+  const int tid = threadIdx.x;
+  if (tid >= nseq * T) return;
+  const int sq = tid / T, j = tid - sq * T;
+  const C* a = A + sq * SL;
+  C x[E];
+  const int pj = pad(j);
+#pragma unroll
+  for (int u = 0; u < NB; u++)
+#pragma unroll
+    for (int m = 0; m < R; m++) x[u * R + m] = a[pad_at<T, Q>(pj, j, u, m)];
+#pragma unroll
+  for (int u = 0; u < NB; u++) {
+    C* xb = x + u * R;
+    const int jb = j + u * T, k = jb & (NS - 1);
+    if (NS > 1 && k) {
+      const int base = k * (L / (R * NS));
+#pragma unroll
+      for (int m = 1; m < R; m++) xb[m] = cmul(xb[m], twiddle<L, true>(tws, m * base));
+    }
+    dft<R, true>(xb);
+    const int o = (jb - k) * R + k;
+#pragma unroll
+    for (int q = 0; q < (HOUT ? R / 2 : R); q++) st(sq, o + q * NS, xb[out_reg<R>(q)]);
+  }
+}
+
 struct FadeArgs {
   int enabled;
   Scalars* sc;           // receives fadeCorr (from the first CTA)
@@ -398,6 +461,27 @@ __device__ __forceinline__ double fade_cell(const GridDesc& g, int gx, int gy, d
   return __dadd_rn(__dmul_rn(b, 1 - f2), fadeCorrection);   // never contracted into an FMA
 }
 
+// Real FFT of length 2L from the complex FFT Z of length L of its value
+// pairs, even/odd split: X[k] = Fe[k] + W^k Fo[k], W = exp(-i pi / L),
+// k in [0, L]; written to row row0 + r of out.
+template <int L>
+__device__ __forceinline__ void r2c_split(const double2* A, int nb, int row0, double2* __restrict__ out,
+                                          int outStride, const double2* __restrict__ tw, int twLen)
+{
+  constexpr int SL = Len<L, E_ROWS>::SL, NT = Len<L, E_ROWS>::NT;
+  const int twStep = twLen / (2 * L);
+  for (int idx = threadIdx.x; idx < nb * (L + 1); idx += NT) {
+    const int r = idx / (L + 1), k = idx - r * (L + 1);
+    const double2 Zk = A[r * SL + pad(k == L ? 0 : k)];
+    const double2 Zc = conjg(A[r * SL + pad(k == 0 ? 0 : L - k)]);
+    const double2 Fe = make_double2(0.5 * (Zk.x + Zc.x), 0.5 * (Zk.y + Zc.y));
+    const double2 d = csub(Zk, Zc);
+    const double2 Fo = make_double2(0.5 * d.y, -0.5 * d.x);   // (Zk - Zc) / (2i)
+    const double2 X = cadd(Fe, cmul(tw[k * twStep], Fo));
+    out[(size_t)(row0 + r) * outStride + k] = X;
+  }
+}
+
 // inMode 0: rows of `in`; 1: the free-space Green's function on the MY x MX
 // padded grid (FFTW_freespace.cpp:108-119) computed on the fly.  Each row of 2L
 // reals is the complex sequence (x[2n], x[2n+1]) of length L.
@@ -416,16 +500,44 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
   const int row0 = blockIdx.x * RB;
   const int nb = min(RB, nrows - row0);
   if (inMode == 0) {
-    for (int idx = threadIdx.x; idx < RB * L; idx += NT) {
-      const int r = idx / L, n = idx & (L - 1), row = row0 + r;
-      if (r >= nb) continue;
-      double2* dst = A + r * SL + pad(n);
-      if (2 * n + 1 < ncolsIn) cp_async16(dst, in + (size_t)row * inStride + 2 * n);
-      else if (2 * n < ncolsIn) *dst = make_double2(in[(size_t)row * inStride + 2 * n], 0);
-      else if (!HIN || n < L / 2) *dst = make_double2(0, 0);   // with HIN the upper half is never read
-    }
-    cp_async_commit();
-  } else {
+    // the first pass reads the rows itself, fading the band cells as it
+    // goes (cub2rhs, PoissonSolver.cpp:61-141) and writing them back
+    __shared__ double sCorr0;
+    if (fa.enabled) fade_corr_cta(fa, &sCorr0);
+    load_twiddles<L>(tws, tw, twLen);
+    __syncthreads();
+    const double corr = fa.enabled ? sCorr0 : 0.0;
+    const int bandX = fa.enabled ? (int)(fa.g.fadeLenX / fa.g.h) + 2 : 0;
+    const int bandY = fa.enabled ? (int)(fa.g.fadeLenY / fa.g.h) + 2 : 0;
+    auto ld = [&](int r, int n) {
+      const int row = row0 + r;
+      const double* src = in + (size_t)row * inStride + 2 * n;
+      double2 v = make_double2(0, 0);
+      if (2 * n + 1 < ncolsIn) v = *reinterpret_cast<const double2*>(src);
+      else if (2 * n < ncolsIn) v.x = src[0];
+      if (fa.enabled && 2 * n + 1 < ncolsIn) {
+        const bool rowBand = row < bandY || row >= fa.g.ny - bandY;
+        if (rowBand || 2 * n < bandX || 2 * n + 1 >= fa.g.nx - bandX) {
+          double* x = &v.x;
+          for (int q = 0; q < 2; q++) {
+            const int col = 2 * n + q;
+            if (rowBand || col < bandX || col >= fa.g.nx - bandX) {
+              x[q] = fade_cell(fa.g, col, row, x[q], corr);
+              fa.writeback[(size_t)row * inStride + col] = x[q];
+            }
+          }
+        }
+      }
+      return v;
+    };
+    fft_first_pass_global<L, E_ROWS, HIN, E_ROWS>(A, nb, ld);
+    __syncthreads();
+    fft_passes<L, E_ROWS, false, false, false, E_ROWS>(A, nb, tws);
+    r2c_split<L>(A, nb, row0, out, outStride, tw, twLen);
+    return;
+  }
+  {
+    // inMode 1: the Green's function, formed in place
     for (int idx = threadIdx.x; idx < RB * L; idx += NT) {
       const int r = idx / L, n = idx & (L - 1), row = row0 + r;
       if (r >= nb) continue;
@@ -451,48 +563,10 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
       A[r * SL + pad(n)] = make_double2(x[0], x[1]);
     }
   }
-  __shared__ double sCorr;
-  if (fa.enabled) fade_corr_cta(fa, &sCorr);   // while the rows are in flight
   load_twiddles<L>(tws, tw, twLen);
-  cp_async_wait<0>();
   __syncthreads();
-  if (fa.enabled) {
-    // fade band: cells within fadeLen (+2 cells margin) of an edge, faded in
-    // place and written back (cub2rhs, PoissonSolver.cpp:61-141)
-    const double corr = sCorr;
-    const int bandX = (int)(fa.g.fadeLenX / fa.g.h) + 2;
-    const int bandY = (int)(fa.g.fadeLenY / fa.g.h) + 2;
-    for (int idx = threadIdx.x; idx < RB * L; idx += NT) {
-      const int r = idx / L, n = idx & (L - 1), row = row0 + r;
-      if (r >= nb || 2 * n + 1 >= ncolsIn) continue;
-      const bool rowBand = row < bandY || row >= fa.g.ny - bandY;
-      if (!rowBand && 2 * n >= bandX && 2 * n + 1 < fa.g.nx - bandX) continue;   // both cells inside
-      double2 v = A[r * SL + pad(n)];
-      double* x = &v.x;
-      for (int q = 0; q < 2; q++) {
-        const int col = 2 * n + q;
-        if (rowBand || col < bandX || col >= fa.g.nx - bandX) {
-          x[q] = fade_cell(fa.g, col, row, x[q], corr);
-          fa.writeback[(size_t)row * inStride + col] = x[q];
-        }
-      }
-      A[r * SL + pad(n)] = v;
-    }
-    __syncthreads();
-  }
   fft_inplace<L, false, HIN, false, E_ROWS>(A, nb, tws);
-  // even/odd split: X[k] = Fe[k] + W^k Fo[k], W = exp(-i pi / L), k in [0, L]
-  const int twStep = twLen / (2 * L);
-  for (int idx = threadIdx.x; idx < nb * (L + 1); idx += NT) {
-    const int r = idx / (L + 1), k = idx - r * (L + 1);
-    const double2 Zk = A[r * SL + pad(k == L ? 0 : k)];
-    const double2 Zc = conjg(A[r * SL + pad(k == 0 ? 0 : L - k)]);
-    const double2 Fe = make_double2(0.5 * (Zk.x + Zc.x), 0.5 * (Zk.y + Zc.y));
-    const double2 d = csub(Zk, Zc);
-    const double2 Fo = make_double2(0.5 * d.y, -0.5 * d.x);   // (Zk - Zc) / (2i)
-    const double2 X = cadd(Fe, cmul(tw[k * twStep], Fo));
-    out[(size_t)(row0 + r) * outStride + k] = X;
-  }
+  r2c_split<L>(A, nb, row0, out, outStride, tw, twLen);
 }
 
 // mode 0: forward, x G^ (real, symmetric in ky), inverse, keep nrowsOut rows
@@ -620,15 +694,14 @@ k_rows_c2r(const double2* __restrict__ in, int inStride, int nrows, double* __re
     a[pad(kk[1])] = res[1];
   }
   __syncthreads();
-  fft_inplace<L, true, false, HOUT, E_C2R>(A, nb, tws);
-  const int half = (ncolsOut + 1) / 2;
-  for (int idx = threadIdx.x; idx < nb * half; idx += NT) {
-    const int r = idx / half, n = idx - r * half;
-    const double2 v = A[r * SL + pad(n)];
+  // the inverse FFT; its last pass writes the value pairs of the row
+  constexpr int NSL = last_ns<L, E_C2R>();
+  fft_passes_below<L, 1, NSL, true, false, E_C2R>(A, nb, tws);
+  fft_last_pass_global<L, L / NSL, NSL, HOUT, E_C2R>(A, nb, tws, [&](int r, int n, double2 v) {
     double* o = out + (size_t)(row0 + r) * outStride;
     if (2 * n + 1 < ncolsOut) *reinterpret_cast<double2*>(o + 2 * n) = v;
-    else o[2 * n] = v.x;
-  }
+    else if (2 * n < ncolsOut) o[2 * n] = v.x;
+  });
 }
 
 // ---- FP32 transforms (CUP2D_PREC_FP32) ------------------------------------

@@ -66,6 +66,8 @@ extern "C" {
                                 /* from the obstacle tiles when read)         */
 #define CUP2D_FIELD_UDEF_Y 6
 #define CUP2D_FIELD_SDF 7       /* max signed distance of all shapes         */
+#define CUP2D_FIELD_INVRHO 8    /* 1/rho (SimulationData::invRho; 1 unless a */
+                                /* body has rhoS != 1)                        */
 
 /* Simulation parameters: the runtime arguments parsed by
  * Simulation::parseRuntime (Simulation.cpp:66-104). */
@@ -85,6 +87,14 @@ typedef struct cup2d_config {
   int iterative;           /* -iterativePenalization: PressureIterator_unif     */
                            /* replaces PressureSingle (Simulation.cpp:213-216);  */
                            /* operator-by-operator steps only                    */
+  double gravity[2];       /* SimulationData::gravity (SimulationData.h:57,     */
+                           /* (0, -9.8)); read by the variable-density pipeline  */
+  int implicit_penalization; /* PressureSingle as compiled without           */
+                           /* EXPL_INTEGRATE_MOM (PressureSingle.cpp:20): the    */
+                           /* lambda-implicit momenta F = h^2 rho X/(1+X) with   */
+                           /* X = chi lambda dt, and penalization alpha =        */
+                           /* 1/(1 + lambda dt chi) (UpdateObjects.cpp:128-210); */
+                           /* 0: the shipped explicit forms                      */
 } cup2d_config;
 
 /* Shape descriptors (the key=value parameters of Shape.cpp:331-345,
@@ -163,6 +173,13 @@ int cup2d_put_objects(cup2d_ctx* ctx, double dt);      /* PutObjectsOnGrid.cpp:1
 int cup2d_adv_diff(cup2d_ctx* ctx, double dt);         /* advDiff.cpp:36-118            */
 int cup2d_pressure_single(cup2d_ctx* ctx, double dt);  /* PressureSingle.cpp:346-373    */
 int cup2d_compute_forces(cup2d_ctx* ctx, double dt);   /* ComputeForces.cpp:16-111      */
+/* PoissonSolver::solve(BSRC, BDST) (PoissonSolver.h:35-40), the second
+ * plug-in point: the context's solver (cup2d_config.poisson) on the RHS in
+ * field `src` into field `dst` (CUP2D_FIELD_*, device-resident; src == dst
+ * allowed, as in solve(tmp, tmp)).  As cub2rhs does (PoissonSolver.cpp:
+ * 101-118), the boundary-strip fade with its mean correction is applied to
+ * `src` in place.  The stage calls above run it on their own buffers. */
+int cup2d_poisson_solve(cup2d_ctx* ctx, int src, int dst);
 /* With cup2d_config.iterative, cup2d_pressure_single runs the iterated
  * penalization and projection of PressureIterator_unif::operator()
  * (PressureIterator_unif.cpp:214-270): it waits for each iteration's

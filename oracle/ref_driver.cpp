@@ -23,6 +23,10 @@
 #include "Operators/advDiff.h"
 #include "Operators/PressureSingle.h"
 #include "Operators/PressureIterator_unif.h"
+#include "Operators/advDiffGrav.h"
+#include "Operators/PressureIterator_approx.h"
+#include "Operators/UpdateObjects.h"
+#include "Poisson/PoissonSolver.h"
 #include "Operators/ComputeForces.h"
 #include "Obstacles/ShapesSimple.h"
 #include "Obstacles/StefanFish.h"
@@ -66,6 +70,48 @@ struct Argv {
   char** argv() { return ptrs.data(); }
 };
 
+// The iterated operators keep their iteration count (oldNsteps, the
+// iterations of the last call) private, PressureSingle its steps.  An explicit template instantiation
+// may name a private member (access is not checked there), which hands the
+// harness a pointer to it without touching the reference's sources.
+struct IterCountTag { typedef int PressureIterator_unif::*type; };
+IterCountTag::type member_of(IterCountTag);
+template <class Tag, typename Tag::type M>
+struct MemberPtr { friend typename Tag::type member_of(Tag) { return M; } };
+template struct MemberPtr<IterCountTag, &PressureIterator_unif::oldNsteps>;
+struct VarRhoCountTag { typedef int PressureVarRho_approx::*type; };
+VarRhoCountTag::type member_of(VarRhoCountTag);
+template struct MemberPtr<VarRhoCountTag, &PressureVarRho_approx::oldNsteps>;
+
+struct PsRhsTag { typedef void (PressureSingle::*type)(const double) const; };
+PsRhsTag::type member_of(PsRhsTag);
+template struct MemberPtr<PsRhsTag, &PressureSingle::updatePressureRHS>;
+struct PsCorrTag { typedef void (PressureSingle::*type)(const double) const; };
+PsCorrTag::type member_of(PsCorrTag);
+template struct MemberPtr<PsCorrTag, &PressureSingle::pressureCorrection>;
+struct PsSolverTag { typedef PoissonSolver* const PressureSingle::*type; };
+PsSolverTag::type member_of(PsSolverTag);
+template struct MemberPtr<PsSolverTag, &PressureSingle::pressureSolver>;
+
+// PressureSingle as compiled without EXPL_INTEGRATE_MOM (a #define at
+// PressureSingle.cpp:20): its RHS, solve and pressure correction
+// (PressureSingle.cpp:346-360), then the lambda-implicit momenta, velocity
+// update, collisions and penalization, which UpdateObjects::operator()
+// (UpdateObjects.cpp:213-224) runs in the same order with that switch off
+// (UpdateObjects.cpp:19); harness option -implicitPenalization 1.
+struct PressureSingleImplicit : public Operator {
+  PressureSingle ps;
+  UpdateObjects uo;
+  explicit PressureSingleImplicit(SimulationData& s) : Operator(s), ps(s), uo(s) {}
+  void operator()(const double dt) override {
+    (ps.*member_of(PsRhsTag()))(dt);
+    (ps.*member_of(PsSolverTag()))->solve(sim.tmp->getBlocksInfo(), sim.pres->getBlocksInfo());
+    (ps.*member_of(PsCorrTag()))(dt);
+    uo(dt);
+  }
+  std::string getName() override { return "PressureSingle(implicit penalization)"; }
+};
+
 struct RefSim
 {
   Argv args;
@@ -73,6 +119,7 @@ struct RefSim
   SimulationData sim;
   std::vector<Operator*> pipeline;
   std::string workdir;
+  bool implicitPenalization = false;
 
   explicit RefSim(const std::string& line)
     : args(line), parser(args.argc(), args.argv()) {}
@@ -104,6 +151,7 @@ struct RefSim
     sim.fadeLenY = parser("-fadeLen").asDouble(0.01) * sim.extent;
     sim.verbose = parser("-verbose").asInt(1);
     sim.iterativePenalization = parser("-iterativePenalization").asInt(0);
+    implicitPenalization = parser("-implicitPenalization").asInt(0) != 0;   // harness option
     sim.muteAll = parser("-muteAll").asInt(0);
     if (sim.muteAll) sim.verbose = 0;
   }
@@ -136,7 +184,10 @@ struct RefSim
     }
     if (sim.shapes.empty()) throw std::runtime_error("no shapes");
     sim.checkVariableDensity();
-    if (sim.bVariableDensity) throw std::runtime_error("variable density is outside the oracle harness");
+    // Simulation.cpp:194-199: without -iterativePenalization the variable-
+    // density branch needs HYPRE (PressureVarRho_proper), absent here
+    if (sim.bVariableDensity && !sim.iterativePenalization)
+      throw std::runtime_error("variable density without -iterativePenalization needs HYPRE");
   }
 
   void init() {  // Simulation.cpp:175-230, constant-density branch
@@ -145,11 +196,19 @@ struct RefSim
     { IC ic(sim); ic(0); }
     sim.bStaggeredGrid = false;
     pipeline.push_back(new PutObjectsOnGrid(sim));
-    pipeline.push_back(new advDiff(sim));
-    // Simulation.cpp:213-216: -iterativePenalization selects the iterated
-    // penalization/projection operator in place of PressureSingle
-    if (sim.iterativePenalization) pipeline.push_back(new PressureIterator_unif(sim));
-    else pipeline.push_back(new PressureSingle(sim));
+    if (sim.bVariableDensity) {
+      // Simulation.cpp:183-192: the variable-density branch with the
+      // iterated penalization
+      pipeline.push_back(new advDiffGrav(sim));
+      pipeline.push_back(new PressureVarRho_approx(sim));
+    } else {
+      pipeline.push_back(new advDiff(sim));
+      // Simulation.cpp:213-216: -iterativePenalization selects the iterated
+      // penalization/projection operator in place of PressureSingle
+      if (sim.iterativePenalization) pipeline.push_back(new PressureIterator_unif(sim));
+      else if (implicitPenalization) pipeline.push_back(new PressureSingleImplicit(sim));
+      else pipeline.push_back(new PressureSingle(sim));
+    }
     pipeline.push_back(new ComputeForces(sim));
     reset();
     sim.dt = 0;
@@ -221,15 +280,6 @@ Real* field_ptr(RefSim* r, int which, size_t b, int ix, int iy) {
 
 thread_local std::string g_err;
 
-// The iterated operator keeps its iteration count (oldNsteps, the
-// iterations of its last call) private.  An explicit template instantiation
-// may name a private member (access is not checked there), which hands the
-// harness a pointer to it without touching the reference's sources.
-struct IterCountTag { typedef int PressureIterator_unif::*type; };
-IterCountTag::type member_of(IterCountTag);
-template <class Tag, typename Tag::type M>
-struct MemberPtr { friend typename Tag::type member_of(Tag) { return M; } };
-template struct MemberPtr<IterCountTag, &PressureIterator_unif::oldNsteps>;
 
 } // namespace
 
@@ -273,11 +323,34 @@ double ref_calc_dt(void* h) { return ((RefSim*)h)->calcMaxTimestep(); }
 int ref_advance(void* h) { return ((RefSim*)h)->advance(((RefSim*)h)->sim.dt) ? 1 : 0; }
 double ref_max_u(void* h) { const auto op = findMaxU(((RefSim*)h)->sim); return op.run(); }
 
-// Iterations of the last PressureIterator_unif call (its oldNsteps), or -1
-// when the pipeline runs PressureSingle.
+// Iterations of the last PressureIterator_unif or PressureVarRho_approx
+// call (its oldNsteps), or -1 when the pipeline runs PressureSingle.
 int ref_iterations(void* h) {
-  auto* op = dynamic_cast<PressureIterator_unif*>(((RefSim*)h)->pipeline[2]);
-  return op ? op->*member_of(IterCountTag()) : -1;
+  Operator* p = ((RefSim*)h)->pipeline[2];
+  if (auto* op = dynamic_cast<PressureIterator_unif*>(p)) return op->*member_of(IterCountTag());
+  if (auto* op = dynamic_cast<PressureVarRho_approx*>(p)) return op->*member_of(VarRhoCountTag());
+  return -1;
+}
+// SimulationData::gravity (SimulationData.h:57), fixed at (0, -9.8) there
+void ref_set_gravity(void* h, double gx, double gy) {
+  ((RefSim*)h)->sim.gravity[0] = gx; ((RefSim*)h)->sim.gravity[1] = gy;
+}
+int ref_variable_density(void* h) { return ((RefSim*)h)->sim.bVariableDensity ? 1 : 0; }
+// PoissonSolver::solve(BSRC, BDST) of a solver made by the reference's own
+// factory (PoissonSolver.cpp:23-59) on scalar fields (2 chi, 3 pres, 4 tmp,
+// 7 invRho); returns -1 for a non-scalar field
+int ref_poisson_solve(void* h, int src, int dst) {
+  SimulationData& s = ((RefSim*)h)->sim;
+  auto grid = [&](int w) -> ScalarGrid* {
+    switch (w) { case 2: return s.chi; case 3: return s.pres; case 4: return s.tmp; case 7: return s.invRho;
+                 default: return nullptr; }
+  };
+  ScalarGrid *gs = grid(src), *gd = grid(dst);
+  if (!gs || !gd) return -1;
+  PoissonSolver* solver = PoissonSolver::makeSolver(s);
+  solver->solve(gs->getBlocksInfo(), gd->getBlocksInfo());
+  delete solver;
+  return 0;
 }
 
 // The RL actuation of a StefanFish (StefanFish.cpp:373-577): act, the

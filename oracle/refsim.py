@@ -1,11 +1,13 @@
 """Oracle test infrastructure: ctypes wrapper of oracle/_ref/libcup2d_ref.so.
 
 The library is the reference's OWN operator sources (PutObjectsOnGrid.cpp,
-advDiff.cpp, PressureSingle.cpp, ComputeForces.cpp, Helpers.cpp, Shape.cpp,
+advDiff.cpp, PressureSingle.cpp, PressureIterator_unif.cpp, advDiffGrav.cpp,
+PressureIterator_approx.cpp, ComputeForces.cpp, Helpers.cpp, Shape.cpp,
 Obstacles/*.cpp, Poisson/PoissonSolver.cpp, Poisson/FFTW_freespace.cpp,
 SimulationData.cpp) compiled unmodified against the project-written shims in
-oracle/shim, driven by oracle/ref_driver.cpp, which restates the
-constant-density branch of Simulation.cpp:66-305.
+oracle/shim, driven by oracle/ref_driver.cpp, which restates
+Simulation.cpp:66-305: the constant-density branch and the variable-density
+one with -iterativePenalization (advDiffGrav + PressureVarRho_approx).
 
 Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of bench.py
 use this module; the product never does.
@@ -35,7 +37,8 @@ SHAPE_FIELDS = [
 ]
 FIELDS = {"u": 0, "v": 1, "chi": 2, "pres": 3, "tmp": 4, "udef_x": 5, "udef_y": 6,
           "invRho": 7, "tmpV_x": 8, "tmpV_y": 9}
-OPS = {"PutObjectsOnGrid": 0, "advDiff": 1, "PressureSingle": 2, "ComputeForces": 3}
+OPS = {"PutObjectsOnGrid": 0, "advDiff": 1, "PressureSingle": 2, "ComputeForces": 3,
+       "advDiffGrav": 1, "PressureVarRho_approx": 2}
 
 _lib = None
 
@@ -67,7 +70,8 @@ def lib():
     L.ref_create.argtypes = [ctypes.c_char_p]
     L.ref_last_error.restype = ctypes.c_char_p
     L.ref_destroy.argtypes = [vp]
-    for name in ("ref_nx", "ref_ny", "ref_stepid", "ref_nshapes", "ref_advance", "ref_iterations"):
+    for name in ("ref_nx", "ref_ny", "ref_stepid", "ref_nshapes", "ref_advance", "ref_iterations",
+                 "ref_variable_density"):
         getattr(L, name).argtypes = [vp]
         getattr(L, name).restype = i
     for name in ("ref_h", "ref_time", "ref_dt", "ref_lambda", "ref_calc_dt", "ref_max_u"):
@@ -75,6 +79,9 @@ def lib():
         getattr(L, name).restype = d
     L.ref_uinf.argtypes = [vp, dp]
     L.ref_set_uinf.argtypes = [vp, d, d]
+    L.ref_set_gravity.argtypes = [vp, d, d]
+    L.ref_poisson_solve.argtypes = [vp, i, i]
+    L.ref_poisson_solve.restype = i
     L.ref_set_time.argtypes = [vp, d, i, d]
     L.ref_run_op.argtypes = [vp, i, d]
     L.ref_reset.argtypes = [vp]
@@ -199,9 +206,21 @@ class RefSim:
         return dt
 
     def iterations(self):
-        """Iterations of the last PressureIterator_unif call (-1 without
-        -iterativePenalization)."""
+        """Iterations of the last PressureIterator_unif or
+        PressureVarRho_approx call (-1 without -iterativePenalization)."""
         return self.L.ref_iterations(self.h_)
+
+    def variable_density(self):
+        """SimulationData::bVariableDensity (a shape with rhoS != 1)."""
+        return self.L.ref_variable_density(self.h_) == 1
+
+    def poisson_solve(self, src="tmp", dst="pres"):
+        """PoissonSolver::solve(src, dst) with a solver from makeSolver."""
+        assert self.L.ref_poisson_solve(self.h_, FIELDS[src], FIELDS[dst]) == 0
+
+    def set_gravity(self, gx, gy):
+        """SimulationData::gravity, (0, -9.8) unless set."""
+        self.L.ref_set_gravity(self.h_, gx, gy)
 
     def fish_act(self, k, t, action):
         """StefanFish::act(t, action) on shape k."""

@@ -1,0 +1,139 @@
+"""The variable-density pipeline (a body with rhoS != 1 under
+-iterativePenalization 1: PutObjectsOnGrid's 1/rho blend, advDiffGrav and
+PressureVarRho_approx, Simulation.cpp:183-192) against the reference's own
+operators on the same inputs: operator by operator, then whole steps with
+the same iteration count per step."""
+import numpy as np
+import pytest
+
+from cubismup_2d_b200 import Cup2DError, Simulation
+from cubismup_2d_b200.abi import ENOTSUP, ESTATE
+from cubismup_2d_b200.synthetic import noise_field
+
+pytestmark = pytest.mark.gpu
+
+VR = "-extent 1 -CFL 0.1 -muteAll 1 -iterativePenalization 1 "
+HEAVY = ("-bpdx 4 -bpdy 4 -nu 1e-3 -poissonType freespace " + VR +
+         "-shapes 'disk radius=0.1 xpos=0.5 ypos=0.6 rhoS=1.5'")
+LIGHT = ("-bpdx 4 -bpdy 4 -nu 1e-3 " + VR +                      # cosine solver, rho0 = 0.8
+         "-shapes 'disk radius=0.08 xpos=0.45 ypos=0.4 rhoS=0.8'")
+PAIR = ("-bpdx 8 -bpdy 4 -nu 1e-3 -poissonType freespace " + VR +
+        "-shapes 'disk radius=0.07 xpos=0.42 ypos=0.25 rhoS=2,"
+        "disk radius=0.07 xpos=0.58 ypos=0.26 rhoS=0.9'")
+TOL = 1e-9
+
+
+def _pair(refsim, args, seed=7):
+    r = refsim.RefSim(args)
+    s = Simulation(args)
+    s.init()
+    for comp, name in enumerate(("u", "v")):
+        a = r.get(name) + 0.05 * noise_field(seed, comp, r.ny, r.nx)
+        r.set(name, a)
+        s.ctx.set(name, a)
+    return r, s
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.mark.parametrize("args", [HEAVY, LIGHT, PAIR], ids=["heavy", "light_cosine", "pair"])
+def test_operators_match_reference(ref, args):
+    r, s = _pair(ref, args)
+    assert r.variable_density()
+    assert [op.name for op in s.pipeline] == ["PutObjectsOnGrid", "advDiffGrav",
+                                               "PressureVarRho_approx", "ComputeForces"]
+    dt = r.calc_dt()
+    s.ctx.calc_dt()
+    r.run_op("PutObjectsOnGrid", dt)
+    s.pipeline[0](dt)
+    # the blend is a per-cell expression of chi and rho: bitwise
+    assert np.array_equal(s.ctx.get("invRho"), r.get("invRho"))
+    assert np.array_equal(s.ctx.get("chi"), r.get("chi"))
+    r.run_op("advDiffGrav", dt)
+    s.pipeline[1](dt)
+    for f in ("u", "v"):
+        assert _rel(s.ctx.get(f), r.get(f)) <= 1e-13, f
+    r.run_op("PressureVarRho_approx", dt)
+    s.pipeline[2](dt)
+    assert s.ctx.iteration_stats()[0] == r.iterations()
+    errs = {f: _rel(s.ctx.get(f), r.get(f)) for f in ("u", "v", "pres")}
+    assert all(e <= TOL for e in errs.values()), errs
+    # pressureCorrectionInit clears the grid's uDef
+    assert not np.any(s.ctx.get("udef_x")) and not np.any(r.get("udef_x"))
+
+
+@pytest.mark.parametrize("args", [HEAVY, PAIR], ids=["heavy", "pair"])
+def test_steps_match_reference(ref, args):
+    r, s = _pair(ref, args)
+    for _ in range(3):
+        r.step()
+        s.advance(s.calcMaxTimestep())
+        assert s.ctx.iteration_stats()[0] == r.iterations()
+    s.ctx.sync()
+    errs = {f: _rel(s.ctx.get(f), r.get(f)) for f in ("u", "v", "pres", "chi", "invRho")}
+    assert all(e <= TOL for e in errs.values()), errs
+    for k in range(s.ctx.nshapes):
+        a, b = s.ctx.shape(k), r.shape(k)
+        for key in ("u", "v", "omega", "center_x", "center_y", "M", "J", "penalM", "penalJ",
+                    "fluidMomX", "fluidMomY", "forcex", "forcey"):
+            scale = max(abs(b[key]), 1e-12)
+            assert abs(a[key] - b[key]) <= 1e-8 * scale, (k, key, a[key], b[key])
+
+
+def test_heavy_disk_sinks_and_light_disk_rises(ref):
+    for args, sign in ((HEAVY, -1), (LIGHT, 1)):
+        s = Simulation(args)
+        s.init()
+        for _ in range(4):
+            s.advance(s.calcMaxTimestep())
+        assert np.sign(s.ctx.shape(0)["v"]) == sign
+
+
+def test_gravity_is_a_parameter(ref):
+    args = HEAVY + " -gravity '0.5 -2'"
+    s = Simulation(args)
+    r = ref.RefSim(HEAVY)
+    r.set_gravity(0.5, -2.0)
+    s.init()
+    for _ in range(2):
+        r.step()
+        s.advance(s.calcMaxTimestep())
+    s.ctx.sync()
+    for f in ("u", "v", "pres"):
+        assert _rel(s.ctx.get(f), r.get(f)) <= TOL, f
+    assert s.ctx.shape(0)["u"] > 0
+
+
+def test_without_iterated_penalization_refused():
+    with pytest.raises(Cup2DError) as e:
+        Simulation(HEAVY.replace("-iterativePenalization 1", "")).init()
+    assert e.value.code == ENOTSUP
+
+
+def test_invrho_field_of_constant_density():
+    s = Simulation("-bpdx 2 -bpdy 2 -shapes 'disk radius=0.1'")
+    s.init()
+    assert np.all(s.ctx.get("invRho") == 1.0)
+    with pytest.raises(Cup2DError) as e:
+        s.ctx.set("invRho", np.ones((s.ctx.ny, s.ctx.nx)))
+    assert e.value.code == ESTATE
+
+
+def test_checkpoint_restart_continues_bitwise():
+    a = Simulation(PAIR)
+    a.init()
+    for _ in range(2):
+        a.advance(a.calcMaxTimestep())
+    blob = a.ctx.checkpoint()
+    b = Simulation(PAIR)
+    b.init()
+    b.ctx.restore(blob)
+    for s in (a, b):
+        for _ in range(2):
+            s.advance(s.calcMaxTimestep())
+        s.ctx.sync()
+    for f in ("u", "v", "pres", "invRho"):
+        assert np.array_equal(a.ctx.get(f), b.ctx.get(f)), f
+    assert a.ctx.iteration_stats() == b.ctx.iteration_stats()
