@@ -69,9 +69,37 @@ __device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
 // halves of the shared-memory banks), the staged quarter twiddle table
 // (w^j, j < L/4), the sequences per CTA B and the threads per CTA NT
 // (L/E per sequence: every thread owns E = 16 or 8 elements of a pass).
+// ---- per-pass twiddle tables ---------------------------------------------
+// The passes of fft_inplace<L, ..., E> (fft_passes): sub-transform sizes
+// NS = 1, E, E^2, ... with radix E while NS E <= L, then one pass of radix
+// L/NS.  The pass over sub-transforms of size NS scales input m of the
+// butterfly with k = j mod NS by W^(m k), W = exp(-2 pi i/(R NS)).  For each
+// pass with NS > 1 the tables hold W^(p k), k < NS, for the powers p = 1, 2,
+// 4, 8 below R (one table of NS entries each): the butterflies of a warp
+// read consecutive entries (no shared-memory bank conflicts, where indexing
+// one table by m k made every lane of a warp hit the same banks), and the
+// other powers are products of at most three table values.
+constexpr int tw_npow(int R) { return R >= 16 ? 4 : (R >= 8 ? 3 : (R >= 4 ? 2 : (R >= 2 ? 1 : 0))); }
+// offset of the tables of the pass over sub-transforms of size NS
+template <int L, int E> constexpr int tw_off(int NS) {
+  int off = 0, ns = 1;
+  while (ns < L && ns < NS) {
+    const int r = ns * E <= L ? E : L / ns;
+    if (ns > 1) off += tw_npow(r) * ns;
+    ns *= r;
+  }
+  return off;
+}
+template <int L, int E> constexpr int tw_size() { return tw_off<L, E>(L); }
+// entries staged per CTA: enough for the element counts E = 8 and 16
+template <int L> constexpr int tw_max() {
+  const int a = tw_size<L, 8>(), b = tw_size<L, 16>();
+  return a > b ? (a > 0 ? a : 1) : (b > 0 ? b : 1);
+}
+
 template <int L, int E = 16> struct Len {
   static constexpr int SL = L + L / 16 + 4;
-  static constexpr int TW = L / 4;
+  static constexpr int TW = tw_max<L>();
   static constexpr int B = 2048 / L < 1 ? 1 : (2048 / L > 8 ? 8 : 2048 / L);
   static constexpr int NT0 = B * L / E;
   static constexpr int NT = NT0 < 64 ? 64 : (NT0 > 512 ? 512 : NT0);
@@ -96,26 +124,60 @@ constexpr int E_ROWS32 = 8;
 constexpr int E_C2R32 = 8;
 constexpr int E_COLS32 = 16;
 
-// Twiddles w^j = exp(-2 pi i j / L), j < L/4, staged in shared memory.
-template <int L, class C>
+// Stages the per-pass tables of fft_inplace<L, ..., E> from the global
+// table tw[j] = exp(-2 pi i j / twLen) (twLen a multiple of 4 L).
+template <int L, int E, class C>
 __device__ __forceinline__ void load_twiddles(C* tws, const C* __restrict__ tw, int twLen) {
-  const int step = twLen / L;
-  for (int j = threadIdx.x; j < Len<L>::TW; j += blockDim.x) tws[j] = tw[j * step];
+  constexpr int total = tw_size<L, E>();
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    int ns = 1, off = 0;
+    while (ns < L) {
+      const int r = ns * E <= L ? E : L / ns;
+      if (ns > 1) {
+        const int n = tw_npow(r) * ns;
+        if (i < off + n) {
+          const int t = i - off, pi = t / ns, k = t - pi * ns;
+          tws[i] = tw[(size_t)(k << pi) * (size_t)(twLen / (r * ns))];
+          break;
+        }
+        off += n;
+      }
+      ns *= r;
+    }
+  }
 }
 
-// w^idx (idx < L) from the quarter table: w^(qL/4 + r) = (-i)^q w^r, the
-// rotation being exact; conjugated for the inverse transform.
-template <int L, bool INV, class C>
-__device__ __forceinline__ C twiddle(const C* tws, int idx) {
-  const int q = idx / (L / 4), r = idx & (L / 4 - 1);
-  const C w = tws[r];
-  C v;
-  if (q == 0) v = w;
-  else if (q == 1) v = mk<C>(w.y, -w.x);
-  else if (q == 2) v = mk<C>(-w.x, -w.y);
-  else v = mk<C>(-w.y, w.x);
-  if (INV) v.y = -v.y;
-  return v;
+// Scales xb[m], 0 < m < R, of the butterfly k of the pass over
+// sub-transforms of size NS by W^(m k) (conjugated for the inverse).
+template <int L, int E, int R, int NS, bool INV, class C>
+__device__ __forceinline__ void apply_twiddles(C* xb, const C* tws, int k) {
+  const C* t = tws + tw_off<L, E>(NS) + k;
+  auto ld = [&](int pi) { C w = t[pi * NS]; if (INV) w.y = -w.y; return w; };
+  const C w1 = ld(0);
+  xb[1] = cmul(xb[1], w1);
+  if constexpr (R > 2) {
+    const C w2 = ld(1), w3 = cmul(w1, w2);
+    xb[2] = cmul(xb[2], w2);
+    xb[3] = cmul(xb[3], w3);
+    if constexpr (R > 4) {
+      const C w4 = ld(2);
+      xb[4] = cmul(xb[4], w4);
+      xb[5] = cmul(xb[5], cmul(w1, w4));
+      xb[6] = cmul(xb[6], cmul(w2, w4));
+      xb[7] = cmul(xb[7], cmul(w3, w4));
+      if constexpr (R > 8) {
+        const C w8 = ld(3), w12 = cmul(w4, w8);
+        xb[8] = cmul(xb[8], w8);
+        xb[9] = cmul(xb[9], cmul(w1, w8));
+        xb[10] = cmul(xb[10], cmul(w2, w8));
+        xb[11] = cmul(xb[11], cmul(w3, w8));
+        xb[12] = cmul(xb[12], w12);
+        xb[13] = cmul(xb[13], cmul(w1, w12));
+        xb[14] = cmul(xb[14], cmul(w2, w12));
+        xb[15] = cmul(xb[15], cmul(w3, w12));
+      }
+    }
+  }
 }
 
 // asynchronous global -> shared copies (sm_80+ cp.async), so that every
@@ -251,11 +313,7 @@ __device__ __forceinline__ void fft_pass(C* A, int nseq, const C* tws)
     for (int u = 0; u < NB; u++) {
       C* xb = x + u * R;
       const int jb = j + u * T, k = jb & (NS - 1);
-      if (NS > 1 && k) {
-        const int base = k * (L / (R * NS));
-#pragma unroll
-        for (int m = 1; m < R; m++) xb[m] = cmul(xb[m], twiddle<L, INV>(tws, m * base));
-      }
+      if (NS > 1 && k) apply_twiddles<L, E, R, NS, INV>(xb, tws, k);
       dft<R, INV>(xb);
       const int o = (jb - k) * R + k, po = pad(o);
 #pragma unroll
@@ -345,10 +403,7 @@ __device__ __forceinline__ void fft_convolve(C* A, int nseq, const C* tws, Mul m
     for (int u = 0; u < NB; u++) {
       C* xb = x + u * R;
       const int jb = j + u * T;
-      if (jb) {
-#pragma unroll
-        for (int m = 1; m < R; m++) xb[m] = cmul(xb[m], twiddle<L, false>(tws, m * jb));
-      }
+      if (jb) apply_twiddles<L, E, R, NS, false>(xb, tws, jb);
       dft<R, false>(xb);
 #pragma unroll
       for (int q = 0; q < R; q++) y[u + NB * q] = mul(sq, jb + q * NS, xb[out_reg<R>(q)]);
@@ -412,11 +467,7 @@ __device__ __forceinline__ void fft_last_pass_global(C* A, int nseq, const C* tw
   for (int u = 0; u < NB; u++) {
     C* xb = x + u * R;
     const int jb = j + u * T, k = jb & (NS - 1);
-    if (NS > 1 && k) {
-      const int base = k * (L / (R * NS));
-#pragma unroll
-      for (int m = 1; m < R; m++) xb[m] = cmul(xb[m], twiddle<L, true>(tws, m * base));
-    }
+    if (NS > 1 && k) apply_twiddles<L, E, R, NS, true>(xb, tws, k);
     dft<R, true>(xb);
     const int o = (jb - k) * R + k;
 #pragma unroll
@@ -504,7 +555,7 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
     // goes (cub2rhs, PoissonSolver.cpp:61-141) and writing them back
     __shared__ double sCorr0;
     if (fa.enabled) fade_corr_cta(fa, &sCorr0);
-    load_twiddles<L>(tws, tw, twLen);
+    load_twiddles<L, E_ROWS>(tws, tw, twLen);
     __syncthreads();
     const double corr = fa.enabled ? sCorr0 : 0.0;
     const int bandX = fa.enabled ? (int)(fa.g.fadeLenX / fa.g.h) + 2 : 0;
@@ -563,7 +614,7 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
       A[r * SL + pad(n)] = make_double2(x[0], x[1]);
     }
   }
-  load_twiddles<L>(tws, tw, twLen);
+  load_twiddles<L, E_ROWS>(tws, tw, twLen);
   __syncthreads();
   fft_inplace<L, false, HIN, false, E_ROWS>(A, nb, tws);
   r2c_split<L>(A, nb, row0, out, outStride, tw, twLen);
@@ -607,7 +658,7 @@ k_cols(double2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrows
     const int r = nrowsIn + idx / CB, j = idx & (CB - 1);
     A[j * SL + pad(r)] = make_double2(0, 0);
   }
-  load_twiddles<L>(tws, tw, twLen);
+  load_twiddles<L, E_COLS>(tws, tw, twLen);
   if (mode == 1) {
     cp_async_wait<0>();
     __syncthreads();
@@ -665,7 +716,7 @@ k_rows_c2r(const double2* __restrict__ in, int inStride, int nrows, double* __re
     if (r < nb) cp_async16(A + r * SL + pad(k), in + (size_t)(row0 + r) * inStride + k);
   }
   cp_async_commit();
-  load_twiddles<L>(tws, tw, twLen);
+  load_twiddles<L, E_C2R>(tws, tw, twLen);
   cp_async_wait<0>();
   __syncthreads();
   // z[k] = s + i t, s = X_k + conj(X_{L-k}), t = W^-k (X_k - conj(X_{L-k})):
@@ -736,7 +787,7 @@ k_rows_r2c32(const double* __restrict__ in, int inStride, int nrows, int ncolsIn
   }
   __shared__ double sCorr;
   if (fa.enabled) fade_corr_cta(fa, &sCorr);
-  load_twiddles<L>(tws, tw, twLen);
+  load_twiddles<L, E_ROWS32>(tws, tw, twLen);
   __syncthreads();
   const double corr = fa.enabled ? sCorr : 0.0;
   const int bandX = fa.enabled ? (int)(fa.g.fadeLenX / fa.g.h) + 2 : 0;
@@ -809,7 +860,7 @@ k_cols32(float2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrow
     const int r = nrowsIn + idx / CB, j = idx & (CB - 1);
     A[j * SL + pad(r)] = make_float2(0, 0);
   }
-  load_twiddles<L>(tws, tw, twLen);
+  load_twiddles<L, E_COLS32>(tws, tw, twLen);
   cp_async_wait<0>();
   __syncthreads();
   if (mode == 0) {
@@ -857,7 +908,7 @@ k_rows_c2r32(const float2* __restrict__ in, int inStride, int nrows, double* __r
     if (r < nb) cp_async8(A + r * SL + pad(k), in + (size_t)(row0 + r) * inStride + k);
   }
   cp_async_commit();
-  load_twiddles<L>(tws, tw, twLen);
+  load_twiddles<L, E_C2R32>(tws, tw, twLen);
   cp_async_wait<0>();
   __syncthreads();
   for (int idx = threadIdx.x; idx < RB * H; idx += NT) {
@@ -916,7 +967,7 @@ k_dct_rows_fwd(const double* in, int Nx, int nrows, double* __restrict__ D, int 
   double* Bx = reinterpret_cast<double*>(tws + Len<L>::TW);     // staged real row values
   __shared__ double sCorr;
   fade_corr_cta(fa, &sCorr);
-  load_twiddles<L>(tws, tw, twLen);
+  load_twiddles<L, 16>(tws, tw, twLen);
   const int row0 = blockIdx.x * rb;
   const int nb = min(rb, nrows - row0);
   __syncthreads();
@@ -971,7 +1022,7 @@ k_dct_cols(double* D, int Nx, int Ny, int cb, const float* __restrict__ cosX, co
   extern __shared__ double2 sm[];
   double2* A = sm;
   double2* tws = sm + cb * SL;
-  load_twiddles<L>(tws, tw, twLen);
+  load_twiddles<L, 16>(tws, tw, twLen);
   const int n = Ny;                                   // L = 2n
   const int c0 = blockIdx.x * cb * 2;                 // first column of this CTA
   const int np = min(cb, (Nx - c0) / 2);              // column pairs
@@ -1042,7 +1093,7 @@ k_dct_rows_inv(const double* __restrict__ D, int Nx, int nrows, double* __restri
   extern __shared__ double2 sm[];
   double2* A = sm;
   double2* tws = sm + rb * SL;
-  load_twiddles<L>(tws, tw, twLen);
+  load_twiddles<L, 16>(tws, tw, twLen);
   const int row0 = blockIdx.x * rb;
   const int nb = min(rb, nrows - row0);
   const int st2 = twLen / (2 * L), st4 = twLen / (4 * L);
