@@ -178,22 +178,101 @@ k_outflow_flux(GridDesc g, const Scalars* sc, const double* __restrict__ u, cons
 // adv_cell on the staged tile: U, V hold the block's cells and a two-cell
 // halo (tile position (lx + 2, ly + 2) for block cell (lx, ly)); the domain
 // edge tests use the global cell (gx, gy), as adv_cell does
+// EDGE = false: a cell whose four neighbours are all inside the domain (no
+// ghost tests); COMP: both components (2), or only u (0) or v (1).  The
+// same expressions in every case.
+template <bool EDGE = true, int COMP = 2>
 __device__ __forceinline__ void adv_cell_tile(const GridDesc& g, const AdvCoef& k, const double* U,
                                               const double* V, int lx, int ly, int gx, int gy,
                                               double& unew, double& vnew) {
   const int t = (ly + 2) * ADV_HT + lx + 2;
   const double ucc = U[t], vcc = V[t];
   double ulx, vlx, upx, vpx, uly, vly, upy, vpy;
-  if (gx > 0) { ulx = U[t - 1]; vlx = V[t - 1]; } else { ulx = ucc * k.fadeW; vlx = vcc * k.fadeW; }
-  if (gx < g.nx - 1) { upx = U[t + 1]; vpx = V[t + 1]; } else { upx = ucc * k.fadeE; vpx = vcc * k.fadeE; }
-  if (gy > 0) { uly = U[t - ADV_HT]; vly = V[t - ADV_HT]; } else { uly = ucc * k.fadeS; vly = vcc * k.fadeS; }
-  if (gy < g.ny - 1) { upy = U[t + ADV_HT]; vpy = V[t + ADV_HT]; } else { upy = ucc * k.fadeN; vpy = vcc * k.fadeN; }
-  const double dUadv = (ucc + k.U0) * (upx - ulx) + (vcc + k.U1) * (upy - uly);
-  const double dUdif = upx + upy + ulx + uly - 4 * ucc;
-  const double dVadv = (ucc + k.U0) * (vpx - vlx) + (vcc + k.U1) * (vpy - vly);
-  const double dVdif = vpx + vpy + vlx + vly - 4 * vcc;
-  unew = ucc + (k.afac * dUadv + k.dfac * dUdif);
-  vnew = vcc + (k.afac * dVadv + k.dfac * dVdif);
+  if (!EDGE || gx > 0) { ulx = U[t - 1]; vlx = V[t - 1]; } else { ulx = ucc * k.fadeW; vlx = vcc * k.fadeW; }
+  if (!EDGE || gx < g.nx - 1) { upx = U[t + 1]; vpx = V[t + 1]; } else { upx = ucc * k.fadeE; vpx = vcc * k.fadeE; }
+  if (!EDGE || gy > 0) { uly = U[t - ADV_HT]; vly = V[t - ADV_HT]; } else { uly = ucc * k.fadeS; vly = vcc * k.fadeS; }
+  if (!EDGE || gy < g.ny - 1) { upy = U[t + ADV_HT]; vpy = V[t + ADV_HT]; } else { upy = ucc * k.fadeN; vpy = vcc * k.fadeN; }
+  if (COMP != 1) {
+    const double dUadv = (ucc + k.U0) * (upx - ulx) + (vcc + k.U1) * (upy - uly);
+    const double dUdif = upx + upy + ulx + uly - 4 * ucc;
+    unew = ucc + (k.afac * dUadv + k.dfac * dUdif);
+  }
+  if (COMP != 0) {
+    const double dVadv = (ucc + k.U0) * (vpx - vlx) + (vcc + k.U1) * (vpy - vly);
+    const double dVdif = vpx + vpy + vlx + vly - 4 * vcc;
+    vnew = vcc + (k.afac * dVadv + k.dfac * dVdif);
+  }
+}
+
+// k_advdiff after its tiles landed: the update with the outflow
+// correction, the halo of the new velocity, the divergence and the fade
+// sums.  EDGE = false for a block away from the domain edge.
+template <bool EDGE>
+__device__ __forceinline__ void advdiff_tile_body(const GridDesc& g, const AdvCoef& kc, const double* tU,
+                                                  const double* tV, double (*su)[BS + 2], double (*sv)[BS],
+                                                  double corr, double facDiv, double* __restrict__ un,
+                                                  double* __restrict__ vn, double* __restrict__ rhs,
+                                                  const int* __restrict__ fadeSlot,
+                                                  double* __restrict__ fadePartials) {
+  const int bx = blockIdx.x, by = blockIdx.y, tx = threadIdx.x, ty = threadIdx.y, tid = lin_tid();
+  const int nx = g.nx, ny = g.ny;
+  const int gx = bx * BS + tx;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int iy = ty + 8 * r, gy = by * BS + iy;
+    double unew, vnew;
+    adv_cell_tile<EDGE>(g, kc, tU, tV, tx, iy, gx, gy, unew, vnew);
+    if (EDGE) {
+      if (gx == 0) unew = unew + corr;                   // advDiff.cpp:107-115
+      if (gx == nx - 1) unew = unew - corr;
+      if (gy == 0) vnew = vnew + corr;
+      if (gy == ny - 1) vnew = vnew - corr;
+    }
+    const size_t c = (size_t)gy * nx + gx;
+    un[c] = unew; vn[c] = vnew;
+    su[iy][tx + 1] = unew; sv[iy + 1][tx] = vnew;
+  }
+  // halo: warps 0-3, one lane per cell (u west / east column, v south /
+  // north row of the neighbouring blocks)
+  if (ty < 4) {
+    const int side = ty;
+    const bool have = side == 0 ? bx > 0 : side == 1 ? bx < g.bpdx - 1 : side == 2 ? by > 0 : by < g.bpdy - 1;
+    if (have) {
+      const int lx = side == 0 ? -1 : side == 1 ? BS : tx;
+      const int ly = side == 2 ? -1 : side == 3 ? BS : tx;
+      double unew, vnew;
+      if (side < 2) {                                  // only u of the west / east columns
+        adv_cell_tile<EDGE, 0>(g, kc, tU, tV, lx, ly, bx * BS + lx, by * BS + ly, unew, vnew);
+        su[tx][side == 0 ? 0 : BS + 1] = unew;
+      } else {                                         // only v of the south / north rows
+        adv_cell_tile<EDGE, 1>(g, kc, tU, tV, lx, ly, bx * BS + lx, by * BS + ly, unew, vnew);
+        sv[side == 2 ? 0 : BS + 1][tx] = vnew;
+      }
+    }
+  }
+  __syncthreads();
+  const bool touch = fade_touch(g, bx, by);
+  double s[3] = {0, 0, 0};
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int iy = ty + 8 * r, gy = by * BS + iy;
+    const double uW = !EDGE || gx > 0 ? su[iy][tx] : su[iy][tx + 1];
+    const double uE = !EDGE || gx < nx - 1 ? su[iy][tx + 2] : su[iy][tx + 1];
+    const double vS = !EDGE || gy > 0 ? sv[iy][tx] : sv[iy + 1][tx];
+    const double vN = !EDGE || gy < ny - 1 ? sv[iy + 2][tx] : sv[iy + 1][tx];
+    const double divVx = uE - uW, divVy = vN - vS;
+    const double b = facDiv * (divVx + divVy);
+    rhs[(size_t)gy * nx + gx] = b;
+    if (touch) fade_accumulate(g, bx, by, tx, iy, b, s);
+  }
+  if (touch) {                                         // uniform over the CTA
+    __shared__ double red[96];
+    block_sum<3>(s, red);
+    if (tid == 0) {
+      const int q = fadeSlot[bx + g.bpdx * by];
+      for (int k = 0; k < 3; k++) fadePartials[3 * q + k] = s[k];
+    }
+  }
 }
 
 // advDiff.cpp:57-116 with PressureSingle.cpp:112-128 in place, one CTA per
@@ -236,66 +315,25 @@ k_advdiff(const __grid_constant__ CUtensorMap tmU, const __grid_constant__ CUten
   const double facDiv = 0.5 * g.h / sc->dt;
   const int nx = g.nx, ny = g.ny;
   const int gx = bx * BS + tx;
-  const bool landed = mbar_wait_bounded(&bar, 0, TMA_WAIT_NS);
+  // one thread waits for the tiles (the others at the CTA barrier, where
+  // they take no issue slots); its acquire of the barrier's phase and the
+  // CTA barrier make the tiles visible to every thread
+  bool landed = true;
+  if (tid == 0) landed = mbar_wait_bounded(&bar, 0, TMA_WAIT_NS);
   if (__syncthreads_or(!landed)) {
-    // the loads did not land: report, give them the same time again, leave
-    // (the whole CTA takes this branch)
-    if (tid == 0) atomicOr(&sc->status, ST_TIMEOUT);
-    mbar_wait_bounded(&bar, 0, TMA_WAIT_NS);
+    // the loads did not land: report, give them the same time again (the
+    // CTA's shared memory stays while thread 0 waits), leave
+    if (tid == 0) {
+      atomicOr(&sc->status, ST_TIMEOUT);
+      mbar_wait_bounded(&bar, 0, TMA_WAIT_NS);
+    }
     return;
   }
-#pragma unroll
-  for (int r = 0; r < 4; r++) {
-    const int iy = ty + 8 * r, gy = by * BS + iy;
-    double unew, vnew;
-    adv_cell_tile(g, kc, tU, tV, tx, iy, gx, gy, unew, vnew);
-    if (gx == 0) unew = unew + corr;                     // advDiff.cpp:107-115
-    if (gx == nx - 1) unew = unew - corr;
-    if (gy == 0) vnew = vnew + corr;
-    if (gy == ny - 1) vnew = vnew - corr;
-    const size_t c = (size_t)gy * nx + gx;
-    un[c] = unew; vn[c] = vnew;
-    su[iy][tx + 1] = unew; sv[iy + 1][tx] = vnew;
-  }
-  // halo: warps 0-3, one lane per cell (u west / east column, v south /
-  // north row of the neighbouring blocks)
-  if (ty < 4) {
-    const int side = ty;
-    const bool have = side == 0 ? bx > 0 : side == 1 ? bx < g.bpdx - 1 : side == 2 ? by > 0 : by < g.bpdy - 1;
-    if (have) {
-      const int lx = side == 0 ? -1 : side == 1 ? BS : tx;
-      const int ly = side == 2 ? -1 : side == 3 ? BS : tx;
-      double unew, vnew;
-      adv_cell_tile(g, kc, tU, tV, lx, ly, bx * BS + lx, by * BS + ly, unew, vnew);
-      if (side == 0) su[tx][0] = unew;
-      else if (side == 1) su[tx][BS + 1] = unew;
-      else if (side == 2) sv[0][tx] = vnew;
-      else sv[BS + 1][tx] = vnew;
-    }
-  }
-  __syncthreads();
-  const bool touch = fade_touch(g, bx, by);
-  double s[3] = {0, 0, 0};
-#pragma unroll
-  for (int r = 0; r < 4; r++) {
-    const int iy = ty + 8 * r, gy = by * BS + iy;
-    const double uW = gx > 0 ? su[iy][tx] : su[iy][tx + 1];
-    const double uE = gx < nx - 1 ? su[iy][tx + 2] : su[iy][tx + 1];
-    const double vS = gy > 0 ? sv[iy][tx] : sv[iy + 1][tx];
-    const double vN = gy < ny - 1 ? sv[iy + 2][tx] : sv[iy + 1][tx];
-    const double divVx = uE - uW, divVy = vN - vS;
-    const double b = facDiv * (divVx + divVy);
-    rhs[(size_t)gy * nx + gx] = b;
-    if (touch) fade_accumulate(g, bx, by, tx, iy, b, s);
-  }
-  if (touch) {                                         // uniform over the CTA
-    __shared__ double red[96];
-    block_sum<3>(s, red);
-    if (tid == 0) {
-      const int q = fadeSlot[bx + g.bpdx * by];
-      for (int k = 0; k < 3; k++) fadePartials[3 * q + k] = s[k];
-    }
-  }
+  // blocks away from the domain edge: no ghost, outflow or one-sided tests
+  if (bx > 0 && by > 0 && bx < g.bpdx - 1 && by < g.bpdy - 1)
+    advdiff_tile_body<false>(g, kc, tU, tV, su, sv, corr, facDiv, un, vn, rhs, fadeSlot, fadePartials);
+  else
+    advdiff_tile_body<true>(g, kc, tU, tV, su, sv, corr, facDiv, un, vn, rhs, fadeSlot, fadePartials);
 }
 
 // PressureSingle.cpp:112-128: tmp = (h / 2dt) * div_2h(u); zero-gradient ghosts

@@ -116,7 +116,10 @@ template <int L, int E = 16> struct Len {
 #ifndef CUP2D_E_C2R
 #define CUP2D_E_C2R 16
 #endif
-constexpr int E_ROWS = 8;
+#ifndef CUP2D_E_ROWS
+#define CUP2D_E_ROWS 8
+#endif
+constexpr int E_ROWS = CUP2D_E_ROWS;
 constexpr int E_C2R = CUP2D_E_C2R;
 constexpr int E_COLS = CUP2D_E_COLS;
 // the same for the FP32 transforms (half the registers per value)

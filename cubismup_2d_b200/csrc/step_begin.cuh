@@ -61,14 +61,23 @@ __device__ __forceinline__ bool max_u_cta(const GridDesc& g, Scalars* sc,
   const size_t n2 = (size_t)g.nx * g.ny / 2;        // Nx is a multiple of 32
   const double2* u2 = reinterpret_cast<const double2*>(u);
   const double2* v2 = reinterpret_cast<const double2*>(v);
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const double2 a2 = u2[i], b2 = v2[i];
-    // Helpers.cpp:160-166: max of |u+uinf|, |v+vinf|, |u|, |v|
+  // Helpers.cpp:160-166: max of |u+uinf|, |v+vinf|, |u|, |v| (four
+  // iterations' loads issued before their maxima, for bytes in flight)
+  auto take = [&](double2 a2, double2 b2) {
     m = fmax(m, cell_speed(a2.x, b2.x, UINF, VINF));
     m = fmax(m, cell_speed(a2.y, b2.y, UINF, VINF));
     bad |= !isfinite(a2.x) || !isfinite(b2.x) || !isfinite(a2.y) || !isfinite(b2.y);
+  };
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  for (; i + 3 * stride < n2; i += 4 * stride) {
+    double2 a2[4], b2[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) { a2[q] = u2[i + q * stride]; b2[q] = v2[i + q * stride]; }
+#pragma unroll
+    for (int q = 0; q < 4; q++) take(a2[q], b2[q]);
   }
+  for (; i < n2; i += stride) take(u2[i], v2[i]);
   m = block_max(m, red);
   const int anyBad = __syncthreads_or(bad);
   if (lin_tid() == 0) {

@@ -20,6 +20,10 @@ LIGHT = ("-bpdx 4 -bpdy 4 -nu 1e-3 " + VR +                      # cosine solver
 PAIR = ("-bpdx 8 -bpdy 4 -nu 1e-3 -poissonType freespace " + VR +
         "-shapes 'disk radius=0.07 xpos=0.42 ypos=0.25 rhoS=2,"
         "disk radius=0.07 xpos=0.58 ypos=0.26 rhoS=0.9'")
+# a swimmer beside the falling body: the fish's udef in the momenta and the
+# penalization of PressureVarRho_approx (its rho is 1 on the fish's tiles)
+FISH_DISK = ("-bpdx 8 -bpdy 4 -nu 1e-4 -poissonType freespace " + VR +
+             "-shapes 'stefanfish L=0.18 T=1 xpos=0.35 ypos=0.25, disk radius=0.05 xpos=0.75 ypos=0.3 rhoS=1.5'")
 TOL = 1e-9
 
 
@@ -64,7 +68,7 @@ def test_operators_match_reference(ref, args):
     assert not np.any(s.ctx.get("udef_x")) and not np.any(r.get("udef_x"))
 
 
-@pytest.mark.parametrize("args", [HEAVY, PAIR], ids=["heavy", "pair"])
+@pytest.mark.parametrize("args", [HEAVY, PAIR, FISH_DISK], ids=["heavy", "pair", "fish_and_disk"])
 def test_steps_match_reference(ref, args):
     r, s = _pair(ref, args)
     for _ in range(3):
