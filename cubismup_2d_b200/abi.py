@@ -42,6 +42,7 @@ EXPORTS = [
     "cup2d_ensemble_sync", "cup2d_ensemble_get_shapes", "cup2d_ensemble_last_error",
     "cup2d_ensemble_destroy",
     "cup2d_fish_act", "cup2d_fish_period", "cup2d_fish_state", "cup2d_dump", "cup2d_poisson_solve",
+    "cup2d_tuning_get",
     "cup2d_adv_diff_noalloc",
 ]
 KERNELS = {"advdiff": 0, "rhs_div": 1, "pcorr": 2, "fft_rows_fwd": 3, "fft_cols": 4,
@@ -54,7 +55,7 @@ class Config(ctypes.Structure):
                 ("nu", ctypes.c_double), ("fadeLen", ctypes.c_double), ("nsteps", ctypes.c_int),
                 ("tend", ctypes.c_double), ("poisson", ctypes.c_int), ("precision", ctypes.c_int),
                 ("device", ctypes.c_int), ("iterative", ctypes.c_int),
-                ("gravity", ctypes.c_double * 2), ("implicit_penalization", ctypes.c_int)]
+                ("gravity", ctypes.c_double * 2), ("implicit_penalization", ctypes.c_int), ("autotune", ctypes.c_int)]
 
 
 class ShapeParams(ctypes.Structure):
@@ -76,6 +77,11 @@ SHAPE_STATE_FIELDS = [
     "torque", "torque_P", "torque_V", "drag", "thrust", "circulation",
     "Pout", "PoutBnd", "defPower", "defPowerBnd", "Pthrust", "Pdrag", "EffPDef", "EffPDefBnd",
 ]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("fft_rows_fwd_e", ctypes.c_int), ("fft_rows_inv_e", ctypes.c_int), ("tuned", ctypes.c_int),
+                ("us", ctypes.c_double * 4)]
 
 
 class ShapeState(ctypes.Structure):
@@ -135,6 +141,7 @@ def lib():
     L.cup2d_adv_diff_noalloc.argtypes = [vp, vp, vp, vp, i, i, d, d, d, d, d, vp]
     L.cup2d_dump.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p]
     L.cup2d_poisson_solve.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    L.cup2d_tuning_get.argtypes = [vp, ctypes.POINTER(Tuning)]
     L.cup2d_fish_act.argtypes = [vp, i, d, dp, i]
     L.cup2d_fish_period.argtypes = [vp, i, dp]
     L.cup2d_fish_state.argtypes = [vp, i, i, dp, i]
@@ -205,6 +212,7 @@ def parse_args(argline):
     cfg.iterative = int(args.get("iterativePenalization", 0)) != 0     # Simulation.cpp:101
     # PressureSingle without EXPL_INTEGRATE_MOM (a compile-time switch there)
     cfg.implicit_penalization = int(args.get("implicitPenalization", 0)) != 0
+    cfg.autotune = int(args.get("autotune", 0)) != 0       # time the transform variants at set-up
     if "gravity" in args:                  # the reference fixes it at (0, -9.8), SimulationData.h:57
         gx, gy = (float(x) for x in args["gravity"].split())
         cfg.gravity[0], cfg.gravity[1] = gx, gy
@@ -298,6 +306,14 @@ class Context:
 
     def compute_forces(self, dt=-1.0):
         self._ck(self.L.cup2d_compute_forces(self.h_, dt))
+
+    def tuning(self):
+        """The transform variants in use (values per thread of the forward and
+        inverse row passes) and, with -autotune 1, the times measured (us)."""
+        t = Tuning()
+        self._ck(self.L.cup2d_tuning_get(self.h_, ctypes.byref(t)))
+        return {"fft_rows_fwd_e": t.fft_rows_fwd_e, "fft_rows_inv_e": t.fft_rows_inv_e,
+                "tuned": bool(t.tuned), "us": list(t.us)}
 
     def poisson_solve(self, src="tmp", dst="pres"):
         """PoissonSolver::solve(BSRC, BDST): the context's solver on field

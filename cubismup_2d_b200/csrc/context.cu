@@ -499,6 +499,9 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
   if (cudaMemset(c.counters, 0, sizeof(unsigned) * Ctx::NCOUNTERS) != cudaSuccess) { cup2d_destroy(ctx); return CUP2D_ECUDA; }
   c.poisson = poisson_create(c);
   if (!c.poisson) { cup2d_destroy(ctx); return create_fail(CUP2D_ENOMEM, "Poisson solver set-up failed"); }
+  if (cfg->autotune && poisson_autotune(c) != cudaSuccess) {
+    cup2d_destroy(ctx); return create_fail(CUP2D_ECUDA, "transform autotuning failed");
+  }
   if (cudaStreamSynchronize(c.stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
     cup2d_destroy(ctx); return CUP2D_ECUDA;
   }
@@ -757,6 +760,12 @@ int cup2d_init(cup2d_ctx* ctx) {
   if ((rc = check_launch(ctx))) return rc;
   c.initialised = true;
   c.midByGraph = false;
+  return CUP2D_OK;
+}
+
+int cup2d_tuning_get(cup2d_ctx* ctx, cup2d_tuning* out) {
+  if (!ctx || !out) return CUP2D_EINVAL;
+  poisson_tuning(ctx->c, out);
   return CUP2D_OK;
 }
 

@@ -79,6 +79,8 @@ bool poisson_size_ok(int type, int nx, int ny);
 const char* poisson_size_limits(int type);
 void poisson_destroy(Poisson* p);
 void poisson_solve(Ctx& c);                          // PoissonSolver::solve of the chosen solver
+cudaError_t poisson_autotune(Ctx& c);                // the row passes' variants timed on this grid
+void poisson_tuning(const Ctx& c, cup2d_tuning* out);
 void poisson_rows_fwd(Ctx& c);
 void poisson_cols(Ctx& c);
 void poisson_rows_inv(Ctx& c);

@@ -20,7 +20,12 @@
 // log2 L is odd) in shared memory padded by one element per 16 against bank
 // conflicts, twiddles from one host-computed table; one CTA transforms a few
 // rows (or columns) with L/4 threads each.
+#include <algorithm>
+#include <array>
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 #include "context.hpp"
 
@@ -43,6 +48,12 @@ struct Poisson {
   float* ghat32 = nullptr;   // ghat rounded to FP32
   int rb = 1, cb = 1;        // rows / columns per CTA
   int MX = 0, MY = 0;        // free space: the padded grid (powers of two >= 2Nx, 2Ny)
+  // elements per thread of the forward and inverse row passes (FP64 free
+  // space and periodic), and the times the autotuner measured (us; r2c with
+  // 8 and 16, c2r with 8 and 16; zero when not tuned)
+  int eR2C = 8, eC2R = 16;
+  bool tuned = false;
+  double tuneUs[4] = {0, 0, 0, 0};
 };
 
 namespace {
@@ -106,22 +117,14 @@ template <int L, int E = 16> struct Len {
   static constexpr int REGS = E == 16 ? 128 : 64;   // register budget per thread
   static constexpr int MINB = 65536 / (NT * REGS) < 1 ? 1 : 65536 / (NT * REGS);
 };
-// elements per thread of the forward row pass (few rows: twice the threads
-// of E = 16 for latency hiding, at one more shared-memory pass; measured
-// faster), of the inverse row pass and of the column pass (measured faster
-// with E = 16)
-#ifndef CUP2D_E_COLS
-#define CUP2D_E_COLS 16
-#endif
-#ifndef CUP2D_E_C2R
-#define CUP2D_E_C2R 16
-#endif
-#ifndef CUP2D_E_ROWS
-#define CUP2D_E_ROWS 8
-#endif
-constexpr int E_ROWS = CUP2D_E_ROWS;
-constexpr int E_C2R = CUP2D_E_C2R;
-constexpr int E_COLS = CUP2D_E_COLS;
+// elements per thread: the row passes have two instantiations each (8 and
+// 16: a forward row of 4096 points runs faster with 16, shorter rows with
+// 8, measured on B200), chosen per grid at set-up (table below, or timed
+// by poisson_autotune); the column pass uses 16 (faster at every length
+// measured)
+constexpr int E_ROWS = 8;
+constexpr int E_C2R = 16;
+constexpr int E_COLS = 16;
 // the same for the FP32 transforms (half the registers per value)
 constexpr int E_ROWS32 = 8;
 constexpr int E_C2R32 = 8;
@@ -518,11 +521,11 @@ __device__ __forceinline__ double fade_cell(const GridDesc& g, int gx, int gy, d
 // Real FFT of length 2L from the complex FFT Z of length L of its value
 // pairs, even/odd split: X[k] = Fe[k] + W^k Fo[k], W = exp(-i pi / L),
 // k in [0, L]; written to row row0 + r of out.
-template <int L>
+template <int L, int ER>
 __device__ __forceinline__ void r2c_split(const double2* A, int nb, int row0, double2* __restrict__ out,
                                           int outStride, const double2* __restrict__ tw, int twLen)
 {
-  constexpr int SL = Len<L, E_ROWS>::SL, NT = Len<L, E_ROWS>::NT;
+  constexpr int SL = Len<L, ER>::SL, NT = Len<L, ER>::NT;
   const int twStep = twLen / (2 * L);
   for (int idx = threadIdx.x; idx < nb * (L + 1); idx += NT) {
     const int r = idx / (L + 1), k = idx - r * (L + 1);
@@ -539,15 +542,15 @@ __device__ __forceinline__ void r2c_split(const double2* A, int nb, int row0, do
 // inMode 0: rows of `in`; 1: the free-space Green's function on the MY x MX
 // padded grid (FFTW_freespace.cpp:108-119) computed on the fly.  Each row of 2L
 // reals is the complex sequence (x[2n], x[2n+1]) of length L.
-template <int L, bool HIN>
-__global__ void __launch_bounds__(Len<L, E_ROWS>::NT, Len<L, E_ROWS>::MINB)
+template <int L, bool HIN, int ER>
+__global__ void __launch_bounds__(Len<L, ER>::NT, Len<L, ER>::MINB)
 k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
            double2* __restrict__ out, int outStride,
            const double2* __restrict__ tw, int twLen, FadeArgs fa, double h, int MX, int MY)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_R2C);
-  constexpr int SL = Len<L, E_ROWS>::SL, RB = Len<L, E_ROWS>::B, NT = Len<L, E_ROWS>::NT;
+  constexpr int SL = Len<L, ER>::SL, RB = Len<L, ER>::B, NT = Len<L, ER>::NT;
   extern __shared__ double2 sm[];
   double2* A = sm;
   double2* tws = sm + RB * SL;
@@ -558,7 +561,7 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
     // goes (cub2rhs, PoissonSolver.cpp:61-141) and writing them back
     __shared__ double sCorr0;
     if (fa.enabled) fade_corr_cta(fa, &sCorr0);
-    load_twiddles<L, E_ROWS>(tws, tw, twLen);
+    load_twiddles<L, ER>(tws, tw, twLen);
     __syncthreads();
     const double corr = fa.enabled ? sCorr0 : 0.0;
     const int bandX = fa.enabled ? (int)(fa.g.fadeLenX / fa.g.h) + 2 : 0;
@@ -584,10 +587,10 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
       }
       return v;
     };
-    fft_first_pass_global<L, E_ROWS, HIN, E_ROWS>(A, nb, ld);
+    fft_first_pass_global<L, ER, HIN, ER>(A, nb, ld);
     __syncthreads();
-    fft_passes<L, E_ROWS, false, false, false, E_ROWS>(A, nb, tws);
-    r2c_split<L>(A, nb, row0, out, outStride, tw, twLen);
+    fft_passes<L, ER, false, false, false, ER>(A, nb, tws);
+    r2c_split<L, ER>(A, nb, row0, out, outStride, tw, twLen);
     return;
   }
   {
@@ -617,10 +620,10 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
       A[r * SL + pad(n)] = make_double2(x[0], x[1]);
     }
   }
-  load_twiddles<L, E_ROWS>(tws, tw, twLen);
+  load_twiddles<L, ER>(tws, tw, twLen);
   __syncthreads();
-  fft_inplace<L, false, HIN, false, E_ROWS>(A, nb, tws);
-  r2c_split<L>(A, nb, row0, out, outStride, tw, twLen);
+  fft_inplace<L, false, HIN, false, ER>(A, nb, tws);
+  r2c_split<L, ER>(A, nb, row0, out, outStride, tw, twLen);
 }
 
 // mode 0: forward, x G^ (real, symmetric in ky), inverse, keep nrowsOut rows
@@ -699,14 +702,14 @@ k_cols(double2* __restrict__ data, int stride, int ncols, int nrowsIn, int nrows
 }
 
 // inverse real FFT of length 2L from X[0..L]; writes the first ncolsOut values
-template <int L, bool HOUT>
-__global__ void __launch_bounds__(Len<L, E_C2R>::NT, Len<L, E_C2R>::MINB)
+template <int L, bool HOUT, int EC>
+__global__ void __launch_bounds__(Len<L, EC>::NT, Len<L, EC>::MINB)
 k_rows_c2r(const double2* __restrict__ in, int inStride, int nrows, double* __restrict__ out,
            int outStride, int ncolsOut, const double2* __restrict__ tw, int twLen)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_C2R);
-  constexpr int SL = Len<L, E_C2R>::SL, RB = Len<L, E_C2R>::B, NT = Len<L, E_C2R>::NT, H = L / 2;
+  constexpr int SL = Len<L, EC>::SL, RB = Len<L, EC>::B, NT = Len<L, EC>::NT, H = L / 2;
   extern __shared__ double2 sm[];
   double2* A = sm;
   double2* tws = sm + RB * SL;
@@ -719,7 +722,7 @@ k_rows_c2r(const double2* __restrict__ in, int inStride, int nrows, double* __re
     if (r < nb) cp_async16(A + r * SL + pad(k), in + (size_t)(row0 + r) * inStride + k);
   }
   cp_async_commit();
-  load_twiddles<L, E_C2R>(tws, tw, twLen);
+  load_twiddles<L, EC>(tws, tw, twLen);
   cp_async_wait<0>();
   __syncthreads();
   // z[k] = s + i t, s = X_k + conj(X_{L-k}), t = W^-k (X_k - conj(X_{L-k})):
@@ -749,9 +752,9 @@ k_rows_c2r(const double2* __restrict__ in, int inStride, int nrows, double* __re
   }
   __syncthreads();
   // the inverse FFT; its last pass writes the value pairs of the row
-  constexpr int NSL = last_ns<L, E_C2R>();
-  fft_passes_below<L, 1, NSL, true, false, E_C2R>(A, nb, tws);
-  fft_last_pass_global<L, L / NSL, NSL, HOUT, E_C2R>(A, nb, tws, [&](int r, int n, double2 v) {
+  constexpr int NSL = last_ns<L, EC>();
+  fft_passes_below<L, 1, NSL, true, false, EC>(A, nb, tws);
+  fft_last_pass_global<L, L / NSL, NSL, HOUT, EC>(A, nb, tws, [&](int r, int n, double2 v) {
     double* o = out + (size_t)(row0 + r) * outStride;
     if (2 * n + 1 < ncolsOut) *reinterpret_cast<double2*>(o + 2 * n) = v;
     else if (2 * n < ncolsOut) o[2 * n] = v.x;
@@ -1140,8 +1143,10 @@ template <int L> inline size_t smem_for32(size_t extraReals = 0) {
 #define CUP2D_FFT_LENGTHS(X) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
 
 void set_all_smem() {
-#define X(L) set_smem((const void*)k_rows_r2c<L, false>); set_smem((const void*)k_rows_r2c<L, true>); \
-             set_smem((const void*)k_rows_c2r<L, false>); set_smem((const void*)k_rows_c2r<L, true>); \
+#define X(L) set_smem((const void*)k_rows_r2c<L, false, 8>); set_smem((const void*)k_rows_r2c<L, true, 8>); \
+             set_smem((const void*)k_rows_r2c<L, false, 16>); set_smem((const void*)k_rows_r2c<L, true, 16>); \
+             set_smem((const void*)k_rows_c2r<L, false, 8>); set_smem((const void*)k_rows_c2r<L, true, 8>); \
+             set_smem((const void*)k_rows_c2r<L, false, 16>); set_smem((const void*)k_rows_c2r<L, true, 16>); \
              set_smem((const void*)k_cols<L, false>); set_smem((const void*)k_cols<L, true>); \
              set_smem((const void*)k_dct_rows_fwd<L>); \
              set_smem((const void*)k_dct_cols<L>); set_smem((const void*)k_dct_rows_inv<L>); \
@@ -1152,15 +1157,27 @@ void set_all_smem() {
 #undef X
 }
 
+template <int LL, int ER>
+void rows_r2c_e(cudaStream_t st, const double* in, int inStride, int nrows, int ncolsIn, int inMode,
+                double2* out, int outStride, const double2* tw, int twLen, FadeArgs fa, double h, int MX, int MY,
+                bool halfIn) {
+  const int grid = (nrows + Len<LL>::B - 1) / Len<LL>::B;
+  if (halfIn) launch_k(k_rows_r2c<LL, true, ER>, grid, Len<LL, ER>::NT, smem_for<LL>(), st,
+                       in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, MX, MY);
+  else launch_k(k_rows_r2c<LL, false, ER>, grid, Len<LL, ER>::NT, smem_for<LL>(), st,
+                in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, MX, MY);
+}
+
+// e: elements per thread (8 or 16)
 bool rows_r2c(int L, cudaStream_t st, const double* in, int inStride, int nrows, int ncolsIn, int inMode,
               double2* out, int outStride, const double2* tw, int twLen, FadeArgs fa, double h, int MX, int MY,
-              bool halfIn) {
+              bool halfIn, int e) {
   switch (L) {
 #define X(LL) case LL: \
-    if (halfIn) launch_k(k_rows_r2c<LL, true>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_ROWS>::NT, smem_for<LL>(), st,  \
-        in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, MX, MY); \
-    else launch_k(k_rows_r2c<LL, false>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_ROWS>::NT, smem_for<LL>(), st,  \
-        in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, MX, MY); \
+    if (e == 16) rows_r2c_e<LL, 16>(st, in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, \
+                                    MX, MY, halfIn); \
+    else rows_r2c_e<LL, 8>(st, in, inStride, nrows, ncolsIn, inMode, out, outStride, tw, twLen, fa, h, MX, MY, \
+                           halfIn); \
     return true;
     CUP2D_FFT_LENGTHS(X)
 #undef X
@@ -1185,14 +1202,23 @@ bool cols(int L, cudaStream_t st, double2* data, int stride, int ncols, int nrow
   return false;
 }
 
+template <int LL, int EC>
+void rows_c2r_e(cudaStream_t st, const double2* in, int inStride, int nrows, double* out, int outStride,
+                int ncolsOut, const double2* tw, int twLen, bool halfOut) {
+  const int grid = (nrows + Len<LL>::B - 1) / Len<LL>::B;
+  if (halfOut) launch_k(k_rows_c2r<LL, true, EC>, grid, Len<LL, EC>::NT, smem_for<LL>(), st,
+                        in, inStride, nrows, out, outStride, ncolsOut, tw, twLen);
+  else launch_k(k_rows_c2r<LL, false, EC>, grid, Len<LL, EC>::NT, smem_for<LL>(), st,
+                in, inStride, nrows, out, outStride, ncolsOut, tw, twLen);
+}
+
+// e: elements per thread (8 or 16)
 bool rows_c2r(int L, cudaStream_t st, const double2* in, int inStride, int nrows, double* out, int outStride,
-              int ncolsOut, const double2* tw, int twLen, bool halfOut) {
+              int ncolsOut, const double2* tw, int twLen, bool halfOut, int e) {
   switch (L) {
 #define X(LL) case LL: \
-    if (halfOut) launch_k(k_rows_c2r<LL, true>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_C2R>::NT, smem_for<LL>(), st,  \
-        in, inStride, nrows, out, outStride, ncolsOut, tw, twLen); \
-    else launch_k(k_rows_c2r<LL, false>, (nrows + Len<LL>::B - 1) / Len<LL>::B, Len<LL, E_C2R>::NT, smem_for<LL>(), st,  \
-        in, inStride, nrows, out, outStride, ncolsOut, tw, twLen); \
+    if (e == 8) rows_c2r_e<LL, 8>(st, in, inStride, nrows, out, outStride, ncolsOut, tw, twLen, halfOut); \
+    else rows_c2r_e<LL, 16>(st, in, inStride, nrows, out, outStride, ncolsOut, tw, twLen, halfOut); \
     return true;
     CUP2D_FFT_LENGTHS(X)
 #undef X
@@ -1330,6 +1356,11 @@ Poisson* poisson_create(Ctx& c) {
     P->Lrow = Nx;          // DCT of length Nx via a real FFT of length 2Nx
     P->Lcol = 2 * Ny;      // DCT of length Ny via a complex FFT of length 2Ny
   }
+  // the built-in choice, measured on B200 (forward rows of 4096 points: 115
+  // us with 16 elements per thread against 127 with 8; 1024 points: 17 us
+  // with 8 against 21; the inverse pass: 16 at both)
+  P->eR2C = P->Lrow >= 4096 ? 16 : 8;
+  P->eC2R = 16;
   if (!is_pow2(P->Lrow) || !is_pow2(P->Lcol) || P->Lrow < 16 || P->Lcol < 16 ||
       P->Lrow > 4096 || P->Lcol > 4096) { delete P; return nullptr; }   // shared-memory limit
   P->nkx = P->Lrow + 1;
@@ -1359,8 +1390,9 @@ Poisson* poisson_create(Ctx& c) {
     // G^ = Re FFT[G] / (MX MY) on the MY x MX padded grid, kept for ky <= MY/2
     if (cudaMalloc(&P->ghat, sizeof(double) * (P->Lcol / 2 + 1) * P->nkx) != cudaSuccess) { poisson_destroy(P); return nullptr; }
     FadeArgs fa{}; fa.enabled = 0;
+    // (always with 8 elements per thread: G^ does not depend on the tuning)
     rows_r2c(P->Lrow, c.stream, nullptr, 0, P->MY, P->MX, 1, P->spec, P->nkx, P->tw, P->twLen, fa, c.g.h,
-             P->MX, P->MY, false);
+             P->MX, P->MY, false, 8);
     CUP2D_LAUNCHED(c);
     const double norm = 1.0 / ((double)P->MX * (double)P->MY);
     cols(P->Lcol, c.stream, P->spec, P->nkx, P->nkx, P->MY, P->Lcol / 2 + 1, P->ghat, 1, P->tw, P->twLen, norm, 0, 0);
@@ -1412,7 +1444,7 @@ void poisson_rows_fwd(Ctx& c) {
                P->twLen, fa, P->type == CUP2D_POISSON_FREESPACE);
   else
     rows_r2c(P->Lrow, c.stream, c.rhs, Nx, Ny, Nx, 0, P->spec, P->nkx, P->tw, P->twLen, fa, c.g.h, P->MX, P->MY,
-             P->type == CUP2D_POISSON_FREESPACE);
+             P->type == CUP2D_POISSON_FREESPACE, P->eR2C);
   CUP2D_LAUNCHED(c);
 }
 
@@ -1451,8 +1483,82 @@ void poisson_rows_inv(Ctx& c) {
                P->tw32, P->twLen, P->type == CUP2D_POISSON_FREESPACE);
   else
     rows_c2r(P->Lrow, c.stream, P->spec, P->nkx, Ny, c.pres, Nx, Nx, P->tw, P->twLen,
-             P->type == CUP2D_POISSON_FREESPACE);                 // free space keeps the first half
+             P->type == CUP2D_POISSON_FREESPACE, P->eC2R);        // free space keeps the first half
   CUP2D_LAUNCHED(c);
+}
+
+namespace {
+// choices already made in this process, per transform set-up: every context
+// of a grid takes the same variants (so their results agree bitwise)
+using TuneKey = std::tuple<int, int, int, int, int>;   // solver, Lrow, Lcol, Nx, Ny
+std::mutex g_tuneMu;
+std::map<TuneKey, std::array<int, 2>> g_tuned;
+
+// median device time (us) of 5 launches after one warm-up, CUDA events on st
+template <class F> double median_us(cudaStream_t st, F launch) {
+  cudaEvent_t a, b;
+  if (cudaEventCreate(&a) != cudaSuccess) return -1;
+  if (cudaEventCreate(&b) != cudaSuccess) { cudaEventDestroy(a); return -1; }
+  launch();
+  std::array<float, 5> t{};
+  for (float& x : t) {
+    cudaEventRecord(a, st);
+    launch();
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&x, a, b);
+  }
+  cudaEventDestroy(a); cudaEventDestroy(b);
+  std::sort(t.begin(), t.end());
+  return 1e3 * t[2];
+}
+} // namespace
+
+// The project autotuner: for the FP64 free-space and periodic solves, times
+// the forward and the inverse row pass with 8 and with 16 elements per
+// thread on this grid (the context's own RHS and pressure buffers, fade
+// off: run at set-up, before the fields hold state) and keeps the faster of
+// each.  A grid tuned before in this process reuses that choice.
+cudaError_t poisson_autotune(Ctx& c) {
+  Poisson* P = c.poisson;
+  if (P->type == CUP2D_POISSON_COSINE || P->fp32) return cudaSuccess;
+  const TuneKey key{P->type, P->Lrow, P->Lcol, c.g.nx, c.g.ny};
+  std::lock_guard<std::mutex> lock(g_tuneMu);
+  auto it = g_tuned.find(key);
+  if (it != g_tuned.end()) {
+    P->eR2C = it->second[0]; P->eC2R = it->second[1];
+    P->tuned = true;
+    return cudaSuccess;
+  }
+  const int Nx = c.g.nx, Ny = c.g.ny;
+  const bool fs = P->type == CUP2D_POISSON_FREESPACE;
+  FadeArgs fa{}; fa.enabled = 0;
+  for (int q = 0; q < 2; q++) {
+    const int e = q ? 16 : 8;
+    P->tuneUs[q] = median_us(c.stream, [&] {
+      rows_r2c(P->Lrow, c.stream, c.rhs, Nx, Ny, Nx, 0, P->spec, P->nkx, P->tw, P->twLen, fa, c.g.h, P->MX,
+               P->MY, fs, e);
+    });
+    P->tuneUs[2 + q] = median_us(c.stream, [&] {
+      rows_c2r(P->Lrow, c.stream, P->spec, P->nkx, Ny, c.pres, Nx, Nx, P->tw, P->twLen, fs, e);
+    });
+  }
+  const cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return err;
+  for (double t : P->tuneUs) if (!(t > 0)) return cudaErrorUnknown;
+  P->eR2C = P->tuneUs[1] < P->tuneUs[0] ? 16 : 8;
+  P->eC2R = P->tuneUs[3] < P->tuneUs[2] ? 16 : 8;
+  P->tuned = true;
+  g_tuned[key] = {P->eR2C, P->eC2R};
+  return cudaSuccess;
+}
+
+void poisson_tuning(const Ctx& c, cup2d_tuning* out) {
+  const Poisson* P = c.poisson;
+  out->fft_rows_fwd_e = P->eR2C;
+  out->fft_rows_inv_e = P->eC2R;
+  out->tuned = P->tuned ? 1 : 0;
+  for (int q = 0; q < 4; q++) out->us[q] = P->tuneUs[q];
 }
 
 void poisson_solve(Ctx& c) {

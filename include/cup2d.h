@@ -95,6 +95,12 @@ typedef struct cup2d_config {
                            /* X = chi lambda dt, and penalization alpha =        */
                            /* 1/(1 + lambda dt chi) (UpdateObjects.cpp:128-210); */
                            /* 0: the shipped explicit forms                      */
+  int autotune;            /* 1: cup2d_create times the FFT row passes' variants */
+                           /* (8 or 16 values per thread) on this grid and keeps */
+                           /* the faster of each (results differ from the        */
+                           /* built-in choice only by rounding); a grid tuned    */
+                           /* before in the process reuses that choice, so       */
+                           /* contexts of one grid agree bitwise.  0: built-in   */
 } cup2d_config;
 
 /* Shape descriptors (the key=value parameters of Shape.cpp:331-345,
@@ -163,6 +169,16 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
 int cup2d_init(cup2d_ctx* ctx);
 
 /* ---- the pipeline (Simulation::advance order) ------------------------- */
+/* The transform variants in use (and, when cup2d_config.autotune was set,
+ * the times measured for them: forward rows with 8 and 16 values per
+ * thread, inverse rows with 8 and 16, in microseconds; zero otherwise). */
+typedef struct cup2d_tuning {
+  int fft_rows_fwd_e, fft_rows_inv_e;
+  int tuned;
+  double us[4];
+} cup2d_tuning;
+int cup2d_tuning_get(cup2d_ctx* ctx, cup2d_tuning* out);
+
 /* Simulation::calcMaxTimestep (Simulation.cpp:254-277) incl. findMaxU
  * (Helpers.cpp:136-176).  dt stays on the device; if dt_out is non-NULL the
  * call synchronises and returns it. */
