@@ -549,6 +549,8 @@ def run_ours(args, world, rank, local, pg):
     # step: dt read back (calcMaxTimestep prints it), dt passed to the four
     # operators, shape state (forces) read back for the force log.
     ne = max(20, args.steps // 5)
+    from cubismup_2d_b200.abi import ShapeState
+    st0 = ShapeState()                     # the forces, read each step into one struct
     if pg is not None:
         pg.barrier()
     torch.cuda.synchronize()
@@ -558,7 +560,7 @@ def run_ours(args, world, rank, local, pg):
         for op in sim.pipeline:
             op(dt)
         ctx.end_step()
-        _ = ctx.shape(0)
+        ctx.shape_state(0, st0)
     ctx.sync()
     e2e_s = max_over_ranks(pg, time.perf_counter() - t0)
     e2e = world * cells * ne / e2e_s / 1e9

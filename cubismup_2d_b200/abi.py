@@ -344,6 +344,13 @@ class Context:
         self._ck(self.L.cup2d_get_shape(self.h_, k, ctypes.byref(s)))
         return {n: getattr(s, n) for n in SHAPE_STATE_FIELDS}
 
+    def shape_state(self, k=0, out=None):
+        """cup2d_get_shape into a cup2d_shape_state (`out`, reused when
+        given), as a C or C++ caller reads it: no per-field conversion."""
+        s = out if out is not None else ShapeState()
+        self._ck(self.L.cup2d_get_shape(self.h_, k, ctypes.byref(s)))
+        return s
+
     def set_shape(self, k, state):
         s = ShapeState()
         self._ck(self.L.cup2d_get_shape(self.h_, k, ctypes.byref(s)))

@@ -180,6 +180,12 @@ k_advdiff_grav(GridDesc g, const Scalars* sc, Grav G, const double* __restrict__
 // pressureCorrectionInit (PressureIterator_approx.cpp:81-122): the fluid
 // velocity corrected by the last pressure, vPres = V + pFac dP/dx invRho,
 // and the velocity RHS div V - chi div UDEF; the penalization force F = 0.
+// The reference clears each block's uDef inside the loop that reads uDef
+// with one ghost layer (:119), blocks in index order (x fastest): run in
+// that order, a block's west and south neighbours are already cleared, so
+// its ghost cells there read zero.  div UDEF follows that order (the one a
+// single thread gives; with more threads the reference's result depends on
+// their schedule).
 __global__ void __launch_bounds__(256)
 k_vr_init(GridDesc g, const Scalars* sc, const double* __restrict__ P, const double* __restrict__ u,
           const double* __restrict__ v, const double* __restrict__ udx, const double* __restrict__ udy,
@@ -194,7 +200,9 @@ k_vr_init(GridDesc g, const Scalars* sc, const double* __restrict__ P, const dou
     const int gy = blockIdx.y * BS + threadIdx.y + 8 * r;
     const size_t c = (size_t)gy * g.nx + gx;
     const double divVf = fdx(g, u, gx, gy) + fdy(g, v, gx, gy);
-    const double divDef = fdx(g, udx, gx, gy) + fdy(g, udy, gx, gy);
+    const double udW = gx % BS == 0 && gx > 0 ? 0.0 : at(g, udx, gx, gy, -1, 0);
+    const double udS = gy % BS == 0 && gy > 0 ? 0.0 : at(g, udy, gx, gy, 0, -1);
+    const double divDef = (at(g, udx, gx, gy, 1, 0) - udW) / 2 + (at(g, udy, gx, gy, 0, 1) - udS) / 2;
     uf[c] = u[c] + pFac * fdx(g, P, gx, gy) * ir[c];
     vf[c] = v[c] + pFac * fdy(g, P, gx, gy) * ir[c];
     prhs[c] = divVf - chi[c] * divDef;

@@ -33,6 +33,7 @@
 #include "Obstacles/CarlingFish.h"
 #include "Utils/FactoryFileLineParser.h"
 
+#include <omp.h>
 #include <algorithm>
 #include <cstring>
 #include <sstream>
@@ -336,6 +337,9 @@ void ref_set_gravity(void* h, double gx, double gy) {
   ((RefSim*)h)->sim.gravity[0] = gx; ((RefSim*)h)->sim.gravity[1] = gy;
 }
 int ref_variable_density(void* h) { return ((RefSim*)h)->sim.bVariableDensity ? 1 : 0; }
+// OpenMP threads of the reference's parallel loops (returns the previous
+// count): one thread gives the order-dependent loops their sequential result
+int ref_set_threads(int n) { const int old = omp_get_max_threads(); omp_set_num_threads(n); return old; }
 // PoissonSolver::solve(BSRC, BDST) of a solver made by the reference's own
 // factory (PoissonSolver.cpp:23-59) on scalar fields (2 chi, 3 pres, 4 tmp,
 // 7 invRho); returns -1 for a non-scalar field

@@ -80,6 +80,8 @@ def lib():
     L.ref_uinf.argtypes = [vp, dp]
     L.ref_set_uinf.argtypes = [vp, d, d]
     L.ref_set_gravity.argtypes = [vp, d, d]
+    L.ref_set_threads.argtypes = [i]
+    L.ref_set_threads.restype = i
     L.ref_poisson_solve.argtypes = [vp, i, i]
     L.ref_poisson_solve.restype = i
     L.ref_set_time.argtypes = [vp, d, i, d]
@@ -106,6 +108,11 @@ def lib():
 
 def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def set_threads(n):
+    """OpenMP threads of the reference's loops; returns the previous count."""
+    return lib().ref_set_threads(n)
 
 
 class RefSim:

@@ -52,3 +52,20 @@ def test_reference_implicit_penalization_composes(ref):
         b.step()
     assert np.all(np.isfinite(a.get("u")))
     assert not np.array_equal(a.get("u"), b.get("u"))
+
+
+def test_reference_udef_clearing_depends_on_block_order(ref):
+    """PressureVarRho_approx with a swimmer: the single-thread run is
+    reproducible (the order the CUDA path follows)."""
+    args = ("-bpdx 4 -bpdy 2 -extent 1 -CFL 0.1 -nu 1e-4 -muteAll 1 -iterativePenalization 1 "
+            "-shapes 'stefanfish L=0.3 T=1 xpos=0.3 ypos=0.25, disk radius=0.05 xpos=0.75 ypos=0.3 rhoS=1.5'")
+    old = ref.set_threads(1)
+    try:
+        runs = []
+        for _ in range(2):
+            r = ref.RefSim(args)
+            r.step()
+            runs.append(r.get("u"))
+        assert np.array_equal(runs[0], runs[1])
+    finally:
+        ref.set_threads(old)
