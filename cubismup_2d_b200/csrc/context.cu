@@ -141,19 +141,6 @@ struct StreamScope {
   ~StreamScope() { c.stream = saved; }
 };
 
-// A graph step's final velocity is set once penalization is done: its
-// findMaxU for the next step runs on side2 beside the force pass and joins
-// before the step ends (evMaxFree).
-void launch_max_next_beside(Ctx& c) {
-  cudaEventRecord(c.evPres, c.stream);
-  cudaStreamWaitEvent(c.side2, c.evPres, 0);
-  {
-    StreamScope scope(c, c.side2);
-    launch_max_next(c);
-  }
-  cudaEventRecord(c.evMaxFree, c.side2);
-}
-
 // PressureSingle.cpp:216-241 and 362-372: the pressure correction and the
 // momentum integrals run side by side (the integrals evaluate the corrected
 // velocity of their own cells), then collisions and penalization.  The
@@ -162,21 +149,19 @@ void launch_pressure_tail(Ctx& c) {
   const double* ui = c.u();
   const double* vi = c.v();
   if (c.nshapes == 0) {
-    launch_pcorr(c);
-    if (c.graphStep) launch_max_next_beside(c);
+    launch_pcorr(c, c.graphStep);            // with the next step's findMaxU (graph steps)
     return;
   }
   cudaEventRecord(c.evPres, c.stream);
   cudaStreamWaitEvent(c.side2, c.evPres, 0);
   {
     StreamScope scope(c, c.side2);
-    launch_pcorr(c);                        // flips the current velocity buffer
+    launch_pcorr(c, c.graphStep);            // flips the current velocity buffer
   }
   cudaEventRecord(c.evMom, c.side2);
   launch_momenta(c, ui, vi);
   cudaStreamWaitEvent(c.stream, c.evMom, 0);
   launch_collide_penalize(c);
-  if (c.graphStep) launch_max_next_beside(c);
 }
 
 // One pass of Simulation::simulate's loop body (Simulation.cpp:245-251) as a
@@ -191,8 +176,9 @@ void launch_pressure_tail(Ctx& c) {
 //          once step_begin has set it
 //   side2: once the tiles are placed, advDiff's outflow flux, then advDiff
 //          with the RHS divergence in place (advDiff reads no obstacle data);
-//          later the pressure correction, then the next step's findMaxU
-//          beside the force pass
+//          later the pressure correction (with the next step's findMaxU
+//          over the blocks without obstacle tiles; the tiles' part follows
+//          the penalization on main)
 void enqueue_step(Ctx& c) {
   struct GraphStepFlag { Ctx& c; explicit GraphStepFlag(Ctx& cc) : c(cc) { c.graphStep = true; }
                          ~GraphStepFlag() { c.graphStep = false; } } flag(c);
@@ -246,7 +232,6 @@ void enqueue_step(Ctx& c) {
   launch_pressure_tail(c);
   launch_forces(c, c.forcesOut);
   if (anyAhead) cudaStreamWaitEvent(c.stream, c.evJoin, 0);
-  cudaStreamWaitEvent(c.stream, c.evMaxFree, 0);
   launch_end_step_dt(c);                    // t += dt, and the next step's dt
 }
 
@@ -490,8 +475,7 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
               cudaEventCreateWithFlags(&c.evObjDone, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evPres, cudaEventDisableTiming) != cudaSuccess ||
               cudaEventCreateWithFlags(&c.evMom, cudaEventDisableTiming) != cudaSuccess ||
-              cudaEventCreateWithFlags(&c.evPlaced, cudaEventDisableTiming) != cudaSuccess ||
-              cudaEventCreateWithFlags(&c.evMaxFree, cudaEventDisableTiming) != cudaSuccess))
+              cudaEventCreateWithFlags(&c.evPlaced, cudaEventDisableTiming) != cudaSuccess))
     rc = fail(ctx, CUP2D_ECUDA, "stream/event creation failed");
   if (!rc && fish_setup_kernels() != cudaSuccess)
     rc = fail(ctx, CUP2D_ECUDA, "shared-memory limits of the fish kernels could not be set");
@@ -538,7 +522,6 @@ int cup2d_destroy(cup2d_ctx* ctx) {
   if (c.evPres) cudaEventDestroy(c.evPres);
   if (c.evMom) cudaEventDestroy(c.evMom);
   if (c.evPlaced) cudaEventDestroy(c.evPlaced);
-  if (c.evMaxFree) cudaEventDestroy(c.evMaxFree);
   for (auto& t : c.tiles) {
     cudaFree(t.tiles); cudaFree(t.slot); cudaFree(t.chi); cudaFree(t.dist); cudaFree(t.udx);
     cudaFree(t.udy); cudaFree(t.sD); cudaFree(t.sdx); cudaFree(t.sdy);

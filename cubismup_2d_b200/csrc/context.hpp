@@ -72,7 +72,6 @@ struct Ctx {
   cudaEvent_t evPres = nullptr, evMom = nullptr;
   cudaEvent_t evPlaced = nullptr;   // recorded after the obstacle tiles are placed
   bool recordPlaced = false;
-  cudaEvent_t evMaxFree = nullptr;  // the next step's speed maximum over free cells
   bool graphStep = false;           // enqueue_step is recording a graph step
   // the operator-by-operator path forms the next step's fish midlines on
   // `side` (evSideMid after them), checked by the next call; midByGraph:

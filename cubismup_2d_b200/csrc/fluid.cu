@@ -34,7 +34,7 @@ k_max_u_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh,
 __global__ void k_set_dt(Scalars* sc, double dt) { pdl_begin(); CUP2D_TRACE_SCOPE(TR_SETDT); sc->dt = dt; }
 
 // End of a step (Simulation.cpp:289-290): t += dt, step += 1, then the next step's
-// calcMaxTimestep from the maximum k_max_next formed on the final velocity
+// calcMaxTimestep from the maximum k_pcorr<true> and k_forces formed on the final velocity
 // (max is exact in any order: dtNext equals what k_max_u_dt would form).
 __global__ void k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh)
 {
@@ -50,7 +50,7 @@ __global__ void k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int n
 
 // End of an operator-by-operator step: findMaxU on the final velocity (its
 // last CTA), then t += dt, step += 1 and the next step's calcMaxTimestep --
-// a graph step's k_max_next and k_end_step_dt in one launch.
+// a graph step's findMaxU parts and k_end_step_dt in one launch.
 __global__ void __launch_bounds__(512)
 k_end_step_max(GridDesc g, Scalars* sc, const DevShape* sh, int nsh, const double* __restrict__ u,
                const double* __restrict__ v, double* partials, unsigned* counter, double* dtOut)
@@ -448,52 +448,49 @@ __global__ void k_fade_slots(GridDesc g, int* fadeSlot)
 
 // PressureSingle.cpp:216-241: V += -(dt/2h) grad_2h P; zero-gradient P ghosts.
 // Reads the velocity written by advDiff (ui, vi) and writes the current one.
+// MAXNEXT (graph steps): the next step's findMaxU (Helpers.cpp:136-176) is
+// formed on the step's final velocity in two parts meeting in sc->maxNext by
+// exact atomic max: here over the blocks no shape has a tile in (the
+// penalization leaves them as they are), and by the force pass over the
+// tiles once they are penalized.
+template <bool MAXNEXT>
 __global__ void __launch_bounds__(256)
-k_pcorr(GridDesc g, const Scalars* sc, const double* __restrict__ p,
+k_pcorr(GridDesc g, Scalars* sc, AllTiles T, int nsh, const double* __restrict__ p,
         const double* __restrict__ ui, const double* __restrict__ vi,
         double* __restrict__ uo, double* __restrict__ vo)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_PCORR);
   const double pFac = -0.5 * sc->dt / g.h;
+  const double UINF = sc->uinfx, VINF = sc->uinfy;
   const int nx = g.nx, ny = g.ny;
   const int gx = blockIdx.x * BS + threadIdx.x;
+  double m = 0.0;
+  int bad = 0;
 #pragma unroll
   for (int r = 0; r < 4; r++) {
     const int gy = blockIdx.y * BS + threadIdx.y + 8 * r;
     const size_t c = (size_t)gy * nx + gx;
     const double pW = p[gx > 0 ? c - 1 : c], pE = p[gx < nx - 1 ? c + 1 : c];
     const double pS = p[gy > 0 ? c - nx : c], pN = p[gy < ny - 1 ? c + nx : c];
-    uo[c] = ui[c] + pFac * (pE - pW);
-    vo[c] = vi[c] + pFac * (pN - pS);
+    const double un = ui[c] + pFac * (pE - pW), vn = vi[c] + pFac * (pN - pS);
+    uo[c] = un;
+    vo[c] = vn;
+    if (MAXNEXT) {
+      m = fmax(m, cell_speed(un, vn, UINF, VINF));
+      bad |= !isfinite(un) || !isfinite(vn);
+    }
   }
-}
-
-// The next step's findMaxU (Helpers.cpp:136-176) on the step's final
-// velocity, beside the force pass (which only reads it).  Per-CTA maxima
-// meet in sc->maxNext by exact atomic max.
-__global__ void __launch_bounds__(256)
-k_max_next(GridDesc g, Scalars* sc, const double* __restrict__ u, const double* __restrict__ v)
-{
-  pdl_begin();
-  CUP2D_TRACE_SCOPE(TR_MAXNEXT);
+  if (!MAXNEXT) return;
+  const int b = blockIdx.x + g.bpdx * blockIdx.y;
+  bool tile = false;
+  for (int k = 0; k < nsh; k++) tile |= T.t[k].slot[b] >= 0;
+  if (tile) return;                                    // uniform over the CTA
   __shared__ double red[32];
-  const double UINF = sc->uinfx, VINF = sc->uinfy;
-  double m = 0.0;
-  int bad = 0;
-  const size_t n2 = (size_t)g.nx * g.ny / 2;
-  const double2* u2 = reinterpret_cast<const double2*>(u);
-  const double2* v2 = reinterpret_cast<const double2*>(v);
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2; i += (size_t)gridDim.x * blockDim.x) {
-    const double2 a = u2[i], b = v2[i];
-    m = fmax(m, cell_speed(a.x, b.x, UINF, VINF));
-    m = fmax(m, cell_speed(a.y, b.y, UINF, VINF));
-    bad |= !isfinite(a.x) || !isfinite(b.x) || !isfinite(a.y) || !isfinite(b.y);
-  }
   m = block_max(m, red);
   const int anyBad = __syncthreads_or(bad);
   if (lin_tid() == 0) {
-    atomic_max_double(&sc->maxNext, m);
+    atomic_max_nonneg(&sc->maxNext, m);
     if (anyBad) atomicOr(&sc->status, ST_NAN);
   }
 }
@@ -542,11 +539,6 @@ void launch_max_u_dt(Ctx& c) {
 
 void launch_set_dt(Ctx& c, double dt) {
   launch_k(k_set_dt, 1, 1, 0, c.stream, c.dsc, dt);
-  CUP2D_LAUNCHED(c);
-}
-
-void launch_max_next(Ctx& c) {
-  launch_k(k_max_next, max_grid(c), 256, 0, c.stream, c.g, c.dsc, c.u(), c.v());
   CUP2D_LAUNCHED(c);
 }
 
@@ -619,13 +611,19 @@ void launch_rhs_iter(Ctx& c) {
 
 void launch_pcorr_from(Ctx& c, const double* ui, const double* vi, double* uo, double* vo) {
   dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
-  launch_k(k_pcorr, grid, block, 0, c.stream, c.g, c.dsc, c.pres, ui, vi, uo, vo);
+  launch_k(k_pcorr<false>, grid, block, 0, c.stream, c.g, c.dsc, AllTiles{}, 0, (const double*)c.pres, ui, vi,
+           uo, vo);
   CUP2D_LAUNCHED(c);
 }
 
-void launch_pcorr(Ctx& c) {
+void launch_pcorr(Ctx& c, bool maxNext) {
   dim3 grid(c.g.bpdx, c.g.bpdy), block(32, 8);
-  launch_k(k_pcorr, grid, block, 0, c.stream, c.g, c.dsc, c.pres, c.u(), c.v(), c.uo(), c.vo());
+  if (maxNext)
+    launch_k(k_pcorr<true>, grid, block, 0, c.stream, c.g, c.dsc, all_tiles(c), c.nshapes, (const double*)c.pres,
+             (const double*)c.u(), (const double*)c.v(), c.uo(), c.vo());
+  else
+    launch_k(k_pcorr<false>, grid, block, 0, c.stream, c.g, c.dsc, AllTiles{}, 0, (const double*)c.pres,
+             (const double*)c.u(), (const double*)c.v(), c.uo(), c.vo());
   CUP2D_LAUNCHED(c);
   c.cur = 1 - c.cur;
 }

@@ -391,6 +391,13 @@ __device__ __forceinline__ bool last_block_done(unsigned* counter, unsigned nblo
 }
 
 // atomic max on doubles through the ordered-integer mapping of IEEE-754
+// Max of non-negative doubles (speeds: +0 and up, +inf, never NaN): their
+// bit patterns order as the values do, so one native 64-bit unsigned atomic
+// max (no compare-and-swap retries) suffices where many CTAs finishing at
+// once contend on one address.
+__device__ __forceinline__ void atomic_max_nonneg(double* addr, double val) {
+  atomicMax(reinterpret_cast<unsigned long long*>(addr), static_cast<unsigned long long>(__double_as_longlong(val)));
+}
 __device__ __forceinline__ void atomic_max_double(double* addr, double val) {
   unsigned long long* a = reinterpret_cast<unsigned long long*>(addr);
   unsigned long long old = *a, assumed;

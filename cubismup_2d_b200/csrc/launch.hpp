@@ -33,9 +33,10 @@ void launch_fade_sums(Ctx& c);                       // PoissonSolver.cpp:61-100
 void launch_rhs_iter(Ctx& c);                        // PressureIterator_unif.cpp:22-49
 void launch_pcorr_from(Ctx& c, const double* ui, const double* vi, double* uo, double* vo);
 int build_fade_slots(Ctx& c);                        // PoissonSolver.cpp:71-79, once per grid
-void launch_pcorr(Ctx& c);                           // PressureSingle.cpp:216-241
+// PressureSingle.cpp:216-241; maxNext: with the next step's findMaxU over
+// the blocks outside every shape's tiles (graph steps)
+void launch_pcorr(Ctx& c, bool maxNext = false);
 void launch_end_step_dt(Ctx& c);                     // Simulation.cpp:289-290 + the next step's calcMaxTimestep
-void launch_max_next(Ctx& c);                        // its findMaxU on the final velocity
 void launch_take_dt_next(Ctx& c);                    // calcMaxTimestep from the carried dt
 // findMaxU + Simulation.cpp:289-290 + the next dt (also to dtOut: mapped host memory, or null)
 void launch_end_step_max(Ctx& c, double* dtOut = nullptr);

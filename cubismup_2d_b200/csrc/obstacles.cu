@@ -600,7 +600,7 @@ k_penalize(GridDesc g, const Scalars* sc, const DevShape* sh, int k, ObstTiles t
 // (Shape.cpp:252-282): per surface point traction, 17 sums per tile, then
 // the fixed-order sum over tiles and the derived powers/efficiencies.
 __global__ void __launch_bounds__(1024)
-k_forces(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ u,
+k_forces(GridDesc g, Scalars* sc, int maxNext, DevShape* sh, AllTiles T, const double* __restrict__ u,
          const double* __restrict__ v, const double* __restrict__ p,
          double* partials, int partStride, unsigned* counters, cup2d_shape_state* out)
 {
@@ -611,6 +611,11 @@ k_forces(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ u,
   DevShape& S = sh[k];
   const ObstTiles& t = T.t[k];
   double* part = partials + (size_t)k * partStride;
+  // maxNext (graph steps): the next step's findMaxU over this shape's tiles,
+  // penalized by now (the blocks outside every tile are k_pcorr<true>'s)
+  const double UINF = sc->uinfx, VINF = sc->uinfy;
+  double mx = 0.0;
+  int bad = 0;
   for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
   double F[NFORCE];
 #pragma unroll
@@ -619,6 +624,12 @@ k_forces(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ u,
     const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
     const int ix = threadIdx.x, iy = threadIdx.y;
     const size_t o = (size_t)s * BS2 + iy * BS + ix;
+    if (maxNext) {
+      const size_t c = (size_t)(by * BS + iy) * g.nx + bx * BS + ix;
+      const double a = u[c], w = v[c];
+      mx = fmax(mx, cell_speed(a, w, UINF, VINF));
+      bad |= !isfinite(a) || !isfinite(w);
+    }
     if (t.sD[o] > 0) {
       const int gx = bx * BS + ix, gy = by * BS + iy;
       auto I = [&](int x, int y) -> size_t {
@@ -665,6 +676,15 @@ k_forces(GridDesc g, DevShape* sh, AllTiles T, const double* __restrict__ u,
   }
   block_sum<NFORCE>(F, red);
   if (lin_tid() == 0) for (int q = 0; q < NFORCE; q++) part[NFORCE * s + q] = F[q];
+  }
+  if (maxNext) {                                       // uniform over the launch
+    __shared__ double redm[32];
+    mx = block_max(mx, redm);
+    const int anyBad = __syncthreads_or(bad);
+    if (lin_tid() == 0) {
+      atomic_max_nonneg(&sc->maxNext, mx);
+      if (anyBad) atomicOr(&sc->status, ST_NAN);
+    }
   }
   if (!last_block_done(counters + k, gridDim.x)) return;
   if (lin_tid() >= 32) return;                          // one warp finishes
@@ -852,8 +872,8 @@ void launch_forces(Ctx& c, cup2d_shape_state* out) {
   if (c.nshapes == 0) return;
   const AllTiles T = all_tiles(c);
   launch_k(k_forces, dim3(tile_ctas(c, c.maxCapacity), c.nshapes), dim3(32, 32), 0, c.stream,
-      c.g, c.dshapes, T, c.u(), c.v(), c.pres, shape_partials(c), (int)shape_region(c),
-      c.counters + CNT_FORCES, out);
+      c.g, c.dsc, c.graphStep ? 1 : 0, c.dshapes, T, (const double*)c.u(), (const double*)c.v(),
+      (const double*)c.pres, shape_partials(c), (int)shape_region(c), c.counters + CNT_FORCES, out);
   CUP2D_LAUNCHED(c);
 }
 
