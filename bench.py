@@ -538,6 +538,8 @@ def run_ours(args, world, rank, local, pg):
         fp32 = {"value": world * cells * args.steps / (ms32 / 1e3) / 1e9, "unit": "Gcell-steps/s",
                 "ms_per_step": ms32 / args.steps, "speedup_vs_fp64": total_ms / ms32,
                 "pres_rel_err_1step": perr,
+                "transform_ms": {k: round(b.ctx.time_kernel(k, 20, flush_l2=True), 5)
+                                 for k in ("fft_rows_fwd", "fft_cols", "fft_rows_inv")},
                 "note": "FP32 free-space Poisson transforms; fields, stencils, obstacle sums and "
                         "forces FP64; Cd within 1e-4 of FP64 is checked by tests/test_gpu_fp32.py"}
         del b

@@ -245,8 +245,10 @@ int cup2d_kernel_launches(const cup2d_ctx* ctx, long long* count);
  * a 256 MB device buffer (allocated by the first such call, kept until
  * cup2d_destroy) is written before every launch, outside the events, so
  * that each launch reads its inputs from HBM, not from the 126 MB L2.  The
- * kernels re-read and re-write their own buffers, so state stays valid but
- * is not a physical step.  which: CUP2D_KERNEL_*. */
+ * kernels re-read and re-write the context's own buffers (the column pass,
+ * for one, multiplies the spectrum by the Green's function at every launch),
+ * so afterwards the fields hold no physical state: re-initialise the context
+ * or load a checkpoint before stepping on.  which: CUP2D_KERNEL_*. */
 #define CUP2D_KERNEL_ADVDIFF 0      /* advDiff update + RHS divergence (one kernel) */
 #define CUP2D_KERNEL_RHS_DIV 1
 #define CUP2D_KERNEL_PCORR 2
