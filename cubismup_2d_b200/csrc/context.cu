@@ -289,7 +289,9 @@ int pressure_iterative(cup2d_ctx* ctx) {
 // relative pressure change relDP; converged (max(relDF, relDP) below the
 // adaptive target, or more than 100 iterations, or more than twice the
 // previous call's count), finalizePressure updates the velocity; each
-// iteration ends with pres = tmp.  The target adapts as in the reference.
+// iteration ends with pres = tmp (the two buffers trade places; the next
+// RHS overwrites tmp), and the call with tmp = pres, as the reference leaves
+// them.  The target adapts as in the reference.
 }  // namespace
 cudaError_t fill_udef_grid(Ctx& c);
 namespace {
@@ -321,9 +323,10 @@ int pressure_varrho(cup2d_ctx* ctx) {
     relDP = c.pin->it.relDP;
     const bool converged = std::max(relDF, relDP) < st.target || iter > 2 * st.oldNsteps || iter > 100;
     if (converged) launch_vr_pcorr(c, true);     // finalizePressure
-    CK(cudaMemcpyAsync(c.pres, c.rhs, nb, cudaMemcpyDeviceToDevice, c.stream));
+    std::swap(c.pres, c.rhs);                     // pres = tmp
     if (converged) break;
   }
+  CK(cudaMemcpyAsync(c.rhs, c.pres, nb, cudaMemcpyDeviceToDevice, c.stream));
   st.oldNsteps = iter + 1;
   if (st.oldNsteps > 30) st.target = std::max({relDF, relDP, st.target});
   if (st.oldNsteps > 10) st.target *= 1.01;
