@@ -37,7 +37,7 @@ EXPORTS = [
     "cup2d_get_field", "cup2d_set_field",
     "cup2d_get_shape", "cup2d_set_shape", "cup2d_get_scalars", "cup2d_set_scalars",
     "cup2d_grid_size", "cup2d_kernel_launches", "cup2d_time_kernel", "cup2d_advance_timed",
-    "cup2d_checkpoint_size", "cup2d_checkpoint_save", "cup2d_checkpoint_load",
+    "cup2d_checkpoint_size", "cup2d_checkpoint_save", "cup2d_checkpoint_load", "cup2d_adjoint_run",
     "cup2d_ensemble_create", "cup2d_ensemble_advance", "cup2d_ensemble_advance_timed",
     "cup2d_ensemble_sync", "cup2d_ensemble_get_shapes", "cup2d_ensemble_last_error",
     "cup2d_ensemble_destroy",
@@ -130,6 +130,7 @@ def lib():
     L.cup2d_checkpoint_size.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
     L.cup2d_checkpoint_save.argtypes = [vp, vp, ctypes.c_size_t]
     L.cup2d_checkpoint_load.argtypes = [vp, vp, ctypes.c_size_t]
+    L.cup2d_adjoint_run.argtypes = [vp, i, i, dp, dp, dp, dp, dp, dp, dp]
     L.cup2d_ensemble_create.argtypes = [ctypes.POINTER(vp), i, ctypes.POINTER(vp)]
     L.cup2d_ensemble_advance.argtypes = [vp, i]
     L.cup2d_ensemble_advance_timed.argtypes = [vp, i, dp]
@@ -403,6 +404,31 @@ class Context:
         ptr, size = _buffer(out)
         self._ck(self.L.cup2d_checkpoint_save(self.h_, ptr, size))
         return out
+
+    def adjoint(self, nsteps, box, every=20, dt=None, gradient=True):
+        """The objective J = (1/nsteps) sum over the steps' velocities of
+        (h^2/2) sum_box (u^2 + v^2) (box = (x0, x1, y0, y1) in domain units)
+        over nsteps steps from the current state, and its gradient with
+        respect to the current velocity by the discrete adjoint (forward
+        recomputed from checkpoints every ``every`` steps).  dt: the frozen
+        step sizes (nsteps values) or None for calcMaxTimestep's.  Returns
+        (J, grad_u, grad_v, dts, (forward_ms, backward_ms)); the gradients are
+        None when gradient is False.  The context ends in the forward's
+        final state."""
+        dp = ctypes.POINTER(ctypes.c_double)
+        b = np.ascontiguousarray(box, dtype=np.float64)
+        dts = np.empty(nsteps, dtype=np.float64)
+        dti = None if dt is None else np.ascontiguousarray(dt, dtype=np.float64)
+        if dti is not None and dti.size != nsteps:
+            raise ValueError("dt needs nsteps values")
+        J = ctypes.c_double()
+        ms = np.zeros(2, dtype=np.float64)
+        gu = np.empty((self.ny, self.nx), dtype=np.float64) if gradient else None
+        gv = np.empty((self.ny, self.nx), dtype=np.float64) if gradient else None
+        ptr = lambda a: None if a is None else a.ctypes.data_as(dp)  # noqa: E731
+        self._ck(self.L.cup2d_adjoint_run(self.h_, nsteps, every, ptr(b), ptr(dti), ptr(dts), ctypes.byref(J),
+                                          ptr(gu), ptr(gv), ptr(ms)))
+        return J.value, gu, gv, dts, (float(ms[0]), float(ms[1]))
 
     def restore(self, blob):
         """Loads a checkpoint of this configuration (host array or device tensor)."""

@@ -19,7 +19,8 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libcup2d.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["context.cu", "fluid.cu", "obstacles.cu", "fish.cu", "poisson.cu", "noalloc.cu", "varrho.cu"]
+SOURCES = ["context.cu", "fluid.cu", "obstacles.cu", "fish.cu", "poisson.cu", "noalloc.cu", "varrho.cu",
+           "adjoint.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-fmad=false", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "--expt-relaxed-constexpr"]

@@ -1,0 +1,596 @@
+// Discrete adjoint of the step (no counterpart in the reference): the
+// gradient of a time-averaged kinetic energy in a probe box with respect to
+// the initial velocity field, for a body whose motion does not depend on
+// the flow (forced in x, y and angle, fixed on the grid: chi is constant).
+//
+// The step u^n -> u^(n+1) (operator order of Simulation::advance):
+//   u1 = A(u^n)             advDiff with its inflow fades and outflow
+//                           correction (advDiff.cpp:36-116)
+//   T  = (h/2dt) D u1       the RHS divergence (PressureSingle.cpp:112-128)
+//   f  = O(T)               the obstacle terms (PressureSingle.cpp:130-213)
+//   b  = F(f)               the boundary-strip fade (PoissonSolver.cpp:61-118)
+//   p  = K b                the Poisson convolution
+//   u2 = u1 - (dt/2h) G p   pressureCorrection (PressureSingle.cpp:216-241)
+//   u^(n+1) = Pen(u2)       penalize (PressureSingle.cpp:69-108)
+// with the body velocity forced.  A, O and F are nonlinear; each is
+// linearized about the forward values of its step (O and F are piecewise
+// linear in their input: the linearization is the active piece, with the
+// rank-one terms of their sign-selected corrections).  The backward step
+// applies the transposes in reverse order: Pen^T, then lambda_p = -(dt/2h)
+// G^T lambda, K^T = K (the free-space, periodic and cosine convolutions are
+// symmetric), F'^T, O'^T, (h/2dt) D^T added to lambda, A'^T.
+//
+// The forward is stored as checkpoints (the context's own checkpoint blob,
+// kept in device memory) every `every` steps; the backward recomputes each
+// segment forward from its checkpoint, keeping the values the
+// linearizations need, then runs the segment's adjoint steps.  dt is frozen
+// (the forward's schedule, or one given): it is not differentiated.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <string>
+#include <vector>
+#include "context.hpp"
+
+namespace cup2d {
+
+namespace {
+
+// zero-gradient neighbour indices (the labs' clamped ghosts)
+struct Nb { size_t c, W, E, S, N; int x, y; };
+__device__ __forceinline__ Nb nb_of(const GridDesc& g, int gx, int gy) {
+  Nb n;
+  n.x = gx; n.y = gy;
+  n.c = (size_t)gy * g.nx + gx;
+  n.W = gx > 0 ? n.c - 1 : n.c;
+  n.E = gx < g.nx - 1 ? n.c + 1 : n.c;
+  n.S = gy > 0 ? n.c - g.nx : n.c;
+  n.N = gy < g.ny - 1 ? n.c + g.nx : n.c;
+  return n;
+}
+
+// transpose of q -> fac (q[E] - q[W]) (x) and fac (q[N] - q[S]) (y) with
+// clamped ghosts, evaluated at cell j: the cells whose E / W / N / S
+// neighbour is j
+__device__ __forceinline__ double diff_T(const GridDesc& g, const double* __restrict__ lx,
+                                         const double* __restrict__ ly, const Nb& j) {
+  const int nx = g.nx, ny = g.ny;
+  double a = 0;
+  if (j.x >= 1) a += lx[j.c - 1];          // j is the E neighbour of j - 1
+  if (j.x == nx - 1) a += lx[j.c];         // j is its own (clamped) E neighbour
+  if (j.x <= nx - 2) a -= lx[j.c + 1];     // j is the W neighbour of j + 1
+  if (j.x == 0) a -= lx[j.c];
+  if (j.y >= 1) a += ly[j.c - nx];
+  if (j.y == ny - 1) a += ly[j.c];
+  if (j.y <= ny - 2) a -= ly[j.c + nx];
+  if (j.y == 0) a -= ly[j.c];
+  return a;
+}
+
+// lambda_p = pFac G^T (lu, lv): the pressure correction's transpose
+__global__ void __launch_bounds__(256)
+k_adj_grad_T(GridDesc g, double pFac, const double* __restrict__ lu, const double* __restrict__ lv,
+             double* __restrict__ lp)
+{
+  const int gx = blockIdx.x * BS + threadIdx.x;
+  for (int r = 0; r < 4; r++) {
+    const Nb j = nb_of(g, gx, blockIdx.y * BS + threadIdx.y + 8 * r);
+    lp[j.c] = pFac * diff_T(g, lu, lv, j);
+  }
+}
+
+// (lu, lv) += facDiv D^T lr: the RHS divergence's transpose
+__global__ void __launch_bounds__(256)
+k_adj_div_T(GridDesc g, double facDiv, const double* __restrict__ lr, double* __restrict__ lu,
+            double* __restrict__ lv)
+{
+  const int gx = blockIdx.x * BS + threadIdx.x;
+  const int nx = g.nx, ny = g.ny;
+  for (int r = 0; r < 4; r++) {
+    const Nb j = nb_of(g, gx, blockIdx.y * BS + threadIdx.y + 8 * r);
+    double ax = 0, ay = 0;
+    if (j.x >= 1) ax += lr[j.c - 1];
+    if (j.x == nx - 1) ax += lr[j.c];
+    if (j.x <= nx - 2) ax -= lr[j.c + 1];
+    if (j.x == 0) ax -= lr[j.c];
+    if (j.y >= 1) ay += lr[j.c - nx];
+    if (j.y == ny - 1) ay += lr[j.c];
+    if (j.y <= ny - 2) ay -= lr[j.c + nx];
+    if (j.y == 0) ay -= lr[j.c];
+    lu[j.c] += facDiv * ax;
+    lv[j.c] += facDiv * ay;
+  }
+}
+
+// Pen^T: lambda *= 1 - chi where the shape owns the cell (penalize's alpha)
+__global__ void __launch_bounds__(1024)
+k_adj_pen(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
+          double* lu, double* lv)
+{
+  const DevShape& S = sh[k];
+  for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
+    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+    const size_t o = (size_t)s * BS2 + threadIdx.y * BS + threadIdx.x;
+    const size_t c = (size_t)(by * BS + threadIdx.y) * g.nx + bx * BS + threadIdx.x;
+    const double X = t.chi[o];
+    if (chig[c] > X || X <= 0) continue;
+    lu[c] *= 1 - X;
+    lv[c] *= 1 - X;
+  }
+}
+
+// ---- the obstacle RHS terms O (k_rhs_obst, k_rhs_corr) --------------------
+// over the shape's tile cells not owned by a larger chi: T' = T - X T; the
+// sums s = sum -X T, pos / neg over perimeter cells of T' > 0 / T' < 0, and
+// with the adjoint input lo (the adjoint of O's output): Lp = sum over
+// perimeter T' > 0 of T' lo, Ln = the same over T' < 0.
+// acc: s, pos, neg, Lp, Ln
+__device__ __forceinline__ bool obst_cell(const GridDesc& g, const ObstTiles& t, int s, const double* chig,
+                                          size_t& c, double& X, bool& perim) {
+  const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+  const int gx = bx * BS + threadIdx.x, gy = by * BS + threadIdx.y;
+  auto CHI = [&](int x, int y) -> double {
+    x = x < 0 ? 0 : (x >= g.nx ? g.nx - 1 : x);
+    y = y < 0 ? 0 : (y >= g.ny ? g.ny - 1 : y);
+    return chig[(size_t)y * g.nx + x];
+  };
+  X = t.chi[(size_t)s * BS2 + threadIdx.y * BS + threadIdx.x];
+  c = (size_t)gy * g.nx + gx;
+  if (CHI(gx, gy) > X) return false;
+  const double gxx = CHI(gx + 1, gy) - CHI(gx - 1, gy), gxy = CHI(gx, gy + 1) - CHI(gx, gy - 1);
+  perim = gxx * gxx + gxy * gxy > 0;
+  return true;
+}
+
+__global__ void __launch_bounds__(1024)
+k_adj_obst_sums(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
+                const double* __restrict__ T, const double* __restrict__ lo, double* acc)
+{
+  const DevShape& S = sh[k];
+  double a[5] = {0, 0, 0, 0, 0};
+  for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
+    size_t c; double X; bool perim = false;
+    if (!obst_cell(g, t, s, chig, c, X, perim)) continue;
+    const double T0 = T[c], src = -X * T0, Tp = T0 + src;
+    a[0] += src;
+    if (perim && Tp > 0) { a[1] += Tp; a[3] += Tp * lo[c]; }
+    if (perim && Tp < 0) { a[2] -= Tp; a[4] += Tp * lo[c]; }
+  }
+  for (int q = 0; q < 5; q++) {
+    double v = a[q];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v != 0) atomicAdd(&acc[q], v);
+  }
+}
+
+// lT = O'^T lo over the processed cells (other cells: lT = lo, copied by the
+// caller beforehand)
+__global__ void __launch_bounds__(1024)
+k_adj_obst_apply(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
+                 const double* __restrict__ T, const double* __restrict__ lo, const double* __restrict__ acc,
+                 double* __restrict__ lT)
+{
+  const DevShape& S = sh[k];
+  const double s = acc[0], pos = acc[1], neg = acc[2], Lp = acc[3], Ln = acc[4];
+  const double posF = fmax(pos, EPSd), negF = fmax(neg, EPSd);
+  const double corr = s / (s > 0 ? posF : negF);
+  for (int st = blockIdx.x; st < S.ntiles; st += gridDim.x) {
+    size_t c; double X; bool perim = false;
+    if (!obst_cell(g, t, st, chig, c, X, perim)) continue;
+    const double T0 = T[c], Tp = T0 + (-X * T0), a = 1 - X;
+    double r;
+    if (s > 0) {
+      // corr = s / pos: T'' = T' (1 - corr) on perimeter cells of T' > 0
+      const bool q = perim && Tp > 0 && corr > 0;
+      const double dcorr = (-X - (pos > EPSd && q ? corr * a : 0.0)) / posF;   // d corr / d T_c
+      r = a * (q ? 1 - corr : 1.0) * lo[c] + dcorr * (-Lp);
+    } else {
+      // corr = s / neg (<= 0): T'' = T' (1 + corr) on perimeter cells of T' < 0
+      const bool q = perim && Tp < 0 && corr < 0;
+      const double dcorr = (-X + (neg > EPSd && q ? corr * a : 0.0)) / negF;
+      r = a * (q ? 1 + corr : 1.0) * lo[c] + dcorr * Ln;
+    }
+    lT[c] = r;
+  }
+}
+
+// ---- the boundary-strip fade F (cub2rhs) ----------------------------------
+__device__ __forceinline__ double fade_w2(const GridDesc& g, int gx, int gy) {
+  const double fadeLenX = g.fadeLenX, invFadeX = 1 / fmax(fadeLenX, EPSd);
+  const double fadeLenY = g.fadeLenY, invFadeY = 1 / fmax(fadeLenY, EPSd);
+  const double px = cell_x(g, gx >> 5, gx & 31), py = cell_y(g, gy >> 5, gy & 31);
+  const double yt = invFadeY * fmax(0.0, fadeLenY - g.ext[1] + py);
+  const double yb = invFadeY * fmax(0.0, fadeLenY - py);
+  const double xt = invFadeX * fmax(0.0, fadeLenX - g.ext[0] + px);
+  const double xb = invFadeX * fmax(0.0, fadeLenX - px);
+  const double fa = fmin(fmax(fmax(yt, yb), fmax(xt, xb)), 1.0);
+  return fa * fa;
+}
+
+// over the strip blocks: S = sum w2 f, Sp, Sn (as the forward), Lp = sum
+// over w2 f > 0 of w2 f lb, Ln = sum over w2 f < 0 of w2 f lb
+__global__ void __launch_bounds__(256)
+k_adj_fade_sums(GridDesc g, const double* __restrict__ f, const double* __restrict__ lb, double* acc)
+{
+  const int bx = blockIdx.x, by = blockIdx.y;
+  if (!fade_touch(g, bx, by)) return;
+  const int gx = bx * BS + threadIdx.x;
+  double a[5] = {0, 0, 0, 0, 0};
+  for (int r = 0; r < 4; r++) {
+    const int gy = by * BS + threadIdx.y + 8 * r;
+    const size_t c = (size_t)gy * g.nx + gx;
+    const double w2 = fade_w2(g, gx, gy), fw = f[c] * w2;
+    a[0] += fw;
+    if (fw > 0) { a[1] += fw; a[3] += fw * lb[c]; }
+    if (fw < 0) { a[2] -= fw; a[4] += fw * lb[c]; }
+  }
+  for (int q = 0; q < 5; q++) {
+    double v = a[q];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v != 0) atomicAdd(&acc[q], v);
+  }
+}
+
+// lf = F'^T lb
+__global__ void __launch_bounds__(256)
+k_adj_fade_apply(GridDesc g, const double* __restrict__ f, const double* __restrict__ lb,
+                 const double* __restrict__ acc, double* __restrict__ lf)
+{
+  const double S = acc[0], Sp = acc[1], Sn = acc[2], Lp = acc[3], Ln = acc[4];
+  const double SpF = fmax(Sp, EPSd), SnF = fmax(Sn, EPSd);
+  const double corr = S > 0 ? S / SpF : S / SnF;
+  const int gx = blockIdx.x * BS + threadIdx.x;
+  for (int r = 0; r < 4; r++) {
+    const int gy = blockIdx.y * BS + threadIdx.y + 8 * r;
+    const size_t c = (size_t)gy * g.nx + gx;
+    const double w2 = fade_touch(g, blockIdx.x, blockIdx.y) ? fade_w2(g, gx, gy) : 0.0;
+    const double fw = f[c] * w2;
+    double r_;
+    if (S > 0) {
+      const bool P = fw > 0;
+      const double dcorr = (w2 - (Sp > EPSd && P ? corr * w2 : 0.0)) / SpF;   // d corr / d f_c
+      r_ = (1 - w2) * lb[c] + (P ? corr * w2 * lb[c] : 0.0) + dcorr * Lp;
+    } else {
+      const bool N = fw < 0;
+      const double dcorr = (w2 + (Sn > EPSd && N ? corr * w2 : 0.0)) / SnF;
+      r_ = (1 - w2) * lb[c] - (N ? corr * w2 * lb[c] : 0.0) - dcorr * Ln;
+    }
+    lf[c] = r_;
+  }
+}
+
+// ---- advDiff, linearized about u^n (advDiff.cpp:57-116) -------------------
+struct AdvC { double afac, dfac, fW, fS, fE, fN, U0, U1; int nb; };
+
+// Gamma = sum of sigma lambda over the boundary cells (sigma: +1 on the W
+// column / S row, -1 on the E column / N row; u on the columns, v on the
+// rows): the outflow correction's rank-one transpose
+__global__ void __launch_bounds__(256)
+k_adj_adv_gamma(GridDesc g, const double* __restrict__ lu, const double* __restrict__ lv, double* acc)
+{
+  const int nx = g.nx, ny = g.ny, n = 2 * (nx + ny);
+  double a = 0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    if (q < ny) a += lu[(size_t)q * nx];
+    else if (q < 2 * ny) a -= lu[(size_t)(q - ny) * nx + nx - 1];
+    else if (q < 2 * ny + nx) a += lv[q - 2 * ny];
+    else a -= lv[(size_t)(ny - 1) * nx + (q - 2 * ny - nx)];
+  }
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if ((threadIdx.x & 31) == 0 && a != 0) atomicAdd(acc, a);
+}
+
+// lambda before the correction: lambda - sigma Gamma / Nb
+__device__ __forceinline__ double lpre_u(const GridDesc& g, const double* lu, size_t c, int x, double gn) {
+  double v = lu[c];
+  if (x == 0) v -= gn;
+  if (x == g.nx - 1) v += gn;
+  return v;
+}
+__device__ __forceinline__ double lpre_v(const GridDesc& g, const double* lv, size_t c, int y, double gn) {
+  double v = lv[c];
+  if (y == 0) v -= gn;
+  if (y == g.ny - 1) v += gn;
+  return v;
+}
+
+__global__ void __launch_bounds__(256)
+k_adj_advdiff(GridDesc g, AdvC k, const double* __restrict__ u, const double* __restrict__ v,
+              const double* __restrict__ lu, const double* __restrict__ lv, const double* __restrict__ acc,
+              double* __restrict__ ou, double* __restrict__ ov)
+{
+  const double gn = acc[0] / k.nb;
+  const int nx = g.nx, ny = g.ny;
+  const int gx = blockIdx.x * BS + threadIdx.x;
+  for (int r = 0; r < 4; r++) {
+    const int gy = blockIdx.y * BS + threadIdx.y + 8 * r;
+    const Nb j = nb_of(g, gx, gy);
+    // the forward's neighbour values at j (ghosts: the cell scaled by the fade)
+    const double uc = u[j.c], vc = v[j.c];
+    const double uW = j.x > 0 ? u[j.W] : uc * k.fW, uE = j.x < nx - 1 ? u[j.E] : uc * k.fE;
+    const double uS = j.y > 0 ? u[j.S] : uc * k.fS, uN = j.y < ny - 1 ? u[j.N] : uc * k.fN;
+    const double vW = j.x > 0 ? v[j.W] : vc * k.fW, vE = j.x < nx - 1 ? v[j.E] : vc * k.fE;
+    const double vS = j.y > 0 ? v[j.S] : vc * k.fS, vN = j.y < ny - 1 ? v[j.N] : vc * k.fN;
+    const double Lu = lpre_u(g, lu, j.c, j.x, gn), Lv = lpre_v(g, lv, j.c, j.y, gn);
+    // coefficients of the neighbours in u'_j, v'_j (the same for both)
+    const double cE = k.afac * (uc + k.U0) + k.dfac, cW = -k.afac * (uc + k.U0) + k.dfac;
+    const double cN = k.afac * (vc + k.U1) + k.dfac, cS = -k.afac * (vc + k.U1) + k.dfac;
+    // j's own terms, with its ghost neighbours folded in
+    double du = 1 + k.afac * (uE - uW) - 4 * k.dfac, dv = 1 + k.afac * (vN - vS) - 4 * k.dfac;
+    double g_ = 0;
+    if (j.x == 0) g_ += cW * k.fW;
+    if (j.x == nx - 1) g_ += cE * k.fE;
+    if (j.y == 0) g_ += cS * k.fS;
+    if (j.y == ny - 1) g_ += cN * k.fN;
+    double au = (du + g_) * Lu + k.afac * (vE - vW) * Lv;
+    double av = (dv + g_) * Lv + k.afac * (uN - uS) * Lu;
+    // neighbours d whose stencil holds j
+    if (j.x >= 1) {                                   // j is the E neighbour of d = j - 1
+      const size_t d = j.c - 1;
+      const double cEd = k.afac * (u[d] + k.U0) + k.dfac;
+      au += cEd * lpre_u(g, lu, d, j.x - 1, gn);
+      av += cEd * lpre_v(g, lv, d, j.y, gn);
+    }
+    if (j.x <= nx - 2) {                              // the W neighbour of d = j + 1
+      const size_t d = j.c + 1;
+      const double cWd = -k.afac * (u[d] + k.U0) + k.dfac;
+      au += cWd * lpre_u(g, lu, d, j.x + 1, gn);
+      av += cWd * lpre_v(g, lv, d, j.y, gn);
+    }
+    if (j.y >= 1) {                                   // the N neighbour of d = j - nx
+      const size_t d = j.c - nx;
+      const double cNd = k.afac * (v[d] + k.U1) + k.dfac;
+      au += cNd * lpre_u(g, lu, d, j.x, gn);
+      av += cNd * lpre_v(g, lv, d, j.y - 1, gn);
+    }
+    if (j.y <= ny - 2) {                              // the S neighbour of d = j + nx
+      const size_t d = j.c + nx;
+      const double cSd = -k.afac * (v[d] + k.U1) + k.dfac;
+      au += cSd * lpre_u(g, lu, d, j.x, gn);
+      av += cSd * lpre_v(g, lv, d, j.y + 1, gn);
+    }
+    ou[j.c] = au;
+    ov[j.c] = av;
+  }
+}
+
+// ---- the objective: (1/N) sum over steps of (h^2/2) sum_box (u^2 + v^2) ---
+struct ProbeBox { int x0, x1, y0, y1; };
+__global__ void __launch_bounds__(256)
+k_adj_probe(GridDesc g, ProbeBox bx, const double* __restrict__ u, const double* __restrict__ v, double w,
+            double* acc, double* lu, double* lv)
+{
+  double a = 0;
+  const int W = bx.x1 - bx.x0, H = bx.y1 - bx.y0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < W * H; q += gridDim.x * blockDim.x) {
+    const size_t c = (size_t)(bx.y0 + q / W) * g.nx + bx.x0 + q % W;
+    const double uc = u[c], vc = v[c];
+    if (acc) a += 0.5 * w * (uc * uc + vc * vc);
+    if (lu) { lu[c] += w * uc; lv[c] += w * vc; }
+  }
+  if (!acc) return;
+  for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+  if ((threadIdx.x & 31) == 0 && a != 0) atomicAdd(acc, a);
+}
+
+} // namespace
+} // namespace cup2d
+
+using namespace cup2d;
+
+namespace {
+
+int adj_fail(cup2d_ctx* ctx, int code, const std::string& msg) {
+  ctx->c.err = msg;
+  return code;
+}
+
+#define ACK(call)                                                               \
+  do {                                                                          \
+    cudaError_t e_ = (call);                                                    \
+    if (e_ != cudaSuccess) return adj_fail(ctx, CUP2D_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define ARC(call)                                                               \
+  do { const int r_ = (call); if (r_ != CUP2D_OK) return r_; } while (0)
+
+// device scratch of the adjoint run, freed on every exit
+struct AdjBufs {
+  std::vector<void*> p;
+  ~AdjBufs() { for (void* q : p) cudaFree(q); }
+  template <typename T> T* get(size_t n) {
+    void* q = nullptr;
+    if (cudaMalloc(&q, sizeof(T) * (n ? n : 1)) != cudaSuccess) return nullptr;
+    p.push_back(q);
+    return static_cast<T*>(q);
+  }
+};
+
+AdvC adv_coef_host(const Ctx& c, double dt, double U0, double U1) {
+  AdvC k;
+  const double h = c.g.h;
+  k.U0 = U0; k.U1 = U1;
+  k.afac = -0.5 * dt / h;
+  k.dfac = (c.g.nu / h) * (dt / h);
+  const double nor = std::max({std::fabs(U0), std::fabs(U1), DBL_EPSILON});
+  auto fade = [](double r) { return 1 - r * r / 100; };   // BC_KILL_FAC = 100
+  k.fW = fade(std::max(U0, 0.0) / nor); k.fS = fade(std::max(U1, 0.0) / nor);
+  k.fE = fade(std::min(U0, 0.0) / nor); k.fN = fade(std::min(U1, 0.0) / nor);
+  k.nb = 2 * (BS * c.g.bpdy) + 2 * (BS * c.g.bpdx);
+  return k;
+}
+
+} // namespace
+
+extern "C" {
+
+int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const double box[4], const double* dt_in,
+                      double* dt_out, double* J, double* grad_u, double* grad_v, double* ms) {
+  if (!ctx || nsteps <= 0 || every <= 0 || !box || !J) return CUP2D_EINVAL;
+  Ctx& c = ctx->c;
+  if (!c.initialised) return adj_fail(ctx, CUP2D_ESTATE, "not initialised");
+  if (c.cfg.iterative || c.varRho || c.cfg.implicit_penalization || c.cfg.precision != CUP2D_PREC_FP64)
+    return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint covers the FP64 PressureSingle pipeline (explicit penalization)");
+  if (c.cfg.poisson != CUP2D_POISSON_FREESPACE)
+    return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint covers the free-space solver");
+  if (c.nshapes != 1)
+    return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint covers one body");
+  const ShapeCfg& sf = c.hshapes[0].cfg;
+  if (!(sf.bForcedx && sf.bForcedy && sf.bBlockang && sf.bFixedx && sf.bFixedy))
+    return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint needs a body forced in x, y and angle and fixed on the grid "
+                                        "(its motion, and so chi, must not depend on the flow)");
+  const GridDesc& g = c.g;
+  const size_t n = c.ncells(), nb = sizeof(double) * n;
+  ProbeBox bx;
+  bx.x0 = std::max(0, (int)std::floor(box[0] / g.h)); bx.x1 = std::min(g.nx, (int)std::ceil(box[1] / g.h));
+  bx.y0 = std::max(0, (int)std::floor(box[2] / g.h)); bx.y1 = std::min(g.ny, (int)std::ceil(box[3] / g.h));
+  if (bx.x1 <= bx.x0 || bx.y1 <= bx.y0) return adj_fail(ctx, CUP2D_EINVAL, "empty probe box");
+  const double wJ = g.h * g.h / nsteps;
+  const dim3 grid2(g.bpdx, g.bpdy), blk2(32, 8);
+  const int probeGrid = std::min(1024, ((bx.x1 - bx.x0) * (bx.y1 - bx.y0) + 255) / 256);
+
+  AdjBufs B;
+  size_t ckBytes = 0;
+  ARC(cup2d_checkpoint_size(ctx, &ckBytes));
+  const int nseg = (nsteps + every - 1) / every;
+  std::vector<void*> ck(nseg + 1);
+  for (int s = 0; s <= nseg; s++)
+    if (!(ck[s] = B.get<char>(ckBytes))) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint checkpoints");
+  double* acc = B.get<double>(8);
+  if (!acc) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint scratch");
+  std::vector<double> dts(nsteps), U0s(nsteps), U1s(nsteps);
+  struct Ev {
+    cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+    ~Ev() { for (cudaEvent_t x : e) if (x) cudaEventDestroy(x); }
+  } ev;
+  for (cudaEvent_t& x : ev.e) ACK(cudaEventCreate(&x));
+  cudaEvent_t e0 = ev.e[0], e1 = ev.e[1], e2 = ev.e[2];
+
+  // one step of the operator path with dt given; T / F, when non-null,
+  // receive the RHS before the obstacle terms and before the fade
+  auto step = [&](double dt, double* T, double* F) -> int {
+    ARC(cup2d_put_objects(ctx, dt));
+    ARC(cup2d_adv_diff(ctx, dt));
+    ARC(pressure_single_keep(ctx, dt, T, F));
+    ARC(cup2d_end_step(ctx));
+    return CUP2D_OK;
+  };
+
+  // forward: checkpoints, the dt schedule, J
+  ACK(cudaMemsetAsync(acc, 0, sizeof(double) * 8, c.stream));
+  ACK(cudaEventRecord(e0, c.stream));
+  for (int i = 0; i < nsteps; i++) {
+    if (i % every == 0) ARC(cup2d_checkpoint_save(ctx, ck[i / every], ckBytes));
+    double dt;
+    if (dt_in) dt = dt_in[i];
+    else ARC(cup2d_calc_dt(ctx, &dt));
+    dts[i] = dt;
+    double t_, dtd, ux, uy; int st;
+    ARC(step(dt, nullptr, nullptr));
+    // u_inf of the step (set by the placement from the forced body)
+    ARC(cup2d_get_scalars(ctx, &t_, &dtd, &st, &ux, &uy));
+    U0s[i] = ux; U1s[i] = uy;
+    k_adj_probe<<<probeGrid, 256, 0, c.stream>>>(g, bx, c.u(), c.v(), wJ, acc, nullptr, nullptr);
+    ACK(cudaGetLastError());
+  }
+  ACK(cudaEventRecord(e1, c.stream));
+  ARC(cup2d_checkpoint_save(ctx, ck[nseg], ckBytes));      // the final state, restored at the end
+  {
+    // the body stays forced over the whole run (Shape.cpp: forced while
+    // time < timeForced)
+    double tEnd, dtd, ux, uy; int st;
+    ARC(cup2d_get_scalars(ctx, &tEnd, &dtd, &st, &ux, &uy));
+    if (!(tEnd <= sf.timeForced))
+      return adj_fail(ctx, CUP2D_ENOTSUP, "the body is released (timeForced) within the run");
+  }
+  ACK(cudaMemcpyAsync(J, acc, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  ACK(cudaStreamSynchronize(c.stream));
+  if (dt_out) std::copy(dts.begin(), dts.end(), dt_out);
+  float fms = 0;
+  ACK(cudaEventElapsedTime(&fms, e0, e1));
+  if (ms) { ms[0] = fms; ms[1] = 0; }
+  if (!grad_u || !grad_v) { ARC(cup2d_checkpoint_load(ctx, ck[nseg], ckBytes)); return CUP2D_OK; }
+
+  // backward
+  const size_t segN = (size_t)every;
+  double* su = B.get<double>(n * segN);      // u^n of the segment's steps
+  double* sv = B.get<double>(n * segN);
+  double* sT = B.get<double>(n * segN);      // RHS before the obstacle terms
+  double* sF = B.get<double>(n * segN);      // RHS before the fade
+  double* pu = B.get<double>(n * segN);      // u^(n+1)
+  double* pv = B.get<double>(n * segN);
+  double* lu = B.get<double>(n);
+  double* lv = B.get<double>(n);
+  double* l1 = B.get<double>(n);
+  double* l2 = B.get<double>(n);
+  double* l3 = B.get<double>(n);
+  double* tu = B.get<double>(n);
+  double* tv = B.get<double>(n);
+  if (!su || !sv || !sT || !sF || !pu || !pv || !lu || !lv || !l1 || !l2 || !l3 || !tu || !tv)
+    return adj_fail(ctx, CUP2D_ENOMEM, "adjoint segment buffers");
+  ACK(cudaMemsetAsync(lu, 0, nb, c.stream));
+  ACK(cudaMemsetAsync(lv, 0, nb, c.stream));
+  ACK(cudaEventRecord(e2, c.stream));
+  const AllTiles T0 = all_tiles(c);
+  const int tctas = tile_ctas(c, c.tiles[0].capacity);
+  for (int s = nseg - 1; s >= 0; s--) {
+    const int i0 = s * every, i1 = std::min(nsteps, i0 + every);
+    ARC(cup2d_checkpoint_load(ctx, ck[s], ckBytes));
+    for (int i = i0; i < i1; i++) {
+      const size_t o = (size_t)(i - i0) * n;
+      ACK(cudaMemcpyAsync(su + o, c.u(), nb, cudaMemcpyDeviceToDevice, c.stream));
+      ACK(cudaMemcpyAsync(sv + o, c.v(), nb, cudaMemcpyDeviceToDevice, c.stream));
+      ARC(step(dts[i], sT + o, sF + o));
+      ACK(cudaMemcpyAsync(pu + o, c.u(), nb, cudaMemcpyDeviceToDevice, c.stream));
+      ACK(cudaMemcpyAsync(pv + o, c.v(), nb, cudaMemcpyDeviceToDevice, c.stream));
+    }
+    for (int i = i1 - 1; i >= i0; i--) {
+      const size_t o = (size_t)(i - i0) * n;
+      const double dt = dts[i];
+      // the objective's term of u^(i+1)
+      k_adj_probe<<<probeGrid, 256, 0, c.stream>>>(g, bx, pu + o, pv + o, wJ, nullptr, lu, lv);
+      // penalization
+      k_adj_pen<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], c.chi, lu, lv);
+      // pressure correction: lambda_p, then the convolution
+      k_adj_grad_T<<<grid2, blk2, 0, c.stream>>>(g, -0.5 * dt / g.h, lu, lv, l1);
+      ACK(cudaGetLastError());
+      {
+        double* const R = c.rhs;
+        double* const P = c.pres;
+        c.rhs = l1; c.pres = l2; c.solveNoFade = true;
+        poisson_solve(c);
+        c.rhs = R; c.pres = P; c.solveNoFade = false;
+      }
+      // the fade: l2 -> l3
+      ACK(cudaMemsetAsync(acc, 0, sizeof(double) * 8, c.stream));
+      k_adj_fade_sums<<<grid2, blk2, 0, c.stream>>>(g, sF + o, l2, acc);
+      k_adj_fade_apply<<<grid2, blk2, 0, c.stream>>>(g, sF + o, l2, acc, l3);
+      // the obstacle terms: l3 -> l1 (cells outside the shape's tiles pass)
+      ACK(cudaMemcpyAsync(l1, l3, nb, cudaMemcpyDeviceToDevice, c.stream));
+      ACK(cudaMemsetAsync(acc, 0, sizeof(double) * 8, c.stream));
+      k_adj_obst_sums<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], c.chi, sT + o, l3, acc);
+      k_adj_obst_apply<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], c.chi, sT + o, l3, acc, l1);
+      // the divergence, added to lambda of u1
+      k_adj_div_T<<<grid2, blk2, 0, c.stream>>>(g, 0.5 * g.h / dt, l1, lu, lv);
+      // advDiff about u^i
+      ACK(cudaMemsetAsync(acc, 0, sizeof(double) * 8, c.stream));
+      k_adj_adv_gamma<<<std::min(148, (2 * (g.nx + g.ny) + 255) / 256), 256, 0, c.stream>>>(g, lu, lv, acc);
+      k_adj_advdiff<<<grid2, blk2, 0, c.stream>>>(g, adv_coef_host(c, dt, U0s[i], U1s[i]), su + o, sv + o,
+                                                 lu, lv, acc, tu, tv);
+      ACK(cudaGetLastError());
+      std::swap(lu, tu);
+      std::swap(lv, tv);
+    }
+  }
+  ACK(cudaEventRecord(e1, c.stream));
+  ACK(cudaMemcpyAsync(grad_u, lu, nb, cudaMemcpyDeviceToHost, c.stream));
+  ACK(cudaMemcpyAsync(grad_v, lv, nb, cudaMemcpyDeviceToHost, c.stream));
+  ACK(cudaStreamSynchronize(c.stream));
+  float bms = 0;
+  ACK(cudaEventElapsedTime(&bms, e2, e1));
+  if (ms) ms[1] = bms;
+  ARC(cup2d_checkpoint_load(ctx, ck[nseg], ckBytes));
+  return CUP2D_OK;
+}
+
+} // extern "C"

@@ -15,8 +15,6 @@
 
 using namespace cup2d;
 
-struct cup2d_ctx { Ctx c; };
-
 namespace {
 
 #define CK(call)                                                                \
@@ -890,7 +888,7 @@ int cup2d_adv_diff(cup2d_ctx* ctx, double dt) {
   return check_launch(ctx);
 }
 
-int cup2d_pressure_single(cup2d_ctx* ctx, double dt) {
+extern "C++" int pressure_single_keep(cup2d_ctx* ctx, double dt, double* keepDiv, double* keepObst) {
   STAGE_PROLOGUE
   c.placedPending = false;
   if (c.varRho) {
@@ -903,11 +901,16 @@ int cup2d_pressure_single(cup2d_ctx* ctx, double dt) {
   }
   if (!c.rhsFresh) launch_rhs_div(c);       // else formed by advDiff at this dt
   c.rhsFresh = false;
+  const size_t nb = sizeof(double) * c.ncells();
+  if (keepDiv) CK(cudaMemcpyAsync(keepDiv, c.rhs, nb, cudaMemcpyDeviceToDevice, c.stream));
   launch_rhs_obstacles(c);
+  if (keepObst) CK(cudaMemcpyAsync(keepObst, c.rhs, nb, cudaMemcpyDeviceToDevice, c.stream));
   poisson_solve(c);
   launch_pressure_tail(c);
   return check_launch(ctx);
 }
+
+int cup2d_pressure_single(cup2d_ctx* ctx, double dt) { return pressure_single_keep(ctx, dt, nullptr, nullptr); }
 
 static double* field_ptr(Ctx& c, int which);
 

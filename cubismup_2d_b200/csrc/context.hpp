@@ -120,6 +120,10 @@ struct Ctx {
   // with the value after its own advance to know a member's read-back is current
   unsigned long long stateSeq = 0;
 
+  // the Poisson solve of the adjoint: the convolution alone, without
+  // cub2rhs's fade (the adjoint applies the fade's transpose itself)
+  bool solveNoFade = false;
+
   cudaGraphExec_t graph = nullptr;
   void* flushBuf = nullptr;      // cup2d_time_kernel's L2 flush (256 MB, allocated on demand)
   unsigned long long* hashAcc = nullptr;   // checkpoint checksum accumulator (on demand)
@@ -183,3 +187,12 @@ inline double* shape_partials(const Ctx& c) { return c.partials + (size_t)3 * c.
 #define CUP2D_LAUNCHED(c) ((c).launches++)
 
 } // namespace cup2d
+
+// the opaque handle of the C ABI
+struct cup2d_ctx { cup2d::Ctx c; };
+
+// cup2d_pressure_single, keeping copies of the RHS before the obstacle
+// terms (keepDiv) and before the fade (keepObst) when these are non-null
+// (the adjoint's recomputation; a constant-density context without the
+// iterated penalization)
+int pressure_single_keep(cup2d_ctx* ctx, double dt, double* keepDiv, double* keepObst);

@@ -1432,7 +1432,7 @@ void poisson_destroy(Poisson* P) {
 void poisson_rows_fwd(Ctx& c) {
   Poisson* P = c.poisson;
   const int Nx = c.g.nx, Ny = c.g.ny;
-  FadeArgs fa{1, c.dsc, c.g, c.rhs, fade_partials(c), c.nfade};
+  FadeArgs fa{c.solveNoFade ? 0 : 1, c.dsc, c.g, c.rhs, fade_partials(c), c.nfade};
   if (P->type == CUP2D_POISSON_COSINE) {
     dct_rows_fwd(P->Lrow, c.stream, c.rhs, Nx, Ny, reinterpret_cast<double*>(P->spec), P->tw, P->twLen, fa);
     CUP2D_LAUNCHED(c);

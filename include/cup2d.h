@@ -296,6 +296,32 @@ int cup2d_checkpoint_size(cup2d_ctx* ctx, size_t* bytes);
 int cup2d_checkpoint_save(cup2d_ctx* ctx, void* buf, size_t bytes);
 int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes);
 
+/* ---- discrete adjoint ---------------------------------------------------- */
+/* No counterpart in the reference.  Runs nsteps operator-path steps
+ * (PutObjectsOnGrid, advDiff, PressureSingle) from the current state and
+ * returns the objective
+ *   J = (1/nsteps) sum_{n=1..nsteps} (h^2/2) sum_{cells in box} (u^2 + v^2)
+ * of the velocity after each step, box = {x0, x1, y0, y1} in domain units
+ * (the cells whose index ranges [floor(x0/h), ceil(x1/h)) etc. cover), and,
+ * when grad_u and grad_v are non-null (host arrays of Nx*Ny, row-major),
+ * dJ/du and dJ/dv of the initial velocity by the transposed steps, each
+ * step's operators linearized about its forward values and applied in
+ * reverse order, with the forward recomputed from device checkpoints taken
+ * every `every` steps.
+ *  - dt_in: the step sizes (nsteps values), or null for calcMaxTimestep's;
+ *    dt_out (nsteps values, or null) receives the schedule used.  dt is not
+ *    differentiated (a frozen schedule);
+ *  - ms (2 values, or null): device time of the forward (with its
+ *    checkpoints) and of the backward (recomputation and transposed steps);
+ *  - covered: FP64, the free-space solver, explicit penalization without
+ *    the iterated or variable-density pipelines, one body forced in x, y
+ *    and angle and fixed on the grid for the whole run (its chi and
+ *    velocity do not depend on the flow); anything else CUP2D_ENOTSUP;
+ *  - the context ends in the forward's final state (as after nsteps
+ *    steps); synchronises. */
+int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const double box[4], const double* dt_in,
+                      double* dt_out, double* J, double* grad_u, double* grad_v, double* ms);
+
 /* ---- batched ensemble --------------------------------------------------- */
 /* No counterpart in the reference (it runs one Simulation per process):
  * n independent simulations on one device, of any grid sizes and shapes,
