@@ -49,6 +49,10 @@ KERNELS = {"advdiff": 0, "rhs_div": 1, "pcorr": 2, "fft_rows_fwd": 3, "fft_cols"
            "fft_rows_inv": 5, "max_u": 6, "objects": 7, "outflow": 8}
 
 
+class AdjointObjective(ctypes.Structure):
+    _fields_ = [("box", ctypes.c_double * 4), ("w_energy", ctypes.c_double), ("w_force", ctypes.c_double * 2)]
+
+
 class Config(ctypes.Structure):
     _fields_ = [("bpdx", ctypes.c_int), ("bpdy", ctypes.c_int), ("extent", ctypes.c_double),
                 ("CFL", ctypes.c_double), ("lambda_", ctypes.c_double), ("dlm", ctypes.c_double),
@@ -130,7 +134,7 @@ def lib():
     L.cup2d_checkpoint_size.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
     L.cup2d_checkpoint_save.argtypes = [vp, vp, ctypes.c_size_t]
     L.cup2d_checkpoint_load.argtypes = [vp, vp, ctypes.c_size_t]
-    L.cup2d_adjoint_run.argtypes = [vp, i, i, dp, dp, dp, dp, dp, dp, dp]
+    L.cup2d_adjoint_run.argtypes = [vp, i, i, ctypes.POINTER(AdjointObjective), dp, dp, dp, dp, dp, dp, dp]
     L.cup2d_ensemble_create.argtypes = [ctypes.POINTER(vp), i, ctypes.POINTER(vp)]
     L.cup2d_ensemble_advance.argtypes = [vp, i]
     L.cup2d_ensemble_advance_timed.argtypes = [vp, i, dp]
@@ -405,18 +409,24 @@ class Context:
         self._ck(self.L.cup2d_checkpoint_save(self.h_, ptr, size))
         return out
 
-    def adjoint(self, nsteps, box, every=20, dt=None, gradient=True):
-        """The objective J = (1/nsteps) sum over the steps' velocities of
-        (h^2/2) sum_box (u^2 + v^2) (box = (x0, x1, y0, y1) in domain units)
-        over nsteps steps from the current state, and its gradient with
-        respect to the current velocity by the discrete adjoint (forward
-        recomputed from checkpoints every ``every`` steps).  dt: the frozen
-        step sizes (nsteps values) or None for calcMaxTimestep's.  Returns
-        (J, grad_u, grad_v, dts, (forward_ms, backward_ms)); the gradients are
-        None when gradient is False.  The context ends in the forward's
-        final state."""
+    def adjoint(self, nsteps, box=None, every=20, dt=None, gradient=True, w_energy=1.0, w_force=(0.0, 0.0)):
+        """The time-averaged objective over nsteps steps from the current state,
+        J = (1/nsteps) sum_n [w_energy (h^2/2) sum_box (u^2 + v^2) + w_force . force]
+        (box = (x0, x1, y0, y1) in domain units; force = ComputeForces'
+        (forcex, forcey) on the body), and its gradient with respect to the
+        current velocity and to the body's velocity by the discrete adjoint
+        (forward recomputed from checkpoints every ``every`` steps).  dt: the
+        frozen step sizes (nsteps values) or None for calcMaxTimestep's.
+        Returns (J, grad_u, grad_v, grad_body, dts, (forward_ms, backward_ms));
+        the gradients are None when gradient is False.  The context ends in
+        the forward's final state."""
         dp = ctypes.POINTER(ctypes.c_double)
-        b = np.ascontiguousarray(box, dtype=np.float64)
+        obj = AdjointObjective()
+        if box is not None:
+            for k in range(4):
+                obj.box[k] = float(box[k])
+        obj.w_energy = float(w_energy) if box is not None else 0.0
+        obj.w_force[0], obj.w_force[1] = float(w_force[0]), float(w_force[1])
         dts = np.empty(nsteps, dtype=np.float64)
         dti = None if dt is None else np.ascontiguousarray(dt, dtype=np.float64)
         if dti is not None and dti.size != nsteps:
@@ -425,10 +435,11 @@ class Context:
         ms = np.zeros(2, dtype=np.float64)
         gu = np.empty((self.ny, self.nx), dtype=np.float64) if gradient else None
         gv = np.empty((self.ny, self.nx), dtype=np.float64) if gradient else None
+        gb = np.zeros(2, dtype=np.float64) if gradient else None
         ptr = lambda a: None if a is None else a.ctypes.data_as(dp)  # noqa: E731
-        self._ck(self.L.cup2d_adjoint_run(self.h_, nsteps, every, ptr(b), ptr(dti), ptr(dts), ctypes.byref(J),
-                                          ptr(gu), ptr(gv), ptr(ms)))
-        return J.value, gu, gv, dts, (float(ms[0]), float(ms[1]))
+        self._ck(self.L.cup2d_adjoint_run(self.h_, nsteps, every, ctypes.byref(obj), ptr(dti), ptr(dts),
+                                          ctypes.byref(J), ptr(gu), ptr(gv), ptr(gb), ptr(ms)))
+        return J.value, gu, gv, gb, dts, (float(ms[0]), float(ms[1]))
 
     def restore(self, blob):
         """Loads a checkpoint of this configuration (host array or device tensor)."""

@@ -102,21 +102,73 @@ k_adj_div_T(GridDesc g, double facDiv, const double* __restrict__ lr, double* __
   }
 }
 
-// Pen^T: lambda *= 1 - chi where the shape owns the cell (penalize's alpha)
+// Pen^T: lambda *= 1 - chi where the shape owns the cell (penalize's
+// alpha); gb += sum chi lambda, the derivative of u = (1 - chi) u + chi U_s
+// with respect to the body velocity U_s (its rotation and deformation parts
+// are not differentiated)
 __global__ void __launch_bounds__(1024)
 k_adj_pen(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
-          double* lu, double* lv)
+          double* lu, double* lv, double* gb)
 {
   const DevShape& S = sh[k];
+  double a[2] = {0, 0};
   for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
     const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
     const size_t o = (size_t)s * BS2 + threadIdx.y * BS + threadIdx.x;
     const size_t c = (size_t)(by * BS + threadIdx.y) * g.nx + bx * BS + threadIdx.x;
     const double X = t.chi[o];
     if (chig[c] > X || X <= 0) continue;
+    a[0] += X * lu[c];
+    a[1] += X * lv[c];
     lu[c] *= 1 - X;
     lv[c] *= 1 - X;
   }
+  for (int q = 0; q < 2; q++) {
+    double v = a[q];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v != 0) atomicAdd(&gb[q], v);
+  }
+}
+
+// ---- the body's force (ComputeForces.cpp:16-111, the surface cells of
+// k_forces): forcex = sum over cells with a surface delta of
+//   nu/h [ (u_E - u_W) nx + (u_N - u_S + v_E - v_W) ny / 2 ] - p nx
+// and forcey alike, linear in u, v and p with clamped neighbours.  With
+// weights (wx, wy) on (forcex, forcey): part 0 adds the velocity terms'
+// transpose to (lu, lv), part 1 the pressure term's to lp.
+__global__ void __launch_bounds__(1024)
+k_adj_force(GridDesc g, const DevShape* sh, int k, ObstTiles t, double wx, double wy, int part,
+            double* lu, double* lv, double* lp)
+{
+  const DevShape& S = sh[k];
+  for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
+    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+    const size_t o = (size_t)s * BS2 + threadIdx.y * BS + threadIdx.x;
+    if (!(t.sD[o] > 0)) continue;
+    const int gx = bx * BS + threadIdx.x, gy = by * BS + threadIdx.y;
+    const Nb j = nb_of(g, gx, gy);
+    const double nX = t.sdx[o], nY = t.sdy[o];
+    if (part == 1) {
+      atomicAdd(&lp[j.c], -(wx * nX + wy * nY));
+      continue;
+    }
+    const double NUoH = g.nu / g.h;
+    const double a = wx * NUoH * nX;                     // on u_E - u_W
+    const double q = (wx * nY + wy * nX) * NUoH / 2;     // on u_N - u_S and on v_E - v_W
+    const double d = wy * NUoH * nY;                     // on v_N - v_S
+    atomicAdd(&lu[j.E], a); atomicAdd(&lu[j.W], -a);
+    atomicAdd(&lu[j.N], q); atomicAdd(&lu[j.S], -q);
+    atomicAdd(&lv[j.E], q); atomicAdd(&lv[j.W], -q);
+    atomicAdd(&lv[j.N], d); atomicAdd(&lv[j.S], -d);
+  }
+}
+
+// the objective's force term of a step: acc += wx forcex + wy forcey of
+// the state k_forces left
+__global__ void k_adj_force_sum(const DevShape* sh, int k, double wx, double wy, double* acc)
+{
+  const cup2d_shape_state& s = sh[k].s;
+  *acc += wx * s.forcex + wy * s.forcey;
 }
 
 // ---- the obstacle RHS terms O (k_rhs_obst, k_rhs_corr) --------------------
@@ -260,7 +312,8 @@ k_adj_fade_apply(GridDesc g, const double* __restrict__ f, const double* __restr
 }
 
 // ---- advDiff, linearized about u^n (advDiff.cpp:57-116) -------------------
-struct AdvC { double afac, dfac, fW, fS, fE, fN, U0, U1; int nb; };
+// dW..dN: the inflow fades' derivatives with respect to (U0, U1)
+struct AdvC { double afac, dfac, fW, fS, fE, fN, U0, U1; double dW[2], dS[2], dE[2], dN[2]; int nb; };
 
 // Gamma = sum of sigma lambda over the boundary cells (sigma: +1 on the W
 // column / S row, -1 on the E column / N row; u on the columns, v on the
@@ -294,14 +347,17 @@ __device__ __forceinline__ double lpre_v(const GridDesc& g, const double* lv, si
   return v;
 }
 
+// (ou, ov) = A'^T (lu, lv); gb -= the derivative with respect to the lab
+// velocity (U0, U1) = -(body velocity) of a fixed body
 __global__ void __launch_bounds__(256)
 k_adj_advdiff(GridDesc g, AdvC k, const double* __restrict__ u, const double* __restrict__ v,
               const double* __restrict__ lu, const double* __restrict__ lv, const double* __restrict__ acc,
-              double* __restrict__ ou, double* __restrict__ ov)
+              double* __restrict__ ou, double* __restrict__ ov, double* gb)
 {
   const double gn = acc[0] / k.nb;
   const int nx = g.nx, ny = g.ny;
   const int gx = blockIdx.x * BS + threadIdx.x;
+  double dU[2] = {0, 0};
   for (int r = 0; r < 4; r++) {
     const int gy = blockIdx.y * BS + threadIdx.y + 8 * r;
     const Nb j = nb_of(g, gx, gy);
@@ -324,6 +380,18 @@ k_adj_advdiff(GridDesc g, AdvC k, const double* __restrict__ u, const double* __
     if (j.y == ny - 1) g_ += cN * k.fN;
     double au = (du + g_) * Lu + k.afac * (vE - vW) * Lv;
     double av = (dv + g_) * Lv + k.afac * (uN - uS) * Lu;
+    // d(u'_j, v'_j)/dU: the advecting velocity, and the fades of j's ghosts
+    {
+      double e[2] = {0, 0};                             // sum over j's ghosts of c_ghost df/dU
+      for (int q = 0; q < 2; q++) {
+        if (j.x == 0) e[q] += cW * k.dW[q];
+        if (j.x == nx - 1) e[q] += cE * k.dE[q];
+        if (j.y == 0) e[q] += cS * k.dS[q];
+        if (j.y == ny - 1) e[q] += cN * k.dN[q];
+      }
+      dU[0] += Lu * (k.afac * (uE - uW) + e[0] * uc) + Lv * (k.afac * (vE - vW) + e[0] * vc);
+      dU[1] += Lu * (k.afac * (uN - uS) + e[1] * uc) + Lv * (k.afac * (vN - vS) + e[1] * vc);
+    }
     // neighbours d whose stencil holds j
     if (j.x >= 1) {                                   // j is the E neighbour of d = j - 1
       const size_t d = j.c - 1;
@@ -351,6 +419,11 @@ k_adj_advdiff(GridDesc g, AdvC k, const double* __restrict__ u, const double* __
     }
     ou[j.c] = au;
     ov[j.c] = av;
+  }
+  for (int q = 0; q < 2; q++) {
+    double w = dU[q];
+    for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+    if ((threadIdx.x & 31) == 0 && w != 0) atomicAdd(&gb[q], -w);
   }
 }
 
@@ -412,10 +485,24 @@ AdvC adv_coef_host(const Ctx& c, double dt, double U0, double U1) {
   k.U0 = U0; k.U1 = U1;
   k.afac = -0.5 * dt / h;
   k.dfac = (c.g.nu / h) * (dt / h);
+  // fades 1 - r^2/100 of r = max/min(U, 0) / nor, nor = max(|U0|, |U1|, eps)
   const double nor = std::max({std::fabs(U0), std::fabs(U1), DBL_EPSILON});
-  auto fade = [](double r) { return 1 - r * r / 100; };   // BC_KILL_FAC = 100
-  k.fW = fade(std::max(U0, 0.0) / nor); k.fS = fade(std::max(U1, 0.0) / nor);
-  k.fE = fade(std::min(U0, 0.0) / nor); k.fN = fade(std::min(U1, 0.0) / nor);
+  double dnor[2] = {0, 0};
+  if (std::fabs(U0) >= std::fabs(U1) && std::fabs(U0) > DBL_EPSILON) dnor[0] = U0 > 0 ? 1 : -1;
+  else if (std::fabs(U1) > DBL_EPSILON) dnor[1] = U1 > 0 ? 1 : -1;
+  auto fade = [&](double m, int comp, bool pos, double* d) {
+    // m = max(U, 0) (pos) or min(U, 0) of component comp
+    const double r = m / nor;
+    const double Uc = comp == 0 ? U0 : U1;
+    const bool active = pos ? Uc > 0 : Uc < 0;
+    for (int q = 0; q < 2; q++) {
+      const double dr = (q == comp && active ? 1.0 / nor : 0.0) - m / (nor * nor) * dnor[q];
+      d[q] = -2 * r / 100 * dr;
+    }
+    return 1 - r * r / 100;                               // BC_KILL_FAC = 100
+  };
+  k.fW = fade(std::max(U0, 0.0), 0, true, k.dW); k.fS = fade(std::max(U1, 0.0), 1, true, k.dS);
+  k.fE = fade(std::min(U0, 0.0), 0, false, k.dE); k.fN = fade(std::min(U1, 0.0), 1, false, k.dN);
   k.nb = 2 * (BS * c.g.bpdy) + 2 * (BS * c.g.bpdx);
   return k;
 }
@@ -424,9 +511,10 @@ AdvC adv_coef_host(const Ctx& c, double dt, double U0, double U1) {
 
 extern "C" {
 
-int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const double box[4], const double* dt_in,
-                      double* dt_out, double* J, double* grad_u, double* grad_v, double* ms) {
-  if (!ctx || nsteps <= 0 || every <= 0 || !box || !J) return CUP2D_EINVAL;
+int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint_objective* obj,
+                      const double* dt_in, double* dt_out, double* J, double* grad_u, double* grad_v,
+                      double* grad_body, double* ms) {
+  if (!ctx || nsteps <= 0 || every <= 0 || !obj || !J) return CUP2D_EINVAL;
   Ctx& c = ctx->c;
   if (!c.initialised) return adj_fail(ctx, CUP2D_ESTATE, "not initialised");
   if (c.cfg.iterative || c.varRho || c.cfg.implicit_penalization || c.cfg.precision != CUP2D_PREC_FP64)
@@ -436,18 +524,31 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const double box[4]
   if (c.nshapes != 1)
     return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint covers one body");
   const ShapeCfg& sf = c.hshapes[0].cfg;
+  if (sf.kind != CUP2D_SHAPE_DISK)
+    return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint covers a disk (a swimmer's chi and udef move with its gait)");
   if (!(sf.bForcedx && sf.bForcedy && sf.bBlockang && sf.bFixedx && sf.bFixedy))
     return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint needs a body forced in x, y and angle and fixed on the grid "
                                         "(its motion, and so chi, must not depend on the flow)");
   const GridDesc& g = c.g;
+  {
+    double t0, dtd, ux, uy; int st;
+    ARC(cup2d_get_scalars(ctx, &t0, &dtd, &st, &ux, &uy));
+    if (sf.kind == CUP2D_SHAPE_DISK && sf.tAccel > 0 && t0 < sf.tAccel)
+      return adj_fail(ctx, CUP2D_ENOTSUP, "the body is still accelerating (tAccel): its velocity is not held");
+  }
   const size_t n = c.ncells(), nb = sizeof(double) * n;
-  ProbeBox bx;
-  bx.x0 = std::max(0, (int)std::floor(box[0] / g.h)); bx.x1 = std::min(g.nx, (int)std::ceil(box[1] / g.h));
-  bx.y0 = std::max(0, (int)std::floor(box[2] / g.h)); bx.y1 = std::min(g.ny, (int)std::ceil(box[3] / g.h));
-  if (bx.x1 <= bx.x0 || bx.y1 <= bx.y0) return adj_fail(ctx, CUP2D_EINVAL, "empty probe box");
-  const double wJ = g.h * g.h / nsteps;
+  const bool energy = obj->w_energy != 0;
+  const bool force = obj->w_force[0] != 0 || obj->w_force[1] != 0;
+  ProbeBox bx{0, 0, 0, 0};
+  if (energy) {
+    bx.x0 = std::max(0, (int)std::floor(obj->box[0] / g.h)); bx.x1 = std::min(g.nx, (int)std::ceil(obj->box[1] / g.h));
+    bx.y0 = std::max(0, (int)std::floor(obj->box[2] / g.h)); bx.y1 = std::min(g.ny, (int)std::ceil(obj->box[3] / g.h));
+    if (bx.x1 <= bx.x0 || bx.y1 <= bx.y0) return adj_fail(ctx, CUP2D_EINVAL, "empty probe box");
+  }
+  const double wE = obj->w_energy * g.h * g.h / nsteps;   // the energy term's weight per step
+  const double wFx = obj->w_force[0] / nsteps, wFy = obj->w_force[1] / nsteps;
   const dim3 grid2(g.bpdx, g.bpdy), blk2(32, 8);
-  const int probeGrid = std::min(1024, ((bx.x1 - bx.x0) * (bx.y1 - bx.y0) + 255) / 256);
+  const int probeGrid = energy ? std::min(1024, ((bx.x1 - bx.x0) * (bx.y1 - bx.y0) + 255) / 256) : 1;
 
   AdjBufs B;
   size_t ckBytes = 0;
@@ -456,8 +557,9 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const double box[4]
   std::vector<void*> ck(nseg + 1);
   for (int s = 0; s <= nseg; s++)
     if (!(ck[s] = B.get<char>(ckBytes))) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint checkpoints");
-  double* acc = B.get<double>(8);
-  if (!acc) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint scratch");
+  double* acc = B.get<double>(8);          // [0..4] reductions of a transposed stage
+  double* obv = B.get<double>(4);          // [0] J, [1..2] the body-velocity gradient
+  if (!acc || !obv) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint scratch");
   std::vector<double> dts(nsteps), U0s(nsteps), U1s(nsteps);
   struct Ev {
     cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
@@ -466,18 +568,20 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const double box[4]
   for (cudaEvent_t& x : ev.e) ACK(cudaEventCreate(&x));
   cudaEvent_t e0 = ev.e[0], e1 = ev.e[1], e2 = ev.e[2];
 
-  // one step of the operator path with dt given; T / F, when non-null,
-  // receive the RHS before the obstacle terms and before the fade
+  // one step of Simulation::advance with dt given (PutObjectsOnGrid, advDiff,
+  // PressureSingle, ComputeForces); T / F, when non-null, receive the RHS
+  // before the obstacle terms and before the fade
   auto step = [&](double dt, double* T, double* F) -> int {
     ARC(cup2d_put_objects(ctx, dt));
     ARC(cup2d_adv_diff(ctx, dt));
     ARC(pressure_single_keep(ctx, dt, T, F));
+    ARC(cup2d_compute_forces(ctx, dt));
     ARC(cup2d_end_step(ctx));
     return CUP2D_OK;
   };
 
   // forward: checkpoints, the dt schedule, J
-  ACK(cudaMemsetAsync(acc, 0, sizeof(double) * 8, c.stream));
+  ACK(cudaMemsetAsync(obv, 0, sizeof(double) * 4, c.stream));
   ACK(cudaEventRecord(e0, c.stream));
   for (int i = 0; i < nsteps; i++) {
     if (i % every == 0) ARC(cup2d_checkpoint_save(ctx, ck[i / every], ckBytes));
@@ -485,12 +589,13 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const double box[4]
     if (dt_in) dt = dt_in[i];
     else ARC(cup2d_calc_dt(ctx, &dt));
     dts[i] = dt;
-    double t_, dtd, ux, uy; int st;
     ARC(step(dt, nullptr, nullptr));
-    // u_inf of the step (set by the placement from the forced body)
+    // the lab velocity of the step (set by the placement from the forced body)
+    double t_, dtd, ux, uy; int st;
     ARC(cup2d_get_scalars(ctx, &t_, &dtd, &st, &ux, &uy));
     U0s[i] = ux; U1s[i] = uy;
-    k_adj_probe<<<probeGrid, 256, 0, c.stream>>>(g, bx, c.u(), c.v(), wJ, acc, nullptr, nullptr);
+    if (energy) k_adj_probe<<<probeGrid, 256, 0, c.stream>>>(g, bx, c.u(), c.v(), wE, obv, nullptr, nullptr);
+    if (force) k_adj_force_sum<<<1, 1, 0, c.stream>>>(c.dshapes, 0, wFx, wFy, obv);
     ACK(cudaGetLastError());
   }
   ACK(cudaEventRecord(e1, c.stream));
@@ -503,13 +608,13 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const double box[4]
     if (!(tEnd <= sf.timeForced))
       return adj_fail(ctx, CUP2D_ENOTSUP, "the body is released (timeForced) within the run");
   }
-  ACK(cudaMemcpyAsync(J, acc, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  ACK(cudaMemcpyAsync(J, obv, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
   ACK(cudaStreamSynchronize(c.stream));
   if (dt_out) std::copy(dts.begin(), dts.end(), dt_out);
   float fms = 0;
   ACK(cudaEventElapsedTime(&fms, e0, e1));
   if (ms) { ms[0] = fms; ms[1] = 0; }
-  if (!grad_u || !grad_v) { ARC(cup2d_checkpoint_load(ctx, ck[nseg], ckBytes)); return CUP2D_OK; }
+  if (!grad_u && !grad_v && !grad_body) { ARC(cup2d_checkpoint_load(ctx, ck[nseg], ckBytes)); return CUP2D_OK; }
 
   // backward
   const size_t segN = (size_t)every;
@@ -517,8 +622,8 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const double box[4]
   double* sv = B.get<double>(n * segN);
   double* sT = B.get<double>(n * segN);      // RHS before the obstacle terms
   double* sF = B.get<double>(n * segN);      // RHS before the fade
-  double* pu = B.get<double>(n * segN);      // u^(n+1)
-  double* pv = B.get<double>(n * segN);
+  double* pu = energy ? B.get<double>(n * segN) : sv;   // u^(n+1) (the energy term)
+  double* pv = energy ? B.get<double>(n * segN) : sv;
   double* lu = B.get<double>(n);
   double* lv = B.get<double>(n);
   double* l1 = B.get<double>(n);
@@ -530,6 +635,7 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const double box[4]
     return adj_fail(ctx, CUP2D_ENOMEM, "adjoint segment buffers");
   ACK(cudaMemsetAsync(lu, 0, nb, c.stream));
   ACK(cudaMemsetAsync(lv, 0, nb, c.stream));
+  ACK(cudaMemsetAsync(obv + 1, 0, sizeof(double) * 2, c.stream));
   ACK(cudaEventRecord(e2, c.stream));
   const AllTiles T0 = all_tiles(c);
   const int tctas = tile_ctas(c, c.tiles[0].capacity);
@@ -541,18 +647,24 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const double box[4]
       ACK(cudaMemcpyAsync(su + o, c.u(), nb, cudaMemcpyDeviceToDevice, c.stream));
       ACK(cudaMemcpyAsync(sv + o, c.v(), nb, cudaMemcpyDeviceToDevice, c.stream));
       ARC(step(dts[i], sT + o, sF + o));
-      ACK(cudaMemcpyAsync(pu + o, c.u(), nb, cudaMemcpyDeviceToDevice, c.stream));
-      ACK(cudaMemcpyAsync(pv + o, c.v(), nb, cudaMemcpyDeviceToDevice, c.stream));
+      if (energy) {
+        ACK(cudaMemcpyAsync(pu + o, c.u(), nb, cudaMemcpyDeviceToDevice, c.stream));
+        ACK(cudaMemcpyAsync(pv + o, c.v(), nb, cudaMemcpyDeviceToDevice, c.stream));
+      }
     }
     for (int i = i1 - 1; i >= i0; i--) {
       const size_t o = (size_t)(i - i0) * n;
       const double dt = dts[i];
-      // the objective's term of u^(i+1)
-      k_adj_probe<<<probeGrid, 256, 0, c.stream>>>(g, bx, pu + o, pv + o, wJ, nullptr, lu, lv);
+      // the objective's terms of u^(i+1), p^(i+1)
+      if (energy) k_adj_probe<<<probeGrid, 256, 0, c.stream>>>(g, bx, pu + o, pv + o, wE, nullptr, lu, lv);
+      if (force)
+        k_adj_force<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], wFx, wFy, 0, lu, lv, nullptr);
       // penalization
-      k_adj_pen<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], c.chi, lu, lv);
-      // pressure correction: lambda_p, then the convolution
+      k_adj_pen<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], c.chi, lu, lv, obv + 1);
+      // pressure correction: lambda_p, the force's pressure term, then the convolution
       k_adj_grad_T<<<grid2, blk2, 0, c.stream>>>(g, -0.5 * dt / g.h, lu, lv, l1);
+      if (force)
+        k_adj_force<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], wFx, wFy, 1, nullptr, nullptr, l1);
       ACK(cudaGetLastError());
       {
         double* const R = c.rhs;
@@ -576,15 +688,16 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const double box[4]
       ACK(cudaMemsetAsync(acc, 0, sizeof(double) * 8, c.stream));
       k_adj_adv_gamma<<<std::min(148, (2 * (g.nx + g.ny) + 255) / 256), 256, 0, c.stream>>>(g, lu, lv, acc);
       k_adj_advdiff<<<grid2, blk2, 0, c.stream>>>(g, adv_coef_host(c, dt, U0s[i], U1s[i]), su + o, sv + o,
-                                                 lu, lv, acc, tu, tv);
+                                                 lu, lv, acc, tu, tv, obv + 1);
       ACK(cudaGetLastError());
       std::swap(lu, tu);
       std::swap(lv, tv);
     }
   }
   ACK(cudaEventRecord(e1, c.stream));
-  ACK(cudaMemcpyAsync(grad_u, lu, nb, cudaMemcpyDeviceToHost, c.stream));
-  ACK(cudaMemcpyAsync(grad_v, lv, nb, cudaMemcpyDeviceToHost, c.stream));
+  if (grad_u) ACK(cudaMemcpyAsync(grad_u, lu, nb, cudaMemcpyDeviceToHost, c.stream));
+  if (grad_v) ACK(cudaMemcpyAsync(grad_v, lv, nb, cudaMemcpyDeviceToHost, c.stream));
+  if (grad_body) ACK(cudaMemcpyAsync(grad_body, obv + 1, sizeof(double) * 2, cudaMemcpyDeviceToHost, c.stream));
   ACK(cudaStreamSynchronize(c.stream));
   float bms = 0;
   ACK(cudaEventElapsedTime(&bms, e2, e1));

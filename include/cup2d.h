@@ -297,30 +297,39 @@ int cup2d_checkpoint_save(cup2d_ctx* ctx, void* buf, size_t bytes);
 int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes);
 
 /* ---- discrete adjoint ---------------------------------------------------- */
-/* No counterpart in the reference.  Runs nsteps operator-path steps
- * (PutObjectsOnGrid, advDiff, PressureSingle) from the current state and
- * returns the objective
- *   J = (1/nsteps) sum_{n=1..nsteps} (h^2/2) sum_{cells in box} (u^2 + v^2)
- * of the velocity after each step, box = {x0, x1, y0, y1} in domain units
- * (the cells whose index ranges [floor(x0/h), ceil(x1/h)) etc. cover), and,
- * when grad_u and grad_v are non-null (host arrays of Nx*Ny, row-major),
- * dJ/du and dJ/dv of the initial velocity by the transposed steps, each
- * step's operators linearized about its forward values and applied in
- * reverse order, with the forward recomputed from device checkpoints taken
- * every `every` steps.
+/* No counterpart in the reference.  Runs nsteps steps of Simulation::advance
+ * (PutObjectsOnGrid, advDiff, PressureSingle, ComputeForces) from the
+ * current state and returns the time-averaged objective
+ *   J = (1/nsteps) sum_{n=1..nsteps} [ w_energy (h^2/2) sum_box (u^2 + v^2)
+ *                                      + w_force . (forcex, forcey) ]
+ * of each step's final velocity and ComputeForces' force on the body
+ * (box = {x0, x1, y0, y1} in domain units: the cells whose index ranges
+ * [floor(x0/h), ceil(x1/h)) etc. cover), and, by the transposed steps, its
+ * gradient with respect to the initial velocity (grad_u, grad_v: host
+ * arrays of Nx*Ny, row-major, or null) and to the body's velocity
+ * (grad_body: 2 values, or null), each step's operators linearized about
+ * its forward values and applied in reverse order, the forward recomputed
+ * from device checkpoints taken every `every` steps.
  *  - dt_in: the step sizes (nsteps values), or null for calcMaxTimestep's;
  *    dt_out (nsteps values, or null) receives the schedule used.  dt is not
  *    differentiated (a frozen schedule);
  *  - ms (2 values, or null): device time of the forward (with its
  *    checkpoints) and of the backward (recomputation and transposed steps);
  *  - covered: FP64, the free-space solver, explicit penalization without
- *    the iterated or variable-density pipelines, one body forced in x, y
- *    and angle and fixed on the grid for the whole run (its chi and
- *    velocity do not depend on the flow); anything else CUP2D_ENOTSUP;
+ *    the iterated or variable-density pipelines, one disk forced in x, y
+ *    and angle and fixed on the grid for the whole run, past its tAccel
+ *    ramp (its chi does not move and its velocity is held; the lab velocity
+ *    is minus the body's); anything else CUP2D_ENOTSUP;
  *  - the context ends in the forward's final state (as after nsteps
  *    steps); synchronises. */
-int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const double box[4], const double* dt_in,
-                      double* dt_out, double* J, double* grad_u, double* grad_v, double* ms);
+typedef struct cup2d_adjoint_objective {
+  double box[4];          /* the kinetic-energy probe: x0, x1, y0, y1      */
+  double w_energy;        /* its weight (0: no energy term, box unused)    */
+  double w_force[2];      /* weights of the body's forcex and forcey       */
+} cup2d_adjoint_objective;
+int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint_objective* obj,
+                      const double* dt_in, double* dt_out, double* J, double* grad_u, double* grad_v,
+                      double* grad_body, double* ms);
 
 /* ---- batched ensemble --------------------------------------------------- */
 /* No counterpart in the reference (it runs one Simulation per process):

@@ -373,6 +373,11 @@ void ref_set_pose(void* h, int id, double cx, double cy, double px, double py, d
   s->center[0] = px; s->center[1] = py;
   s->setOrientation(ang);
 }
+// Shape::u, v, omega (Shape.h:45-47): a forced body keeps them (Shape.cpp:52-59)
+void ref_set_shape_velocity(void* h, int id, double u, double v, double omega) {
+  Shape* s = ((RefSim*)h)->sim.shapes[id];
+  s->u = u; s->v = v; s->omega = omega;
+}
 double ref_fish_period(void* h, int id) {
   auto* f = dynamic_cast<StefanFish*>(((RefSim*)h)->sim.shapes[id]);
   return f ? f->getLearnTPeriod() : -1;

@@ -93,6 +93,7 @@ def lib():
     L.ref_get_obstacle.argtypes = [vp, i, dp]
     L.ref_get_obstacle.restype = ctypes.c_long
     L.ref_set_pose.argtypes = [vp, i, d, d, d, d, d]
+    L.ref_set_shape_velocity.argtypes = [vp, i, d, d, d]
     L.ref_fish_act.argtypes = [vp, i, d, dp, i]
     L.ref_fish_act.restype = i
     L.ref_fish_period.argtypes = [vp, i]
@@ -248,6 +249,10 @@ class RefSim:
         """Shape::setCenterOfMass / center / setOrientation (as an RL driver's
         resetIC does, main_RL_leadFollow.cpp:27-41)."""
         self.L.ref_set_pose(self.h_, k, com[0], com[1], center[0], center[1], orientation)
+
+    def set_shape_velocity(self, k, u, v, omega):
+        """Shape::u, v, omega of shape k (a forced body keeps them)."""
+        self.L.ref_set_shape_velocity(self.h_, k, u, v, omega)
 
     def run_op(self, name, dt):
         self.L.ref_run_op(self.h_, OPS[name], dt)

@@ -103,10 +103,11 @@ def test_header_compiles_as_c_and_matches_the_binding(tmp_path):
     src.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "cup2d.h"\n'
         "int main(void) {\n"
-        '  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(cup2d_config), sizeof(cup2d_shape_params),\n'
-        "         sizeof(cup2d_shape_state), offsetof(cup2d_config, iterative),\n"
+        '  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(cup2d_config),\n'
+        "         sizeof(cup2d_shape_params), sizeof(cup2d_shape_state), offsetof(cup2d_config, iterative),\n"
         "         offsetof(cup2d_shape_state, forcex), offsetof(cup2d_config, gravity),\n"
-        "         offsetof(cup2d_config, autotune), sizeof(cup2d_tuning), offsetof(cup2d_tuning, us));\n"
+        "         offsetof(cup2d_config, autotune), sizeof(cup2d_tuning), offsetof(cup2d_tuning, us),\n"
+        "         sizeof(cup2d_adjoint_objective), offsetof(cup2d_adjoint_objective, w_force));\n"
         "  return 0;\n}\n")
     exe = tmp_path / "layout"
     r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
@@ -115,4 +116,5 @@ def test_header_compiles_as_c_and_matches_the_binding(tmp_path):
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
     assert got == [ctypes.sizeof(abi.Config), ctypes.sizeof(abi.ShapeParams), ctypes.sizeof(abi.ShapeState),
                    abi.Config.iterative.offset, abi.ShapeState.forcex.offset, abi.Config.gravity.offset,
-                   abi.Config.autotune.offset, ctypes.sizeof(abi.Tuning), abi.Tuning.us.offset]
+                   abi.Config.autotune.offset, ctypes.sizeof(abi.Tuning), abi.Tuning.us.offset,
+                   ctypes.sizeof(abi.AdjointObjective), abi.AdjointObjective.w_force.offset]

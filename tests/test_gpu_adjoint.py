@@ -1,9 +1,13 @@
-"""The discrete adjoint (cup2d_adjoint_run; no counterpart in the reference):
-the objective against the plain forward steps, the gradient with respect to
-the initial velocity against central finite differences of the FP64 forward
-along localized directions (in the wake, at the body, at the domain edge
-where the fades and the outflow correction act), independence of the
-checkpoint interval, the final state, and the configurations it refuses."""
+"""The discrete adjoint (cup2d_adjoint_run; no counterpart in the reference).
+Objectives: the time-averaged kinetic energy in a box behind a forced
+cylinder, and its time-averaged force (ComputeForces' forcex / forcey).
+Checked: the objective against the plain operator steps; the gradient with
+respect to the initial velocity along localized directions (in the wake, at
+the body, at the domain edge where the fades and the outflow correction
+act) and with respect to the body's velocity, against central finite
+differences of this FP64 forward and of the reference's own steps (the
+compiled oracle); independence of the checkpoint interval; the final state;
+the torch.autograd binding; the configurations it refuses."""
 import numpy as np
 import pytest
 
@@ -17,6 +21,15 @@ FORCED = (BASE + "-bpdx 8 -bpdy 4 -poissonType freespace "
           "-shapes 'disk radius=0.06 xpos=0.3 ypos=0.25 bForced=1 bFixed=1 xvel=0.2'")
 BOX = (0.36, 0.62, 0.14, 0.36)
 NSTEPS = 16
+BUMPS = {"wake": (0.45, 0.27, 0.04), "body": (0.3, 0.31, 0.03),
+         "edge": (0.97, 0.22, 0.05), "inflow": (0.05, 0.3, 0.05)}
+# central differences at 1e-6: the fade's and the obstacle terms' sign tests
+# make the forward piecewise smooth, and a larger step crosses their
+# switches (1e-4 does, at the edge and the inflow)
+EPS = 1e-6
+ENERGY = dict(box=BOX)
+DRAG = dict(box=None, w_force=(1.0, 0.0))
+BOTH = dict(box=BOX, w_energy=1.0, w_force=(1e-4, 2e-4))
 
 
 def _developed(args=FORCED, warm=40):
@@ -28,79 +41,190 @@ def _developed(args=FORCED, warm=40):
     return s
 
 
-def _bump(s, cx, cy, sig, au, av):
-    n = s.ctx
-    x = (np.arange(n.nx) + 0.5) * n.h
-    y = (np.arange(n.ny) + 0.5) * n.h
+def _bump(ctx, where, au=0.7, av=-0.4):
+    cx, cy, sig = BUMPS[where]
+    x = (np.arange(ctx.nx) + 0.5) * ctx.h
+    y = (np.arange(ctx.ny) + 0.5) * ctx.h
     X, Y = np.meshgrid(x, y)
     g = np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / sig ** 2)
     return au * g, av * g
 
 
-def _objective(s, dts):
-    """J of the plain operator path: (1/N) sum_n (h^2/2) sum_box |u^n|^2."""
+def _fd(ctx, blob, dts, obj, du=None, dv=None, dub=None):
+    """Central difference of J along (du, dv) of the initial velocity and dub
+    of the body velocity, the dt schedule frozen."""
+    u0, v0 = ctx.get("u"), ctx.get("v")
+    ub = ctx.shape(0)
+    Js = []
+    for sgn in (1, -1):
+        ctx.restore(blob)
+        if du is not None:
+            ctx.set("u", u0 + sgn * EPS * du)
+            ctx.set("v", v0 + sgn * EPS * dv)
+        if dub is not None:
+            ctx.set_shape(0, {"u": ub["u"] + sgn * EPS * dub[0], "v": ub["v"] + sgn * EPS * dub[1]})
+        Js.append(ctx.adjoint(NSTEPS, dt=dts, gradient=False, **obj)[0])
+    ctx.restore(blob)
+    return (Js[0] - Js[1]) / (2 * EPS)
+
+
+def _objective_plain(s, dts, obj):
+    """J along the plain operator path."""
     n = s.ctx
-    i0, i1 = int(np.floor(BOX[0] / n.h)), int(np.ceil(BOX[1] / n.h))
-    j0, j1 = int(np.floor(BOX[2] / n.h)), int(np.ceil(BOX[3] / n.h))
+    box = obj.get("box")
+    wE = obj.get("w_energy", 1.0) if box is not None else 0.0
+    wF = obj.get("w_force", (0.0, 0.0))
     J = 0.0
     for dt in dts:
         s.advance(dt)
-        u, v = n.get("u")[j0:j1, i0:i1], n.get("v")[j0:j1, i0:i1]
-        J += 0.5 * n.h ** 2 * float(np.sum(u * u + v * v))
+        if wE:
+            i0, i1 = int(np.floor(box[0] / n.h)), int(np.ceil(box[1] / n.h))
+            j0, j1 = int(np.floor(box[2] / n.h)), int(np.ceil(box[3] / n.h))
+            u, v = n.get("u")[j0:j1, i0:i1], n.get("v")[j0:j1, i0:i1]
+            J += wE * 0.5 * n.h ** 2 * float(np.sum(u * u + v * v))
+        st = n.shape(0)
+        J += wF[0] * st["forcex"] + wF[1] * st["forcey"]
     return J / len(dts)
 
 
-def test_objective_and_final_state_match_plain_steps():
+@pytest.mark.parametrize("obj", [ENERGY, DRAG, BOTH], ids=["energy", "drag", "both"])
+def test_objective_and_final_state_match_plain_steps(obj):
     s = _developed()
     blob = s.ctx.checkpoint()
-    J, gu, gv, dts, ms = s.ctx.adjoint(NSTEPS, BOX, every=5)
+    J, gu, gv, gb, dts, ms = s.ctx.adjoint(NSTEPS, every=5, **obj)
     assert np.all(dts > 0) and ms[0] > 0 and ms[1] > 0
     assert np.all(np.isfinite(gu)) and np.all(np.isfinite(gv)) and np.any(gu != 0)
+    assert np.all(np.isfinite(gb))
     ua, va = s.ctx.get("u"), s.ctx.get("v")
     s.ctx.restore(blob)
-    Jp = _objective(s, dts)
-    assert abs(J - Jp) <= 1e-13 * abs(Jp), (J, Jp)
+    Jp = _objective_plain(s, dts, obj)
+    assert abs(J - Jp) <= 1e-12 * abs(Jp), (J, Jp)
     # the context ends in the forward's final state
     assert np.array_equal(ua, s.ctx.get("u")) and np.array_equal(va, s.ctx.get("v"))
 
 
-@pytest.mark.parametrize("where", ["wake", "body", "edge", "inflow"])
-def test_gradient_matches_finite_differences(where):
+@pytest.mark.parametrize("where", list(BUMPS))
+def test_energy_gradient_matches_finite_differences(where):
     s = _developed()
     blob = s.ctx.checkpoint()
-    J, gu, gv, dts, _ = s.ctx.adjoint(NSTEPS, BOX, every=5)
+    J, gu, gv, gb, dts, _ = s.ctx.adjoint(NSTEPS, every=5, **ENERGY)
     s.ctx.restore(blob)
-    u0, v0 = s.ctx.get("u"), s.ctx.get("v")
-    cx, cy, sig = {"wake": (0.45, 0.27, 0.04), "body": (0.3, 0.31, 0.03),
-                   "edge": (0.97, 0.22, 0.05), "inflow": (0.05, 0.3, 0.05)}[where]
-    du, dv = _bump(s, cx, cy, sig, 0.7, -0.4)
+    du, dv = _bump(s.ctx, where)
     ad = float(np.sum(gu * du) + np.sum(gv * dv))
-    # central differences at 1e-6: the fade's and the obstacle terms' sign
-    # tests make the forward piecewise smooth, and a larger step crosses
-    # their switches (1e-4 does, at the edge and the inflow)
-    eps = 1e-6
-    Js = []
-    for sgn in (1, -1):
-        s.ctx.restore(blob)
-        s.ctx.set("u", u0 + sgn * eps * du)
-        s.ctx.set("v", v0 + sgn * eps * dv)
-        Js.append(s.ctx.adjoint(NSTEPS, BOX, dt=dts, gradient=False)[0])
-    fd = (Js[0] - Js[1]) / (2 * eps)
+    fd = _fd(s.ctx, blob, dts, ENERGY, du, dv)
     assert abs(fd) > 1e-8 * abs(J), (where, fd, J)
     assert abs(ad - fd) <= 2e-6 * abs(fd), (where, ad, fd)
+
+
+@pytest.mark.parametrize("where", ["body", "wake", "inflow"])
+def test_drag_gradient_matches_finite_differences(where):
+    s = _developed()
+    blob = s.ctx.checkpoint()
+    J, gu, gv, gb, dts, _ = s.ctx.adjoint(NSTEPS, every=5, **DRAG)
+    s.ctx.restore(blob)
+    du, dv = _bump(s.ctx, where)
+    ad = float(np.sum(gu * du) + np.sum(gv * dv))
+    fd = _fd(s.ctx, blob, dts, DRAG, du, dv)
+    assert abs(ad - fd) <= 1e-5 * max(abs(fd), 1e-3 * abs(J)), (where, ad, fd)
+
+
+@pytest.mark.parametrize("obj", [ENERGY, DRAG], ids=["energy", "drag"])
+def test_body_velocity_gradient_matches_finite_differences(obj):
+    s = _developed()
+    blob = s.ctx.checkpoint()
+    J, gu, gv, gb, dts, _ = s.ctx.adjoint(NSTEPS, every=5, **obj)
+    s.ctx.restore(blob)
+    # the y component is near zero (the flow is almost symmetric about the
+    # cylinder's axis): the differences' rounding, about 1e-16 |J| / EPS,
+    # bounds what they can resolve there
+    floor = 1e-13 * abs(J) / EPS
+    for comp in (0, 1):
+        d = (1.0, 0.0) if comp == 0 else (0.0, 1.0)
+        fd = _fd(s.ctx, blob, dts, obj, dub=d)
+        assert abs(gb[comp] - fd) <= 1e-5 * abs(fd) + floor, (comp, gb[comp], fd)
+    assert abs(gb[0]) > 1e3 * floor
+
+
+def test_gradient_matches_reference_finite_differences(ref):
+    """Central differences of the reference's own steps (the compiled
+    oracle), from the same state with the same dt schedule."""
+    s = _developed()
+    blob = s.ctx.checkpoint()
+    J, gu, gv, gb, dts, _ = s.ctx.adjoint(NSTEPS, every=5, **BOTH)
+    s.ctx.restore(blob)
+    u0, v0 = s.ctx.get("u"), s.ctx.get("v")
+    ub = s.ctx.shape(0)
+    du, dv = _bump(s.ctx, "body")
+    n = s.ctx
+    i0, i1 = int(np.floor(BOX[0] / n.h)), int(np.ceil(BOX[1] / n.h))
+    j0, j1 = int(np.floor(BOX[2] / n.h)), int(np.ceil(BOX[3] / n.h))
+
+    def ref_J(eu, eb):
+        r = ref.RefSim(FORCED)
+        r.set("u", u0 + eu * du)
+        r.set("v", v0 + eu * dv)
+        r.set_shape_velocity(0, ub["u"] + eb, ub["v"], ub["omega"])
+        Jr = 0.0
+        for dt in dts:
+            r.set_time(r.time, r.step_id, dt)
+            r.advance()
+            u, v = r.get("u")[j0:j1, i0:i1], r.get("v")[j0:j1, i0:i1]
+            st = r.shape(0)
+            Jr += (0.5 * n.h ** 2 * float(np.sum(u * u + v * v)) + BOTH["w_force"][0] * st["forcex"]
+                   + BOTH["w_force"][1] * st["forcey"])
+        r.close()
+        return Jr / len(dts)
+
+    J0 = ref_J(0.0, 0.0)
+    assert abs(J0 - J) <= 1e-9 * abs(J), (J0, J)
+    fd_u = (ref_J(EPS, 0.0) - ref_J(-EPS, 0.0)) / (2 * EPS)
+    ad_u = float(np.sum(gu * du) + np.sum(gv * dv))
+    assert abs(ad_u - fd_u) <= 1e-5 * abs(fd_u), (ad_u, fd_u)
+    fd_b = (ref_J(0.0, EPS) - ref_J(0.0, -EPS)) / (2 * EPS)
+    assert abs(gb[0] - fd_b) <= 1e-5 * abs(fd_b), (gb[0], fd_b)
 
 
 def test_checkpoint_interval_does_not_change_the_gradient():
     s = _developed()
     blob = s.ctx.checkpoint()
-    ref = s.ctx.adjoint(NSTEPS, BOX, every=NSTEPS)
+    ref = s.ctx.adjoint(NSTEPS, every=NSTEPS, **BOTH)
     scale = max(np.max(np.abs(ref[1])), np.max(np.abs(ref[2])))
     for every in (1, 3):
         s.ctx.restore(blob)
-        J, gu, gv, dts, _ = s.ctx.adjoint(NSTEPS, BOX, every=every, dt=ref[3])
+        J, gu, gv, gb, dts, _ = s.ctx.adjoint(NSTEPS, every=every, dt=ref[4], **BOTH)
         assert abs(J - ref[0]) <= 1e-13 * abs(ref[0])
         assert np.max(np.abs(gu - ref[1])) <= 1e-12 * scale
         assert np.max(np.abs(gv - ref[2])) <= 1e-12 * scale
+        assert np.allclose(gb, ref[3], rtol=1e-11, atol=0)
+
+
+def test_autograd_binding():
+    torch = pytest.importorskip("torch")
+    from adjoint_binding import objective
+    s = _developed()
+    blob = s.ctx.checkpoint()
+    J, gu, gv, gb, dts, _ = s.ctx.adjoint(NSTEPS, every=5, **BOTH)
+    s.ctx.restore(blob)
+    u0 = torch.from_numpy(s.ctx.get("u")).requires_grad_()
+    v0 = torch.from_numpy(s.ctx.get("v")).requires_grad_()
+    st = s.ctx.shape(0)
+    ub = torch.tensor([st["u"], st["v"]], dtype=torch.float64, requires_grad=True)
+    kw = dict(BOTH, dt=dts, every=5)
+    Jt = objective(s.ctx, blob, NSTEPS, u0, v0, ub, **kw)
+    Jt.backward()
+    assert abs(Jt.item() - J) <= 1e-13 * abs(J)
+    scale = np.max(np.abs(gu))
+    assert np.max(np.abs(u0.grad.numpy() - gu)) <= 1e-12 * scale
+    assert np.max(np.abs(v0.grad.numpy() - gv)) <= 1e-12 * scale
+    assert np.allclose(ub.grad.numpy(), gb, rtol=1e-11, atol=0)
+    # a small step against the gradient lowers the objective by about
+    # alpha |grad|^2
+    with torch.no_grad():
+        n2 = float((u0.grad ** 2).sum() + (v0.grad ** 2).sum() + (ub.grad ** 2).sum())
+        alpha = 1e-3 * abs(J) / n2
+        J2 = objective(s.ctx, blob, NSTEPS, u0 - alpha * u0.grad, v0 - alpha * v0.grad, ub - alpha * ub.grad, **kw)
+    assert J2.item() < J
+    assert abs((J - J2.item()) / (alpha * n2) - 1) < 1e-2
 
 
 @pytest.mark.parametrize("args", [
@@ -108,7 +232,8 @@ def test_checkpoint_interval_does_not_change_the_gradient():
     BASE + "-bpdx 8 -bpdy 4 -poissonType freespace -shapes 'disk radius=0.06 xpos=0.3 ypos=0.25 xvel=0.2'",
     BASE + "-bpdx 8 -bpdy 4 -poissonType freespace -shapes 'stefanfish L=0.18 T=1 xpos=0.4 ypos=0.25'",
     FORCED + " -iterativePenalization 1",
-], ids=["cosine_solver", "free_disk", "swimmer", "iterated"])
+    FORCED.replace("xvel=0.2", "xvel=0.2 tAccel=5"),
+], ids=["cosine_solver", "free_disk", "swimmer", "iterated", "accelerating"])
 def test_uncovered_configurations_refused(args):
     s = Simulation(args)
     s.init()
