@@ -503,6 +503,44 @@ def falling_measurement(local, rank, pg, warmup=3, steps=6):
     return out
 
 
+def adjoint_measurement(local, rank, pg, warm=50, nsteps=200, every=20):
+    """The discrete adjoint on the forced cylinder (512x256): the gradient of
+    the time-averaged drag force over 200 steps (checkpoints every 20) with
+    respect to the initial velocity and the body's velocity; its cost against
+    the same 200 steps as graph steps and as operator steps, and the body
+    velocity gradient against a central difference of the forward."""
+    name, argline = WORKLOADS["cylinder"]
+    sim = make_sim(argline, local, rank)
+    ctx = sim.ctx
+    ctx.advance(warm)
+    ctx.sync()
+    blob = ctx.checkpoint()
+    obj = dict(box=None, w_force=(1.0, 0.0))
+    ctx.adjoint(nsteps, every=every, **obj)             # warm-up (allocations, first launches)
+    ctx.restore(blob)
+    J, gu, gv, gb, dts, ms = ctx.adjoint(nsteps, every=every, **obj)
+    ctx.restore(blob)
+    graph_ms = ctx.time_step(nsteps)
+    eps, ub, Js = 1e-6, ctx.shape(0)["u"], []
+    for sgn in (1, -1):
+        ctx.restore(blob)
+        ctx.set_shape(0, {"u": ub + sgn * eps})
+        Js.append(ctx.adjoint(nsteps, dt=dts, gradient=False, **obj)[0])
+    fd = (Js[0] - Js[1]) / (2 * eps)
+    bwd = max_over_ranks(pg, ms[1])
+    out = {"workload": name, "steps": nsteps, "checkpoint_every": every, "warm_steps_before": warm,
+           "objective": "time-averaged forcex (ComputeForces) over the steps",
+           "J": J, "forward_graph_ms": graph_ms, "forward_operator_ms_with_checkpoints": ms[0],
+           "backward_ms": bwd, "adjoint_over_forward": bwd / graph_ms,
+           "adjoint_over_forward_operator": bwd / ms[0],
+           "fd_check": {"parameter": "body velocity u", "adjoint": float(gb[0]), "central_difference": fd,
+                        "eps": eps, "rel_err": abs(gb[0] - fd) / max(abs(fd), 1e-300)},
+           "timing": "CUDA events on the context's stream; backward = the recomputation from the "
+                     "checkpoints plus the transposed steps; forward = the same 200 steps as graph steps"}
+    del sim
+    return out
+
+
 def run_ours(args, world, rank, local, pg):
     import torch
     name, argline = WORKLOADS[args.workload]
@@ -588,6 +626,7 @@ def run_ours(args, world, rank, local, pg):
     falling = None
     if not args.no_large and not args.no_falling:
         falling = falling_measurement(local, rank, pg)
+    adjoint = None if args.no_adjoint else adjoint_measurement(local, rank, pg)
 
     line = None
     if rank == 0:
@@ -619,6 +658,7 @@ def run_ours(args, world, rank, local, pg):
             "poisson_vs_cufft": cufft,
             "fp32": fp32,
             "falling_cylinder_large": falling,
+            "adjoint": adjoint,
             "cpu_baseline": cpu,
         }
     return line
@@ -748,6 +788,7 @@ def main():
     ap.add_argument("--no-cufft", action="store_true", help="skip the cuFFT comparison")
     ap.add_argument("--no-falling", action="store_true",
                     help="skip the 4096x2048 case with the falling cylinder (variable density)")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
     if args.impl == "reference":
