@@ -17,8 +17,11 @@
 // linear in their input: the linearization is the active piece, with the
 // rank-one terms of their sign-selected corrections).  The backward step
 // applies the transposes in reverse order: Pen^T, then lambda_p = -(dt/2h)
-// G^T lambda, K^T = K (the free-space, periodic and cosine convolutions are
-// symmetric), F'^T, O'^T, (h/2dt) D^T added to lambda, A'^T.
+// G^T lambda, K^T = K, F'^T, O'^T, (h/2dt) D^T added to lambda, A'^T.  The
+// three solvers are symmetric: the free-space and periodic ones convolve
+// with an even kernel, and the cosine one is DCT-III . diag . DCT-II, where
+// the DCT-III is the DCT-II's transpose times a diagonal weight (its zero
+// term's) that commutes with the multiplier.
 //
 // The forward is stored as checkpoints (the context's own checkpoint blob,
 // kept in device memory) every `every` steps; the backward recomputes each
@@ -519,8 +522,6 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   if (!c.initialised) return adj_fail(ctx, CUP2D_ESTATE, "not initialised");
   if (c.cfg.iterative || c.varRho || c.cfg.implicit_penalization || c.cfg.precision != CUP2D_PREC_FP64)
     return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint covers the FP64 PressureSingle pipeline (explicit penalization)");
-  if (c.cfg.poisson != CUP2D_POISSON_FREESPACE)
-    return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint covers the free-space solver");
   if (c.nshapes != 1)
     return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint covers one body");
   const ShapeCfg& sf = c.hshapes[0].cfg;

@@ -972,19 +972,19 @@ k_dct_rows_fwd(const double* in, int Nx, int nrows, double* __restrict__ D, int 
   double2* tws = sm + rb * SL;
   double* Bx = reinterpret_cast<double*>(tws + Len<L>::TW);     // staged real row values
   __shared__ double sCorr;
-  fade_corr_cta(fa, &sCorr);
+  if (fa.enabled) fade_corr_cta(fa, &sCorr);
   load_twiddles<L, 16>(tws, tw, twLen);
   const int row0 = blockIdx.x * rb;
   const int nb = min(rb, nrows - row0);
   __syncthreads();
-  const double corr = sCorr;
-  const int bandX = (int)(fa.g.fadeLenX / fa.g.h) + 2;
-  const int bandY = (int)(fa.g.fadeLenY / fa.g.h) + 2;
+  const double corr = fa.enabled ? sCorr : 0.0;
+  const int bandX = fa.enabled ? (int)(fa.g.fadeLenX / fa.g.h) + 2 : 0;
+  const int bandY = fa.enabled ? (int)(fa.g.fadeLenY / fa.g.h) + 2 : 0;
   // faded row values, then the even extension y[j] = x[j] (j < n), x[2n-1-j]
   for (int idx = threadIdx.x; idx < nb * L; idx += blockDim.x) {
     const int r = idx / L, col = idx - r * L, row = row0 + r;
     double v = in[(size_t)row * Nx + col];
-    if (row < bandY || row >= fa.g.ny - bandY || col < bandX || col >= fa.g.nx - bandX) {
+    if (fa.enabled && (row < bandY || row >= fa.g.ny - bandY || col < bandX || col >= fa.g.nx - bandX)) {
       v = fade_cell(fa.g, col, row, v, corr);
       fa.writeback[(size_t)row * Nx + col] = v;
     }

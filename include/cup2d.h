@@ -315,8 +315,8 @@ int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes);
  *    differentiated (a frozen schedule);
  *  - ms (2 values, or null): device time of the forward (with its
  *    checkpoints) and of the backward (recomputation and transposed steps);
- *  - covered: FP64, the free-space solver, explicit penalization without
- *    the iterated or variable-density pipelines, one disk forced in x, y
+ *  - covered: FP64, any of the three solvers, explicit penalization
+ *    without the iterated or variable-density pipelines, one disk forced in x, y
  *    and angle and fixed on the grid for the whole run, past its tAccel
  *    ramp (its chi does not move and its velocity is held; the lab velocity
  *    is minus the body's); anything else CUP2D_ENOTSUP;
