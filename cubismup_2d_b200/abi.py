@@ -50,7 +50,8 @@ KERNELS = {"advdiff": 0, "rhs_div": 1, "pcorr": 2, "fft_rows_fwd": 3, "fft_cols"
 
 
 class AdjointObjective(ctypes.Structure):
-    _fields_ = [("box", ctypes.c_double * 4), ("w_energy", ctypes.c_double), ("w_force", ctypes.c_double * 2)]
+    _fields_ = [("box", ctypes.c_double * 4), ("w_energy", ctypes.c_double), ("w_force", ctypes.c_double * 2),
+                ("w_body", ctypes.c_double * 3)]
 
 
 class Config(ctypes.Structure):
@@ -409,12 +410,14 @@ class Context:
         self._ck(self.L.cup2d_checkpoint_save(self.h_, ptr, size))
         return out
 
-    def adjoint(self, nsteps, box=None, every=20, dt=None, gradient=True, w_energy=1.0, w_force=(0.0, 0.0)):
+    def adjoint(self, nsteps, box=None, every=20, dt=None, gradient=True, w_energy=1.0, w_force=(0.0, 0.0),
+                w_body=(0.0, 0.0, 0.0)):
         """The time-averaged objective over nsteps steps from the current state,
-        J = (1/nsteps) sum_n [w_energy (h^2/2) sum_box (u^2 + v^2) + w_force . force]
-        (box = (x0, x1, y0, y1) in domain units; force = ComputeForces'
-        (forcex, forcey) on the body), and its gradient with respect to the
-        current velocity and to the body's velocity by the discrete adjoint
+        J = (1/nsteps) sum_n [w_energy (h^2/2) sum_box (u^2 + v^2) + w_force . force
+        + w_body . (u_b, v_b, omega)] (box = (x0, x1, y0, y1) in domain units;
+        force = ComputeForces' (forcex, forcey) on the body), and its gradient
+        with respect to the current velocity and to the body's velocity (u_b,
+        v_b, omega: a forced body's held one, a free body's initial one) by the discrete adjoint
         (forward recomputed from checkpoints every ``every`` steps).  dt: the
         frozen step sizes (nsteps values) or None for calcMaxTimestep's.
         Returns (J, grad_u, grad_v, grad_body, dts, (forward_ms, backward_ms));
@@ -427,6 +430,8 @@ class Context:
                 obj.box[k] = float(box[k])
         obj.w_energy = float(w_energy) if box is not None else 0.0
         obj.w_force[0], obj.w_force[1] = float(w_force[0]), float(w_force[1])
+        for k in range(3):
+            obj.w_body[k] = float(w_body[k])
         dts = np.empty(nsteps, dtype=np.float64)
         dti = None if dt is None else np.ascontiguousarray(dt, dtype=np.float64)
         if dti is not None and dti.size != nsteps:
@@ -435,7 +440,7 @@ class Context:
         ms = np.zeros(2, dtype=np.float64)
         gu = np.empty((self.ny, self.nx), dtype=np.float64) if gradient else None
         gv = np.empty((self.ny, self.nx), dtype=np.float64) if gradient else None
-        gb = np.zeros(2, dtype=np.float64) if gradient else None
+        gb = np.zeros(3, dtype=np.float64) if gradient else None
         ptr = lambda a: None if a is None else a.ctypes.data_as(dp)  # noqa: E731
         self._ck(self.L.cup2d_adjoint_run(self.h_, nsteps, every, ctypes.byref(obj), ptr(dti), ptr(dts),
                                           ctypes.byref(J), ptr(gu), ptr(gv), ptr(gb), ptr(ms)))

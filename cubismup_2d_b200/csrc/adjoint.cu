@@ -34,6 +34,7 @@
 #include <string>
 #include <vector>
 #include "context.hpp"
+#include "rigid_body.cuh"
 
 namespace cup2d {
 
@@ -106,31 +107,75 @@ k_adj_div_T(GridDesc g, double facDiv, const double* __restrict__ lr, double* __
 }
 
 // Pen^T: lambda *= 1 - chi where the shape owns the cell (penalize's
-// alpha); gb += sum chi lambda, the derivative of u = (1 - chi) u + chi U_s
-// with respect to the body velocity U_s (its rotation and deformation parts
-// are not differentiated)
+// alpha); gb += the derivative of u = (1 - chi) u + chi U_s, U_s = (u_b -
+// omega p_y, v_b + omega p_x) about the centre of mass, with respect to the
+// body velocity (u_b, v_b, omega)
 __global__ void __launch_bounds__(1024)
 k_adj_pen(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
           double* lu, double* lv, double* gb)
 {
   const DevShape& S = sh[k];
-  double a[2] = {0, 0};
+  const double Cx = S.s.com[0], Cy = S.s.com[1];
+  double a[3] = {0, 0, 0};
   for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
     const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
     const size_t o = (size_t)s * BS2 + threadIdx.y * BS + threadIdx.x;
     const size_t c = (size_t)(by * BS + threadIdx.y) * g.nx + bx * BS + threadIdx.x;
     const double X = t.chi[o];
     if (chig[c] > X || X <= 0) continue;
+    const double p0 = cell_x(g, bx, threadIdx.x) - Cx, p1 = cell_y(g, by, threadIdx.y) - Cy;
     a[0] += X * lu[c];
     a[1] += X * lv[c];
+    a[2] += X * (p0 * lv[c] - p1 * lu[c]);
     lu[c] *= 1 - X;
     lv[c] *= 1 - X;
   }
-  for (int q = 0; q < 2; q++) {
+  for (int q = 0; q < 3; q++) {
     double v = a[q];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if ((threadIdx.x & 31) == 0 && v != 0) atomicAdd(&gb[q], v);
   }
+}
+
+// ---- a free body: Shape::updateVelocity's 3x3 solve (Shape.cpp:25-59) of
+// the momentum integrals (PressureSingle.cpp:23-67), transposed.  With chi
+// fixed the matrix (penalM, penalJ, penalDX, penalDY) is a constant and
+// symmetric: lb = A^-1 lx, by the forward's own LU.
+__global__ void k_adj_solve(const DevShape* sh, int k, const double* lx, double* lb)
+{
+  const cup2d_shape_state& s = sh[k].s;
+  double A[3][3] = {{s.penalM, 0, -s.penalDY}, {0, s.penalM, s.penalDX}, {-s.penalDY, s.penalDX, s.penalJ}};
+  const double b[3] = {lx[0], lx[1], lx[2]};
+  lu_solve3(A, b, lb);
+}
+
+// the momenta's transpose: (fluidMomX, fluidMomY, fluidAngMom) = sum F (u,
+// v, p_x v - p_y u), F = h^2 rho chi, over the tile cells with chi > 0, of
+// the pressure-corrected velocity: lambda += F (lb_0 - p_y lb_2, lb_1 + p_x lb_2)
+__global__ void __launch_bounds__(1024)
+k_adj_momenta(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ lb,
+              double* lu, double* lv)
+{
+  const DevShape& S = sh[k];
+  const double Cx = S.s.com[0], Cy = S.s.com[1];
+  const double l0 = lb[0], l1 = lb[1], l2 = lb[2];
+  for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
+    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+    const size_t o = (size_t)s * BS2 + threadIdx.y * BS + threadIdx.x;
+    const double chi = t.chi[o];
+    if (!(chi > 0)) continue;
+    const size_t c = (size_t)(by * BS + threadIdx.y) * g.nx + bx * BS + threadIdx.x;
+    const double p0 = cell_x(g, bx, threadIdx.x) - Cx, p1 = cell_y(g, by, threadIdx.y) - Cy;
+    const double F = g.h * g.h * S.rhoTile * chi;
+    lu[c] += F * (l0 - p1 * l2);
+    lv[c] += F * (l1 + p0 * l2);
+  }
+}
+
+// the objective's body-velocity weights of a step, added to lx
+__global__ void k_adj_add3(double* lx, double a, double b, double c)
+{
+  lx[0] += a; lx[1] += b; lx[2] += c;
 }
 
 // ---- the body's force (ComputeForces.cpp:16-111, the surface cells of
@@ -166,12 +211,13 @@ k_adj_force(GridDesc g, const DevShape* sh, int k, ObstTiles t, double wx, doubl
   }
 }
 
-// the objective's force term of a step: acc += wx forcex + wy forcey of
-// the state k_forces left
-__global__ void k_adj_force_sum(const DevShape* sh, int k, double wx, double wy, double* acc)
+// the objective's body terms of a step: acc += wx forcex + wy forcey + wb .
+// (u, v, omega) of the state the step left
+__global__ void k_adj_body_sum(const DevShape* sh, int k, double wx, double wy, double wb0, double wb1,
+                               double wb2, double* acc)
 {
   const cup2d_shape_state& s = sh[k].s;
-  *acc += wx * s.forcex + wy * s.forcey;
+  *acc += wx * s.forcex + wy * s.forcey + (wb0 * s.u + wb1 * s.v + wb2 * s.omega);
 }
 
 // ---- the obstacle RHS terms O (k_rhs_obst, k_rhs_corr) --------------------
@@ -527,19 +573,25 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   const ShapeCfg& sf = c.hshapes[0].cfg;
   if (sf.kind != CUP2D_SHAPE_DISK)
     return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint covers a disk (a swimmer's chi and udef move with its gait)");
-  if (!(sf.bForcedx && sf.bForcedy && sf.bBlockang && sf.bFixedx && sf.bFixedy))
-    return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint needs a body forced in x, y and angle and fixed on the grid "
-                                        "(its motion, and so chi, must not depend on the flow)");
+  // forced: the body velocity is held (a parameter); free: solved each step
+  // from the momentum integrals.  Either way fixed on the grid, so chi does
+  // not move.
+  const bool forced = sf.bForcedx && sf.bForcedy && sf.bBlockang;
+  const bool freeBody = !sf.bForcedx && !sf.bForcedy && !sf.bBlockang;
+  if (!(sf.bFixedx && sf.bFixedy) || !(forced || freeBody))
+    return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint needs a disk fixed on the grid (bFixed: chi does not move), "
+                                        "either forced in x, y and angle or free in all three");
   const GridDesc& g = c.g;
   {
     double t0, dtd, ux, uy; int st;
     ARC(cup2d_get_scalars(ctx, &t0, &dtd, &st, &ux, &uy));
-    if (sf.kind == CUP2D_SHAPE_DISK && sf.tAccel > 0 && t0 < sf.tAccel)
+    if (forced && sf.tAccel > 0 && t0 < sf.tAccel)
       return adj_fail(ctx, CUP2D_ENOTSUP, "the body is still accelerating (tAccel): its velocity is not held");
   }
   const size_t n = c.ncells(), nb = sizeof(double) * n;
   const bool energy = obj->w_energy != 0;
   const bool force = obj->w_force[0] != 0 || obj->w_force[1] != 0;
+  const bool bodyTerm = obj->w_body[0] != 0 || obj->w_body[1] != 0 || obj->w_body[2] != 0;
   ProbeBox bx{0, 0, 0, 0};
   if (energy) {
     bx.x0 = std::max(0, (int)std::floor(obj->box[0] / g.h)); bx.x1 = std::min(g.nx, (int)std::ceil(obj->box[1] / g.h));
@@ -548,6 +600,7 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   }
   const double wE = obj->w_energy * g.h * g.h / nsteps;   // the energy term's weight per step
   const double wFx = obj->w_force[0] / nsteps, wFy = obj->w_force[1] / nsteps;
+  const double wB[3] = {obj->w_body[0] / nsteps, obj->w_body[1] / nsteps, obj->w_body[2] / nsteps};
   const dim3 grid2(g.bpdx, g.bpdy), blk2(32, 8);
   const int probeGrid = energy ? std::min(1024, ((bx.x1 - bx.x0) * (bx.y1 - bx.y0) + 255) / 256) : 1;
 
@@ -559,7 +612,11 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   for (int s = 0; s <= nseg; s++)
     if (!(ck[s] = B.get<char>(ckBytes))) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint checkpoints");
   double* acc = B.get<double>(8);          // [0..4] reductions of a transposed stage
-  double* obv = B.get<double>(4);          // [0] J, [1..2] the body-velocity gradient
+  // [0] J; [1..3] the body-velocity gradient (forced: the held velocity's,
+  // accumulated over the steps; free: the adjoint of the step's output
+  // velocity); [4..6] a free body's adjoint of the previous output, formed
+  // by advDiff's lab velocity; [8..10] the solve's transpose
+  double* obv = B.get<double>(12);
   if (!acc || !obv) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint scratch");
   std::vector<double> dts(nsteps), U0s(nsteps), U1s(nsteps);
   struct Ev {
@@ -582,7 +639,7 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   };
 
   // forward: checkpoints, the dt schedule, J
-  ACK(cudaMemsetAsync(obv, 0, sizeof(double) * 4, c.stream));
+  ACK(cudaMemsetAsync(obv, 0, sizeof(double) * 12, c.stream));
   ACK(cudaEventRecord(e0, c.stream));
   for (int i = 0; i < nsteps; i++) {
     if (i % every == 0) ARC(cup2d_checkpoint_save(ctx, ck[i / every], ckBytes));
@@ -596,7 +653,8 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
     ARC(cup2d_get_scalars(ctx, &t_, &dtd, &st, &ux, &uy));
     U0s[i] = ux; U1s[i] = uy;
     if (energy) k_adj_probe<<<probeGrid, 256, 0, c.stream>>>(g, bx, c.u(), c.v(), wE, obv, nullptr, nullptr);
-    if (force) k_adj_force_sum<<<1, 1, 0, c.stream>>>(c.dshapes, 0, wFx, wFy, obv);
+    if (force || bodyTerm)
+      k_adj_body_sum<<<1, 1, 0, c.stream>>>(c.dshapes, 0, wFx, wFy, wB[0], wB[1], wB[2], obv);
     ACK(cudaGetLastError());
   }
   ACK(cudaEventRecord(e1, c.stream));
@@ -636,8 +694,11 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
     return adj_fail(ctx, CUP2D_ENOMEM, "adjoint segment buffers");
   ACK(cudaMemsetAsync(lu, 0, nb, c.stream));
   ACK(cudaMemsetAsync(lv, 0, nb, c.stream));
-  ACK(cudaMemsetAsync(obv + 1, 0, sizeof(double) * 2, c.stream));
+  ACK(cudaMemsetAsync(obv + 1, 0, sizeof(double) * 11, c.stream));
   ACK(cudaEventRecord(e2, c.stream));
+  double* lx = obv + 1;                      // the body-velocity adjoint (see above)
+  double* lxPrev = obv + 4;
+  double* lb = obv + 8;
   const AllTiles T0 = all_tiles(c);
   const int tctas = tile_ctas(c, c.tiles[0].capacity);
   for (int s = nseg - 1; s >= 0; s--) {
@@ -656,12 +717,19 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
     for (int i = i1 - 1; i >= i0; i--) {
       const size_t o = (size_t)(i - i0) * n;
       const double dt = dts[i];
-      // the objective's terms of u^(i+1), p^(i+1)
+      // the objective's terms of u^(i+1), p^(i+1) and the body velocity
       if (energy) k_adj_probe<<<probeGrid, 256, 0, c.stream>>>(g, bx, pu + o, pv + o, wE, nullptr, lu, lv);
       if (force)
         k_adj_force<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], wFx, wFy, 0, lu, lv, nullptr);
+      if (bodyTerm) k_adj_add3<<<1, 1, 0, c.stream>>>(lx, wB[0], wB[1], wB[2]);
       // penalization
-      k_adj_pen<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], c.chi, lu, lv, obv + 1);
+      k_adj_pen<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], c.chi, lu, lv, lx);
+      if (freeBody) {
+        // the body velocity of the step came from the momentum integrals of
+        // the pressure-corrected velocity
+        k_adj_solve<<<1, 1, 0, c.stream>>>(c.dshapes, 0, lx, lb);
+        k_adj_momenta<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], lb, lu, lv);
+      }
       // pressure correction: lambda_p, the force's pressure term, then the convolution
       k_adj_grad_T<<<grid2, blk2, 0, c.stream>>>(g, -0.5 * dt / g.h, lu, lv, l1);
       if (force)
@@ -688,17 +756,23 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
       // advDiff about u^i
       ACK(cudaMemsetAsync(acc, 0, sizeof(double) * 8, c.stream));
       k_adj_adv_gamma<<<std::min(148, (2 * (g.nx + g.ny) + 255) / 256), 256, 0, c.stream>>>(g, lu, lv, acc);
+      // (a free body: its previous velocity set the lab velocity of this
+      // step; a forced one: its held velocity, accumulated)
       k_adj_advdiff<<<grid2, blk2, 0, c.stream>>>(g, adv_coef_host(c, dt, U0s[i], U1s[i]), su + o, sv + o,
-                                                 lu, lv, acc, tu, tv, obv + 1);
+                                                 lu, lv, acc, tu, tv, freeBody ? lxPrev : lx);
       ACK(cudaGetLastError());
       std::swap(lu, tu);
       std::swap(lv, tv);
+      if (freeBody) {
+        ACK(cudaMemcpyAsync(lx, lxPrev, sizeof(double) * 3, cudaMemcpyDeviceToDevice, c.stream));
+        ACK(cudaMemsetAsync(lxPrev, 0, sizeof(double) * 3, c.stream));
+      }
     }
   }
   ACK(cudaEventRecord(e1, c.stream));
   if (grad_u) ACK(cudaMemcpyAsync(grad_u, lu, nb, cudaMemcpyDeviceToHost, c.stream));
   if (grad_v) ACK(cudaMemcpyAsync(grad_v, lv, nb, cudaMemcpyDeviceToHost, c.stream));
-  if (grad_body) ACK(cudaMemcpyAsync(grad_body, obv + 1, sizeof(double) * 2, cudaMemcpyDeviceToHost, c.stream));
+  if (grad_body) ACK(cudaMemcpyAsync(grad_body, lx, sizeof(double) * 3, cudaMemcpyDeviceToHost, c.stream));
   ACK(cudaStreamSynchronize(c.stream));
   float bms = 0;
   ACK(cudaEventElapsedTime(&bms, e2, e1));

@@ -301,13 +301,16 @@ int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes);
  * (PutObjectsOnGrid, advDiff, PressureSingle, ComputeForces) from the
  * current state and returns the time-averaged objective
  *   J = (1/nsteps) sum_{n=1..nsteps} [ w_energy (h^2/2) sum_box (u^2 + v^2)
- *                                      + w_force . (forcex, forcey) ]
- * of each step's final velocity and ComputeForces' force on the body
+ *                                      + w_force . (forcex, forcey)
+ *                                      + w_body . (u_b, v_b, omega) ]
+ * of each step's final velocity, ComputeForces' force on the body and the
+ * body's velocity
  * (box = {x0, x1, y0, y1} in domain units: the cells whose index ranges
  * [floor(x0/h), ceil(x1/h)) etc. cover), and, by the transposed steps, its
  * gradient with respect to the initial velocity (grad_u, grad_v: host
  * arrays of Nx*Ny, row-major, or null) and to the body's velocity
- * (grad_body: 2 values, or null), each step's operators linearized about
+ * (grad_body: 3 values, u_b, v_b, omega, or null: a forced body's held
+ * velocity, or a free body's initial one), each step's operators linearized about
  * its forward values and applied in reverse order, the forward recomputed
  * from device checkpoints taken every `every` steps.
  *  - dt_in: the step sizes (nsteps values), or null for calcMaxTimestep's;
@@ -316,16 +319,19 @@ int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes);
  *  - ms (2 values, or null): device time of the forward (with its
  *    checkpoints) and of the backward (recomputation and transposed steps);
  *  - covered: FP64, any of the three solvers, explicit penalization
- *    without the iterated or variable-density pipelines, one disk forced in x, y
- *    and angle and fixed on the grid for the whole run, past its tAccel
- *    ramp (its chi does not move and its velocity is held; the lab velocity
- *    is minus the body's); anything else CUP2D_ENOTSUP;
+ *    without the iterated or variable-density pipelines, one disk fixed on
+ *    the grid (bFixed: its chi does not move; the lab velocity is minus the
+ *    body's), either forced in x, y and angle for the whole run and past
+ *    its tAccel ramp (its velocity is held), or free in all three (its
+ *    velocity solved each step from the momentum integrals, Shape.cpp:25-59,
+ *    and differentiated through them); anything else CUP2D_ENOTSUP;
  *  - the context ends in the forward's final state (as after nsteps
  *    steps); synchronises. */
 typedef struct cup2d_adjoint_objective {
   double box[4];          /* the kinetic-energy probe: x0, x1, y0, y1      */
   double w_energy;        /* its weight (0: no energy term, box unused)    */
   double w_force[2];      /* weights of the body's forcex and forcey       */
+  double w_body[3];       /* weights of the body's velocity u, v, omega    */
 } cup2d_adjoint_objective;
 int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint_objective* obj,
                       const double* dt_in, double* dt_out, double* J, double* grad_u, double* grad_v,

@@ -1,6 +1,6 @@
 """A thin torch.autograd binding over cup2d_adjoint_run, for tests: the
 objective of nsteps steps from a saved state, as a function of the initial
-velocity (u0, v0) and of the forced body's velocity ub = (u, v), whose
+velocity (u0, v0) and of the body's velocity ub = (u, v, omega), whose
 backward returns the discrete adjoint's gradients.  Each call restores the
 checkpoint first, so repeated evaluations start from the same state."""
 import torch
@@ -12,7 +12,7 @@ class AdjointObjective(torch.autograd.Function):
         ctx.restore(blob)
         ctx.set("u", u0.detach().cpu().numpy())
         ctx.set("v", v0.detach().cpu().numpy())
-        ctx.set_shape(0, {"u": float(ub[0]), "v": float(ub[1])})
+        ctx.set_shape(0, {"u": float(ub[0]), "v": float(ub[1]), "omega": float(ub[2])})
         need = any(fctx.needs_input_grad[:3])
         J, gu, gv, gb, dts, _ = ctx.adjoint(nsteps, gradient=need, **kwargs)
         fctx.dts = dts

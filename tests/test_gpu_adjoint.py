@@ -19,6 +19,10 @@ pytestmark = pytest.mark.gpu
 BASE = "-extent 1 -CFL 0.1 -nu 1e-3 -lambda 1e4 -muteAll 1 "
 FORCED = (BASE + "-bpdx 8 -bpdy 4 -poissonType freespace "
           "-shapes 'disk radius=0.06 xpos=0.3 ypos=0.25 bForced=1 bFixed=1 xvel=0.2'")
+# a free disk held on the grid (bFixed: the frame follows it), started at
+# 0.2: its velocity comes from the momentum integrals every step
+FREE = (BASE + "-bpdx 8 -bpdy 4 -poissonType freespace "
+        "-shapes 'disk radius=0.06 xpos=0.3 ypos=0.25 bFixed=1 xvel=0.2'")
 BOX = (0.36, 0.62, 0.14, 0.36)
 NSTEPS = 16
 BUMPS = {"wake": (0.45, 0.27, 0.04), "body": (0.3, 0.31, 0.03),
@@ -30,6 +34,7 @@ EPS = 1e-6
 ENERGY = dict(box=BOX)
 DRAG = dict(box=None, w_force=(1.0, 0.0))
 BOTH = dict(box=BOX, w_energy=1.0, w_force=(1e-4, 2e-4))
+ALL = dict(box=BOX, w_energy=1.0, w_force=(1e-4, 2e-4), w_body=(1e-3, 2e-3, 1e-4))
 
 
 def _developed(args=FORCED, warm=40):
@@ -37,6 +42,22 @@ def _developed(args=FORCED, warm=40):
     s.init()
     for _ in range(warm):
         s.advance(s.calcMaxTimestep())
+    s.ctx.sync()
+    return s
+
+
+def _developed_free():
+    """The free disk in the developed flow of the forced one (its velocity,
+    -0.2, and the fields after the forced warm-up): a free body's state at
+    rest would leave the RHS near zero, where the obstacle terms' and the
+    fade's sign tests switch under any finite difference."""
+    f = _developed(FORCED)
+    u, v, st = f.ctx.get("u"), f.ctx.get("v"), f.ctx.shape(0)
+    s = Simulation(FREE)
+    s.init()
+    s.ctx.set("u", u)
+    s.ctx.set("v", v)
+    s.ctx.set_shape(0, {"u": st["u"], "v": st["v"], "omega": st["omega"]})
     s.ctx.sync()
     return s
 
@@ -62,7 +83,9 @@ def _fd(ctx, blob, dts, obj, du=None, dv=None, dub=None):
             ctx.set("u", u0 + sgn * EPS * du)
             ctx.set("v", v0 + sgn * EPS * dv)
         if dub is not None:
-            ctx.set_shape(0, {"u": ub["u"] + sgn * EPS * dub[0], "v": ub["v"] + sgn * EPS * dub[1]})
+            dub3 = tuple(dub) + (0.0,) * (3 - len(dub))
+            ctx.set_shape(0, {"u": ub["u"] + sgn * EPS * dub3[0], "v": ub["v"] + sgn * EPS * dub3[1],
+                              "omega": ub["omega"] + sgn * EPS * dub3[2]})
         Js.append(ctx.adjoint(NSTEPS, dt=dts, gradient=False, **obj)[0])
     ctx.restore(blob)
     return (Js[0] - Js[1]) / (2 * EPS)
@@ -155,17 +178,61 @@ def test_body_velocity_gradient_matches_finite_differences(obj):
     # cylinder's axis): the differences' rounding, about 1e-16 |J| / EPS,
     # bounds what they can resolve there
     floor = 1e-13 * abs(J) / EPS
-    for comp in (0, 1):
-        d = (1.0, 0.0) if comp == 0 else (0.0, 1.0)
+    for comp in (0, 1, 2):
+        d = [0.0, 0.0, 0.0]
+        d[comp] = 1.0
         fd = _fd(s.ctx, blob, dts, obj, dub=d)
         assert abs(gb[comp] - fd) <= 1e-5 * abs(fd) + floor, (comp, gb[comp], fd)
     assert abs(gb[0]) > 1e3 * floor
 
 
-def test_gradient_matches_reference_finite_differences(ref):
+@pytest.mark.parametrize("where", ["body", "wake", "edge"])
+def test_free_body_gradient_matches_finite_differences(where):
+    """A free disk: the momentum integrals, the 3x3 solve and the body
+    velocity's role as the next step's lab velocity, transposed."""
+    s = _developed_free()
+    blob = s.ctx.checkpoint()
+    J, gu, gv, gb, dts, _ = s.ctx.adjoint(NSTEPS, every=5, **ALL)
+    s.ctx.restore(blob)
+    du, dv = _bump(s.ctx, where)
+    ad = float(np.sum(gu * du) + np.sum(gv * dv))
+    fd = _fd(s.ctx, blob, dts, ALL, du, dv)
+    assert abs(ad - fd) <= 1e-5 * abs(fd), (where, ad, fd)
+    if where == "body":
+        # the initial body velocity sets the first step's lab velocity only
+        floor = 1e-13 * abs(J) / EPS
+        for comp in (0, 1):
+            d = [0.0, 0.0, 0.0]
+            d[comp] = 1.0
+            fd = _fd(s.ctx, blob, dts, ALL, dub=d)
+            assert abs(gb[comp] - fd) <= 1e-5 * abs(fd) + floor, (comp, gb[comp], fd)
+        assert gb[2] == 0.0
+
+
+def test_free_body_objective_matches_plain_steps():
+    s = _developed_free()
+    blob = s.ctx.checkpoint()
+    J, gu, gv, gb, dts, _ = s.ctx.adjoint(NSTEPS, every=5, **ALL)
+    s.ctx.restore(blob)
+    n = s.ctx
+    Jp = 0.0
+    i0, i1 = int(np.floor(BOX[0] / n.h)), int(np.ceil(BOX[1] / n.h))
+    j0, j1 = int(np.floor(BOX[2] / n.h)), int(np.ceil(BOX[3] / n.h))
+    for dt in dts:
+        s.advance(dt)
+        u, v = n.get("u")[j0:j1, i0:i1], n.get("v")[j0:j1, i0:i1]
+        st = n.shape(0)
+        Jp += (0.5 * n.h ** 2 * float(np.sum(u * u + v * v)) + 1e-4 * st["forcex"] + 2e-4 * st["forcey"]
+               + 1e-3 * st["u"] + 2e-3 * st["v"] + 1e-4 * st["omega"])
+    Jp /= len(dts)
+    assert abs(J - Jp) <= 1e-12 * abs(Jp), (J, Jp)
+
+
+@pytest.mark.parametrize("args", [FORCED, FREE], ids=["forced", "free"])
+def test_gradient_matches_reference_finite_differences(ref, args):
     """Central differences of the reference's own steps (the compiled
     oracle), from the same state with the same dt schedule."""
-    s = _developed()
+    s = _developed() if args == FORCED else _developed_free()
     blob = s.ctx.checkpoint()
     J, gu, gv, gb, dts, _ = s.ctx.adjoint(NSTEPS, every=5, **BOTH)
     s.ctx.restore(blob)
@@ -177,7 +244,7 @@ def test_gradient_matches_reference_finite_differences(ref):
     j0, j1 = int(np.floor(BOX[2] / n.h)), int(np.ceil(BOX[3] / n.h))
 
     def ref_J(eu, eb):
-        r = ref.RefSim(FORCED)
+        r = ref.RefSim(args)
         r.set("u", u0 + eu * du)
         r.set("v", v0 + eu * dv)
         r.set_shape_velocity(0, ub["u"] + eb, ub["v"], ub["omega"])
@@ -225,7 +292,7 @@ def test_autograd_binding():
     u0 = torch.from_numpy(s.ctx.get("u")).requires_grad_()
     v0 = torch.from_numpy(s.ctx.get("v")).requires_grad_()
     st = s.ctx.shape(0)
-    ub = torch.tensor([st["u"], st["v"]], dtype=torch.float64, requires_grad=True)
+    ub = torch.tensor([st["u"], st["v"], st["omega"]], dtype=torch.float64, requires_grad=True)
     kw = dict(BOTH, dt=dts, every=5)
     Jt = objective(s.ctx, blob, NSTEPS, u0, v0, ub, **kw)
     Jt.backward()
@@ -247,10 +314,12 @@ def test_autograd_binding():
 @pytest.mark.parametrize("args", [
     FORCED + " -precision fp32",
     BASE + "-bpdx 8 -bpdy 4 -poissonType freespace -shapes 'disk radius=0.06 xpos=0.3 ypos=0.25 xvel=0.2'",
+    BASE + "-bpdx 8 -bpdy 4 -poissonType freespace "
+    "-shapes 'disk radius=0.06 xpos=0.3 ypos=0.25 bFixed=1 bForcedx=1 xvel=0.2'",
     BASE + "-bpdx 8 -bpdy 4 -poissonType freespace -shapes 'stefanfish L=0.18 T=1 xpos=0.4 ypos=0.25'",
     FORCED + " -iterativePenalization 1",
     FORCED.replace("xvel=0.2", "xvel=0.2 tAccel=5"),
-], ids=["fp32", "free_disk", "swimmer", "iterated", "accelerating"])
+], ids=["fp32", "moving_disk", "half_forced", "swimmer", "iterated", "accelerating"])
 def test_uncovered_configurations_refused(args):
     s = Simulation(args)
     s.init()
