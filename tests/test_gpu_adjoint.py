@@ -265,7 +265,10 @@ def test_gradient_matches_reference_finite_differences(ref, args):
     ad_u = float(np.sum(gu * du) + np.sum(gv * dv))
     assert abs(ad_u - fd_u) <= 1e-5 * abs(fd_u), (ad_u, fd_u)
     fd_b = (ref_J(0.0, EPS) - ref_J(0.0, -EPS)) / (2 * EPS)
-    assert abs(gb[0] - fd_b) <= 1e-5 * abs(fd_b), (gb[0], fd_b)
+    # a free body's initial velocity sets only the first step's lab
+    # velocity: a small derivative, resolved down to the differences of the
+    # two codes' summation orders (about 1e-12 |J| per evaluation)
+    assert abs(gb[0] - fd_b) <= 1e-5 * abs(fd_b) + 1e-12 * abs(J) / EPS, (gb[0], fd_b)
 
 
 def test_checkpoint_interval_does_not_change_the_gradient():
