@@ -536,7 +536,7 @@ def adjoint_measurement(local, rank, pg, warm=50, nsteps=200, every=20):
            "fd_check": {"parameter": "body velocity u", "adjoint": float(gb[0]), "central_difference": fd,
                         "eps": eps, "rel_err": abs(gb[0] - fd) / max(abs(fd), 1e-300)},
            "timing": "CUDA events on the context's stream; backward = the recomputation from the "
-                     "checkpoints plus the transposed steps; forward = the same 200 steps as graph steps"}
+                     f"checkpoints plus the transposed steps; forward = the same {nsteps} steps as graph steps"}
     del sim
     return out
 
@@ -789,8 +789,20 @@ def main():
     ap.add_argument("--no-falling", action="store_true",
                     help="skip the 4096x2048 case with the falling cylinder (variable density)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint measurement")
+    ap.add_argument("--adjoint-only", type=int, default=0, metavar="N",
+                    help="run only the adjoint measurement, over N steps in one checkpoint segment")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup()
+    if args.adjoint_only > 0:
+        import torch
+        torch.cuda.set_device(local)
+        out = adjoint_measurement(local, rank, pg, nsteps=args.adjoint_only, every=args.adjoint_only)
+        if rank == 0:
+            print(json.dumps(out))
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
     if args.impl == "reference":
         # a step of the reference at 1024x512 takes ~0.1 s on 16 host cores:
         # bound the sample to 20 timed steps (same warm-up as our arm)

@@ -264,12 +264,11 @@ k_adj_obst_sums(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double
   }
 }
 
-// lT = O'^T lo over the processed cells (other cells: lT = lo, copied by the
-// caller beforehand)
+// l = O'^T l in place over the processed cells (each reads and writes its
+// own cell; the others pass unchanged)
 __global__ void __launch_bounds__(1024)
 k_adj_obst_apply(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
-                 const double* __restrict__ T, const double* __restrict__ lo, const double* __restrict__ acc,
-                 double* __restrict__ lT)
+                 const double* __restrict__ T, double* lo, const double* __restrict__ acc)
 {
   const DevShape& S = sh[k];
   const double s = acc[0], pos = acc[1], neg = acc[2], Lp = acc[3], Ln = acc[4];
@@ -291,7 +290,7 @@ k_adj_obst_apply(GridDesc g, const DevShape* sh, int k, ObstTiles t, const doubl
       const double dcorr = (-X + (neg > EPSd && q ? corr * a : 0.0)) / negF;
       r = a * (q ? 1 + corr : 1.0) * lo[c] + dcorr * Ln;
     }
-    lT[c] = r;
+    lo[c] = r;
   }
 }
 
@@ -332,11 +331,12 @@ k_adj_fade_sums(GridDesc g, const double* __restrict__ f, const double* __restri
   }
 }
 
-// lf = F'^T lb
+// lb = F'^T lb
 __global__ void __launch_bounds__(256)
-k_adj_fade_apply(GridDesc g, const double* __restrict__ f, const double* __restrict__ lb,
-                 const double* __restrict__ acc, double* __restrict__ lf)
+k_adj_fade_apply(GridDesc g, const double* __restrict__ f, double* lb, const double* __restrict__ acc)
 {
+  // in place; outside the strip blocks w2 = 0 and lambda passes unchanged
+  if (!fade_touch(g, blockIdx.x, blockIdx.y)) return;
   const double S = acc[0], Sp = acc[1], Sn = acc[2], Lp = acc[3], Ln = acc[4];
   const double SpF = fmax(Sp, EPSd), SnF = fmax(Sn, EPSd);
   const double corr = S > 0 ? S / SpF : S / SnF;
@@ -344,7 +344,7 @@ k_adj_fade_apply(GridDesc g, const double* __restrict__ f, const double* __restr
   for (int r = 0; r < 4; r++) {
     const int gy = blockIdx.y * BS + threadIdx.y + 8 * r;
     const size_t c = (size_t)gy * g.nx + gx;
-    const double w2 = fade_touch(g, blockIdx.x, blockIdx.y) ? fade_w2(g, gx, gy) : 0.0;
+    const double w2 = fade_w2(g, gx, gy);
     const double fw = f[c] * w2;
     double r_;
     if (S > 0) {
@@ -356,7 +356,7 @@ k_adj_fade_apply(GridDesc g, const double* __restrict__ f, const double* __restr
       const double dcorr = (w2 + (Sn > EPSd && N ? corr * w2 : 0.0)) / SnF;
       r_ = (1 - w2) * lb[c] - (N ? corr * w2 * lb[c] : 0.0) - dcorr * Ln;
     }
-    lf[c] = r_;
+    lb[c] = r_;
   }
 }
 
@@ -687,10 +687,9 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   double* lv = B.get<double>(n);
   double* l1 = B.get<double>(n);
   double* l2 = B.get<double>(n);
-  double* l3 = B.get<double>(n);
   double* tu = B.get<double>(n);
   double* tv = B.get<double>(n);
-  if (!su || !sv || !sT || !sF || !pu || !pv || !lu || !lv || !l1 || !l2 || !l3 || !tu || !tv)
+  if (!su || !sv || !sT || !sF || !pu || !pv || !lu || !lv || !l1 || !l2 || !tu || !tv)
     return adj_fail(ctx, CUP2D_ENOMEM, "adjoint segment buffers");
   ACK(cudaMemsetAsync(lu, 0, nb, c.stream));
   ACK(cudaMemsetAsync(lv, 0, nb, c.stream));
@@ -742,17 +741,16 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
         poisson_solve(c);
         c.rhs = R; c.pres = P; c.solveNoFade = false;
       }
-      // the fade: l2 -> l3
+      // the fade, then the obstacle terms, both in place on l2 (over the
+      // strip blocks and the shape's tiles)
       ACK(cudaMemsetAsync(acc, 0, sizeof(double) * 8, c.stream));
       k_adj_fade_sums<<<grid2, blk2, 0, c.stream>>>(g, sF + o, l2, acc);
-      k_adj_fade_apply<<<grid2, blk2, 0, c.stream>>>(g, sF + o, l2, acc, l3);
-      // the obstacle terms: l3 -> l1 (cells outside the shape's tiles pass)
-      ACK(cudaMemcpyAsync(l1, l3, nb, cudaMemcpyDeviceToDevice, c.stream));
+      k_adj_fade_apply<<<grid2, blk2, 0, c.stream>>>(g, sF + o, l2, acc);
       ACK(cudaMemsetAsync(acc, 0, sizeof(double) * 8, c.stream));
-      k_adj_obst_sums<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], c.chi, sT + o, l3, acc);
-      k_adj_obst_apply<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], c.chi, sT + o, l3, acc, l1);
+      k_adj_obst_sums<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], c.chi, sT + o, l2, acc);
+      k_adj_obst_apply<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], c.chi, sT + o, l2, acc);
       // the divergence, added to lambda of u1
-      k_adj_div_T<<<grid2, blk2, 0, c.stream>>>(g, 0.5 * g.h / dt, l1, lu, lv);
+      k_adj_div_T<<<grid2, blk2, 0, c.stream>>>(g, 0.5 * g.h / dt, l2, lu, lv);
       // advDiff about u^i
       ACK(cudaMemsetAsync(acc, 0, sizeof(double) * 8, c.stream));
       k_adj_adv_gamma<<<std::min(148, (2 * (g.nx + g.ny) + 255) / 256), 256, 0, c.stream>>>(g, lu, lv, acc);

@@ -271,6 +271,31 @@ def test_gradient_matches_reference_finite_differences(ref, args):
     assert abs(gb[0] - fd_b) <= 1e-5 * abs(fd_b) + 1e-12 * abs(J) / EPS, (gb[0], fd_b)
 
 
+def test_benchmark_cylinder_gradient():
+    """The benchmark's forced cylinder (512x256, Re=100): the drag's
+    body-velocity gradient over 200 steps, checkpoints every 20, against a
+    central difference, and its cost against the same steps as graph steps."""
+    args = ("-bpdx 16 -bpdy 8 -extent 1 -CFL 0.1 -nu 1.5e-4 -lambda 1e4 -poissonType freespace -muteAll 1 "
+            "-shapes 'disk radius=0.0375 xpos=0.2 ypos=0.25 bForced=1 bFixed=1 xvel=0.2'")
+    s = Simulation(args)
+    s.init()
+    s.ctx.advance(50)
+    s.ctx.sync()
+    blob = s.ctx.checkpoint()
+    J, gu, gv, gb, dts, ms = s.ctx.adjoint(200, every=20, **DRAG)
+    s.ctx.restore(blob)
+    graph_ms = s.ctx.time_step(200)
+    eps, ub = 1e-6, s.ctx.shape(0)["u"]
+    Js = []
+    for sgn in (1, -1):
+        s.ctx.restore(blob)
+        s.ctx.set_shape(0, {"u": ub + sgn * eps})
+        Js.append(s.ctx.adjoint(200, dt=dts, gradient=False, **DRAG)[0])
+    fd = (Js[0] - Js[1]) / (2 * eps)
+    assert abs(gb[0] - fd) <= 1e-4 * abs(fd), (gb[0], fd)
+    assert ms[1] < 6 * graph_ms, (ms, graph_ms)
+
+
 def test_checkpoint_interval_does_not_change_the_gradient():
     s = _developed()
     blob = s.ctx.checkpoint()
