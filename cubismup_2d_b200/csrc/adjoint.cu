@@ -571,16 +571,18 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   if (c.nshapes != 1)
     return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint covers one body");
   const ShapeCfg& sf = c.hshapes[0].cfg;
-  if (sf.kind != CUP2D_SHAPE_DISK)
-    return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint covers a disk (a swimmer's chi and udef move with its gait)");
   // forced: the body velocity is held (a parameter); free: solved each step
-  // from the momentum integrals.  Either way fixed on the grid, so chi does
-  // not move.
+  // from the momentum integrals.  Either way fixed on the grid: a disk's chi
+  // does not move, a swimmer's moves with its gait alone (the recomputation
+  // keeps each step's obstacle tiles).
   const bool forced = sf.bForcedx && sf.bForcedy && sf.bBlockang;
   const bool freeBody = !sf.bForcedx && !sf.bForcedy && !sf.bBlockang;
   if (!(sf.bFixedx && sf.bFixedy) || !(forced || freeBody))
-    return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint needs a disk fixed on the grid (bFixed: chi does not move), "
+    return adj_fail(ctx, CUP2D_ENOTSUP, "the adjoint needs a body fixed on the grid (bFixed), "
                                         "either forced in x, y and angle or free in all three");
+  if (sf.kind != CUP2D_SHAPE_DISK && (!forced || sf.pid || sf.pidpos))
+    return adj_fail(ctx, CUP2D_ENOTSUP, "a swimmer must be tethered (forced in x, y and angle, no PID "
+                                        "controller): a free swimmer's rotation moves its chi with the flow");
   const GridDesc& g = c.g;
   {
     double t0, dtd, ux, uy; int st;
@@ -691,6 +693,26 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   double* tv = B.get<double>(n);
   if (!su || !sv || !sT || !sF || !pu || !pv || !lu || !lv || !l1 || !l2 || !tu || !tv)
     return adj_fail(ctx, CUP2D_ENOMEM, "adjoint segment buffers");
+  // each recomputed step's obstacle state: the shape (tile count, centre of
+  // mass, momenta), its tiles and the grid's chi
+  const ObstTiles live = c.tiles[0];
+  const int cap = live.capacity;
+  const size_t tb = (size_t)cap * BS2;
+  DevShape* shSnap = B.get<DevShape>(segN);
+  int* tlSnap = B.get<int>((size_t)cap * segN);
+  double* tSnap[6];
+  for (int q = 0; q < 6; q++) tSnap[q] = B.get<double>(tb * segN);   // chi, udx, udy, sD, sdx, sdy
+  double* chiSnap = B.get<double>(n * segN);
+  if (!shSnap || !tlSnap || !chiSnap) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint obstacle snapshots");
+  for (double* q : tSnap) if (!q) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint obstacle snapshots");
+  auto tilesAt = [&](int j) {
+    ObstTiles t = live;
+    t.tiles = tlSnap + (size_t)j * cap;
+    t.chi = tSnap[0] + j * tb; t.udx = tSnap[1] + j * tb; t.udy = tSnap[2] + j * tb;
+    t.sD = tSnap[3] + j * tb; t.sdx = tSnap[4] + j * tb; t.sdy = tSnap[5] + j * tb;
+    t.dist = nullptr; t.slot = nullptr;
+    return t;
+  };
   ACK(cudaMemsetAsync(lu, 0, nb, c.stream));
   ACK(cudaMemsetAsync(lv, 0, nb, c.stream));
   ACK(cudaMemsetAsync(obv + 1, 0, sizeof(double) * 11, c.stream));
@@ -698,8 +720,7 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   double* lx = obv + 1;                      // the body-velocity adjoint (see above)
   double* lxPrev = obv + 4;
   double* lb = obv + 8;
-  const AllTiles T0 = all_tiles(c);
-  const int tctas = tile_ctas(c, c.tiles[0].capacity);
+  const int tctas = tile_ctas(c, cap);
   for (int s = nseg - 1; s >= 0; s--) {
     const int i0 = s * every, i1 = std::min(nsteps, i0 + every);
     ARC(cup2d_checkpoint_load(ctx, ck[s], ckBytes));
@@ -708,6 +729,17 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
       ACK(cudaMemcpyAsync(su + o, c.u(), nb, cudaMemcpyDeviceToDevice, c.stream));
       ACK(cudaMemcpyAsync(sv + o, c.v(), nb, cudaMemcpyDeviceToDevice, c.stream));
       ARC(step(dts[i], sT + o, sF + o));
+      {
+        const int j = i - i0;
+        const ObstTiles t = tilesAt(j);
+        ACK(cudaMemcpyAsync(shSnap + j, c.dshapes, sizeof(DevShape), cudaMemcpyDeviceToDevice, c.stream));
+        ACK(cudaMemcpyAsync(t.tiles, live.tiles, sizeof(int) * cap, cudaMemcpyDeviceToDevice, c.stream));
+        const double* src[6] = {live.chi, live.udx, live.udy, live.sD, live.sdx, live.sdy};
+        double* dst[6] = {t.chi, t.udx, t.udy, t.sD, t.sdx, t.sdy};
+        for (int q = 0; q < 6; q++)
+          ACK(cudaMemcpyAsync(dst[q], src[q], sizeof(double) * tb, cudaMemcpyDeviceToDevice, c.stream));
+        ACK(cudaMemcpyAsync(chiSnap + o, c.chi, nb, cudaMemcpyDeviceToDevice, c.stream));
+      }
       if (energy) {
         ACK(cudaMemcpyAsync(pu + o, c.u(), nb, cudaMemcpyDeviceToDevice, c.stream));
         ACK(cudaMemcpyAsync(pv + o, c.v(), nb, cudaMemcpyDeviceToDevice, c.stream));
@@ -716,23 +748,26 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
     for (int i = i1 - 1; i >= i0; i--) {
       const size_t o = (size_t)(i - i0) * n;
       const double dt = dts[i];
+      const DevShape* shI = shSnap + (i - i0);          // the step's obstacle state
+      const ObstTiles tI = tilesAt(i - i0);
+      const double* chiI = chiSnap + o;
       // the objective's terms of u^(i+1), p^(i+1) and the body velocity
       if (energy) k_adj_probe<<<probeGrid, 256, 0, c.stream>>>(g, bx, pu + o, pv + o, wE, nullptr, lu, lv);
       if (force)
-        k_adj_force<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], wFx, wFy, 0, lu, lv, nullptr);
+        k_adj_force<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, wFx, wFy, 0, lu, lv, nullptr);
       if (bodyTerm) k_adj_add3<<<1, 1, 0, c.stream>>>(lx, wB[0], wB[1], wB[2]);
       // penalization
-      k_adj_pen<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], c.chi, lu, lv, lx);
+      k_adj_pen<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, chiI, lu, lv, lx);
       if (freeBody) {
         // the body velocity of the step came from the momentum integrals of
         // the pressure-corrected velocity
-        k_adj_solve<<<1, 1, 0, c.stream>>>(c.dshapes, 0, lx, lb);
-        k_adj_momenta<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], lb, lu, lv);
+        k_adj_solve<<<1, 1, 0, c.stream>>>(shI, 0, lx, lb);
+        k_adj_momenta<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, lb, lu, lv);
       }
       // pressure correction: lambda_p, the force's pressure term, then the convolution
       k_adj_grad_T<<<grid2, blk2, 0, c.stream>>>(g, -0.5 * dt / g.h, lu, lv, l1);
       if (force)
-        k_adj_force<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], wFx, wFy, 1, nullptr, nullptr, l1);
+        k_adj_force<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, wFx, wFy, 1, nullptr, nullptr, l1);
       ACK(cudaGetLastError());
       {
         double* const R = c.rhs;
@@ -747,8 +782,8 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
       k_adj_fade_sums<<<grid2, blk2, 0, c.stream>>>(g, sF + o, l2, acc);
       k_adj_fade_apply<<<grid2, blk2, 0, c.stream>>>(g, sF + o, l2, acc);
       ACK(cudaMemsetAsync(acc, 0, sizeof(double) * 8, c.stream));
-      k_adj_obst_sums<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], c.chi, sT + o, l2, acc);
-      k_adj_obst_apply<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, T0.t[0], c.chi, sT + o, l2, acc);
+      k_adj_obst_sums<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, chiI, sT + o, l2, acc);
+      k_adj_obst_apply<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, chiI, sT + o, l2, acc);
       // the divergence, added to lambda of u1
       k_adj_div_T<<<grid2, blk2, 0, c.stream>>>(g, 0.5 * g.h / dt, l2, lu, lv);
       // advDiff about u^i

@@ -23,6 +23,10 @@ FORCED = (BASE + "-bpdx 8 -bpdy 4 -poissonType freespace "
 # 0.2: its velocity comes from the momentum integrals every step
 FREE = (BASE + "-bpdx 8 -bpdy 4 -poissonType freespace "
         "-shapes 'disk radius=0.06 xpos=0.3 ypos=0.25 bFixed=1 xvel=0.2'")
+# a tethered swimmer: StefanFish held on the grid (forced, fixed) in a 0.2
+# stream; its chi and udef move with its gait alone
+TETHERED = (BASE.replace("-nu 1e-3", "-nu 1e-4") + "-bpdx 8 -bpdy 4 -poissonType freespace "
+            "-shapes 'stefanfish L=0.18 T=1 xpos=0.35 ypos=0.25 bFixed=1 bForced=1 xvel=0.2'")
 BOX = (0.36, 0.62, 0.14, 0.36)
 NSTEPS = 16
 BUMPS = {"wake": (0.45, 0.27, 0.04), "body": (0.3, 0.31, 0.03),
@@ -209,6 +213,23 @@ def test_free_body_gradient_matches_finite_differences(where):
         assert gb[2] == 0.0
 
 
+@pytest.mark.parametrize("obj", [ENERGY, DRAG], ids=["energy", "drag"])
+def test_tethered_swimmer_gradient_matches_finite_differences(obj):
+    """A deforming body: each transposed step uses the obstacle tiles its
+    forward step placed (kept by the recomputation)."""
+    s = _developed(TETHERED, warm=60)
+    blob = s.ctx.checkpoint()
+    J, gu, gv, gb, dts, _ = s.ctx.adjoint(NSTEPS, every=5, **obj)
+    s.ctx.restore(blob)
+    for where in ("body", "wake"):
+        du, dv = _bump(s.ctx, where)
+        ad = float(np.sum(gu * du) + np.sum(gv * dv))
+        fd = _fd(s.ctx, blob, dts, obj, du, dv)
+        assert abs(ad - fd) <= 1e-5 * abs(fd), (where, ad, fd)
+    fd = _fd(s.ctx, blob, dts, obj, dub=(1.0, 0.0, 0.0))
+    assert abs(gb[0] - fd) <= 1e-5 * abs(fd), (gb[0], fd)
+
+
 def test_free_body_objective_matches_plain_steps():
     s = _developed_free()
     blob = s.ctx.checkpoint()
@@ -345,9 +366,11 @@ def test_autograd_binding():
     BASE + "-bpdx 8 -bpdy 4 -poissonType freespace "
     "-shapes 'disk radius=0.06 xpos=0.3 ypos=0.25 bFixed=1 bForcedx=1 xvel=0.2'",
     BASE + "-bpdx 8 -bpdy 4 -poissonType freespace -shapes 'stefanfish L=0.18 T=1 xpos=0.4 ypos=0.25'",
+    BASE + "-bpdx 8 -bpdy 4 -poissonType freespace "
+    "-shapes 'stefanfish L=0.18 T=1 xpos=0.4 ypos=0.25 bFixed=1 bForced=1 pid=1'",
     FORCED + " -iterativePenalization 1",
     FORCED.replace("xvel=0.2", "xvel=0.2 tAccel=5"),
-], ids=["fp32", "moving_disk", "half_forced", "swimmer", "iterated", "accelerating"])
+], ids=["fp32", "moving_disk", "half_forced", "free_swimmer", "pid_swimmer", "iterated", "accelerating"])
 def test_uncovered_configurations_refused(args):
     s = Simulation(args)
     s.init()
