@@ -41,7 +41,7 @@ EXPORTS = [
     "cup2d_ensemble_create", "cup2d_ensemble_advance", "cup2d_ensemble_advance_timed",
     "cup2d_ensemble_sync", "cup2d_ensemble_get_shapes", "cup2d_ensemble_last_error",
     "cup2d_ensemble_destroy",
-    "cup2d_fish_act", "cup2d_fish_period", "cup2d_fish_state", "cup2d_dump", "cup2d_poisson_solve",
+    "cup2d_fish_gait_get", "cup2d_fish_gait_set", "cup2d_fish_act", "cup2d_fish_period", "cup2d_fish_state", "cup2d_dump", "cup2d_poisson_solve",
     "cup2d_tuning_get",
     "cup2d_adv_diff_noalloc",
 ]
@@ -135,7 +135,9 @@ def lib():
     L.cup2d_checkpoint_size.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
     L.cup2d_checkpoint_save.argtypes = [vp, vp, ctypes.c_size_t]
     L.cup2d_checkpoint_load.argtypes = [vp, vp, ctypes.c_size_t]
-    L.cup2d_adjoint_run.argtypes = [vp, i, i, ctypes.POINTER(AdjointObjective), dp, dp, dp, dp, dp, dp, dp]
+    L.cup2d_adjoint_run.argtypes = [vp, i, i, ctypes.POINTER(AdjointObjective), dp, dp, dp, dp, dp, dp, dp, dp]
+    L.cup2d_fish_gait_get.argtypes = [vp, i, dp]
+    L.cup2d_fish_gait_set.argtypes = [vp, i, dp]
     L.cup2d_ensemble_create.argtypes = [ctypes.POINTER(vp), i, ctypes.POINTER(vp)]
     L.cup2d_ensemble_advance.argtypes = [vp, i]
     L.cup2d_ensemble_advance_timed.argtypes = [vp, i, dp]
@@ -410,8 +412,20 @@ class Context:
         self._ck(self.L.cup2d_checkpoint_save(self.h_, ptr, size))
         return out
 
+    def fish_gait(self, k=0):
+        """The gait parameters of curvature swimmer k: (amplitudeFactor, phi,
+        the six scales of StefanFish's curvature control values)."""
+        a = np.zeros(8, dtype=np.float64)
+        self._ck(self.L.cup2d_fish_gait_get(self.h_, k, _dp(a)))
+        return a
+
+    def set_fish_gait(self, k, theta):
+        a = np.ascontiguousarray(theta, dtype=np.float64)
+        assert a.size == 8
+        self._ck(self.L.cup2d_fish_gait_set(self.h_, k, _dp(a)))
+
     def adjoint(self, nsteps, box=None, every=20, dt=None, gradient=True, w_energy=1.0, w_force=(0.0, 0.0),
-                w_body=(0.0, 0.0, 0.0)):
+                w_body=(0.0, 0.0, 0.0), gait=False):
         """The time-averaged objective over nsteps steps from the current state,
         J = (1/nsteps) sum_n [w_energy (h^2/2) sum_box (u^2 + v^2) + w_force . force
         + w_body . (u_b, v_b, omega)] (box = (x0, x1, y0, y1) in domain units;
@@ -420,9 +434,10 @@ class Context:
         v_b, omega: a forced body's held one, a free body's initial one) by the discrete adjoint
         (forward recomputed from checkpoints every ``every`` steps).  dt: the
         frozen step sizes (nsteps values) or None for calcMaxTimestep's.
-        Returns (J, grad_u, grad_v, grad_body, dts, (forward_ms, backward_ms));
-        the gradients are None when gradient is False.  The context ends in
-        the forward's final state."""
+        Returns (J, grad_u, grad_v, grad_body, dts, (forward_ms, backward_ms)),
+        the gradients None when gradient is False; with gait=True (a tethered
+        curvature swimmer) grad_gait (8 values, fish_gait's order) is appended.
+        The context ends in the forward's final state."""
         dp = ctypes.POINTER(ctypes.c_double)
         obj = AdjointObjective()
         if box is not None:
@@ -441,10 +456,12 @@ class Context:
         gu = np.empty((self.ny, self.nx), dtype=np.float64) if gradient else None
         gv = np.empty((self.ny, self.nx), dtype=np.float64) if gradient else None
         gb = np.zeros(3, dtype=np.float64) if gradient else None
+        gg = np.zeros(8, dtype=np.float64) if gait else None
         ptr = lambda a: None if a is None else a.ctypes.data_as(dp)  # noqa: E731
         self._ck(self.L.cup2d_adjoint_run(self.h_, nsteps, every, ctypes.byref(obj), ptr(dti), ptr(dts),
-                                          ctypes.byref(J), ptr(gu), ptr(gv), ptr(gb), ptr(ms)))
-        return J.value, gu, gv, gb, dts, (float(ms[0]), float(ms[1]))
+                                          ctypes.byref(J), ptr(gu), ptr(gv), ptr(gb), ptr(gg), ptr(ms)))
+        out = (J.value, gu, gv, gb, dts, (float(ms[0]), float(ms[1])))
+        return out + (gg,) if gait else out
 
     def restore(self, blob):
         """Loads a checkpoint of this configuration (host array or device tensor)."""

@@ -294,6 +294,109 @@ k_adj_obst_apply(GridDesc g, const DevShape* sh, int k, ObstTiles t, const doubl
   }
 }
 
+// ---- the gait gradient of a tethered swimmer ------------------------------
+// Each step's objective sensitivity to the body's geometry on the grid
+// (dense planes of the step): gX to chi, gU / gV to the penalization's
+// target velocity U_s = (u_b - omega p_y + udef_x, v_b + omega p_x + udef_y),
+// gSX / gSY to the force kernel's surface normals (sdx, sdy).  The gait moves
+// only these (the body is held), so dJ/dtheta = sum over the steps of
+// <g, d(chi, U_s, sdx, sdy)/dtheta>, the latter by central differences of
+// the placement alone (flow-independent for a held body).
+//
+// Penalization and forces, from lambda on u^(n+1) (before Pen^T):
+// d u^(n+1)/d chi = U_s - u2, d u^(n+1)/d U_s = chi; forcex = sum nu/h [(u_E -
+// u_W) sdx + (u_N - u_S + v_E - v_W) sdy / 2] - p sdx, forcey alike.
+__global__ void __launch_bounds__(1024)
+k_adj_geo_pen(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
+              const double* __restrict__ u1, const double* __restrict__ v1, const double* __restrict__ p,
+              double pFac, const double* __restrict__ un, const double* __restrict__ vn,
+              const double* __restrict__ lu, const double* __restrict__ lv, double wFx, double wFy,
+              double* gX, double* gU, double* gV, double* gSX, double* gSY)
+{
+  const DevShape& S = sh[k];
+  const double Cx = S.s.com[0], Cy = S.s.com[1];
+  const double NUoH = g.nu / g.h;
+  for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
+    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+    const size_t o = (size_t)s * BS2 + threadIdx.y * BS + threadIdx.x;
+    const int gx = bx * BS + threadIdx.x, gy = by * BS + threadIdx.y;
+    const Nb j = nb_of(g, gx, gy);
+    const double X = t.chi[o];
+    if (chig[j.c] > X) continue;
+    const double p0 = cell_x(g, bx, threadIdx.x) - Cx, p1 = cell_y(g, by, threadIdx.y) - Cy;
+    double ux, uy;
+    udef_at(t, o, S, p0, p1, ux, uy);
+    const double US = S.s.u - S.s.omega * p1 + ux, VS = S.s.v + S.s.omega * p0 + uy;
+    const double u2 = u1[j.c] + pFac * (p[j.E] - p[j.W]), v2 = v1[j.c] + pFac * (p[j.N] - p[j.S]);
+    const double Lu = lu[j.c], Lv = lv[j.c];
+    gX[j.c] = Lu * (US - u2) + Lv * (VS - v2);
+    gU[j.c] = Lu * X;
+    gV[j.c] = Lv * X;
+    const double D11 = NUoH * (un[j.E] - un[j.W]), D22 = NUoH * (vn[j.N] - vn[j.S]);
+    const double D12 = NUoH / 2 * (un[j.N] - un[j.S] + vn[j.E] - vn[j.W]);
+    const double P = p[j.c];
+    gSX[j.c] = wFx * (D11 - P) + wFy * D12;
+    gSY[j.c] = wFx * D12 + wFy * (D22 - P);
+  }
+}
+
+// The obstacle terms' part of gX, from lambda on their output (lo) and the
+// sums of k_adj_obst_sums: with T' = (1 - chi) T and s = sum -chi T,
+// dJ/dchi = -T (dJ/dT' + dJ/ds) on the active piece.  Before
+// k_adj_obst_apply overwrites lo.
+__global__ void __launch_bounds__(1024)
+k_adj_geo_obst(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
+               const double* __restrict__ T, const double* __restrict__ lo, const double* __restrict__ acc,
+               double* gX)
+{
+  const DevShape& S = sh[k];
+  const double s = acc[0], pos = acc[1], neg = acc[2], Lp = acc[3], Ln = acc[4];
+  const double posF = fmax(pos, EPSd), negF = fmax(neg, EPSd);
+  const double corr = s / (s > 0 ? posF : negF);
+  for (int st = blockIdx.x; st < S.ntiles; st += gridDim.x) {
+    size_t c; double X; bool perim = false;
+    if (!obst_cell(g, t, st, chig, c, X, perim)) continue;
+    const double T0 = T[c], Tp = T0 + (-X * T0);
+    double GT, Gs;
+    if (s > 0) {
+      const bool P = perim && Tp > 0;
+      GT = lo[c] * (P && corr > 0 ? 1 - corr : 1.0) + (P && pos > EPSd ? corr / posF * Lp : 0.0);
+      Gs = -Lp / posF;
+    } else {
+      const bool N = perim && Tp < 0;
+      GT = lo[c] * (N && corr < 0 ? 1 + corr : 1.0) + (N && neg > EPSd ? corr / negF * Ln : 0.0);
+      Gs = Ln / negF;
+    }
+    gX[c] += -T0 * (GT + Gs);
+  }
+}
+
+// <g, geometry> over the tiles of the current placement (the replay of a
+// perturbed gait): acc += sum gX chi + gU U_s + gV V_s + gSX sdx + gSY sdy
+__global__ void __launch_bounds__(1024)
+k_adj_geo_dot(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
+              const double* __restrict__ gX, const double* __restrict__ gU, const double* __restrict__ gV,
+              const double* __restrict__ gSX, const double* __restrict__ gSY, double* acc)
+{
+  const DevShape& S = sh[k];
+  const double Cx = S.s.com[0], Cy = S.s.com[1];
+  double a = 0;
+  for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
+    const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
+    const size_t o = (size_t)s * BS2 + threadIdx.y * BS + threadIdx.x;
+    const size_t c = (size_t)(by * BS + threadIdx.y) * g.nx + bx * BS + threadIdx.x;
+    const double X = t.chi[o];
+    if (chig[c] > X) continue;
+    const double p0 = cell_x(g, bx, threadIdx.x) - Cx, p1 = cell_y(g, by, threadIdx.y) - Cy;
+    double ux, uy;
+    udef_at(t, o, S, p0, p1, ux, uy);
+    const double US = S.s.u - S.s.omega * p1 + ux, VS = S.s.v + S.s.omega * p0 + uy;
+    a += gX[c] * X + gU[c] * US + gV[c] * VS + gSX[c] * t.sdx[o] + gSY[c] * t.sdy[o];
+  }
+  for (int q = 16; q > 0; q >>= 1) a += __shfl_xor_sync(0xffffffffu, a, q);
+  if ((threadIdx.x & 31) == 0 && a != 0) atomicAdd(acc, a);
+}
+
 // ---- the boundary-strip fade F (cub2rhs) ----------------------------------
 __device__ __forceinline__ double fade_w2(const GridDesc& g, int gx, int gy) {
   const double fadeLenX = g.fadeLenX, invFadeX = 1 / fmax(fadeLenX, EPSd);
@@ -562,7 +665,7 @@ extern "C" {
 
 int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint_objective* obj,
                       const double* dt_in, double* dt_out, double* J, double* grad_u, double* grad_v,
-                      double* grad_body, double* ms) {
+                      double* grad_body, double* grad_gait, double* ms) {
   if (!ctx || nsteps <= 0 || every <= 0 || !obj || !J) return CUP2D_EINVAL;
   Ctx& c = ctx->c;
   if (!c.initialised) return adj_fail(ctx, CUP2D_ESTATE, "not initialised");
@@ -583,6 +686,10 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   if (sf.kind != CUP2D_SHAPE_DISK && (!forced || sf.pid || sf.pidpos))
     return adj_fail(ctx, CUP2D_ENOTSUP, "a swimmer must be tethered (forced in x, y and angle, no PID "
                                         "controller): a free swimmer's rotation moves its chi with the flow");
+  const bool gait = grad_gait != nullptr;
+  const bool curvFish = sf.kind == CUP2D_SHAPE_STEFANFISH || sf.kind == CUP2D_SHAPE_ENVELOPEFISH;
+  if (gait && !(curvFish && forced))
+    return adj_fail(ctx, CUP2D_ENOTSUP, "the gait gradient needs a tethered curvature swimmer");
   const GridDesc& g = c.g;
   {
     double t0, dtd, ux, uy; int st;
@@ -631,9 +738,13 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   // one step of Simulation::advance with dt given (PutObjectsOnGrid, advDiff,
   // PressureSingle, ComputeForces); T / F, when non-null, receive the RHS
   // before the obstacle terms and before the fade
-  auto step = [&](double dt, double* T, double* F) -> int {
+  auto step = [&](double dt, double* T, double* F, double* U1, double* V1) -> int {
     ARC(cup2d_put_objects(ctx, dt));
     ARC(cup2d_adv_diff(ctx, dt));
+    if (U1) {                                   // advDiff's velocity
+      ACK(cudaMemcpyAsync(U1, c.u(), nb, cudaMemcpyDeviceToDevice, c.stream));
+      ACK(cudaMemcpyAsync(V1, c.v(), nb, cudaMemcpyDeviceToDevice, c.stream));
+    }
     ARC(pressure_single_keep(ctx, dt, T, F));
     ARC(cup2d_compute_forces(ctx, dt));
     ARC(cup2d_end_step(ctx));
@@ -649,7 +760,7 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
     if (dt_in) dt = dt_in[i];
     else ARC(cup2d_calc_dt(ctx, &dt));
     dts[i] = dt;
-    ARC(step(dt, nullptr, nullptr));
+    ARC(step(dt, nullptr, nullptr, nullptr, nullptr));
     // the lab velocity of the step (set by the placement from the forced body)
     double t_, dtd, ux, uy; int st;
     ARC(cup2d_get_scalars(ctx, &t_, &dtd, &st, &ux, &uy));
@@ -675,7 +786,10 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   float fms = 0;
   ACK(cudaEventElapsedTime(&fms, e0, e1));
   if (ms) { ms[0] = fms; ms[1] = 0; }
-  if (!grad_u && !grad_v && !grad_body) { ARC(cup2d_checkpoint_load(ctx, ck[nseg], ckBytes)); return CUP2D_OK; }
+  if (!grad_u && !grad_v && !grad_body && !gait) {
+    ARC(cup2d_checkpoint_load(ctx, ck[nseg], ckBytes));
+    return CUP2D_OK;
+  }
 
   // backward
   const size_t segN = (size_t)every;
@@ -683,8 +797,22 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   double* sv = B.get<double>(n * segN);
   double* sT = B.get<double>(n * segN);      // RHS before the obstacle terms
   double* sF = B.get<double>(n * segN);      // RHS before the fade
-  double* pu = energy ? B.get<double>(n * segN) : sv;   // u^(n+1) (the energy term)
-  double* pv = energy ? B.get<double>(n * segN) : sv;
+  const bool keepNext = energy || gait;
+  double* pu = keepNext ? B.get<double>(n * segN) : sv;   // u^(n+1) (the energy term, the gait)
+  double* pv = keepNext ? B.get<double>(n * segN) : sv;
+  // the gait: advDiff's velocity and the pressure of each step, and the
+  // geometry sensitivities of every step of the run
+  double* su1 = gait ? B.get<double>(n * segN) : nullptr;
+  double* sv1 = gait ? B.get<double>(n * segN) : nullptr;
+  double* sp = gait ? B.get<double>(n * segN) : nullptr;
+  double* gG[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};   // gX, gU, gV, gSX, gSY
+  if (gait) {
+    for (double*& q : gG) {
+      if (!(q = B.get<double>(n * (size_t)nsteps))) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint gait planes");
+      ACK(cudaMemsetAsync(q, 0, nb * nsteps, c.stream));
+    }
+    if (!su1 || !sv1 || !sp) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint segment buffers");
+  }
   double* lu = B.get<double>(n);
   double* lv = B.get<double>(n);
   double* l1 = B.get<double>(n);
@@ -728,7 +856,8 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
       const size_t o = (size_t)(i - i0) * n;
       ACK(cudaMemcpyAsync(su + o, c.u(), nb, cudaMemcpyDeviceToDevice, c.stream));
       ACK(cudaMemcpyAsync(sv + o, c.v(), nb, cudaMemcpyDeviceToDevice, c.stream));
-      ARC(step(dts[i], sT + o, sF + o));
+      ARC(step(dts[i], sT + o, sF + o, gait ? su1 + o : nullptr, gait ? sv1 + o : nullptr));
+      if (gait) ACK(cudaMemcpyAsync(sp + o, c.pres, nb, cudaMemcpyDeviceToDevice, c.stream));
       {
         const int j = i - i0;
         const ObstTiles t = tilesAt(j);
@@ -740,7 +869,7 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
           ACK(cudaMemcpyAsync(dst[q], src[q], sizeof(double) * tb, cudaMemcpyDeviceToDevice, c.stream));
         ACK(cudaMemcpyAsync(chiSnap + o, c.chi, nb, cudaMemcpyDeviceToDevice, c.stream));
       }
-      if (energy) {
+      if (keepNext) {
         ACK(cudaMemcpyAsync(pu + o, c.u(), nb, cudaMemcpyDeviceToDevice, c.stream));
         ACK(cudaMemcpyAsync(pv + o, c.v(), nb, cudaMemcpyDeviceToDevice, c.stream));
       }
@@ -756,6 +885,12 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
       if (force)
         k_adj_force<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, wFx, wFy, 0, lu, lv, nullptr);
       if (bodyTerm) k_adj_add3<<<1, 1, 0, c.stream>>>(lx, wB[0], wB[1], wB[2]);
+      if (gait) {
+        const size_t og = (size_t)i * n;
+        k_adj_geo_pen<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, chiI, su1 + o, sv1 + o, sp + o,
+            -0.5 * dt / g.h, pu + o, pv + o, lu, lv, wFx, wFy, gG[0] + og, gG[1] + og, gG[2] + og, gG[3] + og,
+            gG[4] + og);
+      }
       // penalization
       k_adj_pen<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, chiI, lu, lv, lx);
       if (freeBody) {
@@ -783,6 +918,9 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
       k_adj_fade_apply<<<grid2, blk2, 0, c.stream>>>(g, sF + o, l2, acc);
       ACK(cudaMemsetAsync(acc, 0, sizeof(double) * 8, c.stream));
       k_adj_obst_sums<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, chiI, sT + o, l2, acc);
+      if (gait)
+        k_adj_geo_obst<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, chiI, sT + o, l2, acc,
+                                                            gG[0] + (size_t)i * n);
       k_adj_obst_apply<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, chiI, sT + o, l2, acc);
       // the divergence, added to lambda of u1
       k_adj_div_T<<<grid2, blk2, 0, c.stream>>>(g, 0.5 * g.h / dt, l2, lu, lv);
@@ -810,6 +948,41 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   float bms = 0;
   ACK(cudaEventElapsedTime(&bms, e2, e1));
   if (ms) ms[1] = bms;
+  if (gait) {
+    // d(geometry)/dtheta by central differences of the placement alone: from
+    // the run's first checkpoint, each perturbed gait replays the steps'
+    // PutObjectsOnGrid (and the step end: time, the next midline) with the
+    // frozen dt, and <g, geometry> is summed over the steps
+    double theta[CUP2D_GAIT_PARAMS];
+    ARC(cup2d_fish_gait_get(ctx, 0, theta));
+    const int np = sf.kind == CUP2D_SHAPE_STEFANFISH ? CUP2D_GAIT_PARAMS : 2;   // the envelope has no nodes
+    const double eps = 1e-6;
+    for (int q = 0; q < CUP2D_GAIT_PARAMS; q++) grad_gait[q] = 0;
+    for (int q = 0; q < np; q++) {
+      double Cpm[2];
+      for (int sg = 0; sg < 2; sg++) {
+        ARC(cup2d_fish_gait_set(ctx, 0, theta));          // the checkpoints' gait
+        ARC(cup2d_checkpoint_load(ctx, ck[0], ckBytes));
+        double th[CUP2D_GAIT_PARAMS];
+        std::copy(theta, theta + CUP2D_GAIT_PARAMS, th);
+        th[q] += sg == 0 ? eps : -eps;
+        ARC(cup2d_fish_gait_set(ctx, 0, th));
+        ACK(cudaMemsetAsync(acc, 0, sizeof(double), c.stream));
+        for (int i = 0; i < nsteps; i++) {
+          ARC(cup2d_put_objects(ctx, dts[i]));
+          const size_t og = (size_t)i * n;
+          k_adj_geo_dot<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, c.tiles[0], c.chi, gG[0] + og,
+                                                             gG[1] + og, gG[2] + og, gG[3] + og, gG[4] + og, acc);
+          ACK(cudaGetLastError());
+          ARC(cup2d_end_step(ctx));
+        }
+        ACK(cudaMemcpyAsync(&Cpm[sg], acc, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+        ACK(cudaStreamSynchronize(c.stream));
+      }
+      grad_gait[q] = (Cpm[0] - Cpm[1]) / (2 * eps);
+    }
+    ARC(cup2d_fish_gait_set(ctx, 0, theta));
+  }
   ARC(cup2d_checkpoint_load(ctx, ck[nseg], ckBytes));
   return CUP2D_OK;
 }

@@ -73,6 +73,25 @@ void natural_spline(const double* x, const double* y, int n, const double* xx, d
   }
 }
 
+// The curvature amplitude along the body, sampled at rS: StefanFish's
+// control values (StefanFish.cpp:187-193), each times its scale, splined
+// onto rS; the envelope swimmer's carangiform envelope (cup2d.h).
+std::vector<double> curvature_profile(const ShapeCfg& f, const std::vector<double>& rS) {
+  const int Nm = (int)rS.size();
+  const double L = f.length;
+  const double pts[6] = {0, .15 * L, .4 * L, .65 * L, .9 * L, L};
+  const double base[6] = {0.82014 / L, 1.46515 / L, 2.57136 / L, 3.75425 / L, 5.09147 / L, 5.70449 / L};
+  std::vector<double> p1f(Nm);
+  if (f.kind == CUP2D_SHAPE_ENVELOPEFISH) {
+    for (int i = 0; i < Nm; i++) p1f[i] = 0.82 * (rS[i] / L + 0.0025) / 1.0025 / L;
+  } else {
+    double vals[6];
+    for (int j = 0; j < 6; j++) vals[j] = base[j] * f.curvScale[j];
+    natural_spline(pts, vals, 6, rS.data(), p1f.data(), Nm);
+  }
+  return p1f;
+}
+
 // FishData arclength grid (FishLibrary.cpp:14-38, FishLibrary.h:62-74) and
 // the width profile of CurvatureFish/AmplitudeFish (StefanFish.cpp:175-182).
 bool fish_grid(double L, double h, std::vector<double>& rS, std::vector<double>& width) {
@@ -583,6 +602,7 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
   f.origAng = p->angle * M_PI / 180;
   f.radius = p->radius; f.tAccel = p->tAccel;
   f.length = p->L; f.Tperiod = p->T; f.phaseShift = p->phi; f.ampFac = p->amplitudeFactor;
+  for (double& x : f.curvScale) x = 1;
   const bool curvatureFish = kind == CUP2D_SHAPE_STEFANFISH || kind == CUP2D_SHAPE_ENVELOPEFISH;
   f.pid = curvatureFish && p->pid != 0;             // other shapes ignore -pid (StefanFish.cpp:209-211)
   f.pidpos = curvatureFish && p->pidpos != 0;
@@ -659,15 +679,7 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
     CK(cudaMemcpy(F.ipIdx, ipIdx.data(), sizeof(int2) * F.nint, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(F.nw, nw.data(), sizeof(int) * Nm, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(F.off, off.data(), sizeof(int) * (Nm + 1), cudaMemcpyHostToDevice));
-    // curvature control values, StefanFish.cpp:187-193, splined onto rS
-    const double L = f.length;
-    const double pts[6] = {0, .15 * L, .4 * L, .65 * L, .9 * L, L};
-    const double vals[6] = {0.82014 / L, 1.46515 / L, 2.57136 / L, 3.75425 / L, 5.09147 / L, 5.70449 / L};
-    std::vector<double> p1f(Nm);
-    if (kind == CUP2D_SHAPE_ENVELOPEFISH)      // the carangiform envelope (cup2d.h)
-      for (int i = 0; i < Nm; i++) p1f[i] = 0.82 * (rS[i] / L + 0.0025) / 1.0025 / L;
-    else
-      natural_spline(pts, vals, 6, rS.data(), p1f.data(), Nm);
+    const std::vector<double> p1f = curvature_profile(f, rS);
     CK(cudaMemcpy(F.rS, rS.data(), sizeof(double) * Nm, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(F.width, width.data(), sizeof(double) * Nm, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(F.p1f, p1f.data(), sizeof(double) * Nm, cudaMemcpyHostToDevice));
@@ -1509,7 +1521,7 @@ struct CkptHeader {
   double extent, CFL, lambda, dlm, nu, fadeLen;
   uint64_t checksum;              // ckpt_hash over the sections (0 in the comparison copy)
 };
-constexpr uint32_t CKPT_VERSION = 3;
+constexpr uint32_t CKPT_VERSION = 4;
 
 // The payload checksum: over each section's 8-byte words (the last one
 // zero-padded), the sum modulo 2^64 of SplitMix64 of the word mixed with its
@@ -1835,6 +1847,48 @@ int cup2d_fish_act(cup2d_ctx* ctx, int id, double t_action, const double* a, int
   // midlines formed ahead are of the old actuation: mark both buffers empty
   // (their time NaN) so that the next placement forms its midline again
   const FishArrays& F = c.fish[id];
+  CK(cudaMemset(F.integ + 7, 0xff, sizeof(double)));
+  CK(cudaMemset(F.integ + 15, 0xff, sizeof(double)));
+  c.sideMidPending = false;
+  c.midByGraph = false;
+  forget_chain(c);
+  c.shapesAtEvent = c.shapesMapped = false;
+  c.stateSeq++;
+  return CUP2D_OK;
+}
+
+int cup2d_fish_gait_get(cup2d_ctx* ctx, int id, double* theta) {
+  if (!ctx || !theta) return CUP2D_EINVAL;
+  int rc = fish_of(ctx, id);
+  if (rc) return rc;
+  const ShapeCfg& f = ctx->c.hshapes[id].cfg;
+  theta[0] = f.ampFac;
+  theta[1] = f.phaseShift;
+  for (int j = 0; j < 6; j++) theta[2 + j] = f.curvScale[j];
+  return CUP2D_OK;
+}
+
+int cup2d_fish_gait_set(cup2d_ctx* ctx, int id, const double* theta) {
+  if (!ctx || !theta) return CUP2D_EINVAL;
+  int rc = fish_of(ctx, id);
+  if (rc) return rc;
+  Ctx& c = ctx->c;
+  if (c.hshapes[id].cfg.kind != CUP2D_SHAPE_STEFANFISH)
+    for (int j = 0; j < 6; j++)
+      if (theta[2 + j] != 1) return fail(ctx, CUP2D_EINVAL, "the envelope swimmer has no curvature control values");
+  if ((rc = quiesce_all(ctx))) return rc;
+  CK(cudaMemcpy(&c.hshapes[id], c.dshapes + id, sizeof(DevShape), cudaMemcpyDeviceToHost));
+  ShapeCfg& f = c.hshapes[id].cfg;
+  f.ampFac = theta[0];
+  f.phaseShift = theta[1];
+  for (int j = 0; j < 6; j++) f.curvScale[j] = theta[2 + j];
+  CK(cudaMemcpy(&c.dshapes[id].cfg, &f, sizeof(ShapeCfg), cudaMemcpyHostToDevice));
+  const FishArrays& F = c.fish[id];
+  std::vector<double> rS(F.nm);
+  CK(cudaMemcpy(rS.data(), F.rS, sizeof(double) * F.nm, cudaMemcpyDeviceToHost));
+  const std::vector<double> p1f = curvature_profile(f, rS);
+  CK(cudaMemcpy(F.p1f, p1f.data(), sizeof(double) * F.nm, cudaMemcpyHostToDevice));
+  // midlines formed ahead are of the old gait (as after cup2d_fish_act)
   CK(cudaMemset(F.integ + 7, 0xff, sizeof(double)));
   CK(cudaMemset(F.integ + 15, 0xff, sizeof(double)));
   c.sideMidPending = false;

@@ -78,6 +78,7 @@ struct ShapeCfg {
   double origC[2], origAng;
   double radius, tAccel;                          // Disk
   double length, Tperiod, phaseShift, ampFac;     // Fish
+  double curvScale[6];                            // StefanFish: scales of its curvature control values
   int capacity;                                   // obstacle tile slots
   int nm;                                         // fish midline points
   int pid, pidpos;                                // StefanFish -pid / -pidpos (StefanFish.cpp:209-211)

@@ -313,6 +313,14 @@ int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes);
  * velocity, or a free body's initial one), each step's operators linearized about
  * its forward values and applied in reverse order, the forward recomputed
  * from device checkpoints taken every `every` steps.
+ *  - grad_gait (CUP2D_GAIT_PARAMS values, or null): for a tethered curvature
+ *    swimmer, dJ/dtheta of its gait parameters (cup2d_fish_gait_get): the
+ *    flow part by the adjoint (each step's sensitivity to the body's chi,
+ *    target velocity and surface normals on the grid), the geometry's
+ *    dependence on theta by central differences of the placement alone
+ *    (which the flow does not move for a held body), replayed from the
+ *    run's first checkpoint (the envelope swimmer: amplitude and phase
+ *    only, the other six 0);
  *  - dt_in: the step sizes (nsteps values), or null for calcMaxTimestep's;
  *    dt_out (nsteps values, or null) receives the schedule used.  dt is not
  *    differentiated (a frozen schedule);
@@ -324,7 +332,10 @@ int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes);
  *    body's), either forced in x, y and angle for the whole run and past
  *    its tAccel ramp (its velocity is held), or free in all three (its
  *    velocity solved each step from the momentum integrals, Shape.cpp:25-59,
- *    and differentiated through them); anything else CUP2D_ENOTSUP;
+ *    and differentiated through them); or a curvature swimmer held the same
+ *    way (forced in all three, no PID: its chi and udef move with its gait
+ *    alone, each step's kept by the recomputation); anything else
+ *    CUP2D_ENOTSUP;
  *  - the context ends in the forward's final state (as after nsteps
  *    steps); synchronises. */
 typedef struct cup2d_adjoint_objective {
@@ -335,7 +346,7 @@ typedef struct cup2d_adjoint_objective {
 } cup2d_adjoint_objective;
 int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint_objective* obj,
                       const double* dt_in, double* dt_out, double* J, double* grad_u, double* grad_v,
-                      double* grad_body, double* ms);
+                      double* grad_body, double* grad_gait, double* ms);
 
 /* ---- batched ensemble --------------------------------------------------- */
 /* No counterpart in the reference (it runs one Simulation per process):
@@ -379,6 +390,16 @@ int cup2d_ensemble_destroy(cup2d_ensemble* ens);
  * undulation's phase.  Between steps; the midline is re-formed from the next
  * placement.  Only for StefanFish / envelope swimmers. */
 int cup2d_fish_act(cup2d_ctx* ctx, int id, double t_action, const double* a, int na);
+/* The gait parameters of a curvature swimmer (no counterpart in the
+ * reference as one set): theta[0] = amplitudeFactor (the -amplitudeFactor of
+ * the shape descriptor), theta[1] = phi (-phi), theta[2..7] = scales of
+ * StefanFish's six curvature control values (StefanFish.cpp:187-193; 1 as
+ * built; the envelope swimmer has none: they stay 1).  set: between steps;
+ * the midline is re-formed from the next placement; a checkpoint loads only
+ * into a context of the same gait. */
+#define CUP2D_GAIT_PARAMS 8
+int cup2d_fish_gait_get(cup2d_ctx* ctx, int id, double* theta);
+int cup2d_fish_gait_set(cup2d_ctx* ctx, int id, const double* theta);
 /* StefanFish::getLearnTPeriod (StefanFish.cpp:379-383): the current period. */
 int cup2d_fish_period(cup2d_ctx* ctx, int id, double* period);
 /* StefanFish::state (StefanFish.cpp:397-577) relative to shape `other`, with

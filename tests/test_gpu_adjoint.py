@@ -230,6 +230,64 @@ def test_tethered_swimmer_gradient_matches_finite_differences(obj):
     assert abs(gb[0] - fd) <= 1e-5 * abs(fd), (gb[0], fd)
 
 
+def _fd_gait(ctx, blob, dts, obj, q, theta, eps=1e-6):
+    Js = []
+    for sgn in (1, -1):
+        ctx.restore(blob)
+        th = np.array(theta, dtype=np.float64)
+        th[q] += sgn * eps
+        ctx.set_fish_gait(0, th)
+        Js.append(ctx.adjoint(NSTEPS, dt=dts, gradient=False, **obj)[0])
+        ctx.set_fish_gait(0, theta)
+    ctx.restore(blob)
+    return (Js[0] - Js[1]) / (2 * eps)
+
+
+@pytest.fixture(scope="module")
+def swimming():
+    """The tethered swimmer past its first period (the gait's ramp), by
+    graph steps, and its checkpoint."""
+    s = Simulation(TETHERED)
+    s.init()
+    s.ctx.advance(1200)
+    s.ctx.sync()
+    assert s.ctx.scalars()["time"] > 1.0
+    return s, s.ctx.checkpoint()
+
+
+@pytest.mark.parametrize("obj", [DRAG, ENERGY], ids=["drag", "energy"])
+def test_gait_gradient_matches_finite_differences(swimming, obj):
+    """dJ/d(amplitude, phase, the six curvature control scales) of a
+    tethered StefanFish: the adjoint's per-step geometry sensitivities
+    contracted with the placement's central differences, against central
+    differences of the whole simulation (measured agreement 1e-8..1e-6)."""
+    s, blob = swimming
+    s.ctx.restore(blob)
+    theta = s.ctx.fish_gait(0)
+    assert np.array_equal(theta, [1, 0, 1, 1, 1, 1, 1, 1])
+    J, gu, gv, gb, dts, ms, gg = s.ctx.adjoint(NSTEPS, every=5, gait=True, **obj)
+    s.ctx.restore(blob)
+    assert np.array_equal(s.ctx.fish_gait(0), theta)
+    scale = np.max(np.abs(gg))
+    assert scale > 0
+    for q in range(8):
+        fd = _fd_gait(s.ctx, blob, dts, obj, q, theta)
+        assert abs(gg[q] - fd) <= 1e-5 * abs(fd) + 1e-7 * scale, (q, gg[q], fd)
+
+
+def test_gait_set_round_trip(swimming):
+    s, blob = swimming
+    s.ctx.restore(blob)
+    th = np.array([1.1, 0.3, 1, 0.9, 1.2, 1, 1, 0.8])
+    s.ctx.set_fish_gait(0, th)
+    assert np.array_equal(s.ctx.fish_gait(0), th)
+    # a checkpoint loads only into a context of its gait
+    with pytest.raises(Cup2DError):
+        s.ctx.restore(blob)
+    s.ctx.set_fish_gait(0, [1, 0, 1, 1, 1, 1, 1, 1])
+    s.ctx.restore(blob)
+
+
 def test_free_body_objective_matches_plain_steps():
     s = _developed_free()
     blob = s.ctx.checkpoint()
