@@ -541,6 +541,62 @@ def adjoint_measurement(local, rank, pg, warm=50, nsteps=200, every=20):
     return out
 
 
+def gait_measurement(local, rank, pg, warm=1500, nsteps=200, every=20):
+    """The gait gradient of a tethered StefanFish (512x256, held in a 0.2
+    stream, past its first period): d(time-averaged forcex over 200 steps)
+    / d(amplitude, phase, six curvature control scales), its cost against
+    the same steps as graph steps, and the amplitude component against a
+    central difference of the whole simulation."""
+    argline = ("-bpdx 16 -bpdy 8 -extent 1 -CFL 0.1 -nu 2e-5 -lambda 1e4 -poissonType freespace -muteAll 1 "
+               "-shapes 'stefanfish L=0.2 T=1 xpos=0.4 ypos=0.25 bFixed=1 bForced=1 xvel=0.2'")
+    sim = make_sim(argline, local, rank)
+    ctx = sim.ctx
+    ctx.advance(warm)
+    ctx.sync()
+    blob = ctx.checkpoint()
+    obj = dict(box=None, w_force=(1.0, 0.0))
+    eps = 1e-7                      # the placement's and the whole simulation's difference step
+    J, gu, gv, gb, dts, ms, gg = ctx.adjoint(nsteps, every=every, gait=True, gait_step=eps, **obj)
+    ctx.restore(blob)
+    graph_ms = ctx.time_step(nsteps)
+    theta = ctx.fish_gait(0)
+
+    def central(n, q, dt):
+        Js = []
+        for sgn in (1, -1):
+            ctx.restore(blob)
+            th = theta.copy()
+            th[q] += sgn * eps
+            ctx.set_fish_gait(0, th)
+            Js.append(ctx.adjoint(n, dt=dt, gradient=False, **obj)[0])
+            ctx.set_fish_gait(0, theta)
+        return (Js[0] - Js[1]) / (2 * eps)
+
+    fd = central(nsteps, 0, dts)
+    # a short horizon (fewer raster switches within the step)
+    ctx.restore(blob)
+    short = 16
+    _, _, _, _, dts16, _, gg16 = ctx.adjoint(short, every=short, gait=True, gait_step=eps, **obj)
+    fd16 = [central(short, q, dts16) for q in range(8)]
+    ctx.restore(blob)
+    out = {"workload": "tethered_stefanfish_512x256_fp64", "steps": nsteps, "checkpoint_every": every,
+           "warm_graph_steps_before": warm,
+           "objective": "time-averaged forcex (ComputeForces) over the steps",
+           "parameters": ["amplitudeFactor", "phi", "curvature scale 1..6"],
+           "J": J, "grad_gait": [float(x) for x in gg],
+           "forward_graph_ms": graph_ms, "backward_ms": ms[1], "gait_replay_ms": ms[2],
+           "adjoint_over_forward": ms[1] / graph_ms,
+           "gradient_over_forward": (ms[1] + ms[2]) / graph_ms,
+           "fd_check": {"parameter": "amplitudeFactor", "adjoint": float(gg[0]), "central_difference": fd,
+                        "eps": eps, "rel_err": abs(gg[0] - fd) / max(abs(fd), 1e-300)},
+           "fd_check_16_steps": {"adjoint": [float(x) for x in gg16], "central_difference": fd16,
+                                 "max_rel_err": max(abs(a - b) / max(abs(b), 1e-300) for a, b in zip(gg16, fd16))},
+           "method": "flow: discrete adjoint with checkpointed recomputation; the body geometry's "
+                     "dependence on the gait: central differences of the placement alone (16 replays)"}
+    del sim
+    return out
+
+
 def run_ours(args, world, rank, local, pg):
     import torch
     name, argline = WORKLOADS[args.workload]
@@ -627,6 +683,8 @@ def run_ours(args, world, rank, local, pg):
     if not args.no_large and not args.no_falling:
         falling = falling_measurement(local, rank, pg)
     adjoint = None if args.no_adjoint else adjoint_measurement(local, rank, pg)
+    if adjoint is not None:
+        adjoint["gait"] = gait_measurement(local, rank, pg)
 
     line = None
     if rank == 0:

@@ -51,7 +51,7 @@ KERNELS = {"advdiff": 0, "rhs_div": 1, "pcorr": 2, "fft_rows_fwd": 3, "fft_cols"
 
 class AdjointObjective(ctypes.Structure):
     _fields_ = [("box", ctypes.c_double * 4), ("w_energy", ctypes.c_double), ("w_force", ctypes.c_double * 2),
-                ("w_body", ctypes.c_double * 3)]
+                ("w_body", ctypes.c_double * 3), ("gait_step", ctypes.c_double)]
 
 
 class Config(ctypes.Structure):
@@ -425,7 +425,7 @@ class Context:
         self._ck(self.L.cup2d_fish_gait_set(self.h_, k, _dp(a)))
 
     def adjoint(self, nsteps, box=None, every=20, dt=None, gradient=True, w_energy=1.0, w_force=(0.0, 0.0),
-                w_body=(0.0, 0.0, 0.0), gait=False):
+                w_body=(0.0, 0.0, 0.0), gait=False, gait_step=0.0):
         """The time-averaged objective over nsteps steps from the current state,
         J = (1/nsteps) sum_n [w_energy (h^2/2) sum_box (u^2 + v^2) + w_force . force
         + w_body . (u_b, v_b, omega)] (box = (x0, x1, y0, y1) in domain units;
@@ -436,7 +436,9 @@ class Context:
         frozen step sizes (nsteps values) or None for calcMaxTimestep's.
         Returns (J, grad_u, grad_v, grad_body, dts, (forward_ms, backward_ms)),
         the gradients None when gradient is False; with gait=True (a tethered
-        curvature swimmer) grad_gait (8 values, fish_gait's order) is appended.
+        curvature swimmer) the times gain the placement replays' and
+        grad_gait (8 values, fish_gait's order) is appended; gait_step: the
+        placement's central-difference step (0: 1e-7).
         The context ends in the forward's final state."""
         dp = ctypes.POINTER(ctypes.c_double)
         obj = AdjointObjective()
@@ -447,12 +449,13 @@ class Context:
         obj.w_force[0], obj.w_force[1] = float(w_force[0]), float(w_force[1])
         for k in range(3):
             obj.w_body[k] = float(w_body[k])
+        obj.gait_step = float(gait_step)
         dts = np.empty(nsteps, dtype=np.float64)
         dti = None if dt is None else np.ascontiguousarray(dt, dtype=np.float64)
         if dti is not None and dti.size != nsteps:
             raise ValueError("dt needs nsteps values")
         J = ctypes.c_double()
-        ms = np.zeros(2, dtype=np.float64)
+        ms = np.zeros(3, dtype=np.float64)
         gu = np.empty((self.ny, self.nx), dtype=np.float64) if gradient else None
         gv = np.empty((self.ny, self.nx), dtype=np.float64) if gradient else None
         gb = np.zeros(3, dtype=np.float64) if gradient else None
@@ -460,8 +463,9 @@ class Context:
         ptr = lambda a: None if a is None else a.ctypes.data_as(dp)  # noqa: E731
         self._ck(self.L.cup2d_adjoint_run(self.h_, nsteps, every, ctypes.byref(obj), ptr(dti), ptr(dts),
                                           ctypes.byref(J), ptr(gu), ptr(gv), ptr(gb), ptr(gg), ptr(ms)))
-        out = (J.value, gu, gv, gb, dts, (float(ms[0]), float(ms[1])))
-        return out + (gg,) if gait else out
+        if gait:
+            return J.value, gu, gv, gb, dts, (float(ms[0]), float(ms[1]), float(ms[2])), gg
+        return J.value, gu, gv, gb, dts, (float(ms[0]), float(ms[1]))
 
     def restore(self, blob):
         """Loads a checkpoint of this configuration (host array or device tensor)."""

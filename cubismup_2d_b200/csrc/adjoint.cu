@@ -619,6 +619,16 @@ int adj_fail(cup2d_ctx* ctx, int code, const std::string& msg) {
 #define ARC(call)                                                               \
   do { const int r_ = (call); if (r_ != CUP2D_OK) return r_; } while (0)
 
+// a checkpoint of the run, loaded back (the error names which)
+#define ALOAD(idx)                                                              \
+  do {                                                                          \
+    const int r_ = cup2d_checkpoint_load(ctx, ck[idx], ckBytes);                \
+    if (r_ != CUP2D_OK) {                                                       \
+      ctx->c.err += " (the adjoint's checkpoint " + std::to_string(idx) + " of " + std::to_string(nseg) + ")"; \
+      return r_;                                                                \
+    }                                                                           \
+  } while (0)
+
 // device scratch of the adjoint run, freed on every exit
 struct AdjBufs {
   std::vector<void*> p;
@@ -785,9 +795,9 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   if (dt_out) std::copy(dts.begin(), dts.end(), dt_out);
   float fms = 0;
   ACK(cudaEventElapsedTime(&fms, e0, e1));
-  if (ms) { ms[0] = fms; ms[1] = 0; }
+  if (ms) { ms[0] = fms; ms[1] = 0; if (gait) ms[2] = 0; }
   if (!grad_u && !grad_v && !grad_body && !gait) {
-    ARC(cup2d_checkpoint_load(ctx, ck[nseg], ckBytes));
+    ALOAD(nseg);
     return CUP2D_OK;
   }
 
@@ -851,7 +861,7 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   const int tctas = tile_ctas(c, cap);
   for (int s = nseg - 1; s >= 0; s--) {
     const int i0 = s * every, i1 = std::min(nsteps, i0 + every);
-    ARC(cup2d_checkpoint_load(ctx, ck[s], ckBytes));
+    ALOAD(s);
     for (int i = i0; i < i1; i++) {
       const size_t o = (size_t)(i - i0) * n;
       ACK(cudaMemcpyAsync(su + o, c.u(), nb, cudaMemcpyDeviceToDevice, c.stream));
@@ -956,13 +966,14 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
     double theta[CUP2D_GAIT_PARAMS];
     ARC(cup2d_fish_gait_get(ctx, 0, theta));
     const int np = sf.kind == CUP2D_SHAPE_STEFANFISH ? CUP2D_GAIT_PARAMS : 2;   // the envelope has no nodes
-    const double eps = 1e-6;
+    const double eps = obj->gait_step > 0 ? obj->gait_step : 1e-7;
+    ACK(cudaEventRecord(e2, c.stream));
     for (int q = 0; q < CUP2D_GAIT_PARAMS; q++) grad_gait[q] = 0;
     for (int q = 0; q < np; q++) {
       double Cpm[2];
       for (int sg = 0; sg < 2; sg++) {
         ARC(cup2d_fish_gait_set(ctx, 0, theta));          // the checkpoints' gait
-        ARC(cup2d_checkpoint_load(ctx, ck[0], ckBytes));
+        ALOAD(0);
         double th[CUP2D_GAIT_PARAMS];
         std::copy(theta, theta + CUP2D_GAIT_PARAMS, th);
         th[q] += sg == 0 ? eps : -eps;
@@ -981,9 +992,14 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
       }
       grad_gait[q] = (Cpm[0] - Cpm[1]) / (2 * eps);
     }
+    ACK(cudaEventRecord(e1, c.stream));
+    ACK(cudaEventSynchronize(e1));
+    float gms = 0;
+    ACK(cudaEventElapsedTime(&gms, e2, e1));
+    if (ms) ms[2] = gms;
     ARC(cup2d_fish_gait_set(ctx, 0, theta));
   }
-  ARC(cup2d_checkpoint_load(ctx, ck[nseg], ckBytes));
+  ALOAD(nseg);
   return CUP2D_OK;
 }
 

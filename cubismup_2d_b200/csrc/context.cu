@@ -500,7 +500,8 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
   if (!rc && fish_setup_kernels() != cudaSuccess)
     rc = fail(ctx, CUP2D_ECUDA, "shared-memory limits of the fish kernels could not be set");
   if (rc) { cup2d_destroy(ctx); return rc; }
-  if (cudaMemset(c.counters, 0, sizeof(unsigned) * Ctx::NCOUNTERS) != cudaSuccess) { cup2d_destroy(ctx); return CUP2D_ECUDA; }
+  if (cudaMemsetAsync(c.counters, 0, sizeof(unsigned) * Ctx::NCOUNTERS, c.stream) != cudaSuccess ||
+      cudaStreamSynchronize(c.stream) != cudaSuccess) { cup2d_destroy(ctx); return CUP2D_ECUDA; }
   c.poisson = poisson_create(c);
   if (!c.poisson) { cup2d_destroy(ctx); return create_fail(CUP2D_ENOMEM, "Poisson solver set-up failed"); }
   if (cfg->autotune && poisson_autotune(c) != cudaSuccess) {
@@ -628,7 +629,7 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
   double** arrs[] = {&t.chi, &t.dist, &t.udx, &t.udy, &t.sD, &t.sdx, &t.sdy};
   for (auto a : arrs) if (!rc) rc = dalloc(ctx, a, (size_t)cap * BS2);
   if (rc) return rc;
-  CK(cudaMemset(t.slot, 0xff, sizeof(int) * c.g.nblocks));
+  CK(cudaMemsetAsync(t.slot, 0xff, sizeof(int) * c.g.nblocks, c.stream));
   FishArrays F{};
   if (kind != CUP2D_SHAPE_DISK) {
     std::vector<double> rS, width;
@@ -660,7 +661,7 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
       F.frame.uX = F.frame.uY = F.frame.lX = F.frame.lY = nullptr;
     }
     // no midline formed yet: integrals (with their time) NaN (all-ones bytes)
-    CK(cudaMemset(F.integ, 0xff, sizeof(double) * 16));
+    CK(cudaMemsetAsync(F.integ, 0xff, sizeof(double) * 16, c.stream));
     // interior-point layout of PutFishOnBlocks::constructInternl
     // (FishLibrary.cpp:594-596): Nw = floor(width/h) points each side
     std::vector<int> nw(Nm), off(Nm + 1, 0);
@@ -676,13 +677,13 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
     std::vector<int2> ipIdx(F.nint);
     for (int i = 0; i < Nm; i++)
       for (int j = 0; j < (nw[i] > 0 ? 2 * nw[i] - 1 : 0); j++) ipIdx[off[i] + j] = make_int2(i, -nw[i] + 1 + j);
-    CK(cudaMemcpy(F.ipIdx, ipIdx.data(), sizeof(int2) * F.nint, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(F.nw, nw.data(), sizeof(int) * Nm, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(F.off, off.data(), sizeof(int) * (Nm + 1), cudaMemcpyHostToDevice));
+    CK(h2d_sync(F.ipIdx, ipIdx.data(), sizeof(int2) * F.nint, c.stream));
+    CK(h2d_sync(F.nw, nw.data(), sizeof(int) * Nm, c.stream));
+    CK(h2d_sync(F.off, off.data(), sizeof(int) * (Nm + 1), c.stream));
     const std::vector<double> p1f = curvature_profile(f, rS);
-    CK(cudaMemcpy(F.rS, rS.data(), sizeof(double) * Nm, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(F.width, width.data(), sizeof(double) * Nm, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(F.p1f, p1f.data(), sizeof(double) * Nm, cudaMemcpyHostToDevice));
+    CK(h2d_sync(F.rS, rS.data(), sizeof(double) * Nm, c.stream));
+    CK(h2d_sync(F.width, width.data(), sizeof(double) * Nm, c.stream));
+    CK(h2d_sync(F.p1f, p1f.data(), sizeof(double) * Nm, c.stream));
     CK(fish_width_cubes(F, c.stream));
     CK(cudaStreamSynchronize(c.stream));
   }
@@ -1110,7 +1111,7 @@ int cup2d_set_field(cup2d_ctx* ctx, int which, const double* host_in) {
   // the other uDef component keeps the values a read would have given
   if ((which == CUP2D_FIELD_UDEF_X || which == CUP2D_FIELD_UDEF_Y) && c.udefStale) CK(fill_udef_grid(c));
   CK(cudaStreamSynchronize(c.stream));
-  CK(cudaMemcpy(p, host_in, sizeof(double) * c.ncells(), cudaMemcpyHostToDevice));
+  CK(h2d_sync(p, host_in, sizeof(double) * c.ncells(), c.stream));
   forget_chain(c);
   c.stateSeq++;
   CK(invalidate_dt_next(c));
@@ -1151,7 +1152,7 @@ int cup2d_set_shape(cup2d_ctx* ctx, int id, const cup2d_shape_state* in) {
   CK(cudaStreamSynchronize(c.stream));
   CK(cudaMemcpy(&c.hshapes[id], c.dshapes + id, sizeof(DevShape), cudaMemcpyDeviceToHost));
   c.hshapes[id].s = *in;
-  CK(cudaMemcpy(c.dshapes + id, &c.hshapes[id], sizeof(DevShape), cudaMemcpyHostToDevice));
+  CK(h2d_sync(c.dshapes + id, &c.hshapes[id], sizeof(DevShape), c.stream));
   forget_chain(c);
   c.shapesAtEvent = c.shapesMapped = false;
   c.stateSeq++;
@@ -1181,7 +1182,7 @@ int cup2d_set_scalars(cup2d_ctx* ctx, double time, double dt, int step, double u
   CK(cudaMemcpy(&s, c.dsc, sizeof(Scalars), cudaMemcpyDeviceToHost));
   s.time = time; s.dt = dt; s.step = step; s.uinfx = uinfx; s.uinfy = uinfy;
   s.dtNextValid = 0;
-  CK(cudaMemcpy(c.dsc, &s, sizeof(Scalars), cudaMemcpyHostToDevice));
+  CK(h2d_sync(c.dsc, &s, sizeof(Scalars), c.stream));
   c.midByGraph = false;
   c.devDt = dt;
   c.dtValidMaybe = c.dtCarried = false;
@@ -1668,17 +1669,22 @@ int cup2d_checkpoint_save(cup2d_ctx* ctx, void* buf, size_t bytes) {
   for (int k = 0; k < c.nshapes; k++) cfgs[k] = c.hshapes[k].cfg;
   std::vector<uint64_t> sizes(secs.size());
   for (size_t i = 0; i < secs.size(); i++) sizes[i] = secs[i].bytes;
+  // every copy on the context's stream, then a wait: a device buffer's
+  // copies (device to device, asynchronous to the host) are complete before
+  // the next step's kernels may change the state
   size_t off = 0;
-  CK(cudaMemcpy(out + off, &h, sizeof(h), cudaMemcpyDefault));
+  CK(cudaMemcpyAsync(out + off, &h, sizeof(h), cudaMemcpyDefault, c.stream));
   off += sizeof(h);
-  if (c.nshapes) CK(cudaMemcpy(out + off, cfgs.data(), sizeof(ShapeCfg) * c.nshapes, cudaMemcpyDefault));
+  if (c.nshapes)
+    CK(cudaMemcpyAsync(out + off, cfgs.data(), sizeof(ShapeCfg) * c.nshapes, cudaMemcpyDefault, c.stream));
   off += sizeof(ShapeCfg) * c.nshapes;
-  CK(cudaMemcpy(out + off, sizes.data(), sizeof(uint64_t) * sizes.size(), cudaMemcpyDefault));
+  CK(cudaMemcpyAsync(out + off, sizes.data(), sizeof(uint64_t) * sizes.size(), cudaMemcpyDefault, c.stream));
   off += sizeof(uint64_t) * sizes.size();
   for (const CkptSection& x : secs) {
-    CK(cudaMemcpy(out + off, x.p, x.bytes, cudaMemcpyDefault));
+    CK(cudaMemcpyAsync(out + off, x.p, x.bytes, cudaMemcpyDefault, c.stream));
     off += x.bytes;
   }
+  CK(cudaStreamSynchronize(c.stream));
   return CUP2D_OK;
 }
 
@@ -1727,10 +1733,11 @@ int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes) {
     if ((rc = ckpt_hash(ctx, src, !onDevice, &sum))) return rc;
     if (sum != stored) return fail(ctx, CUP2D_EINVAL, "checkpoint payload damaged (checksum differs)");
   }
-  for (const CkptSection& x : secs) {
-    CK(cudaMemcpy(x.p, in + off, x.bytes, cudaMemcpyDefault));
+  for (const CkptSection& x : secs) {        // on the context's stream (see the save)
+    CK(cudaMemcpyAsync(x.p, in + off, x.bytes, cudaMemcpyDefault, c.stream));
     off += x.bytes;
   }
+  CK(cudaStreamSynchronize(c.stream));
   // host state of a context between steps, knowing nothing of the device
   c.cur = 0;
   if (c.nshapes)
@@ -1774,7 +1781,7 @@ extern "C" int cup2d_trace(cup2d_ctx* ctx, unsigned long long* out, int reset) {
   if (reset) {
     std::vector<unsigned long long> init(2 * TR_N + 8 * TRACE_ITEMS, 0);
     for (int i = 0; i < TR_N; i++) { init[2 * i] = ~0ULL; init[2 * i + 1] = 0; }
-    cudaMemcpy(buf, init.data(), sizeof(unsigned long long) * init.size(), cudaMemcpyHostToDevice);
+    h2d_sync(buf, init.data(), sizeof(unsigned long long) * init.size(), ctx->c.stream);
   }
   return CUP2D_OK;
 }
@@ -1843,12 +1850,13 @@ int cup2d_fish_act(cup2d_ctx* ctx, int id, double t_action, const double* a, int
     C.periodPIDval = S.cfg.Tperiod * (1 + a[1]);
     C.periodPIDdif = 0;
   }
-  CK(cudaMemcpy(&c.dshapes[id].ctl, &C, sizeof(FishCtl), cudaMemcpyHostToDevice));
+  CK(h2d_sync(&c.dshapes[id].ctl, &C, sizeof(FishCtl), c.stream));
   // midlines formed ahead are of the old actuation: mark both buffers empty
   // (their time NaN) so that the next placement forms its midline again
   const FishArrays& F = c.fish[id];
-  CK(cudaMemset(F.integ + 7, 0xff, sizeof(double)));
-  CK(cudaMemset(F.integ + 15, 0xff, sizeof(double)));
+  CK(cudaMemsetAsync(F.integ + 7, 0xff, sizeof(double), c.stream));
+  CK(cudaMemsetAsync(F.integ + 15, 0xff, sizeof(double), c.stream));
+  CK(cudaStreamSynchronize(c.stream));
   c.sideMidPending = false;
   c.midByGraph = false;
   forget_chain(c);
@@ -1882,15 +1890,16 @@ int cup2d_fish_gait_set(cup2d_ctx* ctx, int id, const double* theta) {
   f.ampFac = theta[0];
   f.phaseShift = theta[1];
   for (int j = 0; j < 6; j++) f.curvScale[j] = theta[2 + j];
-  CK(cudaMemcpy(&c.dshapes[id].cfg, &f, sizeof(ShapeCfg), cudaMemcpyHostToDevice));
+  CK(h2d_sync(&c.dshapes[id].cfg, &f, sizeof(ShapeCfg), c.stream));
   const FishArrays& F = c.fish[id];
   std::vector<double> rS(F.nm);
   CK(cudaMemcpy(rS.data(), F.rS, sizeof(double) * F.nm, cudaMemcpyDeviceToHost));
   const std::vector<double> p1f = curvature_profile(f, rS);
-  CK(cudaMemcpy(F.p1f, p1f.data(), sizeof(double) * F.nm, cudaMemcpyHostToDevice));
+  CK(h2d_sync(F.p1f, p1f.data(), sizeof(double) * F.nm, c.stream));
   // midlines formed ahead are of the old gait (as after cup2d_fish_act)
-  CK(cudaMemset(F.integ + 7, 0xff, sizeof(double)));
-  CK(cudaMemset(F.integ + 15, 0xff, sizeof(double)));
+  CK(cudaMemsetAsync(F.integ + 7, 0xff, sizeof(double), c.stream));
+  CK(cudaMemsetAsync(F.integ + 15, 0xff, sizeof(double), c.stream));
+  CK(cudaStreamSynchronize(c.stream));
   c.sideMidPending = false;
   c.midByGraph = false;
   forget_chain(c);

@@ -21,6 +21,16 @@ inline cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, siz
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
+// A host-to-device copy ordered on `stream` and complete on return.  A plain
+// cudaMemcpy runs on the legacy default stream, which the context's
+// non-blocking streams do not wait for: from pageable memory it may return
+// before its DMA lands, and a kernel launched next on the context's stream
+// could read the old values.
+inline cudaError_t h2d_sync(void* dst, const void* src, size_t bytes, cudaStream_t stream) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream);
+  return e == cudaSuccess ? cudaStreamSynchronize(stream) : e;
+}
+
 // fluid.cu
 void launch_max_u_dt(Ctx& c);                        // Helpers.cpp:136-176 + Simulation.cpp:254-277
 void launch_set_dt(Ctx& c, double dt);               // Operator::operator()(dt) argument

@@ -1371,7 +1371,7 @@ Poisson* poisson_create(Ctx& c) {
     tw[k] = make_double2((double)cosl(a), (double)sinl(a));
   }
   if (cudaMalloc(&P->tw, sizeof(double2) * P->twLen) != cudaSuccess) { delete P; return nullptr; }
-  cudaMemcpy(P->tw, tw.data(), sizeof(double2) * P->twLen, cudaMemcpyHostToDevice);
+  h2d_sync(P->tw, tw.data(), sizeof(double2) * P->twLen, c.stream);
   const size_t specRows = (size_t)P->Lcol;
   if (cudaMalloc(&P->spec, sizeof(double2) * specRows * P->nkx) != cudaSuccess) { poisson_destroy(P); return nullptr; }
   set_all_smem();
@@ -1383,8 +1383,8 @@ Poisson* poisson_create(Ctx& c) {
     for (int i = 0; i < Nx; i++) cx[i] = (float)std::cos(M_PI / Nx * 2.0 * i);
     if (cudaMalloc(&P->cosX, sizeof(float) * Nx) != cudaSuccess ||
         cudaMalloc(&P->cosY, sizeof(float) * Ny) != cudaSuccess) { poisson_destroy(P); return nullptr; }
-    cudaMemcpy(P->cosX, cx.data(), sizeof(float) * Nx, cudaMemcpyHostToDevice);
-    cudaMemcpy(P->cosY, cy.data(), sizeof(float) * Ny, cudaMemcpyHostToDevice);
+    h2d_sync(P->cosX, cx.data(), sizeof(float) * Nx, c.stream);
+    h2d_sync(P->cosY, cy.data(), sizeof(float) * Ny, c.stream);
   }
   if (P->type == CUP2D_POISSON_FREESPACE) {
     // G^ = Re FFT[G] / (MX MY) on the MY x MX padded grid, kept for ky <= MY/2
@@ -1404,7 +1404,7 @@ Poisson* poisson_create(Ctx& c) {
     std::vector<float2> tw32(P->twLen);
     for (int k = 0; k < P->twLen; k++) tw32[k] = make_float2((float)tw[k].x, (float)tw[k].y);
     if (cudaMalloc(&P->tw32, sizeof(float2) * P->twLen) != cudaSuccess) { poisson_destroy(P); return nullptr; }
-    cudaMemcpy(P->tw32, tw32.data(), sizeof(float2) * P->twLen, cudaMemcpyHostToDevice);
+    h2d_sync(P->tw32, tw32.data(), sizeof(float2) * P->twLen, c.stream);
     if (P->type == CUP2D_POISSON_FREESPACE) {
       const size_t ng = (size_t)(P->Lcol / 2 + 1) * P->nkx;
       std::vector<double> g64(ng);
@@ -1413,7 +1413,7 @@ Poisson* poisson_create(Ctx& c) {
           cudaMemcpy(g64.data(), P->ghat, sizeof(double) * ng, cudaMemcpyDeviceToHost) != cudaSuccess ||
           cudaMalloc(&P->ghat32, sizeof(float) * ng) != cudaSuccess) { poisson_destroy(P); return nullptr; }
       for (size_t i = 0; i < ng; i++) g32[i] = (float)g64[i];
-      cudaMemcpy(P->ghat32, g32.data(), sizeof(float) * ng, cudaMemcpyHostToDevice);
+      h2d_sync(P->ghat32, g32.data(), sizeof(float) * ng, c.stream);
     }
   }
   return P;

@@ -324,8 +324,9 @@ int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes);
  *  - dt_in: the step sizes (nsteps values), or null for calcMaxTimestep's;
  *    dt_out (nsteps values, or null) receives the schedule used.  dt is not
  *    differentiated (a frozen schedule);
- *  - ms (2 values, or null): device time of the forward (with its
- *    checkpoints) and of the backward (recomputation and transposed steps);
+ *  - ms (2 values, 3 with grad_gait, or null): device time of the forward
+ *    (with its checkpoints), of the backward (recomputation and transposed
+ *    steps), and of the gait's placement replays;
  *  - covered: FP64, any of the three solvers, explicit penalization
  *    without the iterated or variable-density pipelines, one disk fixed on
  *    the grid (bFixed: its chi does not move; the lab velocity is minus the
@@ -343,6 +344,11 @@ typedef struct cup2d_adjoint_objective {
   double w_energy;        /* its weight (0: no energy term, box unused)    */
   double w_force[2];      /* weights of the body's forcex and forcey       */
   double w_body[3];       /* weights of the body's velocity u, v, omega    */
+  double gait_step;       /* the gait gradient's central-difference step   */
+                          /* of the placement (0: 1e-7); the forward is     */
+                          /* piecewise smooth (raster switches), so a      */
+                          /* whole-simulation difference compares at the    */
+                          /* same step                                      */
 } cup2d_adjoint_objective;
 int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint_objective* obj,
                       const double* dt_in, double* dt_out, double* J, double* grad_u, double* grad_v,

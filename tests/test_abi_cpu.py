@@ -107,7 +107,7 @@ def test_header_compiles_as_c_and_matches_the_binding(tmp_path):
         "         sizeof(cup2d_shape_params), sizeof(cup2d_shape_state), offsetof(cup2d_config, iterative),\n"
         "         offsetof(cup2d_shape_state, forcex), offsetof(cup2d_config, gravity),\n"
         "         offsetof(cup2d_config, autotune), sizeof(cup2d_tuning), offsetof(cup2d_tuning, us),\n"
-        "         sizeof(cup2d_adjoint_objective), offsetof(cup2d_adjoint_objective, w_force));\n"
+        "         sizeof(cup2d_adjoint_objective), offsetof(cup2d_adjoint_objective, gait_step));\n"
         "  return 0;\n}\n")
     exe = tmp_path / "layout"
     r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
@@ -117,4 +117,4 @@ def test_header_compiles_as_c_and_matches_the_binding(tmp_path):
     assert got == [ctypes.sizeof(abi.Config), ctypes.sizeof(abi.ShapeParams), ctypes.sizeof(abi.ShapeState),
                    abi.Config.iterative.offset, abi.ShapeState.forcex.offset, abi.Config.gravity.offset,
                    abi.Config.autotune.offset, ctypes.sizeof(abi.Tuning), abi.Tuning.us.offset,
-                   ctypes.sizeof(abi.AdjointObjective), abi.AdjointObjective.w_force.offset]
+                   ctypes.sizeof(abi.AdjointObjective), abi.AdjointObjective.gait_step.offset]
