@@ -831,19 +831,23 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   double* tv = B.get<double>(n);
   if (!su || !sv || !sT || !sF || !pu || !pv || !lu || !lv || !l1 || !l2 || !tu || !tv)
     return adj_fail(ctx, CUP2D_ENOMEM, "adjoint segment buffers");
-  // each recomputed step's obstacle state: the shape (tile count, centre of
-  // mass, momenta), its tiles and the grid's chi
+  // a swimmer: each recomputed step's obstacle state (the shape's tile
+  // count and centre of mass, its tiles, the grid's chi); a disk's does not
+  // change from step to step, and the live one serves
   const ObstTiles live = c.tiles[0];
   const int cap = live.capacity;
   const size_t tb = (size_t)cap * BS2;
-  DevShape* shSnap = B.get<DevShape>(segN);
-  int* tlSnap = B.get<int>((size_t)cap * segN);
+  const bool keepObst = sf.kind != CUP2D_SHAPE_DISK;
+  const size_t segK = keepObst ? segN : 0;
+  DevShape* shSnap = B.get<DevShape>(segK);
+  int* tlSnap = B.get<int>((size_t)cap * segK);
   double* tSnap[6];
-  for (int q = 0; q < 6; q++) tSnap[q] = B.get<double>(tb * segN);   // chi, udx, udy, sD, sdx, sdy
-  double* chiSnap = B.get<double>(n * segN);
+  for (int q = 0; q < 6; q++) tSnap[q] = B.get<double>(tb * segK);   // chi, udx, udy, sD, sdx, sdy
+  double* chiSnap = B.get<double>(n * segK);
   if (!shSnap || !tlSnap || !chiSnap) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint obstacle snapshots");
   for (double* q : tSnap) if (!q) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint obstacle snapshots");
   auto tilesAt = [&](int j) {
+    if (!keepObst) return live;
     ObstTiles t = live;
     t.tiles = tlSnap + (size_t)j * cap;
     t.chi = tSnap[0] + j * tb; t.udx = tSnap[1] + j * tb; t.udy = tSnap[2] + j * tb;
@@ -868,7 +872,7 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
       ACK(cudaMemcpyAsync(sv + o, c.v(), nb, cudaMemcpyDeviceToDevice, c.stream));
       ARC(step(dts[i], sT + o, sF + o, gait ? su1 + o : nullptr, gait ? sv1 + o : nullptr));
       if (gait) ACK(cudaMemcpyAsync(sp + o, c.pres, nb, cudaMemcpyDeviceToDevice, c.stream));
-      {
+      if (keepObst) {
         const int j = i - i0;
         const ObstTiles t = tilesAt(j);
         ACK(cudaMemcpyAsync(shSnap + j, c.dshapes, sizeof(DevShape), cudaMemcpyDeviceToDevice, c.stream));
@@ -887,9 +891,9 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
     for (int i = i1 - 1; i >= i0; i--) {
       const size_t o = (size_t)(i - i0) * n;
       const double dt = dts[i];
-      const DevShape* shI = shSnap + (i - i0);          // the step's obstacle state
+      const DevShape* shI = keepObst ? shSnap + (i - i0) : c.dshapes;   // the step's obstacle state
       const ObstTiles tI = tilesAt(i - i0);
-      const double* chiI = chiSnap + o;
+      const double* chiI = keepObst ? chiSnap + o : c.chi;
       // the objective's terms of u^(i+1), p^(i+1) and the body velocity
       if (energy) k_adj_probe<<<probeGrid, 256, 0, c.stream>>>(g, bx, pu + o, pv + o, wE, nullptr, lu, lv);
       if (force)
