@@ -368,7 +368,7 @@ def dense_roofline(ctx, peak, peak_kind, workload, reps=30):
     return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": achieved / peak, "traffic": TRAFFIC_BYTES.get((workload, dom)),
             "algorithmic_bytes_per_launch": ALGO_BYTES_PER_CELL[dom] * cells,
-            "timing": "CUDA events around each launch, L2 flushed (256 MB write) before each",
+            "timing": "CUDA events around each launch, L2 flushed before each by reading a 256 MB buffer (clean lines: no write-back charged to the launch)",
             "kernels": per}
 
 

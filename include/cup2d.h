@@ -243,8 +243,10 @@ int cup2d_kernel_launches(const cup2d_ctx* ctx, long long* count);
  * `reps` times on the context's stream and returns the mean milliseconds of
  * one launch, each launch bracketed by its own CUDA events.  With flush_l2,
  * a 256 MB device buffer (allocated by the first such call, kept until
- * cup2d_destroy) is written before every launch, outside the events, so
- * that each launch reads its inputs from HBM, not from the 126 MB L2.  The
+ * cup2d_destroy) is read before every launch, outside the events, so that
+ * each launch reads its inputs from HBM, not from the 126 MB L2, and evicts
+ * only clean lines (a buffer written instead would leave the L2 dirty, and
+ * the timed launch would pay for writing it back).  The
  * kernels re-read and re-write the context's own buffers (the column pass,
  * for one, multiplies the spectrum by the Green's function at every launch),
  * so afterwards the fields hold no physical state: re-initialise the context
