@@ -69,15 +69,17 @@ __device__ __forceinline__ bool max_u_cta(const GridDesc& g, Scalars* sc,
     bad |= !isfinite(a2.x) || !isfinite(b2.x) || !isfinite(a2.y) || !isfinite(b2.y);
   };
   const size_t stride = (size_t)gridDim.x * blockDim.x;
-  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  for (; i + 3 * stride < n2; i += 4 * stride) {
+  // the last pass's loads are predicated rather than issued one at a
+  // time, so that the tail keeps four of them in flight too
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2; i += 4 * stride) {
     double2 a2[4], b2[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) { a2[q] = u2[i + q * stride]; b2[q] = v2[i + q * stride]; }
+    for (int q = 0; q < 4; q++)
+      if (i + q * stride < n2) { a2[q] = u2[i + q * stride]; b2[q] = v2[i + q * stride]; }
 #pragma unroll
-    for (int q = 0; q < 4; q++) take(a2[q], b2[q]);
+    for (int q = 0; q < 4; q++)
+      if (i + q * stride < n2) take(a2[q], b2[q]);
   }
-  for (; i < n2; i += stride) take(u2[i], v2[i]);
   m = block_max(m, red);
   const int anyBad = __syncthreads_or(bad);
   if (lin_tid() == 0) {
