@@ -277,6 +277,42 @@ def test_gait_gradient_matches_finite_differences(swimming, obj):
         assert abs(gg[q] - fd) <= 1e-5 * abs(fd) + 1e-7 * scale, (q, gg[q], fd)
 
 
+def test_gait_gradient_matches_reference_finite_differences(ref):
+    """The tethered swimmer from rest over 216 steps (its gait ramping up):
+    the amplitude and phase components against central differences of the
+    reference's own StefanFish (-amplitudeFactor, -phi) from the same
+    state with the same dt schedule (measured agreement ~4e-6)."""
+    from cubismup_2d_b200.synthetic import noise_field
+    n = 216
+    s = Simulation(TETHERED)
+    s.init()
+    r0 = ref.RefSim(TETHERED)
+    ic = {}
+    for comp, name in enumerate(("u", "v")):
+        ic[name] = r0.get(name) + 0.05 * noise_field(3, comp, r0.ny, r0.nx)
+        s.ctx.set(name, ic[name])
+    r0.close()
+    J, gu, gv, gb, dts, ms, gg = s.ctx.adjoint(n, every=24, gait=True, gait_step=1e-6, **DRAG)
+
+    def ref_J(extra):
+        r = ref.RefSim(TETHERED.replace("xvel=0.2'", "xvel=0.2 " + extra + "'"))
+        r.set("u", ic["u"])
+        r.set("v", ic["v"])
+        Jr = 0.0
+        for dt in dts:
+            r.set_time(r.time, r.step_id, dt)
+            r.advance()
+            Jr += r.shape(0)["forcex"]
+        r.close()
+        return Jr / n
+
+    assert abs(ref_J("") - J) <= 1e-12 * abs(J)
+    for q, key, base in ((0, "amplitudeFactor", 1.0), (1, "phi", 0.0)):
+        vp, vm = base + 1e-6, base - 1e-6
+        fd = (ref_J(f"{key}={vp!r}") - ref_J(f"{key}={vm!r}")) / (vp - vm)
+        assert abs(gg[q] - fd) <= 2e-5 * abs(fd), (key, gg[q], fd)
+
+
 def test_gait_set_round_trip(swimming):
     s, blob = swimming
     s.ctx.restore(blob)
