@@ -313,6 +313,26 @@ def test_gait_gradient_matches_reference_finite_differences(ref):
         assert abs(gg[q] - fd) <= 2e-5 * abs(fd), (key, gg[q], fd)
 
 
+def test_envelope_swimmer_gait():
+    """The envelope swimmer: amplitude and phase (it has no curvature
+    control values: their scales stay 1 and their gradient 0)."""
+    args = TETHERED.replace("stefanfish", "envelopefish")
+    s = Simulation(args)
+    s.init()
+    s.ctx.advance(1200)
+    s.ctx.sync()
+    blob = s.ctx.checkpoint()
+    theta = s.ctx.fish_gait(0)
+    with pytest.raises(Cup2DError):
+        s.ctx.set_fish_gait(0, [1, 0, 1.1, 1, 1, 1, 1, 1])
+    J, gu, gv, gb, dts, ms, gg = s.ctx.adjoint(NSTEPS, every=8, gait=True, gait_step=1e-6, **DRAG)
+    s.ctx.restore(blob)
+    assert np.all(gg[2:] == 0) and np.all(gg[:2] != 0)
+    for q in (0, 1):
+        fd = _fd_gait(s.ctx, blob, dts, DRAG, q, theta)
+        assert abs(gg[q] - fd) <= 1e-5 * abs(fd), (q, gg[q], fd)
+
+
 def test_gait_set_round_trip(swimming):
     s, blob = swimming
     s.ctx.restore(blob)
