@@ -162,18 +162,18 @@ struct StreamScope {
 // momentum integrals run side by side (the integrals evaluate the corrected
 // velocity of their own cells), then collisions and penalization.  The
 // integrals, the longer of the two, stay on the main stream.
-void launch_pressure_tail(Ctx& c) {
+void launch_pressure_tail(Ctx& c, bool maxNext) {
   const double* ui = c.u();
   const double* vi = c.v();
   if (c.nshapes == 0) {
-    launch_pcorr(c, c.graphStep);            // with the next step's findMaxU (graph steps)
+    launch_pcorr(c, maxNext);                // with the next step's findMaxU
     return;
   }
   cudaEventRecord(c.evPres, c.stream);
   cudaStreamWaitEvent(c.side2, c.evPres, 0);
   {
     StreamScope scope(c, c.side2);
-    launch_pcorr(c, c.graphStep);            // flips the current velocity buffer
+    launch_pcorr(c, maxNext);                // flips the current velocity buffer
   }
   cudaEventRecord(c.evMom, c.side2);
   launch_momenta(c, ui, vi);
@@ -246,8 +246,8 @@ void enqueue_step(Ctx& c) {
   cudaStreamWaitEvent(c.stream, c.evObjDone, 0);
   launch_rhs_obstacles(c);
   poisson_solve(c);
-  launch_pressure_tail(c);
-  launch_forces(c, c.forcesOut);
+  launch_pressure_tail(c, true);
+  launch_forces(c, c.forcesOut, true);
   if (anyAhead) cudaStreamWaitEvent(c.stream, c.evJoin, 0);
   launch_end_step_dt(c);                    // t += dt, and the next step's dt
 }
@@ -369,7 +369,7 @@ cudaError_t invalidate_dt_next(Ctx& c) {
 
 // An ABI call outside the operator sequence: the in-place RHS and the
 // placement mark no longer describe the state the next stage sees.
-void forget_chain(Ctx& c) { c.rhsFresh = false; c.placedPending = false; }
+void forget_chain(Ctx& c) { c.rhsFresh = false; c.placedPending = false; c.maxNextState = 0; }
 
 // PutObjectsOnGrid.cpp:195 and 149-184: uDef cleared, then every shape's
 // deformation velocity added where its chi is the grid's, from the tiles of
@@ -846,6 +846,7 @@ int cup2d_put_objects(cup2d_ctx* ctx, double dt) {
     launch_objects_rest(c);
     c.recordPlaced = false;
   }
+  if (c.nshapes == 0) CK(cudaMemsetAsync(&c.dsc->maxNext, 0, sizeof(double), c.stream));
   if (c.varRho) launch_invrho(c);            // PutObjectsOnGrid.cpp:65-73, 197
   if (c.cfg.iterative) {
     // PutObjectsOnGrid.cpp:195, 237-238: the grid's deformation velocity,
@@ -867,6 +868,9 @@ int cup2d_put_objects(cup2d_ctx* ctx, double dt) {
   }
   c.midByGraph = false;
   c.placedPending = c.nshapes > 0;
+  // k_obj_begin reset sc->maxNext: the next step's findMaxU may be formed by
+  // this step's own kernels (constant density, PressureSingle)
+  c.maxNextState = c.varRho || c.cfg.iterative ? 0 : 1;
   return check_launch(ctx);
 }
 
@@ -906,10 +910,12 @@ extern "C++" int pressure_single_keep(cup2d_ctx* ctx, double dt, double* keepDiv
   c.placedPending = false;
   if (c.varRho) {
     c.rhsFresh = false;
+    c.maxNextState = 0;
     return pressure_varrho(ctx);
   }
   if (c.cfg.iterative) {
     c.rhsFresh = false;
+    c.maxNextState = 0;
     return pressure_iterative(ctx);
   }
   if (!c.rhsFresh) launch_rhs_div(c);       // else formed by advDiff at this dt
@@ -919,7 +925,9 @@ extern "C++" int pressure_single_keep(cup2d_ctx* ctx, double dt, double* keepDiv
   launch_rhs_obstacles(c);
   if (keepObst) CK(cudaMemcpyAsync(keepObst, c.rhs, nb, cudaMemcpyDeviceToDevice, c.stream));
   poisson_solve(c);
-  launch_pressure_tail(c);
+  const bool maxNext = c.maxNextState == 1;  // reset by this step's placement
+  launch_pressure_tail(c, maxNext);
+  c.maxNextState = maxNext ? 2 : 0;
   return check_launch(ctx);
 }
 
@@ -955,8 +963,10 @@ int cup2d_poisson_solve(cup2d_ctx* ctx, int src, int dst) {
 
 int cup2d_compute_forces(cup2d_ctx* ctx, double dt) {
   STAGE_PROLOGUE
+  const bool maxNext = c.maxNextState == 2;  // after this step's pressure correction
   forget_chain(c);
-  launch_forces(c, c.mapDev->shapes);       // the final states also to mapped host memory
+  launch_forces(c, c.mapDev->shapes, maxNext);   // the final states also to mapped host memory
+  c.maxNextState = maxNext ? 3 : 0;
   CK(cudaEventRecord(c.evForces, c.stream));
   c.shapesMapped = true;
   return check_launch(ctx);
@@ -970,12 +980,17 @@ int cup2d_end_step(cup2d_ctx* ctx) {
   if (!ctx) return CUP2D_EINVAL;
   Ctx& c = ctx->c;
   if (!c.initialised) return fail(ctx, CUP2D_ESTATE, "not initialised");
+  // the step's own kernels formed the next findMaxU (placement, pressure
+  // correction, forces, nothing else in between): the maximum is exact in
+  // any order, so the dt is the one a full-grid findMaxU would give
+  const bool fused = c.maxNextState == 3;
   forget_chain(c);
   c.stateSeq++;
   // nothing from here on writes the shape states
   CK(cudaEventRecord(c.evShapes, c.stream));
   c.shapesAtEvent = true;
-  launch_end_step_max(c, &c.mapDev->dtNext);   // the next dt also to mapped host memory
+  if (fused) launch_end_step_dt(c, &c.mapDev->dtNext);   // the next dt also to mapped host memory
+  else launch_end_step_max(c, &c.mapDev->dtNext);
   CK(cudaEventRecord(c.evDtNext, c.stream));
   c.dtValidMaybe = c.dtCarried = true;
   return check_launch(ctx);

@@ -97,7 +97,15 @@ struct Ctx {
   //                the tiles of the last PutObjectsOnGrid: PressureSingle
   //                never reads it, so plain and graph steps leave it and
   //                cup2d_get_field fills it from the tiles on demand
+  //   maxNextState the next step's findMaxU formed by the operator path's
+  //                own kernels, as in a graph step: 1 sc->maxNext reset by
+  //                this step's PutObjectsOnGrid, 2 and the pressure
+  //                correction's part (the blocks outside the tiles) added, 3
+  //                and the force pass's part (the tiles, penalized) added --
+  //                the step end then takes dt from it instead of a full-grid
+  //                findMaxU; 0 otherwise (any other call in between)
   double devDt = 0.0;
+  int maxNextState = 0;
   bool dtValidMaybe = false, dtCarried = false, rhsFresh = false, placedPending = false;
   bool udefStale = false;
   bool shapesAtEvent = false;

@@ -36,16 +36,18 @@ __global__ void k_set_dt(Scalars* sc, double dt) { pdl_begin(); CUP2D_TRACE_SCOP
 // End of a step (Simulation.cpp:289-290): t += dt, step += 1, then the next step's
 // calcMaxTimestep from the maximum k_pcorr<true> and k_forces formed on the final velocity
 // (max is exact in any order: dtNext equals what k_max_u_dt would form).
-__global__ void k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh)
+__global__ void k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh, double* dtOut)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_ENDSTEP);
   const double m = sc->maxNext;
   sc->time += sc->dt;
   sc->step += 1;
-  sc->dtNext = dt_from_max_u(g, sc, sh, nsh, m);
+  const double dtn = dt_from_max_u(g, sc, sh, nsh, m);
+  sc->dtNext = dtn;
   sc->maxUNext = m;
   sc->dtNextValid = 1;
+  if (dtOut) *dtOut = dtn;                    // to mapped host memory
 }
 
 // End of an operator-by-operator step: findMaxU on the final velocity (its
@@ -553,8 +555,8 @@ void launch_take_dt_next(Ctx& c) {
   CUP2D_LAUNCHED(c);
 }
 
-void launch_end_step_dt(Ctx& c) {
-  launch_k(k_end_step_dt, 1, 1, 0, c.stream, c.g, c.dsc, c.dshapes, c.nshapes);
+void launch_end_step_dt(Ctx& c, double* dtOut) {
+  launch_k(k_end_step_dt, 1, 1, 0, c.stream, c.g, c.dsc, (const DevShape*)c.dshapes, c.nshapes, dtOut);
   CUP2D_LAUNCHED(c);
 }
 

@@ -46,7 +46,9 @@ int build_fade_slots(Ctx& c);                        // PoissonSolver.cpp:71-79,
 // PressureSingle.cpp:216-241; maxNext: with the next step's findMaxU over
 // the blocks outside every shape's tiles (graph steps)
 void launch_pcorr(Ctx& c, bool maxNext = false);
-void launch_end_step_dt(Ctx& c);                     // Simulation.cpp:289-290 + the next step's calcMaxTimestep
+// Simulation.cpp:289-290 + the next step's calcMaxTimestep from sc->maxNext
+// (also to dtOut: mapped host memory, or null)
+void launch_end_step_dt(Ctx& c, double* dtOut = nullptr);
 void launch_take_dt_next(Ctx& c);                    // calcMaxTimestep from the carried dt
 // findMaxU + Simulation.cpp:289-290 + the next dt (also to dtOut: mapped host memory, or null)
 void launch_end_step_max(Ctx& c, double* dtOut = nullptr);
@@ -79,7 +81,8 @@ struct PenalCtas;
 void launch_reldf(Ctx& c, const PenalCtas& nc);
 void launch_collide_penalize(Ctx& c);                // PressureSingle.cpp:69-108, 243-344
 // ComputeForces.cpp:16-111; out (mapped host memory, or null): each shape's final state
-void launch_forces(Ctx& c, cup2d_shape_state* out = nullptr);
+// maxNext: with the next step's findMaxU over the shapes' tiles
+void launch_forces(Ctx& c, cup2d_shape_state* out, bool maxNext);
 
 // poisson.cu
 struct Poisson;

@@ -32,7 +32,10 @@ k_obj_begin(GridDesc g, Scalars* sc, DevShape* sh, int nsh, AllTiles T, double* 
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_OBJBEGIN);
   clear_old_tiles(g, sh, nsh, T.t, chi, sdf, blockIdx.x, gridDim.x);
-  if (threadIdx.x == 0 && blockIdx.x == 0) bodies_motion(g, sc, sh, nsh);
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    sc->maxNext = 0.0;                        // the next step's findMaxU, formed by this step
+    bodies_motion(g, sc, sh, nsh);
+  }
 }
 
 // Fused start of a graph step: calcMaxTimestep's reduction (every CTA), the
@@ -868,11 +871,11 @@ void launch_collide_penalize(Ctx& c) {
   }
 }
 
-void launch_forces(Ctx& c, cup2d_shape_state* out) {
+void launch_forces(Ctx& c, cup2d_shape_state* out, bool maxNext) {
   if (c.nshapes == 0) return;
   const AllTiles T = all_tiles(c);
   launch_k(k_forces, dim3(tile_ctas(c, c.maxCapacity), c.nshapes), dim3(32, 32), 0, c.stream,
-      c.g, c.dsc, c.graphStep ? 1 : 0, c.dshapes, T, (const double*)c.u(), (const double*)c.v(),
+      c.g, c.dsc, maxNext ? 1 : 0, c.dshapes, T, (const double*)c.u(), (const double*)c.v(),
       (const double*)c.pres, shape_partials(c), (int)shape_region(c), c.counters + CNT_FORCES, out);
   CUP2D_LAUNCHED(c);
 }
