@@ -802,7 +802,7 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   }
 
   // backward
-  const size_t segN = (size_t)every;
+  const size_t segN = (size_t)std::min(every, nsteps);   // steps of a segment
   double* su = B.get<double>(n * segN);      // u^n of the segment's steps
   double* sv = B.get<double>(n * segN);
   double* sT = B.get<double>(n * segN);      // RHS before the obstacle terms

@@ -340,7 +340,8 @@ int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes);
  *    alone, each step's kept by the recomputation); anything else
  *    CUP2D_ENOTSUP;
  *  - the context ends in the forward's final state (as after nsteps
- *    steps); synchronises. */
+ *    steps), its gait as it was; synchronises.  After an error its state is
+ *    unspecified: load a checkpoint taken before the call. */
 typedef struct cup2d_adjoint_objective {
   double box[4];          /* the kinetic-energy probe: x0, x1, y0, y1      */
   double w_energy;        /* its weight (0: no energy term, box unused)    */
