@@ -333,6 +333,29 @@ def test_envelope_swimmer_gait():
         assert abs(gg[q] - fd) <= 1e-5 * abs(fd), (q, gg[q], fd)
 
 
+def test_gait_descent_lowers_drag(swimming):
+    """Steps against the gait gradient: a small one lowers the time-averaged
+    drag by alpha |grad|^2 (first order); a larger one (a few 1e-3 in theta)
+    still lowers it, though the raster's switches make the drag only
+    piecewise smooth in the gait (measured: 0.67 of the first-order
+    decrease)."""
+    s, blob = swimming
+    s.ctx.restore(blob)
+    theta = s.ctx.fish_gait(0)
+    J, gu, gv, gb, dts, ms, gg = s.ctx.adjoint(NSTEPS, every=8, gait=True, gait_step=1e-6, **DRAG)
+    n2 = float(np.sum(gg * gg))
+    for frac, check_first_order in ((1e-4, True), (3e-2, False)):
+        alpha = frac * abs(J) / n2
+        s.ctx.restore(blob)
+        s.ctx.set_fish_gait(0, theta - alpha * gg)
+        J2 = s.ctx.adjoint(NSTEPS, dt=dts, gradient=False, **DRAG)[0]
+        s.ctx.set_fish_gait(0, theta)
+        assert J2 < J, (frac, J, J2)
+        if check_first_order:
+            assert abs((J - J2) / (alpha * n2) - 1) < 1e-2, (J, J2, alpha * n2)
+    s.ctx.restore(blob)
+
+
 def test_gait_set_round_trip(swimming):
     s, blob = swimming
     s.ctx.restore(blob)
