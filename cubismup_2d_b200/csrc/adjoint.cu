@@ -29,6 +29,9 @@
 // linearizations need, then runs the segment's adjoint steps.  dt is frozen
 // (the forward's schedule, or one given): it is not differentiated.
 #include <algorithm>
+#include <array>
+#include <chrono>
+#include <thread>
 #include <cfloat>
 #include <cmath>
 #include <string>
@@ -669,6 +672,25 @@ AdvC adv_coef_host(const Ctx& c, double dt, double U0, double U1) {
   return k;
 }
 
+// Contexts of ctx's configuration and shapes, initialised, for the gait's
+// placement replays (one per perturbed gait, run side by side); kept in
+// ctx.  Returns false if they cannot be made (the replays then run one
+// after another on ctx itself).
+bool gait_shadows(cup2d_ctx* ctx, int n) {
+  Ctx& c = ctx->c;
+  while ((int)c.gaitShadows.size() < n) {
+    cup2d_ctx* sh = nullptr;
+    cup2d_config cfg = c.cfg;
+    if (cup2d_create(&cfg, &sh) != CUP2D_OK) return false;
+    bool ok = true;
+    for (size_t k = 0; ok && k < c.shapeParams.size(); k++)
+      ok = cup2d_add_shape(sh, c.shapeKinds[k], &c.shapeParams[k], nullptr) == CUP2D_OK;
+    if (!ok || cup2d_init(sh) != CUP2D_OK) { cup2d_destroy(sh); return false; }
+    c.gaitShadows.push_back(sh);
+  }
+  return true;
+}
+
 } // namespace
 
 extern "C" {
@@ -971,36 +993,61 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
     ARC(cup2d_fish_gait_get(ctx, 0, theta));
     const int np = sf.kind == CUP2D_SHAPE_STEFANFISH ? CUP2D_GAIT_PARAMS : 2;   // the envelope has no nodes
     const double eps = obj->gait_step > 0 ? obj->gait_step : 1e-7;
-    ACK(cudaEventRecord(e2, c.stream));
     for (int q = 0; q < CUP2D_GAIT_PARAMS; q++) grad_gait[q] = 0;
-    for (int q = 0; q < np; q++) {
-      double Cpm[2];
-      for (int sg = 0; sg < 2; sg++) {
-        ARC(cup2d_fish_gait_set(ctx, 0, theta));          // the checkpoints' gait
-        ALOAD(0);
-        double th[CUP2D_GAIT_PARAMS];
-        std::copy(theta, theta + CUP2D_GAIT_PARAMS, th);
-        th[q] += sg == 0 ? eps : -eps;
-        ARC(cup2d_fish_gait_set(ctx, 0, th));
-        ACK(cudaMemsetAsync(acc, 0, sizeof(double), c.stream));
-        for (int i = 0; i < nsteps; i++) {
-          ARC(cup2d_put_objects(ctx, dts[i]));
-          const size_t og = (size_t)i * n;
-          k_adj_geo_dot<<<tctas, dim3(32, 32), 0, c.stream>>>(g, c.dshapes, 0, c.tiles[0], c.chi, gG[0] + og,
-                                                             gG[1] + og, gG[2] + og, gG[3] + og, gG[4] + og, acc);
-          ACK(cudaGetLastError());
-          ARC(cup2d_end_step(ctx));
-        }
-        ACK(cudaMemcpyAsync(&Cpm[sg], acc, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-        ACK(cudaStreamSynchronize(c.stream));
+    // one replay: from the first checkpoint, with gait th, on context x
+    // (acc: its contraction, a device double of x's)
+    auto replay = [&](cup2d_ctx* x, const double* th, double* accx, double* out) -> int {
+      Ctx& cx = x->c;
+      if (cudaSetDevice(cx.device) != cudaSuccess) return CUP2D_ECUDA;
+      int rc = cup2d_fish_gait_set(x, 0, theta);        // the checkpoints' gait
+      if (!rc) rc = cup2d_checkpoint_load(x, ck[0], ckBytes);
+      if (!rc) rc = cup2d_fish_gait_set(x, 0, th);
+      if (rc) return rc;
+      if (cudaMemsetAsync(accx, 0, sizeof(double), cx.stream) != cudaSuccess) return CUP2D_ECUDA;
+      for (int i = 0; i < nsteps && !rc; i++) {
+        rc = cup2d_put_objects(x, dts[i]);
+        if (rc) break;
+        const size_t og = (size_t)i * n;
+        k_adj_geo_dot<<<tctas, dim3(32, 32), 0, cx.stream>>>(g, cx.dshapes, 0, cx.tiles[0], cx.chi, gG[0] + og,
+                                                            gG[1] + og, gG[2] + og, gG[3] + og, gG[4] + og, accx);
+        if (cudaGetLastError() != cudaSuccess) return CUP2D_ECUDA;
+        rc = cup2d_end_step(x);
       }
-      grad_gait[q] = (Cpm[0] - Cpm[1]) / (2 * eps);
+      if (rc) return rc;
+      if (cudaMemcpyAsync(out, accx, sizeof(double), cudaMemcpyDeviceToHost, cx.stream) != cudaSuccess ||
+          cudaStreamSynchronize(cx.stream) != cudaSuccess) return CUP2D_ECUDA;
+      return CUP2D_OK;
+    };
+    const int nrep = 2 * np;
+    std::vector<double> Cpm(nrep, 0.0);
+    std::vector<std::array<double, CUP2D_GAIT_PARAMS>> ths(nrep);
+    for (int j = 0; j < nrep; j++) {
+      std::copy(theta, theta + CUP2D_GAIT_PARAMS, ths[j].begin());
+      ths[j][j / 2] += j % 2 == 0 ? eps : -eps;
     }
-    ACK(cudaEventRecord(e1, c.stream));
-    ACK(cudaEventSynchronize(e1));
-    float gms = 0;
-    ACK(cudaEventElapsedTime(&gms, e2, e1));
-    if (ms) ms[2] = gms;
+    // side by side on contexts of this configuration, one host thread each
+    // (the replays are latency-bound: the midline and the frame are
+    // one-CTA kernels), else one after another on this context
+    double* accs = B.get<double>(nrep);
+    const bool side = accs && gait_shadows(ctx, nrep);   // (made on first use, not timed)
+    // host clock: the replays run on other contexts' streams
+    const auto t0 = std::chrono::steady_clock::now();
+    if (side) {
+      std::vector<int> rcs(nrep, CUP2D_OK);
+      std::vector<std::thread> pool;
+      for (int j = 0; j < nrep; j++)
+        pool.emplace_back([&, j] { rcs[j] = replay(c.gaitShadows[j], ths[j].data(), accs + j, &Cpm[j]); });
+      for (std::thread& t : pool) t.join();
+      for (int j = 0; j < nrep; j++)
+        if (rcs[j]) return adj_fail(ctx, rcs[j], std::string("gait replay: ") + c.gaitShadows[j]->c.err);
+    } else {
+      for (int j = 0; j < nrep; j++) {
+        const int rc = replay(ctx, ths[j].data(), acc, &Cpm[j]);
+        if (rc) return rc;
+      }
+    }
+    for (int q = 0; q < np; q++) grad_gait[q] = (Cpm[2 * q] - Cpm[2 * q + 1]) / (2 * eps);
+    if (ms) ms[2] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     ARC(cup2d_fish_gait_set(ctx, 0, theta));
   }
   ALOAD(nseg);

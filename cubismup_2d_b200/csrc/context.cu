@@ -517,6 +517,8 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
 int cup2d_destroy(cup2d_ctx* ctx) {
   if (!ctx) return CUP2D_OK;
   Ctx& c = ctx->c;
+  for (cup2d_ctx* sh : c.gaitShadows) cup2d_destroy(sh);
+  c.gaitShadows.clear();
   if (c.stream) cudaStreamSynchronize(c.stream);
   invalidate_graph(c);
   for (int b = 0; b < 2; b++) for (int d = 0; d < 2; d++) cudaFree(c.vel[b][d]);
@@ -688,6 +690,8 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
     CK(cudaStreamSynchronize(c.stream));
   }
   c.hshapes.push_back(S);
+  c.shapeParams.push_back(*p);
+  c.shapeKinds.push_back(kind);
   c.tiles.push_back(t);
   c.fish.push_back(F);
   if (id) *id = c.nshapes;

@@ -132,6 +132,13 @@ struct Ctx {
   // cub2rhs's fade (the adjoint applies the fade's transpose itself)
   bool solveNoFade = false;
 
+  // the shape descriptors as given to cup2d_add_shape, and contexts of the
+  // same configuration kept for the adjoint's gait replays (created on
+  // first use, destroyed with this context)
+  std::vector<cup2d_shape_params> shapeParams;
+  std::vector<int> shapeKinds;
+  std::vector<struct cup2d_ctx*> gaitShadows;
+
   cudaGraphExec_t graph = nullptr;
   void* flushBuf = nullptr;      // cup2d_time_kernel's L2 flush (256 MB, allocated on demand)
   unsigned long long* hashAcc = nullptr;   // checkpoint checksum accumulator (on demand)

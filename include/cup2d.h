@@ -328,7 +328,10 @@ int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes);
  *    differentiated (a frozen schedule);
  *  - ms (2 values, 3 with grad_gait, or null): device time of the forward
  *    (with its checkpoints), of the backward (recomputation and transposed
- *    steps), and of the gait's placement replays;
+ *    steps), and host time of the gait's placement replays (run side by
+ *    side on contexts of the same configuration, made on the first call and
+ *    kept until cup2d_destroy; one after another on ctx if they cannot be
+ *    made);
  *  - covered: FP64, any of the three solvers, explicit penalization
  *    without the iterated or variable-density pipelines, one disk fixed on
  *    the grid (bFixed: its chi does not move; the lab velocity is minus the
