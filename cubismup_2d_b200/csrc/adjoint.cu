@@ -1,7 +1,9 @@
 // Discrete adjoint of the step (no counterpart in the reference): the
-// gradient of a time-averaged kinetic energy in a probe box with respect to
-// the initial velocity field, for a body whose motion does not depend on
-// the flow (forced in x, y and angle, fixed on the grid: chi is constant).
+// gradient of a time-averaged objective (kinetic energy in a probe box, the
+// body's force, the body's velocity) with respect to the initial velocity
+// field, the body's velocity and, for a tethered swimmer, its gait, for a
+// body held on the grid (bFixed): a disk forced or free, or a curvature
+// swimmer forced in x, y and angle (its chi moves with its gait alone).
 //
 // The step u^n -> u^(n+1) (operator order of Simulation::advance):
 //   u1 = A(u^n)             advDiff with its inflow fades and outflow
@@ -11,8 +13,11 @@
 //   b  = F(f)               the boundary-strip fade (PoissonSolver.cpp:61-118)
 //   p  = K b                the Poisson convolution
 //   u2 = u1 - (dt/2h) G p   pressureCorrection (PressureSingle.cpp:216-241)
-//   u^(n+1) = Pen(u2)       penalize (PressureSingle.cpp:69-108)
-// with the body velocity forced.  A, O and F are nonlinear; each is
+//   U_b = A^-1 b(u2)        a free body: integrateMomenta + updateVelocity
+//                           (PressureSingle.cpp:23-67, Shape.cpp:25-59)
+//   u^(n+1) = Pen(u2, U_b)  penalize (PressureSingle.cpp:69-108)
+//   F^n = forces(u, p)      ComputeForces (ComputeForces.cpp:16-111)
+// with U_b held for a forced body.  A, O and F are nonlinear; each is
 // linearized about the forward values of its step (O and F are piecewise
 // linear in their input: the linearization is the active piece, with the
 // rank-one terms of their sign-selected corrections).  The backward step
@@ -26,15 +31,18 @@
 // The forward is stored as checkpoints (the context's own checkpoint blob,
 // kept in device memory) every `every` steps; the backward recomputes each
 // segment forward from its checkpoint, keeping the values the
-// linearizations need, then runs the segment's adjoint steps.  dt is frozen
-// (the forward's schedule, or one given): it is not differentiated.
+// linearizations need (and, for a swimmer, each step's obstacle tiles),
+// then runs the segment's adjoint steps.  dt is frozen (the forward's
+// schedule, or one given): it is not differentiated.  The gait gradient
+// contracts each step's sensitivity to the body's geometry with central
+// differences of the placement (see k_adj_geo_pen).
 #include <algorithm>
 #include <array>
-#include <chrono>
-#include <thread>
 #include <cfloat>
+#include <chrono>
 #include <cmath>
 #include <string>
+#include <thread>
 #include <vector>
 #include "context.hpp"
 #include "rigid_body.cuh"
