@@ -590,6 +590,24 @@ k_adj_advdiff(GridDesc g, AdvC k, const double* __restrict__ u, const double* __
   }
 }
 
+// ---- the recomputation's copies, one launch for many regions ------------
+constexpr int MAX_COPIES = 16;
+struct CopyList {
+  const unsigned* src[MAX_COPIES];
+  unsigned* dst[MAX_COPIES];
+  size_t words[MAX_COPIES];                       // 4-byte words
+  int n;
+};
+static_assert(sizeof(DevShape) % 4 == 0, "the shape snapshot is copied in 4-byte words");
+__global__ void __launch_bounds__(256) k_copy_many(CopyList L) {
+  for (int q = 0; q < L.n; q++) {
+    const unsigned* __restrict__ a = L.src[q];
+    unsigned* __restrict__ b = L.dst[q];
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < L.words[q]; i += (size_t)gridDim.x * blockDim.x)
+      b[i] = a[i];
+  }
+}
+
 // ---- the objective: (1/N) sum over steps of (h^2/2) sum_box (u^2 + v^2) ---
 struct ProbeBox { int x0, x1, y0, y1; };
 __global__ void __launch_bounds__(256)
@@ -833,13 +851,14 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
 
   // backward
   const size_t segN = (size_t)std::min(every, nsteps);   // steps of a segment
-  double* su = B.get<double>(n * segN);      // u^n of the segment's steps
-  double* sv = B.get<double>(n * segN);
+  // the velocity at the segment's start and after each of its steps (u^n of
+  // step j > 0 is u^(n+1) of step j - 1)
+  double* su = B.get<double>(n);
+  double* sv = B.get<double>(n);
   double* sT = B.get<double>(n * segN);      // RHS before the obstacle terms
   double* sF = B.get<double>(n * segN);      // RHS before the fade
-  const bool keepNext = energy || gait;
-  double* pu = keepNext ? B.get<double>(n * segN) : sv;   // u^(n+1) (the energy term, the gait)
-  double* pv = keepNext ? B.get<double>(n * segN) : sv;
+  double* pu = B.get<double>(n * segN);
+  double* pv = B.get<double>(n * segN);
   // the gait: advDiff's velocity and the pressure of each step, and the
   // geometry sensitivities of every step of the run
   double* su1 = gait ? B.get<double>(n * segN) : nullptr;
@@ -896,27 +915,34 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   for (int s = nseg - 1; s >= 0; s--) {
     const int i0 = s * every, i1 = std::min(nsteps, i0 + every);
     ALOAD(s);
+    ACK(cudaMemcpyAsync(su, c.u(), nb, cudaMemcpyDeviceToDevice, c.stream));
+    ACK(cudaMemcpyAsync(sv, c.v(), nb, cudaMemcpyDeviceToDevice, c.stream));
     for (int i = i0; i < i1; i++) {
       const size_t o = (size_t)(i - i0) * n;
-      ACK(cudaMemcpyAsync(su + o, c.u(), nb, cudaMemcpyDeviceToDevice, c.stream));
-      ACK(cudaMemcpyAsync(sv + o, c.v(), nb, cudaMemcpyDeviceToDevice, c.stream));
       ARC(step(dts[i], sT + o, sF + o, gait ? su1 + o : nullptr, gait ? sv1 + o : nullptr));
-      if (gait) ACK(cudaMemcpyAsync(sp + o, c.pres, nb, cudaMemcpyDeviceToDevice, c.stream));
+      // what the step leaves, in one launch
+      CopyList L{};
+      auto add = [&](const void* src, void* dst, size_t bytes) {
+        L.src[L.n] = static_cast<const unsigned*>(src);
+        L.dst[L.n] = static_cast<unsigned*>(dst);
+        L.words[L.n] = bytes / 4;
+        L.n++;
+      };
+      add(c.u(), pu + o, nb);
+      add(c.v(), pv + o, nb);
+      if (gait) add(c.pres, sp + o, nb);
       if (keepObst) {
         const int j = i - i0;
         const ObstTiles t = tilesAt(j);
-        ACK(cudaMemcpyAsync(shSnap + j, c.dshapes, sizeof(DevShape), cudaMemcpyDeviceToDevice, c.stream));
-        ACK(cudaMemcpyAsync(t.tiles, live.tiles, sizeof(int) * cap, cudaMemcpyDeviceToDevice, c.stream));
+        add(c.dshapes, shSnap + j, sizeof(DevShape));
+        add(live.tiles, t.tiles, sizeof(int) * cap);
         const double* src[6] = {live.chi, live.udx, live.udy, live.sD, live.sdx, live.sdy};
         double* dst[6] = {t.chi, t.udx, t.udy, t.sD, t.sdx, t.sdy};
-        for (int q = 0; q < 6; q++)
-          ACK(cudaMemcpyAsync(dst[q], src[q], sizeof(double) * tb, cudaMemcpyDeviceToDevice, c.stream));
-        ACK(cudaMemcpyAsync(chiSnap + o, c.chi, nb, cudaMemcpyDeviceToDevice, c.stream));
+        for (int q = 0; q < 6; q++) add(src[q], dst[q], sizeof(double) * tb);
+        add(c.chi, chiSnap + o, nb);
       }
-      if (keepNext) {
-        ACK(cudaMemcpyAsync(pu + o, c.u(), nb, cudaMemcpyDeviceToDevice, c.stream));
-        ACK(cudaMemcpyAsync(pv + o, c.v(), nb, cudaMemcpyDeviceToDevice, c.stream));
-      }
+      k_copy_many<<<2 * c.sms, 256, 0, c.stream>>>(L);
+      ACK(cudaGetLastError());
     }
     for (int i = i1 - 1; i >= i0; i--) {
       const size_t o = (size_t)(i - i0) * n;
@@ -973,7 +999,9 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
       k_adj_adv_gamma<<<std::min(148, (2 * (g.nx + g.ny) + 255) / 256), 256, 0, c.stream>>>(g, lu, lv, acc);
       // (a free body: its previous velocity set the lab velocity of this
       // step; a forced one: its held velocity, accumulated)
-      k_adj_advdiff<<<grid2, blk2, 0, c.stream>>>(g, adv_coef_host(c, dt, U0s[i], U1s[i]), su + o, sv + o,
+      const double* un0 = i == i0 ? su : pu + o - n;     // u^n of the step
+      const double* vn0 = i == i0 ? sv : pv + o - n;
+      k_adj_advdiff<<<grid2, blk2, 0, c.stream>>>(g, adv_coef_host(c, dt, U0s[i], U1s[i]), un0, vn0,
                                                  lu, lv, acc, tu, tv, freeBody ? lxPrev : lx);
       ACK(cudaGetLastError());
       std::swap(lu, tu);
