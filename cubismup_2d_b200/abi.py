@@ -51,7 +51,7 @@ KERNELS = {"advdiff": 0, "rhs_div": 1, "pcorr": 2, "fft_rows_fwd": 3, "fft_cols"
 
 class AdjointObjective(ctypes.Structure):
     _fields_ = [("box", ctypes.c_double * 4), ("w_energy", ctypes.c_double), ("w_force", ctypes.c_double * 2),
-                ("w_body", ctypes.c_double * 3), ("gait_step", ctypes.c_double)]
+                ("w_body", ctypes.c_double * 3), ("w_torque", ctypes.c_double), ("gait_step", ctypes.c_double)]
 
 
 class Config(ctypes.Structure):
@@ -425,10 +425,10 @@ class Context:
         self._ck(self.L.cup2d_fish_gait_set(self.h_, k, _dp(a)))
 
     def adjoint(self, nsteps, box=None, every=20, dt=None, gradient=True, w_energy=1.0, w_force=(0.0, 0.0),
-                w_body=(0.0, 0.0, 0.0), gait=False, gait_step=0.0):
+                w_body=(0.0, 0.0, 0.0), w_torque=0.0, gait=False, gait_step=0.0):
         """The time-averaged objective over nsteps steps from the current state,
         J = (1/nsteps) sum_n [w_energy (h^2/2) sum_box (u^2 + v^2) + w_force . force
-        + w_body . (u_b, v_b, omega)] (box = (x0, x1, y0, y1) in domain units;
+        + w_torque |torque| + w_body . (u_b, v_b, omega)] (box = (x0, x1, y0, y1) in domain units;
         force = ComputeForces' (forcex, forcey) on the body), and its gradient
         with respect to the current velocity and to the body's velocity (u_b,
         v_b, omega: a forced body's held one, a free body's initial one) by the discrete adjoint
@@ -450,6 +450,7 @@ class Context:
         for k in range(3):
             obj.w_body[k] = float(w_body[k])
         obj.gait_step = float(gait_step)
+        obj.w_torque = float(w_torque)
         dts = np.empty(nsteps, dtype=np.float64)
         dti = None if dt is None else np.ascontiguousarray(dt, dtype=np.float64)
         if dti is not None and dti.size != nsteps:

@@ -192,14 +192,16 @@ __global__ void k_adj_add3(double* lx, double a, double b, double c)
 // ---- the body's force (ComputeForces.cpp:16-111, the surface cells of
 // k_forces): forcex = sum over cells with a surface delta of
 //   nu/h [ (u_E - u_W) nx + (u_N - u_S + v_E - v_W) ny / 2 ] - p nx
-// and forcey alike, linear in u, v and p with clamped neighbours.  With
-// weights (wx, wy) on (forcex, forcey): part 0 adds the velocity terms'
+// and forcey alike, and the torque sum p_x fy - p_y fx about the centre of
+// mass, linear in u, v and p with clamped neighbours.  With weights (wx, wy,
+// wt) on (forcex, forcey, torque): part 0 adds the velocity terms'
 // transpose to (lu, lv), part 1 the pressure term's to lp.
 __global__ void __launch_bounds__(1024)
-k_adj_force(GridDesc g, const DevShape* sh, int k, ObstTiles t, double wx, double wy, int part,
+k_adj_force(GridDesc g, const DevShape* sh, int k, ObstTiles t, double wx, double wy, double wt, int part,
             double* lu, double* lv, double* lp)
 {
   const DevShape& S = sh[k];
+  const double Cx = S.s.com[0], Cy = S.s.com[1];
   for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
     const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
     const size_t o = (size_t)s * BS2 + threadIdx.y * BS + threadIdx.x;
@@ -207,14 +209,16 @@ k_adj_force(GridDesc g, const DevShape* sh, int k, ObstTiles t, double wx, doubl
     const int gx = bx * BS + threadIdx.x, gy = by * BS + threadIdx.y;
     const Nb j = nb_of(g, gx, gy);
     const double nX = t.sdx[o], nY = t.sdy[o];
+    // torque = sum p_x fy - p_y fx about the centre of mass (weight wt)
+    const double P0 = cell_x(g, bx, threadIdx.x) - Cx, P1 = cell_y(g, by, threadIdx.y) - Cy;
     if (part == 1) {
-      atomicAdd(&lp[j.c], -(wx * nX + wy * nY));
+      atomicAdd(&lp[j.c], -(wx * nX + wy * nY) + wt * (P1 * nX - P0 * nY));
       continue;
     }
     const double NUoH = g.nu / g.h;
-    const double a = wx * NUoH * nX;                     // on u_E - u_W
-    const double q = (wx * nY + wy * nX) * NUoH / 2;     // on u_N - u_S and on v_E - v_W
-    const double d = wy * NUoH * nY;                     // on v_N - v_S
+    const double a = (wx - wt * P1) * nX * NUoH;                              // on u_E - u_W
+    const double q = (wx * nY + wy * nX + wt * (P0 * nX - P1 * nY)) * NUoH / 2;  // on u_N - u_S, v_E - v_W
+    const double d = (wy + wt * P0) * nY * NUoH;                              // on v_N - v_S
     atomicAdd(&lu[j.E], a); atomicAdd(&lu[j.W], -a);
     atomicAdd(&lu[j.N], q); atomicAdd(&lu[j.S], -q);
     atomicAdd(&lv[j.E], q); atomicAdd(&lv[j.W], -q);
@@ -222,13 +226,14 @@ k_adj_force(GridDesc g, const DevShape* sh, int k, ObstTiles t, double wx, doubl
   }
 }
 
-// the objective's body terms of a step: acc += wx forcex + wy forcey + wb .
-// (u, v, omega) of the state the step left
-__global__ void k_adj_body_sum(const DevShape* sh, int k, double wx, double wy, double wb0, double wb1,
-                               double wb2, double* acc)
+// the objective's body terms of a step: acc += wx forcex + wy forcey + wt
+// |torque| + wb . (u, v, omega) of the state the step left; *tau = torque
+__global__ void k_adj_body_sum(const DevShape* sh, int k, double wx, double wy, double wt, double wb0,
+                               double wb1, double wb2, double* acc, double* tau)
 {
   const cup2d_shape_state& s = sh[k].s;
-  *acc += wx * s.forcex + wy * s.forcey + (wb0 * s.u + wb1 * s.v + wb2 * s.omega);
+  *acc += wx * s.forcex + wy * s.forcey + wt * fabs(s.torque) + (wb0 * s.u + wb1 * s.v + wb2 * s.omega);
+  *tau = s.torque;
 }
 
 // ---- the obstacle RHS terms O (k_rhs_obst, k_rhs_corr) --------------------
@@ -316,17 +321,23 @@ k_adj_obst_apply(GridDesc g, const DevShape* sh, int k, ObstTiles t, const doubl
 //
 // Penalization and forces, from lambda on u^(n+1) (before Pen^T):
 // d u^(n+1)/d chi = U_s - u2, d u^(n+1)/d U_s = chi; forcex = sum nu/h [(u_E -
-// u_W) sdx + (u_N - u_S + v_E - v_W) sdy / 2] - p sdx, forcey alike.
+// u_W) sdx + (u_N - u_S + v_E - v_W) sdy / 2] - p sdx, forcey alike, the
+// torque sum p_x fy - p_y fx about the centre of mass C (gCom: d/dC).
 __global__ void __launch_bounds__(1024)
 k_adj_geo_pen(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
               const double* __restrict__ u1, const double* __restrict__ v1, const double* __restrict__ p,
               double pFac, const double* __restrict__ un, const double* __restrict__ vn,
-              const double* __restrict__ lu, const double* __restrict__ lv, double wFx, double wFy,
-              double* gX, double* gU, double* gV, double* gSX, double* gSY)
+              const double* __restrict__ lu, const double* __restrict__ lv, double wFx, double wFy, double wt,
+              double* gX, double* gU, double* gV, double* gSX, double* gSY, double* gCom)
 {
   const DevShape& S = sh[k];
   const double Cx = S.s.com[0], Cy = S.s.com[1];
   const double NUoH = g.nu / g.h;
+  // the torque about the centre of mass: d/dC = (-forcey, forcex)
+  if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
+    gCom[0] = -wt * S.s.forcey;
+    gCom[1] = wt * S.s.forcex;
+  }
   for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
     const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
     const size_t o = (size_t)s * BS2 + threadIdx.y * BS + threadIdx.x;
@@ -346,8 +357,8 @@ k_adj_geo_pen(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* 
     const double D11 = NUoH * (un[j.E] - un[j.W]), D22 = NUoH * (vn[j.N] - vn[j.S]);
     const double D12 = NUoH / 2 * (un[j.N] - un[j.S] + vn[j.E] - vn[j.W]);
     const double P = p[j.c];
-    gSX[j.c] = wFx * (D11 - P) + wFy * D12;
-    gSY[j.c] = wFx * D12 + wFy * (D22 - P);
+    gSX[j.c] = wFx * (D11 - P) + wFy * D12 + wt * (p0 * D12 - p1 * (D11 - P));
+    gSY[j.c] = wFx * D12 + wFy * (D22 - P) + wt * (p0 * (D22 - P) - p1 * D12);
   }
 }
 
@@ -383,15 +394,18 @@ k_adj_geo_obst(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double*
 }
 
 // <g, geometry> over the tiles of the current placement (the replay of a
-// perturbed gait): acc += sum gX chi + gU U_s + gV V_s + gSX sdx + gSY sdy
+// perturbed gait): acc += sum gX chi + gU U_s + gV V_s + gSX sdx + gSY sdy,
+// plus gCom . C
 __global__ void __launch_bounds__(1024)
 k_adj_geo_dot(GridDesc g, const DevShape* sh, int k, ObstTiles t, const double* __restrict__ chig,
               const double* __restrict__ gX, const double* __restrict__ gU, const double* __restrict__ gV,
-              const double* __restrict__ gSX, const double* __restrict__ gSY, double* acc)
+              const double* __restrict__ gSX, const double* __restrict__ gSY, const double* __restrict__ gCom,
+              double* acc)
 {
   const DevShape& S = sh[k];
   const double Cx = S.s.com[0], Cy = S.s.com[1];
   double a = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) a = gCom[0] * Cx + gCom[1] * Cy;
   for (int s = blockIdx.x; s < S.ntiles; s += gridDim.x) {
     const int b = t.tiles[s], bx = b % g.bpdx, by = b / g.bpdx;
     const size_t o = (size_t)s * BS2 + threadIdx.y * BS + threadIdx.x;
@@ -757,7 +771,7 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   }
   const size_t n = c.ncells(), nb = sizeof(double) * n;
   const bool energy = obj->w_energy != 0;
-  const bool force = obj->w_force[0] != 0 || obj->w_force[1] != 0;
+  const bool force = obj->w_force[0] != 0 || obj->w_force[1] != 0 || obj->w_torque != 0;
   const bool bodyTerm = obj->w_body[0] != 0 || obj->w_body[1] != 0 || obj->w_body[2] != 0;
   ProbeBox bx{0, 0, 0, 0};
   if (energy) {
@@ -766,7 +780,7 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
     if (bx.x1 <= bx.x0 || bx.y1 <= bx.y0) return adj_fail(ctx, CUP2D_EINVAL, "empty probe box");
   }
   const double wE = obj->w_energy * g.h * g.h / nsteps;   // the energy term's weight per step
-  const double wFx = obj->w_force[0] / nsteps, wFy = obj->w_force[1] / nsteps;
+  const double wFx = obj->w_force[0] / nsteps, wFy = obj->w_force[1] / nsteps, wT = obj->w_torque / nsteps;
   const double wB[3] = {obj->w_body[0] / nsteps, obj->w_body[1] / nsteps, obj->w_body[2] / nsteps};
   const dim3 grid2(g.bpdx, g.bpdy), blk2(32, 8);
   const int probeGrid = energy ? std::min(1024, ((bx.x1 - bx.x0) * (bx.y1 - bx.y0) + 255) / 256) : 1;
@@ -784,7 +798,8 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   // velocity); [4..6] a free body's adjoint of the previous output, formed
   // by advDiff's lab velocity; [8..10] the solve's transpose
   double* obv = B.get<double>(12);
-  if (!acc || !obv) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint scratch");
+  double* tauRec = B.get<double>(nsteps);    // each step's torque (the |torque| term's sign)
+  if (!acc || !obv || !tauRec) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint scratch");
   std::vector<double> dts(nsteps), U0s(nsteps), U1s(nsteps);
   struct Ev {
     cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
@@ -825,7 +840,7 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
     U0s[i] = ux; U1s[i] = uy;
     if (energy) k_adj_probe<<<probeGrid, 256, 0, c.stream>>>(g, bx, c.u(), c.v(), wE, obv, nullptr, nullptr);
     if (force || bodyTerm)
-      k_adj_body_sum<<<1, 1, 0, c.stream>>>(c.dshapes, 0, wFx, wFy, wB[0], wB[1], wB[2], obv);
+      k_adj_body_sum<<<1, 1, 0, c.stream>>>(c.dshapes, 0, wFx, wFy, wT, wB[0], wB[1], wB[2], obv, tauRec + i);
     ACK(cudaGetLastError());
   }
   ACK(cudaEventRecord(e1, c.stream));
@@ -839,7 +854,11 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
       return adj_fail(ctx, CUP2D_ENOTSUP, "the body is released (timeForced) within the run");
   }
   ACK(cudaMemcpyAsync(J, obv, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  std::vector<double> taus(nsteps, 0.0), wTs(nsteps, 0.0);
+  if (force || bodyTerm)
+    ACK(cudaMemcpyAsync(taus.data(), tauRec, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, c.stream));
   ACK(cudaStreamSynchronize(c.stream));
+  for (int i = 0; i < nsteps; i++) wTs[i] = taus[i] > 0 ? wT : (taus[i] < 0 ? -wT : 0.0);   // d|torque|
   if (dt_out) std::copy(dts.begin(), dts.end(), dt_out);
   float fms = 0;
   ACK(cudaEventElapsedTime(&fms, e0, e1));
@@ -865,7 +884,10 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
   double* sv1 = gait ? B.get<double>(n * segN) : nullptr;
   double* sp = gait ? B.get<double>(n * segN) : nullptr;
   double* gG[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};   // gX, gU, gV, gSX, gSY
+  double* gCom = gait ? B.get<double>(2 * (size_t)nsteps) : nullptr;  // d/d(centre of mass)
   if (gait) {
+    if (!gCom) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint gait planes");
+    ACK(cudaMemsetAsync(gCom, 0, sizeof(double) * 2 * nsteps, c.stream));
     for (double*& q : gG) {
       if (!(q = B.get<double>(n * (size_t)nsteps))) return adj_fail(ctx, CUP2D_ENOMEM, "adjoint gait planes");
       ACK(cudaMemsetAsync(q, 0, nb * nsteps, c.stream));
@@ -953,13 +975,13 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
       // the objective's terms of u^(i+1), p^(i+1) and the body velocity
       if (energy) k_adj_probe<<<probeGrid, 256, 0, c.stream>>>(g, bx, pu + o, pv + o, wE, nullptr, lu, lv);
       if (force)
-        k_adj_force<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, wFx, wFy, 0, lu, lv, nullptr);
+        k_adj_force<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, wFx, wFy, wTs[i], 0, lu, lv, nullptr);
       if (bodyTerm) k_adj_add3<<<1, 1, 0, c.stream>>>(lx, wB[0], wB[1], wB[2]);
       if (gait) {
         const size_t og = (size_t)i * n;
         k_adj_geo_pen<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, chiI, su1 + o, sv1 + o, sp + o,
-            -0.5 * dt / g.h, pu + o, pv + o, lu, lv, wFx, wFy, gG[0] + og, gG[1] + og, gG[2] + og, gG[3] + og,
-            gG[4] + og);
+            -0.5 * dt / g.h, pu + o, pv + o, lu, lv, wFx, wFy, wTs[i], gG[0] + og, gG[1] + og, gG[2] + og,
+            gG[3] + og, gG[4] + og, gCom + 2 * (size_t)i);
       }
       // penalization
       k_adj_pen<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, chiI, lu, lv, lx);
@@ -972,7 +994,7 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
       // pressure correction: lambda_p, the force's pressure term, then the convolution
       k_adj_grad_T<<<grid2, blk2, 0, c.stream>>>(g, -0.5 * dt / g.h, lu, lv, l1);
       if (force)
-        k_adj_force<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, wFx, wFy, 1, nullptr, nullptr, l1);
+        k_adj_force<<<tctas, dim3(32, 32), 0, c.stream>>>(g, shI, 0, tI, wFx, wFy, wTs[i], 1, nullptr, nullptr, l1);
       ACK(cudaGetLastError());
       {
         double* const R = c.rhs;
@@ -1045,7 +1067,8 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
         if (rc) break;
         const size_t og = (size_t)i * n;
         k_adj_geo_dot<<<tctas, dim3(32, 32), 0, cx.stream>>>(g, cx.dshapes, 0, cx.tiles[0], cx.chi, gG[0] + og,
-                                                            gG[1] + og, gG[2] + og, gG[3] + og, gG[4] + og, accx);
+                                                            gG[1] + og, gG[2] + og, gG[3] + og, gG[4] + og,
+                                                            gCom + 2 * (size_t)i, accx);
         if (cudaGetLastError() != cudaSuccess) return CUP2D_ECUDA;
         rc = cup2d_end_step(x);
       }

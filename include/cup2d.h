@@ -304,6 +304,7 @@ int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes);
  * current state and returns the time-averaged objective
  *   J = (1/nsteps) sum_{n=1..nsteps} [ w_energy (h^2/2) sum_box (u^2 + v^2)
  *                                      + w_force . (forcex, forcey)
+ *                                      + w_torque |torque|
  *                                      + w_body . (u_b, v_b, omega) ]
  * of each step's final velocity, ComputeForces' force on the body and the
  * body's velocity
@@ -350,6 +351,7 @@ typedef struct cup2d_adjoint_objective {
   double w_energy;        /* its weight (0: no energy term, box unused)    */
   double w_force[2];      /* weights of the body's forcex and forcey       */
   double w_body[3];       /* weights of the body's velocity u, v, omega    */
+  double w_torque;        /* weight of |torque| (ComputeForces' torque)    */
   double gait_step;       /* the gait gradient's central-difference step   */
                           /* of the placement (0: 1e-7); the forward is     */
                           /* piecewise smooth (raster switches), so a      */

@@ -333,6 +333,38 @@ def test_envelope_swimmer_gait():
         assert abs(gg[q] - fd) <= 1e-5 * abs(fd), (q, gg[q], fd)
 
 
+# the benchmark's adjoint objective on a held swimmer: its drag (the thrust
+# it would swim with, negated) and 0.1 of its mean |torque|
+THRUST_TORQUE = dict(box=None, w_force=(1.0, 0.0), w_torque=0.1)
+
+
+def test_torque_objective_gradient(swimming):
+    """The |torque| term: the field gradient and the gait gradient (the
+    torque's surface normals and its centre of mass) against central
+    differences."""
+    s, blob = swimming
+    s.ctx.restore(blob)
+    theta = s.ctx.fish_gait(0)
+    J, gu, gv, gb, dts, ms, gg = s.ctx.adjoint(NSTEPS, every=8, gait=True, gait_step=1e-6, **THRUST_TORQUE)
+    s.ctx.restore(blob)
+    Jp = 0.0
+    for dt in dts:
+        s.advance(dt)
+        st = s.ctx.shape(0)
+        Jp += st["forcex"] + 0.1 * abs(st["torque"])
+    assert abs(J - Jp / NSTEPS) <= 1e-12 * abs(J), (J, Jp / NSTEPS)
+    s.ctx.restore(blob)
+    for where in ("body", "wake"):
+        du, dv = _bump(s.ctx, where)
+        ad = float(np.sum(gu * du) + np.sum(gv * dv))
+        fd = _fd(s.ctx, blob, dts, THRUST_TORQUE, du, dv)
+        assert abs(ad - fd) <= 1e-5 * abs(fd), (where, ad, fd)
+    scale = np.max(np.abs(gg))
+    for q in range(8):
+        fd = _fd_gait(s.ctx, blob, dts, THRUST_TORQUE, q, theta)
+        assert abs(gg[q] - fd) <= 1e-5 * abs(fd) + 1e-7 * scale, (q, gg[q], fd)
+
+
 def test_gait_descent_lowers_drag(swimming):
     """Steps against the gait gradient: a small one lowers the time-averaged
     drag by alpha |grad|^2 (first order); a larger one (a few 1e-3 in theta)
