@@ -413,8 +413,10 @@ class Context:
         return out
 
     def fish_gait(self, k=0):
-        """The gait parameters of curvature swimmer k: (amplitudeFactor, phi,
-        the six scales of StefanFish's curvature control values)."""
+        """The gait parameters of curvature swimmer k: StefanFish's
+        (amplitudeFactor, phi, the six scales of its curvature control
+        values), or the envelope swimmer's eight Fourier coefficients of its
+        curvature amplitude."""
         a = np.zeros(8, dtype=np.float64)
         self._ck(self.L.cup2d_fish_gait_get(self.h_, k, _dp(a)))
         return a

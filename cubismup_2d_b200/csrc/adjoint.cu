@@ -1049,7 +1049,7 @@ int cup2d_adjoint_run(cup2d_ctx* ctx, int nsteps, int every, const cup2d_adjoint
     // frozen dt, and <g, geometry> is summed over the steps
     double theta[CUP2D_GAIT_PARAMS];
     ARC(cup2d_fish_gait_get(ctx, 0, theta));
-    const int np = sf.kind == CUP2D_SHAPE_STEFANFISH ? CUP2D_GAIT_PARAMS : 2;   // the envelope has no nodes
+    const int np = CUP2D_GAIT_PARAMS;
     const double eps = obj->gait_step > 0 ? obj->gait_step : 1e-7;
     for (int q = 0; q < CUP2D_GAIT_PARAMS; q++) grad_gait[q] = 0;
     // one replay: from the first checkpoint, with gait th, on context x

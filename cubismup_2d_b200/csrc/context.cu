@@ -75,7 +75,9 @@ void natural_spline(const double* x, const double* y, int n, const double* xx, d
 
 // The curvature amplitude along the body, sampled at rS: StefanFish's
 // control values (StefanFish.cpp:187-193), each times its scale, splined
-// onto rS; the envelope swimmer's carangiform envelope (cup2d.h).
+// onto rS; the envelope swimmer's carangiform envelope (cup2d.h) times the
+// Fourier series f_0 + sum_{k=1..7} (f_k - 1) cos(k pi s / L) of its
+// coefficients (1 as built: the envelope itself).
 std::vector<double> curvature_profile(const ShapeCfg& f, const std::vector<double>& rS) {
   const int Nm = (int)rS.size();
   const double L = f.length;
@@ -83,7 +85,14 @@ std::vector<double> curvature_profile(const ShapeCfg& f, const std::vector<doubl
   const double base[6] = {0.82014 / L, 1.46515 / L, 2.57136 / L, 3.75425 / L, 5.09147 / L, 5.70449 / L};
   std::vector<double> p1f(Nm);
   if (f.kind == CUP2D_SHAPE_ENVELOPEFISH) {
-    for (int i = 0; i < Nm; i++) p1f[i] = 0.82 * (rS[i] / L + 0.0025) / 1.0025 / L;
+    for (int i = 0; i < Nm; i++) {
+      double m = f.envFourier[0];
+      for (int k = 1; k < 8; k++) {
+        if (f.envFourier[k] == 1) continue;
+        m += (f.envFourier[k] - 1) * std::cos(k * M_PI * rS[i] / L);
+      }
+      p1f[i] = 0.82 * (rS[i] / L + 0.0025) / 1.0025 / L * m;
+    }
   } else {
     double vals[6];
     for (int j = 0; j < 6; j++) vals[j] = base[j] * f.curvScale[j];
@@ -606,6 +615,7 @@ int cup2d_add_shape(cup2d_ctx* ctx, int kind, const cup2d_shape_params* p, int* 
   f.radius = p->radius; f.tAccel = p->tAccel;
   f.length = p->L; f.Tperiod = p->T; f.phaseShift = p->phi; f.ampFac = p->amplitudeFactor;
   for (double& x : f.curvScale) x = 1;
+  for (double& x : f.envFourier) x = 1;
   const bool curvatureFish = kind == CUP2D_SHAPE_STEFANFISH || kind == CUP2D_SHAPE_ENVELOPEFISH;
   f.pid = curvatureFish && p->pid != 0;             // other shapes ignore -pid (StefanFish.cpp:209-211)
   f.pidpos = curvatureFish && p->pidpos != 0;
@@ -1563,7 +1573,7 @@ struct CkptHeader {
   double extent, CFL, lambda, dlm, nu, fadeLen;
   uint64_t checksum;              // ckpt_hash over the sections (0 in the comparison copy)
 };
-constexpr uint32_t CKPT_VERSION = 4;
+constexpr uint32_t CKPT_VERSION = 5;
 
 // The payload checksum: over each section's 8-byte words (the last one
 // zero-padded), the sum modulo 2^64 of SplitMix64 of the word mixed with its
@@ -1911,6 +1921,10 @@ int cup2d_fish_gait_get(cup2d_ctx* ctx, int id, double* theta) {
   int rc = fish_of(ctx, id);
   if (rc) return rc;
   const ShapeCfg& f = ctx->c.hshapes[id].cfg;
+  if (f.kind == CUP2D_SHAPE_ENVELOPEFISH) {
+    for (int j = 0; j < 8; j++) theta[j] = f.envFourier[j];
+    return CUP2D_OK;
+  }
   theta[0] = f.ampFac;
   theta[1] = f.phaseShift;
   for (int j = 0; j < 6; j++) theta[2 + j] = f.curvScale[j];
@@ -1922,15 +1936,16 @@ int cup2d_fish_gait_set(cup2d_ctx* ctx, int id, const double* theta) {
   int rc = fish_of(ctx, id);
   if (rc) return rc;
   Ctx& c = ctx->c;
-  if (c.hshapes[id].cfg.kind != CUP2D_SHAPE_STEFANFISH)
-    for (int j = 0; j < 6; j++)
-      if (theta[2 + j] != 1) return fail(ctx, CUP2D_EINVAL, "the envelope swimmer has no curvature control values");
   if ((rc = quiesce_all(ctx))) return rc;
   CK(cudaMemcpy(&c.hshapes[id], c.dshapes + id, sizeof(DevShape), cudaMemcpyDeviceToHost));
   ShapeCfg& f = c.hshapes[id].cfg;
-  f.ampFac = theta[0];
-  f.phaseShift = theta[1];
-  for (int j = 0; j < 6; j++) f.curvScale[j] = theta[2 + j];
+  if (f.kind == CUP2D_SHAPE_ENVELOPEFISH) {
+    for (int j = 0; j < 8; j++) f.envFourier[j] = theta[j];
+  } else {
+    f.ampFac = theta[0];
+    f.phaseShift = theta[1];
+    for (int j = 0; j < 6; j++) f.curvScale[j] = theta[2 + j];
+  }
   CK(h2d_sync(&c.dshapes[id].cfg, &f, sizeof(ShapeCfg), c.stream));
   const FishArrays& F = c.fish[id];
   std::vector<double> rS(F.nm);

@@ -79,6 +79,7 @@ struct ShapeCfg {
   double radius, tAccel;                          // Disk
   double length, Tperiod, phaseShift, ampFac;     // Fish
   double curvScale[6];                            // StefanFish: scales of its curvature control values
+  double envFourier[8];                           // envelope swimmer: its amplitude's Fourier coefficients
   int capacity;                                   // obstacle tile slots
   int nm;                                         // fish midline points
   int pid, pidpos;                                // StefanFish -pid / -pidpos (StefanFish.cpp:209-211)

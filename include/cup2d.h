@@ -322,8 +322,7 @@ int cup2d_checkpoint_load(cup2d_ctx* ctx, const void* buf, size_t bytes);
  *    target velocity and surface normals on the grid), the geometry's
  *    dependence on theta by central differences of the placement alone
  *    (which the flow does not move for a held body), replayed from the
- *    run's first checkpoint (the envelope swimmer: amplitude and phase
- *    only, the other six 0);
+ *    run's first checkpoint;
  *  - dt_in: the step sizes (nsteps values), or null for calcMaxTimestep's;
  *    dt_out (nsteps values, or null) receives the schedule used.  dt is not
  *    differentiated (a frozen schedule);
@@ -405,12 +404,14 @@ int cup2d_ensemble_destroy(cup2d_ensemble* ens);
  * placement.  Only for StefanFish / envelope swimmers. */
 int cup2d_fish_act(cup2d_ctx* ctx, int id, double t_action, const double* a, int na);
 /* The gait parameters of a curvature swimmer (no counterpart in the
- * reference as one set): theta[0] = amplitudeFactor (the -amplitudeFactor of
- * the shape descriptor), theta[1] = phi (-phi), theta[2..7] = scales of
- * StefanFish's six curvature control values (StefanFish.cpp:187-193; 1 as
- * built; the envelope swimmer has none: they stay 1).  set: between steps;
- * the midline is re-formed from the next placement; a checkpoint loads only
- * into a context of the same gait. */
+ * reference as one set).  StefanFish: theta[0] = amplitudeFactor (the
+ * -amplitudeFactor of the shape descriptor), theta[1] = phi (-phi),
+ * theta[2..7] = scales of its six curvature control values
+ * (StefanFish.cpp:187-193; 1 as built).  The envelope swimmer: the Fourier
+ * coefficients f_0..f_7 of its curvature amplitude, the envelope times
+ * f_0 + sum_{k=1..7} (f_k - 1) cos(k pi s / L) (1 as built: the envelope).
+ * set: between steps; the midline is re-formed from the next placement; a
+ * checkpoint loads only into a context of the same gait. */
 #define CUP2D_GAIT_PARAMS 8
 int cup2d_fish_gait_get(cup2d_ctx* ctx, int id, double* theta);
 int cup2d_fish_gait_set(cup2d_ctx* ctx, int id, const double* theta);
