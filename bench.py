@@ -677,10 +677,34 @@ def run_ours(args, world, rank, local, pg):
     if not args.no_large and args.workload != LARGE_CASE:
         lname, largs = WORKLOADS[LARGE_CASE]
         big = make_sim(largs, local, rank)
+        big32 = None if args.no_fp32 else make_sim(largs + " -precision fp32", local, rank)
+        big.ctx.advance(1)
+        step_large = {}
+        if big32 is not None:
+            big32.ctx.advance(1)
+            pa, pb = big.ctx.get("pres"), big32.ctx.get("pres")
+            step_large["pres_rel_err_1step_fp32"] = float(np.max(np.abs(pb - pa)) / max(np.max(np.abs(pa)), 1e-300))
+            del pa, pb
         big.ctx.advance(3)
         big.ctx.sync()
         roof_large = dense_roofline(big.ctx, peak, peak_kind, LARGE_CASE)
         roof_large["workload"] = lname
+        # the whole graph step at this size, FP64 and with the FP32 Poisson
+        # transforms, timed as the headline's steps (L2 flushed before each)
+        nl = 30
+        ms64, _ = timed_steps(big.ctx, nl, flush, pg)
+        step_large["fp64_ms_per_step"] = max_over_ranks(pg, ms64) / nl
+        if big32 is not None:
+            big32.ctx.advance(3)
+            big32.ctx.sync()
+            ms32, _ = timed_steps(big32.ctx, nl, flush, pg)
+            step_large["fp32_transforms_ms_per_step"] = max_over_ranks(pg, ms32) / nl
+            step_large["fp32_transforms_speedup"] = ms64 / ms32
+            step_large["fp32_transform_ms"] = {k: round(big32.ctx.time_kernel(k, 20, flush_l2=True), 5)
+                                               for k in ("fft_rows_fwd", "fft_cols", "fft_rows_inv")}
+            del big32
+        step_large["steps"] = nl
+        roof_large["step"] = step_large
         if not args.no_cufft:
             roof_large["cufft"] = cufft_comparison(big.ctx, flush)
         del big
