@@ -134,6 +134,28 @@ def test_pressure_stage(ref, args):
     compare_shape(r, s, ["penalM", "penalJ", "fluidMomX", "fluidMomY"], 1e-10, label="momenta")
 
 
+def test_pressure_stage_alone_and_rhs_bitwise(ref):
+    """PressureSingle called without advDiff before it forms its divergence
+    in k_rhs_div (PressureSingle.cpp:112-128): the stage matches the
+    reference's, and in the blocks that neither the obstacle terms nor the
+    fade reach (blocks 4-6 x 1-2 of 8 x 4, the disk in blocks 0-2) the RHS is
+    (h/2dt)((u_E - u_W) + (v_N - v_S)) bit for bit."""
+    args = ("-bpdx 8 -bpdy 4 -extent 1 -CFL 0.1 -nu 1e-3 -lambda 1e4 -poissonType freespace -muteAll 1 "
+            "-shapes 'disk radius=0.05 xpos=0.2 ypos=0.25 bForced=1 bFixed=1 xvel=0.2'")
+    r, s = make_pair(ref, args, noise_seed=13)
+    u, v = s.ctx.get("u"), s.ctx.get("v")
+    dt = 1e-3
+    r.run_op("PressureSingle", dt); s.ctx.pressure_single(dt)
+    compare_fields(r, s, ["tmp"], 1e-12, "rhs")
+    compare_fields(r, s, ["pres"], 1e-10, "pressure")
+    compare_fields(r, s, ["u", "v"], 1e-10, "velocity")
+    fac = 0.5 * s.ctx.h / dt
+    b = fac * ((u[1:-1, 2:] - u[1:-1, :-2]) + (v[2:, 1:-1] - v[:-2, 1:-1]))
+    rhs = s.ctx.get("tmp")[1:-1, 1:-1]
+    rows, cols = slice(32 - 1, 96 - 1), slice(128 - 1, 224 - 1)   # blocks by 1-2, bx 4-6
+    assert np.array_equal(rhs[rows, cols], b[rows, cols])
+
+
 def test_forces_stage(ref):
     r, s = make_pair(ref, DISK, noise_seed=3)
     dt = 1e-3
