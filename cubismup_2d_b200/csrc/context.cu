@@ -1573,7 +1573,7 @@ struct CkptHeader {
   double extent, CFL, lambda, dlm, nu, fadeLen;
   uint64_t checksum;              // ckpt_hash over the sections (0 in the comparison copy)
 };
-constexpr uint32_t CKPT_VERSION = 5;
+constexpr uint32_t CKPT_VERSION = 6;
 
 // The payload checksum: over each section's 8-byte words (the last one
 // zero-padded), the sum modulo 2^64 of SplitMix64 of the word mixed with its

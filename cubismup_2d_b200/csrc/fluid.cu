@@ -152,6 +152,12 @@ k_outflow_flux(GridDesc g, const Scalars* sc, const double* __restrict__ u, cons
   CUP2D_TRACE_SCOPE(TR_ADVDIFF);
   __shared__ double red[32];
   const AdvCoef kc = adv_coef(g, sc);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {            // for the update kernel after this one
+    scw->advCoef[0] = kc.afac; scw->advCoef[1] = kc.dfac;
+    scw->advCoef[2] = kc.fadeW; scw->advCoef[3] = kc.fadeS;
+    scw->advCoef[4] = kc.fadeE; scw->advCoef[5] = kc.fadeN;
+    scw->facDiv = 0.5 * g.h / sc->dt;
+  }
   const int nx = g.nx, ny = g.ny, nitems = 2 * (nx + ny);
   double IF = 0;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nitems; q += gridDim.x * blockDim.x) {
@@ -312,9 +318,15 @@ k_advdiff(const __grid_constant__ CUtensorMap tmU, const __grid_constant__ CUten
     tma_load_2d(tU, &tmU, bx * BS - 2, by * BS - 2, &bar);
     tma_load_2d(tV, &tmV, bx * BS - 2, by * BS - 2, &bar);
   }
-  const AdvCoef kc = adv_coef(g, sc);          // while the tiles are in flight
+  // the step's coefficients, as k_outflow_flux (launched before every
+  // update) formed them, read while the tiles are in flight
+  AdvCoef kc;
+  kc.afac = sc->advCoef[0]; kc.dfac = sc->advCoef[1];
+  kc.fadeW = sc->advCoef[2]; kc.fadeS = sc->advCoef[3];
+  kc.fadeE = sc->advCoef[4]; kc.fadeN = sc->advCoef[5];
+  kc.U0 = sc->uinfx; kc.U1 = sc->uinfy;
   const double corr = sc->outflowCorr;
-  const double facDiv = 0.5 * g.h / sc->dt;
+  const double facDiv = sc->facDiv;
   const int nx = g.nx, ny = g.ny;
   const int gx = bx * BS + tx;
   // one thread waits for the tiles (the others at the CTA barrier, where

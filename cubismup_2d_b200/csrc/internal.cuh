@@ -68,6 +68,10 @@ struct Scalars {
   // run (the step's dt was carried), else the launch after the step's dt does
   int midlineEarly;
   IterState it;                   // iterated penalization (-iterativePenalization)
+  // advDiff's coefficients of the step (afac, dfac, the W, S, E, N inflow
+  // fades) and the RHS factor h/(2 dt), formed once by the outflow-flux
+  // kernel that precedes every advDiff update
+  double advCoef[6], facDiv;
 };
 
 struct ShapeCfg {
