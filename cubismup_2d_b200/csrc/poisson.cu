@@ -130,27 +130,31 @@ constexpr int E_ROWS32 = 8;
 constexpr int E_C2R32 = 8;
 constexpr int E_COLS32 = 16;
 
+constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
+
 // Stages the per-pass tables of fft_inplace<L, ..., E> from the global
-// table tw[j] = exp(-2 pi i j / twLen) (twLen a multiple of 4 L).
+// table tw[j] = exp(-2 pi i j / twLen) (twLen a power of two, a multiple of
+// 4 L): the tables of the pass over sub-transforms of size NS and of every
+// later pass.  Entry t = p NS + k of a pass of radix R holds
+// W^(k 2^p) = tw[(k 2^p) twLen / (R NS)]; the passes' sizes are
+// compile-time powers of two, so every index is a shift.
+template <int L, int E, int NS, class C>
+__device__ __forceinline__ void load_twiddles_from(C* tws, const C* __restrict__ tw, int twShift) {
+  if constexpr (NS < L) {
+    constexpr int R = NS * E <= L ? E : L / NS;
+    if constexpr (NS > 1) {
+      constexpr int n = tw_npow(R) * NS, off = tw_off<L, E>(NS), sh = ilog2(R * NS);
+      for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int p = t / NS, k = t - p * NS;
+        tws[off + t] = tw[(size_t)(k << p) << (twShift - sh)];
+      }
+    }
+    load_twiddles_from<L, E, NS * R>(tws, tw, twShift);
+  }
+}
 template <int L, int E, class C>
 __device__ __forceinline__ void load_twiddles(C* tws, const C* __restrict__ tw, int twLen) {
-  constexpr int total = tw_size<L, E>();
-  for (int i = threadIdx.x; i < total; i += blockDim.x) {
-    int ns = 1, off = 0;
-    while (ns < L) {
-      const int r = ns * E <= L ? E : L / ns;
-      if (ns > 1) {
-        const int n = tw_npow(r) * ns;
-        if (i < off + n) {
-          const int t = i - off, pi = t / ns, k = t - pi * ns;
-          tws[i] = tw[(size_t)(k << pi) * (size_t)(twLen / (r * ns))];
-          break;
-        }
-        off += n;
-      }
-      ns *= r;
-    }
-  }
+  load_twiddles_from<L, E, 1>(tws, tw, __ffs(twLen) - 1);
 }
 
 // Scales xb[m], 0 < m < R, of the butterfly k of the pass over
@@ -488,6 +492,7 @@ struct FadeArgs {
   double* writeback;     // rhs buffer receives the faded values (cub2rhs writes tmp)
   const double* partials;   // fade sums of the strip blocks, three each
   int nstrip;
+  int bandX, bandY;         // cells of the fade band from each edge, (int)(fadeLen / h) + 2 (host-formed)
 };
 
 // fadeCorr for this CTA, formed by warp 0 (blockDim.x >= 32) into *s;
@@ -564,8 +569,8 @@ k_rows_r2c(const double* in, int inStride, int nrows, int ncolsIn, int inMode,
     load_twiddles<L, ER>(tws, tw, twLen);
     __syncthreads();
     const double corr = fa.enabled ? sCorr0 : 0.0;
-    const int bandX = fa.enabled ? (int)(fa.g.fadeLenX / fa.g.h) + 2 : 0;
-    const int bandY = fa.enabled ? (int)(fa.g.fadeLenY / fa.g.h) + 2 : 0;
+    const int bandX = fa.enabled ? fa.bandX : 0;
+    const int bandY = fa.enabled ? fa.bandY : 0;
     auto ld = [&](int r, int n) {
       const int row = row0 + r;
       const double* src = in + (size_t)row * inStride + 2 * n;
@@ -796,8 +801,8 @@ k_rows_r2c32(const double* __restrict__ in, int inStride, int nrows, int ncolsIn
   load_twiddles<L, E_ROWS32>(tws, tw, twLen);
   __syncthreads();
   const double corr = fa.enabled ? sCorr : 0.0;
-  const int bandX = fa.enabled ? (int)(fa.g.fadeLenX / fa.g.h) + 2 : 0;
-  const int bandY = fa.enabled ? (int)(fa.g.fadeLenY / fa.g.h) + 2 : 0;
+  const int bandX = fa.enabled ? fa.bandX : 0;
+  const int bandY = fa.enabled ? fa.bandY : 0;
 #pragma unroll
   for (int u = 0; u < PER; u++) {
     const int idx = threadIdx.x + u * NT;
@@ -978,8 +983,8 @@ k_dct_rows_fwd(const double* in, int Nx, int nrows, double* __restrict__ D, int 
   const int nb = min(rb, nrows - row0);
   __syncthreads();
   const double corr = fa.enabled ? sCorr : 0.0;
-  const int bandX = fa.enabled ? (int)(fa.g.fadeLenX / fa.g.h) + 2 : 0;
-  const int bandY = fa.enabled ? (int)(fa.g.fadeLenY / fa.g.h) + 2 : 0;
+  const int bandX = fa.enabled ? fa.bandX : 0;
+  const int bandY = fa.enabled ? fa.bandY : 0;
   // faded row values, then the even extension y[j] = x[j] (j < n), x[2n-1-j]
   for (int idx = threadIdx.x; idx < nb * L; idx += blockDim.x) {
     const int r = idx / L, col = idx - r * L, row = row0 + r;
@@ -1432,7 +1437,8 @@ void poisson_destroy(Poisson* P) {
 void poisson_rows_fwd(Ctx& c) {
   Poisson* P = c.poisson;
   const int Nx = c.g.nx, Ny = c.g.ny;
-  FadeArgs fa{c.solveNoFade ? 0 : 1, c.dsc, c.g, c.rhs, fade_partials(c), c.nfade};
+  FadeArgs fa{c.solveNoFade ? 0 : 1, c.dsc, c.g, c.rhs, fade_partials(c), c.nfade,
+              (int)(c.g.fadeLenX / c.g.h) + 2, (int)(c.g.fadeLenY / c.g.h) + 2};
   if (P->type == CUP2D_POISSON_COSINE) {
     dct_rows_fwd(P->Lrow, c.stream, c.rhs, Nx, Ny, reinterpret_cast<double*>(P->spec), P->tw, P->twLen, fa);
     CUP2D_LAUNCHED(c);
