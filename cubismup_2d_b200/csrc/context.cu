@@ -2,6 +2,8 @@
 // in Simulation::advance order, CUDA-graph replay of whole steps, and state
 // exchange.  No entry point aborts: failures come back as status codes.
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
@@ -509,6 +511,7 @@ int cup2d_create(const cup2d_config* cfg, cup2d_ctx** out) {
   if (!rc && fish_setup_kernels() != cudaSuccess)
     rc = fail(ctx, CUP2D_ECUDA, "shared-memory limits of the fish kernels could not be set");
   if (rc) { cup2d_destroy(ctx); return rc; }
+  std::memset(c.map, 0, sizeof(Ctx::HostMapped));     // the signal words start below every launch's value
   if (cudaMemsetAsync(c.counters, 0, sizeof(unsigned) * Ctx::NCOUNTERS, c.stream) != cudaSuccess ||
       cudaStreamSynchronize(c.stream) != cudaSuccess) { cup2d_destroy(ctx); return CUP2D_ECUDA; }
   c.poisson = poisson_create(c);
@@ -791,6 +794,24 @@ int cup2d_iteration_stats(cup2d_ctx* ctx, int* iterations, double* rel_df) {
   return CUP2D_OK;
 }
 
+// Waits for a kernel's signal in mapped host memory: the word reaches want
+// (the kernel wrote its data first, behind a system-scope fence).  Spins on
+// the word for up to 20 ms -- waking on it costs less than on the event --
+// then waits on the event recorded after that kernel, which also reports
+// an error of the stream (a kernel that never signals ends up there).
+static cudaError_t wait_mapped(const unsigned long long* word, unsigned long long want, cudaEvent_t ev) {
+  const volatile unsigned long long* w = word;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (unsigned it = 0;; it++) {
+    if (*w >= want) {
+      std::atomic_thread_fence(std::memory_order_acquire);
+      return cudaSuccess;
+    }
+    if ((it & 255) == 255 && std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(20)) break;
+  }
+  return cudaEventSynchronize(ev);
+}
+
 int cup2d_calc_dt(cup2d_ctx* ctx, double* dt_out) {
   if (!ctx || !ctx->c.initialised) return ctx ? fail(ctx, CUP2D_ESTATE, "not initialised") : CUP2D_EINVAL;
   Ctx& c = ctx->c;
@@ -803,7 +824,7 @@ int cup2d_calc_dt(cup2d_ctx* ctx, double* dt_out) {
     if (rc) return rc;
     c.devDt = NAN;
     if (dt_out) {
-      CK(cudaEventSynchronize(c.evDtNext));
+      CK(wait_mapped(&c.map->seqDt, c.mapSeqDt, c.evDtNext));
       *dt_out = c.devDt = *(volatile const double*)&c.map->dtNext;
     }
     return CUP2D_OK;
@@ -979,7 +1000,8 @@ int cup2d_compute_forces(cup2d_ctx* ctx, double dt) {
   STAGE_PROLOGUE
   const bool maxNext = c.maxNextState == 2;  // after this step's pressure correction
   forget_chain(c);
-  launch_forces(c, c.mapDev->shapes, maxNext);   // the final states also to mapped host memory
+  c.mapSeqForces = ++c.mapSeq;
+  launch_forces(c, c.mapDev->shapes, maxNext, c.mapDev->seqShape, c.mapSeqForces);   // the final states also to mapped host memory
   c.maxNextState = maxNext ? 3 : 0;
   CK(cudaEventRecord(c.evForces, c.stream));
   c.shapesMapped = true;
@@ -1003,8 +1025,10 @@ int cup2d_end_step(cup2d_ctx* ctx) {
   // nothing from here on writes the shape states
   CK(cudaEventRecord(c.evShapes, c.stream));
   c.shapesAtEvent = true;
-  if (fused) launch_end_step_dt(c, &c.mapDev->dtNext);   // the next dt also to mapped host memory
-  else launch_end_step_max(c, &c.mapDev->dtNext);
+  c.mapSeqDt = ++c.mapSeq;
+  // the next dt also to mapped host memory
+  if (fused) launch_end_step_dt(c, &c.mapDev->dtNext, &c.mapDev->seqDt, c.mapSeqDt);
+  else launch_end_step_max(c, &c.mapDev->dtNext, &c.mapDev->seqDt, c.mapSeqDt);
   CK(cudaEventRecord(c.evDtNext, c.stream));
   c.dtValidMaybe = c.dtCarried = true;
   return check_launch(ctx);
@@ -1153,7 +1177,7 @@ int cup2d_get_shape(cup2d_ctx* ctx, int id, cup2d_shape_state* out) {
   if (id < 0 || id >= c.nshapes) return fail(ctx, CUP2D_EINVAL, "bad shape id");
   if (c.shapesMapped) {
     // written to mapped host memory by the force pass, the last writer
-    CK(cudaEventSynchronize(c.evForces));
+    CK(wait_mapped(&c.map->seqShape[id], c.mapSeqForces, c.evForces));
     const volatile double* src = reinterpret_cast<const volatile double*>(&c.map->shapes[id]);
     double* dst = reinterpret_cast<double*>(&c.hshapes[id].s);
     for (size_t q = 0; q < sizeof(cup2d_shape_state) / sizeof(double); q++) dst[q] = src[q];

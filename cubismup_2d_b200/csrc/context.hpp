@@ -116,7 +116,14 @@ struct Ctx {
   // mapped pinned memory the operator path's kernels write directly (no copy
   // engine): the next dt (step end) and each shape's final state (force
   // pass).  shapesMapped: map->shapes is current once evForces completes.
-  struct HostMapped { double dtNext; cup2d_shape_state shapes[MAX_SHAPES]; };
+  // seqDt / seqShape[k]: written by the step end / the force pass after
+  // dtNext / shapes[k] (behind a system-scope fence) with the value of
+  // mapSeq at that launch; the host spins on them (wait_mapped)
+  struct HostMapped {
+    double dtNext;
+    cup2d_shape_state shapes[MAX_SHAPES];
+    unsigned long long seqDt, seqShape[MAX_SHAPES];
+  };
   HostMapped* map = nullptr;      // host address
   HostMapped* mapDev = nullptr;   // its device address
   cudaEvent_t evForces = nullptr;
@@ -127,6 +134,9 @@ struct Ctx {
   // bumped by every call that may change the state; an ensemble compares it
   // with the value after its own advance to know a member's read-back is current
   unsigned long long stateSeq = 0;
+  // launches that signal the host through HostMapped, counted; the values
+  // the last step end and the last force pass were given
+  unsigned long long mapSeq = 0, mapSeqDt = 0, mapSeqForces = 0;
 
   // the Poisson solve of the adjoint: the convolution alone, without
   // cub2rhs's fade (the adjoint applies the fade's transpose itself)

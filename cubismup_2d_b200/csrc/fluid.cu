@@ -36,7 +36,8 @@ __global__ void k_set_dt(Scalars* sc, double dt) { pdl_begin(); CUP2D_TRACE_SCOP
 // End of a step (Simulation.cpp:289-290): t += dt, step += 1, then the next step's
 // calcMaxTimestep from the maximum k_pcorr<true> and k_forces formed on the final velocity
 // (max is exact in any order: dtNext equals what k_max_u_dt would form).
-__global__ void k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh, double* dtOut)
+__global__ void k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int nsh, double* dtOut,
+                              unsigned long long* seqOut, unsigned long long seqVal)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_ENDSTEP);
@@ -48,6 +49,7 @@ __global__ void k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int n
   sc->maxUNext = m;
   sc->dtNextValid = 1;
   if (dtOut) *dtOut = dtn;                    // to mapped host memory
+  signal_host(seqOut, seqVal);
 }
 
 // End of an operator-by-operator step: findMaxU on the final velocity (its
@@ -55,7 +57,8 @@ __global__ void k_end_step_dt(GridDesc g, Scalars* sc, const DevShape* sh, int n
 // a graph step's findMaxU parts and k_end_step_dt in one launch.
 __global__ void __launch_bounds__(512)
 k_end_step_max(GridDesc g, Scalars* sc, const DevShape* sh, int nsh, const double* __restrict__ u,
-               const double* __restrict__ v, double* partials, unsigned* counter, double* dtOut)
+               const double* __restrict__ v, double* partials, unsigned* counter, double* dtOut,
+               unsigned long long* seqOut, unsigned long long seqVal)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_ENDSTEP);
@@ -69,6 +72,7 @@ k_end_step_max(GridDesc g, Scalars* sc, const DevShape* sh, int nsh, const doubl
   sc->maxUNext = m;
   sc->dtNextValid = 1;
   if (dtOut) *dtOut = dtn;                    // to mapped host memory
+  signal_host(seqOut, seqVal);
 }
 
 // calcMaxTimestep of a state whose dt the last step end already formed
@@ -581,9 +585,9 @@ void launch_set_dt(Ctx& c, double dt) {
   CUP2D_LAUNCHED(c);
 }
 
-void launch_end_step_max(Ctx& c, double* dtOut) {
+void launch_end_step_max(Ctx& c, double* dtOut, unsigned long long* seqOut, unsigned long long seqVal) {
   launch_k(k_end_step_max, max_grid(c), 512, 0, c.stream, c.g, c.dsc, (const DevShape*)c.dshapes, c.nshapes,
-           (const double*)c.u(), (const double*)c.v(), c.partials, c.counters + CNT_MAXU, dtOut);
+           (const double*)c.u(), (const double*)c.v(), c.partials, c.counters + CNT_MAXU, dtOut, seqOut, seqVal);
   CUP2D_LAUNCHED(c);
 }
 
@@ -592,8 +596,9 @@ void launch_take_dt_next(Ctx& c) {
   CUP2D_LAUNCHED(c);
 }
 
-void launch_end_step_dt(Ctx& c, double* dtOut) {
-  launch_k(k_end_step_dt, 1, 1, 0, c.stream, c.g, c.dsc, (const DevShape*)c.dshapes, c.nshapes, dtOut);
+void launch_end_step_dt(Ctx& c, double* dtOut, unsigned long long* seqOut, unsigned long long seqVal) {
+  launch_k(k_end_step_dt, 1, 1, 0, c.stream, c.g, c.dsc, (const DevShape*)c.dshapes, c.nshapes, dtOut,
+           seqOut, seqVal);
   CUP2D_LAUNCHED(c);
 }
 

@@ -446,6 +446,15 @@ __device__ __forceinline__ double gy_pos(const GridDesc& g, int gy) {
 // threads, thread (tx, ty) adds rows ty + 8r, r = 0..3, then block_sum<3>
 // over the CTA (further warps adding zeros), so the sums are the same
 // whichever kernel wrote them last.
+// A kernel's last word to mapped host memory: everything it wrote before
+// becomes visible to the host first (system-scope fence), then the host's
+// spin word takes seqVal.
+__device__ __forceinline__ void signal_host(unsigned long long* seqOut, unsigned long long seqVal) {
+  if (!seqOut) return;
+  __threadfence_system();
+  *reinterpret_cast<volatile unsigned long long*>(seqOut) = seqVal;
+}
+
 __device__ __forceinline__ bool fade_touch(const GridDesc& g, int bx, int by) {
   const double minx = cell_x(g, bx, 0), maxx = cell_x(g, bx, BS - 1);
   const double miny = cell_y(g, by, 0), maxy = cell_y(g, by, BS - 1);

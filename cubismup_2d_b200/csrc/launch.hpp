@@ -48,10 +48,14 @@ int build_fade_slots(Ctx& c);                        // PoissonSolver.cpp:71-79,
 void launch_pcorr(Ctx& c, bool maxNext = false);
 // Simulation.cpp:289-290 + the next step's calcMaxTimestep from sc->maxNext
 // (also to dtOut: mapped host memory, or null)
-void launch_end_step_dt(Ctx& c, double* dtOut = nullptr);
+// dtOut (mapped host memory): the next dt; then seqOut = seqVal behind a
+// system-scope fence, the word the host spins on
+void launch_end_step_dt(Ctx& c, double* dtOut = nullptr, unsigned long long* seqOut = nullptr,
+                        unsigned long long seqVal = 0);
 void launch_take_dt_next(Ctx& c);                    // calcMaxTimestep from the carried dt
 // findMaxU + Simulation.cpp:289-290 + the next dt (also to dtOut: mapped host memory, or null)
-void launch_end_step_max(Ctx& c, double* dtOut = nullptr);
+void launch_end_step_max(Ctx& c, double* dtOut = nullptr, unsigned long long* seqOut = nullptr,
+                         unsigned long long seqVal = 0);
 void launch_ic(Ctx& c);                              // Helpers.cpp:38-82
 void launch_apply_obj_vel(Ctx& c);                   // Helpers.cpp:290-307
 
@@ -82,7 +86,10 @@ void launch_reldf(Ctx& c, const PenalCtas& nc);
 void launch_collide_penalize(Ctx& c);                // PressureSingle.cpp:69-108, 243-344
 // ComputeForces.cpp:16-111; out (mapped host memory, or null): each shape's final state
 // maxNext: with the next step's findMaxU over the shapes' tiles
-void launch_forces(Ctx& c, cup2d_shape_state* out, bool maxNext);
+// out (mapped host memory, or null): each shape's final state; then
+// seqOut[k] = seqVal behind a system-scope fence
+void launch_forces(Ctx& c, cup2d_shape_state* out, bool maxNext, unsigned long long* seqOut = nullptr,
+                   unsigned long long seqVal = 0);
 
 // poisson.cu
 struct Poisson;

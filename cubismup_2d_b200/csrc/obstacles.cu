@@ -605,7 +605,8 @@ k_penalize(GridDesc g, const Scalars* sc, const DevShape* sh, int k, ObstTiles t
 __global__ void __launch_bounds__(1024)
 k_forces(GridDesc g, Scalars* sc, int maxNext, DevShape* sh, AllTiles T, const double* __restrict__ u,
          const double* __restrict__ v, const double* __restrict__ p,
-         double* partials, int partStride, unsigned* counters, cup2d_shape_state* out)
+         double* partials, int partStride, unsigned* counters, cup2d_shape_state* out,
+         unsigned long long* seqOut, unsigned long long seqVal)
 {
   pdl_begin();
   CUP2D_TRACE_SCOPE(TR_FORCES);
@@ -708,6 +709,7 @@ k_forces(GridDesc g, Scalars* sc, int maxNext, DevShape* sh, AllTiles T, const d
   st.EffPDef = st.Pthrust / fmax(denUnb, EPSd);
   st.EffPDefBnd = st.Pthrust / fmax(demBnd, EPSd);
   if (out) out[k] = st;                       // the final state, to mapped host memory
+  signal_host(seqOut ? seqOut + k : nullptr, seqVal);
 }
 
 
@@ -871,12 +873,14 @@ void launch_collide_penalize(Ctx& c) {
   }
 }
 
-void launch_forces(Ctx& c, cup2d_shape_state* out, bool maxNext) {
+void launch_forces(Ctx& c, cup2d_shape_state* out, bool maxNext, unsigned long long* seqOut,
+                   unsigned long long seqVal) {
   if (c.nshapes == 0) return;
   const AllTiles T = all_tiles(c);
   launch_k(k_forces, dim3(tile_ctas(c, c.maxCapacity), c.nshapes), dim3(32, 32), 0, c.stream,
       c.g, c.dsc, maxNext ? 1 : 0, c.dshapes, T, (const double*)c.u(), (const double*)c.v(),
-      (const double*)c.pres, shape_partials(c), (int)shape_region(c), c.counters + CNT_FORCES, out);
+      (const double*)c.pres, shape_partials(c), (int)shape_region(c), c.counters + CNT_FORCES, out,
+      seqOut, seqVal);
   CUP2D_LAUNCHED(c);
 }
 
