@@ -181,7 +181,10 @@ int cup2d_tuning_get(cup2d_ctx* ctx, cup2d_tuning* out);
 
 /* Simulation::calcMaxTimestep (Simulation.cpp:254-277) incl. findMaxU
  * (Helpers.cpp:136-176).  dt stays on the device; if dt_out is non-NULL the
- * call synchronises and returns it. */
+ * call synchronises and returns it.  After cup2d_end_step the dt is already
+ * formed: the call then waits for it by spinning on a word the step end
+ * writes to mapped host memory (one host thread busy for up to 20 ms), and
+ * only then on the stream's event. */
 int cup2d_calc_dt(cup2d_ctx* ctx, double* dt_out);
 /* One Operator::operator()(dt) each.  dt < 0 means "use the device dt from
  * cup2d_calc_dt"; dt >= 0 overrides it, as the reference's argument does.  */
@@ -227,6 +230,9 @@ int cup2d_sync(cup2d_ctx* ctx);
 /* ---- state exchange --------------------------------------------------- */
 int cup2d_get_field(cup2d_ctx* ctx, int which, double* host_out);
 int cup2d_set_field(cup2d_ctx* ctx, int which, const double* host_in);
+/* After cup2d_compute_forces the force pass writes the final state to
+ * mapped host memory and then a sequence word; cup2d_get_shape spins on that
+ * word (up to 20 ms) before it waits on the stream's event. */
 int cup2d_get_shape(cup2d_ctx* ctx, int id, cup2d_shape_state* out);
 int cup2d_set_shape(cup2d_ctx* ctx, int id, const cup2d_shape_state* in);
 /* time, dt, step, uinf (SimulationData.h:45-49) */
