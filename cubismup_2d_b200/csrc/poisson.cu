@@ -525,22 +525,38 @@ __device__ __forceinline__ double fade_cell(const GridDesc& g, int gx, int gy, d
 
 // Real FFT of length 2L from the complex FFT Z of length L of its value
 // pairs, even/odd split: X[k] = Fe[k] + W^k Fo[k], W = exp(-i pi / L),
-// k in [0, L]; written to row row0 + r of out.
-template <int L, int ER>
-__device__ __forceinline__ void r2c_split(const double2* A, int nb, int row0, double2* __restrict__ out,
-                                          int outStride, const double2* __restrict__ tw, int twLen)
+// k in [0, L]; written to row row0 + r of out.  Thread t takes k = t + q NT
+// of every row; its twiddles are read first, all in flight at once (read
+// inside the loop, every iteration waited for its own).
+template <int L, int ER, class C>
+__device__ __forceinline__ void r2c_split(const C* A, int nb, int row0, C* __restrict__ out,
+                                          int outStride, const C* __restrict__ tw, int twLen)
 {
-  constexpr int SL = Len<L, ER>::SL, NT = Len<L, ER>::NT;
+  using R = typename CT<C>::R;
+  constexpr int SL = Len<L, ER>::SL, NT = Len<L, ER>::NT, KPT = (L + 1 + NT - 1) / NT;
+  constexpr int KB = KPT < 8 ? KPT : 8;                 // twiddles in flight per batch
   const int twStep = twLen / (2 * L);
-  for (int idx = threadIdx.x; idx < nb * (L + 1); idx += NT) {
-    const int r = idx / (L + 1), k = idx - r * (L + 1);
-    const double2 Zk = A[r * SL + pad(k == L ? 0 : k)];
-    const double2 Zc = conjg(A[r * SL + pad(k == 0 ? 0 : L - k)]);
-    const double2 Fe = make_double2(0.5 * (Zk.x + Zc.x), 0.5 * (Zk.y + Zc.y));
-    const double2 d = csub(Zk, Zc);
-    const double2 Fo = make_double2(0.5 * d.y, -0.5 * d.x);   // (Zk - Zc) / (2i)
-    const double2 X = cadd(Fe, cmul(tw[k * twStep], Fo));
-    out[(size_t)(row0 + r) * outStride + k] = X;
+#pragma unroll
+  for (int q0 = 0; q0 < KPT; q0 += KB) {
+    C w[KB];
+#pragma unroll
+    for (int q = 0; q < KB; q++) {
+      const int k = threadIdx.x + (q0 + q) * NT;
+      w[q] = q0 + q < KPT && k <= L ? tw[k * twStep] : mk<C>(0, 0);
+    }
+#pragma unroll
+    for (int q = 0; q < KB; q++) {
+      const int k = threadIdx.x + (q0 + q) * NT;
+      if (q0 + q >= KPT || k > L) break;                // k grows with q
+      for (int r = 0; r < nb; r++) {
+        const C Zk = A[r * SL + pad(k == L ? 0 : k)];
+        const C Zc = conjg(A[r * SL + pad(k == 0 ? 0 : L - k)]);
+        const C Fe = mk<C>(R(0.5) * (Zk.x + Zc.x), R(0.5) * (Zk.y + Zc.y));
+        const C d = csub(Zk, Zc);
+        const C Fo = mk<C>(R(0.5) * d.y, R(-0.5) * d.x);  // (Zk - Zc) / (2i)
+        out[(size_t)(row0 + r) * outStride + k] = cadd(Fe, cmul(w[q], Fo));
+      }
+    }
   }
 }
 
@@ -728,32 +744,47 @@ k_rows_c2r(const double2* __restrict__ in, int inStride, int nrows, double* __re
   }
   cp_async_commit();
   load_twiddles<L, EC>(tws, tw, twLen);
+  // the split's W^-k of the pairs (k, L - k) this thread forms, read while
+  // the rows land
+  constexpr int KPT = (H + NT - 1) / NT;
+  double2 wk[KPT][2];
+#pragma unroll
+  for (int q = 0; q < KPT; q++) {
+    const int k = threadIdx.x + q * NT;
+    if (k < H) {
+      wk[q][0] = conjg(tw[k * twStep]);
+      wk[q][1] = conjg(tw[(k == 0 ? H : L - k) * twStep]);
+    }
+  }
   cp_async_wait<0>();
   __syncthreads();
   // z[k] = s + i t, s = X_k + conj(X_{L-k}), t = W^-k (X_k - conj(X_{L-k})):
-  // thread (r, k), k < L/2, forms the pair k, L-k in place; k = 0 also L/2
-  for (int idx = threadIdx.x; idx < RB * H; idx += NT) {
-    const int r = idx / H, k = idx & (H - 1);
-    if (r >= nb) continue;
-    double2* a = A + r * SL;
+  // thread (k, r), k < L/2, forms the pair k, L-k of every row in place;
+  // k = 0 also L/2
+#pragma unroll
+  for (int q = 0; q < KPT; q++) {
+    const int k = threadIdx.x + q * NT;
+    if (k >= H) continue;
     const int kk[2] = {k, k == 0 ? H : L - k};
-    double2 Xa = a[pad(k)], Xb = a[pad(k == 0 ? L : L - k)];
-    if (k == 0) { Xa.y = 0; Xb.y = 0; }         // c2r ignores Im X[0], Im X[L]
-    double2 res[2];
-    for (int e = 0; e < 2; e++) {
-      const int kq = kk[e];
-      double2 Xk, XL;
-      if (e == 0) { Xk = Xa; XL = Xb; }
-      else if (k == 0) { Xk = a[pad(H)]; XL = Xk; }
-      else { Xk = Xb; XL = Xa; }
-      const double2 Xc = conjg(XL);
-      const double2 sv = cadd(Xk, Xc), d = csub(Xk, Xc);
-      const double2 wi = conjg(tw[kq * twStep]);   // W^-k
-      const double2 t = cmul(wi, d);
-      res[e] = make_double2(sv.x - t.y, sv.y + t.x);
+    for (int r = 0; r < nb; r++) {
+      double2* a = A + r * SL;
+      double2 Xa = a[pad(k)], Xb = a[pad(k == 0 ? L : L - k)];
+      if (k == 0) { Xa.y = 0; Xb.y = 0; }         // c2r ignores Im X[0], Im X[L]
+      double2 res[2];
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        double2 Xk, XL;
+        if (e == 0) { Xk = Xa; XL = Xb; }
+        else if (k == 0) { Xk = a[pad(H)]; XL = Xk; }
+        else { Xk = Xb; XL = Xa; }
+        const double2 Xc = conjg(XL);
+        const double2 sv = cadd(Xk, Xc), d = csub(Xk, Xc);
+        const double2 t = cmul(wk[q][e], d);
+        res[e] = make_double2(sv.x - t.y, sv.y + t.x);
+      }
+      a[pad(kk[0])] = res[0];
+      a[pad(kk[1])] = res[1];
     }
-    a[pad(kk[0])] = res[0];
-    a[pad(kk[1])] = res[1];
   }
   __syncthreads();
   // the inverse FFT; its last pass writes the value pairs of the row
@@ -825,17 +856,7 @@ k_rows_r2c32(const double* __restrict__ in, int inStride, int nrows, int ncolsIn
   }
   __syncthreads();
   fft_inplace<L, false, HIN, false, E_ROWS32>(A, nb, tws);
-  // even/odd split: X[k] = Fe[k] + W^k Fo[k], W = exp(-i pi / L), k in [0, L]
-  const int twStep = twLen / (2 * L);
-  for (int idx = threadIdx.x; idx < nb * (L + 1); idx += NT) {
-    const int r = idx / (L + 1), k = idx - r * (L + 1);
-    const float2 Zk = A[r * SL + pad(k == L ? 0 : k)];
-    const float2 Zc = conjg(A[r * SL + pad(k == 0 ? 0 : L - k)]);
-    const float2 Fe = make_float2(0.5f * (Zk.x + Zc.x), 0.5f * (Zk.y + Zc.y));
-    const float2 d = csub(Zk, Zc);
-    const float2 Fo = make_float2(0.5f * d.y, -0.5f * d.x);
-    out[(size_t)(row0 + r) * outStride + k] = cadd(Fe, cmul(tw[k * twStep], Fo));
-  }
+  r2c_split<L, E_ROWS32>(A, nb, row0, out, outStride, tw, twLen);
 }
 
 // mode 0: forward, x G^, inverse, keep nrowsOut rows; mode 2: the periodic
@@ -920,29 +941,44 @@ k_rows_c2r32(const float2* __restrict__ in, int inStride, int nrows, double* __r
   }
   cp_async_commit();
   load_twiddles<L, E_C2R32>(tws, tw, twLen);
+  // the split's W^-k of the pairs (k, L - k) this thread forms, read while
+  // the rows land (as in k_rows_c2r)
+  constexpr int KPT = (H + NT - 1) / NT;
+  float2 wk[KPT][2];
+#pragma unroll
+  for (int q = 0; q < KPT; q++) {
+    const int k = threadIdx.x + q * NT;
+    if (k < H) {
+      wk[q][0] = conjg(tw[k * twStep]);
+      wk[q][1] = conjg(tw[(k == 0 ? H : L - k) * twStep]);
+    }
+  }
   cp_async_wait<0>();
   __syncthreads();
-  for (int idx = threadIdx.x; idx < RB * H; idx += NT) {
-    const int r = idx / H, k = idx & (H - 1);
-    if (r >= nb) continue;
-    float2* a = A + r * SL;
+#pragma unroll
+  for (int q = 0; q < KPT; q++) {
+    const int k = threadIdx.x + q * NT;
+    if (k >= H) continue;
     const int kk[2] = {k, k == 0 ? H : L - k};
-    float2 Xa = a[pad(k)], Xb = a[pad(k == 0 ? L : L - k)];
-    if (k == 0) { Xa.y = 0; Xb.y = 0; }
-    float2 res[2];
-    for (int e = 0; e < 2; e++) {
-      const int kq = kk[e];
-      float2 Xk, XL;
-      if (e == 0) { Xk = Xa; XL = Xb; }
-      else if (k == 0) { Xk = a[pad(H)]; XL = Xk; }
-      else { Xk = Xb; XL = Xa; }
-      const float2 Xc = conjg(XL);
-      const float2 sv = cadd(Xk, Xc), d = csub(Xk, Xc);
-      const float2 t = cmul(conjg(tw[kq * twStep]), d);
-      res[e] = make_float2(sv.x - t.y, sv.y + t.x);
+    for (int r = 0; r < nb; r++) {
+      float2* a = A + r * SL;
+      float2 Xa = a[pad(k)], Xb = a[pad(k == 0 ? L : L - k)];
+      if (k == 0) { Xa.y = 0; Xb.y = 0; }
+      float2 res[2];
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        float2 Xk, XL;
+        if (e == 0) { Xk = Xa; XL = Xb; }
+        else if (k == 0) { Xk = a[pad(H)]; XL = Xk; }
+        else { Xk = Xb; XL = Xa; }
+        const float2 Xc = conjg(XL);
+        const float2 sv = cadd(Xk, Xc), d = csub(Xk, Xc);
+        const float2 t = cmul(wk[q][e], d);
+        res[e] = make_float2(sv.x - t.y, sv.y + t.x);
+      }
+      a[pad(kk[0])] = res[0];
+      a[pad(kk[1])] = res[1];
     }
-    a[pad(kk[0])] = res[0];
-    a[pad(kk[1])] = res[1];
   }
   __syncthreads();
   fft_inplace<L, true, false, HOUT, E_C2R32>(A, nb, tws);
