@@ -1043,6 +1043,8 @@ k_dct_rows_fwd(const double* in, int Nx, int nrows, double* __restrict__ D, int 
   fft_inplace<L, false>(A, nb, tws);
   double2* Z = A;
   const int st2 = twLen / (2 * L), st4 = twLen / (4 * L);
+  // four iterations' global loads in flight before the first store
+#pragma unroll 4
   for (int idx = threadIdx.x; idx < nb * L; idx += blockDim.x) {
     const int r = idx / L, k = idx - r * L;
     const double2 Zk = Z[r * SL + pad(k)];
@@ -1091,6 +1093,7 @@ k_dct_cols(double* D, int Nx, int Ny, int cb, const float* __restrict__ cosX, co
   const double norm_factor = 0.25 / (MX * MY);
   // separate the two real columns, DCT-II values, multiplier, then the
   // Hermitian spectra of both DCT-III inputs packed as Za + i Zb
+#pragma unroll 4
   for (int idx = threadIdx.x; idx < np * n; idx += blockDim.x) {
     const int q = idx / n, k = idx - q * n;
     const double2 Zk = Z[q * SL + pad(k)];
@@ -1122,6 +1125,7 @@ k_dct_cols(double* D, int Nx, int Ny, int cb, const float* __restrict__ cosX, co
   __syncthreads();
   fft_inplace<L, true, false, true>(W, np, tws);          // outputs m < n = L/2
   double2* Y = W;
+#pragma unroll 4
   for (int idx = threadIdx.x; idx < np * n; idx += blockDim.x) {
     const int m = idx / np, q = idx - m * np;
     *reinterpret_cast<double2*>(D + (size_t)m * Nx + c0 + 2 * q) = Y[q * SL + pad(m)];
@@ -1144,6 +1148,8 @@ k_dct_rows_inv(const double* __restrict__ D, int Nx, int nrows, double* __restri
   const int row0 = blockIdx.x * rb;
   const int nb = min(rb, nrows - row0);
   const int st2 = twLen / (2 * L), st4 = twLen / (4 * L);
+  // four iterations' global loads in flight before the first store
+#pragma unroll 4
   for (int idx = threadIdx.x; idx < nb * L; idx += blockDim.x) {
     const int r = idx / L, k = idx - r * L;
     const double* Yr = D + (size_t)(row0 + r) * Nx;
